@@ -1,0 +1,246 @@
+/*
+ * twofold_b200 — C ABI of the B200 contact pipeline behind twofold::World::step.
+ *
+ * One tf_world holds one or more independent worlds ("a batch"). A plain world is a batch of one.
+ * Every world has its own body and shape index spaces, numbered from 0 in creation order with freed
+ * slots reused under a bumped generation, exactly as the reference World numbers them
+ * (src/world.cpp:1751-1782 createBody, :1820-1857 addShape). Handles are {index, generation}.
+ *
+ * Conventions
+ *   - Plain C types, host pointers, caller-owned buffers. No C++ or torch types cross this boundary.
+ *   - Every entry point returns an int status: TF_OK (0) or a negative TF_E* code. tf_last_error()
+ *     gives a one-line message for the calling thread's last failure.
+ *   - Invalid handles follow the reference's convention (src/world.cpp:352-371): getters fill zeros,
+ *     setters do nothing; they are not errors.
+ *   - tf_world_step with dt <= 0 or non-finite dt does nothing (src/world.cpp:1565).
+ *   - Device state lives in a library-owned arena on the device chosen at creation. State reads
+ *     (tf_body_get_*) copy back on demand.
+ *
+ * Reference interface each group replaces (paths inside AnvilFx/twofold):
+ *   tf_settings        <- WorldSettings            include/twofold/world.h:216-241
+ *   tf_body_desc       <- BodyDesc                 include/twofold/world.h:108-123
+ *   tf_shape_desc      <- ShapeDesc + Geometry     include/twofold/world.h:51-106
+ *   tf_world_create    <- World::World             include/twofold/world.h:364
+ *   tf_body_create     <- World::createBody        include/twofold/world.h:381
+ *   tf_shape_add       <- World::addShape          include/twofold/world.h:386
+ *   tf_world_step      <- World::step              include/twofold/world.h:378
+ *   tf_body_get_state  <- World::transform/linearVelocity/angularVelocity  world.h:404-411
+ *   tf_world_contacts  <- World::contacts          include/twofold/world.h:473
+ *   tf_world_profile   <- World::profile           include/twofold/world.h:379
+ */
+#ifndef TWOFOLD_B200_H
+#define TWOFOLD_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(_WIN32)
+#define TF_API __declspec(dllexport)
+#else
+#define TF_API __attribute__((visibility("default")))
+#endif
+
+#define TF_ABI_VERSION 1
+
+enum tf_status {
+    TF_OK = 0,
+    TF_E_INVALID = -1,   /* bad argument (null pointer, out-of-range world, bad enum) */
+    TF_E_CUDA = -2,      /* a CUDA call failed; the message names it */
+    TF_E_CAPACITY = -3,  /* a device buffer overflowed and could not be grown */
+    TF_E_NUMERIC = -4,   /* the step produced a non-finite body state */
+    TF_E_TIMEOUT = -5,   /* a bounded device wait ran out */
+    TF_E_UNSUPPORTED = -6 /* the scene uses a feature this build does not run on the device */
+};
+
+/* Device-side error bits, as returned by tf_world_device_status. */
+enum tf_device_flags {
+    TF_DEV_PAIR_OVERFLOW = 1u << 0,
+    TF_DEV_CONTACT_OVERFLOW = 1u << 1,
+    TF_DEV_NONFINITE = 1u << 2,
+    TF_DEV_TIMEOUT = 1u << 3,
+    TF_DEV_UNSUPPORTED_PAIR = 1u << 4,
+    TF_DEV_CONTINUOUS_SKIPPED = 1u << 5, /* a shape moved far enough to need a sweep, which runs on the host */
+    TF_DEV_LIST_OVERFLOW = 1u << 6
+};
+
+enum tf_motion_type { TF_STATIC = 0, TF_KINEMATIC = 1, TF_DYNAMIC = 2 };
+
+enum tf_lock_flags {
+    TF_LOCK_TRANSLATION_X = 1 << 0,
+    TF_LOCK_TRANSLATION_Y = 1 << 1,
+    TF_LOCK_TRANSLATION_Z = 1 << 2,
+    TF_LOCK_ROTATION_X = 1 << 3,
+    TF_LOCK_ROTATION_Y = 1 << 4,
+    TF_LOCK_ROTATION_Z = 1 << 5,
+    TF_LOCK_PLANAR = (1 << 2) | (1 << 3) | (1 << 4)
+};
+
+enum tf_geometry { TF_SPHERE = 0, TF_BOX = 1, TF_CYLINDER = 2, TF_PRISM = 3, TF_HULL = 4, TF_HALFSPACE = 5, TF_MESH = 6 };
+
+typedef struct tf_id {
+    uint32_t index;
+    uint32_t generation;
+} tf_id;
+
+/* WorldSettings, field for field (include/twofold/world.h:216-241). */
+typedef struct tf_settings {
+    float gravity[3];
+    float length_unit;
+    int32_t substeps;
+    float contact_hertz;
+    float contact_damping_ratio;
+    float max_pushout_speed;
+    float max_linear_speed;
+    float max_angular_speed;
+    float restitution_threshold;
+    float hit_threshold;
+    float sleep_threshold;
+    float time_to_sleep;
+    float contact_reuse_distance;
+    float contact_reuse_angle;
+    float joint_hertz;
+    float joint_damping_ratio;
+    int32_t continuous;
+} tf_settings;
+
+/* BodyDesc (include/twofold/world.h:108-123). Quaternions are x, y, z, w. */
+typedef struct tf_body_desc {
+    int32_t type;
+    float position[3];
+    float rotation[4];
+    float linear_velocity[3];
+    float angular_velocity[3];
+    float linear_damping;
+    float angular_damping;
+    float gravity_scale;
+    uint32_t locks;
+    float lock_frame[4];
+    int32_t awake;
+    int32_t can_sleep;
+} tf_body_desc;
+
+/* ShapeDesc plus its Geometry alternative (include/twofold/world.h:51-106).
+ *   TF_SPHERE: radius.  TF_BOX: half_extents.  TF_CYLINDER: radius, half_height.
+ *   TF_PRISM: points = point_count (x, y) pairs, z_min, z_max.
+ *   TF_HULL: points = point_count (x, y, z) triples, max_vertices.
+ *   TF_HALFSPACE: no parameters (static bodies only).
+ * points is read during tf_shape_add only. */
+typedef struct tf_shape_desc {
+    int32_t geometry;
+    float radius;
+    float half_extents[3];
+    float half_height;
+    const float* points;
+    int32_t point_count;
+    int32_t max_vertices;
+    float z_min;
+    float z_max;
+    float position[3];
+    float rotation[4];
+    float density;
+    float friction;
+    float restitution;
+    float rolling_resistance;
+    uint32_t category;
+    uint32_t mask;
+    int32_t sensor;
+} tf_shape_desc;
+
+/* StepProfile (include/twofold/world.h:346-360). Times are device milliseconds per phase. */
+typedef struct tf_profile {
+    float total;
+    float broadphase;
+    float narrowphase;
+    float solver;
+    float continuous;
+    float sleep;
+    int32_t candidate_pairs;
+    int32_t swept_pairs;
+    int32_t impacts;
+    int32_t manifolds;
+    int32_t touching_contacts;
+    int32_t awake_bodies;
+    int32_t awake_islands;
+} tf_profile;
+
+/* One contact of World::contacts (ContactInfo, include/twofold/world.h:252-266) plus the
+ * pair key, part and clipped feature the parity tests compare. */
+typedef struct tf_contact {
+    uint64_t key;
+    uint32_t part;
+    uint32_t shape_a, shape_b;
+    uint32_t body_a, body_b;
+    int32_t point_count;
+    int32_t feature_kind; /* 0 none, 1 face of A, 2 face of B, 3 edge pair */
+    int32_t feature_a, feature_b;
+    float normal[3];
+    float friction, restitution, rolling_resistance;
+    float rolling_impulse[3];
+    float points[4][3];
+    float separations[4];
+    float normal_impulses[4];
+    float tangent_impulses[4][3];
+} tf_contact;
+
+TF_API int tf_abi_version(void);
+TF_API const char* tf_last_error(void);
+TF_API void tf_default_settings(tf_settings* out);
+
+/* Creates n_worlds empty worlds sharing settings on CUDA device `device`. */
+TF_API int tf_world_create(const tf_settings* settings, int32_t n_worlds, int32_t device, void** out_world);
+TF_API int tf_world_destroy(void* world);
+TF_API int tf_world_count(void* world, int32_t* n_worlds);
+TF_API int tf_world_set_settings(void* world, const tf_settings* settings);
+
+TF_API int tf_body_create(void* world, int32_t w, const tf_body_desc* desc, tf_id* out_body);
+TF_API int tf_shape_add(void* world, int32_t w, tf_id body, const tf_shape_desc* desc, tf_id* out_shape);
+/* Bulk forms: n bodies into worlds world_of[i]; n shapes onto body_of[i] (indices in world_of[i]). */
+TF_API int tf_bodies_create(void* world, int32_t n, const int32_t* world_of, const tf_body_desc* descs,
+                            tf_id* out_bodies);
+TF_API int tf_shapes_add(void* world, int32_t n, const int32_t* world_of, const uint32_t* body_of,
+                         const tf_shape_desc* descs, tf_id* out_shapes);
+
+/* Steps every world of the batch n_steps times by dt. Returns TF_OK, or an error with the device
+ * flags available from tf_world_device_status. */
+TF_API int tf_world_step(void* world, float dt, int32_t n_steps);
+/* Records n_steps steps of every world into a CUDA graph on first use and replays it afterwards. */
+TF_API int tf_world_step_graph(void* world, float dt, int32_t n_steps);
+TF_API int tf_world_synchronize(void* world);
+TF_API int tf_world_device_status(void* world, uint32_t* flags);
+
+/* Body state of world w: position, rotation (x,y,z,w), linear and angular velocity. */
+TF_API int tf_body_get_state(void* world, int32_t w, tf_id body, float position[3], float rotation[4],
+                             float linear_velocity[3], float angular_velocity[3]);
+TF_API int tf_body_set_velocity(void* world, int32_t w, tf_id body, const float linear_velocity[3],
+                                const float angular_velocity[3]);
+/* Mass, local center and local inertia (row-major 3x3) as World::massProperties returns them. */
+TF_API int tf_body_get_mass(void* world, int32_t w, tf_id body, float* mass, float center[3], float inertia[9]);
+TF_API int tf_body_is_awake(void* world, int32_t w, tf_id body, int32_t* awake);
+
+/* All body states of the batch in body order, world after world. Arrays hold total-body entries;
+ * any pointer may be null. counts_out[w] gets the body count of world w when non-null. */
+TF_API int tf_world_body_count(void* world, int64_t* total_bodies);
+TF_API int tf_world_get_states(void* world, float* positions, float* rotations, float* linear_velocities,
+                               float* angular_velocities, int32_t* awake);
+
+/* Contacts of world w after the last step, in (key, part) order. include_speculative as in
+ * World::contacts. Writes up to capacity entries and the total count. */
+TF_API int tf_world_contacts(void* world, int32_t w, int32_t include_speculative, tf_contact* out,
+                             int32_t capacity, int32_t* count);
+/* Sorted, unique shape-pair keys (minShape << 32 | maxShape) the last broadphase produced. */
+TF_API int tf_world_candidates(void* world, int32_t w, uint64_t* out, int32_t capacity, int32_t* count);
+TF_API int tf_world_profile(void* world, int32_t w, tf_profile* out);
+/* Sum over worlds of awake dynamic bodies after the last step. */
+TF_API int tf_world_awake_bodies(void* world, int64_t* count);
+
+/* Number of kernel launches the library issued since creation (for launch accounting). */
+TF_API int tf_world_launch_count(void* world, int64_t* launches);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

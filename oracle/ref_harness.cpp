@@ -1,0 +1,293 @@
+// Test infrastructure only: the oracle side of every parity check. Only tests/, the smoke check and the
+// CPU-baseline leg of bench.py load the library this file builds into.
+//
+// It compiles the unmodified AnvilFx/twofold sources (src/*.cpp, include/twofold/*.h) and wraps one
+// reference World per handle behind the same plain-C descriptors the B200 library takes
+// (include/twofold_b200.h), so both sides are built from identical inputs. src/world.cpp is compiled as
+// part of this translation unit, so the harness can read World::Impl state that the public API hides:
+// the sorted candidate keys (src/world.cpp:868-870) and each contact's clipped feature
+// (src/internal.h:482-488).
+#include <atomic>
+#include <cstring>
+#include <thread>
+#include <vector>
+
+// World::impl_ is private in include/twofold/world.h:507-509. The harness reads it, so the class is
+// seen with public members in this translation unit only.
+#define private public
+#include "world.cpp"
+#undef private
+
+#include "twofold_b200.h"
+
+using namespace twofold;
+
+namespace {
+
+WorldSettings toSettings(const tf_settings* s) {
+    WorldSettings w;
+    if (!s) { return w; }
+    w.gravity = { s->gravity[0], s->gravity[1], s->gravity[2] };
+    w.lengthUnit = s->length_unit;
+    w.substeps = s->substeps;
+    w.contactHertz = s->contact_hertz;
+    w.contactDampingRatio = s->contact_damping_ratio;
+    w.maxPushoutSpeed = s->max_pushout_speed;
+    w.maxLinearSpeed = s->max_linear_speed;
+    w.maxAngularSpeed = s->max_angular_speed;
+    w.restitutionThreshold = s->restitution_threshold;
+    w.hitThreshold = s->hit_threshold;
+    w.sleepThreshold = s->sleep_threshold;
+    w.timeToSleep = s->time_to_sleep;
+    w.contactReuseDistance = s->contact_reuse_distance;
+    w.contactReuseAngle = s->contact_reuse_angle;
+    w.jointHertz = s->joint_hertz;
+    w.jointDampingRatio = s->joint_damping_ratio;
+    w.continuous = s->continuous != 0;
+    return w;
+}
+
+Vec3 v3(const float* p) { return { p[0], p[1], p[2] }; }
+Quat q4(const float* p) { return { p[0], p[1], p[2], p[3] }; }
+
+BodyDesc toBody(const tf_body_desc* d) {
+    BodyDesc b;
+    b.type = (MotionType)d->type;
+    b.position = v3(d->position);
+    b.rotation = q4(d->rotation);
+    b.linearVelocity = v3(d->linear_velocity);
+    b.angularVelocity = v3(d->angular_velocity);
+    b.linearDamping = d->linear_damping;
+    b.angularDamping = d->angular_damping;
+    b.gravityScale = d->gravity_scale;
+    b.locks = (uint8_t)d->locks;
+    b.lockFrame = q4(d->lock_frame);
+    b.awake = d->awake != 0;
+    b.canSleep = d->can_sleep != 0;
+    return b;
+}
+
+bool toShape(const tf_shape_desc* d, ShapeDesc& s) {
+    switch (d->geometry) {
+    case TF_SPHERE: s.geometry = Sphere{ d->radius }; break;
+    case TF_BOX: s.geometry = Box{ v3(d->half_extents) }; break;
+    case TF_CYLINDER: s.geometry = Cylinder{ d->radius, d->half_height }; break;
+    case TF_PRISM: {
+        Prism p;
+        for (int i = 0; i < d->point_count; ++i) { p.polygon.push_back({ d->points[2 * i], d->points[2 * i + 1] }); }
+        p.zMin = d->z_min;
+        p.zMax = d->z_max;
+        s.geometry = p;
+        break;
+    }
+    case TF_HULL: {
+        Hull h;
+        for (int i = 0; i < d->point_count; ++i) { h.points.push_back(v3(d->points + 3 * i)); }
+        h.maxVertices = d->max_vertices;
+        s.geometry = h;
+        break;
+    }
+    case TF_HALFSPACE: s.geometry = HalfSpace{}; break;
+    default: return false;
+    }
+    s.position = v3(d->position);
+    s.rotation = q4(d->rotation);
+    s.density = d->density;
+    s.friction = d->friction;
+    s.restitution = d->restitution;
+    s.rollingResistance = d->rolling_resistance;
+    s.category = d->category;
+    s.mask = d->mask;
+    s.sensor = d->sensor != 0;
+    return true;
+}
+
+void put3(float* o, const Vec3& v) {
+    if (!o) { return; }
+    o[0] = v.x;
+    o[1] = v.y;
+    o[2] = v.z;
+}
+
+void put4(float* o, const Quat& q) {
+    if (!o) { return; }
+    o[0] = q.x;
+    o[1] = q.y;
+    o[2] = q.z;
+    o[3] = q.w;
+}
+
+World* W(void* h) { return static_cast<World*>(h); }
+
+}
+
+extern "C" {
+
+TF_API void* ref_world_create(const tf_settings* s) { return new World(toSettings(s)); }
+TF_API void* ref_world_copy(void* h) { return new World(*W(h)); }
+TF_API void ref_world_destroy(void* h) { delete W(h); }
+
+TF_API int ref_body_create(void* h, const tf_body_desc* d, tf_id* out) {
+    const BodyId id = W(h)->createBody(toBody(d));
+    out->index = id.index;
+    out->generation = id.generation;
+    return 0;
+}
+
+TF_API int ref_shape_add(void* h, tf_id body, const tf_shape_desc* d, tf_id* out) {
+    ShapeDesc s;
+    if (!toShape(d, s)) { return -1; }
+    const ShapeId id = W(h)->addShape({ body.index, body.generation }, s);
+    out->index = id.index;
+    out->generation = id.generation;
+    return 0;
+}
+
+// Bulk scene build: n bodies, then shapes onto body_of[i] (an index into the bodies just made).
+TF_API int ref_scene_build(void* h, int nb, const tf_body_desc* bodies, int ns, const uint32_t* body_of,
+                           const tf_shape_desc* shapes) {
+    std::vector<BodyId> ids((size_t)nb);
+    for (int i = 0; i < nb; ++i) { ids[(size_t)i] = W(h)->createBody(toBody(&bodies[i])); }
+    for (int i = 0; i < ns; ++i) {
+        ShapeDesc s;
+        if (!toShape(&shapes[i], s)) { return -1; }
+        W(h)->addShape(ids[body_of[i]], s);
+    }
+    return 0;
+}
+
+TF_API int ref_world_step(void* h, float dt, int n) {
+    for (int i = 0; i < n; ++i) { W(h)->step(dt); }
+    return 0;
+}
+
+TF_API int ref_body_count(void* h) { return (int)W(h)->impl_->bodies.size(); }
+
+// Every body slot in index order; dead slots read as zeros.
+TF_API int ref_world_get_states(void* h, float* p, float* q, float* v, float* w, int32_t* awake) {
+    const auto& bodies = W(h)->impl_->bodies;
+    for (size_t i = 0; i < bodies.size(); ++i) {
+        const Body& b = bodies[i];
+        put3(p ? p + 3 * i : nullptr, b.xf.p);
+        put4(q ? q + 4 * i : nullptr, b.xf.q);
+        put3(v ? v + 3 * i : nullptr, b.v);
+        put3(w ? w + 3 * i : nullptr, b.w);
+        if (awake) { awake[i] = b.awake ? 1 : 0; }
+    }
+    return (int)bodies.size();
+}
+
+TF_API int ref_body_set_velocity(void* h, tf_id body, const float* v, const float* w) {
+    W(h)->setLinearVelocity({ body.index, body.generation }, v3(v));
+    W(h)->setAngularVelocity({ body.index, body.generation }, v3(w));
+    return 0;
+}
+
+TF_API int ref_body_get_mass(void* h, tf_id body, float* mass, float* center, float* inertia) {
+    const MassProperties m = W(h)->massProperties({ body.index, body.generation });
+    *mass = m.mass;
+    put3(center, m.center);
+    for (int r = 0; r < 3; ++r) { put3(inertia + 3 * r, m.inertia.r[r]); }
+    return 0;
+}
+
+TF_API int ref_world_candidates(void* h, uint64_t* out, int cap, int* count) {
+    const auto& c = W(h)->impl_->candidatePairs;
+    *count = (int)c.size();
+    for (size_t i = 0; i < c.size() && (int)i < cap; ++i) { out[i] = c[i]; }
+    return 0;
+}
+
+// The internal contact list in (key, part) order. mode 0: touching only (as World::contacts()),
+// 1: every contact not removed, 2: the raw list.
+TF_API int ref_world_contacts(void* h, int mode, tf_contact* out, int cap, int* count) {
+    const World::Impl& w = *W(h)->impl_;
+    int n = 0;
+    for (const Contact& c : w.contacts) {
+        if (mode < 2 && (c.removed || (mode == 0 && !c.touching()))) { continue; }
+        if (n < cap) {
+            tf_contact& o = out[n];
+            std::memset(&o, 0, sizeof(o));
+            o.key = c.key;
+            o.part = c.part;
+            o.shape_a = c.shapeA;
+            o.shape_b = c.shapeB;
+            o.body_a = c.bodyA;
+            o.body_b = c.bodyB;
+            o.point_count = c.count;
+            o.feature_kind = (int)c.feature.kind;
+            o.feature_a = c.feature.a;
+            o.feature_b = c.feature.b;
+            put3(o.normal, c.normal);
+            o.friction = c.friction;
+            o.restitution = c.restitution;
+            o.rolling_resistance = c.rollingResistance;
+            put3(o.rolling_impulse, c.rollingImpulse);
+            for (int i = 0; i < c.count; ++i) {
+                put3(o.points[i], w.bodies[c.bodyA].xf.apply(c.points[i].localA));
+                o.separations[i] = c.points[i].separation;
+                o.normal_impulses[i] = c.points[i].normalImpulse;
+                put3(o.tangent_impulses[i], c.points[i].tangentImpulse);
+            }
+        }
+        ++n;
+    }
+    *count = n;
+    return 0;
+}
+
+TF_API int ref_world_profile(void* h, tf_profile* out) {
+    const StepProfile& p = W(h)->profile();
+    out->total = p.total;
+    out->broadphase = p.broadphase;
+    out->narrowphase = p.narrowphase;
+    out->solver = p.solver;
+    out->continuous = p.continuous;
+    out->sleep = p.sleep;
+    out->candidate_pairs = p.candidatePairs;
+    out->swept_pairs = p.sweptPairs;
+    out->impacts = p.impacts;
+    out->manifolds = p.manifolds;
+    out->touching_contacts = p.touchingContacts;
+    out->awake_bodies = p.awakeBodies;
+    out->awake_islands = p.awakeIslands;
+    return 0;
+}
+
+TF_API int ref_awake_dynamic(void* h) {
+    int n = 0;
+    for (const Body& b : W(h)->impl_->bodies) { n += (b.alive && b.type == MotionType::Dynamic && b.awake) ? 1 : 0; }
+    return n;
+}
+
+// Steps n independent worlds `steps` times each: every world is stepped start to finish by one thread
+// taken from a pool of `threads`, worlds handed out in order as threads come free. Writes the awake
+// dynamic body count summed over every step of every world to body_steps.
+TF_API int ref_worlds_step_parallel(void** worlds, int n, float dt, int steps, int threads, int64_t* body_steps) {
+    std::atomic<int> next{ 0 };
+    std::atomic<int64_t> total{ 0 };
+    auto work = [&] {
+        int64_t mine = 0;
+        for (int i = next++; i < n; i = next++) {
+            World* w = W(worlds[i]);
+            for (int s = 0; s < steps; ++s) {
+                w->step(dt);
+                mine += w->profile().awakeBodies;
+            }
+        }
+        total += mine;
+    };
+    if (threads <= 1) {
+        work();
+    } else {
+        std::vector<std::thread> pool;
+        for (int t = 0; t < threads; ++t) { pool.emplace_back(work); }
+        for (std::thread& t : pool) { t.join(); }
+    }
+    if (body_steps) { *body_steps = total.load(); }
+    return 0;
+}
+
+TF_API int ref_hardware_threads(void) { return (int)std::thread::hardware_concurrency(); }
+
+}

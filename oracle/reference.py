@@ -1,0 +1,134 @@
+"""Test infrastructure only: Python access to the oracle (the unmodified AnvilFx/twofold World, built by
+oracle/Makefile into oracle/_ref/libtwofold_ref.so). Only tests/, the smoke check and bench.py's
+CPU-baseline leg use this module, and only as the checker or the timed CPU baseline.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+from twofold_b200 import abi
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_LIB = os.path.join(HERE, "_ref", "libtwofold_ref.so")
+
+_lib = None
+
+
+def available():
+    return os.path.exists(REF_LIB)
+
+
+def load():
+    global _lib
+    if _lib is None:
+        if not available():
+            raise RuntimeError(f"{REF_LIB} is missing; build it with `make -C oracle`")
+        lib = C.CDLL(REF_LIB)
+        P = C.c_void_p
+        sig = {
+            "ref_world_create": ([C.POINTER(abi.tf_settings)], P),
+            "ref_world_copy": ([P], P),
+            "ref_world_destroy": ([P], None),
+            "ref_body_create": ([P, C.POINTER(abi.tf_body_desc), C.POINTER(abi.tf_id)], C.c_int),
+            "ref_shape_add": ([P, abi.tf_id, C.POINTER(abi.tf_shape_desc), C.POINTER(abi.tf_id)], C.c_int),
+            "ref_scene_build": ([P, C.c_int, P, C.c_int, P, P], C.c_int),
+            "ref_world_step": ([P, C.c_float, C.c_int], C.c_int),
+            "ref_body_count": ([P], C.c_int),
+            "ref_world_get_states": ([P, P, P, P, P, P], C.c_int),
+            "ref_body_set_velocity": ([P, abi.tf_id, P, P], C.c_int),
+            "ref_body_get_mass": ([P, abi.tf_id, P, P, P], C.c_int),
+            "ref_world_candidates": ([P, P, C.c_int, C.POINTER(C.c_int)], C.c_int),
+            "ref_world_contacts": ([P, C.c_int, C.POINTER(abi.tf_contact), C.c_int, C.POINTER(C.c_int)], C.c_int),
+            "ref_world_profile": ([P, C.POINTER(abi.tf_profile)], C.c_int),
+            "ref_awake_dynamic": ([P], C.c_int),
+            "ref_worlds_step_parallel": ([P, C.c_int, C.c_float, C.c_int, C.c_int, C.POINTER(C.c_int64)], C.c_int),
+            "ref_hardware_threads": ([], C.c_int),
+        }
+        for name, (args, res) in sig.items():
+            f = getattr(lib, name)
+            f.argtypes = args
+            f.restype = res
+        _lib = lib
+    return _lib
+
+
+class RefWorld:
+    """One reference World built from a scenes.World."""
+
+    def __init__(self, world, settings=None, _handle=None):
+        self.lib = load()
+        if _handle is not None:
+            self.h = _handle
+            return
+        s = settings if settings is not None else abi.default_settings()
+        self.h = self.lib.ref_world_create(C.byref(s))
+        rc = self.lib.ref_scene_build(self.h, len(world.bodies), world.bodies.ctypes.data, len(world.shapes),
+                                      world.body_of.ctypes.data, world.shapes.ctypes.data)
+        if rc != 0:
+            raise RuntimeError("reference scene build failed")
+
+    def copy(self):
+        return RefWorld(None, _handle=self.lib.ref_world_copy(self.h))
+
+    def __del__(self):
+        if getattr(self, "h", None) and _lib is not None:
+            _lib.ref_world_destroy(self.h)
+            self.h = None
+
+    def step(self, dt, n=1):
+        self.lib.ref_world_step(self.h, C.c_float(dt), n)
+
+    def states(self):
+        n = self.lib.ref_body_count(self.h)
+        p = np.zeros((n, 3), np.float32)
+        q = np.zeros((n, 4), np.float32)
+        v = np.zeros((n, 3), np.float32)
+        w = np.zeros((n, 3), np.float32)
+        awake = np.zeros(n, np.int32)
+        self.lib.ref_world_get_states(self.h, p.ctypes.data, q.ctypes.data, v.ctypes.data, w.ctypes.data,
+                                      awake.ctypes.data)
+        return {"p": p, "q": q, "v": v, "w": w, "awake": awake}
+
+    def candidates(self):
+        n = C.c_int(0)
+        self.lib.ref_world_candidates(self.h, None, 0, C.byref(n))
+        out = np.zeros(max(n.value, 1), np.uint64)
+        self.lib.ref_world_candidates(self.h, out.ctypes.data, n.value, C.byref(n))
+        return out[:n.value]
+
+    def contacts(self, mode=1):
+        n = C.c_int(0)
+        self.lib.ref_world_contacts(self.h, mode, None, 0, C.byref(n))
+        arr = (abi.tf_contact * max(n.value, 1))()
+        self.lib.ref_world_contacts(self.h, mode, arr, n.value, C.byref(n))
+        return list(arr)[:n.value]
+
+    def profile(self):
+        p = abi.tf_profile()
+        self.lib.ref_world_profile(self.h, C.byref(p))
+        return p
+
+    def mass(self, index, generation=0):
+        m = C.c_float(0)
+        c = np.zeros(3, np.float32)
+        i = np.zeros(9, np.float32)
+        self.lib.ref_body_get_mass(self.h, abi.tf_id(index, generation), C.byref(m), c.ctypes.data, i.ctypes.data)
+        return m.value, c, i.reshape(3, 3)
+
+    def awake_dynamic(self):
+        return self.lib.ref_awake_dynamic(self.h)
+
+
+def step_parallel(ref_worlds, dt, steps, threads):
+    """Steps independent reference worlds, each by one thread from a pool of `threads`. Returns the
+    awake-dynamic body-steps summed over every step of every world."""
+    lib = load()
+    arr = (C.c_void_p * len(ref_worlds))(*[r.h for r in ref_worlds])
+    total = C.c_int64(0)
+    lib.ref_worlds_step_parallel(arr, len(ref_worlds), C.c_float(dt), steps, threads, C.byref(total))
+    return total.value
+
+
+def hardware_threads():
+    return load().ref_hardware_threads()

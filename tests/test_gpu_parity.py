@@ -1,0 +1,143 @@
+"""Parity of the B200 step against the oracle (the reference's own World::step) on identical input.
+
+Bars, per the contact pipeline's contract: the broadphase pair list, manifold point counts and feature ids
+match bit for bit; positions, rotations and velocities after one step agree within 1e-5 (normwise
+relative); repeated GPU runs are bit-identical. Longer runs check the same tolerance, which only holds if
+every step matches closely.
+"""
+import numpy as np
+import pytest
+
+import reference as R
+from parity import contact_table, first_difference, rel_err, state_errors, states_bitwise_equal
+from twofold_b200 import scenes
+from twofold_b200.world import Batch
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-5
+
+needs_oracle = pytest.mark.skipif(not R.available(), reason="oracle library not built")
+
+
+def _compare_world(batch, wi, ref, label):
+    mine = batch.world_states(wi)
+    theirs = ref.states()
+    errs = state_errors(mine, theirs)
+    assert max(errs.values()) <= TOL, f"{label}: state error {errs}"
+    return errs
+
+
+def _check_pairs_and_manifolds(batch, wi, ref, label):
+    cm, cr = batch.candidates(wi), ref.candidates()
+    assert np.array_equal(cm, cr), f"{label}: candidate pairs differ at {first_difference(list(cm), list(cr))}"
+    em, pm = contact_table(batch.contacts(wi, mode=1))
+    er, pr = contact_table(ref.contacts(mode=1))
+    assert em == er, f"{label}: contact keys/counts/features differ at {first_difference(em, er)}"
+    assert rel_err(pm, pr) <= TOL, f"{label}: contact points differ by {rel_err(pm, pr)}"
+
+
+@needs_oracle
+@pytest.mark.parametrize("kind", ["box_on_ground", "sphere_on_ground", "boxes"])
+@pytest.mark.parametrize("steps", [1, 30])
+def test_small_worlds_match_reference(kind, steps):
+    w = scenes.single(kind)
+    sc = scenes.Scene(kind, [w])
+    b = Batch.from_scene(sc)
+    r = R.RefWorld(w, sc.settings)
+    for _ in range(steps):
+        b.step_checked(sc.dt)
+        r.step(sc.dt)
+    _check_pairs_and_manifolds(b, 0, r, f"{kind} after {steps}")
+    _compare_world(b, 0, r, f"{kind} after {steps}")
+
+
+@needs_oracle
+@pytest.mark.parametrize("seed", range(4))
+def test_tumbling_boxes_match_reference(seed):
+    w = scenes.single("boxes", n=12, seed=seed)
+    sc = scenes.Scene("boxes", [w])
+    b = Batch.from_scene(sc)
+    r = R.RefWorld(w, sc.settings)
+    for s in range(120):
+        b.step_checked(sc.dt)
+        r.step(sc.dt)
+        if s % 10 == 9:
+            _check_pairs_and_manifolds(b, 0, r, f"boxes seed {seed} step {s + 1}")
+            _compare_world(b, 0, r, f"boxes seed {seed} step {s + 1}")
+
+
+@needs_oracle
+def test_pyramid_one_step_matches_reference():
+    sc = scenes.config1()
+    b = Batch.from_scene(sc)
+    r = R.RefWorld(sc.worlds[0], sc.settings)
+    b.step_checked(sc.dt)
+    r.step(sc.dt)
+    assert len(b.candidates(0)) == 590
+    _check_pairs_and_manifolds(b, 0, r, "pyramid step 1")
+    _compare_world(b, 0, r, "pyramid step 1")
+
+
+@needs_oracle
+def test_pyramid_full_run_matches_reference():
+    sc = scenes.config1()
+    b = Batch.from_scene(sc)
+    r = R.RefWorld(sc.worlds[0], sc.settings)
+    for s in range(sc.steps):
+        b.step_checked(sc.dt)
+        r.step(sc.dt)
+        if s % 50 == 49:
+            _check_pairs_and_manifolds(b, 0, r, f"pyramid step {s + 1}")
+            _compare_world(b, 0, r, f"pyramid step {s + 1}")
+
+
+@needs_oracle
+@pytest.mark.parametrize("steps", [1, 60])
+def test_batched_uneven_worlds_match_reference(steps):
+    sc = scenes.config4(n_worlds=24)
+    b = Batch.from_scene(sc)
+    refs = [R.RefWorld(w, sc.settings) for w in sc.worlds]
+    for _ in range(steps):
+        b.step_checked(sc.dt)
+        for r in refs:
+            r.step(sc.dt)
+    for wi, r in enumerate(refs):
+        assert r.profile().impacts == 0  # the host-side sweep never moved a body here
+        _check_pairs_and_manifolds(b, wi, r, f"world {wi} after {steps}")
+        _compare_world(b, wi, r, f"world {wi} after {steps}")
+
+
+@needs_oracle
+def test_impact_worlds_match_reference():
+    sc = scenes.config5(n_worlds=8)
+    b = Batch.from_scene(sc)
+    refs = [R.RefWorld(w, sc.settings) for w in sc.worlds]
+    for s in range(40):
+        b.step_checked(sc.dt)
+        for r in refs:
+            r.step(sc.dt)
+    for wi, r in enumerate(refs):
+        _check_pairs_and_manifolds(b, wi, r, f"impact world {wi}")
+        _compare_world(b, wi, r, f"impact world {wi}")
+
+
+def test_repeated_runs_are_bit_identical():
+    sc = scenes.config4(n_worlds=16)
+    out = []
+    for _ in range(2):
+        b = Batch.from_scene(sc)
+        b.step_checked(sc.dt, 20)
+        out.append(b.states())
+        b.close()
+    assert states_bitwise_equal(out[0], out[1])
+
+
+def test_graph_replay_matches_direct_launches():
+    sc = scenes.config4(n_worlds=16)
+    a = Batch.from_scene(sc)
+    g = Batch.from_scene(sc)
+    a.step_checked(sc.dt, 8)
+    g.step_checked(sc.dt, 4, graph=True)
+    g.step_checked(sc.dt, 4, graph=True)
+    assert states_bitwise_equal(a.states(), g.states())

@@ -1,0 +1,267 @@
+"""ctypes mirror of include/twofold_b200.h and the loader for the CUDA library.
+
+The library is the product: `load()` raises when libtwofold_b200.so is missing instead of falling back
+to anything else.
+"""
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libtwofold_b200.so")
+
+TF_OK = 0
+TF_STATIC, TF_KINEMATIC, TF_DYNAMIC = 0, 1, 2
+TF_SPHERE, TF_BOX, TF_CYLINDER, TF_PRISM, TF_HULL, TF_HALFSPACE, TF_MESH = range(7)
+TF_LOCK_PLANAR = (1 << 2) | (1 << 3) | (1 << 4)
+
+
+class tf_id(C.Structure):
+    _fields_ = [("index", C.c_uint32), ("generation", C.c_uint32)]
+
+
+class tf_settings(C.Structure):
+    _fields_ = [
+        ("gravity", C.c_float * 3),
+        ("length_unit", C.c_float),
+        ("substeps", C.c_int32),
+        ("contact_hertz", C.c_float),
+        ("contact_damping_ratio", C.c_float),
+        ("max_pushout_speed", C.c_float),
+        ("max_linear_speed", C.c_float),
+        ("max_angular_speed", C.c_float),
+        ("restitution_threshold", C.c_float),
+        ("hit_threshold", C.c_float),
+        ("sleep_threshold", C.c_float),
+        ("time_to_sleep", C.c_float),
+        ("contact_reuse_distance", C.c_float),
+        ("contact_reuse_angle", C.c_float),
+        ("joint_hertz", C.c_float),
+        ("joint_damping_ratio", C.c_float),
+        ("continuous", C.c_int32),
+    ]
+
+
+def default_settings(**over):
+    """WorldSettings defaults (include/twofold/world.h:216-241)."""
+    s = tf_settings()
+    s.gravity[:] = [0.0, -9.81, 0.0]
+    s.length_unit = 1.0
+    s.substeps = 4
+    s.contact_hertz = 30.0
+    s.contact_damping_ratio = 10.0
+    s.max_pushout_speed = 3.0
+    s.max_linear_speed = 1000.0
+    s.max_angular_speed = 1000.0
+    s.restitution_threshold = 1.0
+    s.hit_threshold = 1.0
+    s.sleep_threshold = 0.05
+    s.time_to_sleep = 0.5
+    s.contact_reuse_distance = 0.0005
+    s.contact_reuse_angle = 0.035
+    s.joint_hertz = 60.0
+    s.joint_damping_ratio = 2.0
+    s.continuous = 1
+    for k, v in over.items():
+        if k == "gravity":
+            s.gravity[:] = list(v)
+        else:
+            setattr(s, k, v)
+    return s
+
+
+class tf_body_desc(C.Structure):
+    _fields_ = [
+        ("type", C.c_int32),
+        ("position", C.c_float * 3),
+        ("rotation", C.c_float * 4),
+        ("linear_velocity", C.c_float * 3),
+        ("angular_velocity", C.c_float * 3),
+        ("linear_damping", C.c_float),
+        ("angular_damping", C.c_float),
+        ("gravity_scale", C.c_float),
+        ("locks", C.c_uint32),
+        ("lock_frame", C.c_float * 4),
+        ("awake", C.c_int32),
+        ("can_sleep", C.c_int32),
+    ]
+
+
+class tf_shape_desc(C.Structure):
+    _fields_ = [
+        ("geometry", C.c_int32),
+        ("radius", C.c_float),
+        ("half_extents", C.c_float * 3),
+        ("half_height", C.c_float),
+        ("points", C.POINTER(C.c_float)),
+        ("point_count", C.c_int32),
+        ("max_vertices", C.c_int32),
+        ("z_min", C.c_float),
+        ("z_max", C.c_float),
+        ("position", C.c_float * 3),
+        ("rotation", C.c_float * 4),
+        ("density", C.c_float),
+        ("friction", C.c_float),
+        ("restitution", C.c_float),
+        ("rolling_resistance", C.c_float),
+        ("category", C.c_uint32),
+        ("mask", C.c_uint32),
+        ("sensor", C.c_int32),
+    ]
+
+
+class tf_profile(C.Structure):
+    _fields_ = [
+        ("total", C.c_float),
+        ("broadphase", C.c_float),
+        ("narrowphase", C.c_float),
+        ("solver", C.c_float),
+        ("continuous", C.c_float),
+        ("sleep", C.c_float),
+        ("candidate_pairs", C.c_int32),
+        ("swept_pairs", C.c_int32),
+        ("impacts", C.c_int32),
+        ("manifolds", C.c_int32),
+        ("touching_contacts", C.c_int32),
+        ("awake_bodies", C.c_int32),
+        ("awake_islands", C.c_int32),
+    ]
+
+
+class tf_contact(C.Structure):
+    _fields_ = [
+        ("key", C.c_uint64),
+        ("part", C.c_uint32),
+        ("shape_a", C.c_uint32),
+        ("shape_b", C.c_uint32),
+        ("body_a", C.c_uint32),
+        ("body_b", C.c_uint32),
+        ("point_count", C.c_int32),
+        ("feature_kind", C.c_int32),
+        ("feature_a", C.c_int32),
+        ("feature_b", C.c_int32),
+        ("normal", C.c_float * 3),
+        ("friction", C.c_float),
+        ("restitution", C.c_float),
+        ("rolling_resistance", C.c_float),
+        ("rolling_impulse", C.c_float * 3),
+        ("points", (C.c_float * 3) * 4),
+        ("separations", C.c_float * 4),
+        ("normal_impulses", C.c_float * 4),
+        ("tangent_impulses", (C.c_float * 3) * 4),
+    ]
+
+
+def body_desc(type=TF_DYNAMIC, position=(0, 0, 0), rotation=(0, 0, 0, 1), linear_velocity=(0, 0, 0),
+              angular_velocity=(0, 0, 0), linear_damping=0.0, angular_damping=0.0, gravity_scale=1.0, locks=0,
+              lock_frame=(0, 0, 0, 1), awake=True, can_sleep=True):
+    """BodyDesc defaults (include/twofold/world.h:108-123)."""
+    d = tf_body_desc()
+    d.type = type
+    d.position[:] = list(position)
+    d.rotation[:] = list(rotation)
+    d.linear_velocity[:] = list(linear_velocity)
+    d.angular_velocity[:] = list(angular_velocity)
+    d.linear_damping = linear_damping
+    d.angular_damping = angular_damping
+    d.gravity_scale = gravity_scale
+    d.locks = locks
+    d.lock_frame[:] = list(lock_frame)
+    d.awake = 1 if awake else 0
+    d.can_sleep = 1 if can_sleep else 0
+    return d
+
+
+def shape_desc(geometry=TF_BOX, radius=0.5, half_extents=(0.5, 0.5, 0.5), half_height=0.5, points=None,
+               max_vertices=64, z_min=-0.5, z_max=0.5, position=(0, 0, 0), rotation=(0, 0, 0, 1), density=1.0,
+               friction=0.5, restitution=0.0, rolling_resistance=0.0, category=1, mask=0xFFFFFFFF, sensor=False):
+    """ShapeDesc defaults (include/twofold/world.h:90-106). `points` must stay alive until the shape is added."""
+    d = tf_shape_desc()
+    d.geometry = geometry
+    d.radius = radius
+    d.half_extents[:] = list(half_extents)
+    d.half_height = half_height
+    if points is not None:
+        d.points = points.ctypes.data_as(C.POINTER(C.c_float))
+        d.point_count = points.shape[0]
+    d.max_vertices = max_vertices
+    d.z_min = z_min
+    d.z_max = z_max
+    d.position[:] = list(position)
+    d.rotation[:] = list(rotation)
+    d.density = density
+    d.friction = friction
+    d.restitution = restitution
+    d.rolling_resistance = rolling_resistance
+    d.category = category
+    d.mask = mask
+    d.sensor = 1 if sensor else 0
+    return d
+
+
+_lib = None
+
+
+def _declare(lib):
+    P = C.c_void_p
+    sig = {
+        "tf_abi_version": ([], C.c_int),
+        "tf_last_error": ([], C.c_char_p),
+        "tf_default_settings": ([C.POINTER(tf_settings)], None),
+        "tf_world_create": ([C.POINTER(tf_settings), C.c_int32, C.c_int32, C.POINTER(P)], C.c_int),
+        "tf_world_destroy": ([P], C.c_int),
+        "tf_world_count": ([P, C.POINTER(C.c_int32)], C.c_int),
+        "tf_world_set_settings": ([P, C.POINTER(tf_settings)], C.c_int),
+        "tf_body_create": ([P, C.c_int32, C.POINTER(tf_body_desc), C.POINTER(tf_id)], C.c_int),
+        "tf_shape_add": ([P, C.c_int32, tf_id, C.POINTER(tf_shape_desc), C.POINTER(tf_id)], C.c_int),
+        "tf_bodies_create": ([P, C.c_int32, P, C.POINTER(tf_body_desc), P], C.c_int),
+        "tf_shapes_add": ([P, C.c_int32, P, P, C.POINTER(tf_shape_desc), P], C.c_int),
+        "tf_world_step": ([P, C.c_float, C.c_int32], C.c_int),
+        "tf_world_step_graph": ([P, C.c_float, C.c_int32], C.c_int),
+        "tf_world_synchronize": ([P], C.c_int),
+        "tf_world_device_status": ([P, C.POINTER(C.c_uint32)], C.c_int),
+        "tf_body_get_state": ([P, C.c_int32, tf_id, P, P, P, P], C.c_int),
+        "tf_body_set_velocity": ([P, C.c_int32, tf_id, P, P], C.c_int),
+        "tf_body_get_mass": ([P, C.c_int32, tf_id, P, P, P], C.c_int),
+        "tf_body_is_awake": ([P, C.c_int32, tf_id, C.POINTER(C.c_int32)], C.c_int),
+        "tf_world_body_count": ([P, C.POINTER(C.c_int64)], C.c_int),
+        "tf_world_get_states": ([P, P, P, P, P, P], C.c_int),
+        "tf_world_contacts": ([P, C.c_int32, C.c_int32, C.POINTER(tf_contact), C.c_int32, C.POINTER(C.c_int32)],
+                              C.c_int),
+        "tf_world_candidates": ([P, C.c_int32, P, C.c_int32, C.POINTER(C.c_int32)], C.c_int),
+        "tf_world_profile": ([P, C.c_int32, C.POINTER(tf_profile)], C.c_int),
+        "tf_world_awake_bodies": ([P, C.POINTER(C.c_int64)], C.c_int),
+        "tf_world_launch_count": ([P, C.POINTER(C.c_int64)], C.c_int),
+    }
+    for name, (args, res) in sig.items():
+        f = getattr(lib, name)
+        f.argtypes = args
+        f.restype = res
+    return lib
+
+
+# Every symbol include/twofold_b200.h declares.
+EXPORTED = [
+    "tf_abi_version", "tf_last_error", "tf_default_settings", "tf_world_create", "tf_world_destroy",
+    "tf_world_count", "tf_world_set_settings", "tf_body_create", "tf_shape_add", "tf_bodies_create",
+    "tf_shapes_add", "tf_world_step", "tf_world_step_graph", "tf_world_synchronize", "tf_world_device_status",
+    "tf_body_get_state", "tf_body_set_velocity", "tf_body_get_mass", "tf_body_is_awake", "tf_world_body_count",
+    "tf_world_get_states", "tf_world_contacts", "tf_world_candidates", "tf_world_profile", "tf_world_awake_bodies",
+    "tf_world_launch_count",
+]
+
+
+def load():
+    """Loads the in-tree CUDA library. Raises if it was not built: there is no other implementation."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing; build it with twofold_b200.build.build()")
+        _lib = _declare(C.CDLL(LIB_PATH))
+    return _lib
+
+
+def check(rc, lib=None):
+    if rc != TF_OK:
+        lib = lib or load()
+        msg = lib.tf_last_error()
+        raise RuntimeError(f"twofold_b200 error {rc}: {msg.decode() if msg else ''}")

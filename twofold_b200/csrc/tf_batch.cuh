@@ -1,0 +1,55 @@
+// Every device array of a batch, passed by value to each kernel.
+#pragma once
+
+#include "tf_collide.cuh"
+#include "tf_types.cuh"
+
+namespace tfb {
+
+struct Batch {
+    int nWorlds;
+    const uint32_t* order;  // worlds, largest first; CTA k takes order[k], order[k + gridDim.x], ...
+    const WorldInfo* info;
+    WorldCounts* counts;
+
+    DBody* bodies;
+    DShape* shapes;
+    const uint32_t* shapeList;  // per body, its shapes (global indices)
+    const uint32_t* planeList;  // per world, its half-space shapes (global indices)
+    CollideCtx cx;
+
+    // Per body.
+    float* grow;
+    uint32_t* bodyColors;
+    uint8_t* struck;
+    uint8_t* wakeMark;
+    uint32_t* unionParent;
+    float* islandTime;
+
+    // Per candidate (candFirst + i).
+    uint64_t* cand;
+    DContact* stage;
+    uint8_t* stageUsed;
+
+    // Per contact slot (contactFirst + i). Contacts double-buffer across steps.
+    DContact* contacts;   // current
+    DContact* previous;   // last step's, read while the current list is built
+    uint32_t* active;
+    uint32_t* impact;
+    uint32_t* colored;        // active contacts grouped by color
+    uint32_t* impactColored;
+    uint32_t* rest;           // active contacts solved one at a time, in active order
+    uint32_t* impactRest;
+    uint8_t* color;           // by contact
+    uint8_t* cflags;          // by contact: kFast, kFastSolid
+    uint64_t* mergeKeyA;
+    uint32_t* mergePartA;
+    uint32_t* mergeIdxA;
+    uint64_t* mergeKeyB;
+    uint32_t* mergePartB;
+    uint32_t* mergeIdxB;
+};
+
+constexpr uint8_t kFlagFast = 1, kFlagFastSolid = 2, kFlagActive = 4;
+
+}

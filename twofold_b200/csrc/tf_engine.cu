@@ -1,0 +1,1139 @@
+// Host side of the library: the C ABI (include/twofold_b200.h), host mirrors of every world, the device
+// arena and the per-step kernel sequence.
+//
+// Host mirrors are authoritative until the first step; afterwards the device holds the dynamic state and
+// the mirrors are refreshed from it on demand. A structural change (a body or shape added after stepping)
+// pulls the device state back, rebuilds the layout and pushes everything again, contacts included, so
+// warm starting survives it.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/twofold_b200.h"
+#include "tf_build.h"
+#include "tf_kernels.cuh"
+
+namespace tfb {
+
+namespace {
+
+thread_local std::string g_error;
+
+int fail(int code, const std::string& msg) {
+    g_error = msg;
+    return code;
+}
+
+#define TF_CUDA(call)                                                                                    \
+    do {                                                                                                 \
+        cudaError_t e_ = (call);                                                                         \
+        if (e_ != cudaSuccess) { return fail(TF_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); } \
+    } while (0)
+
+constexpr float kTreeMargin = 0.1f;
+constexpr float kFeatureTurn = 0.1f;
+
+struct HostBody {
+    DBody d{};
+    uint32_t generation = 0;
+    std::vector<uint32_t> shapes;  // world-local shape indices
+    bool massOverride = false;
+    MassProps overrideMass;
+};
+
+struct HostWorld {
+    std::vector<HostBody> bodies;
+    std::vector<uint32_t> freeBodies;
+    std::vector<HostShape> shapes;
+    std::vector<uint32_t> freeShapes;
+    std::vector<uint32_t> planes;  // half-space shapes in the order they were tracked
+    std::vector<DContact> contacts;  // last pulled from the device (world-local indices)
+};
+
+// One device allocation per array; sized at layout time.
+template <class T>
+struct DevArray {
+    T* ptr = nullptr;
+    size_t n = 0;
+    int alloc(size_t count) {
+        if (count <= n && ptr) { return TF_OK; }
+        if (ptr) { cudaFree(ptr); }
+        ptr = nullptr;
+        n = 0;
+        const size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
+        cudaError_t e = cudaMalloc(&ptr, bytes);
+        if (e != cudaSuccess) { return fail(TF_E_CUDA, std::string("cudaMalloc: ") + cudaGetErrorString(e)); }
+        n = std::max<size_t>(count, 1);
+        return TF_OK;
+    }
+    void release() {
+        if (ptr) { cudaFree(ptr); }
+        ptr = nullptr;
+        n = 0;
+    }
+};
+
+Vec3 v3of(const float* p) { return { p[0], p[1], p[2] }; }
+Quat q4of(const float* p) { return { p[0], p[1], p[2], p[3] }; }
+
+}  // namespace
+
+class Engine {
+public:
+    tf_settings settings{};
+    int device = 0;
+    std::vector<HostWorld> worlds;
+    cudaStream_t stream = nullptr;
+    int smCount = 148;
+    int blockSize = 128;
+    int64_t launches = 0;
+
+    bool layoutDirty = true;   // device arrays do not match the mirrors' structure
+    bool bodiesDirty = true;   // host body state newer than the device's
+    bool onDevice = false;     // the device holds the newest dynamic state
+    bool hostFresh = true;     // host mirrors hold the newest dynamic state
+    std::vector<tf_profile> profiles;
+
+    // Layout.
+    std::vector<WorldInfo> info;
+    std::vector<uint32_t> order;
+    std::vector<uint32_t> bodyBase, shapeBase;
+    size_t totalBodies = 0, totalShapes = 0, totalCand = 0, totalContacts = 0;
+    uint32_t sortCap = 0;
+    float capFactor = 6.0f;
+    BoxTopology boxTopology{};
+
+    // Device arrays.
+    DevArray<WorldInfo> dInfo;
+    DevArray<WorldCounts> dCounts;
+    DevArray<uint32_t> dOrder;
+    DevArray<DBody> dBodies;
+    DevArray<DShape> dShapes;
+    DevArray<uint32_t> dShapeList, dPlaneList;
+    DevArray<DPoly> dPolys;
+    DevArray<Vec3> dVerts, dNormals, dArcs;
+    DevArray<int32_t> dIndices;
+    DevArray<DFace> dFaces;
+    DevArray<float> dOffsets;
+    DevArray<DEdge> dEdges;
+    DevArray<float> dGrow, dIslandTime;
+    DevArray<uint32_t> dBodyColors, dUnionParent;
+    DevArray<uint8_t> dStruck, dWakeMark;
+    DevArray<uint64_t> dCand;
+    DevArray<DContact> dStage;
+    DevArray<uint8_t> dStageUsed;
+    DevArray<DContact> dContacts[2];
+    int cur = 0;
+    DevArray<uint32_t> dActive, dImpact, dColored, dImpactColored, dRest, dImpactRest;
+    DevArray<uint8_t> dColor, dCflags;
+    DevArray<uint64_t> dMergeKeyA, dMergeKeyB;
+    DevArray<uint32_t> dMergePartA, dMergePartB, dMergeIdxA, dMergeIdxB;
+
+    // Graph replay.
+    cudaGraphExec_t graphExec = nullptr;
+    int graphSteps = 0;
+    float graphDt = 0.0f;
+
+    ~Engine() {
+        if (graphExec) { cudaGraphExecDestroy(graphExec); }
+        if (stream) { cudaStreamDestroy(stream); }
+    }
+
+    int init(const tf_settings* s, int nWorlds, int dev) {
+        settings = *s;
+        device = dev;
+        worlds.resize((size_t)nWorlds);
+        profiles.assign((size_t)nWorlds, tf_profile{});
+        // Box face and edge numbering from a unit box, as the reference derives it (src/collide3d.cpp:456-476).
+        const HostPoly p = makeBox({ 1.0f, 1.0f, 1.0f });
+        for (int f = 0; f < (int)p.normals.size(); ++f) {
+            const float n[3] = { p.normals[f].x, p.normals[f].y, p.normals[f].z };
+            for (int k = 0; k < 3; ++k) {
+                if (std::fabs(n[k]) > 0.5f) { boxTopology.face[k][n[k] > 0.0f] = f; }
+            }
+        }
+        auto edgeBetween = [&](int f0, int f1) {
+            for (size_t i = 0; i < p.edges.size(); ++i) {
+                const DEdge& e = p.edges[i];
+                if ((e.f0 == f0 && e.f1 == f1) || (e.f0 == f1 && e.f1 == f0)) { return (int)i; }
+            }
+            return -1;
+        };
+        for (int i = 0; i < 3; ++i) {
+            for (int s1 = 0; s1 < 2; ++s1) {
+                for (int s2 = 0; s2 < 2; ++s2) {
+                    boxTopology.edge[i][s1][s2] = edgeBetween(boxTopology.face[(i + 1) % 3][s1], boxTopology.face[(i + 2) % 3][s2]);
+                }
+            }
+        }
+        return TF_OK;
+    }
+
+    // CUDA is first touched by the first step, so scenes can be built and inspected without a device.
+    int ensureDevice() {
+        if (stream) { return TF_OK; }
+        TF_CUDA(cudaSetDevice(device));
+        TF_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+        TF_CUDA(cudaDeviceGetAttribute(&smCount, cudaDevAttrMultiProcessorCount, device));
+        return TF_OK;
+    }
+
+    // ---- host-side world building (src/world.cpp:1751-1857) ----
+
+    void hostShapeBounds(HostShape& s, const Transform& xf) {
+        DPoly poly{};
+        PolyTables pt{};
+        if (s.hasPoly) {
+            poly.vFirst = 0;
+            poly.vCount = (int)s.poly.vertices.size();
+            pt.polys = &poly;
+            pt.verts = s.poly.vertices.data();
+        }
+        DShape d = s.d;
+        d.poly = 0;
+        shapeBounds(d, pt, xf, s.d.lo, s.d.hi);
+    }
+
+    // Shape bounds and the body's union (Impl::bound, src/world.cpp:244-258).
+    bool bound(HostWorld& W, HostBody& hb) {
+        bool any = false;
+        DBody& b = hb.d;
+        for (uint32_t si : hb.shapes) {
+            HostShape& s = W.shapes[si];
+            hostShapeBounds(s, b.xf * s.d.local);
+            if (s.d.kind == kHalfSpace) { continue; }
+            b.lo = any ? minVec(b.lo, s.d.lo) : s.d.lo;
+            b.hi = any ? maxVec(b.hi, s.d.hi) : s.d.hi;
+            any = true;
+        }
+        b.hasBounds = any ? 1u : 0u;
+        return any;
+    }
+
+    // src/world.cpp:439-479.
+    void updateMass(HostWorld& W, HostBody& hb) {
+        DBody& b = hb.d;
+        MassProps mp;
+        if (hb.massOverride) {
+            mp = hb.overrideMass;
+        } else {
+            Vec3 weighted{ 0, 0, 0 };
+            std::vector<MassProps> parts;
+            for (uint32_t si : hb.shapes) {
+                const HostShape& s = W.shapes[si];
+                if (s.d.sensor) { continue; }
+                const MassProps sm = shapeMass(s);
+                if (sm.mass <= 0.0f) { continue; }
+                mp.mass += sm.mass;
+                weighted += sm.center * sm.mass;
+                parts.push_back(sm);
+            }
+            if (mp.mass > 0.0f) {
+                mp.center = weighted / mp.mass;
+                for (const MassProps& sm : parts) {
+                    const Vec3 d = sm.center - mp.center;
+                    const float dd = dot(d, d);
+                    mp.inertia = mp.inertia + sm.inertia + (mdiag({ dd, dd, dd }) - outer(d, d)) * sm.mass;
+                }
+            }
+        }
+        b.localCenter = mp.center;
+        b.mass = mp.mass;
+        b.inertia = mp.inertia;
+        if (b.type == kDynamic && b.mass <= 0.0f) {
+            b.mass = 1.0f;
+            b.inertia = mid();
+        }
+        b.invMass = (b.type == kDynamic && b.mass > 0.0f) ? 1.0f / b.mass : 0.0f;
+        b.com = apply(b.xf, b.localCenter);
+        b.extent = 0.0f;
+        for (uint32_t si : hb.shapes) {
+            const HostShape& s = W.shapes[si];
+            if (s.d.kind == kHalfSpace || s.d.sensor) { continue; }
+            b.extent = maxf(b.extent, s.d.extent + length(s.d.local.p - b.localCenter));
+        }
+        updateInverseMass(b);
+    }
+
+    int createBody(int w, const tf_body_desc* d, tf_id* out) {
+        if (w < 0 || w >= (int)worlds.size() || !d) { return fail(TF_E_INVALID, "createBody: bad world or descriptor"); }
+        if (d->type < 0 || d->type > 2) { return fail(TF_E_INVALID, "createBody: bad motion type"); }
+        if ((d->locks & kLockPlanar) == kLockPlanar) {
+            return fail(TF_E_UNSUPPORTED, "createBody: bodies locked to a plane are not run by this build");
+        }
+        int rc = pull();
+        if (rc != TF_OK) { return rc; }
+        HostWorld& W = worlds[(size_t)w];
+        uint32_t i;
+        if (!W.freeBodies.empty()) {
+            i = W.freeBodies.back();
+            W.freeBodies.pop_back();
+        } else {
+            i = (uint32_t)W.bodies.size();
+            W.bodies.emplace_back();
+        }
+        HostBody& hb = W.bodies[i];
+        const uint32_t gen = hb.generation;
+        hb = HostBody{};
+        hb.generation = gen;
+        DBody& b = hb.d;
+        b.alive = 1;
+        b.type = (uint32_t)d->type;
+        b.xf = { v3of(d->position), normalize(q4of(d->rotation)) };
+        b.v = d->type == TF_STATIC ? zero3() : v3of(d->linear_velocity);
+        b.w = d->type == TF_STATIC ? zero3() : v3of(d->angular_velocity);
+        b.linearDamping = d->linear_damping;
+        b.angularDamping = d->angular_damping;
+        b.gravityScale = d->gravity_scale;
+        b.locks = d->locks & 0x3fu;
+        b.lockFrame = normalize(q4of(d->lock_frame));
+        b.awake = d->awake ? 1u : 0u;
+        b.canSleep = d->can_sleep ? 1u : 0u;
+        b.kept = 1.0f;
+        b.island = UINT32_MAX;
+        b.dq = qid();
+        b.qBase = qid();
+        b.q0 = qid();
+        b.linearProj = mid();
+        b.angularProj = mid();
+        updateMass(W, hb);
+        b.v = b.linearProj * b.v;
+        b.w = b.angularProj * b.w;
+        layoutDirty = true;
+        if (out) { *out = { i, hb.generation }; }
+        return TF_OK;
+    }
+
+    HostBody* body(int w, tf_id id) {
+        if (w < 0 || w >= (int)worlds.size()) { return nullptr; }
+        HostWorld& W = worlds[(size_t)w];
+        if (id.index >= W.bodies.size()) { return nullptr; }
+        HostBody& b = W.bodies[id.index];
+        return (b.d.alive && b.generation == id.generation) ? &b : nullptr;
+    }
+
+    int addShape(int w, tf_id bid, const tf_shape_desc* d, tf_id* out) {
+        if (out) { *out = { UINT32_MAX, 0 }; }
+        if (!d) { return fail(TF_E_INVALID, "addShape: null descriptor"); }
+        int rc = pull();
+        if (rc != TF_OK) { return rc; }
+        HostBody* hb = body(w, bid);
+        if (!hb) { return TF_OK; }  // invalid handle: nothing happens, as in the reference
+        HostWorld& W = worlds[(size_t)w];
+        HostShape s;
+        s.d.alive = 1;
+        s.d.body = bid.index;
+        s.d.local = { v3of(d->position), normalize(q4of(d->rotation)) };
+        s.density = d->density;
+        s.d.friction = d->friction;
+        s.d.restitution = d->restitution;
+        s.d.rollingResistance = d->rolling_resistance;
+        s.d.category = d->category;
+        s.d.mask = d->mask;
+        s.d.sensor = d->sensor ? 1u : 0u;
+        s.d.poly = -1;
+        if (!buildShapeGeometry(s, d->geometry, d->radius, v3of(d->half_extents))) {
+            return fail(TF_E_UNSUPPORTED, "addShape: only spheres, boxes and half-spaces are run by this build");
+        }
+        if (s.d.sensor) { return fail(TF_E_UNSUPPORTED, "addShape: sensors are not run by this build"); }
+        if (s.d.kind == kHalfSpace && hb->d.type != kStatic) {
+            return fail(TF_E_UNSUPPORTED, "addShape: half-spaces belong to static bodies");
+        }
+        uint32_t i;
+        if (!W.freeShapes.empty()) {
+            i = W.freeShapes.back();
+            W.freeShapes.pop_back();
+        } else {
+            i = (uint32_t)W.shapes.size();
+            W.shapes.emplace_back();
+        }
+        const uint32_t gen = W.shapes[i].generation;
+        s.generation = gen;
+        s.d.index = i;
+        W.shapes[i] = s;
+        hb->shapes.push_back(i);
+        if (s.d.kind == kHalfSpace) { W.planes.push_back(i); }
+        bound(W, *hb);
+        updateMass(W, *hb);
+        layoutDirty = true;
+        if (out) { *out = { i, gen }; }
+        return TF_OK;
+    }
+
+    // ---- layout and transfer ----
+
+    // Brings the device's dynamic state and contacts back into the host mirrors.
+    int pull() {
+        if (!onDevice || hostFresh) { return TF_OK; }
+        TF_CUDA(cudaStreamSynchronize(stream));
+        std::vector<DBody> bodies(totalBodies);
+        std::vector<DShape> shapes(totalShapes);
+        std::vector<WorldCounts> counts(worlds.size());
+        TF_CUDA(cudaMemcpy(bodies.data(), dBodies.ptr, totalBodies * sizeof(DBody), cudaMemcpyDeviceToHost));
+        TF_CUDA(cudaMemcpy(shapes.data(), dShapes.ptr, totalShapes * sizeof(DShape), cudaMemcpyDeviceToHost));
+        TF_CUDA(cudaMemcpy(counts.data(), dCounts.ptr, worlds.size() * sizeof(WorldCounts), cudaMemcpyDeviceToHost));
+        for (size_t w = 0; w < worlds.size(); ++w) {
+            HostWorld& W = worlds[w];
+            const WorldInfo& wi = info[w];
+            for (size_t i = 0; i < W.bodies.size(); ++i) {
+                DBody d = bodies[wi.bodyFirst + i];
+                // Keep the host's own bookkeeping fields.
+                d.shapeFirst = W.bodies[i].d.shapeFirst;
+                d.shapeCount = W.bodies[i].d.shapeCount;
+                d.world = W.bodies[i].d.world;
+                W.bodies[i].d = d;
+            }
+            for (size_t i = 0; i < W.shapes.size(); ++i) {
+                W.shapes[i].d.lo = shapes[wi.shapeFirst + i].lo;
+                W.shapes[i].d.hi = shapes[wi.shapeFirst + i].hi;
+            }
+            const uint32_t nc = std::min(counts[w].contactCount, wi.contactCap);
+            W.contacts.resize(nc);
+            if (nc) {
+                TF_CUDA(cudaMemcpy(W.contacts.data(), dContacts[cur].ptr + wi.contactFirst, nc * sizeof(DContact),
+                                   cudaMemcpyDeviceToHost));
+            }
+            for (DContact& c : W.contacts) {
+                c.bodyA -= wi.bodyFirst;
+                c.bodyB -= wi.bodyFirst;
+                c.shapeA -= wi.shapeFirst;
+                c.shapeB -= wi.shapeFirst;
+            }
+        }
+        hostFresh = true;
+        return TF_OK;
+    }
+
+    int layout() {
+        if (graphExec) {
+            cudaGraphExecDestroy(graphExec);
+            graphExec = nullptr;
+        }
+        const size_t nw = worlds.size();
+        info.assign(nw, WorldInfo{});
+        size_t nb = 0, ns = 0, ncand = 0, ncon = 0, nplanes = 0;
+        std::vector<DPoly> polys;
+        std::vector<Vec3> verts, normals, arcs;
+        std::vector<int32_t> indices;
+        std::vector<DFace> faces;
+        std::vector<float> offsets;
+        std::vector<DEdge> edges;
+        uint32_t maxCap = 0;
+        for (size_t w = 0; w < nw; ++w) {
+            const HostWorld& W = worlds[w];
+            WorldInfo& wi = info[w];
+            wi.bodyFirst = (uint32_t)nb;
+            wi.bodyCount = (uint32_t)W.bodies.size();
+            wi.shapeFirst = (uint32_t)ns;
+            wi.shapeCount = (uint32_t)W.shapes.size();
+            wi.planeFirst = (uint32_t)nplanes;
+            wi.planeCount = (uint32_t)W.planes.size();
+            const uint32_t cap = (uint32_t)std::ceil(capFactor * (float)W.shapes.size()) + 64u;
+            wi.candFirst = (uint32_t)ncand;
+            wi.candCap = cap;
+            wi.contactFirst = (uint32_t)ncon;
+            wi.contactCap = std::max<uint32_t>(cap + 64u, (uint32_t)W.contacts.size() + 64u);
+            nb += wi.bodyCount;
+            ns += wi.shapeCount;
+            nplanes += wi.planeCount;
+            ncand += wi.candCap;
+            ncon += wi.contactCap;
+            maxCap = std::max(maxCap, cap);
+        }
+        totalBodies = nb;
+        totalShapes = ns;
+        totalCand = ncand;
+        totalContacts = ncon;
+        std::vector<DBody> bodies(nb);
+        std::vector<DShape> shapes(ns);
+        std::vector<uint32_t> shapeList(ns), planeList(std::max<size_t>(nplanes, 1));
+        std::vector<DContact> contacts(ncon);
+        std::vector<WorldCounts> counts(nw);
+        for (size_t w = 0; w < nw; ++w) {
+            HostWorld& W = worlds[w];
+            const WorldInfo& wi = info[w];
+            uint32_t listPos = wi.shapeFirst;
+            for (size_t i = 0; i < W.bodies.size(); ++i) {
+                HostBody& hb = W.bodies[i];
+                DBody d = hb.d;
+                d.shapeFirst = listPos;
+                d.shapeCount = (uint32_t)hb.shapes.size();
+                d.world = (uint32_t)w;
+                for (uint32_t si : hb.shapes) { shapeList[listPos++] = wi.shapeFirst + si; }
+                hb.d.shapeFirst = d.shapeFirst;
+                hb.d.shapeCount = d.shapeCount;
+                hb.d.world = d.world;
+                bodies[wi.bodyFirst + i] = d;
+            }
+            for (size_t i = 0; i < W.shapes.size(); ++i) {
+                const HostShape& s = W.shapes[i];
+                DShape d = s.d;
+                d.body = wi.bodyFirst + s.d.body;
+                d.poly = -1;
+                if (s.hasPoly && s.d.alive) {
+                    DPoly p{};
+                    p.vFirst = (int32_t)verts.size();
+                    p.vCount = (int32_t)s.poly.vertices.size();
+                    p.fFirst = (int32_t)normals.size();
+                    p.fCount = (int32_t)s.poly.faces.size();
+                    p.eFirst = (int32_t)edges.size();
+                    p.eCount = (int32_t)s.poly.edges.size();
+                    p.iFirst = (int32_t)indices.size();
+                    p.iCount = (int32_t)s.poly.indices.size();
+                    p.centroid = s.poly.centroid;
+                    p.lo = s.poly.lo;
+                    p.hi = s.poly.hi;
+                    verts.insert(verts.end(), s.poly.vertices.begin(), s.poly.vertices.end());
+                    normals.insert(normals.end(), s.poly.normals.begin(), s.poly.normals.end());
+                    offsets.insert(offsets.end(), s.poly.offsets.begin(), s.poly.offsets.end());
+                    faces.insert(faces.end(), s.poly.faces.begin(), s.poly.faces.end());
+                    edges.insert(edges.end(), s.poly.edges.begin(), s.poly.edges.end());
+                    arcs.insert(arcs.end(), s.poly.arcs.begin(), s.poly.arcs.end());
+                    indices.insert(indices.end(), s.poly.indices.begin(), s.poly.indices.end());
+                    d.poly = (int32_t)polys.size();
+                    polys.push_back(p);
+                }
+                shapes[wi.shapeFirst + i] = d;
+            }
+            for (size_t k = 0; k < W.planes.size(); ++k) { planeList[wi.planeFirst + k] = wi.shapeFirst + W.planes[k]; }
+            for (size_t k = 0; k < W.contacts.size() && k < wi.contactCap; ++k) {
+                DContact c = W.contacts[k];
+                c.bodyA += wi.bodyFirst;
+                c.bodyB += wi.bodyFirst;
+                c.shapeA += wi.shapeFirst;
+                c.shapeB += wi.shapeFirst;
+                contacts[wi.contactFirst + k] = c;
+            }
+            counts[w] = WorldCounts{};
+            counts[w].contactCount = (uint32_t)std::min<size_t>(W.contacts.size(), wi.contactCap);
+        }
+        order.resize(nw);
+        for (size_t w = 0; w < nw; ++w) { order[w] = (uint32_t)w; }
+        std::stable_sort(order.begin(), order.end(),
+                         [&](uint32_t a, uint32_t b) { return info[a].bodyCount > info[b].bodyCount; });
+        sortCap = 1;
+        while (sortCap < maxCap) { sortCap <<= 1; }
+        sortCap = std::min<uint32_t>(sortCap, 8192u);
+
+        int rc;
+#define TF_ALLOC(arr, count) \
+    if ((rc = (arr).alloc(count)) != TF_OK) { return rc; }
+        TF_ALLOC(dInfo, nw);
+        TF_ALLOC(dCounts, nw);
+        TF_ALLOC(dOrder, nw);
+        TF_ALLOC(dBodies, nb);
+        TF_ALLOC(dShapes, ns);
+        TF_ALLOC(dShapeList, ns);
+        TF_ALLOC(dPlaneList, planeList.size());
+        TF_ALLOC(dPolys, polys.size());
+        TF_ALLOC(dVerts, verts.size());
+        TF_ALLOC(dNormals, normals.size());
+        TF_ALLOC(dArcs, arcs.size());
+        TF_ALLOC(dIndices, indices.size());
+        TF_ALLOC(dFaces, faces.size());
+        TF_ALLOC(dOffsets, offsets.size());
+        TF_ALLOC(dEdges, edges.size());
+        TF_ALLOC(dGrow, nb);
+        TF_ALLOC(dIslandTime, nb);
+        TF_ALLOC(dBodyColors, nb);
+        TF_ALLOC(dUnionParent, nb);
+        TF_ALLOC(dStruck, nb);
+        TF_ALLOC(dWakeMark, nb);
+        TF_ALLOC(dCand, ncand);
+        TF_ALLOC(dStage, ncand);
+        TF_ALLOC(dStageUsed, ncand);
+        TF_ALLOC(dContacts[0], ncon);
+        TF_ALLOC(dContacts[1], ncon);
+        TF_ALLOC(dActive, ncon);
+        TF_ALLOC(dImpact, ncon);
+        TF_ALLOC(dColored, ncon);
+        TF_ALLOC(dImpactColored, ncon);
+        TF_ALLOC(dRest, ncon);
+        TF_ALLOC(dImpactRest, ncon);
+        TF_ALLOC(dColor, ncon);
+        TF_ALLOC(dCflags, ncon);
+        TF_ALLOC(dMergeKeyA, ncon);
+        TF_ALLOC(dMergeKeyB, ncon);
+        TF_ALLOC(dMergePartA, ncon);
+        TF_ALLOC(dMergePartB, ncon);
+        TF_ALLOC(dMergeIdxA, ncon);
+        TF_ALLOC(dMergeIdxB, ncon);
+#undef TF_ALLOC
+        auto up = [&](void* dst, const void* src, size_t bytes) -> int {
+            if (bytes == 0) { return TF_OK; }
+            cudaError_t e = cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice);
+            if (e != cudaSuccess) { return fail(TF_E_CUDA, std::string("upload: ") + cudaGetErrorString(e)); }
+            return TF_OK;
+        };
+        cur = 0;
+        if ((rc = up(dInfo.ptr, info.data(), nw * sizeof(WorldInfo))) != TF_OK) { return rc; }
+        if ((rc = up(dCounts.ptr, counts.data(), nw * sizeof(WorldCounts))) != TF_OK) { return rc; }
+        if ((rc = up(dOrder.ptr, order.data(), nw * sizeof(uint32_t))) != TF_OK) { return rc; }
+        if ((rc = up(dBodies.ptr, bodies.data(), nb * sizeof(DBody))) != TF_OK) { return rc; }
+        if ((rc = up(dShapes.ptr, shapes.data(), ns * sizeof(DShape))) != TF_OK) { return rc; }
+        if ((rc = up(dShapeList.ptr, shapeList.data(), ns * sizeof(uint32_t))) != TF_OK) { return rc; }
+        if ((rc = up(dPlaneList.ptr, planeList.data(), planeList.size() * sizeof(uint32_t))) != TF_OK) { return rc; }
+        if ((rc = up(dPolys.ptr, polys.data(), polys.size() * sizeof(DPoly))) != TF_OK) { return rc; }
+        if ((rc = up(dVerts.ptr, verts.data(), verts.size() * sizeof(Vec3))) != TF_OK) { return rc; }
+        if ((rc = up(dNormals.ptr, normals.data(), normals.size() * sizeof(Vec3))) != TF_OK) { return rc; }
+        if ((rc = up(dArcs.ptr, arcs.data(), arcs.size() * sizeof(Vec3))) != TF_OK) { return rc; }
+        if ((rc = up(dIndices.ptr, indices.data(), indices.size() * sizeof(int32_t))) != TF_OK) { return rc; }
+        if ((rc = up(dFaces.ptr, faces.data(), faces.size() * sizeof(DFace))) != TF_OK) { return rc; }
+        if ((rc = up(dOffsets.ptr, offsets.data(), offsets.size() * sizeof(float))) != TF_OK) { return rc; }
+        if ((rc = up(dEdges.ptr, edges.data(), edges.size() * sizeof(DEdge))) != TF_OK) { return rc; }
+        if ((rc = up(dContacts[0].ptr, contacts.data(), ncon * sizeof(DContact))) != TF_OK) { return rc; }
+        TF_CUDA(cudaMemset(dWakeMark.ptr, 0, nb));
+        layoutDirty = false;
+        bodiesDirty = false;
+        onDevice = true;
+        hostFresh = true;
+        return TF_OK;
+    }
+
+    // Pushes host body state (after a setter) without changing the layout.
+    int pushBodies() {
+        std::vector<DBody> bodies(totalBodies);
+        for (size_t w = 0; w < worlds.size(); ++w) {
+            for (size_t i = 0; i < worlds[w].bodies.size(); ++i) { bodies[info[w].bodyFirst + i] = worlds[w].bodies[i].d; }
+        }
+        TF_CUDA(cudaMemcpy(dBodies.ptr, bodies.data(), totalBodies * sizeof(DBody), cudaMemcpyHostToDevice));
+        bodiesDirty = false;
+        return TF_OK;
+    }
+
+    int prepareDevice() {
+        const int rc0 = ensureDevice();
+        if (rc0 != TF_OK) { return rc0; }
+        if (layoutDirty) {
+            int rc = pull();
+            if (rc != TF_OK) { return rc; }
+            return layout();
+        }
+        if (bodiesDirty) { return pushBodies(); }
+        return TF_OK;
+    }
+
+    StepParams params(float dt) const {
+        StepParams P{};
+        const tf_settings& s = settings;
+        const int n = std::max(1, (int)s.substeps);
+        P.gravity = v3of(s.gravity);
+        P.lengthUnit = s.length_unit;
+        P.substeps = n;
+        P.dt = dt;
+        P.h = dt / (float)n;
+        P.invH = 1.0f / P.h;
+        const float hertz = minf(s.contact_hertz, 0.25f * P.invH);
+        P.contactSoft = makeSoft(hertz, s.contact_damping_ratio, P.h);
+        P.staticSoft = makeSoft(2.0f * hertz, s.contact_damping_ratio, P.h);
+        P.maxPushout = s.max_pushout_speed * s.length_unit;
+        P.restitutionThreshold = s.restitution_threshold * s.length_unit;
+        P.maxLinearSpeed = s.max_linear_speed * s.length_unit;
+        P.maxAngularSpeed = s.max_angular_speed;
+        P.sleepThreshold = s.sleep_threshold * s.length_unit;
+        P.timeToSleep = s.time_to_sleep;
+        P.reuseDistance = s.contact_reuse_distance * s.length_unit;
+        P.reuseCos = std::cos(0.5f * s.contact_reuse_angle);
+        P.featureTurnCos = std::cos(0.5f * kFeatureTurn);
+        P.treeMargin = kTreeMargin * s.length_unit;
+        P.tol.linearSlop = 0.005f * s.length_unit;
+        P.tol.speculative = 4.0f * P.tol.linearSlop;
+        P.continuous = s.continuous;
+        return P;
+    }
+
+    Batch batch(int cur_) {
+        Batch B{};
+        B.nWorlds = (int)worlds.size();
+        B.order = dOrder.ptr;
+        B.info = dInfo.ptr;
+        B.counts = dCounts.ptr;
+        B.bodies = dBodies.ptr;
+        B.shapes = dShapes.ptr;
+        B.shapeList = dShapeList.ptr;
+        B.planeList = dPlaneList.ptr;
+        B.cx.pt = { dPolys.ptr, dVerts.ptr, dIndices.ptr, dFaces.ptr, dNormals.ptr, dOffsets.ptr, dEdges.ptr, dArcs.ptr };
+        B.cx.boxes = boxTopology;
+        B.grow = dGrow.ptr;
+        B.bodyColors = dBodyColors.ptr;
+        B.struck = dStruck.ptr;
+        B.wakeMark = dWakeMark.ptr;
+        B.unionParent = dUnionParent.ptr;
+        B.islandTime = dIslandTime.ptr;
+        B.cand = dCand.ptr;
+        B.stage = dStage.ptr;
+        B.stageUsed = dStageUsed.ptr;
+        B.contacts = dContacts[cur_].ptr;
+        B.previous = dContacts[1 - cur_].ptr;
+        B.active = dActive.ptr;
+        B.impact = dImpact.ptr;
+        B.colored = dColored.ptr;
+        B.impactColored = dImpactColored.ptr;
+        B.rest = dRest.ptr;
+        B.impactRest = dImpactRest.ptr;
+        B.color = dColor.ptr;
+        B.cflags = dCflags.ptr;
+        B.mergeKeyA = dMergeKeyA.ptr;
+        B.mergePartA = dMergePartA.ptr;
+        B.mergeIdxA = dMergeIdxA.ptr;
+        B.mergeKeyB = dMergeKeyB.ptr;
+        B.mergePartB = dMergePartB.ptr;
+        B.mergeIdxB = dMergeIdxB.ptr;
+        return B;
+    }
+
+    // Issues one step on the stream: the new contact list goes into buffer `into`, the old one is read from
+    // the other buffer.
+    int enqueueStep(float dt, int into, cudaEvent_t* marks) {
+        const StepParams P = params(dt);
+        Batch B = batch(into);
+        B.cx.tol = P.tol;
+        const int grid = (int)std::min<size_t>(worlds.size(), (size_t)smCount * 8);
+        const int tb = blockSize;
+        const size_t sortBytes = (size_t)sortCap * sizeof(uint64_t);
+        if (marks) { cudaEventRecord(marks[0], stream); }
+        k_broadphase<<<grid, tb, sortBytes, stream>>>(B, P, sortCap);
+        if (marks) { cudaEventRecord(marks[1], stream); }
+        k_narrowphase<<<grid, tb, 0, stream>>>(B, P);
+        k_wake<<<grid, 32, 0, stream>>>(B);
+        if (marks) { cudaEventRecord(marks[2], stream); }
+        k_prepare<<<grid, tb, 0, stream>>>(B, P);
+        for (int i = 0; i < P.substeps; ++i) { k_substep<<<grid, tb, 0, stream>>>(B, P, i); }
+        k_finish<<<grid, tb, 0, stream>>>(B, P);
+        if (marks) { cudaEventRecord(marks[3], stream); }
+        launches += 5 + P.substeps;
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) { return fail(TF_E_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e)); }
+        return TF_OK;
+    }
+
+    int configureKernels() {
+        static bool done = false;
+        if (done) { return TF_OK; }
+        TF_CUDA(cudaFuncSetAttribute(k_broadphase, cudaFuncAttributeMaxDynamicSharedMemorySize, 8192 * 8));
+        done = true;
+        return TF_OK;
+    }
+
+    int step(float dt, int nSteps) {
+        if (!(dt > 0.0f) || !std::isfinite(dt) || nSteps <= 0) { return TF_OK; }
+        TF_CUDA(cudaSetDevice(device));
+        int rc = configureKernels();
+        if (rc != TF_OK) { return rc; }
+        rc = prepareDevice();
+        if (rc != TF_OK) { return rc; }
+        cudaEvent_t marks[4];
+        for (cudaEvent_t& e : marks) { TF_CUDA(cudaEventCreate(&e)); }
+        for (int s = 0; s < nSteps; ++s) {
+            const int into = 1 - cur;
+            rc = enqueueStep(dt, into, s == nSteps - 1 ? marks : nullptr);
+            if (rc != TF_OK) { break; }
+            cur = into;
+        }
+        hostFresh = false;
+        cudaError_t e = cudaStreamSynchronize(stream);
+        if (e == cudaSuccess) {
+            float bp = 0, np = 0, sv = 0;
+            cudaEventElapsedTime(&bp, marks[0], marks[1]);
+            cudaEventElapsedTime(&np, marks[1], marks[2]);
+            cudaEventElapsedTime(&sv, marks[2], marks[3]);
+            for (tf_profile& p : profiles) {
+                p.broadphase = bp;
+                p.narrowphase = np;
+                p.solver = sv;
+                p.total = bp + np + sv;
+            }
+        }
+        for (cudaEvent_t& ev : marks) { cudaEventDestroy(ev); }
+        if (e != cudaSuccess) { return fail(TF_E_CUDA, std::string("step: ") + cudaGetErrorString(e)); }
+        if (rc != TF_OK) { return rc; }
+        return checkFlags();
+    }
+
+    // Records n steps into a CUDA graph on first use (the contact buffers alternate, so n even keeps the
+    // same buffer at the end), then replays it.
+    int stepGraph(float dt, int nSteps) {
+        if (!(dt > 0.0f) || !std::isfinite(dt) || nSteps <= 0) { return TF_OK; }
+        TF_CUDA(cudaSetDevice(device));
+        int rc = configureKernels();
+        if (rc != TF_OK) { return rc; }
+        rc = prepareDevice();
+        if (rc != TF_OK) { return rc; }
+        if (graphExec && (graphSteps != nSteps || graphDt != dt)) {
+            cudaGraphExecDestroy(graphExec);
+            graphExec = nullptr;
+        }
+        if (!graphExec) {
+            cudaGraph_t graph;
+            TF_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+            int c = cur;
+            for (int s = 0; s < nSteps; ++s) {
+                const int into = 1 - c;
+                rc = enqueueStep(dt, into, nullptr);
+                if (rc != TF_OK) { break; }
+                c = into;
+            }
+            cudaError_t e = cudaStreamEndCapture(stream, &graph);
+            if (rc != TF_OK) { return rc; }
+            if (e != cudaSuccess) { return fail(TF_E_CUDA, std::string("graph capture: ") + cudaGetErrorString(e)); }
+            e = cudaGraphInstantiate(&graphExec, graph, 0);
+            cudaGraphDestroy(graph);
+            if (e != cudaSuccess) { return fail(TF_E_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e)); }
+            graphSteps = nSteps;
+            graphDt = dt;
+            graphStart = cur;
+        }
+        if (cur != graphStart) {
+            // The recorded graph starts from the other buffer; record a fresh one.
+            cudaGraphExecDestroy(graphExec);
+            graphExec = nullptr;
+            return stepGraph(dt, nSteps);
+        }
+        TF_CUDA(cudaGraphLaunch(graphExec, stream));
+        launches += (int64_t)nSteps * (5 + std::max(1, (int)settings.substeps));
+        if (nSteps % 2) { cur = 1 - cur; }
+        hostFresh = false;
+        TF_CUDA(cudaStreamSynchronize(stream));
+        return checkFlags();
+    }
+    int graphStart = 0;
+
+    int checkFlags() {
+        std::vector<WorldCounts> counts(worlds.size());
+        TF_CUDA(cudaMemcpy(counts.data(), dCounts.ptr, worlds.size() * sizeof(WorldCounts), cudaMemcpyDeviceToHost));
+        uint32_t flags = 0;
+        for (size_t w = 0; w < worlds.size(); ++w) {
+            flags |= counts[w].flags;
+            tf_profile& p = profiles[w];
+            p.candidate_pairs = (int32_t)counts[w].candCount;
+            p.manifolds = (int32_t)counts[w].contactCount;
+            p.awake_bodies = (int32_t)counts[w].awakeBodies;
+            p.awake_islands = (int32_t)counts[w].awakeIslands;
+        }
+        lastCounts = counts;
+        deviceFlags = flags;
+        if (flags & (kDevPairOverflow | kDevContactOverflow)) {
+            capFactor *= 2.0f;
+            layoutDirty = true;
+            return fail(TF_E_CAPACITY, "a device list overflowed; capacities grow for the next step");
+        }
+        if (flags & kDevUnsupported) { return fail(TF_E_UNSUPPORTED, "the step met a pair this build cannot collide"); }
+        if (flags & kDevNonFinite) { return fail(TF_E_NUMERIC, "a body state became non-finite"); }
+        return TF_OK;
+    }
+    std::vector<WorldCounts> lastCounts;
+    uint32_t deviceFlags = 0;
+};
+
+}  // namespace tfb
+
+using tfb::Engine;
+
+namespace {
+Engine* E(void* h) { return static_cast<Engine*>(h); }
+}
+
+extern "C" {
+
+TF_API int tf_abi_version(void) { return TF_ABI_VERSION; }
+
+TF_API const char* tf_last_error(void) { return tfb::g_error.c_str(); }
+
+TF_API void tf_default_settings(tf_settings* s) {
+    if (!s) { return; }
+    *s = tf_settings{};
+    s->gravity[0] = 0.0f;
+    s->gravity[1] = -9.81f;
+    s->gravity[2] = 0.0f;
+    s->length_unit = 1.0f;
+    s->substeps = 4;
+    s->contact_hertz = 30.0f;
+    s->contact_damping_ratio = 10.0f;
+    s->max_pushout_speed = 3.0f;
+    s->max_linear_speed = 1000.0f;
+    s->max_angular_speed = 1000.0f;
+    s->restitution_threshold = 1.0f;
+    s->hit_threshold = 1.0f;
+    s->sleep_threshold = 0.05f;
+    s->time_to_sleep = 0.5f;
+    s->contact_reuse_distance = 0.0005f;
+    s->contact_reuse_angle = 0.035f;
+    s->joint_hertz = 60.0f;
+    s->joint_damping_ratio = 2.0f;
+    s->continuous = 1;
+}
+
+TF_API int tf_world_create(const tf_settings* settings, int32_t n_worlds, int32_t device, void** out) {
+    if (!out || n_worlds <= 0) { return tfb::fail(TF_E_INVALID, "tf_world_create: bad arguments"); }
+    *out = nullptr;
+    tf_settings s;
+    if (settings) {
+        s = *settings;
+    } else {
+        tf_default_settings(&s);
+    }
+    std::unique_ptr<Engine> e(new Engine());
+    const int rc = e->init(&s, n_worlds, device);
+    if (rc != TF_OK) { return rc; }
+    *out = e.release();
+    return TF_OK;
+}
+
+TF_API int tf_world_destroy(void* h) {
+    delete E(h);
+    return TF_OK;
+}
+
+TF_API int tf_world_count(void* h, int32_t* n) {
+    if (!h || !n) { return tfb::fail(TF_E_INVALID, "tf_world_count: null"); }
+    *n = (int32_t)E(h)->worlds.size();
+    return TF_OK;
+}
+
+TF_API int tf_world_set_settings(void* h, const tf_settings* s) {
+    if (!h || !s) { return tfb::fail(TF_E_INVALID, "tf_world_set_settings: null"); }
+    E(h)->settings = *s;
+    return TF_OK;
+}
+
+TF_API int tf_body_create(void* h, int32_t w, const tf_body_desc* d, tf_id* out) {
+    if (!h) { return tfb::fail(TF_E_INVALID, "tf_body_create: null world"); }
+    return E(h)->createBody(w, d, out);
+}
+
+TF_API int tf_shape_add(void* h, int32_t w, tf_id body, const tf_shape_desc* d, tf_id* out) {
+    if (!h) { return tfb::fail(TF_E_INVALID, "tf_shape_add: null world"); }
+    return E(h)->addShape(w, body, d, out);
+}
+
+TF_API int tf_bodies_create(void* h, int32_t n, const int32_t* world_of, const tf_body_desc* descs, tf_id* out) {
+    if (!h || (n > 0 && (!world_of || !descs))) { return tfb::fail(TF_E_INVALID, "tf_bodies_create: null"); }
+    for (int32_t i = 0; i < n; ++i) {
+        const int rc = E(h)->createBody(world_of[i], &descs[i], out ? &out[i] : nullptr);
+        if (rc != TF_OK) { return rc; }
+    }
+    return TF_OK;
+}
+
+TF_API int tf_shapes_add(void* h, int32_t n, const int32_t* world_of, const uint32_t* body_of,
+                         const tf_shape_desc* descs, tf_id* out) {
+    if (!h || (n > 0 && (!world_of || !body_of || !descs))) { return tfb::fail(TF_E_INVALID, "tf_shapes_add: null"); }
+    Engine* e = E(h);
+    for (int32_t i = 0; i < n; ++i) {
+        const int w = world_of[i];
+        if (w < 0 || w >= (int)e->worlds.size() || body_of[i] >= e->worlds[(size_t)w].bodies.size()) {
+            return tfb::fail(TF_E_INVALID, "tf_shapes_add: bad body");
+        }
+        const tf_id body{ body_of[i], e->worlds[(size_t)w].bodies[body_of[i]].generation };
+        const int rc = e->addShape(w, body, &descs[i], out ? &out[i] : nullptr);
+        if (rc != TF_OK) { return rc; }
+    }
+    return TF_OK;
+}
+
+TF_API int tf_world_step(void* h, float dt, int32_t n) {
+    if (!h) { return tfb::fail(TF_E_INVALID, "tf_world_step: null world"); }
+    return E(h)->step(dt, n);
+}
+
+TF_API int tf_world_step_graph(void* h, float dt, int32_t n) {
+    if (!h) { return tfb::fail(TF_E_INVALID, "tf_world_step_graph: null world"); }
+    return E(h)->stepGraph(dt, n);
+}
+
+TF_API int tf_world_synchronize(void* h) {
+    if (!h) { return tfb::fail(TF_E_INVALID, "tf_world_synchronize: null world"); }
+    if (!E(h)->stream) { return TF_OK; }
+    cudaError_t e = cudaStreamSynchronize(E(h)->stream);
+    return e == cudaSuccess ? TF_OK : tfb::fail(TF_E_CUDA, cudaGetErrorString(e));
+}
+
+TF_API int tf_world_device_status(void* h, uint32_t* flags) {
+    if (!h || !flags) { return tfb::fail(TF_E_INVALID, "tf_world_device_status: null"); }
+    *flags = E(h)->deviceFlags;
+    return TF_OK;
+}
+
+TF_API int tf_body_get_state(void* h, int32_t w, tf_id id, float p[3], float q[4], float v[3], float av[3]) {
+    if (!h) { return tfb::fail(TF_E_INVALID, "tf_body_get_state: null world"); }
+    Engine* e = E(h);
+    const int rc = e->pull();
+    if (rc != TF_OK) { return rc; }
+    tfb::HostBody* b = e->body(w, id);
+    const tfb::DBody zero{};
+    const tfb::DBody& d = b ? b->d : zero;
+    if (p) { p[0] = d.xf.p.x, p[1] = d.xf.p.y, p[2] = d.xf.p.z; }
+    if (q) { q[0] = b ? d.xf.q.x : 0.0f, q[1] = b ? d.xf.q.y : 0.0f, q[2] = b ? d.xf.q.z : 0.0f, q[3] = b ? d.xf.q.w : 1.0f; }
+    if (v) { v[0] = d.v.x, v[1] = d.v.y, v[2] = d.v.z; }
+    if (av) { av[0] = d.w.x, av[1] = d.w.y, av[2] = d.w.z; }
+    return TF_OK;
+}
+
+TF_API int tf_body_set_velocity(void* h, int32_t w, tf_id id, const float v[3], const float av[3]) {
+    if (!h) { return tfb::fail(TF_E_INVALID, "tf_body_set_velocity: null world"); }
+    Engine* e = E(h);
+    int rc = e->pull();
+    if (rc != TF_OK) { return rc; }
+    tfb::HostBody* b = e->body(w, id);
+    if (!b || b->d.type == tfb::kStatic) { return TF_OK; }
+    if (b->d.type == tfb::kDynamic && !b->d.awake) {
+        return tfb::fail(TF_E_UNSUPPORTED, "tf_body_set_velocity: waking a sleeping body from the host is not run by this build");
+    }
+    if (v) { b->d.v = b->d.linearProj * tfb::Vec3{ v[0], v[1], v[2] }; }
+    if (av) { b->d.w = b->d.angularProj * tfb::Vec3{ av[0], av[1], av[2] }; }
+    e->bodiesDirty = true;
+    return TF_OK;
+}
+
+TF_API int tf_body_get_mass(void* h, int32_t w, tf_id id, float* mass, float center[3], float inertia[9]) {
+    if (!h) { return tfb::fail(TF_E_INVALID, "tf_body_get_mass: null world"); }
+    tfb::HostBody* b = E(h)->body(w, id);
+    const tfb::DBody zero{};
+    const tfb::DBody& d = b ? b->d : zero;
+    if (mass) { *mass = d.mass; }
+    if (center) { center[0] = d.localCenter.x, center[1] = d.localCenter.y, center[2] = d.localCenter.z; }
+    if (inertia) {
+        for (int r = 0; r < 3; ++r) {
+            inertia[3 * r + 0] = d.inertia.r[r].x;
+            inertia[3 * r + 1] = d.inertia.r[r].y;
+            inertia[3 * r + 2] = d.inertia.r[r].z;
+        }
+    }
+    return TF_OK;
+}
+
+TF_API int tf_body_is_awake(void* h, int32_t w, tf_id id, int32_t* awake) {
+    if (!h || !awake) { return tfb::fail(TF_E_INVALID, "tf_body_is_awake: null"); }
+    Engine* e = E(h);
+    const int rc = e->pull();
+    if (rc != TF_OK) { return rc; }
+    tfb::HostBody* b = e->body(w, id);
+    *awake = (b && b->d.awake) ? 1 : 0;
+    return TF_OK;
+}
+
+TF_API int tf_world_body_count(void* h, int64_t* total) {
+    if (!h || !total) { return tfb::fail(TF_E_INVALID, "tf_world_body_count: null"); }
+    int64_t n = 0;
+    for (const auto& W : E(h)->worlds) { n += (int64_t)W.bodies.size(); }
+    *total = n;
+    return TF_OK;
+}
+
+TF_API int tf_world_get_states(void* h, float* p, float* q, float* v, float* w, int32_t* awake) {
+    if (!h) { return tfb::fail(TF_E_INVALID, "tf_world_get_states: null world"); }
+    Engine* e = E(h);
+    const int rc = e->pull();
+    if (rc != TF_OK) { return rc; }
+    size_t k = 0;
+    for (const auto& W : e->worlds) {
+        for (const auto& hb : W.bodies) {
+            const tfb::DBody& d = hb.d;
+            if (p) { p[3 * k] = d.xf.p.x, p[3 * k + 1] = d.xf.p.y, p[3 * k + 2] = d.xf.p.z; }
+            if (q) { q[4 * k] = d.xf.q.x, q[4 * k + 1] = d.xf.q.y, q[4 * k + 2] = d.xf.q.z, q[4 * k + 3] = d.xf.q.w; }
+            if (v) { v[3 * k] = d.v.x, v[3 * k + 1] = d.v.y, v[3 * k + 2] = d.v.z; }
+            if (w) { w[3 * k] = d.w.x, w[3 * k + 1] = d.w.y, w[3 * k + 2] = d.w.z; }
+            if (awake) { awake[k] = d.awake ? 1 : 0; }
+            ++k;
+        }
+    }
+    return TF_OK;
+}
+
+TF_API int tf_world_contacts(void* h, int32_t w, int32_t mode, tf_contact* out, int32_t cap, int32_t* count) {
+    if (!h || !count) { return tfb::fail(TF_E_INVALID, "tf_world_contacts: null"); }
+    Engine* e = E(h);
+    if (w < 0 || w >= (int)e->worlds.size()) { return tfb::fail(TF_E_INVALID, "tf_world_contacts: bad world"); }
+    const int rc = e->pull();
+    if (rc != TF_OK) { return rc; }
+    const auto& W = e->worlds[(size_t)w];
+    int32_t n = 0;
+    for (const tfb::DContact& c : W.contacts) {
+        bool touching = false;
+        for (int i = 0; i < c.count; ++i) {
+            touching = touching || c.points[i].separation < 0.0f || c.points[i].normalImpulse > 0.0f;
+        }
+        if (mode < 2 && ((c.flags & tfb::kCRemoved) || (mode == 0 && !touching))) { continue; }
+        if (out && n < cap) {
+            tf_contact& o = out[n];
+            std::memset(&o, 0, sizeof(o));
+            o.key = c.key;
+            o.part = c.part;
+            o.shape_a = c.shapeA;
+            o.shape_b = c.shapeB;
+            o.body_a = c.bodyA;
+            o.body_b = c.bodyB;
+            o.point_count = c.count;
+            o.feature_kind = c.featKind;
+            o.feature_a = c.featA;
+            o.feature_b = c.featB;
+            o.normal[0] = c.normal.x, o.normal[1] = c.normal.y, o.normal[2] = c.normal.z;
+            o.friction = c.friction;
+            o.restitution = c.restitution;
+            o.rolling_resistance = c.rollingResistance;
+            o.rolling_impulse[0] = c.rollingImpulse.x, o.rolling_impulse[1] = c.rollingImpulse.y,
+            o.rolling_impulse[2] = c.rollingImpulse.z;
+            const tfb::Transform xa = W.bodies[c.bodyA].d.xf;
+            for (int i = 0; i < c.count; ++i) {
+                const tfb::Vec3 pw = tfb::apply(xa, c.points[i].localA);
+                o.points[i][0] = pw.x, o.points[i][1] = pw.y, o.points[i][2] = pw.z;
+                o.separations[i] = c.points[i].separation;
+                o.normal_impulses[i] = c.points[i].normalImpulse;
+                o.tangent_impulses[i][0] = c.points[i].tangentImpulse.x;
+                o.tangent_impulses[i][1] = c.points[i].tangentImpulse.y;
+                o.tangent_impulses[i][2] = c.points[i].tangentImpulse.z;
+            }
+        }
+        ++n;
+    }
+    *count = n;
+    return TF_OK;
+}
+
+TF_API int tf_world_candidates(void* h, int32_t w, uint64_t* out, int32_t cap, int32_t* count) {
+    if (!h || !count) { return tfb::fail(TF_E_INVALID, "tf_world_candidates: null"); }
+    Engine* e = E(h);
+    if (w < 0 || w >= (int)e->worlds.size()) { return tfb::fail(TF_E_INVALID, "tf_world_candidates: bad world"); }
+    if (e->lastCounts.empty() || e->layoutDirty) {
+        *count = 0;
+        return TF_OK;
+    }
+    const uint32_t n = e->lastCounts[(size_t)w].candCount;
+    *count = (int32_t)n;
+    if (out && cap > 0) {
+        const size_t m = std::min<size_t>(n, (size_t)cap);
+        cudaError_t err = cudaMemcpy(out, e->dCand.ptr + e->info[(size_t)w].candFirst, m * sizeof(uint64_t), cudaMemcpyDeviceToHost);
+        if (err != cudaSuccess) { return tfb::fail(TF_E_CUDA, cudaGetErrorString(err)); }
+    }
+    return TF_OK;
+}
+
+TF_API int tf_world_profile(void* h, int32_t w, tf_profile* out) {
+    if (!h || !out) { return tfb::fail(TF_E_INVALID, "tf_world_profile: null"); }
+    Engine* e = E(h);
+    if (w < 0 || w >= (int)e->worlds.size()) { return tfb::fail(TF_E_INVALID, "tf_world_profile: bad world"); }
+    *out = e->profiles[(size_t)w];
+    return TF_OK;
+}
+
+TF_API int tf_world_awake_bodies(void* h, int64_t* count) {
+    if (!h || !count) { return tfb::fail(TF_E_INVALID, "tf_world_awake_bodies: null"); }
+    int64_t n = 0;
+    for (const auto& c : E(h)->lastCounts) { n += c.awakeBodies; }
+    *count = n;
+    return TF_OK;
+}
+
+TF_API int tf_world_launch_count(void* h, int64_t* launches) {
+    if (!h || !launches) { return tfb::fail(TF_E_INVALID, "tf_world_launch_count: null"); }
+    *launches = E(h)->launches;
+    return TF_OK;
+}
+
+}

@@ -1,0 +1,984 @@
+// The step kernels. Each kernel processes whole worlds: CTA k takes worlds order[k], order[k + gridDim.x],
+// ... (largest first), and within a world its threads split bodies, candidates or one color's contacts,
+// with __syncthreads() between dependent phases. Work that the reference does in one sequential pass
+// whose result depends on order (graph coloring, union-find islands, the wake flood and contacts solved
+// one at a time) runs on the world's first thread, in the reference's order.
+//
+// Kernel sequence of one step (src/world.cpp:1564-1727):
+//   k_broadphase   growth, body-pair and half-space candidates, sort + unique   (world.cpp:752-870)
+//   k_narrowphase  reuse or collide each candidate, carry impulses, merge       (world.cpp:872-993)
+//   k_wake         wake sleeping bodies touched by moving ones                  (world.cpp:705-735)
+//   k_prepare      step state, active/fast/impact lists, prepare, coloring     (world.cpp:1589-1657)
+//   k_substep x n  refresh, integrate, warm start, solve, integrate, relax      (world.cpp:1658-1681)
+//   k_finish       restitution, limits, refit bounds, sweep test, sleep         (world.cpp:1682-1726)
+#pragma once
+
+#include "tf_batch.cuh"
+#include "tf_solver.cuh"
+
+namespace tfb {
+
+constexpr int kMaxBlock = 512;
+constexpr uint32_t kDevPairOverflow = 1u << 0, kDevContactOverflow = 1u << 1, kDevNonFinite = 1u << 2,
+                   kDevUnsupported = 1u << 4, kDevSweepSkipped = 1u << 5, kDevListOverflow = 1u << 6;
+
+// Exclusive prefix sum over the block. Every thread calls it; blockDim.x is a multiple of 32.
+__device__ __forceinline__ uint32_t blockExclusiveScan(uint32_t v, uint32_t& total) {
+    __shared__ uint32_t warpSums[kMaxBlock / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    uint32_t x = v;
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) { x += y; }
+    }
+    if (lane == 31) { warpSums[warp] = x; }
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t s = lane < nw ? warpSums[lane] : 0u;
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, s, o);
+            if (lane >= o) { s += y; }
+        }
+        if (lane < nw) { warpSums[lane] = s; }
+    }
+    __syncthreads();
+    const uint32_t prefix = (warp > 0 ? warpSums[warp - 1] : 0u) + x - v;
+    total = warpSums[nw - 1];
+    __syncthreads();
+    return prefix;
+}
+
+// Calls emit(i, position) for every i < n where pred(i) holds, positions dense and in index order.
+template <class Pred, class Emit>
+__device__ uint32_t blockCompact(uint32_t n, Pred pred, Emit emit) {
+    uint32_t base = 0;
+    for (uint32_t start = 0; start < n; start += blockDim.x) {
+        const uint32_t i = start + threadIdx.x;
+        const bool f = i < n && pred(i);
+        uint32_t tot;
+        const uint32_t pos = blockExclusiveScan(f ? 1u : 0u, tot);
+        if (f) { emit(i, base + pos); }
+        base += tot;
+    }
+    return base;
+}
+
+__device__ __forceinline__ uint64_t pairKey(uint32_t a, uint32_t b) {
+    return ((uint64_t)(a < b ? a : b) << 32) | (uint64_t)(a < b ? b : a);
+}
+
+__device__ __forceinline__ void emitCandidate(const Batch& B, const WorldInfo& wi, uint32_t* count, uint64_t key) {
+    const uint32_t pos = atomicAdd(count, 1u);
+    if (pos < wi.candCap) { B.cand[wi.candFirst + pos] = key; }
+}
+
+// ---------------------------------------------------------------------------------------------------------
+// Broadphase (src/world.cpp:752-870).
+
+// The shapes of two overlapping bodies, paired by their grown bounds (src/world.cpp:788-842).
+__device__ void pairBodies(const Batch& B, const WorldInfo& wi, uint32_t ga, uint32_t gb, uint32_t* count) {
+    const DBody& ba = B.bodies[ga];
+    const DBody& bb = B.bodies[gb];
+    if (!ba.alive || !bb.alive || !ba.hasBounds || !bb.hasBounds) { return; }
+    if (ba.type != kDynamic && bb.type != kDynamic) { return; }
+    if (!movingAwake(ba) && !movingAwake(bb)) { return; }
+    const float gA = B.grow[ga], gB = B.grow[gb];
+    const float g = gA + gB;
+    const Vec3 reach{ g, g, g };
+    if (!boxesOverlap(ba.lo - reach, ba.hi + reach, bb.lo, bb.hi)) { return; }
+    const Vec3 nearLoA = bb.lo - reach, nearHiA = bb.hi + reach;
+    const Vec3 nearLoB = ba.lo - reach, nearHiB = ba.hi + reach;
+    const Vec3 grownA{ gA, gA, gA }, grownB{ gB, gB, gB };
+    for (uint32_t x = 0; x < ba.shapeCount; ++x) {
+        const DShape& s = B.shapes[B.shapeList[ba.shapeFirst + x]];
+        if (s.kind == kHalfSpace || s.sensor || !boxesOverlap(s.lo, s.hi, nearLoA, nearHiA)) { continue; }
+        const Vec3 xlo = s.lo - grownA, xhi = s.hi + grownA;
+        for (uint32_t y = 0; y < bb.shapeCount; ++y) {
+            const DShape& t = B.shapes[B.shapeList[bb.shapeFirst + y]];
+            if (t.kind == kHalfSpace || t.sensor || !boxesOverlap(t.lo, t.hi, nearLoB, nearHiB)) { continue; }
+            if (!boxesOverlap(xlo, xhi, t.lo - grownB, t.hi + grownB)) { continue; }
+            if (!(s.category & t.mask) || !(t.category & s.mask)) { continue; }
+            emitCandidate(B, wi, count, pairKey(s.index, t.index));
+        }
+    }
+}
+
+// A half-space against one body's shapes (src/world.cpp:844-867).
+__device__ void pairPlane(const Batch& B, const WorldInfo& wi, uint32_t gp, uint32_t gb, uint32_t* count) {
+    const DShape& sp = B.shapes[gp];
+    const DBody& pb = B.bodies[sp.body];
+    const DBody& b = B.bodies[gb];
+    const bool planeMoving = movingAwake(pb);
+    if (!b.alive || gb == sp.body || (!planeMoving && !movingAwake(b))) { return; }
+    const float gp_ = B.grow[sp.body];
+    const Transform xp = pb.xf * sp.local;
+    const Vec3 n = rotate(xp.q, Vec3{ 0, 0, 1 });
+    const float offset = dot(n, xp.p);
+    const float g = gp_ + B.grow[gb];
+    auto reaches = [&](const Vec3& lo, const Vec3& hi) {
+        const Vec3 c = (lo + hi) * 0.5f, e = (hi - lo) * 0.5f + Vec3{ g, g, g };
+        return dot(c, n) - offset <= e.x * fabsf(n.x) + e.y * fabsf(n.y) + e.z * fabsf(n.z);
+    };
+    if (b.hasBounds && !reaches(b.lo, b.hi)) { return; }
+    for (uint32_t x = 0; x < b.shapeCount; ++x) {
+        const uint32_t gs = B.shapeList[b.shapeFirst + x];
+        const DShape& s = B.shapes[gs];
+        if (s.kind != kHalfSpace && !reaches(s.lo, s.hi)) { continue; }
+        // pairable(sp, s): neither a sensor, different bodies, one of them dynamic.
+        if (sp.sensor || s.sensor || sp.body == s.body) { continue; }
+        if (pb.type != kDynamic && b.type != kDynamic) { continue; }
+        // test(pi, si) (src/world.cpp:798-808).
+        const float ga = B.grow[sp.body], gbb = B.grow[s.body];
+        const Vec3 g3a{ ga, ga, ga }, g3b{ gbb, gbb, gbb };
+        if (!boxesOverlap(sp.lo - g3a, sp.hi + g3a, s.lo - g3b, s.hi + g3b)) { continue; }
+        if (!(sp.category & s.mask) || !(s.category & sp.mask)) { continue; }
+        emitCandidate(B, wi, count, pairKey(sp.index, s.index));
+    }
+}
+
+// Sorts keys[0, n) ascending in shared memory and removes repeats; returns the unique count written back to
+// out[0, unique).
+__device__ uint32_t sortUnique(uint64_t* s, uint32_t n, uint64_t* out) {
+    uint32_t p = 1;
+    while (p < n) { p <<= 1; }
+    for (uint32_t i = n + threadIdx.x; i < p; i += blockDim.x) { s[i] = ~0ull; }
+    __syncthreads();
+    for (uint32_t k = 2; k <= p; k <<= 1) {
+        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+            for (uint32_t i = threadIdx.x; i < p; i += blockDim.x) {
+                const uint32_t ixj = i ^ j;
+                if (ixj > i) {
+                    const uint64_t a = s[i], b = s[ixj];
+                    const bool up = (i & k) == 0;
+                    if ((a > b) == up) {
+                        s[i] = b;
+                        s[ixj] = a;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
+    const uint32_t unique = blockCompact(
+        n, [&](uint32_t i) { return i == 0 || s[i] != s[i - 1]; }, [&](uint32_t i, uint32_t pos) { out[pos] = s[i]; });
+    __syncthreads();
+    return unique;
+}
+
+__global__ void __launch_bounds__(kMaxBlock) k_broadphase(Batch B, StepParams P, uint32_t sortCap) {
+    extern __shared__ uint64_t s_keys[];
+    __shared__ uint32_t s_count;
+    for (int o = blockIdx.x; o < B.nWorlds; o += gridDim.x) {
+        const uint32_t w = B.order[o];
+        const WorldInfo wi = B.info[w];
+        WorldCounts& wc = B.counts[w];
+        if (threadIdx.x == 0) { s_count = 0; }
+        // Growth by the speculative distance and the travel over the step (src/world.cpp:754-765).
+        for (uint32_t i = threadIdx.x; i < wi.bodyCount; i += blockDim.x) {
+            const DBody& b = B.bodies[wi.bodyFirst + i];
+            float g = P.tol.speculative;
+            if (b.alive && b.type != kStatic && !(lengthSquared(b.v) == 0.0f && lengthSquared(b.w) == 0.0f)) {
+                g += (length(b.v) + length(b.w) * b.extent) * P.dt;
+            }
+            B.grow[wi.bodyFirst + i] = g;
+        }
+        __syncthreads();
+        const uint32_t n = wi.bodyCount;
+        for (uint32_t a = 0; a + 1 < n; ++a) {
+            for (uint32_t b = a + 1 + threadIdx.x; b < n; b += blockDim.x) {
+                pairBodies(B, wi, wi.bodyFirst + a, wi.bodyFirst + b, &s_count);
+            }
+        }
+        for (uint32_t pl = 0; pl < wi.planeCount; ++pl) {
+            const uint32_t gp = B.planeList[wi.planeFirst + pl];
+            for (uint32_t b = threadIdx.x; b < n; b += blockDim.x) { pairPlane(B, wi, gp, wi.bodyFirst + b, &s_count); }
+        }
+        __syncthreads();
+        uint32_t count = s_count;
+        if (count > wi.candCap) {
+            if (threadIdx.x == 0) {
+                wc.flags |= kDevPairOverflow;
+                wc.candNeeded = max(wc.candNeeded, count);
+            }
+            count = wi.candCap;
+        }
+        if (count > sortCap) {
+            if (threadIdx.x == 0) {
+                wc.flags |= kDevUnsupported;
+                wc.candCount = 0;
+            }
+            __syncthreads();
+            continue;
+        }
+        for (uint32_t i = threadIdx.x; i < count; i += blockDim.x) { s_keys[i] = B.cand[wi.candFirst + i]; }
+        __syncthreads();
+        const uint32_t unique = sortUnique(s_keys, count, B.cand + wi.candFirst);
+        if (threadIdx.x == 0) {
+            wc.candCount = unique;
+            wc.candNeeded = max(wc.candNeeded, count);
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------------------------------------
+// Narrowphase and contact bookkeeping (src/world.cpp:872-1025).
+
+__device__ __forceinline__ Vec3 lift(const DBody& a, const DBody& b, const Vec3& normal, float separation, float spec) {
+    if (isPlanar(a) || isPlanar(b)) { return zero3(); }
+    return separation > spec ? normal * (0.5f * separation) : zero3();
+}
+
+// src/world.cpp:1002-1009.
+__device__ __forceinline__ bool stillFits(const DContact& c, const DBody& a, const DBody& b, const StepParams& P) {
+    if (!(c.flags & kCReusable)) { return false; }
+    const float reach = P.reuseDistance;
+    if (lengthSquared(unrotate(a.xf.q, b.com - a.com) - c.baseOffset) > reach * reach) { return false; }
+    const Quat turn = conjugate(a.xf.q) * b.xf.q;
+    return fabsf(dot(turn, c.baseTurn)) >= P.reuseCos;
+}
+
+// src/world.cpp:1012-1025.
+__device__ void measureAgain(const DBody& a, const DBody& b, DContact& c, const StepParams& P) {
+    c.normal = rotate(a.xf.q, c.localNormal);
+    c.tangent1 = perpendicular(c.normal);
+    c.tangent2 = cross(c.normal, c.tangent1);
+    for (int i = 0; i < c.count; ++i) {
+        DPoint& p = c.points[i];
+        const Vec3 pa = apply(a.xf, p.surfaceA), pb = apply(b.xf, p.surfaceB);
+        const Vec3 mid = (pa + pb) * 0.5f;
+        p.separation = dot(pb - pa, c.normal);
+        const Vec3 up = lift(a, b, c.normal, p.separation, P.tol.speculative);
+        p.anchorA = mid - up - a.com;
+        p.anchorB = mid + up - b.com;
+        p.tangentImpulse = p.tangentImpulse - c.normal * dot(c.normal, p.tangentImpulse);
+    }
+}
+
+// Each new point continues the nearest old point in reach; an old point continued by several new points
+// splits its impulse among them (src/world.cpp:102-124).
+__device__ void carryImpulses(const DContact& old, DContact& c, float matchSq) {
+    int from[4], claims[4] = { 0, 0, 0, 0 };
+    for (int i = 0; i < c.count; ++i) {
+        from[i] = -1;
+        float bestSq = matchSq;
+        for (int k = 0; k < old.count; ++k) {
+            const float d = lengthSquared(old.points[k].localA - c.points[i].localA);
+            if (d <= bestSq) {
+                from[i] = k;
+                bestSq = d;
+            }
+        }
+        if (from[i] >= 0) { ++claims[from[i]]; }
+    }
+    for (int i = 0; i < c.count; ++i) {
+        if (from[i] < 0) { continue; }
+        const DPoint& o = old.points[from[i]];
+        const float share = 1.0f / (float)claims[from[i]];
+        c.points[i].normalImpulse = o.normalImpulse * share;
+        c.points[i].tangentImpulse = (o.tangentImpulse - c.normal * dot(c.normal, o.tangentImpulse)) * share;
+    }
+    c.rollingImpulse = old.rollingImpulse;
+}
+
+__device__ __forceinline__ int nearestPoint(const DContact& old, const Vec3& localA) {
+    int best = -1;
+    float bestSq = FLT_MAX;
+    for (int k = 0; k < old.count; ++k) {
+        const float d = lengthSquared(old.points[k].localA - localA);
+        if (d < bestSq) {
+            best = k;
+            bestSq = d;
+        }
+    }
+    return best;
+}
+
+// Collides one shape pair over dt as Impl::collidePair does for non-mesh, non-planar pairs
+// (src/world.cpp:505-533). Returns false for a pair this build cannot collide.
+__device__ bool collidePair(const Batch& B, const StepParams& P, const DShape& sa, const DShape& sb, float dt,
+                            Manifold& m, int reuseKind, int reuseA, int reuseB) {
+    const DBody& ba = B.bodies[sa.body];
+    const DBody& bb = B.bodies[sb.body];
+    const float travel = relativeTravel(ba, bb, dt);
+    const float margin = P.tol.speculative + travel;
+    const Transform xa = ba.xf * sa.local;
+    const Transform xb = bb.xf * sb.local;
+    const Motion mo{ ba.v, ba.w, ba.com, bb.v, bb.w, bb.com, dt, travel > P.tol.speculative };
+    return collideShapes(B.cx, sa, xa, sb, xb, margin, mo, m, reuseKind, reuseA, reuseB);
+}
+
+// First index in [0, n) whose key is not below key.
+__device__ __forceinline__ uint32_t lowerKey(const DContact* c, uint32_t n, uint64_t key) {
+    uint32_t lo = 0, hi = n;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (c[mid].key < key) {
+            lo = mid + 1;
+        } else {
+            hi = mid;
+        }
+    }
+    return lo;
+}
+
+// One candidate: keep and measure the old contact when the pair barely moved, else collide it and carry the
+// old impulses over (src/world.cpp:883-959).
+__device__ void narrowOne(const Batch& B, const StepParams& P, const WorldInfo& wi, WorldCounts& wc, uint32_t i,
+                          const DContact* old, uint32_t oldCount) {
+    const uint64_t key = B.cand[wi.candFirst + i];
+    const uint32_t ia = (uint32_t)(key >> 32), ib = (uint32_t)(key & 0xffffffffu);
+    const uint32_t gsa = wi.shapeFirst + ia, gsb = wi.shapeFirst + ib;
+    const DShape sa = B.shapes[gsa];
+    const DShape sb = B.shapes[gsb];
+    const DBody& ba = B.bodies[sa.body];
+    const DBody& bb = B.bodies[sb.body];
+    const uint32_t lo = lowerKey(old, oldCount, key);
+    uint32_t hi = lo;
+    while (hi < oldCount && old[hi].key == key) { ++hi; }
+    const bool hasOld = lo < hi;
+    bool keep = hasOld;
+    for (uint32_t it = lo; it < hi && keep; ++it) { keep = stillFits(old[it], ba, bb, P); }
+    const bool touched = hasOld && (old[lo].flags & kCTouched);
+    DContact& out = B.stage[wi.candFirst + i];
+    uint8_t used = 0;
+    if (keep) {
+        if (hi - lo > 1) { atomicOr(&wc.flags, kDevUnsupported); }
+        out = old[lo];
+        measureAgain(ba, bb, out, P);
+        used = 1;
+    } else {
+        if (isPlanar(ba) || isPlanar(bb)) { atomicOr(&wc.flags, kDevUnsupported); }
+        Manifold m;
+        if (!collidePair(B, P, sa, sb, P.dt, m, kFeatNone, -1, -1)) { atomicOr(&wc.flags, kDevUnsupported); }
+        if (m.count > 0) {
+            DContact c{};
+            c.key = key;
+            c.part = 0;
+            c.shapeA = gsa;
+            c.shapeB = gsb;
+            c.bodyA = sa.body;
+            c.bodyB = sb.body;
+            c.flags = touched ? kCTouched : 0u;
+            c.featKind = m.featKind;
+            c.featA = m.featA;
+            c.featB = m.featB;
+            c.normal = m.normal;
+            c.tangent1 = perpendicular(m.normal);
+            c.tangent2 = cross(m.normal, c.tangent1);
+            c.count = m.count;
+            for (int k = 0; k < m.count; ++k) {
+                DPoint& p = c.points[k];
+                const Vec3 pos = m.points[k].position;
+                const float sep = m.points[k].separation;
+                const Vec3 half = m.normal * (0.5f * sep);
+                p.surfaceA = applyInverse(ba.xf, pos - half);
+                p.surfaceB = applyInverse(bb.xf, pos + half);
+                p.localA = applyInverse(ba.xf, pos);
+                p.separation = sep;
+                const Vec3 up = lift(ba, bb, m.normal, sep, P.tol.speculative);
+                p.anchorA = pos - up - ba.com;
+                p.anchorB = pos + up - bb.com;
+            }
+            // remember (src/world.cpp:995-1000).
+            c.localNormal = unrotate(ba.xf.q, c.normal);
+            c.baseOffset = unrotate(ba.xf.q, bb.com - ba.com);
+            c.baseTurn = conjugate(ba.xf.q) * bb.xf.q;
+            c.flags |= kCReusable;
+            // The old contact of the pair whose normal is closest (src/world.cpp:543-549).
+            int best = -1;
+            for (uint32_t it = lo; it < hi; ++it) {
+                if (old[it].count > 0 && (best < 0 || dot(old[it].normal, c.normal) > dot(old[best].normal, c.normal))) {
+                    best = (int)it;
+                }
+            }
+            if (best >= 0) { carryImpulses(old[best], c, P.tol.speculative * P.tol.speculative); }
+            out = c;
+            used = 1;
+        }
+    }
+    if (used) {
+        out.friction = sqrtf(sa.friction * sb.friction);
+        out.restitution = maxf(sa.restitution, sb.restitution);
+        out.rollingResistance = maxf(sa.rollingResistance, sb.rollingResistance);
+        if (ba.type == kDynamic && !ba.awake && movingAwake(bb)) {
+            B.wakeMark[sa.body] = 1;
+            wc.wakePending = 1;
+        }
+        if (bb.type == kDynamic && !bb.awake && movingAwake(ba)) {
+            B.wakeMark[sb.body] = 1;
+            wc.wakePending = 1;
+        }
+    }
+    B.stageUsed[wi.candFirst + i] = used;
+}
+
+__device__ __forceinline__ bool keyLess(uint64_t ka, uint32_t pa, uint64_t kb, uint32_t pb) {
+    return ka != kb ? ka < kb : pa < pb;
+}
+
+__global__ void __launch_bounds__(kMaxBlock) k_narrowphase(Batch B, StepParams P) {
+    for (int o = blockIdx.x; o < B.nWorlds; o += gridDim.x) {
+        const uint32_t w = B.order[o];
+        const WorldInfo wi = B.info[w];
+        WorldCounts& wc = B.counts[w];
+        const uint32_t nc = wc.candCount;
+        const uint32_t oldCount = wc.contactCount;
+        const DContact* old = B.previous + wi.contactFirst;
+        for (uint32_t i = threadIdx.x; i < nc; i += blockDim.x) { narrowOne(B, P, wi, wc, i, old, oldCount); }
+        __syncthreads();
+        const uint32_t cf = wi.contactFirst;
+        const uint32_t nC = blockCompact(
+            nc, [&](uint32_t i) { return B.stageUsed[wi.candFirst + i] != 0; },
+            [&](uint32_t i, uint32_t pos) {
+                const DContact& c = B.stage[wi.candFirst + i];
+                B.mergeKeyA[cf + pos] = c.key;
+                B.mergePartA[cf + pos] = c.part;
+                B.mergeIdxA[cf + pos] = i;
+            });
+        // Contacts of pairs where nothing moves and one body is dynamic (asleep) stay as they were
+        // (src/world.cpp:961-988).
+        const uint32_t nK = blockCompact(
+            oldCount,
+            [&](uint32_t j) {
+                const DContact& c = old[j];
+                const DBody& a = B.bodies[c.bodyA];
+                const DBody& b = B.bodies[c.bodyB];
+                if ((c.flags & kCRemoved) || movingAwake(a) || movingAwake(b)) { return false; }
+                return !(a.type != kDynamic && b.type != kDynamic);
+            },
+            [&](uint32_t j, uint32_t pos) {
+                B.mergeKeyB[cf + pos] = old[j].key;
+                B.mergePartB[cf + pos] = old[j].part;
+                B.mergeIdxB[cf + pos] = j;
+            });
+        __syncthreads();
+        const uint32_t total = nC + nK;
+        if (total > wi.contactCap && threadIdx.x == 0) {
+            wc.flags |= kDevContactOverflow;
+            wc.contactNeeded = max(wc.contactNeeded, total);
+        }
+        // Stable merge by (key, part): collided contacts first among equals, as std::inplace_merge keeps them.
+        for (uint32_t x = threadIdx.x; x < nC; x += blockDim.x) {
+            const uint64_t k = B.mergeKeyA[cf + x];
+            const uint32_t p = B.mergePartA[cf + x];
+            uint32_t l = 0, h = nK;
+            while (l < h) {
+                const uint32_t mid = (l + h) >> 1;
+                if (keyLess(B.mergeKeyB[cf + mid], B.mergePartB[cf + mid], k, p)) {
+                    l = mid + 1;
+                } else {
+                    h = mid;
+                }
+            }
+            const uint32_t pos = x + l;
+            if (pos < wi.contactCap) { B.contacts[cf + pos] = B.stage[wi.candFirst + B.mergeIdxA[cf + x]]; }
+        }
+        for (uint32_t y = threadIdx.x; y < nK; y += blockDim.x) {
+            const uint64_t k = B.mergeKeyB[cf + y];
+            const uint32_t p = B.mergePartB[cf + y];
+            uint32_t l = 0, h = nC;
+            while (l < h) {
+                const uint32_t mid = (l + h) >> 1;
+                if (!keyLess(k, p, B.mergeKeyA[cf + mid], B.mergePartA[cf + mid])) {
+                    l = mid + 1;
+                } else {
+                    h = mid;
+                }
+            }
+            const uint32_t pos = y + l;
+            if (pos < wi.contactCap) { B.contacts[cf + pos] = old[B.mergeIdxB[cf + y]]; }
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            wc.contactCount = total < wi.contactCap ? total : wi.contactCap;
+            wc.contactNeeded = max(wc.contactNeeded, total);
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------------------------------------
+// Waking (src/world.cpp:705-735): sleeping bodies a moving body reached wake, and so does everything linked
+// to them by a contact with points. Runs on the world's first thread.
+
+__global__ void k_wake(Batch B) {
+    if (threadIdx.x != 0) { return; }
+    for (int o = blockIdx.x; o < B.nWorlds; o += gridDim.x) {
+        const uint32_t w = B.order[o];
+        const WorldInfo wi = B.info[w];
+        WorldCounts& wc = B.counts[w];
+        if (!wc.wakePending) { continue; }
+        wc.wakePending = 0;
+        uint32_t* stack = B.unionParent + wi.bodyFirst;
+        uint32_t top = 0;
+        for (uint32_t i = 0; i < wi.bodyCount; ++i) {
+            const uint32_t g = wi.bodyFirst + i;
+            if (!B.wakeMark[g]) { continue; }
+            const DBody& b = B.bodies[g];
+            if (b.alive && b.type == kDynamic && !b.awake && top < wi.bodyCount) { stack[top++] = g; } else { B.wakeMark[g] = 0; }
+        }
+        const DContact* cs = B.contacts + wi.contactFirst;
+        const uint32_t nc = wc.contactCount;
+        while (top > 0) {
+            const uint32_t g = stack[--top];
+            DBody& b = B.bodies[g];
+            B.wakeMark[g] = 0;
+            if (b.awake) { continue; }
+            b.awake = 1;
+            b.sleepTime = 0.0f;
+            updateInverseMass(b);
+            for (uint32_t ci = 0; ci < nc; ++ci) {
+                const DContact& c = cs[ci];
+                if (c.bodyA != g && c.bodyB != g) { continue; }
+                if (ci > 0 && cs[ci - 1].key == c.key) { continue; }  // one link per pair
+                const uint32_t other = c.bodyA == g ? c.bodyB : c.bodyA;
+                const DBody& ob = B.bodies[other];
+                if (ob.type != kDynamic || ob.awake || B.wakeMark[other]) { continue; }
+                bool linked = false;
+                for (uint32_t k = ci; k < nc && cs[k].key == c.key; ++k) { linked = linked || cs[k].count > 0; }
+                if (linked && top < wi.bodyCount) {
+                    B.wakeMark[other] = 1;
+                    stack[top++] = other;
+                }
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------------------------
+// Step state, lists, preparation and coloring (src/world.cpp:1589-1657, src/lanes.cpp:356-407).
+
+__global__ void __launch_bounds__(kMaxBlock) k_prepare(Batch B, StepParams P) {
+    for (int o = blockIdx.x; o < B.nWorlds; o += gridDim.x) {
+        const uint32_t w = B.order[o];
+        const WorldInfo wi = B.info[w];
+        WorldCounts& wc = B.counts[w];
+        for (uint32_t i = threadIdx.x; i < wi.bodyCount; i += blockDim.x) {
+            const uint32_t g = wi.bodyFirst + i;
+            DBody& b = B.bodies[g];
+            B.bodyColors[g] = 0;
+            B.struck[g] = 0;
+            if (!b.alive) { continue; }
+            b.q0 = b.xf.q;
+            b.qBase = b.xf.q;
+            b.com0 = b.com;
+            b.expectedTravel = (length(b.v) + length(b.w) * b.extent) * P.dt;
+            b.dp = zero3();
+            b.dq = qid();
+            updateInverseMass(b);
+        }
+        __syncthreads();
+        const uint32_t cf = wi.contactFirst;
+        const uint32_t nc = wc.contactCount;
+        DContact* cs = B.contacts + cf;
+        const uint32_t nActive = blockCompact(
+            nc,
+            [&](uint32_t i) {
+                const DBody& a = B.bodies[cs[i].bodyA];
+                const DBody& b = B.bodies[cs[i].bodyB];
+                const bool on = (a.type == kDynamic && a.awake) || (b.type == kDynamic && b.awake);
+                uint8_t f = 0;
+                if (on && relativeTravel(a, b, P.dt) > P.tol.speculative) {
+                    f |= kFlagFast;
+                    if (!isPlanar(a) && !isPlanar(b)) { f |= kFlagFastSolid; }
+                }
+                B.cflags[cf + i] = f | (on ? kFlagActive : 0);
+                return on;
+            },
+            [&](uint32_t i, uint32_t pos) { B.active[cf + pos] = i; });
+        const uint32_t* act = B.active + cf;
+        for (uint32_t x = threadIdx.x; x < nActive; x += blockDim.x) {
+            DContact& c = cs[act[x]];
+            prepareContact(B.bodies[c.bodyA], B.bodies[c.bodyB], c);
+        }
+        __syncthreads();
+        // Bodies of pairs closing faster than the restitution threshold are struck (src/world.cpp:1029-1049).
+        for (uint32_t x = threadIdx.x; x < nActive; x += blockDim.x) {
+            const DContact& c = cs[act[x]];
+            for (int i = 0; i < c.count; ++i) {
+                if (c.points[i].relativeVelocity >= -P.restitutionThreshold) { continue; }
+                if (B.bodies[c.bodyA].type == kDynamic) { B.struck[c.bodyA] = 1; }
+                if (B.bodies[c.bodyB].type == kDynamic) { B.struck[c.bodyB] = 1; }
+                break;
+            }
+        }
+        __syncthreads();
+        const uint32_t nImpact = blockCompact(
+            nActive,
+            [&](uint32_t x) {
+                const DContact& c = cs[act[x]];
+                return B.struck[c.bodyA] || B.struck[c.bodyB];
+            },
+            [&](uint32_t x, uint32_t pos) { B.impact[cf + pos] = act[x]; });
+        // Greedy coloring in active order, lowest free of 32 colors over the moving bodies
+        // (src/lanes.cpp:356-374); then the bucket order the lane batches follow (src/lanes.cpp:376-407).
+        if (threadIdx.x == 0) {
+            for (uint32_t x = 0; x < nActive; ++x) {
+                const uint32_t ci = act[x];
+                DContact& c = cs[ci];
+                uint8_t k = kNoColor;
+                c.flags &= ~kCLaned;
+                if (!(c.flags & kCPlanar) && !(c.rollingResistance > 0.0f)) {
+                    const DBody& a = B.bodies[c.bodyA];
+                    const DBody& b = B.bodies[c.bodyB];
+                    const bool ma = movingBody(a), mb = movingBody(b);
+                    const uint32_t taken = (ma ? B.bodyColors[c.bodyA] : 0u) | (mb ? B.bodyColors[c.bodyB] : 0u);
+                    if (taken != 0xffffffffu) {
+                        const int f = __ffs(~taken) - 1;
+                        if (ma) { B.bodyColors[c.bodyA] |= 1u << f; }
+                        if (mb) { B.bodyColors[c.bodyB] |= 1u << f; }
+                        k = (uint8_t)f;
+                        c.flags |= kCLaned;
+                    }
+                }
+                B.color[cf + ci] = k;
+            }
+            // Active list grouped by color, each color in active order; uncolored contacts form the rest.
+            uint32_t sizes[kColors + 1];
+            for (int k = 0; k <= kColors; ++k) { sizes[k] = 0; }
+            for (uint32_t x = 0; x < nActive; ++x) { ++sizes[B.color[cf + act[x]]]; }
+            uint32_t start[kColors + 1], sum = 0, used = 0;
+            for (int k = 0; k <= kColors; ++k) {
+                start[k] = sum;
+                wc.colorStart[k] = sum;
+                sum += sizes[k];
+                if (k < kColors && sizes[k] > 0) { used = (uint32_t)k + 1; }
+            }
+            wc.colorCount = used;
+            uint32_t restN = 0;
+            for (uint32_t x = 0; x < nActive; ++x) {
+                const uint32_t ci = act[x];
+                const uint8_t k = B.color[cf + ci];
+                if (k == kNoColor) {
+                    B.rest[cf + restN++] = ci;
+                } else {
+                    B.colored[cf + start[k]++] = ci;
+                }
+            }
+            wc.restCount = restN;
+            // The impact list takes the same colors.
+            for (int k = 0; k <= kColors; ++k) { sizes[k] = 0; }
+            for (uint32_t x = 0; x < nImpact; ++x) { ++sizes[B.color[cf + B.impact[cf + x]]]; }
+            sum = 0;
+            used = 0;
+            for (int k = 0; k <= kColors; ++k) {
+                start[k] = sum;
+                wc.impactColorStart[k] = sum;
+                sum += sizes[k];
+                if (k < kColors && sizes[k] > 0) { used = (uint32_t)k + 1; }
+            }
+            wc.impactColorCount = used;
+            restN = 0;
+            for (uint32_t x = 0; x < nImpact; ++x) {
+                const uint32_t ci = B.impact[cf + x];
+                const uint8_t k = B.color[cf + ci];
+                if (k == kNoColor) {
+                    B.impactRest[cf + restN++] = ci;
+                } else {
+                    B.impactColored[cf + start[k]++] = ci;
+                }
+            }
+            wc.impactRestCount = restN;
+            wc.activeCount = nActive;
+            wc.impactCount = nImpact;
+            uint32_t f = 0, fs = 0;
+            for (uint32_t x = 0; x < nActive; ++x) {
+                const uint8_t fl = B.cflags[cf + act[x]];
+                f += (fl & kFlagFast) ? 1 : 0;
+                fs += (fl & kFlagFastSolid) ? 1 : 0;
+            }
+            wc.fastCount = f;
+            wc.fastSolidCount = fs;
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------------------------------------
+// The substep (src/world.cpp:1658-1681).
+
+// Calls f(contact index) for every contact of each color in turn, the colors apart by a block barrier.
+template <class F>
+__device__ void forEachColor(const uint32_t* list, const uint32_t* start, uint32_t colors, F f) {
+    for (uint32_t k = 0; k < colors; ++k) {
+        const uint32_t end = start[k + 1];
+        for (uint32_t x = start[k] + threadIdx.x; x < end; x += blockDim.x) { f(list[x]); }
+        __syncthreads();
+    }
+}
+
+// A fast pair collided again with the remaining time (src/world.cpp:1074-1138).
+__device__ void refreshContact(const Batch& B, const StepParams& P, DContact& c, float remaining) {
+    const DBody& a = B.bodies[c.bodyA];
+    const DBody& b = B.bodies[c.bodyB];
+    const DShape sa = B.shapes[c.shapeA];
+    const DShape sb = B.shapes[c.shapeB];
+    // Polyhedra that turned little against each other keep the edge pair they met on (src/world.cpp:1051-1055).
+    const Quat now = conjugate(a.xf.q) * b.xf.q, then = conjugate(a.q0) * b.q0;
+    const bool little = fabsf(dot(now, then)) >= P.featureTurnCos;
+    Manifold m;
+    collidePair(B, P, sa, sb, remaining, m, little ? c.featKind : kFeatNone, c.featA, c.featB);
+    if (m.count == 0) {
+        c.count = 0;
+        return;
+    }
+    const DContact old = c;
+    c.flags &= ~kCReusable;
+    c.featKind = m.featKind;
+    c.featA = m.featA;
+    c.featB = m.featB;
+    c.normal = m.normal;
+    c.tangent1 = perpendicular(m.normal);
+    c.tangent2 = cross(m.normal, c.tangent1);
+    c.count = m.count;
+    for (int i = 0; i < m.count; ++i) {
+        DPoint& p = c.points[i];
+        p = DPoint{};
+        p.localA = applyInverse(a.xf, m.points[i].position);
+        p.separation = m.points[i].separation;
+        const Vec3 up = lift(a, b, m.normal, p.separation, P.tol.speculative);
+        p.anchorA = m.points[i].position - up - a.com;
+        p.anchorB = m.points[i].position + up - b.com;
+    }
+    prepareContact(a, b, c);
+    for (int i = 0; i < c.count; ++i) {
+        DPoint& p = c.points[i];
+        const int k = nearestPoint(old, p.localA);
+        if (k < 0) { continue; }
+        p.relativeVelocity = old.points[k].relativeVelocity;
+        p.maxNormalImpulse = old.points[k].maxNormalImpulse;
+    }
+    carryImpulses(old, c, P.tol.speculative * P.tol.speculative);
+}
+
+__global__ void __launch_bounds__(kMaxBlock) k_substep(Batch B, StepParams P, int sub) {
+    for (int o = blockIdx.x; o < B.nWorlds; o += gridDim.x) {
+        const uint32_t w = B.order[o];
+        const WorldInfo wi = B.info[w];
+        WorldCounts& wc = B.counts[w];
+        const uint32_t cf = wi.contactFirst;
+        DContact* cs = B.contacts + cf;
+        const uint32_t nActive = wc.activeCount;
+        const uint32_t* act = B.active + cf;
+        const int n = P.substeps;
+        const uint8_t againFlag = sub == n / 2 ? kFlagFast : kFlagFastSolid;
+        const uint32_t againCount = sub == n / 2 ? wc.fastCount : wc.fastSolidCount;
+        if (sub > 0 && againCount > 0) {
+            for (uint32_t i = threadIdx.x; i < wi.bodyCount; i += blockDim.x) {
+                DBody& b = B.bodies[wi.bodyFirst + i];
+                if (b.alive && b.type == kDynamic && b.awake) { updateInverseMass(b); }
+            }
+            __syncthreads();
+            for (uint32_t x = threadIdx.x; x < nActive; x += blockDim.x) {
+                const uint32_t ci = act[x];
+                if (B.cflags[cf + ci] & againFlag) { continue; }
+                DContact& c = cs[ci];
+                rebaseContact(B.bodies[c.bodyA], B.bodies[c.bodyB], c);
+            }
+            __syncthreads();
+            for (uint32_t i = threadIdx.x; i < wi.bodyCount; i += blockDim.x) {
+                DBody& b = B.bodies[wi.bodyFirst + i];
+                b.dp = zero3();
+                b.dq = qid();
+                b.qBase = b.xf.q;
+            }
+            __syncthreads();
+            const float remaining = (float)(n - sub) * P.h;
+            for (uint32_t x = threadIdx.x; x < nActive; x += blockDim.x) {
+                const uint32_t ci = act[x];
+                if (!(B.cflags[cf + ci] & againFlag)) { continue; }
+                refreshContact(B, P, cs[ci], remaining);
+            }
+            __syncthreads();
+        }
+        for (uint32_t i = threadIdx.x; i < wi.bodyCount; i += blockDim.x) {
+            integrateVelocity(B.bodies[wi.bodyFirst + i], P);
+        }
+        __syncthreads();
+        auto warm = [&](uint32_t ci, bool laned) {
+            DContact& c = cs[ci];
+            warmStartContact(B.bodies[c.bodyA], B.bodies[c.bodyB], c, laned);
+        };
+        auto solve = [&](uint32_t ci, bool bias) {
+            DContact& c = cs[ci];
+            solveContact(B.bodies[c.bodyA], B.bodies[c.bodyB], c, P, bias);
+        };
+        const uint32_t* colored = B.colored + cf;
+        const uint32_t* rest = B.rest + cf;
+        const uint32_t* icolored = B.impactColored + cf;
+        const uint32_t* irest = B.impactRest + cf;
+        forEachColor(colored, wc.colorStart, wc.colorCount, [&](uint32_t ci) { warm(ci, true); });
+        if (threadIdx.x == 0) {
+            for (uint32_t x = 0; x < wc.restCount; ++x) { warm(rest[x], false); }
+        }
+        __syncthreads();
+        for (int pass = 0; pass < 2; ++pass) {
+            const bool bias = pass == 0;
+            forEachColor(colored, wc.colorStart, wc.colorCount, [&](uint32_t ci) { solve(ci, bias); });
+            if (threadIdx.x == 0) {
+                for (uint32_t x = 0; x < wc.restCount; ++x) { solve(rest[x], bias); }
+            }
+            __syncthreads();
+            if (wc.impactCount > 0) {
+                forEachColor(icolored, wc.impactColorStart, wc.impactColorCount, [&](uint32_t ci) { solve(ci, bias); });
+                if (threadIdx.x == 0) {
+                    for (uint32_t x = 0; x < wc.impactRestCount; ++x) { solve(irest[x], bias); }
+                }
+                __syncthreads();
+            }
+            if (bias) {
+                for (uint32_t i = threadIdx.x; i < wi.bodyCount; i += blockDim.x) {
+                    integratePosition(B.bodies[wi.bodyFirst + i], P);
+                }
+                __syncthreads();
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------------------------
+// After the substeps (src/world.cpp:1682-1726).
+
+__device__ __forceinline__ uint32_t findRoot(uint32_t* parent, uint32_t x) {
+    while (parent[x] != x) {
+        parent[x] = parent[parent[x]];
+        x = parent[x];
+    }
+    return x;
+}
+
+__global__ void __launch_bounds__(kMaxBlock) k_finish(Batch B, StepParams P) {
+    for (int o = blockIdx.x; o < B.nWorlds; o += gridDim.x) {
+        const uint32_t w = B.order[o];
+        const WorldInfo wi = B.info[w];
+        WorldCounts& wc = B.counts[w];
+        const uint32_t cf = wi.contactFirst;
+        DContact* cs = B.contacts + cf;
+        // Restitution: colored contacts by color, then the rest in active order.
+        forEachColor(B.colored + cf, wc.colorStart, wc.colorCount, [&](uint32_t ci) {
+            DContact& c = cs[ci];
+            restituteContact(B.bodies[c.bodyA], B.bodies[c.bodyB], c, P, true);
+        });
+        if (threadIdx.x == 0) {
+            for (uint32_t x = 0; x < wc.restCount; ++x) {
+                DContact& c = cs[B.rest[cf + x]];
+                restituteContact(B.bodies[c.bodyA], B.bodies[c.bodyB], c, P, false);
+            }
+        }
+        __syncthreads();
+        uint32_t sweep = 0;
+        for (uint32_t i = threadIdx.x; i < wi.bodyCount; i += blockDim.x) {
+            const uint32_t g = wi.bodyFirst + i;
+            DBody& b = B.bodies[g];
+            if (!b.alive) { continue; }
+            limitSpeed(b, P.maxLinearSpeed, P.maxAngularSpeed);
+            b.force = zero3();
+            b.torque = zero3();
+            if (b.hasTarget) {
+                b.xf = b.target;
+                b.com = apply(b.xf, b.localCenter);
+                b.hasTarget = 0;
+            }
+            if (!(b.type != kStatic && !(b.type == kDynamic && !b.awake))) { continue; }
+            // Leaf refit over the new pose (src/world.cpp:1713-1718): shape bounds and the body's union.
+            bool any = false;
+            for (uint32_t x = 0; x < b.shapeCount; ++x) {
+                DShape& s = B.shapes[B.shapeList[b.shapeFirst + x]];
+                Vec3 lo, hi;
+                shapeBounds(s, B.cx.pt, b.xf * s.local, lo, hi);
+                s.lo = lo;
+                s.hi = hi;
+                if (s.kind == kHalfSpace) { continue; }
+                b.lo = any ? minVec(b.lo, lo) : lo;
+                b.hi = any ? maxVec(b.hi, hi) : hi;
+                any = true;
+            }
+            // Shapes that moved well past what the speculative contacts covered would be swept against
+            // their surroundings (src/world.cpp:1260-1278). This build counts them; the sweep itself is not run.
+            if (P.continuous && b.type == kDynamic && b.awake) {
+                const float moved = length(b.com - b.com0);
+                Quat d = normalize(b.xf.q * conjugate(b.q0));
+                if (d.w < 0.0f) { d = -d; }
+                const float sine = length(qvec(d));
+                const float angle = sine > 1.0e-7f ? 2.0f * atan2f(sine, d.w) : 0.0f;
+                for (uint32_t x = 0; x < b.shapeCount; ++x) {
+                    const DShape& s = B.shapes[B.shapeList[b.shapeFirst + x]];
+                    if (s.kind == kMesh || s.sensor) { continue; }
+                    const float reach = length(s.local.p - b.localCenter) + s.extent;
+                    const float travel = moved + angle * reach;
+                    if (travel > b.expectedTravel && travel > b.expectedTravel + 0.5f * s.minExtent) { ++sweep; }
+                }
+            }
+        }
+        if (sweep > 0) {
+            atomicAdd(&wc.sweepShapes, sweep);
+            atomicOr(&wc.flags, kDevSweepSkipped);
+        }
+        // Sleep (src/world.cpp:1174-1247).
+        const float threshold = P.sleepThreshold;
+        for (uint32_t i = threadIdx.x; i < wi.bodyCount; i += blockDim.x) {
+            const uint32_t g = wi.bodyFirst + i;
+            DBody& b = B.bodies[g];
+            B.unionParent[g] = i;
+            B.islandTime[g] = FLT_MAX;
+            if (!b.alive || b.type != kDynamic || !b.awake) { continue; }
+            const float speed = maxf(length(b.v), length(b.w) * b.extent);
+            if (!b.canSleep || speed > threshold) {
+                b.sleepTime = 0.0f;
+            } else {
+                b.sleepTime += P.dt;
+            }
+            if (!(isfinite(b.v.x) && isfinite(b.v.y) && isfinite(b.v.z) && isfinite(b.xf.p.x) && isfinite(b.xf.p.y) &&
+                  isfinite(b.xf.p.z))) {
+                atomicOr(&wc.flags, kDevNonFinite);
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            uint32_t* parent = B.unionParent + wi.bodyFirst;
+            float* islandTime = B.islandTime + wi.bodyFirst;
+            const uint32_t nc = wc.contactCount;
+            for (uint32_t ci = 0; ci < nc; ++ci) {
+                const DContact& c = cs[ci];
+                if (c.count == 0) { continue; }
+                DBody& a = B.bodies[c.bodyA];
+                DBody& b = B.bodies[c.bodyB];
+                const bool da = a.type == kDynamic && a.awake;
+                const bool db = b.type == kDynamic && b.awake;
+                if (da && db) {
+                    const uint32_t ra = findRoot(parent, c.bodyA - wi.bodyFirst), rb = findRoot(parent, c.bodyB - wi.bodyFirst);
+                    if (ra != rb) { parent[ra > rb ? ra : rb] = ra < rb ? ra : rb; }
+                } else if (da && b.type == kKinematic && movingAwake(b)) {
+                    a.sleepTime = 0.0f;
+                } else if (db && a.type == kKinematic && movingAwake(a)) {
+                    b.sleepTime = 0.0f;
+                }
+            }
+            uint32_t awakeBodies = 0, islands = 0;
+            for (uint32_t i = 0; i < wi.bodyCount; ++i) {
+                DBody& b = B.bodies[wi.bodyFirst + i];
+                if (!b.alive || b.type != kDynamic || !b.awake) { continue; }
+                const uint32_t r = findRoot(parent, i);
+                b.island = r;
+                ++awakeBodies;
+                if (r == i) { ++islands; }
+                islandTime[r] = minf(islandTime[r], b.sleepTime);
+            }
+            for (uint32_t i = 0; i < wi.bodyCount; ++i) {
+                DBody& b = B.bodies[wi.bodyFirst + i];
+                if (!b.alive || b.type != kDynamic || !b.awake) { continue; }
+                if (islandTime[findRoot(parent, i)] < P.timeToSleep) { continue; }
+                b.awake = 0;
+                b.v = zero3();
+                b.w = zero3();
+                updateInverseMass(b);
+            }
+            wc.awakeBodies = awakeBodies;
+            wc.awakeIslands = islands;
+        }
+        __syncthreads();
+    }
+}
+
+}

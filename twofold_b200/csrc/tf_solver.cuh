@@ -1,0 +1,271 @@
+// Contact preparation, solve, restitution and integration for one contact or one body.
+//
+// The reference solves colored contacts four at a time in SSE/NEON lanes and the rest one at a time; both
+// give the same bits (src/lanes.h:16-17, src/lanes.cpp:220-315 against src/solver.cpp:360-421). Here one
+// thread solves one contact with the scalar sequence, which is therefore exact for laned and rest contacts
+// alike. Contacts of one color move no body in common, so a color's contacts run in parallel with results
+// identical to any sequential order.
+//
+// Effective masses are not stored: each solve rebuilds a point's axes from its anchors and the bodies'
+// world inverse mass and inertia, which change only where the reference rebuilds its axes (step start and
+// the mid-step refresh), so the rebuilt axes are the reference's stored axes bit for bit.
+#pragma once
+
+#include "tf_body.cuh"
+#include "tf_collide.cuh"
+
+namespace tfb {
+
+// One direction at a contact point (src/internal.h:508-520, src/solver.cpp:5-17).
+struct Axis {
+    Vec3 armA, armB;
+    Vec3 linearA, angularA;
+    Vec3 linearB, angularB;
+    float mass;
+};
+
+TF_HD Axis makeAxis(const DBody& a, const DBody& b, const Vec3& ra, const Vec3& rb, const Vec3& d) {
+    Axis x;
+    x.armA = cross(ra, d);
+    x.armB = cross(rb, d);
+    x.linearA = a.invMassWorld * d;
+    x.angularA = a.invInertiaWorld * x.armA;
+    x.linearB = b.invMassWorld * d;
+    x.angularB = b.invInertiaWorld * x.armB;
+    const float k = dot(d, x.linearA) + dot(d, x.linearB) + dot(x.armA, x.angularA) + dot(x.armB, x.angularB);
+    x.mass = k > 1e-6f * (a.invMass + b.invMass) ? 1.0f / k : 0.0f;
+    return x;
+}
+
+TF_HD float speedAlong(const DBody& a, const DBody& b, const Vec3& d, const Axis& x) {
+    return dot(d, b.v - a.v) + dot(x.armB, b.w) - dot(x.armA, a.w);
+}
+
+TF_HD void pushMoving(DBody& a, DBody& b, const Axis& x, float impulse, bool moveA, bool moveB) {
+    if (moveA) {
+        a.v -= x.linearA * impulse;
+        a.w -= x.angularA * impulse;
+    }
+    if (moveB) {
+        b.v += x.linearB * impulse;
+        b.w += x.angularB * impulse;
+    }
+}
+
+// Where the body has turned r since the substep's base pose (src/solver.cpp:58-61).
+TF_HD Vec3 turned(const DBody& b, const Vec3& r) {
+    return b.dq.x == 0.0f && b.dq.y == 0.0f && b.dq.z == 0.0f ? r : rotate(b.dq, r);
+}
+
+TF_HD bool anchored(const DBody& b) { return b.type != kDynamic || !b.awake; }
+
+TF_HD Softness makeSoft(float hertz, float zeta, float h) {
+    if (hertz == 0.0f) { return { 0.0f, 1.0f, 0.0f }; }
+    const float omega = 2.0f * 3.14159265358979f * hertz;
+    const float a1 = 2.0f * zeta + h * omega;
+    const float a2 = h * omega * a1;
+    const float a3 = 1.0f / (1.0f + a2);
+    return { omega / a1, a2 * a3, a3 };
+}
+
+// Whether every body the contact moves is a dynamic body locked to one plane n holding the normal
+// (src/solver.cpp:66-81).
+TF_HD bool planarContact(const DBody& a, const DBody& b, const Vec3& normal, Vec3& n) {
+    const DBody* first = nullptr;
+    const DBody* both[2] = { &a, &b };
+    for (int k = 0; k < 2; ++k) {
+        const DBody* x = both[k];
+        if (x->type == kStatic) { continue; }
+        if (x->type == kKinematic || !isPlanar(*x)) { return false; }
+        if (!first) {
+            first = x;
+            n = planeNormal(*x);
+        } else if (fabsf(dot(n, planeNormal(*x))) < 0.9999f) {
+            return false;
+        }
+    }
+    return first && fabsf(dot(normal, n)) < 1e-3f;
+}
+
+// Adjusted separation, approach speed and rolling radius at the step's start (src/solver.cpp:264-291).
+// Planar contacts are not run by this build (the caller refuses scenes with planar bodies).
+TF_HD void prepareContact(const DBody& a, const DBody& b, DContact& c) {
+    Vec3 plane = c.plane;
+    const bool planar = planarContact(a, b, c.normal, plane);
+    c.plane = plane;
+    c.flags = planar ? (c.flags | kCPlanar) : (c.flags & ~kCPlanar);
+    for (int i = 0; i < c.count; ++i) {
+        DPoint& p = c.points[i];
+        p.adjustedSeparation = p.separation - dot(p.anchorB - p.anchorA, c.normal);
+        p.relativeVelocity = dot(c.normal, b.v - a.v) + dot(cross(p.anchorB, c.normal), b.w) -
+                             dot(cross(p.anchorA, c.normal), a.w);
+        p.maxNormalImpulse = 0.0f;
+    }
+    if (c.rollingResistance > 0.0f && c.count > 0) {
+        float ha = 0.0f, hb = 0.0f;
+        for (int i = 0; i < c.count; ++i) {
+            ha += fabsf(dot(c.points[i].anchorA, c.normal));
+            hb += fabsf(dot(c.points[i].anchorB, c.normal));
+        }
+        if (a.type != kDynamic) { ha = 0.0f; }
+        if (b.type != kDynamic) { hb = 0.0f; }
+        c.rollingRadius = maxf(ha, hb) / (float)c.count;
+    }
+}
+
+// Re-expresses anchors as the bodies' current lever arms before their dp and dq are reset
+// (src/solver.cpp:293-306).
+TF_HD void rebaseContact(const DBody& a, const DBody& b, DContact& c) {
+    const float shift = dot(b.dp - a.dp, c.normal);
+    for (int i = 0; i < c.count; ++i) {
+        DPoint& p = c.points[i];
+        p.anchorA = rotate(a.dq, p.anchorA);
+        p.anchorB = rotate(b.dq, p.anchorB);
+        p.adjustedSeparation += shift;
+    }
+}
+
+// Applies the stored impulses (src/solver.cpp:319-358 and src/lanes.cpp:195-217). A laned contact pushes only
+// the bodies that move; a contact solved on its own pushes both, as the reference's scalar warm start does
+// (the anchored body's zero inverse mass leaves it unchanged). Contacts solved on their own run one at a
+// time, so the unmasked push never races.
+TF_HD void warmStartContact(DBody& a, DBody& b, const DContact& c, bool laned) {
+    const bool moveA = !laned || !anchored(a), moveB = !laned || !anchored(b);
+    for (int i = 0; i < c.count; ++i) {
+        const DPoint& p = c.points[i];
+        const Axis xn = makeAxis(a, b, p.anchorA, p.anchorB, c.normal);
+        const Axis x1 = makeAxis(a, b, p.anchorA, p.anchorB, c.tangent1);
+        const Axis x2 = makeAxis(a, b, p.anchorA, p.anchorB, c.tangent2);
+        pushMoving(a, b, xn, p.normalImpulse, moveA, moveB);
+        pushMoving(a, b, x1, dot(p.tangentImpulse, c.tangent1), moveA, moveB);
+        pushMoving(a, b, x2, dot(p.tangentImpulse, c.tangent2), moveA, moveB);
+    }
+    if (c.rollingResistance > 0.0f) {
+        a.w -= a.invInertiaWorld * c.rollingImpulse;
+        b.w += b.invInertiaWorld * c.rollingImpulse;
+    }
+}
+
+// One step along the relative spin, held to the rolling limit (src/solver.cpp:225-251). Rolling contacts are
+// never laned, so this runs one contact at a time and pushes both bodies as the reference does.
+TF_HD void resistTurning(DBody& a, DBody& b, DContact& c) {
+    const Vec3 spin = b.w - a.w;
+    const float speed = length(spin);
+    Vec3 total = c.rollingImpulse;
+    if (speed > 0.0f) {
+        const Vec3 d = spin * (1.0f / speed);
+        const Vec3 ia = a.invInertiaWorld * d, ib = b.invInertiaWorld * d;
+        const float k = dot(d, ia) + dot(d, ib);
+        if (k > 0.0f) {
+            const float lambda = -speed / k;
+            total += d * lambda;
+            a.w -= ia * lambda;
+            b.w += ib * lambda;
+        }
+    }
+    float normal = 0.0f;
+    for (int i = 0; i < c.count; ++i) { normal += c.points[i].normalImpulse; }
+    const float limit = c.rollingResistance * c.rollingRadius * normal;
+    const float mag = length(total);
+    if (mag > limit) {
+        const Vec3 fix = total * (limit / mag) - total;
+        a.w -= a.invInertiaWorld * fix;
+        b.w += b.invInertiaWorld * fix;
+        total += fix;
+    }
+    c.rollingImpulse = total;
+}
+
+// The soft normal rows, then friction (forward in the biased pass, reverse in relax), then rolling
+// (src/solver.cpp:360-421).
+TF_HD void solveContact(DBody& a, DBody& b, DContact& c, const StepParams& P, bool useBias) {
+    const bool moveA = !anchored(a), moveB = !anchored(b);
+    const Softness soft = (!moveA || !moveB) ? P.staticSoft : P.contactSoft;
+    const Vec3 dp = b.dp - a.dp;
+    for (int i = 0; i < c.count; ++i) {
+        DPoint& p = c.points[i];
+        const Vec3 d = dp + turned(b, p.anchorB) - turned(a, p.anchorA);
+        const float sep = dot(d, c.normal) + p.adjustedSeparation;
+        float bias = 0.0f, massScale = 1.0f, impulseScale = 0.0f;
+        if (sep > 0.0f) {
+            bias = sep * P.invH;
+        } else if (useBias) {
+            bias = maxf(soft.biasRate * sep, -P.maxPushout);
+            massScale = soft.massScale;
+            impulseScale = soft.impulseScale;
+        }
+        const Axis x = makeAxis(a, b, p.anchorA, p.anchorB, c.normal);
+        const float vn = speedAlong(a, b, c.normal, x);
+        float impulse = -x.mass * massScale * (vn + bias) - impulseScale * p.normalImpulse;
+        const float total = maxf(p.normalImpulse + impulse, 0.0f);
+        impulse = total - p.normalImpulse;
+        p.normalImpulse = total;
+        p.maxNormalImpulse = maxf(p.maxNormalImpulse, impulse);
+        pushMoving(a, b, x, impulse, moveA, moveB);
+    }
+    for (int j = 0; j < c.count; ++j) {
+        const int i = useBias ? j : c.count - 1 - j;
+        DPoint& p = c.points[i];
+        const Axis x1 = makeAxis(a, b, p.anchorA, p.anchorB, c.tangent1);
+        const Axis x2 = makeAxis(a, b, p.anchorA, p.anchorB, c.tangent2);
+        const float old1 = dot(p.tangentImpulse, c.tangent1), old2 = dot(p.tangentImpulse, c.tangent2);
+        float t1 = old1 - x1.mass * speedAlong(a, b, c.tangent1, x1);
+        float t2 = old2 - x2.mass * speedAlong(a, b, c.tangent2, x2);
+        const float limit = c.friction * p.normalImpulse;
+        const float mag = sqrtf(t1 * t1 + t2 * t2);
+        if (mag > limit) {
+            const float scale = mag > 0.0f ? limit / mag : 0.0f;
+            t1 *= scale;
+            t2 *= scale;
+        }
+        p.tangentImpulse = c.tangent1 * t1 + c.tangent2 * t2;
+        pushMoving(a, b, x1, t1 - old1, moveA, moveB);
+        pushMoving(a, b, x2, t2 - old2, moveA, moveB);
+    }
+    if (c.rollingResistance > 0.0f) { resistTurning(a, b, c); }
+}
+
+// One restitution pass over the points that approached fast (src/solver.cpp:423-460, src/lanes.cpp:318-352),
+// pushing as warmStartContact does.
+TF_HD void restituteContact(DBody& a, DBody& b, DContact& c, const StepParams& P, bool laned) {
+    if (c.restitution == 0.0f) { return; }
+    const bool moveA = !laned || !anchored(a), moveB = !laned || !anchored(b);
+    for (int i = 0; i < c.count; ++i) {
+        DPoint& p = c.points[i];
+        if (p.relativeVelocity > -P.restitutionThreshold || p.maxNormalImpulse == 0.0f) { continue; }
+        const Axis x = makeAxis(a, b, p.anchorA, p.anchorB, c.normal);
+        const float vn = speedAlong(a, b, c.normal, x);
+        float impulse = -x.mass * (vn + c.restitution * p.relativeVelocity);
+        const float total = maxf(p.normalImpulse + impulse, 0.0f);
+        impulse = total - p.normalImpulse;
+        p.normalImpulse = total;
+        p.maxNormalImpulse = maxf(p.maxNormalImpulse, impulse);
+        pushMoving(a, b, x, impulse, moveA, moveB);
+    }
+}
+
+// Gravity, forces, damping, locks and the speed limits (src/world.cpp:1141-1151).
+TF_HD void integrateVelocity(DBody& b, const StepParams& P) {
+    if (!b.alive || b.type != kDynamic || !b.awake) { return; }
+    const float h = P.h;
+    b.v = b.v + (P.gravity * b.gravityScale + b.force * b.invMass) * h;
+    b.v = b.linearProj * (b.v * (1.0f / (1.0f + h * b.linearDamping)));
+    b.w = b.w + b.invInertiaWorld * b.torque * h;
+    b.w = b.angularProj * (b.w * (1.0f / (1.0f + h * b.angularDamping)));
+    limitSpeed(b, P.maxLinearSpeed, P.maxAngularSpeed);
+}
+
+// The speed limits, then the pose update (src/world.cpp:1161-1172).
+TF_HD void integratePosition(DBody& b, const StepParams& P) {
+    if (b.alive) { limitSpeed(b, P.maxLinearSpeed, P.maxAngularSpeed); }
+    if (!b.alive || b.type == kStatic) { return; }
+    if (b.type == kDynamic && !b.awake) { return; }
+    const float h = P.h;
+    b.com += b.v * h;
+    b.dp += b.v * h;
+    b.xf.q = integrate(b.xf.q, b.w, h);
+    b.dq = b.xf.q * conjugate(b.qBase);
+    b.xf.p = b.com - rotate(b.xf.q, b.localCenter);
+}
+
+}

@@ -1,0 +1,233 @@
+// Device-resident state of a batch of worlds.
+//
+// Bodies, shapes and contacts are arrays of plain structs in HBM, one segment per world. Their fields
+// follow the reference's Body (src/internal.h:257-325), Shape (:152-187) and Contact (:428-503) so each
+// kernel reads like the step it restates; the structs hold no pointers and copy to and from the host as
+// bytes. Indices stored in bodies, shapes and contacts are global (across the batch); contact keys use
+// the world-local shape indices, as the reference's keys do (src/world.cpp:42).
+#pragma once
+
+#include "tf_math.cuh"
+
+namespace tfb {
+
+enum BodyType : uint32_t { kStatic = 0, kKinematic = 1, kDynamic = 2 };
+
+// ShapeKind (src/internal.h:113).
+enum ShapeKind : uint32_t { kSphere = 0, kConvex = 1, kHalfSpace = 2, kMesh = 3, kCylinder = 4 };
+
+// Feature::Kind (src/internal.h:335).
+enum FeatureKind : int32_t { kFeatNone = 0, kFeatFaceA = 1, kFeatFaceB = 2, kFeatEdges = 3 };
+
+constexpr uint32_t kLockTX = 1u << 0, kLockTY = 1u << 1, kLockTZ = 1u << 2;
+constexpr uint32_t kLockRX = 1u << 3, kLockRY = 1u << 4, kLockRZ = 1u << 5;
+constexpr uint32_t kLockPlanar = kLockTZ | kLockRX | kLockRY;
+
+constexpr int kColors = 32;
+constexpr int kNoColor = kColors;
+
+struct alignas(16) DBody {
+    // Read and written by every solve.
+    Vec3 v;
+    Vec3 w;
+    Vec3 dp;
+    Quat dq;
+    Mat3 invMassWorld;
+    Mat3 invInertiaWorld;
+    float invMass;
+    float planeInvMass;
+    float planeInvInertia;
+    uint32_t type;
+    uint32_t awake;
+    uint32_t alive;
+
+    Transform xf;
+    Vec3 com;
+    Vec3 localCenter;
+    float extent;
+    Vec3 force;
+    Vec3 torque;
+    float mass;
+    Mat3 inertia;
+    float linearDamping;
+    float angularDamping;
+    float gravityScale;
+    uint32_t locks;
+    Quat lockFrame;
+    uint32_t canSleep;
+    float sleepTime;
+    uint32_t island;
+    uint32_t hasTarget;
+    Transform target;
+    // Bounds of the body's shapes other than half-spaces; hasBounds is 0 when it has none (no tree leaf).
+    Vec3 lo, hi;
+    uint32_t hasBounds;
+    float kept;
+    Mat3 linearProj;
+    Mat3 angularProj;
+    Quat qBase;
+    Quat q0;
+    Vec3 com0;
+    float expectedTravel;
+    // The body's shapes: shapeList[shapeFirst .. shapeFirst + shapeCount), global shape indices.
+    uint32_t shapeFirst;
+    uint32_t shapeCount;
+    uint32_t world;
+    uint32_t pad;
+};
+
+struct alignas(16) DShape {
+    uint32_t body;      // global body index
+    uint32_t index;     // index within its world, the one contact keys use
+    uint32_t kind;      // ShapeKind
+    uint32_t geometry;  // tf_geometry
+    Transform local;
+    float friction;
+    float restitution;
+    float rollingResistance;
+    uint32_t category;
+    uint32_t mask;
+    uint32_t sensor;
+    uint32_t alive;
+    float radius;
+    float halfHeight;
+    Vec3 halfExtents;
+    int32_t poly;  // index into the polyhedron table, -1 for none
+    float extent;
+    float minExtent;
+    Vec3 centroid;
+    Vec3 lo, hi;
+};
+
+// A convex polyhedron (src/internal.h:89-111) stored as ranges of the shared tables.
+struct DPoly {
+    int32_t vFirst, vCount;
+    int32_t fFirst, fCount;  // faces, normals and offsets share this range
+    int32_t eFirst, eCount;  // edges and arcs share this range
+    int32_t iFirst, iCount;  // face vertex loops
+    Vec3 centroid;
+    Vec3 lo, hi;
+};
+
+// Face and edge fields index within their own polyhedron (vertex k is verts[vFirst + k]).
+struct DFace {
+    int32_t first, count;  // into the polyhedron's index range
+};
+
+struct DEdge {
+    int32_t v0, v1, f0, f1;
+    float length;
+};
+
+struct alignas(16) DPoint {
+    Vec3 anchorA, anchorB;
+    float adjustedSeparation;
+    float normalImpulse;
+    Vec3 tangentImpulse;
+    float maxNormalImpulse;
+    float relativeVelocity;
+    float separation;
+    Vec3 surfaceA, surfaceB;
+    Vec3 localA;
+    float pad;
+};
+
+constexpr uint32_t kCPlanar = 1u << 0, kCReusable = 1u << 1, kCRemoved = 1u << 2, kCTouched = 1u << 3,
+                   kCLaned = 1u << 4;
+
+struct alignas(16) DContact {
+    uint64_t key;
+    uint32_t part;
+    uint32_t shapeA, shapeB;  // global
+    uint32_t bodyA, bodyB;    // global
+    int32_t count;
+    uint32_t flags;
+    Vec3 normal, tangent1, tangent2;
+    float friction;
+    float restitution;
+    float rollingResistance;
+    float rollingRadius;
+    Vec3 rollingImpulse;
+    Vec3 plane;
+    Vec3 localNormal;
+    Vec3 baseOffset;
+    Quat baseTurn;
+    int32_t featKind, featA, featB;
+    DPoint points[4];
+};
+
+// The planar axes of a contact point (src/internal.h:528-531).
+struct DPlanarAxes {
+    float normalA, normalB, normalMass;
+    float tangentA, tangentB, tangentMass;
+};
+
+// Per-world placement of every array segment, fixed between re-layouts.
+struct WorldInfo {
+    uint32_t bodyFirst, bodyCount;
+    uint32_t shapeFirst, shapeCount;
+    uint32_t candFirst, candCap;      // candidate keys
+    uint32_t contactFirst, contactCap;  // contacts, both buffers, and every per-contact list
+    uint32_t planeFirst, planeCount;  // half-space shapes, global indices in planeList
+};
+
+// Per-world results and lists of the current step.
+struct WorldCounts {
+    uint32_t candCount;
+    uint32_t contactCount;  // in the current contact buffer
+    uint32_t activeCount;
+    uint32_t impactCount;
+    uint32_t fastCount;
+    uint32_t fastSolidCount;
+    uint32_t restCount;        // active contacts solved one at a time
+    uint32_t impactRestCount;
+    uint32_t colorCount;       // 1 + highest color used, active list
+    uint32_t impactColorCount;
+    uint32_t awakeBodies;
+    uint32_t awakeIslands;
+    uint32_t touching;
+    uint32_t wakePending;
+    uint32_t flags;            // tf_device_flags
+    uint32_t candNeeded;       // largest count seen, for growing capacities
+    uint32_t contactNeeded;
+    uint32_t sweepShapes;      // shapes the continuous pass would sweep
+    uint32_t colorStart[kColors + 1];
+    uint32_t impactColorStart[kColors + 1];
+};
+
+struct Tolerances {
+    float linearSlop;
+    float speculative;
+};
+
+struct Softness {
+    float biasRate;
+    float massScale;
+    float impulseScale;
+};
+
+// WorldSettings plus everything derived from it that the kernels need (src/world.cpp:222-229, 1634-1642).
+struct StepParams {
+    Vec3 gravity;
+    float lengthUnit;
+    int substeps;
+    float dt;
+    float h;
+    float invH;
+    Softness contactSoft;
+    Softness staticSoft;
+    float maxPushout;
+    float restitutionThreshold;
+    float maxLinearSpeed;   // already scaled by lengthUnit
+    float maxAngularSpeed;
+    float sleepThreshold;   // scaled
+    float timeToSleep;
+    float reuseDistance;    // scaled
+    float reuseCos;         // cos(0.5 * contactReuseAngle), computed on the host with the C library
+    float featureTurnCos;   // cos(0.5 * 0.1), same
+    float treeMargin;       // kTreeMargin * lengthUnit
+    Tolerances tol;
+    int continuous;
+};
+
+}

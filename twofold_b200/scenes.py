@@ -1,0 +1,264 @@
+"""Seeded synthetic scenes for the five benchmark configurations, as descriptor arrays.
+
+Both the B200 library and the reference oracle are built from exactly these arrays, so both sides step
+identical input. No public dataset exists for this path; every scene is generated from a seed.
+
+A `Scene` is a list of worlds. Each world holds numpy structured arrays laid out like tf_body_desc and
+tf_shape_desc (include/twofold_b200.h) plus `body_of`, the index of each shape's body in its world.
+"""
+import ctypes as C
+import math
+
+import numpy as np
+
+from . import abi
+
+
+def _dtype_of(struct):
+    names, formats, offsets = [], [], []
+    for name, ctype in struct._fields_:
+        off = getattr(struct, name).offset
+        if isinstance(ctype, type) and issubclass(ctype, C._Pointer):
+            fmt = np.uint64
+        else:
+            fmt = np.dtype(ctype)
+        names.append(name)
+        formats.append(fmt)
+        offsets.append(off)
+    return np.dtype({"names": names, "formats": formats, "offsets": offsets, "itemsize": C.sizeof(struct)})
+
+
+BODY_DTYPE = _dtype_of(abi.tf_body_desc)
+SHAPE_DTYPE = _dtype_of(abi.tf_shape_desc)
+
+F32 = np.float32
+
+
+def _f(x):
+    return np.float32(x)
+
+
+def from_to_z_to_y():
+    """Quat::fromTo({0,0,1}, {0,1,0}) in float arithmetic (include/twofold/math.h:150-156)."""
+    # d = 0, c = cross(z, y) = (-1, 0, 0), s = sqrt((1 + d) * 2)
+    s = np.sqrt(_f(2.0), dtype=F32)
+    return (_f(-1.0) / s, _f(0.0), _f(0.0), _f(0.5) * s)
+
+
+GROUND_ROTATION = from_to_z_to_y()
+
+
+class World:
+    def __init__(self, bodies, shapes, body_of, meta=None):
+        self.bodies = bodies
+        self.shapes = shapes
+        self.body_of = np.ascontiguousarray(body_of, dtype=np.uint32)
+        self.meta = meta or {}
+        self.keepalive = []
+
+    @property
+    def dynamic_count(self):
+        return int(np.count_nonzero(self.bodies["type"] == abi.TF_DYNAMIC))
+
+
+class Scene:
+    def __init__(self, name, worlds, settings=None, dt=1.0 / 60.0, steps=1):
+        self.name = name
+        self.worlds = worlds
+        self.settings = settings if settings is not None else abi.default_settings()
+        self.dt = float(np.float32(dt))
+        self.steps = steps
+
+    @property
+    def body_count(self):
+        return sum(len(w.bodies) for w in self.worlds)
+
+    @property
+    def dynamic_count(self):
+        return sum(w.dynamic_count for w in self.worlds)
+
+
+def _bodies(n):
+    b = np.zeros(n, dtype=BODY_DTYPE)
+    b["type"] = abi.TF_DYNAMIC
+    b["rotation"][:, 3] = 1.0
+    b["lock_frame"][:, 3] = 1.0
+    b["gravity_scale"] = 1.0
+    b["awake"] = 1
+    b["can_sleep"] = 1
+    return b
+
+
+def _shapes(n):
+    s = np.zeros(n, dtype=SHAPE_DTYPE)
+    s["geometry"] = abi.TF_BOX
+    s["radius"] = 0.5
+    s["half_extents"] = 0.5
+    s["half_height"] = 0.5
+    s["max_vertices"] = 64
+    s["z_min"] = -0.5
+    s["z_max"] = 0.5
+    s["rotation"][:, 3] = 1.0
+    s["density"] = 1.0
+    s["friction"] = 0.5
+    s["category"] = 1
+    s["mask"] = 0xFFFFFFFF
+    return s
+
+
+def _ground(bodies, shapes, friction=0.6, restitution=0.0):
+    """A static half-space y <= 0, as tests/test_world.cpp:16-26 adds it."""
+    bodies["type"][0] = abi.TF_STATIC
+    bodies["rotation"][0] = GROUND_ROTATION
+    shapes["geometry"][0] = abi.TF_HALFSPACE
+    shapes["friction"][0] = friction
+    shapes["restitution"][0] = restitution
+
+
+def _uniform_quats(rng, n):
+    """Shoemake's uniform random rotations."""
+    u1, u2, u3 = rng.random(n), rng.random(n), rng.random(n)
+    a, b = np.sqrt(1.0 - u1), np.sqrt(u1)
+    q = np.stack([a * np.sin(2 * np.pi * u2), a * np.cos(2 * np.pi * u2), b * np.sin(2 * np.pi * u3),
+                  b * np.cos(2 * np.pi * u3)], axis=1)
+    return q.astype(F32)
+
+
+def pyramid(rows=20, pitch=1.0, jitter=1e-4, seed=0, friction=0.6, sleep=False):
+    """Box pyramid: `rows` layers of unit boxes (half extents 0.5, density 1) on a static half-space,
+    row r holding rows - r boxes at pitch spacing, every coordinate jittered by U[-jitter, jitter]."""
+    n = rows * (rows + 1) // 2
+    rng = np.random.default_rng(seed)
+    bodies, shapes = _bodies(n + 1), _shapes(n + 1)
+    _ground(bodies, shapes, friction=friction)
+    k = 1
+    for r in range(rows):
+        for i in range(rows - r):
+            x = (i - (rows - 1 - r) / 2.0) * pitch
+            y = 0.5 + r * pitch
+            bodies["position"][k] = (x, y, 0.0)
+            k += 1
+    bodies["position"][1:] += rng.uniform(-jitter, jitter, size=(n, 3)).astype(F32)
+    bodies["can_sleep"][1:] = 1 if sleep else 0
+    shapes["friction"][1:] = friction
+    return World(bodies, shapes, np.arange(n + 1), meta={"kind": "pyramid"})
+
+
+def config1():
+    """Box pyramid, plain method: 20 layers, 210 dynamic unit boxes, sleeping off, 300 steps."""
+    return Scene("box_pyramid_210", [pyramid(20)], steps=300)
+
+
+def _world_c4(rng, n_bodies):
+    bodies, shapes = _bodies(n_bodies + 1), _shapes(n_bodies + 1)
+    friction = _f(rng.uniform(0.2, 1.0))
+    restitution = _f(rng.uniform(0.0, 0.3))
+    _ground(bodies, shapes, friction=friction, restitution=restitution)
+    is_box = rng.random(n_bodies) < 0.7
+    half = rng.uniform(0.2, 0.6, size=(n_bodies, 3)).astype(F32)
+    radius = rng.uniform(0.2, 0.5, size=n_bodies).astype(F32)
+    g = np.where(is_box, abi.TF_BOX, abi.TF_SPHERE)
+    shapes["geometry"][1:] = g
+    shapes["half_extents"][1:] = half
+    shapes["radius"][1:] = radius
+    shapes["friction"][1:] = friction
+    shapes["restitution"][1:] = restitution
+    if rng.random() < 0.5:
+        # Stack: columns on a 1.3 m grid over the 10 x 10 m footprint, layers 1.3 m apart.
+        cols = 7
+        idx = np.arange(n_bodies)
+        layer, cell = idx // (cols * cols), idx % (cols * cols)
+        cx, cz = cell % cols, cell // cols
+        pos = np.stack([(cx - (cols - 1) / 2.0) * 1.3, 0.65 + 1.3 * layer, (cz - (cols - 1) / 2.0) * 1.3], axis=1)
+        bodies["position"][1:] = pos.astype(F32)
+        kind = "stack"
+    else:
+        # Scatter: jittered cells over the footprint, rising from 1 m, randomly turned. Cells are wide enough
+        # that bounding spheres (at most 1.04 m for the largest box) never overlap.
+        cols, pitch = 5, 2.1
+        idx = np.arange(n_bodies)
+        layer, cell = idx // (cols * cols), idx % (cols * cols)
+        cx, cz = cell % cols, cell // cols
+        jit = rng.uniform(-0.02, 0.02, size=(n_bodies, 3))
+        pos = np.stack([(cx - (cols - 1) / 2.0) * pitch, 1.1 + pitch * layer, (cz - (cols - 1) / 2.0) * pitch],
+                       axis=1) + jit
+        bodies["position"][1:] = pos.astype(F32)
+        bodies["rotation"][1:] = _uniform_quats(rng, n_bodies)
+        kind = "scatter"
+    return World(bodies, shapes, np.arange(n_bodies + 1), meta={"kind": kind})
+
+
+def config4(n_worlds=4096, seed=0, min_bodies=8, max_bodies=512):
+    """Batched uneven worlds: body counts log-uniform in [8, 512], 70% boxes and 30% spheres in a random
+    stack or scatter above a half-space, per-world friction U[0.2, 1] and restitution U[0, 0.3]."""
+    worlds = []
+    for w in range(n_worlds):
+        rng = np.random.default_rng([seed, w])
+        n = int(math.floor(math.exp(rng.uniform(math.log(min_bodies), math.log(max_bodies + 1)))))
+        n = max(min_bodies, min(max_bodies, n))
+        worlds.append(_world_c4(rng, n))
+    return Scene("batched_uneven_4096", worlds, steps=240)
+
+
+def impact_world(rng):
+    """One world of the differentiable impact: a 4x4x4 wall of 0.25 m boxes hit by a dense sphere."""
+    n = 64
+    bodies, shapes = _bodies(n + 2), _shapes(n + 2)
+    friction = _f(rng.uniform(0.3, 0.9))
+    _ground(bodies, shapes, friction=friction)
+    mass = rng.uniform(0.5, 2.0, size=n).astype(F32)
+    k = 1
+    for i in range(4):
+        for j in range(4):
+            for kk in range(4):
+                bodies["position"][k] = (3.0 + 0.5 * (i - 1.5), 0.25 + 0.5 * j, 0.5 * (kk - 1.5))
+                k += 1
+    shapes["half_extents"][1:n + 1] = 0.25
+    shapes["density"][1:n + 1] = mass / _f(0.125)
+    shapes["friction"][1:] = friction
+    bodies["position"][n + 1] = (0.0, 0.5, 0.0)
+    bodies["linear_velocity"][n + 1] = (np.array([10.0, 2.0, 0.0]) + rng.normal(0.0, 1.0, size=3)).astype(F32)
+    shapes["geometry"][n + 1] = abi.TF_SPHERE
+    shapes["radius"][n + 1] = 0.25
+    shapes["density"][n + 1] = 8.0
+    return World(bodies, shapes, np.arange(n + 2), meta={"kind": "impact", "mass": mass})
+
+
+def config5(n_worlds=1024, seed=0):
+    """Differentiable batched impact: 1024 walls of 64 boxes hit by a sphere, 120 steps."""
+    worlds = [impact_world(np.random.default_rng([seed, 5, w])) for w in range(n_worlds)]
+    return Scene("impact_1024", worlds, steps=120)
+
+
+def single(kind="box_on_ground", **kw):
+    """Small hand-checkable worlds used by the unit parity tests."""
+    if kind == "box_on_ground":
+        b, s = _bodies(2), _shapes(2)
+        _ground(b, s)
+        b["position"][1] = kw.get("position", (0.0, 2.0, 0.0))
+        b["rotation"][1] = kw.get("rotation", (0, 0, 0, 1))
+        s["friction"][1] = 0.6
+        return World(b, s, np.arange(2))
+    if kind == "sphere_on_ground":
+        b, s = _bodies(2), _shapes(2)
+        _ground(b, s)
+        b["position"][1] = kw.get("position", (0.0, 2.0, 0.0))
+        s["geometry"][1] = abi.TF_SPHERE
+        s["radius"][1] = kw.get("radius", 0.5)
+        s["restitution"][1] = kw.get("restitution", 0.0)
+        return World(b, s, np.arange(2))
+    if kind == "boxes":
+        # n randomly turned boxes dropped in a column onto a static box floor.
+        n = kw.get("n", 8)
+        rng = np.random.default_rng(kw.get("seed", 0))
+        b, s = _bodies(n + 1), _shapes(n + 1)
+        b["type"][0] = abi.TF_STATIC
+        b["position"][0] = (0.0, -0.5, 0.0)
+        s["half_extents"][0] = (10.0, 0.5, 10.0)
+        for i in range(1, n + 1):
+            b["position"][i] = (rng.uniform(-0.3, 0.3), 0.6 + 1.2 * i, rng.uniform(-0.3, 0.3))
+        b["rotation"][1:] = _uniform_quats(rng, n)
+        s["half_extents"][1:] = rng.uniform(0.2, 0.5, size=(n, 3)).astype(F32)
+        s["friction"] = 0.6
+        return World(b, s, np.arange(n + 1))
+    raise ValueError(kind)

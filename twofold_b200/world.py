@@ -1,0 +1,112 @@
+"""Python view of the C ABI: a batch of worlds built from scenes.Scene descriptor arrays.
+
+This is how tests and bench.py drive the library; every call goes through libtwofold_b200.so.
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import abi
+
+
+class Batch:
+    """One tf_world handle holding len(worlds) independent worlds on one CUDA device."""
+
+    def __init__(self, worlds, settings=None, device=0):
+        self.lib = abi.load()
+        self.settings = settings if settings is not None else abi.default_settings()
+        self.n = len(worlds)
+        h = C.c_void_p()
+        abi.check(self.lib.tf_world_create(C.byref(self.settings), self.n, device, C.byref(h)), self.lib)
+        self.h = h
+        self.body_counts = []
+        for wi, w in enumerate(worlds):
+            nb, ns = len(w.bodies), len(w.shapes)
+            world_of = np.full(nb, wi, np.int32)
+            abi.check(self.lib.tf_bodies_create(self.h, nb, world_of.ctypes.data,
+                                                w.bodies.ctypes.data_as(C.POINTER(abi.tf_body_desc)), None), self.lib)
+            world_of = np.full(ns, wi, np.int32)
+            abi.check(self.lib.tf_shapes_add(self.h, ns, world_of.ctypes.data, w.body_of.ctypes.data,
+                                             w.shapes.ctypes.data_as(C.POINTER(abi.tf_shape_desc)), None), self.lib)
+            self.body_counts.append(nb)
+        self.offsets = np.concatenate([[0], np.cumsum(self.body_counts)]).astype(np.int64)
+
+    @classmethod
+    def from_scene(cls, scene, device=0):
+        return cls(scene.worlds, scene.settings, device)
+
+    def close(self):
+        if self.h:
+            self.lib.tf_world_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def step(self, dt, n=1, graph=False):
+        fn = self.lib.tf_world_step_graph if graph else self.lib.tf_world_step
+        return fn(self.h, C.c_float(dt), n)
+
+    def step_checked(self, dt, n=1, graph=False):
+        abi.check(self.step(dt, n, graph), self.lib)
+
+    def states(self):
+        total = int(self.offsets[-1])
+        p = np.zeros((total, 3), np.float32)
+        q = np.zeros((total, 4), np.float32)
+        v = np.zeros((total, 3), np.float32)
+        w = np.zeros((total, 3), np.float32)
+        awake = np.zeros(total, np.int32)
+        abi.check(self.lib.tf_world_get_states(self.h, p.ctypes.data, q.ctypes.data, v.ctypes.data, w.ctypes.data,
+                                               awake.ctypes.data), self.lib)
+        return {"p": p, "q": q, "v": v, "w": w, "awake": awake}
+
+    def world_states(self, wi):
+        s = self.states()
+        a, b = self.offsets[wi], self.offsets[wi + 1]
+        return {k: v[a:b] for k, v in s.items()}
+
+    def candidates(self, wi=0):
+        n = C.c_int32(0)
+        abi.check(self.lib.tf_world_candidates(self.h, wi, None, 0, C.byref(n)), self.lib)
+        out = np.zeros(max(n.value, 1), np.uint64)
+        abi.check(self.lib.tf_world_candidates(self.h, wi, out.ctypes.data, n.value, C.byref(n)), self.lib)
+        return out[:n.value]
+
+    def contacts(self, wi=0, mode=1):
+        n = C.c_int32(0)
+        abi.check(self.lib.tf_world_contacts(self.h, wi, mode, None, 0, C.byref(n)), self.lib)
+        arr = (abi.tf_contact * max(n.value, 1))()
+        abi.check(self.lib.tf_world_contacts(self.h, wi, mode, arr, n.value, C.byref(n)), self.lib)
+        return list(arr)[:n.value]
+
+    def profile(self, wi=0):
+        p = abi.tf_profile()
+        abi.check(self.lib.tf_world_profile(self.h, wi, C.byref(p)), self.lib)
+        return p
+
+    def mass(self, wi, index, generation=0):
+        m = C.c_float(0)
+        c = np.zeros(3, np.float32)
+        i = np.zeros(9, np.float32)
+        abi.check(self.lib.tf_body_get_mass(self.h, wi, abi.tf_id(index, generation), C.byref(m), c.ctypes.data,
+                                            i.ctypes.data), self.lib)
+        return m.value, c, i.reshape(3, 3)
+
+    def awake_bodies(self):
+        n = C.c_int64(0)
+        abi.check(self.lib.tf_world_awake_bodies(self.h, C.byref(n)), self.lib)
+        return n.value
+
+    def launches(self):
+        n = C.c_int64(0)
+        abi.check(self.lib.tf_world_launch_count(self.h, C.byref(n)), self.lib)
+        return n.value
+
+    def device_flags(self):
+        f = C.c_uint32(0)
+        abi.check(self.lib.tf_world_device_status(self.h, C.byref(f)), self.lib)
+        return f.value
