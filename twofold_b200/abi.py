@@ -7,7 +7,8 @@ import ctypes as C
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libtwofold_b200.so")
+# TWOFOLD_B200_LIB selects another build of the same library (for instance the index-checking one).
+LIB_PATH = os.environ.get("TWOFOLD_B200_LIB") or os.path.join(HERE, "libtwofold_b200.so")
 
 TF_OK = 0
 TF_STATIC, TF_KINEMATIC, TF_DYNAMIC = 0, 1, 2

@@ -39,10 +39,12 @@ def stale():
     return any(os.path.getmtime(p) > t for p in SOURCES + HEADERS + [__file__])
 
 
-def build(force=False, verbose=False):
-    if not force and not stale():
+def build(force=False, verbose=False, out=None, defines=()):
+    """Builds the library; `defines` adds -D flags (TF_DEVICE_CHECKS builds the index-checking variant)."""
+    target = out or OUT
+    if not force and out is None and not stale():
         return OUT
-    cmd = [nvcc()] + NVCC_FLAGS + ["-shared", "-o", OUT] + SOURCES
+    cmd = [nvcc()] + NVCC_FLAGS + [f"-D{d}" for d in defines] + ["-shared", "-o", target] + SOURCES
     res = subprocess.run(cmd, capture_output=True, text=True)
     log = res.stdout + res.stderr
     with open(os.path.join(HERE, "build.log"), "w") as f:
@@ -52,9 +54,11 @@ def build(force=False, verbose=False):
         raise RuntimeError("nvcc failed building libtwofold_b200.so")
     if verbose:
         sys.stderr.write(log)
-    return OUT
+    return target
 
 
 if __name__ == "__main__":
-    build(force="--force" in sys.argv, verbose=True)
-    print(OUT)
+    if "--checked" in sys.argv:
+        print(build(force=True, out=sys.argv[sys.argv.index("--checked") + 1], defines=("TF_DEVICE_CHECKS",)))
+    else:
+        print(build(force="--force" in sys.argv, verbose=True))

@@ -11,6 +11,9 @@ struct Batch {
     const uint32_t* order;  // worlds, largest first; CTA k takes order[k], order[k + gridDim.x], ...
     const WorldInfo* info;
     WorldCounts* counts;
+    // Index (within the current launch sequence) of the first step that overflowed a list; later kernels
+    // of that step and every step after it do nothing, so the host can grow the lists and run it again.
+    uint32_t* abortStep;
 
     DBody* bodies;
     DShape* shapes;
@@ -48,7 +51,23 @@ struct Batch {
     uint64_t* mergeKeyB;
     uint32_t* mergePartB;
     uint32_t* mergeIdxB;
+
+    // Debug builds (TF_DEVICE_CHECKS) record the first failed index check here: code, world, value.
+    uint32_t* debug;
+    uint32_t nPolys;
+    uint32_t totalBodies;
 };
+
+#if defined(TF_DEVICE_CHECKS)
+// Records the first failure and evaluates to false so the caller skips the access.
+#define TF_OK_INDEX(B, cond, code, world, value)                                                     \
+    ((cond) ? true                                                                                  \
+            : (atomicCAS(&(B).debug[0], 0u, (uint32_t)(code)) == 0u                                 \
+                   ? ((B).debug[1] = (uint32_t)(world), (B).debug[2] = (uint32_t)(value), false)    \
+                   : false))
+#else
+#define TF_OK_INDEX(B, cond, code, world, value) true
+#endif
 
 constexpr uint8_t kFlagFast = 1, kFlagFastSolid = 2, kFlagActive = 4;
 

@@ -10,6 +10,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <string>
@@ -134,6 +135,15 @@ public:
     DevArray<uint8_t> dColor, dCflags;
     DevArray<uint64_t> dMergeKeyA, dMergeKeyB;
     DevArray<uint32_t> dMergePartA, dMergePartB, dMergeIdxA, dMergeIdxB;
+    DevArray<uint32_t> dAbort;
+    DevArray<uint32_t> dDebug;
+    size_t nPolys = 0;
+
+    // Shared-memory staging sizes for this layout, and per-world list capacities raised after an overflow.
+    uint32_t stageBodies = 1, stageContacts = 1;
+    size_t prepareSmem = 0, finishSmem = 0;
+    std::vector<uint32_t> minCandCap, minContactCap;
+    bool sortLimitHit = false;
 
     // Graph replay.
     cudaGraphExec_t graphExec = nullptr;
@@ -378,9 +388,18 @@ public:
         TF_CUDA(cudaMemcpy(bodies.data(), dBodies.ptr, totalBodies * sizeof(DBody), cudaMemcpyDeviceToHost));
         TF_CUDA(cudaMemcpy(shapes.data(), dShapes.ptr, totalShapes * sizeof(DShape), cudaMemcpyDeviceToHost));
         TF_CUDA(cudaMemcpy(counts.data(), dCounts.ptr, worlds.size() * sizeof(WorldCounts), cudaMemcpyDeviceToHost));
+        minCandCap.resize(worlds.size(), 0);
+        minContactCap.resize(worlds.size(), 0);
         for (size_t w = 0; w < worlds.size(); ++w) {
             HostWorld& W = worlds[w];
             const WorldInfo& wi = info[w];
+            if (counts[w].candNeeded > wi.candCap) {
+                minCandCap[w] = std::max(minCandCap[w], counts[w].candNeeded + counts[w].candNeeded / 4 + 64);
+            }
+            if (counts[w].contactNeeded > wi.contactCap) {
+                minContactCap[w] = std::max(minContactCap[w], counts[w].contactNeeded + counts[w].contactNeeded / 4 + 64);
+            }
+            if (counts[w].candNeeded > 8192u) { sortLimitHit = true; }
             for (size_t i = 0; i < W.bodies.size(); ++i) {
                 DBody d = bodies[wi.bodyFirst + i];
                 // Keep the host's own bookkeeping fields.
@@ -424,7 +443,9 @@ public:
         std::vector<DFace> faces;
         std::vector<float> offsets;
         std::vector<DEdge> edges;
-        uint32_t maxCap = 0;
+        uint32_t maxCap = 0, maxBodies = 0, maxContacts = 0;
+        minCandCap.resize(nw, 0);
+        minContactCap.resize(nw, 0);
         for (size_t w = 0; w < nw; ++w) {
             const HostWorld& W = worlds[w];
             WorldInfo& wi = info[w];
@@ -434,11 +455,13 @@ public:
             wi.shapeCount = (uint32_t)W.shapes.size();
             wi.planeFirst = (uint32_t)nplanes;
             wi.planeCount = (uint32_t)W.planes.size();
-            const uint32_t cap = (uint32_t)std::ceil(capFactor * (float)W.shapes.size()) + 64u;
+            const uint32_t cap = std::max((uint32_t)std::ceil(capFactor * (float)W.shapes.size()) + 64u, minCandCap[w]);
             wi.candFirst = (uint32_t)ncand;
             wi.candCap = cap;
             wi.contactFirst = (uint32_t)ncon;
-            wi.contactCap = std::max<uint32_t>(cap + 64u, (uint32_t)W.contacts.size() + 64u);
+            wi.contactCap = std::max({ cap + 64u, (uint32_t)W.contacts.size() + 64u, minContactCap[w] });
+            maxBodies = std::max(maxBodies, wi.bodyCount);
+            maxContacts = std::max(maxContacts, wi.contactCap);
             nb += wi.bodyCount;
             ns += wi.shapeCount;
             nplanes += wi.planeCount;
@@ -453,7 +476,9 @@ public:
         std::vector<DBody> bodies(nb);
         std::vector<DShape> shapes(ns);
         std::vector<uint32_t> shapeList(ns), planeList(std::max<size_t>(nplanes, 1));
-        std::vector<DContact> contacts(ncon);
+        // Contacts carried over from the device: packed, with one (slot, first, count) run per world.
+        std::vector<DContact> packed;
+        std::vector<size_t> runSlot, runFirst, runCount;
         std::vector<WorldCounts> counts(nw);
         for (size_t w = 0; w < nw; ++w) {
             HostWorld& W = worlds[w];
@@ -502,13 +527,18 @@ public:
                 shapes[wi.shapeFirst + i] = d;
             }
             for (size_t k = 0; k < W.planes.size(); ++k) { planeList[wi.planeFirst + k] = wi.shapeFirst + W.planes[k]; }
+            if (!W.contacts.empty()) {
+                runSlot.push_back(wi.contactFirst);
+                runFirst.push_back(packed.size());
+                runCount.push_back(std::min<size_t>(W.contacts.size(), wi.contactCap));
+            }
             for (size_t k = 0; k < W.contacts.size() && k < wi.contactCap; ++k) {
                 DContact c = W.contacts[k];
                 c.bodyA += wi.bodyFirst;
                 c.bodyB += wi.bodyFirst;
                 c.shapeA += wi.shapeFirst;
                 c.shapeB += wi.shapeFirst;
-                contacts[wi.contactFirst + k] = c;
+                packed.push_back(c);
             }
             counts[w] = WorldCounts{};
             counts[w].contactCount = (uint32_t)std::min<size_t>(W.contacts.size(), wi.contactCap);
@@ -520,6 +550,10 @@ public:
         sortCap = 1;
         while (sortCap < maxCap) { sortCap <<= 1; }
         sortCap = std::min<uint32_t>(sortCap, 8192u);
+        stageBodies = std::max<uint32_t>(1, std::min(kStageBodies, maxBodies));
+        stageContacts = std::max<uint32_t>(1, std::min(kStageContacts, maxContacts));
+        prepareSmem = ((size_t)stageBodies * 4 + (size_t)stageContacts * 9 + 15) / 16 * 16;
+        finishSmem = (size_t)stageBodies * 8 + (size_t)stageContacts * 8;
 
         int rc;
 #define TF_ALLOC(arr, count) \
@@ -564,6 +598,9 @@ public:
         TF_ALLOC(dMergePartB, ncon);
         TF_ALLOC(dMergeIdxA, ncon);
         TF_ALLOC(dMergeIdxB, ncon);
+        TF_ALLOC(dAbort, 1);
+        TF_ALLOC(dDebug, 4);
+        nPolys = polys.size();
 #undef TF_ALLOC
         auto up = [&](void* dst, const void* src, size_t bytes) -> int {
             if (bytes == 0) { return TF_OK; }
@@ -587,8 +624,13 @@ public:
         if ((rc = up(dFaces.ptr, faces.data(), faces.size() * sizeof(DFace))) != TF_OK) { return rc; }
         if ((rc = up(dOffsets.ptr, offsets.data(), offsets.size() * sizeof(float))) != TF_OK) { return rc; }
         if ((rc = up(dEdges.ptr, edges.data(), edges.size() * sizeof(DEdge))) != TF_OK) { return rc; }
-        if ((rc = up(dContacts[0].ptr, contacts.data(), ncon * sizeof(DContact))) != TF_OK) { return rc; }
+        for (size_t r = 0; r < runSlot.size(); ++r) {
+            if ((rc = up(dContacts[0].ptr + runSlot[r], packed.data() + runFirst[r], runCount[r] * sizeof(DContact))) != TF_OK) {
+                return rc;
+            }
+        }
         TF_CUDA(cudaMemset(dWakeMark.ptr, 0, nb));
+        TF_CUDA(cudaMemset(dDebug.ptr, 0, 4 * sizeof(uint32_t)));
         layoutDirty = false;
         bodiesDirty = false;
         onDevice = true;
@@ -652,6 +694,7 @@ public:
         Batch B{};
         B.nWorlds = (int)worlds.size();
         B.order = dOrder.ptr;
+        B.abortStep = dAbort.ptr;
         B.info = dInfo.ptr;
         B.counts = dCounts.ptr;
         B.bodies = dBodies.ptr;
@@ -685,12 +728,15 @@ public:
         B.mergeKeyB = dMergeKeyB.ptr;
         B.mergePartB = dMergePartB.ptr;
         B.mergeIdxB = dMergeIdxB.ptr;
+        B.debug = dDebug.ptr;
+        B.nPolys = (uint32_t)nPolys;
+        B.totalBodies = (uint32_t)totalBodies;
         return B;
     }
 
     // Issues one step on the stream: the new contact list goes into buffer `into`, the old one is read from
     // the other buffer.
-    int enqueueStep(float dt, int into, cudaEvent_t* marks) {
+    int enqueueStep(float dt, int into, int serial, cudaEvent_t* marks) {
         const StepParams P = params(dt);
         Batch B = batch(into);
         B.cx.tol = P.tol;
@@ -698,14 +744,14 @@ public:
         const int tb = blockSize;
         const size_t sortBytes = (size_t)sortCap * sizeof(uint64_t);
         if (marks) { cudaEventRecord(marks[0], stream); }
-        k_broadphase<<<grid, tb, sortBytes, stream>>>(B, P, sortCap);
+        k_broadphase<<<grid, tb, sortBytes, stream>>>(B, P, sortCap, serial);
         if (marks) { cudaEventRecord(marks[1], stream); }
-        k_narrowphase<<<grid, tb, 0, stream>>>(B, P);
-        k_wake<<<grid, 32, 0, stream>>>(B);
+        k_narrowphase<<<grid, tb, 0, stream>>>(B, P, serial);
+        k_wake<<<grid, 32, 0, stream>>>(B, serial);
         if (marks) { cudaEventRecord(marks[2], stream); }
-        k_prepare<<<grid, tb, 0, stream>>>(B, P);
-        for (int i = 0; i < P.substeps; ++i) { k_substep<<<grid, tb, 0, stream>>>(B, P, i); }
-        k_finish<<<grid, tb, 0, stream>>>(B, P);
+        k_prepare<<<grid, tb, prepareSmem, stream>>>(B, P, stageBodies, stageContacts, serial);
+        for (int i = 0; i < P.substeps; ++i) { k_substep<<<grid, tb, 0, stream>>>(B, P, i, serial); }
+        k_finish<<<grid, tb, finishSmem, stream>>>(B, P, stageBodies, stageContacts, serial);
         if (marks) { cudaEventRecord(marks[3], stream); }
         launches += 5 + P.substeps;
         cudaError_t e = cudaGetLastError();
@@ -717,42 +763,83 @@ public:
         static bool done = false;
         if (done) { return TF_OK; }
         TF_CUDA(cudaFuncSetAttribute(k_broadphase, cudaFuncAttributeMaxDynamicSharedMemorySize, 8192 * 8));
+        TF_CUDA(cudaFuncSetAttribute(k_prepare, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)(kStageBodies * 4 + kStageContacts * 9 + 16)));
+        TF_CUDA(cudaFuncSetAttribute(k_finish, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)(kStageBodies * 8 + kStageContacts * 8)));
         done = true;
         return TF_OK;
+    }
+
+    // Reads how many of the steps just issued completed: all of them, or those before the first one that
+    // overflowed a list (it and every later step did nothing).
+    int completedSteps(int issued, int* completed) {
+        uint32_t abort = 0;
+        TF_CUDA(cudaMemcpy(&abort, dAbort.ptr, sizeof(abort), cudaMemcpyDeviceToHost));
+        *completed = abort == 0xffffffffu ? issued : (int)abort;
+        return TF_OK;
+    }
+
+    // Grows the lists of the worlds that overflowed and lays the batch out again from the device state
+    // the completed steps left.
+    int growAfterAbort() {
+        if (std::getenv("TWOFOLD_B200_TRACE")) { std::fprintf(stderr, "twofold_b200: list overflow, growing and laying out again\n"); }
+        sortLimitHit = false;
+        hostFresh = false;
+        onDevice = true;
+        int rc = pull();
+        if (rc != TF_OK) { return rc; }
+        if (sortLimitHit) {
+            return fail(TF_E_UNSUPPORTED, "a world has more candidate pairs than one block sorts (8192)");
+        }
+        return layout();
     }
 
     int step(float dt, int nSteps) {
         if (!(dt > 0.0f) || !std::isfinite(dt) || nSteps <= 0) { return TF_OK; }
         TF_CUDA(cudaSetDevice(device));
-        int rc = configureKernels();
+        int rc = prepareDevice();
         if (rc != TF_OK) { return rc; }
-        rc = prepareDevice();
+        rc = configureKernels();
         if (rc != TF_OK) { return rc; }
         cudaEvent_t marks[4];
         for (cudaEvent_t& e : marks) { TF_CUDA(cudaEventCreate(&e)); }
-        for (int s = 0; s < nSteps; ++s) {
-            const int into = 1 - cur;
-            rc = enqueueStep(dt, into, s == nSteps - 1 ? marks : nullptr);
-            if (rc != TF_OK) { break; }
-            cur = into;
-        }
-        hostFresh = false;
-        cudaError_t e = cudaStreamSynchronize(stream);
-        if (e == cudaSuccess) {
-            float bp = 0, np = 0, sv = 0;
-            cudaEventElapsedTime(&bp, marks[0], marks[1]);
-            cudaEventElapsedTime(&np, marks[1], marks[2]);
-            cudaEventElapsedTime(&sv, marks[2], marks[3]);
-            for (tf_profile& p : profiles) {
-                p.broadphase = bp;
-                p.narrowphase = np;
-                p.solver = sv;
-                p.total = bp + np + sv;
+        int done = 0;
+        for (int attempt = 0; done < nSteps && attempt < 8; ++attempt) {
+            TF_CUDA(cudaMemsetAsync(dAbort.ptr, 0xff, sizeof(uint32_t), stream));
+            const int start = cur;
+            const int issue = nSteps - done;
+            int c = cur;
+            for (int s = 0; s < issue && rc == TF_OK; ++s) {
+                rc = enqueueStep(dt, 1 - c, s, s == issue - 1 ? marks : nullptr);
+                c = 1 - c;
             }
+            cudaError_t e = cudaStreamSynchronize(stream);
+            if (e != cudaSuccess) { rc = fail(TF_E_CUDA, std::string("step: ") + cudaGetErrorString(e)); }
+            if (rc != TF_OK) { break; }
+            int completed = 0;
+            if ((rc = completedSteps(issue, &completed)) != TF_OK) { break; }
+            cur = (completed % 2) ? 1 - start : start;
+            done += completed;
+            hostFresh = false;
+            if (completed == issue) {
+                float bp = 0, np = 0, sv = 0;
+                cudaEventElapsedTime(&bp, marks[0], marks[1]);
+                cudaEventElapsedTime(&np, marks[1], marks[2]);
+                cudaEventElapsedTime(&sv, marks[2], marks[3]);
+                for (tf_profile& p : profiles) {
+                    p.broadphase = bp;
+                    p.narrowphase = np;
+                    p.solver = sv;
+                    p.total = bp + np + sv;
+                }
+                break;
+            }
+            if ((rc = growAfterAbort()) != TF_OK) { break; }
         }
         for (cudaEvent_t& ev : marks) { cudaEventDestroy(ev); }
-        if (e != cudaSuccess) { return fail(TF_E_CUDA, std::string("step: ") + cudaGetErrorString(e)); }
         if (rc != TF_OK) { return rc; }
+        if (done < nSteps) { return fail(TF_E_CAPACITY, "device lists kept overflowing"); }
         return checkFlags();
     }
 
@@ -761,9 +848,9 @@ public:
     int stepGraph(float dt, int nSteps) {
         if (!(dt > 0.0f) || !std::isfinite(dt) || nSteps <= 0) { return TF_OK; }
         TF_CUDA(cudaSetDevice(device));
-        int rc = configureKernels();
+        int rc = prepareDevice();
         if (rc != TF_OK) { return rc; }
-        rc = prepareDevice();
+        rc = configureKernels();
         if (rc != TF_OK) { return rc; }
         if (graphExec && (graphSteps != nSteps || graphDt != dt)) {
             cudaGraphExecDestroy(graphExec);
@@ -775,7 +862,7 @@ public:
             int c = cur;
             for (int s = 0; s < nSteps; ++s) {
                 const int into = 1 - c;
-                rc = enqueueStep(dt, into, nullptr);
+                rc = enqueueStep(dt, into, s, nullptr);
                 if (rc != TF_OK) { break; }
                 c = into;
             }
@@ -795,16 +882,34 @@ public:
             graphExec = nullptr;
             return stepGraph(dt, nSteps);
         }
+        TF_CUDA(cudaMemsetAsync(dAbort.ptr, 0xff, sizeof(uint32_t), stream));
         TF_CUDA(cudaGraphLaunch(graphExec, stream));
         launches += (int64_t)nSteps * (5 + std::max(1, (int)settings.substeps));
-        if (nSteps % 2) { cur = 1 - cur; }
-        hostFresh = false;
         TF_CUDA(cudaStreamSynchronize(stream));
+        int completed = 0;
+        if ((rc = completedSteps(nSteps, &completed)) != TF_OK) { return rc; }
+        const int start = cur;
+        cur = (completed % 2) ? 1 - start : start;
+        hostFresh = false;
+        if (completed < nSteps) {
+            // A list overflowed: grow it and finish the remaining steps with direct launches.
+            if ((rc = growAfterAbort()) != TF_OK) { return rc; }
+            return step(dt, nSteps - completed);
+        }
         return checkFlags();
     }
     int graphStart = 0;
 
     int checkFlags() {
+#if defined(TF_DEVICE_CHECKS)
+        uint32_t dbg[4] = { 0, 0, 0, 0 };
+        TF_CUDA(cudaMemcpy(dbg, dDebug.ptr, sizeof(dbg), cudaMemcpyDeviceToHost));
+        if (dbg[0] != 0) {
+            char msg[160];
+            snprintf(msg, sizeof(msg), "device index check %u failed (world/base %u, value %u)", dbg[0], dbg[1], dbg[2]);
+            return fail(TF_E_INVALID, msg);
+        }
+#endif
         std::vector<WorldCounts> counts(worlds.size());
         TF_CUDA(cudaMemcpy(counts.data(), dCounts.ptr, worlds.size() * sizeof(WorldCounts), cudaMemcpyDeviceToHost));
         uint32_t flags = 0;
@@ -818,11 +923,6 @@ public:
         }
         lastCounts = counts;
         deviceFlags = flags;
-        if (flags & (kDevPairOverflow | kDevContactOverflow)) {
-            capFactor *= 2.0f;
-            layoutDirty = true;
-            return fail(TF_E_CAPACITY, "a device list overflowed; capacities grow for the next step");
-        }
         if (flags & kDevUnsupported) { return fail(TF_E_UNSUPPORTED, "the step met a pair this build cannot collide"); }
         if (flags & kDevNonFinite) { return fail(TF_E_NUMERIC, "a body state became non-finite"); }
         return TF_OK;

@@ -48,7 +48,8 @@ __device__ __forceinline__ uint32_t blockExclusiveScan(uint32_t v, uint32_t& tot
     return prefix;
 }
 
-// Calls emit(i, position) for every i < n where pred(i) holds, positions dense and in index order.
+// Calls emit(i, position) for every i < n where pred(i) holds, positions dense and in index order. Ends with
+// a block barrier, so everything emit wrote is visible to every thread on return.
 template <class Pred, class Emit>
 __device__ uint32_t blockCompact(uint32_t n, Pred pred, Emit emit) {
     uint32_t base = 0;
@@ -60,6 +61,7 @@ __device__ uint32_t blockCompact(uint32_t n, Pred pred, Emit emit) {
         if (f) { emit(i, base + pos); }
         base += tot;
     }
+    __syncthreads();
     return base;
 }
 
@@ -165,9 +167,21 @@ __device__ uint32_t sortUnique(uint64_t* s, uint32_t n, uint64_t* out) {
     return unique;
 }
 
-__global__ void __launch_bounds__(kMaxBlock) k_broadphase(Batch B, StepParams P, uint32_t sortCap) {
+// Reads the abort word once per CTA: true when an earlier step of this launch sequence overflowed a list,
+// or this step did in an earlier kernel.
+__device__ __forceinline__ bool stepAborted(const Batch& B, int serial) {
+    __shared__ int s_skip;
+    if (threadIdx.x == 0) { s_skip = *(volatile uint32_t*)B.abortStep <= (uint32_t)serial; }
+    __syncthreads();
+    const bool skip = s_skip != 0;
+    __syncthreads();
+    return skip;
+}
+
+__global__ void __launch_bounds__(kMaxBlock) k_broadphase(Batch B, StepParams P, uint32_t sortCap, int serial) {
     extern __shared__ uint64_t s_keys[];
     __shared__ uint32_t s_count;
+    if (stepAborted(B, serial)) { return; }
     for (int o = blockIdx.x; o < B.nWorlds; o += gridDim.x) {
         const uint32_t w = B.order[o];
         const WorldInfo wi = B.info[w];
@@ -194,18 +208,13 @@ __global__ void __launch_bounds__(kMaxBlock) k_broadphase(Batch B, StepParams P,
             for (uint32_t b = threadIdx.x; b < n; b += blockDim.x) { pairPlane(B, wi, gp, wi.bodyFirst + b, &s_count); }
         }
         __syncthreads();
-        uint32_t count = s_count;
-        if (count > wi.candCap) {
+        const uint32_t count = s_count;
+        if (count > wi.candCap || count > sortCap) {
+            // The list did not fit: this step stops here and the host grows the world's lists.
             if (threadIdx.x == 0) {
-                wc.flags |= kDevPairOverflow;
+                wc.flags |= count > wi.candCap ? kDevPairOverflow : kDevUnsupported;
                 wc.candNeeded = max(wc.candNeeded, count);
-            }
-            count = wi.candCap;
-        }
-        if (count > sortCap) {
-            if (threadIdx.x == 0) {
-                wc.flags |= kDevUnsupported;
-                wc.candCount = 0;
+                atomicMin(B.abortStep, (uint32_t)serial);
             }
             __syncthreads();
             continue;
@@ -298,6 +307,12 @@ __device__ __forceinline__ int nearestPoint(const DContact& old, const Vec3& loc
 // (src/world.cpp:505-533). Returns false for a pair this build cannot collide.
 __device__ bool collidePair(const Batch& B, const StepParams& P, const DShape& sa, const DShape& sb, float dt,
                             Manifold& m, int reuseKind, int reuseA, int reuseB) {
+    if (!TF_OK_INDEX(B, (sa.poly < 0 || (uint32_t)sa.poly < B.nPolys) && (sb.poly < 0 || (uint32_t)sb.poly < B.nPolys) &&
+                            sa.body < B.totalBodies && sb.body < B.totalBodies,
+                     30, sa.body, sb.body)) {
+        m.count = 0;
+        return true;
+    }
     const DBody& ba = B.bodies[sa.body];
     const DBody& bb = B.bodies[sb.body];
     const float travel = relativeTravel(ba, bb, dt);
@@ -328,9 +343,22 @@ __device__ void narrowOne(const Batch& B, const StepParams& P, const WorldInfo& 
                           const DContact* old, uint32_t oldCount) {
     const uint64_t key = B.cand[wi.candFirst + i];
     const uint32_t ia = (uint32_t)(key >> 32), ib = (uint32_t)(key & 0xffffffffu);
+    if (!TF_OK_INDEX(B, ia < wi.shapeCount && ib < wi.shapeCount, 1, wi.bodyFirst, ia)) {
+        B.stageUsed[wi.candFirst + i] = 0;
+        return;
+    }
     const uint32_t gsa = wi.shapeFirst + ia, gsb = wi.shapeFirst + ib;
     const DShape sa = B.shapes[gsa];
     const DShape sb = B.shapes[gsb];
+    if (!TF_OK_INDEX(B, sa.body - wi.bodyFirst < wi.bodyCount && sb.body - wi.bodyFirst < wi.bodyCount, 2,
+                     wi.bodyFirst, sa.body)) {
+        B.stageUsed[wi.candFirst + i] = 0;
+        return;
+    }
+    if (!TF_OK_INDEX(B, oldCount <= wi.contactCap, 3, wi.bodyFirst, oldCount)) {
+        B.stageUsed[wi.candFirst + i] = 0;
+        return;
+    }
     const DBody& ba = B.bodies[sa.body];
     const DBody& bb = B.bodies[sb.body];
     const uint32_t lo = lowerKey(old, oldCount, key);
@@ -417,7 +445,8 @@ __device__ __forceinline__ bool keyLess(uint64_t ka, uint32_t pa, uint64_t kb, u
     return ka != kb ? ka < kb : pa < pb;
 }
 
-__global__ void __launch_bounds__(kMaxBlock) k_narrowphase(Batch B, StepParams P) {
+__global__ void __launch_bounds__(kMaxBlock) k_narrowphase(Batch B, StepParams P, int serial) {
+    if (stepAborted(B, serial)) { return; }
     for (int o = blockIdx.x; o < B.nWorlds; o += gridDim.x) {
         const uint32_t w = B.order[o];
         const WorldInfo wi = B.info[w];
@@ -442,6 +471,10 @@ __global__ void __launch_bounds__(kMaxBlock) k_narrowphase(Batch B, StepParams P
             oldCount,
             [&](uint32_t j) {
                 const DContact& c = old[j];
+                if (!TF_OK_INDEX(B, c.bodyA - wi.bodyFirst < wi.bodyCount && c.bodyB - wi.bodyFirst < wi.bodyCount, 4,
+                                 wi.bodyFirst, j)) {
+                    return false;
+                }
                 const DBody& a = B.bodies[c.bodyA];
                 const DBody& b = B.bodies[c.bodyB];
                 if ((c.flags & kCRemoved) || movingAwake(a) || movingAwake(b)) { return false; }
@@ -454,9 +487,14 @@ __global__ void __launch_bounds__(kMaxBlock) k_narrowphase(Batch B, StepParams P
             });
         __syncthreads();
         const uint32_t total = nC + nK;
-        if (total > wi.contactCap && threadIdx.x == 0) {
-            wc.flags |= kDevContactOverflow;
-            wc.contactNeeded = max(wc.contactNeeded, total);
+        if (total > wi.contactCap) {
+            if (threadIdx.x == 0) {
+                wc.flags |= kDevContactOverflow;
+                wc.contactNeeded = max(wc.contactNeeded, total);
+                atomicMin(B.abortStep, (uint32_t)serial);
+            }
+            __syncthreads();
+            continue;
         }
         // Stable merge by (key, part): collided contacts first among equals, as std::inplace_merge keeps them.
         for (uint32_t x = threadIdx.x; x < nC; x += blockDim.x) {
@@ -471,8 +509,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_narrowphase(Batch B, StepParams P
                     h = mid;
                 }
             }
-            const uint32_t pos = x + l;
-            if (pos < wi.contactCap) { B.contacts[cf + pos] = B.stage[wi.candFirst + B.mergeIdxA[cf + x]]; }
+            B.contacts[cf + x + l] = B.stage[wi.candFirst + B.mergeIdxA[cf + x]];
         }
         for (uint32_t y = threadIdx.x; y < nK; y += blockDim.x) {
             const uint64_t k = B.mergeKeyB[cf + y];
@@ -486,12 +523,11 @@ __global__ void __launch_bounds__(kMaxBlock) k_narrowphase(Batch B, StepParams P
                     h = mid;
                 }
             }
-            const uint32_t pos = y + l;
-            if (pos < wi.contactCap) { B.contacts[cf + pos] = old[B.mergeIdxB[cf + y]]; }
+            B.contacts[cf + y + l] = old[B.mergeIdxB[cf + y]];
         }
         __syncthreads();
         if (threadIdx.x == 0) {
-            wc.contactCount = total < wi.contactCap ? total : wi.contactCap;
+            wc.nextContactCount = total;
             wc.contactNeeded = max(wc.contactNeeded, total);
         }
         __syncthreads();
@@ -500,9 +536,10 @@ __global__ void __launch_bounds__(kMaxBlock) k_narrowphase(Batch B, StepParams P
 
 // ---------------------------------------------------------------------------------------------------------
 // Waking (src/world.cpp:705-735): sleeping bodies a moving body reached wake, and so does everything linked
-// to them by a contact with points. Runs on the world's first thread.
+// to them by a contact with points. Runs on the world's first thread; it is rare.
 
-__global__ void k_wake(Batch B) {
+__global__ void k_wake(Batch B, int serial) {
+    if (stepAborted(B, serial)) { return; }
     if (threadIdx.x != 0) { return; }
     for (int o = blockIdx.x; o < B.nWorlds; o += gridDim.x) {
         const uint32_t w = B.order[o];
@@ -516,10 +553,14 @@ __global__ void k_wake(Batch B) {
             const uint32_t g = wi.bodyFirst + i;
             if (!B.wakeMark[g]) { continue; }
             const DBody& b = B.bodies[g];
-            if (b.alive && b.type == kDynamic && !b.awake && top < wi.bodyCount) { stack[top++] = g; } else { B.wakeMark[g] = 0; }
+            if (b.alive && b.type == kDynamic && !b.awake && top < wi.bodyCount) {
+                stack[top++] = g;
+            } else {
+                B.wakeMark[g] = 0;
+            }
         }
         const DContact* cs = B.contacts + wi.contactFirst;
-        const uint32_t nc = wc.contactCount;
+        const uint32_t nc = wc.nextContactCount;
         while (top > 0) {
             const uint32_t g = stack[--top];
             DBody& b = B.bodies[g];
@@ -549,15 +590,88 @@ __global__ void k_wake(Batch B) {
 // ---------------------------------------------------------------------------------------------------------
 // Step state, lists, preparation and coloring (src/world.cpp:1589-1657, src/lanes.cpp:356-407).
 
-__global__ void __launch_bounds__(kMaxBlock) k_prepare(Batch B, StepParams P) {
+// Shared-memory staging of a world's coloring and islands, sized per batch by the host (at most these).
+// Larger worlds run the same code on global scratch.
+constexpr uint32_t kStageBodies = 4096;
+constexpr uint32_t kStageContacts = 8192;
+constexpr uint32_t kNone = 0xffffffffu;
+
+// Greedy lowest free color of 32 over the moving bodies, in list order (src/lanes.cpp:356-374). endA/endB
+// hold each contact's moving bodies (kNone for one that does not move) or kNone in both with colorable 0.
+__device__ void colorSequential(uint32_t n, const uint32_t* endA, const uint32_t* endB, const uint8_t* colorable,
+                                uint32_t* masks, uint8_t* color) {
+    for (uint32_t x = 0; x < n; ++x) {
+        uint8_t k = kNoColor;
+        if (colorable[x]) {
+            const uint32_t a = endA[x], b = endB[x];
+            const uint32_t taken = (a != kNone ? masks[a] : 0u) | (b != kNone ? masks[b] : 0u);
+            if (taken != 0xffffffffu) {
+                const int f = __ffs(~taken) - 1;
+                if (a != kNone) { masks[a] |= 1u << f; }
+                if (b != kNone) { masks[b] |= 1u << f; }
+                k = (uint8_t)f;
+            }
+        }
+        color[x] = k;
+    }
+}
+
+// Groups a contact list by color: every color's contacts (any order within a color, which solves the same)
+// into colored, colors in ascending order, the uncolored ones into rest in list order.
+__device__ void bucketByColor(uint32_t n, const uint32_t* list, const uint8_t* colorOf, uint32_t* colored,
+                              uint32_t* rest, uint32_t* startOut, uint32_t& colorsUsed, uint32_t& restCount) {
+    __shared__ uint32_t s_size[kColors + 1];
+    __shared__ uint32_t s_fill[kColors + 1];
+    for (uint32_t k = threadIdx.x; k <= kColors; k += blockDim.x) { s_size[k] = 0; }
+    __syncthreads();
+    for (uint32_t x = threadIdx.x; x < n; x += blockDim.x) { atomicAdd(&s_size[colorOf[list[x]]], 1u); }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t sum = 0, used = 0;
+        for (int k = 0; k <= kColors; ++k) {
+            startOut[k] = sum;
+            s_fill[k] = sum;
+            sum += s_size[k];
+            if (k < kColors && s_size[k] > 0) { used = (uint32_t)k + 1; }
+        }
+        colorsUsed = used;
+    }
+    __syncthreads();
+    for (uint32_t x = threadIdx.x; x < n; x += blockDim.x) {
+        const uint8_t k = colorOf[list[x]];
+        if (k != kNoColor) {
+            const uint32_t at = atomicAdd(&s_fill[k], 1u);
+#if defined(TF_DEVICE_CHECKS)
+            if (at >= n) { continue; }
+#endif
+            colored[at] = list[x];
+        }
+    }
+    const uint32_t r = blockCompact(n, [&](uint32_t x) { return colorOf[list[x]] == kNoColor; },
+                                    [&](uint32_t x, uint32_t pos) { rest[pos] = list[x]; });
+    if (threadIdx.x == 0) { restCount = r; }
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(kMaxBlock) k_prepare(Batch B, StepParams P, uint32_t stageBodies,
+                                                       uint32_t stageContacts, int serial) {
+    extern __shared__ __align__(16) unsigned char s_raw[];
+    __shared__ uint32_t s_fast, s_fastSolid;
+    if (stepAborted(B, serial)) { return; }
     for (int o = blockIdx.x; o < B.nWorlds; o += gridDim.x) {
         const uint32_t w = B.order[o];
         const WorldInfo wi = B.info[w];
         WorldCounts& wc = B.counts[w];
+        uint32_t nc = wc.nextContactCount;
+        if (!TF_OK_INDEX(B, nc <= wi.contactCap, 6, w, nc)) { nc = 0; }
+        if (threadIdx.x == 0) {
+            wc.contactCount = nc;
+            s_fast = 0;
+            s_fastSolid = 0;
+        }
         for (uint32_t i = threadIdx.x; i < wi.bodyCount; i += blockDim.x) {
             const uint32_t g = wi.bodyFirst + i;
             DBody& b = B.bodies[g];
-            B.bodyColors[g] = 0;
             B.struck[g] = 0;
             if (!b.alive) { continue; }
             b.q0 = b.xf.q;
@@ -570,29 +684,63 @@ __global__ void __launch_bounds__(kMaxBlock) k_prepare(Batch B, StepParams P) {
         }
         __syncthreads();
         const uint32_t cf = wi.contactFirst;
-        const uint32_t nc = wc.contactCount;
         DContact* cs = B.contacts + cf;
         const uint32_t nActive = blockCompact(
             nc,
             [&](uint32_t i) {
+                if (!TF_OK_INDEX(B, cs[i].bodyA - wi.bodyFirst < wi.bodyCount && cs[i].bodyB - wi.bodyFirst < wi.bodyCount &&
+                                    cs[i].count >= 0 && cs[i].count <= 4, 5, wi.bodyFirst, i)) {
+                    B.cflags[cf + i] = 0;
+                    return false;
+                }
                 const DBody& a = B.bodies[cs[i].bodyA];
                 const DBody& b = B.bodies[cs[i].bodyB];
                 const bool on = (a.type == kDynamic && a.awake) || (b.type == kDynamic && b.awake);
                 uint8_t f = 0;
                 if (on && relativeTravel(a, b, P.dt) > P.tol.speculative) {
                     f |= kFlagFast;
-                    if (!isPlanar(a) && !isPlanar(b)) { f |= kFlagFastSolid; }
+                    atomicAdd(&s_fast, 1u);
+                    if (!isPlanar(a) && !isPlanar(b)) {
+                        f |= kFlagFastSolid;
+                        atomicAdd(&s_fastSolid, 1u);
+                    }
                 }
                 B.cflags[cf + i] = f | (on ? kFlagActive : 0);
                 return on;
             },
             [&](uint32_t i, uint32_t pos) { B.active[cf + pos] = i; });
         const uint32_t* act = B.active + cf;
+        // Staging for the coloring: shared memory when the world fits, else the world's global scratch.
+        const bool staged = wi.bodyCount <= stageBodies && nActive <= stageContacts;
+        uint32_t* masks = staged ? reinterpret_cast<uint32_t*>(s_raw) : B.bodyColors + wi.bodyFirst;
+        uint32_t* endA = staged ? masks + stageBodies : B.mergeIdxA + cf;
+        uint32_t* endB = staged ? endA + stageContacts : B.mergeIdxB + cf;
+        uint8_t* colorable = staged ? reinterpret_cast<uint8_t*>(endB + stageContacts) : B.cflags + cf;
+        // Colors by active position; moved to contact order below. The merge scratch is free by now.
+        uint8_t* colorTmp = reinterpret_cast<uint8_t*>(B.mergePartA + cf);
+        for (uint32_t i = threadIdx.x; i < wi.bodyCount; i += blockDim.x) { masks[i] = 0; }
         for (uint32_t x = threadIdx.x; x < nActive; x += blockDim.x) {
+            if (!TF_OK_INDEX(B, act[x] < nc, 7, w, x)) { continue; }
             DContact& c = cs[act[x]];
-            prepareContact(B.bodies[c.bodyA], B.bodies[c.bodyB], c);
+            const DBody& a = B.bodies[c.bodyA];
+            const DBody& b = B.bodies[c.bodyB];
+            prepareContact(a, b, c);
+            c.flags &= ~kCLaned;
+            const bool can = !(c.flags & kCPlanar) && !(c.rollingResistance > 0.0f);
+            endA[x] = movingBody(a) ? c.bodyA - wi.bodyFirst : kNone;
+            endB[x] = movingBody(b) ? c.bodyB - wi.bodyFirst : kNone;
+            if (staged) { colorable[x] = can ? 1 : 0; }
         }
         __syncthreads();
+        if (!staged) {
+            // The global form reuses cflags for colorable, so keep the fast flags in the upper bits.
+            for (uint32_t x = threadIdx.x; x < nActive; x += blockDim.x) {
+                const DContact& c = cs[act[x]];
+                const bool can = !(c.flags & kCPlanar) && !(c.rollingResistance > 0.0f);
+                B.cflags[cf + act[x]] = (B.cflags[cf + act[x]] & ~8) | (can ? 8 : 0);
+            }
+            __syncthreads();
+        }
         // Bodies of pairs closing faster than the restitution threshold are struck (src/world.cpp:1029-1049).
         for (uint32_t x = threadIdx.x; x < nActive; x += blockDim.x) {
             const DContact& c = cs[act[x]];
@@ -603,6 +751,33 @@ __global__ void __launch_bounds__(kMaxBlock) k_prepare(Batch B, StepParams P) {
                 break;
             }
         }
+        if (threadIdx.x == 0) {
+            if (staged) {
+                colorSequential(nActive, endA, endB, colorable, masks, colorTmp);
+            } else {
+                for (uint32_t x = 0; x < nActive; ++x) {
+                    uint8_t k = kNoColor;
+                    if (B.cflags[cf + act[x]] & 8) {
+                        const uint32_t a = endA[x], b = endB[x];
+                        const uint32_t taken = (a != kNone ? masks[a] : 0u) | (b != kNone ? masks[b] : 0u);
+                        if (taken != 0xffffffffu) {
+                            const int f = __ffs(~taken) - 1;
+                            if (a != kNone) { masks[a] |= 1u << f; }
+                            if (b != kNone) { masks[b] |= 1u << f; }
+                            k = (uint8_t)f;
+                        }
+                    }
+                    colorTmp[x] = k;
+                }
+            }
+        }
+        __syncthreads();
+        uint8_t* colorOf = B.color + cf;
+        for (uint32_t x = threadIdx.x; x < nActive; x += blockDim.x) {
+            const uint8_t k = colorTmp[x];
+            colorOf[act[x]] = k;
+            if (k != kNoColor) { cs[act[x]].flags |= kCLaned; }
+        }
         __syncthreads();
         const uint32_t nImpact = blockCompact(
             nActive,
@@ -611,85 +786,14 @@ __global__ void __launch_bounds__(kMaxBlock) k_prepare(Batch B, StepParams P) {
                 return B.struck[c.bodyA] || B.struck[c.bodyB];
             },
             [&](uint32_t x, uint32_t pos) { B.impact[cf + pos] = act[x]; });
-        // Greedy coloring in active order, lowest free of 32 colors over the moving bodies
-        // (src/lanes.cpp:356-374); then the bucket order the lane batches follow (src/lanes.cpp:376-407).
+        bucketByColor(nActive, act, colorOf, B.colored + cf, B.rest + cf, wc.colorStart, wc.colorCount, wc.restCount);
+        bucketByColor(nImpact, B.impact + cf, colorOf, B.impactColored + cf, B.impactRest + cf, wc.impactColorStart,
+                      wc.impactColorCount, wc.impactRestCount);
         if (threadIdx.x == 0) {
-            for (uint32_t x = 0; x < nActive; ++x) {
-                const uint32_t ci = act[x];
-                DContact& c = cs[ci];
-                uint8_t k = kNoColor;
-                c.flags &= ~kCLaned;
-                if (!(c.flags & kCPlanar) && !(c.rollingResistance > 0.0f)) {
-                    const DBody& a = B.bodies[c.bodyA];
-                    const DBody& b = B.bodies[c.bodyB];
-                    const bool ma = movingBody(a), mb = movingBody(b);
-                    const uint32_t taken = (ma ? B.bodyColors[c.bodyA] : 0u) | (mb ? B.bodyColors[c.bodyB] : 0u);
-                    if (taken != 0xffffffffu) {
-                        const int f = __ffs(~taken) - 1;
-                        if (ma) { B.bodyColors[c.bodyA] |= 1u << f; }
-                        if (mb) { B.bodyColors[c.bodyB] |= 1u << f; }
-                        k = (uint8_t)f;
-                        c.flags |= kCLaned;
-                    }
-                }
-                B.color[cf + ci] = k;
-            }
-            // Active list grouped by color, each color in active order; uncolored contacts form the rest.
-            uint32_t sizes[kColors + 1];
-            for (int k = 0; k <= kColors; ++k) { sizes[k] = 0; }
-            for (uint32_t x = 0; x < nActive; ++x) { ++sizes[B.color[cf + act[x]]]; }
-            uint32_t start[kColors + 1], sum = 0, used = 0;
-            for (int k = 0; k <= kColors; ++k) {
-                start[k] = sum;
-                wc.colorStart[k] = sum;
-                sum += sizes[k];
-                if (k < kColors && sizes[k] > 0) { used = (uint32_t)k + 1; }
-            }
-            wc.colorCount = used;
-            uint32_t restN = 0;
-            for (uint32_t x = 0; x < nActive; ++x) {
-                const uint32_t ci = act[x];
-                const uint8_t k = B.color[cf + ci];
-                if (k == kNoColor) {
-                    B.rest[cf + restN++] = ci;
-                } else {
-                    B.colored[cf + start[k]++] = ci;
-                }
-            }
-            wc.restCount = restN;
-            // The impact list takes the same colors.
-            for (int k = 0; k <= kColors; ++k) { sizes[k] = 0; }
-            for (uint32_t x = 0; x < nImpact; ++x) { ++sizes[B.color[cf + B.impact[cf + x]]]; }
-            sum = 0;
-            used = 0;
-            for (int k = 0; k <= kColors; ++k) {
-                start[k] = sum;
-                wc.impactColorStart[k] = sum;
-                sum += sizes[k];
-                if (k < kColors && sizes[k] > 0) { used = (uint32_t)k + 1; }
-            }
-            wc.impactColorCount = used;
-            restN = 0;
-            for (uint32_t x = 0; x < nImpact; ++x) {
-                const uint32_t ci = B.impact[cf + x];
-                const uint8_t k = B.color[cf + ci];
-                if (k == kNoColor) {
-                    B.impactRest[cf + restN++] = ci;
-                } else {
-                    B.impactColored[cf + start[k]++] = ci;
-                }
-            }
-            wc.impactRestCount = restN;
             wc.activeCount = nActive;
             wc.impactCount = nImpact;
-            uint32_t f = 0, fs = 0;
-            for (uint32_t x = 0; x < nActive; ++x) {
-                const uint8_t fl = B.cflags[cf + act[x]];
-                f += (fl & kFlagFast) ? 1 : 0;
-                fs += (fl & kFlagFastSolid) ? 1 : 0;
-            }
-            wc.fastCount = f;
-            wc.fastSolidCount = fs;
+            wc.fastCount = s_fast;
+            wc.fastSolidCount = s_fastSolid;
         }
         __syncthreads();
     }
@@ -706,6 +810,21 @@ __device__ void forEachColor(const uint32_t* list, const uint32_t* start, uint32
         for (uint32_t x = start[k] + threadIdx.x; x < end; x += blockDim.x) { f(list[x]); }
         __syncthreads();
     }
+}
+
+// In checked builds, whether contact ci of a world can be read: in the list, with bodies in the world.
+__device__ __forceinline__ bool contactOk(const Batch& B, const WorldInfo& wi, const WorldCounts& wc,
+                                          uint32_t ci, int code) {
+#if defined(TF_DEVICE_CHECKS)
+    if (!TF_OK_INDEX(B, ci < wc.contactCount, code, wi.bodyFirst, ci)) { return false; }
+    const DContact& c = B.contacts[wi.contactFirst + ci];
+    return TF_OK_INDEX(B, c.bodyA - wi.bodyFirst < wi.bodyCount && c.bodyB - wi.bodyFirst < wi.bodyCount &&
+                              c.shapeA - wi.shapeFirst < wi.shapeCount && c.shapeB - wi.shapeFirst < wi.shapeCount &&
+                              c.count >= 0 && c.count <= 4,
+                       code + 1, wi.bodyFirst, ci);
+#else
+    return true;
+#endif
 }
 
 // A fast pair collided again with the remaining time (src/world.cpp:1074-1138).
@@ -752,7 +871,8 @@ __device__ void refreshContact(const Batch& B, const StepParams& P, DContact& c,
     carryImpulses(old, c, P.tol.speculative * P.tol.speculative);
 }
 
-__global__ void __launch_bounds__(kMaxBlock) k_substep(Batch B, StepParams P, int sub) {
+__global__ void __launch_bounds__(kMaxBlock) k_substep(Batch B, StepParams P, int sub, int serial) {
+    if (stepAborted(B, serial)) { return; }
     for (int o = blockIdx.x; o < B.nWorlds; o += gridDim.x) {
         const uint32_t w = B.order[o];
         const WorldInfo wi = B.info[w];
@@ -773,6 +893,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_substep(Batch B, StepParams P, in
             for (uint32_t x = threadIdx.x; x < nActive; x += blockDim.x) {
                 const uint32_t ci = act[x];
                 if (B.cflags[cf + ci] & againFlag) { continue; }
+                if (!contactOk(B, wi, wc, ci, 16)) { continue; }
                 DContact& c = cs[ci];
                 rebaseContact(B.bodies[c.bodyA], B.bodies[c.bodyB], c);
             }
@@ -788,6 +909,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_substep(Batch B, StepParams P, in
             for (uint32_t x = threadIdx.x; x < nActive; x += blockDim.x) {
                 const uint32_t ci = act[x];
                 if (!(B.cflags[cf + ci] & againFlag)) { continue; }
+                if (!contactOk(B, wi, wc, ci, 14)) { continue; }
                 refreshContact(B, P, cs[ci], remaining);
             }
             __syncthreads();
@@ -797,10 +919,12 @@ __global__ void __launch_bounds__(kMaxBlock) k_substep(Batch B, StepParams P, in
         }
         __syncthreads();
         auto warm = [&](uint32_t ci, bool laned) {
+            if (!contactOk(B, wi, wc, ci, 10)) { return; }
             DContact& c = cs[ci];
             warmStartContact(B.bodies[c.bodyA], B.bodies[c.bodyB], c, laned);
         };
         auto solve = [&](uint32_t ci, bool bias) {
+            if (!contactOk(B, wi, wc, ci, 12)) { return; }
             DContact& c = cs[ci];
             solveContact(B.bodies[c.bodyA], B.bodies[c.bodyB], c, P, bias);
         };
@@ -848,29 +972,53 @@ __device__ __forceinline__ uint32_t findRoot(uint32_t* parent, uint32_t x) {
     return x;
 }
 
-__global__ void __launch_bounds__(kMaxBlock) k_finish(Batch B, StepParams P) {
+__device__ __forceinline__ uint32_t rootOf(const uint32_t* parent, uint32_t x) {
+    while (parent[x] != x) { x = parent[x]; }
+    return x;
+}
+
+__global__ void __launch_bounds__(kMaxBlock) k_finish(Batch B, StepParams P, uint32_t stageBodies,
+                                                      uint32_t stageContacts, int serial) {
+    extern __shared__ __align__(16) unsigned char s_raw[];
+    __shared__ uint32_t s_awake, s_islands, s_sweep;
+    if (stepAborted(B, serial)) { return; }
     for (int o = blockIdx.x; o < B.nWorlds; o += gridDim.x) {
         const uint32_t w = B.order[o];
         const WorldInfo wi = B.info[w];
         WorldCounts& wc = B.counts[w];
         const uint32_t cf = wi.contactFirst;
         DContact* cs = B.contacts + cf;
+        if (threadIdx.x == 0) {
+            s_awake = 0;
+            s_islands = 0;
+            s_sweep = 0;
+        }
         // Restitution: colored contacts by color, then the rest in active order.
         forEachColor(B.colored + cf, wc.colorStart, wc.colorCount, [&](uint32_t ci) {
+            if (!contactOk(B, wi, wc, ci, 18)) { return; }
             DContact& c = cs[ci];
             restituteContact(B.bodies[c.bodyA], B.bodies[c.bodyB], c, P, true);
         });
         if (threadIdx.x == 0) {
             for (uint32_t x = 0; x < wc.restCount; ++x) {
+                if (!contactOk(B, wi, wc, B.rest[cf + x], 20)) { continue; }
                 DContact& c = cs[B.rest[cf + x]];
                 restituteContact(B.bodies[c.bodyA], B.bodies[c.bodyB], c, P, false);
             }
         }
         __syncthreads();
-        uint32_t sweep = 0;
+        const uint32_t nc = wc.contactCount;
+        const bool staged = wi.bodyCount <= stageBodies && nc <= stageContacts;
+        uint32_t* parent = staged ? reinterpret_cast<uint32_t*>(s_raw) : B.unionParent + wi.bodyFirst;
+        uint32_t* islandTime = staged ? parent + stageBodies : reinterpret_cast<uint32_t*>(B.islandTime + wi.bodyFirst);
+        uint32_t* uA = staged ? islandTime + stageBodies : B.mergeIdxA + cf;
+        uint32_t* uB = staged ? uA + stageContacts : B.mergeIdxB + cf;
+        const float threshold = P.sleepThreshold;
         for (uint32_t i = threadIdx.x; i < wi.bodyCount; i += blockDim.x) {
             const uint32_t g = wi.bodyFirst + i;
             DBody& b = B.bodies[g];
+            parent[i] = i;
+            islandTime[i] = __float_as_uint(FLT_MAX);
             if (!b.alive) { continue; }
             limitSpeed(b, P.maxLinearSpeed, P.maxAngularSpeed);
             b.force = zero3();
@@ -880,49 +1028,41 @@ __global__ void __launch_bounds__(kMaxBlock) k_finish(Batch B, StepParams P) {
                 b.com = apply(b.xf, b.localCenter);
                 b.hasTarget = 0;
             }
-            if (!(b.type != kStatic && !(b.type == kDynamic && !b.awake))) { continue; }
-            // Leaf refit over the new pose (src/world.cpp:1713-1718): shape bounds and the body's union.
-            bool any = false;
-            for (uint32_t x = 0; x < b.shapeCount; ++x) {
-                DShape& s = B.shapes[B.shapeList[b.shapeFirst + x]];
-                Vec3 lo, hi;
-                shapeBounds(s, B.cx.pt, b.xf * s.local, lo, hi);
-                s.lo = lo;
-                s.hi = hi;
-                if (s.kind == kHalfSpace) { continue; }
-                b.lo = any ? minVec(b.lo, lo) : lo;
-                b.hi = any ? maxVec(b.hi, hi) : hi;
-                any = true;
-            }
-            // Shapes that moved well past what the speculative contacts covered would be swept against
-            // their surroundings (src/world.cpp:1260-1278). This build counts them; the sweep itself is not run.
-            if (P.continuous && b.type == kDynamic && b.awake) {
-                const float moved = length(b.com - b.com0);
-                Quat d = normalize(b.xf.q * conjugate(b.q0));
-                if (d.w < 0.0f) { d = -d; }
-                const float sine = length(qvec(d));
-                const float angle = sine > 1.0e-7f ? 2.0f * atan2f(sine, d.w) : 0.0f;
+            if (b.type != kStatic && !(b.type == kDynamic && !b.awake)) {
+                // Leaf refit over the new pose (src/world.cpp:1713-1718): shape bounds and the body's union.
+                bool any = false;
                 for (uint32_t x = 0; x < b.shapeCount; ++x) {
-                    const DShape& s = B.shapes[B.shapeList[b.shapeFirst + x]];
-                    if (s.kind == kMesh || s.sensor) { continue; }
-                    const float reach = length(s.local.p - b.localCenter) + s.extent;
-                    const float travel = moved + angle * reach;
-                    if (travel > b.expectedTravel && travel > b.expectedTravel + 0.5f * s.minExtent) { ++sweep; }
+                    DShape& s = B.shapes[B.shapeList[b.shapeFirst + x]];
+                    Vec3 lo, hi;
+                    shapeBounds(s, B.cx.pt, b.xf * s.local, lo, hi);
+                    s.lo = lo;
+                    s.hi = hi;
+                    if (s.kind == kHalfSpace) { continue; }
+                    b.lo = any ? minVec(b.lo, lo) : lo;
+                    b.hi = any ? maxVec(b.hi, hi) : hi;
+                    any = true;
+                }
+                // Shapes that moved well past what the speculative contacts covered would be swept against
+                // their surroundings (src/world.cpp:1260-1278). They are counted; the sweep is not run here.
+                if (P.continuous && b.type == kDynamic && b.awake) {
+                    const float moved = length(b.com - b.com0);
+                    Quat d = normalize(b.xf.q * conjugate(b.q0));
+                    if (d.w < 0.0f) { d = -d; }
+                    const float sine = length(qvec(d));
+                    const float angle = sine > 1.0e-7f ? 2.0f * atan2f(sine, d.w) : 0.0f;
+                    for (uint32_t x = 0; x < b.shapeCount; ++x) {
+                        const DShape& s = B.shapes[B.shapeList[b.shapeFirst + x]];
+                        if (s.kind == kMesh || s.sensor) { continue; }
+                        const float reach = length(s.local.p - b.localCenter) + s.extent;
+                        const float travel = moved + angle * reach;
+                        if (travel > b.expectedTravel && travel > b.expectedTravel + 0.5f * s.minExtent) {
+                            atomicAdd(&s_sweep, 1u);
+                        }
+                    }
                 }
             }
-        }
-        if (sweep > 0) {
-            atomicAdd(&wc.sweepShapes, sweep);
-            atomicOr(&wc.flags, kDevSweepSkipped);
-        }
-        // Sleep (src/world.cpp:1174-1247).
-        const float threshold = P.sleepThreshold;
-        for (uint32_t i = threadIdx.x; i < wi.bodyCount; i += blockDim.x) {
-            const uint32_t g = wi.bodyFirst + i;
-            DBody& b = B.bodies[g];
-            B.unionParent[g] = i;
-            B.islandTime[g] = FLT_MAX;
-            if (!b.alive || b.type != kDynamic || !b.awake) { continue; }
+            // Sleep timers (src/world.cpp:1176-1185).
+            if (b.type != kDynamic || !b.awake) { continue; }
             const float speed = maxf(length(b.v), length(b.w) * b.extent);
             if (!b.canSleep || speed > threshold) {
                 b.sleepTime = 0.0f;
@@ -935,47 +1075,65 @@ __global__ void __launch_bounds__(kMaxBlock) k_finish(Batch B, StepParams P) {
             }
         }
         __syncthreads();
-        if (threadIdx.x == 0) {
-            uint32_t* parent = B.unionParent + wi.bodyFirst;
-            float* islandTime = B.islandTime + wi.bodyFirst;
-            const uint32_t nc = wc.contactCount;
-            for (uint32_t ci = 0; ci < nc; ++ci) {
+        // Islands over contacts with points (src/world.cpp:1187-1233). The roots are each component's lowest
+        // body whatever order the unions run in, so only the unions themselves run on one thread.
+        const uint32_t nu = blockCompact(
+            nc,
+            [&](uint32_t ci) {
+                if (!contactOk(B, wi, wc, ci, 22)) { return false; }
                 const DContact& c = cs[ci];
-                if (c.count == 0) { continue; }
+                if (c.count == 0) { return false; }
                 DBody& a = B.bodies[c.bodyA];
                 DBody& b = B.bodies[c.bodyB];
                 const bool da = a.type == kDynamic && a.awake;
                 const bool db = b.type == kDynamic && b.awake;
-                if (da && db) {
-                    const uint32_t ra = findRoot(parent, c.bodyA - wi.bodyFirst), rb = findRoot(parent, c.bodyB - wi.bodyFirst);
-                    if (ra != rb) { parent[ra > rb ? ra : rb] = ra < rb ? ra : rb; }
-                } else if (da && b.type == kKinematic && movingAwake(b)) {
+                if (da && db) { return true; }
+                if (da && b.type == kKinematic && movingAwake(b)) {
                     a.sleepTime = 0.0f;
                 } else if (db && a.type == kKinematic && movingAwake(a)) {
                     b.sleepTime = 0.0f;
                 }
+                return false;
+            },
+            [&](uint32_t ci, uint32_t pos) {
+                uA[pos] = cs[ci].bodyA - wi.bodyFirst;
+                uB[pos] = cs[ci].bodyB - wi.bodyFirst;
+            });
+        if (threadIdx.x == 0) {
+            for (uint32_t x = 0; x < nu; ++x) {
+                if (!TF_OK_INDEX(B, uA[x] < wi.bodyCount && uB[x] < wi.bodyCount, 24, w, x)) { continue; }
+                const uint32_t ra = findRoot(parent, uA[x]), rb = findRoot(parent, uB[x]);
+                if (ra != rb) { parent[ra > rb ? ra : rb] = ra < rb ? ra : rb; }
             }
-            uint32_t awakeBodies = 0, islands = 0;
-            for (uint32_t i = 0; i < wi.bodyCount; ++i) {
-                DBody& b = B.bodies[wi.bodyFirst + i];
-                if (!b.alive || b.type != kDynamic || !b.awake) { continue; }
-                const uint32_t r = findRoot(parent, i);
-                b.island = r;
-                ++awakeBodies;
-                if (r == i) { ++islands; }
-                islandTime[r] = minf(islandTime[r], b.sleepTime);
+        }
+        __syncthreads();
+        for (uint32_t i = threadIdx.x; i < wi.bodyCount; i += blockDim.x) {
+            DBody& b = B.bodies[wi.bodyFirst + i];
+            if (!b.alive || b.type != kDynamic || !b.awake) { continue; }
+            const uint32_t r = rootOf(parent, i);
+            b.island = r;
+            atomicAdd(&s_awake, 1u);
+            if (r == i) { atomicAdd(&s_islands, 1u); }
+            atomicMin(&islandTime[r], __float_as_uint(b.sleepTime));
+        }
+        __syncthreads();
+        for (uint32_t i = threadIdx.x; i < wi.bodyCount; i += blockDim.x) {
+            DBody& b = B.bodies[wi.bodyFirst + i];
+            if (!b.alive || b.type != kDynamic || !b.awake) { continue; }
+            if (__uint_as_float(islandTime[rootOf(parent, i)]) < P.timeToSleep) { continue; }
+            b.awake = 0;
+            b.v = zero3();
+            b.w = zero3();
+            updateInverseMass(b);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            wc.awakeBodies = s_awake;
+            wc.awakeIslands = s_islands;
+            if (s_sweep > 0) {
+                wc.sweepShapes += s_sweep;
+                wc.flags |= kDevSweepSkipped;
             }
-            for (uint32_t i = 0; i < wi.bodyCount; ++i) {
-                DBody& b = B.bodies[wi.bodyFirst + i];
-                if (!b.alive || b.type != kDynamic || !b.awake) { continue; }
-                if (islandTime[findRoot(parent, i)] < P.timeToSleep) { continue; }
-                b.awake = 0;
-                b.v = zero3();
-                b.w = zero3();
-                updateInverseMass(b);
-            }
-            wc.awakeBodies = awakeBodies;
-            wc.awakeIslands = islands;
         }
         __syncthreads();
     }

@@ -174,7 +174,8 @@ struct WorldInfo {
 // Per-world results and lists of the current step.
 struct WorldCounts {
     uint32_t candCount;
-    uint32_t contactCount;  // in the current contact buffer
+    uint32_t contactCount;      // in the current contact buffer
+    uint32_t nextContactCount;  // in the buffer the narrowphase just filled
     uint32_t activeCount;
     uint32_t impactCount;
     uint32_t fastCount;
