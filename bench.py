@@ -1,0 +1,355 @@
+#!/usr/bin/env python
+"""Benchmark: body-steps per second of the batched uneven-worlds workload.
+
+Workload: 4096 independent worlds (per GPU) of 8-512 bodies each (log-uniform), 70% boxes and 30% spheres
+in a seeded stack or scatter above a half-space, dt 1/60, 4 substeps. Every step runs the whole contact
+pipeline of every world on the device (broadphase, narrowphase, coloring, the substepped soft solve,
+restitution, sleep) from one CUDA graph per step.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--worlds 4096] [--impl b200|reference]
+
+value: awake dynamic bodies summed over the K timed steps of all worlds on all GPUs, divided by the device
+time of those steps (CUDA events on the library's stream; max over ranks). Under torchrun every rank steps its
+own 4096 worlds (weak scaling, no collective in the step).
+
+e2e: the same metric through the public C ABI on a fresh batch stepped the same way, with each step's
+inputs (per-body forces, from pinned host memory) copied in and every body's pose copied out inside the
+timed region, timed by the host clock.
+
+--impl reference: the unmodified reference World::step (compiled from its own sources into
+oracle/_ref/libtwofold_ref.so) on a bounded sample of the same worlds, one world per thread from a pool of
+every host core.
+"""
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+METRIC = "body-steps/s"
+UNIT = "body-steps/s"
+SAMPLE_STRIDE = 4  # the CPU sample steps every 4th world
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=60)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--worlds", type=int, default=4096)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def config(args, n_gpus):
+    return {
+        "workload": "batched_uneven_worlds",
+        "worlds_per_gpu": args.worlds,
+        "bodies_per_world": "log-uniform 8-512, 70% boxes / 30% spheres, stack or scatter, half-space ground",
+        "dt": "1/60",
+        "substeps": 4,
+        "timed_steps": f"{args.warmup + 1}..{args.warmup + args.steps} of the 240-step run",
+        "parallelism": f"independent worlds, {n_gpus} GPU(s), no collective in the step",
+        "l2_flush": "not needed: the step's resident state (bodies, contacts, axes) is far larger than L2",
+    }
+
+
+# ------------------------------------------------------------------------------------------------------------
+# Distributed plumbing
+
+
+class Dist:
+    def __init__(self):
+        self.world_size = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+        if self.world_size > 1:
+            import datetime
+
+            import torch
+            import torch.distributed as dist
+
+            torch.cuda.set_device(self.local_rank)
+            os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                    device_id=torch.device("cuda", self.local_rank))
+            self.pg = dist
+
+    def barrier(self):
+        import torch
+
+        if torch.cuda.is_available():
+            torch.cuda.synchronize()
+        if self.pg:
+            self.pg.barrier()
+            torch.cuda.synchronize()
+
+    def reduce(self, value, op):
+        if not self.pg:
+            return value
+        import torch
+
+        t = torch.tensor([float(value)], dtype=torch.float64, device=f"cuda:{self.local_rank}")
+        self.pg.all_reduce(t, op=getattr(self.pg.ReduceOp, op))
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.pg.destroy_process_group()
+
+
+# ------------------------------------------------------------------------------------------------------------
+# Clocks during the timed region
+
+
+class ClockSampler:
+    FIELDS = ["clocks.sm", "clocks.max.sm", "clocks_event_reasons.active", "clocks_event_reasons.hw_slowdown",
+              "clocks_event_reasons.hw_thermal_slowdown", "clocks_event_reasons.sw_thermal_slowdown",
+              "clocks_event_reasons.sw_power_cap"]
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", "--query-gpu=" + ",".join(self.FIELDS), "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                smax.append(float(parts[1]))
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[3:7]):
+                if flag.lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ------------------------------------------------------------------------------------------------------------
+# The reference on the host cores
+
+
+def reference_rate(worlds, settings, dt, warmup, steps, threads):
+    """Reference World::step on `worlds`, one world per thread; body-steps/s over the last `steps` steps."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import reference as R
+
+    refs = [R.RefWorld(w, settings) for w in worlds]
+    if warmup:
+        R.step_parallel(refs, dt, warmup, threads)
+    t0 = time.perf_counter()
+    body_steps = R.step_parallel(refs, dt, steps, threads)
+    elapsed = time.perf_counter() - t0
+    return body_steps / elapsed, body_steps, elapsed
+
+
+def run_reference(args, dist):
+    if dist.rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import reference as R
+    from twofold_b200 import scenes
+
+    if not R.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libtwofold_ref.so was not built"}))
+        return
+    sc = scenes.config4(n_worlds=args.worlds)
+    sample = sc.worlds[::SAMPLE_STRIDE]
+    threads = R.hardware_threads()
+    rate, body_steps, elapsed = reference_rate(sample, sc.settings, sc.dt, args.warmup, args.steps, threads)
+    desc = (f"every {SAMPLE_STRIDE}th world ({len(sample)} of {args.worlds}), steps {args.warmup + 1}-"
+            f"{args.warmup + args.steps}, {body_steps} body-steps in {elapsed:.2f} s")
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": elapsed / args.steps * 1e3 * SAMPLE_STRIDE,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": config(args, args.gpus),
+        "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": "reference", "sample": desc},
+        "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+
+
+# ------------------------------------------------------------------------------------------------------------
+# The B200 library
+
+
+def substep_bytes(work):
+    """Algorithmic bytes of one k_substep launch: each awake body read and written once (160 B) and, in each
+    of its 3 passes (warm start, biased solve, relax), each active contact (64 B) and contact point (84 B)."""
+    return 160 * work["awake"] + 3 * (64 * work["active_contacts"] + 84 * work["active_points"])
+
+
+def load_traffic():
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            return json.load(f)
+    return {}
+
+
+def run_b200(args, dist):
+    from twofold_b200 import abi, scenes
+    from twofold_b200.world import Batch
+
+    abi.load()
+    n = dist.world_size
+    sc = scenes.config4(n_worlds=args.worlds, seed=dist.rank)
+    dt = sc.dt
+    batch = Batch.from_scene(sc, device=dist.local_rank)
+    for _ in range(args.warmup):
+        batch.step_checked(dt, 1, graph=True)
+    launches0 = batch.launches()
+    steps0 = batch.body_steps()
+    dist.barrier()
+    device_ms = 0.0
+    t0 = time.perf_counter()
+    with ClockSampler(dist.local_rank) as clocks:
+        for _ in range(args.steps):
+            batch.step_checked(dt, 1, graph=True)
+            device_ms += batch.elapsed_ms()
+    wall = time.perf_counter() - t0
+    dist.barrier()
+    body_steps = batch.body_steps() - steps0
+    launches = batch.launches() - launches0
+    max_ms = dist.reduce(device_ms, "MAX")
+    total_body_steps = dist.reduce(body_steps, "SUM")
+    value = total_body_steps / (max_ms / 1e3)
+
+    # Per-kernel times of the next 3 steps, each launch bracketed by CUDA events on the library's stream.
+    batch.set_profiling(True)
+    batch.step_checked(dt, 3)
+    kt = batch.kernel_times()
+    work = batch.work_counts()
+    batch.set_profiling(False)
+    top = max(kt, key=lambda k: kt[k][0])
+    peaks = {}
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(peaks_path):
+        with open(peaks_path) as f:
+            peaks = json.load(f)
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    sub_ms = kt["k_substep"][0] / max(kt["k_substep"][1], 1)
+    achieved = substep_bytes(work) / (sub_ms / 1e3) / 1e9
+    traffic = load_traffic().get("k_substep_bytes_per_launch")
+
+    # End to end: a fresh batch, the same warm-up, then per step: forces in, step, poses out.
+    del batch
+    e2e_batch = Batch.from_scene(sc, device=dist.local_rank)
+    total = int(e2e_batch.offsets[-1])
+    try:
+        import torch
+
+        forces = torch.zeros((total, 3), dtype=torch.float32).pin_memory().numpy()
+        poses = torch.zeros((total, 3), dtype=torch.float32).pin_memory().numpy()
+        rots = torch.zeros((total, 4), dtype=torch.float32).pin_memory().numpy()
+    except Exception:
+        forces = np.zeros((total, 3), np.float32)
+        poses = np.zeros((total, 3), np.float32)
+        rots = np.zeros((total, 4), np.float32)
+    for _ in range(args.warmup):
+        e2e_batch.step_checked(dt, 1, graph=True)
+    e_steps0 = e2e_batch.body_steps()
+    dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        e2e_batch.add_forces(forces)
+        e2e_batch.step_checked(dt, 1, graph=True)
+        e2e_batch.read_poses(poses, rots)
+    e_wall = time.perf_counter() - t0
+    dist.barrier()
+    e_body_steps = dist.reduce(e2e_batch.body_steps() - e_steps0, "SUM")
+    e_wall = dist.reduce(e_wall, "MAX")
+    del e2e_batch
+
+    cpu = None
+    if dist.rank == 0 and n == 1 and not args.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import reference as R
+
+        if R.available():
+            threads = R.hardware_threads()
+            sample = sc.worlds[::SAMPLE_STRIDE]
+            rate, bsteps, el = reference_rate(sample, sc.settings, dt, args.warmup, args.steps, threads)
+            cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": "reference",
+                   "sample": f"every {SAMPLE_STRIDE}th world ({len(sample)} of {args.worlds}), steps "
+                             f"{args.warmup + 1}-{args.warmup + args.steps}, {bsteps} body-steps in {el:.2f} s"}
+
+    if dist.rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": n, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": max_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic (seeded scenes, seed = rank)", "config": config(args, n),
+            "e2e": {"value": e_body_steps / e_wall, "unit": UNIT, "h2d_bytes_per_step": int(forces.nbytes),
+                    "d2h_bytes_per_step": int(poses.nbytes + rots.nbytes)},
+            "gpu_launches": int(launches),
+            "roofline": {"bound": "hbm", "kernel": "k_substep", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "peak_source": "measured hbm_gbs (MEASURED_PEAKS.json)" if "hbm_gbs" in peaks else "fallback",
+                         "algorithmic_bytes_per_launch": substep_bytes(work), "avg_launch_ms": sub_ms,
+                         "timed_on": "3 direct steps after the timed region, per-launch CUDA events",
+                         "top_kernel_by_time": top},
+            "kernel_ms_per_step": {k: v[0] / 3 for k, v in kt.items()},
+            "work_last_step": work,
+            "wall_s_timed_region": wall,
+            "clocks": clocks.summary(),
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line))
+
+
+def main():
+    args = parse()
+    dist = Dist()
+    try:
+        if args.impl == "reference":
+            run_reference(args, dist)
+        else:
+            run_b200(args, dist)
+    finally:
+        dist.close()
+
+
+if __name__ == "__main__":
+    main()

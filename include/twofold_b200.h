@@ -239,6 +239,34 @@ TF_API int tf_world_awake_bodies(void* world, int64_t* count);
 /* Number of kernel launches the library issued since creation (for launch accounting). */
 TF_API int tf_world_launch_count(void* world, int64_t* launches);
 
+/* Device time in milliseconds of the last tf_world_step / tf_world_step_graph call, measured with CUDA
+ * events on the library's stream around the step launches. */
+TF_API int tf_world_elapsed_ms(void* world, float* ms);
+
+/* Awake dynamic bodies summed over every step of every world since creation, as each step's
+ * StepProfile::awakeBodies counts them (src/world.cpp:1227-1235). */
+TF_API int tf_world_body_steps(void* world, int64_t* body_steps);
+
+/* Forces and torques (3 floats per body, all bodies of the batch in body order) added to every awake
+ * dynamic body for the next step only, as World::addForce / addTorque with wake = false
+ * (include/twofold/world.h:449-451). Either pointer may be null. */
+TF_API int tf_world_add_forces(void* world, const float* forces, const float* torques);
+
+/* Positions and rotations (x, y, z, w) of every body of the batch in body order, copied straight from the
+ * device without refreshing any other host state (World::transform, include/twofold/world.h:404). */
+TF_API int tf_world_read_poses(void* world, float* positions, float* rotations);
+
+/* Per-kernel device timing of direct (non-graph) steps. When on, every kernel launch is bracketed by CUDA
+ * events; tf_world_kernel_times returns, for each kernel in the order tf_kernel_name gives, the summed
+ * milliseconds and the launch count since profiling was turned on. */
+TF_API int tf_world_set_profiling(void* world, int32_t on);
+TF_API int tf_world_kernel_times(void* world, float* ms, int64_t* launches, int32_t capacity, int32_t* count);
+TF_API const char* tf_kernel_name(int32_t kernel);
+
+/* Work of the last step, summed over the batch: out[0] bodies, [1] awake dynamic bodies, [2] candidate
+ * pairs, [3] contacts, [4] active contacts, [5] active contact points. */
+TF_API int tf_world_work_counts(void* world, int64_t out[6]);
+
 #ifdef __cplusplus
 }
 #endif

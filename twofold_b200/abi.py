@@ -232,6 +232,14 @@ def _declare(lib):
         "tf_world_profile": ([P, C.c_int32, C.POINTER(tf_profile)], C.c_int),
         "tf_world_awake_bodies": ([P, C.POINTER(C.c_int64)], C.c_int),
         "tf_world_launch_count": ([P, C.POINTER(C.c_int64)], C.c_int),
+        "tf_world_elapsed_ms": ([P, C.POINTER(C.c_float)], C.c_int),
+        "tf_world_body_steps": ([P, C.POINTER(C.c_int64)], C.c_int),
+        "tf_world_add_forces": ([P, P, P], C.c_int),
+        "tf_world_read_poses": ([P, P, P], C.c_int),
+        "tf_world_set_profiling": ([P, C.c_int32], C.c_int),
+        "tf_world_kernel_times": ([P, P, P, C.c_int32, C.POINTER(C.c_int32)], C.c_int),
+        "tf_kernel_name": ([C.c_int32], C.c_char_p),
+        "tf_world_work_counts": ([P, P], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name)
@@ -247,7 +255,9 @@ EXPORTED = [
     "tf_shapes_add", "tf_world_step", "tf_world_step_graph", "tf_world_synchronize", "tf_world_device_status",
     "tf_body_get_state", "tf_body_set_velocity", "tf_body_get_mass", "tf_body_is_awake", "tf_world_body_count",
     "tf_world_get_states", "tf_world_contacts", "tf_world_candidates", "tf_world_profile", "tf_world_awake_bodies",
-    "tf_world_launch_count",
+    "tf_world_launch_count", "tf_world_elapsed_ms", "tf_world_body_steps", "tf_world_add_forces",
+    "tf_world_read_poses", "tf_world_set_profiling", "tf_world_kernel_times", "tf_kernel_name",
+    "tf_world_work_counts",
 ]
 
 

@@ -39,22 +39,36 @@ def stale():
     return any(os.path.getmtime(p) > t for p in SOURCES + HEADERS + [__file__])
 
 
-def build(force=False, verbose=False, out=None, defines=()):
-    """Builds the library; `defines` adds -D flags (TF_DEVICE_CHECKS builds the index-checking variant)."""
-    target = out or OUT
-    if not force and out is None and not stale():
-        return OUT
-    cmd = [nvcc()] + NVCC_FLAGS + [f"-D{d}" for d in defines] + ["-shared", "-o", target] + SOURCES
-    res = subprocess.run(cmd, capture_output=True, text=True)
-    log = res.stdout + res.stderr
-    with open(os.path.join(HERE, "build.log"), "w") as f:
-        f.write(" ".join(cmd) + "\n" + log)
-    if res.returncode != 0:
-        sys.stderr.write(log)
-        raise RuntimeError("nvcc failed building libtwofold_b200.so")
-    if verbose:
-        sys.stderr.write(log)
-    return target
+CHECKED_OUT = os.path.join(HERE, "libtwofold_b200_checked.so")
+
+
+def _command(target, defines):
+    return [nvcc()] + NVCC_FLAGS + [f"-D{d}" for d in defines] + ["-shared", "-o", target] + SOURCES
+
+
+def build(force=False, verbose=False, out=None, defines=(), checked=True):
+    """Builds libtwofold_b200.so and, alongside it, libtwofold_b200_checked.so: the same library with every
+    device index check on (TF_DEVICE_CHECKS), which records the first out-of-range index instead of using it.
+    `out`/`defines` build a single variant instead."""
+    if out is not None:
+        jobs = [(out, tuple(defines))]
+    else:
+        if not force and not stale() and (not checked or os.path.exists(CHECKED_OUT)):
+            return OUT
+        jobs = [(OUT, ())] + ([(CHECKED_OUT, ("TF_DEVICE_CHECKS",))] if checked else [])
+    procs = [(t, subprocess.Popen(_command(t, d), stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True))
+             for t, d in jobs]
+    for target, proc in procs:
+        log = proc.communicate()[0]
+        if target == OUT:
+            with open(os.path.join(HERE, "build.log"), "w") as f:
+                f.write(" ".join(_command(target, ())) + "\n" + log)
+        if proc.returncode != 0:
+            sys.stderr.write(log)
+            raise RuntimeError(f"nvcc failed building {os.path.basename(target)}")
+        if verbose:
+            sys.stderr.write(log)
+    return jobs[0][0]
 
 
 if __name__ == "__main__":

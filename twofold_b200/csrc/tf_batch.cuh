@@ -2,6 +2,7 @@
 #pragma once
 
 #include "tf_collide.cuh"
+#include "tf_solver.cuh"
 #include "tf_types.cuh"
 
 namespace tfb {
@@ -44,6 +45,7 @@ struct Batch {
     uint32_t* rest;           // active contacts solved one at a time, in active order
     uint32_t* impactRest;
     uint8_t* color;           // by contact
+    Axis* axes;               // by contact, kAxesPerContact each
     uint8_t* cflags;          // by contact: kFast, kFastSolid
     uint64_t* mergeKeyA;
     uint32_t* mergePartA;

@@ -83,7 +83,8 @@ TF_HD bool movingAwake(const DBody& b) {
 TF_HD bool movingBody(const DBody& b) { return b.type == kDynamic && b.awake; }
 
 // Scales down the velocities of an awake dynamic body past the speed limits (src/solver.cpp:30-41).
-TF_HD void limitSpeed(DBody& b, float maxSpeed, float maxSpin) {
+template <class BodyT>
+TF_HD void limitSpeed(BodyT& b, float maxSpeed, float maxSpin) {
     if (b.type != kDynamic || !b.awake) { return; }
     const float speed = length(b.v), spin = length(b.w);
     if (speed > maxSpeed) {

@@ -133,6 +133,7 @@ public:
     int cur = 0;
     DevArray<uint32_t> dActive, dImpact, dColored, dImpactColored, dRest, dImpactRest;
     DevArray<uint8_t> dColor, dCflags;
+    DevArray<Axis> dAxes;
     DevArray<uint64_t> dMergeKeyA, dMergeKeyB;
     DevArray<uint32_t> dMergePartA, dMergePartB, dMergeIdxA, dMergeIdxB;
     DevArray<uint32_t> dAbort;
@@ -140,18 +141,42 @@ public:
     size_t nPolys = 0;
 
     // Shared-memory staging sizes for this layout, and per-world list capacities raised after an overflow.
-    uint32_t stageBodies = 1, stageContacts = 1;
-    size_t prepareSmem = 0, finishSmem = 0;
+    uint32_t stageBodies = 1, stageContacts = 1, stageBroad = 1, stageSolve = 1;
+    size_t prepareSmem = 0, finishSmem = 0, broadSmem = 0, solveSmem = 0;
+    int solveBlock = 128;
     std::vector<uint32_t> minCandCap, minContactCap;
     bool sortLimitHit = false;
 
-    // Graph replay.
-    cudaGraphExec_t graphExec = nullptr;
+    // Host traffic staging and timing.
+    DevArray<float> dHostIn, dHostOut;
+    cudaEvent_t callStart = nullptr, callStop = nullptr;
+    float lastElapsedMs = 0.0f;
+    int64_t bodyStepsTotal = 0;
+    bool profiling = false;
+    static constexpr int kKernelKinds = 7;  // broadphase, narrowphase, wake, prepare, refresh, substep, finish
+    double kernelMs[kKernelKinds] = {};
+    int64_t kernelLaunches[kKernelKinds] = {};
+    std::vector<cudaEvent_t> eventPool;
+    std::vector<int> eventKind;
+    int eventsUsed = 0;
+
+    // Graph replay: one recorded graph per contact buffer a sequence starts from.
+    cudaGraphExec_t graphs[2] = { nullptr, nullptr };
     int graphSteps = 0;
     float graphDt = 0.0f;
 
+    void dropGraphs() {
+        for (cudaGraphExec_t& g : graphs) {
+            if (g) { cudaGraphExecDestroy(g); }
+            g = nullptr;
+        }
+    }
+
     ~Engine() {
-        if (graphExec) { cudaGraphExecDestroy(graphExec); }
+        for (cudaEvent_t e : eventPool) { cudaEventDestroy(e); }
+        if (callStart) { cudaEventDestroy(callStart); }
+        if (callStop) { cudaEventDestroy(callStop); }
+        dropGraphs();
         if (stream) { cudaStreamDestroy(stream); }
     }
 
@@ -191,7 +216,43 @@ public:
         TF_CUDA(cudaSetDevice(device));
         TF_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
         TF_CUDA(cudaDeviceGetAttribute(&smCount, cudaDevAttrMultiProcessorCount, device));
+        TF_CUDA(cudaEventCreate(&callStart));
+        TF_CUDA(cudaEventCreate(&callStop));
         return TF_OK;
+    }
+
+    // Brackets one kernel launch with events when per-kernel profiling is on (direct launches only).
+    template <class Launch>
+    void timed(int kind, bool record, Launch&& launch) {
+        if (!record) {
+            launch();
+            return;
+        }
+        if (eventsUsed + 2 > (int)eventPool.size()) {
+            for (int k = 0; k < 64; ++k) {
+                cudaEvent_t e;
+                cudaEventCreate(&e);
+                eventPool.push_back(e);
+                eventKind.push_back(0);
+            }
+        }
+        cudaEventRecord(eventPool[eventsUsed], stream);
+        launch();
+        cudaEventRecord(eventPool[eventsUsed + 1], stream);
+        eventKind[eventsUsed] = kind;
+        eventsUsed += 2;
+    }
+
+    // Adds the bracketed kernel times of the steps just synchronized to the per-kernel totals.
+    void collectKernelTimes() {
+        for (int k = 0; k + 1 < eventsUsed; k += 2) {
+            float ms = 0.0f;
+            if (cudaEventElapsedTime(&ms, eventPool[k], eventPool[k + 1]) == cudaSuccess) {
+                kernelMs[eventKind[k]] += ms;
+                kernelLaunches[eventKind[k]] += 1;
+            }
+        }
+        eventsUsed = 0;
     }
 
     // ---- host-side world building (src/world.cpp:1751-1857) ----
@@ -430,10 +491,8 @@ public:
     }
 
     int layout() {
-        if (graphExec) {
-            cudaGraphExecDestroy(graphExec);
-            graphExec = nullptr;
-        }
+        bodyStepsBase = bodyStepsTotal;
+        dropGraphs();
         const size_t nw = worlds.size();
         info.assign(nw, WorldInfo{});
         size_t nb = 0, ns = 0, ncand = 0, ncon = 0, nplanes = 0;
@@ -554,6 +613,10 @@ public:
         stageContacts = std::max<uint32_t>(1, std::min(kStageContacts, maxContacts));
         prepareSmem = ((size_t)stageBodies * 4 + (size_t)stageContacts * 9 + 15) / 16 * 16;
         finishSmem = (size_t)stageBodies * 8 + (size_t)stageContacts * 8;
+        stageBroad = std::max<uint32_t>(1, std::min(kBroadStage, maxBodies));
+        broadSmem = (size_t)sortCap * sizeof(uint64_t) + (size_t)stageBroad * sizeof(PairBody);
+        stageSolve = std::max<uint32_t>(1, std::min(kSolveStage, maxBodies));
+        solveSmem = (size_t)stageSolve * kSBodyWords * sizeof(float);
 
         int rc;
 #define TF_ALLOC(arr, count) \
@@ -592,6 +655,7 @@ public:
         TF_ALLOC(dImpactRest, ncon);
         TF_ALLOC(dColor, ncon);
         TF_ALLOC(dCflags, ncon);
+        TF_ALLOC(dAxes, ncon * kAxesPerContact);
         TF_ALLOC(dMergeKeyA, ncon);
         TF_ALLOC(dMergeKeyB, ncon);
         TF_ALLOC(dMergePartA, ncon);
@@ -722,6 +786,7 @@ public:
         B.impactRest = dImpactRest.ptr;
         B.color = dColor.ptr;
         B.cflags = dCflags.ptr;
+        B.axes = dAxes.ptr;
         B.mergeKeyA = dMergeKeyA.ptr;
         B.mergePartA = dMergePartA.ptr;
         B.mergeIdxA = dMergeIdxA.ptr;
@@ -736,24 +801,27 @@ public:
 
     // Issues one step on the stream: the new contact list goes into buffer `into`, the old one is read from
     // the other buffer.
-    int enqueueStep(float dt, int into, int serial, cudaEvent_t* marks) {
+    int enqueueStep(float dt, int into, int serial, cudaEvent_t* marks, bool capturing = false) {
         const StepParams P = params(dt);
         Batch B = batch(into);
         B.cx.tol = P.tol;
         const int grid = (int)std::min<size_t>(worlds.size(), (size_t)smCount * 8);
         const int tb = blockSize;
-        const size_t sortBytes = (size_t)sortCap * sizeof(uint64_t);
+        const bool rec = profiling && !capturing;
         if (marks) { cudaEventRecord(marks[0], stream); }
-        k_broadphase<<<grid, tb, sortBytes, stream>>>(B, P, sortCap, serial);
+        timed(0, rec, [&] { k_broadphase<<<grid, tb, broadSmem, stream>>>(B, P, sortCap, stageBroad, serial); });
         if (marks) { cudaEventRecord(marks[1], stream); }
-        k_narrowphase<<<grid, tb, 0, stream>>>(B, P, serial);
-        k_wake<<<grid, 32, 0, stream>>>(B, serial);
+        timed(1, rec, [&] { k_narrowphase<<<grid, tb, 0, stream>>>(B, P, serial); });
+        timed(2, rec, [&] { k_wake<<<grid, 32, 0, stream>>>(B, serial); });
         if (marks) { cudaEventRecord(marks[2], stream); }
-        k_prepare<<<grid, tb, prepareSmem, stream>>>(B, P, stageBodies, stageContacts, serial);
-        for (int i = 0; i < P.substeps; ++i) { k_substep<<<grid, tb, 0, stream>>>(B, P, i, serial); }
-        k_finish<<<grid, tb, finishSmem, stream>>>(B, P, stageBodies, stageContacts, serial);
+        timed(3, rec, [&] { k_prepare<<<grid, tb, prepareSmem, stream>>>(B, P, stageBodies, stageContacts, serial); });
+        for (int i = 0; i < P.substeps; ++i) {
+            if (i > 0) { timed(4, rec, [&] { k_refresh<<<grid, tb, 0, stream>>>(B, P, i, serial); }); }
+            timed(5, rec, [&] { k_substep<<<grid, solveBlock, solveSmem, stream>>>(B, P, stageSolve, serial); });
+        }
+        timed(6, rec, [&] { k_finish<<<grid, tb, finishSmem, stream>>>(B, P, stageBodies, stageContacts, serial); });
         if (marks) { cudaEventRecord(marks[3], stream); }
-        launches += 5 + P.substeps;
+        launches += 5 + 2 * P.substeps - 1;
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) { return fail(TF_E_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e)); }
         return TF_OK;
@@ -762,7 +830,10 @@ public:
     int configureKernels() {
         static bool done = false;
         if (done) { return TF_OK; }
-        TF_CUDA(cudaFuncSetAttribute(k_broadphase, cudaFuncAttributeMaxDynamicSharedMemorySize, 8192 * 8));
+        TF_CUDA(cudaFuncSetAttribute(k_broadphase, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)(8192 * sizeof(uint64_t) + kBroadStage * sizeof(PairBody))));
+        TF_CUDA(cudaFuncSetAttribute(k_substep, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)(kSolveStage * kSBodyWords * sizeof(float))));
         TF_CUDA(cudaFuncSetAttribute(k_prepare, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)(kStageBodies * 4 + kStageContacts * 9 + 16)));
         TF_CUDA(cudaFuncSetAttribute(k_finish, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -805,6 +876,7 @@ public:
         cudaEvent_t marks[4];
         for (cudaEvent_t& e : marks) { TF_CUDA(cudaEventCreate(&e)); }
         int done = 0;
+        TF_CUDA(cudaEventRecord(callStart, stream));
         for (int attempt = 0; done < nSteps && attempt < 8; ++attempt) {
             TF_CUDA(cudaMemsetAsync(dAbort.ptr, 0xff, sizeof(uint32_t), stream));
             const int start = cur;
@@ -814,9 +886,12 @@ public:
                 rc = enqueueStep(dt, 1 - c, s, s == issue - 1 ? marks : nullptr);
                 c = 1 - c;
             }
+            cudaEventRecord(callStop, stream);
             cudaError_t e = cudaStreamSynchronize(stream);
             if (e != cudaSuccess) { rc = fail(TF_E_CUDA, std::string("step: ") + cudaGetErrorString(e)); }
             if (rc != TF_OK) { break; }
+            cudaEventElapsedTime(&lastElapsedMs, callStart, callStop);
+            collectKernelTimes();
             int completed = 0;
             if ((rc = completedSteps(issue, &completed)) != TF_OK) { break; }
             cur = (completed % 2) ? 1 - start : start;
@@ -852,17 +927,15 @@ public:
         if (rc != TF_OK) { return rc; }
         rc = configureKernels();
         if (rc != TF_OK) { return rc; }
-        if (graphExec && (graphSteps != nSteps || graphDt != dt)) {
-            cudaGraphExecDestroy(graphExec);
-            graphExec = nullptr;
-        }
+        if (graphSteps != nSteps || graphDt != dt) { dropGraphs(); }
+        cudaGraphExec_t& graphExec = graphs[cur];
         if (!graphExec) {
             cudaGraph_t graph;
             TF_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
             int c = cur;
             for (int s = 0; s < nSteps; ++s) {
                 const int into = 1 - c;
-                rc = enqueueStep(dt, into, s, nullptr);
+                rc = enqueueStep(dt, into, s, nullptr, true);
                 if (rc != TF_OK) { break; }
                 c = into;
             }
@@ -874,18 +947,14 @@ public:
             if (e != cudaSuccess) { return fail(TF_E_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e)); }
             graphSteps = nSteps;
             graphDt = dt;
-            graphStart = cur;
-        }
-        if (cur != graphStart) {
-            // The recorded graph starts from the other buffer; record a fresh one.
-            cudaGraphExecDestroy(graphExec);
-            graphExec = nullptr;
-            return stepGraph(dt, nSteps);
         }
         TF_CUDA(cudaMemsetAsync(dAbort.ptr, 0xff, sizeof(uint32_t), stream));
+        TF_CUDA(cudaEventRecord(callStart, stream));
         TF_CUDA(cudaGraphLaunch(graphExec, stream));
-        launches += (int64_t)nSteps * (5 + std::max(1, (int)settings.substeps));
+        TF_CUDA(cudaEventRecord(callStop, stream));
+        launches += (int64_t)nSteps * (4 + 2 * std::max(1, (int)settings.substeps));
         TF_CUDA(cudaStreamSynchronize(stream));
+        TF_CUDA(cudaEventElapsedTime(&lastElapsedMs, callStart, callStop));
         int completed = 0;
         if ((rc = completedSteps(nSteps, &completed)) != TF_OK) { return rc; }
         const int start = cur;
@@ -898,7 +967,6 @@ public:
         }
         return checkFlags();
     }
-    int graphStart = 0;
 
     int checkFlags() {
 #if defined(TF_DEVICE_CHECKS)
@@ -913,8 +981,10 @@ public:
         std::vector<WorldCounts> counts(worlds.size());
         TF_CUDA(cudaMemcpy(counts.data(), dCounts.ptr, worlds.size() * sizeof(WorldCounts), cudaMemcpyDeviceToHost));
         uint32_t flags = 0;
+        int64_t bodySteps = 0;
         for (size_t w = 0; w < worlds.size(); ++w) {
             flags |= counts[w].flags;
+            bodySteps += (int64_t)counts[w].bodySteps;
             tf_profile& p = profiles[w];
             p.candidate_pairs = (int32_t)counts[w].candCount;
             p.manifolds = (int32_t)counts[w].contactCount;
@@ -923,12 +993,55 @@ public:
         }
         lastCounts = counts;
         deviceFlags = flags;
+        bodyStepsTotal = bodyStepsBase + bodySteps;
         if (flags & kDevUnsupported) { return fail(TF_E_UNSUPPORTED, "the step met a pair this build cannot collide"); }
         if (flags & kDevNonFinite) { return fail(TF_E_NUMERIC, "a body state became non-finite"); }
         return TF_OK;
     }
     std::vector<WorldCounts> lastCounts;
     uint32_t deviceFlags = 0;
+    int64_t bodyStepsBase = 0;  // body steps of layouts before the current one
+
+    int addForces(const float* f, const float* t) {
+        int rc = ensureDevice();
+        if (rc != TF_OK) { return rc; }
+        if ((rc = prepareDevice()) != TF_OK) { return rc; }
+        const size_t n = totalBodies;
+        if ((rc = dHostIn.alloc(6 * n)) != TF_OK) { return rc; }
+        if (f) { TF_CUDA(cudaMemcpyAsync(dHostIn.ptr, f, 3 * n * sizeof(float), cudaMemcpyHostToDevice, stream)); }
+        if (t) { TF_CUDA(cudaMemcpyAsync(dHostIn.ptr + 3 * n, t, 3 * n * sizeof(float), cudaMemcpyHostToDevice, stream)); }
+        k_add_forces<<<(unsigned)((n + 255) / 256), 256, 0, stream>>>(dBodies.ptr, (uint32_t)n, f ? dHostIn.ptr : nullptr,
+                                                                     t ? dHostIn.ptr + 3 * n : nullptr);
+        ++launches;
+        TF_CUDA(cudaGetLastError());
+        hostFresh = false;
+        return TF_OK;
+    }
+
+    int readPoses(float* p, float* q) {
+        if (!onDevice || layoutDirty) {
+            // Nothing stepped yet: the host mirrors are current.
+            size_t k = 0;
+            for (const auto& W : worlds) {
+                for (const auto& hb : W.bodies) {
+                    if (p) { p[3 * k] = hb.d.xf.p.x, p[3 * k + 1] = hb.d.xf.p.y, p[3 * k + 2] = hb.d.xf.p.z; }
+                    if (q) { q[4 * k] = hb.d.xf.q.x, q[4 * k + 1] = hb.d.xf.q.y, q[4 * k + 2] = hb.d.xf.q.z, q[4 * k + 3] = hb.d.xf.q.w; }
+                    ++k;
+                }
+            }
+            return TF_OK;
+        }
+        const size_t n = totalBodies;
+        int rc = dHostOut.alloc(7 * n);
+        if (rc != TF_OK) { return rc; }
+        k_pack_poses<<<(unsigned)((n + 255) / 256), 256, 0, stream>>>(dBodies.ptr, (uint32_t)n, dHostOut.ptr, dHostOut.ptr + 3 * n);
+        ++launches;
+        TF_CUDA(cudaGetLastError());
+        if (p) { TF_CUDA(cudaMemcpyAsync(p, dHostOut.ptr, 3 * n * sizeof(float), cudaMemcpyDeviceToHost, stream)); }
+        if (q) { TF_CUDA(cudaMemcpyAsync(q, dHostOut.ptr + 3 * n, 4 * n * sizeof(float), cudaMemcpyDeviceToHost, stream)); }
+        TF_CUDA(cudaStreamSynchronize(stream));
+        return TF_OK;
+    }
 };
 
 }  // namespace tfb
@@ -1227,6 +1340,70 @@ TF_API int tf_world_awake_bodies(void* h, int64_t* count) {
     int64_t n = 0;
     for (const auto& c : E(h)->lastCounts) { n += c.awakeBodies; }
     *count = n;
+    return TF_OK;
+}
+
+TF_API int tf_world_elapsed_ms(void* h, float* ms) {
+    if (!h || !ms) { return tfb::fail(TF_E_INVALID, "tf_world_elapsed_ms: null"); }
+    *ms = E(h)->lastElapsedMs;
+    return TF_OK;
+}
+
+TF_API int tf_world_body_steps(void* h, int64_t* n) {
+    if (!h || !n) { return tfb::fail(TF_E_INVALID, "tf_world_body_steps: null"); }
+    *n = E(h)->bodyStepsTotal;
+    return TF_OK;
+}
+
+TF_API int tf_world_add_forces(void* h, const float* forces, const float* torques) {
+    if (!h) { return tfb::fail(TF_E_INVALID, "tf_world_add_forces: null world"); }
+    return E(h)->addForces(forces, torques);
+}
+
+TF_API int tf_world_read_poses(void* h, float* positions, float* rotations) {
+    if (!h) { return tfb::fail(TF_E_INVALID, "tf_world_read_poses: null world"); }
+    return E(h)->readPoses(positions, rotations);
+}
+
+TF_API int tf_world_set_profiling(void* h, int32_t on) {
+    if (!h) { return tfb::fail(TF_E_INVALID, "tf_world_set_profiling: null world"); }
+    Engine* e = E(h);
+    e->profiling = on != 0;
+    for (int k = 0; k < Engine::kKernelKinds; ++k) {
+        e->kernelMs[k] = 0.0;
+        e->kernelLaunches[k] = 0;
+    }
+    return TF_OK;
+}
+
+TF_API int tf_world_kernel_times(void* h, float* ms, int64_t* launches, int32_t capacity, int32_t* count) {
+    if (!h || !count) { return tfb::fail(TF_E_INVALID, "tf_world_kernel_times: null"); }
+    Engine* e = E(h);
+    *count = Engine::kKernelKinds;
+    for (int k = 0; k < Engine::kKernelKinds && k < capacity; ++k) {
+        if (ms) { ms[k] = (float)e->kernelMs[k]; }
+        if (launches) { launches[k] = e->kernelLaunches[k]; }
+    }
+    return TF_OK;
+}
+
+TF_API const char* tf_kernel_name(int32_t k) {
+    static const char* names[] = { "k_broadphase", "k_narrowphase", "k_wake", "k_prepare", "k_refresh", "k_substep", "k_finish" };
+    return (k >= 0 && k < 7) ? names[k] : "";
+}
+
+TF_API int tf_world_work_counts(void* h, int64_t out[6]) {
+    if (!h || !out) { return tfb::fail(TF_E_INVALID, "tf_world_work_counts: null"); }
+    Engine* e = E(h);
+    for (int k = 0; k < 6; ++k) { out[k] = 0; }
+    out[0] = (int64_t)e->totalBodies;
+    for (const auto& c : e->lastCounts) {
+        out[1] += c.awakeBodies;
+        out[2] += c.candCount;
+        out[3] += c.contactCount;
+        out[4] += c.activeCount;
+        out[5] += c.activePoints;
+    }
     return TF_OK;
 }
 

@@ -77,34 +77,6 @@ __device__ __forceinline__ void emitCandidate(const Batch& B, const WorldInfo& w
 // ---------------------------------------------------------------------------------------------------------
 // Broadphase (src/world.cpp:752-870).
 
-// The shapes of two overlapping bodies, paired by their grown bounds (src/world.cpp:788-842).
-__device__ void pairBodies(const Batch& B, const WorldInfo& wi, uint32_t ga, uint32_t gb, uint32_t* count) {
-    const DBody& ba = B.bodies[ga];
-    const DBody& bb = B.bodies[gb];
-    if (!ba.alive || !bb.alive || !ba.hasBounds || !bb.hasBounds) { return; }
-    if (ba.type != kDynamic && bb.type != kDynamic) { return; }
-    if (!movingAwake(ba) && !movingAwake(bb)) { return; }
-    const float gA = B.grow[ga], gB = B.grow[gb];
-    const float g = gA + gB;
-    const Vec3 reach{ g, g, g };
-    if (!boxesOverlap(ba.lo - reach, ba.hi + reach, bb.lo, bb.hi)) { return; }
-    const Vec3 nearLoA = bb.lo - reach, nearHiA = bb.hi + reach;
-    const Vec3 nearLoB = ba.lo - reach, nearHiB = ba.hi + reach;
-    const Vec3 grownA{ gA, gA, gA }, grownB{ gB, gB, gB };
-    for (uint32_t x = 0; x < ba.shapeCount; ++x) {
-        const DShape& s = B.shapes[B.shapeList[ba.shapeFirst + x]];
-        if (s.kind == kHalfSpace || s.sensor || !boxesOverlap(s.lo, s.hi, nearLoA, nearHiA)) { continue; }
-        const Vec3 xlo = s.lo - grownA, xhi = s.hi + grownA;
-        for (uint32_t y = 0; y < bb.shapeCount; ++y) {
-            const DShape& t = B.shapes[B.shapeList[bb.shapeFirst + y]];
-            if (t.kind == kHalfSpace || t.sensor || !boxesOverlap(t.lo, t.hi, nearLoB, nearHiB)) { continue; }
-            if (!boxesOverlap(xlo, xhi, t.lo - grownB, t.hi + grownB)) { continue; }
-            if (!(s.category & t.mask) || !(t.category & s.mask)) { continue; }
-            emitCandidate(B, wi, count, pairKey(s.index, t.index));
-        }
-    }
-}
-
 // A half-space against one body's shapes (src/world.cpp:844-867).
 __device__ void pairPlane(const Batch& B, const WorldInfo& wi, uint32_t gp, uint32_t gb, uint32_t* count) {
     const DShape& sp = B.shapes[gp];
@@ -178,29 +150,100 @@ __device__ __forceinline__ bool stepAborted(const Batch& B, int serial) {
     return skip;
 }
 
-__global__ void __launch_bounds__(kMaxBlock) k_broadphase(Batch B, StepParams P, uint32_t sortCap, int serial) {
-    extern __shared__ uint64_t s_keys[];
+// The shapes of two bodies whose grown bounds overlap, paired by their own grown bounds
+// (src/world.cpp:819-842).
+__device__ void pairShapes(const Batch& B, const WorldInfo& wi, const DBody& ba, const DBody& bb, float gA, float gB,
+                           const Vec3& loA, const Vec3& hiA, const Vec3& loB, const Vec3& hiB, const Vec3& reach,
+                           uint32_t* count) {
+    const Vec3 nearLoA = loB - reach, nearHiA = hiB + reach;
+    const Vec3 nearLoB = loA - reach, nearHiB = hiA + reach;
+    const Vec3 grownA{ gA, gA, gA }, grownB{ gB, gB, gB };
+    for (uint32_t x = 0; x < ba.shapeCount; ++x) {
+        const DShape& s = B.shapes[B.shapeList[ba.shapeFirst + x]];
+        if (s.kind == kHalfSpace || s.sensor || !boxesOverlap(s.lo, s.hi, nearLoA, nearHiA)) { continue; }
+        const Vec3 xlo = s.lo - grownA, xhi = s.hi + grownA;
+        for (uint32_t y = 0; y < bb.shapeCount; ++y) {
+            const DShape& t = B.shapes[B.shapeList[bb.shapeFirst + y]];
+            if (t.kind == kHalfSpace || t.sensor || !boxesOverlap(t.lo, t.hi, nearLoB, nearHiB)) { continue; }
+            if (!boxesOverlap(xlo, xhi, t.lo - grownB, t.hi + grownB)) { continue; }
+            if (!(s.category & t.mask) || !(t.category & s.mask)) { continue; }
+            emitCandidate(B, wi, count, pairKey(s.index, t.index));
+        }
+    }
+}
+
+constexpr uint32_t kBodyLive = 1u, kBodyDynamic = 2u, kBodyMoving = 4u;
+// Largest worlds whose bodies the broadphase and the substep stage in shared memory.
+constexpr uint32_t kBroadStage = 2048;
+constexpr uint32_t kSolveStage = 1400;
+
+// A body as the pair test sees it: bounds, growth and the three flags above.
+struct PairBody {
+    Vec3 lo, hi;
+    float grow;
+    uint32_t flags;
+};
+
+__device__ __forceinline__ PairBody pairBodyOf(const Batch& B, uint32_t g) {
+    const DBody& b = B.bodies[g];
+    PairBody p;
+    p.lo = b.lo;
+    p.hi = b.hi;
+    p.grow = B.grow[g];
+    p.flags = ((b.alive && b.hasBounds) ? kBodyLive : 0u) | (b.type == kDynamic ? kBodyDynamic : 0u) |
+              (movingAwake(b) ? kBodyMoving : 0u);
+    return p;
+}
+
+// Body pairs whose grown bounds overlap, then their shapes (src/world.cpp:788-842), and half-space pairs
+// (:844-867); the keys are sorted and made unique (:868-869). Bodies and growths are staged in shared
+// memory for worlds of up to stageN bodies; a warp takes one body and its lanes the bodies after it.
+__global__ void __launch_bounds__(kMaxBlock) k_broadphase(Batch B, StepParams P, uint32_t sortCap, uint32_t stageN,
+                                                          int serial) {
+    extern __shared__ __align__(16) uint64_t s_keys[];
     __shared__ uint32_t s_count;
+    PairBody* staged = reinterpret_cast<PairBody*>(s_keys + sortCap);
     if (stepAborted(B, serial)) { return; }
     for (int o = blockIdx.x; o < B.nWorlds; o += gridDim.x) {
         const uint32_t w = B.order[o];
         const WorldInfo wi = B.info[w];
         WorldCounts& wc = B.counts[w];
+        const uint32_t n = wi.bodyCount;
+        const bool useStage = n <= stageN;
         if (threadIdx.x == 0) { s_count = 0; }
         // Growth by the speculative distance and the travel over the step (src/world.cpp:754-765).
-        for (uint32_t i = threadIdx.x; i < wi.bodyCount; i += blockDim.x) {
+        for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
             const DBody& b = B.bodies[wi.bodyFirst + i];
             float g = P.tol.speculative;
             if (b.alive && b.type != kStatic && !(lengthSquared(b.v) == 0.0f && lengthSquared(b.w) == 0.0f)) {
                 g += (length(b.v) + length(b.w) * b.extent) * P.dt;
             }
             B.grow[wi.bodyFirst + i] = g;
+            if (useStage) {
+                PairBody p;
+                p.lo = b.lo;
+                p.hi = b.hi;
+                p.grow = g;
+                p.flags = ((b.alive && b.hasBounds) ? kBodyLive : 0u) | (b.type == kDynamic ? kBodyDynamic : 0u) |
+                          (movingAwake(b) ? kBodyMoving : 0u);
+                staged[i] = p;
+            }
         }
         __syncthreads();
-        const uint32_t n = wi.bodyCount;
-        for (uint32_t a = 0; a + 1 < n; ++a) {
-            for (uint32_t b = a + 1 + threadIdx.x; b < n; b += blockDim.x) {
-                pairBodies(B, wi, wi.bodyFirst + a, wi.bodyFirst + b, &s_count);
+        const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
+        for (uint32_t a = warp; a + 1 < n; a += warps) {
+            const PairBody A = useStage ? staged[a] : pairBodyOf(B, wi.bodyFirst + a);
+            if (!(A.flags & kBodyLive)) { continue; }
+            for (uint32_t b = a + 1 + lane; b < n; b += 32) {
+                const PairBody Bb = useStage ? staged[b] : pairBodyOf(B, wi.bodyFirst + b);
+                if (!(Bb.flags & kBodyLive)) { continue; }
+                if (!((A.flags | Bb.flags) & kBodyDynamic)) { continue; }
+                if (!((A.flags | Bb.flags) & kBodyMoving)) { continue; }
+                const float g = A.grow + Bb.grow;
+                const Vec3 reach{ g, g, g };
+                if (!boxesOverlap(A.lo - reach, A.hi + reach, Bb.lo, Bb.hi)) { continue; }
+                pairShapes(B, wi, B.bodies[wi.bodyFirst + a], B.bodies[wi.bodyFirst + b], A.grow, Bb.grow, A.lo, A.hi,
+                           Bb.lo, Bb.hi, reach, &s_count);
             }
         }
         for (uint32_t pl = 0; pl < wi.planeCount; ++pl) {
@@ -725,6 +768,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_prepare(Batch B, StepParams P, ui
             const DBody& a = B.bodies[c.bodyA];
             const DBody& b = B.bodies[c.bodyB];
             prepareContact(a, b, c);
+            makeContactAxes(a, b, c, B.axes + (size_t)(cf + act[x]) * kAxesPerContact);
             c.flags &= ~kCLaned;
             const bool can = !(c.flags & kCPlanar) && !(c.rollingResistance > 0.0f);
             endA[x] = movingBody(a) ? c.bodyA - wi.bodyFirst : kNone;
@@ -789,6 +833,16 @@ __global__ void __launch_bounds__(kMaxBlock) k_prepare(Batch B, StepParams P, ui
         bucketByColor(nActive, act, colorOf, B.colored + cf, B.rest + cf, wc.colorStart, wc.colorCount, wc.restCount);
         bucketByColor(nImpact, B.impact + cf, colorOf, B.impactColored + cf, B.impactRest + cf, wc.impactColorStart,
                       wc.impactColorCount, wc.impactRestCount);
+        {
+            __shared__ uint32_t s_points;
+            if (threadIdx.x == 0) { s_points = 0; }
+            __syncthreads();
+            uint32_t mine = 0;
+            for (uint32_t x = threadIdx.x; x < nActive; x += blockDim.x) { mine += (uint32_t)cs[act[x]].count; }
+            atomicAdd(&s_points, mine);
+            __syncthreads();
+            if (threadIdx.x == 0) { wc.activePoints = s_points; }
+        }
         if (threadIdx.x == 0) {
             wc.activeCount = nActive;
             wc.impactCount = nImpact;
@@ -871,62 +925,273 @@ __device__ void refreshContact(const Batch& B, const StepParams& P, DContact& c,
     carryImpulses(old, c, P.tol.speculative * P.tol.speculative);
 }
 
-__global__ void __launch_bounds__(kMaxBlock) k_substep(Batch B, StepParams P, int sub, int serial) {
+// The solver state of one body, as the substep keeps it in registers: what warm start, solve and
+// restitution read and write. Field names match DBody so the same solver templates run on either.
+struct SBody {
+    Vec3 v, w, dp;
+    Quat dq;
+    Mat3 invMassWorld, invInertiaWorld;
+    float invMass;
+    uint32_t type, awake;
+};
+
+// What integrateVelocity reads and writes (src/world.cpp:1141-1151).
+struct VelBody {
+    uint32_t alive, type, awake;
+    Vec3 v, w, force, torque;
+    float gravityScale, invMass, linearDamping, angularDamping, kept;
+    Mat3 linearProj, angularProj, invInertiaWorld;
+};
+
+// What integratePosition reads and writes (src/world.cpp:1161-1172).
+struct PosBody {
+    uint32_t alive, type, awake;
+    Vec3 v, w, com, dp, localCenter;
+    Quat dq, qBase;
+    Transform xf;
+    float kept;
+};
+
+constexpr int kSBodyWords = 33;
+
+// Where one world's solver state lives during a substep: shared memory (structure of arrays, stride words
+// apart) for worlds that fit, else the bodies in global memory.
+struct SolverStore {
+    float* s;
+    uint32_t stride;
+    bool staged;
+    DBody* g;
+
+    __device__ __forceinline__ float& at(int word, uint32_t i) const { return s[word * stride + i]; }
+
+    __device__ SBody load(uint32_t i) const {
+        SBody b;
+        if (!staged) {
+            const DBody& d = g[i];
+            b.v = d.v;
+            b.w = d.w;
+            b.dp = d.dp;
+            b.dq = d.dq;
+            b.invMassWorld = d.invMassWorld;
+            b.invInertiaWorld = d.invInertiaWorld;
+            b.invMass = d.invMass;
+            b.type = d.type;
+            b.awake = d.awake;
+            return b;
+        }
+        b.v = { at(0, i), at(1, i), at(2, i) };
+        b.w = { at(3, i), at(4, i), at(5, i) };
+        b.dp = { at(6, i), at(7, i), at(8, i) };
+        b.dq = { at(9, i), at(10, i), at(11, i), at(12, i) };
+        for (int r = 0; r < 3; ++r) {
+            b.invMassWorld.r[r] = { at(13 + 3 * r, i), at(14 + 3 * r, i), at(15 + 3 * r, i) };
+            b.invInertiaWorld.r[r] = { at(22 + 3 * r, i), at(23 + 3 * r, i), at(24 + 3 * r, i) };
+        }
+        b.invMass = at(31, i);
+        const uint32_t f = __float_as_uint(at(32, i));
+        b.type = f & 0xffu;
+        b.awake = f >> 8;
+        return b;
+    }
+
+    __device__ void storeVW(uint32_t i, const SBody& b) const {
+        if (!staged) {
+            g[i].v = b.v;
+            g[i].w = b.w;
+            return;
+        }
+        at(0, i) = b.v.x;
+        at(1, i) = b.v.y;
+        at(2, i) = b.v.z;
+        at(3, i) = b.w.x;
+        at(4, i) = b.w.y;
+        at(5, i) = b.w.z;
+    }
+
+    // Copies a body's solver fields from global memory into the store.
+    __device__ void stage(uint32_t i) const {
+        const DBody& d = g[i];
+        at(0, i) = d.v.x, at(1, i) = d.v.y, at(2, i) = d.v.z;
+        at(3, i) = d.w.x, at(4, i) = d.w.y, at(5, i) = d.w.z;
+        at(6, i) = d.dp.x, at(7, i) = d.dp.y, at(8, i) = d.dp.z;
+        at(9, i) = d.dq.x, at(10, i) = d.dq.y, at(11, i) = d.dq.z, at(12, i) = d.dq.w;
+        for (int r = 0; r < 3; ++r) {
+            at(13 + 3 * r, i) = d.invMassWorld.r[r].x;
+            at(14 + 3 * r, i) = d.invMassWorld.r[r].y;
+            at(15 + 3 * r, i) = d.invMassWorld.r[r].z;
+            at(22 + 3 * r, i) = d.invInertiaWorld.r[r].x;
+            at(23 + 3 * r, i) = d.invInertiaWorld.r[r].y;
+            at(24 + 3 * r, i) = d.invInertiaWorld.r[r].z;
+        }
+        at(31, i) = d.invMass;
+        at(32, i) = __uint_as_float(d.type | (d.awake << 8));
+    }
+
+    // Writes the fields a substep changes back to global memory.
+    __device__ void unstage(uint32_t i) const {
+        DBody& d = g[i];
+        d.v = { at(0, i), at(1, i), at(2, i) };
+        d.w = { at(3, i), at(4, i), at(5, i) };
+        d.dp = { at(6, i), at(7, i), at(8, i) };
+        d.dq = { at(9, i), at(10, i), at(11, i), at(12, i) };
+    }
+
+    __device__ void integrateVelocityAt(uint32_t i, const StepParams& P) const {
+        DBody& d = g[i];
+        if (!d.alive || d.type != kDynamic || !d.awake) { return; }
+        if (!staged) {
+            integrateVelocity(d, P);
+            return;
+        }
+        VelBody b;
+        b.alive = d.alive;
+        b.type = d.type;
+        b.awake = d.awake;
+        b.v = { at(0, i), at(1, i), at(2, i) };
+        b.w = { at(3, i), at(4, i), at(5, i) };
+        b.force = d.force;
+        b.torque = d.torque;
+        b.gravityScale = d.gravityScale;
+        b.invMass = d.invMass;
+        b.linearDamping = d.linearDamping;
+        b.angularDamping = d.angularDamping;
+        b.kept = d.kept;
+        b.linearProj = d.linearProj;
+        b.angularProj = d.angularProj;
+        for (int r = 0; r < 3; ++r) {
+            b.invInertiaWorld.r[r] = { at(22 + 3 * r, i), at(23 + 3 * r, i), at(24 + 3 * r, i) };
+        }
+        integrateVelocity(b, P);
+        at(0, i) = b.v.x, at(1, i) = b.v.y, at(2, i) = b.v.z;
+        at(3, i) = b.w.x, at(4, i) = b.w.y, at(5, i) = b.w.z;
+        d.kept = b.kept;
+    }
+
+    __device__ void integratePositionAt(uint32_t i, const StepParams& P) const {
+        DBody& d = g[i];
+        if (!staged) {
+            integratePosition(d, P);
+            return;
+        }
+        PosBody b;
+        b.alive = d.alive;
+        b.type = d.type;
+        b.awake = d.awake;
+        b.v = { at(0, i), at(1, i), at(2, i) };
+        b.w = { at(3, i), at(4, i), at(5, i) };
+        b.dp = { at(6, i), at(7, i), at(8, i) };
+        b.dq = { at(9, i), at(10, i), at(11, i), at(12, i) };
+        b.com = d.com;
+        b.localCenter = d.localCenter;
+        b.qBase = d.qBase;
+        b.xf = d.xf;
+        b.kept = d.kept;
+        integratePosition(b, P);
+        at(0, i) = b.v.x, at(1, i) = b.v.y, at(2, i) = b.v.z;
+        at(3, i) = b.w.x, at(4, i) = b.w.y, at(5, i) = b.w.z;
+        at(6, i) = b.dp.x, at(7, i) = b.dp.y, at(8, i) = b.dp.z;
+        at(9, i) = b.dq.x, at(10, i) = b.dq.y, at(11, i) = b.dq.z, at(12, i) = b.dq.w;
+        d.com = b.com;
+        d.xf = b.xf;
+        d.kept = b.kept;
+    }
+};
+
+// Fast pairs collided again before a substep (src/world.cpp:1658-1668): inverse mass refreshed, other
+// contacts rebased, dp and dq reset, fast contacts collided with the time left. Does nothing in worlds
+// without such pairs, so it can sit in a recorded graph before every substep but the first.
+__global__ void __launch_bounds__(kMaxBlock) k_refresh(Batch B, StepParams P, int sub, int serial) {
     if (stepAborted(B, serial)) { return; }
     for (int o = blockIdx.x; o < B.nWorlds; o += gridDim.x) {
         const uint32_t w = B.order[o];
         const WorldInfo wi = B.info[w];
         WorldCounts& wc = B.counts[w];
+        const int n = P.substeps;
+        const uint8_t againFlag = sub == n / 2 ? kFlagFast : kFlagFastSolid;
+        const uint32_t againCount = sub == n / 2 ? wc.fastCount : wc.fastSolidCount;
+        if (!(sub > 0 && againCount > 0)) { continue; }
         const uint32_t cf = wi.contactFirst;
         DContact* cs = B.contacts + cf;
         const uint32_t nActive = wc.activeCount;
         const uint32_t* act = B.active + cf;
-        const int n = P.substeps;
-        const uint8_t againFlag = sub == n / 2 ? kFlagFast : kFlagFastSolid;
-        const uint32_t againCount = sub == n / 2 ? wc.fastCount : wc.fastSolidCount;
-        if (sub > 0 && againCount > 0) {
-            for (uint32_t i = threadIdx.x; i < wi.bodyCount; i += blockDim.x) {
-                DBody& b = B.bodies[wi.bodyFirst + i];
-                if (b.alive && b.type == kDynamic && b.awake) { updateInverseMass(b); }
-            }
-            __syncthreads();
-            for (uint32_t x = threadIdx.x; x < nActive; x += blockDim.x) {
-                const uint32_t ci = act[x];
-                if (B.cflags[cf + ci] & againFlag) { continue; }
-                if (!contactOk(B, wi, wc, ci, 16)) { continue; }
-                DContact& c = cs[ci];
-                rebaseContact(B.bodies[c.bodyA], B.bodies[c.bodyB], c);
-            }
-            __syncthreads();
-            for (uint32_t i = threadIdx.x; i < wi.bodyCount; i += blockDim.x) {
-                DBody& b = B.bodies[wi.bodyFirst + i];
-                b.dp = zero3();
-                b.dq = qid();
-                b.qBase = b.xf.q;
-            }
-            __syncthreads();
-            const float remaining = (float)(n - sub) * P.h;
-            for (uint32_t x = threadIdx.x; x < nActive; x += blockDim.x) {
-                const uint32_t ci = act[x];
-                if (!(B.cflags[cf + ci] & againFlag)) { continue; }
-                if (!contactOk(B, wi, wc, ci, 14)) { continue; }
-                refreshContact(B, P, cs[ci], remaining);
-            }
-            __syncthreads();
-        }
         for (uint32_t i = threadIdx.x; i < wi.bodyCount; i += blockDim.x) {
-            integrateVelocity(B.bodies[wi.bodyFirst + i], P);
+            DBody& b = B.bodies[wi.bodyFirst + i];
+            if (b.alive && b.type == kDynamic && b.awake) { updateInverseMass(b); }
         }
         __syncthreads();
+        for (uint32_t x = threadIdx.x; x < nActive; x += blockDim.x) {
+            const uint32_t ci = act[x];
+            if (B.cflags[cf + ci] & againFlag) { continue; }
+            if (!contactOk(B, wi, wc, ci, 16)) { continue; }
+            DContact& c = cs[ci];
+            rebaseContact(B.bodies[c.bodyA], B.bodies[c.bodyB], c);
+        }
+        __syncthreads();
+        for (uint32_t i = threadIdx.x; i < wi.bodyCount; i += blockDim.x) {
+            DBody& b = B.bodies[wi.bodyFirst + i];
+            b.dp = zero3();
+            b.dq = qid();
+            b.qBase = b.xf.q;
+        }
+        __syncthreads();
+        const float remaining = (float)(n - sub) * P.h;
+        for (uint32_t x = threadIdx.x; x < nActive; x += blockDim.x) {
+            const uint32_t ci = act[x];
+            if (!(B.cflags[cf + ci] & againFlag)) { continue; }
+            if (!contactOk(B, wi, wc, ci, 14)) { continue; }
+            refreshContact(B, P, cs[ci], remaining);
+        }
+        __syncthreads();
+        // Every active contact's axes again, from the refreshed inertia and the new anchors.
+        for (uint32_t x = threadIdx.x; x < nActive; x += blockDim.x) {
+            const uint32_t ci = act[x];
+            if (!contactOk(B, wi, wc, ci, 26)) { continue; }
+            const DContact& c = cs[ci];
+            makeContactAxes(B.bodies[c.bodyA], B.bodies[c.bodyB], c, B.axes + (size_t)(cf + ci) * kAxesPerContact);
+        }
+        __syncthreads();
+    }
+}
+
+// Integrate velocities, warm start, biased solve, integrate positions, relax (src/world.cpp:1669-1680), with
+// the world's bodies staged in shared memory when they fit (stageBodies of them).
+__global__ void __launch_bounds__(kMaxBlock) k_substep(Batch B, StepParams P, uint32_t stageBodies, int serial) {
+    extern __shared__ __align__(16) float s_bodies[];
+    if (stepAborted(B, serial)) { return; }
+    for (int o = blockIdx.x; o < B.nWorlds; o += gridDim.x) {
+        const uint32_t w = B.order[o];
+        const WorldInfo wi = B.info[w];
+        const WorldCounts& wc = B.counts[w];
+        const uint32_t cf = wi.contactFirst;
+        DContact* cs = B.contacts + cf;
+        const uint32_t nb = wi.bodyCount;
+        const SolverStore st{ s_bodies, stageBodies, nb <= stageBodies, B.bodies + wi.bodyFirst };
+        if (st.staged) {
+            for (uint32_t i = threadIdx.x; i < nb; i += blockDim.x) { st.stage(i); }
+            __syncthreads();
+        }
+        for (uint32_t i = threadIdx.x; i < nb; i += blockDim.x) { st.integrateVelocityAt(i, P); }
+        __syncthreads();
+        const uint32_t base = wi.bodyFirst;
+        // A laned contact's bodies are stored only where they move, so a static body shared by a color's
+        // contacts is never written concurrently; a contact solved on its own stores both, as the reference does.
         auto warm = [&](uint32_t ci, bool laned) {
             if (!contactOk(B, wi, wc, ci, 10)) { return; }
-            DContact& c = cs[ci];
-            warmStartContact(B.bodies[c.bodyA], B.bodies[c.bodyB], c, laned);
+            const DContact& c = cs[ci];
+            const uint32_t ia = c.bodyA - base, ib = c.bodyB - base;
+            SBody a = st.load(ia), b = st.load(ib);
+            warmStartContact(a, b, c, laned, B.axes + (size_t)(cf + ci) * kAxesPerContact);
+            if (!laned || !anchored(a)) { st.storeVW(ia, a); }
+            if (!laned || !anchored(b)) { st.storeVW(ib, b); }
         };
-        auto solve = [&](uint32_t ci, bool bias) {
+        auto solve = [&](uint32_t ci, bool bias, bool laned) {
             if (!contactOk(B, wi, wc, ci, 12)) { return; }
             DContact& c = cs[ci];
-            solveContact(B.bodies[c.bodyA], B.bodies[c.bodyB], c, P, bias);
+            const uint32_t ia = c.bodyA - base, ib = c.bodyB - base;
+            SBody a = st.load(ia), b = st.load(ib);
+            solveContact(a, b, c, P, bias, B.axes + (size_t)(cf + ci) * kAxesPerContact);
+            if (!laned || !anchored(a)) { st.storeVW(ia, a); }
+            if (!laned || !anchored(b)) { st.storeVW(ib, b); }
         };
         const uint32_t* colored = B.colored + cf;
         const uint32_t* rest = B.rest + cf;
@@ -939,24 +1204,27 @@ __global__ void __launch_bounds__(kMaxBlock) k_substep(Batch B, StepParams P, in
         __syncthreads();
         for (int pass = 0; pass < 2; ++pass) {
             const bool bias = pass == 0;
-            forEachColor(colored, wc.colorStart, wc.colorCount, [&](uint32_t ci) { solve(ci, bias); });
+            forEachColor(colored, wc.colorStart, wc.colorCount, [&](uint32_t ci) { solve(ci, bias, true); });
             if (threadIdx.x == 0) {
-                for (uint32_t x = 0; x < wc.restCount; ++x) { solve(rest[x], bias); }
+                for (uint32_t x = 0; x < wc.restCount; ++x) { solve(rest[x], bias, false); }
             }
             __syncthreads();
             if (wc.impactCount > 0) {
-                forEachColor(icolored, wc.impactColorStart, wc.impactColorCount, [&](uint32_t ci) { solve(ci, bias); });
+                forEachColor(icolored, wc.impactColorStart, wc.impactColorCount,
+                             [&](uint32_t ci) { solve(ci, bias, true); });
                 if (threadIdx.x == 0) {
-                    for (uint32_t x = 0; x < wc.impactRestCount; ++x) { solve(irest[x], bias); }
+                    for (uint32_t x = 0; x < wc.impactRestCount; ++x) { solve(irest[x], bias, false); }
                 }
                 __syncthreads();
             }
             if (bias) {
-                for (uint32_t i = threadIdx.x; i < wi.bodyCount; i += blockDim.x) {
-                    integratePosition(B.bodies[wi.bodyFirst + i], P);
-                }
+                for (uint32_t i = threadIdx.x; i < nb; i += blockDim.x) { st.integratePositionAt(i, P); }
                 __syncthreads();
             }
+        }
+        if (st.staged) {
+            for (uint32_t i = threadIdx.x; i < nb; i += blockDim.x) { st.unstage(i); }
+            __syncthreads();
         }
     }
 }
@@ -997,13 +1265,14 @@ __global__ void __launch_bounds__(kMaxBlock) k_finish(Batch B, StepParams P, uin
         forEachColor(B.colored + cf, wc.colorStart, wc.colorCount, [&](uint32_t ci) {
             if (!contactOk(B, wi, wc, ci, 18)) { return; }
             DContact& c = cs[ci];
-            restituteContact(B.bodies[c.bodyA], B.bodies[c.bodyB], c, P, true);
+            restituteContact(B.bodies[c.bodyA], B.bodies[c.bodyB], c, P, true, B.axes + (size_t)(cf + ci) * kAxesPerContact);
         });
         if (threadIdx.x == 0) {
             for (uint32_t x = 0; x < wc.restCount; ++x) {
                 if (!contactOk(B, wi, wc, B.rest[cf + x], 20)) { continue; }
                 DContact& c = cs[B.rest[cf + x]];
-                restituteContact(B.bodies[c.bodyA], B.bodies[c.bodyB], c, P, false);
+                restituteContact(B.bodies[c.bodyA], B.bodies[c.bodyB], c, P, false,
+                                 B.axes + (size_t)(cf + B.rest[cf + x]) * kAxesPerContact);
             }
         }
         __syncthreads();
@@ -1130,6 +1399,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_finish(Batch B, StepParams P, uin
         if (threadIdx.x == 0) {
             wc.awakeBodies = s_awake;
             wc.awakeIslands = s_islands;
+            wc.bodySteps += s_awake;
             if (s_sweep > 0) {
                 wc.sweepShapes += s_sweep;
                 wc.flags |= kDevSweepSkipped;
@@ -1137,6 +1407,32 @@ __global__ void __launch_bounds__(kMaxBlock) k_finish(Batch B, StepParams P, uin
         }
         __syncthreads();
     }
+}
+
+// ---------------------------------------------------------------------------------------------------------
+// Host traffic of a running batch: per-step forces in, poses out.
+
+// World::addForce / addTorque with wake = false on every body (src/world.cpp:2118-2142).
+__global__ void k_add_forces(DBody* bodies, uint32_t n, const float* __restrict__ f, const float* __restrict__ t) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) { return; }
+    DBody& b = bodies[i];
+    if (!b.alive || b.type != kDynamic || !b.awake) { return; }
+    if (f) { b.force += Vec3{ f[3 * i], f[3 * i + 1], f[3 * i + 2] }; }
+    if (t) { b.torque += Vec3{ t[3 * i], t[3 * i + 1], t[3 * i + 2] }; }
+}
+
+__global__ void k_pack_poses(const DBody* bodies, uint32_t n, float* __restrict__ p, float* __restrict__ q) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) { return; }
+    const Transform xf = bodies[i].xf;
+    p[3 * i] = xf.p.x;
+    p[3 * i + 1] = xf.p.y;
+    p[3 * i + 2] = xf.p.z;
+    q[4 * i] = xf.q.x;
+    q[4 * i + 1] = xf.q.y;
+    q[4 * i + 2] = xf.q.z;
+    q[4 * i + 3] = xf.q.w;
 }
 
 }

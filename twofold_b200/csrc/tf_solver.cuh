@@ -6,9 +6,8 @@
 // alike. Contacts of one color move no body in common, so a color's contacts run in parallel with results
 // identical to any sequential order.
 //
-// Effective masses are not stored: each solve rebuilds a point's axes from its anchors and the bodies'
-// world inverse mass and inertia, which change only where the reference rebuilds its axes (step start and
-// the mid-step refresh), so the rebuilt axes are the reference's stored axes bit for bit.
+// Each point's three axes (lever arms, velocity change per unit impulse, effective mass) are built where the
+// reference builds them, at the step's start and after a mid-step refresh, and read by every pass between.
 #pragma once
 
 #include "tf_body.cuh"
@@ -17,14 +16,20 @@
 namespace tfb {
 
 // One direction at a contact point (src/internal.h:508-520, src/solver.cpp:5-17).
-struct Axis {
+struct alignas(16) Axis {
     Vec3 armA, armB;
     Vec3 linearA, angularA;
     Vec3 linearB, angularB;
     float mass;
+    float pad;
 };
 
-TF_HD Axis makeAxis(const DBody& a, const DBody& b, const Vec3& ra, const Vec3& rb, const Vec3& d) {
+// A contact's axes are built once per step and again after a mid-step refresh, as the reference builds them
+// (src/lanes.cpp:66-110, src/solver.cpp:43-50), and stored 3 per point: normal, tangent1, tangent2.
+constexpr int kAxesPerContact = 12;
+
+template <class BodyT>
+TF_HD Axis makeAxis(const BodyT& a, const BodyT& b, const Vec3& ra, const Vec3& rb, const Vec3& d) {
     Axis x;
     x.armA = cross(ra, d);
     x.armB = cross(rb, d);
@@ -37,11 +42,13 @@ TF_HD Axis makeAxis(const DBody& a, const DBody& b, const Vec3& ra, const Vec3& 
     return x;
 }
 
-TF_HD float speedAlong(const DBody& a, const DBody& b, const Vec3& d, const Axis& x) {
+template <class BodyT>
+TF_HD float speedAlong(const BodyT& a, const BodyT& b, const Vec3& d, const Axis& x) {
     return dot(d, b.v - a.v) + dot(x.armB, b.w) - dot(x.armA, a.w);
 }
 
-TF_HD void pushMoving(DBody& a, DBody& b, const Axis& x, float impulse, bool moveA, bool moveB) {
+template <class BodyT>
+TF_HD void pushMoving(BodyT& a, BodyT& b, const Axis& x, float impulse, bool moveA, bool moveB) {
     if (moveA) {
         a.v -= x.linearA * impulse;
         a.w -= x.angularA * impulse;
@@ -53,11 +60,13 @@ TF_HD void pushMoving(DBody& a, DBody& b, const Axis& x, float impulse, bool mov
 }
 
 // Where the body has turned r since the substep's base pose (src/solver.cpp:58-61).
-TF_HD Vec3 turned(const DBody& b, const Vec3& r) {
+template <class BodyT>
+TF_HD Vec3 turned(const BodyT& b, const Vec3& r) {
     return b.dq.x == 0.0f && b.dq.y == 0.0f && b.dq.z == 0.0f ? r : rotate(b.dq, r);
 }
 
-TF_HD bool anchored(const DBody& b) { return b.type != kDynamic || !b.awake; }
+template <class BodyT>
+TF_HD bool anchored(const BodyT& b) { return b.type != kDynamic || !b.awake; }
 
 TF_HD Softness makeSoft(float hertz, float zeta, float h) {
     if (hertz == 0.0f) { return { 0.0f, 1.0f, 0.0f }; }
@@ -113,6 +122,18 @@ TF_HD void prepareContact(const DBody& a, const DBody& b, DContact& c) {
     }
 }
 
+// The axes of every point of a contact (src/solver.cpp:43-50), from the bodies' current world inverse mass
+// and inertia.
+template <class BodyT>
+TF_HD void makeContactAxes(const BodyT& a, const BodyT& b, const DContact& c, Axis* out) {
+    for (int i = 0; i < c.count; ++i) {
+        const DPoint& p = c.points[i];
+        out[3 * i] = makeAxis(a, b, p.anchorA, p.anchorB, c.normal);
+        out[3 * i + 1] = makeAxis(a, b, p.anchorA, p.anchorB, c.tangent1);
+        out[3 * i + 2] = makeAxis(a, b, p.anchorA, p.anchorB, c.tangent2);
+    }
+}
+
 // Re-expresses anchors as the bodies' current lever arms before their dp and dq are reset
 // (src/solver.cpp:293-306).
 TF_HD void rebaseContact(const DBody& a, const DBody& b, DContact& c) {
@@ -129,13 +150,12 @@ TF_HD void rebaseContact(const DBody& a, const DBody& b, DContact& c) {
 // the bodies that move; a contact solved on its own pushes both, as the reference's scalar warm start does
 // (the anchored body's zero inverse mass leaves it unchanged). Contacts solved on their own run one at a
 // time, so the unmasked push never races.
-TF_HD void warmStartContact(DBody& a, DBody& b, const DContact& c, bool laned) {
+template <class BodyT>
+TF_HD void warmStartContact(BodyT& a, BodyT& b, const DContact& c, bool laned, const Axis* ax) {
     const bool moveA = !laned || !anchored(a), moveB = !laned || !anchored(b);
     for (int i = 0; i < c.count; ++i) {
         const DPoint& p = c.points[i];
-        const Axis xn = makeAxis(a, b, p.anchorA, p.anchorB, c.normal);
-        const Axis x1 = makeAxis(a, b, p.anchorA, p.anchorB, c.tangent1);
-        const Axis x2 = makeAxis(a, b, p.anchorA, p.anchorB, c.tangent2);
+        const Axis xn = ax[3 * i], x1 = ax[3 * i + 1], x2 = ax[3 * i + 2];
         pushMoving(a, b, xn, p.normalImpulse, moveA, moveB);
         pushMoving(a, b, x1, dot(p.tangentImpulse, c.tangent1), moveA, moveB);
         pushMoving(a, b, x2, dot(p.tangentImpulse, c.tangent2), moveA, moveB);
@@ -148,7 +168,8 @@ TF_HD void warmStartContact(DBody& a, DBody& b, const DContact& c, bool laned) {
 
 // One step along the relative spin, held to the rolling limit (src/solver.cpp:225-251). Rolling contacts are
 // never laned, so this runs one contact at a time and pushes both bodies as the reference does.
-TF_HD void resistTurning(DBody& a, DBody& b, DContact& c) {
+template <class BodyT>
+TF_HD void resistTurning(BodyT& a, BodyT& b, DContact& c) {
     const Vec3 spin = b.w - a.w;
     const float speed = length(spin);
     Vec3 total = c.rollingImpulse;
@@ -178,7 +199,8 @@ TF_HD void resistTurning(DBody& a, DBody& b, DContact& c) {
 
 // The soft normal rows, then friction (forward in the biased pass, reverse in relax), then rolling
 // (src/solver.cpp:360-421).
-TF_HD void solveContact(DBody& a, DBody& b, DContact& c, const StepParams& P, bool useBias) {
+template <class BodyT>
+TF_HD void solveContact(BodyT& a, BodyT& b, DContact& c, const StepParams& P, bool useBias, const Axis* ax) {
     const bool moveA = !anchored(a), moveB = !anchored(b);
     const Softness soft = (!moveA || !moveB) ? P.staticSoft : P.contactSoft;
     const Vec3 dp = b.dp - a.dp;
@@ -194,7 +216,7 @@ TF_HD void solveContact(DBody& a, DBody& b, DContact& c, const StepParams& P, bo
             massScale = soft.massScale;
             impulseScale = soft.impulseScale;
         }
-        const Axis x = makeAxis(a, b, p.anchorA, p.anchorB, c.normal);
+        const Axis x = ax[3 * i];
         const float vn = speedAlong(a, b, c.normal, x);
         float impulse = -x.mass * massScale * (vn + bias) - impulseScale * p.normalImpulse;
         const float total = maxf(p.normalImpulse + impulse, 0.0f);
@@ -206,8 +228,7 @@ TF_HD void solveContact(DBody& a, DBody& b, DContact& c, const StepParams& P, bo
     for (int j = 0; j < c.count; ++j) {
         const int i = useBias ? j : c.count - 1 - j;
         DPoint& p = c.points[i];
-        const Axis x1 = makeAxis(a, b, p.anchorA, p.anchorB, c.tangent1);
-        const Axis x2 = makeAxis(a, b, p.anchorA, p.anchorB, c.tangent2);
+        const Axis x1 = ax[3 * i + 1], x2 = ax[3 * i + 2];
         const float old1 = dot(p.tangentImpulse, c.tangent1), old2 = dot(p.tangentImpulse, c.tangent2);
         float t1 = old1 - x1.mass * speedAlong(a, b, c.tangent1, x1);
         float t2 = old2 - x2.mass * speedAlong(a, b, c.tangent2, x2);
@@ -227,13 +248,14 @@ TF_HD void solveContact(DBody& a, DBody& b, DContact& c, const StepParams& P, bo
 
 // One restitution pass over the points that approached fast (src/solver.cpp:423-460, src/lanes.cpp:318-352),
 // pushing as warmStartContact does.
-TF_HD void restituteContact(DBody& a, DBody& b, DContact& c, const StepParams& P, bool laned) {
+template <class BodyT>
+TF_HD void restituteContact(BodyT& a, BodyT& b, DContact& c, const StepParams& P, bool laned, const Axis* ax) {
     if (c.restitution == 0.0f) { return; }
     const bool moveA = !laned || !anchored(a), moveB = !laned || !anchored(b);
     for (int i = 0; i < c.count; ++i) {
         DPoint& p = c.points[i];
         if (p.relativeVelocity > -P.restitutionThreshold || p.maxNormalImpulse == 0.0f) { continue; }
-        const Axis x = makeAxis(a, b, p.anchorA, p.anchorB, c.normal);
+        const Axis x = ax[3 * i];
         const float vn = speedAlong(a, b, c.normal, x);
         float impulse = -x.mass * (vn + c.restitution * p.relativeVelocity);
         const float total = maxf(p.normalImpulse + impulse, 0.0f);
@@ -245,7 +267,8 @@ TF_HD void restituteContact(DBody& a, DBody& b, DContact& c, const StepParams& P
 }
 
 // Gravity, forces, damping, locks and the speed limits (src/world.cpp:1141-1151).
-TF_HD void integrateVelocity(DBody& b, const StepParams& P) {
+template <class BodyT>
+TF_HD void integrateVelocity(BodyT& b, const StepParams& P) {
     if (!b.alive || b.type != kDynamic || !b.awake) { return; }
     const float h = P.h;
     b.v = b.v + (P.gravity * b.gravityScale + b.force * b.invMass) * h;
@@ -256,7 +279,8 @@ TF_HD void integrateVelocity(DBody& b, const StepParams& P) {
 }
 
 // The speed limits, then the pose update (src/world.cpp:1161-1172).
-TF_HD void integratePosition(DBody& b, const StepParams& P) {
+template <class BodyT>
+TF_HD void integratePosition(BodyT& b, const StepParams& P) {
     if (b.alive) { limitSpeed(b, P.maxLinearSpeed, P.maxAngularSpeed); }
     if (!b.alive || b.type == kStatic) { return; }
     if (b.type == kDynamic && !b.awake) { return; }

@@ -192,8 +192,10 @@ struct WorldCounts {
     uint32_t candNeeded;       // largest count seen, for growing capacities
     uint32_t contactNeeded;
     uint32_t sweepShapes;      // shapes the continuous pass would sweep
+    uint32_t activePoints;     // contact points of the active list
     uint32_t colorStart[kColors + 1];
     uint32_t impactColorStart[kColors + 1];
+    unsigned long long bodySteps;  // awake dynamic bodies summed over every step since the layout
 };
 
 struct Tolerances {

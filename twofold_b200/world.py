@@ -110,3 +110,42 @@ class Batch:
         f = C.c_uint32(0)
         abi.check(self.lib.tf_world_device_status(self.h, C.byref(f)), self.lib)
         return f.value
+
+    # Timing and host traffic of a running batch.
+
+    def elapsed_ms(self):
+        ms = C.c_float(0)
+        abi.check(self.lib.tf_world_elapsed_ms(self.h, C.byref(ms)), self.lib)
+        return ms.value
+
+    def body_steps(self):
+        n = C.c_int64(0)
+        abi.check(self.lib.tf_world_body_steps(self.h, C.byref(n)), self.lib)
+        return n.value
+
+    def add_forces(self, forces=None, torques=None):
+        """forces/torques: float32 arrays (total_bodies, 3), ideally in pinned host memory."""
+        f = forces.ctypes.data if forces is not None else None
+        t = torques.ctypes.data if torques is not None else None
+        abi.check(self.lib.tf_world_add_forces(self.h, f, t), self.lib)
+
+    def read_poses(self, positions, rotations):
+        abi.check(self.lib.tf_world_read_poses(self.h, positions.ctypes.data, rotations.ctypes.data), self.lib)
+
+    def set_profiling(self, on=True):
+        abi.check(self.lib.tf_world_set_profiling(self.h, 1 if on else 0), self.lib)
+
+    def kernel_times(self):
+        """{kernel name: (total ms, launches)} since profiling was turned on."""
+        ms = np.zeros(16, np.float32)
+        n = np.zeros(16, np.int64)
+        cnt = C.c_int32(0)
+        abi.check(self.lib.tf_world_kernel_times(self.h, ms.ctypes.data, n.ctypes.data, 16, C.byref(cnt)), self.lib)
+        return {self.lib.tf_kernel_name(k).decode(): (float(ms[k]), int(n[k])) for k in range(cnt.value)}
+
+    def work_counts(self):
+        """Work of the last step: bodies, awake, candidates, contacts, active contacts, active points."""
+        out = np.zeros(6, np.int64)
+        abi.check(self.lib.tf_world_work_counts(self.h, out.ctypes.data), self.lib)
+        keys = ("bodies", "awake", "candidates", "contacts", "active_contacts", "active_points")
+        return dict(zip(keys, (int(x) for x in out)))
