@@ -267,6 +267,16 @@ TF_API const char* tf_kernel_name(int32_t kernel);
  * pairs, [3] contacts, [4] active contacts, [5] active contact points. */
 TF_API int tf_world_work_counts(void* world, int64_t out[6]);
 
+/* Launch shape of one kernel (0 broadphase, 1 narrowphase, 2 wake, 3 prepare, 4 refresh, 5 substep,
+ * 6 finish; -1 every kernel): threads per CTA (a multiple of 32, at most 512), the world size in bodies
+ * above which a world is stepped by a whole CTA (smaller worlds take one warp each), and the shared memory
+ * a CTA stages worlds in (clamped to what the device allows). Takes effect at the next step. No
+ * counterpart in the reference, which steps each world on one host thread; the autotuner uses it. */
+TF_API int tf_world_set_launch(void* world, int32_t kernel, int32_t threads, int32_t big_bodies, int32_t smem_bytes);
+/* The shape in use: out[0] threads, [1] big-world threshold, [2] shared bytes, [3] grid size, [4] bodies
+ * a whole-CTA world can stage, [5] bodies a warp's world can stage. */
+TF_API int tf_world_get_launch(void* world, int32_t kernel, uint32_t out[6]);
+
 #ifdef __cplusplus
 }
 #endif

@@ -54,6 +54,9 @@ struct Batch {
     uint32_t* mergePartB;
     uint32_t* mergeIdxB;
 
+    uint32_t* work;        // per launch of a step, the next world to hand out (zeroed when the step starts)
+    uint32_t* rowScratch;  // per shape, the candidate key sort's row counts
+
     // Debug builds (TF_DEVICE_CHECKS) record the first failed index check here: code, world, value.
     uint32_t* debug;
     uint32_t nPolys;

@@ -12,6 +12,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <memory>
 #include <string>
 #include <vector>
@@ -106,7 +107,6 @@ public:
     std::vector<uint32_t> order;
     std::vector<uint32_t> bodyBase, shapeBase;
     size_t totalBodies = 0, totalShapes = 0, totalCand = 0, totalContacts = 0;
-    uint32_t sortCap = 0;
     float capFactor = 6.0f;
     BoxTopology boxTopology{};
 
@@ -140,12 +140,25 @@ public:
     DevArray<uint32_t> dDebug;
     size_t nPolys = 0;
 
-    // Shared-memory staging sizes for this layout, and per-world list capacities raised after an overflow.
-    uint32_t stageBodies = 1, stageContacts = 1, stageBroad = 1, stageSolve = 1;
-    size_t prepareSmem = 0, finishSmem = 0, broadSmem = 0, solveSmem = 0;
-    int solveBlock = 128;
+    // How each kernel is launched: threads per CTA, the world size above which a world gets the whole CTA
+    // (smaller worlds get a warp each), and the dynamic shared memory a CTA stages worlds in. A caller's
+    // choice (tf_world_set_launch) overrides the defaults derived from the batch's world sizes.
+    struct LaunchShape {
+        uint32_t threads = 256, bigBodies = 0, smemBytes = 0;
+        bool chosen = false;
+    };
+    // broadphase, narrowphase, wake, prepare, refresh, substep, finish
+    static constexpr int kKernels = 7;
+    LaunchShape shapes[kKernels];
+    Split splits[kKernels];
+    int grids[kKernels] = {};
+    std::map<const void*, size_t> dynSmemLimit;
+    bool kernelsConfigured = false;
+    uint32_t maxWorldBodies = 0, maxWorldContacts = 0, medianWorldBodies = 0;
+    std::vector<uint32_t> sortedSizes;  // world body counts, largest first
+    bool laidOut = false;
+    DevArray<uint32_t> dWork, dRowScratch;
     std::vector<uint32_t> minCandCap, minContactCap;
-    bool sortLimitHit = false;
 
     // Host traffic staging and timing.
     DevArray<float> dHostIn, dHostOut;
@@ -460,7 +473,6 @@ public:
             if (counts[w].contactNeeded > wi.contactCap) {
                 minContactCap[w] = std::max(minContactCap[w], counts[w].contactNeeded + counts[w].contactNeeded / 4 + 64);
             }
-            if (counts[w].candNeeded > 8192u) { sortLimitHit = true; }
             for (size_t i = 0; i < W.bodies.size(); ++i) {
                 DBody d = bodies[wi.bodyFirst + i];
                 // Keep the host's own bookkeeping fields.
@@ -606,17 +618,20 @@ public:
         for (size_t w = 0; w < nw; ++w) { order[w] = (uint32_t)w; }
         std::stable_sort(order.begin(), order.end(),
                          [&](uint32_t a, uint32_t b) { return info[a].bodyCount > info[b].bodyCount; });
-        sortCap = 1;
-        while (sortCap < maxCap) { sortCap <<= 1; }
-        sortCap = std::min<uint32_t>(sortCap, 8192u);
-        stageBodies = std::max<uint32_t>(1, std::min(kStageBodies, maxBodies));
-        stageContacts = std::max<uint32_t>(1, std::min(kStageContacts, maxContacts));
-        prepareSmem = ((size_t)stageBodies * 4 + (size_t)stageContacts * 9 + 15) / 16 * 16;
-        finishSmem = (size_t)stageBodies * 8 + (size_t)stageContacts * 8;
-        stageBroad = std::max<uint32_t>(1, std::min(kBroadStage, maxBodies));
-        broadSmem = (size_t)sortCap * sizeof(uint64_t) + (size_t)stageBroad * sizeof(PairBody);
-        stageSolve = std::max<uint32_t>(1, std::min(kSolveStage, maxBodies));
-        solveSmem = (size_t)stageSolve * kSBodyWords * sizeof(float);
+        maxWorldBodies = maxBodies;
+        maxWorldContacts = maxContacts;
+        {
+            std::vector<uint32_t> sizes(nw);
+            for (size_t w = 0; w < nw; ++w) { sizes[w] = info[w].bodyCount; }
+            std::sort(sizes.begin(), sizes.end(), std::greater<uint32_t>());
+            medianWorldBodies = nw ? sizes[nw / 2] : 0;
+            sortedSizes = std::move(sizes);
+        }
+        laidOut = true;
+        {
+            const int rc0 = configureLaunches();
+            if (rc0 != TF_OK) { return rc0; }
+        }
 
         int rc;
 #define TF_ALLOC(arr, count) \
@@ -662,6 +677,8 @@ public:
         TF_ALLOC(dMergePartB, ncon);
         TF_ALLOC(dMergeIdxA, ncon);
         TF_ALLOC(dMergeIdxB, ncon);
+        TF_ALLOC(dWork, kSlotCount);
+        TF_ALLOC(dRowScratch, ns);
         TF_ALLOC(dAbort, 1);
         TF_ALLOC(dDebug, 4);
         nPolys = polys.size();
@@ -728,7 +745,7 @@ public:
     StepParams params(float dt) const {
         StepParams P{};
         const tf_settings& s = settings;
-        const int n = std::max(1, (int)s.substeps);
+        const int n = std::min(kMaxSubsteps, std::max(1, (int)s.substeps));
         P.gravity = v3of(s.gravity);
         P.lengthUnit = s.length_unit;
         P.substeps = n;
@@ -793,6 +810,8 @@ public:
         B.mergeKeyB = dMergeKeyB.ptr;
         B.mergePartB = dMergePartB.ptr;
         B.mergeIdxB = dMergeIdxB.ptr;
+        B.work = dWork.ptr;
+        B.rowScratch = dRowScratch.ptr;
         B.debug = dDebug.ptr;
         B.nPolys = (uint32_t)nPolys;
         B.totalBodies = (uint32_t)totalBodies;
@@ -805,21 +824,22 @@ public:
         const StepParams P = params(dt);
         Batch B = batch(into);
         B.cx.tol = P.tol;
-        const int grid = (int)std::min<size_t>(worlds.size(), (size_t)smCount * 8);
-        const int tb = blockSize;
         const bool rec = profiling && !capturing;
+        auto threads = [&](int k) { return (int)shapes[k].threads; };
+        auto smem = [&](int k) { return (size_t)splits[k].smemBytes; };
+        cudaMemsetAsync(dWork.ptr, 0, kSlotCount * sizeof(uint32_t), stream);
         if (marks) { cudaEventRecord(marks[0], stream); }
-        timed(0, rec, [&] { k_broadphase<<<grid, tb, broadSmem, stream>>>(B, P, sortCap, stageBroad, serial); });
+        timed(0, rec, [&] { k_broadphase<<<grids[0], threads(0), smem(0), stream>>>(B, P, splits[0], serial); });
         if (marks) { cudaEventRecord(marks[1], stream); }
-        timed(1, rec, [&] { k_narrowphase<<<grid, tb, 0, stream>>>(B, P, serial); });
-        timed(2, rec, [&] { k_wake<<<grid, 32, 0, stream>>>(B, serial); });
+        timed(1, rec, [&] { k_narrowphase<<<grids[1], threads(1), 0, stream>>>(B, P, splits[1], serial); });
+        timed(2, rec, [&] { k_wake<<<grids[2], threads(2), 0, stream>>>(B, splits[2], serial); });
         if (marks) { cudaEventRecord(marks[2], stream); }
-        timed(3, rec, [&] { k_prepare<<<grid, tb, prepareSmem, stream>>>(B, P, stageBodies, stageContacts, serial); });
+        timed(3, rec, [&] { k_prepare<<<grids[3], threads(3), smem(3), stream>>>(B, P, splits[3], serial); });
         for (int i = 0; i < P.substeps; ++i) {
-            if (i > 0) { timed(4, rec, [&] { k_refresh<<<grid, tb, 0, stream>>>(B, P, i, serial); }); }
-            timed(5, rec, [&] { k_substep<<<grid, solveBlock, solveSmem, stream>>>(B, P, stageSolve, serial); });
+            if (i > 0) { timed(4, rec, [&] { k_refresh<<<grids[4], threads(4), 0, stream>>>(B, P, splits[4], i, serial); }); }
+            timed(5, rec, [&] { k_substep<<<grids[5], threads(5), smem(5), stream>>>(B, P, splits[5], i, serial); });
         }
-        timed(6, rec, [&] { k_finish<<<grid, tb, finishSmem, stream>>>(B, P, stageBodies, stageContacts, serial); });
+        timed(6, rec, [&] { k_finish<<<grids[6], threads(6), smem(6), stream>>>(B, P, splits[6], serial); });
         if (marks) { cudaEventRecord(marks[3], stream); }
         launches += 5 + 2 * P.substeps - 1;
         cudaError_t e = cudaGetLastError();
@@ -828,17 +848,118 @@ public:
     }
 
     int configureKernels() {
-        static bool done = false;
-        if (done) { return TF_OK; }
-        TF_CUDA(cudaFuncSetAttribute(k_broadphase, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)(8192 * sizeof(uint64_t) + kBroadStage * sizeof(PairBody))));
-        TF_CUDA(cudaFuncSetAttribute(k_substep, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)(kSolveStage * kSBodyWords * sizeof(float))));
-        TF_CUDA(cudaFuncSetAttribute(k_prepare, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)(kStageBodies * 4 + kStageContacts * 9 + 16)));
-        TF_CUDA(cudaFuncSetAttribute(k_finish, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)(kStageBodies * 8 + kStageContacts * 8)));
+        if (kernelsConfigured) { return TF_OK; }
+        bool& done = kernelsConfigured;
+        int maxSmem = 0;
+        TF_CUDA(cudaDeviceGetAttribute(&maxSmem, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
+        // Dynamic shared memory may use what the kernel's static shared variables leave.
+        auto allow = [&](const void* fn) -> int {
+            cudaFuncAttributes a{};
+            TF_CUDA(cudaFuncGetAttributes(&a, fn));
+            TF_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, maxSmem - (int)a.sharedSizeBytes));
+            dynSmemLimit[fn] = (size_t)(maxSmem - (int)a.sharedSizeBytes);
+            return TF_OK;
+        };
+        int rc;
+        if ((rc = allow((const void*)k_broadphase)) != TF_OK) { return rc; }
+        if ((rc = allow((const void*)k_substep)) != TF_OK) { return rc; }
+        if ((rc = allow((const void*)k_prepare)) != TF_OK) { return rc; }
+        if ((rc = allow((const void*)k_finish)) != TF_OK) { return rc; }
         done = true;
+        return TF_OK;
+    }
+
+    // Default launch shapes: batches of few worlds give every world a whole CTA (512 threads when a world
+    // has more than 512 bodies); batches of many worlds give worlds of up to 96 bodies a warp each and the
+    // larger ones the CTA. 64 KB of staging per CTA leaves room for three CTAs on an SM.
+    LaunchShape defaultShape(int k) const {
+        LaunchShape s;
+        const bool many = worlds.size() >= (size_t)smCount * 4;
+        s.threads = !many && maxWorldBodies > 512 ? 512u : 256u;
+        s.bigBodies = many ? 96u : 0u;
+        const bool stages = k == 0 || k == 3 || k == 5 || k == 6;
+        s.smemBytes = stages ? 64u * 1024u : 0u;
+        return s;
+    }
+
+    // Bodies (and active contacts) one staging slice of `bytes` holds, for the kernels that stage.
+    static StageSizes stageFor(int k, uint32_t bytes) {
+        StageSizes st{ 0, 0 };
+        switch (k) {
+            case 0:  // broadphase: a PairBody per body
+                st.bodies = bytes / (uint32_t)sizeof(PairBody);
+                break;
+            case 3:  // prepare: a color mask per body, two endpoints per active contact, ~3 contacts per body
+                st.bodies = bytes > 512 ? (bytes - 512) / 28 : 0;
+                st.contacts = 3 * st.bodies + 64;
+                break;
+            case 5:  // substep: the solver state of each body
+                st.bodies = bytes / (uint32_t)(kSBodyWords * sizeof(float));
+                break;
+            case 6:  // finish: parent and island time per body, a union pair per contact
+                st.bodies = bytes > 512 ? (bytes - 512) / 32 : 0;
+                st.contacts = 3 * st.bodies + 64;
+                break;
+            default:
+                break;
+        }
+        if (st.contacts == 64 && st.bodies == 0) { st.contacts = 0; }
+        return st;
+    }
+
+    // Turns the launch shapes into kernel arguments and grid sizes for the current layout.
+    int configureLaunches() {
+        int rc = configureKernels();
+        if (rc != TF_OK) { return rc; }
+        const void* fns[kKernels] = { (const void*)k_broadphase, (const void*)k_narrowphase, (const void*)k_wake,
+                                      (const void*)k_prepare,    (const void*)k_refresh,     (const void*)k_substep,
+                                      (const void*)k_finish };
+        for (int k = 0; k < kKernels; ++k) {
+            LaunchShape& sh = shapes[k];
+            if (!sh.chosen) { sh = defaultShape(k); }
+            const uint32_t warps = sh.threads / 32;
+            auto lim = dynSmemLimit.find(fns[k]);
+            const uint32_t limit = lim == dynSmemLimit.end() ? 0u : (uint32_t)lim->second;
+            const uint32_t bytes = std::min(sh.smemBytes, limit) / (16 * warps) * (16 * warps);
+            Split& sp = splits[k];
+            sp.bigBodies = sh.bigBodies;
+            sp.smemBytes = bytes;
+            sp.big = stageFor(k, bytes);
+            sp.small = stageFor(k, bytes / warps);
+            int perSm = 0;
+            TF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, fns[k], (int)sh.threads, bytes));
+            if (perSm < 1) { return fail(TF_E_INVALID, "launch shape does not fit on an SM"); }
+            const size_t big = (size_t)(std::upper_bound(sortedSizes.begin(), sortedSizes.end(), sh.bigBodies,
+                                                         std::greater<uint32_t>()) -
+                                        sortedSizes.begin());
+            const size_t needed = big + (sortedSizes.size() - big + warps - 1) / warps;
+            grids[k] = (int)std::max<size_t>(1, std::min<size_t>(needed, (size_t)smCount * perSm));
+        }
+        return TF_OK;
+    }
+
+    // Chooses how a kernel (or every kernel, k < 0) is launched; takes effect at the next step.
+    int setLaunch(int k, uint32_t threads, uint32_t bigBodies, uint32_t smemBytes) {
+        if (k >= kKernels || threads < 32 || threads > (uint32_t)kMaxBlock || threads % 32 != 0) {
+            return fail(TF_E_INVALID, "launch shape: kernel index or thread count out of range");
+        }
+        for (int i = 0; i < kKernels; ++i) {
+            if (k >= 0 && i != k) { continue; }
+            shapes[i] = LaunchShape{ threads, bigBodies, smemBytes, true };
+        }
+        dropGraphs();
+        if (laidOut) { return configureLaunches(); }
+        return TF_OK;
+    }
+
+    int getLaunch(int k, uint32_t* out) const {
+        if (k < 0 || k >= kKernels) { return TF_E_INVALID; }
+        out[0] = shapes[k].threads;
+        out[1] = shapes[k].bigBodies;
+        out[2] = splits[k].smemBytes;
+        out[3] = (uint32_t)grids[k];
+        out[4] = splits[k].big.bodies;
+        out[5] = splits[k].small.bodies;
         return TF_OK;
     }
 
@@ -855,14 +976,10 @@ public:
     // the completed steps left.
     int growAfterAbort() {
         if (std::getenv("TWOFOLD_B200_TRACE")) { std::fprintf(stderr, "twofold_b200: list overflow, growing and laying out again\n"); }
-        sortLimitHit = false;
         hostFresh = false;
         onDevice = true;
         int rc = pull();
         if (rc != TF_OK) { return rc; }
-        if (sortLimitHit) {
-            return fail(TF_E_UNSUPPORTED, "a world has more candidate pairs than one block sorts (8192)");
-        }
         return layout();
     }
 
@@ -1410,6 +1527,21 @@ TF_API int tf_world_work_counts(void* h, int64_t out[6]) {
 TF_API int tf_world_launch_count(void* h, int64_t* launches) {
     if (!h || !launches) { return tfb::fail(TF_E_INVALID, "tf_world_launch_count: null"); }
     *launches = E(h)->launches;
+    return TF_OK;
+}
+
+TF_API int tf_world_set_launch(void* h, int32_t kernel, int32_t threads, int32_t big_bodies, int32_t smem_bytes) {
+    if (!h) { return tfb::fail(TF_E_INVALID, "tf_world_set_launch: null"); }
+    if (big_bodies < 0 || smem_bytes < 0) { return tfb::fail(TF_E_INVALID, "tf_world_set_launch: negative size"); }
+    Engine* e = E(h);
+    if (cudaSetDevice(e->device) != cudaSuccess) { return tfb::fail(TF_E_CUDA, "tf_world_set_launch: cudaSetDevice"); }
+    return e->setLaunch(kernel, (uint32_t)threads, (uint32_t)big_bodies, (uint32_t)smem_bytes);
+}
+
+TF_API int tf_world_get_launch(void* h, int32_t kernel, uint32_t out[6]) {
+    if (!h || !out) { return tfb::fail(TF_E_INVALID, "tf_world_get_launch: null"); }
+    const int rc = E(h)->getLaunch(kernel, out);
+    if (rc != TF_OK) { return tfb::fail(rc, "tf_world_get_launch: bad kernel index"); }
     return TF_OK;
 }
 

@@ -1,15 +1,18 @@
-// The step kernels. Each kernel processes whole worlds: CTA k takes worlds order[k], order[k + gridDim.x],
-// ... (largest first), and within a world its threads split bodies, candidates or one color's contacts,
-// with __syncthreads() between dependent phases. Work that the reference does in one sequential pass
-// whose result depends on order (graph coloring, union-find islands, the wake flood and contacts solved
-// one at a time) runs on the world's first thread, in the reference's order.
+// The step kernels. Each kernel walks whole worlds with thread groups: a group (one warp, or 64 to 512
+// threads) steps one world at a time, and groups take worlds in largest-first order from a per-launch
+// counter, so small worlds pack many to an SM and large ones get whole CTAs. Within a world a group's threads
+// split bodies, candidates or one color's contacts, with a group barrier between dependent phases. Work that
+// the reference does in one sequential pass whose result depends on order (graph coloring, union-find unions,
+// the wake flood and contacts solved one at a time) runs on the group's first thread, in the reference's
+// order, over shared memory when the world fits the group's slice and over L1/L2-cached scratch otherwise.
 //
 // Kernel sequence of one step (src/world.cpp:1564-1727):
-//   k_broadphase   growth, body-pair and half-space candidates, sort + unique   (world.cpp:752-870)
+//   k_broadphase   growth, body-pair and half-space candidates, sorted unique keys (world.cpp:752-870)
 //   k_narrowphase  reuse or collide each candidate, carry impulses, merge       (world.cpp:872-993)
 //   k_wake         wake sleeping bodies touched by moving ones                  (world.cpp:705-735)
-//   k_prepare      step state, active/fast/impact lists, prepare, coloring     (world.cpp:1589-1657)
-//   k_substep x n  refresh, integrate, warm start, solve, integrate, relax      (world.cpp:1658-1681)
+//   k_prepare      step state, active/fast/impact lists, prepare, axes, colors   (world.cpp:1589-1657)
+//   k_refresh      fast pairs collided again before substeps 2..n               (world.cpp:1658-1668)
+//   k_substep      integrate, warm start, solve, integrate, relax               (world.cpp:1669-1680)
 //   k_finish       restitution, limits, refit bounds, sweep test, sleep         (world.cpp:1682-1726)
 #pragma once
 
@@ -19,50 +22,155 @@
 namespace tfb {
 
 constexpr int kMaxBlock = 512;
+constexpr int kMaxGroups = kMaxBlock / 32;
 constexpr uint32_t kDevPairOverflow = 1u << 0, kDevContactOverflow = 1u << 1, kDevNonFinite = 1u << 2,
                    kDevUnsupported = 1u << 4, kDevSweepSkipped = 1u << 5, kDevListOverflow = 1u << 6;
 
-// Exclusive prefix sum over the block. Every thread calls it; blockDim.x is a multiple of 32.
-__device__ __forceinline__ uint32_t blockExclusiveScan(uint32_t v, uint32_t& total) {
-    __shared__ uint32_t warpSums[kMaxBlock / 32];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+// Where each launch of a step takes its worlds from (one counter each, zeroed when the step starts).
+// Up to kMaxSubsteps substeps per step.
+constexpr int kMaxSubsteps = 32;
+enum WorkSlot : int {
+    kSlotBroad = 0, kSlotNarrow = 1, kSlotWake = 2, kSlotPrepare = 3,
+    kSlotRefresh = 4,                            // + substep index
+    kSlotSubstep = kSlotRefresh + kMaxSubsteps,  // + substep index
+    kSlotFinish = kSlotSubstep + kMaxSubsteps,
+    kSlotCount = kSlotFinish + 1
+};
+
+// A group of threads that steps one world at a time: one warp, several warps, or the whole CTA.
+struct Group {
+    uint32_t tid, size, id, count, lane, warp, warps;
+
+    __device__ __forceinline__ void sync() const {
+        if (count == 1) {
+            __syncthreads();
+        } else if (size == 32) {
+            __syncwarp();
+        } else {
+            asm volatile("bar.sync %0, %1;" ::"r"(id + 1), "r"(size) : "memory");
+        }
+    }
+};
+
+// blockDim.x is a multiple of size, size a multiple of 32, at most kMaxGroups groups.
+__device__ __forceinline__ Group makeGroup(uint32_t size) {
+    Group g;
+    g.size = size;
+    g.count = blockDim.x / size;
+    g.id = threadIdx.x / size;
+    g.tid = threadIdx.x % size;
+    g.lane = threadIdx.x & 31;
+    g.warp = g.tid >> 5;
+    g.warps = size >> 5;
+    return g;
+}
+
+// How a launch hands out worlds. A CTA takes worlds in largest-first order (B.order) and steps a world with
+// more than bigBodies bodies with all its threads; once it draws a world at or under that size every later
+// world is too, and its warps go on alone, a world each. Each mode has its own shared-memory staging
+// capacity: the whole dynamic allocation for a CTA-sized group, an equal share per warp otherwise.
+struct StageSizes {
+    uint32_t bodies, contacts;
+};
+struct Split {
+    uint32_t bigBodies;
+    StageSizes big, small;
+    uint32_t smemBytes;
+};
+
+__device__ __forceinline__ uint32_t grabWarp(uint32_t* counter) {
+    uint32_t v = 0;
+    if ((threadIdx.x & 31) == 0) { v = atomicAdd(counter, 1u); }
+    return __shfl_sync(0xffffffffu, v, 0);
+}
+
+// Calls body(group, world, slice, stage sizes) for every world of the batch, each exactly once.
+template <class Body>
+__device__ void forWorlds(const Batch& B, int slotIndex, const Split& sp, unsigned char* smem, Body&& body) {
+    __shared__ uint32_t s_world, s_big;
+    const uint32_t nw = (uint32_t)B.nWorlds;
+    uint32_t* counter = B.work + slotIndex;
+    const Group cta = makeGroup(blockDim.x);
+    for (;;) {
+        if (threadIdx.x == 0) {
+            const uint32_t o = atomicAdd(counter, 1u);
+            s_world = o;
+            s_big = (o < nw && B.info[B.order[o]].bodyCount > sp.bigBodies) ? 1u : 0u;
+        }
+        __syncthreads();
+        const uint32_t o = s_world, big = s_big;
+        __syncthreads();
+        if (o >= nw) { return; }
+        if (big) {
+            body(cta, B.order[o], smem, sp.big);
+            continue;
+        }
+        const Group wg = makeGroup(32);
+        unsigned char* slice = smem + (size_t)wg.id * (sp.smemBytes / wg.count);
+        uint32_t mine = wg.id == 0 ? o : grabWarp(counter);
+        while (mine < nw) {
+            body(wg, B.order[mine], slice, sp.small);
+            mine = grabWarp(counter);
+        }
+        return;
+    }
+}
+
+// Exclusive prefix sum over the group; every thread of the group calls it.
+__device__ __forceinline__ uint32_t groupScan(const Group& g, uint32_t v, uint32_t& total) {
+    __shared__ uint32_t sums[kMaxGroups][kMaxBlock / 32];
     uint32_t x = v;
     for (int o = 1; o < 32; o <<= 1) {
         const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-        if (lane >= o) { x += y; }
+        if ((int)g.lane >= o) { x += y; }
     }
-    if (lane == 31) { warpSums[warp] = x; }
-    __syncthreads();
-    if (warp == 0) {
-        uint32_t s = lane < nw ? warpSums[lane] : 0u;
+    if (g.warps == 1) {
+        total = __shfl_sync(0xffffffffu, x, 31);
+        return x - v;
+    }
+    if (g.lane == 31) { sums[g.id][g.warp] = x; }
+    g.sync();
+    if (g.warp == 0) {
+        uint32_t s = g.lane < g.warps ? sums[g.id][g.lane] : 0u;
         for (int o = 1; o < 32; o <<= 1) {
             const uint32_t y = __shfl_up_sync(0xffffffffu, s, o);
-            if (lane >= o) { s += y; }
+            if ((int)g.lane >= o) { s += y; }
         }
-        if (lane < nw) { warpSums[lane] = s; }
+        if (g.lane < g.warps) { sums[g.id][g.lane] = s; }
     }
-    __syncthreads();
-    const uint32_t prefix = (warp > 0 ? warpSums[warp - 1] : 0u) + x - v;
-    total = warpSums[nw - 1];
-    __syncthreads();
+    g.sync();
+    const uint32_t prefix = (g.warp > 0 ? sums[g.id][g.warp - 1] : 0u) + x - v;
+    total = sums[g.id][g.warps - 1];
+    g.sync();
     return prefix;
 }
 
 // Calls emit(i, position) for every i < n where pred(i) holds, positions dense and in index order. Ends with
-// a block barrier, so everything emit wrote is visible to every thread on return.
+// a group barrier, so everything emit wrote is visible to the whole group on return.
 template <class Pred, class Emit>
-__device__ uint32_t blockCompact(uint32_t n, Pred pred, Emit emit) {
+__device__ uint32_t groupCompact(const Group& g, uint32_t n, Pred pred, Emit emit) {
     uint32_t base = 0;
-    for (uint32_t start = 0; start < n; start += blockDim.x) {
-        const uint32_t i = start + threadIdx.x;
+    for (uint32_t start = 0; start < n; start += g.size) {
+        const uint32_t i = start + g.tid;
         const bool f = i < n && pred(i);
         uint32_t tot;
-        const uint32_t pos = blockExclusiveScan(f ? 1u : 0u, tot);
+        const uint32_t pos = groupScan(g, f ? 1u : 0u, tot);
         if (f) { emit(i, base + pos); }
         base += tot;
     }
-    __syncthreads();
+    g.sync();
     return base;
+}
+
+// Reads the abort word once per CTA at a kernel's start: true when an earlier step of this launch sequence
+// overflowed a list, or this step did in an earlier kernel.
+__device__ __forceinline__ bool stepAborted(const Batch& B, int serial) {
+    __shared__ int s_skip;
+    if (threadIdx.x == 0) { s_skip = *(volatile uint32_t*)B.abortStep <= (uint32_t)serial; }
+    __syncthreads();
+    const bool skip = s_skip != 0;
+    __syncthreads();
+    return skip;
 }
 
 __device__ __forceinline__ uint64_t pairKey(uint32_t a, uint32_t b) {
@@ -76,7 +184,6 @@ __device__ __forceinline__ void emitCandidate(const Batch& B, const WorldInfo& w
 
 // ---------------------------------------------------------------------------------------------------------
 // Broadphase (src/world.cpp:752-870).
-
 // A half-space against one body's shapes (src/world.cpp:844-867).
 __device__ void pairPlane(const Batch& B, const WorldInfo& wi, uint32_t gp, uint32_t gb, uint32_t* count) {
     const DShape& sp = B.shapes[gp];
@@ -110,46 +217,6 @@ __device__ void pairPlane(const Batch& B, const WorldInfo& wi, uint32_t gp, uint
     }
 }
 
-// Sorts keys[0, n) ascending in shared memory and removes repeats; returns the unique count written back to
-// out[0, unique).
-__device__ uint32_t sortUnique(uint64_t* s, uint32_t n, uint64_t* out) {
-    uint32_t p = 1;
-    while (p < n) { p <<= 1; }
-    for (uint32_t i = n + threadIdx.x; i < p; i += blockDim.x) { s[i] = ~0ull; }
-    __syncthreads();
-    for (uint32_t k = 2; k <= p; k <<= 1) {
-        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
-            for (uint32_t i = threadIdx.x; i < p; i += blockDim.x) {
-                const uint32_t ixj = i ^ j;
-                if (ixj > i) {
-                    const uint64_t a = s[i], b = s[ixj];
-                    const bool up = (i & k) == 0;
-                    if ((a > b) == up) {
-                        s[i] = b;
-                        s[ixj] = a;
-                    }
-                }
-            }
-            __syncthreads();
-        }
-    }
-    const uint32_t unique = blockCompact(
-        n, [&](uint32_t i) { return i == 0 || s[i] != s[i - 1]; }, [&](uint32_t i, uint32_t pos) { out[pos] = s[i]; });
-    __syncthreads();
-    return unique;
-}
-
-// Reads the abort word once per CTA: true when an earlier step of this launch sequence overflowed a list,
-// or this step did in an earlier kernel.
-__device__ __forceinline__ bool stepAborted(const Batch& B, int serial) {
-    __shared__ int s_skip;
-    if (threadIdx.x == 0) { s_skip = *(volatile uint32_t*)B.abortStep <= (uint32_t)serial; }
-    __syncthreads();
-    const bool skip = s_skip != 0;
-    __syncthreads();
-    return skip;
-}
-
 // The shapes of two bodies whose grown bounds overlap, paired by their own grown bounds
 // (src/world.cpp:819-842).
 __device__ void pairShapes(const Batch& B, const WorldInfo& wi, const DBody& ba, const DBody& bb, float gA, float gB,
@@ -174,8 +241,6 @@ __device__ void pairShapes(const Batch& B, const WorldInfo& wi, const DBody& ba,
 
 constexpr uint32_t kBodyLive = 1u, kBodyDynamic = 2u, kBodyMoving = 4u;
 // Largest worlds whose bodies the broadphase and the substep stage in shared memory.
-constexpr uint32_t kBroadStage = 2048;
-constexpr uint32_t kSolveStage = 1400;
 
 // A body as the pair test sees it: bounds, growth and the three flags above.
 struct PairBody {
@@ -195,84 +260,125 @@ __device__ __forceinline__ PairBody pairBodyOf(const Batch& B, uint32_t g) {
     return p;
 }
 
+// Sorts the world's count keys (minShape << 32 | maxShape, at B.cand) ascending and removes repeats: a
+// counting sort by the first shape, then each row sorted on its own (rows are short), then compaction back
+// into B.cand. Returns the unique count.
+__device__ uint32_t sortKeys(const Group& g, const Batch& B, const WorldInfo& wi, uint32_t count) {
+    uint32_t* row = B.rowScratch + wi.shapeFirst;
+    uint64_t* tmp = B.mergeKeyA + wi.contactFirst;
+    uint64_t* keys = B.cand + wi.candFirst;
+    const uint32_t rows = wi.shapeCount;
+    for (uint32_t r = g.tid; r < rows; r += g.size) { row[r] = 0; }
+    g.sync();
+    for (uint32_t i = g.tid; i < count; i += g.size) { atomicAdd(&row[(uint32_t)(keys[i] >> 32)], 1u); }
+    g.sync();
+    uint32_t base = 0;
+    for (uint32_t start = 0; start < rows; start += g.size) {
+        const uint32_t r = start + g.tid;
+        const uint32_t v = r < rows ? row[r] : 0u;
+        uint32_t tot;
+        const uint32_t pre = groupScan(g, v, tot);
+        if (r < rows) { row[r] = base + pre; }
+        base += tot;
+    }
+    g.sync();
+    // Scattering advances each row's start to its end.
+    for (uint32_t i = g.tid; i < count; i += g.size) {
+        const uint64_t k = keys[i];
+        tmp[atomicAdd(&row[(uint32_t)(k >> 32)], 1u)] = k;
+    }
+    g.sync();
+    for (uint32_t r = g.tid; r < rows; r += g.size) {
+        const uint32_t s = r > 0 ? row[r - 1] : 0u, e = row[r];
+        for (uint32_t i = s + 1; i < e; ++i) {
+            const uint64_t k = tmp[i];
+            uint32_t j = i;
+            while (j > s && tmp[j - 1] > k) {
+                tmp[j] = tmp[j - 1];
+                --j;
+            }
+            tmp[j] = k;
+        }
+    }
+    g.sync();
+    return groupCompact(
+        g, count, [&](uint32_t i) { return i == 0 || tmp[i] != tmp[i - 1]; }, [&](uint32_t i, uint32_t pos) { keys[pos] = tmp[i]; });
+}
+
 // Body pairs whose grown bounds overlap, then their shapes (src/world.cpp:788-842), and half-space pairs
-// (:844-867); the keys are sorted and made unique (:868-869). Bodies and growths are staged in shared
-// memory for worlds of up to stageN bodies; a warp takes one body and its lanes the bodies after it.
-__global__ void __launch_bounds__(kMaxBlock) k_broadphase(Batch B, StepParams P, uint32_t sortCap, uint32_t stageN,
-                                                          int serial) {
-    extern __shared__ __align__(16) uint64_t s_keys[];
-    __shared__ uint32_t s_count;
-    PairBody* staged = reinterpret_cast<PairBody*>(s_keys + sortCap);
+// (:844-867); the keys are sorted and made unique (:868-869). A warp of the group takes one body and its
+// lanes the bodies after it. Bodies are staged in the group's shared slice when at most stageN of them.
+__global__ void __launch_bounds__(kMaxBlock) k_broadphase(Batch B, StepParams P, Split sp, int serial) {
+    extern __shared__ __align__(16) unsigned char s_raw[];
+    __shared__ uint32_t s_count[kMaxGroups];
     if (stepAborted(B, serial)) { return; }
-    for (int o = blockIdx.x; o < B.nWorlds; o += gridDim.x) {
-        const uint32_t w = B.order[o];
+    forWorlds(B, kSlotBroad, sp, s_raw, [&](const Group& g, uint32_t w, unsigned char* slice, const StageSizes& ss) {
+        PairBody* staged = reinterpret_cast<PairBody*>(slice);
+        const uint32_t stageN = ss.bodies;
         const WorldInfo wi = B.info[w];
         WorldCounts& wc = B.counts[w];
         const uint32_t n = wi.bodyCount;
         const bool useStage = n <= stageN;
-        if (threadIdx.x == 0) { s_count = 0; }
+        if (g.tid == 0) { s_count[g.id] = 0; }
         // Growth by the speculative distance and the travel over the step (src/world.cpp:754-765).
-        for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+        for (uint32_t i = g.tid; i < n; i += g.size) {
             const DBody& b = B.bodies[wi.bodyFirst + i];
-            float g = P.tol.speculative;
+            float gr = P.tol.speculative;
             if (b.alive && b.type != kStatic && !(lengthSquared(b.v) == 0.0f && lengthSquared(b.w) == 0.0f)) {
-                g += (length(b.v) + length(b.w) * b.extent) * P.dt;
+                gr += (length(b.v) + length(b.w) * b.extent) * P.dt;
             }
-            B.grow[wi.bodyFirst + i] = g;
+            B.grow[wi.bodyFirst + i] = gr;
             if (useStage) {
                 PairBody p;
                 p.lo = b.lo;
                 p.hi = b.hi;
-                p.grow = g;
+                p.grow = gr;
                 p.flags = ((b.alive && b.hasBounds) ? kBodyLive : 0u) | (b.type == kDynamic ? kBodyDynamic : 0u) |
                           (movingAwake(b) ? kBodyMoving : 0u);
                 staged[i] = p;
             }
         }
-        __syncthreads();
-        const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
-        for (uint32_t a = warp; a + 1 < n; a += warps) {
+        g.sync();
+        uint32_t* count = &s_count[g.id];
+        for (uint32_t a = g.warp; a + 1 < n; a += g.warps) {
             const PairBody A = useStage ? staged[a] : pairBodyOf(B, wi.bodyFirst + a);
             if (!(A.flags & kBodyLive)) { continue; }
-            for (uint32_t b = a + 1 + lane; b < n; b += 32) {
+            for (uint32_t b = a + 1 + g.lane; b < n; b += 32) {
                 const PairBody Bb = useStage ? staged[b] : pairBodyOf(B, wi.bodyFirst + b);
                 if (!(Bb.flags & kBodyLive)) { continue; }
                 if (!((A.flags | Bb.flags) & kBodyDynamic)) { continue; }
                 if (!((A.flags | Bb.flags) & kBodyMoving)) { continue; }
-                const float g = A.grow + Bb.grow;
-                const Vec3 reach{ g, g, g };
+                const float gg = A.grow + Bb.grow;
+                const Vec3 reach{ gg, gg, gg };
                 if (!boxesOverlap(A.lo - reach, A.hi + reach, Bb.lo, Bb.hi)) { continue; }
                 pairShapes(B, wi, B.bodies[wi.bodyFirst + a], B.bodies[wi.bodyFirst + b], A.grow, Bb.grow, A.lo, A.hi,
-                           Bb.lo, Bb.hi, reach, &s_count);
+                           Bb.lo, Bb.hi, reach, count);
             }
         }
         for (uint32_t pl = 0; pl < wi.planeCount; ++pl) {
             const uint32_t gp = B.planeList[wi.planeFirst + pl];
-            for (uint32_t b = threadIdx.x; b < n; b += blockDim.x) { pairPlane(B, wi, gp, wi.bodyFirst + b, &s_count); }
+            for (uint32_t b = g.tid; b < n; b += g.size) { pairPlane(B, wi, gp, wi.bodyFirst + b, count); }
         }
-        __syncthreads();
-        const uint32_t count = s_count;
-        if (count > wi.candCap || count > sortCap) {
+        g.sync();
+        const uint32_t total = *count;
+        if (total > wi.candCap) {
             // The list did not fit: this step stops here and the host grows the world's lists.
-            if (threadIdx.x == 0) {
-                wc.flags |= count > wi.candCap ? kDevPairOverflow : kDevUnsupported;
-                wc.candNeeded = max(wc.candNeeded, count);
+            if (g.tid == 0) {
+                wc.flags |= kDevPairOverflow;
+                wc.candNeeded = max(wc.candNeeded, total);
                 atomicMin(B.abortStep, (uint32_t)serial);
             }
-            __syncthreads();
-            continue;
+            g.sync();
+            return;
         }
-        for (uint32_t i = threadIdx.x; i < count; i += blockDim.x) { s_keys[i] = B.cand[wi.candFirst + i]; }
-        __syncthreads();
-        const uint32_t unique = sortUnique(s_keys, count, B.cand + wi.candFirst);
-        if (threadIdx.x == 0) {
+        const uint32_t unique = sortKeys(g, B, wi, total);
+        if (g.tid == 0) {
             wc.candCount = unique;
-            wc.candNeeded = max(wc.candNeeded, count);
+            wc.candNeeded = max(wc.candNeeded, total);
         }
-        __syncthreads();
-    }
+        g.sync();
+    });
 }
-
 // ---------------------------------------------------------------------------------------------------------
 // Narrowphase and contact bookkeeping (src/world.cpp:872-1025).
 
@@ -488,20 +594,19 @@ __device__ __forceinline__ bool keyLess(uint64_t ka, uint32_t pa, uint64_t kb, u
     return ka != kb ? ka < kb : pa < pb;
 }
 
-__global__ void __launch_bounds__(kMaxBlock) k_narrowphase(Batch B, StepParams P, int serial) {
+__global__ void __launch_bounds__(kMaxBlock) k_narrowphase(Batch B, StepParams P, Split sp, int serial) {
     if (stepAborted(B, serial)) { return; }
-    for (int o = blockIdx.x; o < B.nWorlds; o += gridDim.x) {
-        const uint32_t w = B.order[o];
+    forWorlds(B, kSlotNarrow, sp, nullptr, [&](const Group& g, uint32_t w, unsigned char*, const StageSizes&) {
         const WorldInfo wi = B.info[w];
         WorldCounts& wc = B.counts[w];
         const uint32_t nc = wc.candCount;
         const uint32_t oldCount = wc.contactCount;
         const DContact* old = B.previous + wi.contactFirst;
-        for (uint32_t i = threadIdx.x; i < nc; i += blockDim.x) { narrowOne(B, P, wi, wc, i, old, oldCount); }
-        __syncthreads();
+        for (uint32_t i = g.tid; i < nc; i += g.size) { narrowOne(B, P, wi, wc, i, old, oldCount); }
+        g.sync();
         const uint32_t cf = wi.contactFirst;
-        const uint32_t nC = blockCompact(
-            nc, [&](uint32_t i) { return B.stageUsed[wi.candFirst + i] != 0; },
+        const uint32_t nC = groupCompact(
+            g, nc, [&](uint32_t i) { return B.stageUsed[wi.candFirst + i] != 0; },
             [&](uint32_t i, uint32_t pos) {
                 const DContact& c = B.stage[wi.candFirst + i];
                 B.mergeKeyA[cf + pos] = c.key;
@@ -510,8 +615,8 @@ __global__ void __launch_bounds__(kMaxBlock) k_narrowphase(Batch B, StepParams P
             });
         // Contacts of pairs where nothing moves and one body is dynamic (asleep) stay as they were
         // (src/world.cpp:961-988).
-        const uint32_t nK = blockCompact(
-            oldCount,
+        const uint32_t nK = groupCompact(
+            g, oldCount,
             [&](uint32_t j) {
                 const DContact& c = old[j];
                 if (!TF_OK_INDEX(B, c.bodyA - wi.bodyFirst < wi.bodyCount && c.bodyB - wi.bodyFirst < wi.bodyCount, 4,
@@ -528,19 +633,18 @@ __global__ void __launch_bounds__(kMaxBlock) k_narrowphase(Batch B, StepParams P
                 B.mergePartB[cf + pos] = old[j].part;
                 B.mergeIdxB[cf + pos] = j;
             });
-        __syncthreads();
         const uint32_t total = nC + nK;
         if (total > wi.contactCap) {
-            if (threadIdx.x == 0) {
+            if (g.tid == 0) {
                 wc.flags |= kDevContactOverflow;
                 wc.contactNeeded = max(wc.contactNeeded, total);
                 atomicMin(B.abortStep, (uint32_t)serial);
             }
-            __syncthreads();
-            continue;
+            g.sync();
+            return;
         }
         // Stable merge by (key, part): collided contacts first among equals, as std::inplace_merge keeps them.
-        for (uint32_t x = threadIdx.x; x < nC; x += blockDim.x) {
+        for (uint32_t x = g.tid; x < nC; x += g.size) {
             const uint64_t k = B.mergeKeyA[cf + x];
             const uint32_t p = B.mergePartA[cf + x];
             uint32_t l = 0, h = nK;
@@ -554,7 +658,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_narrowphase(Batch B, StepParams P
             }
             B.contacts[cf + x + l] = B.stage[wi.candFirst + B.mergeIdxA[cf + x]];
         }
-        for (uint32_t y = threadIdx.x; y < nK; y += blockDim.x) {
+        for (uint32_t y = g.tid; y < nK; y += g.size) {
             const uint64_t k = B.mergeKeyB[cf + y];
             const uint32_t p = B.mergePartB[cf + y];
             uint32_t l = 0, h = nC;
@@ -568,55 +672,54 @@ __global__ void __launch_bounds__(kMaxBlock) k_narrowphase(Batch B, StepParams P
             }
             B.contacts[cf + y + l] = old[B.mergeIdxB[cf + y]];
         }
-        __syncthreads();
-        if (threadIdx.x == 0) {
+        g.sync();
+        if (g.tid == 0) {
             wc.nextContactCount = total;
             wc.contactNeeded = max(wc.contactNeeded, total);
         }
-        __syncthreads();
-    }
+        g.sync();
+    });
 }
 
 // ---------------------------------------------------------------------------------------------------------
 // Waking (src/world.cpp:705-735): sleeping bodies a moving body reached wake, and so does everything linked
-// to them by a contact with points. Runs on the world's first thread; it is rare.
+// to them by a contact with points. Runs on the group's first thread; it is rare.
 
-__global__ void k_wake(Batch B, int serial) {
+__global__ void __launch_bounds__(kMaxBlock) k_wake(Batch B, Split sp, int serial) {
     if (stepAborted(B, serial)) { return; }
-    if (threadIdx.x != 0) { return; }
-    for (int o = blockIdx.x; o < B.nWorlds; o += gridDim.x) {
-        const uint32_t w = B.order[o];
+    forWorlds(B, kSlotWake, sp, nullptr, [&](const Group& g, uint32_t w, unsigned char*, const StageSizes&) {
+        if (g.tid != 0) { return; }
         const WorldInfo wi = B.info[w];
         WorldCounts& wc = B.counts[w];
-        if (!wc.wakePending) { continue; }
+        if (!wc.wakePending) { return; }
         wc.wakePending = 0;
         uint32_t* stack = B.unionParent + wi.bodyFirst;
         uint32_t top = 0;
         for (uint32_t i = 0; i < wi.bodyCount; ++i) {
-            const uint32_t g = wi.bodyFirst + i;
-            if (!B.wakeMark[g]) { continue; }
-            const DBody& b = B.bodies[g];
+            const uint32_t gb = wi.bodyFirst + i;
+            if (!B.wakeMark[gb]) { continue; }
+            const DBody& b = B.bodies[gb];
             if (b.alive && b.type == kDynamic && !b.awake && top < wi.bodyCount) {
-                stack[top++] = g;
+                stack[top++] = gb;
             } else {
-                B.wakeMark[g] = 0;
+                B.wakeMark[gb] = 0;
             }
         }
         const DContact* cs = B.contacts + wi.contactFirst;
         const uint32_t nc = wc.nextContactCount;
         while (top > 0) {
-            const uint32_t g = stack[--top];
-            DBody& b = B.bodies[g];
-            B.wakeMark[g] = 0;
+            const uint32_t gb = stack[--top];
+            DBody& b = B.bodies[gb];
+            B.wakeMark[gb] = 0;
             if (b.awake) { continue; }
             b.awake = 1;
             b.sleepTime = 0.0f;
             updateInverseMass(b);
             for (uint32_t ci = 0; ci < nc; ++ci) {
                 const DContact& c = cs[ci];
-                if (c.bodyA != g && c.bodyB != g) { continue; }
+                if (c.bodyA != gb && c.bodyB != gb) { continue; }
                 if (ci > 0 && cs[ci - 1].key == c.key) { continue; }  // one link per pair
-                const uint32_t other = c.bodyA == g ? c.bodyB : c.bodyA;
+                const uint32_t other = c.bodyA == gb ? c.bodyB : c.bodyA;
                 const DBody& ob = B.bodies[other];
                 if (ob.type != kDynamic || ob.awake || B.wakeMark[other]) { continue; }
                 bool linked = false;
@@ -627,26 +730,25 @@ __global__ void k_wake(Batch B, int serial) {
                 }
             }
         }
-    }
+    });
 }
 
 // ---------------------------------------------------------------------------------------------------------
 // Step state, lists, preparation and coloring (src/world.cpp:1589-1657, src/lanes.cpp:356-407).
 
-// Shared-memory staging of a world's coloring and islands, sized per batch by the host (at most these).
-// Larger worlds run the same code on global scratch.
-constexpr uint32_t kStageBodies = 4096;
-constexpr uint32_t kStageContacts = 8192;
-constexpr uint32_t kNone = 0xffffffffu;
+constexpr uint32_t kNone = 0x7fffffffu;
+constexpr uint32_t kNotColorable = 0x80000000u;
 
 // Greedy lowest free color of 32 over the moving bodies, in list order (src/lanes.cpp:356-374). endA/endB
-// hold each contact's moving bodies (kNone for one that does not move) or kNone in both with colorable 0.
-__device__ void colorSequential(uint32_t n, const uint32_t* endA, const uint32_t* endB, const uint8_t* colorable,
-                                uint32_t* masks, uint8_t* color) {
+// hold each contact's moving bodies (kNone for one that does not move); endA carries kNotColorable for a
+// planar or rolling contact, which takes no color.
+__device__ void colorSequential(uint32_t n, const uint32_t* endA, const uint32_t* endB, uint32_t* masks,
+                                uint8_t* color) {
     for (uint32_t x = 0; x < n; ++x) {
         uint8_t k = kNoColor;
-        if (colorable[x]) {
-            const uint32_t a = endA[x], b = endB[x];
+        const uint32_t ea = endA[x];
+        if (!(ea & kNotColorable)) {
+            const uint32_t a = ea, b = endB[x];
             const uint32_t taken = (a != kNone ? masks[a] : 0u) | (b != kNone ? masks[b] : 0u);
             if (taken != 0xffffffffu) {
                 const int f = __ffs(~taken) - 1;
@@ -661,61 +763,65 @@ __device__ void colorSequential(uint32_t n, const uint32_t* endA, const uint32_t
 
 // Groups a contact list by color: every color's contacts (any order within a color, which solves the same)
 // into colored, colors in ascending order, the uncolored ones into rest in list order.
-__device__ void bucketByColor(uint32_t n, const uint32_t* list, const uint8_t* colorOf, uint32_t* colored,
+__device__ void bucketByColor(const Group& g, uint32_t n, const uint32_t* list, const uint8_t* colorOf, uint32_t* colored,
                               uint32_t* rest, uint32_t* startOut, uint32_t& colorsUsed, uint32_t& restCount) {
-    __shared__ uint32_t s_size[kColors + 1];
-    __shared__ uint32_t s_fill[kColors + 1];
-    for (uint32_t k = threadIdx.x; k <= kColors; k += blockDim.x) { s_size[k] = 0; }
-    __syncthreads();
-    for (uint32_t x = threadIdx.x; x < n; x += blockDim.x) { atomicAdd(&s_size[colorOf[list[x]]], 1u); }
-    __syncthreads();
-    if (threadIdx.x == 0) {
+    __shared__ uint32_t s_size[kMaxGroups][kColors + 1];
+    __shared__ uint32_t s_fill[kMaxGroups][kColors + 1];
+    uint32_t* size = s_size[g.id];
+    uint32_t* fill = s_fill[g.id];
+    for (uint32_t k = g.tid; k <= kColors; k += g.size) { size[k] = 0; }
+    g.sync();
+    for (uint32_t x = g.tid; x < n; x += g.size) { atomicAdd(&size[colorOf[list[x]]], 1u); }
+    g.sync();
+    if (g.tid == 0) {
         uint32_t sum = 0, used = 0;
         for (int k = 0; k <= kColors; ++k) {
             startOut[k] = sum;
-            s_fill[k] = sum;
-            sum += s_size[k];
-            if (k < kColors && s_size[k] > 0) { used = (uint32_t)k + 1; }
+            fill[k] = sum;
+            sum += size[k];
+            if (k < kColors && size[k] > 0) { used = (uint32_t)k + 1; }
         }
         colorsUsed = used;
     }
-    __syncthreads();
-    for (uint32_t x = threadIdx.x; x < n; x += blockDim.x) {
+    g.sync();
+    for (uint32_t x = g.tid; x < n; x += g.size) {
         const uint8_t k = colorOf[list[x]];
         if (k != kNoColor) {
-            const uint32_t at = atomicAdd(&s_fill[k], 1u);
+            const uint32_t at = atomicAdd(&fill[k], 1u);
 #if defined(TF_DEVICE_CHECKS)
             if (at >= n) { continue; }
 #endif
             colored[at] = list[x];
         }
     }
-    const uint32_t r = blockCompact(n, [&](uint32_t x) { return colorOf[list[x]] == kNoColor; },
+    const uint32_t r = groupCompact(g, n, [&](uint32_t x) { return colorOf[list[x]] == kNoColor; },
                                     [&](uint32_t x, uint32_t pos) { rest[pos] = list[x]; });
-    if (threadIdx.x == 0) { restCount = r; }
-    __syncthreads();
+    if (g.tid == 0) { restCount = r; }
+    g.sync();
 }
 
-__global__ void __launch_bounds__(kMaxBlock) k_prepare(Batch B, StepParams P, uint32_t stageBodies,
-                                                       uint32_t stageContacts, int serial) {
+// Coloring is staged in the group's shared slice (masks by body, endpoints by active contact) when the world
+// fits stageBodies bodies and stageContacts active contacts, else in the world's global scratch.
+__global__ void __launch_bounds__(kMaxBlock) k_prepare(Batch B, StepParams P, Split sp, int serial) {
     extern __shared__ __align__(16) unsigned char s_raw[];
-    __shared__ uint32_t s_fast, s_fastSolid;
+    __shared__ uint32_t s_fast[kMaxGroups], s_fastSolid[kMaxGroups], s_points[kMaxGroups];
     if (stepAborted(B, serial)) { return; }
-    for (int o = blockIdx.x; o < B.nWorlds; o += gridDim.x) {
-        const uint32_t w = B.order[o];
+    forWorlds(B, kSlotPrepare, sp, s_raw, [&](const Group& g, uint32_t w, unsigned char* slice, const StageSizes& ss) {
+        const uint32_t stageBodies = ss.bodies, stageContacts = ss.contacts;
         const WorldInfo wi = B.info[w];
         WorldCounts& wc = B.counts[w];
         uint32_t nc = wc.nextContactCount;
         if (!TF_OK_INDEX(B, nc <= wi.contactCap, 6, w, nc)) { nc = 0; }
-        if (threadIdx.x == 0) {
+        if (g.tid == 0) {
             wc.contactCount = nc;
-            s_fast = 0;
-            s_fastSolid = 0;
+            s_fast[g.id] = 0;
+            s_fastSolid[g.id] = 0;
+            s_points[g.id] = 0;
         }
-        for (uint32_t i = threadIdx.x; i < wi.bodyCount; i += blockDim.x) {
-            const uint32_t g = wi.bodyFirst + i;
-            DBody& b = B.bodies[g];
-            B.struck[g] = 0;
+        for (uint32_t i = g.tid; i < wi.bodyCount; i += g.size) {
+            const uint32_t gb = wi.bodyFirst + i;
+            DBody& b = B.bodies[gb];
+            B.struck[gb] = 0;
             if (!b.alive) { continue; }
             b.q0 = b.xf.q;
             b.qBase = b.xf.q;
@@ -725,11 +831,11 @@ __global__ void __launch_bounds__(kMaxBlock) k_prepare(Batch B, StepParams P, ui
             b.dq = qid();
             updateInverseMass(b);
         }
-        __syncthreads();
+        g.sync();
         const uint32_t cf = wi.contactFirst;
         DContact* cs = B.contacts + cf;
-        const uint32_t nActive = blockCompact(
-            nc,
+        const uint32_t nActive = groupCompact(
+            g, nc,
             [&](uint32_t i) {
                 if (!TF_OK_INDEX(B, cs[i].bodyA - wi.bodyFirst < wi.bodyCount && cs[i].bodyB - wi.bodyFirst < wi.bodyCount &&
                                     cs[i].count >= 0 && cs[i].count <= 4, 5, wi.bodyFirst, i)) {
@@ -742,10 +848,10 @@ __global__ void __launch_bounds__(kMaxBlock) k_prepare(Batch B, StepParams P, ui
                 uint8_t f = 0;
                 if (on && relativeTravel(a, b, P.dt) > P.tol.speculative) {
                     f |= kFlagFast;
-                    atomicAdd(&s_fast, 1u);
+                    atomicAdd(&s_fast[g.id], 1u);
                     if (!isPlanar(a) && !isPlanar(b)) {
                         f |= kFlagFastSolid;
-                        atomicAdd(&s_fastSolid, 1u);
+                        atomicAdd(&s_fastSolid[g.id], 1u);
                     }
                 }
                 B.cflags[cf + i] = f | (on ? kFlagActive : 0);
@@ -753,16 +859,15 @@ __global__ void __launch_bounds__(kMaxBlock) k_prepare(Batch B, StepParams P, ui
             },
             [&](uint32_t i, uint32_t pos) { B.active[cf + pos] = i; });
         const uint32_t* act = B.active + cf;
-        // Staging for the coloring: shared memory when the world fits, else the world's global scratch.
         const bool staged = wi.bodyCount <= stageBodies && nActive <= stageContacts;
-        uint32_t* masks = staged ? reinterpret_cast<uint32_t*>(s_raw) : B.bodyColors + wi.bodyFirst;
+        uint32_t* masks = staged ? reinterpret_cast<uint32_t*>(slice) : B.bodyColors + wi.bodyFirst;
         uint32_t* endA = staged ? masks + stageBodies : B.mergeIdxA + cf;
         uint32_t* endB = staged ? endA + stageContacts : B.mergeIdxB + cf;
-        uint8_t* colorable = staged ? reinterpret_cast<uint8_t*>(endB + stageContacts) : B.cflags + cf;
         // Colors by active position; moved to contact order below. The merge scratch is free by now.
         uint8_t* colorTmp = reinterpret_cast<uint8_t*>(B.mergePartA + cf);
-        for (uint32_t i = threadIdx.x; i < wi.bodyCount; i += blockDim.x) { masks[i] = 0; }
-        for (uint32_t x = threadIdx.x; x < nActive; x += blockDim.x) {
+        for (uint32_t i = g.tid; i < wi.bodyCount; i += g.size) { masks[i] = 0; }
+        uint32_t points = 0;
+        for (uint32_t x = g.tid; x < nActive; x += g.size) {
             if (!TF_OK_INDEX(B, act[x] < nc, 7, w, x)) { continue; }
             DContact& c = cs[act[x]];
             const DBody& a = B.bodies[c.bodyA];
@@ -770,102 +875,61 @@ __global__ void __launch_bounds__(kMaxBlock) k_prepare(Batch B, StepParams P, ui
             prepareContact(a, b, c);
             makeContactAxes(a, b, c, B.axes + (size_t)(cf + act[x]) * kAxesPerContact);
             c.flags &= ~kCLaned;
+            points += (uint32_t)c.count;
             const bool can = !(c.flags & kCPlanar) && !(c.rollingResistance > 0.0f);
-            endA[x] = movingBody(a) ? c.bodyA - wi.bodyFirst : kNone;
+            endA[x] = (movingBody(a) ? c.bodyA - wi.bodyFirst : kNone) | (can ? 0u : kNotColorable);
             endB[x] = movingBody(b) ? c.bodyB - wi.bodyFirst : kNone;
-            if (staged) { colorable[x] = can ? 1 : 0; }
-        }
-        __syncthreads();
-        if (!staged) {
-            // The global form reuses cflags for colorable, so keep the fast flags in the upper bits.
-            for (uint32_t x = threadIdx.x; x < nActive; x += blockDim.x) {
-                const DContact& c = cs[act[x]];
-                const bool can = !(c.flags & kCPlanar) && !(c.rollingResistance > 0.0f);
-                B.cflags[cf + act[x]] = (B.cflags[cf + act[x]] & ~8) | (can ? 8 : 0);
-            }
-            __syncthreads();
-        }
-        // Bodies of pairs closing faster than the restitution threshold are struck (src/world.cpp:1029-1049).
-        for (uint32_t x = threadIdx.x; x < nActive; x += blockDim.x) {
-            const DContact& c = cs[act[x]];
+            // Bodies of pairs closing faster than the restitution threshold are struck (src/world.cpp:1029-1049).
             for (int i = 0; i < c.count; ++i) {
                 if (c.points[i].relativeVelocity >= -P.restitutionThreshold) { continue; }
-                if (B.bodies[c.bodyA].type == kDynamic) { B.struck[c.bodyA] = 1; }
-                if (B.bodies[c.bodyB].type == kDynamic) { B.struck[c.bodyB] = 1; }
+                if (a.type == kDynamic) { B.struck[c.bodyA] = 1; }
+                if (b.type == kDynamic) { B.struck[c.bodyB] = 1; }
                 break;
             }
         }
-        if (threadIdx.x == 0) {
-            if (staged) {
-                colorSequential(nActive, endA, endB, colorable, masks, colorTmp);
-            } else {
-                for (uint32_t x = 0; x < nActive; ++x) {
-                    uint8_t k = kNoColor;
-                    if (B.cflags[cf + act[x]] & 8) {
-                        const uint32_t a = endA[x], b = endB[x];
-                        const uint32_t taken = (a != kNone ? masks[a] : 0u) | (b != kNone ? masks[b] : 0u);
-                        if (taken != 0xffffffffu) {
-                            const int f = __ffs(~taken) - 1;
-                            if (a != kNone) { masks[a] |= 1u << f; }
-                            if (b != kNone) { masks[b] |= 1u << f; }
-                            k = (uint8_t)f;
-                        }
-                    }
-                    colorTmp[x] = k;
-                }
-            }
-        }
-        __syncthreads();
+        atomicAdd(&s_points[g.id], points);
+        g.sync();
+        if (g.tid == 0) { colorSequential(nActive, endA, endB, masks, colorTmp); }
+        g.sync();
         uint8_t* colorOf = B.color + cf;
-        for (uint32_t x = threadIdx.x; x < nActive; x += blockDim.x) {
+        for (uint32_t x = g.tid; x < nActive; x += g.size) {
             const uint8_t k = colorTmp[x];
             colorOf[act[x]] = k;
             if (k != kNoColor) { cs[act[x]].flags |= kCLaned; }
         }
-        __syncthreads();
-        const uint32_t nImpact = blockCompact(
-            nActive,
+        g.sync();
+        const uint32_t nImpact = groupCompact(
+            g, nActive,
             [&](uint32_t x) {
                 const DContact& c = cs[act[x]];
                 return B.struck[c.bodyA] || B.struck[c.bodyB];
             },
             [&](uint32_t x, uint32_t pos) { B.impact[cf + pos] = act[x]; });
-        bucketByColor(nActive, act, colorOf, B.colored + cf, B.rest + cf, wc.colorStart, wc.colorCount, wc.restCount);
-        bucketByColor(nImpact, B.impact + cf, colorOf, B.impactColored + cf, B.impactRest + cf, wc.impactColorStart,
+        bucketByColor(g, nActive, act, colorOf, B.colored + cf, B.rest + cf, wc.colorStart, wc.colorCount, wc.restCount);
+        bucketByColor(g, nImpact, B.impact + cf, colorOf, B.impactColored + cf, B.impactRest + cf, wc.impactColorStart,
                       wc.impactColorCount, wc.impactRestCount);
-        {
-            __shared__ uint32_t s_points;
-            if (threadIdx.x == 0) { s_points = 0; }
-            __syncthreads();
-            uint32_t mine = 0;
-            for (uint32_t x = threadIdx.x; x < nActive; x += blockDim.x) { mine += (uint32_t)cs[act[x]].count; }
-            atomicAdd(&s_points, mine);
-            __syncthreads();
-            if (threadIdx.x == 0) { wc.activePoints = s_points; }
-        }
-        if (threadIdx.x == 0) {
+        if (g.tid == 0) {
             wc.activeCount = nActive;
             wc.impactCount = nImpact;
-            wc.fastCount = s_fast;
-            wc.fastSolidCount = s_fastSolid;
+            wc.fastCount = s_fast[g.id];
+            wc.fastSolidCount = s_fastSolid[g.id];
+            wc.activePoints = s_points[g.id];
         }
-        __syncthreads();
-    }
+        g.sync();
+    });
 }
-
 // ---------------------------------------------------------------------------------------------------------
 // The substep (src/world.cpp:1658-1681).
 
-// Calls f(contact index) for every contact of each color in turn, the colors apart by a block barrier.
+// Calls f(contact index) for every contact of each color in turn, the colors apart by a group barrier.
 template <class F>
-__device__ void forEachColor(const uint32_t* list, const uint32_t* start, uint32_t colors, F f) {
+__device__ void forEachColor(const Group& g, const uint32_t* list, const uint32_t* start, uint32_t colors, F f) {
     for (uint32_t k = 0; k < colors; ++k) {
         const uint32_t end = start[k + 1];
-        for (uint32_t x = start[k] + threadIdx.x; x < end; x += blockDim.x) { f(list[x]); }
-        __syncthreads();
+        for (uint32_t x = start[k] + g.tid; x < end; x += g.size) { f(list[x]); }
+        g.sync();
     }
 }
-
 // In checked builds, whether contact ci of a world can be read: in the list, with bodies in the world.
 __device__ __forceinline__ bool contactOk(const Batch& B, const WorldInfo& wi, const WorldCounts& wc,
                                           uint32_t ci, int code) {
@@ -1098,81 +1162,82 @@ struct SolverStore {
 };
 
 // Fast pairs collided again before a substep (src/world.cpp:1658-1668): inverse mass refreshed, other
-// contacts rebased, dp and dq reset, fast contacts collided with the time left. Does nothing in worlds
-// without such pairs, so it can sit in a recorded graph before every substep but the first.
-__global__ void __launch_bounds__(kMaxBlock) k_refresh(Batch B, StepParams P, int sub, int serial) {
+// contacts rebased, dp and dq reset, fast contacts collided with the time left, every active contact's axes
+// built again. Does nothing in worlds without such pairs, so it can sit in a recorded graph before every
+// substep but the first.
+__global__ void __launch_bounds__(kMaxBlock) k_refresh(Batch B, StepParams P, Split sp, int sub, int serial) {
     if (stepAborted(B, serial)) { return; }
-    for (int o = blockIdx.x; o < B.nWorlds; o += gridDim.x) {
-        const uint32_t w = B.order[o];
+    forWorlds(B, kSlotRefresh + sub, sp, nullptr, [&](const Group& g, uint32_t w, unsigned char*, const StageSizes&) {
         const WorldInfo wi = B.info[w];
         WorldCounts& wc = B.counts[w];
         const int n = P.substeps;
         const uint8_t againFlag = sub == n / 2 ? kFlagFast : kFlagFastSolid;
         const uint32_t againCount = sub == n / 2 ? wc.fastCount : wc.fastSolidCount;
-        if (!(sub > 0 && againCount > 0)) { continue; }
+        if (!(sub > 0 && againCount > 0)) { return; }
         const uint32_t cf = wi.contactFirst;
         DContact* cs = B.contacts + cf;
         const uint32_t nActive = wc.activeCount;
         const uint32_t* act = B.active + cf;
-        for (uint32_t i = threadIdx.x; i < wi.bodyCount; i += blockDim.x) {
+        for (uint32_t i = g.tid; i < wi.bodyCount; i += g.size) {
             DBody& b = B.bodies[wi.bodyFirst + i];
             if (b.alive && b.type == kDynamic && b.awake) { updateInverseMass(b); }
         }
-        __syncthreads();
-        for (uint32_t x = threadIdx.x; x < nActive; x += blockDim.x) {
+        g.sync();
+        for (uint32_t x = g.tid; x < nActive; x += g.size) {
             const uint32_t ci = act[x];
             if (B.cflags[cf + ci] & againFlag) { continue; }
             if (!contactOk(B, wi, wc, ci, 16)) { continue; }
             DContact& c = cs[ci];
             rebaseContact(B.bodies[c.bodyA], B.bodies[c.bodyB], c);
         }
-        __syncthreads();
-        for (uint32_t i = threadIdx.x; i < wi.bodyCount; i += blockDim.x) {
+        g.sync();
+        for (uint32_t i = g.tid; i < wi.bodyCount; i += g.size) {
             DBody& b = B.bodies[wi.bodyFirst + i];
             b.dp = zero3();
             b.dq = qid();
             b.qBase = b.xf.q;
         }
-        __syncthreads();
+        g.sync();
         const float remaining = (float)(n - sub) * P.h;
-        for (uint32_t x = threadIdx.x; x < nActive; x += blockDim.x) {
+        for (uint32_t x = g.tid; x < nActive; x += g.size) {
             const uint32_t ci = act[x];
             if (!(B.cflags[cf + ci] & againFlag)) { continue; }
             if (!contactOk(B, wi, wc, ci, 14)) { continue; }
             refreshContact(B, P, cs[ci], remaining);
         }
-        __syncthreads();
-        // Every active contact's axes again, from the refreshed inertia and the new anchors.
-        for (uint32_t x = threadIdx.x; x < nActive; x += blockDim.x) {
+        g.sync();
+        for (uint32_t x = g.tid; x < nActive; x += g.size) {
             const uint32_t ci = act[x];
             if (!contactOk(B, wi, wc, ci, 26)) { continue; }
             const DContact& c = cs[ci];
             makeContactAxes(B.bodies[c.bodyA], B.bodies[c.bodyB], c, B.axes + (size_t)(cf + ci) * kAxesPerContact);
         }
-        __syncthreads();
-    }
+        g.sync();
+    });
 }
 
-// Integrate velocities, warm start, biased solve, integrate positions, relax (src/world.cpp:1669-1680), with
-// the world's bodies staged in shared memory when they fit (stageBodies of them).
-__global__ void __launch_bounds__(kMaxBlock) k_substep(Batch B, StepParams P, uint32_t stageBodies, int serial) {
-    extern __shared__ __align__(16) float s_bodies[];
+// Integrate velocities, warm start, biased solve, integrate positions, relax (src/world.cpp:1669-1680). The
+// world's solver state is staged in the group's shared slice when it has at most stageN bodies.
+__global__ void __launch_bounds__(kMaxBlock) k_substep(Batch B, StepParams P, Split sp, int sub, int serial) {
+    extern __shared__ __align__(16) unsigned char s_raw[];
     if (stepAborted(B, serial)) { return; }
-    for (int o = blockIdx.x; o < B.nWorlds; o += gridDim.x) {
-        const uint32_t w = B.order[o];
+    forWorlds(B, kSlotSubstep + sub, sp, s_raw, [&](const Group& g, uint32_t w, unsigned char* sliceRaw, const StageSizes& ss) {
+        float* slice = reinterpret_cast<float*>(sliceRaw);
+        const uint32_t stageN = ss.bodies;
         const WorldInfo wi = B.info[w];
         const WorldCounts& wc = B.counts[w];
         const uint32_t cf = wi.contactFirst;
         DContact* cs = B.contacts + cf;
         const uint32_t nb = wi.bodyCount;
-        const SolverStore st{ s_bodies, stageBodies, nb <= stageBodies, B.bodies + wi.bodyFirst };
+        const SolverStore st{ slice, stageN, nb <= stageN, B.bodies + wi.bodyFirst };
         if (st.staged) {
-            for (uint32_t i = threadIdx.x; i < nb; i += blockDim.x) { st.stage(i); }
-            __syncthreads();
+            for (uint32_t i = g.tid; i < nb; i += g.size) { st.stage(i); }
+            g.sync();
         }
-        for (uint32_t i = threadIdx.x; i < nb; i += blockDim.x) { st.integrateVelocityAt(i, P); }
-        __syncthreads();
+        for (uint32_t i = g.tid; i < nb; i += g.size) { st.integrateVelocityAt(i, P); }
+        g.sync();
         const uint32_t base = wi.bodyFirst;
+        const Axis* axes = B.axes + (size_t)cf * kAxesPerContact;
         // A laned contact's bodies are stored only where they move, so a static body shared by a color's
         // contacts is never written concurrently; a contact solved on its own stores both, as the reference does.
         auto warm = [&](uint32_t ci, bool laned) {
@@ -1180,7 +1245,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_substep(Batch B, StepParams P, ui
             const DContact& c = cs[ci];
             const uint32_t ia = c.bodyA - base, ib = c.bodyB - base;
             SBody a = st.load(ia), b = st.load(ib);
-            warmStartContact(a, b, c, laned, B.axes + (size_t)(cf + ci) * kAxesPerContact);
+            warmStartContact(a, b, c, laned, axes + (size_t)ci * kAxesPerContact);
             if (!laned || !anchored(a)) { st.storeVW(ia, a); }
             if (!laned || !anchored(b)) { st.storeVW(ib, b); }
         };
@@ -1189,7 +1254,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_substep(Batch B, StepParams P, ui
             DContact& c = cs[ci];
             const uint32_t ia = c.bodyA - base, ib = c.bodyB - base;
             SBody a = st.load(ia), b = st.load(ib);
-            solveContact(a, b, c, P, bias, B.axes + (size_t)(cf + ci) * kAxesPerContact);
+            solveContact(a, b, c, P, bias, axes + (size_t)ci * kAxesPerContact);
             if (!laned || !anchored(a)) { st.storeVW(ia, a); }
             if (!laned || !anchored(b)) { st.storeVW(ib, b); }
         };
@@ -1197,36 +1262,36 @@ __global__ void __launch_bounds__(kMaxBlock) k_substep(Batch B, StepParams P, ui
         const uint32_t* rest = B.rest + cf;
         const uint32_t* icolored = B.impactColored + cf;
         const uint32_t* irest = B.impactRest + cf;
-        forEachColor(colored, wc.colorStart, wc.colorCount, [&](uint32_t ci) { warm(ci, true); });
-        if (threadIdx.x == 0) {
+        forEachColor(g, colored, wc.colorStart, wc.colorCount, [&](uint32_t ci) { warm(ci, true); });
+        if (g.tid == 0) {
             for (uint32_t x = 0; x < wc.restCount; ++x) { warm(rest[x], false); }
         }
-        __syncthreads();
+        g.sync();
         for (int pass = 0; pass < 2; ++pass) {
             const bool bias = pass == 0;
-            forEachColor(colored, wc.colorStart, wc.colorCount, [&](uint32_t ci) { solve(ci, bias, true); });
-            if (threadIdx.x == 0) {
+            forEachColor(g, colored, wc.colorStart, wc.colorCount, [&](uint32_t ci) { solve(ci, bias, true); });
+            if (g.tid == 0) {
                 for (uint32_t x = 0; x < wc.restCount; ++x) { solve(rest[x], bias, false); }
             }
-            __syncthreads();
+            g.sync();
             if (wc.impactCount > 0) {
-                forEachColor(icolored, wc.impactColorStart, wc.impactColorCount,
+                forEachColor(g, icolored, wc.impactColorStart, wc.impactColorCount,
                              [&](uint32_t ci) { solve(ci, bias, true); });
-                if (threadIdx.x == 0) {
+                if (g.tid == 0) {
                     for (uint32_t x = 0; x < wc.impactRestCount; ++x) { solve(irest[x], bias, false); }
                 }
-                __syncthreads();
+                g.sync();
             }
             if (bias) {
-                for (uint32_t i = threadIdx.x; i < nb; i += blockDim.x) { st.integratePositionAt(i, P); }
-                __syncthreads();
+                for (uint32_t i = g.tid; i < nb; i += g.size) { st.integratePositionAt(i, P); }
+                g.sync();
             }
         }
         if (st.staged) {
-            for (uint32_t i = threadIdx.x; i < nb; i += blockDim.x) { st.unstage(i); }
-            __syncthreads();
+            for (uint32_t i = g.tid; i < nb; i += g.size) { st.unstage(i); }
+            g.sync();
         }
-    }
+    });
 }
 
 // ---------------------------------------------------------------------------------------------------------
@@ -1245,47 +1310,49 @@ __device__ __forceinline__ uint32_t rootOf(const uint32_t* parent, uint32_t x) {
     return x;
 }
 
-__global__ void __launch_bounds__(kMaxBlock) k_finish(Batch B, StepParams P, uint32_t stageBodies,
-                                                      uint32_t stageContacts, int serial) {
+// Union-find is staged in the group's shared slice (parent and island time by body, union pairs by contact)
+// when the world fits, else in its global scratch.
+__global__ void __launch_bounds__(kMaxBlock) k_finish(Batch B, StepParams P, Split sp, int serial) {
     extern __shared__ __align__(16) unsigned char s_raw[];
-    __shared__ uint32_t s_awake, s_islands, s_sweep;
+    __shared__ uint32_t s_awake[kMaxGroups], s_islands[kMaxGroups], s_sweep[kMaxGroups];
     if (stepAborted(B, serial)) { return; }
-    for (int o = blockIdx.x; o < B.nWorlds; o += gridDim.x) {
-        const uint32_t w = B.order[o];
+    forWorlds(B, kSlotFinish, sp, s_raw, [&](const Group& g, uint32_t w, unsigned char* slice, const StageSizes& ss) {
+        const uint32_t stageBodies = ss.bodies, stageContacts = ss.contacts;
         const WorldInfo wi = B.info[w];
         WorldCounts& wc = B.counts[w];
         const uint32_t cf = wi.contactFirst;
         DContact* cs = B.contacts + cf;
-        if (threadIdx.x == 0) {
-            s_awake = 0;
-            s_islands = 0;
-            s_sweep = 0;
+        const Axis* axes = B.axes + (size_t)cf * kAxesPerContact;
+        if (g.tid == 0) {
+            s_awake[g.id] = 0;
+            s_islands[g.id] = 0;
+            s_sweep[g.id] = 0;
         }
         // Restitution: colored contacts by color, then the rest in active order.
-        forEachColor(B.colored + cf, wc.colorStart, wc.colorCount, [&](uint32_t ci) {
+        forEachColor(g, B.colored + cf, wc.colorStart, wc.colorCount, [&](uint32_t ci) {
             if (!contactOk(B, wi, wc, ci, 18)) { return; }
             DContact& c = cs[ci];
-            restituteContact(B.bodies[c.bodyA], B.bodies[c.bodyB], c, P, true, B.axes + (size_t)(cf + ci) * kAxesPerContact);
+            restituteContact(B.bodies[c.bodyA], B.bodies[c.bodyB], c, P, true, axes + (size_t)ci * kAxesPerContact);
         });
-        if (threadIdx.x == 0) {
+        if (g.tid == 0) {
             for (uint32_t x = 0; x < wc.restCount; ++x) {
-                if (!contactOk(B, wi, wc, B.rest[cf + x], 20)) { continue; }
-                DContact& c = cs[B.rest[cf + x]];
-                restituteContact(B.bodies[c.bodyA], B.bodies[c.bodyB], c, P, false,
-                                 B.axes + (size_t)(cf + B.rest[cf + x]) * kAxesPerContact);
+                const uint32_t ci = B.rest[cf + x];
+                if (!contactOk(B, wi, wc, ci, 20)) { continue; }
+                DContact& c = cs[ci];
+                restituteContact(B.bodies[c.bodyA], B.bodies[c.bodyB], c, P, false, axes + (size_t)ci * kAxesPerContact);
             }
         }
-        __syncthreads();
+        g.sync();
         const uint32_t nc = wc.contactCount;
         const bool staged = wi.bodyCount <= stageBodies && nc <= stageContacts;
-        uint32_t* parent = staged ? reinterpret_cast<uint32_t*>(s_raw) : B.unionParent + wi.bodyFirst;
+        uint32_t* parent = staged ? reinterpret_cast<uint32_t*>(slice) : B.unionParent + wi.bodyFirst;
         uint32_t* islandTime = staged ? parent + stageBodies : reinterpret_cast<uint32_t*>(B.islandTime + wi.bodyFirst);
         uint32_t* uA = staged ? islandTime + stageBodies : B.mergeIdxA + cf;
         uint32_t* uB = staged ? uA + stageContacts : B.mergeIdxB + cf;
         const float threshold = P.sleepThreshold;
-        for (uint32_t i = threadIdx.x; i < wi.bodyCount; i += blockDim.x) {
-            const uint32_t g = wi.bodyFirst + i;
-            DBody& b = B.bodies[g];
+        for (uint32_t i = g.tid; i < wi.bodyCount; i += g.size) {
+            const uint32_t gb = wi.bodyFirst + i;
+            DBody& b = B.bodies[gb];
             parent[i] = i;
             islandTime[i] = __float_as_uint(FLT_MAX);
             if (!b.alive) { continue; }
@@ -1325,7 +1392,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_finish(Batch B, StepParams P, uin
                         const float reach = length(s.local.p - b.localCenter) + s.extent;
                         const float travel = moved + angle * reach;
                         if (travel > b.expectedTravel && travel > b.expectedTravel + 0.5f * s.minExtent) {
-                            atomicAdd(&s_sweep, 1u);
+                            atomicAdd(&s_sweep[g.id], 1u);
                         }
                     }
                 }
@@ -1343,11 +1410,11 @@ __global__ void __launch_bounds__(kMaxBlock) k_finish(Batch B, StepParams P, uin
                 atomicOr(&wc.flags, kDevNonFinite);
             }
         }
-        __syncthreads();
+        g.sync();
         // Islands over contacts with points (src/world.cpp:1187-1233). The roots are each component's lowest
         // body whatever order the unions run in, so only the unions themselves run on one thread.
-        const uint32_t nu = blockCompact(
-            nc,
+        const uint32_t nu = groupCompact(
+            g, nc,
             [&](uint32_t ci) {
                 if (!contactOk(B, wi, wc, ci, 22)) { return false; }
                 const DContact& c = cs[ci];
@@ -1368,25 +1435,25 @@ __global__ void __launch_bounds__(kMaxBlock) k_finish(Batch B, StepParams P, uin
                 uA[pos] = cs[ci].bodyA - wi.bodyFirst;
                 uB[pos] = cs[ci].bodyB - wi.bodyFirst;
             });
-        if (threadIdx.x == 0) {
+        if (g.tid == 0) {
             for (uint32_t x = 0; x < nu; ++x) {
                 if (!TF_OK_INDEX(B, uA[x] < wi.bodyCount && uB[x] < wi.bodyCount, 24, w, x)) { continue; }
                 const uint32_t ra = findRoot(parent, uA[x]), rb = findRoot(parent, uB[x]);
                 if (ra != rb) { parent[ra > rb ? ra : rb] = ra < rb ? ra : rb; }
             }
         }
-        __syncthreads();
-        for (uint32_t i = threadIdx.x; i < wi.bodyCount; i += blockDim.x) {
+        g.sync();
+        for (uint32_t i = g.tid; i < wi.bodyCount; i += g.size) {
             DBody& b = B.bodies[wi.bodyFirst + i];
             if (!b.alive || b.type != kDynamic || !b.awake) { continue; }
             const uint32_t r = rootOf(parent, i);
             b.island = r;
-            atomicAdd(&s_awake, 1u);
-            if (r == i) { atomicAdd(&s_islands, 1u); }
+            atomicAdd(&s_awake[g.id], 1u);
+            if (r == i) { atomicAdd(&s_islands[g.id], 1u); }
             atomicMin(&islandTime[r], __float_as_uint(b.sleepTime));
         }
-        __syncthreads();
-        for (uint32_t i = threadIdx.x; i < wi.bodyCount; i += blockDim.x) {
+        g.sync();
+        for (uint32_t i = g.tid; i < wi.bodyCount; i += g.size) {
             DBody& b = B.bodies[wi.bodyFirst + i];
             if (!b.alive || b.type != kDynamic || !b.awake) { continue; }
             if (__uint_as_float(islandTime[rootOf(parent, i)]) < P.timeToSleep) { continue; }
@@ -1395,20 +1462,19 @@ __global__ void __launch_bounds__(kMaxBlock) k_finish(Batch B, StepParams P, uin
             b.w = zero3();
             updateInverseMass(b);
         }
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            wc.awakeBodies = s_awake;
-            wc.awakeIslands = s_islands;
-            wc.bodySteps += s_awake;
-            if (s_sweep > 0) {
-                wc.sweepShapes += s_sweep;
+        g.sync();
+        if (g.tid == 0) {
+            wc.awakeBodies = s_awake[g.id];
+            wc.awakeIslands = s_islands[g.id];
+            wc.bodySteps += s_awake[g.id];
+            if (s_sweep[g.id] > 0) {
+                wc.sweepShapes += s_sweep[g.id];
                 wc.flags |= kDevSweepSkipped;
             }
         }
-        __syncthreads();
-    }
+        g.sync();
+    });
 }
-
 // ---------------------------------------------------------------------------------------------------------
 // Host traffic of a running batch: per-step forces in, poses out.
 
@@ -1436,3 +1502,4 @@ __global__ void k_pack_poses(const DBody* bodies, uint32_t n, float* __restrict_
 }
 
 }
+

@@ -149,3 +149,19 @@ class Batch:
         abi.check(self.lib.tf_world_work_counts(self.h, out.ctypes.data), self.lib)
         keys = ("bodies", "awake", "candidates", "contacts", "active_contacts", "active_points")
         return dict(zip(keys, (int(x) for x in out)))
+
+    KERNELS = ("broadphase", "narrowphase", "wake", "prepare", "refresh", "substep", "finish")
+
+    def set_launch(self, kernel, threads, big_bodies, smem_bytes):
+        """Launch shape of one kernel (name or index; None for all): threads per CTA, the world size above
+        which a world gets the whole CTA, and the CTA's staging bytes."""
+        k = -1 if kernel is None else (self.KERNELS.index(kernel) if isinstance(kernel, str) else int(kernel))
+        abi.check(self.lib.tf_world_set_launch(self.h, k, int(threads), int(big_bodies), int(smem_bytes)), self.lib)
+
+    def launch(self, kernel):
+        """The launch shape in use for one kernel, after the batch was laid out on the device."""
+        k = self.KERNELS.index(kernel) if isinstance(kernel, str) else int(kernel)
+        out = np.zeros(6, np.uint32)
+        abi.check(self.lib.tf_world_get_launch(self.h, k, out.ctypes.data), self.lib)
+        keys = ("threads", "big_bodies", "smem_bytes", "grid", "stage_big", "stage_small")
+        return dict(zip(keys, (int(x) for x in out)))
