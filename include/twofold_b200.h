@@ -267,6 +267,11 @@ TF_API const char* tf_kernel_name(int32_t kernel);
  * pairs, [3] contacts, [4] active contacts, [5] active contact points. */
 TF_API int tf_world_work_counts(void* world, int64_t out[6]);
 
+/* Solver work of world w in the last step: out[0] active contacts, [1] colors, [2] contacts solved one at a
+ * time (planar, rolling or beyond the last color), [3] impact contacts, [4] impact colors, [5] impact
+ * contacts solved one at a time, [6] fast contacts, [7] fast contacts between solid bodies. */
+TF_API int tf_world_solver_counts(void* world, int32_t w, int32_t out[8]);
+
 /* Launch shape of one kernel (0 broadphase, 1 narrowphase, 2 wake, 3 prepare, 4 refresh, 5 substep,
  * 6 finish; -1 every kernel): threads per CTA (a multiple of 32, at most 512), the world size in bodies
  * above which a world is stepped by a whole CTA (smaller worlds take one warp each), and the shared memory

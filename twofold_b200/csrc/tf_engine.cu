@@ -63,6 +63,10 @@ template <class T>
 struct DevArray {
     T* ptr = nullptr;
     size_t n = 0;
+    DevArray() = default;
+    DevArray(const DevArray&) = delete;
+    DevArray& operator=(const DevArray&) = delete;
+    ~DevArray() { release(); }
     int alloc(size_t count) {
         if (count <= n && ptr) { return TF_OK; }
         if (ptr) { cudaFree(ptr); }
@@ -185,7 +189,9 @@ public:
         }
     }
 
+    // The device arrays free themselves after this body, with the engine's device still current.
     ~Engine() {
+        if (stream) { cudaSetDevice(device); }
         for (cudaEvent_t e : eventPool) { cudaEventDestroy(e); }
         if (callStart) { cudaEventDestroy(callStart); }
         if (callStop) { cudaEventDestroy(callStop); }
@@ -1527,6 +1533,24 @@ TF_API int tf_world_work_counts(void* h, int64_t out[6]) {
 TF_API int tf_world_launch_count(void* h, int64_t* launches) {
     if (!h || !launches) { return tfb::fail(TF_E_INVALID, "tf_world_launch_count: null"); }
     *launches = E(h)->launches;
+    return TF_OK;
+}
+
+TF_API int tf_world_solver_counts(void* h, int32_t w, int32_t out[8]) {
+    if (!h || !out) { return tfb::fail(TF_E_INVALID, "tf_world_solver_counts: null"); }
+    Engine* e = E(h);
+    if (w < 0 || w >= (int)e->worlds.size()) { return tfb::fail(TF_E_INVALID, "tf_world_solver_counts: bad world"); }
+    for (int k = 0; k < 8; ++k) { out[k] = 0; }
+    if (e->lastCounts.size() != e->worlds.size()) { return TF_OK; }
+    const tfb::WorldCounts& c = e->lastCounts[(size_t)w];
+    out[0] = (int32_t)c.activeCount;
+    out[1] = (int32_t)c.colorCount;
+    out[2] = (int32_t)c.restCount;
+    out[3] = (int32_t)c.impactCount;
+    out[4] = (int32_t)c.impactColorCount;
+    out[5] = (int32_t)c.impactRestCount;
+    out[6] = (int32_t)c.fastCount;
+    out[7] = (int32_t)c.fastSolidCount;
     return TF_OK;
 }
 

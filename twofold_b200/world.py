@@ -150,6 +150,13 @@ class Batch:
         keys = ("bodies", "awake", "candidates", "contacts", "active_contacts", "active_points")
         return dict(zip(keys, (int(x) for x in out)))
 
+    def solver_counts(self, wi):
+        """Solver work of world wi in the last step."""
+        out = np.zeros(8, np.int32)
+        abi.check(self.lib.tf_world_solver_counts(self.h, wi, out.ctypes.data), self.lib)
+        keys = ("active", "colors", "rest", "impact", "impact_colors", "impact_rest", "fast", "fast_solid")
+        return dict(zip(keys, (int(x) for x in out)))
+
     KERNELS = ("broadphase", "narrowphase", "wake", "prepare", "refresh", "substep", "finish")
 
     def set_launch(self, kernel, threads, big_bodies, smem_bytes):
