@@ -1,0 +1,528 @@
+// twofold::World over the B200 contact pipeline: the drop-in C++ surface for World::step.
+//
+// Code written against the reference's include/twofold/world.h (World, BodyDesc, ShapeDesc, WorldSettings,
+// StepProfile, ContactInfo, the id types and geometry alternatives) compiles against this header for the
+// part of the API the contact pipeline covers: building bodies and shapes, step(), reading poses,
+// velocities, mass, sleep state, contacts and the step profile, setting velocities and adding forces.
+// Every call forwards to the C ABI in twofold_b200.h; the library owns the device state.
+//
+// Same conventions as the reference (include/twofold/world.h:362-510, src/world.cpp:352-371): invalid ids
+// make getters return defaults and setters do nothing; step() ignores dt <= 0 or non-finite dt; nothing
+// throws. What the reference reports by silence this header also records: status() is the last C ABI
+// status (TF_OK or a negative TF_E* code) and statusMessage() its text.
+//
+// Differences a caller can see:
+//   - Geometry: spheres, boxes and half-spaces run on the device. Cylinders, prisms, hulls and meshes are
+//     refused by addShape (an invalid ShapeId, status TF_E_UNSUPPORTED), as are sensors and planar locks.
+//   - addForce/addTorque queue the force for the next step and act on awake bodies only (wake = false).
+//   - Copying a World is not provided; move it instead.
+//   - The math types carry the reference's fields and a few operators, not all of math.h.
+#pragma once
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <memory>
+#include <string>
+#include <variant>
+#include <vector>
+
+#include "../twofold_b200.h"
+
+namespace twofold {
+
+struct Vec2 {
+    float x = 0, y = 0;
+    Vec2() = default;
+    constexpr Vec2(float x_, float y_) : x(x_), y(y_) {}
+};
+
+struct Vec3 {
+    float x = 0, y = 0, z = 0;
+    Vec3() = default;
+    constexpr Vec3(float x_, float y_, float z_) : x(x_), y(y_), z(z_) {}
+    Vec3 operator+(const Vec3& b) const { return { x + b.x, y + b.y, z + b.z }; }
+    Vec3 operator-(const Vec3& b) const { return { x - b.x, y - b.y, z - b.z }; }
+    Vec3 operator-() const { return { -x, -y, -z }; }
+    Vec3 operator*(float s) const { return { x * s, y * s, z * s }; }
+};
+
+inline float dot(const Vec3& a, const Vec3& b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+inline Vec3 cross(const Vec3& a, const Vec3& b) { return { a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x }; }
+inline float length(const Vec3& v) { return std::sqrt(dot(v, v)); }
+
+struct Mat3 {
+    Vec3 r[3] = { { 1, 0, 0 }, { 0, 1, 0 }, { 0, 0, 1 } };
+    static Mat3 zero() {
+        Mat3 m;
+        m.r[0] = m.r[1] = m.r[2] = Vec3{};
+        return m;
+    }
+};
+
+struct Quat {
+    float x = 0, y = 0, z = 0, w = 1;
+    Quat() = default;
+    constexpr Quat(float x_, float y_, float z_, float w_) : x(x_), y(y_), z(z_), w(w_) {}
+    // v + 2w (u x v) + 2 u x (u x v), u the vector part.
+    Vec3 rotate(const Vec3& v) const {
+        const Vec3 u{ x, y, z };
+        const Vec3 t = cross(u, v) * 2.0f;
+        return v + t * w + cross(u, t);
+    }
+};
+
+struct Transform {
+    Vec3 p;
+    Quat q;
+    Vec3 apply(const Vec3& v) const { return p + q.rotate(v); }
+};
+
+struct BodyId {
+    uint32_t index = UINT32_MAX;
+    uint32_t generation = 0;
+    bool operator==(const BodyId& b) const { return index == b.index && generation == b.generation; }
+    bool operator!=(const BodyId& b) const { return !(*this == b); }
+};
+
+struct ShapeId {
+    uint32_t index = UINT32_MAX;
+    uint32_t generation = 0;
+    bool operator==(const ShapeId& b) const { return index == b.index && generation == b.generation; }
+    bool operator!=(const ShapeId& b) const { return !(*this == b); }
+};
+
+enum class MotionType : uint8_t { Static, Kinematic, Dynamic };
+
+enum LockFlags : uint8_t {
+    LockTranslationX = TF_LOCK_TRANSLATION_X,
+    LockTranslationY = TF_LOCK_TRANSLATION_Y,
+    LockTranslationZ = TF_LOCK_TRANSLATION_Z,
+    LockRotationX = TF_LOCK_ROTATION_X,
+    LockRotationY = TF_LOCK_ROTATION_Y,
+    LockRotationZ = TF_LOCK_ROTATION_Z,
+    LockPlanar = TF_LOCK_PLANAR,
+};
+
+struct Sphere {
+    float radius = 0.5f;
+};
+struct Box {
+    Vec3 halfExtents{ 0.5f, 0.5f, 0.5f };
+};
+struct Cylinder {
+    float radius = 0.5f;
+    float halfHeight = 0.5f;
+};
+struct Prism {
+    std::vector<Vec2> polygon;
+    float zMin = -0.5f;
+    float zMax = 0.5f;
+};
+struct Hull {
+    std::vector<Vec3> points;
+    int maxVertices = 64;
+};
+struct HalfSpace {};
+class TriangleMesh;
+struct Mesh {
+    std::shared_ptr<const TriangleMesh> mesh;
+};
+using Geometry = std::variant<Sphere, Box, Cylinder, Prism, Hull, HalfSpace, Mesh>;
+
+struct ShapeDesc {
+    Geometry geometry = Box{};
+    Vec3 position;
+    Quat rotation;
+    float density = 1.0f;
+    float friction = 0.5f;
+    float restitution = 0.0f;
+    float rollingResistance = 0.0f;
+    uint32_t category = 1;
+    uint32_t mask = 0xffffffffu;
+    bool sensor = false;
+    void* userData = nullptr;
+};
+
+struct BodyDesc {
+    MotionType type = MotionType::Dynamic;
+    Vec3 position;
+    Quat rotation;
+    Vec3 linearVelocity;
+    Vec3 angularVelocity;
+    float linearDamping = 0.0f;
+    float angularDamping = 0.0f;
+    float gravityScale = 1.0f;
+    uint8_t locks = 0;
+    Quat lockFrame;
+    bool awake = true;
+    bool canSleep = true;
+    void* userData = nullptr;
+};
+
+struct MassProperties {
+    float mass = 0.0f;
+    Vec3 center;
+    Mat3 inertia = Mat3::zero();
+};
+
+struct WorldSettings {
+    Vec3 gravity{ 0.0f, -9.81f, 0.0f };
+    float lengthUnit = 1.0f;
+    int substeps = 4;
+    float contactHertz = 30.0f;
+    float contactDampingRatio = 10.0f;
+    float maxPushoutSpeed = 3.0f;
+    float maxLinearSpeed = 1000.0f;
+    float maxAngularSpeed = 1000.0f;
+    float restitutionThreshold = 1.0f;
+    float hitThreshold = 1.0f;
+    float sleepThreshold = 0.05f;
+    float timeToSleep = 0.5f;
+    float contactReuseDistance = 0.0005f;
+    float contactReuseAngle = 0.035f;
+    float jointHertz = 60.0f;
+    float jointDampingRatio = 2.0f;
+    bool continuous = true;
+};
+
+struct ContactInfo {
+    BodyId bodyA;
+    BodyId bodyB;
+    ShapeId shapeA;
+    ShapeId shapeB;
+    Vec3 normal;
+    float friction = 0.0f;
+    float restitution = 0.0f;
+    float rollingResistance = 0.0f;
+    Vec3 rollingImpulse;
+    int pointCount = 0;
+    Vec3 points[4];
+    float separations[4] = {};
+    float normalImpulses[4] = {};
+    Vec3 tangentImpulses[4];
+};
+
+struct StepProfile {
+    float total = 0.0f;
+    float broadphase = 0.0f;
+    float narrowphase = 0.0f;
+    float solver = 0.0f;
+    float continuous = 0.0f;
+    float sleep = 0.0f;
+    int candidatePairs = 0;
+    int sweptPairs = 0;
+    int impacts = 0;
+    int manifolds = 0;
+    int touchingContacts = 0;
+    int awakeBodies = 0;
+    int awakeIslands = 0;
+};
+
+class World {
+public:
+    explicit World(const WorldSettings& settings = {}, int device = 0) : settings_(settings) {
+        const tf_settings s = toC(settings);
+        void* h = nullptr;
+        status_ = tf_world_create(&s, 1, device, &h);
+        handle_ = h;
+    }
+    ~World() {
+        if (handle_) { tf_world_destroy(handle_); }
+    }
+    World(const World&) = delete;
+    World& operator=(const World&) = delete;
+    World(World&& o) noexcept { *this = std::move(o); }
+    World& operator=(World&& o) noexcept {
+        if (this != &o) {
+            if (handle_) { tf_world_destroy(handle_); }
+            handle_ = o.handle_;
+            o.handle_ = nullptr;
+            settings_ = o.settings_;
+            profile_ = o.profile_;
+            bodies_ = std::move(o.bodies_);
+            shapes_ = std::move(o.shapes_);
+            forces_ = std::move(o.forces_);
+            torques_ = std::move(o.torques_);
+            forcesPending_ = o.forcesPending_;
+            status_ = o.status_;
+        }
+        return *this;
+    }
+
+    const WorldSettings& settings() const { return settings_; }
+    void setSettings(const WorldSettings& settings) {
+        settings_ = settings;
+        const tf_settings s = toC(settings);
+        note(tf_world_set_settings(handle_, &s));
+    }
+    void setGravity(const Vec3& gravity) {
+        WorldSettings s = settings_;
+        s.gravity = gravity;
+        setSettings(s);
+    }
+
+    void step(float dt) {
+        if (!(dt > 0.0f) || !std::isfinite(dt) || !handle_) { return; }
+        if (forcesPending_) {
+            note(tf_world_add_forces(handle_, forces_.data(), torques_.data()));
+            std::fill(forces_.begin(), forces_.end(), 0.0f);
+            std::fill(torques_.begin(), torques_.end(), 0.0f);
+            forcesPending_ = false;
+        }
+        if (!note(tf_world_step(handle_, dt, 1))) { return; }
+        tf_profile p{};
+        if (note(tf_world_profile(handle_, 0, &p))) {
+            profile_.total = p.total;
+            profile_.broadphase = p.broadphase;
+            profile_.narrowphase = p.narrowphase;
+            profile_.solver = p.solver;
+            profile_.continuous = p.continuous;
+            profile_.sleep = p.sleep;
+            profile_.candidatePairs = p.candidate_pairs;
+            profile_.sweptPairs = p.swept_pairs;
+            profile_.impacts = p.impacts;
+            profile_.manifolds = p.manifolds;
+            profile_.touchingContacts = p.touching_contacts;
+            profile_.awakeBodies = p.awake_bodies;
+            profile_.awakeIslands = p.awake_islands;
+        }
+    }
+    const StepProfile& profile() const { return profile_; }
+
+    BodyId createBody(const BodyDesc& d) {
+        tf_body_desc c{};
+        c.type = d.type == MotionType::Static ? TF_STATIC : d.type == MotionType::Kinematic ? TF_KINEMATIC : TF_DYNAMIC;
+        put3(c.position, d.position);
+        put4(c.rotation, d.rotation);
+        put3(c.linear_velocity, d.linearVelocity);
+        put3(c.angular_velocity, d.angularVelocity);
+        c.linear_damping = d.linearDamping;
+        c.angular_damping = d.angularDamping;
+        c.gravity_scale = d.gravityScale;
+        c.locks = d.locks;
+        put4(c.lock_frame, d.lockFrame);
+        c.awake = d.awake ? 1 : 0;
+        c.can_sleep = d.canSleep ? 1 : 0;
+        tf_id id{ UINT32_MAX, 0 };
+        if (!note(tf_body_create(handle_, 0, &c, &id))) { return {}; }
+        if (id.index >= bodies_.size()) { bodies_.resize(id.index + 1, BodyId{}); }
+        bodies_[id.index] = BodyId{ id.index, id.generation };
+        forces_.resize(3 * bodies_.size(), 0.0f);
+        torques_.resize(3 * bodies_.size(), 0.0f);
+        return bodies_[id.index];
+    }
+
+    ShapeId addShape(BodyId body, const ShapeDesc& d) {
+        if (!isValid(body)) { return {}; }
+        tf_shape_desc c{};
+        std::vector<float> points;
+        if (const Sphere* s = std::get_if<Sphere>(&d.geometry)) {
+            c.geometry = TF_SPHERE;
+            c.radius = s->radius;
+        } else if (const Box* b = std::get_if<Box>(&d.geometry)) {
+            c.geometry = TF_BOX;
+            put3(c.half_extents, b->halfExtents);
+        } else if (const Cylinder* y = std::get_if<Cylinder>(&d.geometry)) {
+            c.geometry = TF_CYLINDER;
+            c.radius = y->radius;
+            c.half_height = y->halfHeight;
+        } else if (const Prism* p = std::get_if<Prism>(&d.geometry)) {
+            c.geometry = TF_PRISM;
+            for (const Vec2& v : p->polygon) { points.insert(points.end(), { v.x, v.y }); }
+            c.point_count = (int32_t)p->polygon.size();
+            c.z_min = p->zMin;
+            c.z_max = p->zMax;
+        } else if (const Hull* hl = std::get_if<Hull>(&d.geometry)) {
+            c.geometry = TF_HULL;
+            for (const Vec3& v : hl->points) { points.insert(points.end(), { v.x, v.y, v.z }); }
+            c.point_count = (int32_t)hl->points.size();
+            c.max_vertices = hl->maxVertices;
+        } else if (std::holds_alternative<HalfSpace>(d.geometry)) {
+            c.geometry = TF_HALFSPACE;
+        } else {
+            c.geometry = TF_MESH;
+        }
+        c.points = points.empty() ? nullptr : points.data();
+        put3(c.position, d.position);
+        put4(c.rotation, d.rotation);
+        c.density = d.density;
+        c.friction = d.friction;
+        c.restitution = d.restitution;
+        c.rolling_resistance = d.rollingResistance;
+        c.category = d.category;
+        c.mask = d.mask;
+        c.sensor = d.sensor ? 1 : 0;
+        tf_id id{ UINT32_MAX, 0 };
+        if (!note(tf_shape_add(handle_, 0, tf_id{ body.index, body.generation }, &c, &id))) { return {}; }
+        if (id.index >= shapes_.size()) { shapes_.resize(id.index + 1, ShapeId{}); }
+        shapes_[id.index] = ShapeId{ id.index, id.generation };
+        return shapes_[id.index];
+    }
+
+    bool isValid(BodyId body) const { return body.index < bodies_.size() && bodies_[body.index] == body; }
+    bool isValid(ShapeId shape) const { return shape.index < shapes_.size() && shapes_[shape.index] == shape; }
+    std::vector<BodyId> bodies() const {
+        std::vector<BodyId> out;
+        for (const BodyId& b : bodies_) {
+            if (b.index != UINT32_MAX) { out.push_back(b); }
+        }
+        return out;
+    }
+
+    Transform transform(BodyId body) const {
+        Transform t;
+        Vec3 v, w;
+        state(body, t, v, w);
+        return t;
+    }
+    Vec3 position(BodyId body) const { return transform(body).p; }
+    Quat rotation(BodyId body) const { return transform(body).q; }
+    Vec3 centerOfMass(BodyId body) const { return transform(body).apply(massProperties(body).center); }
+    Vec3 linearVelocity(BodyId body) const {
+        Transform t;
+        Vec3 v, w;
+        state(body, t, v, w);
+        return v;
+    }
+    Vec3 angularVelocity(BodyId body) const {
+        Transform t;
+        Vec3 v, w;
+        state(body, t, v, w);
+        return w;
+    }
+    void setLinearVelocity(BodyId body, const Vec3& v) { setVelocities(body, &v, nullptr); }
+    void setAngularVelocity(BodyId body, const Vec3& w) { setVelocities(body, nullptr, &w); }
+
+    void addForce(BodyId body, const Vec3& force, bool = true) { queue(forces_, body, force); }
+    void addTorque(BodyId body, const Vec3& torque, bool = true) { queue(torques_, body, torque); }
+
+    MassProperties massProperties(BodyId body) const {
+        MassProperties m;
+        if (!isValid(body)) { return m; }
+        float mass = 0, center[3] = {}, inertia[9] = {};
+        if (!note(tf_body_get_mass(handle_, 0, tf_id{ body.index, body.generation }, &mass, center, inertia))) { return m; }
+        m.mass = mass;
+        m.center = Vec3{ center[0], center[1], center[2] };
+        for (int i = 0; i < 3; ++i) { m.inertia.r[i] = Vec3{ inertia[3 * i], inertia[3 * i + 1], inertia[3 * i + 2] }; }
+        return m;
+    }
+
+    bool isAwake(BodyId body) const {
+        int32_t awake = 0;
+        if (!isValid(body)) { return false; }
+        note(tf_body_is_awake(handle_, 0, tf_id{ body.index, body.generation }, &awake));
+        return awake != 0;
+    }
+
+    std::vector<ContactInfo> contacts(bool includeSpeculative = false) const {
+        std::vector<ContactInfo> out;
+        int32_t n = 0;
+        const int mode = includeSpeculative ? 1 : 0;
+        if (!note(tf_world_contacts(handle_, 0, mode, nullptr, 0, &n)) || n == 0) { return out; }
+        std::vector<tf_contact> raw((size_t)n);
+        if (!note(tf_world_contacts(handle_, 0, mode, raw.data(), n, &n))) { return out; }
+        for (const tf_contact& c : raw) {
+            ContactInfo o;
+            o.bodyA = bodyAt(c.body_a);
+            o.bodyB = bodyAt(c.body_b);
+            o.shapeA = shapeAt(c.shape_a);
+            o.shapeB = shapeAt(c.shape_b);
+            o.normal = Vec3{ c.normal[0], c.normal[1], c.normal[2] };
+            o.friction = c.friction;
+            o.restitution = c.restitution;
+            o.rollingResistance = c.rolling_resistance;
+            o.rollingImpulse = Vec3{ c.rolling_impulse[0], c.rolling_impulse[1], c.rolling_impulse[2] };
+            o.pointCount = c.point_count;
+            for (int i = 0; i < c.point_count && i < 4; ++i) {
+                o.points[i] = Vec3{ c.points[i][0], c.points[i][1], c.points[i][2] };
+                o.separations[i] = c.separations[i];
+                o.normalImpulses[i] = c.normal_impulses[i];
+                o.tangentImpulses[i] = Vec3{ c.tangent_impulses[i][0], c.tangent_impulses[i][1], c.tangent_impulses[i][2] };
+            }
+            out.push_back(o);
+        }
+        return out;
+    }
+
+    // The last C ABI status and its message; TF_OK after calls that succeeded.
+    int status() const { return status_; }
+    std::string statusMessage() const { return status_ == TF_OK ? std::string() : std::string(tf_last_error()); }
+    // The C ABI handle, for calls this class does not wrap (batched stepping, launch shapes, profiling).
+    void* handle() const { return handle_; }
+
+private:
+    static void put3(float* o, const Vec3& v) { o[0] = v.x, o[1] = v.y, o[2] = v.z; }
+    static void put4(float* o, const Quat& q) { o[0] = q.x, o[1] = q.y, o[2] = q.z, o[3] = q.w; }
+
+    static tf_settings toC(const WorldSettings& s) {
+        tf_settings c{};
+        put3(c.gravity, s.gravity);
+        c.length_unit = s.lengthUnit;
+        c.substeps = s.substeps;
+        c.contact_hertz = s.contactHertz;
+        c.contact_damping_ratio = s.contactDampingRatio;
+        c.max_pushout_speed = s.maxPushoutSpeed;
+        c.max_linear_speed = s.maxLinearSpeed;
+        c.max_angular_speed = s.maxAngularSpeed;
+        c.restitution_threshold = s.restitutionThreshold;
+        c.hit_threshold = s.hitThreshold;
+        c.sleep_threshold = s.sleepThreshold;
+        c.time_to_sleep = s.timeToSleep;
+        c.contact_reuse_distance = s.contactReuseDistance;
+        c.contact_reuse_angle = s.contactReuseAngle;
+        c.joint_hertz = s.jointHertz;
+        c.joint_damping_ratio = s.jointDampingRatio;
+        c.continuous = s.continuous ? 1 : 0;
+        return c;
+    }
+
+    bool note(int rc) const {
+        status_ = rc;
+        return rc == TF_OK;
+    }
+
+    void state(BodyId body, Transform& t, Vec3& v, Vec3& w) const {
+        if (!isValid(body)) { return; }
+        float p[3] = {}, q[4] = { 0, 0, 0, 1 }, lv[3] = {}, av[3] = {};
+        if (!note(tf_body_get_state(handle_, 0, tf_id{ body.index, body.generation }, p, q, lv, av))) { return; }
+        t.p = Vec3{ p[0], p[1], p[2] };
+        t.q = Quat{ q[0], q[1], q[2], q[3] };
+        v = Vec3{ lv[0], lv[1], lv[2] };
+        w = Vec3{ av[0], av[1], av[2] };
+    }
+
+    void setVelocities(BodyId body, const Vec3* v, const Vec3* w) {
+        if (!isValid(body)) { return; }
+        Transform t;
+        Vec3 lv, av;
+        state(body, t, lv, av);
+        if (v) { lv = *v; }
+        if (w) { av = *w; }
+        float a[3], b[3];
+        put3(a, lv);
+        put3(b, av);
+        note(tf_body_set_velocity(handle_, 0, tf_id{ body.index, body.generation }, a, b));
+    }
+
+    void queue(std::vector<float>& into, BodyId body, const Vec3& f) {
+        if (!isValid(body)) { return; }
+        float* o = into.data() + 3 * (size_t)body.index;
+        o[0] += f.x, o[1] += f.y, o[2] += f.z;
+        forcesPending_ = true;
+    }
+
+    BodyId bodyAt(uint32_t i) const { return i < bodies_.size() ? bodies_[i] : BodyId{}; }
+    ShapeId shapeAt(uint32_t i) const { return i < shapes_.size() ? shapes_[i] : ShapeId{}; }
+
+    void* handle_ = nullptr;
+    WorldSettings settings_;
+    StepProfile profile_;
+    std::vector<BodyId> bodies_;
+    std::vector<ShapeId> shapes_;
+    std::vector<float> forces_, torques_;
+    bool forcesPending_ = false;
+    mutable int status_ = TF_OK;
+};
+
+}  // namespace twofold

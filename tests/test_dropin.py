@@ -1,0 +1,55 @@
+"""The drop-in C++ surface: tests/dropin/pyramid_step.cpp, written against the reference's public World API,
+builds unchanged against include/twofold_b200/world.hpp, and run on the GPU it prints what the reference
+printed (tests/golden/dropin_pyramid.txt, made by tests/golden/make_dropin_golden.py) within 1e-5.
+"""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from parity import rel_err
+from twofold_b200 import abi
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+PROGRAM = os.path.join(HERE, "dropin", "pyramid_step.cpp")
+GOLDEN = os.path.join(HERE, "golden", "dropin_pyramid.txt")
+TOL = 1e-5
+
+
+def _compile(out, link):
+    cmd = ["g++", "-std=c++17", "-O2", "-ffp-contract=off", f"-I{os.path.join(ROOT, 'include')}",
+           '-DTWOFOLD_HEADER="twofold_b200/world.hpp"', PROGRAM]
+    if link:
+        libdir = os.path.dirname(abi.LIB_PATH)
+        cmd += ["-o", out, f"-L{libdir}", "-l:" + os.path.basename(abi.LIB_PATH), f"-Wl,-rpath,{libdir}"]
+    else:
+        cmd += ["-fsyntax-only"]
+    subprocess.run(cmd, check=True, capture_output=True, text=True)
+
+
+def _parse(text):
+    lines = [l for l in text.splitlines() if l and not l.startswith("#")]
+    manifolds = int(lines[0].split()[1])
+    rows = np.array([[float(x) for x in l.split()] for l in lines[1:]])
+    return manifolds, rows
+
+
+def test_dropin_program_compiles_against_the_facade():
+    _compile(None, link=False)
+
+
+@pytest.mark.gpu
+def test_dropin_program_matches_the_reference(tmp_path):
+    exe = str(tmp_path / "pyramid_b200")
+    _compile(exe, link=True)
+    out = subprocess.run([exe, "6", "60"], check=True, capture_output=True, text=True).stdout
+    m_mine, mine = _parse(out)
+    with open(GOLDEN) as f:
+        m_ref, ref = _parse(f.read())
+    assert m_mine == m_ref
+    assert np.array_equal(mine[:, 0], ref[:, 0])
+    for name, cols in (("p", slice(1, 4)), ("q", slice(4, 8)), ("v", slice(8, 11)), ("w", slice(11, 14))):
+        err = rel_err(mine[:, cols], ref[:, cols])
+        assert err <= TOL, f"{name} differs by {err}"
