@@ -249,7 +249,7 @@ TF_API int tf_world_body_steps(void* world, int64_t* body_steps);
 
 /* Forces and torques (3 floats per body, all bodies of the batch in body order) added to every awake
  * dynamic body for the next step only, as World::addForce / addTorque with wake = false
- * (include/twofold/world.h:449-451). Either pointer may be null. */
+ * (include/twofold/world.h:421-423). Either pointer may be null. */
 TF_API int tf_world_add_forces(void* world, const float* forces, const float* torques);
 
 /* Positions and rotations (x, y, z, w) of every body of the batch in body order, copied straight from the
