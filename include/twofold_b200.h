@@ -282,6 +282,29 @@ TF_API int tf_world_set_launch(void* world, int32_t kernel, int32_t threads, int
  * a whole-CTA world can stage, [5] bodies a warp's world can stage. */
 TF_API int tf_world_get_launch(void* world, int32_t kernel, uint32_t out[6]);
 
+/* ---- Candidate pairs without device allocation (no counterpart in the reference) ----
+ *
+ * The broadphase's candidate pairs for one world whose bodies have one shape each (shape index = body
+ * index), from device arrays the caller owns: lo and hi (n x 3 floats, the shapes' world bounds), grow (n
+ * floats, each body's growth for the step) and flags (n words of TF_PAIR_* bits). The pair rules are the
+ * step's (World::Impl::updateContacts, src/world.cpp:788-842, for single-shape bodies), and the result is
+ * what tf_world_candidates reports for such a world: keys min << 32 | max, sorted and unique. Up to
+ * `capacity` keys go to the device array `keys`; the device word `count` receives the number of unique
+ * keys (more than capacity when they did not all fit), or -1 when the pair tests found more than
+ * TF_NOALLOC_MAX_PAIRS keys before repeats were dropped (keys is then left as it was).
+ *
+ * It allocates nothing: its scratch is a fixed array in the library's device image. n above
+ * TF_NOALLOC_MAX_BODIES is refused with TF_E_CAPACITY. The work is queued on `stream` (a cudaStream_t; NULL
+ * for the default stream) on the current device and the call returns without waiting. The first call on a
+ * device looks up the scratch's address there (with that device current), so make it before any stream
+ * capture. Calls whose work overlaps on one device (other streams, other host threads) share the scratch and
+ * race; order them on one stream. */
+#define TF_NOALLOC_MAX_BODIES 4096
+#define TF_NOALLOC_MAX_PAIRS 32768
+enum tf_pair_flags { TF_PAIR_LIVE = 1u << 0, TF_PAIR_DYNAMIC = 1u << 1, TF_PAIR_MOVING = 1u << 2 };
+TF_API int tf_candidates_noalloc(const float* lo, const float* hi, const float* grow, const uint32_t* flags, int32_t n,
+                                 uint64_t* keys, int32_t capacity, int32_t* count, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -11,6 +11,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.environ.get("TWOFOLD_B200_LIB") or os.path.join(HERE, "libtwofold_b200.so")
 
 TF_OK = 0
+TF_E_INVALID, TF_E_CUDA, TF_E_CAPACITY, TF_E_NUMERIC, TF_E_TIMEOUT, TF_E_UNSUPPORTED = -1, -2, -3, -4, -5, -6
+TF_PAIR_LIVE, TF_PAIR_DYNAMIC, TF_PAIR_MOVING = 1, 2, 4
+TF_NOALLOC_MAX_BODIES, TF_NOALLOC_MAX_PAIRS = 4096, 32768
 TF_STATIC, TF_KINEMATIC, TF_DYNAMIC = 0, 1, 2
 TF_SPHERE, TF_BOX, TF_CYLINDER, TF_PRISM, TF_HULL, TF_HALFSPACE, TF_MESH = range(7)
 TF_LOCK_PLANAR = (1 << 2) | (1 << 3) | (1 << 4)
@@ -243,6 +246,7 @@ def _declare(lib):
         "tf_world_solver_counts": ([P, C.c_int32, P], C.c_int),
         "tf_world_set_launch": ([P, C.c_int32, C.c_int32, C.c_int32, C.c_int32], C.c_int),
         "tf_world_get_launch": ([P, C.c_int32, P], C.c_int),
+        "tf_candidates_noalloc": ([P, P, P, P, C.c_int32, P, C.c_int32, P, P], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name)
@@ -260,7 +264,7 @@ EXPORTED = [
     "tf_world_get_states", "tf_world_contacts", "tf_world_candidates", "tf_world_profile", "tf_world_awake_bodies",
     "tf_world_launch_count", "tf_world_elapsed_ms", "tf_world_body_steps", "tf_world_add_forces",
     "tf_world_read_poses", "tf_world_set_profiling", "tf_world_kernel_times", "tf_kernel_name",
-    "tf_world_work_counts", "tf_world_solver_counts", "tf_world_set_launch", "tf_world_get_launch",
+    "tf_world_work_counts", "tf_world_solver_counts", "tf_world_set_launch", "tf_world_get_launch", "tf_candidates_noalloc",
 ]
 
 

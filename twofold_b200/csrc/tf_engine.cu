@@ -90,6 +90,9 @@ Quat q4of(const float* p) { return { p[0], p[1], p[2], p[3] }; }
 
 }  // namespace
 
+// Records a failure from another translation unit of the library for tf_last_error.
+int noteError(int code, const std::string& msg) { return fail(code, msg); }
+
 class Engine {
 public:
     tf_settings settings{};
