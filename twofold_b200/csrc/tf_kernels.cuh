@@ -84,35 +84,40 @@ __device__ __forceinline__ uint32_t grabWarp(uint32_t* counter) {
     return __shfl_sync(0xffffffffu, v, 0);
 }
 
-// Calls body(group, world, slice, stage sizes) for every world of the batch, each exactly once.
+// Calls body(group, world, slice, stage sizes) for every world of the batch, each exactly once. The body has
+// one call site, so it is inlined and reads the kernel's parameters in place.
 template <class Body>
-__device__ void forWorlds(const Batch& B, int slotIndex, const Split& sp, unsigned char* smem, Body&& body) {
+__device__ __forceinline__ void forWorlds(const Batch& B, int slotIndex, const Split& sp, unsigned char* smem,
+                                          Body&& body) {
     __shared__ uint32_t s_world, s_big;
     const uint32_t nw = (uint32_t)B.nWorlds;
     uint32_t* counter = B.work + slotIndex;
-    const Group cta = makeGroup(blockDim.x);
+    bool warpMode = false;
     for (;;) {
-        if (threadIdx.x == 0) {
-            const uint32_t o = atomicAdd(counter, 1u);
-            s_world = o;
-            s_big = (o < nw && B.info[B.order[o]].bodyCount > sp.bigBodies) ? 1u : 0u;
+        uint32_t o;
+        if (!warpMode) {
+            if (threadIdx.x == 0) {
+                const uint32_t t = atomicAdd(counter, 1u);
+                s_world = t;
+                s_big = (t < nw && B.info[B.order[t]].bodyCount > sp.bigBodies) ? 1u : 0u;
+            }
+            __syncthreads();
+            o = s_world;
+            const uint32_t big = s_big;
+            __syncthreads();
+            if (o >= nw) { return; }
+            if (!big) {
+                // Every later world is small too: from here on each warp takes worlds on its own.
+                warpMode = true;
+                if ((threadIdx.x >> 5) != 0) { o = grabWarp(counter); }
+            }
+        } else {
+            o = grabWarp(counter);
         }
-        __syncthreads();
-        const uint32_t o = s_world, big = s_big;
-        __syncthreads();
         if (o >= nw) { return; }
-        if (big) {
-            body(cta, B.order[o], smem, sp.big);
-            continue;
-        }
-        const Group wg = makeGroup(32);
-        unsigned char* slice = smem + (size_t)wg.id * (sp.smemBytes / wg.count);
-        uint32_t mine = wg.id == 0 ? o : grabWarp(counter);
-        while (mine < nw) {
-            body(wg, B.order[mine], slice, sp.small);
-            mine = grabWarp(counter);
-        }
-        return;
+        const Group g = makeGroup(warpMode ? 32u : blockDim.x);
+        unsigned char* slice = warpMode && smem ? smem + (size_t)g.id * (sp.smemBytes / g.count) : smem;
+        body(g, B.order[o], slice, warpMode ? sp.small : sp.big);
     }
 }
 
@@ -873,7 +878,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_prepare(Batch B, StepParams P, Sp
             const DBody& a = B.bodies[c.bodyA];
             const DBody& b = B.bodies[c.bodyB];
             prepareContact(a, b, c);
-            makeContactAxes(a, b, c, B.axes + (size_t)(cf + act[x]) * kAxesPerContact);
+            makeContactAxes(axisBodyOf(a), axisBodyOf(b), c, B.axes + (size_t)(cf + act[x]) * kAxesPerContact);
             c.flags &= ~kCLaned;
             points += (uint32_t)c.count;
             const bool can = !(c.flags & kCPlanar) && !(c.rollingResistance > 0.0f);
@@ -989,13 +994,12 @@ __device__ void refreshContact(const Batch& B, const StepParams& P, DContact& c,
     carryImpulses(old, c, P.tol.speculative * P.tol.speculative);
 }
 
-// The solver state of one body, as the substep keeps it in registers: what warm start, solve and
-// restitution read and write. Field names match DBody so the same solver templates run on either.
+// The solver state of one body as a contact solved on its own (planar, rolling or past the last color) reads
+// and writes it. Field names match DBody so the same solver templates run on either.
 struct SBody {
     Vec3 v, w, dp;
     Quat dq;
-    Mat3 invMassWorld, invInertiaWorld;
-    float invMass;
+    Mat3 invInertiaWorld;
     uint32_t type, awake;
 };
 
@@ -1016,7 +1020,8 @@ struct PosBody {
     float kept;
 };
 
-constexpr int kSBodyWords = 33;
+// Staged words per body: v 0-2, w 3-5, dp 6-8, dq 9-12, type | awake << 8 in 13, inverse world inertia 14-22.
+constexpr int kSBodyWords = 23;
 
 // Where one world's solver state lives during a substep: shared memory (structure of arrays, stride words
 // apart) for worlds that fit, else the bodies in global memory.
@@ -1028,17 +1033,14 @@ struct SolverStore {
 
     __device__ __forceinline__ float& at(int word, uint32_t i) const { return s[word * stride + i]; }
 
-    __device__ SBody load(uint32_t i) const {
-        SBody b;
+    __device__ LanedBody loadLaned(uint32_t i) const {
+        LanedBody b;
         if (!staged) {
             const DBody& d = g[i];
             b.v = d.v;
             b.w = d.w;
             b.dp = d.dp;
             b.dq = d.dq;
-            b.invMassWorld = d.invMassWorld;
-            b.invInertiaWorld = d.invInertiaWorld;
-            b.invMass = d.invMass;
             b.type = d.type;
             b.awake = d.awake;
             return b;
@@ -1047,18 +1049,38 @@ struct SolverStore {
         b.w = { at(3, i), at(4, i), at(5, i) };
         b.dp = { at(6, i), at(7, i), at(8, i) };
         b.dq = { at(9, i), at(10, i), at(11, i), at(12, i) };
-        for (int r = 0; r < 3; ++r) {
-            b.invMassWorld.r[r] = { at(13 + 3 * r, i), at(14 + 3 * r, i), at(15 + 3 * r, i) };
-            b.invInertiaWorld.r[r] = { at(22 + 3 * r, i), at(23 + 3 * r, i), at(24 + 3 * r, i) };
-        }
-        b.invMass = at(31, i);
-        const uint32_t f = __float_as_uint(at(32, i));
+        const uint32_t f = __float_as_uint(at(13, i));
         b.type = f & 0xffu;
         b.awake = f >> 8;
         return b;
     }
 
-    __device__ void storeVW(uint32_t i, const SBody& b) const {
+    __device__ SBody load(uint32_t i) const {
+        SBody b;
+        if (!staged) {
+            const DBody& d = g[i];
+            b.v = d.v;
+            b.w = d.w;
+            b.dp = d.dp;
+            b.dq = d.dq;
+            b.invInertiaWorld = d.invInertiaWorld;
+            b.type = d.type;
+            b.awake = d.awake;
+            return b;
+        }
+        const LanedBody l = loadLaned(i);
+        b.v = l.v;
+        b.w = l.w;
+        b.dp = l.dp;
+        b.dq = l.dq;
+        b.type = l.type;
+        b.awake = l.awake;
+        for (int r = 0; r < 3; ++r) { b.invInertiaWorld.r[r] = { at(14 + 3 * r, i), at(15 + 3 * r, i), at(16 + 3 * r, i) }; }
+        return b;
+    }
+
+    template <class BodyT>
+    __device__ void storeVW(uint32_t i, const BodyT& b) const {
         if (!staged) {
             g[i].v = b.v;
             g[i].w = b.w;
@@ -1079,16 +1101,12 @@ struct SolverStore {
         at(3, i) = d.w.x, at(4, i) = d.w.y, at(5, i) = d.w.z;
         at(6, i) = d.dp.x, at(7, i) = d.dp.y, at(8, i) = d.dp.z;
         at(9, i) = d.dq.x, at(10, i) = d.dq.y, at(11, i) = d.dq.z, at(12, i) = d.dq.w;
+        at(13, i) = __uint_as_float(d.type | (d.awake << 8));
         for (int r = 0; r < 3; ++r) {
-            at(13 + 3 * r, i) = d.invMassWorld.r[r].x;
-            at(14 + 3 * r, i) = d.invMassWorld.r[r].y;
-            at(15 + 3 * r, i) = d.invMassWorld.r[r].z;
-            at(22 + 3 * r, i) = d.invInertiaWorld.r[r].x;
-            at(23 + 3 * r, i) = d.invInertiaWorld.r[r].y;
-            at(24 + 3 * r, i) = d.invInertiaWorld.r[r].z;
+            at(14 + 3 * r, i) = d.invInertiaWorld.r[r].x;
+            at(15 + 3 * r, i) = d.invInertiaWorld.r[r].y;
+            at(16 + 3 * r, i) = d.invInertiaWorld.r[r].z;
         }
-        at(31, i) = d.invMass;
-        at(32, i) = __uint_as_float(d.type | (d.awake << 8));
     }
 
     // Writes the fields a substep changes back to global memory.
@@ -1123,7 +1141,7 @@ struct SolverStore {
         b.linearProj = d.linearProj;
         b.angularProj = d.angularProj;
         for (int r = 0; r < 3; ++r) {
-            b.invInertiaWorld.r[r] = { at(22 + 3 * r, i), at(23 + 3 * r, i), at(24 + 3 * r, i) };
+            b.invInertiaWorld.r[r] = { at(14 + 3 * r, i), at(15 + 3 * r, i), at(16 + 3 * r, i) };
         }
         integrateVelocity(b, P);
         at(0, i) = b.v.x, at(1, i) = b.v.y, at(2, i) = b.v.z;
@@ -1210,7 +1228,8 @@ __global__ void __launch_bounds__(kMaxBlock) k_refresh(Batch B, StepParams P, Sp
             const uint32_t ci = act[x];
             if (!contactOk(B, wi, wc, ci, 26)) { continue; }
             const DContact& c = cs[ci];
-            makeContactAxes(B.bodies[c.bodyA], B.bodies[c.bodyB], c, B.axes + (size_t)(cf + ci) * kAxesPerContact);
+            makeContactAxes(axisBodyOf(B.bodies[c.bodyA]), axisBodyOf(B.bodies[c.bodyB]), c,
+                            B.axes + (size_t)(cf + ci) * kAxesPerContact);
         }
         g.sync();
     });
@@ -1240,23 +1259,39 @@ __global__ void __launch_bounds__(kMaxBlock) k_substep(Batch B, StepParams P, Sp
         const Axis* axes = B.axes + (size_t)cf * kAxesPerContact;
         // A laned contact's bodies are stored only where they move, so a static body shared by a color's
         // contacts is never written concurrently; a contact solved on its own stores both, as the reference does.
+        // Laned contacts (planar and rolling contacts never are) run the register-staged forms; contacts solved
+        // on their own run the general ones.
         auto warm = [&](uint32_t ci, bool laned) {
             if (!contactOk(B, wi, wc, ci, 10)) { return; }
-            const DContact& c = cs[ci];
+            DContact& c = cs[ci];
             const uint32_t ia = c.bodyA - base, ib = c.bodyB - base;
+            if (laned) {
+                LanedBody a = st.loadLaned(ia), b = st.loadLaned(ib);
+                warmStartLaned(a, b, c, axes + (size_t)ci * kAxesPerContact);
+                if (!anchored(a)) { st.storeVW(ia, a); }
+                if (!anchored(b)) { st.storeVW(ib, b); }
+                return;
+            }
             SBody a = st.load(ia), b = st.load(ib);
-            warmStartContact(a, b, c, laned, axes + (size_t)ci * kAxesPerContact);
-            if (!laned || !anchored(a)) { st.storeVW(ia, a); }
-            if (!laned || !anchored(b)) { st.storeVW(ib, b); }
+            warmStartContact(a, b, c, false, axes + (size_t)ci * kAxesPerContact);
+            st.storeVW(ia, a);
+            st.storeVW(ib, b);
         };
         auto solve = [&](uint32_t ci, bool bias, bool laned) {
             if (!contactOk(B, wi, wc, ci, 12)) { return; }
             DContact& c = cs[ci];
             const uint32_t ia = c.bodyA - base, ib = c.bodyB - base;
+            if (laned) {
+                LanedBody a = st.loadLaned(ia), b = st.loadLaned(ib);
+                solveLaned(a, b, c, P, bias, axes + (size_t)ci * kAxesPerContact);
+                if (!anchored(a)) { st.storeVW(ia, a); }
+                if (!anchored(b)) { st.storeVW(ib, b); }
+                return;
+            }
             SBody a = st.load(ia), b = st.load(ib);
             solveContact(a, b, c, P, bias, axes + (size_t)ci * kAxesPerContact);
-            if (!laned || !anchored(a)) { st.storeVW(ia, a); }
-            if (!laned || !anchored(b)) { st.storeVW(ib, b); }
+            st.storeVW(ia, a);
+            st.storeVW(ib, b);
         };
         const uint32_t* colored = B.colored + cf;
         const uint32_t* rest = B.rest + cf;

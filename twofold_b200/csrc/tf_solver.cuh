@@ -28,6 +28,17 @@ struct alignas(16) Axis {
 // (src/lanes.cpp:66-110, src/solver.cpp:43-50), and stored 3 per point: normal, tangent1, tangent2.
 constexpr int kAxesPerContact = 12;
 
+// The body fields an axis is built from, read once into registers before a contact's axes are written.
+struct AxisBody {
+    Mat3 invMassWorld, invInertiaWorld;
+    float invMass;
+};
+
+template <class BodyT>
+TF_HD AxisBody axisBodyOf(const BodyT& b) {
+    return { b.invMassWorld, b.invInertiaWorld, b.invMass };
+}
+
 template <class BodyT>
 TF_HD Axis makeAxis(const BodyT& a, const BodyT& b, const Vec3& ra, const Vec3& rb, const Vec3& d) {
     Axis x;
@@ -125,7 +136,7 @@ TF_HD void prepareContact(const DBody& a, const DBody& b, DContact& c) {
 // The axes of every point of a contact (src/solver.cpp:43-50), from the bodies' current world inverse mass
 // and inertia.
 template <class BodyT>
-TF_HD void makeContactAxes(const BodyT& a, const BodyT& b, const DContact& c, Axis* out) {
+TF_HD void makeContactAxes(const BodyT& a, const BodyT& b, const DContact& c, Axis* __restrict__ out) {
     for (int i = 0; i < c.count; ++i) {
         const DPoint& p = c.points[i];
         out[3 * i] = makeAxis(a, b, p.anchorA, p.anchorB, c.normal);
@@ -151,7 +162,7 @@ TF_HD void rebaseContact(const DBody& a, const DBody& b, DContact& c) {
 // (the anchored body's zero inverse mass leaves it unchanged). Contacts solved on their own run one at a
 // time, so the unmasked push never races.
 template <class BodyT>
-TF_HD void warmStartContact(BodyT& a, BodyT& b, const DContact& c, bool laned, const Axis* ax) {
+TF_HD void warmStartContact(BodyT& a, BodyT& b, const DContact& c, bool laned, const Axis* __restrict__ ax) {
     const bool moveA = !laned || !anchored(a), moveB = !laned || !anchored(b);
     for (int i = 0; i < c.count; ++i) {
         const DPoint& p = c.points[i];
@@ -200,7 +211,7 @@ TF_HD void resistTurning(BodyT& a, BodyT& b, DContact& c) {
 // The soft normal rows, then friction (forward in the biased pass, reverse in relax), then rolling
 // (src/solver.cpp:360-421).
 template <class BodyT>
-TF_HD void solveContact(BodyT& a, BodyT& b, DContact& c, const StepParams& P, bool useBias, const Axis* ax) {
+TF_HD void solveContact(BodyT& a, BodyT& b, DContact& c, const StepParams& P, bool useBias, const Axis* __restrict__ ax) {
     const bool moveA = !anchored(a), moveB = !anchored(b);
     const Softness soft = (!moveA || !moveB) ? P.staticSoft : P.contactSoft;
     const Vec3 dp = b.dp - a.dp;
@@ -246,10 +257,130 @@ TF_HD void solveContact(BodyT& a, BodyT& b, DContact& c, const StepParams& P, bo
     if (c.rollingResistance > 0.0f) { resistTurning(a, b, c); }
 }
 
+// The solver state a laned contact reads and writes: velocities, the substep's displacement and turn, and
+// the flags that say whether the body moves. Laned contacts are never planar or rolling, so they need no
+// inertia.
+struct LanedBody {
+    Vec3 v, w, dp;
+    Quat dq;
+    uint32_t type, awake;
+};
+
+// warmStartContact for a laned contact, its points' impulses read into registers before any body is pushed.
+template <class BodyT>
+TF_HD void warmStartLaned(BodyT& a, BodyT& b, const DContact& c, const Axis* __restrict__ ax) {
+    const bool moveA = !anchored(a), moveB = !anchored(b);
+    const int n = c.count;
+    const Vec3 t1 = c.tangent1, t2 = c.tangent2;
+    float ni[4] = { 0, 0, 0, 0 };
+    Vec3 ti[4] = {};
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        if (i < n) {
+            ni[i] = c.points[i].normalImpulse;
+            ti[i] = c.points[i].tangentImpulse;
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        if (i < n) {
+            const Axis xn = ax[3 * i], x1 = ax[3 * i + 1], x2 = ax[3 * i + 2];
+            pushMoving(a, b, xn, ni[i], moveA, moveB);
+            pushMoving(a, b, x1, dot(ti[i], t1), moveA, moveB);
+            pushMoving(a, b, x2, dot(ti[i], t2), moveA, moveB);
+        }
+    }
+}
+
+// solveContact for a laned contact (no rolling row): the same operations in the same order, with the points'
+// state read into registers first and written back once at the end.
+template <class BodyT>
+TF_HD void solveLaned(BodyT& a, BodyT& b, DContact& c, const StepParams& P, bool useBias, const Axis* __restrict__ ax) {
+    const bool moveA = !anchored(a), moveB = !anchored(b);
+    const Softness soft = (!moveA || !moveB) ? P.staticSoft : P.contactSoft;
+    const int n = c.count;
+    const Vec3 normal = c.normal, t1 = c.tangent1, t2 = c.tangent2;
+    const float friction = c.friction;
+    Vec3 rA[4] = {}, rB[4] = {}, ti[4] = {};
+    float adj[4] = { 0, 0, 0, 0 }, ni[4] = { 0, 0, 0, 0 }, mi[4] = { 0, 0, 0, 0 };
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        if (i < n) {
+            const DPoint& p = c.points[i];
+            rA[i] = p.anchorA;
+            rB[i] = p.anchorB;
+            adj[i] = p.adjustedSeparation;
+            ni[i] = p.normalImpulse;
+            mi[i] = p.maxNormalImpulse;
+            ti[i] = p.tangentImpulse;
+        }
+    }
+    const Vec3 dp = b.dp - a.dp;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        if (i < n) {
+            const Vec3 d = dp + turned(b, rB[i]) - turned(a, rA[i]);
+            const float sep = dot(d, normal) + adj[i];
+            float bias = 0.0f, massScale = 1.0f, impulseScale = 0.0f;
+            if (sep > 0.0f) {
+                bias = sep * P.invH;
+            } else if (useBias) {
+                bias = maxf(soft.biasRate * sep, -P.maxPushout);
+                massScale = soft.massScale;
+                impulseScale = soft.impulseScale;
+            }
+            const Axis x = ax[3 * i];
+            const float vn = speedAlong(a, b, normal, x);
+            float impulse = -x.mass * massScale * (vn + bias) - impulseScale * ni[i];
+            const float total = maxf(ni[i] + impulse, 0.0f);
+            impulse = total - ni[i];
+            ni[i] = total;
+            mi[i] = maxf(mi[i], impulse);
+            pushMoving(a, b, x, impulse, moveA, moveB);
+        }
+    }
+    auto row = [&](int i) {
+        const Axis x1 = ax[3 * i + 1], x2 = ax[3 * i + 2];
+        const float old1 = dot(ti[i], t1), old2 = dot(ti[i], t2);
+        float f1 = old1 - x1.mass * speedAlong(a, b, t1, x1);
+        float f2 = old2 - x2.mass * speedAlong(a, b, t2, x2);
+        const float limit = friction * ni[i];
+        const float mag = sqrtf(f1 * f1 + f2 * f2);
+        if (mag > limit) {
+            const float scale = mag > 0.0f ? limit / mag : 0.0f;
+            f1 *= scale;
+            f2 *= scale;
+        }
+        ti[i] = t1 * f1 + t2 * f2;
+        pushMoving(a, b, x1, f1 - old1, moveA, moveB);
+        pushMoving(a, b, x2, f2 - old2, moveA, moveB);
+    };
+    if (useBias) {
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            if (i < n) { row(i); }
+        }
+    } else {
+#pragma unroll
+        for (int i = 3; i >= 0; --i) {
+            if (i < n) { row(i); }
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        if (i < n) {
+            DPoint& p = c.points[i];
+            p.normalImpulse = ni[i];
+            p.maxNormalImpulse = mi[i];
+            p.tangentImpulse = ti[i];
+        }
+    }
+}
+
 // One restitution pass over the points that approached fast (src/solver.cpp:423-460, src/lanes.cpp:318-352),
 // pushing as warmStartContact does.
 template <class BodyT>
-TF_HD void restituteContact(BodyT& a, BodyT& b, DContact& c, const StepParams& P, bool laned, const Axis* ax) {
+TF_HD void restituteContact(BodyT& a, BodyT& b, DContact& c, const StepParams& P, bool laned, const Axis* __restrict__ ax) {
     if (c.restitution == 0.0f) { return; }
     const bool moveA = !laned || !anchored(a), moveB = !laned || !anchored(b);
     for (int i = 0; i < c.count; ++i) {
