@@ -54,6 +54,14 @@ struct Batch {
     uint32_t* mergePartB;
     uint32_t* mergeIdxB;
 
+    // Flat work lists, filled as the step goes, each item a (world, index within the world) pair. Candidate
+    // pairs, one list per pair class (candItemStride apart), for the pair collisions; the active contacts of
+    // worlds refreshed mid-step, one list per pair class of fast contacts and one more for the rest
+    // (contactItemStride apart). Their lengths are the work counters from kSlotCandItems and kSlotFastItems.
+    uint2* candItems;
+    uint2* contactItems;
+    uint32_t candItemStride, contactItemStride;
+
     uint32_t* work;        // per launch of a step, the next world to hand out (zeroed when the step starts)
     uint32_t* rowScratch;  // per shape, the candidate key sort's row counts
 

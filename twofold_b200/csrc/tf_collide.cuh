@@ -1033,8 +1033,21 @@ TF_HD void collideHalfSpace(const CollideCtx& cx, const Transform& xh, const DSh
     reduceManifold(pts, np, n, band, m, 0.0f, motion.fast);
 }
 
+// Pair classes, by shape kinds. A kernel instantiated for one class compiles only that class's collision
+// code; kClassAny compiles every path.
+enum PairClass : int { kClassAny = -1, kClassSpheres = 0, kClassSpherePoly = 1, kClassPlane = 2, kClassConvex = 3 };
+constexpr int kPairClasses = 4;
+
+TF_HD int pairClass(uint32_t ka, uint32_t kb) {
+    if (ka == kHalfSpace || kb == kHalfSpace) { return kClassPlane; }
+    if (ka == kSphere && kb == kSphere) { return kClassSpheres; }
+    if (ka == kSphere || kb == kSphere) { return kClassSpherePoly; }
+    return kClassConvex;
+}
+
 // Shape-kind dispatch (src/collide3d.cpp:1778-1811). Returns false for a pair this build cannot collide
-// (cylinders and meshes), leaving m empty.
+// (cylinders and meshes), leaving m empty. For a class other than kClassAny the pair must be of that class.
+template <int Cls = kClassAny>
 TF_HD bool collideShapes(const CollideCtx& cx, const DShape& a, const Transform& xa, const DShape& b,
                          const Transform& xb, float margin, const Motion& motion, Manifold& m, int reuseKind,
                          int reuseA, int reuseB) {
@@ -1045,19 +1058,35 @@ TF_HD bool collideShapes(const CollideCtx& cx, const DShape& a, const Transform&
     const uint32_t ka = a.kind, kb = b.kind;
     if (ka == kHalfSpace && kb == kHalfSpace) { return true; }
     if (ka == kMesh || kb == kMesh || ka == kCylinder || kb == kCylinder) { return false; }
-    if (ka == kHalfSpace) {
-        collideHalfSpace(cx, xa, b, xb, margin, cx.tol.linearSlop, motion, m);
-    } else if (kb == kHalfSpace) {
-        collideHalfSpace(cx, xb, a, xa, margin, cx.tol.linearSlop, motion.swapped(), m);
-        m.normal = -m.normal;
-    } else if (ka == kSphere && kb == kSphere) {
-        collideSpheres(xa.p, a.radius, xb.p, b.radius, margin, m);
-    } else if (ka == kSphere) {
-        collideSpherePoly(cx, b, xb, xa.p, a.radius, margin, m);
-        m.normal = -m.normal;
-    } else if (kb == kSphere) {
-        collideSpherePoly(cx, a, xa, xb.p, b.radius, margin, m);
-    } else {
+    if constexpr (Cls == kClassAny || Cls == kClassPlane) {
+        if (ka == kHalfSpace) {
+            collideHalfSpace(cx, xa, b, xb, margin, cx.tol.linearSlop, motion, m);
+            return true;
+        }
+        if (kb == kHalfSpace) {
+            collideHalfSpace(cx, xb, a, xa, margin, cx.tol.linearSlop, motion.swapped(), m);
+            m.normal = -m.normal;
+            return true;
+        }
+    }
+    if constexpr (Cls == kClassAny || Cls == kClassSpheres) {
+        if (ka == kSphere && kb == kSphere) {
+            collideSpheres(xa.p, a.radius, xb.p, b.radius, margin, m);
+            return true;
+        }
+    }
+    if constexpr (Cls == kClassAny || Cls == kClassSpherePoly) {
+        if (ka == kSphere) {
+            collideSpherePoly(cx, b, xb, xa.p, a.radius, margin, m);
+            m.normal = -m.normal;
+            return true;
+        }
+        if (kb == kSphere) {
+            collideSpherePoly(cx, a, xa, xb.p, b.radius, margin, m);
+            return true;
+        }
+    }
+    if constexpr (Cls == kClassAny || Cls == kClassConvex) {
         collideConvex(cx, a, xa, b, xb, margin, motion, m, reuseKind, reuseA, reuseB);
     }
     return true;

@@ -154,17 +154,20 @@ public:
         uint32_t threads = 256, bigBodies = 0, smemBytes = 0;
         bool chosen = false;
     };
-    // broadphase, narrowphase, wake, prepare, refresh, substep, finish
-    static constexpr int kKernels = 7;
+    // broadphase, narrowphase, wake, prepare, refresh, substep, finish, collide. Refresh and collide run one
+    // thread per work item over the whole grid; their shapes use only the thread count.
+    static constexpr int kKernels = 8;
     LaunchShape shapes[kKernels];
     Split splits[kKernels];
     int grids[kKernels] = {};
+    int flatGrids[9] = {};  // k_collide per pair class, then k_refresh for the light list and per pair class
     std::map<const void*, size_t> dynSmemLimit;
     bool kernelsConfigured = false;
     uint32_t maxWorldBodies = 0, maxWorldContacts = 0, medianWorldBodies = 0;
     std::vector<uint32_t> sortedSizes;  // world body counts, largest first
     bool laidOut = false;
     DevArray<uint32_t> dWork, dRowScratch;
+    DevArray<uint2> dCandItems, dContactItems;
     std::vector<uint32_t> minCandCap, minContactCap;
 
     // Host traffic staging and timing.
@@ -173,7 +176,7 @@ public:
     float lastElapsedMs = 0.0f;
     int64_t bodyStepsTotal = 0;
     bool profiling = false;
-    static constexpr int kKernelKinds = 7;  // broadphase, narrowphase, wake, prepare, refresh, substep, finish
+    static constexpr int kKernelKinds = 8;  // broadphase, narrowphase, wake, prepare, refresh, substep, finish, collide
     double kernelMs[kKernelKinds] = {};
     int64_t kernelLaunches[kKernelKinds] = {};
     std::vector<cudaEvent_t> eventPool;
@@ -687,6 +690,8 @@ public:
         TF_ALLOC(dMergeIdxA, ncon);
         TF_ALLOC(dMergeIdxB, ncon);
         TF_ALLOC(dWork, kSlotCount);
+        TF_ALLOC(dCandItems, ncand * kPairClasses);
+        TF_ALLOC(dContactItems, ncon * (kPairClasses + 1));
         TF_ALLOC(dRowScratch, ns);
         TF_ALLOC(dAbort, 1);
         TF_ALLOC(dDebug, 4);
@@ -820,6 +825,10 @@ public:
         B.mergePartB = dMergePartB.ptr;
         B.mergeIdxB = dMergeIdxB.ptr;
         B.work = dWork.ptr;
+        B.candItems = dCandItems.ptr;
+        B.contactItems = dContactItems.ptr;
+        B.candItemStride = (uint32_t)(dCandItems.n / kPairClasses);
+        B.contactItemStride = (uint32_t)(dContactItems.n / (kPairClasses + 1));
         B.rowScratch = dRowScratch.ptr;
         B.debug = dDebug.ptr;
         B.nPolys = (uint32_t)nPolys;
@@ -840,17 +849,31 @@ public:
         if (marks) { cudaEventRecord(marks[0], stream); }
         timed(0, rec, [&] { k_broadphase<<<grids[0], threads(0), smem(0), stream>>>(B, P, splits[0], serial); });
         if (marks) { cudaEventRecord(marks[1], stream); }
+        timed(7, rec, [&] {
+            k_collide<kClassSpheres><<<flatGrids[0], threads(7), 0, stream>>>(B, P, serial);
+            k_collide<kClassSpherePoly><<<flatGrids[1], threads(7), 0, stream>>>(B, P, serial);
+            k_collide<kClassPlane><<<flatGrids[2], threads(7), 0, stream>>>(B, P, serial);
+            k_collide<kClassConvex><<<flatGrids[3], threads(7), 0, stream>>>(B, P, serial);
+        });
         timed(1, rec, [&] { k_narrowphase<<<grids[1], threads(1), 0, stream>>>(B, P, splits[1], serial); });
         timed(2, rec, [&] { k_wake<<<grids[2], threads(2), 0, stream>>>(B, splits[2], serial); });
         if (marks) { cudaEventRecord(marks[2], stream); }
         timed(3, rec, [&] { k_prepare<<<grids[3], threads(3), smem(3), stream>>>(B, P, splits[3], serial); });
         for (int i = 0; i < P.substeps; ++i) {
-            if (i > 0) { timed(4, rec, [&] { k_refresh<<<grids[4], threads(4), 0, stream>>>(B, P, splits[4], i, serial); }); }
+            if (i > 0) {
+                timed(4, rec, [&] {
+                    k_refresh<kClassAny><<<flatGrids[4], threads(4), 0, stream>>>(B, P, i, serial);
+                    k_refresh<kClassSpheres><<<flatGrids[5], threads(4), 0, stream>>>(B, P, i, serial);
+                    k_refresh<kClassSpherePoly><<<flatGrids[6], threads(4), 0, stream>>>(B, P, i, serial);
+                    k_refresh<kClassPlane><<<flatGrids[7], threads(4), 0, stream>>>(B, P, i, serial);
+                    k_refresh<kClassConvex><<<flatGrids[8], threads(4), 0, stream>>>(B, P, i, serial);
+                });
+            }
             timed(5, rec, [&] { k_substep<<<grids[5], threads(5), smem(5), stream>>>(B, P, splits[5], i, serial); });
         }
         timed(6, rec, [&] { k_finish<<<grids[6], threads(6), smem(6), stream>>>(B, P, splits[6], serial); });
         if (marks) { cudaEventRecord(marks[3], stream); }
-        launches += 5 + 2 * P.substeps - 1;
+        launches += 9 + P.substeps + 5 * (P.substeps - 1);
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) { return fail(TF_E_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e)); }
         return TF_OK;
@@ -878,13 +901,16 @@ public:
         return TF_OK;
     }
 
+    static bool flatKernel(int k) { return k == 4 || k == 7; }
+    static constexpr uint32_t kMaxFlatBlock = 256;
+
     // Default launch shapes: batches of few worlds give every world a whole CTA (512 threads when a world
     // has more than 512 bodies); batches of many worlds give worlds of up to 96 bodies a warp each and the
     // larger ones the CTA. 64 KB of staging per CTA leaves room for three CTAs on an SM.
     LaunchShape defaultShape(int k) const {
         LaunchShape s;
         const bool many = worlds.size() >= (size_t)smCount * 4;
-        s.threads = !many && maxWorldBodies > 512 ? 512u : 256u;
+        s.threads = !many && maxWorldBodies > 512 && !flatKernel(k) ? 512u : 256u;
         s.bigBodies = many ? 96u : 0u;
         const bool stages = k == 0 || k == 3 || k == 5 || k == 6;
         s.smemBytes = stages ? 64u * 1024u : 0u;
@@ -921,8 +947,9 @@ public:
         int rc = configureKernels();
         if (rc != TF_OK) { return rc; }
         const void* fns[kKernels] = { (const void*)k_broadphase, (const void*)k_narrowphase, (const void*)k_wake,
-                                      (const void*)k_prepare,    (const void*)k_refresh,     (const void*)k_substep,
-                                      (const void*)k_finish };
+                                      (const void*)k_prepare,    (const void*)k_refresh<kClassAny>,
+                                      (const void*)k_substep,    (const void*)k_finish,
+                                      (const void*)k_collide<kClassConvex> };
         for (int k = 0; k < kKernels; ++k) {
             LaunchShape& sh = shapes[k];
             if (!sh.chosen) { sh = defaultShape(k); }
@@ -942,7 +969,21 @@ public:
                                                          std::greater<uint32_t>()) -
                                         sortedSizes.begin());
             const size_t needed = big + (sortedSizes.size() - big + warps - 1) / warps;
-            grids[k] = (int)std::max<size_t>(1, std::min<size_t>(needed, (size_t)smCount * perSm));
+            grids[k] = flatKernel(k) ? smCount * perSm
+                                     : (int)std::max<size_t>(1, std::min<size_t>(needed, (size_t)smCount * perSm));
+        }
+        // The flat kernels, one grid per instantiation: as many CTAs as fit on the device at once.
+        const void* flat[9] = { (const void*)k_collide<kClassSpheres>,    (const void*)k_collide<kClassSpherePoly>,
+                                (const void*)k_collide<kClassPlane>,      (const void*)k_collide<kClassConvex>,
+                                (const void*)k_refresh<kClassAny>,        (const void*)k_refresh<kClassSpheres>,
+                                (const void*)k_refresh<kClassSpherePoly>, (const void*)k_refresh<kClassPlane>,
+                                (const void*)k_refresh<kClassConvex> };
+        for (int f = 0; f < 9; ++f) {
+            int perSm = 0;
+            const int threads = (int)shapes[f < 4 ? 7 : 4].threads;
+            TF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, flat[f], threads, 0));
+            if (perSm < 1) { return fail(TF_E_INVALID, "launch shape does not fit on an SM"); }
+            flatGrids[f] = smCount * perSm;
         }
         return TF_OK;
     }
@@ -951,6 +992,9 @@ public:
     int setLaunch(int k, uint32_t threads, uint32_t bigBodies, uint32_t smemBytes) {
         if (k >= kKernels || threads < 32 || threads > (uint32_t)kMaxBlock || threads % 32 != 0) {
             return fail(TF_E_INVALID, "launch shape: kernel index or thread count out of range");
+        }
+        if (threads > kMaxFlatBlock && (k < 0 || flatKernel(k))) {
+            return fail(TF_E_INVALID, "launch shape: the refresh and collide kernels take at most 256 threads");
         }
         for (int i = 0; i < kKernels; ++i) {
             if (k >= 0 && i != k) { continue; }
@@ -1514,8 +1558,9 @@ TF_API int tf_world_kernel_times(void* h, float* ms, int64_t* launches, int32_t 
 }
 
 TF_API const char* tf_kernel_name(int32_t k) {
-    static const char* names[] = { "k_broadphase", "k_narrowphase", "k_wake", "k_prepare", "k_refresh", "k_substep", "k_finish" };
-    return (k >= 0 && k < 7) ? names[k] : "";
+    static const char* names[] = { "k_broadphase", "k_narrowphase", "k_wake", "k_prepare",
+                                   "k_refresh",    "k_substep",     "k_finish", "k_collide" };
+    return (k >= 0 && k < 8) ? names[k] : "";
 }
 
 TF_API int tf_world_work_counts(void* h, int64_t out[6]) {

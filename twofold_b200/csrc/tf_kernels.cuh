@@ -34,7 +34,10 @@ enum WorkSlot : int {
     kSlotRefresh = 4,                            // + substep index
     kSlotSubstep = kSlotRefresh + kMaxSubsteps,  // + substep index
     kSlotFinish = kSlotSubstep + kMaxSubsteps,
-    kSlotCount = kSlotFinish + 1
+    kSlotCandItems = kSlotFinish + 1,                    // + pair class: candidate items of that class
+    kSlotFastItems = kSlotCandItems + kPairClasses,       // + pair class: fast contacts of that class; + kPairClasses:
+                                                          // the other active contacts of refreshed worlds
+    kSlotCount = kSlotFastItems + kPairClasses + 1
 };
 
 // A group of threads that steps one world at a time: one warp, several warps, or the whole CTA.
@@ -313,9 +316,10 @@ __device__ uint32_t sortKeys(const Group& g, const Batch& B, const WorldInfo& wi
 // Body pairs whose grown bounds overlap, then their shapes (src/world.cpp:788-842), and half-space pairs
 // (:844-867); the keys are sorted and made unique (:868-869). A warp of the group takes one body and its
 // lanes the bodies after it. Bodies are staged in the group's shared slice when at most stageN of them.
-__global__ void __launch_bounds__(kMaxBlock) k_broadphase(Batch B, StepParams P, Split sp, int serial) {
+__global__ void __launch_bounds__(kMaxBlock) k_broadphase(const __grid_constant__ Batch B, const __grid_constant__ StepParams P, const __grid_constant__ Split sp, int serial) {
     extern __shared__ __align__(16) unsigned char s_raw[];
     __shared__ uint32_t s_count[kMaxGroups];
+    __shared__ uint32_t s_class[kMaxGroups][kPairClasses], s_classBase[kMaxGroups][kPairClasses];
     if (stepAborted(B, serial)) { return; }
     forWorlds(B, kSlotBroad, sp, s_raw, [&](const Group& g, uint32_t w, unsigned char* slice, const StageSizes& ss) {
         PairBody* staged = reinterpret_cast<PairBody*>(slice);
@@ -381,9 +385,33 @@ __global__ void __launch_bounds__(kMaxBlock) k_broadphase(Batch B, StepParams P,
             wc.candCount = unique;
             wc.candNeeded = max(wc.candNeeded, total);
         }
+        // The pairs join the flat list of their class: counted per class, a block of each list reserved for
+        // the world, then scattered into it.
+        uint32_t* cls = s_class[g.id];
+        if (g.tid < kPairClasses) { cls[g.tid] = 0; }
+        g.sync();
+        auto classOf = [&](uint32_t i) {
+            const uint64_t key = B.cand[wi.candFirst + i];
+            const uint32_t ka = B.shapes[wi.shapeFirst + (uint32_t)(key >> 32)].kind;
+            const uint32_t kb = B.shapes[wi.shapeFirst + (uint32_t)(key & 0xffffffffu)].kind;
+            return pairClass(ka, kb);
+        };
+        for (uint32_t i = g.tid; i < unique; i += g.size) { atomicAdd(&cls[classOf(i)], 1u); }
+        g.sync();
+        if (g.tid < kPairClasses) {
+            s_classBase[g.id][g.tid] = atomicAdd(B.work + kSlotCandItems + g.tid, cls[g.tid]);
+            cls[g.tid] = 0;
+        }
+        g.sync();
+        for (uint32_t i = g.tid; i < unique; i += g.size) {
+            const int c = classOf(i);
+            const uint32_t pos = s_classBase[g.id][c] + atomicAdd(&cls[c], 1u);
+            B.candItems[(size_t)c * B.candItemStride + pos] = make_uint2(w, i);
+        }
         g.sync();
     });
 }
+
 // ---------------------------------------------------------------------------------------------------------
 // Narrowphase and contact bookkeeping (src/world.cpp:872-1025).
 
@@ -459,6 +487,7 @@ __device__ __forceinline__ int nearestPoint(const DContact& old, const Vec3& loc
 
 // Collides one shape pair over dt as Impl::collidePair does for non-mesh, non-planar pairs
 // (src/world.cpp:505-533). Returns false for a pair this build cannot collide.
+template <int Cls = kClassAny>
 __device__ bool collidePair(const Batch& B, const StepParams& P, const DShape& sa, const DShape& sb, float dt,
                             Manifold& m, int reuseKind, int reuseA, int reuseB) {
     if (!TF_OK_INDEX(B, (sa.poly < 0 || (uint32_t)sa.poly < B.nPolys) && (sb.poly < 0 || (uint32_t)sb.poly < B.nPolys) &&
@@ -474,7 +503,7 @@ __device__ bool collidePair(const Batch& B, const StepParams& P, const DShape& s
     const Transform xa = ba.xf * sa.local;
     const Transform xb = bb.xf * sb.local;
     const Motion mo{ ba.v, ba.w, ba.com, bb.v, bb.w, bb.com, dt, travel > P.tol.speculative };
-    return collideShapes(B.cx, sa, xa, sb, xb, margin, mo, m, reuseKind, reuseA, reuseB);
+    return collideShapes<Cls>(B.cx, sa, xa, sb, xb, margin, mo, m, reuseKind, reuseA, reuseB);
 }
 
 // First index in [0, n) whose key is not below key.
@@ -493,6 +522,7 @@ __device__ __forceinline__ uint32_t lowerKey(const DContact* c, uint32_t n, uint
 
 // One candidate: keep and measure the old contact when the pair barely moved, else collide it and carry the
 // old impulses over (src/world.cpp:883-959).
+template <int Cls = kClassAny>
 __device__ void narrowOne(const Batch& B, const StepParams& P, const WorldInfo& wi, WorldCounts& wc, uint32_t i,
                           const DContact* old, uint32_t oldCount) {
     const uint64_t key = B.cand[wi.candFirst + i];
@@ -532,7 +562,7 @@ __device__ void narrowOne(const Batch& B, const StepParams& P, const WorldInfo& 
     } else {
         if (isPlanar(ba) || isPlanar(bb)) { atomicOr(&wc.flags, kDevUnsupported); }
         Manifold m;
-        if (!collidePair(B, P, sa, sb, P.dt, m, kFeatNone, -1, -1)) { atomicOr(&wc.flags, kDevUnsupported); }
+        if (!collidePair<Cls>(B, P, sa, sb, P.dt, m, kFeatNone, -1, -1)) { atomicOr(&wc.flags, kDevUnsupported); }
         if (m.count > 0) {
             DContact c{};
             c.key = key;
@@ -595,11 +625,27 @@ __device__ void narrowOne(const Batch& B, const StepParams& P, const WorldInfo& 
     B.stageUsed[wi.candFirst + i] = used;
 }
 
+// The candidate pairs of one class, over every world, one thread per pair (src/world.cpp:874-960); each
+// result lands in the pair's own staging slot, so pairs need no order among themselves.
+template <int Cls>
+__global__ void __launch_bounds__(256) k_collide(const __grid_constant__ Batch B, const __grid_constant__ StepParams P,
+                                                 int serial) {
+    if (stepAborted(B, serial)) { return; }
+    const uint32_t n = *(volatile uint32_t*)(B.work + kSlotCandItems + Cls);
+    const uint2* items = B.candItems + (size_t)Cls * B.candItemStride;
+    for (uint32_t item = blockIdx.x * blockDim.x + threadIdx.x; item < n; item += gridDim.x * blockDim.x) {
+        const uint2 it = items[item];
+        const WorldInfo wi = B.info[it.x];
+        WorldCounts& wc = B.counts[it.x];
+        narrowOne<Cls>(B, P, wi, wc, it.y, B.previous + wi.contactFirst, wc.contactCount);
+    }
+}
+
 __device__ __forceinline__ bool keyLess(uint64_t ka, uint32_t pa, uint64_t kb, uint32_t pb) {
     return ka != kb ? ka < kb : pa < pb;
 }
 
-__global__ void __launch_bounds__(kMaxBlock) k_narrowphase(Batch B, StepParams P, Split sp, int serial) {
+__global__ void __launch_bounds__(kMaxBlock) k_narrowphase(const __grid_constant__ Batch B, const __grid_constant__ StepParams P, const __grid_constant__ Split sp, int serial) {
     if (stepAborted(B, serial)) { return; }
     forWorlds(B, kSlotNarrow, sp, nullptr, [&](const Group& g, uint32_t w, unsigned char*, const StageSizes&) {
         const WorldInfo wi = B.info[w];
@@ -607,8 +653,6 @@ __global__ void __launch_bounds__(kMaxBlock) k_narrowphase(Batch B, StepParams P
         const uint32_t nc = wc.candCount;
         const uint32_t oldCount = wc.contactCount;
         const DContact* old = B.previous + wi.contactFirst;
-        for (uint32_t i = g.tid; i < nc; i += g.size) { narrowOne(B, P, wi, wc, i, old, oldCount); }
-        g.sync();
         const uint32_t cf = wi.contactFirst;
         const uint32_t nC = groupCompact(
             g, nc, [&](uint32_t i) { return B.stageUsed[wi.candFirst + i] != 0; },
@@ -690,7 +734,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_narrowphase(Batch B, StepParams P
 // Waking (src/world.cpp:705-735): sleeping bodies a moving body reached wake, and so does everything linked
 // to them by a contact with points. Runs on the group's first thread; it is rare.
 
-__global__ void __launch_bounds__(kMaxBlock) k_wake(Batch B, Split sp, int serial) {
+__global__ void __launch_bounds__(kMaxBlock) k_wake(const __grid_constant__ Batch B, const __grid_constant__ Split sp, int serial) {
     if (stepAborted(B, serial)) { return; }
     forWorlds(B, kSlotWake, sp, nullptr, [&](const Group& g, uint32_t w, unsigned char*, const StageSizes&) {
         if (g.tid != 0) { return; }
@@ -807,9 +851,10 @@ __device__ void bucketByColor(const Group& g, uint32_t n, const uint32_t* list, 
 
 // Coloring is staged in the group's shared slice (masks by body, endpoints by active contact) when the world
 // fits stageBodies bodies and stageContacts active contacts, else in the world's global scratch.
-__global__ void __launch_bounds__(kMaxBlock) k_prepare(Batch B, StepParams P, Split sp, int serial) {
+__global__ void __launch_bounds__(kMaxBlock) k_prepare(const __grid_constant__ Batch B, const __grid_constant__ StepParams P, const __grid_constant__ Split sp, int serial) {
     extern __shared__ __align__(16) unsigned char s_raw[];
     __shared__ uint32_t s_fast[kMaxGroups], s_fastSolid[kMaxGroups], s_points[kMaxGroups];
+    __shared__ uint32_t s_class[kMaxGroups][kPairClasses + 1], s_classBase[kMaxGroups][kPairClasses + 1];
     if (stepAborted(B, serial)) { return; }
     forWorlds(B, kSlotPrepare, sp, s_raw, [&](const Group& g, uint32_t w, unsigned char* slice, const StageSizes& ss) {
         const uint32_t stageBodies = ss.bodies, stageContacts = ss.contacts;
@@ -864,6 +909,31 @@ __global__ void __launch_bounds__(kMaxBlock) k_prepare(Batch B, StepParams P, Sp
             },
             [&](uint32_t i, uint32_t pos) { B.active[cf + pos] = i; });
         const uint32_t* act = B.active + cf;
+        // A world with fast contacts is refreshed between substeps: its fast contacts join the flat list of
+        // their pair class, its other active contacts the light list.
+        if (s_fast[g.id] > 0) {
+            uint32_t* cls = s_class[g.id];
+            if (g.tid <= kPairClasses) { cls[g.tid] = 0; }
+            g.sync();
+            auto listOf = [&](uint32_t x) {
+                const uint32_t ci = act[x];
+                if (!(B.cflags[cf + ci] & kFlagFast)) { return kPairClasses; }
+                return pairClass(B.shapes[cs[ci].shapeA].kind, B.shapes[cs[ci].shapeB].kind);
+            };
+            for (uint32_t x = g.tid; x < nActive; x += g.size) { atomicAdd(&cls[listOf(x)], 1u); }
+            g.sync();
+            if (g.tid <= kPairClasses) {
+                s_classBase[g.id][g.tid] = atomicAdd(B.work + kSlotFastItems + g.tid, cls[g.tid]);
+                cls[g.tid] = 0;
+            }
+            g.sync();
+            for (uint32_t x = g.tid; x < nActive; x += g.size) {
+                const int l = listOf(x);
+                const uint32_t pos = s_classBase[g.id][l] + atomicAdd(&cls[l], 1u);
+                B.contactItems[(size_t)l * B.contactItemStride + pos] = make_uint2(w, act[x]);
+            }
+            g.sync();
+        }
         const bool staged = wi.bodyCount <= stageBodies && nActive <= stageContacts;
         uint32_t* masks = staged ? reinterpret_cast<uint32_t*>(slice) : B.bodyColors + wi.bodyFirst;
         uint32_t* endA = staged ? masks + stageBodies : B.mergeIdxA + cf;
@@ -951,6 +1021,7 @@ __device__ __forceinline__ bool contactOk(const Batch& B, const WorldInfo& wi, c
 }
 
 // A fast pair collided again with the remaining time (src/world.cpp:1074-1138).
+template <int Cls = kClassAny>
 __device__ void refreshContact(const Batch& B, const StepParams& P, DContact& c, float remaining) {
     const DBody& a = B.bodies[c.bodyA];
     const DBody& b = B.bodies[c.bodyB];
@@ -960,7 +1031,7 @@ __device__ void refreshContact(const Batch& B, const StepParams& P, DContact& c,
     const Quat now = conjugate(a.xf.q) * b.xf.q, then = conjugate(a.q0) * b.q0;
     const bool little = fabsf(dot(now, then)) >= P.featureTurnCos;
     Manifold m;
-    collidePair(B, P, sa, sb, remaining, m, little ? c.featKind : kFeatNone, c.featA, c.featB);
+    collidePair<Cls>(B, P, sa, sb, remaining, m, little ? c.featKind : kFeatNone, c.featA, c.featB);
     if (m.count == 0) {
         c.count = 0;
         return;
@@ -1179,65 +1250,49 @@ struct SolverStore {
     }
 };
 
-// Fast pairs collided again before a substep (src/world.cpp:1658-1668): inverse mass refreshed, other
-// contacts rebased, dp and dq reset, fast contacts collided with the time left, every active contact's axes
-// built again. Does nothing in worlds without such pairs, so it can sit in a recorded graph before every
-// substep but the first.
-__global__ void __launch_bounds__(kMaxBlock) k_refresh(Batch B, StepParams P, Split sp, int sub, int serial) {
+// Whether the substep `sub` starts with a refresh of world wc: fast pairs are collided again at the middle
+// substep, pairs of solid bodies also at every other substep but the first (src/world.cpp:1658-1668).
+__device__ __forceinline__ bool refreshedAt(const WorldCounts& wc, int sub, int n) {
+    return sub > 0 && (sub == n / 2 ? wc.fastCount : wc.fastSolidCount) > 0;
+}
+
+// The contact half of a refresh, over the worlds refreshed at this substep: other contacts are rebased,
+// fast ones collided again with the time left, and every active contact's axes built again. One thread per
+// contact; the contacts come from one flat list, a pair class of fast contacts (Cls) or the other active
+// contacts (kClassAny). The body half runs in the substeps around it: the substep before updates the world
+// inverse inertia at its end, the substep after resets dp and dq before anything reads them.
+template <int Cls>
+__global__ void __launch_bounds__(256) k_refresh(const __grid_constant__ Batch B, const __grid_constant__ StepParams P,
+                                                 int sub, int serial) {
     if (stepAborted(B, serial)) { return; }
-    forWorlds(B, kSlotRefresh + sub, sp, nullptr, [&](const Group& g, uint32_t w, unsigned char*, const StageSizes&) {
-        const WorldInfo wi = B.info[w];
-        WorldCounts& wc = B.counts[w];
-        const int n = P.substeps;
-        const uint8_t againFlag = sub == n / 2 ? kFlagFast : kFlagFastSolid;
-        const uint32_t againCount = sub == n / 2 ? wc.fastCount : wc.fastSolidCount;
-        if (!(sub > 0 && againCount > 0)) { return; }
-        const uint32_t cf = wi.contactFirst;
-        DContact* cs = B.contacts + cf;
-        const uint32_t nActive = wc.activeCount;
-        const uint32_t* act = B.active + cf;
-        for (uint32_t i = g.tid; i < wi.bodyCount; i += g.size) {
-            DBody& b = B.bodies[wi.bodyFirst + i];
-            if (b.alive && b.type == kDynamic && b.awake) { updateInverseMass(b); }
+    const int n = P.substeps;
+    const uint8_t againFlag = sub == n / 2 ? kFlagFast : kFlagFastSolid;
+    const float remaining = (float)(n - sub) * P.h;
+    const int list = Cls == kClassAny ? kPairClasses : Cls;
+    const uint32_t items = *(volatile uint32_t*)(B.work + kSlotFastItems + list);
+    const uint2* its = B.contactItems + (size_t)list * B.contactItemStride;
+    for (uint32_t item = blockIdx.x * blockDim.x + threadIdx.x; item < items; item += gridDim.x * blockDim.x) {
+        const uint2 it = its[item];
+        const WorldCounts& wc = B.counts[it.x];
+        if (!refreshedAt(wc, sub, n)) { continue; }
+        const WorldInfo wi = B.info[it.x];
+        const uint32_t ci = it.y;
+        if (!contactOk(B, wi, wc, ci, 16)) { continue; }
+        DContact& c = B.contacts[wi.contactFirst + ci];
+        bool again = false;
+        if constexpr (Cls != kClassAny) { again = (B.cflags[wi.contactFirst + ci] & againFlag) != 0; }
+        if constexpr (Cls != kClassAny) {
+            if (again) { refreshContact<Cls>(B, P, c, remaining); }
         }
-        g.sync();
-        for (uint32_t x = g.tid; x < nActive; x += g.size) {
-            const uint32_t ci = act[x];
-            if (B.cflags[cf + ci] & againFlag) { continue; }
-            if (!contactOk(B, wi, wc, ci, 16)) { continue; }
-            DContact& c = cs[ci];
-            rebaseContact(B.bodies[c.bodyA], B.bodies[c.bodyB], c);
-        }
-        g.sync();
-        for (uint32_t i = g.tid; i < wi.bodyCount; i += g.size) {
-            DBody& b = B.bodies[wi.bodyFirst + i];
-            b.dp = zero3();
-            b.dq = qid();
-            b.qBase = b.xf.q;
-        }
-        g.sync();
-        const float remaining = (float)(n - sub) * P.h;
-        for (uint32_t x = g.tid; x < nActive; x += g.size) {
-            const uint32_t ci = act[x];
-            if (!(B.cflags[cf + ci] & againFlag)) { continue; }
-            if (!contactOk(B, wi, wc, ci, 14)) { continue; }
-            refreshContact(B, P, cs[ci], remaining);
-        }
-        g.sync();
-        for (uint32_t x = g.tid; x < nActive; x += g.size) {
-            const uint32_t ci = act[x];
-            if (!contactOk(B, wi, wc, ci, 26)) { continue; }
-            const DContact& c = cs[ci];
-            makeContactAxes(axisBodyOf(B.bodies[c.bodyA]), axisBodyOf(B.bodies[c.bodyB]), c,
-                            B.axes + (size_t)(cf + ci) * kAxesPerContact);
-        }
-        g.sync();
-    });
+        if (!again) { rebaseContact(B.bodies[c.bodyA], B.bodies[c.bodyB], c); }
+        makeContactAxes(axisBodyOf(B.bodies[c.bodyA]), axisBodyOf(B.bodies[c.bodyB]), c,
+                        B.axes + (size_t)(wi.contactFirst + ci) * kAxesPerContact);
+    }
 }
 
 // Integrate velocities, warm start, biased solve, integrate positions, relax (src/world.cpp:1669-1680). The
 // world's solver state is staged in the group's shared slice when it has at most stageN bodies.
-__global__ void __launch_bounds__(kMaxBlock) k_substep(Batch B, StepParams P, Split sp, int sub, int serial) {
+__global__ void __launch_bounds__(kMaxBlock) k_substep(const __grid_constant__ Batch B, const __grid_constant__ StepParams P, const __grid_constant__ Split sp, int sub, int serial) {
     extern __shared__ __align__(16) unsigned char s_raw[];
     if (stepAborted(B, serial)) { return; }
     forWorlds(B, kSlotSubstep + sub, sp, s_raw, [&](const Group& g, uint32_t w, unsigned char* sliceRaw, const StageSizes& ss) {
@@ -1249,6 +1304,16 @@ __global__ void __launch_bounds__(kMaxBlock) k_substep(Batch B, StepParams P, Sp
         DContact* cs = B.contacts + cf;
         const uint32_t nb = wi.bodyCount;
         const SolverStore st{ slice, stageN, nb <= stageN, B.bodies + wi.bodyFirst };
+        if (refreshedAt(wc, sub, P.substeps)) {
+            // The body half of this substep's refresh: a new base pose (src/world.cpp:1663-1666).
+            for (uint32_t i = g.tid; i < nb; i += g.size) {
+                DBody& d = st.g[i];
+                d.dp = zero3();
+                d.dq = qid();
+                d.qBase = d.xf.q;
+            }
+            g.sync();
+        }
         if (st.staged) {
             for (uint32_t i = g.tid; i < nb; i += g.size) { st.stage(i); }
             g.sync();
@@ -1326,6 +1391,14 @@ __global__ void __launch_bounds__(kMaxBlock) k_substep(Batch B, StepParams P, Sp
             for (uint32_t i = g.tid; i < nb; i += g.size) { st.unstage(i); }
             g.sync();
         }
+        if (sub + 1 < P.substeps && refreshedAt(wc, sub + 1, P.substeps)) {
+            // The next substep starts with a refresh, whose axes use the inverse inertia at the new pose
+            // (src/world.cpp:1660-1662).
+            for (uint32_t i = g.tid; i < nb; i += g.size) {
+                DBody& d = st.g[i];
+                if (d.alive && d.type == kDynamic && d.awake) { updateInverseMass(d); }
+            }
+        }
     });
 }
 
@@ -1347,7 +1420,7 @@ __device__ __forceinline__ uint32_t rootOf(const uint32_t* parent, uint32_t x) {
 
 // Union-find is staged in the group's shared slice (parent and island time by body, union pairs by contact)
 // when the world fits, else in its global scratch.
-__global__ void __launch_bounds__(kMaxBlock) k_finish(Batch B, StepParams P, Split sp, int serial) {
+__global__ void __launch_bounds__(kMaxBlock) k_finish(const __grid_constant__ Batch B, const __grid_constant__ StepParams P, const __grid_constant__ Split sp, int serial) {
     extern __shared__ __align__(16) unsigned char s_raw[];
     __shared__ uint32_t s_awake[kMaxGroups], s_islands[kMaxGroups], s_sweep[kMaxGroups];
     if (stepAborted(B, serial)) { return; }

@@ -157,7 +157,7 @@ class Batch:
         keys = ("active", "colors", "rest", "impact", "impact_colors", "impact_rest", "fast", "fast_solid")
         return dict(zip(keys, (int(x) for x in out)))
 
-    KERNELS = ("broadphase", "narrowphase", "wake", "prepare", "refresh", "substep", "finish")
+    KERNELS = ("broadphase", "narrowphase", "wake", "prepare", "refresh", "substep", "finish", "collide")
 
     def set_launch(self, kernel, threads, big_bodies, smem_bytes):
         """Launch shape of one kernel (name or index; None for all): threads per CTA, the world size above
