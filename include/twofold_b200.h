@@ -272,8 +272,22 @@ TF_API int tf_world_work_counts(void* world, int64_t out[6]);
  * contacts solved one at a time, [6] fast contacts, [7] fast contacts between solid bodies. */
 TF_API int tf_world_solver_counts(void* world, int32_t w, int32_t out[8]);
 
+/* Snapshots of the dynamic device state (bodies, shape bounds, contacts with their impulses, sleep and wake
+ * bookkeeping) in numbered slots, copied on the device without a host round trip. A snapshot can be put back
+ * until the batch is laid out again (a body or shape added, or a device list grown), after which
+ * tf_world_restore_state returns TF_E_INVALID. No counterpart in the reference, where copying a World is
+ * the snapshot (include/twofold/world.h:366-369). */
+TF_API int tf_world_save_state(void* world, int32_t slot);
+TF_API int tf_world_restore_state(void* world, int32_t slot);
+
+/* Times candidate launch shapes for every kernel on the batch's current state (trial_steps steps per
+ * candidate, the state put back after each) and keeps the fastest; the batch ends in the state it started
+ * in. out, when non-null, receives 8 x 3 words: threads, big-world threshold and shared bytes per kernel,
+ * in tf_world_set_launch's kernel order (plus 7 = the pair collisions). No counterpart in the reference. */
+TF_API int tf_world_autotune(void* world, float dt, int32_t trial_steps, uint32_t* out);
+
 /* Launch shape of one kernel (0 broadphase, 1 narrowphase, 2 wake, 3 prepare, 4 refresh, 5 substep,
- * 6 finish; -1 every kernel): threads per CTA (a multiple of 32, at most 512), the world size in bodies
+ * 6 finish, 7 pair collisions; -1 every kernel): threads per CTA (a multiple of 32, at most 512), the world size in bodies
  * above which a world is stepped by a whole CTA (smaller worlds take one warp each), and the shared memory
  * a CTA stages worlds in (clamped to what the device allows). Takes effect at the next step. No
  * counterpart in the reference, which steps each world on one host thread; the autotuner uses it. */

@@ -165,6 +165,21 @@ public:
     bool kernelsConfigured = false;
     uint32_t maxWorldBodies = 0, maxWorldContacts = 0, medianWorldBodies = 0;
     std::vector<uint32_t> sortedSizes;  // world body counts, largest first
+    uint64_t layoutGen = 0;              // bumped by every layout; snapshots hold only within one
+
+    // A copy of the dynamic device state a step reads: bodies, shapes (their bounds), the current contact
+    // list, the per-world counts and the per-body wake marks. Valid while the layout it was taken in stands.
+    struct Snapshot {
+        DevArray<DBody> bodies;
+        DevArray<DShape> shapes;
+        DevArray<DContact> contacts;
+        DevArray<WorldCounts> counts;
+        DevArray<uint8_t> struck, wakeMark;
+        int cur = 0;
+        uint64_t layoutGen = 0;
+        int64_t bodyStepsTotal = 0, bodyStepsBase = 0;
+    };
+    std::map<int, std::unique_ptr<Snapshot>> snapshots;
     bool laidOut = false;
     DevArray<uint32_t> dWork, dRowScratch;
     DevArray<uint2> dCandItems, dContactItems;
@@ -515,6 +530,7 @@ public:
     }
 
     int layout() {
+        ++layoutGen;
         bodyStepsBase = bodyStepsTotal;
         dropGraphs();
         const size_t nw = worlds.size();
@@ -1013,6 +1029,151 @@ public:
         out[3] = (uint32_t)grids[k];
         out[4] = splits[k].big.bodies;
         out[5] = splits[k].small.bodies;
+        return TF_OK;
+    }
+
+    template <class T>
+    int copyArray(DevArray<T>& to, const DevArray<T>& from) {
+        int rc = to.alloc(from.n);
+        if (rc != TF_OK) { return rc; }
+        TF_CUDA(cudaMemcpyAsync(to.ptr, from.ptr, from.n * sizeof(T), cudaMemcpyDeviceToDevice, stream));
+        return TF_OK;
+    }
+
+    // Copies the dynamic device state into snapshot `slot` (stream-ordered; nothing waits).
+    int saveState(int slot) {
+        TF_CUDA(cudaSetDevice(device));
+        int rc = prepareDevice();
+        if (rc != TF_OK) { return rc; }
+        std::unique_ptr<Snapshot>& sp = snapshots[slot];
+        if (!sp) { sp.reset(new Snapshot()); }
+        Snapshot& S = *sp;
+        if ((rc = copyArray(S.bodies, dBodies)) != TF_OK) { return rc; }
+        if ((rc = copyArray(S.shapes, dShapes)) != TF_OK) { return rc; }
+        if ((rc = copyArray(S.contacts, dContacts[cur])) != TF_OK) { return rc; }
+        if ((rc = copyArray(S.counts, dCounts)) != TF_OK) { return rc; }
+        if ((rc = copyArray(S.struck, dStruck)) != TF_OK) { return rc; }
+        if ((rc = copyArray(S.wakeMark, dWakeMark)) != TF_OK) { return rc; }
+        S.cur = cur;
+        S.layoutGen = layoutGen;
+        S.bodyStepsTotal = bodyStepsTotal;
+        S.bodyStepsBase = bodyStepsBase;
+        return TF_OK;
+    }
+
+    // Puts snapshot `slot` back. Refused when the batch was laid out again since (a list grew, or a body or
+    // shape was added): the snapshot's arrays no longer match the device's.
+    int restoreState(int slot) {
+        TF_CUDA(cudaSetDevice(device));
+        auto it = snapshots.find(slot);
+        if (it == snapshots.end()) { return fail(TF_E_INVALID, "restore: no snapshot in that slot"); }
+        Snapshot& S = *it->second;
+        if (S.layoutGen != layoutGen || layoutDirty) {
+            return fail(TF_E_INVALID, "restore: the batch was laid out again since the snapshot was taken");
+        }
+        cur = S.cur;
+        int rc;
+        if ((rc = copyArray(dBodies, S.bodies)) != TF_OK) { return rc; }
+        if ((rc = copyArray(dShapes, S.shapes)) != TF_OK) { return rc; }
+        if ((rc = copyArray(dContacts[cur], S.contacts)) != TF_OK) { return rc; }
+        if ((rc = copyArray(dCounts, S.counts)) != TF_OK) { return rc; }
+        if ((rc = copyArray(dStruck, S.struck)) != TF_OK) { return rc; }
+        if ((rc = copyArray(dWakeMark, S.wakeMark)) != TF_OK) { return rc; }
+        bodyStepsTotal = S.bodyStepsTotal;
+        bodyStepsBase = S.bodyStepsBase;
+        hostFresh = false;
+        onDevice = true;
+        bodiesDirty = false;
+        return TF_OK;
+    }
+
+    // Times candidate launch shapes on the batch's current state and keeps the fastest per kernel. Every
+    // candidate gives the same results (the pipeline's output does not depend on launch shapes), so each
+    // trial runs every kernel with its own next candidate and reads all kernel times at once. The state is
+    // put back after every trial and at the end. out (8 x 3: threads, big-world threshold, shared bytes per
+    // kernel) receives the choice when non-null.
+    int autotune(float dt, int trialSteps, uint32_t* out) {
+        if (!(dt > 0.0f) || !std::isfinite(dt) || trialSteps <= 0) { return fail(TF_E_INVALID, "autotune: bad dt or steps"); }
+        TF_CUDA(cudaSetDevice(device));
+        int rc = prepareDevice();
+        if (rc != TF_OK) { return rc; }
+        if ((rc = pull()) != TF_OK) { return rc; }
+        const std::vector<HostWorld> saved = worlds;  // for a trial that grows a list and lays out again
+        const int64_t savedTotal = bodyStepsTotal, savedBase = bodyStepsBase;
+        const int kSlot = -1;
+        if ((rc = saveState(kSlot)) != TF_OK) { return rc; }
+        std::vector<LaunchShape> cands[kKernels];
+        for (int k = 0; k < kKernels; ++k) {
+            if (flatKernel(k)) {
+                for (uint32_t t : { 64u, 128u, 256u }) { cands[k].push_back(LaunchShape{ t, 0u, 0u, true }); }
+                continue;
+            }
+            const bool stages = k == 0 || k == 3 || k == 5 || k == 6;
+            for (uint32_t t : { 128u, 256u, 512u }) {
+                for (uint32_t big : { 0u, 32u, 64u, 128u, 256u }) {
+                    if (stages) {
+                        for (uint32_t sm : { 48u * 1024u, 96u * 1024u }) { cands[k].push_back(LaunchShape{ t, big, sm, true }); }
+                    } else {
+                        cands[k].push_back(LaunchShape{ t, big, 0u, true });
+                    }
+                }
+            }
+        }
+        size_t trials = 0;
+        for (auto& c : cands) { trials = std::max(trials, c.size()); }
+        double best[kKernels];
+        LaunchShape chosen[kKernels];
+        for (int k = 0; k < kKernels; ++k) {
+            best[k] = 1e300;
+            chosen[k] = shapes[k];
+        }
+        const bool wasProfiling = profiling;
+        profiling = true;
+        for (size_t t = 0; t < trials && rc == TF_OK; ++t) {
+            for (int k = 0; k < kKernels; ++k) { shapes[k] = cands[k][t % cands[k].size()]; }
+            dropGraphs();
+            if ((rc = configureLaunches()) != TF_OK) { break; }
+            if (restoreState(kSlot) != TF_OK) {
+                // A trial grew a list: lay the saved state out again and take the snapshot anew.
+                worlds = saved;
+                hostFresh = true;
+                layoutDirty = true;
+                if ((rc = prepareDevice()) != TF_OK || (rc = saveState(kSlot)) != TF_OK) { break; }
+            }
+            if ((rc = step(dt, 1)) != TF_OK) { break; }
+            for (int k = 0; k < kKernelKinds; ++k) {
+                kernelMs[k] = 0.0;
+                kernelLaunches[k] = 0;
+            }
+            if ((rc = step(dt, trialSteps)) != TF_OK) { break; }
+            for (int k = 0; k < kKernels; ++k) {
+                if (t < cands[k].size() && kernelMs[k] < best[k]) {
+                    best[k] = kernelMs[k];
+                    chosen[k] = shapes[k];
+                }
+            }
+        }
+        profiling = wasProfiling;
+        for (int k = 0; k < kKernels; ++k) { shapes[k] = chosen[k]; }
+        dropGraphs();
+        const int rcShape = configureLaunches();
+        if (restoreState(kSlot) != TF_OK) {
+            worlds = saved;
+            hostFresh = true;
+            layoutDirty = true;
+        }
+        bodyStepsTotal = savedTotal;
+        bodyStepsBase = savedBase;
+        snapshots.erase(kSlot);
+        if (rc != TF_OK) { return rc; }
+        if (rcShape != TF_OK) { return rcShape; }
+        if (out) {
+            for (int k = 0; k < kKernels; ++k) {
+                out[3 * k] = shapes[k].threads;
+                out[3 * k + 1] = shapes[k].bigBodies;
+                out[3 * k + 2] = shapes[k].smemBytes;
+            }
+        }
         return TF_OK;
     }
 
@@ -1582,6 +1743,23 @@ TF_API int tf_world_launch_count(void* h, int64_t* launches) {
     if (!h || !launches) { return tfb::fail(TF_E_INVALID, "tf_world_launch_count: null"); }
     *launches = E(h)->launches;
     return TF_OK;
+}
+
+TF_API int tf_world_save_state(void* h, int32_t slot) {
+    if (!h) { return tfb::fail(TF_E_INVALID, "tf_world_save_state: null"); }
+    if (slot < 0) { return tfb::fail(TF_E_INVALID, "tf_world_save_state: negative slot"); }
+    return E(h)->saveState(slot);
+}
+
+TF_API int tf_world_restore_state(void* h, int32_t slot) {
+    if (!h) { return tfb::fail(TF_E_INVALID, "tf_world_restore_state: null"); }
+    if (slot < 0) { return tfb::fail(TF_E_INVALID, "tf_world_restore_state: negative slot"); }
+    return E(h)->restoreState(slot);
+}
+
+TF_API int tf_world_autotune(void* h, float dt, int32_t trial_steps, uint32_t* out) {
+    if (!h) { return tfb::fail(TF_E_INVALID, "tf_world_autotune: null"); }
+    return E(h)->autotune(dt, trial_steps, out);
 }
 
 TF_API int tf_world_solver_counts(void* h, int32_t w, int32_t out[8]) {

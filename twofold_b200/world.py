@@ -165,6 +165,20 @@ class Batch:
         k = -1 if kernel is None else (self.KERNELS.index(kernel) if isinstance(kernel, str) else int(kernel))
         abi.check(self.lib.tf_world_set_launch(self.h, k, int(threads), int(big_bodies), int(smem_bytes)), self.lib)
 
+    def save_state(self, slot=0):
+        """Snapshot of the batch's dynamic state on the device."""
+        abi.check(self.lib.tf_world_save_state(self.h, slot), self.lib)
+
+    def restore_state(self, slot=0):
+        abi.check(self.lib.tf_world_restore_state(self.h, slot), self.lib)
+
+    def autotune(self, dt, trial_steps=2):
+        """Picks each kernel's launch shape by timing candidates on the current state (left as it was).
+        Returns {kernel: (threads, big-world threshold, shared bytes)}."""
+        out = np.zeros(3 * len(self.KERNELS), np.uint32)
+        abi.check(self.lib.tf_world_autotune(self.h, C.c_float(dt), trial_steps, out.ctypes.data), self.lib)
+        return {k: tuple(int(x) for x in out[3 * i:3 * i + 3]) for i, k in enumerate(self.KERNELS)}
+
     def launch(self, kernel):
         """The launch shape in use for one kernel, after the batch was laid out on the device."""
         k = self.KERNELS.index(kernel) if isinstance(kernel, str) else int(kernel)
