@@ -272,6 +272,31 @@ TF_API int tf_world_work_counts(void* world, int64_t out[6]);
  * contacts solved one at a time, [6] fast contacts, [7] fast contacts between solid bodies. */
 TF_API int tf_world_solver_counts(void* world, int32_t w, int32_t out[8]);
 
+/* ---- Differentiation (no counterpart in the reference) ----
+ *
+ * tf_tape_record steps the batch n_steps times by dt (as tf_world_step does) and records what each step's
+ * solve saw: the contacts with their anchors, frames, adjusted separations and warm-start impulses, the
+ * color lists, and the awake bodies. The recorded run is the differentiable model: the substepped soft solve
+ * and integration with each step's contact set held fixed (no mid-step collision; speed limits inactive).
+ *
+ * tf_adjoint_forward runs the model from the recorded initial state in float (precision 32) or double (64)
+ * and writes the final state: 13 doubles per body of the batch, center of mass (3), rotation (x, y, z, w),
+ * linear and angular velocity. initial_state (same layout), mass (per body) and friction (per shape of the
+ * batch) replace the recorded values when non-null; a body's local inverse inertia scales with 1/mass.
+ * It keeps the state at every step boundary on the device.
+ *
+ * tf_adjoint_backward takes d loss / d final state (13 per body) and writes d loss / d initial state,
+ * d loss / d mass and d loss / d friction (any output may be null). It recomputes each step from its
+ * checkpoint and walks it in reverse, in the precision of the last forward run.
+ *
+ * tf_adjoint_elapsed_ms: device time of the last forward and backward runs, ms[0] and ms[1]. */
+TF_API int tf_tape_record(void* world, float dt, int32_t n_steps);
+TF_API int tf_adjoint_forward(void* world, int32_t precision, const double* initial_state, const double* mass,
+                              const double* friction, double* final_state);
+TF_API int tf_adjoint_backward(void* world, const double* grad_final, double* grad_initial, double* grad_mass,
+                               double* grad_friction);
+TF_API int tf_adjoint_elapsed_ms(void* world, float ms[2]);
+
 /* Snapshots of the dynamic device state (bodies, shape bounds, contacts with their impulses, sleep and wake
  * bookkeeping) in numbered slots, copied on the device without a host round trip. A snapshot can be put back
  * until the batch is laid out again (a body or shape added, or a device list grown), after which

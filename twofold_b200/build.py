@@ -12,7 +12,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libtwofold_b200.so")
 
-SOURCES = [os.path.join(CSRC, "tf_engine.cu"), os.path.join(CSRC, "tf_noalloc.cu")]
+SOURCES = [os.path.join(CSRC, f) for f in ("tf_engine.cu", "tf_noalloc.cu", "tf_adjoint.cu")]
 HEADERS = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))] + [
     os.path.join(ROOT, "include", "twofold_b200.h")]
 

@@ -1,0 +1,1362 @@
+// The differentiable model of a recorded run and its hand-written adjoint, in float and in double.
+//
+// The model is the substepped soft solve with integration (src/world.cpp:1649-1684, src/solver.cpp:319-460 in
+// the reference) with each step's contact set held fixed: the contacts, their anchors, frames, adjusted
+// separations and warm-start impulses, the color lists and the awake flags come from the recorded step
+// (tf_tape.h). What flows through it: the bodies' centers of mass, rotations and velocities, the masses
+// (inverse mass, and local inverse inertia scaling with it) and the shapes' friction (a contact's friction is
+// sqrt(friction A * friction B), src/world.cpp:39-40, 951-955). Contacts keep their step-start anchors for
+// the whole step (no mid-step collision) and the speed limits are taken as inactive.
+//
+// Forward: one warp per world walks every step, writing the state at each step boundary (the checkpoints).
+// Backward: for each step from the last, the warp runs the step again from its checkpoint, logging the
+// inputs of every contact solve and integration, then walks the same operations in reverse, carrying
+// adjoints of the state back to the step's start and adding up the adjoints of masses and frictions.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/twofold_b200.h"
+#include "tf_tape.h"
+
+namespace tfb {
+
+int noteError(int code, const std::string& msg);
+
+namespace adj {
+
+// ---------------------------------------------------------------------------------------------------------
+// Small vector algebra in T.
+
+template <class T>
+struct V3 {
+    T x, y, z;
+};
+template <class T>
+struct Q4 {
+    T x, y, z, w;
+};
+template <class T>
+struct M3 {
+    V3<T> r[3];
+};
+
+template <class T> __device__ __forceinline__ V3<T> operator+(V3<T> a, V3<T> b) { return { a.x + b.x, a.y + b.y, a.z + b.z }; }
+template <class T> __device__ __forceinline__ V3<T> operator-(V3<T> a, V3<T> b) { return { a.x - b.x, a.y - b.y, a.z - b.z }; }
+template <class T> __device__ __forceinline__ V3<T> operator*(V3<T> a, T s) { return { a.x * s, a.y * s, a.z * s }; }
+template <class T> __device__ __forceinline__ T dot(V3<T> a, V3<T> b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+template <class T> __device__ __forceinline__ V3<T> cross(V3<T> a, V3<T> b) {
+    return { a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x };
+}
+template <class T> __device__ __forceinline__ V3<T> mul(const M3<T>& m, V3<T> v) { return { dot(m.r[0], v), dot(m.r[1], v), dot(m.r[2], v) }; }
+template <class T> __device__ __forceinline__ void addOuter(M3<T>& m, V3<T> a, V3<T> b, T s) {
+    m.r[0] = m.r[0] + b * (a.x * s);
+    m.r[1] = m.r[1] + b * (a.y * s);
+    m.r[2] = m.r[2] + b * (a.z * s);
+}
+template <class T> __device__ __forceinline__ M3<T> zeroM() { return { { { 0, 0, 0 }, { 0, 0, 0 }, { 0, 0, 0 } } }; }
+template <class T> __device__ __forceinline__ V3<T> zeroV() { return { 0, 0, 0 }; }
+template <class T> __device__ __forceinline__ M3<T> transposeM(const M3<T>& m) {
+    return { { { m.r[0].x, m.r[1].x, m.r[2].x }, { m.r[0].y, m.r[1].y, m.r[2].y }, { m.r[0].z, m.r[1].z, m.r[2].z } } };
+}
+template <class T> __device__ __forceinline__ M3<T> mmul(const M3<T>& a, const M3<T>& b) {
+    const M3<T> bt = transposeM(b);
+    M3<T> o;
+    for (int i = 0; i < 3; ++i) { o.r[i] = { dot(a.r[i], bt.r[0]), dot(a.r[i], bt.r[1]), dot(a.r[i], bt.r[2]) }; }
+    return o;
+}
+template <class T> __device__ __forceinline__ M3<T> madd(const M3<T>& a, const M3<T>& b) {
+    return { { a.r[0] + b.r[0], a.r[1] + b.r[1], a.r[2] + b.r[2] } };
+}
+
+// Hamilton product and its adjoints with respect to each factor.
+template <class T> __device__ __forceinline__ Q4<T> qmul(Q4<T> a, Q4<T> b) {
+    return { a.w * b.x + a.x * b.w + a.y * b.z - a.z * b.y, a.w * b.y - a.x * b.z + a.y * b.w + a.z * b.x,
+             a.w * b.z + a.x * b.y - a.y * b.x + a.z * b.w, a.w * b.w - a.x * b.x - a.y * b.y - a.z * b.z };
+}
+template <class T> __device__ __forceinline__ Q4<T> qmulAdjA(Q4<T> g, Q4<T> b) {
+    return { g.x * b.w - g.y * b.z + g.z * b.y - g.w * b.x, g.x * b.z + g.y * b.w - g.z * b.x - g.w * b.y,
+             -g.x * b.y + g.y * b.x + g.z * b.w - g.w * b.z, g.x * b.x + g.y * b.y + g.z * b.z + g.w * b.w };
+}
+template <class T> __device__ __forceinline__ Q4<T> qmulAdjB(Q4<T> g, Q4<T> a) {
+    return { g.x * a.w + g.y * a.z - g.z * a.y - g.w * a.x, -g.x * a.z + g.y * a.w + g.z * a.x - g.w * a.y,
+             g.x * a.y - g.y * a.x + g.z * a.w - g.w * a.z, g.x * a.x + g.y * a.y + g.z * a.z + g.w * a.w };
+}
+template <class T> __device__ __forceinline__ Q4<T> conj(Q4<T> q) { return { -q.x, -q.y, -q.z, q.w }; }
+template <class T> __device__ __forceinline__ Q4<T> qadd(Q4<T> a, Q4<T> b) { return { a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w }; }
+
+// rotate(q, v) = v + w t + u x t with t = 2 u x v (u the vector part), as math.h writes it.
+template <class T> __device__ __forceinline__ V3<T> rotate(Q4<T> q, V3<T> v) {
+    const V3<T> u{ q.x, q.y, q.z };
+    const V3<T> t = cross(u, v) * T(2);
+    return v + t * q.w + cross(u, t);
+}
+// Adjoint of rotate: given g = d/d(result), adds d/dq to qg and returns d/dv.
+template <class T> __device__ __forceinline__ V3<T> rotateAdj(Q4<T> q, V3<T> v, V3<T> g, Q4<T>& qg) {
+    const V3<T> u{ q.x, q.y, q.z };
+    const V3<T> t = cross(u, v) * T(2);
+    const V3<T> tg = g * q.w + cross(g, u);
+    const V3<T> ug = cross(t, g) + cross(v, tg) * T(2);
+    qg.x += ug.x;
+    qg.y += ug.y;
+    qg.z += ug.z;
+    qg.w += dot(g, t);
+    return g + cross(tg, u) * T(2);
+}
+
+template <class T> __device__ __forceinline__ M3<T> toMat3(Q4<T> q) {
+    const T xx = q.x * q.x, yy = q.y * q.y, zz = q.z * q.z, xy = q.x * q.y, xz = q.x * q.z, yz = q.y * q.z;
+    const T wx = q.w * q.x, wy = q.w * q.y, wz = q.w * q.z;
+    M3<T> m;
+    m.r[0] = { 1 - 2 * (yy + zz), 2 * (xy - wz), 2 * (xz + wy) };
+    m.r[1] = { 2 * (xy + wz), 1 - 2 * (xx + zz), 2 * (yz - wx) };
+    m.r[2] = { 2 * (xz - wy), 2 * (yz + wx), 1 - 2 * (xx + yy) };
+    return m;
+}
+template <class T> __device__ __forceinline__ Q4<T> toMat3Adj(Q4<T> q, const M3<T>& g) {
+    const T x = q.x, y = q.y, z = q.z, w = q.w;
+    const V3<T>* r = g.r;
+    Q4<T> o;
+    o.x = r[0].y * 2 * y + r[0].z * 2 * z + r[1].x * 2 * y - r[1].y * 4 * x - r[1].z * 2 * w + r[2].x * 2 * z +
+          r[2].y * 2 * w - r[2].z * 4 * x;
+    o.y = -r[0].x * 4 * y + r[0].y * 2 * x + r[0].z * 2 * w + r[1].x * 2 * x + r[1].z * 2 * z - r[2].x * 2 * w +
+          r[2].y * 2 * z - r[2].z * 4 * y;
+    o.z = -r[0].x * 4 * z - r[0].y * 2 * w + r[0].z * 2 * x + r[1].x * 2 * w - r[1].y * 4 * z + r[1].z * 2 * y +
+          r[2].x * 2 * x + r[2].y * 2 * y;
+    o.w = -r[0].y * 2 * z + r[0].z * 2 * y + r[1].x * 2 * z - r[1].z * 2 * x - r[2].x * 2 * y + r[2].y * 2 * x;
+    return o;
+}
+
+template <class T> __device__ __forceinline__ T sqrtT(T x) { return sqrt(x); }
+
+// integrate(q, w, h) = normalize(q + (h/2) (w, 0) q) (math.h:227-230).
+template <class T> __device__ __forceinline__ Q4<T> integrateQ(Q4<T> q, V3<T> w, T h) {
+    const Q4<T> d = qmul(Q4<T>{ w.x, w.y, w.z, T(0) }, q);
+    const T c = T(0.5) * h;
+    const Q4<T> u{ q.x + c * d.x, q.y + c * d.y, q.z + c * d.z, q.w + c * d.w };
+    const T l = sqrtT(u.x * u.x + u.y * u.y + u.z * u.z + u.w * u.w);
+    return l > T(0) ? Q4<T>{ u.x / l, u.y / l, u.z / l, u.w / l } : Q4<T>{ 0, 0, 0, 1 };
+}
+template <class T> __device__ __forceinline__ void integrateQAdj(Q4<T> q, V3<T> w, T h, Q4<T> g, Q4<T>& qg, V3<T>& wg) {
+    const Q4<T> d = qmul(Q4<T>{ w.x, w.y, w.z, T(0) }, q);
+    const T c = T(0.5) * h;
+    const Q4<T> u{ q.x + c * d.x, q.y + c * d.y, q.z + c * d.z, q.w + c * d.w };
+    const T l = sqrtT(u.x * u.x + u.y * u.y + u.z * u.z + u.w * u.w);
+    if (!(l > T(0))) { return; }
+    const Q4<T> n{ u.x / l, u.y / l, u.z / l, u.w / l };
+    const T gn = g.x * n.x + g.y * n.y + g.z * n.z + g.w * n.w;
+    const Q4<T> ug{ (g.x - n.x * gn) / l, (g.y - n.y * gn) / l, (g.z - n.z * gn) / l, (g.w - n.w * gn) / l };
+    qg = qadd(qg, ug);
+    const Q4<T> dg{ ug.x * c, ug.y * c, ug.z * c, ug.w * c };
+    const Q4<T> wq = qmulAdjA(dg, q);
+    wg.x += wq.x;
+    wg.y += wq.y;
+    wg.z += wq.z;
+    qg = qadd(qg, qmulAdjB(dg, Q4<T>{ w.x, w.y, w.z, T(0) }));
+}
+
+template <class T> __device__ __forceinline__ void atomicAddT(T* p, T v) { atomicAdd(p, v); }
+
+// ---------------------------------------------------------------------------------------------------------
+// Model data.
+
+template <class T>
+struct Softness {
+    T biasRate, massScale, impulseScale;
+};
+
+// Per-step state of one contact point while the step runs.
+template <class T>
+struct PointState {
+    T n;      // normal impulse
+    V3<T> t;  // tangent impulse
+    T maxN;   // largest normal impulse added this step
+};
+
+template <class T>
+struct Model {
+    AdjointSetup S;
+    T h, invH, dt;
+    V3<T> gravity;
+    Softness<T> contactSoft, staticSoft;
+    T maxPushout, restThreshold;
+    // Parameters in T.
+    const T* mass;      // per body
+    const T* friction;  // per shape
+    const T* init;      // per body 13: com, q, v, w (the initial state)
+    // Checkpoints: (nSteps + 1) x totalBodies x 13.
+    T* states;
+    // Per body working arrays of the current step.
+    T* invM;    // 1
+    T* invI;    // 9 world inverse inertia
+    T* dp;      // 3
+    T* dq;      // 4
+    T* qBase;   // 4
+    PointState<T>* points;  // contactSlots x 4
+    // Backward only.
+    T* stateAdj;   // totalBodies x 13
+    T* dpAdj;      // 3
+    T* dqAdj;      // 4
+    T* qBaseAdj;   // 4
+    T* invMAdj;    // 1
+    T* invIAdj;    // 9
+    PointState<T>* pointAdj;  // contactSlots x 4
+    T* massAdj;      // per body (output, summed)
+    T* frictionAdj;  // per shape (output, summed)
+    T* log;          // per world: logStride values
+    uint64_t logStride;
+    T* integLog;     // per substep and body: q (4) and w (3) before the position update, dp (3) after it
+};
+
+constexpr int kIntegWords = 10;
+
+constexpr int kState = 13;
+
+template <class T> __device__ __forceinline__ V3<T> ld3(const T* p) { return { p[0], p[1], p[2] }; }
+template <class T> __device__ __forceinline__ void st3(T* p, V3<T> v) { p[0] = v.x, p[1] = v.y, p[2] = v.z; }
+template <class T> __device__ __forceinline__ Q4<T> ld4(const T* p) { return { p[0], p[1], p[2], p[3] }; }
+template <class T> __device__ __forceinline__ void st4(T* p, Q4<T> q) { p[0] = q.x, p[1] = q.y, p[2] = q.z, p[3] = q.w; }
+template <class T> __device__ __forceinline__ V3<T> fl3(const float* p) { return { T(p[0]), T(p[1]), T(p[2]) }; }
+template <class T> __device__ __forceinline__ M3<T> ldM(const T* p) {
+    return { { { p[0], p[1], p[2] }, { p[3], p[4], p[5] }, { p[6], p[7], p[8] } } };
+}
+template <class T> __device__ __forceinline__ void stM(T* p, const M3<T>& m) {
+    for (int r = 0; r < 3; ++r) { p[3 * r] = m.r[r].x, p[3 * r + 1] = m.r[r].y, p[3 * r + 2] = m.r[r].z; }
+}
+
+// A body as a contact solve sees it.
+template <class T>
+struct SBody {
+    V3<T> v, w, dp;
+    Q4<T> dq;
+    T im;
+    M3<T> I;
+    bool moves;
+};
+
+// One direction at a contact point: lever arms are constants (recorded anchors x direction).
+template <class T>
+struct Axis {
+    V3<T> d, armA, armB, angA, angB;
+    T dd, k, mass;
+    bool on;
+};
+
+template <class T>
+__device__ __forceinline__ Axis<T> makeAxis(const SBody<T>& a, const SBody<T>& b, V3<T> ra, V3<T> rb, V3<T> d) {
+    Axis<T> x;
+    x.d = d;
+    x.armA = cross(ra, d);
+    x.armB = cross(rb, d);
+    x.angA = mul(a.I, x.armA);
+    x.angB = mul(b.I, x.armB);
+    x.dd = dot(d, d);
+    x.k = a.im * x.dd + b.im * x.dd + dot(x.armA, x.angA) + dot(x.armB, x.angB);
+    x.on = x.k > T(1e-6) * (a.im + b.im);
+    x.mass = x.on ? T(1) / x.k : T(0);
+    return x;
+}
+
+// Adjoint of the effective mass: mass = 1/k with k from both bodies' inverse mass and inertia.
+template <class T>
+__device__ __forceinline__ void axisMassAdj(const Axis<T>& x, T massAdj, T& imA, M3<T>& IA, T& imB, M3<T>& IB) {
+    if (!x.on) { return; }
+    const T kg = -massAdj * x.mass * x.mass;
+    imA += kg * x.dd;
+    imB += kg * x.dd;
+    addOuter(IA, x.armA, x.armA, kg);
+    addOuter(IB, x.armB, x.armB, kg);
+}
+
+template <class T>
+__device__ __forceinline__ T speedAlong(const SBody<T>& a, const SBody<T>& b, const Axis<T>& x) {
+    return dot(x.d, b.v - a.v) + dot(x.armB, b.w) - dot(x.armA, a.w);
+}
+
+template <class T>
+__device__ __forceinline__ void push(SBody<T>& a, SBody<T>& b, const Axis<T>& x, T impulse) {
+    if (a.moves) {
+        a.v = a.v - x.d * (a.im * impulse);
+        a.w = a.w - x.angA * impulse;
+    }
+    if (b.moves) {
+        b.v = b.v + x.d * (b.im * impulse);
+        b.w = b.w + x.angB * impulse;
+    }
+}
+
+// Adjoints of one body during a contact's reverse pass.
+template <class T>
+struct BodyAdj {
+    V3<T> v, w, dp;
+    Q4<T> dq;
+    T im;
+    M3<T> I;
+};
+
+template <class T>
+__device__ __forceinline__ T pushAdj(const SBody<T>& a, const SBody<T>& b, const Axis<T>& x, T impulse, BodyAdj<T>& ga,
+                                     BodyAdj<T>& gb) {
+    T g = 0;
+    if (a.moves) {
+        g -= a.im * dot(x.d, ga.v) + dot(x.angA, ga.w);
+        ga.im -= impulse * dot(x.d, ga.v);
+        addOuter(ga.I, ga.w, x.armA, -impulse);
+    }
+    if (b.moves) {
+        g += b.im * dot(x.d, gb.v) + dot(x.angB, gb.w);
+        gb.im += impulse * dot(x.d, gb.v);
+        addOuter(gb.I, gb.w, x.armB, impulse);
+    }
+    return g;
+}
+
+template <class T>
+__device__ __forceinline__ void speedAdj(const Axis<T>& x, T g, BodyAdj<T>& ga, BodyAdj<T>& gb) {
+    ga.v = ga.v - x.d * g;
+    gb.v = gb.v + x.d * g;
+    ga.w = ga.w - x.armA * g;
+    gb.w = gb.w + x.armB * g;
+}
+
+// The recorded contact in T.
+template <class T>
+struct CData {
+    int count;
+    V3<T> n, t1, t2;
+    V3<T> ra[4], rb[4];
+    T adjSep[4], relVel[4];
+    T restitution;
+};
+
+template <class T>
+__device__ __forceinline__ CData<T> loadContact(const TapeContact& c) {
+    CData<T> d;
+    d.count = c.count;
+    d.n = fl3<T>(c.normal);
+    d.t1 = fl3<T>(c.t1);
+    d.t2 = fl3<T>(c.t2);
+    for (int i = 0; i < 4; ++i) {
+        d.ra[i] = fl3<T>(c.anchorA[i]);
+        d.rb[i] = fl3<T>(c.anchorB[i]);
+        d.adjSep[i] = T(c.adjSep[i]);
+        d.relVel[i] = T(c.relVel[i]);
+    }
+    d.restitution = T(c.restitution);
+    return d;
+}
+
+// ---------------------------------------------------------------------------------------------------------
+// Contact operations: forward, and reverse from the logged inputs.
+
+enum Op : int { kWarm = 0, kBias = 1, kRelax = 2, kRestitute = 3 };
+
+// What a contact operation reads from its bodies and points, logged before it runs.
+template <class T>
+struct CallIn {
+    V3<T> va, wa, vb, wb;
+    PointState<T> p[4];
+};
+template <class T>
+__host__ __device__ constexpr int callWords() { return 12 + 4 * 5; }
+
+template <class T>
+__device__ __forceinline__ void writeCall(T* log, const SBody<T>& a, const SBody<T>& b, const PointState<T>* p) {
+    st3(log, a.v), st3(log + 3, a.w), st3(log + 6, b.v), st3(log + 9, b.w);
+    for (int i = 0; i < 4; ++i) {
+        log[12 + 5 * i] = p[i].n;
+        st3(log + 13 + 5 * i, p[i].t);
+        log[16 + 5 * i] = p[i].maxN;
+    }
+}
+template <class T>
+__device__ __forceinline__ void readCall(const T* log, SBody<T>& a, SBody<T>& b, PointState<T>* p) {
+    a.v = ld3(log), a.w = ld3(log + 3), b.v = ld3(log + 6), b.w = ld3(log + 9);
+    for (int i = 0; i < 4; ++i) {
+        p[i].n = log[12 + 5 * i];
+        p[i].t = ld3(log + 13 + 5 * i);
+        p[i].maxN = log[16 + 5 * i];
+    }
+}
+
+// The normal row of point i (src/solver.cpp:364-392). Returns the impulse added.
+template <class T>
+__device__ __forceinline__ T normalRow(const Model<T>& M, SBody<T>& a, SBody<T>& b, const CData<T>& c, int i,
+                                       PointState<T>& p, bool useBias, const Softness<T>& soft) {
+    const Axis<T> x = makeAxis(a, b, c.ra[i], c.rb[i], c.n);
+    const V3<T> d = b.dp - a.dp + rotate(b.dq, c.rb[i]) - rotate(a.dq, c.ra[i]);
+    const T sep = dot(d, c.n) + c.adjSep[i];
+    T bias = 0, ms = 1, is = 0;
+    if (sep > T(0)) {
+        bias = sep * M.invH;
+    } else if (useBias) {
+        bias = fmax(soft.biasRate * sep, -M.maxPushout);
+        ms = soft.massScale;
+        is = soft.impulseScale;
+    }
+    const T vn = speedAlong(a, b, x);
+    const T imp = -x.mass * ms * (vn + bias) - is * p.n;
+    const T total = fmax(p.n + imp, T(0));
+    const T delta = total - p.n;
+    p.n = total;
+    p.maxN = fmax(p.maxN, delta);
+    push(a, b, x, delta);
+    return delta;
+}
+
+template <class T>
+__device__ __forceinline__ void normalRowAdj(const Model<T>& M, const SBody<T>& a, const SBody<T>& b, const CData<T>& c,
+                                             int i, const PointState<T>& p0, bool useBias, const Softness<T>& soft,
+                                             BodyAdj<T>& ga, BodyAdj<T>& gb, PointState<T>& gp) {
+    const Axis<T> x = makeAxis(a, b, c.ra[i], c.rb[i], c.n);
+    const V3<T> d = b.dp - a.dp + rotate(b.dq, c.rb[i]) - rotate(a.dq, c.ra[i]);
+    const T sep = dot(d, c.n) + c.adjSep[i];
+    T bias = 0, ms = 1, is = 0;
+    int biasKind = 0;  // 0 none, 1 sep * invH, 2 biasRate * sep, 3 clamped at -maxPushout
+    if (sep > T(0)) {
+        bias = sep * M.invH;
+        biasKind = 1;
+    } else if (useBias) {
+        const T b1 = soft.biasRate * sep;
+        biasKind = b1 > -M.maxPushout ? 2 : 3;
+        bias = fmax(b1, -M.maxPushout);
+        ms = soft.massScale;
+        is = soft.impulseScale;
+    }
+    const T vn = speedAlong(a, b, x);
+    const T imp = -x.mass * ms * (vn + bias) - is * p0.n;
+    const T total = fmax(p0.n + imp, T(0));
+    const T delta = total - p0.n;
+    // Reverse: push, max, total, impulse.
+    T deltaG = pushAdj(a, b, x, delta, ga, gb);
+    if (delta > p0.maxN) {
+        deltaG += gp.maxN;
+        gp.maxN = 0;
+    }
+    T totalG = gp.n + deltaG;
+    T nG = -deltaG;
+    T impG = 0;
+    if (p0.n + imp > T(0)) {
+        nG += totalG;
+        impG = totalG;
+    }
+    const T massG = -impG * ms * (vn + bias);
+    const T vnG = -impG * x.mass * ms;
+    const T biasG = vnG;
+    nG += -impG * is;
+    gp.n = nG;
+    speedAdj(x, vnG, ga, gb);
+    axisMassAdj(x, massG, ga.im, ga.I, gb.im, gb.I);
+    T sepG = 0;
+    if (biasKind == 1) { sepG = biasG * M.invH; }
+    if (biasKind == 2) { sepG = biasG * soft.biasRate; }
+    if (sepG != T(0)) {
+        const V3<T> dg = c.n * sepG;
+        gb.dp = gb.dp + dg;
+        ga.dp = ga.dp - dg;
+        rotateAdj(b.dq, c.rb[i], dg, gb.dq);
+        rotateAdj(a.dq, c.ra[i], dg * T(-1), ga.dq);
+    }
+}
+
+// The friction rows of point i (src/solver.cpp:393-418).
+template <class T>
+__device__ __forceinline__ void frictionRow(SBody<T>& a, SBody<T>& b, const CData<T>& c, int i, PointState<T>& p, T mu) {
+    const Axis<T> x1 = makeAxis(a, b, c.ra[i], c.rb[i], c.t1);
+    const Axis<T> x2 = makeAxis(a, b, c.ra[i], c.rb[i], c.t2);
+    const T old1 = dot(p.t, c.t1), old2 = dot(p.t, c.t2);
+    T f1 = old1 - x1.mass * speedAlong(a, b, x1);
+    T f2 = old2 - x2.mass * speedAlong(a, b, x2);
+    const T limit = mu * p.n;
+    const T mag = sqrtT(f1 * f1 + f2 * f2);
+    if (mag > limit) {
+        const T scale = mag > T(0) ? limit / mag : T(0);
+        f1 *= scale;
+        f2 *= scale;
+    }
+    p.t = c.t1 * f1 + c.t2 * f2;
+    push(a, b, x1, f1 - old1);
+    push(a, b, x2, f2 - old2);
+}
+
+template <class T>
+__device__ __forceinline__ void frictionRowAdj(const SBody<T>& a, const SBody<T>& b, const CData<T>& c, int i,
+                                               const PointState<T>& p0, T mu, BodyAdj<T>& ga, BodyAdj<T>& gb,
+                                               PointState<T>& gp, T& muG) {
+    const Axis<T> x1 = makeAxis(a, b, c.ra[i], c.rb[i], c.t1);
+    const Axis<T> x2 = makeAxis(a, b, c.ra[i], c.rb[i], c.t2);
+    const T old1 = dot(p0.t, c.t1), old2 = dot(p0.t, c.t2);
+    const T s1 = speedAlong(a, b, x1), s2 = speedAlong(a, b, x2);
+    const T f1 = old1 - x1.mass * s1, f2 = old2 - x2.mass * s2;
+    const T limit = mu * p0.n;
+    const T mag = sqrtT(f1 * f1 + f2 * f2);
+    // With no friction allowed (limit 0) the row adds nothing whatever f is, also at f = 0 where the forward
+    // takes the unclamped branch with the same result: the derivative is that of the clamp.
+    const bool clamp = mag > limit || limit == T(0);
+    const T scale = mag > limit ? (mag > T(0) ? limit / mag : T(0)) : (limit == T(0) ? T(0) : T(1));
+    const T g1 = f1 * scale, g2 = f2 * scale;
+    // Reverse the pushes (they commute), the stored tangent impulse, the cone, the rows.
+    const T d1G = pushAdj(a, b, x1, g1 - old1, ga, gb);
+    const T d2G = pushAdj(a, b, x2, g2 - old2, ga, gb);
+    T g1G = d1G + dot(gp.t, c.t1);
+    T g2G = d2G + dot(gp.t, c.t2);
+    T old1G = -d1G, old2G = -d2G;
+    T f1G = g1G, f2G = g2G;
+    if (clamp && mag > T(0)) {
+        const T scaleG = g1G * f1 + g2G * f2;
+        f1G = g1G * scale;
+        f2G = g2G * scale;
+        const T limitG = scaleG / mag;
+        const T magG = -scaleG * limit / (mag * mag);
+        f1G += magG * f1 / mag;
+        f2G += magG * f2 / mag;
+        muG += limitG * p0.n;
+        gp.n += limitG * mu;
+    } else if (clamp) {
+        f1G = 0;
+        f2G = 0;
+    }
+    old1G += f1G;
+    old2G += f2G;
+    axisMassAdj(x1, -f1G * s1, ga.im, ga.I, gb.im, gb.I);
+    axisMassAdj(x2, -f2G * s2, ga.im, ga.I, gb.im, gb.I);
+    speedAdj(x1, -f1G * x1.mass, ga, gb);
+    speedAdj(x2, -f2G * x2.mass, ga, gb);
+    gp.t = c.t1 * old1G + c.t2 * old2G;
+}
+
+// The restitution row of point i (src/solver.cpp:423-460); does nothing when the point does not qualify.
+template <class T>
+__device__ __forceinline__ bool restitutes(const Model<T>& M, const CData<T>& c, int i, const PointState<T>& p) {
+    return !(c.relVel[i] > -M.restThreshold || p.maxN == T(0));
+}
+
+template <class T>
+__device__ __forceinline__ void restituteRow(const Model<T>& M, SBody<T>& a, SBody<T>& b, const CData<T>& c, int i,
+                                             PointState<T>& p) {
+    const Axis<T> x = makeAxis(a, b, c.ra[i], c.rb[i], c.n);
+    const T vn = speedAlong(a, b, x);
+    const T imp = -x.mass * (vn + c.restitution * c.relVel[i]);
+    const T total = fmax(p.n + imp, T(0));
+    const T delta = total - p.n;
+    p.n = total;
+    p.maxN = fmax(p.maxN, delta);
+    push(a, b, x, delta);
+}
+
+template <class T>
+__device__ __forceinline__ void restituteRowAdj(const Model<T>& M, const SBody<T>& a, const SBody<T>& b, const CData<T>& c,
+                                                int i, const PointState<T>& p0, BodyAdj<T>& ga, BodyAdj<T>& gb,
+                                                PointState<T>& gp) {
+    const Axis<T> x = makeAxis(a, b, c.ra[i], c.rb[i], c.n);
+    const T vn = speedAlong(a, b, x);
+    const T imp = -x.mass * (vn + c.restitution * c.relVel[i]);
+    const T total = fmax(p0.n + imp, T(0));
+    const T delta = total - p0.n;
+    T deltaG = pushAdj(a, b, x, delta, ga, gb);
+    if (delta > p0.maxN) {
+        deltaG += gp.maxN;
+        gp.maxN = 0;
+    }
+    const T totalG = gp.n + deltaG;
+    T nG = -deltaG;
+    T impG = 0;
+    if (p0.n + imp > T(0)) {
+        nG += totalG;
+        impG = totalG;
+    }
+    gp.n = nG;
+    const T massG = -impG * (vn + c.restitution * c.relVel[i]);
+    speedAdj(x, -impG * x.mass, ga, gb);
+    axisMassAdj(x, massG, ga.im, ga.I, gb.im, gb.I);
+}
+
+// One operation on one contact, forward. The points' state comes in and goes out through p.
+template <class T>
+__device__ void contactOp(const Model<T>& M, int op, SBody<T>& a, SBody<T>& b, const CData<T>& c, PointState<T>* p,
+                          T mu) {
+    const Softness<T> soft = (!a.moves || !b.moves) ? M.staticSoft : M.contactSoft;
+    const int n = c.count;
+    if (op == kWarm) {
+        for (int i = 0; i < n; ++i) {
+            const Axis<T> xn = makeAxis(a, b, c.ra[i], c.rb[i], c.n);
+            const Axis<T> x1 = makeAxis(a, b, c.ra[i], c.rb[i], c.t1);
+            const Axis<T> x2 = makeAxis(a, b, c.ra[i], c.rb[i], c.t2);
+            push(a, b, xn, p[i].n);
+            push(a, b, x1, dot(p[i].t, c.t1));
+            push(a, b, x2, dot(p[i].t, c.t2));
+        }
+        return;
+    }
+    if (op == kRestitute) {
+        if (c.restitution == T(0)) { return; }
+        for (int i = 0; i < n; ++i) {
+            if (restitutes(M, c, i, p[i])) { restituteRow(M, a, b, c, i, p[i]); }
+        }
+        return;
+    }
+    const bool useBias = op == kBias;
+    for (int i = 0; i < n; ++i) { normalRow(M, a, b, c, i, p[i], useBias, soft); }
+    for (int j = 0; j < n; ++j) {
+        const int i = useBias ? j : n - 1 - j;
+        frictionRow(a, b, c, i, p[i], mu);
+    }
+}
+
+// The same operation in reverse: replays it from its logged inputs to have every row's input, then walks the
+// rows backwards. ga, gb, gp hold the adjoints after the operation on entry and before it on return.
+template <class T>
+__device__ void contactOpAdj(const Model<T>& M, int op, const SBody<T>& a0, const SBody<T>& b0, const CData<T>& c,
+                             const PointState<T>* p0, T mu, BodyAdj<T>& ga, BodyAdj<T>& gb, PointState<T>* gp, T& muG) {
+    const Softness<T> soft = (!a0.moves || !b0.moves) ? M.staticSoft : M.contactSoft;
+    const int n = c.count;
+    if (op == kWarm) {
+        for (int i = 0; i < n; ++i) {
+            const Axis<T> xn = makeAxis(a0, b0, c.ra[i], c.rb[i], c.n);
+            const Axis<T> x1 = makeAxis(a0, b0, c.ra[i], c.rb[i], c.t1);
+            const Axis<T> x2 = makeAxis(a0, b0, c.ra[i], c.rb[i], c.t2);
+            const T l1 = dot(p0[i].t, c.t1), l2 = dot(p0[i].t, c.t2);
+            gp[i].n += pushAdj(a0, b0, xn, p0[i].n, ga, gb);
+            const T g1 = pushAdj(a0, b0, x1, l1, ga, gb);
+            const T g2 = pushAdj(a0, b0, x2, l2, ga, gb);
+            gp[i].t = gp[i].t + c.t1 * g1 + c.t2 * g2;
+        }
+        return;
+    }
+    // Rows of this operation in order, each with the bodies and point state it started from.
+    constexpr int kMaxRows = 8;
+    SBody<T> ra[kMaxRows], rb[kMaxRows];
+    PointState<T> rp[kMaxRows];
+    int rowPoint[kMaxRows], rowKind[kMaxRows];  // kind 0 normal, 1 friction, 2 restitution
+    int rows = 0;
+    SBody<T> a = a0, b = b0;
+    PointState<T> p[4];
+    for (int i = 0; i < 4; ++i) { p[i] = p0[i]; }
+    if (op == kRestitute) {
+        if (c.restitution == T(0)) { return; }
+        for (int i = 0; i < n; ++i) {
+            if (!restitutes(M, c, i, p[i])) { continue; }
+            ra[rows] = a, rb[rows] = b, rp[rows] = p[i], rowPoint[rows] = i, rowKind[rows] = 2, ++rows;
+            restituteRow(M, a, b, c, i, p[i]);
+        }
+    } else {
+        const bool useBias = op == kBias;
+        for (int i = 0; i < n; ++i) {
+            ra[rows] = a, rb[rows] = b, rp[rows] = p[i], rowPoint[rows] = i, rowKind[rows] = 0, ++rows;
+            normalRow(M, a, b, c, i, p[i], useBias, soft);
+        }
+        for (int j = 0; j < n; ++j) {
+            const int i = useBias ? j : n - 1 - j;
+            ra[rows] = a, rb[rows] = b, rp[rows] = p[i], rowPoint[rows] = i, rowKind[rows] = 1, ++rows;
+            frictionRow(a, b, c, i, p[i], mu);
+        }
+    }
+    for (int r = rows - 1; r >= 0; --r) {
+        const int i = rowPoint[r];
+        if (rowKind[r] == 0) {
+            normalRowAdj(M, ra[r], rb[r], c, i, rp[r], op == kBias, soft, ga, gb, gp[i]);
+        } else if (rowKind[r] == 1) {
+            frictionRowAdj(ra[r], rb[r], c, i, rp[r], mu, ga, gb, gp[i], muG);
+        } else {
+            restituteRowAdj(M, ra[r], rb[r], c, i, rp[r], ga, gb, gp[i]);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------------------------
+// One world's step, forward (with optional logging) and in reverse. One warp per world.
+
+struct WorldView {
+    uint32_t bodyFirst, bodyCount, shapeFirst;
+    const TapeWorld* tw;
+    const TapeContact* contacts;
+    const uint32_t* colored;
+    const uint32_t* impactColored;
+    const uint32_t* rest;
+    const uint32_t* impactRest;
+    const uint8_t* awake;
+};
+
+__device__ __forceinline__ WorldView viewOf(const AdjointSetup& S, int step, uint32_t w) {
+    const TapeStep ts = S.steps[step];
+    WorldView v;
+    v.bodyFirst = S.bodyFirst[w];
+    v.bodyCount = S.bodyCount[w];
+    v.shapeFirst = S.shapeFirst[w];
+    v.tw = ts.worlds + w;
+    const uint32_t cf = v.tw->contactFirst;
+    v.contacts = ts.contacts + cf;
+    v.colored = ts.colored + cf;
+    v.impactColored = ts.impactColored + cf;
+    v.rest = ts.rest + cf;
+    v.impactRest = ts.impactRest + cf;
+    v.awake = ts.awake;
+    return v;
+}
+
+template <class T>
+__device__ __forceinline__ bool movesIn(const Model<T>& M, const WorldView& V, uint32_t g) {
+    return M.S.dynamic[g] && V.awake[g];
+}
+
+template <class T>
+__device__ __forceinline__ SBody<T> bodyOf(const Model<T>& M, const WorldView& V, uint32_t g, const T* state) {
+    SBody<T> b;
+    b.v = ld3(state + (size_t)g * kState + 7);
+    b.w = ld3(state + (size_t)g * kState + 10);
+    b.dp = ld3(M.dp + 3 * (size_t)g);
+    b.dq = ld4(M.dq + 4 * (size_t)g);
+    b.im = M.invM[g];
+    b.I = ldM(M.invI + 9 * (size_t)g);
+    b.moves = movesIn(M, V, g);
+    return b;
+}
+
+template <class T>
+__device__ __forceinline__ T contactFriction(const Model<T>& M, const WorldView& V, const TapeContact& tc) {
+    return sqrtT(M.friction[V.shapeFirst + tc.shapeA] * M.friction[V.shapeFirst + tc.shapeB]);
+}
+
+// The list walks of one pass, in the order the step pipeline runs them.
+struct PassList {
+    const uint32_t* list;
+    const uint32_t* start;  // color starts, or null for a one-at-a-time list
+    uint32_t count;         // colors, or list length
+};
+
+__device__ __forceinline__ int passLists(const WorldView& V, int op, PassList* out) {
+    const TapeWorld& tw = *V.tw;
+    int n = 0;
+    out[n++] = { V.colored, tw.colorStart, tw.colorCount };
+    out[n++] = { V.rest, nullptr, tw.restCount };
+    if (op != kWarm && op != kRestitute && tw.impactColorStart[tw.impactColorCount] + tw.impactRestCount > 0) {
+        out[n++] = { V.impactColored, tw.impactColorStart, tw.impactColorCount };
+        out[n++] = { V.impactRest, nullptr, tw.impactRestCount };
+    }
+    return n;
+}
+
+// Forward of one step of one world. state: in at `in`, out at `out` (may be the same). When log is non-null the
+// inputs of every contact operation and position update are written there for the reverse pass.
+template <class T>
+__device__ void stepWorld(const Model<T>& M, int step, uint32_t w, const T* in, T* out, T* log, T* integLog) {
+    const uint32_t lane = threadIdx.x & 31;
+    const WorldView V = viewOf(M.S, step, w);
+    const int n = M.S.substeps;
+    // Step start: world inverse inertia at this pose, zero displacement, warm-start impulses.
+    for (uint32_t i = lane; i < V.bodyCount; i += 32) {
+        const uint32_t g = V.bodyFirst + i;
+        const T* s = in + (size_t)g * kState;
+        T* o = out + (size_t)g * kState;
+        for (int k = 0; k < kState; ++k) { o[k] = s[k]; }
+        const bool moves = movesIn(M, V, g);
+        const Q4<T> q = ld4(s + 3);
+        T im = 0;
+        M3<T> I = zeroM<T>();
+        if (moves) {
+            const T scale = T(M.S.mass[g]) / M.mass[g];
+            im = T(1) / M.mass[g];
+            const M3<T> r = toMat3(q);
+            M3<T> L;
+            for (int a = 0; a < 3; ++a) {
+                L.r[a] = { T(M.S.invInertiaLocal[9 * g + 3 * a]) * scale, T(M.S.invInertiaLocal[9 * g + 3 * a + 1]) * scale,
+                           T(M.S.invInertiaLocal[9 * g + 3 * a + 2]) * scale };
+            }
+            I = mmul(r, mmul(L, transposeM(r)));
+        }
+        M.invM[g] = im;
+        stM(M.invI + 9 * (size_t)g, I);
+        st3(M.dp + 3 * (size_t)g, zeroV<T>());
+        st4(M.dq + 4 * (size_t)g, Q4<T>{ 0, 0, 0, 1 });
+        st4(M.qBase + 4 * (size_t)g, q);
+    }
+    const uint32_t cf = V.tw->contactFirst;
+    for (uint32_t ci = lane; ci < V.tw->contactCount; ci += 32) {
+        const TapeContact& tc = V.contacts[ci];
+        for (int i = 0; i < 4; ++i) {
+            PointState<T>& p = M.points[(size_t)(cf + ci) * 4 + i];
+            p.n = T(tc.normalImpulse[i]);
+            p.t = fl3<T>(tc.tangentImpulse[i]);
+            p.maxN = 0;
+        }
+    }
+    __syncwarp();
+    uint64_t cursor = 0;  // log index of the next operation; every lane keeps the same count
+    auto runOp = [&](int op, uint32_t ci, uint64_t at) {
+        const TapeContact& tc = V.contacts[ci];
+        const CData<T> c = loadContact<T>(tc);
+        const uint32_t ga = V.bodyFirst + tc.a, gb = V.bodyFirst + tc.b;
+        SBody<T> a = bodyOf(M, V, ga, out), b = bodyOf(M, V, gb, out);
+        PointState<T>* p = M.points + (size_t)(cf + ci) * 4;
+        PointState<T> ps[4];
+        for (int i = 0; i < 4; ++i) { ps[i] = p[i]; }
+        if (log) { writeCall(log + at * callWords<T>(), a, b, ps); }
+        contactOp(M, op, a, b, c, ps, contactFriction(M, V, tc));
+        for (int i = 0; i < 4; ++i) { p[i] = ps[i]; }
+        if (a.moves) {
+            st3(out + (size_t)ga * kState + 7, a.v);
+            st3(out + (size_t)ga * kState + 10, a.w);
+        }
+        if (b.moves) {
+            st3(out + (size_t)gb * kState + 7, b.v);
+            st3(out + (size_t)gb * kState + 10, b.w);
+        }
+    };
+    // One pass: colored lists color by color (a lane per contact), one-at-a-time lists on lane 0.
+    auto pass = [&](int op) {
+        PassList lists[4];
+        const int nl = passLists(V, op, lists);
+        for (int l = 0; l < nl; ++l) {
+            const PassList& L = lists[l];
+            if (L.start) {
+                const uint32_t first = L.start[0];
+                for (uint32_t k = 0; k < L.count; ++k) {
+                    for (uint32_t x = L.start[k] + lane; x < L.start[k + 1]; x += 32) { runOp(op, L.list[x], cursor + (x - first)); }
+                    __syncwarp();
+                }
+                cursor += L.start[L.count] - first;
+            } else {
+                if (lane == 0) {
+                    for (uint32_t x = 0; x < L.count; ++x) { runOp(op, L.list[x], cursor + x); }
+                }
+                cursor += L.count;
+                __syncwarp();
+            }
+        }
+    };
+    for (int sub = 0; sub < n; ++sub) {
+        for (uint32_t i = lane; i < V.bodyCount; i += 32) {
+            const uint32_t g = V.bodyFirst + i;
+            if (!movesIn(M, V, g)) { continue; }
+            T* o = out + (size_t)g * kState;
+            const V3<T> v = ld3(o + 7), wv = ld3(o + 10);
+            const T gs = T(M.S.gravityScale[g]);
+            const V3<T> nv = (v + M.gravity * (gs * M.h)) * (T(1) / (T(1) + M.h * T(M.S.linearDamping[g])));
+            const V3<T> nw = wv * (T(1) / (T(1) + M.h * T(M.S.angularDamping[g])));
+            st3(o + 7, nv);
+            st3(o + 10, nw);
+        }
+        __syncwarp();
+        pass(kWarm);
+        pass(kBias);
+        for (uint32_t i = lane; i < V.bodyCount; i += 32) {
+            const uint32_t g = V.bodyFirst + i;
+            if (!movesIn(M, V, g)) { continue; }
+            T* o = out + (size_t)g * kState;
+            const V3<T> v = ld3(o + 7), wv = ld3(o + 10);
+            const Q4<T> q = ld4(o + 3);
+            st3(o, ld3(o) + v * M.h);
+            const V3<T> ndp = ld3(M.dp + 3 * (size_t)g) + v * M.h;
+            st3(M.dp + 3 * (size_t)g, ndp);
+            if (integLog) {
+                T* L = integLog + ((size_t)sub * M.S.totalBodies + g) * kIntegWords;
+                st4(L, q);
+                st3(L + 4, wv);
+                st3(L + 7, ndp);
+            }
+            const Q4<T> nq = integrateQ(q, wv, M.h);
+            st4(o + 3, nq);
+            st4(M.dq + 4 * (size_t)g, qmul(nq, conj(ld4(M.qBase + 4 * (size_t)g))));
+        }
+        __syncwarp();
+        pass(kRelax);
+    }
+    pass(kRestitute);
+}
+
+// Reverse of one world's step: adjoints of the state at the step's end in M.stateAdj become those at its start.
+// Needs the log and integLog that stepWorld wrote for this step, and the bodies' dp/dq of every substep, which
+// it recomputes by replaying the integration from the checkpoint as it goes back.
+template <class T>
+__device__ void stepWorldAdj(const Model<T>& M, int step, uint32_t w, const T* in, const T* log, const T* integLog,
+                             uint64_t calls) {
+    const uint32_t lane = threadIdx.x & 31;
+    const WorldView V = viewOf(M.S, step, w);
+    const int n = M.S.substeps;
+    const uint32_t cf = V.tw->contactFirst;
+    // dp, dq and invM, invI of the step: recomputed from the checkpoint and the integration log.
+    for (uint32_t i = lane; i < V.bodyCount; i += 32) {
+        const uint32_t g = V.bodyFirst + i;
+        st3(M.dpAdj + 3 * (size_t)g, zeroV<T>());
+        st4(M.dqAdj + 4 * (size_t)g, Q4<T>{ 0, 0, 0, 0 });
+        st4(M.qBaseAdj + 4 * (size_t)g, Q4<T>{ 0, 0, 0, 0 });
+        M.invMAdj[g] = 0;
+        stM(M.invIAdj + 9 * (size_t)g, zeroM<T>());
+    }
+    for (uint32_t ci = lane; ci < V.tw->contactCount; ci += 32) {
+        for (int i = 0; i < 4; ++i) { M.pointAdj[(size_t)(cf + ci) * 4 + i] = PointState<T>{ 0, zeroV<T>(), 0 }; }
+    }
+    __syncwarp();
+    // dp and dq a body had during substep `sub`'s passes: before its position update (warm start, biased
+    // solve) or after it (relax, restitution), from the integration log of the recomputed step.
+    auto setDisplacement = [&](int sub, bool afterUpdate) {
+        for (uint32_t i = lane; i < V.bodyCount; i += 32) {
+            const uint32_t g = V.bodyFirst + i;
+            const int k = afterUpdate ? sub : sub - 1;  // the last position update before the pass
+            if (!movesIn(M, V, g) || k < 0) {
+                st3(M.dp + 3 * (size_t)g, zeroV<T>());
+                st4(M.dq + 4 * (size_t)g, Q4<T>{ 0, 0, 0, 1 });
+                continue;
+            }
+            const T* L = integLog + ((size_t)k * M.S.totalBodies + g) * kIntegWords;
+            const Q4<T> qb = ld4(in + (size_t)g * kState + 3);
+            st3(M.dp + 3 * (size_t)g, ld3(L + 7));
+            st4(M.dq + 4 * (size_t)g, qmul(integrateQ(ld4(L), ld3(L + 4), M.h), conj(qb)));
+        }
+        __syncwarp();
+    };
+    uint64_t cursor = calls;  // one past the last call of the step
+    auto opAdj = [&](int op, uint32_t ci, uint64_t at) {
+        const TapeContact& tc = V.contacts[ci];
+        const CData<T> c = loadContact<T>(tc);
+        const uint32_t ga = V.bodyFirst + tc.a, gb = V.bodyFirst + tc.b;
+        SBody<T> a, b;
+        PointState<T> p0[4];
+        readCall(log + at * callWords<T>(), a, b, p0);
+        a.dp = ld3(M.dp + 3 * (size_t)ga), a.dq = ld4(M.dq + 4 * (size_t)ga), a.im = M.invM[ga];
+        a.I = ldM(M.invI + 9 * (size_t)ga), a.moves = movesIn(M, V, ga);
+        b.dp = ld3(M.dp + 3 * (size_t)gb), b.dq = ld4(M.dq + 4 * (size_t)gb), b.im = M.invM[gb];
+        b.I = ldM(M.invI + 9 * (size_t)gb), b.moves = movesIn(M, V, gb);
+        T* sa = M.stateAdj + (size_t)ga * kState;
+        T* sb = M.stateAdj + (size_t)gb * kState;
+        BodyAdj<T> gA{ zeroV<T>(), zeroV<T>(), zeroV<T>(), Q4<T>{ 0, 0, 0, 0 }, 0, zeroM<T>() };
+        BodyAdj<T> gB = gA;
+        // Moving bodies belong to this contact alone within its color: their adjoints are read and written in
+        // place. Anchored bodies are shared: their contributions are added atomically.
+        if (a.moves) { gA.v = ld3(sa + 7), gA.w = ld3(sa + 10); }
+        if (b.moves) { gB.v = ld3(sb + 7), gB.w = ld3(sb + 10); }
+        PointState<T>* gp = M.pointAdj + (size_t)(cf + ci) * 4;
+        PointState<T> g4[4];
+        for (int i = 0; i < 4; ++i) { g4[i] = gp[i]; }
+        T muG = 0;
+        const T mu = contactFriction(M, V, tc);
+        contactOpAdj(M, op, a, b, c, p0, mu, gA, gB, g4, muG);
+        for (int i = 0; i < 4; ++i) { gp[i] = g4[i]; }
+        auto put = [&](bool moves, uint32_t g, T* s, const BodyAdj<T>& G) {
+            if (moves) {
+                st3(s + 7, G.v);
+                st3(s + 10, G.w);
+                st3(M.dpAdj + 3 * (size_t)g, ld3(M.dpAdj + 3 * (size_t)g) + G.dp);
+                st4(M.dqAdj + 4 * (size_t)g, qadd(ld4(M.dqAdj + 4 * (size_t)g), G.dq));
+                M.invMAdj[g] += G.im;
+                T* I = M.invIAdj + 9 * (size_t)g;
+                for (int r = 0; r < 3; ++r) { I[3 * r] += G.I.r[r].x, I[3 * r + 1] += G.I.r[r].y, I[3 * r + 2] += G.I.r[r].z; }
+            } else {
+                atomicAddT(s + 7, G.v.x), atomicAddT(s + 8, G.v.y), atomicAddT(s + 9, G.v.z);
+                atomicAddT(s + 10, G.w.x), atomicAddT(s + 11, G.w.y), atomicAddT(s + 12, G.w.z);
+            }
+        };
+        put(a.moves, ga, sa, gA);
+        put(b.moves, gb, sb, gB);
+        if (muG != T(0)) {
+            // mu = sqrt(fa fb): d mu / d fa = fb / (2 mu).
+            const T fa = M.friction[V.shapeFirst + tc.shapeA], fb = M.friction[V.shapeFirst + tc.shapeB];
+            if (mu > T(0)) {
+                atomicAddT(M.frictionAdj + V.shapeFirst + tc.shapeA, muG * fb / (T(2) * mu));
+                atomicAddT(M.frictionAdj + V.shapeFirst + tc.shapeB, muG * fa / (T(2) * mu));
+            }
+        }
+    };
+    auto passAdj = [&](int op) {
+        PassList lists[4];
+        const int nl = passLists(V, op, lists);
+        for (int l = nl - 1; l >= 0; --l) {
+            const PassList& L = lists[l];
+            if (L.start) {
+                const uint32_t first = L.start[0];
+                cursor -= L.start[L.count] - first;
+                for (int k = (int)L.count - 1; k >= 0; --k) {
+                    for (uint32_t x = L.start[k] + lane; x < L.start[k + 1]; x += 32) { opAdj(op, L.list[x], cursor + (x - first)); }
+                    __syncwarp();
+                }
+            } else {
+                cursor -= L.count;
+                if (lane == 0) {
+                    for (int x = (int)L.count - 1; x >= 0; --x) { opAdj(op, L.list[x], cursor + (uint64_t)x); }
+                }
+                __syncwarp();
+            }
+        }
+    };
+    setDisplacement(n - 1, true);
+    passAdj(kRestitute);
+    for (int sub = n - 1; sub >= 0; --sub) {
+        setDisplacement(sub, true);
+        passAdj(kRelax);
+        // Position update in reverse.
+        for (uint32_t i = lane; i < V.bodyCount; i += 32) {
+            const uint32_t g = V.bodyFirst + i;
+            if (!movesIn(M, V, g)) { continue; }
+            T* s = M.stateAdj + (size_t)g * kState;
+            const T* L = integLog + ((size_t)sub * M.S.totalBodies + g) * kIntegWords;
+            const Q4<T> q = ld4(L);
+            const V3<T> wv = ld3(L + 4);
+            const Q4<T> nq = integrateQ(q, wv, M.h);
+            const Q4<T> qb = ld4(in + (size_t)g * kState + 3);
+            // dq' = q' qBase*: its adjoint goes to q' and to qBase.
+            const Q4<T> dqG = ld4(M.dqAdj + 4 * (size_t)g);
+            Q4<T> qG = qadd(ld4(s + 3), qmulAdjA(dqG, conj(qb)));
+            const Q4<T> cG = qmulAdjB(dqG, nq);
+            st4(M.qBaseAdj + 4 * (size_t)g, qadd(ld4(M.qBaseAdj + 4 * (size_t)g), Q4<T>{ -cG.x, -cG.y, -cG.z, cG.w }));
+            st4(M.dqAdj + 4 * (size_t)g, Q4<T>{ 0, 0, 0, 0 });
+            Q4<T> qPrevG{ 0, 0, 0, 0 };
+            V3<T> wG = ld3(s + 10);
+            integrateQAdj(q, wv, M.h, qG, qPrevG, wG);
+            st4(s + 3, qPrevG);
+            st3(s + 10, wG);
+            // com' = com + v h and dp' = dp + v h.
+            const V3<T> vG = ld3(s + 7) + ld3(s) * M.h + ld3(M.dpAdj + 3 * (size_t)g) * M.h;
+            st3(s + 7, vG);
+        }
+        __syncwarp();
+        setDisplacement(sub, false);
+        passAdj(kBias);
+        passAdj(kWarm);
+        // Velocity update in reverse.
+        for (uint32_t i = lane; i < V.bodyCount; i += 32) {
+            const uint32_t g = V.bodyFirst + i;
+            if (!movesIn(M, V, g)) { continue; }
+            T* s = M.stateAdj + (size_t)g * kState;
+            st3(s + 7, ld3(s + 7) * (T(1) / (T(1) + M.h * T(M.S.linearDamping[g]))));
+            st3(s + 10, ld3(s + 10) * (T(1) / (T(1) + M.h * T(M.S.angularDamping[g]))));
+        }
+        __syncwarp();
+    }
+    // Step start in reverse: qBase = q, the world inverse inertia r L r^T and the inverse mass 1/m.
+    for (uint32_t i = lane; i < V.bodyCount; i += 32) {
+        const uint32_t g = V.bodyFirst + i;
+        T* s = M.stateAdj + (size_t)g * kState;
+        st4(s + 3, qadd(ld4(s + 3), ld4(M.qBaseAdj + 4 * (size_t)g)));
+        if (!movesIn(M, V, g)) { continue; }
+        const Q4<T> q = ld4(in + (size_t)g * kState + 3);
+        const T m = M.mass[g];
+        const T scale = T(M.S.mass[g]) / m;
+        M3<T> L;
+        for (int a = 0; a < 3; ++a) {
+            L.r[a] = { T(M.S.invInertiaLocal[9 * g + 3 * a]) * scale, T(M.S.invInertiaLocal[9 * g + 3 * a + 1]) * scale,
+                       T(M.S.invInertiaLocal[9 * g + 3 * a + 2]) * scale };
+        }
+        const M3<T> r = toMat3(q);
+        const M3<T> G = ldM(M.invIAdj + 9 * (size_t)g);
+        // I = r L r^T: dr = G r L^T + G^T r L, dL = r^T G r.
+        const M3<T> rG = madd(mmul(G, mmul(r, transposeM(L))), mmul(transposeM(G), mmul(r, L)));
+        const M3<T> LG = mmul(transposeM(r), mmul(G, r));
+        T lG = 0;  // sum of dL_ij L_ij, for the mass
+        for (int a = 0; a < 3; ++a) { lG += dot(LG.r[a], L.r[a]); }
+        st4(s + 3, qadd(ld4(s + 3), toMat3Adj(q, rG)));
+        // im = 1/m and L = L0 m0 / m: both scale as 1/m.
+        M.massAdj[g] += -(M.invMAdj[g] / (m * m)) - lG / m;
+    }
+    __syncwarp();
+}
+
+// ---------------------------------------------------------------------------------------------------------
+// Kernels: one warp per world, every step of the run.
+
+template <class T>
+__global__ void __launch_bounds__(128) k_model_forward(Model<T> M) {
+    const uint32_t w = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
+    if (w >= (uint32_t)M.S.nWorlds) { return; }
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t b0 = M.S.bodyFirst[w], nb = M.S.bodyCount[w];
+    for (uint32_t i = lane; i < nb; i += 32) {
+        const uint32_t g = b0 + i;
+        for (int k = 0; k < kState; ++k) { M.states[(size_t)g * kState + k] = M.init[(size_t)g * kState + k]; }
+    }
+    __syncwarp();
+    const size_t stride = (size_t)M.S.totalBodies * kState;
+    for (int s = 0; s < M.S.nSteps; ++s) {
+        stepWorld<T>(M, s, w, M.states + s * stride, M.states + (s + 1) * stride, nullptr, nullptr);
+        __syncwarp();
+    }
+}
+
+template <class T>
+__global__ void __launch_bounds__(128) k_model_backward(Model<T> M) {
+    const uint32_t w = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
+    if (w >= (uint32_t)M.S.nWorlds) { return; }
+    const size_t stride = (size_t)M.S.totalBodies * kState;
+    T* log = M.log + (size_t)w * M.logStride;
+    T* scratch = M.states + (size_t)(M.S.nSteps + 1) * stride;  // one state of scratch after the checkpoints
+    for (int s = M.S.nSteps - 1; s >= 0; --s) {
+        // Recompute the step from its checkpoint, logging every operation's inputs.
+        stepWorld(M, s, w, M.states + s * stride, scratch, log, M.integLog);
+        __syncwarp();
+        // The number of contact operations the step logged: every pass walks its lists once.
+        const WorldView V = viewOf(M.S, s, w);
+        const TapeWorld& tw = *V.tw;
+        const uint64_t colored = tw.colorStart[tw.colorCount] + tw.restCount;
+        const uint64_t impact = tw.impactColorStart[tw.impactColorCount] + tw.impactRestCount;
+        const uint64_t calls = (uint64_t)M.S.substeps * (3 * colored + 2 * impact) + colored;
+        stepWorldAdj(M, s, w, M.states + s * stride, log, M.integLog, calls);
+        __syncwarp();
+    }
+}
+
+// ---------------------------------------------------------------------------------------------------------
+// Host side: buffers of one differentiation run, in the precision it was started with.
+
+struct Run {
+    int precision = 0;
+    size_t elem = 0;
+    std::vector<void*> owned;
+    void* mass = nullptr;
+    void* friction = nullptr;
+    void* init = nullptr;
+    void* states = nullptr;
+    void *invM = nullptr, *invI = nullptr, *dp = nullptr, *dq = nullptr, *qBase = nullptr, *points = nullptr;
+    void *stateAdj = nullptr, *dpAdj = nullptr, *dqAdj = nullptr, *qBaseAdj = nullptr, *invMAdj = nullptr,
+         *invIAdj = nullptr, *pointAdj = nullptr, *massAdj = nullptr, *frictionAdj = nullptr, *log = nullptr,
+         *integLog = nullptr;
+    uint64_t logStride = 0;
+    bool forwardDone = false;
+    float forwardMs = 0.0f, backwardMs = 0.0f;
+
+    ~Run() { release(); }
+    void release() {
+        for (void* p : owned) { cudaFree(p); }
+        owned.clear();
+        for (void** p : { &mass, &friction, &init, &states, &invM, &invI, &dp, &dq, &qBase, &points, &stateAdj, &dpAdj,
+                          &dqAdj, &qBaseAdj, &invMAdj, &invIAdj, &pointAdj, &massAdj, &frictionAdj, &log, &integLog }) {
+            *p = nullptr;
+        }
+        forwardDone = false;
+    }
+    int alloc(void** p, size_t bytes) {
+        cudaError_t e = cudaMalloc(p, bytes < 16 ? 16 : bytes);
+        if (e != cudaSuccess) { return noteError(TF_E_CUDA, std::string("adjoint: cudaMalloc: ") + cudaGetErrorString(e)); }
+        owned.push_back(*p);
+        return TF_OK;
+    }
+};
+
+#define TF_ADJ_CUDA(call)                                                                                         \
+    do {                                                                                                          \
+        cudaError_t e_ = (call);                                                                                  \
+        if (e_ != cudaSuccess) { return noteError(TF_E_CUDA, std::string("adjoint: " #call ": ") + cudaGetErrorString(e_)); } \
+    } while (0)
+
+template <class T>
+Model<T> modelOf(const AdjointSetup& S, Run& r) {
+    Model<T> M;
+    M.S = S;
+    M.dt = T(S.dt);
+    M.h = T(S.dt) / T(S.substeps);
+    M.invH = T(1) / M.h;
+    M.gravity = { T(S.gravity[0]), T(S.gravity[1]), T(S.gravity[2]) };
+    M.contactSoft = { T(S.contactSoft[0]), T(S.contactSoft[1]), T(S.contactSoft[2]) };
+    M.staticSoft = { T(S.staticSoft[0]), T(S.staticSoft[1]), T(S.staticSoft[2]) };
+    M.maxPushout = T(S.maxPushout);
+    M.restThreshold = T(S.restitutionThreshold);
+    M.mass = (const T*)r.mass;
+    M.friction = (const T*)r.friction;
+    M.init = (const T*)r.init;
+    M.states = (T*)r.states;
+    M.invM = (T*)r.invM;
+    M.invI = (T*)r.invI;
+    M.dp = (T*)r.dp;
+    M.dq = (T*)r.dq;
+    M.qBase = (T*)r.qBase;
+    M.points = (PointState<T>*)r.points;
+    M.stateAdj = (T*)r.stateAdj;
+    M.dpAdj = (T*)r.dpAdj;
+    M.dqAdj = (T*)r.dqAdj;
+    M.qBaseAdj = (T*)r.qBaseAdj;
+    M.invMAdj = (T*)r.invMAdj;
+    M.invIAdj = (T*)r.invIAdj;
+    M.pointAdj = (PointState<T>*)r.pointAdj;
+    M.massAdj = (T*)r.massAdj;
+    M.frictionAdj = (T*)r.frictionAdj;
+    M.log = (T*)r.log;
+    M.logStride = r.logStride;
+    M.integLog = (T*)r.integLog;
+    return M;
+}
+
+// Host values in double to device values in T.
+template <class T>
+int upload(void* dst, const std::vector<double>& src, cudaStream_t stream) {
+    std::vector<T> t(src.begin(), src.end());
+    TF_ADJ_CUDA(cudaMemcpyAsync(dst, t.data(), t.size() * sizeof(T), cudaMemcpyHostToDevice, stream));
+    TF_ADJ_CUDA(cudaStreamSynchronize(stream));
+    return TF_OK;
+}
+template <class T>
+int download(std::vector<double>& dst, const void* src, size_t n, cudaStream_t stream) {
+    std::vector<T> t(n);
+    TF_ADJ_CUDA(cudaMemcpyAsync(t.data(), src, n * sizeof(T), cudaMemcpyDeviceToHost, stream));
+    TF_ADJ_CUDA(cudaStreamSynchronize(stream));
+    dst.assign(t.begin(), t.end());
+    return TF_OK;
+}
+
+template <class T>
+int forwardT(Run& r, const AdjointSetup& S, cudaStream_t stream, const double* init, const double* mass,
+             const double* friction, double* finalState) {
+    const size_t nb = S.totalBodies, ns = S.totalShapes;
+    r.release();
+    r.elem = sizeof(T);
+    int rc;
+    const size_t stateBytes = nb * kState * sizeof(T);
+    if ((rc = r.alloc(&r.mass, nb * sizeof(T))) || (rc = r.alloc(&r.friction, ns * sizeof(T))) ||
+        (rc = r.alloc(&r.init, stateBytes)) || (rc = r.alloc(&r.states, stateBytes * (size_t)(S.nSteps + 2))) ||
+        (rc = r.alloc(&r.invM, nb * sizeof(T))) || (rc = r.alloc(&r.invI, 9 * nb * sizeof(T))) ||
+        (rc = r.alloc(&r.dp, 3 * nb * sizeof(T))) || (rc = r.alloc(&r.dq, 4 * nb * sizeof(T))) ||
+        (rc = r.alloc(&r.qBase, 4 * nb * sizeof(T))) ||
+        (rc = r.alloc(&r.points, (size_t)S.contactSlots * 4 * sizeof(PointState<T>)))) {
+        return rc;
+    }
+    // Parameters: the caller's, else the recorded ones.
+    std::vector<double> h(nb * kState);
+    {
+        std::vector<float> com(3 * nb), q(4 * nb), v(3 * nb), w(3 * nb);
+        TF_ADJ_CUDA(cudaMemcpy(com.data(), S.com0, com.size() * 4, cudaMemcpyDeviceToHost));
+        TF_ADJ_CUDA(cudaMemcpy(q.data(), S.q0, q.size() * 4, cudaMemcpyDeviceToHost));
+        TF_ADJ_CUDA(cudaMemcpy(v.data(), S.v0, v.size() * 4, cudaMemcpyDeviceToHost));
+        TF_ADJ_CUDA(cudaMemcpy(w.data(), S.w0, w.size() * 4, cudaMemcpyDeviceToHost));
+        for (size_t g = 0; g < nb; ++g) {
+            for (int k = 0; k < 3; ++k) { h[g * kState + k] = com[3 * g + k]; }
+            for (int k = 0; k < 4; ++k) { h[g * kState + 3 + k] = q[4 * g + k]; }
+            for (int k = 0; k < 3; ++k) { h[g * kState + 7 + k] = v[3 * g + k]; }
+            for (int k = 0; k < 3; ++k) { h[g * kState + 10 + k] = w[3 * g + k]; }
+        }
+        if (init) { h.assign(init, init + nb * kState); }
+    }
+    if ((rc = upload<T>(r.init, h, stream)) != TF_OK) { return rc; }
+    std::vector<double> m(nb), f(ns);
+    {
+        std::vector<float> mf(nb), ff(ns);
+        TF_ADJ_CUDA(cudaMemcpy(mf.data(), S.mass, nb * 4, cudaMemcpyDeviceToHost));
+        TF_ADJ_CUDA(cudaMemcpy(ff.data(), S.friction, ns * 4, cudaMemcpyDeviceToHost));
+        for (size_t g = 0; g < nb; ++g) { m[g] = mass ? mass[g] : (double)mf[g]; }
+        for (size_t k = 0; k < ns; ++k) { f[k] = friction ? friction[k] : (double)ff[k]; }
+    }
+    for (size_t g = 0; g < nb; ++g) {
+        if (!(m[g] > 0.0)) { m[g] = 1.0; }  // bodies without mass (static ones) never use it
+    }
+    if ((rc = upload<T>(r.mass, m, stream)) != TF_OK || (rc = upload<T>(r.friction, f, stream)) != TF_OK) { return rc; }
+    Model<T> M = modelOf<T>(S, r);
+    cudaEvent_t e0, e1;
+    TF_ADJ_CUDA(cudaEventCreate(&e0));
+    TF_ADJ_CUDA(cudaEventCreate(&e1));
+    cudaEventRecord(e0, stream);
+    const int blocks = (S.nWorlds + 3) / 4;
+    k_model_forward<T><<<blocks, 128, 0, stream>>>(M);
+    cudaEventRecord(e1, stream);
+    TF_ADJ_CUDA(cudaGetLastError());
+    TF_ADJ_CUDA(cudaStreamSynchronize(stream));
+    cudaEventElapsedTime(&r.forwardMs, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    std::vector<double> out;
+    if ((rc = download<T>(out, (const char*)r.states + stateBytes * (size_t)S.nSteps, nb * kState, stream)) != TF_OK) { return rc; }
+    if (finalState) { std::copy(out.begin(), out.end(), finalState); }
+    r.forwardDone = true;
+    return TF_OK;
+}
+
+// The largest number of contact operations one world logs in one step.
+int maxCalls(const AdjointSetup& S, uint64_t* out) {
+    std::vector<TapeStep> steps(S.nSteps);
+    TF_ADJ_CUDA(cudaMemcpy(steps.data(), S.steps, steps.size() * sizeof(TapeStep), cudaMemcpyDeviceToHost));
+    std::vector<TapeWorld> tw(S.nWorlds);
+    uint64_t most = 1;
+    for (const TapeStep& ts : steps) {
+        TF_ADJ_CUDA(cudaMemcpy(tw.data(), ts.worlds, tw.size() * sizeof(TapeWorld), cudaMemcpyDeviceToHost));
+        for (const TapeWorld& w : tw) {
+            const uint64_t colored = w.colorStart[w.colorCount] + w.restCount;
+            const uint64_t impact = w.impactColorStart[w.impactColorCount] + w.impactRestCount;
+            most = std::max<uint64_t>(most, (uint64_t)S.substeps * (3 * colored + 2 * impact) + colored);
+        }
+    }
+    *out = most;
+    return TF_OK;
+}
+
+template <class T>
+int backwardT(Run& r, const AdjointSetup& S, cudaStream_t stream, const double* gradFinal, double* gradInit,
+              double* gradMass, double* gradFriction) {
+    const size_t nb = S.totalBodies, ns = S.totalShapes;
+    int rc;
+    uint64_t calls = 0;
+    if ((rc = maxCalls(S, &calls)) != TF_OK) { return rc; }
+    r.logStride = calls * (uint64_t)callWords<T>();
+    if (!r.stateAdj) {
+        if ((rc = r.alloc(&r.stateAdj, nb * kState * sizeof(T))) || (rc = r.alloc(&r.dpAdj, 3 * nb * sizeof(T))) ||
+            (rc = r.alloc(&r.dqAdj, 4 * nb * sizeof(T))) || (rc = r.alloc(&r.qBaseAdj, 4 * nb * sizeof(T))) ||
+            (rc = r.alloc(&r.invMAdj, nb * sizeof(T))) || (rc = r.alloc(&r.invIAdj, 9 * nb * sizeof(T))) ||
+            (rc = r.alloc(&r.pointAdj, (size_t)S.contactSlots * 4 * sizeof(PointState<T>))) ||
+            (rc = r.alloc(&r.massAdj, nb * sizeof(T))) || (rc = r.alloc(&r.frictionAdj, ns * sizeof(T))) ||
+            (rc = r.alloc(&r.integLog, (size_t)S.substeps * nb * kIntegWords * sizeof(T))) ||
+            (rc = r.alloc(&r.log, (size_t)S.nWorlds * r.logStride * sizeof(T)))) {
+            return rc;
+        }
+    }
+    std::vector<double> g(gradFinal, gradFinal + nb * kState);
+    if ((rc = upload<T>(r.stateAdj, g, stream)) != TF_OK) { return rc; }
+    TF_ADJ_CUDA(cudaMemsetAsync(r.massAdj, 0, nb * sizeof(T), stream));
+    TF_ADJ_CUDA(cudaMemsetAsync(r.frictionAdj, 0, ns * sizeof(T), stream));
+    Model<T> M = modelOf<T>(S, r);
+    cudaEvent_t e0, e1;
+    TF_ADJ_CUDA(cudaEventCreate(&e0));
+    TF_ADJ_CUDA(cudaEventCreate(&e1));
+    cudaEventRecord(e0, stream);
+    const int blocks = (S.nWorlds + 3) / 4;
+    k_model_backward<T><<<blocks, 128, 0, stream>>>(M);
+    cudaEventRecord(e1, stream);
+    TF_ADJ_CUDA(cudaGetLastError());
+    TF_ADJ_CUDA(cudaStreamSynchronize(stream));
+    cudaEventElapsedTime(&r.backwardMs, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    std::vector<double> out;
+    if (gradInit) {
+        if ((rc = download<T>(out, r.stateAdj, nb * kState, stream)) != TF_OK) { return rc; }
+        std::copy(out.begin(), out.end(), gradInit);
+    }
+    if (gradMass) {
+        if ((rc = download<T>(out, r.massAdj, nb, stream)) != TF_OK) { return rc; }
+        std::copy(out.begin(), out.end(), gradMass);
+    }
+    if (gradFriction) {
+        if ((rc = download<T>(out, r.frictionAdj, ns, stream)) != TF_OK) { return rc; }
+        std::copy(out.begin(), out.end(), gradFriction);
+    }
+    return TF_OK;
+}
+
+}  // namespace adj
+
+// Entry points for the C ABI (tf_engine.cu): one run per batch.
+void* adjointCreate() { return new adj::Run(); }
+void adjointDestroy(void* run) { delete static_cast<adj::Run*>(run); }
+
+int adjointForward(void* run, const AdjointSetup& S, void* stream, int precision, const double* init, const double* mass,
+                   const double* friction, double* finalState) {
+    adj::Run& r = *static_cast<adj::Run*>(run);
+    r.precision = precision;
+    const cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (precision == 64) { return adj::forwardT<double>(r, S, st, init, mass, friction, finalState); }
+    if (precision == 32) { return adj::forwardT<float>(r, S, st, init, mass, friction, finalState); }
+    return noteError(TF_E_INVALID, "adjoint: precision must be 32 or 64");
+}
+
+int adjointBackward(void* run, const AdjointSetup& S, void* stream, const double* gradFinal, double* gradInit,
+                    double* gradMass, double* gradFriction) {
+    adj::Run& r = *static_cast<adj::Run*>(run);
+    if (!r.forwardDone) { return noteError(TF_E_INVALID, "adjoint: backward needs a forward run first"); }
+    const cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (r.precision == 64) { return adj::backwardT<double>(r, S, st, gradFinal, gradInit, gradMass, gradFriction); }
+    return adj::backwardT<float>(r, S, st, gradFinal, gradInit, gradMass, gradFriction);
+}
+
+void adjointTimes(void* run, float* ms) {
+    const adj::Run& r = *static_cast<adj::Run*>(run);
+    ms[0] = r.forwardMs;
+    ms[1] = r.backwardMs;
+}
+
+}  // namespace tfb

@@ -20,6 +20,7 @@
 #include "../../include/twofold_b200.h"
 #include "tf_build.h"
 #include "tf_kernels.cuh"
+#include "tf_tape.h"
 
 namespace tfb {
 
@@ -92,6 +93,15 @@ Quat q4of(const float* p) { return { p[0], p[1], p[2], p[3] }; }
 
 // Records a failure from another translation unit of the library for tf_last_error.
 int noteError(int code, const std::string& msg) { return fail(code, msg); }
+
+// The differentiable model (tf_adjoint.cu).
+void* adjointCreate();
+void adjointDestroy(void* run);
+int adjointForward(void* run, const AdjointSetup& S, void* stream, int precision, const double* init, const double* mass,
+                   const double* friction, double* finalState);
+int adjointBackward(void* run, const AdjointSetup& S, void* stream, const double* gradFinal, double* gradInit,
+                    double* gradMass, double* gradFriction);
+void adjointTimes(void* run, float* ms);
 
 class Engine {
 public:
@@ -213,6 +223,7 @@ public:
     // The device arrays free themselves after this body, with the engine's device still current.
     ~Engine() {
         if (stream) { cudaSetDevice(device); }
+        if (adjRun) { adjointDestroy(adjRun); }
         for (cudaEvent_t e : eventPool) { cudaEventDestroy(e); }
         if (callStart) { cudaEventDestroy(callStart); }
         if (callStop) { cudaEventDestroy(callStop); }
@@ -875,6 +886,10 @@ public:
         timed(2, rec, [&] { k_wake<<<grids[2], threads(2), 0, stream>>>(B, splits[2], serial); });
         if (marks) { cudaEventRecord(marks[2], stream); }
         timed(3, rec, [&] { k_prepare<<<grids[3], threads(3), smem(3), stream>>>(B, P, splits[3], serial); });
+        if (recording && !capturing) {
+            const int rc = recordStep(B, serial);
+            if (rc != TF_OK) { return rc; }
+        }
         for (int i = 0; i < P.substeps; ++i) {
             if (i > 0) {
                 timed(4, rec, [&] {
@@ -1029,6 +1044,148 @@ public:
         out[3] = (uint32_t)grids[k];
         out[4] = splits[k].big.bodies;
         out[5] = splits[k].small.bodies;
+        return TF_OK;
+    }
+
+    // ---- Recording for the adjoint: what each step's solve saw (twofold_b200/csrc/tf_tape.h) ----
+
+    struct TapeBuffers {
+        DevArray<TapeWorld> worlds;
+        DevArray<TapeContact> contacts;
+        DevArray<uint32_t> colored, impactColored, rest, impactRest;
+        DevArray<uint8_t> awake;
+    };
+    std::vector<std::unique_ptr<TapeBuffers>> tape;
+    int tapeCursor = 0;     // the step being recorded
+    bool recording = false;
+    DevArray<TapeStep> dTapeSteps;
+    DevArray<uint32_t> dTBodyFirst, dTBodyCount, dTShapeFirst;
+    DevArray<uint8_t> dTDynamic;
+    DevArray<float> dTGravityScale, dTLinDamp, dTAngDamp, dTMass, dTInvIL, dTCom0, dTQ0, dTV0, dTW0, dTFriction;
+    AdjointSetup adjoint{};
+    bool taped = false;
+    void* adjRun = nullptr;
+
+    // Launched after k_prepare while recording; sizes the step's buffers to the current layout first.
+    int recordStep(const Batch& B, int serial) {
+        if (tapeCursor >= (int)tape.size()) { return fail(TF_E_INVALID, "recording: more steps than the tape holds"); }
+        TapeBuffers& T = *tape[(size_t)tapeCursor];
+        const size_t ncon = dContacts[0].n;
+        int rc;
+        if ((rc = T.worlds.alloc(worlds.size())) != TF_OK || (rc = T.contacts.alloc(ncon)) != TF_OK ||
+            (rc = T.colored.alloc(ncon)) != TF_OK || (rc = T.impactColored.alloc(ncon)) != TF_OK ||
+            (rc = T.rest.alloc(ncon)) != TF_OK || (rc = T.impactRest.alloc(ncon)) != TF_OK ||
+            (rc = T.awake.alloc(totalBodies)) != TF_OK) {
+            return rc;
+        }
+        const TapeStep ts{ T.worlds.ptr, T.contacts.ptr, T.colored.ptr, T.impactColored.ptr, T.rest.ptr, T.impactRest.ptr,
+                           T.awake.ptr };
+        k_tape_record<<<grids[3], shapes[3].threads, 0, stream>>>(B, splits[3], ts, serial);
+        return TF_OK;
+    }
+
+    // Records n steps of dt from the current state (stepping the batch), for the adjoint to replay.
+    int tapeRecord(float dt, int nSteps) {
+        if (!(dt > 0.0f) || !std::isfinite(dt) || nSteps <= 0) { return fail(TF_E_INVALID, "tape: bad dt or steps"); }
+        TF_CUDA(cudaSetDevice(device));
+        int rc = prepareDevice();
+        if (rc != TF_OK) { return rc; }
+        if ((rc = pull()) != TF_OK) { return rc; }
+        // Constants and the initial state, from the host mirrors.
+        const size_t nw = worlds.size();
+        std::vector<uint32_t> bodyFirst(nw), bodyCount(nw), shapeFirst(nw);
+        std::vector<uint8_t> dyn(totalBodies);
+        std::vector<float> gs(totalBodies), ld(totalBodies), ad(totalBodies), mass(totalBodies), invIL(9 * totalBodies);
+        std::vector<float> com(3 * totalBodies), q(4 * totalBodies), v(3 * totalBodies), w(3 * totalBodies);
+        std::vector<float> friction(totalShapes);
+        for (size_t k = 0; k < nw; ++k) {
+            const HostWorld& W = worlds[k];
+            bodyFirst[k] = info[k].bodyFirst;
+            bodyCount[k] = info[k].bodyCount;
+            shapeFirst[k] = info[k].shapeFirst;
+            for (size_t i = 0; i < W.bodies.size(); ++i) {
+                const DBody& d = W.bodies[i].d;
+                const size_t g = info[k].bodyFirst + i;
+                if (d.alive && d.locks != 0) { return fail(TF_E_UNSUPPORTED, "tape: locked bodies are not differentiated"); }
+                dyn[g] = d.alive && d.type == kDynamic ? 1 : 0;
+                gs[g] = d.gravityScale;
+                ld[g] = d.linearDamping;
+                ad[g] = d.angularDamping;
+                mass[g] = d.mass;
+                const Mat3 ii = dyn[g] ? inverse(d.inertia) : mzero();
+                for (int r = 0; r < 3; ++r) {
+                    invIL[9 * g + 3 * r] = ii.r[r].x, invIL[9 * g + 3 * r + 1] = ii.r[r].y, invIL[9 * g + 3 * r + 2] = ii.r[r].z;
+                }
+                com[3 * g] = d.com.x, com[3 * g + 1] = d.com.y, com[3 * g + 2] = d.com.z;
+                q[4 * g] = d.xf.q.x, q[4 * g + 1] = d.xf.q.y, q[4 * g + 2] = d.xf.q.z, q[4 * g + 3] = d.xf.q.w;
+                v[3 * g] = d.v.x, v[3 * g + 1] = d.v.y, v[3 * g + 2] = d.v.z;
+                w[3 * g] = d.w.x, w[3 * g + 1] = d.w.y, w[3 * g + 2] = d.w.z;
+            }
+            for (size_t i = 0; i < W.shapes.size(); ++i) {
+                const DShape& sd = W.shapes[i].d;
+                if (sd.rollingResistance > 0.0f) { return fail(TF_E_UNSUPPORTED, "tape: rolling resistance is not differentiated"); }
+                friction[info[k].shapeFirst + i] = sd.friction;
+            }
+        }
+        auto up = [&](auto& arr, const auto& host) -> int {
+            int r = arr.alloc(host.size());
+            if (r != TF_OK) { return r; }
+            TF_CUDA(cudaMemcpy(arr.ptr, host.data(), host.size() * sizeof(host[0]), cudaMemcpyHostToDevice));
+            return TF_OK;
+        };
+        if ((rc = up(dTBodyFirst, bodyFirst)) || (rc = up(dTBodyCount, bodyCount)) || (rc = up(dTShapeFirst, shapeFirst)) ||
+            (rc = up(dTDynamic, dyn)) || (rc = up(dTGravityScale, gs)) || (rc = up(dTLinDamp, ld)) ||
+            (rc = up(dTAngDamp, ad)) || (rc = up(dTMass, mass)) || (rc = up(dTInvIL, invIL)) || (rc = up(dTCom0, com)) ||
+            (rc = up(dTQ0, q)) || (rc = up(dTV0, v)) || (rc = up(dTW0, w)) || (rc = up(dTFriction, friction))) {
+            return rc;
+        }
+        tape.clear();
+        for (int k = 0; k < nSteps; ++k) { tape.emplace_back(new TapeBuffers()); }
+        taped = false;
+        recording = true;
+        for (tapeCursor = 0; tapeCursor < nSteps && rc == TF_OK; ++tapeCursor) { rc = step(dt, 1); }
+        recording = false;
+        if (rc != TF_OK) { return rc; }
+        std::vector<TapeStep> steps;
+        size_t slots = 0;
+        for (auto& T : tape) {
+            steps.push_back(TapeStep{ T->worlds.ptr, T->contacts.ptr, T->colored.ptr, T->impactColored.ptr, T->rest.ptr,
+                                      T->impactRest.ptr, T->awake.ptr });
+            slots = std::max(slots, T->contacts.n);
+        }
+        if ((rc = up(dTapeSteps, steps)) != TF_OK) { return rc; }
+        const StepParams P = params(dt);
+        AdjointSetup& A = adjoint;
+        A.nWorlds = (int)nw;
+        A.nSteps = nSteps;
+        A.totalBodies = (uint32_t)totalBodies;
+        A.totalShapes = (uint32_t)totalShapes;
+        A.contactSlots = (uint32_t)slots;
+        A.bodyFirst = dTBodyFirst.ptr;
+        A.bodyCount = dTBodyCount.ptr;
+        A.shapeFirst = dTShapeFirst.ptr;
+        A.steps = dTapeSteps.ptr;
+        A.dynamic = dTDynamic.ptr;
+        A.gravityScale = dTGravityScale.ptr;
+        A.linearDamping = dTLinDamp.ptr;
+        A.angularDamping = dTAngDamp.ptr;
+        A.mass = dTMass.ptr;
+        A.invInertiaLocal = dTInvIL.ptr;
+        A.com0 = dTCom0.ptr;
+        A.q0 = dTQ0.ptr;
+        A.v0 = dTV0.ptr;
+        A.w0 = dTW0.ptr;
+        A.friction = dTFriction.ptr;
+        A.gravity[0] = P.gravity.x, A.gravity[1] = P.gravity.y, A.gravity[2] = P.gravity.z;
+        A.dt = dt;
+        A.substeps = P.substeps;
+        A.contactSoft[0] = P.contactSoft.biasRate, A.contactSoft[1] = P.contactSoft.massScale,
+        A.contactSoft[2] = P.contactSoft.impulseScale;
+        A.staticSoft[0] = P.staticSoft.biasRate, A.staticSoft[1] = P.staticSoft.massScale,
+        A.staticSoft[2] = P.staticSoft.impulseScale;
+        A.maxPushout = P.maxPushout;
+        A.restitutionThreshold = P.restitutionThreshold;
+        taped = true;
         return TF_OK;
     }
 
@@ -1742,6 +1899,38 @@ TF_API int tf_world_work_counts(void* h, int64_t out[6]) {
 TF_API int tf_world_launch_count(void* h, int64_t* launches) {
     if (!h || !launches) { return tfb::fail(TF_E_INVALID, "tf_world_launch_count: null"); }
     *launches = E(h)->launches;
+    return TF_OK;
+}
+
+TF_API int tf_tape_record(void* h, float dt, int32_t n_steps) {
+    if (!h) { return tfb::fail(TF_E_INVALID, "tf_tape_record: null"); }
+    return E(h)->tapeRecord(dt, n_steps);
+}
+
+TF_API int tf_adjoint_forward(void* h, int32_t precision, const double* initial_state, const double* mass,
+                              const double* friction, double* final_state) {
+    if (!h) { return tfb::fail(TF_E_INVALID, "tf_adjoint_forward: null"); }
+    Engine* e = E(h);
+    if (!e->taped) { return tfb::fail(TF_E_INVALID, "tf_adjoint_forward: record a run with tf_tape_record first"); }
+    if (cudaSetDevice(e->device) != cudaSuccess) { return tfb::fail(TF_E_CUDA, "tf_adjoint_forward: cudaSetDevice"); }
+    if (!e->adjRun) { e->adjRun = tfb::adjointCreate(); }
+    return tfb::adjointForward(e->adjRun, e->adjoint, e->stream, precision, initial_state, mass, friction, final_state);
+}
+
+TF_API int tf_adjoint_backward(void* h, const double* grad_final, double* grad_initial, double* grad_mass,
+                               double* grad_friction) {
+    if (!h || !grad_final) { return tfb::fail(TF_E_INVALID, "tf_adjoint_backward: null"); }
+    Engine* e = E(h);
+    if (!e->adjRun) { return tfb::fail(TF_E_INVALID, "tf_adjoint_backward: run tf_adjoint_forward first"); }
+    if (cudaSetDevice(e->device) != cudaSuccess) { return tfb::fail(TF_E_CUDA, "tf_adjoint_backward: cudaSetDevice"); }
+    return tfb::adjointBackward(e->adjRun, e->adjoint, e->stream, grad_final, grad_initial, grad_mass, grad_friction);
+}
+
+TF_API int tf_adjoint_elapsed_ms(void* h, float ms[2]) {
+    if (!h || !ms) { return tfb::fail(TF_E_INVALID, "tf_adjoint_elapsed_ms: null"); }
+    Engine* e = E(h);
+    ms[0] = ms[1] = 0.0f;
+    if (e->adjRun) { tfb::adjointTimes(e->adjRun, ms); }
     return TF_OK;
 }
 

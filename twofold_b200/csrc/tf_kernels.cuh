@@ -18,6 +18,7 @@
 
 #include "tf_batch.cuh"
 #include "tf_solver.cuh"
+#include "tf_tape.h"
 
 namespace tfb {
 
@@ -37,7 +38,8 @@ enum WorkSlot : int {
     kSlotCandItems = kSlotFinish + 1,                    // + pair class: candidate items of that class
     kSlotFastItems = kSlotCandItems + kPairClasses,       // + pair class: fast contacts of that class; + kPairClasses:
                                                           // the other active contacts of refreshed worlds
-    kSlotCount = kSlotFastItems + kPairClasses + 1
+    kSlotTape = kSlotFastItems + kPairClasses + 1,      // the recording kernel's world counter
+    kSlotCount = kSlotTape + 1
 };
 
 // A group of threads that steps one world at a time: one warp, several warps, or the whole CTA.
@@ -1587,6 +1589,72 @@ __global__ void __launch_bounds__(kMaxBlock) k_finish(const __grid_constant__ Ba
 // Host traffic of a running batch: per-step forces in, poses out.
 
 // World::addForce / addTorque with wake = false on every body (src/world.cpp:2118-2142).
+// Records what this step's solve will see, right after preparation: every contact of every world with its
+// lists and the awake dynamic bodies. One group per world.
+__global__ void __launch_bounds__(kMaxBlock) k_tape_record(const __grid_constant__ Batch B, const __grid_constant__ Split sp,
+                                                           TapeStep T, int serial) {
+    if (stepAborted(B, serial)) { return; }
+    forWorlds(B, kSlotTape, sp, nullptr, [&](const Group& g, uint32_t w, unsigned char*, const StageSizes&) {
+        const WorldInfo wi = B.info[w];
+        const WorldCounts& wc = B.counts[w];
+        const uint32_t cf = wi.contactFirst;
+        if (g.tid == 0) {
+            TapeWorld& tw = T.worlds[w];
+            tw.contactFirst = cf;
+            tw.contactCount = wc.contactCount;
+            tw.colorCount = wc.colorCount;
+            tw.impactColorCount = wc.impactColorCount;
+            tw.restCount = wc.restCount;
+            tw.impactRestCount = wc.impactRestCount;
+            for (int k = 0; k < kTapeColors; ++k) {
+                tw.colorStart[k] = wc.colorStart[k];
+                tw.impactColorStart[k] = wc.impactColorStart[k];
+            }
+        }
+        for (uint32_t i = g.tid; i < wc.contactCount; i += g.size) {
+            const DContact& c = B.contacts[cf + i];
+            TapeContact t;
+            t.a = c.bodyA - wi.bodyFirst;
+            t.b = c.bodyB - wi.bodyFirst;
+            t.shapeA = c.shapeA - wi.shapeFirst;
+            t.shapeB = c.shapeB - wi.shapeFirst;
+            t.count = c.count;
+            t.restitution = c.restitution;
+            const Vec3 dirs[3] = { c.normal, c.tangent1, c.tangent2 };
+            float* out[3] = { t.normal, t.t1, t.t2 };
+            for (int d = 0; d < 3; ++d) {
+                out[d][0] = dirs[d].x;
+                out[d][1] = dirs[d].y;
+                out[d][2] = dirs[d].z;
+            }
+            for (int k = 0; k < 4; ++k) {
+                const DPoint& p = c.points[k];
+                const bool on = k < c.count;
+                t.anchorA[k][0] = on ? p.anchorA.x : 0.0f, t.anchorA[k][1] = on ? p.anchorA.y : 0.0f;
+                t.anchorA[k][2] = on ? p.anchorA.z : 0.0f;
+                t.anchorB[k][0] = on ? p.anchorB.x : 0.0f, t.anchorB[k][1] = on ? p.anchorB.y : 0.0f;
+                t.anchorB[k][2] = on ? p.anchorB.z : 0.0f;
+                t.adjSep[k] = on ? p.adjustedSeparation : 0.0f;
+                t.relVel[k] = on ? p.relativeVelocity : 0.0f;
+                t.normalImpulse[k] = on ? p.normalImpulse : 0.0f;
+                t.tangentImpulse[k][0] = on ? p.tangentImpulse.x : 0.0f;
+                t.tangentImpulse[k][1] = on ? p.tangentImpulse.y : 0.0f;
+                t.tangentImpulse[k][2] = on ? p.tangentImpulse.z : 0.0f;
+            }
+            T.contacts[cf + i] = t;
+        }
+        const uint32_t nColored = wc.colorStart[wc.colorCount], nImpact = wc.impactColorStart[wc.impactColorCount];
+        for (uint32_t x = g.tid; x < nColored; x += g.size) { T.colored[cf + x] = B.colored[cf + x]; }
+        for (uint32_t x = g.tid; x < nImpact; x += g.size) { T.impactColored[cf + x] = B.impactColored[cf + x]; }
+        for (uint32_t x = g.tid; x < wc.restCount; x += g.size) { T.rest[cf + x] = B.rest[cf + x]; }
+        for (uint32_t x = g.tid; x < wc.impactRestCount; x += g.size) { T.impactRest[cf + x] = B.impactRest[cf + x]; }
+        for (uint32_t i = g.tid; i < wi.bodyCount; i += g.size) {
+            T.awake[wi.bodyFirst + i] = movingBody(B.bodies[wi.bodyFirst + i]) ? 1 : 0;
+        }
+        g.sync();
+    });
+}
+
 __global__ void k_add_forces(DBody* bodies, uint32_t n, const float* __restrict__ f, const float* __restrict__ t) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) { return; }

@@ -179,6 +179,40 @@ class Batch:
         abi.check(self.lib.tf_world_autotune(self.h, C.c_float(dt), trial_steps, out.ctypes.data), self.lib)
         return {k: tuple(int(x) for x in out[3 * i:3 * i + 3]) for i, k in enumerate(self.KERNELS)}
 
+    # ---- differentiation ----
+
+    def tape_record(self, dt, n_steps):
+        """Steps n_steps times, recording each step's contact set for the differentiable model."""
+        abi.check(self.lib.tf_tape_record(self.h, C.c_float(dt), n_steps), self.lib)
+
+    def adjoint_forward(self, precision=64, initial=None, mass=None, friction=None):
+        """The model from the recorded initial state; returns the final state, (bodies, 13) float64:
+        center of mass, rotation (x, y, z, w), linear and angular velocity."""
+        total = int(self.offsets[-1])
+        out = np.zeros((total, 13), np.float64)
+        args = []
+        for a in (initial, mass, friction):
+            args.append(None if a is None else np.ascontiguousarray(a, np.float64))
+        ptr = [None if a is None else a.ctypes.data for a in args]
+        abi.check(self.lib.tf_adjoint_forward(self.h, precision, ptr[0], ptr[1], ptr[2], out.ctypes.data), self.lib)
+        return out
+
+    def adjoint_backward(self, grad_final, n_shapes):
+        """d loss / d (initial state, mass, friction) from d loss / d final state (bodies, 13)."""
+        total = int(self.offsets[-1])
+        g = np.ascontiguousarray(grad_final, np.float64)
+        gi = np.zeros((total, 13), np.float64)
+        gm = np.zeros(total, np.float64)
+        gf = np.zeros(n_shapes, np.float64)
+        abi.check(self.lib.tf_adjoint_backward(self.h, g.ctypes.data, gi.ctypes.data, gm.ctypes.data, gf.ctypes.data),
+                  self.lib)
+        return gi, gm, gf
+
+    def adjoint_ms(self):
+        ms = np.zeros(2, np.float32)
+        abi.check(self.lib.tf_adjoint_elapsed_ms(self.h, ms.ctypes.data), self.lib)
+        return float(ms[0]), float(ms[1])
+
     def launch(self, kernel):
         """The launch shape in use for one kernel, after the batch was laid out on the device."""
         k = self.KERNELS.index(kernel) if isinstance(kernel, str) else int(kernel)
