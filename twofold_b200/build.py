@@ -42,8 +42,36 @@ def stale():
 CHECKED_OUT = os.path.join(HERE, "libtwofold_b200_checked.so")
 
 
+# The differentiable model (tf_adjoint.cu) is not held to the reference's bits, so it may contract
+# multiply-adds; every other source is compiled without contraction.
+CONTRACTED = {"tf_adjoint.cu"}
+BUILD_DIR = os.path.join(HERE, "_build")
+
+
+def _flags(source):
+    flags = list(NVCC_FLAGS)
+    if os.path.basename(source) in CONTRACTED:
+        flags[flags.index("--fmad=false")] = "--fmad=true"
+    return flags
+
+
+def _object(source, variant):
+    return os.path.join(BUILD_DIR, variant, os.path.basename(source)[:-3] + ".o")
+
+
+def _compile_command(source, variant, defines):
+    return [nvcc()] + _flags(source) + [f"-D{d}" for d in defines] + ["-c", "-o", _object(source, variant), source]
+
+
+def _link_command(target, variant):
+    return [nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", target] + \
+        [_object(src, variant) for src in SOURCES]
+
+
 def _command(target, defines):
-    return [nvcc()] + NVCC_FLAGS + [f"-D{d}" for d in defines] + ["-shared", "-o", target] + SOURCES
+    """The compile commands (one per source) and the link command of one library variant."""
+    variant = os.path.basename(target)[:-3]
+    return [_compile_command(src, variant, defines) for src in SOURCES], _link_command(target, variant)
 
 
 def build(force=False, verbose=False, out=None, defines=(), checked=True):
@@ -56,18 +84,32 @@ def build(force=False, verbose=False, out=None, defines=(), checked=True):
         if not force and not stale() and (not checked or os.path.exists(CHECKED_OUT)):
             return OUT
         jobs = [(OUT, ())] + ([(CHECKED_OUT, ("TF_DEVICE_CHECKS",))] if checked else [])
-    procs = [(t, subprocess.Popen(_command(t, d), stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True))
-             for t, d in jobs]
-    for target, proc in procs:
-        log = proc.communicate()[0]
+    # Every source of every variant compiles in parallel; each variant links once its objects are done.
+    procs = []
+    for target, defines in jobs:
+        compiles, link = _command(target, defines)
+        os.makedirs(os.path.dirname(_object(SOURCES[0], os.path.basename(target)[:-3])), exist_ok=True)
+        for cmd in compiles:
+            procs.append((target, cmd, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)))
+    logs = {}
+    for target, cmd, proc in procs:
+        out = proc.communicate()[0]
+        logs.setdefault(target, []).append(" ".join(cmd) + "\n" + out)
+        if proc.returncode != 0:
+            sys.stderr.write(out)
+            raise RuntimeError(f"nvcc failed compiling {cmd[-1]} for {os.path.basename(target)}")
+    for target, defines in jobs:
+        link = _command(target, defines)[1]
+        res = subprocess.run(link, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)
+        logs[target].append(" ".join(link) + "\n" + res.stdout)
+        if res.returncode != 0:
+            sys.stderr.write(res.stdout)
+            raise RuntimeError(f"nvcc failed linking {os.path.basename(target)}")
         if target == OUT:
             with open(os.path.join(HERE, "build.log"), "w") as f:
-                f.write(" ".join(_command(target, ())) + "\n" + log)
-        if proc.returncode != 0:
-            sys.stderr.write(log)
-            raise RuntimeError(f"nvcc failed building {os.path.basename(target)}")
+                f.write("\n".join(logs[target]))
         if verbose:
-            sys.stderr.write(log)
+            sys.stderr.write("\n".join(logs[target]))
     return jobs[0][0]
 
 

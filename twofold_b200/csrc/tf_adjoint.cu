@@ -361,7 +361,21 @@ struct CallIn {
     PointState<T> p[4];
 };
 template <class T>
-__host__ __device__ constexpr int callWords() { return 12 + 4 * 5; }
+__host__ __device__ constexpr int callWords();
+// Per row of a solve (up to 8: a normal and a friction row per point): the velocities and the point state it
+// started from, logged during the recomputation so that the reverse pass need not replay the operation.
+constexpr int kRowWords = 17;
+template <class T>
+__device__ __forceinline__ void writeRow(T* log, int r, const V3<T>& va, const V3<T>& wa, const V3<T>& vb, const V3<T>& wb,
+                                         const PointState<T>& p) {
+    T* o = log + 32 + r * kRowWords;
+    st3(o, va), st3(o + 3, wa), st3(o + 6, vb), st3(o + 9, wb);
+    o[12] = p.n;
+    st3(o + 13, p.t);
+    o[16] = p.maxN;
+}
+template <class T>
+__host__ __device__ constexpr int callWords() { return 12 + 4 * 5 + kRowWords * 8; }
 
 template <class T>
 __device__ __forceinline__ void writeCall(T* log, const SBody<T>& a, const SBody<T>& b, const PointState<T>* p) {
@@ -577,7 +591,7 @@ __device__ __forceinline__ void restituteRowAdj(const Model<T>& M, const SBody<T
 // One operation on one contact, forward. The points' state comes in and goes out through p.
 template <class T>
 __device__ void contactOp(const Model<T>& M, int op, SBody<T>& a, SBody<T>& b, const CData<T>& c, PointState<T>* p,
-                          T mu) {
+                          T mu, T* rowLog = nullptr) {
     const Softness<T> soft = (!a.moves || !b.moves) ? M.staticSoft : M.contactSoft;
     const int n = c.count;
     if (op == kWarm) {
@@ -599,9 +613,14 @@ __device__ void contactOp(const Model<T>& M, int op, SBody<T>& a, SBody<T>& b, c
         return;
     }
     const bool useBias = op == kBias;
-    for (int i = 0; i < n; ++i) { normalRow(M, a, b, c, i, p[i], useBias, soft); }
+    for (int i = 0; i < n; ++i) {
+        if (rowLog) { writeRow(rowLog, i, a.v, a.w, b.v, b.w, p[i]); }
+        normalRow(M, a, b, c, i, p[i], useBias, soft);
+    }
+    // Friction forward in the biased pass and backward in the relax pass; row n + j is the j-th friction row.
     for (int j = 0; j < n; ++j) {
         const int i = useBias ? j : n - 1 - j;
+        if (rowLog) { writeRow(rowLog, n + j, a.v, a.w, b.v, b.w, p[i]); }
         frictionRow(a, b, c, i, p[i], mu);
     }
 }
@@ -610,7 +629,8 @@ __device__ void contactOp(const Model<T>& M, int op, SBody<T>& a, SBody<T>& b, c
 // rows backwards. ga, gb, gp hold the adjoints after the operation on entry and before it on return.
 template <class T>
 __device__ void contactOpAdj(const Model<T>& M, int op, const SBody<T>& a0, const SBody<T>& b0, const CData<T>& c,
-                             const PointState<T>* p0, T mu, BodyAdj<T>& ga, BodyAdj<T>& gb, PointState<T>* gp, T& muG) {
+                             const PointState<T>* p0, T mu, BodyAdj<T>& ga, BodyAdj<T>& gb, PointState<T>* gp, T& muG,
+                             const T* rowLog) {
     const Softness<T> soft = (!a0.moves || !b0.moves) ? M.staticSoft : M.contactSoft;
     const int n = c.count;
     if (op == kWarm) {
@@ -626,42 +646,67 @@ __device__ void contactOpAdj(const Model<T>& M, int op, const SBody<T>& a0, cons
         }
         return;
     }
-    // Rows of this operation in order, each with the bodies and point state it started from.
+    if (op != kRestitute) {
+        // A solve: its rows' inputs were logged when the step was recomputed; walk them backwards.
+        const bool useBias = op == kBias;
+        SBody<T> a = a0, b = b0;
+        for (int r = 2 * n - 1; r >= 0; --r) {
+            const T* o = rowLog + 32 + r * kRowWords;
+            a.v = ld3(o), a.w = ld3(o + 3), b.v = ld3(o + 6), b.w = ld3(o + 9);
+            const PointState<T> pr{ o[12], ld3(o + 13), o[16] };
+            if (r < n) {
+                normalRowAdj(M, a, b, c, r, pr, useBias, soft, ga, gb, gp[r]);
+            } else {
+                const int j = r - n;
+                const int i = useBias ? j : n - 1 - j;
+                frictionRowAdj(a, b, c, i, pr, mu, ga, gb, gp[i], muG);
+            }
+        }
+        return;
+    }
+    // Restitution: replay the operation from its logged inputs to have every row's input (the rest of the
+    // bodies' state is constant over it), then walk the rows backwards.
     constexpr int kMaxRows = 8;
-    SBody<T> ra[kMaxRows], rb[kMaxRows];
-    PointState<T> rp[kMaxRows];
-    int rowPoint[kMaxRows], rowKind[kMaxRows];  // kind 0 normal, 1 friction, 2 restitution
+    struct Row {
+        V3<T> va, wa, vb, wb;
+        PointState<T> p;
+        int point, kind;  // kind 0 normal, 1 friction, 2 restitution
+    };
+    Row rowIn[kMaxRows];
     int rows = 0;
     SBody<T> a = a0, b = b0;
     PointState<T> p[4];
     for (int i = 0; i < 4; ++i) { p[i] = p0[i]; }
+    auto keep = [&](int i, int kind) { rowIn[rows++] = Row{ a.v, a.w, b.v, b.w, p[i], i, kind }; };
     if (op == kRestitute) {
         if (c.restitution == T(0)) { return; }
         for (int i = 0; i < n; ++i) {
             if (!restitutes(M, c, i, p[i])) { continue; }
-            ra[rows] = a, rb[rows] = b, rp[rows] = p[i], rowPoint[rows] = i, rowKind[rows] = 2, ++rows;
+            keep(i, 2);
             restituteRow(M, a, b, c, i, p[i]);
         }
     } else {
         const bool useBias = op == kBias;
         for (int i = 0; i < n; ++i) {
-            ra[rows] = a, rb[rows] = b, rp[rows] = p[i], rowPoint[rows] = i, rowKind[rows] = 0, ++rows;
+            keep(i, 0);
             normalRow(M, a, b, c, i, p[i], useBias, soft);
         }
         for (int j = 0; j < n; ++j) {
             const int i = useBias ? j : n - 1 - j;
-            ra[rows] = a, rb[rows] = b, rp[rows] = p[i], rowPoint[rows] = i, rowKind[rows] = 1, ++rows;
+            keep(i, 1);
             frictionRow(a, b, c, i, p[i], mu);
         }
     }
     for (int r = rows - 1; r >= 0; --r) {
-        const int i = rowPoint[r];
-        if (rowKind[r] == 0) {
-            normalRowAdj(M, ra[r], rb[r], c, i, rp[r], op == kBias, soft, ga, gb, gp[i]);
-        } else if (rowKind[r] == 1) {
-            frictionRowAdj(ra[r], rb[r], c, i, rp[r], mu, ga, gb, gp[i], muG);
+        const Row& R = rowIn[r];
+        a.v = R.va, a.w = R.wa, b.v = R.vb, b.w = R.wb;
+        const int i = R.point;
+        if (R.kind == 0) {
+            normalRowAdj(M, a, b, c, i, R.p, op == kBias, soft, ga, gb, gp[i]);
+        } else if (R.kind == 1) {
+            frictionRowAdj(a, b, c, i, R.p, mu, ga, gb, gp[i], muG);
         } else {
-            restituteRowAdj(M, ra[r], rb[r], c, i, rp[r], ga, gb, gp[i]);
+            restituteRowAdj(M, a, b, c, i, R.p, ga, gb, gp[i]);
         }
     }
 }
@@ -794,7 +839,7 @@ __device__ void stepWorld(const Model<T>& M, int step, uint32_t w, const T* in, 
         PointState<T> ps[4];
         for (int i = 0; i < 4; ++i) { ps[i] = p[i]; }
         if (log) { writeCall(log + at * callWords<T>(), a, b, ps); }
-        contactOp(M, op, a, b, c, ps, contactFriction(M, V, tc));
+        contactOp(M, op, a, b, c, ps, contactFriction(M, V, tc), log ? log + at * callWords<T>() : (T*)nullptr);
         for (int i = 0; i < 4; ++i) { p[i] = ps[i]; }
         if (a.moves) {
             st3(out + (size_t)ga * kState + 7, a.v);
@@ -933,7 +978,7 @@ __device__ void stepWorldAdj(const Model<T>& M, int step, uint32_t w, const T* i
         for (int i = 0; i < 4; ++i) { g4[i] = gp[i]; }
         T muG = 0;
         const T mu = contactFriction(M, V, tc);
-        contactOpAdj(M, op, a, b, c, p0, mu, gA, gB, g4, muG);
+        contactOpAdj(M, op, a, b, c, p0, mu, gA, gB, g4, muG, log + at * callWords<T>());
         for (int i = 0; i < 4; ++i) { gp[i] = g4[i]; }
         auto put = [&](bool moves, uint32_t g, T* s, const BodyAdj<T>& G) {
             if (moves) {
@@ -944,7 +989,9 @@ __device__ void stepWorldAdj(const Model<T>& M, int step, uint32_t w, const T* i
                 M.invMAdj[g] += G.im;
                 T* I = M.invIAdj + 9 * (size_t)g;
                 for (int r = 0; r < 3; ++r) { I[3 * r] += G.I.r[r].x, I[3 * r + 1] += G.I.r[r].y, I[3 * r + 2] += G.I.r[r].z; }
-            } else {
+            } else if (M.S.dynamic[g]) {
+                // A sleeping dynamic body: its velocity carries back to steps where it moved. A static body's
+                // never changes, so nothing is added for it.
                 atomicAddT(s + 7, G.v.x), atomicAddT(s + 8, G.v.y), atomicAddT(s + 9, G.v.z);
                 atomicAddT(s + 10, G.w.x), atomicAddT(s + 11, G.w.y), atomicAddT(s + 12, G.w.z);
             }
@@ -1057,7 +1104,7 @@ __device__ void stepWorldAdj(const Model<T>& M, int step, uint32_t w, const T* i
 // Kernels: one warp per world, every step of the run.
 
 template <class T>
-__global__ void __launch_bounds__(128) k_model_forward(Model<T> M) {
+__global__ void __launch_bounds__(128) k_model_forward(const __grid_constant__ Model<T> M) {
     const uint32_t w = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
     if (w >= (uint32_t)M.S.nWorlds) { return; }
     const uint32_t lane = threadIdx.x & 31;
@@ -1075,7 +1122,7 @@ __global__ void __launch_bounds__(128) k_model_forward(Model<T> M) {
 }
 
 template <class T>
-__global__ void __launch_bounds__(128) k_model_backward(Model<T> M) {
+__global__ void __launch_bounds__(128) k_model_backward(const __grid_constant__ Model<T> M) {
     const uint32_t w = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
     if (w >= (uint32_t)M.S.nWorlds) { return; }
     const size_t stride = (size_t)M.S.totalBodies * kState;
