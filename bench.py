@@ -48,6 +48,7 @@ def parse():
     ap.add_argument("--worlds", type=int, default=4096)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true", help="skip the plain-path and adjoint measurements")
     return ap.parse_args()
 
 
@@ -229,6 +230,61 @@ def load_traffic():
     return {}
 
 
+PLAIN_STRIDE = 64  # every 64th world stepped on its own
+
+
+def plain_rate(sc, args, device):
+    """Body-steps/s of the plain path: worlds stepped one by one, each a batch of one world on the same GPU
+    (its own graph per step), over a sample of the workload's worlds; device time summed over the worlds."""
+    from twofold_b200.world import Batch
+
+    ms, body_steps = 0.0, 0
+    sample = sc.worlds[::PLAIN_STRIDE]
+    for w in sample:
+        one = Batch([w], sc.settings, device=device)
+        for _ in range(args.warmup):
+            one.step_checked(sc.dt, 1, graph=True)
+        b0 = one.body_steps()
+        for _ in range(args.steps):
+            one.step_checked(sc.dt, 1, graph=True)
+            ms += one.elapsed_ms()
+        body_steps += one.body_steps() - b0
+        one.close()
+    return {"value": body_steps / (ms / 1e3), "unit": UNIT, "device_ms": ms,
+            "sample": f"every {PLAIN_STRIDE}th world ({len(sample)} of {len(sc.worlds)}), each alone, steps "
+                      f"{args.warmup + 1}-{args.warmup + args.steps}"}
+
+
+def adjoint_cost(device, n_worlds=1024, steps=120):
+    """The differentiable impact workload: record 120 steps of 1024 worlds, run the model forward and the adjoint
+    backward in float; device times of both, and of the pipeline's own 120 steps of the same worlds."""
+    from twofold_b200 import scenes
+    from twofold_b200.world import Batch
+
+    sc = scenes.config5(n_worlds=n_worlds)
+    pipe = Batch.from_scene(sc, device=device)
+    pipe_ms = 0.0
+    for _ in range(steps):
+        pipe.step_checked(sc.dt, 1, graph=True)
+        pipe_ms += pipe.elapsed_ms()
+    pipe.close()
+    b = Batch.from_scene(sc, device=device)
+    b.tape_record(sc.dt, steps)
+    n_shapes = sum(len(w.shapes) for w in sc.worlds)
+    final = b.adjoint_forward(32)
+    grad = np.zeros_like(final)
+    boxes = np.zeros(len(final), bool)
+    for wi in range(n_worlds):
+        boxes[b.offsets[wi] + 1:b.offsets[wi] + 65] = True
+    grad[boxes, 0] = 2 * final[boxes, 0]  # loss: sum of the boxes' squared final x
+    b.adjoint_backward(grad, n_shapes)
+    fwd, bwd = b.adjoint_ms()
+    b.close()
+    return {"workload": f"impact walls, {n_worlds} worlds x 66 bodies, {steps} steps, checkpoint every step",
+            "precision": "f32", "model_forward_ms": fwd, "backward_ms": bwd, "backward_over_forward": bwd / fwd,
+            "pipeline_forward_ms": pipe_ms, "backward_over_pipeline_forward": bwd / pipe_ms}
+
+
 def run_b200(args, dist):
     from twofold_b200 import abi, scenes
     from twofold_b200.world import Batch
@@ -309,6 +365,14 @@ def run_b200(args, dist):
     e_wall = dist.reduce(e_wall, "MAX")
     del e2e_batch
 
+    # The plain path for comparison: a sample of the same worlds, each stepped alone as a batch of one.
+    plain = None
+    if dist.rank == 0 and not args.no_extras:
+        plain = plain_rate(sc, args, dist.local_rank)
+    adjoint = None
+    if dist.rank == 0 and not args.no_extras:
+        adjoint = adjoint_cost(dist.local_rank)
+
     cpu = None
     if dist.rank == 0 and n == 1 and not args.no_cpu_baseline:
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -343,6 +407,8 @@ def run_b200(args, dist):
             "wall_s_timed_region": wall,
             "clocks": clocks.summary(),
             "cpu_baseline": cpu,
+            "plain_one_by_one": plain,
+            "adjoint": adjoint,
         }
         print(json.dumps(line))
 
