@@ -1269,7 +1269,9 @@ public:
             for (uint32_t t : { 128u, 256u, 512u }) {
                 for (uint32_t big : { 0u, 32u, 64u, 128u, 256u }) {
                     if (stages) {
-                        for (uint32_t sm : { 48u * 1024u, 96u * 1024u }) { cands[k].push_back(LaunchShape{ t, big, sm, true }); }
+                        for (uint32_t sm : { 32u * 1024u, 48u * 1024u, 96u * 1024u }) {
+                            cands[k].push_back(LaunchShape{ t, big, sm, true });
+                        }
                     } else {
                         cands[k].push_back(LaunchShape{ t, big, 0u, true });
                     }

@@ -1093,8 +1093,10 @@ struct PosBody {
     float kept;
 };
 
-// Staged words per body: v 0-2, w 3-5, dp 6-8, dq 9-12, type | awake << 8 in 13, inverse world inertia 14-22.
-constexpr int kSBodyWords = 23;
+// Staged words per body: v 0-2, w 3-5, dp 6-8, dq 9-12, type | awake << 8 in 13: what a laned solve reads
+// and writes. The inverse world inertia (torques, contacts solved on their own) stays in global memory, so
+// more bodies fit a slice.
+constexpr int kSBodyWords = 14;
 
 // Where one world's solver state lives during a substep: shared memory (structure of arrays, stride words
 // apart) for worlds that fit, else the bodies in global memory.
@@ -1148,7 +1150,7 @@ struct SolverStore {
         b.dq = l.dq;
         b.type = l.type;
         b.awake = l.awake;
-        for (int r = 0; r < 3; ++r) { b.invInertiaWorld.r[r] = { at(14 + 3 * r, i), at(15 + 3 * r, i), at(16 + 3 * r, i) }; }
+        b.invInertiaWorld = g[i].invInertiaWorld;
         return b;
     }
 
@@ -1175,11 +1177,6 @@ struct SolverStore {
         at(6, i) = d.dp.x, at(7, i) = d.dp.y, at(8, i) = d.dp.z;
         at(9, i) = d.dq.x, at(10, i) = d.dq.y, at(11, i) = d.dq.z, at(12, i) = d.dq.w;
         at(13, i) = __uint_as_float(d.type | (d.awake << 8));
-        for (int r = 0; r < 3; ++r) {
-            at(14 + 3 * r, i) = d.invInertiaWorld.r[r].x;
-            at(15 + 3 * r, i) = d.invInertiaWorld.r[r].y;
-            at(16 + 3 * r, i) = d.invInertiaWorld.r[r].z;
-        }
     }
 
     // Writes the fields a substep changes back to global memory.
@@ -1213,9 +1210,7 @@ struct SolverStore {
         b.kept = d.kept;
         b.linearProj = d.linearProj;
         b.angularProj = d.angularProj;
-        for (int r = 0; r < 3; ++r) {
-            b.invInertiaWorld.r[r] = { at(14 + 3 * r, i), at(15 + 3 * r, i), at(16 + 3 * r, i) };
-        }
+        b.invInertiaWorld = d.invInertiaWorld;
         integrateVelocity(b, P);
         at(0, i) = b.v.x, at(1, i) = b.v.y, at(2, i) = b.v.z;
         at(3, i) = b.w.x, at(4, i) = b.w.y, at(5, i) = b.w.z;
