@@ -68,6 +68,23 @@ def test_tumbling_boxes_match_reference(seed):
 
 
 @needs_oracle
+@pytest.mark.parametrize("seed", range(3))
+def test_prism_worlds_match_reference(seed):
+    """Prisms (general polyhedra: face and edge queries with the Gauss-map pruning, clipping) against boxes,
+    prisms and a half-space, including outlines the cleaning rewrote."""
+    w = scenes.prisms(n=24, seed=seed)
+    sc = scenes.Scene("prisms", [w])
+    b = Batch.from_scene(sc)
+    r = R.RefWorld(w, sc.settings)
+    for s in range(90):
+        b.step_checked(sc.dt)
+        r.step(sc.dt)
+        if s in (0, 29, 59, 89):
+            _check_pairs_and_manifolds(b, 0, r, f"prisms seed {seed} step {s + 1}")
+            _compare_world(b, 0, r, f"prisms seed {seed} step {s + 1}")
+
+
+@needs_oracle
 def test_pyramid_one_step_matches_reference():
     sc = scenes.config1()
     b = Batch.from_scene(sc)

@@ -47,3 +47,8 @@ def test_odd_box_sizes_are_cleaned_like_the_reference():
     w.shapes["geometry"][4] = 0  # sphere
     w.shapes["radius"][4] = 0.0
     _check_masses(scenes.Scene("odd", [w]))
+
+
+def test_prism_outlines_are_cleaned_like_the_reference():
+    """Prisms with clockwise, repeated, collinear and flat outlines (src/shape.cpp:13-130)."""
+    _check_masses(scenes.Scene("prisms", [scenes.prisms(n=40, seed=s) for s in range(3)]))

@@ -179,6 +179,93 @@ inline float solidRadius(float r) {
 
 constexpr float kPiF = 3.14159265358979f;
 
+// ---- Prism outlines (src/shape.cpp:13-130) ----
+
+// The polygon in counter-clockwise order (src/shape.cpp:13-18).
+inline std::vector<Vec2> counterClockwise(std::vector<Vec2> poly) {
+    float area = 0.0f;
+    for (size_t i = 0; i < poly.size(); ++i) { area += cross(poly[i], poly[(i + 1) % poly.size()]); }
+    if (area < 0.0f) { std::reverse(poly.begin(), poly.end()); }
+    return poly;
+}
+
+inline bool turnsLeft(const Vec2& a, const Vec2& b, const Vec2& c, float limit) {
+    return cross(b - a, c - b) > limit * length(c - a);
+}
+
+// Whether the outline winds once counter-clockwise with every corner clear of its neighbours' line
+// (src/shape.cpp:30-43). The winding sums the host C library's atan2, as the reference does.
+inline bool cleanOutline(const std::vector<Vec2>& poly, float limit) {
+    const size_t n = poly.size();
+    if (n < 3) { return false; }
+    float turning = 0.0f;
+    for (size_t i = 0; i < n; ++i) {
+        const Vec2& a = poly[i];
+        const Vec2& b = poly[(i + 1) % n];
+        const Vec2& c = poly[(i + 2) % n];
+        if (!turnsLeft(a, b, c, limit)) { return false; }
+        turning += std::atan2(cross(b - a, c - b), dot(b - a, c - b));
+    }
+    return turning < 3.0f * kPiF;
+}
+
+// The convex outline of the points by a monotone chain over (x, y) order, dropping repeated and nearly
+// collinear points; two points far enough apart become a thin rectangle, fewer a square around c
+// (src/shape.cpp:47-69).
+inline std::vector<Vec2> solidOutline(std::vector<Vec2> pts, float limit, float slab, const Vec2& c) {
+    std::sort(pts.begin(), pts.end(), [](const Vec2& a, const Vec2& b) { return a.x < b.x || (a.x == b.x && a.y < b.y); });
+    std::vector<Vec2> out;
+    for (int pass = 0; pass < 2 && !pts.empty(); ++pass) {
+        const size_t base = out.size();
+        for (const Vec2& p : pts) {
+            while (out.size() >= base + 2 && !turnsLeft(out[out.size() - 2], out.back(), p, limit)) { out.pop_back(); }
+            out.push_back(p);
+        }
+        out.pop_back();
+        std::reverse(pts.begin(), pts.end());
+    }
+    if (out.size() >= 3) { return out; }
+    if (out.size() == 2 && length(out[1] - out[0]) > limit) {
+        const Vec2 d = normalize(out[1] - out[0]);
+        const Vec2 side = Vec2{ -d.y, d.x } * slab;
+        return { out[0] - side, out[1] - side, out[1] + side, out[0] + side };
+    }
+    return { c + Vec2{ -slab, -slab }, c + Vec2{ slab, -slab }, c + Vec2{ slab, slab }, c + Vec2{ -slab, slab } };
+}
+
+// A prism cleaned as buildShape cleans it (src/shape.cpp:102-130): non-finite points dropped, the outline made
+// counter-clockwise and replaced by its convex outline when it is not clean, no height thickened to a slab.
+inline void solidPrism(std::vector<Vec2>& polygon, float& zMin, float& zMax) {
+    std::vector<Vec2> pts;
+    for (const Vec2& p : polygon) {
+        if (std::isfinite(p.x) && std::isfinite(p.y)) { pts.push_back(p); }
+    }
+    if (!std::isfinite(zMin)) { zMin = 0.0f; }
+    if (!std::isfinite(zMax)) { zMax = 0.0f; }
+    if (zMax < zMin) { std::swap(zMin, zMax); }
+    pts = counterClockwise(std::move(pts));
+    Vec2 lo{ 0, 0 }, hi{ 0, 0 };
+    if (!pts.empty()) { lo = hi = pts[0]; }
+    for (const Vec2& p : pts) {
+        lo = { std::min(lo.x, p.x), std::min(lo.y, p.y) };
+        hi = { std::max(hi.x, p.x), std::max(hi.y, p.y) };
+    }
+    const float width = length(hi - lo);
+    const float wide = std::max(std::fabs(lo.x), std::fabs(hi.x)) + std::max(std::fabs(lo.y), std::fabs(hi.y));
+    const float height = zMax - zMin;
+    const float size = std::sqrt(width * width + height * height);
+    const float limit = thinLimit(size, wide + std::max(std::fabs(zMin), std::fabs(zMax)));
+    const float slab = slabFor(size, limit);
+    const float flat = thinLimit(width, wide);
+    if (!cleanOutline(pts, flat)) { pts = solidOutline(std::move(pts), flat, slab, (lo + hi) * 0.5f); }
+    polygon = std::move(pts);
+    if (height <= limit) {
+        const float mid = 0.5f * (zMin + zMax);
+        zMin = mid - slab;
+        zMax = mid + slab;
+    }
+}
+
 // The built form of one shape: the device record plus its polyhedron (empty for spheres and half-spaces).
 struct HostShape {
     DShape d{};
@@ -190,7 +277,8 @@ struct HostShape {
 
 // Shape kind, cleaned size, polyhedron, extent, centroid and minExtent (src/shape.cpp:149-202). Returns
 // false for geometry this build does not make.
-inline bool buildShapeGeometry(HostShape& s, int geometry, float radius, const Vec3& halfExtents) {
+inline bool buildShapeGeometry(HostShape& s, int geometry, float radius, const Vec3& halfExtents,
+                               const float* points = nullptr, int pointCount = 0, float zMin = -0.5f, float zMax = 0.5f) {
     DShape& d = s.d;
     d.radius = 0.0f;
     d.halfHeight = 0.0f;
@@ -206,6 +294,13 @@ inline bool buildShapeGeometry(HostShape& s, int geometry, float radius, const V
         d.kind = kConvex;
         d.halfExtents = solidBox(halfExtents);
         s.poly = makeBox(d.halfExtents);
+        s.hasPoly = true;
+    } else if (geometry == 3 /* TF_PRISM */) {
+        d.kind = kConvex;
+        std::vector<Vec2> polygon;
+        for (int i = 0; i < pointCount && points; ++i) { polygon.push_back({ points[2 * i], points[2 * i + 1] }); }
+        solidPrism(polygon, zMin, zMax);
+        s.poly = makePrism(polygon, zMin, zMax);
         s.hasPoly = true;
     } else if (geometry == 5 /* TF_HALFSPACE */) {
         d.kind = kHalfSpace;

@@ -230,6 +230,50 @@ def config5(n_worlds=1024, seed=0):
     return Scene("impact_1024", worlds, steps=120)
 
 
+def _set_points(world, index, pts):
+    """Points of shape `index` (prism outline as (x, y) pairs, or hull points), kept alive with the world."""
+    arr = np.ascontiguousarray(pts, dtype=F32)
+    world.keepalive.append(arr)
+    world.shapes["points"][index] = arr.ctypes.data
+    world.shapes["point_count"][index] = len(arr)
+
+
+def prisms(n=24, seed=0, degenerate=True):
+    """Prisms of 3-8 vertices and boxes, randomly turned, dropped in a loose column onto a half-space. With
+    `degenerate`, some outlines are clockwise, repeat a point, hold a nearly collinear point, or are flat, so
+    the outline cleaning runs on every path."""
+    rng = np.random.default_rng([seed, 3])
+    b, s = _bodies(n + 1), _shapes(n + 1)
+    _ground(b, s, friction=0.6)
+    w = World(b, s, np.arange(n + 1))
+    b["rotation"][1:] = _uniform_quats(rng, n)
+    for i in range(1, n + 1):
+        b["position"][i] = (rng.uniform(-1.5, 1.5), 0.8 + 0.9 * i, rng.uniform(-1.5, 1.5))
+        s["friction"][i] = _f(rng.uniform(0.3, 0.9))
+        if i % 4 == 0:
+            s["half_extents"][i] = rng.uniform(0.2, 0.5, size=3).astype(F32)
+            continue
+        k = int(rng.integers(3, 9))
+        r = rng.uniform(0.2, 0.6)
+        ang = np.sort(rng.uniform(0.0, 2 * math.pi, size=k))
+        pts = np.stack([r * np.cos(ang), r * np.sin(ang)], 1).astype(F32)
+        if degenerate and i % 5 == 1:
+            pts = pts[::-1]                                  # clockwise
+        if degenerate and i % 7 == 2:
+            pts = np.concatenate([pts, pts[:1]])             # a repeated point
+        if degenerate and i % 9 == 3:
+            mid = (pts[0] + pts[1]) * F32(0.5)
+            pts = np.concatenate([pts[:1], mid[None], pts[1:]])  # a point on an edge
+        s["geometry"][i] = abi.TF_PRISM
+        _set_points(w, i, pts)
+        z = rng.uniform(0.15, 0.5)
+        s["z_min"][i] = _f(-z)
+        s["z_max"][i] = _f(z)
+        if degenerate and i % 11 == 4:
+            s["z_max"][i] = s["z_min"][i]                    # flat: thickened to a slab
+    return w
+
+
 def single(kind="box_on_ground", **kw):
     """Small hand-checkable worlds used by the unit parity tests."""
     if kind == "box_on_ground":
