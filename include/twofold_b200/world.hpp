@@ -12,7 +12,7 @@
 // status (TF_OK or a negative TF_E* code) and statusMessage() its text.
 //
 // Differences a caller can see:
-//   - Geometry: spheres, boxes, prisms and half-spaces run on the device. Cylinders, hulls and meshes are
+//   - Geometry: spheres, boxes, prisms, hulls and half-spaces run on the device. Cylinders and meshes are
 //     refused by addShape (an invalid ShapeId, status TF_E_UNSUPPORTED), as are sensors and planar locks.
 //   - addForce/addTorque queue the force for the next step and act on awake bodies only (wake = false).
 //   - Copying a World is not provided; move it instead.

@@ -85,6 +85,25 @@ def test_prism_worlds_match_reference(seed):
 
 
 @needs_oracle
+@pytest.mark.parametrize("seed", range(3))
+def test_hull_worlds_match_reference(seed):
+    """Hulls (computeHull's polyhedra, up to 16 vertices) against hulls, boxes, spheres and a half-space. The
+    degenerate clouds (thickened to slabs a few millimetres thin) stay out: the reference sweeps such thin
+    shapes continuously, which this build does not run (its host-build test covers their hulls)."""
+    w = scenes.hulls(n=24, seed=seed, degenerate=False)
+    sc = scenes.Scene("hulls", [w])
+    b = Batch.from_scene(sc)
+    r = R.RefWorld(w, sc.settings)
+    for s in range(90):
+        b.step_checked(sc.dt)
+        r.step(sc.dt)
+        assert r.profile().impacts == 0
+        if s in (0, 29, 59, 89):
+            _check_pairs_and_manifolds(b, 0, r, f"hulls seed {seed} step {s + 1}")
+            _compare_world(b, 0, r, f"hulls seed {seed} step {s + 1}")
+
+
+@needs_oracle
 def test_pyramid_one_step_matches_reference():
     sc = scenes.config1()
     b = Batch.from_scene(sc)

@@ -52,3 +52,13 @@ def test_odd_box_sizes_are_cleaned_like_the_reference():
 def test_prism_outlines_are_cleaned_like_the_reference():
     """Prisms with clockwise, repeated, collinear and flat outlines (src/shape.cpp:13-130)."""
     _check_masses(scenes.Scene("prisms", [scenes.prisms(n=40, seed=s) for s in range(3)]))
+
+
+def test_hulls_are_built_like_the_reference():
+    """computeHull (src/hull.cpp) restated: vertex and face order decide the masses' float sums, so equal bits
+    mean equal hulls; flat, collinear, single-point and repeated clouds included."""
+    _check_masses(scenes.Scene("hulls", [scenes.hulls(n=48, seed=s) for s in range(3)]))
+
+
+def test_hull_vertex_limits_are_kept_like_the_reference():
+    _check_masses(scenes.Scene("hulls", [scenes.hulls(n=30, seed=7, max_vertices=m) for m in (4, 6, 8, 64)]))

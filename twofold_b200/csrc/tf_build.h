@@ -12,6 +12,7 @@
 #include <utility>
 #include <vector>
 
+#include "tf_hull.h"
 #include "tf_math.cuh"
 #include "tf_types.cuh"
 
@@ -278,7 +279,8 @@ struct HostShape {
 // Shape kind, cleaned size, polyhedron, extent, centroid and minExtent (src/shape.cpp:149-202). Returns
 // false for geometry this build does not make.
 inline bool buildShapeGeometry(HostShape& s, int geometry, float radius, const Vec3& halfExtents,
-                               const float* points = nullptr, int pointCount = 0, float zMin = -0.5f, float zMax = 0.5f) {
+                               const float* points = nullptr, int pointCount = 0, float zMin = -0.5f, float zMax = 0.5f,
+                               int maxVertices = 64) {
     DShape& d = s.d;
     d.radius = 0.0f;
     d.halfHeight = 0.0f;
@@ -301,6 +303,14 @@ inline bool buildShapeGeometry(HostShape& s, int geometry, float radius, const V
         for (int i = 0; i < pointCount && points; ++i) { polygon.push_back({ points[2 * i], points[2 * i + 1] }); }
         solidPrism(polygon, zMin, zMax);
         s.poly = makePrism(polygon, zMin, zMax);
+        s.hasPoly = true;
+    } else if (geometry == 4 /* TF_HULL */) {
+        d.kind = kConvex;
+        std::vector<Vec3> cloud;
+        for (int i = 0; i < pointCount && points; ++i) { cloud.push_back({ points[3 * i], points[3 * i + 1], points[3 * i + 2] }); }
+        HullResult mesh = computeHull(cloud, maxVertices);
+        if (mesh.vertices.empty()) { mesh = computeHull({ Vec3{ 0, 0, 0 } }, maxVertices); }
+        s.poly = makePolyhedron(std::move(mesh.vertices), mesh.faces);
         s.hasPoly = true;
     } else if (geometry == 5 /* TF_HALFSPACE */) {
         d.kind = kHalfSpace;

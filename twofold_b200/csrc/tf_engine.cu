@@ -460,10 +460,12 @@ public:
         s.d.mask = d->mask;
         s.d.sensor = d->sensor ? 1u : 0u;
         s.d.poly = -1;
-        if (d->geometry == TF_PRISM && d->point_count > 0 && !d->points) { return fail(TF_E_INVALID, "addShape: prism without points"); }
+        if ((d->geometry == TF_PRISM || d->geometry == TF_HULL) && d->point_count > 0 && !d->points) {
+            return fail(TF_E_INVALID, "addShape: prism or hull without points");
+        }
         if (!buildShapeGeometry(s, d->geometry, d->radius, v3of(d->half_extents), d->points, d->point_count, d->z_min,
-                                d->z_max)) {
-            return fail(TF_E_UNSUPPORTED, "addShape: only spheres, boxes, prisms and half-spaces are run by this build");
+                                d->z_max, d->max_vertices)) {
+            return fail(TF_E_UNSUPPORTED, "addShape: only spheres, boxes, prisms, hulls and half-spaces are run by this build");
         }
         if (s.d.sensor) { return fail(TF_E_UNSUPPORTED, "addShape: sensors are not run by this build"); }
         if (s.d.kind == kHalfSpace && hb->d.type != kStatic) {

@@ -274,6 +274,46 @@ def prisms(n=24, seed=0, degenerate=True):
     return w
 
 
+def _sphere_points(rng, n, r):
+    v = rng.normal(size=(n, 3))
+    return (v / np.linalg.norm(v, axis=1, keepdims=True) * r).astype(F32)
+
+
+def hulls(n=24, seed=0, degenerate=True, max_vertices=16):
+    """Hulls of 16 points uniform on a 0.5 m sphere (vertex limit 16), some boxes and spheres, randomly turned
+    and dropped in a loose column onto a half-space. With `degenerate`, some clouds are flat, collinear, a
+    single point, or repeat points, so the hull's thickening and tolerance paths run."""
+    rng = np.random.default_rng([seed, 2])
+    b, s = _bodies(n + 1), _shapes(n + 1)
+    _ground(b, s, friction=0.6)
+    w = World(b, s, np.arange(n + 1))
+    b["rotation"][1:] = _uniform_quats(rng, n)
+    for i in range(1, n + 1):
+        b["position"][i] = (rng.uniform(-1.5, 1.5), 0.8 + 1.0 * i, rng.uniform(-1.5, 1.5))
+        s["friction"][i] = _f(rng.uniform(0.3, 0.9))
+        s["density"][i] = _f(rng.uniform(0.5, 2.0))
+        if i % 6 == 0:
+            s["half_extents"][i] = rng.uniform(0.2, 0.5, size=3).astype(F32)
+            continue
+        if i % 6 == 3:
+            s["geometry"][i] = abi.TF_SPHERE
+            s["radius"][i] = _f(rng.uniform(0.2, 0.5))
+            continue
+        pts = _sphere_points(rng, 16, 0.5)
+        if degenerate and i % 7 == 1:
+            pts[:, 2] = 0.0                                          # flat
+        if degenerate and i % 11 == 2:
+            pts = (np.outer(rng.uniform(-0.5, 0.5, 16), [1, 2, 3]) / 4).astype(F32)  # collinear
+        if degenerate and i % 13 == 4:
+            pts = np.zeros((3, 3), F32)                              # one point
+        if degenerate and i % 5 == 2:
+            pts = np.concatenate([pts, pts[:4]])                     # repeated points
+        s["geometry"][i] = abi.TF_HULL
+        s["max_vertices"][i] = max_vertices
+        _set_points(w, i, pts)
+    return w
+
+
 def single(kind="box_on_ground", **kw):
     """Small hand-checkable worlds used by the unit parity tests."""
     if kind == "box_on_ground":
