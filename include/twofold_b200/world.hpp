@@ -13,7 +13,9 @@
 //
 // Differences a caller can see:
 //   - Geometry: spheres, boxes, prisms, hulls and half-spaces run on the device. Cylinders and meshes are
-//     refused by addShape (an invalid ShapeId, status TF_E_UNSUPPORTED), as are sensors and planar locks.
+//     refused by addShape (an invalid ShapeId, status TF_E_UNSUPPORTED), as are sensors. Bodies locked to
+//     a plane run when every such body of the world is locked to the same plane; createBody refuses a
+//     second plane (an invalid BodyId, status TF_E_UNSUPPORTED).
 //   - addForce/addTorque queue the force for the next step and act on awake bodies only (wake = false).
 //   - Copying a World is not provided; move it instead.
 //   - The math types carry the reference's fields and a few operators, not all of math.h.

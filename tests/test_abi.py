@@ -73,3 +73,18 @@ def test_unsupported_geometry_is_refused():
     rc = lib.tf_shape_add(h, 0, bid, C.byref(abi.shape_desc(geometry=abi.TF_CYLINDER)), C.byref(sid))
     assert rc == -6  # TF_E_UNSUPPORTED
     lib.tf_world_destroy(h)
+
+
+def test_bodies_locked_to_two_planes_in_one_world_are_refused():
+    """Bodies locked to a plane run when every one of a world is locked to the same plane."""
+    lib = abi.load()
+    h = C.c_void_p()
+    abi.check(lib.tf_world_create(None, 2, 0, C.byref(h)))
+    bid = abi.tf_id()
+    planar = abi.body_desc(locks=abi.TF_LOCK_PLANAR)
+    abi.check(lib.tf_body_create(h, 0, C.byref(planar), C.byref(bid)))
+    abi.check(lib.tf_body_create(h, 0, C.byref(planar), C.byref(bid)))
+    turned = abi.body_desc(locks=abi.TF_LOCK_PLANAR, lock_frame=(0.0, 0.70710677, 0.0, 0.70710677))
+    assert lib.tf_body_create(h, 0, C.byref(turned), C.byref(bid)) == abi.TF_E_UNSUPPORTED
+    abi.check(lib.tf_body_create(h, 1, C.byref(turned), C.byref(bid)))
+    lib.tf_world_destroy(h)

@@ -386,12 +386,23 @@ public:
     int createBody(int w, const tf_body_desc* d, tf_id* out) {
         if (w < 0 || w >= (int)worlds.size() || !d) { return fail(TF_E_INVALID, "createBody: bad world or descriptor"); }
         if (d->type < 0 || d->type > 2) { return fail(TF_E_INVALID, "createBody: bad motion type"); }
-        if ((d->locks & kLockPlanar) == kLockPlanar) {
-            return fail(TF_E_UNSUPPORTED, "createBody: bodies locked to a plane are not run by this build");
-        }
         int rc = pull();
         if (rc != TF_OK) { return rc; }
         HostWorld& W = worlds[(size_t)w];
+        if ((d->locks & kLockPlanar) == kLockPlanar) {
+            // Every planar pair of a world is then solved in one plane, whose placements the kernels keep
+            // per body.
+            const Quat frame = normalize(q4of(d->lock_frame));
+            for (const HostBody& o : W.bodies) {
+                if (!o.d.alive || !isPlanar(o.d)) { continue; }
+                const Quat f = o.d.lockFrame;
+                if (!(f.x == frame.x && f.y == frame.y && f.z == frame.z && f.w == frame.w)) {
+                    return fail(TF_E_UNSUPPORTED,
+                                "createBody: bodies locked to different planes in one world are not run by this build");
+                }
+                break;
+            }
+        }
         uint32_t i;
         if (!W.freeBodies.empty()) {
             i = W.freeBodies.back();
@@ -569,6 +580,13 @@ public:
             wi.shapeCount = (uint32_t)W.shapes.size();
             wi.planeFirst = (uint32_t)nplanes;
             wi.planeCount = (uint32_t)W.planes.size();
+            wi.planeBody = UINT32_MAX;
+            for (size_t i = 0; i < W.bodies.size(); ++i) {
+                if (W.bodies[i].d.alive && isPlanar(W.bodies[i].d)) {
+                    wi.planeBody = wi.bodyFirst + (uint32_t)i;
+                    break;
+                }
+            }
             const uint32_t cap = std::max((uint32_t)std::ceil(capFactor * (float)W.shapes.size()) + 64u, minCandCap[w]);
             wi.candFirst = (uint32_t)ncand;
             wi.candCap = cap;

@@ -17,6 +17,7 @@
 #pragma once
 
 #include "tf_batch.cuh"
+#include "tf_planar.cuh"
 #include "tf_solver.cuh"
 #include "tf_tape.h"
 
@@ -487,8 +488,39 @@ __device__ __forceinline__ int nearestPoint(const DContact& old, const Vec3& loc
     return best;
 }
 
-// Collides one shape pair over dt as Impl::collidePair does for non-mesh, non-planar pairs
-// (src/world.cpp:505-533). Returns false for a pair this build cannot collide.
+// A pair whose dynamic bodies are locked to the plane n (src/world.cpp:514-518): both bodies are placed in
+// the plane, whatever the profiles turn out to be, and marked so the round's placements are kept once every
+// pair is done. Returns collidePlanar's answer. Kept out of line: the 3D paths around it need its registers.
+__device__ __noinline__ int collidePlanarPair(const Batch& B, const StepParams& P, const DShape& sa, const DShape& sb,
+                                              const Vec3& n, float margin, Manifold& m) {
+    DBody& ba = B.bodies[sa.body];
+    DBody& bb = B.bodies[sb.body];
+    const PlanePose pa = placeInPlane(ba, n);
+    const PlanePose pb = placeInPlane(bb, n);
+    ba.posePending = 1;
+    bb.posePending = 1;
+    m.featKind = kFeatNone;
+    m.featA = m.featB = -1;
+    m.normal = zero3();
+    return collidePlanar(B.cx.pt, sa, pa, sb, pb, margin, P.tol.linearSlop, m);
+}
+
+// Stores the placements of the round of collisions that just ended for the bodies of one world that were
+// placed in it; nothing reads a body's pose while its world is here.
+__device__ void keepPlacements(const Batch& B, const Group& g, const WorldInfo& wi) {
+    if (wi.planeBody == UINT32_MAX) { return; }
+    if (!TF_OK_INDEX(B, wi.planeBody < B.totalBodies, 31, wi.bodyFirst, wi.planeBody)) { return; }
+    const Vec3 n = planeNormal(B.bodies[wi.planeBody]);
+    for (uint32_t i = g.tid; i < wi.bodyCount; i += g.size) {
+        DBody& b = B.bodies[wi.bodyFirst + i];
+        if (!b.posePending) { continue; }
+        keepPose(b, placeInPlane(b, n));
+        b.posePending = 0;
+    }
+}
+
+// Collides one shape pair over dt as Impl::collidePair does for non-mesh pairs (src/world.cpp:505-533).
+// Returns false for a pair this build cannot collide.
 template <int Cls = kClassAny>
 __device__ bool collidePair(const Batch& B, const StepParams& P, const DShape& sa, const DShape& sb, float dt,
                             Manifold& m, int reuseKind, int reuseA, int reuseB) {
@@ -502,6 +534,15 @@ __device__ bool collidePair(const Batch& B, const StepParams& P, const DShape& s
     const DBody& bb = B.bodies[sb.body];
     const float travel = relativeTravel(ba, bb, dt);
     const float margin = P.tol.speculative + travel;
+    Vec3 n;
+    if (sa.kind != kMesh && sb.kind != kMesh && usePlanar(ba, bb, n)) {
+        const int r = collidePlanarPair(B, P, sa, sb, n, margin, m);
+        if (r > 0) { return true; }
+        if (r < 0) {
+            m.count = 0;
+            return false;
+        }
+    }
     const Transform xa = ba.xf * sa.local;
     const Transform xb = bb.xf * sb.local;
     const Motion mo{ ba.v, ba.w, ba.com, bb.v, bb.w, bb.com, dt, travel > P.tol.speculative };
@@ -562,7 +603,6 @@ __device__ void narrowOne(const Batch& B, const StepParams& P, const WorldInfo& 
         measureAgain(ba, bb, out, P);
         used = 1;
     } else {
-        if (isPlanar(ba) || isPlanar(bb)) { atomicOr(&wc.flags, kDevUnsupported); }
         Manifold m;
         if (!collidePair<Cls>(B, P, sa, sb, P.dt, m, kFeatNone, -1, -1)) { atomicOr(&wc.flags, kDevUnsupported); }
         if (m.count > 0) {
@@ -652,6 +692,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_narrowphase(const __grid_constant
     forWorlds(B, kSlotNarrow, sp, nullptr, [&](const Group& g, uint32_t w, unsigned char*, const StageSizes&) {
         const WorldInfo wi = B.info[w];
         WorldCounts& wc = B.counts[w];
+        keepPlacements(B, g, wi);
         const uint32_t nc = wc.candCount;
         const uint32_t oldCount = wc.contactCount;
         const DContact* old = B.previous + wi.contactFirst;
@@ -1073,6 +1114,7 @@ struct SBody {
     Vec3 v, w, dp;
     Quat dq;
     Mat3 invInertiaWorld;
+    float planeInvMass, planeInvInertia;
     uint32_t type, awake;
 };
 
@@ -1139,6 +1181,8 @@ struct SolverStore {
             b.dp = d.dp;
             b.dq = d.dq;
             b.invInertiaWorld = d.invInertiaWorld;
+            b.planeInvMass = d.planeInvMass;
+            b.planeInvInertia = d.planeInvInertia;
             b.type = d.type;
             b.awake = d.awake;
             return b;
@@ -1151,6 +1195,8 @@ struct SolverStore {
         b.type = l.type;
         b.awake = l.awake;
         b.invInertiaWorld = g[i].invInertiaWorld;
+        b.planeInvMass = g[i].planeInvMass;
+        b.planeInvInertia = g[i].planeInvInertia;
         return b;
     }
 
@@ -1302,7 +1348,9 @@ __global__ void __launch_bounds__(kMaxBlock) k_substep(const __grid_constant__ B
         const uint32_t nb = wi.bodyCount;
         const SolverStore st{ slice, stageN, nb <= stageN, B.bodies + wi.bodyFirst };
         if (refreshedAt(wc, sub, P.substeps)) {
-            // The body half of this substep's refresh: a new base pose (src/world.cpp:1663-1666).
+            // The body half of this substep's refresh: the planar placements of its collisions are kept, and
+            // every body takes a new base pose (src/world.cpp:1663-1666).
+            keepPlacements(B, g, wi);
             for (uint32_t i = g.tid; i < nb; i += g.size) {
                 DBody& d = st.g[i];
                 d.dp = zero3();
@@ -1496,7 +1544,8 @@ __global__ void __launch_bounds__(kMaxBlock) k_finish(const __grid_constant__ Ba
                         if (s.kind == kMesh || s.sensor) { continue; }
                         const float reach = length(s.local.p - b.localCenter) + s.extent;
                         const float travel = moved + angle * reach;
-                        if (travel > b.expectedTravel && travel > b.expectedTravel + 0.5f * s.minExtent) {
+                        if (travel > b.expectedTravel &&
+                            travel > b.expectedTravel + 0.5f * innerExtent(B.cx.pt, s, b)) {
                             atomicAdd(&s_sweep[g.id], 1u);
                         }
                     }

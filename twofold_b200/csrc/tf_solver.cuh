@@ -32,12 +32,80 @@ constexpr int kAxesPerContact = 12;
 struct AxisBody {
     Mat3 invMassWorld, invInertiaWorld;
     float invMass;
+    float planeInvMass, planeInvInertia;
 };
 
 template <class BodyT>
 TF_HD AxisBody axisBodyOf(const BodyT& b) {
-    return { b.invMassWorld, b.invInertiaWorld, b.invMass };
+    return { b.invMassWorld, b.invInertiaWorld, b.invMass, b.planeInvMass, b.planeInvInertia };
 }
+
+// A planar contact's point axes (DPlanarAxes) live in the point's normal axis slot: normalA, normalB and
+// normalMass in armA, tangentA, tangentB and tangentMass in armB.
+TF_HD void putPlanarAxes(Axis& x, const DPlanarAxes& p) {
+    x.armA = Vec3{ p.normalA, p.normalB, p.normalMass };
+    x.armB = Vec3{ p.tangentA, p.tangentB, p.tangentMass };
+}
+
+TF_HD DPlanarAxes planarAxesOf(const Axis& x) {
+    return { x.armA.x, x.armA.y, x.armA.z, x.armB.x, x.armB.y, x.armB.z };
+}
+
+// src/solver.cpp:83-86.
+template <class BodyT>
+TF_HD float planarMass(const BodyT& a, const BodyT& b, float armA, float armB) {
+    const float k = a.planeInvMass + b.planeInvMass + a.planeInvInertia * armA * armA + b.planeInvInertia * armB * armB;
+    return k > 1e-6f * (a.invMass + b.invMass) ? 1.0f / k : 0.0f;
+}
+
+// The planar axes of point i (src/solver.cpp:88-101).
+template <class BodyT>
+TF_HD DPlanarAxes makePlanarAxes(const BodyT& a, const BodyT& b, const DContact& c, int i) {
+    const Vec3 n = c.plane;
+    const DPoint& p = c.points[i];
+    DPlanarAxes x;
+    x.normalA = dot(n, cross(p.anchorA, c.normal));
+    x.normalB = dot(n, cross(p.anchorB, c.normal));
+    x.normalMass = planarMass(a, b, x.normalA, x.normalB);
+    x.tangentA = dot(n, cross(p.anchorA, c.tangent1));
+    x.tangentB = dot(n, cross(p.anchorB, c.tangent1));
+    x.tangentMass = planarMass(a, b, x.tangentA, x.tangentB);
+    return x;
+}
+
+// The velocities of a planar contact's bodies, with spin about the plane normal, held while its points are
+// solved (src/solver.cpp:104-134).
+struct PlanarState {
+    Vec3 va, vb;
+    float wa, wb;
+    float ma, mb, ia, ib;
+
+    template <class BodyT>
+    TF_HD PlanarState(const BodyT& a, const BodyT& b, const Vec3& n)
+        : va(a.v), vb(b.v), wa(dot(a.w, n)), wb(dot(b.w, n)), ma(a.planeInvMass), mb(b.planeInvMass),
+          ia(a.planeInvInertia), ib(b.planeInvInertia) {}
+
+    TF_HD float speed(const Vec3& d, float armA, float armB) const { return dot(d, vb - va) + armB * wb - armA * wa; }
+
+    TF_HD void push(const Vec3& d, float armA, float armB, float impulse) {
+        va -= d * (ma * impulse);
+        wa -= ia * armA * impulse;
+        vb += d * (mb * impulse);
+        wb += ib * armB * impulse;
+    }
+
+    template <class BodyT>
+    TF_HD void store(BodyT& a, BodyT& b, const Vec3& n, bool moveA, bool moveB) const {
+        if (moveA) {
+            a.v = va;
+            a.w = n * wa;
+        }
+        if (moveB) {
+            b.v = vb;
+            b.w = n * wb;
+        }
+    }
+};
 
 template <class BodyT>
 TF_HD Axis makeAxis(const BodyT& a, const BodyT& b, const Vec3& ra, const Vec3& rb, const Vec3& d) {
@@ -107,18 +175,30 @@ TF_HD bool planarContact(const DBody& a, const DBody& b, const Vec3& normal, Vec
     return first && fabsf(dot(normal, n)) < 1e-3f;
 }
 
-// Adjusted separation, approach speed and rolling radius at the step's start (src/solver.cpp:264-291).
-// Planar contacts are not run by this build (the caller refuses scenes with planar bodies).
+// Adjusted separation, approach speed and rolling radius at the step's start (src/solver.cpp:264-291). A
+// planar contact's normal is laid in the plane first, with the tangent in the plane and the plane normal as
+// the second tangent.
 TF_HD void prepareContact(const DBody& a, const DBody& b, DContact& c) {
     Vec3 plane = c.plane;
     const bool planar = planarContact(a, b, c.normal, plane);
     c.plane = plane;
     c.flags = planar ? (c.flags | kCPlanar) : (c.flags & ~kCPlanar);
+    if (planar) {
+        c.normal = normalize(c.normal - c.plane * dot(c.normal, c.plane));
+        c.tangent1 = cross(c.plane, c.normal);
+        c.tangent2 = c.plane;
+    }
+    const PlanarState st(a, b, c.plane);
     for (int i = 0; i < c.count; ++i) {
         DPoint& p = c.points[i];
         p.adjustedSeparation = p.separation - dot(p.anchorB - p.anchorA, c.normal);
-        p.relativeVelocity = dot(c.normal, b.v - a.v) + dot(cross(p.anchorB, c.normal), b.w) -
-                             dot(cross(p.anchorA, c.normal), a.w);
+        if (planar) {
+            const DPlanarAxes x = makePlanarAxes(a, b, c, i);
+            p.relativeVelocity = st.speed(c.normal, x.normalA, x.normalB);
+        } else {
+            p.relativeVelocity = dot(c.normal, b.v - a.v) + dot(cross(p.anchorB, c.normal), b.w) -
+                                 dot(cross(p.anchorA, c.normal), a.w);
+        }
         p.maxNormalImpulse = 0.0f;
     }
     if (c.rollingResistance > 0.0f && c.count > 0) {
@@ -134,9 +214,14 @@ TF_HD void prepareContact(const DBody& a, const DBody& b, DContact& c) {
 }
 
 // The axes of every point of a contact (src/solver.cpp:43-50), from the bodies' current world inverse mass
-// and inertia.
+// and inertia; a planar contact's planar axes (src/solver.cpp:88-101), which the reference builds in
+// prepareContact and rebaseContact from the same body state.
 template <class BodyT>
 TF_HD void makeContactAxes(const BodyT& a, const BodyT& b, const DContact& c, Axis* __restrict__ out) {
+    if (c.flags & kCPlanar) {
+        for (int i = 0; i < c.count; ++i) { putPlanarAxes(out[3 * i], makePlanarAxes(a, b, c, i)); }
+        return;
+    }
     for (int i = 0; i < c.count; ++i) {
         const DPoint& p = c.points[i];
         out[3 * i] = makeAxis(a, b, p.anchorA, p.anchorB, c.normal);
@@ -163,6 +248,28 @@ TF_HD void rebaseContact(const DBody& a, const DBody& b, DContact& c) {
 // time, so the unmasked push never races.
 template <class BodyT>
 TF_HD void warmStartContact(BodyT& a, BodyT& b, const DContact& c, bool laned, const Axis* __restrict__ ax) {
+    if (c.flags & kCPlanar) {
+        // src/solver.cpp:325-344: a planar contact holding nothing leaves its bodies as they are.
+        bool held = c.rollingResistance > 0.0f;
+        for (int i = 0; i < c.count; ++i) {
+            held = held || c.points[i].normalImpulse != 0.0f || lengthSquared(c.points[i].tangentImpulse) != 0.0f;
+        }
+        if (!held) { return; }
+        PlanarState st(a, b, c.plane);
+        for (int i = 0; i < c.count; ++i) {
+            const DPoint& p = c.points[i];
+            const DPlanarAxes x = planarAxesOf(ax[3 * i]);
+            st.push(c.normal, x.normalA, x.normalB, p.normalImpulse);
+            st.push(c.tangent1, x.tangentA, x.tangentB, dot(p.tangentImpulse, c.tangent1));
+        }
+        if (c.rollingResistance > 0.0f) {
+            const float r = dot(c.rollingImpulse, c.plane);
+            st.wa -= st.ia * r;
+            st.wb += st.ib * r;
+        }
+        st.store(a, b, c.plane, !anchored(a), !anchored(b));
+        return;
+    }
     const bool moveA = !laned || !anchored(a), moveB = !laned || !anchored(b);
     for (int i = 0; i < c.count; ++i) {
         const DPoint& p = c.points[i];
@@ -208,10 +315,93 @@ TF_HD void resistTurning(BodyT& a, BodyT& b, DContact& c) {
     c.rollingImpulse = total;
 }
 
+// The cosine and sine of a body's turn about n since the substep's base pose (src/solver.cpp:137-141).
+template <class BodyT>
+TF_HD Vec2 planarTurn(const BodyT& b, const Vec3& n) {
+    const Quat& q = b.dq;
+    return Vec2{ q.w * q.w - (q.x * q.x + q.y * q.y + q.z * q.z), 2.0f * q.w * dot(n, Vec3{ q.x, q.y, q.z }) };
+}
+
+// A planar contact's rows in the plane: soft normal rows, one friction row per point along the in-plane
+// tangent, and the rolling row about the plane normal (src/solver.cpp:143-209).
+template <class BodyT>
+TF_HD void solvePlanar(BodyT& a, BodyT& b, DContact& c, const StepParams& P, bool useBias, const Axis* __restrict__ ax) {
+    const bool moveA = !anchored(a), moveB = !anchored(b);
+    const Softness soft = (!moveA || !moveB) ? P.staticSoft : P.contactSoft;
+    const float shift = dot(b.dp - a.dp, c.normal);
+    const Vec2 ta = planarTurn(a, c.plane), tb = planarTurn(b, c.plane);
+    PlanarState st(a, b, c.plane);
+    bool changed = false;
+    for (int i = 0; i < c.count; ++i) {
+        DPoint& p = c.points[i];
+        const DPlanarAxes x = planarAxesOf(ax[3 * i]);
+        // A turned anchor reaches along the normal by its tangent arm times the cosine plus its normal arm
+        // times the sine.
+        const float reachA = ta.x * x.tangentA + ta.y * x.normalA;
+        const float reachB = tb.x * x.tangentB + tb.y * x.normalB;
+        const float sep = shift + reachB - reachA + p.adjustedSeparation;
+        float bias = 0.0f, massScale = 1.0f, impulseScale = 0.0f;
+        if (sep > 0.0f) {
+            bias = sep * P.invH;
+        } else if (useBias) {
+            bias = maxf(soft.biasRate * sep, -P.maxPushout);
+            massScale = soft.massScale;
+            impulseScale = soft.impulseScale;
+        }
+        const float vn = st.speed(c.normal, x.normalA, x.normalB);
+        float impulse = -x.normalMass * massScale * (vn + bias) - impulseScale * p.normalImpulse;
+        const float total = maxf(p.normalImpulse + impulse, 0.0f);
+        impulse = total - p.normalImpulse;
+        p.normalImpulse = total;
+        p.maxNormalImpulse = maxf(p.maxNormalImpulse, impulse);
+        if (impulse != 0.0f) {
+            st.push(c.normal, x.normalA, x.normalB, impulse);
+            changed = true;
+        }
+    }
+    for (int j = 0; j < c.count; ++j) {
+        const int i = useBias ? j : c.count - 1 - j;
+        DPoint& p = c.points[i];
+        const DPlanarAxes x = planarAxesOf(ax[3 * i]);
+        const float old = dot(p.tangentImpulse, c.tangent1);
+        // With no normal impulse the friction limit is zero, so a point holding no friction keeps none.
+        if (p.normalImpulse == 0.0f && old == 0.0f) { continue; }
+        changed = true;
+        const float limit = c.friction * p.normalImpulse;
+        const float t = minf(maxf(old - x.tangentMass * st.speed(c.tangent1, x.tangentA, x.tangentB), -limit), limit);
+        p.tangentImpulse = c.tangent1 * t;
+        st.push(c.tangent1, x.tangentA, x.tangentB, t - old);
+    }
+    if (c.rollingResistance > 0.0f) {
+        changed = true;
+        float total = dot(c.rollingImpulse, c.plane);
+        const float spin = st.wb - st.wa;
+        const float k = st.ia + st.ib;
+        if (spin != 0.0f && k > 0.0f) {
+            const float lambda = -spin / k;
+            total += lambda;
+            st.wa -= st.ia * lambda;
+            st.wb += st.ib * lambda;
+        }
+        float normal = 0.0f;
+        for (int i = 0; i < c.count; ++i) { normal += c.points[i].normalImpulse; }
+        const float limit = c.rollingResistance * c.rollingRadius * normal;
+        const float held = minf(maxf(total, -limit), limit);
+        st.wa -= st.ia * (held - total);
+        st.wb += st.ib * (held - total);
+        c.rollingImpulse = c.plane * held;
+    }
+    if (changed) { st.store(a, b, c.plane, moveA, moveB); }
+}
+
 // The soft normal rows, then friction (forward in the biased pass, reverse in relax), then rolling
 // (src/solver.cpp:360-421).
 template <class BodyT>
 TF_HD void solveContact(BodyT& a, BodyT& b, DContact& c, const StepParams& P, bool useBias, const Axis* __restrict__ ax) {
+    if (c.flags & kCPlanar) {
+        solvePlanar(a, b, c, P, useBias, ax);
+        return;
+    }
     const bool moveA = !anchored(a), moveB = !anchored(b);
     const Softness soft = (!moveA || !moveB) ? P.staticSoft : P.contactSoft;
     const Vec3 dp = b.dp - a.dp;
@@ -382,6 +572,24 @@ TF_HD void solveLaned(BodyT& a, BodyT& b, DContact& c, const StepParams& P, bool
 template <class BodyT>
 TF_HD void restituteContact(BodyT& a, BodyT& b, DContact& c, const StepParams& P, bool laned, const Axis* __restrict__ ax) {
     if (c.restitution == 0.0f) { return; }
+    if (c.flags & kCPlanar) {
+        // src/solver.cpp:430-445: the bodies are stored back whether or not a point took an impulse.
+        PlanarState st(a, b, c.plane);
+        for (int i = 0; i < c.count; ++i) {
+            DPoint& p = c.points[i];
+            if (p.relativeVelocity > -P.restitutionThreshold || p.maxNormalImpulse == 0.0f) { continue; }
+            const DPlanarAxes x = planarAxesOf(ax[3 * i]);
+            const float vn = st.speed(c.normal, x.normalA, x.normalB);
+            float impulse = -x.normalMass * (vn + c.restitution * p.relativeVelocity);
+            const float total = maxf(p.normalImpulse + impulse, 0.0f);
+            impulse = total - p.normalImpulse;
+            p.normalImpulse = total;
+            p.maxNormalImpulse = maxf(p.maxNormalImpulse, impulse);
+            st.push(c.normal, x.normalA, x.normalB, impulse);
+        }
+        st.store(a, b, c.plane, !anchored(a), !anchored(b));
+        return;
+    }
     const bool moveA = !laned || !anchored(a), moveB = !laned || !anchored(b);
     for (int i = 0; i < c.count; ++i) {
         DPoint& p = c.points[i];

@@ -73,7 +73,13 @@ struct alignas(16) DBody {
     uint32_t shapeFirst;
     uint32_t shapeCount;
     uint32_t world;
-    uint32_t pad;
+    // Set by every planar pair that placed the body in the current round of collisions; the round's
+    // placement is stored, and this cleared, once all its pairs are done.
+    uint32_t posePending;
+    // The part of the body's pose in a plane that lasts between rounds (src/internal.h:141-148): the plane
+    // normal it was placed for, that normal in the body's frame (the key) with the 2D axes around it, and the
+    // plane's own 2D axes. Zero until the body is first placed.
+    Vec3 poseNormal, poseKey, poseU, poseV, poseAxisU, poseAxisV;
 };
 
 struct alignas(16) DShape {
@@ -169,6 +175,9 @@ struct WorldInfo {
     uint32_t candFirst, candCap;      // candidate keys
     uint32_t contactFirst, contactCap;  // contacts, both buffers, and every per-contact list
     uint32_t planeFirst, planeCount;  // half-space shapes, global indices in planeList
+    // A body locked to a plane (global index), UINT32_MAX for none. Every such body of a world is locked to
+    // the same plane, so this one's normal is the normal of every planar pair in the world.
+    uint32_t planeBody;
 };
 
 // Per-world results and lists of the current step.

@@ -314,6 +314,70 @@ def hulls(n=24, seed=0, degenerate=True, max_vertices=16):
     return w
 
 
+def planar(n=16384, cols=46, spheres=256, seed=0, sphere_height=(10.0, 600.0), floor="box", restitution=0.0):
+    """Bodies locked to the z = 0 plane (lock frame identity): half boxes with half extents x, y ~ U[0.2, 0.6]
+    and z = 0.5, half prisms of 3-8 vertices at sorted random angles on a circle of radius U[0.2, 0.6] with z in
+    [-0.5, 0.5]; friction U[0.3, 0.9], a random turn in the plane; laid out on a `cols`-column grid of 1.7 m
+    centred on x = 0, rows from y = 2 at 1.7 m. Static container: a floor box reaching 1.9 m past the grid
+    (41 m half width at 46 columns) with 0.5 m walls 60 m tall at its ends, or a half-space floor alone
+    (`floor="halfspace"`). `spheres` free spheres (r 0.5, density 4, not locked) at x ~ U over the grid,
+    y ~ U[sphere_height], z = 0."""
+    rng = np.random.default_rng([seed, 3, 3])
+    n_static = 3 if floor == "box" else 1
+    total = n_static + n + spheres
+    b, s = _bodies(total), _shapes(total)
+    w = World(b, s, np.arange(total), meta={"kind": "planar", "floor": floor})
+    half = 0.85 * cols + 1.9
+    b["type"][:n_static] = abi.TF_STATIC
+    if floor == "box":
+        b["position"][0] = (0.0, -0.5, 0.0)
+        s["half_extents"][0] = (half, 0.5, 2.0)
+        for k, side in ((1, -1.0), (2, 1.0)):
+            b["position"][k] = (side * (half - 0.5), 30.0, 0.0)
+            s["half_extents"][k] = (0.5, 30.0, 2.0)
+        s["friction"][:n_static] = 0.6
+    else:
+        _ground(b, s, friction=0.6)
+    s["restitution"][:] = restitution
+    first = n_static
+    idx = np.arange(n)
+    row, col = idx // cols, idx % cols
+    b["position"][first:first + n, 0] = (-0.85 * (cols - 1) + 1.7 * col).astype(F32)
+    b["position"][first:first + n, 1] = (2.0 + 1.7 * row).astype(F32)
+    angle = rng.uniform(0.0, 2 * math.pi, size=n)
+    b["rotation"][first:first + n] = np.stack(
+        [np.zeros(n), np.zeros(n), np.sin(0.5 * angle), np.cos(0.5 * angle)], 1).astype(F32)
+    b["locks"][first:first + n] = abi.TF_LOCK_PLANAR
+    s["friction"][first:first + n] = rng.uniform(0.3, 0.9, size=n).astype(F32)
+    for i in range(n):
+        k = first + i
+        if i % 2 == 0:
+            s["half_extents"][k] = (rng.uniform(0.2, 0.6), rng.uniform(0.2, 0.6), 0.5)
+            continue
+        m = int(rng.integers(3, 9))
+        r = rng.uniform(0.2, 0.6)
+        ang = np.sort(rng.uniform(0.0, 2 * math.pi, size=m))
+        s["geometry"][k] = abi.TF_PRISM
+        _set_points(w, k, np.stack([r * np.cos(ang), r * np.sin(ang)], 1))
+        s["z_min"][k] = -0.5
+        s["z_max"][k] = 0.5
+    first += n
+    if spheres:
+        sl = slice(first, first + spheres)
+        b["position"][sl, 0] = rng.uniform(-0.85 * (cols - 1), 0.85 * (cols - 1), size=spheres).astype(F32)
+        b["position"][sl, 1] = rng.uniform(sphere_height[0], sphere_height[1], size=spheres).astype(F32)
+        s["geometry"][sl] = abi.TF_SPHERE
+        s["radius"][sl] = 0.5
+        s["density"][sl] = 4.0
+    return w
+
+
+def config3():
+    """Planar pile: 16,384 bodies locked to the z = 0 plane in a static box container, with 256 free spheres
+    dropped among them, 600 steps."""
+    return Scene("planar_16384", [planar()], steps=600)
+
+
 def single(kind="box_on_ground", **kw):
     """Small hand-checkable worlds used by the unit parity tests."""
     if kind == "box_on_ground":
