@@ -62,7 +62,7 @@ enum tf_device_flags {
     TF_DEV_NONFINITE = 1u << 2,
     TF_DEV_TIMEOUT = 1u << 3,
     TF_DEV_UNSUPPORTED_PAIR = 1u << 4,
-    TF_DEV_CONTINUOUS_SKIPPED = 1u << 5, /* a shape moved far enough to need a sweep, which runs on the host */
+    TF_DEV_CONTINUOUS_SKIPPED = 1u << 5, /* not set: the continuous pass runs on the device */
     TF_DEV_LIST_OVERFLOW = 1u << 6
 };
 

@@ -65,6 +65,16 @@ struct Batch {
     uint32_t* work;        // per launch of a step, the next world to hand out (zeroed when the step starts)
     uint32_t* rowScratch;  // per shape, the candidate key sort's row counts
 
+    // Continuous collision: per shape, its bounds over the whole step and (from shapeFirst) the world's fast
+    // shapes in shape order; per body, its earliest hit as (time bits << 32 | pair order), its group's
+    // earliest as (time bits << 32 | body), and the union-find parent of the bodies that hit one another.
+    Vec3* sweptLo;
+    Vec3* sweptHi;
+    uint32_t* sweepList;
+    unsigned long long* hitKey;
+    unsigned long long* groupKey;
+    uint32_t* hitParent;
+
     // Debug builds (TF_DEVICE_CHECKS) record the first failed index check here: code, world, value.
     uint32_t* debug;
     uint32_t nPolys;

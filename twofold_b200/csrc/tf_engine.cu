@@ -192,6 +192,9 @@ public:
     std::map<int, std::unique_ptr<Snapshot>> snapshots;
     bool laidOut = false;
     DevArray<uint32_t> dWork, dRowScratch;
+    DevArray<Vec3> dSweptLo, dSweptHi;
+    DevArray<uint32_t> dSweepList, dHitParent;
+    DevArray<unsigned long long> dHitKey, dGroupKey;
     DevArray<uint2> dCandItems, dContactItems;
     std::vector<uint32_t> minCandCap, minContactCap;
 
@@ -742,6 +745,12 @@ public:
         TF_ALLOC(dCandItems, ncand * kPairClasses);
         TF_ALLOC(dContactItems, ncon * (kPairClasses + 1));
         TF_ALLOC(dRowScratch, ns);
+        TF_ALLOC(dSweptLo, ns);
+        TF_ALLOC(dSweptHi, ns);
+        TF_ALLOC(dSweepList, ns);
+        TF_ALLOC(dHitParent, nb);
+        TF_ALLOC(dHitKey, nb);
+        TF_ALLOC(dGroupKey, nb);
         TF_ALLOC(dAbort, 1);
         TF_ALLOC(dDebug, 4);
         nPolys = polys.size();
@@ -879,6 +888,12 @@ public:
         B.candItemStride = (uint32_t)(dCandItems.n / kPairClasses);
         B.contactItemStride = (uint32_t)(dContactItems.n / (kPairClasses + 1));
         B.rowScratch = dRowScratch.ptr;
+        B.sweptLo = dSweptLo.ptr;
+        B.sweptHi = dSweptHi.ptr;
+        B.sweepList = dSweepList.ptr;
+        B.hitParent = dHitParent.ptr;
+        B.hitKey = dHitKey.ptr;
+        B.groupKey = dGroupKey.ptr;
         B.debug = dDebug.ptr;
         B.nPolys = (uint32_t)nPolys;
         B.totalBodies = (uint32_t)totalBodies;
@@ -1502,12 +1517,15 @@ public:
             p.manifolds = (int32_t)counts[w].contactCount;
             p.awake_bodies = (int32_t)counts[w].awakeBodies;
             p.awake_islands = (int32_t)counts[w].awakeIslands;
+            p.swept_pairs = (int32_t)counts[w].sweptPairs;
+            p.impacts = (int32_t)counts[w].impacts;
         }
         lastCounts = counts;
         deviceFlags = flags;
         bodyStepsTotal = bodyStepsBase + bodySteps;
         if (flags & kDevUnsupported) { return fail(TF_E_UNSUPPORTED, "the step met a pair this build cannot collide"); }
         if (flags & kDevNonFinite) { return fail(TF_E_NUMERIC, "a body state became non-finite"); }
+        if (flags & kDevTimeout) { return fail(TF_E_TIMEOUT, "a bounded device wait gave up"); }
         return TF_OK;
     }
     std::vector<WorldCounts> lastCounts;

@@ -17,6 +17,7 @@
 #pragma once
 
 #include "tf_batch.cuh"
+#include "tf_continuous.cuh"
 #include "tf_planar.cuh"
 #include "tf_solver.cuh"
 #include "tf_tape.h"
@@ -26,7 +27,7 @@ namespace tfb {
 constexpr int kMaxBlock = 512;
 constexpr int kMaxGroups = kMaxBlock / 32;
 constexpr uint32_t kDevPairOverflow = 1u << 0, kDevContactOverflow = 1u << 1, kDevNonFinite = 1u << 2,
-                   kDevUnsupported = 1u << 4, kDevSweepSkipped = 1u << 5, kDevListOverflow = 1u << 6;
+                   kDevTimeout = 1u << 3, kDevUnsupported = 1u << 4, kDevListOverflow = 1u << 6;
 
 // Where each launch of a step takes its worlds from (one counter each, zeroed when the step starts).
 // Up to kMaxSubsteps substeps per step.
@@ -1463,11 +1464,149 @@ __device__ __forceinline__ uint32_t rootOf(const uint32_t* parent, uint32_t x) {
     return x;
 }
 
+// bound(): every shape's bounds at the body's pose, and the union of those that are not half-spaces
+// (src/world.cpp:240-253).
+__device__ void boundBody(const Batch& B, DBody& b) {
+    bool any = false;
+    for (uint32_t x = 0; x < b.shapeCount; ++x) {
+        DShape& s = B.shapes[B.shapeList[b.shapeFirst + x]];
+        Vec3 lo, hi;
+        shapeBounds(s, B.cx.pt, b.xf * s.local, lo, hi);
+        s.lo = lo;
+        s.hi = hi;
+        if (s.kind == kHalfSpace) { continue; }
+        b.lo = any ? minVec(b.lo, lo) : lo;
+        b.hi = any ? maxVec(b.hi, hi) : hi;
+        any = true;
+    }
+}
+
+constexpr unsigned long long kNoHit = ~0ull;
+
+// The root of x among bodies whose unions may still be running: parents only ever point to lower bodies.
+__device__ __forceinline__ uint32_t hitRoot(const uint32_t* parent, uint32_t x) {
+    for (;;) {
+        const uint32_t y = ((const volatile uint32_t*)parent)[x];
+        if (y == x) { return x; }
+        x = y;
+    }
+}
+
+// Joins the groups of a and b, the higher root under the lower, so each group's root is its lowest body
+// whatever order the unions run in. A link that loses a race to another is tried again, a bounded number
+// of times.
+__device__ bool uniteHits(uint32_t* parent, uint32_t a, uint32_t b) {
+    for (int attempt = 0; attempt < 4096; ++attempt) {
+        a = hitRoot(parent, a);
+        b = hitRoot(parent, b);
+        if (a == b) { return true; }
+        if (a > b) {
+            const uint32_t t = a;
+            a = b;
+            b = t;
+        }
+        if (atomicCAS(&parent[b], b, a) == b) { return true; }
+    }
+    return false;
+}
+
+// The continuous pass of one world after the leaf refit (src/world.cpp:1271-1418). Each fast shape is swept
+// against every shape whose bounds over the step meet its own; a body keeps its earliest hit (time, then pair
+// order: fast shape, then other shape); dynamic bodies that hit each other form groups, and each awake
+// dynamic body of a group with a hit moves back to the group's earliest hit (time, then lowest body),
+// carried along by the kinematic body that hit, if one did.
+__device__ void sweepWorld(const Batch& B, const StepParams& P, const Group& g, const WorldInfo& wi, WorldCounts& wc,
+                           uint32_t* pairs, uint32_t* impacts) {
+    const uint32_t sf = wi.shapeFirst, ns = wi.shapeCount, bf = wi.bodyFirst, nb = wi.bodyCount;
+    uint32_t* parent = B.hitParent + bf;
+    for (uint32_t i = g.tid; i < ns; i += g.size) {
+        const DShape& s = B.shapes[sf + i];
+        Vec3 lo = s.lo, hi = s.hi;
+        if (s.alive && B.bodies[s.body].type != kStatic) {
+            Vec3 l, h;
+            shapeBounds(s, B.cx.pt, sweepAt(sweepOf(B.bodies[s.body]), 0.0f) * s.local, l, h);
+            lo = minVec(lo, l);
+            hi = maxVec(hi, h);
+        }
+        B.sweptLo[sf + i] = lo;
+        B.sweptHi[sf + i] = hi;
+    }
+    for (uint32_t i = g.tid; i < nb; i += g.size) {
+        B.hitKey[bf + i] = kNoHit;
+        B.groupKey[bf + i] = kNoHit;
+        parent[i] = i;
+    }
+    const uint32_t nf = groupCompact(
+        g, ns,
+        [&](uint32_t i) {
+            const DShape& s = B.shapes[sf + i];
+            if (!s.alive || !TF_OK_INDEX(B, s.body - bf < nb, 32, bf, i)) { return false; }
+            const DBody& b = B.bodies[s.body];
+            if (!b.alive || b.type != kDynamic || !b.awake) { return false; }
+            return sweepsShape(B.cx.pt, s, b, length(b.com - b.com0), sweepOf(b).angle);
+        },
+        [&](uint32_t i, uint32_t pos) { B.sweepList[sf + pos] = i; });
+    const float target = P.tol.linearSlop;
+    const unsigned long long total = (unsigned long long)nf * ns;
+    for (unsigned long long x = g.tid; x < total; x += g.size) {
+        const uint32_t k = (uint32_t)(x / ns), oi = (uint32_t)(x % ns);
+        const uint32_t fi = B.sweepList[sf + k];
+        const DShape& f = B.shapes[sf + fi];
+        const DShape& o = B.shapes[sf + oi];
+        if (!o.alive || o.sensor || o.body == f.body) { continue; }
+        if (!TF_OK_INDEX(B, o.body - bf < nb, 33, bf, oi)) { continue; }
+        if (!boxesOverlap(B.sweptLo[sf + fi], B.sweptHi[sf + fi], B.sweptLo[sf + oi], B.sweptHi[sf + oi])) { continue; }
+        if (!(f.category & o.mask) || !(o.category & f.mask)) { continue; }
+        atomicAdd(pairs, 1u);
+        if (o.kind == kMesh || o.kind == kCylinder || f.kind == kCylinder) {
+            atomicOr(&wc.flags, kDevUnsupported);
+            continue;
+        }
+        const DBody& bo = B.bodies[o.body];
+        float t = 1.0f;
+        if (!sweepPair(B.cx.pt, B.cx, f, B.bodies[f.body], o, bo, target, t)) { continue; }
+        const unsigned long long order = x < 0xffffffffull ? x : 0xfffffffeull;
+        atomicMin(&B.hitKey[f.body], ((unsigned long long)__float_as_uint(t) << 32) | order);
+        if (bo.type == kDynamic && !uniteHits(parent, f.body - bf, o.body - bf)) { atomicOr(&wc.flags, kDevTimeout); }
+    }
+    g.sync();
+    for (uint32_t i = g.tid; i < nb; i += g.size) {
+        const unsigned long long hk = B.hitKey[bf + i];
+        if (hk == kNoHit) { continue; }
+        atomicMin(&B.groupKey[bf + rootOf(parent, i)], (hk & 0xffffffff00000000ull) | i);
+    }
+    g.sync();
+    for (uint32_t i = g.tid; i < nb; i += g.size) {
+        const unsigned long long gk = B.groupKey[bf + rootOf(parent, i)];
+        if (gk == kNoHit) { continue; }
+        const float t = __uint_as_float((uint32_t)(gk >> 32));
+        DBody& b = B.bodies[bf + i];
+        if (t >= 1.0f || !b.alive || b.type != kDynamic || !b.awake) { continue; }
+        // The member whose hit came first, and what it hit.
+        const unsigned long long first = B.hitKey[bf + (uint32_t)gk];
+        const uint32_t oi = (uint32_t)((first & 0xffffffffull) % ns);
+        const DBody& other = B.bodies[B.shapes[sf + oi].body];
+        b.xf = sweepAt(sweepOf(b), t);
+        if (other.type == kKinematic) {
+            // A kinematic body keeps moving after the hit, so what hit it rides along to the end of the step.
+            const Transform k = sweepAt(sweepOf(other), t);
+            const Transform ride{ applyInverse(k, b.xf.p), normalize(conjugate(k.q) * b.xf.q) };
+            b.xf = other.xf * ride;
+        }
+        b.com = apply(b.xf, b.localCenter);
+        updateInverseMass(b);
+        boundBody(B, b);
+        atomicAdd(impacts, 1u);
+    }
+    g.sync();
+}
+
 // Union-find is staged in the group's shared slice (parent and island time by body, union pairs by contact)
 // when the world fits, else in its global scratch.
 __global__ void __launch_bounds__(kMaxBlock) k_finish(const __grid_constant__ Batch B, const __grid_constant__ StepParams P, const __grid_constant__ Split sp, int serial) {
     extern __shared__ __align__(16) unsigned char s_raw[];
-    __shared__ uint32_t s_awake[kMaxGroups], s_islands[kMaxGroups], s_sweep[kMaxGroups];
+    __shared__ uint32_t s_awake[kMaxGroups], s_islands[kMaxGroups], s_sweep[kMaxGroups], s_pairs[kMaxGroups],
+        s_impacts[kMaxGroups];
     if (stepAborted(B, serial)) { return; }
     forWorlds(B, kSlotFinish, sp, s_raw, [&](const Group& g, uint32_t w, unsigned char* slice, const StageSizes& ss) {
         const uint32_t stageBodies = ss.bodies, stageContacts = ss.contacts;
@@ -1518,36 +1657,16 @@ __global__ void __launch_bounds__(kMaxBlock) k_finish(const __grid_constant__ Ba
                 b.hasTarget = 0;
             }
             if (b.type != kStatic && !(b.type == kDynamic && !b.awake)) {
-                // Leaf refit over the new pose (src/world.cpp:1713-1718): shape bounds and the body's union.
-                bool any = false;
-                for (uint32_t x = 0; x < b.shapeCount; ++x) {
-                    DShape& s = B.shapes[B.shapeList[b.shapeFirst + x]];
-                    Vec3 lo, hi;
-                    shapeBounds(s, B.cx.pt, b.xf * s.local, lo, hi);
-                    s.lo = lo;
-                    s.hi = hi;
-                    if (s.kind == kHalfSpace) { continue; }
-                    b.lo = any ? minVec(b.lo, lo) : lo;
-                    b.hi = any ? maxVec(b.hi, hi) : hi;
-                    any = true;
-                }
-                // Shapes that moved well past what the speculative contacts covered would be swept against
-                // their surroundings (src/world.cpp:1260-1278). They are counted; the sweep is not run here.
+                // Leaf refit over the new pose (src/world.cpp:1713-1718).
+                boundBody(B, b);
+                // Shapes that moved well past what the speculative contacts covered are swept against their
+                // surroundings below (src/world.cpp:1280-1292).
                 if (P.continuous && b.type == kDynamic && b.awake) {
                     const float moved = length(b.com - b.com0);
-                    Quat d = normalize(b.xf.q * conjugate(b.q0));
-                    if (d.w < 0.0f) { d = -d; }
-                    const float sine = length(qvec(d));
-                    const float angle = sine > 1.0e-7f ? 2.0f * atan2f(sine, d.w) : 0.0f;
+                    const float angle = sweepOf(b).angle;
                     for (uint32_t x = 0; x < b.shapeCount; ++x) {
                         const DShape& s = B.shapes[B.shapeList[b.shapeFirst + x]];
-                        if (s.kind == kMesh || s.sensor) { continue; }
-                        const float reach = length(s.local.p - b.localCenter) + s.extent;
-                        const float travel = moved + angle * reach;
-                        if (travel > b.expectedTravel &&
-                            travel > b.expectedTravel + 0.5f * innerExtent(B.cx.pt, s, b)) {
-                            atomicAdd(&s_sweep[g.id], 1u);
-                        }
+                        if (sweepsShape(B.cx.pt, s, b, moved, angle)) { atomicAdd(&s_sweep[g.id], 1u); }
                     }
                 }
             }
@@ -1565,6 +1684,11 @@ __global__ void __launch_bounds__(kMaxBlock) k_finish(const __grid_constant__ Ba
             }
         }
         g.sync();
+        if (g.tid == 0) {
+            s_pairs[g.id] = 0;
+            s_impacts[g.id] = 0;
+        }
+        if (P.continuous && s_sweep[g.id] > 0) { sweepWorld(B, P, g, wi, wc, &s_pairs[g.id], &s_impacts[g.id]); }
         // Islands over contacts with points (src/world.cpp:1187-1233). The roots are each component's lowest
         // body whatever order the unions run in, so only the unions themselves run on one thread.
         const uint32_t nu = groupCompact(
@@ -1621,10 +1745,9 @@ __global__ void __launch_bounds__(kMaxBlock) k_finish(const __grid_constant__ Ba
             wc.awakeBodies = s_awake[g.id];
             wc.awakeIslands = s_islands[g.id];
             wc.bodySteps += s_awake[g.id];
-            if (s_sweep[g.id] > 0) {
-                wc.sweepShapes += s_sweep[g.id];
-                wc.flags |= kDevSweepSkipped;
-            }
+            wc.sweepShapes += s_sweep[g.id];
+            wc.sweptPairs = s_pairs[g.id];
+            wc.impacts = s_impacts[g.id];
         }
         g.sync();
     });

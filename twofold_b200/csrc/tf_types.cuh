@@ -200,7 +200,9 @@ struct WorldCounts {
     uint32_t flags;            // tf_device_flags
     uint32_t candNeeded;       // largest count seen, for growing capacities
     uint32_t contactNeeded;
-    uint32_t sweepShapes;      // shapes the continuous pass would sweep
+    uint32_t sweepShapes;      // shapes the continuous pass swept, summed over every step since the layout
+    uint32_t sweptPairs;       // this step's continuous pass: pairs swept, and bodies moved back
+    uint32_t impacts;
     uint32_t activePoints;     // contact points of the active list
     uint32_t colorStart[kColors + 1];
     uint32_t impactColorStart[kColors + 1];

@@ -372,6 +372,49 @@ def planar(n=16384, cols=46, spheres=256, seed=0, sphere_height=(10.0, 600.0), f
     return w
 
 
+def bullets(n=24, seed=0, speed=(40.0, 80.0)):
+    """Fast small bodies that the continuous pass must catch: spheres of radius U[0.03, 0.08], thin boxes
+    (half extents 0.02 x 0.1 x 0.1) and small boxes, shot at U[speed] m/s along x, half of them at a static
+    thin wall (half thickness 0.05) at x = 6 and half at a kinematic wall at x = -6 moving at 1 m/s in +x,
+    past three dynamic thin plates (half thickness 0.02) standing on a half-space between them."""
+    rng = np.random.default_rng([seed, 7])
+    plates = 3
+    total = 3 + plates + n
+    b, s = _bodies(total), _shapes(total)
+    w = World(b, s, np.arange(total), meta={"kind": "bullets"})
+    _ground(b, s, friction=0.6)
+    b["type"][1] = abi.TF_STATIC
+    b["position"][1] = (6.0, 1.5, 0.0)
+    s["half_extents"][1] = (0.05, 1.5, 1.5)
+    b["type"][2] = abi.TF_KINEMATIC
+    b["position"][2] = (-6.0, 1.5, 0.0)
+    b["linear_velocity"][2] = (1.0, 0.0, 0.0)
+    s["half_extents"][2] = (0.1, 1.5, 1.5)
+    for k in range(plates):
+        i = 3 + k
+        b["position"][i] = (-3.0 + 3.0 * k, 0.5, rng.uniform(-0.2, 0.2))
+        s["half_extents"][i] = (0.02, 0.5, 0.5)
+    first = 3 + plates
+    for k in range(n):
+        i = first + k
+        side = 1.0 if k % 2 == 0 else -1.0
+        b["position"][i] = (rng.uniform(-1.5, 1.5), rng.uniform(0.3, 2.6), rng.uniform(-1.2, 1.2))
+        b["linear_velocity"][i] = (side * rng.uniform(*speed), rng.uniform(-2.0, 2.0), rng.uniform(-2.0, 2.0))
+        b["angular_velocity"][i] = rng.uniform(-5.0, 5.0, size=3)
+        b["rotation"][i] = _uniform_quats(rng, 1)[0]
+        kind = k % 3
+        if kind == 0:
+            s["geometry"][i] = abi.TF_SPHERE
+            s["radius"][i] = rng.uniform(0.03, 0.08)
+        elif kind == 1:
+            s["half_extents"][i] = (0.02, 0.1, 0.1)
+        else:
+            s["half_extents"][i] = rng.uniform(0.05, 0.1, size=3)
+        s["density"][i] = 2.0
+    s["friction"][3:] = 0.5
+    return w
+
+
 def config3():
     """Planar pile: 16,384 bodies locked to the z = 0 plane in a static box container, with 256 free spheres
     dropped among them, 600 steps."""
