@@ -1035,8 +1035,12 @@ TF_HD void collideHalfSpace(const CollideCtx& cx, const Transform& xh, const DSh
 
 // Pair classes, by shape kinds. A kernel instantiated for one class compiles only that class's collision
 // code; kClassAny compiles every path.
-enum PairClass : int { kClassAny = -1, kClassSpheres = 0, kClassSpherePoly = 1, kClassPlane = 2, kClassConvex = 3 };
-constexpr int kPairClasses = 4;
+// kClassPlanar holds the pairs solved in a plane (decided by their bodies, not their shapes); its kernels
+// fall back to every 3D path for profiles the plane does not cut.
+enum PairClass : int {
+    kClassAny = -1, kClassSpheres = 0, kClassSpherePoly = 1, kClassPlane = 2, kClassConvex = 3, kClassPlanar = 4
+};
+constexpr int kPairClasses = 5;
 
 TF_HD int pairClass(uint32_t ka, uint32_t kb) {
     if (ka == kHalfSpace || kb == kHalfSpace) { return kClassPlane; }

@@ -170,7 +170,9 @@ public:
     LaunchShape shapes[kKernels];
     Split splits[kKernels];
     int grids[kKernels] = {};
-    int flatGrids[9] = {};  // k_collide per pair class, then k_refresh for the light list and per pair class
+    // k_collide per pair class, then k_refresh for the light list and per pair class.
+    static constexpr int kFlatGrids = 2 * kPairClasses + 1;
+    int flatGrids[kFlatGrids] = {};
     std::map<const void*, size_t> dynSmemLimit;
     bool kernelsConfigured = false;
     uint32_t maxWorldBodies = 0, maxWorldContacts = 0, medianWorldBodies = 0;
@@ -918,6 +920,7 @@ public:
             k_collide<kClassSpherePoly><<<flatGrids[1], threads(7), 0, stream>>>(B, P, serial);
             k_collide<kClassPlane><<<flatGrids[2], threads(7), 0, stream>>>(B, P, serial);
             k_collide<kClassConvex><<<flatGrids[3], threads(7), 0, stream>>>(B, P, serial);
+            k_collide<kClassPlanar><<<flatGrids[4], threads(7), 0, stream>>>(B, P, serial);
         });
         timed(1, rec, [&] { k_narrowphase<<<grids[1], threads(1), 0, stream>>>(B, P, splits[1], serial); });
         timed(2, rec, [&] { k_wake<<<grids[2], threads(2), 0, stream>>>(B, splits[2], serial); });
@@ -930,18 +933,19 @@ public:
         for (int i = 0; i < P.substeps; ++i) {
             if (i > 0) {
                 timed(4, rec, [&] {
-                    k_refresh<kClassAny><<<flatGrids[4], threads(4), 0, stream>>>(B, P, i, serial);
-                    k_refresh<kClassSpheres><<<flatGrids[5], threads(4), 0, stream>>>(B, P, i, serial);
-                    k_refresh<kClassSpherePoly><<<flatGrids[6], threads(4), 0, stream>>>(B, P, i, serial);
-                    k_refresh<kClassPlane><<<flatGrids[7], threads(4), 0, stream>>>(B, P, i, serial);
-                    k_refresh<kClassConvex><<<flatGrids[8], threads(4), 0, stream>>>(B, P, i, serial);
+                    k_refresh<kClassAny><<<flatGrids[5], threads(4), 0, stream>>>(B, P, i, serial);
+                    k_refresh<kClassSpheres><<<flatGrids[6], threads(4), 0, stream>>>(B, P, i, serial);
+                    k_refresh<kClassSpherePoly><<<flatGrids[7], threads(4), 0, stream>>>(B, P, i, serial);
+                    k_refresh<kClassPlane><<<flatGrids[8], threads(4), 0, stream>>>(B, P, i, serial);
+                    k_refresh<kClassConvex><<<flatGrids[9], threads(4), 0, stream>>>(B, P, i, serial);
+                    k_refresh<kClassPlanar><<<flatGrids[10], threads(4), 0, stream>>>(B, P, i, serial);
                 });
             }
             timed(5, rec, [&] { k_substep<<<grids[5], threads(5), smem(5), stream>>>(B, P, splits[5], i, serial); });
         }
         timed(6, rec, [&] { k_finish<<<grids[6], threads(6), smem(6), stream>>>(B, P, splits[6], serial); });
         if (marks) { cudaEventRecord(marks[3], stream); }
-        launches += 9 + P.substeps + 5 * (P.substeps - 1);
+        launches += 5 + kPairClasses + P.substeps + (kPairClasses + 1) * (P.substeps - 1);
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) { return fail(TF_E_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e)); }
         return TF_OK;
@@ -1041,14 +1045,16 @@ public:
                                      : (int)std::max<size_t>(1, std::min<size_t>(needed, (size_t)smCount * perSm));
         }
         // The flat kernels, one grid per instantiation: as many CTAs as fit on the device at once.
-        const void* flat[9] = { (const void*)k_collide<kClassSpheres>,    (const void*)k_collide<kClassSpherePoly>,
-                                (const void*)k_collide<kClassPlane>,      (const void*)k_collide<kClassConvex>,
-                                (const void*)k_refresh<kClassAny>,        (const void*)k_refresh<kClassSpheres>,
-                                (const void*)k_refresh<kClassSpherePoly>, (const void*)k_refresh<kClassPlane>,
-                                (const void*)k_refresh<kClassConvex> };
-        for (int f = 0; f < 9; ++f) {
+        const void* flat[kFlatGrids] = {
+            (const void*)k_collide<kClassSpheres>,  (const void*)k_collide<kClassSpherePoly>,
+            (const void*)k_collide<kClassPlane>,    (const void*)k_collide<kClassConvex>,
+            (const void*)k_collide<kClassPlanar>,   (const void*)k_refresh<kClassAny>,
+            (const void*)k_refresh<kClassSpheres>,  (const void*)k_refresh<kClassSpherePoly>,
+            (const void*)k_refresh<kClassPlane>,    (const void*)k_refresh<kClassConvex>,
+            (const void*)k_refresh<kClassPlanar> };
+        for (int f = 0; f < kFlatGrids; ++f) {
             int perSm = 0;
-            const int threads = (int)shapes[f < 4 ? 7 : 4].threads;
+            const int threads = (int)shapes[f < kPairClasses ? 7 : 4].threads;
             TF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, flat[f], threads, 0));
             if (perSm < 1) { return fail(TF_E_INVALID, "launch shape does not fit on an SM"); }
             flatGrids[f] = smCount * perSm;

@@ -185,6 +185,18 @@ __device__ __forceinline__ bool stepAborted(const Batch& B, int serial) {
     return skip;
 }
 
+// The flat list a pair of shapes (global indices) is collided from: the planar class when its bodies are
+// solved in a plane (src/world.cpp:514), else the class of its shape kinds.
+__device__ __forceinline__ int pairClassOf(const Batch& B, uint32_t a, uint32_t b) {
+    const DShape& sa = B.shapes[a];
+    const DShape& sb = B.shapes[b];
+    Vec3 n;
+    if (sa.kind != kMesh && sb.kind != kMesh && usePlanar(B.bodies[sa.body], B.bodies[sb.body], n)) {
+        return kClassPlanar;
+    }
+    return pairClass(sa.kind, sb.kind);
+}
+
 __device__ __forceinline__ uint64_t pairKey(uint32_t a, uint32_t b) {
     return ((uint64_t)(a < b ? a : b) << 32) | (uint64_t)(a < b ? b : a);
 }
@@ -396,9 +408,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_broadphase(const __grid_constant_
         g.sync();
         auto classOf = [&](uint32_t i) {
             const uint64_t key = B.cand[wi.candFirst + i];
-            const uint32_t ka = B.shapes[wi.shapeFirst + (uint32_t)(key >> 32)].kind;
-            const uint32_t kb = B.shapes[wi.shapeFirst + (uint32_t)(key & 0xffffffffu)].kind;
-            return pairClass(ka, kb);
+            return pairClassOf(B, wi.shapeFirst + (uint32_t)(key >> 32), wi.shapeFirst + (uint32_t)(key & 0xffffffffu));
         };
         for (uint32_t i = g.tid; i < unique; i += g.size) { atomicAdd(&cls[classOf(i)], 1u); }
         g.sync();
@@ -535,19 +545,22 @@ __device__ bool collidePair(const Batch& B, const StepParams& P, const DShape& s
     const DBody& bb = B.bodies[sb.body];
     const float travel = relativeTravel(ba, bb, dt);
     const float margin = P.tol.speculative + travel;
-    Vec3 n;
-    if (sa.kind != kMesh && sb.kind != kMesh && usePlanar(ba, bb, n)) {
-        const int r = collidePlanarPair(B, P, sa, sb, n, margin, m);
-        if (r > 0) { return true; }
-        if (r < 0) {
-            m.count = 0;
-            return false;
+    if constexpr (Cls == kClassAny || Cls == kClassPlanar) {
+        Vec3 n;
+        if (sa.kind != kMesh && sb.kind != kMesh && usePlanar(ba, bb, n)) {
+            const int r = collidePlanarPair(B, P, sa, sb, n, margin, m);
+            if (r > 0) { return true; }
+            if (r < 0) {
+                m.count = 0;
+                return false;
+            }
         }
     }
     const Transform xa = ba.xf * sa.local;
     const Transform xb = bb.xf * sb.local;
     const Motion mo{ ba.v, ba.w, ba.com, bb.v, bb.w, bb.com, dt, travel > P.tol.speculative };
-    return collideShapes<Cls>(B.cx, sa, xa, sb, xb, margin, mo, m, reuseKind, reuseA, reuseB);
+    constexpr int Shapes = Cls == kClassPlanar ? kClassAny : Cls;
+    return collideShapes<Shapes>(B.cx, sa, xa, sb, xb, margin, mo, m, reuseKind, reuseA, reuseB);
 }
 
 // First index in [0, n) whose key is not below key.
@@ -962,7 +975,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_prepare(const __grid_constant__ B
             auto listOf = [&](uint32_t x) {
                 const uint32_t ci = act[x];
                 if (!(B.cflags[cf + ci] & kFlagFast)) { return kPairClasses; }
-                return pairClass(B.shapes[cs[ci].shapeA].kind, B.shapes[cs[ci].shapeB].kind);
+                return pairClassOf(B, cs[ci].shapeA, cs[ci].shapeB);
             };
             for (uint32_t x = g.tid; x < nActive; x += g.size) { atomicAdd(&cls[listOf(x)], 1u); }
             g.sync();
