@@ -127,6 +127,7 @@ typedef struct tf_body_desc {
  *   TF_PRISM: points = point_count (x, y) pairs, z_min, z_max.
  *   TF_HULL: points = point_count (x, y, z) triples, max_vertices.
  *   TF_HALFSPACE: no parameters (static bodies only).
+ *   TF_MESH: mesh = an id from tf_mesh_create (static and kinematic bodies only).
  * points is read during tf_shape_add only. */
 typedef struct tf_shape_desc {
     int32_t geometry;
@@ -147,6 +148,7 @@ typedef struct tf_shape_desc {
     uint32_t category;
     uint32_t mask;
     int32_t sensor;
+    int32_t mesh;
 } tf_shape_desc;
 
 /* StepProfile (include/twofold/world.h:346-360). Times are device milliseconds per phase. */
@@ -195,6 +197,16 @@ TF_API int tf_world_destroy(void* world);
 TF_API int tf_world_count(void* world, int32_t* n_worlds);
 TF_API int tf_world_set_settings(void* world, const tf_settings* settings);
 
+/* TriangleMesh (include/twofold/mesh.h:13-30, src/mesh.cpp:122-245): builds a mesh that every world of the
+ * handle may share; TF_MESH shapes name it by *out_mesh. vertices holds x, y, z per vertex, indices three
+ * per triangle; both are read during the call only. */
+TF_API int tf_mesh_create(void* world, const float* vertices, int32_t vertex_count, const uint32_t* indices,
+                          int32_t index_count, int32_t* out_mesh);
+/* The built mesh (TriangleMesh::vertices, indices, triangleCount and its tree): counts[0] vertices, [1]
+ * triangles, [2] tree nodes. Every output may be null; the others take x, y, z per vertex, three indices,
+ * x, y, z and one edge-flag byte per triangle, lo and hi (6 floats) and first, count (2 ints) per node. */
+TF_API int tf_mesh_read(void* world, int32_t mesh, int32_t counts[3], float* vertices, uint32_t* indices,
+                        float* normals, uint8_t* edges, float* node_bounds, int32_t* node_ranges);
 TF_API int tf_body_create(void* world, int32_t w, const tf_body_desc* desc, tf_id* out_body);
 TF_API int tf_shape_add(void* world, int32_t w, tf_id body, const tf_shape_desc* desc, tf_id* out_shape);
 /* Bulk forms: n bodies into worlds world_of[i]; n shapes onto body_of[i] (indices in world_of[i]). */

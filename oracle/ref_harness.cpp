@@ -47,6 +47,12 @@ WorldSettings toSettings(const tf_settings* s) {
     return w;
 }
 
+// TriangleMeshes made through ref_mesh_create, named by position; they live until the process ends.
+std::vector<std::shared_ptr<const TriangleMesh>>& meshRegistry() {
+    static std::vector<std::shared_ptr<const TriangleMesh>> r;
+    return r;
+}
+
 Vec3 v3(const float* p) { return { p[0], p[1], p[2] }; }
 Quat q4(const float* p) { return { p[0], p[1], p[2], p[3] }; }
 
@@ -88,6 +94,10 @@ bool toShape(const tf_shape_desc* d, ShapeDesc& s) {
         break;
     }
     case TF_HALFSPACE: s.geometry = HalfSpace{}; break;
+    case TF_MESH:
+        if (d->mesh < 0 || (size_t)d->mesh >= meshRegistry().size()) { return false; }
+        s.geometry = Mesh{ meshRegistry()[(size_t)d->mesh] };
+        break;
     default: return false;
     }
     s.position = v3(d->position);
@@ -122,6 +132,38 @@ World* W(void* h) { return static_cast<World*>(h); }
 }
 
 extern "C" {
+
+TF_API int ref_mesh_create(const float* vertices, int nv, const uint32_t* indices, int ni) {
+    std::vector<Vec3> v((size_t)nv);
+    for (int i = 0; i < nv; ++i) { v[(size_t)i] = { vertices[3 * i], vertices[3 * i + 1], vertices[3 * i + 2] }; }
+    meshRegistry().push_back(std::make_shared<const TriangleMesh>(v, std::vector<uint32_t>(indices, indices + ni)));
+    return (int)meshRegistry().size() - 1;
+}
+
+// The built mesh, laid out as tf_mesh_read lays out its own.
+TF_API int ref_mesh_read(int mesh, int32_t counts[3], float* vertices, uint32_t* indices, float* normals,
+                         uint8_t* edges, float* node_bounds, int32_t* node_ranges) {
+    if (mesh < 0 || (size_t)mesh >= meshRegistry().size()) { return -1; }
+    const TriangleMesh::Data& d = meshRegistry()[(size_t)mesh]->data();
+    counts[0] = (int32_t)d.vertices.size();
+    counts[1] = (int32_t)d.normals.size();
+    counts[2] = (int32_t)d.nodes.size();
+    for (size_t i = 0; i < d.vertices.size(); ++i) { put3(vertices ? vertices + 3 * i : nullptr, d.vertices[i]); }
+    if (indices) { std::memcpy(indices, d.indices.data(), d.indices.size() * sizeof(uint32_t)); }
+    for (size_t t = 0; t < d.normals.size(); ++t) {
+        put3(normals ? normals + 3 * t : nullptr, d.normals[t]);
+        if (edges) { edges[t] = d.edges[t]; }
+    }
+    for (size_t n = 0; n < d.nodes.size(); ++n) {
+        put3(node_bounds ? node_bounds + 6 * n : nullptr, d.nodes[n].lo);
+        put3(node_bounds ? node_bounds + 6 * n + 3 : nullptr, d.nodes[n].hi);
+        if (node_ranges) {
+            node_ranges[2 * n] = d.nodes[n].first;
+            node_ranges[2 * n + 1] = d.nodes[n].count;
+        }
+    }
+    return 0;
+}
 
 TF_API void* ref_world_create(const tf_settings* s) { return new World(toSettings(s)); }
 TF_API void* ref_world_copy(void* h) { return new World(*W(h)); }

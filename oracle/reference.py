@@ -33,6 +33,8 @@ def load():
             "ref_body_create": ([P, C.POINTER(abi.tf_body_desc), C.POINTER(abi.tf_id)], C.c_int),
             "ref_shape_add": ([P, abi.tf_id, C.POINTER(abi.tf_shape_desc), C.POINTER(abi.tf_id)], C.c_int),
             "ref_scene_build": ([P, C.c_int, P, C.c_int, P, P], C.c_int),
+            "ref_mesh_create": ([P, C.c_int, P, C.c_int], C.c_int),
+            "ref_mesh_read": ([C.c_int, P, P, P, P, P, P, P], C.c_int),
             "ref_world_step": ([P, C.c_float, C.c_int], C.c_int),
             "ref_body_count": ([P], C.c_int),
             "ref_world_get_states": ([P, P, P, P, P, P], C.c_int),
@@ -53,6 +55,28 @@ def load():
     return _lib
 
 
+def mesh_create(vertices, indices):
+    """A reference TriangleMesh (include/twofold/mesh.h:13-30); returns its id in the harness."""
+    lib = load()
+    v = np.ascontiguousarray(vertices, np.float32).reshape(-1, 3)
+    i = np.ascontiguousarray(indices, np.uint32).reshape(-1)
+    return lib.ref_mesh_create(v.ctypes.data, len(v), i.ctypes.data, len(i))
+
+
+def mesh_read(mesh):
+    """The reference's built mesh, in the layout of twofold_b200.world.Batch.read_mesh."""
+    lib = load()
+    counts = np.zeros(3, np.int32)
+    lib.ref_mesh_read(mesh, counts.ctypes.data, None, None, None, None, None, None)
+    nv, nt, nn = (int(x) for x in counts)
+    out = {"vertices": np.zeros((nv, 3), np.float32), "indices": np.zeros(3 * nt, np.uint32),
+           "normals": np.zeros((nt, 3), np.float32), "edges": np.zeros(nt, np.uint8),
+           "node_bounds": np.zeros((nn, 6), np.float32), "node_ranges": np.zeros((nn, 2), np.int32)}
+    lib.ref_mesh_read(mesh, counts.ctypes.data, *(out[k].ctypes.data for k in
+                      ("vertices", "indices", "normals", "edges", "node_bounds", "node_ranges")))
+    return out
+
+
 class RefWorld:
     """One reference World built from a scenes.World."""
 
@@ -63,8 +87,14 @@ class RefWorld:
             return
         s = settings if settings is not None else abi.default_settings()
         self.h = self.lib.ref_world_create(C.byref(s))
-        rc = self.lib.ref_scene_build(self.h, len(world.bodies), world.bodies.ctypes.data, len(world.shapes),
-                                      world.body_of.ctypes.data, world.shapes.ctypes.data)
+        shapes = world.shapes
+        if getattr(world, "meshes", None):
+            ids = [mesh_create(v, i) for v, i in world.meshes]
+            shapes = world.shapes.copy()
+            named = shapes["geometry"] == abi.TF_MESH
+            shapes["mesh"][named] = np.asarray(ids, np.int32)[shapes["mesh"][named]]
+        rc = self.lib.ref_scene_build(self.h, len(world.bodies), world.bodies.ctypes.data, len(shapes),
+                                      world.body_of.ctypes.data, shapes.ctypes.data)
         if rc != 0:
             raise RuntimeError("reference scene build failed")
 

@@ -62,3 +62,41 @@ def test_hulls_are_built_like_the_reference():
 
 def test_hull_vertex_limits_are_kept_like_the_reference():
     _check_masses(scenes.Scene("hulls", [scenes.hulls(n=30, seed=7, max_vertices=m) for m in (4, 6, 8, 64)]))
+
+
+def _ragged_mesh():
+    """A small mesh with every case the builder cleans: repeated vertices (merged), a non-finite vertex, out of
+    range and repeated indices, a sliver, an edge shared by three triangles, open edges and folded neighbours
+    both ways."""
+    rng = np.random.default_rng(11)
+    v, idx = scenes.terrain_mesh(cells=6, cell=0.7, seed=3)
+    v = np.concatenate([v, v[:5], [[np.nan, 0, 0], [0.0, 5.0, 0.0], [0.0, 5.0, 1e-7], [1.0, 5.0, 0.0]]]).astype(np.float32)
+    n0 = len(v) - 4
+    extra = [n0 - 5, n0 - 4, n0 - 3,          # a triangle on the duplicated vertices
+             0, 1, n0,                          # a non-finite corner: dropped
+             0, 1, 999,                         # out of range: dropped
+             2, 2, 3,                           # a repeated corner: dropped
+             n0 + 1, n0 + 2, n0 + 3,            # a sliver: dropped
+             0, 1, 10, 0, 1, 11]                # the edge 0-1 shared three times
+    idx = np.concatenate([idx, np.asarray(extra, np.uint32)])
+    v[7, 1] += rng.uniform(0.3, 0.6)           # a sharp fold
+    return v, idx
+
+
+@pytest.mark.parametrize("kind", ["terrain", "ragged"])
+def test_meshes_are_built_like_the_reference(kind):
+    v, idx = scenes.terrain_mesh(cells=32, cell=0.5, seed=1) if kind == "terrain" else _ragged_mesh()
+    b = Batch([scenes.single("box_on_ground")])
+    mine = b.read_mesh(b.create_mesh(v, idx))
+    ref = R.mesh_read(R.mesh_create(v, idx))
+    for k in ("vertices", "indices", "normals", "edges", "node_bounds", "node_ranges"):
+        assert mine[k].shape == ref[k].shape, k
+        assert np.array_equal(mine[k].view(np.uint8), ref[k].view(np.uint8)), k
+    assert len(mine["normals"]) > 0
+
+
+def test_terrain_scene_builds_like_the_reference():
+    """Mass, centre and inertia of every body of a small terrain scene (spheres, boxes, hulls over a static
+    mesh), and the mesh shape's own bounds."""
+    sc = scenes.Scene("terrain", [scenes.terrain(cells=16, cols=4, levels=3, pitch=1.6, top=8.0)])
+    _check_masses(sc)

@@ -110,6 +110,7 @@ class tf_shape_desc(C.Structure):
         ("category", C.c_uint32),
         ("mask", C.c_uint32),
         ("sensor", C.c_int32),
+        ("mesh", C.c_int32),
     ]
 
 
@@ -177,7 +178,8 @@ def body_desc(type=TF_DYNAMIC, position=(0, 0, 0), rotation=(0, 0, 0, 1), linear
 
 def shape_desc(geometry=TF_BOX, radius=0.5, half_extents=(0.5, 0.5, 0.5), half_height=0.5, points=None,
                max_vertices=64, z_min=-0.5, z_max=0.5, position=(0, 0, 0), rotation=(0, 0, 0, 1), density=1.0,
-               friction=0.5, restitution=0.0, rolling_resistance=0.0, category=1, mask=0xFFFFFFFF, sensor=False):
+               friction=0.5, restitution=0.0, rolling_resistance=0.0, category=1, mask=0xFFFFFFFF, sensor=False,
+               mesh=-1):
     """ShapeDesc defaults (include/twofold/world.h:90-106). `points` must stay alive until the shape is added."""
     d = tf_shape_desc()
     d.geometry = geometry
@@ -199,6 +201,7 @@ def shape_desc(geometry=TF_BOX, radius=0.5, half_extents=(0.5, 0.5, 0.5), half_h
     d.category = category
     d.mask = mask
     d.sensor = 1 if sensor else 0
+    d.mesh = mesh
     return d
 
 
@@ -215,6 +218,8 @@ def _declare(lib):
         "tf_world_destroy": ([P], C.c_int),
         "tf_world_count": ([P, C.POINTER(C.c_int32)], C.c_int),
         "tf_world_set_settings": ([P, C.POINTER(tf_settings)], C.c_int),
+        "tf_mesh_create": ([P, P, C.c_int32, P, C.c_int32, C.POINTER(C.c_int32)], C.c_int),
+        "tf_mesh_read": ([P, C.c_int32, P, P, P, P, P, P, P], C.c_int),
         "tf_body_create": ([P, C.c_int32, C.POINTER(tf_body_desc), C.POINTER(tf_id)], C.c_int),
         "tf_shape_add": ([P, C.c_int32, tf_id, C.POINTER(tf_shape_desc), C.POINTER(tf_id)], C.c_int),
         "tf_bodies_create": ([P, C.c_int32, P, C.POINTER(tf_body_desc), P], C.c_int),
@@ -265,7 +270,8 @@ def _declare(lib):
 # Every symbol include/twofold_b200.h declares.
 EXPORTED = [
     "tf_abi_version", "tf_last_error", "tf_default_settings", "tf_world_create", "tf_world_destroy",
-    "tf_world_count", "tf_world_set_settings", "tf_body_create", "tf_shape_add", "tf_bodies_create",
+    "tf_world_count", "tf_world_set_settings", "tf_mesh_create", "tf_mesh_read", "tf_body_create", "tf_shape_add",
+    "tf_bodies_create",
     "tf_shapes_add", "tf_world_step", "tf_world_step_graph", "tf_world_synchronize", "tf_world_device_status",
     "tf_body_get_state", "tf_body_set_velocity", "tf_body_get_mass", "tf_body_is_awake", "tf_world_body_count",
     "tf_world_get_states", "tf_world_contacts", "tf_world_candidates", "tf_world_profile", "tf_world_awake_bodies",

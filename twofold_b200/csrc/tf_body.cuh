@@ -18,6 +18,16 @@ struct PolyTables {
     const Vec3* arcs;
 };
 
+// The batch's triangle meshes (DMesh ranges into shared tables).
+struct MeshTables {
+    const DMesh* meshes;
+    const Vec3* verts;
+    const uint32_t* indices;
+    const Vec3* normals;
+    const uint8_t* edges;
+    const MeshNode* nodes;
+};
+
 // Inverse of m restricted to the span of k orthonormal axes (src/world.cpp:44-60).
 TF_HD Mat3 invertSubspace(const Mat3& m, const Vec3* axes, int k) {
     if (k == 0) { return mzero(); }
@@ -118,6 +128,22 @@ TF_HD void shapeBounds(const DShape& s, const PolyTables& pt, const Transform& x
         return;
     }
     const Mat3 r = toMat3(xf.q);
+    if (s.kind == kMesh) {
+        // The mesh's root box turned into the world.
+        if (s.mesh < 0) {
+            lo = hi = xf.p;
+            return;
+        }
+        const Vec3 c = apply(xf, s.centroid);
+        const Vec3 e = s.halfExtents;
+        Vec3 reach;
+        for (int i = 0; i < 3; ++i) {
+            setComp(reach, i, fabsf(r.r[i].x) * e.x + fabsf(r.r[i].y) * e.y + fabsf(r.r[i].z) * e.z);
+        }
+        lo = c - reach;
+        hi = c + reach;
+        return;
+    }
     const DPoly& P = pt.polys[s.poly];
     const Vec3* v = pt.verts + P.vFirst;
     if (s.geometry == 1 /* box */ || s.geometry == 3 /* prism */) {

@@ -13,6 +13,7 @@
 #include <vector>
 
 #include "tf_hull.h"
+#include "tf_mesh.h"
 #include "tf_math.cuh"
 #include "tf_types.cuh"
 
@@ -280,7 +281,7 @@ struct HostShape {
 // false for geometry this build does not make.
 inline bool buildShapeGeometry(HostShape& s, int geometry, float radius, const Vec3& halfExtents,
                                const float* points = nullptr, int pointCount = 0, float zMin = -0.5f, float zMax = 0.5f,
-                               int maxVertices = 64) {
+                               int maxVertices = 64, const HostMesh* mesh = nullptr, int meshId = -1) {
     DShape& d = s.d;
     d.radius = 0.0f;
     d.halfHeight = 0.0f;
@@ -315,6 +316,17 @@ inline bool buildShapeGeometry(HostShape& s, int geometry, float radius, const V
     } else if (geometry == 5 /* TF_HALFSPACE */) {
         d.kind = kHalfSpace;
         d.extent = 0.0f;
+    } else if (geometry == 6 /* TF_MESH */) {
+        d.kind = kMesh;
+        d.extent = 0.0f;
+        d.mesh = -1;
+        if (mesh && !mesh->nodes.empty()) {
+            for (const Vec3& v : mesh->vertices) { d.extent = std::max(d.extent, length(v)); }
+            const MeshNode& root = mesh->nodes[0];
+            d.centroid = (root.lo + root.hi) * 0.5f;
+            d.halfExtents = (root.hi - root.lo) * 0.5f;
+            d.mesh = meshId;
+        }
     } else {
         return false;
     }

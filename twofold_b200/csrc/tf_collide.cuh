@@ -847,6 +847,7 @@ TF_HD bool apart(const Convex& a, const Transform& xa, const Convex& b, const Tr
 // Everything a pair collision needs from the batch.
 struct CollideCtx {
     PolyTables pt;
+    MeshTables mt;
     BoxTopology boxes;
     Tolerances tol;
 };

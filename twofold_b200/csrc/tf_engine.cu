@@ -108,6 +108,7 @@ public:
     tf_settings settings{};
     int device = 0;
     std::vector<HostWorld> worlds;
+    std::vector<HostMesh> meshes;  // shared by every world of the handle
     cudaStream_t stream = nullptr;
     int smCount = 148;
     int blockSize = 128;
@@ -136,6 +137,11 @@ public:
     DevArray<uint32_t> dShapeList, dPlaneList;
     DevArray<DPoly> dPolys;
     DevArray<Vec3> dVerts, dNormals, dArcs;
+    DevArray<DMesh> dMeshes;
+    DevArray<Vec3> dMeshVerts, dMeshNormals;
+    DevArray<uint32_t> dMeshIndices;
+    DevArray<uint8_t> dMeshEdges;
+    DevArray<MeshNode> dMeshNodes;
     DevArray<int32_t> dIndices;
     DevArray<DFace> dFaces;
     DevArray<float> dOffsets;
@@ -476,12 +482,22 @@ public:
         s.d.mask = d->mask;
         s.d.sensor = d->sensor ? 1u : 0u;
         s.d.poly = -1;
+        s.d.mesh = -1;
         if ((d->geometry == TF_PRISM || d->geometry == TF_HULL) && d->point_count > 0 && !d->points) {
             return fail(TF_E_INVALID, "addShape: prism or hull without points");
         }
+        const HostMesh* mesh = nullptr;
+        if (d->geometry == TF_MESH) {
+            if (d->mesh < 0 || (size_t)d->mesh >= meshes.size()) { return fail(TF_E_INVALID, "addShape: unknown mesh"); }
+            if (hb->d.type == kDynamic) {
+                return fail(TF_E_UNSUPPORTED, "addShape: meshes belong to static and kinematic bodies");
+            }
+            mesh = &meshes[(size_t)d->mesh];
+        }
         if (!buildShapeGeometry(s, d->geometry, d->radius, v3of(d->half_extents), d->points, d->point_count, d->z_min,
-                                d->z_max, d->max_vertices)) {
-            return fail(TF_E_UNSUPPORTED, "addShape: only spheres, boxes, prisms, hulls and half-spaces are run by this build");
+                                d->z_max, d->max_vertices, mesh, d->mesh)) {
+            return fail(TF_E_UNSUPPORTED,
+                        "addShape: only spheres, boxes, prisms, hulls, half-spaces and meshes are run by this build");
         }
         if (s.d.sensor) { return fail(TF_E_UNSUPPORTED, "addShape: sensors are not run by this build"); }
         if (s.d.kind == kHalfSpace && hb->d.type != kStatic) {
@@ -717,6 +733,28 @@ public:
         TF_ALLOC(dFaces, faces.size());
         TF_ALLOC(dOffsets, offsets.size());
         TF_ALLOC(dEdges, edges.size());
+        // The meshes, shared by every world: each mesh's arrays one after another.
+        std::vector<DMesh> meshRecs(meshes.size());
+        std::vector<Vec3> meshVerts, meshNormals;
+        std::vector<uint32_t> meshIndices;
+        std::vector<uint8_t> meshEdges;
+        std::vector<MeshNode> meshNodes;
+        for (size_t m = 0; m < meshes.size(); ++m) {
+            const HostMesh& hm = meshes[m];
+            meshRecs[m] = { (int32_t)meshVerts.size(), (int32_t)hm.vertices.size(), (int32_t)meshNormals.size(),
+                            (int32_t)hm.normals.size(), (int32_t)meshNodes.size(), (int32_t)hm.nodes.size() };
+            meshVerts.insert(meshVerts.end(), hm.vertices.begin(), hm.vertices.end());
+            meshIndices.insert(meshIndices.end(), hm.indices.begin(), hm.indices.end());
+            meshNormals.insert(meshNormals.end(), hm.normals.begin(), hm.normals.end());
+            meshEdges.insert(meshEdges.end(), hm.edges.begin(), hm.edges.end());
+            meshNodes.insert(meshNodes.end(), hm.nodes.begin(), hm.nodes.end());
+        }
+        TF_ALLOC(dMeshes, meshRecs.size());
+        TF_ALLOC(dMeshVerts, meshVerts.size());
+        TF_ALLOC(dMeshIndices, meshIndices.size());
+        TF_ALLOC(dMeshNormals, meshNormals.size());
+        TF_ALLOC(dMeshEdges, meshEdges.size());
+        TF_ALLOC(dMeshNodes, meshNodes.size());
         TF_ALLOC(dGrow, nb);
         TF_ALLOC(dIslandTime, nb);
         TF_ALLOC(dBodyColors, nb);
@@ -779,6 +817,12 @@ public:
         if ((rc = up(dFaces.ptr, faces.data(), faces.size() * sizeof(DFace))) != TF_OK) { return rc; }
         if ((rc = up(dOffsets.ptr, offsets.data(), offsets.size() * sizeof(float))) != TF_OK) { return rc; }
         if ((rc = up(dEdges.ptr, edges.data(), edges.size() * sizeof(DEdge))) != TF_OK) { return rc; }
+        if ((rc = up(dMeshes.ptr, meshRecs.data(), meshRecs.size() * sizeof(DMesh))) != TF_OK) { return rc; }
+        if ((rc = up(dMeshVerts.ptr, meshVerts.data(), meshVerts.size() * sizeof(Vec3))) != TF_OK) { return rc; }
+        if ((rc = up(dMeshIndices.ptr, meshIndices.data(), meshIndices.size() * sizeof(uint32_t))) != TF_OK) { return rc; }
+        if ((rc = up(dMeshNormals.ptr, meshNormals.data(), meshNormals.size() * sizeof(Vec3))) != TF_OK) { return rc; }
+        if ((rc = up(dMeshEdges.ptr, meshEdges.data(), meshEdges.size() * sizeof(uint8_t))) != TF_OK) { return rc; }
+        if ((rc = up(dMeshNodes.ptr, meshNodes.data(), meshNodes.size() * sizeof(MeshNode))) != TF_OK) { return rc; }
         for (size_t r = 0; r < runSlot.size(); ++r) {
             if ((rc = up(dContacts[0].ptr + runSlot[r], packed.data() + runFirst[r], runCount[r] * sizeof(DContact))) != TF_OK) {
                 return rc;
@@ -858,6 +902,7 @@ public:
         B.planeList = dPlaneList.ptr;
         B.cx.pt = { dPolys.ptr, dVerts.ptr, dIndices.ptr, dFaces.ptr, dNormals.ptr, dOffsets.ptr, dEdges.ptr, dArcs.ptr };
         B.cx.boxes = boxTopology;
+        B.cx.mt = { dMeshes.ptr, dMeshVerts.ptr, dMeshIndices.ptr, dMeshNormals.ptr, dMeshEdges.ptr, dMeshNodes.ptr };
         B.grow = dGrow.ptr;
         B.bodyColors = dBodyColors.ptr;
         B.struck = dStruck.ptr;
@@ -1648,6 +1693,55 @@ TF_API int tf_world_count(void* h, int32_t* n) {
 TF_API int tf_world_set_settings(void* h, const tf_settings* s) {
     if (!h || !s) { return tfb::fail(TF_E_INVALID, "tf_world_set_settings: null"); }
     E(h)->settings = *s;
+    return TF_OK;
+}
+
+TF_API int tf_mesh_create(void* h, const float* vertices, int32_t vertex_count, const uint32_t* indices,
+                          int32_t index_count, int32_t* out_mesh) {
+    if (!h || !out_mesh) { return tfb::fail(TF_E_INVALID, "tf_mesh_create: null"); }
+    if (vertex_count < 0 || index_count < 0 || (vertex_count > 0 && !vertices) || (index_count > 0 && !indices)) {
+        return tfb::fail(TF_E_INVALID, "tf_mesh_create: bad arrays");
+    }
+    std::vector<tfb::Vec3> v((size_t)vertex_count);
+    for (int32_t i = 0; i < vertex_count; ++i) { v[(size_t)i] = { vertices[3 * i], vertices[3 * i + 1], vertices[3 * i + 2] }; }
+    std::vector<uint32_t> idx(indices, indices + index_count);
+    Engine* e = E(h);
+    *out_mesh = (int32_t)e->meshes.size();
+    e->meshes.push_back(tfb::buildMesh(v, idx));
+    e->layoutDirty = true;
+    return TF_OK;
+}
+
+TF_API int tf_mesh_read(void* h, int32_t mesh, int32_t counts[3], float* vertices, uint32_t* indices, float* normals,
+                        uint8_t* edges, float* node_bounds, int32_t* node_ranges) {
+    if (!h) { return tfb::fail(TF_E_INVALID, "tf_mesh_read: null world"); }
+    Engine* e = E(h);
+    if (mesh < 0 || (size_t)mesh >= e->meshes.size()) { return tfb::fail(TF_E_INVALID, "tf_mesh_read: unknown mesh"); }
+    const tfb::HostMesh& m = e->meshes[(size_t)mesh];
+    if (counts) {
+        counts[0] = (int32_t)m.vertices.size();
+        counts[1] = (int32_t)m.normals.size();
+        counts[2] = (int32_t)m.nodes.size();
+    }
+    for (size_t i = 0; i < m.vertices.size(); ++i) {
+        if (vertices) { vertices[3 * i] = m.vertices[i].x, vertices[3 * i + 1] = m.vertices[i].y, vertices[3 * i + 2] = m.vertices[i].z; }
+    }
+    if (indices) { std::copy(m.indices.begin(), m.indices.end(), indices); }
+    for (size_t t = 0; t < m.normals.size(); ++t) {
+        if (normals) { normals[3 * t] = m.normals[t].x, normals[3 * t + 1] = m.normals[t].y, normals[3 * t + 2] = m.normals[t].z; }
+        if (edges) { edges[t] = m.edges[t]; }
+    }
+    for (size_t n = 0; n < m.nodes.size(); ++n) {
+        const tfb::MeshNode& x = m.nodes[n];
+        if (node_bounds) {
+            const float b[6] = { x.lo.x, x.lo.y, x.lo.z, x.hi.x, x.hi.y, x.hi.z };
+            std::copy(b, b + 6, node_bounds + 6 * n);
+        }
+        if (node_ranges) {
+            node_ranges[2 * n] = x.first;
+            node_ranges[2 * n + 1] = x.count;
+        }
+    }
     return TF_OK;
 }
 

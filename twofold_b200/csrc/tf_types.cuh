@@ -99,6 +99,8 @@ struct alignas(16) DShape {
     float halfHeight;
     Vec3 halfExtents;
     int32_t poly;  // index into the polyhedron table, -1 for none
+    int32_t mesh;  // index into the mesh table, -1 for none; a mesh keeps its root node's center in centroid
+                   // and half size in halfExtents
     float extent;
     float minExtent;
     Vec3 centroid;
@@ -113,6 +115,23 @@ struct DPoly {
     int32_t iFirst, iCount;  // face vertex loops
     Vec3 centroid;
     Vec3 lo, hi;
+};
+
+// A triangle mesh (src/internal.h:47-87) stored as ranges of the shared mesh tables: vertex k is
+// meshVerts[vFirst + k]; triangle t has corners meshIndices[3 * (tFirst + t) + 0..2] (vertex numbers of
+// this mesh), normal meshNormals[tFirst + t] and edge flags meshEdges[tFirst + t]; node i is
+// meshNodes[nFirst + i], its first naming a triangle of a leaf or the first child of an inner node.
+struct DMesh {
+    int32_t vFirst, vCount;
+    int32_t tFirst, tCount;
+    int32_t nFirst, nCount;
+};
+
+// A mesh tree node (src/internal.h:50-54): a leaf holds count triangles from first; an inner node has a
+// count of zero and its children at first and first + 1.
+struct MeshNode {
+    Vec3 lo, hi;
+    int32_t first, count;
 };
 
 // Face and edge fields index within their own polyhedron (vertex k is verts[vFirst + k]).

@@ -55,6 +55,8 @@ class World:
         self.body_of = np.ascontiguousarray(body_of, dtype=np.uint32)
         self.meta = meta or {}
         self.keepalive = []
+        # TriangleMeshes as (vertices (n, 3), indices (3 m,)); a TF_MESH shape's "mesh" is a position here.
+        self.meshes = []
 
     @property
     def dynamic_count(self):
@@ -103,6 +105,7 @@ def _shapes(n):
     s["friction"] = 0.5
     s["category"] = 1
     s["mask"] = 0xFFFFFFFF
+    s["mesh"] = -1
     return s
 
 
@@ -413,6 +416,68 @@ def bullets(n=24, seed=0, speed=(40.0, 80.0)):
         s["density"][i] = 2.0
     s["friction"][3:] = 0.5
     return w
+
+
+def terrain_mesh(cells=256, cell=0.5, seed=0):
+    """A height field of cells x cells squares of `cell` m, centred on the origin, two triangles a square
+    facing +y: h = sum over k < 8 of 0.25 sin(a_k x + b_k z + phi_k), (a_k, b_k) = f_k (cos t_k, sin t_k),
+    f_k ~ U[0.05, 0.5] rad/m, t_k and phi_k ~ U[0, 2 pi). Returns (vertices, indices)."""
+    rng = np.random.default_rng([seed, 2, 1])
+    f = rng.uniform(0.05, 0.5, size=8)
+    t = rng.uniform(0.0, 2 * math.pi, size=8)
+    phi = rng.uniform(0.0, 2 * math.pi, size=8)
+    a, b = f * np.cos(t), f * np.sin(t)
+    g = (np.arange(cells + 1) - cells / 2.0) * cell
+    x, z = np.meshgrid(g, g, indexing="ij")
+    h = sum(0.25 * np.sin(a[k] * x + b[k] * z + phi[k]) for k in range(8))
+    vertices = np.stack([x, h, z], axis=-1).reshape(-1, 3).astype(F32)
+    i, j = np.meshgrid(np.arange(cells), np.arange(cells), indexing="ij")
+    v00 = (i * (cells + 1) + j).reshape(-1)
+    v01, v10, v11 = v00 + 1, v00 + cells + 1, v00 + cells + 2
+    indices = np.stack([v00, v01, v11, v00, v11, v10], axis=1).reshape(-1).astype(np.uint32)
+    return vertices, indices
+
+
+def terrain(cells=256, cell=0.5, cols=32, levels=32, pitch=2.0, top=60.0, seed=0):
+    """Bodies dropped on a static terrain mesh (terrain_mesh): cols x cols columns at `pitch` m, `levels`
+    levels from y = 2 to `top`, positions jittered by U[-0.1, 0.1], cycling through a sphere of radius
+    U[0.25, 0.75], a box of half extents U[0.2, 0.8] and a hull of 16 points uniform on a 0.5 m sphere (at most
+    16 vertices); density U[0.5, 2], uniformly random rotations, default sleeping."""
+    rng = np.random.default_rng([seed, 2, 2])
+    n = cols * cols * levels
+    b, s = _bodies(n + 1), _shapes(n + 1)
+    w = World(b, s, np.arange(n + 1), meta={"kind": "terrain"})
+    w.meshes.append(terrain_mesh(cells, cell, seed))
+    b["type"][0] = abi.TF_STATIC
+    s["geometry"][0] = abi.TF_MESH
+    s["mesh"][0] = 0
+    s["friction"][0] = 0.6
+    idx = np.arange(n)
+    level, col = idx // (cols * cols), idx % (cols * cols)
+    cx, cz = col % cols, col // cols
+    y = 2.0 + (top - 2.0) / max(levels - 1, 1) * level
+    pos = np.stack([(cx - (cols - 1) / 2.0) * pitch, y, (cz - (cols - 1) / 2.0) * pitch], axis=1)
+    b["position"][1:] = (pos + rng.uniform(-0.1, 0.1, size=(n, 3))).astype(F32)
+    b["rotation"][1:] = _uniform_quats(rng, n)
+    s["density"][1:] = rng.uniform(0.5, 2.0, size=n).astype(F32)
+    for k in range(n):
+        i = k + 1
+        kind = k % 3
+        if kind == 0:
+            s["geometry"][i] = abi.TF_SPHERE
+            s["radius"][i] = rng.uniform(0.25, 0.75)
+        elif kind == 1:
+            s["half_extents"][i] = rng.uniform(0.2, 0.8, size=3).astype(F32)
+        else:
+            s["geometry"][i] = abi.TF_HULL
+            s["max_vertices"][i] = 16
+            _set_points(w, i, _sphere_points(rng, 16, 0.5))
+    return w
+
+
+def config2():
+    """Terrain: 32,768 spheres, boxes and hulls dropped on a 256 x 256 cell terrain mesh, 600 steps."""
+    return Scene("terrain_32768", [terrain()], steps=600)
 
 
 def config3():

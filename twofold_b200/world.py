@@ -25,11 +25,39 @@ class Batch:
             world_of = np.full(nb, wi, np.int32)
             abi.check(self.lib.tf_bodies_create(self.h, nb, world_of.ctypes.data,
                                                 w.bodies.ctypes.data_as(C.POINTER(abi.tf_body_desc)), None), self.lib)
+            shapes = w.shapes
+            if getattr(w, "meshes", None):
+                # A world's shapes name its meshes by position; the handle names them by its own ids.
+                ids = [self.create_mesh(v, i) for v, i in w.meshes]
+                shapes = w.shapes.copy()
+                named = shapes["geometry"] == abi.TF_MESH
+                shapes["mesh"][named] = np.asarray(ids, np.int32)[shapes["mesh"][named]]
             world_of = np.full(ns, wi, np.int32)
             abi.check(self.lib.tf_shapes_add(self.h, ns, world_of.ctypes.data, w.body_of.ctypes.data,
-                                             w.shapes.ctypes.data_as(C.POINTER(abi.tf_shape_desc)), None), self.lib)
+                                             shapes.ctypes.data_as(C.POINTER(abi.tf_shape_desc)), None), self.lib)
             self.body_counts.append(nb)
         self.offsets = np.concatenate([[0], np.cumsum(self.body_counts)]).astype(np.int64)
+
+    def create_mesh(self, vertices, indices):
+        """tf_mesh_create: a TriangleMesh every world of the batch may use; returns its id."""
+        v = np.ascontiguousarray(vertices, np.float32).reshape(-1, 3)
+        i = np.ascontiguousarray(indices, np.uint32).reshape(-1)
+        out = C.c_int32(-1)
+        abi.check(self.lib.tf_mesh_create(self.h, v.ctypes.data, len(v), i.ctypes.data, len(i), C.byref(out)), self.lib)
+        return out.value
+
+    def read_mesh(self, mesh):
+        """The built mesh: vertices, indices, normals, edge flags, node bounds (lo, hi) and ranges (first, count)."""
+        counts = np.zeros(3, np.int32)
+        abi.check(self.lib.tf_mesh_read(self.h, mesh, counts.ctypes.data, None, None, None, None, None, None), self.lib)
+        nv, nt, nn = (int(x) for x in counts)
+        out = {"vertices": np.zeros((nv, 3), np.float32), "indices": np.zeros(3 * nt, np.uint32),
+               "normals": np.zeros((nt, 3), np.float32), "edges": np.zeros(nt, np.uint8),
+               "node_bounds": np.zeros((nn, 6), np.float32), "node_ranges": np.zeros((nn, 2), np.int32)}
+        abi.check(self.lib.tf_mesh_read(self.h, mesh, counts.ctypes.data, *(out[k].ctypes.data for k in
+                                        ("vertices", "indices", "normals", "edges", "node_bounds", "node_ranges"))),
+                  self.lib)
+        return out
 
     @classmethod
     def from_scene(cls, scene, device=0):
