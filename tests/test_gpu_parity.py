@@ -121,6 +121,31 @@ def test_planar_worlds_match_reference(floor, seed, restitution):
             _compare_world(b, 0, r, f"planar {floor} seed {seed} step {s + 1}")
 
 
+@needs_oracle
+@pytest.mark.parametrize("seed", range(3))
+def test_terrain_worlds_match_reference(seed):
+    """Spheres, boxes and hulls dropped on a terrain mesh: triangles from the tree, the two-faced triangle
+    collisions, edges and corners without their own normal, manifolds grouped by normal into several
+    contacts per pair (keys with parts), their reuse, and the refresh of fast pairs with the triangles ruled
+    out at the step's start. Pairs, contacts and states are compared along 150 steps, and every step's swept
+    pairs and impacts."""
+    w = scenes.terrain(cells=16, cell=0.5, cols=4, levels=2, pitch=1.7, top=5.0, seed=seed)
+    sc = scenes.Scene("terrain", [w])
+    b = Batch.from_scene(sc)
+    r = R.RefWorld(w, sc.settings)
+    parts = 0
+    for s in range(150):
+        b.step_checked(sc.dt)
+        r.step(sc.dt)
+        mine, theirs = b.profile(0), r.profile()
+        assert (mine.swept_pairs, mine.impacts) == (theirs.swept_pairs, theirs.impacts), f"terrain {seed} step {s + 1}"
+        if s in (0, 1, 10, 30, 60, 90, 120, 149):
+            _check_pairs_and_manifolds(b, 0, r, f"terrain seed {seed} step {s + 1}")
+            _compare_world(b, 0, r, f"terrain seed {seed} step {s + 1}")
+            parts = max(parts, max((c.part for c in r.contacts(mode=1)), default=0))
+    assert parts > 0  # some pair met the terrain with more than one group of triangles
+
+
 def _continuous_world(kind, seed):
     if kind == "hulls":
         return scenes.hulls(n=24, seed=seed, degenerate=True)

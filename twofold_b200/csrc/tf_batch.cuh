@@ -2,6 +2,7 @@
 #pragma once
 
 #include "tf_collide.cuh"
+#include "tf_mesh_collide.cuh"
 #include "tf_solver.cuh"
 #include "tf_types.cuh"
 
@@ -30,10 +31,15 @@ struct Batch {
     uint32_t* unionParent;
     float* islandTime;
 
-    // Per candidate (candFirst + i).
+    // Per candidate (candFirst + i): the key, its first contact, how many contacts it made (more than one for
+    // a mesh pair), and where the ones after the first went (partFirst + stagePart[i], in stageExtra).
     uint64_t* cand;
     DContact* stage;
     uint8_t* stageUsed;
+    uint32_t* stagePart;
+    DContact* stageExtra;
+    // Per world (boundsFirst + i): triangles fast mesh pairs ruled out, each pair's run sorted by triangle.
+    TriangleBound* triBounds;
 
     // Per contact slot (contactFirst + i). Contacts double-buffer across steps.
     DContact* contacts;   // current

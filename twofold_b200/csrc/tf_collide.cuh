@@ -1038,10 +1038,12 @@ TF_HD void collideHalfSpace(const CollideCtx& cx, const Transform& xh, const DSh
 // code; kClassAny compiles every path.
 // kClassPlanar holds the pairs solved in a plane (decided by their bodies, not their shapes); its kernels
 // fall back to every 3D path for profiles the plane does not cut.
+// kClassMesh holds the pairs with a triangle mesh, which may make several contacts.
 enum PairClass : int {
-    kClassAny = -1, kClassSpheres = 0, kClassSpherePoly = 1, kClassPlane = 2, kClassConvex = 3, kClassPlanar = 4
+    kClassAny = -1, kClassSpheres = 0, kClassSpherePoly = 1, kClassPlane = 2, kClassConvex = 3, kClassPlanar = 4,
+    kClassMesh = 5
 };
-constexpr int kPairClasses = 5;
+constexpr int kPairClasses = 6;
 
 TF_HD int pairClass(uint32_t ka, uint32_t kb) {
     if (ka == kHalfSpace || kb == kHalfSpace) { return kClassPlane; }

@@ -3,11 +3,13 @@
 // reach, and a dynamic body that hit something moves back along its sweep to the first hit, together with
 // every dynamic body it hit.
 //
-// The reference turns sweeps with the C library's sinf, cosf and atan2f. Here they are evaluated in double
-// and rounded to float, which gives the correctly rounded value; where the host's float functions round the
-// other way (their documented error reaches past half an ulp) a swept pose differs by one ulp.
+// The reference turns sweeps with the C library's sinf, cosf and atan2f, and measures a body's turn with
+// asinf. Here they are evaluated in double and rounded to float, which gives the correctly rounded value;
+// where the host's float functions round the other way (their documented error reaches past half an ulp) a
+// swept pose differs by one ulp.
 #pragma once
 
+#include "tf_mesh_collide.cuh"
 #include "tf_planar.cuh"
 
 namespace tfb {
@@ -15,6 +17,7 @@ namespace tfb {
 TF_HD float sinRounded(float x) { return (float)sin((double)x); }
 TF_HD float cosRounded(float x) { return (float)cos((double)x); }
 TF_HD float atan2Rounded(float y, float x) { return (float)atan2((double)y, (double)x); }
+TF_HD float asinRounded(float x) { return (float)asin((double)x); }
 
 // A body's motion over the step: its center moves in a line, its rotation turns about one axis
 // (src/internal.h:230-238).
@@ -136,21 +139,64 @@ TF_HD bool sweepsShape(const PolyTables& pt, const DShape& s, const DBody& b, fl
 // Sweeps a fast shape f against shape o: first its core (a sphere of half its inner extent at its
 // centroid), which decides whether it hit, then the whole shape, whose first touch is the time when it
 // finds one (src/world.cpp:1341-1357). Returns whether f hit o, with the time in t.
-TF_HD bool sweepPair(const PolyTables& pt, const CollideCtx& cx, const DShape& f, const DBody& bf, const DShape& o,
-                     const DBody& bo, float target, float& t) {
-    const Sweep sf = sweepOf(bf), so = sweepOf(bo);
-    const Convex core{ &f.centroid, 1, 0.5f * innerExtent(pt, f, bf), false };
+TF_HD bool sweepAgainst(const CollideCtx& cx, const DShape& f, const DBody& bf, const Sweep& sf, const Convex& other,
+                        const Transform& otherLocal, const Sweep& so, float otherReach, float target, float& t) {
+    const Convex core{ &f.centroid, 1, 0.5f * innerExtent(cx.pt, f, bf), false };
     const float coreReach = length(apply(f.local, f.centroid) - bf.localCenter) + core.radius;
-    const Convex other = convexOf(cx, o);
-    const float otherReach = o.kind == kHalfSpace ? 0.0f : shapeReach(o, bo);
     float coreT = 1.0f;
-    if (timeOfImpact(core, f.local, sf, coreReach, other, o.local, so, otherReach, target, coreT) != kHit) {
+    if (timeOfImpact(core, f.local, sf, coreReach, other, otherLocal, so, otherReach, target, coreT) != kHit) {
         return false;
     }
-    if (timeOfImpact(convexOf(cx, f), f.local, sf, shapeReach(f, bf), other, o.local, so, otherReach, target, t) != kHit) {
+    if (timeOfImpact(convexOf(cx, f), f.local, sf, shapeReach(f, bf), other, otherLocal, so, otherReach, target, t) != kHit) {
         t = coreT;
     }
     return true;
+}
+
+// boundsInMesh (src/mesh.cpp:252-263): the box lo, hi of the world in the frame of a mesh at xm.
+TF_HD void boundsInMesh(const Transform& xm, const Vec3& lo, const Vec3& hi, Vec3& meshLo, Vec3& meshHi) {
+    const Vec3 c = applyInverse(xm, (lo + hi) * 0.5f);
+    const Vec3 e = (hi - lo) * 0.5f;
+    const Mat3 r = toMat3(conjugate(xm.q));
+    Vec3 reach;
+    for (int i = 0; i < 3; ++i) {
+        setComp(reach, i, fabsf(r.r[i].x) * e.x + fabsf(r.r[i].y) * e.y + fabsf(r.r[i].z) * e.z);
+    }
+    meshLo = c - reach;
+    meshHi = c + reach;
+}
+
+// Sweeps fast shape f against shape o (src/world.cpp:1341-1389): against a mesh, every triangle the tree
+// finds within f's bounds over the step, from o's pose at both ends of the step, the earliest hit kept.
+// Returns whether f hit o, with the time in t; false in `ok` for a tree deeper than the walk holds.
+TF_HD bool sweepPair(const CollideCtx& cx, const DShape& f, const DBody& bf, const DShape& o, const DBody& bo,
+                     const Vec3& sweptLo, const Vec3& sweptHi, float target, float& t, bool& ok) {
+    const Sweep sf = sweepOf(bf), so = sweepOf(bo);
+    ok = true;
+    if (o.kind != kMesh) {
+        const float otherReach = o.kind == kHalfSpace ? 0.0f : shapeReach(o, bo);
+        return sweepAgainst(cx, f, bf, sf, convexOf(cx, o), o.local, so, otherReach, target, t);
+    }
+    if (o.mesh < 0) { return false; }
+    const DMesh M = cx.mt.meshes[o.mesh];
+    Vec3 lo0, hi0, lo1, hi1;
+    boundsInMesh(sweepAt(so, 0.0f) * o.local, sweptLo, sweptHi, lo0, hi0);
+    boundsInMesh(bo.xf * o.local, sweptLo, sweptHi, lo1, hi1);
+    bool hit = false;
+    t = 1.0f;
+    ok = queryMesh(cx.mt, M, minVec(lo0, lo1), maxVec(hi0, hi1), [&](int tri) {
+        Vec3 c[3];
+        meshCorners(cx.mt, M, tri, c);
+        float triReach = 0.0f;
+        for (int k = 0; k < 3; ++k) { triReach = maxf(triReach, length(apply(o.local, c[k]) - bo.localCenter)); }
+        float tt = 1.0f;
+        const Convex triangle{ c, 3, 0.0f, false };
+        if (sweepAgainst(cx, f, bf, sf, triangle, o.local, so, triReach, target, tt)) {
+            t = minf(t, tt);
+            hit = true;
+        }
+    });
+    return hit;
 }
 
 }

@@ -152,6 +152,9 @@ public:
     DevArray<uint64_t> dCand;
     DevArray<DContact> dStage;
     DevArray<uint8_t> dStageUsed;
+    DevArray<uint32_t> dStagePart;
+    DevArray<DContact> dStageExtra;
+    DevArray<TriangleBound> dTriBounds;
     DevArray<DContact> dContacts[2];
     int cur = 0;
     DevArray<uint32_t> dActive, dImpact, dColored, dImpactColored, dRest, dImpactRest;
@@ -582,7 +585,7 @@ public:
         dropGraphs();
         const size_t nw = worlds.size();
         info.assign(nw, WorldInfo{});
-        size_t nb = 0, ns = 0, ncand = 0, ncon = 0, nplanes = 0;
+        size_t nb = 0, ns = 0, ncand = 0, ncon = 0, nplanes = 0, nparts = 0, nbounds = 0;
         std::vector<DPoly> polys;
         std::vector<Vec3> verts, normals, arcs;
         std::vector<int32_t> indices;
@@ -615,6 +618,14 @@ public:
             wi.contactCap = std::max({ cap + 64u, (uint32_t)W.contacts.size() + 64u, minContactCap[w] });
             maxBodies = std::max(maxBodies, wi.bodyCount);
             maxContacts = std::max(maxContacts, wi.contactCap);
+            bool hasMesh = false;
+            for (const HostShape& hs : W.shapes) { hasMesh = hasMesh || (hs.d.alive && hs.d.kind == kMesh); }
+            wi.partFirst = (uint32_t)nparts;
+            wi.partCap = hasMesh ? cap : 0u;
+            wi.boundsFirst = (uint32_t)nbounds;
+            wi.boundsCap = hasMesh ? 16u * cap : 0u;
+            nparts += wi.partCap;
+            nbounds += wi.boundsCap;
             nb += wi.bodyCount;
             ns += wi.shapeCount;
             nplanes += wi.planeCount;
@@ -764,6 +775,9 @@ public:
         TF_ALLOC(dCand, ncand);
         TF_ALLOC(dStage, ncand);
         TF_ALLOC(dStageUsed, ncand);
+        TF_ALLOC(dStagePart, ncand);
+        TF_ALLOC(dStageExtra, nparts);
+        TF_ALLOC(dTriBounds, nbounds);
         TF_ALLOC(dContacts[0], ncon);
         TF_ALLOC(dContacts[1], ncon);
         TF_ALLOC(dActive, ncon);
@@ -912,6 +926,9 @@ public:
         B.cand = dCand.ptr;
         B.stage = dStage.ptr;
         B.stageUsed = dStageUsed.ptr;
+        B.stagePart = dStagePart.ptr;
+        B.stageExtra = dStageExtra.ptr;
+        B.triBounds = dTriBounds.ptr;
         B.contacts = dContacts[cur_].ptr;
         B.previous = dContacts[1 - cur_].ptr;
         B.active = dActive.ptr;
@@ -966,6 +983,7 @@ public:
             k_collide<kClassPlane><<<flatGrids[2], threads(7), 0, stream>>>(B, P, serial);
             k_collide<kClassConvex><<<flatGrids[3], threads(7), 0, stream>>>(B, P, serial);
             k_collide<kClassPlanar><<<flatGrids[4], threads(7), 0, stream>>>(B, P, serial);
+            k_collide<kClassMesh><<<flatGrids[5], threads(7), 0, stream>>>(B, P, serial);
         });
         timed(1, rec, [&] { k_narrowphase<<<grids[1], threads(1), 0, stream>>>(B, P, splits[1], serial); });
         timed(2, rec, [&] { k_wake<<<grids[2], threads(2), 0, stream>>>(B, splits[2], serial); });
@@ -978,12 +996,13 @@ public:
         for (int i = 0; i < P.substeps; ++i) {
             if (i > 0) {
                 timed(4, rec, [&] {
-                    k_refresh<kClassAny><<<flatGrids[5], threads(4), 0, stream>>>(B, P, i, serial);
-                    k_refresh<kClassSpheres><<<flatGrids[6], threads(4), 0, stream>>>(B, P, i, serial);
-                    k_refresh<kClassSpherePoly><<<flatGrids[7], threads(4), 0, stream>>>(B, P, i, serial);
-                    k_refresh<kClassPlane><<<flatGrids[8], threads(4), 0, stream>>>(B, P, i, serial);
-                    k_refresh<kClassConvex><<<flatGrids[9], threads(4), 0, stream>>>(B, P, i, serial);
-                    k_refresh<kClassPlanar><<<flatGrids[10], threads(4), 0, stream>>>(B, P, i, serial);
+                    k_refresh<kClassAny><<<flatGrids[6], threads(4), 0, stream>>>(B, P, i, serial);
+                    k_refresh<kClassSpheres><<<flatGrids[7], threads(4), 0, stream>>>(B, P, i, serial);
+                    k_refresh<kClassSpherePoly><<<flatGrids[8], threads(4), 0, stream>>>(B, P, i, serial);
+                    k_refresh<kClassPlane><<<flatGrids[9], threads(4), 0, stream>>>(B, P, i, serial);
+                    k_refresh<kClassConvex><<<flatGrids[10], threads(4), 0, stream>>>(B, P, i, serial);
+                    k_refresh<kClassPlanar><<<flatGrids[11], threads(4), 0, stream>>>(B, P, i, serial);
+                    k_refresh<kClassMesh><<<flatGrids[12], threads(4), 0, stream>>>(B, P, i, serial);
                 });
             }
             timed(5, rec, [&] { k_substep<<<grids[5], threads(5), smem(5), stream>>>(B, P, splits[5], i, serial); });
@@ -1093,10 +1112,11 @@ public:
         const void* flat[kFlatGrids] = {
             (const void*)k_collide<kClassSpheres>,  (const void*)k_collide<kClassSpherePoly>,
             (const void*)k_collide<kClassPlane>,    (const void*)k_collide<kClassConvex>,
-            (const void*)k_collide<kClassPlanar>,   (const void*)k_refresh<kClassAny>,
-            (const void*)k_refresh<kClassSpheres>,  (const void*)k_refresh<kClassSpherePoly>,
-            (const void*)k_refresh<kClassPlane>,    (const void*)k_refresh<kClassConvex>,
-            (const void*)k_refresh<kClassPlanar> };
+            (const void*)k_collide<kClassPlanar>,   (const void*)k_collide<kClassMesh>,
+            (const void*)k_refresh<kClassAny>,      (const void*)k_refresh<kClassSpheres>,
+            (const void*)k_refresh<kClassSpherePoly>, (const void*)k_refresh<kClassPlane>,
+            (const void*)k_refresh<kClassConvex>,   (const void*)k_refresh<kClassPlanar>,
+            (const void*)k_refresh<kClassMesh> };
         for (int f = 0; f < kFlatGrids; ++f) {
             int perSm = 0;
             const int threads = (int)shapes[f < kPairClasses ? 7 : 4].threads;

@@ -174,6 +174,23 @@ __device__ uint32_t groupCompact(const Group& g, uint32_t n, Pred pred, Emit emi
     return base;
 }
 
+// Calls emit(i, position, k) for k < count(i) of every i < n, positions dense and in (i, k) order. Ends with a
+// group barrier.
+template <class Count, class Emit>
+__device__ uint32_t groupExpand(const Group& g, uint32_t n, Count count, Emit emit) {
+    uint32_t base = 0;
+    for (uint32_t start = 0; start < n; start += g.size) {
+        const uint32_t i = start + g.tid;
+        const uint32_t c = i < n ? count(i) : 0u;
+        uint32_t tot;
+        const uint32_t pos = groupScan(g, c, tot);
+        for (uint32_t k = 0; k < c; ++k) { emit(i, base + pos + k, k); }
+        base += tot;
+    }
+    g.sync();
+    return base;
+}
+
 // Reads the abort word once per CTA at a kernel's start: true when an earlier step of this launch sequence
 // overflowed a list, or this step did in an earlier kernel.
 __device__ __forceinline__ bool stepAborted(const Batch& B, int serial) {
@@ -190,10 +207,9 @@ __device__ __forceinline__ bool stepAborted(const Batch& B, int serial) {
 __device__ __forceinline__ int pairClassOf(const Batch& B, uint32_t a, uint32_t b) {
     const DShape& sa = B.shapes[a];
     const DShape& sb = B.shapes[b];
+    if (sa.kind == kMesh || sb.kind == kMesh) { return kClassMesh; }
     Vec3 n;
-    if (sa.kind != kMesh && sb.kind != kMesh && usePlanar(B.bodies[sa.body], B.bodies[sb.body], n)) {
-        return kClassPlanar;
-    }
+    if (usePlanar(B.bodies[sa.body], B.bodies[sb.body], n)) { return kClassPlanar; }
     return pairClass(sa.kind, sb.kind);
 }
 
@@ -400,6 +416,8 @@ __global__ void __launch_bounds__(kMaxBlock) k_broadphase(const __grid_constant_
         if (g.tid == 0) {
             wc.candCount = unique;
             wc.candNeeded = max(wc.candNeeded, total);
+            wc.partCount = 0;
+            wc.boundsCount = 0;
         }
         // The pairs join the flat list of their class: counted per class, a block of each list reserved for
         // the world, then scattered into it.
@@ -615,6 +633,7 @@ __device__ void narrowOne(const Batch& B, const StepParams& P, const WorldInfo& 
         if (hi - lo > 1) { atomicOr(&wc.flags, kDevUnsupported); }
         out = old[lo];
         measureAgain(ba, bb, out, P);
+        out.boundsFirst = out.boundsCount = 0;
         used = 1;
     } else {
         Manifold m;
@@ -631,6 +650,7 @@ __device__ void narrowOne(const Batch& B, const StepParams& P, const WorldInfo& 
             c.featKind = m.featKind;
             c.featA = m.featA;
             c.featB = m.featB;
+            c.boundsFirst = c.boundsCount = 0;
             c.normal = m.normal;
             c.tangent1 = perpendicular(m.normal);
             c.tangent2 = cross(m.normal, c.tangent1);
@@ -681,6 +701,172 @@ __device__ void narrowOne(const Batch& B, const StepParams& P, const WorldInfo& 
     B.stageUsed[wi.candFirst + i] = used;
 }
 
+// A pair with a mesh over dt (src/world.cpp:505-533): manifolds with normals from sa to sb, into out.
+__device__ int collideMeshPair(const Batch& B, const StepParams& P, const DShape& sa, const DShape& sb, float dt,
+                               Manifold* out, int& outCount, MeshBounds* bounds) {
+    const DBody& ba = B.bodies[sa.body];
+    const DBody& bb = B.bodies[sb.body];
+    const float travel = relativeTravel(ba, bb, dt);
+    const float margin = P.tol.speculative + travel;
+    const Transform xa = ba.xf * sa.local;
+    const Transform xb = bb.xf * sb.local;
+    const Motion mo{ ba.v, ba.w, ba.com, bb.v, bb.w, bb.com, dt, travel > P.tol.speculative };
+    if (sa.kind == kMesh) { return collideMesh(B.cx, sa, xa, sb, xb, margin, mo, out, outCount, bounds); }
+    const int status = collideMesh(B.cx, sb, xb, sa, xa, margin, mo.swapped(), out, outCount, bounds);
+    for (int i = 0; i < outCount; ++i) { out[i].normal = -out[i].normal; }
+    return status;
+}
+
+// A contact of pair (sa, sb) from one manifold (src/world.cpp:912-939): points on both surfaces, anchors,
+// tangents and the reuse record.
+__device__ void contactFromManifold(const StepParams& P, const DBody& ba, const DBody& bb, const Manifold& m, DContact& c) {
+    c.featKind = m.featKind;
+    c.featA = m.featA;
+    c.featB = m.featB;
+    c.normal = m.normal;
+    c.tangent1 = perpendicular(m.normal);
+    c.tangent2 = cross(m.normal, c.tangent1);
+    c.count = m.count;
+    for (int k = 0; k < m.count; ++k) {
+        DPoint& p = c.points[k];
+        const Vec3 pos = m.points[k].position;
+        const float sep = m.points[k].separation;
+        const Vec3 half = m.normal * (0.5f * sep);
+        p.surfaceA = applyInverse(ba.xf, pos - half);
+        p.surfaceB = applyInverse(bb.xf, pos + half);
+        p.localA = applyInverse(ba.xf, pos);
+        p.separation = sep;
+        const Vec3 up = lift(ba, bb, m.normal, sep, P.tol.speculative);
+        p.anchorA = pos - up - ba.com;
+        p.anchorB = pos + up - bb.com;
+    }
+    c.localNormal = unrotate(ba.xf.q, c.normal);
+    c.baseOffset = unrotate(ba.xf.q, bb.com - ba.com);
+    c.baseTurn = conjugate(ba.xf.q) * bb.xf.q;
+    c.flags |= kCReusable;
+}
+
+// Stops this step (the host grows the world's lists and runs it again) when a mesh pair's parts or triangle
+// bounds do not fit the world's room for them.
+__device__ void meshRoomOverflow(const Batch& B, const WorldInfo& wi, WorldCounts& wc, int serial) {
+    atomicOr(&wc.flags, kDevPairOverflow);
+    atomicMax(&wc.candNeeded, 2 * wi.candCap);
+    atomicMin(B.abortStep, (uint32_t)serial);
+}
+
+// One mesh candidate (src/world.cpp:883-959): the old contacts kept and measured again when the pair barely
+// moved, else one contact per manifold the mesh collision makes, each carrying the impulses of the old
+// contact whose normal is closest. The first contact goes to the candidate's staging slot, the others to
+// the world's extra parts. A fast pair records the triangles it ruled out, for the refresh within the step.
+__device__ void narrowMesh(const Batch& B, const StepParams& P, const WorldInfo& wi, WorldCounts& wc, uint32_t i,
+                           const DContact* old, uint32_t oldCount, int serial) {
+    B.stageUsed[wi.candFirst + i] = 0;
+    const uint64_t key = B.cand[wi.candFirst + i];
+    const uint32_t ia = (uint32_t)(key >> 32), ib = (uint32_t)(key & 0xffffffffu);
+    if (!TF_OK_INDEX(B, ia < wi.shapeCount && ib < wi.shapeCount, 34, wi.bodyFirst, ia)) { return; }
+    const uint32_t gsa = wi.shapeFirst + ia, gsb = wi.shapeFirst + ib;
+    const DShape sa = B.shapes[gsa];
+    const DShape sb = B.shapes[gsb];
+    if (!TF_OK_INDEX(B, oldCount <= wi.contactCap, 35, wi.bodyFirst, oldCount)) { return; }
+    const DBody& ba = B.bodies[sa.body];
+    const DBody& bb = B.bodies[sb.body];
+    const uint32_t lo = lowerKey(old, oldCount, key);
+    uint32_t hi = lo;
+    while (hi < oldCount && old[hi].key == key) { ++hi; }
+    const bool hasOld = lo < hi;
+    bool keep = hasOld;
+    for (uint32_t it = lo; it < hi && keep; ++it) { keep = stillFits(old[it], ba, bb, P); }
+    const bool touched = hasOld && (old[lo].flags & kCTouched);
+
+    Manifold found[kMaxMeshParts];
+    int n = 0;
+    uint32_t boundsFirst = 0, boundsCount = 0;
+    if (keep) {
+        n = (int)(hi - lo);
+        if (n > kMaxMeshParts) {
+            atomicOr(&wc.flags, kDevUnsupported);
+            return;
+        }
+    } else {
+        const bool record = relativeTravel(ba, bb, P.dt) > P.tol.speculative;
+        TriangleBound ruled[kMaxMeshBounds];
+        MeshBounds mb{ record ? ruled : nullptr, 0, nullptr, 0, 0.0f };
+        if (collideMeshPair(B, P, sa, sb, P.dt, found, n, &mb) != kMeshOk) {
+            atomicOr(&wc.flags, kDevUnsupported);
+            return;
+        }
+        if (mb.foundCount > 0) {
+            // By triangle, as the reference sorts each pair's run.
+            for (int x = 1; x < mb.foundCount; ++x) {
+                const TriangleBound t = ruled[x];
+                int y = x - 1;
+                while (y >= 0 && ruled[y].triangle > t.triangle) {
+                    ruled[y + 1] = ruled[y];
+                    --y;
+                }
+                ruled[y + 1] = t;
+            }
+            boundsFirst = atomicAdd(&wc.boundsCount, (uint32_t)mb.foundCount);
+            boundsCount = (uint32_t)mb.foundCount;
+            if (boundsFirst + boundsCount > wi.boundsCap) {
+                meshRoomOverflow(B, wi, wc, serial);
+                return;
+            }
+            for (int x = 0; x < mb.foundCount; ++x) { B.triBounds[wi.boundsFirst + boundsFirst + x] = ruled[x]; }
+        }
+    }
+    if (n == 0) { return; }
+    uint32_t extra = 0;
+    if (n > 1) {
+        extra = atomicAdd(&wc.partCount, (uint32_t)(n - 1));
+        if (extra + (uint32_t)(n - 1) > wi.partCap) {
+            meshRoomOverflow(B, wi, wc, serial);
+            return;
+        }
+    }
+    for (int k = 0; k < n; ++k) {
+        DContact& out = k == 0 ? B.stage[wi.candFirst + i] : B.stageExtra[wi.partFirst + extra + (uint32_t)(k - 1)];
+        if (keep) {
+            out = old[lo + (uint32_t)k];
+            measureAgain(ba, bb, out, P);
+            out.boundsFirst = out.boundsCount = 0;
+        } else {
+            DContact c{};
+            c.key = key;
+            c.part = (uint32_t)k;
+            c.shapeA = gsa;
+            c.shapeB = gsb;
+            c.bodyA = sa.body;
+            c.bodyB = sb.body;
+            c.flags = touched ? kCTouched : 0u;
+            contactFromManifold(P, ba, bb, found[k], c);
+            c.boundsFirst = boundsFirst;
+            c.boundsCount = boundsCount;
+            int best = -1;
+            for (uint32_t it = lo; it < hi; ++it) {
+                if (old[it].count > 0 && (best < 0 || dot(old[it].normal, c.normal) > dot(old[best].normal, c.normal))) {
+                    best = (int)it;
+                }
+            }
+            if (best >= 0) { carryImpulses(old[best], c, P.tol.speculative * P.tol.speculative); }
+            out = c;
+        }
+        out.friction = sqrtf(sa.friction * sb.friction);
+        out.restitution = maxf(sa.restitution, sb.restitution);
+        out.rollingResistance = maxf(sa.rollingResistance, sb.rollingResistance);
+    }
+    if (ba.type == kDynamic && !ba.awake && movingAwake(bb)) {
+        B.wakeMark[sa.body] = 1;
+        wc.wakePending = 1;
+    }
+    if (bb.type == kDynamic && !bb.awake && movingAwake(ba)) {
+        B.wakeMark[sb.body] = 1;
+        wc.wakePending = 1;
+    }
+    B.stagePart[wi.candFirst + i] = extra;
+    B.stageUsed[wi.candFirst + i] = (uint8_t)n;
+}
+
 // The candidate pairs of one class, over every world, one thread per pair (src/world.cpp:874-960); each
 // result lands in the pair's own staging slot, so pairs need no order among themselves.
 template <int Cls>
@@ -693,7 +879,11 @@ __global__ void __launch_bounds__(256) k_collide(const __grid_constant__ Batch B
         const uint2 it = items[item];
         const WorldInfo wi = B.info[it.x];
         WorldCounts& wc = B.counts[it.x];
-        narrowOne<Cls>(B, P, wi, wc, it.y, B.previous + wi.contactFirst, wc.contactCount);
+        if constexpr (Cls == kClassMesh) {
+            narrowMesh(B, P, wi, wc, it.y, B.previous + wi.contactFirst, wc.contactCount, serial);
+        } else {
+            narrowOne<Cls>(B, P, wi, wc, it.y, B.previous + wi.contactFirst, wc.contactCount);
+        }
     }
 }
 
@@ -711,13 +901,16 @@ __global__ void __launch_bounds__(kMaxBlock) k_narrowphase(const __grid_constant
         const uint32_t oldCount = wc.contactCount;
         const DContact* old = B.previous + wi.contactFirst;
         const uint32_t cf = wi.contactFirst;
-        const uint32_t nC = groupCompact(
-            g, nc, [&](uint32_t i) { return B.stageUsed[wi.candFirst + i] != 0; },
-            [&](uint32_t i, uint32_t pos) {
-                const DContact& c = B.stage[wi.candFirst + i];
-                B.mergeKeyA[cf + pos] = c.key;
-                B.mergePartA[cf + pos] = c.part;
-                B.mergeIdxA[cf + pos] = i;
+        // Every candidate's contacts in part order: the first in its staging slot, the others (mesh pairs) in
+        // the world's extra parts, named with the high bit set.
+        const uint32_t nC = groupExpand(
+            g, nc, [&](uint32_t i) { return (uint32_t)B.stageUsed[wi.candFirst + i]; },
+            [&](uint32_t i, uint32_t pos, uint32_t k) {
+                const uint32_t x = k == 0 ? i : (0x80000000u | (B.stagePart[wi.candFirst + i] + k - 1));
+                const DContact* c = k == 0 ? B.stage + wi.candFirst + i : B.stageExtra + wi.partFirst + (x & 0x7fffffffu);
+                B.mergeKeyA[cf + pos] = c->key;
+                B.mergePartA[cf + pos] = c->part;
+                B.mergeIdxA[cf + pos] = x;
             });
         // Contacts of pairs where nothing moves and one body is dynamic (asleep) stay as they were
         // (src/world.cpp:961-988).
@@ -762,7 +955,10 @@ __global__ void __launch_bounds__(kMaxBlock) k_narrowphase(const __grid_constant
                     h = mid;
                 }
             }
-            B.contacts[cf + x + l] = B.stage[wi.candFirst + B.mergeIdxA[cf + x]];
+            const uint32_t src = B.mergeIdxA[cf + x];
+            const DContact* from = (src & 0x80000000u) ? B.stageExtra + wi.partFirst + (src & 0x7fffffffu)
+                                                        : B.stage + wi.candFirst + src;
+            B.contacts[cf + x + l] = *from;
         }
         for (uint32_t y = g.tid; y < nK; y += g.size) {
             const uint64_t k = B.mergeKeyB[cf + y];
@@ -1077,22 +1273,10 @@ __device__ __forceinline__ bool contactOk(const Batch& B, const WorldInfo& wi, c
 #endif
 }
 
-// A fast pair collided again with the remaining time (src/world.cpp:1074-1138).
-template <int Cls = kClassAny>
-__device__ void refreshContact(const Batch& B, const StepParams& P, DContact& c, float remaining) {
-    const DBody& a = B.bodies[c.bodyA];
-    const DBody& b = B.bodies[c.bodyB];
-    const DShape sa = B.shapes[c.shapeA];
-    const DShape sb = B.shapes[c.shapeB];
-    // Polyhedra that turned little against each other keep the edge pair they met on (src/world.cpp:1051-1055).
-    const Quat now = conjugate(a.xf.q) * b.xf.q, then = conjugate(a.q0) * b.q0;
-    const bool little = fabsf(dot(now, then)) >= P.featureTurnCos;
-    Manifold m;
-    collidePair<Cls>(B, P, sa, sb, remaining, m, little ? c.featKind : kFeatNone, c.featA, c.featB);
-    if (m.count == 0) {
-        c.count = 0;
-        return;
-    }
+// A contact takes a manifold of its pair collided again mid-step: new points on body A, the approach speed
+// and largest impulse of the nearest old point, and the old impulses carried (src/world.cpp:1106-1137).
+__device__ void takeRefreshed(const Batch& B, const StepParams& P, const DBody& a, const DBody& b, DContact& c,
+                              const Manifold& m) {
     const DContact old = c;
     c.flags &= ~kCReusable;
     c.featKind = m.featKind;
@@ -1120,6 +1304,72 @@ __device__ void refreshContact(const Batch& B, const StepParams& P, DContact& c,
         p.maxNormalImpulse = old.points[k].maxNormalImpulse;
     }
     carryImpulses(old, c, P.tol.speculative * P.tol.speculative);
+}
+
+// A fast pair collided again with the remaining time (src/world.cpp:1074-1138).
+template <int Cls = kClassAny>
+__device__ void refreshContact(const Batch& B, const StepParams& P, DContact& c, float remaining) {
+    const DBody& a = B.bodies[c.bodyA];
+    const DBody& b = B.bodies[c.bodyB];
+    const DShape sa = B.shapes[c.shapeA];
+    const DShape sb = B.shapes[c.shapeB];
+    // Polyhedra that turned little against each other keep the edge pair they met on (src/world.cpp:1051-1055).
+    const Quat now = conjugate(a.xf.q) * b.xf.q, then = conjugate(a.q0) * b.q0;
+    const bool little = fabsf(dot(now, then)) >= P.featureTurnCos;
+    Manifold m;
+    collidePair<Cls>(B, P, sa, sb, remaining, m, little ? c.featKind : kFeatNone, c.featA, c.featB);
+    if (m.count == 0) {
+        c.count = 0;
+        return;
+    }
+    takeRefreshed(B, P, a, b, c, m);
+}
+
+// How far any point of the body moved since the step started (src/world.cpp:484-488).
+__device__ __forceinline__ float movedThisStep(const DBody& b) {
+    const Quat turn = conjugate(b.q0) * b.xf.q;
+    const float s = minf(sqrtf(turn.x * turn.x + turn.y * turn.y + turn.z * turn.z), 1.0f);
+    return length(b.com - b.com0) + 2.0f * asinRounded(s) * b.extent;
+}
+
+// The contacts of a fast mesh pair, one key run, collided again with the remaining time: the pair is
+// collided once, skipping the triangles its collision at the step's start ruled out while they stay out of
+// reach, and each contact in turn takes the new manifold whose normal is closest to its own; a contact left
+// without one keeps no points (src/world.cpp:1078-1137).
+__device__ void refreshMeshRun(const Batch& B, const StepParams& P, const WorldInfo& wi, WorldCounts& wc, DContact* run,
+                               int count, float remaining) {
+    const DBody& a = B.bodies[run[0].bodyA];
+    const DBody& b = B.bodies[run[0].bodyB];
+    const DShape sa = B.shapes[run[0].shapeA];
+    const DShape sb = B.shapes[run[0].shapeB];
+    MeshBounds mb{ nullptr, 0, nullptr, 0, 0.0f };
+    if (run[0].boundsCount > 0 && TF_OK_INDEX(B, run[0].boundsFirst + run[0].boundsCount <= wi.boundsCap, 36, wi.bodyFirst, 0)) {
+        mb.known = B.triBounds + wi.boundsFirst + run[0].boundsFirst;
+        mb.knownCount = (int)run[0].boundsCount;
+        mb.moved = movedThisStep(a) + movedThisStep(b);
+    }
+    Manifold found[kMaxMeshParts];
+    int n = 0;
+    if (collideMeshPair(B, P, sa, sb, remaining, found, n, &mb) != kMeshOk) {
+        atomicOr(&wc.flags, kDevUnsupported);
+        n = 0;
+    }
+    bool taken[kMaxMeshParts];
+    for (int k = 0; k < n; ++k) { taken[k] = false; }
+    for (int x = 0; x < count; ++x) {
+        DContact& c = run[x];
+        int pick = -1;
+        for (int k = 0; k < n; ++k) {
+            if (taken[k]) { continue; }
+            if (pick < 0 || dot(found[k].normal, c.normal) > dot(found[pick].normal, c.normal)) { pick = k; }
+        }
+        if (pick < 0) {
+            c.count = 0;
+            continue;
+        }
+        taken[pick] = true;
+        takeRefreshed(B, P, a, b, c, found[pick]);
+    }
 }
 
 // The solver state of one body as a contact solved on its own (planar, rolling or past the last color) reads
@@ -1338,6 +1588,25 @@ __global__ void __launch_bounds__(256) k_refresh(const __grid_constant__ Batch B
         DContact& c = B.contacts[wi.contactFirst + ci];
         bool again = false;
         if constexpr (Cls != kClassAny) { again = (B.cflags[wi.contactFirst + ci] & againFlag) != 0; }
+        if constexpr (Cls == kClassMesh) {
+            // The contacts of a mesh pair share a key and sit together; the first takes the whole run.
+            const DContact* cs = B.contacts + wi.contactFirst;
+            if (ci > 0 && cs[ci - 1].key == c.key) { continue; }
+            uint32_t end = ci + 1;
+            while (end < wc.contactCount && cs[end].key == c.key) { ++end; }
+            DContact* run = B.contacts + wi.contactFirst + ci;
+            const int count = (int)(end - ci);
+            if (again) {
+                refreshMeshRun(B, P, wi, B.counts[it.x], run, count, remaining);
+            } else {
+                for (int x = 0; x < count; ++x) { rebaseContact(B.bodies[run[x].bodyA], B.bodies[run[x].bodyB], run[x]); }
+            }
+            for (int x = 0; x < count; ++x) {
+                makeContactAxes(axisBodyOf(B.bodies[run[x].bodyA]), axisBodyOf(B.bodies[run[x].bodyB]), run[x],
+                                B.axes + (size_t)(wi.contactFirst + ci + x) * kAxesPerContact);
+            }
+            continue;
+        }
         if constexpr (Cls != kClassAny) {
             if (again) { refreshContact<Cls>(B, P, c, remaining); }
         }
@@ -1571,13 +1840,16 @@ __device__ void sweepWorld(const Batch& B, const StepParams& P, const Group& g, 
         if (!boxesOverlap(B.sweptLo[sf + fi], B.sweptHi[sf + fi], B.sweptLo[sf + oi], B.sweptHi[sf + oi])) { continue; }
         if (!(f.category & o.mask) || !(o.category & f.mask)) { continue; }
         atomicAdd(pairs, 1u);
-        if (o.kind == kMesh || o.kind == kCylinder || f.kind == kCylinder) {
+        if (o.kind == kCylinder || f.kind == kCylinder) {
             atomicOr(&wc.flags, kDevUnsupported);
             continue;
         }
         const DBody& bo = B.bodies[o.body];
         float t = 1.0f;
-        if (!sweepPair(B.cx.pt, B.cx, f, B.bodies[f.body], o, bo, target, t)) { continue; }
+        bool ok = true;
+        const bool hit = sweepPair(B.cx, f, B.bodies[f.body], o, bo, B.sweptLo[sf + fi], B.sweptHi[sf + fi], target, t, ok);
+        if (!ok) { atomicOr(&wc.flags, kDevUnsupported); }
+        if (!hit) { continue; }
         const unsigned long long order = x < 0xffffffffull ? x : 0xfffffffeull;
         atomicMin(&B.hitKey[f.body], ((unsigned long long)__float_as_uint(t) << 32) | order);
         if (bo.type == kDynamic && !uniteHits(parent, f.body - bf, o.body - bf)) { atomicOr(&wc.flags, kDevTimeout); }

@@ -178,6 +178,9 @@ struct alignas(16) DContact {
     Vec3 baseOffset;
     Quat baseTurn;
     int32_t featKind, featA, featB;
+    // The mesh triangles this pair ruled out by distance when it was collided at the step's start, as a range
+    // of the world's triangle bounds; empty for other pairs and for pairs kept from the last step.
+    uint32_t boundsFirst, boundsCount;
     DPoint points[4];
 };
 
@@ -197,6 +200,10 @@ struct WorldInfo {
     // A body locked to a plane (global index), UINT32_MAX for none. Every such body of a world is locked to
     // the same plane, so this one's normal is the normal of every planar pair in the world.
     uint32_t planeBody;
+    // Mesh pairs: the parts after a pair's first (partFirst, partCap: contact records) and the triangles fast
+    // pairs ruled out (boundsFirst, boundsCap: triangle bounds). Zero capacity in worlds without meshes.
+    uint32_t partFirst, partCap;
+    uint32_t boundsFirst, boundsCap;
 };
 
 // Per-world results and lists of the current step.
@@ -223,6 +230,8 @@ struct WorldCounts {
     uint32_t sweptPairs;       // this step's continuous pass: pairs swept, and bodies moved back
     uint32_t impacts;
     uint32_t activePoints;     // contact points of the active list
+    uint32_t partCount;        // this step's extra mesh parts and triangle bounds used
+    uint32_t boundsCount;
     uint32_t colorStart[kColors + 1];
     uint32_t impactColorStart[kColors + 1];
     unsigned long long bodySteps;  // awake dynamic bodies summed over every step since the layout
