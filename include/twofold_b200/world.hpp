@@ -12,8 +12,9 @@
 // status (TF_OK or a negative TF_E* code) and statusMessage() its text.
 //
 // Differences a caller can see:
-//   - Geometry: spheres, boxes, prisms, hulls and half-spaces run on the device. Cylinders and meshes are
-//     refused by addShape (an invalid ShapeId, status TF_E_UNSUPPORTED), as are sensors. Bodies locked to
+//   - Geometry: spheres, boxes, prisms, hulls, half-spaces and meshes (on static and kinematic bodies) run on
+//     the device. Cylinders are refused by addShape (an invalid ShapeId, status TF_E_UNSUPPORTED), as are
+//     sensors and meshes on dynamic bodies. Bodies locked to
 //     a plane run when every such body of the world is locked to the same plane; createBody refuses a
 //     second plane (an invalid BodyId, status TF_E_UNSUPPORTED).
 //   - addForce/addTorque queue the force for the next step and act on awake bodies only (wake = false).
@@ -24,6 +25,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
+#include <map>
 #include <memory>
 #include <string>
 #include <variant>
@@ -126,7 +128,45 @@ struct Hull {
     int maxVertices = 64;
 };
 struct HalfSpace {};
-class TriangleMesh;
+// TriangleMesh (include/twofold/mesh.h:13-30): triangles indexed three to a face; vertices at the same position
+// are merged and degenerate triangles dropped when it is built. A World sends it to its device the first time
+// one of its shapes uses it.
+class TriangleMesh {
+public:
+    TriangleMesh(const std::vector<Vec3>& vertices, const std::vector<uint32_t>& indices) : inputIndices_(indices) {
+        for (const Vec3& v : vertices) { input_.insert(input_.end(), { v.x, v.y, v.z }); }
+        // The built mesh is read back from a handle that holds only it (no device is touched).
+        void* h = nullptr;
+        if (tf_world_create(nullptr, 1, 0, &h) != TF_OK) { return; }
+        int32_t id = -1;
+        int32_t counts[3] = { 0, 0, 0 };
+        if (tf_mesh_create(h, input_.data(), (int32_t)vertices.size(), indices.data(), (int32_t)indices.size(), &id) == TF_OK &&
+            tf_mesh_read(h, id, counts, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr) == TF_OK) {
+            std::vector<float> v(3 * (size_t)counts[0]);
+            indices_.resize(3 * (size_t)counts[1]);
+            tf_mesh_read(h, id, counts, v.data(), indices_.data(), nullptr, nullptr, nullptr, nullptr);
+            for (int32_t i = 0; i < counts[0]; ++i) { vertices_.push_back({ v[3 * i], v[3 * i + 1], v[3 * i + 2] }); }
+        }
+        tf_world_destroy(h);
+    }
+    TriangleMesh(const TriangleMesh&) = delete;
+    TriangleMesh& operator=(const TriangleMesh&) = delete;
+
+    const std::vector<Vec3>& vertices() const { return vertices_; }
+    // Three per triangle, in the mesh's own order.
+    const std::vector<uint32_t>& indices() const { return indices_; }
+    int triangleCount() const { return (int)(indices_.size() / 3); }
+
+    // What it was built from, for a World to build it again on its device.
+    const std::vector<float>& input() const { return input_; }
+    const std::vector<uint32_t>& inputIndices() const { return inputIndices_; }
+
+private:
+    std::vector<float> input_;
+    std::vector<uint32_t> inputIndices_;
+    std::vector<Vec3> vertices_;
+    std::vector<uint32_t> indices_;
+};
 struct Mesh {
     std::shared_ptr<const TriangleMesh> mesh;
 };
@@ -244,6 +284,8 @@ public:
             profile_ = o.profile_;
             bodies_ = std::move(o.bodies_);
             shapes_ = std::move(o.shapes_);
+            meshIds_ = std::move(o.meshIds_);
+            meshes_ = std::move(o.meshes_);
             forces_ = std::move(o.forces_);
             torques_ = std::move(o.torques_);
             forcesPending_ = o.forcesPending_;
@@ -344,6 +386,20 @@ public:
             c.geometry = TF_HALFSPACE;
         } else {
             c.geometry = TF_MESH;
+            const Mesh& m = std::get<Mesh>(d.geometry);
+            if (!m.mesh) { return {}; }
+            auto found = meshIds_.find(m.mesh.get());
+            if (found == meshIds_.end()) {
+                int32_t id = -1;
+                const std::vector<float>& v = m.mesh->input();
+                const std::vector<uint32_t>& i = m.mesh->inputIndices();
+                if (!note(tf_mesh_create(handle_, v.data(), (int32_t)(v.size() / 3), i.data(), (int32_t)i.size(), &id))) {
+                    return {};
+                }
+                found = meshIds_.emplace(m.mesh.get(), id).first;
+                meshes_.push_back(m.mesh);
+            }
+            c.mesh = found->second;
         }
         c.points = points.empty() ? nullptr : points.data();
         put3(c.position, d.position);
@@ -523,6 +579,8 @@ private:
     std::vector<BodyId> bodies_;
     std::vector<ShapeId> shapes_;
     std::vector<float> forces_, torques_;
+    std::map<const TriangleMesh*, int32_t> meshIds_;           // meshes this handle has built, by mesh
+    std::vector<std::shared_ptr<const TriangleMesh>> meshes_;  // kept alive while their ids are in use
     bool forcesPending_ = false;
     mutable int status_ = TF_OK;
 };

@@ -11,20 +11,21 @@ from twofold_b200 import abi
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_LIB = os.path.join(HERE, "_ref", "libtwofold_ref.so")
+# The same reference with sinf, cosf, atan2f and asinf correctly rounded (oracle/rounded_libm.cpp).
+ROUNDED_LIB = os.path.join(HERE, "_ref", "libtwofold_ref_rounded.so")
 
-_lib = None
-
-
-def available():
-    return os.path.exists(REF_LIB)
+_libs = {}
 
 
-def load():
-    global _lib
-    if _lib is None:
-        if not available():
-            raise RuntimeError(f"{REF_LIB} is missing; build it with `make -C oracle`")
-        lib = C.CDLL(REF_LIB)
+def available(path=REF_LIB):
+    return os.path.exists(path)
+
+
+def load(path=REF_LIB):
+    if path not in _libs:
+        if not available(path):
+            raise RuntimeError(f"{path} is missing; build it with `make -C oracle`")
+        lib = C.CDLL(path)
         P = C.c_void_p
         sig = {
             "ref_world_create": ([C.POINTER(abi.tf_settings)], P),
@@ -51,13 +52,13 @@ def load():
             f = getattr(lib, name)
             f.argtypes = args
             f.restype = res
-        _lib = lib
-    return _lib
+        _libs[path] = lib
+    return _libs[path]
 
 
-def mesh_create(vertices, indices):
+def mesh_create(vertices, indices, lib=REF_LIB):
     """A reference TriangleMesh (include/twofold/mesh.h:13-30); returns its id in the harness."""
-    lib = load()
+    lib = load(lib)
     v = np.ascontiguousarray(vertices, np.float32).reshape(-1, 3)
     i = np.ascontiguousarray(indices, np.uint32).reshape(-1)
     return lib.ref_mesh_create(v.ctypes.data, len(v), i.ctypes.data, len(i))
@@ -80,8 +81,8 @@ def mesh_read(mesh):
 class RefWorld:
     """One reference World built from a scenes.World."""
 
-    def __init__(self, world, settings=None, _handle=None):
-        self.lib = load()
+    def __init__(self, world, settings=None, _handle=None, lib=REF_LIB):
+        self.lib = load(lib)
         if _handle is not None:
             self.h = _handle
             return
@@ -89,7 +90,7 @@ class RefWorld:
         self.h = self.lib.ref_world_create(C.byref(s))
         shapes = world.shapes
         if getattr(world, "meshes", None):
-            ids = [mesh_create(v, i) for v, i in world.meshes]
+            ids = [mesh_create(v, i, lib) for v, i in world.meshes]
             shapes = world.shapes.copy()
             named = shapes["geometry"] == abi.TF_MESH
             shapes["mesh"][named] = np.asarray(ids, np.int32)[shapes["mesh"][named]]
@@ -99,11 +100,13 @@ class RefWorld:
             raise RuntimeError("reference scene build failed")
 
     def copy(self):
-        return RefWorld(None, _handle=self.lib.ref_world_copy(self.h))
+        r = RefWorld(None, _handle=self.lib.ref_world_copy(self.h))
+        r.lib = self.lib
+        return r
 
     def __del__(self):
-        if getattr(self, "h", None) and _lib is not None:
-            _lib.ref_world_destroy(self.h)
+        if getattr(self, "h", None) and getattr(self, "lib", None) is not None:
+            self.lib.ref_world_destroy(self.h)
             self.h = None
 
     def step(self, dt, n=1):

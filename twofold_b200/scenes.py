@@ -438,11 +438,13 @@ def terrain_mesh(cells=256, cell=0.5, seed=0):
     return vertices, indices
 
 
-def terrain(cells=256, cell=0.5, cols=32, levels=32, pitch=2.0, top=60.0, seed=0):
+def terrain(cells=256, cell=0.5, cols=32, levels=32, pitch=2.0, top=60.0, seed=0, flat_hulls=False, spin=0.0):
     """Bodies dropped on a static terrain mesh (terrain_mesh): cols x cols columns at `pitch` m, `levels`
     levels from y = 2 to `top`, positions jittered by U[-0.1, 0.1], cycling through a sphere of radius
     U[0.25, 0.75], a box of half extents U[0.2, 0.8] and a hull of 16 points uniform on a 0.5 m sphere (at most
-    16 vertices); density U[0.5, 2], uniformly random rotations, default sleeping."""
+    16 vertices); density U[0.5, 2], uniformly random rotations, default sleeping. With `flat_hulls` the hulls
+    are 12 points in a plane instead, thickened to slabs a few millimetres thin; with `spin` the terrain is a
+    kinematic body turning about y at that many rad/s."""
     rng = np.random.default_rng([seed, 2, 2])
     n = cols * cols * levels
     b, s = _bodies(n + 1), _shapes(n + 1)
@@ -472,6 +474,16 @@ def terrain(cells=256, cell=0.5, cols=32, levels=32, pitch=2.0, top=60.0, seed=0
             s["geometry"][i] = abi.TF_HULL
             s["max_vertices"][i] = 16
             _set_points(w, i, _sphere_points(rng, 16, 0.5))
+    if flat_hulls:
+        flat = np.random.default_rng([seed, 2, 3])
+        for i in range(1, n + 1):
+            if s["geometry"][i] == abi.TF_HULL:
+                pts = flat.uniform(-0.5, 0.5, size=(12, 3)).astype(F32)
+                pts[:, 1] = 0.0
+                _set_points(w, i, pts)
+    if spin:
+        b["type"][0] = abi.TF_KINEMATIC
+        b["angular_velocity"][0] = (0.0, spin, 0.0)
     return w
 
 
