@@ -146,6 +146,27 @@ def test_terrain_worlds_match_reference(seed):
     assert parts > 0  # some pair met the terrain with more than one group of triangles
 
 
+@needs_oracle
+@pytest.mark.parametrize("kind", ["planar", "terrain"])
+def test_big_worlds_match_reference(kind):
+    """Worlds of more than 1024 bodies find their body pairs with the sweep along x over the whole grid:
+    2048 planar bodies in a container, and 1296 spheres, boxes and hulls on a terrain mesh."""
+    if kind == "planar":
+        w = scenes.planar(n=2048, cols=32, spheres=16, sphere_height=(3.0, 8.0), seed=1)
+    else:
+        w = scenes.terrain(cells=48, cell=0.5, cols=12, levels=9, pitch=1.7, top=16.0, seed=1)
+    sc = scenes.Scene(kind, [w])
+    assert len(w.bodies) > 1024
+    b = Batch.from_scene(sc)
+    r = R.RefWorld(w, sc.settings)
+    for s in range(60):
+        b.step_checked(sc.dt)
+        r.step(sc.dt)
+        if s in (0, 1, 20, 40, 59):
+            _check_pairs_and_manifolds(b, 0, r, f"big {kind} step {s + 1}")
+            _compare_world(b, 0, r, f"big {kind} step {s + 1}")
+
+
 def _continuous_world(kind, seed):
     if kind == "hulls":
         return scenes.hulls(n=24, seed=seed, degenerate=True)

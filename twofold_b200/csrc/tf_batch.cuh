@@ -8,6 +8,16 @@
 
 namespace tfb {
 
+// A body of a big world as the sweep reads it, stored in bucket order: its pair-test record, where its
+// interval along x starts, and which body it is.
+struct SweepRec {
+    Vec3 lo, hi;
+    float grow;
+    uint32_t flags;
+    float start;
+    uint32_t body;
+};
+
 struct Batch {
     int nWorlds;
     const uint32_t* order;  // worlds, largest first; CTA k takes order[k], order[k + gridDim.x], ...
@@ -70,6 +80,21 @@ struct Batch {
 
     uint32_t* work;        // per launch of a step, the next world to hand out (zeroed when the step starts)
     uint32_t* rowScratch;  // per shape, the candidate key sort's row counts
+    uint32_t* rowLong;     // per shape, the sort's long rows
+    uint32_t* rowCount;    // per shape, the sort's counts within one long row
+
+    // Broadphase of worlds of more than kSweepBodies bodies: per body its interval along x (sweepLo, sweepHi)
+    // and, from bodyFirst, the bodies bucketed by the interval's start (sweepOrder); per world, from
+    // bodyFirst + world, the buckets' starts (sweepStart). bigWorlds lists those worlds, bigBodyStart the
+    // running total of their bodies.
+    float* sweepLo;
+    float* sweepHi;
+    uint32_t* sweepOrder;
+    struct SweepRec* sweepRecs;  // per body, from bodyFirst, in bucket order: what the pair test reads
+    uint32_t* sweepStart;
+    const uint32_t* bigWorlds;
+    const uint32_t* bigBodyStart;
+    uint32_t nBigWorlds;
 
     // Continuous collision: per shape, its bounds over the whole step and (from shapeFirst) the world's fast
     // shapes in shape order; per body, its earliest hit as (time bits << 32 | pair order), its group's

@@ -202,8 +202,12 @@ public:
     };
     std::map<int, std::unique_ptr<Snapshot>> snapshots;
     bool laidOut = false;
-    DevArray<uint32_t> dWork, dRowScratch;
+    DevArray<uint32_t> dWork, dRowScratch, dRowLong, dRowCount;
     DevArray<Vec3> dSweptLo, dSweptHi;
+    DevArray<float> dSweepLo, dSweepHi;
+    DevArray<uint32_t> dSweepOrder, dSweepStart, dBigWorlds, dBigBodyStart;
+    DevArray<SweepRec> dSweepRecs;
+    std::vector<uint32_t> bigWorlds, bigBodyStart;  // worlds of more than kSweepBodies bodies
     DevArray<uint32_t> dSweepList, dHitParent;
     DevArray<unsigned long long> dHitKey, dGroupKey;
     DevArray<uint2> dCandItems, dContactItems;
@@ -799,6 +803,23 @@ public:
         TF_ALLOC(dCandItems, ncand * kPairClasses);
         TF_ALLOC(dContactItems, ncon * (kPairClasses + 1));
         TF_ALLOC(dRowScratch, ns);
+        TF_ALLOC(dRowLong, ns);
+        TF_ALLOC(dRowCount, ns);
+        bigWorlds.clear();
+        bigBodyStart.assign(1, 0u);
+        for (uint32_t w : order) {
+            if (info[w].bodyCount > kSweepBodies) {
+                bigWorlds.push_back(w);
+                bigBodyStart.push_back(bigBodyStart.back() + info[w].bodyCount);
+            }
+        }
+        TF_ALLOC(dSweepLo, nb);
+        TF_ALLOC(dSweepHi, nb);
+        TF_ALLOC(dSweepOrder, nb);
+        TF_ALLOC(dSweepRecs, nb);
+        TF_ALLOC(dSweepStart, nb + nw);
+        TF_ALLOC(dBigWorlds, bigWorlds.size());
+        TF_ALLOC(dBigBodyStart, bigBodyStart.size());
         TF_ALLOC(dSweptLo, ns);
         TF_ALLOC(dSweptHi, ns);
         TF_ALLOC(dSweepList, ns);
@@ -831,6 +852,8 @@ public:
         if ((rc = up(dFaces.ptr, faces.data(), faces.size() * sizeof(DFace))) != TF_OK) { return rc; }
         if ((rc = up(dOffsets.ptr, offsets.data(), offsets.size() * sizeof(float))) != TF_OK) { return rc; }
         if ((rc = up(dEdges.ptr, edges.data(), edges.size() * sizeof(DEdge))) != TF_OK) { return rc; }
+        if ((rc = up(dBigWorlds.ptr, bigWorlds.data(), bigWorlds.size() * sizeof(uint32_t))) != TF_OK) { return rc; }
+        if ((rc = up(dBigBodyStart.ptr, bigBodyStart.data(), bigBodyStart.size() * sizeof(uint32_t))) != TF_OK) { return rc; }
         if ((rc = up(dMeshes.ptr, meshRecs.data(), meshRecs.size() * sizeof(DMesh))) != TF_OK) { return rc; }
         if ((rc = up(dMeshVerts.ptr, meshVerts.data(), meshVerts.size() * sizeof(Vec3))) != TF_OK) { return rc; }
         if ((rc = up(dMeshIndices.ptr, meshIndices.data(), meshIndices.size() * sizeof(uint32_t))) != TF_OK) { return rc; }
@@ -952,6 +975,16 @@ public:
         B.candItemStride = (uint32_t)(dCandItems.n / kPairClasses);
         B.contactItemStride = (uint32_t)(dContactItems.n / (kPairClasses + 1));
         B.rowScratch = dRowScratch.ptr;
+        B.rowLong = dRowLong.ptr;
+        B.rowCount = dRowCount.ptr;
+        B.sweepLo = dSweepLo.ptr;
+        B.sweepHi = dSweepHi.ptr;
+        B.sweepOrder = dSweepOrder.ptr;
+        B.sweepRecs = dSweepRecs.ptr;
+        B.sweepStart = dSweepStart.ptr;
+        B.bigWorlds = dBigWorlds.ptr;
+        B.bigBodyStart = dBigBodyStart.ptr;
+        B.nBigWorlds = (uint32_t)bigWorlds.size();
         B.sweptLo = dSweptLo.ptr;
         B.sweptHi = dSweptHi.ptr;
         B.sweepList = dSweepList.ptr;
@@ -975,7 +1008,13 @@ public:
         auto smem = [&](int k) { return (size_t)splits[k].smemBytes; };
         cudaMemsetAsync(dWork.ptr, 0, kSlotCount * sizeof(uint32_t), stream);
         if (marks) { cudaEventRecord(marks[0], stream); }
-        timed(0, rec, [&] { k_broadphase<<<grids[0], threads(0), smem(0), stream>>>(B, P, splits[0], serial); });
+        timed(0, rec, [&] {
+            k_broadphase<<<grids[0], threads(0), smem(0), stream>>>(B, P, splits[0], serial);
+            if (!bigWorlds.empty()) {
+                k_broad_pairs<<<smCount * 8, 256, 0, stream>>>(B, serial);
+                k_broad_finish<<<grids[0], threads(0), 0, stream>>>(B, splits[0], serial);
+            }
+        });
         if (marks) { cudaEventRecord(marks[1], stream); }
         timed(7, rec, [&] {
             k_collide<kClassSpheres><<<flatGrids[0], threads(7), 0, stream>>>(B, P, serial);
@@ -1009,7 +1048,7 @@ public:
         }
         timed(6, rec, [&] { k_finish<<<grids[6], threads(6), smem(6), stream>>>(B, P, splits[6], serial); });
         if (marks) { cudaEventRecord(marks[3], stream); }
-        launches += 5 + kPairClasses + P.substeps + (kPairClasses + 1) * (P.substeps - 1);
+        launches += 5 + kPairClasses + P.substeps + (kPairClasses + 1) * (P.substeps - 1) + (bigWorlds.empty() ? 0 : 2);
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) { return fail(TF_E_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e)); }
         return TF_OK;

@@ -37,7 +37,8 @@ enum WorkSlot : int {
     kSlotRefresh = 4,                            // + substep index
     kSlotSubstep = kSlotRefresh + kMaxSubsteps,  // + substep index
     kSlotFinish = kSlotSubstep + kMaxSubsteps,
-    kSlotCandItems = kSlotFinish + 1,                    // + pair class: candidate items of that class
+    kSlotBroadFinish = kSlotFinish + 1,                  // the big worlds' half of the broadphase
+    kSlotCandItems = kSlotBroadFinish + 1,               // + pair class: candidate items of that class
     kSlotFastItems = kSlotCandItems + kPairClasses,       // + pair class: fast contacts of that class; + kPairClasses:
                                                           // the other active contacts of refreshed worlds
     kSlotTape = kSlotFastItems + kPairClasses + 1,      // the recording kernel's world counter
@@ -300,9 +301,107 @@ __device__ __forceinline__ PairBody pairBodyOf(const Batch& B, uint32_t g) {
     return p;
 }
 
+// Worlds with more bodies than this find their body pairs with a sweep along x over the whole grid instead of
+// testing every pair on one group.
+constexpr uint32_t kSweepBodies = 1024;
+
+// Floats as unsigned keys in the same order, for atomicMin and atomicMax.
+__device__ __forceinline__ uint32_t orderedKey(float f) {
+    const uint32_t b = __float_as_uint(f);
+    return b ^ ((b >> 31) ? 0xffffffffu : 0x80000000u);
+}
+__device__ __forceinline__ float fromOrderedKey(uint32_t k) {
+    return __uint_as_float((k >> 31) ? (k ^ 0x80000000u) : ~k);
+}
+
+// How far a body's interval along x is widened beyond its grown bounds, so that two bodies the pair test
+// accepts always have overlapping intervals whatever the rounding of the test's sums: a millimetre plus a
+// millionth of the coordinate.
+__device__ __forceinline__ float sweepSlack(float x) { return 1e-3f + 1e-6f * fabsf(x); }
+
+// Buckets along x: a quarter as many as bodies, evenly over the range the intervals cover.
+struct SweepGrid {
+    float lo, scale;
+    uint32_t buckets;
+};
+
+__device__ __forceinline__ SweepGrid sweepGrid(const WorldInfo& wi, const WorldCounts& wc) {
+    SweepGrid s;
+    s.buckets = wi.bodyCount / 4 + 1;
+    s.lo = fromOrderedKey(wc.sweepMinKey);
+    const float hi = fromOrderedKey(wc.sweepMaxKey);
+    s.scale = hi > s.lo ? (float)s.buckets / (hi - s.lo) : 0.0f;
+    return s;
+}
+
+__device__ __forceinline__ uint32_t sweepBucket(const SweepGrid& s, float x) {
+    const float f = (x - s.lo) * s.scale;
+    if (!(f > 0.0f)) { return 0u; }
+    return f >= (float)(s.buckets - 1) ? s.buckets - 1 : (uint32_t)f;
+}
+
+// The first half of a big world's broadphase, after the growth: each live body's interval along x, their
+// range, and the bodies counted into buckets by where their intervals start. Bucket b then holds
+// sweepOrder[start[b - 1] .. start[b]), start[-1] being 0.
+__device__ void prepareSweep(const Batch& B, const Group& g, const WorldInfo& wi, WorldCounts& wc, uint32_t w) {
+    const uint32_t n = wi.bodyCount;
+    if (g.tid == 0) {
+        wc.sweepMinKey = 0xffffffffu;
+        wc.sweepMaxKey = 0u;
+        wc.candRaw = 0;
+    }
+    g.sync();
+    for (uint32_t i = g.tid; i < n; i += g.size) {
+        const uint32_t gb = wi.bodyFirst + i;
+        const DBody& b = B.bodies[gb];
+        float lo = FLT_MAX, hi = -FLT_MAX;
+        if (b.alive && b.hasBounds) {
+            const float gr = B.grow[gb];
+            lo = b.lo.x - gr - sweepSlack(b.lo.x);
+            hi = b.hi.x + gr + sweepSlack(b.hi.x);
+            atomicMin(&wc.sweepMinKey, orderedKey(lo));
+            atomicMax(&wc.sweepMaxKey, orderedKey(hi));
+        }
+        B.sweepLo[gb] = lo;
+        B.sweepHi[gb] = hi;
+    }
+    g.sync();
+    const SweepGrid grid = sweepGrid(wi, wc);
+    uint32_t* start = B.sweepStart + wi.bodyFirst + w;
+    for (uint32_t k = g.tid; k < grid.buckets; k += g.size) { start[k] = 0; }
+    g.sync();
+    for (uint32_t i = g.tid; i < n; i += g.size) { atomicAdd(&start[sweepBucket(grid, B.sweepLo[wi.bodyFirst + i])], 1u); }
+    g.sync();
+    uint32_t base = 0;
+    for (uint32_t first = 0; first < grid.buckets; first += g.size) {
+        const uint32_t k = first + g.tid;
+        const uint32_t v = k < grid.buckets ? start[k] : 0u;
+        uint32_t tot;
+        const uint32_t pre = groupScan(g, v, tot);
+        if (k < grid.buckets) { start[k] = base + pre; }
+        base += tot;
+    }
+    g.sync();
+    // Scattering advances each bucket's start to its end.
+    for (uint32_t i = g.tid; i < n; i += g.size) {
+        const uint32_t k = sweepBucket(grid, B.sweepLo[wi.bodyFirst + i]);
+        B.sweepOrder[wi.bodyFirst + atomicAdd(&start[k], 1u)] = i;
+    }
+    g.sync();
+    // The records in bucket order, so a scan over neighbouring buckets reads one contiguous run.
+    for (uint32_t q = g.tid; q < n; q += g.size) {
+        const uint32_t i = B.sweepOrder[wi.bodyFirst + q];
+        const PairBody p = pairBodyOf(B, wi.bodyFirst + i);
+        B.sweepRecs[wi.bodyFirst + q] = SweepRec{ p.lo, p.hi, p.grow, p.flags, B.sweepLo[wi.bodyFirst + i], i };
+    }
+    g.sync();
+}
+
 // Sorts the world's count keys (minShape << 32 | maxShape, at B.cand) ascending and removes repeats: a
 // counting sort by the first shape, then each row sorted on its own (rows are short), then compaction back
 // into B.cand. Returns the unique count.
+constexpr uint32_t kShortRow = 48;  // rows of keys at most this long are sorted by one thread
+
 __device__ uint32_t sortKeys(const Group& g, const Batch& B, const WorldInfo& wi, uint32_t count) {
     uint32_t* row = B.rowScratch + wi.shapeFirst;
     uint64_t* tmp = B.mergeKeyA + wi.contactFirst;
@@ -328,8 +427,10 @@ __device__ uint32_t sortKeys(const Group& g, const Batch& B, const WorldInfo& wi
         tmp[atomicAdd(&row[(uint32_t)(k >> 32)], 1u)] = k;
     }
     g.sync();
+    // Short rows: one thread each, by insertion.
     for (uint32_t r = g.tid; r < rows; r += g.size) {
         const uint32_t s = r > 0 ? row[r - 1] : 0u, e = row[r];
+        if (e - s > kShortRow) { continue; }
         for (uint32_t i = s + 1; i < e; ++i) {
             const uint64_t k = tmp[i];
             uint32_t j = i;
@@ -340,6 +441,38 @@ __device__ uint32_t sortKeys(const Group& g, const Batch& B, const WorldInfo& wi
             tmp[j] = k;
         }
     }
+    // Long rows (a half-space's or a mesh's pairs): one at a time by the whole group, counted by the second
+    // shape. Equal keys may land in any order among themselves, which leaves the same sequence.
+    uint32_t* longRows = B.rowLong + wi.shapeFirst;
+    const uint32_t nLong = groupCompact(
+        g, rows, [&](uint32_t r) { return row[r] - (r > 0 ? row[r - 1] : 0u) > kShortRow; },
+        [&](uint32_t r, uint32_t pos) { longRows[pos] = r; });
+    uint32_t* hist = B.rowCount + wi.shapeFirst;
+    for (uint32_t x = 0; x < nLong; ++x) {
+        const uint32_t r = longRows[x];
+        const uint32_t s = r > 0 ? row[r - 1] : 0u, e = row[r];
+        for (uint32_t c = g.tid; c < rows; c += g.size) { hist[c] = 0; }
+        g.sync();
+        for (uint32_t i = s + g.tid; i < e; i += g.size) { atomicAdd(&hist[(uint32_t)tmp[i]], 1u); }
+        g.sync();
+        uint32_t base = s;
+        for (uint32_t first = 0; first < rows; first += g.size) {
+            const uint32_t c = first + g.tid;
+            const uint32_t v = c < rows ? hist[c] : 0u;
+            uint32_t tot;
+            const uint32_t pre = groupScan(g, v, tot);
+            if (c < rows) { hist[c] = base + pre; }
+            base += tot;
+        }
+        g.sync();
+        for (uint32_t i = s + g.tid; i < e; i += g.size) {
+            const uint64_t k = tmp[i];
+            keys[atomicAdd(&hist[(uint32_t)k], 1u)] = k;
+        }
+        g.sync();
+        for (uint32_t i = s + g.tid; i < e; i += g.size) { tmp[i] = keys[i]; }
+        g.sync();
+    }
     g.sync();
     return groupCompact(
         g, count, [&](uint32_t i) { return i == 0 || tmp[i] != tmp[i - 1]; }, [&](uint32_t i, uint32_t pos) { keys[pos] = tmp[i]; });
@@ -348,6 +481,9 @@ __device__ uint32_t sortKeys(const Group& g, const Batch& B, const WorldInfo& wi
 // Body pairs whose grown bounds overlap, then their shapes (src/world.cpp:788-842), and half-space pairs
 // (:844-867); the keys are sorted and made unique (:868-869). A warp of the group takes one body and its
 // lanes the bodies after it. Bodies are staged in the group's shared slice when at most stageN of them.
+__device__ void finishCandidates(const Batch& B, const Group& g, const WorldInfo& wi, WorldCounts& wc, uint32_t w,
+                                 uint32_t total, int serial, uint32_t* cls, uint32_t* classBase);
+
 __global__ void __launch_bounds__(kMaxBlock) k_broadphase(const __grid_constant__ Batch B, const __grid_constant__ StepParams P, const __grid_constant__ Split sp, int serial) {
     extern __shared__ __align__(16) unsigned char s_raw[];
     __shared__ uint32_t s_count[kMaxGroups];
@@ -380,6 +516,10 @@ __global__ void __launch_bounds__(kMaxBlock) k_broadphase(const __grid_constant_
             }
         }
         g.sync();
+        if (n > kSweepBodies) {
+            prepareSweep(B, g, wi, wc, w);
+            return;
+        }
         uint32_t* count = &s_count[g.id];
         for (uint32_t a = g.warp; a + 1 < n; a += g.warps) {
             const PairBody A = useStage ? staged[a] : pairBodyOf(B, wi.bodyFirst + a);
@@ -401,7 +541,16 @@ __global__ void __launch_bounds__(kMaxBlock) k_broadphase(const __grid_constant_
             for (uint32_t b = g.tid; b < n; b += g.size) { pairPlane(B, wi, gp, wi.bodyFirst + b, count); }
         }
         g.sync();
-        const uint32_t total = *count;
+        finishCandidates(B, g, wi, wc, w, *count, serial, s_class[g.id], s_classBase[g.id]);
+    });
+}
+
+// The end of a world's broadphase: the raw keys sorted and made unique (src/world.cpp:868-869), then the
+// pairs join the flat list of their class: counted per class, a block of each list reserved for the
+// world, then scattered into it. A list that did not fit stops this step, and the host grows it.
+__device__ void finishCandidates(const Batch& B, const Group& g, const WorldInfo& wi, WorldCounts& wc, uint32_t w,
+                                 uint32_t total, int serial, uint32_t* cls, uint32_t* classBase) {
+    {
         if (total > wi.candCap) {
             // The list did not fit: this step stops here and the host grows the world's lists.
             if (g.tid == 0) {
@@ -419,9 +568,6 @@ __global__ void __launch_bounds__(kMaxBlock) k_broadphase(const __grid_constant_
             wc.partCount = 0;
             wc.boundsCount = 0;
         }
-        // The pairs join the flat list of their class: counted per class, a block of each list reserved for
-        // the world, then scattered into it.
-        uint32_t* cls = s_class[g.id];
         if (g.tid < kPairClasses) { cls[g.tid] = 0; }
         g.sync();
         auto classOf = [&](uint32_t i) {
@@ -431,16 +577,75 @@ __global__ void __launch_bounds__(kMaxBlock) k_broadphase(const __grid_constant_
         for (uint32_t i = g.tid; i < unique; i += g.size) { atomicAdd(&cls[classOf(i)], 1u); }
         g.sync();
         if (g.tid < kPairClasses) {
-            s_classBase[g.id][g.tid] = atomicAdd(B.work + kSlotCandItems + g.tid, cls[g.tid]);
+            classBase[g.tid] = atomicAdd(B.work + kSlotCandItems + g.tid, cls[g.tid]);
             cls[g.tid] = 0;
         }
         g.sync();
         for (uint32_t i = g.tid; i < unique; i += g.size) {
             const int c = classOf(i);
-            const uint32_t pos = s_classBase[g.id][c] + atomicAdd(&cls[c], 1u);
+            const uint32_t pos = classBase[c] + atomicAdd(&cls[c], 1u);
             B.candItems[(size_t)c * B.candItemStride + pos] = make_uint2(w, i);
         }
         g.sync();
+    }
+}
+
+// The pair half of a big world's broadphase: each body takes the bodies whose intervals along x start
+// within its own interval (the one starting first takes a pair, so each pair is taken once) and applies the
+// same pair test as the small worlds, in the pair's lower-body-first order. A warp per body, its lanes
+// across the contiguous run of records in the buckets its interval covers, over every big world.
+__global__ void __launch_bounds__(256) k_broad_pairs(const __grid_constant__ Batch B, int serial) {
+    if (stepAborted(B, serial)) { return; }
+    const uint32_t total = B.bigBodyStart[B.nBigWorlds];
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t item = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; item < total; item += warps) {
+        uint32_t k = 0;
+        while (k + 1 < B.nBigWorlds && B.bigBodyStart[k + 1] <= item) { ++k; }
+        const uint32_t w = B.bigWorlds[k];
+        const WorldInfo wi = B.info[w];
+        WorldCounts& wc = B.counts[w];
+        const SweepRec* recs = B.sweepRecs + wi.bodyFirst;
+        const uint32_t* start = B.sweepStart + wi.bodyFirst + w;
+        const SweepRec ri = recs[item - B.bigBodyStart[k]];
+        if (!(ri.flags & kBodyLive)) { continue; }
+        const float lo = ri.start, hi = B.sweepHi[wi.bodyFirst + ri.body];
+        const SweepGrid grid = sweepGrid(wi, wc);
+        const uint32_t b0 = sweepBucket(grid, lo), b1 = sweepBucket(grid, hi);
+        const uint32_t q0 = b0 ? start[b0 - 1] : 0u, q1 = start[b1];
+        for (uint32_t q = q0 + lane; q < q1; q += 32) {
+            const SweepRec rj = recs[q];
+            const uint32_t i = ri.body, j = rj.body;
+            if (j == i || !(rj.start > lo || (rj.start == lo && j > i)) || rj.start > hi) { continue; }
+            const SweepRec& A = i < j ? ri : rj;
+            const SweepRec& Bb = i < j ? rj : ri;
+            if (!(A.flags & kBodyLive) || !(Bb.flags & kBodyLive)) { continue; }
+            if (!((A.flags | Bb.flags) & kBodyDynamic)) { continue; }
+            if (!((A.flags | Bb.flags) & kBodyMoving)) { continue; }
+            const float gg = A.grow + Bb.grow;
+            const Vec3 reach{ gg, gg, gg };
+            if (!boxesOverlap(A.lo - reach, A.hi + reach, Bb.lo, Bb.hi)) { continue; }
+            pairShapes(B, wi, B.bodies[wi.bodyFirst + A.body], B.bodies[wi.bodyFirst + Bb.body], A.grow, Bb.grow, A.lo,
+                       A.hi, Bb.lo, Bb.hi, reach, &wc.candRaw);
+        }
+    }
+}
+
+// The rest of a big world's broadphase: half-space pairs, then the keys sorted and sent to their lists.
+__global__ void __launch_bounds__(kMaxBlock) k_broad_finish(const __grid_constant__ Batch B, const __grid_constant__ Split sp, int serial) {
+    __shared__ uint32_t s_class[kMaxGroups][kPairClasses], s_classBase[kMaxGroups][kPairClasses];
+    if (stepAborted(B, serial)) { return; }
+    forWorlds(B, kSlotBroadFinish, sp, nullptr, [&](const Group& g, uint32_t w, unsigned char*, const StageSizes&) {
+        const WorldInfo wi = B.info[w];
+        if (wi.bodyCount <= kSweepBodies) { return; }
+        WorldCounts& wc = B.counts[w];
+        for (uint32_t pl = 0; pl < wi.planeCount; ++pl) {
+            const uint32_t gp = B.planeList[wi.planeFirst + pl];
+            for (uint32_t b = g.tid; b < wi.bodyCount; b += g.size) { pairPlane(B, wi, gp, wi.bodyFirst + b, &wc.candRaw); }
+        }
+        g.sync();
+        const uint32_t total = *(volatile uint32_t*)&wc.candRaw;
+        finishCandidates(B, g, wi, wc, w, total, serial, s_class[g.id], s_classBase[g.id]);
     });
 }
 

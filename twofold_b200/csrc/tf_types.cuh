@@ -232,6 +232,10 @@ struct WorldCounts {
     uint32_t activePoints;     // contact points of the active list
     uint32_t partCount;        // this step's extra mesh parts and triangle bounds used
     uint32_t boundsCount;
+    // Worlds of more than kSweepBodies bodies: raw pair count of this step's sweep, and the range of the
+    // bodies' intervals along x as order-preserving keys.
+    uint32_t candRaw;
+    uint32_t sweepMinKey, sweepMaxKey;
     uint32_t colorStart[kColors + 1];
     uint32_t impactColorStart[kColors + 1];
     unsigned long long bodySteps;  // awake dynamic bodies summed over every step since the layout
