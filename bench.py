@@ -255,6 +255,42 @@ def plain_rate(sc, args, device):
                       f"{args.warmup + 1}-{args.warmup + args.steps}"}
 
 
+def single_worlds(device, warmup=20, steps=40):
+    """The plain path on the single-world configurations (box pyramid, terrain, planar pile): device ms per
+    step through the C ABI (a CUDA graph per step) over steps warmup+1..warmup+steps, beside the reference
+    stepping the same world the same steps on one host core. A reported comparison, not the headline."""
+    from twofold_b200 import scenes
+    from twofold_b200.world import Batch
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import reference as R
+
+    out = {}
+    for name, make in (("box_pyramid_210", scenes.config1), ("terrain_32768", scenes.config2),
+                       ("planar_16384", scenes.config3)):
+        sc = make()
+        one = Batch(sc.worlds, sc.settings, device=device)
+        for _ in range(warmup):
+            one.step_checked(sc.dt, 1, graph=True)
+        ms = 0.0
+        b0 = one.body_steps()
+        for _ in range(steps):
+            one.step_checked(sc.dt, 1, graph=True)
+            ms += one.elapsed_ms()
+        body_steps = one.body_steps() - b0
+        one.close()
+        entry = {"gpu_ms_per_step": ms / steps, "body_steps_per_s": body_steps / (ms / 1e3)}
+        if R.available():
+            r = R.RefWorld(sc.worlds[0], sc.settings)
+            r.step(sc.dt, warmup)
+            t0 = time.perf_counter()
+            r.step(sc.dt, steps)
+            el = time.perf_counter() - t0
+            entry.update({"reference_ms_per_step": 1e3 * el / steps, "reference_cores": 1})
+        entry["steps"] = f"{warmup + 1}-{warmup + steps}"
+        out[name] = entry
+    return out
+
+
 def adjoint_cost(device, n_worlds=1024, steps=120):
     """The differentiable impact workload: record 120 steps of 1024 worlds, run the model forward and the adjoint
     backward in float; device times of both, and of the pipeline's own 120 steps of the same worlds."""
@@ -372,6 +408,9 @@ def run_b200(args, dist):
     adjoint = None
     if dist.rank == 0 and not args.no_extras:
         adjoint = adjoint_cost(dist.local_rank)
+    singles = None
+    if dist.rank == 0 and n == 1 and not args.no_extras:
+        singles = single_worlds(dist.local_rank)
 
     cpu = None
     if dist.rank == 0 and n == 1 and not args.no_cpu_baseline:
@@ -409,6 +448,7 @@ def run_b200(args, dist):
             "cpu_baseline": cpu,
             "plain_one_by_one": plain,
             "adjoint": adjoint,
+            "single_world_configs": singles,
         }
         print(json.dumps(line))
 

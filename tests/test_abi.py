@@ -63,15 +63,23 @@ def test_step_ignores_a_time_that_is_not_finite():
         assert np.array_equal(before[k], after[k])
 
 
-def test_unsupported_geometry_is_refused():
+def test_unsupported_shapes_are_refused():
+    """Sensors and meshes on dynamic bodies are not run by this build; an unknown geometry is invalid."""
     lib = abi.load()
     h = C.c_void_p()
     abi.check(lib.tf_world_create(None, 1, 0, C.byref(h)))
     bid = abi.tf_id()
     abi.check(lib.tf_body_create(h, 0, C.byref(abi.body_desc()), C.byref(bid)))
     sid = abi.tf_id()
-    rc = lib.tf_shape_add(h, 0, bid, C.byref(abi.shape_desc(geometry=abi.TF_CYLINDER)), C.byref(sid))
-    assert rc == -6  # TF_E_UNSUPPORTED
+    assert lib.tf_shape_add(h, 0, bid, C.byref(abi.shape_desc(sensor=True)), C.byref(sid)) == abi.TF_E_UNSUPPORTED
+    v = np.array([[0, 0, 0], [1, 0, 0], [0, 0, 1]], np.float32)
+    i = np.array([0, 2, 1], np.uint32)
+    mesh = C.c_int32(-1)
+    abi.check(lib.tf_mesh_create(h, v.ctypes.data, 3, i.ctypes.data, 3, C.byref(mesh)))
+    assert lib.tf_shape_add(h, 0, bid, C.byref(abi.shape_desc(geometry=abi.TF_MESH, mesh=mesh.value)),
+                            C.byref(sid)) == abi.TF_E_UNSUPPORTED
+    assert lib.tf_shape_add(h, 0, bid, C.byref(abi.shape_desc(geometry=99)), C.byref(sid)) == abi.TF_E_INVALID
+    abi.check(lib.tf_shape_add(h, 0, bid, C.byref(abi.shape_desc(geometry=abi.TF_CYLINDER)), C.byref(sid)))
     lib.tf_world_destroy(h)
 
 

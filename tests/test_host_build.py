@@ -100,3 +100,12 @@ def test_terrain_scene_builds_like_the_reference():
     mesh), and the mesh shape's own bounds."""
     sc = scenes.Scene("terrain", [scenes.terrain(cells=16, cols=4, levels=3, pitch=1.6, top=8.0)])
     _check_masses(sc)
+
+
+@pytest.mark.parametrize("seed", range(2))
+def test_cylinders_are_built_like_the_reference(seed):
+    """Cylinder cleaning (thin discs and rods thickened), masses and inertias, among boxes, spheres and hulls."""
+    w = scenes.cylinders(24, seed)
+    w.shapes["half_height"][3] = 1e-9                      # a flat disc: thickened to a slab
+    w.shapes["radius"][6] = 0.0                            # a line: thickened
+    _check_masses(scenes.Scene("cylinders", [w]))

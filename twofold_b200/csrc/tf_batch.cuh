@@ -1,7 +1,7 @@
 // Every device array of a batch, passed by value to each kernel.
 #pragma once
 
-#include "tf_collide.cuh"
+#include "tf_dispatch.cuh"
 #include "tf_mesh_collide.cuh"
 #include "tf_solver.cuh"
 #include "tf_types.cuh"

@@ -112,6 +112,16 @@ TF_HD float relativeTravel(const DBody& a, const DBody& b, float dt) {
     return (length(b.v - a.v) + length(a.w) * a.extent + length(b.w) * b.extent) * dt;
 }
 
+// src/shape.cpp:134-140: the half extents of a cylinder turned so its axis is `axis`.
+TF_HD Vec3 cylinderReach(const Vec3& axis, float radius, float halfHeight) {
+    Vec3 r;
+    for (int i = 0; i < 3; ++i) {
+        const float a = comp(axis, i);
+        setComp(r, i, halfHeight * fabsf(a) + radius * sqrtf(maxf(1.0f - a * a, 0.0f)));
+    }
+    return r;
+}
+
 // World bounds of a shape at transform xf (src/shape.cpp:227-295). Boxes and prisms take the reach of their
 // outline and depth; hulls their vertices.
 TF_HD void shapeBounds(const DShape& s, const PolyTables& pt, const Transform& xf, Vec3& lo, Vec3& hi) {
@@ -123,6 +133,12 @@ TF_HD void shapeBounds(const DShape& s, const PolyTables& pt, const Transform& x
     }
     if (s.kind == kSphere) {
         const Vec3 r{ s.radius, s.radius, s.radius };
+        lo = xf.p - r;
+        hi = xf.p + r;
+        return;
+    }
+    if (s.kind == kCylinder) {
+        const Vec3 r = cylinderReach(rotate(xf.q, Vec3{ 0, 0, 1 }), s.radius, s.halfHeight);
         lo = xf.p - r;
         hi = xf.p + r;
         return;

@@ -281,7 +281,8 @@ struct HostShape {
 // false for geometry this build does not make.
 inline bool buildShapeGeometry(HostShape& s, int geometry, float radius, const Vec3& halfExtents,
                                const float* points = nullptr, int pointCount = 0, float zMin = -0.5f, float zMax = 0.5f,
-                               int maxVertices = 64, const HostMesh* mesh = nullptr, int meshId = -1) {
+                               int maxVertices = 64, const HostMesh* mesh = nullptr, int meshId = -1,
+                               float halfHeight = 0.5f) {
     DShape& d = s.d;
     d.radius = 0.0f;
     d.halfHeight = 0.0f;
@@ -298,6 +299,17 @@ inline bool buildShapeGeometry(HostShape& s, int geometry, float radius, const V
         d.halfExtents = solidBox(halfExtents);
         s.poly = makeBox(d.halfExtents);
         s.hasPoly = true;
+    } else if (geometry == 2 /* TF_CYLINDER */) {
+        // solidCylinder (src/shape.cpp:88-95).
+        d.kind = kCylinder;
+        float r = solidSize(radius), h = solidSize(halfHeight);
+        const float size = 2.0f * std::sqrt(r * r + h * h);
+        const float limit = thinLimit(size, r + h);
+        if (2.0f * r <= limit) { r = slabFor(size, limit); }
+        if (2.0f * h <= limit) { h = slabFor(size, limit); }
+        d.radius = r;
+        d.halfHeight = h;
+        d.extent = std::sqrt(r * r + h * h);
     } else if (geometry == 3 /* TF_PRISM */) {
         d.kind = kConvex;
         std::vector<Vec2> polygon;
@@ -353,6 +365,11 @@ inline MassProps shapeMass(const HostShape& s) {
         mp.mass = s.density * (4.0f / 3.0f) * kPiF * r * r * r;
         const float i = 0.4f * mp.mass * r * r;
         mp.inertia = mdiag({ i, i, i });
+    } else if (d.kind == kCylinder) {
+        const float r = d.radius, h = 2.0f * d.halfHeight;
+        mp.mass = s.density * kPiF * r * r * h;
+        const float side = mp.mass * (3.0f * r * r + h * h) / 12.0f;
+        mp.inertia = mdiag({ side, side, 0.5f * mp.mass * r * r });
     } else if (d.kind == kConvex) {
         mp = polyhedronMass(s.poly, s.density);
     } else {

@@ -620,12 +620,24 @@ TF_HD bool boxQueries(const BoxTopology& topology, const Vec3& halfA, const Vec3
 // ---------------------------------------------------------------------------------------------------------
 // GJK (src/distance.cpp): support points in float, simplex weights in double.
 
+// A shape as GJK sees it (src/internal.h:203-211): points (with a rounding radius), a half-space, or a
+// cylinder of radius rim and half height halfHeight about its local z.
 struct Convex {
     const Vec3* points;
     int count;
     float radius;
     bool halfSpace;
+    bool cylinder;
+    float rim, halfHeight;
 };
+
+// src/shape.cpp:142-147: the point of a cylinder farthest along d, in its own frame.
+TF_HD Vec3 cylinderSupport(float radius, float halfHeight, const Vec3& d) {
+    const float z = d.z < 0.0f ? -halfHeight : halfHeight;
+    const float side = sqrtf(d.x * d.x + d.y * d.y);
+    if (side == 0.0f) { return Vec3{ 0.0f, 0.0f, z }; }
+    return Vec3{ d.x * (radius / side), d.y * (radius / side), z };
+}
 
 struct GVertex {
     Vec3 a, b, w;
@@ -653,6 +665,7 @@ struct Simplex {
 
 TF_HD Vec3 gjkSupport(const Convex& c, const Transform& xf, const Vec3& d) {
     const Vec3 local = unrotate(xf.q, d);
+    if (c.cylinder) { return apply(xf, cylinderSupport(c.rim, c.halfHeight, local)); }
     int best = 0;
     float most = dot(c.points[0], local);
     for (int i = 1; i < c.count; ++i) {
@@ -790,10 +803,15 @@ enum Verdict { kOpen = 0, kWithin = 1, kBeyond = 2 };
 
 // GJK from the first points (src/distance.cpp:193-245).
 TF_HD int gjkSearch(const Convex& a, const Transform& xa, const Convex& b, const Transform& xb, float limit, Simplex& s,
-                    Vec3& v, bool& overlap) {
+                    Vec3& v, bool& overlap, const Vec3& start = Vec3{ 0.0f, 0.0f, 0.0f }) {
     const bool bounded = limit >= 0.0f;
-    s.v[0].a = apply(xa, a.points[0]);
-    s.v[0].b = apply(xb, b.points[0]);
+    if (lengthSquared(start) > 0.0f) {
+        s.v[0].a = gjkSupport(a, xa, start);
+        s.v[0].b = gjkSupport(b, xb, -start);
+    } else {
+        s.v[0].a = a.cylinder ? apply(xa, Vec3{ a.rim, 0.0f, a.halfHeight }) : apply(xa, a.points[0]);
+        s.v[0].b = b.cylinder ? apply(xb, Vec3{ b.rim, 0.0f, b.halfHeight }) : apply(xb, b.points[0]);
+    }
     s.v[0].w = s.v[0].b - s.v[0].a;
     s.u[0] = 1.0;
     s.count = 1;
@@ -845,11 +863,20 @@ TF_HD bool apart(const Convex& a, const Transform& xa, const Convex& b, const Tr
 // ---------------------------------------------------------------------------------------------------------
 
 // Everything a pair collision needs from the batch.
+// A cylinder's cap as 24 points, and the turn between neighbouring points (src/collide3d.cpp:720-737,
+// 1157-1168): cosines and sines taken on the host with the C library, as the reference takes them.
+constexpr int kCapPoints = 24;
+struct CapCircle {
+    float cos[kCapPoints], sin[kCapPoints];
+    float turnCos, turnSin;
+};
+
 struct CollideCtx {
     PolyTables pt;
     MeshTables mt;
     BoxTopology boxes;
     Tolerances tol;
+    CapCircle cap;
 };
 
 TF_HD Convex convexOf(const CollideCtx& cx, const DShape& s) {
@@ -858,6 +885,9 @@ TF_HD Convex convexOf(const CollideCtx& cx, const DShape& s) {
     c.radius = 0.0f;
     c.points = nullptr;
     c.count = 0;
+    c.cylinder = s.kind == kCylinder;
+    c.rim = c.cylinder ? s.radius : 0.0f;
+    c.halfHeight = c.cylinder ? s.halfHeight : 0.0f;
     if (s.kind == kSphere) {
         c.points = &s.centroid;
         c.count = 1;
@@ -1003,100 +1033,6 @@ TF_HD void collideSpheres(const Vec3& ca, float ra, const Vec3& cb, float rb, fl
     m.normal = n;
     m.points[0] = { ca + n * (ra + 0.5f * sep), sep, 0.0f };
     m.count = 1;
-}
-
-// Normal out of the half-space (src/collide3d.cpp:1309-1345).
-TF_HD void collideHalfSpace(const CollideCtx& cx, const Transform& xh, const DShape& other, const Transform& xo,
-                            float margin, float band, const Motion& motion, Manifold& m) {
-    const Vec3 n = rotate(xh.q, Vec3{ 0, 0, 1 });
-    const float offset = dot(n, xh.p);
-    if (other.kind == kSphere) {
-        const float d = dot(n, xo.p) - offset;
-        const float sep = d - other.radius;
-        if (sep > margin) { return; }
-        m.normal = n;
-        m.points[0] = { xo.p - n * (0.5f * (d + other.radius)), sep, 0.0f };
-        m.count = 1;
-        return;
-    }
-    const Vec3 localN = unrotate(xo.q, n);
-    const float localOffset = offset - dot(n, xo.p);
-    const DPoly& P = cx.pt.polys[other.poly];
-    MPoint pts[kMaxReduce];
-    int np = 0;
-    for (int k = 0; k < P.vCount && np < kMaxReduce; ++k) {
-        const Vec3 v = cx.pt.verts[P.vFirst + k];
-        const float s = dot(localN, v) - localOffset;
-        if (s > margin) { continue; }
-        const Vec3 w = apply(xo, v);
-        pts[np++] = { w - n * (0.5f * s), s, motion.predict(w, n, s) };
-    }
-    reduceManifold(pts, np, n, band, m, 0.0f, motion.fast);
-}
-
-// Pair classes, by shape kinds. A kernel instantiated for one class compiles only that class's collision
-// code; kClassAny compiles every path.
-// kClassPlanar holds the pairs solved in a plane (decided by their bodies, not their shapes); its kernels
-// fall back to every 3D path for profiles the plane does not cut.
-// kClassMesh holds the pairs with a triangle mesh, which may make several contacts.
-enum PairClass : int {
-    kClassAny = -1, kClassSpheres = 0, kClassSpherePoly = 1, kClassPlane = 2, kClassConvex = 3, kClassPlanar = 4,
-    kClassMesh = 5
-};
-constexpr int kPairClasses = 6;
-
-TF_HD int pairClass(uint32_t ka, uint32_t kb) {
-    if (ka == kHalfSpace || kb == kHalfSpace) { return kClassPlane; }
-    if (ka == kSphere && kb == kSphere) { return kClassSpheres; }
-    if (ka == kSphere || kb == kSphere) { return kClassSpherePoly; }
-    return kClassConvex;
-}
-
-// Shape-kind dispatch (src/collide3d.cpp:1778-1811). Returns false for a pair this build cannot collide
-// (cylinders and meshes), leaving m empty. For a class other than kClassAny the pair must be of that class.
-template <int Cls = kClassAny>
-TF_HD bool collideShapes(const CollideCtx& cx, const DShape& a, const Transform& xa, const DShape& b,
-                         const Transform& xb, float margin, const Motion& motion, Manifold& m, int reuseKind,
-                         int reuseA, int reuseB) {
-    m.count = 0;
-    m.featKind = kFeatNone;
-    m.featA = m.featB = -1;
-    m.normal = zero3();
-    const uint32_t ka = a.kind, kb = b.kind;
-    if (ka == kHalfSpace && kb == kHalfSpace) { return true; }
-    if (ka == kMesh || kb == kMesh || ka == kCylinder || kb == kCylinder) { return false; }
-    if constexpr (Cls == kClassAny || Cls == kClassPlane) {
-        if (ka == kHalfSpace) {
-            collideHalfSpace(cx, xa, b, xb, margin, cx.tol.linearSlop, motion, m);
-            return true;
-        }
-        if (kb == kHalfSpace) {
-            collideHalfSpace(cx, xb, a, xa, margin, cx.tol.linearSlop, motion.swapped(), m);
-            m.normal = -m.normal;
-            return true;
-        }
-    }
-    if constexpr (Cls == kClassAny || Cls == kClassSpheres) {
-        if (ka == kSphere && kb == kSphere) {
-            collideSpheres(xa.p, a.radius, xb.p, b.radius, margin, m);
-            return true;
-        }
-    }
-    if constexpr (Cls == kClassAny || Cls == kClassSpherePoly) {
-        if (ka == kSphere) {
-            collideSpherePoly(cx, b, xb, xa.p, a.radius, margin, m);
-            m.normal = -m.normal;
-            return true;
-        }
-        if (kb == kSphere) {
-            collideSpherePoly(cx, a, xa, xb.p, b.radius, margin, m);
-            return true;
-        }
-    }
-    if constexpr (Cls == kClassAny || Cls == kClassConvex) {
-        collideConvex(cx, a, xa, b, xb, margin, motion, m, reuseKind, reuseA, reuseB);
-    }
-    return true;
 }
 
 }

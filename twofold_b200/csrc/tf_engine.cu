@@ -502,9 +502,8 @@ public:
             mesh = &meshes[(size_t)d->mesh];
         }
         if (!buildShapeGeometry(s, d->geometry, d->radius, v3of(d->half_extents), d->points, d->point_count, d->z_min,
-                                d->z_max, d->max_vertices, mesh, d->mesh)) {
-            return fail(TF_E_UNSUPPORTED,
-                        "addShape: only spheres, boxes, prisms, hulls, half-spaces and meshes are run by this build");
+                                d->z_max, d->max_vertices, mesh, d->mesh, d->half_height)) {
+            return fail(TF_E_INVALID, "addShape: unknown geometry");
         }
         if (s.d.sensor) { return fail(TF_E_UNSUPPORTED, "addShape: sensors are not run by this build"); }
         if (s.d.kind == kHalfSpace && hb->d.type != kStatic) {
@@ -939,6 +938,18 @@ public:
         B.planeList = dPlaneList.ptr;
         B.cx.pt = { dPolys.ptr, dVerts.ptr, dIndices.ptr, dFaces.ptr, dNormals.ptr, dOffsets.ptr, dEdges.ptr, dArcs.ptr };
         B.cx.boxes = boxTopology;
+        // The cap circle and the turn between its points, from the host's C library as the reference takes
+        // them (src/collide3d.cpp:724-731, 1161-1164).
+        for (int k = 0; k < kCapPoints; ++k) {
+            const float t = 2.0f * 3.14159265358979f * (float)k / (float)kCapPoints;
+            B.cx.cap.cos[k] = std::cos(t);
+            B.cx.cap.sin[k] = std::sin(t);
+        }
+        {
+            const float t = 2.0f * 3.14159265358979f / (float)kCapPoints;
+            B.cx.cap.turnCos = std::cos(t);
+            B.cx.cap.turnSin = std::sin(t);
+        }
         B.cx.mt = { dMeshes.ptr, dMeshVerts.ptr, dMeshIndices.ptr, dMeshNormals.ptr, dMeshEdges.ptr, dMeshNodes.ptr };
         B.grow = dGrow.ptr;
         B.bodyColors = dBodyColors.ptr;

@@ -2045,10 +2045,6 @@ __device__ void sweepWorld(const Batch& B, const StepParams& P, const Group& g, 
         if (!boxesOverlap(B.sweptLo[sf + fi], B.sweptHi[sf + fi], B.sweptLo[sf + oi], B.sweptHi[sf + oi])) { continue; }
         if (!(f.category & o.mask) || !(o.category & f.mask)) { continue; }
         atomicAdd(pairs, 1u);
-        if (o.kind == kCylinder || f.kind == kCylinder) {
-            atomicOr(&wc.flags, kDevUnsupported);
-            continue;
-        }
         const DBody& bo = B.bodies[o.body];
         float t = 1.0f;
         bool ok = true;

@@ -4,7 +4,7 @@
 // triangle manifolds whose normals agree within kSameNormal merge into one manifold per group.
 #pragma once
 
-#include "tf_collide.cuh"
+#include "tf_round.cuh"
 
 namespace tfb {
 
@@ -32,47 +32,6 @@ struct MeshBounds {
     int knownCount;
     float moved;
 };
-
-// The point of the triangle closest to p, and its feature: corner k is k, edge k is 3 + k, the face 6
-// (src/collide3d.cpp:987-1024).
-TF_HD Vec3 closestOnTriangle(const Vec3 c[3], const Vec3& p, int& feature) {
-    const Vec3 ab = c[1] - c[0], ac = c[2] - c[0], ap = p - c[0];
-    const float d1 = dot(ab, ap), d2 = dot(ac, ap);
-    if (d1 <= 0.0f && d2 <= 0.0f) {
-        feature = 0;
-        return c[0];
-    }
-    const Vec3 bp = p - c[1];
-    const float d3 = dot(ab, bp), d4 = dot(ac, bp);
-    if (d3 >= 0.0f && d4 <= d3) {
-        feature = 1;
-        return c[1];
-    }
-    const float vc = d1 * d4 - d3 * d2;
-    if (vc <= 0.0f && d1 >= 0.0f && d3 <= 0.0f) {
-        feature = 3;
-        return c[0] + ab * (d1 / (d1 - d3));
-    }
-    const Vec3 cp = p - c[2];
-    const float d5 = dot(ab, cp), d6 = dot(ac, cp);
-    if (d6 >= 0.0f && d5 <= d6) {
-        feature = 2;
-        return c[2];
-    }
-    const float vb = d5 * d2 - d1 * d6;
-    if (vb <= 0.0f && d2 >= 0.0f && d6 <= 0.0f) {
-        feature = 5;
-        return c[0] + ac * (d2 / (d2 - d6));
-    }
-    const float va = d3 * d6 - d5 * d4;
-    if (va <= 0.0f && d4 - d3 >= 0.0f && d5 - d6 >= 0.0f) {
-        feature = 4;
-        return c[1] + (c[2] - c[1]) * ((d4 - d3) / ((d4 - d3) + (d5 - d6)));
-    }
-    feature = 6;
-    const float denom = 1.0f / (va + vb + vc);
-    return c[0] + ab * (vb * denom) + ac * (vc * denom);
-}
 
 // The edge or corner of the triangle farthest along d, numbered as above: the edge when its far corner is
 // within tolerance (src/collide3d.cpp:1437-1443).
@@ -241,7 +200,6 @@ TF_HD int collideMesh(const CollideCtx& cx, const DShape& mesh, const Transform&
                       MeshBounds* bounds) {
     outCount = 0;
     if (mesh.mesh < 0 || other.kind == kHalfSpace || other.kind == kMesh) { return kMeshOk; }
-    if (other.kind == kCylinder) { return kMeshUnsupported; }
     const MeshTables& mt = cx.mt;
     const DMesh M = mt.meshes[mesh.mesh];
     const Tolerances tol = cx.tol;
@@ -296,6 +254,51 @@ TF_HD int collideMesh(const CollideCtx& cx, const DShape& mesh, const Transform&
             const Vec3 w = apply(xm, (surface + center - normal * r) * 0.5f);
             m.points[0] = MPoint{ w, sep, motion.predict(w, m.normal, sep) };
             m.count = 1;
+            keep(m);
+        });
+    } else if (other.kind == kCylinder) {
+        const Solid b = cylinderSolid(other, rel);
+        const Vec3 reach = cylinderReach(b.axis, b.radius, b.halfHeight) + Vec3{ margin, margin, margin };
+        const Convex convexB = convexOf(cx, other);
+        walked = queryMesh(mt, M, b.center - reach, b.center + reach, [&](int t) {
+            if (outOfReach(bounds, t, margin)) { return; }
+            Vec3 c[3];
+            meshCorners(mt, M, t, c);
+            const Vec3 n = mt.normals[M.tFirst + t];
+            TriangleFrame tri;
+            tri.set(c, n);
+            const Solid a = polySolid(ownFrame(tri.t, 0));
+            const Convex triangle{ tri.verts, 3, 0.0f, false };
+            Separation best;
+            if (!separate(a, b, triangle, xm, convexB, xo, xm.q, margin, tol, best)) {
+                ruleOut(bounds, t, best.gap, status);
+                return;
+            }
+            Manifold m;
+            m.count = 0;
+            m.featKind = kFeatNone;
+            m.featA = m.featB = -1;
+            solidContact(cx.cap, a, b, best.normal, best.gap, xm, margin, tol.linearSlop, motion, m);
+            if (m.count == 0) { return; }
+            // An edge or corner without a normal of its own leaves the push to the face.
+            if (fabsf(dot(best.normal, n)) < 0.9999f) {
+                Separation front = noSeparation(), back = noSeparation();
+                tryAxis(a, b, n, front);
+                tryAxis(a, b, -n, back);
+                const int side = front.gap >= back.gap ? 0 : 1;
+                if (!keepsNormal(mt.edges[M.tFirst + t], triangleFeature(c, best.normal, tol.linearSlop), side, best.normal, n)) {
+                    const Separation& face = side == 0 ? front : back;
+                    m.count = 0;
+                    solidContact(cx.cap, a, b, face.normal, face.gap, xm, margin, tol.linearSlop, motion, m);
+                    for (int k = 0; k < m.count; ++k) {
+                        const Vec3 p = applyInverse(xm, m.points[k].position);
+                        if (m.points[k].separation < best.gap - tol.linearSlop && !overTriangle(c, n, p, tol.linearSlop)) {
+                            return;
+                        }
+                    }
+                    if (m.count == 0) { return; }
+                }
+            }
             keep(m);
         });
     } else {

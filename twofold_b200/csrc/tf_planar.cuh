@@ -106,8 +106,7 @@ TF_HD void setDepth(Profile& p, float center, float a, float b) {
 }
 
 // The profile of shape s seen along n, with u and v the 2D axes around n, all in the body's frame
-// (src/collide2d.cpp:47-96). Returns false for a profile this build does not hold (a cylinder, which is not
-// built, or an outline longer than kMaxProfilePoints).
+// (src/collide2d.cpp:47-96). Returns false for an outline longer than kMaxProfilePoints.
 TF_HD bool makeProfile(const PolyTables& pt, const DShape& s, const Vec3& n, const Vec3& u, const Vec3& v, Profile& p) {
     const Transform& xf = s.local;
     const float c = dot(xf.p, n);
@@ -149,7 +148,13 @@ TF_HD bool makeProfile(const PolyTables& pt, const DShape& s, const Vec3& n, con
         return true;
     }
     if (fabsf(a) < kPlaneAligned) { return true; }
-    if (s.kind == kCylinder) { return false; }
+    if (s.kind == kCylinder) {
+        p.center = project2(xf.p, u, v);
+        p.radius = s.radius;
+        setDepth(p, c, -s.halfHeight, s.halfHeight);
+        p.kind = kProfileCircle;
+        return true;
+    }
     if (s.geometry == 3 /* TF_PRISM */ && s.poly >= 0) {
         // A prism's polyhedron starts with its outline at zMin, then the same outline at zMax.
         const DPoly& P = pt.polys[s.poly];
@@ -357,6 +362,66 @@ TF_HD void collidePolygons(const Polygon2& a, const Polygon2& b, float margin, f
     }
 }
 
+// A polygon and a circle; the normal points from the polygon to the circle (src/collide2d.cpp:259-291).
+TF_HD void collidePolygonCircle(const Polygon2& poly, const Vec2& c, float r, float margin, Planar2& out) {
+    int edge = 0;
+    float sep = -FLT_MAX;
+    for (int i = 0; i < poly.count; ++i) {
+        const float s = dot(poly.normals[i], c - poly.points[i]);
+        if (s > sep) {
+            sep = s;
+            edge = i;
+        }
+    }
+    if (sep - r > margin) { return; }
+    const Vec2 v1 = poly.points[edge];
+    const Vec2 v2 = poly.points[(edge + 1) % poly.count];
+    Vec2 surface;
+    if (sep > FLT_EPSILON && dot(c - v1, v2 - v1) < 0.0f) {
+        surface = v1;
+    } else if (sep > FLT_EPSILON && dot(c - v2, v1 - v2) < 0.0f) {
+        surface = v2;
+    } else {
+        const Vec2 n = poly.normals[edge];
+        out.normal = n;
+        out.points[0] = ((c - n * sep) + (c - n * r)) * 0.5f;
+        out.separations[0] = sep - r;
+        out.count = 1;
+        return;
+    }
+    const float dist = length(c - surface);
+    const float s = dist - r;
+    if (s > margin || dist <= 0.0f) { return; }
+    const Vec2 n = (c - surface) * (1.0f / dist);
+    out.normal = n;
+    out.points[0] = (surface + (c - n * r)) * 0.5f;
+    out.separations[0] = s;
+    out.count = 1;
+}
+
+// src/collide2d.cpp:293-303.
+TF_HD void collideCircles(const Vec2& ca, float ra, const Vec2& cb, float rb, float margin, Planar2& out) {
+    const Vec2 d = cb - ca;
+    const float dist = length(d);
+    const float s = dist - ra - rb;
+    if (s > margin) { return; }
+    const Vec2 n = dist > 0.0f ? d * (1.0f / dist) : Vec2{ 1, 0 };
+    out.normal = n;
+    out.points[0] = ca + n * (ra + 0.5f * s);
+    out.separations[0] = s;
+    out.count = 1;
+}
+
+// A half-plane and a circle; the normal points out of the half-plane (src/collide2d.cpp:325-332).
+TF_HD void collideHalfPlaneCircle(const Vec2& normal, float offset, const Vec2& c, float r, float margin, Planar2& out) {
+    const float sep = dot(normal, c) - offset;
+    if (sep - r > margin) { return; }
+    out.normal = normal;
+    out.points[0] = ((c - normal * sep) + (c - normal * r)) * 0.5f;
+    out.separations[0] = sep - r;
+    out.count = 1;
+}
+
 // A half-plane (normal out of it) against a polygon, which touches with the edge facing it most
 // (src/collide2d.cpp:310-323).
 TF_HD void collideHalfPlanePolygon(const Vec2& normal, float offset, const Polygon2& poly, float margin, Planar2& out) {
@@ -382,8 +447,7 @@ TF_HD void collideHalfPlanePolygon(const Vec2& normal, float offset, const Polyg
 
 // collidePlanar (src/collide2d.cpp:335-421) on two shapes already placed: returns 1 when the planar path
 // decided the pair (m.count may be 0), 0 when a profile is empty and the pair goes to the 3D path, and -1
-// for a profile this build does not hold. Circle profiles come only from cylinders, which this build does
-// not make.
+// for a profile this build does not hold.
 TF_HD int collidePlanar(const PolyTables& pt, const DShape& sa, const PlanePose& bodyA, const DShape& sb,
                         const PlanePose& bodyB, float margin, float slop, Manifold& m) {
     m.count = 0;
@@ -391,7 +455,6 @@ TF_HD int collidePlanar(const PolyTables& pt, const DShape& sa, const PlanePose&
     if (!profileOf(pt, sa, bodyA, pa) || !profileOf(pt, sb, bodyB, pb)) { return -1; }
     if (pa.kind == kProfileNone || pb.kind == kProfileNone) { return 0; }
     if (pa.kind == kProfileHalfPlane && pb.kind == kProfileHalfPlane) { return 0; }
-    if (pa.kind == kProfileCircle || pb.kind == kProfileCircle) { return -1; }
 
     // b's profile comes into a's 2D frame by one turn and shift, and its depths by one lift.
     const Vec2 ta = bodyA.turn, tb = bodyB.turn;
@@ -431,12 +494,27 @@ TF_HD int collidePlanar(const PolyTables& pt, const DShape& sa, const PlanePose&
     out.count = 0;
     if (pa.kind == kProfileHalfPlane) {
         const float offset = pa.offset - pa.tilt * zMid;
-        collideHalfPlanePolygon(pa.normal, offset, polyB, margin, out);
+        if (pb.kind == kProfileCircle) {
+            collideHalfPlaneCircle(pa.normal, offset, moved(pb.center), pb.radius, margin, out);
+        } else {
+            collideHalfPlanePolygon(pa.normal, offset, polyB, margin, out);
+        }
     } else if (halfB) {
         const Vec2 normal = turned(pb.normal);
         const float offset = pb.offset + dot(normal, shift) - pb.tilt * (zMid - lift);
-        collideHalfPlanePolygon(normal, offset, polyA, margin, out);
+        if (pa.kind == kProfileCircle) {
+            collideHalfPlaneCircle(normal, offset, pa.center, pa.radius, margin, out);
+        } else {
+            collideHalfPlanePolygon(normal, offset, polyA, margin, out);
+        }
         out.normal = -out.normal;
+    } else if (pa.kind == kProfileCircle && pb.kind == kProfileCircle) {
+        collideCircles(pa.center, pa.radius, moved(pb.center), pb.radius, margin, out);
+    } else if (pa.kind == kProfileCircle) {
+        collidePolygonCircle(polyB, pa.center, pa.radius, margin, out);
+        out.normal = -out.normal;
+    } else if (pb.kind == kProfileCircle) {
+        collidePolygonCircle(polyA, moved(pb.center), pb.radius, margin, out);
     } else {
         collidePolygons(polyA, polyB, margin, slop, out);
     }

@@ -317,14 +317,16 @@ def hulls(n=24, seed=0, degenerate=True, max_vertices=16):
     return w
 
 
-def planar(n=16384, cols=46, spheres=256, seed=0, sphere_height=(10.0, 600.0), floor="box", restitution=0.0):
+def planar(n=16384, cols=46, spheres=256, seed=0, sphere_height=(10.0, 600.0), floor="box", restitution=0.0,
+           discs=False):
     """Bodies locked to the z = 0 plane (lock frame identity): half boxes with half extents x, y ~ U[0.2, 0.6]
     and z = 0.5, half prisms of 3-8 vertices at sorted random angles on a circle of radius U[0.2, 0.6] with z in
     [-0.5, 0.5]; friction U[0.3, 0.9], a random turn in the plane; laid out on a `cols`-column grid of 1.7 m
     centred on x = 0, rows from y = 2 at 1.7 m. Static container: a floor box reaching 1.9 m past the grid
     (41 m half width at 46 columns) with 0.5 m walls 60 m tall at its ends, or a half-space floor alone
     (`floor="halfspace"`). `spheres` free spheres (r 0.5, density 4, not locked) at x ~ U over the grid,
-    y ~ U[sphere_height], z = 0."""
+    y ~ U[sphere_height], z = 0. With `discs`, every third prism is a cylinder of radius U[0.2, 0.6] and half
+    height 0.5 standing on the plane (a circle profile)."""
     rng = np.random.default_rng([seed, 3, 3])
     n_static = 3 if floor == "box" else 1
     total = n_static + n + spheres
@@ -360,6 +362,11 @@ def planar(n=16384, cols=46, spheres=256, seed=0, sphere_height=(10.0, 600.0), f
         m = int(rng.integers(3, 9))
         r = rng.uniform(0.2, 0.6)
         ang = np.sort(rng.uniform(0.0, 2 * math.pi, size=m))
+        if discs and i % 6 == 1:
+            s["geometry"][k] = abi.TF_CYLINDER
+            s["radius"][k] = r
+            s["half_height"][k] = 0.5
+            continue
         s["geometry"][k] = abi.TF_PRISM
         _set_points(w, k, np.stack([r * np.cos(ang), r * np.sin(ang)], 1))
         s["z_min"][k] = -0.5
@@ -438,7 +445,8 @@ def terrain_mesh(cells=256, cell=0.5, seed=0):
     return vertices, indices
 
 
-def terrain(cells=256, cell=0.5, cols=32, levels=32, pitch=2.0, top=60.0, seed=0, flat_hulls=False, spin=0.0):
+def terrain(cells=256, cell=0.5, cols=32, levels=32, pitch=2.0, top=60.0, seed=0, flat_hulls=False, spin=0.0,
+            cylinders=False):
     """Bodies dropped on a static terrain mesh (terrain_mesh): cols x cols columns at `pitch` m, `levels`
     levels from y = 2 to `top`, positions jittered by U[-0.1, 0.1], cycling through a sphere of radius
     U[0.25, 0.75], a box of half extents U[0.2, 0.8] and a hull of 16 points uniform on a 0.5 m sphere (at most
@@ -481,6 +489,13 @@ def terrain(cells=256, cell=0.5, cols=32, levels=32, pitch=2.0, top=60.0, seed=0
                 pts = flat.uniform(-0.5, 0.5, size=(12, 3)).astype(F32)
                 pts[:, 1] = 0.0
                 _set_points(w, i, pts)
+    if cylinders:
+        # Every fourth body a cylinder of radius U[0.15, 0.6] and half height U[0.05, 0.6].
+        cyl = np.random.default_rng([seed, 2, 4])
+        for i in range(4, n + 1, 4):
+            s["geometry"][i] = abi.TF_CYLINDER
+            s["radius"][i] = cyl.uniform(0.15, 0.6)
+            s["half_height"][i] = cyl.uniform(0.05, 0.6)
     if spin:
         b["type"][0] = abi.TF_KINEMATIC
         b["angular_velocity"][0] = (0.0, spin, 0.0)
@@ -490,6 +505,36 @@ def terrain(cells=256, cell=0.5, cols=32, levels=32, pitch=2.0, top=60.0, seed=0
 def config2():
     """Terrain: 32,768 spheres, boxes and hulls dropped on a 256 x 256 cell terrain mesh, 600 steps."""
     return Scene("terrain_32768", [terrain()], steps=600)
+
+
+def cylinders(n=24, seed=0):
+    """Cylinders of every proportion (discs, rods, squat drums; radius U[0.08, 0.5], half height U[0.03, 0.6])
+    with boxes, spheres and hulls, randomly turned, dropped in a loose column onto a half-space: cylinder
+    against cylinder, box, hull, sphere and half-space."""
+    rng = np.random.default_rng([seed, 9])
+    b, s = _bodies(n + 1), _shapes(n + 1)
+    _ground(b, s, friction=0.6)
+    w = World(b, s, np.arange(n + 1), meta={"kind": "cylinders"})
+    b["rotation"][1:] = _uniform_quats(rng, n)
+    for i in range(1, n + 1):
+        b["position"][i] = (rng.uniform(-1.2, 1.2), 0.8 + 0.8 * i, rng.uniform(-1.2, 1.2))
+        b["angular_velocity"][i] = rng.uniform(-2.0, 2.0, size=3)
+        s["friction"][i] = _f(rng.uniform(0.3, 0.9))
+        kind = i % 5
+        if kind in (0, 1, 2):
+            s["geometry"][i] = abi.TF_CYLINDER
+            s["radius"][i] = rng.uniform(0.08, 0.5)
+            s["half_height"][i] = rng.uniform(0.03, 0.6)
+        elif kind == 3:
+            s["half_extents"][i] = rng.uniform(0.15, 0.45, size=3).astype(F32)
+        elif i % 2:
+            s["geometry"][i] = abi.TF_SPHERE
+            s["radius"][i] = rng.uniform(0.15, 0.4)
+        else:
+            s["geometry"][i] = abi.TF_HULL
+            s["max_vertices"][i] = 16
+            _set_points(w, i, _sphere_points(rng, 16, 0.4))
+    return w
 
 
 def config3():
