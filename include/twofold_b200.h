@@ -187,6 +187,22 @@ typedef struct tf_contact {
     float tangent_impulses[4][3];
 } tf_contact;
 
+/* ContactEvent (include/twofold/world.h:269-276) with world-local indices. */
+typedef struct tf_contact_event {
+    uint32_t shape_a, shape_b;
+    uint32_t body_a, body_b;
+    int32_t begin;
+} tf_contact_event;
+
+/* HitEvent (include/twofold/world.h:278-288) with world-local indices. */
+typedef struct tf_hit_event {
+    uint32_t shape_a, shape_b;
+    uint32_t body_a, body_b;
+    float point[3];
+    float normal[3];
+    float speed;
+} tf_hit_event;
+
 TF_API int tf_abi_version(void);
 TF_API const char* tf_last_error(void);
 TF_API void tf_default_settings(tf_settings* out);
@@ -242,6 +258,15 @@ TF_API int tf_world_get_states(void* world, float* positions, float* rotations, 
  * World::contacts. Writes up to capacity entries and the total count. */
 TF_API int tf_world_contacts(void* world, int32_t w, int32_t include_speculative, tf_contact* out,
                              int32_t capacity, int32_t* count);
+/* World::contactEvents (include/twofold/world.h:477; ContactEvent :269-276): the pairs of shapes in world w
+ * that began (begin = 1) or stopped touching in its last step, ordered by shape pair (world-local indices,
+ * shape_a the lower). Sets *count to the number of events and writes at most capacity of them. After
+ * tf_world_restore_state or tf_world_autotune there are none until the next step. */
+TF_API int tf_world_contact_events(void* world, int32_t w, tf_contact_event* out, int32_t capacity, int32_t* count);
+/* World::hitEvents (include/twofold/world.h:478; HitEvent :278-288): for each touching pair whose fastest
+ * pushed point approached faster than hit_threshold in the last step, that point on shape A in the world,
+ * the contact normal (A to B) and the speed; ordered by shape pair. */
+TF_API int tf_world_hit_events(void* world, int32_t w, tf_hit_event* out, int32_t capacity, int32_t* count);
 /* Sorted, unique shape-pair keys (minShape << 32 | maxShape) the last broadphase produced. */
 TF_API int tf_world_candidates(void* world, int32_t w, uint64_t* out, int32_t capacity, int32_t* count);
 TF_API int tf_world_profile(void* world, int32_t w, tf_profile* out);

@@ -3,7 +3,8 @@
 // Code written against the reference's include/twofold/world.h (World, BodyDesc, ShapeDesc, WorldSettings,
 // StepProfile, ContactInfo, the id types and geometry alternatives) compiles against this header for the
 // part of the API the contact pipeline covers: building bodies and shapes, step(), reading poses,
-// velocities, mass, sleep state, contacts and the step profile, setting velocities and adding forces.
+// velocities, mass, sleep state, contacts, contact and hit events and the step profile, setting velocities
+// and adding forces.
 // Every call forwards to the C ABI in twofold_b200.h; the library owns the device state.
 //
 // Same conventions as the reference (include/twofold/world.h:362-510, src/world.cpp:352-371): invalid ids
@@ -243,6 +244,28 @@ struct ContactInfo {
     float separations[4] = {};
     float normalImpulses[4] = {};
     Vec3 tangentImpulses[4];
+};
+
+// Two shapes that started or stopped touching. Shape A has the lower index.
+struct ContactEvent {
+    BodyId bodyA;
+    BodyId bodyB;
+    ShapeId shapeA;
+    ShapeId shapeB;
+    // False when they stopped.
+    bool begin = true;
+};
+
+// The fastest approaching point of a touching pair, when faster than WorldSettings::hitThreshold.
+struct HitEvent {
+    BodyId bodyA;
+    BodyId bodyB;
+    ShapeId shapeA;
+    ShapeId shapeB;
+    Vec3 point;
+    // Points from shape A to shape B.
+    Vec3 normal;
+    float speed = 0.0f;
 };
 
 struct StepProfile {
@@ -503,6 +526,39 @@ public:
         return out;
     }
 
+    // Events of the last step, ordered by shape index (tf_world_contact_events, tf_world_hit_events).
+    const std::vector<ContactEvent>& contactEvents() const {
+        contactEvents_.clear();
+        int32_t n = 0;
+        if (!note(tf_world_contact_events(handle_, 0, nullptr, 0, &n)) || n == 0) { return contactEvents_; }
+        std::vector<tf_contact_event> raw((size_t)n);
+        if (!note(tf_world_contact_events(handle_, 0, raw.data(), n, &n))) { return contactEvents_; }
+        for (const tf_contact_event& e : raw) {
+            contactEvents_.push_back(ContactEvent{ bodyAt(e.body_a), bodyAt(e.body_b), shapeAt(e.shape_a),
+                                                   shapeAt(e.shape_b), e.begin != 0 });
+        }
+        return contactEvents_;
+    }
+    const std::vector<HitEvent>& hitEvents() const {
+        hitEvents_.clear();
+        int32_t n = 0;
+        if (!note(tf_world_hit_events(handle_, 0, nullptr, 0, &n)) || n == 0) { return hitEvents_; }
+        std::vector<tf_hit_event> raw((size_t)n);
+        if (!note(tf_world_hit_events(handle_, 0, raw.data(), n, &n))) { return hitEvents_; }
+        for (const tf_hit_event& e : raw) {
+            HitEvent h;
+            h.bodyA = bodyAt(e.body_a);
+            h.bodyB = bodyAt(e.body_b);
+            h.shapeA = shapeAt(e.shape_a);
+            h.shapeB = shapeAt(e.shape_b);
+            h.point = Vec3{ e.point[0], e.point[1], e.point[2] };
+            h.normal = Vec3{ e.normal[0], e.normal[1], e.normal[2] };
+            h.speed = e.speed;
+            hitEvents_.push_back(h);
+        }
+        return hitEvents_;
+    }
+
     // The last C ABI status and its message; TF_OK after calls that succeeded.
     int status() const { return status_; }
     std::string statusMessage() const { return status_ == TF_OK ? std::string() : std::string(tf_last_error()); }
@@ -583,6 +639,8 @@ private:
     std::vector<std::shared_ptr<const TriangleMesh>> meshes_;  // kept alive while their ids are in use
     bool forcesPending_ = false;
     mutable int status_ = TF_OK;
+    mutable std::vector<ContactEvent> contactEvents_;
+    mutable std::vector<HitEvent> hitEvents_;
 };
 
 }  // namespace twofold

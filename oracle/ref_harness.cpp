@@ -278,6 +278,36 @@ TF_API int ref_world_contacts(void* h, int mode, tf_contact* out, int cap, int* 
     return 0;
 }
 
+// World::contactEvents() and World::hitEvents() of the last step, through the public API, as the library's
+// tf_world_contact_events and tf_world_hit_events lay them out.
+TF_API int ref_world_contact_events(void* h, tf_contact_event* out, int cap, int* count) {
+    const std::vector<ContactEvent>& ev = W(h)->contactEvents();
+    *count = (int)ev.size();
+    for (size_t i = 0; out && i < ev.size() && (int)i < cap; ++i) {
+        out[i].shape_a = ev[i].shapeA.index;
+        out[i].shape_b = ev[i].shapeB.index;
+        out[i].body_a = ev[i].bodyA.index;
+        out[i].body_b = ev[i].bodyB.index;
+        out[i].begin = ev[i].begin ? 1 : 0;
+    }
+    return 0;
+}
+
+TF_API int ref_world_hit_events(void* h, tf_hit_event* out, int cap, int* count) {
+    const std::vector<HitEvent>& ev = W(h)->hitEvents();
+    *count = (int)ev.size();
+    for (size_t i = 0; out && i < ev.size() && (int)i < cap; ++i) {
+        out[i].shape_a = ev[i].shapeA.index;
+        out[i].shape_b = ev[i].shapeB.index;
+        out[i].body_a = ev[i].bodyA.index;
+        out[i].body_b = ev[i].bodyB.index;
+        put3(out[i].point, ev[i].point);
+        put3(out[i].normal, ev[i].normal);
+        out[i].speed = ev[i].speed;
+    }
+    return 0;
+}
+
 TF_API int ref_world_profile(void* h, tf_profile* out) {
     const StepProfile& p = W(h)->profile();
     out->total = p.total;

@@ -44,6 +44,8 @@ def load(path=REF_LIB):
             "ref_world_candidates": ([P, P, C.c_int, C.POINTER(C.c_int)], C.c_int),
             "ref_world_contacts": ([P, C.c_int, C.POINTER(abi.tf_contact), C.c_int, C.POINTER(C.c_int)], C.c_int),
             "ref_world_profile": ([P, C.POINTER(abi.tf_profile)], C.c_int),
+            "ref_world_contact_events": ([P, C.POINTER(abi.tf_contact_event), C.c_int, C.POINTER(C.c_int)], C.c_int),
+            "ref_world_hit_events": ([P, C.POINTER(abi.tf_hit_event), C.c_int, C.POINTER(C.c_int)], C.c_int),
             "ref_awake_dynamic": ([P], C.c_int),
             "ref_worlds_step_parallel": ([P, C.c_int, C.c_float, C.c_int, C.c_int, C.POINTER(C.c_int64)], C.c_int),
             "ref_hardware_threads": ([], C.c_int),
@@ -136,6 +138,21 @@ class RefWorld:
         arr = (abi.tf_contact * max(n.value, 1))()
         self.lib.ref_world_contacts(self.h, mode, arr, n.value, C.byref(n))
         return list(arr)[:n.value]
+
+    def contact_events(self):
+        n = C.c_int(0)
+        self.lib.ref_world_contact_events(self.h, None, 0, C.byref(n))
+        arr = (abi.tf_contact_event * max(n.value, 1))()
+        self.lib.ref_world_contact_events(self.h, arr, n.value, C.byref(n))
+        return [(e.shape_a, e.shape_b, e.body_a, e.body_b, bool(e.begin)) for e in list(arr)[:n.value]]
+
+    def hit_events(self):
+        n = C.c_int(0)
+        self.lib.ref_world_hit_events(self.h, None, 0, C.byref(n))
+        arr = (abi.tf_hit_event * max(n.value, 1))()
+        self.lib.ref_world_hit_events(self.h, arr, n.value, C.byref(n))
+        return [(e.shape_a, e.shape_b, e.body_a, e.body_b, np.array(e.point[:], np.float32),
+                 np.array(e.normal[:], np.float32), np.float32(e.speed)) for e in list(arr)[:n.value]]
 
     def profile(self):
         p = abi.tf_profile()

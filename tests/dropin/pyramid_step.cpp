@@ -47,8 +47,19 @@ int main(int argc, char** argv) {
     sd.friction = 0.4f;
     world.addShape(s, sd);
     boxes.push_back(s);
-    for (int k = 0; k < steps; ++k) { world.step(1.0f / 60.0f); }
+    // Events summed over the run: pairs that began and stopped touching, hits and their speeds.
+    int began = 0, ended = 0, hits = 0;
+    double hitSpeed = 0.0;
+    for (int k = 0; k < steps; ++k) {
+        world.step(1.0f / 60.0f);
+        for (const ContactEvent& e : world.contactEvents()) { (e.begin ? began : ended) += 1; }
+        for (const HitEvent& h : world.hitEvents()) {
+            ++hits;
+            hitSpeed += h.speed;
+        }
+    }
     std::printf("manifolds %d\n", world.profile().manifolds);
+    std::printf("events %d %d %d %.6g %d\n", began, ended, hits, hitSpeed, world.profile().touchingContacts);
     for (const BodyId& b : boxes) {
         const Vec3 p = world.position(b);
         const Quat q = world.rotation(b);

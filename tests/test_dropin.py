@@ -32,8 +32,9 @@ def _compile(out, link):
 def _parse(text):
     lines = [l for l in text.splitlines() if l and not l.startswith("#")]
     manifolds = int(lines[0].split()[1])
-    rows = np.array([[float(x) for x in l.split()] for l in lines[1:]])
-    return manifolds, rows
+    events = [float(x) for x in lines[1].split()[1:]]
+    rows = np.array([[float(x) for x in l.split()] for l in lines[2:]])
+    return (manifolds, events), rows
 
 
 def test_dropin_program_compiles_against_the_facade():
@@ -48,7 +49,11 @@ def test_dropin_program_matches_the_reference(tmp_path):
     m_mine, mine = _parse(out)
     with open(GOLDEN) as f:
         m_ref, ref = _parse(f.read())
-    assert m_mine == m_ref
+    # manifolds; events summed over the run: began, ended, hits (counts exact), hit speeds, touching contacts
+    assert m_mine[0] == m_ref[0]
+    ev_mine, ev_ref = m_mine[1], m_ref[1]
+    assert [ev_mine[i] for i in (0, 1, 2, 4)] == [ev_ref[i] for i in (0, 1, 2, 4)], (ev_mine, ev_ref)
+    assert abs(ev_mine[3] - ev_ref[3]) <= TOL * max(1.0, abs(ev_ref[3]))
     assert np.array_equal(mine[:, 0], ref[:, 0])
     for name, cols in (("p", slice(1, 4)), ("q", slice(4, 8)), ("v", slice(8, 11)), ("w", slice(11, 14))):
         err = rel_err(mine[:, cols], ref[:, cols])

@@ -156,6 +156,28 @@ class tf_contact(C.Structure):
     ]
 
 
+class tf_contact_event(C.Structure):
+    _fields_ = [
+        ("shape_a", C.c_uint32),
+        ("shape_b", C.c_uint32),
+        ("body_a", C.c_uint32),
+        ("body_b", C.c_uint32),
+        ("begin", C.c_int32),
+    ]
+
+
+class tf_hit_event(C.Structure):
+    _fields_ = [
+        ("shape_a", C.c_uint32),
+        ("shape_b", C.c_uint32),
+        ("body_a", C.c_uint32),
+        ("body_b", C.c_uint32),
+        ("point", C.c_float * 3),
+        ("normal", C.c_float * 3),
+        ("speed", C.c_float),
+    ]
+
+
 def body_desc(type=TF_DYNAMIC, position=(0, 0, 0), rotation=(0, 0, 0, 1), linear_velocity=(0, 0, 0),
               angular_velocity=(0, 0, 0), linear_damping=0.0, angular_damping=0.0, gravity_scale=1.0, locks=0,
               lock_frame=(0, 0, 0, 1), awake=True, can_sleep=True):
@@ -237,6 +259,9 @@ def _declare(lib):
         "tf_world_contacts": ([P, C.c_int32, C.c_int32, C.POINTER(tf_contact), C.c_int32, C.POINTER(C.c_int32)],
                               C.c_int),
         "tf_world_candidates": ([P, C.c_int32, P, C.c_int32, C.POINTER(C.c_int32)], C.c_int),
+        "tf_world_contact_events": ([P, C.c_int32, C.POINTER(tf_contact_event), C.c_int32, C.POINTER(C.c_int32)],
+                                    C.c_int),
+        "tf_world_hit_events": ([P, C.c_int32, C.POINTER(tf_hit_event), C.c_int32, C.POINTER(C.c_int32)], C.c_int),
         "tf_world_profile": ([P, C.c_int32, C.POINTER(tf_profile)], C.c_int),
         "tf_world_awake_bodies": ([P, C.POINTER(C.c_int64)], C.c_int),
         "tf_world_launch_count": ([P, C.POINTER(C.c_int64)], C.c_int),
@@ -274,7 +299,7 @@ EXPORTED = [
     "tf_bodies_create",
     "tf_shapes_add", "tf_world_step", "tf_world_step_graph", "tf_world_synchronize", "tf_world_device_status",
     "tf_body_get_state", "tf_body_set_velocity", "tf_body_get_mass", "tf_body_is_awake", "tf_world_body_count",
-    "tf_world_get_states", "tf_world_contacts", "tf_world_candidates", "tf_world_profile", "tf_world_awake_bodies",
+    "tf_world_get_states", "tf_world_contacts", "tf_world_contact_events", "tf_world_hit_events", "tf_world_candidates", "tf_world_profile", "tf_world_awake_bodies",
     "tf_world_launch_count", "tf_world_elapsed_ms", "tf_world_body_steps", "tf_world_add_forces",
     "tf_world_read_poses", "tf_world_set_profiling", "tf_world_kernel_times", "tf_kernel_name",
     "tf_world_work_counts", "tf_world_solver_counts", "tf_world_save_state", "tf_world_restore_state", "tf_world_autotune", "tf_tape_record", "tf_adjoint_forward",

@@ -69,6 +69,10 @@ struct Batch {
     uint64_t* mergeKeyB;
     uint32_t* mergePartB;
     uint32_t* mergeIdxB;
+    // The step's events: contact events from 2 * contactFirst (room for the pairs the narrowphase dropped
+    // and for the end-of-step report), hits from contactFirst.
+    TouchEvent* touchEvents;
+    HitRecord* hitEvents;
 
     // Flat work lists, filled as the step goes, each item a (world, index within the world) pair. Candidate
     // pairs, one list per pair class (candItemStride apart), for the pair collisions; the active contacts of

@@ -162,6 +162,8 @@ public:
     DevArray<Axis> dAxes;
     DevArray<uint64_t> dMergeKeyA, dMergeKeyB;
     DevArray<uint32_t> dMergePartA, dMergePartB, dMergeIdxA, dMergeIdxB;
+    DevArray<TouchEvent> dTouchEvents;
+    DevArray<HitRecord> dHitEvents;
     DevArray<uint32_t> dAbort;
     DevArray<uint32_t> dDebug;
     size_t nPolys = 0;
@@ -798,6 +800,8 @@ public:
         TF_ALLOC(dMergePartB, ncon);
         TF_ALLOC(dMergeIdxA, ncon);
         TF_ALLOC(dMergeIdxB, ncon);
+        TF_ALLOC(dTouchEvents, 2 * ncon);
+        TF_ALLOC(dHitEvents, ncon);
         TF_ALLOC(dWork, kSlotCount);
         TF_ALLOC(dCandItems, ncand * kPairClasses);
         TF_ALLOC(dContactItems, ncon * (kPairClasses + 1));
@@ -922,6 +926,7 @@ public:
         P.tol.linearSlop = 0.005f * s.length_unit;
         P.tol.speculative = 4.0f * P.tol.linearSlop;
         P.continuous = s.continuous;
+        P.hitThreshold = s.hit_threshold * s.length_unit;
         return P;
     }
 
@@ -980,6 +985,8 @@ public:
         B.mergeKeyB = dMergeKeyB.ptr;
         B.mergePartB = dMergePartB.ptr;
         B.mergeIdxB = dMergeIdxB.ptr;
+        B.touchEvents = dTouchEvents.ptr;
+        B.hitEvents = dHitEvents.ptr;
         B.work = dWork.ptr;
         B.candItems = dCandItems.ptr;
         B.contactItems = dContactItems.ptr;
@@ -1399,6 +1406,34 @@ public:
         hostFresh = false;
         onDevice = true;
         bodiesDirty = false;
+        eventsValid = false;  // the event rooms hold the last step run, not the restored one's
+        return TF_OK;
+    }
+
+    // The contact events and hits of world w's last step, in the reference's order: by shape pair, and for
+    // one pair the narrowphase's before the end-of-step report's (src/world.cpp:1694-1700).
+    bool eventsValid = false;
+    int events(size_t w, std::vector<TouchEvent>* touch, std::vector<HitRecord>* hits) {
+        if (touch) { touch->clear(); }
+        if (hits) { hits->clear(); }
+        if (!eventsValid || w >= lastCounts.size() || w >= info.size()) { return TF_OK; }
+        TF_CUDA(cudaSetDevice(device));
+        TF_CUDA(cudaStreamSynchronize(stream));
+        const WorldInfo& wi = info[w];
+        if (touch && lastCounts[w].touchEvents > 0) {
+            touch->resize(std::min<size_t>(lastCounts[w].touchEvents, 2 * (size_t)wi.contactCap));
+            TF_CUDA(cudaMemcpy(touch->data(), dTouchEvents.ptr + 2 * (size_t)wi.contactFirst,
+                               touch->size() * sizeof(TouchEvent), cudaMemcpyDeviceToHost));
+            std::sort(touch->begin(), touch->end(), [](const TouchEvent& a, const TouchEvent& b) {
+                return a.key != b.key ? a.key < b.key : a.late < b.late;
+            });
+        }
+        if (hits && lastCounts[w].hitEvents > 0) {
+            hits->resize(std::min<size_t>(lastCounts[w].hitEvents, (size_t)wi.contactCap));
+            TF_CUDA(cudaMemcpy(hits->data(), dHitEvents.ptr + wi.contactFirst, hits->size() * sizeof(HitRecord),
+                               cudaMemcpyDeviceToHost));
+            std::sort(hits->begin(), hits->end(), [](const HitRecord& a, const HitRecord& b) { return a.key < b.key; });
+        }
         return TF_OK;
     }
 
@@ -1640,8 +1675,10 @@ public:
             p.awake_islands = (int32_t)counts[w].awakeIslands;
             p.swept_pairs = (int32_t)counts[w].sweptPairs;
             p.impacts = (int32_t)counts[w].impacts;
+            p.touching_contacts = (int32_t)counts[w].touching;
         }
         lastCounts = counts;
+        eventsValid = true;
         deviceFlags = flags;
         bodyStepsTotal = bodyStepsBase + bodySteps;
         if (flags & kDevUnsupported) { return fail(TF_E_UNSUPPORTED, "the step met a pair this build cannot collide"); }
@@ -2006,6 +2043,50 @@ TF_API int tf_world_contacts(void* h, int32_t w, int32_t mode, tf_contact* out, 
         ++n;
     }
     *count = n;
+    return TF_OK;
+}
+
+// The bodies of a pair's shapes, world-local; shape indices come from the key (lower index first).
+static void pairOf(const tfb::HostWorld& W, uint64_t key, uint32_t* sa, uint32_t* sb, uint32_t* ba, uint32_t* bb) {
+    *sa = (uint32_t)(key >> 32);
+    *sb = (uint32_t)key;
+    *ba = *sa < W.shapes.size() ? W.shapes[*sa].d.body : UINT32_MAX;
+    *bb = *sb < W.shapes.size() ? W.shapes[*sb].d.body : UINT32_MAX;
+}
+
+TF_API int tf_world_contact_events(void* h, int32_t w, tf_contact_event* out, int32_t cap, int32_t* count) {
+    if (!h || !count) { return tfb::fail(TF_E_INVALID, "tf_world_contact_events: null"); }
+    Engine* e = E(h);
+    if (w < 0 || w >= (int)e->worlds.size()) { return tfb::fail(TF_E_INVALID, "tf_world_contact_events: bad world"); }
+    std::vector<tfb::TouchEvent> ev;
+    const int rc = e->events((size_t)w, &ev, nullptr);
+    if (rc != TF_OK) { return rc; }
+    const tfb::HostWorld& W = e->worlds[(size_t)w];
+    for (size_t i = 0; out && i < ev.size() && (int32_t)i < cap; ++i) {
+        tf_contact_event& o = out[i];
+        pairOf(W, ev[i].key, &o.shape_a, &o.shape_b, &o.body_a, &o.body_b);
+        o.begin = (int32_t)ev[i].begin;
+    }
+    *count = (int32_t)ev.size();
+    return TF_OK;
+}
+
+TF_API int tf_world_hit_events(void* h, int32_t w, tf_hit_event* out, int32_t cap, int32_t* count) {
+    if (!h || !count) { return tfb::fail(TF_E_INVALID, "tf_world_hit_events: null"); }
+    Engine* e = E(h);
+    if (w < 0 || w >= (int)e->worlds.size()) { return tfb::fail(TF_E_INVALID, "tf_world_hit_events: bad world"); }
+    std::vector<tfb::HitRecord> ev;
+    const int rc = e->events((size_t)w, nullptr, &ev);
+    if (rc != TF_OK) { return rc; }
+    const tfb::HostWorld& W = e->worlds[(size_t)w];
+    for (size_t i = 0; out && i < ev.size() && (int32_t)i < cap; ++i) {
+        tf_hit_event& o = out[i];
+        pairOf(W, ev[i].key, &o.shape_a, &o.shape_b, &o.body_a, &o.body_b);
+        o.point[0] = ev[i].point.x, o.point[1] = ev[i].point.y, o.point[2] = ev[i].point.z;
+        o.normal[0] = ev[i].normal.x, o.normal[1] = ev[i].normal.y, o.normal[2] = ev[i].normal.z;
+        o.speed = ev[i].speed;
+    }
+    *count = (int32_t)ev.size();
     return TF_OK;
 }
 

@@ -1101,6 +1101,11 @@ __global__ void __launch_bounds__(kMaxBlock) k_narrowphase(const __grid_constant
     forWorlds(B, kSlotNarrow, sp, nullptr, [&](const Group& g, uint32_t w, unsigned char*, const StageSizes&) {
         const WorldInfo wi = B.info[w];
         WorldCounts& wc = B.counts[w];
+        if (g.tid == 0) {
+            wc.touchEvents = 0;
+            wc.hitEvents = 0;
+            wc.touching = 0;
+        }
         keepPlacements(B, g, wi);
         const uint32_t nc = wc.candCount;
         const uint32_t oldCount = wc.contactCount;
@@ -1119,19 +1124,19 @@ __global__ void __launch_bounds__(kMaxBlock) k_narrowphase(const __grid_constant
             });
         // Contacts of pairs where nothing moves and one body is dynamic (asleep) stay as they were
         // (src/world.cpp:961-988).
+        auto keepOld = [&](uint32_t j) {
+            const DContact& c = old[j];
+            if (!TF_OK_INDEX(B, c.bodyA - wi.bodyFirst < wi.bodyCount && c.bodyB - wi.bodyFirst < wi.bodyCount, 4,
+                             wi.bodyFirst, j)) {
+                return false;
+            }
+            const DBody& a = B.bodies[c.bodyA];
+            const DBody& b = B.bodies[c.bodyB];
+            if ((c.flags & kCRemoved) || movingAwake(a) || movingAwake(b)) { return false; }
+            return !(a.type != kDynamic && b.type != kDynamic);
+        };
         const uint32_t nK = groupCompact(
-            g, oldCount,
-            [&](uint32_t j) {
-                const DContact& c = old[j];
-                if (!TF_OK_INDEX(B, c.bodyA - wi.bodyFirst < wi.bodyCount && c.bodyB - wi.bodyFirst < wi.bodyCount, 4,
-                                 wi.bodyFirst, j)) {
-                    return false;
-                }
-                const DBody& a = B.bodies[c.bodyA];
-                const DBody& b = B.bodies[c.bodyB];
-                if ((c.flags & kCRemoved) || movingAwake(a) || movingAwake(b)) { return false; }
-                return !(a.type != kDynamic && b.type != kDynamic);
-            },
+            g, oldCount, keepOld,
             [&](uint32_t j, uint32_t pos) {
                 B.mergeKeyB[cf + pos] = old[j].key;
                 B.mergePartB[cf + pos] = old[j].part;
@@ -1178,6 +1183,29 @@ __global__ void __launch_bounds__(kMaxBlock) k_narrowphase(const __grid_constant
                 }
             }
             B.contacts[cf + y + l] = old[B.mergeIdxB[cf + y]];
+        }
+        // A touching pair whose old contacts were dropped and that was not collided again has ended
+        // (src/world.cpp:963-981): one event per pair, from its first such contact.
+        for (uint32_t j = g.tid; j < oldCount; j += g.size) {
+            const uint64_t key = old[j].key;
+            if (!(old[j].flags & kCTouched) || keepOld(j)) { continue; }
+            bool first = true;
+            for (uint32_t k = j; k > 0 && old[k - 1].key == key && first; --k) {
+                first = !((old[k - 1].flags & kCTouched) && !keepOld(k - 1));
+            }
+            if (!first) { continue; }
+            uint32_t l = 0, h = nC;
+            while (l < h) {
+                const uint32_t mid = (l + h) >> 1;
+                if (B.mergeKeyA[cf + mid] < key) {
+                    l = mid + 1;
+                } else {
+                    h = mid;
+                }
+            }
+            if (l < nC && B.mergeKeyA[cf + l] == key) { continue; }
+            const uint32_t at = atomicAdd(&wc.touchEvents, 1u);
+            B.touchEvents[2 * (size_t)cf + at] = TouchEvent{ key, 0u, 0u };
         }
         g.sync();
         if (g.tid == 0) {
@@ -2089,6 +2117,70 @@ __device__ void sweepWorld(const Batch& B, const StepParams& P, const Group& g, 
 
 // Union-find is staged in the group's shared slice (parent and island time by body, union pairs by contact)
 // when the world fits, else in its global scratch.
+// Counts the touching contacts, reports the pairs that began or stopped touching and the fastest struck point
+// of each touching pair (src/world.cpp:1424-1468). The first contact of each pair walks the pair's contacts:
+// a pair touches where the solver pushed on a point or a point overlaps (by more than the linear slop once it
+// touched); a hit is a pushed point approaching faster than the threshold in a contact solved this step.
+// Runs after restitution, on the poses the solve left, before kinematic bodies snap to their targets.
+__device__ void reportTouches(const Batch& B, const StepParams& P, const Group& g, const WorldInfo& wi, WorldCounts& wc) {
+    const uint32_t nc = wc.contactCount;
+    DContact* cs = B.contacts + wi.contactFirst;
+    uint32_t touchingHere = 0;
+    for (uint32_t first = g.tid; first < nc; first += g.size) {
+        const uint64_t key = cs[first].key;
+        if (first > 0 && cs[first - 1].key == key) { continue; }
+        const bool was = (cs[first].flags & kCTouched) != 0;
+        const float apart = was ? P.tol.linearSlop : 0.0f;
+        bool touching = false;
+        float fastest = P.hitThreshold;
+        uint32_t struck = UINT32_MAX;
+        int point = 0;
+        uint32_t last = first;
+        for (; last < nc && cs[last].key == key; ++last) {
+            const DContact& c = cs[last];
+            bool pressed = false;
+            for (int i = 0; i < c.count; ++i) {
+                pressed = pressed || c.points[i].separation < 0.0f || c.points[i].normalImpulse > 0.0f;
+            }
+            touchingHere += pressed ? 1u : 0u;
+            if (!TF_OK_INDEX(B, c.bodyA - wi.bodyFirst < wi.bodyCount && c.bodyB - wi.bodyFirst < wi.bodyCount, 22,
+                             wi.bodyFirst, last)) {
+                continue;
+            }
+            const DBody& a = B.bodies[c.bodyA];
+            const DBody& b = B.bodies[c.bodyB];
+            const bool solved = (a.type == kDynamic && a.awake) || (b.type == kDynamic && b.awake);
+            for (int i = 0; i < c.count; ++i) {
+                const DPoint& p = c.points[i];
+                if (p.maxNormalImpulse > 0.0f) {
+                    touching = true;
+                    if (-p.relativeVelocity > fastest && solved) {
+                        fastest = -p.relativeVelocity;
+                        struck = last;
+                        point = i;
+                    }
+                } else if (p.separation < apart) {
+                    touching = true;
+                }
+            }
+        }
+        if (touching != was) {
+            const uint32_t at = atomicAdd(&wc.touchEvents, 1u);
+            B.touchEvents[2 * (size_t)wi.contactFirst + at] = TouchEvent{ key, touching ? 1u : 0u, 1u };
+            for (uint32_t k = first; k < last; ++k) {
+                cs[k].flags = touching ? (cs[k].flags | kCTouched) : (cs[k].flags & ~kCTouched);
+            }
+        }
+        if (struck != UINT32_MAX) {
+            const DContact& c = cs[struck];
+            const uint32_t at = atomicAdd(&wc.hitEvents, 1u);
+            B.hitEvents[(size_t)wi.contactFirst + at] =
+                HitRecord{ key, apply(B.bodies[c.bodyA].xf, c.points[point].localA), c.normal, fastest, 0u };
+        }
+    }
+    if (touchingHere > 0) { atomicAdd(&wc.touching, touchingHere); }
+}
+
 __global__ void __launch_bounds__(kMaxBlock) k_finish(const __grid_constant__ Batch B, const __grid_constant__ StepParams P, const __grid_constant__ Split sp, int serial) {
     extern __shared__ __align__(16) unsigned char s_raw[];
     __shared__ uint32_t s_awake[kMaxGroups], s_islands[kMaxGroups], s_sweep[kMaxGroups], s_pairs[kMaxGroups],
@@ -2120,6 +2212,8 @@ __global__ void __launch_bounds__(kMaxBlock) k_finish(const __grid_constant__ Ba
                 restituteContact(B.bodies[c.bodyA], B.bodies[c.bodyB], c, P, false, axes + (size_t)ci * kAxesPerContact);
             }
         }
+        g.sync();
+        reportTouches(B, P, g, wi, wc);
         g.sync();
         const uint32_t nc = wc.contactCount;
         const bool staged = wi.bodyCount <= stageBodies && nc <= stageContacts;

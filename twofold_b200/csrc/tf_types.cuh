@@ -221,7 +221,9 @@ struct WorldCounts {
     uint32_t impactColorCount;
     uint32_t awakeBodies;
     uint32_t awakeIslands;
-    uint32_t touching;
+    uint32_t touching;          // contacts touching after the solve (StepProfile::touchingContacts)
+    uint32_t touchEvents;       // this step's contact events and hits, in the world's event rooms
+    uint32_t hitEvents;
     uint32_t wakePending;
     uint32_t flags;            // tf_device_flags
     uint32_t candNeeded;       // largest count seen, for growing capacities
@@ -239,6 +241,26 @@ struct WorldCounts {
     uint32_t colorStart[kColors + 1];
     uint32_t impactColorStart[kColors + 1];
     unsigned long long bodySteps;  // awake dynamic bodies summed over every step since the layout
+};
+
+// A contact event of the step (ContactEvent, include/twofold/world.h:269-276) as a kernel appends it: the
+// pair's key (world-local shapes, lower index first) and whether the pair began touching. `late` is 0 for
+// pairs the narrowphase dropped and 1 for the end-of-step report, which is how the reference orders the two
+// for one pair (src/world.cpp:1694-1700); the host sorts a world's events by (key, late).
+struct TouchEvent {
+    uint64_t key;
+    uint32_t begin;
+    uint32_t late;
+};
+
+// A hit (HitEvent, include/twofold/world.h:278-288): the pair's key, the struck point on shape A in the
+// world, the contact normal (A to B) and the approach speed.
+struct HitRecord {
+    uint64_t key;
+    Vec3 point;
+    Vec3 normal;
+    float speed;
+    uint32_t pad;
 };
 
 struct Tolerances {
@@ -274,6 +296,7 @@ struct StepParams {
     float treeMargin;       // kTreeMargin * lengthUnit
     Tolerances tol;
     int continuous;
+    float hitThreshold;     // scaled
 };
 
 }

@@ -111,6 +111,23 @@ class Batch:
         abi.check(self.lib.tf_world_contacts(self.h, wi, mode, arr, n.value, C.byref(n)), self.lib)
         return list(arr)[:n.value]
 
+    def contact_events(self, wi=0):
+        """World::contactEvents of world wi's last step: (shape_a, shape_b, body_a, body_b, begin) tuples."""
+        n = C.c_int32(0)
+        abi.check(self.lib.tf_world_contact_events(self.h, wi, None, 0, C.byref(n)), self.lib)
+        arr = (abi.tf_contact_event * max(n.value, 1))()
+        abi.check(self.lib.tf_world_contact_events(self.h, wi, arr, n.value, C.byref(n)), self.lib)
+        return [(e.shape_a, e.shape_b, e.body_a, e.body_b, bool(e.begin)) for e in list(arr)[:n.value]]
+
+    def hit_events(self, wi=0):
+        """World::hitEvents of world wi's last step: (shape_a, shape_b, body_a, body_b, point, normal, speed)."""
+        n = C.c_int32(0)
+        abi.check(self.lib.tf_world_hit_events(self.h, wi, None, 0, C.byref(n)), self.lib)
+        arr = (abi.tf_hit_event * max(n.value, 1))()
+        abi.check(self.lib.tf_world_hit_events(self.h, wi, arr, n.value, C.byref(n)), self.lib)
+        return [(e.shape_a, e.shape_b, e.body_a, e.body_b, np.array(e.point[:], np.float32),
+                 np.array(e.normal[:], np.float32), np.float32(e.speed)) for e in list(arr)[:n.value]]
+
     def profile(self, wi=0):
         p = abi.tf_profile()
         abi.check(self.lib.tf_world_profile(self.h, wi, C.byref(p)), self.lib)
