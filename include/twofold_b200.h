@@ -187,6 +187,58 @@ typedef struct tf_contact {
     float tangent_impulses[4][3];
 } tf_contact;
 
+/* JointType (include/twofold/world.h:202). */
+enum tf_joint_type {
+    TF_JOINT_POINT = 0, TF_JOINT_FIXED = 1, TF_JOINT_HINGE = 2, TF_JOINT_SLIDER = 3, TF_JOINT_DISTANCE = 4,
+    TF_JOINT_SWING_TWIST = 5
+};
+
+/* JointDesc plus its JointKind alternative (include/twofold/world.h:132-214), in world space at the bodies'
+ * current poses. body_a with index UINT32_MAX joins body B to the world.
+ *   every kind: anchor (a distance joint's anchorA), collide_connected, break_force, break_torque
+ *               (infinity for none).
+ *   TF_JOINT_HINGE:  axis, limited, lower/upper angle, motor_speed, max_motor (torque), friction (torque).
+ *   TF_JOINT_SLIDER: axis, limited, lower/upper translation, motor_speed, max_motor (force), friction (force).
+ *   TF_JOINT_DISTANCE: anchor_b, length (negative: the distance the anchors start at), hertz, damping_ratio,
+ *               limited, lower/upper = minDistance/maxDistance.
+ *   TF_JOINT_SWING_TWIST: axis, normal, swing_y, swing_z, lower/upper twist, friction (torque). */
+typedef struct tf_joint_desc {
+    int32_t type;
+    tf_id body_a;
+    tf_id body_b;
+    float anchor[3];
+    float anchor_b[3];
+    float axis[3];
+    float normal[3];
+    int32_t limited;
+    float lower;
+    float upper;
+    float motor_speed;
+    float max_motor;
+    float friction;
+    float length;
+    float hertz;
+    float damping_ratio;
+    float swing_y;
+    float swing_z;
+    int32_t collide_connected;
+    float break_force;
+    float break_torque;
+} tf_joint_desc;
+
+/* JointInfo (include/twofold/world.h:300-316) with world-local body indices (body_a UINT32_MAX: the world). */
+typedef struct tf_joint_info {
+    int32_t type;
+    uint32_t body_a, body_b;
+    float anchor_a[3];
+    float anchor_b[3];
+    float axis[3];
+    float value;
+    float force[3];
+    float torque[3];
+    int32_t broken;
+} tf_joint_info;
+
 /* ContactEvent (include/twofold/world.h:269-276) with world-local indices. */
 typedef struct tf_contact_event {
     uint32_t shape_a, shape_b;
@@ -233,6 +285,18 @@ TF_API int tf_shapes_add(void* world, int32_t n, const int32_t* world_of, const 
 
 /* Steps every world of the batch n_steps times by dt. Returns TF_OK, or an error with the device
  * flags available from tf_world_device_status. */
+/* World::createJoint (include/twofold/world.h:428; src/world.cpp:2221-2333) in world w. Invalid bodies give
+ * TF_E_INVALID (the reference returns an invalid id). Refused with TF_E_UNSUPPORTED: joining bodies that
+ * already have contacts without collide_connected (the reference drops those contacts), and a sleeping
+ * dynamic end (the reference wakes it). */
+TF_API int tf_joint_create(void* world, int32_t w, const tf_joint_desc* desc, tf_id* out_joint);
+/* World::jointInfo (include/twofold/world.h:441): pose, value, last force and torque, broken. An invalid id
+ * reads as zeros. */
+TF_API int tf_joint_get_info(void* world, int32_t w, tf_id joint, tf_joint_info* out);
+/* World::brokenJoints (include/twofold/world.h:443): the joints that broke in world w's last step, in index
+ * order; *count gets their number, at most capacity are written. */
+TF_API int tf_world_broken_joints(void* world, int32_t w, tf_id* out, int32_t capacity, int32_t* count);
+
 TF_API int tf_world_step(void* world, float dt, int32_t n_steps);
 /* Records n_steps steps of every world into a CUDA graph on first use and replays it afterwards. */
 TF_API int tf_world_step_graph(void* world, float dt, int32_t n_steps);

@@ -278,6 +278,101 @@ TF_API int ref_world_contacts(void* h, int mode, tf_contact* out, int cap, int* 
     return 0;
 }
 
+// World::createJoint from the library's joint descriptor, as the library reads it (tf_joint_desc).
+TF_API int ref_joint_create(void* h, const tf_joint_desc* d, tf_id* out) {
+    JointDesc jd;
+    if (d->body_a.index != UINT32_MAX) { jd.bodyA = BodyId{ d->body_a.index, d->body_a.generation }; }
+    jd.bodyB = BodyId{ d->body_b.index, d->body_b.generation };
+    jd.collideConnected = d->collide_connected != 0;
+    jd.breakForce = d->break_force;
+    jd.breakTorque = d->break_torque;
+    const Vec3 anchor{ d->anchor[0], d->anchor[1], d->anchor[2] };
+    const Vec3 axis{ d->axis[0], d->axis[1], d->axis[2] };
+    switch (d->type) {
+        case TF_JOINT_POINT: jd.kind = PointJoint{ anchor }; break;
+        case TF_JOINT_FIXED: jd.kind = FixedJoint{ anchor }; break;
+        case TF_JOINT_HINGE: {
+            HingeJoint k;
+            k.anchor = anchor;
+            k.axis = axis;
+            k.limited = d->limited != 0;
+            k.lowerAngle = d->lower;
+            k.upperAngle = d->upper;
+            k.motorSpeed = d->motor_speed;
+            k.maxMotorTorque = d->max_motor;
+            k.frictionTorque = d->friction;
+            jd.kind = k;
+            break;
+        }
+        case TF_JOINT_SLIDER: {
+            SliderJoint k;
+            k.anchor = anchor;
+            k.axis = axis;
+            k.limited = d->limited != 0;
+            k.lowerTranslation = d->lower;
+            k.upperTranslation = d->upper;
+            k.motorSpeed = d->motor_speed;
+            k.maxMotorForce = d->max_motor;
+            k.frictionForce = d->friction;
+            jd.kind = k;
+            break;
+        }
+        case TF_JOINT_DISTANCE: {
+            DistanceJoint k;
+            k.anchorA = anchor;
+            k.anchorB = Vec3{ d->anchor_b[0], d->anchor_b[1], d->anchor_b[2] };
+            k.length = d->length;
+            k.hertz = d->hertz;
+            k.dampingRatio = d->damping_ratio;
+            k.limited = d->limited != 0;
+            k.minDistance = d->lower;
+            k.maxDistance = d->upper;
+            jd.kind = k;
+            break;
+        }
+        default: {
+            SwingTwistJoint k;
+            k.anchor = anchor;
+            k.axis = axis;
+            k.normal = Vec3{ d->normal[0], d->normal[1], d->normal[2] };
+            k.swingY = d->swing_y;
+            k.swingZ = d->swing_z;
+            k.lowerTwist = d->lower;
+            k.upperTwist = d->upper;
+            k.frictionTorque = d->friction;
+            jd.kind = k;
+            break;
+        }
+    }
+    const JointId id = W(h)->createJoint(jd);
+    out->index = id.index;
+    out->generation = id.generation;
+    return id.index == UINT32_MAX ? -1 : 0;
+}
+
+TF_API int ref_joint_info(void* h, tf_id joint, tf_joint_info* out) {
+    const JointInfo info = W(h)->jointInfo(JointId{ joint.index, joint.generation });
+    std::memset(out, 0, sizeof(*out));
+    out->type = (int32_t)info.type;
+    out->body_a = info.bodyA.index;
+    out->body_b = info.bodyB.index;
+    put3(out->anchor_a, info.anchorA);
+    put3(out->anchor_b, info.anchorB);
+    put3(out->axis, info.axis);
+    out->value = info.value;
+    put3(out->force, info.force);
+    put3(out->torque, info.torque);
+    out->broken = info.broken ? 1 : 0;
+    return 0;
+}
+
+TF_API int ref_broken_joints(void* h, tf_id* out, int cap, int* count) {
+    const std::vector<JointId> ids = W(h)->brokenJoints();
+    *count = (int)ids.size();
+    for (size_t i = 0; out && i < ids.size() && (int)i < cap; ++i) { out[i] = { ids[i].index, ids[i].generation }; }
+    return 0;
+}
+
 // World::contactEvents() and World::hitEvents() of the last step, through the public API, as the library's
 // tf_world_contact_events and tf_world_hit_events lay them out.
 TF_API int ref_world_contact_events(void* h, tf_contact_event* out, int cap, int* count) {

@@ -44,6 +44,9 @@ def load(path=REF_LIB):
             "ref_world_candidates": ([P, P, C.c_int, C.POINTER(C.c_int)], C.c_int),
             "ref_world_contacts": ([P, C.c_int, C.POINTER(abi.tf_contact), C.c_int, C.POINTER(C.c_int)], C.c_int),
             "ref_world_profile": ([P, C.POINTER(abi.tf_profile)], C.c_int),
+            "ref_joint_create": ([P, C.POINTER(abi.tf_joint_desc), C.POINTER(abi.tf_id)], C.c_int),
+            "ref_joint_info": ([P, abi.tf_id, C.POINTER(abi.tf_joint_info)], C.c_int),
+            "ref_broken_joints": ([P, P, C.c_int, C.POINTER(C.c_int)], C.c_int),
             "ref_world_contact_events": ([P, C.POINTER(abi.tf_contact_event), C.c_int, C.POINTER(C.c_int)], C.c_int),
             "ref_world_hit_events": ([P, C.POINTER(abi.tf_hit_event), C.c_int, C.POINTER(C.c_int)], C.c_int),
             "ref_awake_dynamic": ([P], C.c_int),
@@ -100,6 +103,8 @@ class RefWorld:
                                       world.body_of.ctypes.data, shapes.ctypes.data)
         if rc != 0:
             raise RuntimeError("reference scene build failed")
+        for j in getattr(world, "joints", []):
+            self.joint_create(j)
 
     def copy(self):
         r = RefWorld(None, _handle=self.lib.ref_world_copy(self.h))
@@ -138,6 +143,24 @@ class RefWorld:
         arr = (abi.tf_contact * max(n.value, 1))()
         self.lib.ref_world_contacts(self.h, mode, arr, n.value, C.byref(n))
         return list(arr)[:n.value]
+
+    def joint_create(self, desc):
+        out = abi.tf_id()
+        if self.lib.ref_joint_create(self.h, C.byref(desc), C.byref(out)) != 0:
+            raise ValueError("the reference refused the joint")
+        return out
+
+    def joint_info(self, joint):
+        info = abi.tf_joint_info()
+        self.lib.ref_joint_info(self.h, joint, C.byref(info))
+        return info
+
+    def broken_joints(self):
+        n = C.c_int(0)
+        self.lib.ref_broken_joints(self.h, None, 0, C.byref(n))
+        arr = (abi.tf_id * max(n.value, 1))()
+        self.lib.ref_broken_joints(self.h, arr, n.value, C.byref(n))
+        return [(x.index, x.generation) for x in list(arr)[:n.value]]
 
     def contact_events(self):
         n = C.c_int(0)

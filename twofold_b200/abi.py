@@ -156,6 +156,72 @@ class tf_contact(C.Structure):
     ]
 
 
+TF_JOINT_POINT, TF_JOINT_FIXED, TF_JOINT_HINGE, TF_JOINT_SLIDER, TF_JOINT_DISTANCE, TF_JOINT_SWING_TWIST = range(6)
+
+
+class tf_joint_desc(C.Structure):
+    _fields_ = [
+        ("type", C.c_int32),
+        ("body_a", tf_id),
+        ("body_b", tf_id),
+        ("anchor", C.c_float * 3),
+        ("anchor_b", C.c_float * 3),
+        ("axis", C.c_float * 3),
+        ("normal", C.c_float * 3),
+        ("limited", C.c_int32),
+        ("lower", C.c_float),
+        ("upper", C.c_float),
+        ("motor_speed", C.c_float),
+        ("max_motor", C.c_float),
+        ("friction", C.c_float),
+        ("length", C.c_float),
+        ("hertz", C.c_float),
+        ("damping_ratio", C.c_float),
+        ("swing_y", C.c_float),
+        ("swing_z", C.c_float),
+        ("collide_connected", C.c_int32),
+        ("break_force", C.c_float),
+        ("break_torque", C.c_float),
+    ]
+
+
+def joint_desc(type, body_b, body_a=None, **kw):
+    """A tf_joint_desc with the reference's JointDesc defaults: no limits, no motor, unbreakable, a hinge or
+    swing-twist axis along x (hinge: z), swing and twist free."""
+    d = tf_joint_desc()
+    d.type = type
+    d.body_a = body_a if body_a is not None else tf_id(0xFFFFFFFF, 0)
+    d.body_b = body_b
+    d.axis[:] = [0.0, 0.0, 1.0] if type == TF_JOINT_HINGE else [1.0, 0.0, 0.0]
+    d.normal[:] = [0.0, 1.0, 0.0]
+    d.length = -1.0
+    d.swing_y = d.swing_z = 3.14159265
+    if type == TF_JOINT_SWING_TWIST:
+        d.lower, d.upper = -3.14159265, 3.14159265
+    d.break_force = d.break_torque = float("inf")
+    for k, v in kw.items():
+        if isinstance(v, (list, tuple)):
+            getattr(d, k)[:] = list(v)
+        else:
+            setattr(d, k, v)
+    return d
+
+
+class tf_joint_info(C.Structure):
+    _fields_ = [
+        ("type", C.c_int32),
+        ("body_a", C.c_uint32),
+        ("body_b", C.c_uint32),
+        ("anchor_a", C.c_float * 3),
+        ("anchor_b", C.c_float * 3),
+        ("axis", C.c_float * 3),
+        ("value", C.c_float),
+        ("force", C.c_float * 3),
+        ("torque", C.c_float * 3),
+        ("broken", C.c_int32),
+    ]
+
+
 class tf_contact_event(C.Structure):
     _fields_ = [
         ("shape_a", C.c_uint32),
@@ -246,6 +312,9 @@ def _declare(lib):
         "tf_shape_add": ([P, C.c_int32, tf_id, C.POINTER(tf_shape_desc), C.POINTER(tf_id)], C.c_int),
         "tf_bodies_create": ([P, C.c_int32, P, C.POINTER(tf_body_desc), P], C.c_int),
         "tf_shapes_add": ([P, C.c_int32, P, P, C.POINTER(tf_shape_desc), P], C.c_int),
+        "tf_joint_create": ([P, C.c_int32, C.POINTER(tf_joint_desc), C.POINTER(tf_id)], C.c_int),
+        "tf_joint_get_info": ([P, C.c_int32, tf_id, C.POINTER(tf_joint_info)], C.c_int),
+        "tf_world_broken_joints": ([P, C.c_int32, P, C.c_int32, C.POINTER(C.c_int32)], C.c_int),
         "tf_world_step": ([P, C.c_float, C.c_int32], C.c_int),
         "tf_world_step_graph": ([P, C.c_float, C.c_int32], C.c_int),
         "tf_world_synchronize": ([P], C.c_int),
@@ -297,7 +366,7 @@ EXPORTED = [
     "tf_abi_version", "tf_last_error", "tf_default_settings", "tf_world_create", "tf_world_destroy",
     "tf_world_count", "tf_world_set_settings", "tf_mesh_create", "tf_mesh_read", "tf_body_create", "tf_shape_add",
     "tf_bodies_create",
-    "tf_shapes_add", "tf_world_step", "tf_world_step_graph", "tf_world_synchronize", "tf_world_device_status",
+    "tf_shapes_add", "tf_joint_create", "tf_joint_get_info", "tf_world_broken_joints", "tf_world_step", "tf_world_step_graph", "tf_world_synchronize", "tf_world_device_status",
     "tf_body_get_state", "tf_body_set_velocity", "tf_body_get_mass", "tf_body_is_awake", "tf_world_body_count",
     "tf_world_get_states", "tf_world_contacts", "tf_world_contact_events", "tf_world_hit_events", "tf_world_candidates", "tf_world_profile", "tf_world_awake_bodies",
     "tf_world_launch_count", "tf_world_elapsed_ms", "tf_world_body_steps", "tf_world_add_forces",

@@ -69,6 +69,9 @@ struct Batch {
     uint64_t* mergeKeyB;
     uint32_t* mergePartB;
     uint32_t* mergeIdxB;
+    // Joints and joined body pairs, per world from jointFirst.
+    DJoint* joints;
+    const uint64_t* joined;
     // The step's events: contact events from 2 * contactFirst (room for the pairs the narrowphase dropped
     // and for the end-of-step report), hits from contactFirst.
     TouchEvent* touchEvents;

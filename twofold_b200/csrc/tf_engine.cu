@@ -50,7 +50,13 @@ struct HostBody {
     MassProps overrideMass;
 };
 
+struct HostJoint {
+    DJoint d{};  // ends world-local, kWorldEnd for the world
+    uint32_t generation = 0;
+};
+
 struct HostWorld {
+    std::vector<HostJoint> joints;
     std::vector<HostBody> bodies;
     std::vector<uint32_t> freeBodies;
     std::vector<HostShape> shapes;
@@ -162,6 +168,9 @@ public:
     DevArray<Axis> dAxes;
     DevArray<uint64_t> dMergeKeyA, dMergeKeyB;
     DevArray<uint32_t> dMergePartA, dMergePartB, dMergeIdxA, dMergeIdxB;
+    bool hasJoints = false;  // some world has joints: the substep and finish kernels with joint code run
+    DevArray<DJoint> dJoints;
+    DevArray<uint64_t> dJoined;
     DevArray<TouchEvent> dTouchEvents;
     DevArray<HitRecord> dHitEvents;
     DevArray<uint32_t> dAbort;
@@ -198,6 +207,7 @@ public:
         DevArray<DContact> contacts;
         DevArray<WorldCounts> counts;
         DevArray<uint8_t> struck, wakeMark;
+        DevArray<DJoint> joints;
         int cur = 0;
         uint64_t layoutGen = 0;
         int64_t bodyStepsTotal = 0, bodyStepsBase = 0;
@@ -535,6 +545,167 @@ public:
     // ---- layout and transfer ----
 
     // Brings the device's dynamic state and contacts back into the host mirrors.
+    // World::createJoint (src/world.cpp:2221-2333): the joint's frames in each body at their current poses.
+    // Two parts of the reference's behaviour have no counterpart here and are refused: joining bodies whose
+    // contacts the joint would remove (their pair already touches), and waking a sleeping end from the host.
+    int createJoint(int w, const tf_joint_desc* d, tf_id* out) {
+        if (w < 0 || w >= (int)worlds.size() || !d) { return fail(TF_E_INVALID, "createJoint: bad world or desc"); }
+        if (d->type < TF_JOINT_POINT || d->type > TF_JOINT_SWING_TWIST) { return fail(TF_E_INVALID, "createJoint: bad type"); }
+        int rc = pull();
+        if (rc != TF_OK) { return rc; }
+        HostWorld& W = worlds[(size_t)w];
+        auto valid = [&](tf_id id) {
+            return id.index < W.bodies.size() && W.bodies[id.index].d.alive && W.bodies[id.index].generation == id.generation;
+        };
+        if (!valid(d->body_b)) { return fail(TF_E_INVALID, "createJoint: invalid body B"); }
+        uint32_t ai = kWorldEnd;
+        if (d->body_a.index != UINT32_MAX) {
+            if (!valid(d->body_a) || d->body_a.index == d->body_b.index) { return fail(TF_E_INVALID, "createJoint: invalid body A"); }
+            ai = d->body_a.index;
+        }
+        const uint32_t bi = d->body_b.index;
+        if (!d->collide_connected && ai != kWorldEnd) {
+            for (const DContact& c : W.contacts) {
+                if ((c.bodyA == ai && c.bodyB == bi) || (c.bodyA == bi && c.bodyB == ai)) {
+                    return fail(TF_E_UNSUPPORTED, "createJoint: the bodies already have contacts, which this build does not remove");
+                }
+            }
+        }
+        for (uint32_t e : { ai, bi }) {
+            if (e != kWorldEnd && W.bodies[e].d.type == kDynamic && !W.bodies[e].d.awake) {
+                return fail(TF_E_UNSUPPORTED, "createJoint: waking a sleeping body from the host is not run by this build");
+            }
+        }
+        HostJoint hj;
+        DJoint& j = hj.d;
+        j.alive = 1;
+        j.type = (uint32_t)d->type;
+        j.bodyA = ai;
+        j.bodyB = bi;
+        j.collideConnected = d->collide_connected ? 1u : 0u;
+        j.breakForce = d->break_force;
+        j.breakTorque = d->break_torque;
+        const JBody worldBody = worldEnd();
+        const Transform xa = ai == kWorldEnd ? worldBody.xf : W.bodies[ai].d.xf;
+        const Transform xb = W.bodies[bi].d.xf;
+        const Vec3 anchor = v3of(d->anchor);
+        Vec3 anchorA = anchor, anchorB = anchor, axis{ 1, 0, 0 }, normal = zero3();
+        // The cone's half-angle sine, correctly rounded like every transcendental the device evaluates
+        // (src/world.cpp:21-24).
+        auto coneSine = [](float swing) {
+            if (swing >= kJointPi) { return 1.0f; }
+            return (float)std::sin((double)(0.5f * maxf(swing, 1e-3f)));
+        };
+        switch (d->type) {
+            case TF_JOINT_HINGE:
+            case TF_JOINT_SLIDER:
+                axis = normalize(v3of(d->axis));
+                j.limited = d->limited ? 1u : 0u;
+                j.lower = d->lower;
+                j.upper = d->upper;
+                j.motorSpeed = d->motor_speed;
+                j.maxMotor = d->max_motor;
+                j.maxFriction = d->friction;
+                break;
+            case TF_JOINT_DISTANCE:
+                anchorB = v3of(d->anchor_b);
+                j.length = d->length < 0.0f ? length(anchorB - anchorA) : d->length;
+                j.hertz = d->hertz;
+                j.dampingRatio = d->damping_ratio;
+                j.limited = d->limited ? 1u : 0u;
+                j.lower = d->lower;
+                j.upper = d->upper;
+                break;
+            case TF_JOINT_SWING_TWIST:
+                axis = normalize(v3of(d->axis));
+                normal = v3of(d->normal);
+                j.limited = d->upper - d->lower < 2.0f * kJointPi ? 1u : 0u;
+                j.lower = d->lower;
+                j.upper = d->upper;
+                j.swingY = coneSine(d->swing_y);
+                j.swingZ = coneSine(d->swing_z);
+                j.maxFriction = d->friction;
+                break;
+            default:
+                break;
+        }
+        if (d->type != TF_JOINT_SWING_TWIST) {
+            j.swingY = 1.0f;
+            j.swingZ = 1.0f;
+        }
+        const Vec3 ref = perpendicular(axis);
+        j.localA = applyInverse(xa, anchorA);
+        j.localB = applyInverse(xb, anchorB);
+        j.axisA = unrotate(xa.q, axis);
+        j.axisB = unrotate(xb.q, axis);
+        j.refA = unrotate(xa.q, ref);
+        j.refB = unrotate(xb.q, ref);
+        j.restTurn = conjugate(xa.q) * xb.q;
+        j.frameA = qid();
+        j.frameB = qid();
+        if (d->type == TF_JOINT_SWING_TWIST) {
+            Vec3 y = normal - axis * dot(normal, axis);
+            y = lengthSquared(y) > 1e-12f ? normalize(y) : ref;
+            const Vec3 z = cross(axis, y);
+            Mat3 m;
+            m.r[0] = { axis.x, y.x, z.x };
+            m.r[1] = { axis.y, y.y, z.y };
+            m.r[2] = { axis.z, y.z, z.z };
+            const Quat frame = quatOfMat3(m);
+            j.frameA = normalize(conjugate(xa.q) * frame);
+            j.frameB = normalize(conjugate(xb.q) * frame);
+        }
+        const uint32_t index = (uint32_t)W.joints.size();
+        W.joints.push_back(hj);
+        layoutDirty = true;
+        if (out) { *out = { index, hj.generation }; }
+        return TF_OK;
+    }
+
+    // World::jointInfo (src/world.cpp:410-425) from the host mirrors.
+    int jointInfo(int w, tf_id id, tf_joint_info* out) {
+        if (w < 0 || w >= (int)worlds.size() || !out) { return fail(TF_E_INVALID, "jointInfo: bad world"); }
+        int rc = pull();
+        if (rc != TF_OK) { return rc; }
+        const HostWorld& W = worlds[(size_t)w];
+        std::memset(out, 0, sizeof(*out));
+        out->body_a = UINT32_MAX;
+        if (id.index >= W.joints.size() || W.joints[id.index].generation != id.generation || !W.joints[id.index].d.alive) {
+            return TF_OK;  // an invalid id reads as defaults, as the reference's getters do
+        }
+        const DJoint& j = W.joints[id.index].d;
+        const JBody a = j.bodyA == kWorldEnd ? worldEnd() : jointBodyOf(W.bodies[j.bodyA].d);
+        const JBody b = jointBodyOf(W.bodies[j.bodyB].d);
+        out->type = (int32_t)j.type;
+        out->body_a = j.bodyA;
+        out->body_b = j.bodyB;
+        const Vec3 pa = apply(a.xf, j.localA), pb = apply(b.xf, j.localB), ax = rotate(a.xf.q, j.axisA);
+        out->anchor_a[0] = pa.x, out->anchor_a[1] = pa.y, out->anchor_a[2] = pa.z;
+        out->anchor_b[0] = pb.x, out->anchor_b[1] = pb.y, out->anchor_b[2] = pb.z;
+        out->axis[0] = ax.x, out->axis[1] = ax.y, out->axis[2] = ax.z;
+        out->value = jointValue(j, a, b);
+        out->force[0] = j.force.x, out->force[1] = j.force.y, out->force[2] = j.force.z;
+        out->torque[0] = j.torque.x, out->torque[1] = j.torque.y, out->torque[2] = j.torque.z;
+        out->broken = j.broken ? 1 : 0;
+        return TF_OK;
+    }
+
+    // World::brokenJoints (src/world.cpp:2413-2420): joints that broke in the last step, in index order.
+    int brokenJoints(int w, tf_id* out, int cap, int* count) {
+        if (w < 0 || w >= (int)worlds.size() || !count) { return fail(TF_E_INVALID, "brokenJoints: bad world"); }
+        int rc = pull();
+        if (rc != TF_OK) { return rc; }
+        const HostWorld& W = worlds[(size_t)w];
+        int n = 0;
+        for (size_t k = 0; k < W.joints.size(); ++k) {
+            if (!W.joints[k].d.brokeNow) { continue; }
+            if (out && n < cap) { out[n] = { (uint32_t)k, W.joints[k].generation }; }
+            ++n;
+        }
+        *count = n;
+        return TF_OK;
+    }
+
     int pull() {
         if (!onDevice || hostFresh) { return TF_OK; }
         TF_CUDA(cudaStreamSynchronize(stream));
@@ -579,6 +750,16 @@ public:
                 c.shapeA -= wi.shapeFirst;
                 c.shapeB -= wi.shapeFirst;
             }
+            if (!W.joints.empty() && wi.jointCount == W.joints.size()) {
+                std::vector<DJoint> js(W.joints.size());
+                TF_CUDA(cudaMemcpy(js.data(), dJoints.ptr + wi.jointFirst, js.size() * sizeof(DJoint), cudaMemcpyDeviceToHost));
+                for (size_t k = 0; k < js.size(); ++k) {
+                    DJoint j = js[k];
+                    if (j.bodyA != kWorldEnd) { j.bodyA -= wi.bodyFirst; }
+                    j.bodyB -= wi.bodyFirst;
+                    W.joints[k].d = j;
+                }
+            }
         }
         hostFresh = true;
         return TF_OK;
@@ -590,7 +771,7 @@ public:
         dropGraphs();
         const size_t nw = worlds.size();
         info.assign(nw, WorldInfo{});
-        size_t nb = 0, ns = 0, ncand = 0, ncon = 0, nplanes = 0, nparts = 0, nbounds = 0;
+        size_t nb = 0, ns = 0, ncand = 0, ncon = 0, nplanes = 0, nparts = 0, nbounds = 0, njoints = 0;
         std::vector<DPoly> polys;
         std::vector<Vec3> verts, normals, arcs;
         std::vector<int32_t> indices;
@@ -631,6 +812,9 @@ public:
             wi.boundsCap = hasMesh ? 16u * cap : 0u;
             nparts += wi.partCap;
             nbounds += wi.boundsCap;
+            wi.jointFirst = (uint32_t)njoints;
+            wi.jointCount = (uint32_t)W.joints.size();
+            njoints += wi.jointCount;
             nb += wi.bodyCount;
             ns += wi.shapeCount;
             nplanes += wi.planeCount;
@@ -645,6 +829,8 @@ public:
         std::vector<DBody> bodies(nb);
         std::vector<DShape> shapes(ns);
         std::vector<uint32_t> shapeList(ns), planeList(std::max<size_t>(nplanes, 1));
+        std::vector<DJoint> joints(std::max<size_t>(njoints, 1));
+        std::vector<uint64_t> joined(std::max<size_t>(njoints, 1));
         // Contacts carried over from the device: packed, with one (slot, first, count) run per world.
         std::vector<DContact> packed;
         std::vector<size_t> runSlot, runFirst, runCount;
@@ -696,6 +882,21 @@ public:
                 shapes[wi.shapeFirst + i] = d;
             }
             for (size_t k = 0; k < W.planes.size(); ++k) { planeList[wi.planeFirst + k] = wi.shapeFirst + W.planes[k]; }
+            // Joints with global ends, and the sorted pairs that joints keep from colliding
+            // (src/world.cpp:375-383).
+            std::vector<uint64_t> keys;
+            for (size_t k = 0; k < W.joints.size(); ++k) {
+                DJoint j = W.joints[k].d;
+                if (j.alive && !j.collideConnected && j.bodyA != kWorldEnd) {
+                    keys.push_back(((uint64_t)std::min(j.bodyA, j.bodyB) << 32) | (uint64_t)std::max(j.bodyA, j.bodyB));
+                }
+                if (j.bodyA != kWorldEnd) { j.bodyA += wi.bodyFirst; }
+                j.bodyB += wi.bodyFirst;
+                joints[wi.jointFirst + k] = j;
+            }
+            std::sort(keys.begin(), keys.end());
+            info[w].joinedCount = (uint32_t)keys.size();
+            for (size_t k = 0; k < keys.size(); ++k) { joined[wi.jointFirst + k] = keys[k]; }
             if (!W.contacts.empty()) {
                 runSlot.push_back(wi.contactFirst);
                 runFirst.push_back(packed.size());
@@ -725,6 +926,7 @@ public:
             medianWorldBodies = nw ? sizes[nw / 2] : 0;
             sortedSizes = std::move(sizes);
         }
+        hasJoints = njoints > 0;
         laidOut = true;
         {
             const int rc0 = configureLaunches();
@@ -800,6 +1002,8 @@ public:
         TF_ALLOC(dMergePartB, ncon);
         TF_ALLOC(dMergeIdxA, ncon);
         TF_ALLOC(dMergeIdxB, ncon);
+        TF_ALLOC(dJoints, joints.size());
+        TF_ALLOC(dJoined, joined.size());
         TF_ALLOC(dTouchEvents, 2 * ncon);
         TF_ALLOC(dHitEvents, ncon);
         TF_ALLOC(dWork, kSlotCount);
@@ -847,6 +1051,8 @@ public:
         if ((rc = up(dShapes.ptr, shapes.data(), ns * sizeof(DShape))) != TF_OK) { return rc; }
         if ((rc = up(dShapeList.ptr, shapeList.data(), ns * sizeof(uint32_t))) != TF_OK) { return rc; }
         if ((rc = up(dPlaneList.ptr, planeList.data(), planeList.size() * sizeof(uint32_t))) != TF_OK) { return rc; }
+        if ((rc = up(dJoints.ptr, joints.data(), joints.size() * sizeof(DJoint))) != TF_OK) { return rc; }
+        if ((rc = up(dJoined.ptr, joined.data(), joined.size() * sizeof(uint64_t))) != TF_OK) { return rc; }
         if ((rc = up(dPolys.ptr, polys.data(), polys.size() * sizeof(DPoly))) != TF_OK) { return rc; }
         if ((rc = up(dVerts.ptr, verts.data(), verts.size() * sizeof(Vec3))) != TF_OK) { return rc; }
         if ((rc = up(dNormals.ptr, normals.data(), normals.size() * sizeof(Vec3))) != TF_OK) { return rc; }
@@ -927,6 +1133,7 @@ public:
         P.tol.speculative = 4.0f * P.tol.linearSlop;
         P.continuous = s.continuous;
         P.hitThreshold = s.hit_threshold * s.length_unit;
+        P.jointSoft = makeSoft(minf(s.joint_hertz, 0.5f * P.invH), s.joint_damping_ratio, P.h);
         return P;
     }
 
@@ -985,6 +1192,8 @@ public:
         B.mergeKeyB = dMergeKeyB.ptr;
         B.mergePartB = dMergePartB.ptr;
         B.mergeIdxB = dMergeIdxB.ptr;
+        B.joints = dJoints.ptr;
+        B.joined = dJoined.ptr;
         B.touchEvents = dTouchEvents.ptr;
         B.hitEvents = dHitEvents.ptr;
         B.work = dWork.ptr;
@@ -1062,9 +1271,21 @@ public:
                     k_refresh<kClassMesh><<<flatGrids[12], threads(4), 0, stream>>>(B, P, i, serial);
                 });
             }
-            timed(5, rec, [&] { k_substep<<<grids[5], threads(5), smem(5), stream>>>(B, P, splits[5], i, serial); });
+            timed(5, rec, [&] {
+                if (hasJoints) {
+                    k_substep<true><<<grids[5], threads(5), smem(5), stream>>>(B, P, splits[5], i, serial);
+                } else {
+                    k_substep<false><<<grids[5], threads(5), smem(5), stream>>>(B, P, splits[5], i, serial);
+                }
+            });
         }
-        timed(6, rec, [&] { k_finish<<<grids[6], threads(6), smem(6), stream>>>(B, P, splits[6], serial); });
+        timed(6, rec, [&] {
+            if (hasJoints) {
+                k_finish<true><<<grids[6], threads(6), smem(6), stream>>>(B, P, splits[6], serial);
+            } else {
+                k_finish<false><<<grids[6], threads(6), smem(6), stream>>>(B, P, splits[6], serial);
+            }
+        });
         if (marks) { cudaEventRecord(marks[3], stream); }
         launches += 5 + kPairClasses + P.substeps + (kPairClasses + 1) * (P.substeps - 1) + (bigWorlds.empty() ? 0 : 2);
         cudaError_t e = cudaGetLastError();
@@ -1087,9 +1308,11 @@ public:
         };
         int rc;
         if ((rc = allow((const void*)k_broadphase)) != TF_OK) { return rc; }
-        if ((rc = allow((const void*)k_substep)) != TF_OK) { return rc; }
+        if ((rc = allow((const void*)k_substep<false>)) != TF_OK) { return rc; }
+        if ((rc = allow((const void*)k_substep<true>)) != TF_OK) { return rc; }
         if ((rc = allow((const void*)k_prepare)) != TF_OK) { return rc; }
-        if ((rc = allow((const void*)k_finish)) != TF_OK) { return rc; }
+        if ((rc = allow((const void*)k_finish<false>)) != TF_OK) { return rc; }
+        if ((rc = allow((const void*)k_finish<true>)) != TF_OK) { return rc; }
         done = true;
         return TF_OK;
     }
@@ -1141,7 +1364,8 @@ public:
         if (rc != TF_OK) { return rc; }
         const void* fns[kKernels] = { (const void*)k_broadphase, (const void*)k_narrowphase, (const void*)k_wake,
                                       (const void*)k_prepare,    (const void*)k_refresh<kClassAny>,
-                                      (const void*)k_substep,    (const void*)k_finish,
+                                      hasJoints ? (const void*)k_substep<true> : (const void*)k_substep<false>,
+                                      hasJoints ? (const void*)k_finish<true> : (const void*)k_finish<false>,
                                       (const void*)k_collide<kClassConvex> };
         for (int k = 0; k < kKernels; ++k) {
             LaunchShape& sh = shapes[k];
@@ -1272,6 +1496,7 @@ public:
                 const DBody& d = W.bodies[i].d;
                 const size_t g = info[k].bodyFirst + i;
                 if (d.alive && d.locks != 0) { return fail(TF_E_UNSUPPORTED, "tape: locked bodies are not differentiated"); }
+                if (!W.joints.empty()) { return fail(TF_E_UNSUPPORTED, "tape: joints are not differentiated"); }
                 dyn[g] = d.alive && d.type == kDynamic ? 1 : 0;
                 gs[g] = d.gravityScale;
                 ld[g] = d.linearDamping;
@@ -1376,6 +1601,7 @@ public:
         if ((rc = copyArray(S.counts, dCounts)) != TF_OK) { return rc; }
         if ((rc = copyArray(S.struck, dStruck)) != TF_OK) { return rc; }
         if ((rc = copyArray(S.wakeMark, dWakeMark)) != TF_OK) { return rc; }
+        if ((rc = copyArray(S.joints, dJoints)) != TF_OK) { return rc; }
         S.cur = cur;
         S.layoutGen = layoutGen;
         S.bodyStepsTotal = bodyStepsTotal;
@@ -1401,6 +1627,7 @@ public:
         if ((rc = copyArray(dCounts, S.counts)) != TF_OK) { return rc; }
         if ((rc = copyArray(dStruck, S.struck)) != TF_OK) { return rc; }
         if ((rc = copyArray(dWakeMark, S.wakeMark)) != TF_OK) { return rc; }
+        if ((rc = copyArray(dJoints, S.joints)) != TF_OK) { return rc; }
         bodyStepsTotal = S.bodyStepsTotal;
         bodyStepsBase = S.bodyStepsBase;
         hostFresh = false;
@@ -2088,6 +2315,21 @@ TF_API int tf_world_hit_events(void* h, int32_t w, tf_hit_event* out, int32_t ca
     }
     *count = (int32_t)ev.size();
     return TF_OK;
+}
+
+TF_API int tf_joint_create(void* h, int32_t w, const tf_joint_desc* desc, tf_id* out) {
+    if (!h) { return tfb::fail(TF_E_INVALID, "tf_joint_create: null world"); }
+    return E(h)->createJoint(w, desc, out);
+}
+
+TF_API int tf_joint_get_info(void* h, int32_t w, tf_id joint, tf_joint_info* out) {
+    if (!h) { return tfb::fail(TF_E_INVALID, "tf_joint_get_info: null world"); }
+    return E(h)->jointInfo(w, joint, out);
+}
+
+TF_API int tf_world_broken_joints(void* h, int32_t w, tf_id* out, int32_t cap, int32_t* count) {
+    if (!h) { return tfb::fail(TF_E_INVALID, "tf_world_broken_joints: null world"); }
+    return E(h)->brokenJoints(w, out, cap, count);
 }
 
 TF_API int tf_world_candidates(void* h, int32_t w, uint64_t* out, int32_t cap, int32_t* count) {

@@ -18,6 +18,7 @@
 
 #include "tf_batch.cuh"
 #include "tf_continuous.cuh"
+#include "tf_joint.cuh"
 #include "tf_planar.cuh"
 #include "tf_solver.cuh"
 #include "tf_tape.h"
@@ -224,6 +225,98 @@ __device__ __forceinline__ void emitCandidate(const Batch& B, const WorldInfo& w
 }
 
 // ---------------------------------------------------------------------------------------------------------
+// Joints outside the solve: the pairs they keep from colliding and the links they add for waking.
+
+// Whether a joint that does not collide its bodies holds bodies ga and gb (src/world.cpp:375-388).
+__device__ __forceinline__ bool joinedBodies(const Batch& B, const WorldInfo& wi, uint32_t ga, uint32_t gb) {
+    if (wi.joinedCount == 0) { return false; }
+    const uint32_t a = ga - wi.bodyFirst, b = gb - wi.bodyFirst;
+    const uint64_t key = ((uint64_t)(a < b ? a : b) << 32) | (uint64_t)(a < b ? b : a);
+    const uint64_t* keys = B.joined + wi.jointFirst;
+    uint32_t l = 0, h = wi.joinedCount;
+    while (l < h) {
+        const uint32_t mid = (l + h) >> 1;
+        if (keys[mid] < key) {
+            l = mid + 1;
+        } else {
+            h = mid;
+        }
+    }
+    return l < wi.joinedCount && keys[l] == key;
+}
+
+// Pushes onto a wake stack the sleeping dynamic bodies linked to body gb: by a pair whose contacts have points,
+// or by a joint that holds and is not joined to the world (src/world.cpp:655-700). Marks what it pushes.
+__device__ void pushLinked(const Batch& B, const WorldInfo& wi, uint32_t gb, const DContact* cs, uint32_t nc,
+                           uint32_t* stack, uint32_t& top) {
+    for (uint32_t ci = 0; ci < nc; ++ci) {
+        const DContact& c = cs[ci];
+        if (c.bodyA != gb && c.bodyB != gb) { continue; }
+        if (ci > 0 && cs[ci - 1].key == c.key) { continue; }  // one link per pair
+        const uint32_t other = c.bodyA == gb ? c.bodyB : c.bodyA;
+        const DBody& ob = B.bodies[other];
+        if (ob.type != kDynamic || ob.awake || B.wakeMark[other]) { continue; }
+        bool linked = false;
+        for (uint32_t k = ci; k < nc && cs[k].key == c.key; ++k) { linked = linked || cs[k].count > 0; }
+        if (linked && top < wi.bodyCount) {
+            B.wakeMark[other] = 1;
+            stack[top++] = other;
+        }
+    }
+    const DJoint* js = B.joints + wi.jointFirst;
+    for (uint32_t x = 0; x < wi.jointCount; ++x) {
+        const DJoint& j = js[x];
+        if (!j.alive || j.broken || j.bodyA == kWorldEnd || (j.bodyA != gb && j.bodyB != gb)) { continue; }
+        const uint32_t other = j.bodyA == gb ? j.bodyB : j.bodyA;
+        const DBody& ob = B.bodies[other];
+        if (ob.type != kDynamic || ob.awake || B.wakeMark[other]) { continue; }
+        if (top < wi.bodyCount) {
+            B.wakeMark[other] = 1;
+            stack[top++] = other;
+        }
+    }
+}
+
+// Wakes what a wake stack holds and everything linked to it (src/world.cpp:703-735).
+__device__ void wakeStack(const Batch& B, const WorldInfo& wi, const DContact* cs, uint32_t nc, uint32_t* stack,
+                          uint32_t top) {
+    while (top > 0) {
+        const uint32_t gb = stack[--top];
+        DBody& b = B.bodies[gb];
+        B.wakeMark[gb] = 0;
+        if (b.awake) { continue; }
+        b.awake = 1;
+        b.sleepTime = 0.0f;
+        updateInverseMass(b);
+        pushLinked(B, wi, gb, cs, nc, stack, top);
+    }
+}
+
+// At the start of a step a joint pulls its sleeping dynamic end awake when the other end moves
+// (src/world.cpp:1578-1585); runs on one thread, over the last step's contacts.
+__device__ void wakeJointPulled(const Batch& B, const WorldInfo& wi, const WorldCounts& wc) {
+    uint32_t* stack = B.unionParent + wi.bodyFirst;
+    uint32_t top = 0;
+    const DJoint* js = B.joints + wi.jointFirst;
+    auto moving = [&](uint32_t g) { return g != kWorldEnd && movingAwake(B.bodies[g]); };
+    auto pull = [&](uint32_t g) {
+        if (g == kWorldEnd) { return; }
+        const DBody& b = B.bodies[g];
+        if (b.alive && b.type == kDynamic && !b.awake && !B.wakeMark[g] && top < wi.bodyCount) {
+            B.wakeMark[g] = 1;
+            stack[top++] = g;
+        }
+    };
+    for (uint32_t x = 0; x < wi.jointCount; ++x) {
+        const DJoint& j = js[x];
+        if (!j.alive || j.broken) { continue; }
+        if (moving(j.bodyB)) { pull(j.bodyA); }
+        if (moving(j.bodyA)) { pull(j.bodyB); }
+    }
+    wakeStack(B, wi, B.previous + wi.contactFirst, min(wc.contactCount, wi.contactCap), stack, top);
+}
+
+// ---------------------------------------------------------------------------------------------------------
 // Broadphase (src/world.cpp:752-870).
 // A half-space against one body's shapes (src/world.cpp:844-867).
 __device__ void pairPlane(const Batch& B, const WorldInfo& wi, uint32_t gp, uint32_t gb, uint32_t* count) {
@@ -254,6 +347,7 @@ __device__ void pairPlane(const Batch& B, const WorldInfo& wi, uint32_t gp, uint
         const Vec3 g3a{ ga, ga, ga }, g3b{ gbb, gbb, gbb };
         if (!boxesOverlap(sp.lo - g3a, sp.hi + g3a, s.lo - g3b, s.hi + g3b)) { continue; }
         if (!(sp.category & s.mask) || !(s.category & sp.mask)) { continue; }
+        if (joinedBodies(B, wi, sp.body, s.body)) { continue; }
         emitCandidate(B, wi, count, pairKey(sp.index, s.index));
     }
 }
@@ -263,6 +357,7 @@ __device__ void pairPlane(const Batch& B, const WorldInfo& wi, uint32_t gp, uint
 __device__ void pairShapes(const Batch& B, const WorldInfo& wi, const DBody& ba, const DBody& bb, float gA, float gB,
                            const Vec3& loA, const Vec3& hiA, const Vec3& loB, const Vec3& hiB, const Vec3& reach,
                            uint32_t* count) {
+    if (joinedBodies(B, wi, (uint32_t)(&ba - B.bodies), (uint32_t)(&bb - B.bodies))) { return; }
     const Vec3 nearLoA = loB - reach, nearHiA = hiB + reach;
     const Vec3 nearLoB = loA - reach, nearHiB = hiA + reach;
     const Vec3 grownA{ gA, gA, gA }, grownB{ gB, gB, gB };
@@ -496,6 +591,10 @@ __global__ void __launch_bounds__(kMaxBlock) k_broadphase(const __grid_constant_
         WorldCounts& wc = B.counts[w];
         const uint32_t n = wi.bodyCount;
         const bool useStage = n <= stageN;
+        if (wi.jointCount > 0) {
+            if (g.tid == 0) { wakeJointPulled(B, wi, wc); }
+            g.sync();
+        }
         if (g.tid == 0) { s_count[g.id] = 0; }
         // Growth by the speculative distance and the travel over the step (src/world.cpp:754-765).
         for (uint32_t i = g.tid; i < n; i += g.size) {
@@ -1240,31 +1339,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_wake(const __grid_constant__ Batc
                 B.wakeMark[gb] = 0;
             }
         }
-        const DContact* cs = B.contacts + wi.contactFirst;
-        const uint32_t nc = wc.nextContactCount;
-        while (top > 0) {
-            const uint32_t gb = stack[--top];
-            DBody& b = B.bodies[gb];
-            B.wakeMark[gb] = 0;
-            if (b.awake) { continue; }
-            b.awake = 1;
-            b.sleepTime = 0.0f;
-            updateInverseMass(b);
-            for (uint32_t ci = 0; ci < nc; ++ci) {
-                const DContact& c = cs[ci];
-                if (c.bodyA != gb && c.bodyB != gb) { continue; }
-                if (ci > 0 && cs[ci - 1].key == c.key) { continue; }  // one link per pair
-                const uint32_t other = c.bodyA == gb ? c.bodyB : c.bodyA;
-                const DBody& ob = B.bodies[other];
-                if (ob.type != kDynamic || ob.awake || B.wakeMark[other]) { continue; }
-                bool linked = false;
-                for (uint32_t k = ci; k < nc && cs[k].key == c.key; ++k) { linked = linked || cs[k].count > 0; }
-                if (linked && top < wi.bodyCount) {
-                    B.wakeMark[other] = 1;
-                    stack[top++] = other;
-                }
-            }
-        }
+        wakeStack(B, wi, B.contacts + wi.contactFirst, wc.nextContactCount, stack, top);
     });
 }
 
@@ -1368,6 +1443,17 @@ __global__ void __launch_bounds__(kMaxBlock) k_prepare(const __grid_constant__ B
             updateInverseMass(b);
         }
         g.sync();
+        // Joints: what the step will report for them starts over (src/world.cpp:1647).
+        for (uint32_t x = g.tid; x < wi.jointCount; x += g.size) {
+            DJoint& j = B.joints[wi.jointFirst + x];
+            j.brokeNow = 0;
+            const JBody a = j.bodyA == kWorldEnd ? worldEnd() : jointBodyOf(B.bodies[j.bodyA]);
+            const JBody b = jointBodyOf(B.bodies[j.bodyB]);
+            if (jointActive(j, a, b)) {
+                j.force = zero3();
+                j.torque = zero3();
+            }
+        }
         const uint32_t cf = wi.contactFirst;
         DContact* cs = B.contacts + cf;
         const uint32_t nActive = groupCompact(
@@ -1849,8 +1935,72 @@ __global__ void __launch_bounds__(256) k_refresh(const __grid_constant__ Batch B
     }
 }
 
+// One pass over a world's joints on one thread, before the contacts of that pass (src/world.cpp:1670-1680,
+// src/joint.cpp:568-590): kind 0 scales warm starts by the speed the ends kept under the speed limits
+// (src/joint.cpp:570-593) and warm starts, 1 is the biased solve, 2 the relaxing solve with its reaction. The
+// ends' velocities come from the substep's store.
+__device__ void runJoints(const Batch& B, const StepParams& P, const WorldInfo& wi, const SolverStore& st,
+                                       int kind) {
+    const uint32_t nj = wi.jointCount;
+    DJoint* js = B.joints + wi.jointFirst;
+    auto endOf = [&](uint32_t gbody) {
+        if (gbody == kWorldEnd) { return worldEnd(); }
+        JBody e = jointBodyOf(B.bodies[gbody]);
+        if (st.staged) {
+            const LanedBody l = st.loadLaned(gbody - wi.bodyFirst);
+            e.v = l.v;
+            e.w = l.w;
+        }
+        return e;
+    };
+    auto putEnd = [&](uint32_t gbody, const JBody& e) {
+        if (gbody == kWorldEnd || e.type != kDynamic || !e.awake) { return; }
+        st.storeVW(gbody - wi.bodyFirst, e);
+    };
+    if (kind == 0) {
+        for (uint32_t x = 0; x < nj; ++x) {
+            DJoint& j = js[x];
+            const JBody a = endOf(j.bodyA), b = endOf(j.bodyB);
+            if (!jointActive(j, a, b)) { continue; }
+            const float f = minf(a.kept, b.kept);
+            if (f >= 1.0f) { continue; }
+            j.linearImpulse = j.linearImpulse * f;
+            j.angularImpulse = j.angularImpulse * f;
+            j.frictionTurn = j.frictionTurn * f;
+            j.axialImpulse *= f;
+            j.motorImpulse *= f;
+            j.lowerImpulse *= f;
+            j.upperImpulse *= f;
+            j.frictionImpulse *= f;
+            j.swingImpulse *= f;
+        }
+        for (uint32_t x = 0; x < nj; ++x) {
+            const DJoint& j = js[x];
+            if (!jointActive(j, endOf(j.bodyA), endOf(j.bodyB))) { continue; }
+            if (j.bodyA != kWorldEnd) { B.bodies[j.bodyA].kept = 1.0f; }
+            B.bodies[j.bodyB].kept = 1.0f;
+        }
+    }
+    for (uint32_t x = 0; x < nj; ++x) {
+        DJoint& j = js[x];
+        JBody a = endOf(j.bodyA), b = endOf(j.bodyB);
+        if (!jointActive(j, a, b)) { continue; }
+        if (kind == 0) {
+            warmStartJoint(a, b, j);
+        } else {
+            solveJoint(a, b, j, P, P.jointSoft, kind == 1);
+            if (kind == 2) { addReaction(j); }
+        }
+        putEnd(j.bodyA, a);
+        putEnd(j.bodyB, b);
+    }
+}
+
 // Integrate velocities, warm start, biased solve, integrate positions, relax (src/world.cpp:1669-1680). The
 // world's solver state is staged in the group's shared slice when it has at most stageN bodies.
+// Joints is false for batches without joints: that instantiation carries no joint code, which would cost the
+// contact solve registers.
+template <bool Joints>
 __global__ void __launch_bounds__(kMaxBlock) k_substep(const __grid_constant__ Batch B, const __grid_constant__ StepParams P, const __grid_constant__ Split sp, int sub, int serial) {
     extern __shared__ __align__(16) unsigned char s_raw[];
     if (stepAborted(B, serial)) { return; }
@@ -1881,6 +2031,13 @@ __global__ void __launch_bounds__(kMaxBlock) k_substep(const __grid_constant__ B
         }
         for (uint32_t i = g.tid; i < nb; i += g.size) { st.integrateVelocityAt(i, P); }
         g.sync();
+        const uint32_t nj = wi.jointCount;
+        if constexpr (Joints) {
+            if (nj > 0) {
+                if (g.tid == 0) { runJoints(B, P, wi, st, 0); }
+                g.sync();
+            }
+        }
         const uint32_t base = wi.bodyFirst;
         const Axis* axes = B.axes + (size_t)cf * kAxesPerContact;
         // A laned contact's bodies are stored only where they move, so a static body shared by a color's
@@ -1930,6 +2087,12 @@ __global__ void __launch_bounds__(kMaxBlock) k_substep(const __grid_constant__ B
         g.sync();
         for (int pass = 0; pass < 2; ++pass) {
             const bool bias = pass == 0;
+            if constexpr (Joints) {
+                if (nj > 0) {
+                    if (g.tid == 0) { runJoints(B, P, wi, st, bias ? 1 : 2); }
+                    g.sync();
+                }
+            }
             forEachColor(g, colored, wc.colorStart, wc.colorCount, [&](uint32_t ci) { solve(ci, bias, true); });
             if (g.tid == 0) {
                 for (uint32_t x = 0; x < wc.restCount; ++x) { solve(rest[x], bias, false); }
@@ -2070,6 +2233,7 @@ __device__ void sweepWorld(const Batch& B, const StepParams& P, const Group& g, 
         const DShape& o = B.shapes[sf + oi];
         if (!o.alive || o.sensor || o.body == f.body) { continue; }
         if (!TF_OK_INDEX(B, o.body - bf < nb, 33, bf, oi)) { continue; }
+        if (joinedBodies(B, wi, o.body, f.body)) { continue; }
         if (!boxesOverlap(B.sweptLo[sf + fi], B.sweptHi[sf + fi], B.sweptLo[sf + oi], B.sweptHi[sf + oi])) { continue; }
         if (!(f.category & o.mask) || !(o.category & f.mask)) { continue; }
         atomicAdd(pairs, 1u);
@@ -2117,6 +2281,59 @@ __device__ void sweepWorld(const Batch& B, const StepParams& P, const Group& g, 
 
 // Union-find is staged in the group's shared slice (parent and island time by body, union pairs by contact)
 // when the world fits, else in its global scratch.
+// After the solve (src/world.cpp:1685-1691): active joints turn the step's impulses into a force and torque
+// and break past their limits (src/world.cpp:1543-1560), the rest settle positions in order, twice over, and
+// every awake dynamic body's world inverse mass is built again at its settled pose. One thread runs the
+// joints; every thread first finds whether any joint was active.
+__device__ void finishJoints(const Batch& B, const StepParams& P, const Group& g, const WorldInfo& wi) {
+    DJoint* js = B.joints + wi.jointFirst;
+    auto endOf = [&](uint32_t gbody) { return gbody == kWorldEnd ? worldEnd() : jointBodyOf(B.bodies[gbody]); };
+    bool anyActive = false;
+    for (uint32_t x = 0; x < wi.jointCount && !anyActive; ++x) {
+        anyActive = jointActive(js[x], endOf(js[x].bodyA), endOf(js[x].bodyB));
+    }
+    g.sync();
+    if (!anyActive) { return; }
+    if (g.tid == 0) {
+        for (uint32_t x = 0; x < wi.jointCount; ++x) {
+            DJoint& j = js[x];
+            if (!jointActive(j, endOf(j.bodyA), endOf(j.bodyB))) { continue; }
+            j.force = j.force / P.dt;
+            j.torque = j.torque / P.dt;
+            if (length(j.force) > j.breakForce || length(j.torque) > j.breakTorque) {
+                j.broken = 1;
+                j.brokeNow = 1;
+                j.linearImpulse = zero3();
+                j.angularImpulse = zero3();
+                j.frictionTurn = zero3();
+                j.axialImpulse = j.motorImpulse = j.lowerImpulse = j.upperImpulse = 0.0f;
+                j.frictionImpulse = j.swingImpulse = 0.0f;
+            }
+        }
+        auto putPose = [&](uint32_t gbody, const JBody& e) {
+            if (gbody == kWorldEnd || e.type != kDynamic || !e.awake) { return; }
+            B.bodies[gbody].com = e.com;
+            B.bodies[gbody].xf = e.xf;
+        };
+        for (int it = 0; it < kSettleIterations; ++it) {
+            for (uint32_t x = 0; x < wi.jointCount; ++x) {
+                const DJoint& j = js[x];
+                JBody a = endOf(j.bodyA), b = endOf(j.bodyB);
+                if (!jointActive(j, a, b)) { continue; }
+                settleJoint(a, b, j);
+                putPose(j.bodyA, a);
+                putPose(j.bodyB, b);
+            }
+        }
+    }
+    g.sync();
+    for (uint32_t i = g.tid; i < wi.bodyCount; i += g.size) {
+        DBody& b = B.bodies[wi.bodyFirst + i];
+        if (b.alive && b.type == kDynamic && b.awake) { updateInverseMass(b); }
+    }
+    g.sync();
+}
+
 // Counts the touching contacts, reports the pairs that began or stopped touching and the fastest struck point
 // of each touching pair (src/world.cpp:1424-1468). The first contact of each pair walks the pair's contacts:
 // a pair touches where the solver pushed on a point or a point overlaps (by more than the linear slop once it
@@ -2181,6 +2398,7 @@ __device__ void reportTouches(const Batch& B, const StepParams& P, const Group& 
     if (touchingHere > 0) { atomicAdd(&wc.touching, touchingHere); }
 }
 
+template <bool Joints>
 __global__ void __launch_bounds__(kMaxBlock) k_finish(const __grid_constant__ Batch B, const __grid_constant__ StepParams P, const __grid_constant__ Split sp, int serial) {
     extern __shared__ __align__(16) unsigned char s_raw[];
     __shared__ uint32_t s_awake[kMaxGroups], s_islands[kMaxGroups], s_sweep[kMaxGroups], s_pairs[kMaxGroups],
@@ -2213,6 +2431,9 @@ __global__ void __launch_bounds__(kMaxBlock) k_finish(const __grid_constant__ Ba
             }
         }
         g.sync();
+        if constexpr (Joints) {
+            if (wi.jointCount > 0) { finishJoints(B, P, g, wi); }
+        }
         reportTouches(B, P, g, wi, wc);
         g.sync();
         const uint32_t nc = wc.contactCount;
@@ -2298,6 +2519,24 @@ __global__ void __launch_bounds__(kMaxBlock) k_finish(const __grid_constant__ Ba
                 if (!TF_OK_INDEX(B, uA[x] < wi.bodyCount && uB[x] < wi.bodyCount, 24, w, x)) { continue; }
                 const uint32_t ra = findRoot(parent, uA[x]), rb = findRoot(parent, uB[x]);
                 if (ra != rb) { parent[ra > rb ? ra : rb] = ra < rb ? ra : rb; }
+            }
+            // Joints that hold link their bodies too (src/world.cpp:1210-1222).
+            const DJoint* js = B.joints + wi.jointFirst;
+            for (uint32_t x = 0; x < wi.jointCount; ++x) {
+                const DJoint& j = js[x];
+                if (!j.alive || j.broken) { continue; }
+                DBody* a = j.bodyA == kWorldEnd ? nullptr : &B.bodies[j.bodyA];
+                DBody& b = B.bodies[j.bodyB];
+                const bool da = a && a->type == kDynamic && a->awake;
+                const bool db = b.type == kDynamic && b.awake;
+                if (da && db) {
+                    const uint32_t ra = findRoot(parent, j.bodyA - wi.bodyFirst), rb = findRoot(parent, j.bodyB - wi.bodyFirst);
+                    if (ra != rb) { parent[ra > rb ? ra : rb] = ra < rb ? ra : rb; }
+                } else if (da && b.type == kKinematic && movingAwake(b)) {
+                    a->sleepTime = 0.0f;
+                } else if (db && a && a->type == kKinematic && movingAwake(*a)) {
+                    b.sleepTime = 0.0f;
+                }
             }
         }
         g.sync();

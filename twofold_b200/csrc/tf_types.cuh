@@ -204,6 +204,30 @@ struct WorldInfo {
     // pairs ruled out (boundsFirst, boundsCap: triangle bounds). Zero capacity in worlds without meshes.
     uint32_t partFirst, partCap;
     uint32_t boundsFirst, boundsCap;
+    // Joints from jointFirst in the world's index order, and the body pairs that joints keep from colliding
+    // (sorted keys min << 32 | max of world-local bodies) from the same offset.
+    uint32_t jointFirst, jointCount, joinedCount;
+};
+
+enum JointType : uint32_t { kJointPoint = 0, kJointFixed, kJointHinge, kJointSlider, kJointDistance, kJointSwingTwist };
+// A joint's end that is the world: a static body at the origin.
+constexpr uint32_t kWorldEnd = UINT32_MAX;
+
+// A joint (src/internal.h:508-548): its ends (global body indices, kWorldEnd for the world), its frames in
+// each body, limits, motor, spring and friction, and the impulses it keeps between substeps and steps.
+struct alignas(16) DJoint {
+    uint32_t type, alive, broken, limited;
+    uint32_t bodyA, bodyB;
+    uint32_t collideConnected, brokeNow;  // brokeNow: broke in the current step
+    Vec3 localA, localB, axisA, axisB, refA, refB;
+    Quat restTurn, frameA, frameB;
+    float length, lower, upper, motorSpeed, maxMotor, hertz, dampingRatio, maxFriction;
+    float swingY, swingZ, breakForce, breakTorque;
+    Vec3 linearImpulse, angularImpulse;
+    float axialImpulse, motorImpulse, lowerImpulse, upperImpulse, frictionImpulse, swingImpulse;
+    Vec3 frictionTurn;
+    Vec3 rowForce[2], rowTorque[2];
+    Vec3 force, torque;
 };
 
 // Per-world results and lists of the current step.
@@ -297,6 +321,7 @@ struct StepParams {
     Tolerances tol;
     int continuous;
     float hitThreshold;     // scaled
+    Softness jointSoft;     // src/world.cpp:1640
 };
 
 }

@@ -55,6 +55,8 @@ class World:
         self.body_of = np.ascontiguousarray(body_of, dtype=np.uint32)
         self.meta = meta or {}
         self.keepalive = []
+        # Joints as tf_joint_desc, created after the bodies and shapes; body ids are positions in `bodies`.
+        self.joints = []
         # TriangleMeshes as (vertices (n, 3), indices (3 m,)); a TF_MESH shape's "mesh" is a position here.
         self.meshes = []
 
@@ -541,6 +543,106 @@ def config3():
     """Planar pile: 16,384 bodies locked to the z = 0 plane in a static box container, with 256 free spheres
     dropped among them, 600 steps."""
     return Scene("planar_16384", [planar()], steps=600)
+
+
+def jointed(seed=0):
+    """Every joint kind in one world over a half-space, each with its limits, motor, spring or friction: a
+    swinging chain of point joints from the world, a limited door with hinge friction, a hinge motor driving a
+    paddle off a kinematic body that moves, a limited slider with a motor and a tilted one with friction, a
+    spring, a rod and a rope with distance limits (one end on a body with locked rotation), a fixed pair that
+    falls and comes to rest (its two boxes touch but do not collide), a swing-twist chain with cone and twist
+    limits, two joints that break under load, and loose boxes dropped onto the chain and the door. Seeded
+    jitter moves every body and anchor."""
+    rng = np.random.default_rng(seed)
+    b, s, joints = [], [], []
+
+    def body(pos, half=(0.2, 0.2, 0.2), type=abi.TF_DYNAMIC, vel=(0, 0, 0), spin=(0, 0, 0), density=1.0, locks=0,
+             rot=None, geometry=abi.TF_BOX, radius=0.25):
+        bd = _bodies(1)
+        bd["type"][0] = type
+        bd["position"][0] = np.asarray(pos, np.float32) + rng.uniform(-0.02, 0.02, 3).astype(np.float32)
+        if rot is not None:
+            bd["rotation"][0] = rot
+        bd["linear_velocity"][0] = vel
+        bd["angular_velocity"][0] = spin
+        bd["locks"][0] = locks
+        sd = _shapes(1)
+        sd["geometry"][0] = geometry
+        sd["half_extents"][0] = half
+        sd["radius"][0] = radius
+        sd["density"][0] = density
+        sd["friction"][0] = 0.5
+        b.append(bd)
+        s.append(sd)
+        return len(b) - 1
+
+    def joint(type, bb, ba=None, **kw):
+        kw = dict(kw)
+        for k in ("anchor", "anchor_b"):
+            if k in kw:
+                kw[k] = tuple(np.asarray(kw[k], np.float32) + rng.uniform(-0.01, 0.01, 3).astype(np.float32))
+        joints.append((type, ba, bb, kw))
+
+    ground = body((0, 0, 0), type=abi.TF_STATIC)
+    # A chain of point joints, held out sideways from a world anchor so that it swings.
+    prev = None
+    for i in range(6):
+        k = body((-6.0 + 0.45 * (i + 1), 6.0, 0.0), half=(0.2, 0.1, 0.1))
+        joint(abi.TF_JOINT_POINT, k, prev, anchor=(-6.0 + 0.45 * i + 0.225, 6.0, 0.0))
+        prev = k
+    # A door on a limited hinge about y with friction, pushed open.
+    door = body((-2.0, 1.2, 0.55), half=(0.05, 1.0, 0.5), spin=(0, 3.0, 0))
+    joint(abi.TF_JOINT_HINGE, door, anchor=(-2.0, 1.2, 0.05), axis=(0, 1, 0), limited=1, lower=-0.8, upper=0.6,
+          friction=0.5)
+    # A paddle driven by a hinge motor off a kinematic body that moves along z.
+    hub = body((1.0, 2.0, 0.0), half=(0.1, 0.1, 0.1), type=abi.TF_KINEMATIC, vel=(0, 0, 0.5))
+    paddle = body((1.0, 2.0, 0.6), half=(0.05, 0.05, 0.5))
+    joint(abi.TF_JOINT_HINGE, paddle, hub, anchor=(1.0, 2.0, 0.0), axis=(1, 0, 0), motor_speed=2.0, max_motor=30.0)
+    # Sliders: limited with a motor, and tilted with friction.
+    sl = body((3.0, 1.5, 0.0), half=(0.25, 0.15, 0.15))
+    joint(abi.TF_JOINT_SLIDER, sl, anchor=(3.0, 1.5, 0.0), axis=(1, 0, 0), limited=1, lower=-0.5, upper=0.7,
+          motor_speed=1.0, max_motor=20.0)
+    tilt = body((5.0, 2.0, 0.0), half=(0.2, 0.2, 0.2))
+    joint(abi.TF_JOINT_SLIDER, tilt, anchor=(5.0, 2.0, 0.0), axis=(0.6, -0.8, 0.0), friction=1.5)
+    # Distance joints: a spring from the world, a rod between two boxes, a rope with limits to a body whose
+    # rotation is locked.
+    spring = body((7.0, 3.0, 0.0))
+    joint(abi.TF_JOINT_DISTANCE, spring, anchor=(7.0, 4.5, 0.0), anchor_b=(7.0, 3.2, 0.0), hertz=2.0,
+          damping_ratio=0.3)
+    r1 = body((9.0, 3.0, 0.0), vel=(0, 0, 1.0))
+    r2 = body((9.8, 3.0, 0.0))
+    joint(abi.TF_JOINT_DISTANCE, r2, r1, anchor=(9.0, 3.0, 0.0), anchor_b=(9.8, 3.0, 0.0))
+    rope = body((11.0, 2.5, 0.0), locks=(1 << 3) | (1 << 4) | (1 << 5))
+    joint(abi.TF_JOINT_DISTANCE, rope, anchor=(11.0, 4.0, 0.0), anchor_b=(11.0, 2.7, 0.0), limited=1, lower=0.5,
+          upper=1.6, length=1.0)
+    # A fixed pair, touching but not colliding, falling to rest.
+    f1 = body((13.0, 1.0, 0.0), half=(0.3, 0.3, 0.3))
+    f2 = body((13.55, 1.1, 0.0), half=(0.25, 0.25, 0.25), spin=(0, 0, 1.0))
+    joint(abi.TF_JOINT_FIXED, f2, f1, anchor=(13.3, 1.05, 0.0))
+    # A swing-twist chain with cone and twist limits and friction.
+    prev = None
+    for i in range(3):
+        k = body((15.0, 5.0 - 0.6 * (i + 1), 0.0), half=(0.1, 0.25, 0.1), spin=(1.0, 0.5, 2.0))
+        joint(abi.TF_JOINT_SWING_TWIST, k, prev, anchor=(15.0, 5.0 - 0.6 * i - 0.3, 0.0), axis=(0, -1, 0),
+              normal=(1, 0, 0), swing_y=0.5, swing_z=0.3, lower=-0.3, upper=0.3, friction=0.05)
+        prev = k
+    # Joints that break under load: a point joint with a small force limit, a fixed joint with a torque limit.
+    heavy = body((17.0, 3.0, 0.0), density=8.0)
+    joint(abi.TF_JOINT_POINT, heavy, anchor=(17.0, 3.2, 0.0), break_force=4.9)
+    lever = body((18.5, 3.0, 0.0), half=(0.6, 0.1, 0.1))
+    joint(abi.TF_JOINT_FIXED, lever, anchor=(18.0, 3.0, 0.0), break_torque=0.2)
+    # Loose boxes dropped onto the chain and onto the door.
+    for x, y in ((-4.8, 8.0), (-2.3, 3.5), (-5.2, 9.5)):
+        body((x, y, 0.0), half=(0.15, 0.15, 0.15))
+    bodies, shapes = _bodies(len(b)), _shapes(len(s))
+    for i in range(len(b)):
+        bodies[i] = b[i][0]
+        shapes[i] = s[i][0]
+    _ground(bodies, shapes)
+    w = World(bodies, shapes, np.arange(len(bodies)))
+    for type, ba, bb, kw in joints:
+        w.joints.append(abi.joint_desc(type, abi.tf_id(bb, 0), None if ba is None else abi.tf_id(ba, 0), **kw))
+    return w
 
 
 def single(kind="box_on_ground", **kw):

@@ -35,6 +35,8 @@ class Batch:
             world_of = np.full(ns, wi, np.int32)
             abi.check(self.lib.tf_shapes_add(self.h, ns, world_of.ctypes.data, w.body_of.ctypes.data,
                                              shapes.ctypes.data_as(C.POINTER(abi.tf_shape_desc)), None), self.lib)
+            for j in getattr(w, "joints", []):
+                self.joint_create(wi, j)
             self.body_counts.append(nb)
         self.offsets = np.concatenate([[0], np.cumsum(self.body_counts)]).astype(np.int64)
 
@@ -110,6 +112,23 @@ class Batch:
         arr = (abi.tf_contact * max(n.value, 1))()
         abi.check(self.lib.tf_world_contacts(self.h, wi, mode, arr, n.value, C.byref(n)), self.lib)
         return list(arr)[:n.value]
+
+    def joint_create(self, wi, desc):
+        out = abi.tf_id()
+        abi.check(self.lib.tf_joint_create(self.h, wi, C.byref(desc), C.byref(out)), self.lib)
+        return out
+
+    def joint_info(self, wi, joint):
+        info = abi.tf_joint_info()
+        abi.check(self.lib.tf_joint_get_info(self.h, wi, joint, C.byref(info)), self.lib)
+        return info
+
+    def broken_joints(self, wi=0):
+        n = C.c_int32(0)
+        abi.check(self.lib.tf_world_broken_joints(self.h, wi, None, 0, C.byref(n)), self.lib)
+        arr = (abi.tf_id * max(n.value, 1))()
+        abi.check(self.lib.tf_world_broken_joints(self.h, wi, arr, n.value, C.byref(n)), self.lib)
+        return [(x.index, x.generation) for x in list(arr)[:n.value]]
 
     def contact_events(self, wi=0):
         """World::contactEvents of world wi's last step: (shape_a, shape_b, body_a, body_b, begin) tuples."""
