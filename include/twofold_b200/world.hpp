@@ -4,7 +4,7 @@
 // StepProfile, ContactInfo, the id types and geometry alternatives) compiles against this header for the
 // part of the API the contact pipeline covers: building bodies and shapes, step(), reading poses,
 // velocities, mass, sleep state, contacts, contact and hit events and the step profile, setting velocities
-// and adding forces.
+// and adding forces, and joints (creating them, their info, the joints that broke).
 // Every call forwards to the C ABI in twofold_b200.h; the library owns the device state.
 //
 // Same conventions as the reference (include/twofold/world.h:362-510, src/world.cpp:352-371): invalid ids
@@ -244,6 +244,91 @@ struct ContactInfo {
     float separations[4] = {};
     float normalImpulses[4] = {};
     Vec3 tangentImpulses[4];
+};
+
+struct JointId {
+    uint32_t index = UINT32_MAX;
+    uint32_t generation = 0;
+    bool operator==(const JointId& b) const { return index == b.index && generation == b.generation; }
+    bool operator!=(const JointId& b) const { return !(*this == b); }
+};
+
+// Anchors and axes are in world space, at the poses the bodies have when the joint is made.
+struct PointJoint {
+    Vec3 anchor;
+};
+struct FixedJoint {
+    Vec3 anchor;
+};
+struct HingeJoint {
+    Vec3 anchor;
+    Vec3 axis{ 0, 0, 1 };
+    bool limited = false;
+    float lowerAngle = 0.0f;
+    float upperAngle = 0.0f;
+    float motorSpeed = 0.0f;
+    float maxMotorTorque = 0.0f;
+    float frictionTorque = 0.0f;
+};
+struct SliderJoint {
+    Vec3 anchor;
+    Vec3 axis{ 1, 0, 0 };
+    bool limited = false;
+    float lowerTranslation = 0.0f;
+    float upperTranslation = 0.0f;
+    float motorSpeed = 0.0f;
+    float maxMotorForce = 0.0f;
+    float frictionForce = 0.0f;
+};
+struct DistanceJoint {
+    Vec3 anchorA;
+    Vec3 anchorB;
+    float length = -1.0f;
+    float hertz = 0.0f;
+    float dampingRatio = 0.0f;
+    bool limited = false;
+    float minDistance = 0.0f;
+    float maxDistance = 0.0f;
+};
+struct SwingTwistJoint {
+    Vec3 anchor;
+    Vec3 axis{ 1, 0, 0 };
+    Vec3 normal{ 0, 1, 0 };
+    float swingY = 3.14159265f;
+    float swingZ = 3.14159265f;
+    float lowerTwist = -3.14159265f;
+    float upperTwist = 3.14159265f;
+    float frictionTorque = 0.0f;
+};
+
+using JointKind = std::variant<PointJoint, FixedJoint, HingeJoint, SliderJoint, DistanceJoint, SwingTwistJoint>;
+enum class JointType : uint8_t { Point, Fixed, Hinge, Slider, Distance, SwingTwist };
+
+struct JointDesc {
+    // Left unset, body B is joined to the world.
+    BodyId bodyA;
+    BodyId bodyB;
+    JointKind kind = PointJoint{};
+    bool collideConnected = false;
+    float breakForce = INFINITY;
+    float breakTorque = INFINITY;
+    void* userData = nullptr;
+};
+
+struct JointInfo {
+    JointId joint;
+    JointType type = JointType::Point;
+    BodyId bodyA;
+    BodyId bodyB;
+    Vec3 anchorA;
+    Vec3 anchorB;
+    Vec3 axis;
+    // The hinge angle, slider translation, distance or twist. Zero for point and fixed joints.
+    float value = 0.0f;
+    // Force and torque on body B in the last step the joint was active, the torque about anchor B.
+    Vec3 force;
+    Vec3 torque;
+    bool broken = false;
 };
 
 // Two shapes that started or stopped touching. Shape A has the lower index.
@@ -526,6 +611,100 @@ public:
         return out;
     }
 
+    // Joints (tf_joint_create, tf_joint_get_info, tf_world_broken_joints). createJoint returns an invalid id
+    // for bad bodies, as the reference does, and for what the C ABI refuses (status() tells which).
+    JointId createJoint(const JointDesc& d) {
+        tf_joint_desc c{};
+        c.body_a = d.bodyA.index == UINT32_MAX ? tf_id{ UINT32_MAX, 0 } : tf_id{ d.bodyA.index, d.bodyA.generation };
+        c.body_b = tf_id{ d.bodyB.index, d.bodyB.generation };
+        c.collide_connected = d.collideConnected ? 1 : 0;
+        c.break_force = d.breakForce;
+        c.break_torque = d.breakTorque;
+        c.length = -1.0f;
+        auto put = [](float* o, const Vec3& v) { o[0] = v.x, o[1] = v.y, o[2] = v.z; };
+        if (const PointJoint* k = std::get_if<PointJoint>(&d.kind)) {
+            c.type = TF_JOINT_POINT;
+            put(c.anchor, k->anchor);
+        } else if (const FixedJoint* k = std::get_if<FixedJoint>(&d.kind)) {
+            c.type = TF_JOINT_FIXED;
+            put(c.anchor, k->anchor);
+        } else if (const HingeJoint* k = std::get_if<HingeJoint>(&d.kind)) {
+            c.type = TF_JOINT_HINGE;
+            put(c.anchor, k->anchor);
+            put(c.axis, k->axis);
+            c.limited = k->limited ? 1 : 0;
+            c.lower = k->lowerAngle;
+            c.upper = k->upperAngle;
+            c.motor_speed = k->motorSpeed;
+            c.max_motor = k->maxMotorTorque;
+            c.friction = k->frictionTorque;
+        } else if (const SliderJoint* k = std::get_if<SliderJoint>(&d.kind)) {
+            c.type = TF_JOINT_SLIDER;
+            put(c.anchor, k->anchor);
+            put(c.axis, k->axis);
+            c.limited = k->limited ? 1 : 0;
+            c.lower = k->lowerTranslation;
+            c.upper = k->upperTranslation;
+            c.motor_speed = k->motorSpeed;
+            c.max_motor = k->maxMotorForce;
+            c.friction = k->frictionForce;
+        } else if (const DistanceJoint* k = std::get_if<DistanceJoint>(&d.kind)) {
+            c.type = TF_JOINT_DISTANCE;
+            put(c.anchor, k->anchorA);
+            put(c.anchor_b, k->anchorB);
+            c.length = k->length;
+            c.hertz = k->hertz;
+            c.damping_ratio = k->dampingRatio;
+            c.limited = k->limited ? 1 : 0;
+            c.lower = k->minDistance;
+            c.upper = k->maxDistance;
+        } else if (const SwingTwistJoint* k = std::get_if<SwingTwistJoint>(&d.kind)) {
+            c.type = TF_JOINT_SWING_TWIST;
+            put(c.anchor, k->anchor);
+            put(c.axis, k->axis);
+            put(c.normal, k->normal);
+            c.swing_y = k->swingY;
+            c.swing_z = k->swingZ;
+            c.lower = k->lowerTwist;
+            c.upper = k->upperTwist;
+            c.friction = k->frictionTorque;
+        }
+        tf_id id{};
+        if (!note(tf_joint_create(handle_, 0, &c, &id))) { return {}; }
+        if (joints_.size() <= id.index) { joints_.resize((size_t)id.index + 1); }
+        joints_[id.index] = JointId{ id.index, id.generation };
+        return joints_[id.index];
+    }
+    bool isValid(JointId joint) const { return joint.index < joints_.size() && joints_[joint.index] == joint; }
+    JointInfo jointInfo(JointId joint) const {
+        JointInfo info;
+        if (!isValid(joint)) { return info; }
+        tf_joint_info raw{};
+        if (!note(tf_joint_get_info(handle_, 0, tf_id{ joint.index, joint.generation }, &raw))) { return info; }
+        info.joint = joint;
+        info.type = (JointType)raw.type;
+        if (raw.body_a != UINT32_MAX) { info.bodyA = bodyAt(raw.body_a); }
+        info.bodyB = bodyAt(raw.body_b);
+        info.anchorA = Vec3{ raw.anchor_a[0], raw.anchor_a[1], raw.anchor_a[2] };
+        info.anchorB = Vec3{ raw.anchor_b[0], raw.anchor_b[1], raw.anchor_b[2] };
+        info.axis = Vec3{ raw.axis[0], raw.axis[1], raw.axis[2] };
+        info.value = raw.value;
+        info.force = Vec3{ raw.force[0], raw.force[1], raw.force[2] };
+        info.torque = Vec3{ raw.torque[0], raw.torque[1], raw.torque[2] };
+        info.broken = raw.broken != 0;
+        return info;
+    }
+    // Joints that broke in the last step, in index order.
+    std::vector<JointId> brokenJoints() const {
+        std::vector<JointId> out;
+        int32_t n = 0;
+        if (!note(tf_world_broken_joints(handle_, 0, nullptr, 0, &n)) || n == 0) { return out; }
+        std::vector<tf_id> raw((size_t)n);
+        if (!note(tf_world_broken_joints(handle_, 0, raw.data(), n, &n))) { return out; }
+        for (const tf_id& id : raw) { out.push_back(JointId{ id.index, id.generation }); }
+        return out;
+    }
+
     // Events of the last step, ordered by shape index (tf_world_contact_events, tf_world_hit_events).
     const std::vector<ContactEvent>& contactEvents() const {
         contactEvents_.clear();
@@ -634,6 +813,7 @@ private:
     StepProfile profile_;
     std::vector<BodyId> bodies_;
     std::vector<ShapeId> shapes_;
+    std::vector<JointId> joints_;
     std::vector<float> forces_, torques_;
     std::map<const TriangleMesh*, int32_t> meshIds_;           // meshes this handle has built, by mesh
     std::vector<std::shared_ptr<const TriangleMesh>> meshes_;  // kept alive while their ids are in use

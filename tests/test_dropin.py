@@ -15,12 +15,14 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 PROGRAM = os.path.join(HERE, "dropin", "pyramid_step.cpp")
 GOLDEN = os.path.join(HERE, "golden", "dropin_pyramid.txt")
+JOINTS_PROGRAM = os.path.join(HERE, "dropin", "joints_step.cpp")
+JOINTS_GOLDEN = os.path.join(HERE, "golden", "dropin_joints.txt")
 TOL = 1e-5
 
 
-def _compile(out, link):
+def _compile(out, link, program=PROGRAM):
     cmd = ["g++", "-std=c++17", "-O2", "-ffp-contract=off", f"-I{os.path.join(ROOT, 'include')}",
-           '-DTWOFOLD_HEADER="twofold_b200/world.hpp"', PROGRAM]
+           '-DTWOFOLD_HEADER="twofold_b200/world.hpp"', program]
     if link:
         libdir = os.path.dirname(abi.LIB_PATH)
         cmd += ["-o", out, f"-L{libdir}", "-l:" + os.path.basename(abi.LIB_PATH), f"-Wl,-rpath,{libdir}"]
@@ -39,6 +41,36 @@ def _parse(text):
 
 def test_dropin_program_compiles_against_the_facade():
     _compile(None, link=False)
+    _compile(None, link=False, program=JOINTS_PROGRAM)
+
+
+def _parse_joints(text):
+    lines = [l for l in text.splitlines() if l and not l.startswith("#")]
+    broken = int(lines[0].split()[1])
+    bodies = np.array([[float(x) for x in l.split()] for l in lines[1:] if not l.startswith("joint")])
+    joints = np.array([[float(x) for x in l.split()[1:]] for l in lines[1:] if l.startswith("joint")])
+    return broken, bodies, joints
+
+
+@pytest.mark.gpu
+def test_dropin_joints_program_matches_the_reference(tmp_path):
+    """Every joint kind through the drop-in World::createJoint, jointInfo and brokenJoints."""
+    exe = str(tmp_path / "joints_b200")
+    _compile(exe, link=True, program=JOINTS_PROGRAM)
+    out = subprocess.run([exe, "60"], check=True, capture_output=True, text=True).stdout
+    b_mine, bodies_mine, joints_mine = _parse_joints(out)
+    with open(JOINTS_GOLDEN) as f:
+        b_ref, bodies_ref, joints_ref = _parse_joints(f.read())
+    assert b_mine == b_ref
+    assert np.array_equal(bodies_mine[:, 0], bodies_ref[:, 0])
+    for name, cols in (("p", slice(1, 4)), ("q", slice(4, 8)), ("v", slice(8, 11)), ("w", slice(11, 14))):
+        err = rel_err(bodies_mine[:, cols], bodies_ref[:, cols])
+        assert err <= TOL, f"{name} differs by {err}"
+    # index, type and broken flag exactly; value and force within the tolerance
+    assert np.array_equal(joints_mine[:, [0, 1, 6]], joints_ref[:, [0, 1, 6]])
+    for name, cols in (("value", slice(2, 3)), ("force", slice(3, 6))):
+        err = rel_err(joints_mine[:, cols], joints_ref[:, cols])
+        assert err <= TOL, f"joint {name} differs by {err}"
 
 
 @pytest.mark.gpu
