@@ -206,14 +206,47 @@ struct Model {
     PointState<T>* pointAdj;  // contactSlots x 4
     T* massAdj;      // per body (output, summed)
     T* frictionAdj;  // per shape (output, summed)
-    T* log;          // per world: logStride values
+    T* log;          // per slot and world: logStride values
     uint64_t logStride;
-    T* integLog;     // per substep and body: q (4) and w (3) before the position update, dp (3) after it
+    T* integLog;     // per slot, substep and body: q (4) and w (3) before the position update, dp (3) after it
+    T* scratch;      // per slot: one state
 };
+
 
 constexpr int kIntegWords = 10;
 
+// The working arrays of one step's recomputation. The backward recomputes a chunk of steps at once, one warp
+// per world and step, so each step of the chunk has its own slot; the forward uses slot 0.
+template <class T>
+struct Slot {
+    T* invM;
+    T* invI;
+    T* dp;
+    T* dq;
+    T* qBase;
+    PointState<T>* points;
+    T* log;       // nWorlds x logStride
+    T* integLog;  // substeps x totalBodies x kIntegWords
+    T* scratch;   // totalBodies x kState: the recomputed step's end state
+};
+
 constexpr int kState = 13;
+
+template <class T>
+__device__ __forceinline__ Slot<T> slotOf(const Model<T>& M, uint32_t k) {
+    const size_t nb = M.S.totalBodies;
+    Slot<T> W;
+    W.invM = M.invM + k * nb;
+    W.invI = M.invI + k * 9 * nb;
+    W.dp = M.dp + k * 3 * nb;
+    W.dq = M.dq + k * 4 * nb;
+    W.qBase = M.qBase + k * 4 * nb;
+    W.points = M.points + k * (size_t)M.S.contactSlots * 4;
+    W.log = M.log ? M.log + k * (size_t)M.S.nWorlds * M.logStride : nullptr;
+    W.integLog = M.integLog ? M.integLog + k * (size_t)M.S.substeps * nb * kIntegWords : nullptr;
+    W.scratch = M.scratch ? M.scratch + k * nb * kState : nullptr;
+    return W;
+}
 
 template <class T> __device__ __forceinline__ V3<T> ld3(const T* p) { return { p[0], p[1], p[2] }; }
 template <class T> __device__ __forceinline__ void st3(T* p, V3<T> v) { p[0] = v.x, p[1] = v.y, p[2] = v.z; }
@@ -711,6 +744,15 @@ __device__ void contactOpAdj(const Model<T>& M, int op, const SBody<T>& a0, cons
     }
 }
 
+// Asks for the 128-byte lines of [from, to) in L1, spread over the warp's lanes.
+template <class T>
+__device__ __forceinline__ void prefetchRange(const T* from, const T* to, uint32_t lane) {
+    const char* end = reinterpret_cast<const char*>(to);
+    for (const char* p = reinterpret_cast<const char*>(from) + 128 * lane; p < end; p += 128 * 32) {
+        asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
+    }
+}
+
 // ---------------------------------------------------------------------------------------------------------
 // One world's step, forward (with optional logging) and in reverse. One warp per world.
 
@@ -748,14 +790,14 @@ __device__ __forceinline__ bool movesIn(const Model<T>& M, const WorldView& V, u
 }
 
 template <class T>
-__device__ __forceinline__ SBody<T> bodyOf(const Model<T>& M, const WorldView& V, uint32_t g, const T* state) {
+__device__ __forceinline__ SBody<T> bodyOf(const Model<T>& M, const Slot<T>& W, const WorldView& V, uint32_t g, const T* state) {
     SBody<T> b;
     b.v = ld3(state + (size_t)g * kState + 7);
     b.w = ld3(state + (size_t)g * kState + 10);
-    b.dp = ld3(M.dp + 3 * (size_t)g);
-    b.dq = ld4(M.dq + 4 * (size_t)g);
-    b.im = M.invM[g];
-    b.I = ldM(M.invI + 9 * (size_t)g);
+    b.dp = ld3(W.dp + 3 * (size_t)g);
+    b.dq = ld4(W.dq + 4 * (size_t)g);
+    b.im = W.invM[g];
+    b.I = ldM(W.invI + 9 * (size_t)g);
     b.moves = movesIn(M, V, g);
     return b;
 }
@@ -787,7 +829,8 @@ __device__ __forceinline__ int passLists(const WorldView& V, int op, PassList* o
 // Forward of one step of one world. state: in at `in`, out at `out` (may be the same). When log is non-null the
 // inputs of every contact operation and position update are written there for the reverse pass.
 template <class T>
-__device__ void stepWorld(const Model<T>& M, int step, uint32_t w, const T* in, T* out, T* log, T* integLog) {
+__device__ void stepWorld(const Model<T>& M, const Slot<T>& W, int step, uint32_t w, const T* in, T* out, T* log,
+                          T* integLog) {
     const uint32_t lane = threadIdx.x & 31;
     const WorldView V = viewOf(M.S, step, w);
     const int n = M.S.substeps;
@@ -812,17 +855,17 @@ __device__ void stepWorld(const Model<T>& M, int step, uint32_t w, const T* in, 
             }
             I = mmul(r, mmul(L, transposeM(r)));
         }
-        M.invM[g] = im;
-        stM(M.invI + 9 * (size_t)g, I);
-        st3(M.dp + 3 * (size_t)g, zeroV<T>());
-        st4(M.dq + 4 * (size_t)g, Q4<T>{ 0, 0, 0, 1 });
-        st4(M.qBase + 4 * (size_t)g, q);
+        W.invM[g] = im;
+        stM(W.invI + 9 * (size_t)g, I);
+        st3(W.dp + 3 * (size_t)g, zeroV<T>());
+        st4(W.dq + 4 * (size_t)g, Q4<T>{ 0, 0, 0, 1 });
+        st4(W.qBase + 4 * (size_t)g, q);
     }
     const uint32_t cf = V.tw->contactFirst;
     for (uint32_t ci = lane; ci < V.tw->contactCount; ci += 32) {
         const TapeContact& tc = V.contacts[ci];
         for (int i = 0; i < 4; ++i) {
-            PointState<T>& p = M.points[(size_t)(cf + ci) * 4 + i];
+            PointState<T>& p = W.points[(size_t)(cf + ci) * 4 + i];
             p.n = T(tc.normalImpulse[i]);
             p.t = fl3<T>(tc.tangentImpulse[i]);
             p.maxN = 0;
@@ -834,8 +877,8 @@ __device__ void stepWorld(const Model<T>& M, int step, uint32_t w, const T* in, 
         const TapeContact& tc = V.contacts[ci];
         const CData<T> c = loadContact<T>(tc);
         const uint32_t ga = V.bodyFirst + tc.a, gb = V.bodyFirst + tc.b;
-        SBody<T> a = bodyOf(M, V, ga, out), b = bodyOf(M, V, gb, out);
-        PointState<T>* p = M.points + (size_t)(cf + ci) * 4;
+        SBody<T> a = bodyOf(M, W, V, ga, out), b = bodyOf(M, W, V, gb, out);
+        PointState<T>* p = W.points + (size_t)(cf + ci) * 4;
         PointState<T> ps[4];
         for (int i = 0; i < 4; ++i) { ps[i] = p[i]; }
         if (log) { writeCall(log + at * callWords<T>(), a, b, ps); }
@@ -894,8 +937,8 @@ __device__ void stepWorld(const Model<T>& M, int step, uint32_t w, const T* in, 
             const V3<T> v = ld3(o + 7), wv = ld3(o + 10);
             const Q4<T> q = ld4(o + 3);
             st3(o, ld3(o) + v * M.h);
-            const V3<T> ndp = ld3(M.dp + 3 * (size_t)g) + v * M.h;
-            st3(M.dp + 3 * (size_t)g, ndp);
+            const V3<T> ndp = ld3(W.dp + 3 * (size_t)g) + v * M.h;
+            st3(W.dp + 3 * (size_t)g, ndp);
             if (integLog) {
                 T* L = integLog + ((size_t)sub * M.S.totalBodies + g) * kIntegWords;
                 st4(L, q);
@@ -904,7 +947,7 @@ __device__ void stepWorld(const Model<T>& M, int step, uint32_t w, const T* in, 
             }
             const Q4<T> nq = integrateQ(q, wv, M.h);
             st4(o + 3, nq);
-            st4(M.dq + 4 * (size_t)g, qmul(nq, conj(ld4(M.qBase + 4 * (size_t)g))));
+            st4(W.dq + 4 * (size_t)g, qmul(nq, conj(ld4(W.qBase + 4 * (size_t)g))));
         }
         __syncwarp();
         pass(kRelax);
@@ -916,8 +959,8 @@ __device__ void stepWorld(const Model<T>& M, int step, uint32_t w, const T* in, 
 // Needs the log and integLog that stepWorld wrote for this step, and the bodies' dp/dq of every substep, which
 // it recomputes by replaying the integration from the checkpoint as it goes back.
 template <class T>
-__device__ void stepWorldAdj(const Model<T>& M, int step, uint32_t w, const T* in, const T* log, const T* integLog,
-                             uint64_t calls) {
+__device__ void stepWorldAdj(const Model<T>& M, const Slot<T>& W, int step, uint32_t w, const T* in, const T* log,
+                             const T* integLog, uint64_t calls) {
     const uint32_t lane = threadIdx.x & 31;
     const WorldView V = viewOf(M.S, step, w);
     const int n = M.S.substeps;
@@ -942,14 +985,14 @@ __device__ void stepWorldAdj(const Model<T>& M, int step, uint32_t w, const T* i
             const uint32_t g = V.bodyFirst + i;
             const int k = afterUpdate ? sub : sub - 1;  // the last position update before the pass
             if (!movesIn(M, V, g) || k < 0) {
-                st3(M.dp + 3 * (size_t)g, zeroV<T>());
-                st4(M.dq + 4 * (size_t)g, Q4<T>{ 0, 0, 0, 1 });
+                st3(W.dp + 3 * (size_t)g, zeroV<T>());
+                st4(W.dq + 4 * (size_t)g, Q4<T>{ 0, 0, 0, 1 });
                 continue;
             }
             const T* L = integLog + ((size_t)k * M.S.totalBodies + g) * kIntegWords;
             const Q4<T> qb = ld4(in + (size_t)g * kState + 3);
-            st3(M.dp + 3 * (size_t)g, ld3(L + 7));
-            st4(M.dq + 4 * (size_t)g, qmul(integrateQ(ld4(L), ld3(L + 4), M.h), conj(qb)));
+            st3(W.dp + 3 * (size_t)g, ld3(L + 7));
+            st4(W.dq + 4 * (size_t)g, qmul(integrateQ(ld4(L), ld3(L + 4), M.h), conj(qb)));
         }
         __syncwarp();
     };
@@ -961,10 +1004,10 @@ __device__ void stepWorldAdj(const Model<T>& M, int step, uint32_t w, const T* i
         SBody<T> a, b;
         PointState<T> p0[4];
         readCall(log + at * callWords<T>(), a, b, p0);
-        a.dp = ld3(M.dp + 3 * (size_t)ga), a.dq = ld4(M.dq + 4 * (size_t)ga), a.im = M.invM[ga];
-        a.I = ldM(M.invI + 9 * (size_t)ga), a.moves = movesIn(M, V, ga);
-        b.dp = ld3(M.dp + 3 * (size_t)gb), b.dq = ld4(M.dq + 4 * (size_t)gb), b.im = M.invM[gb];
-        b.I = ldM(M.invI + 9 * (size_t)gb), b.moves = movesIn(M, V, gb);
+        a.dp = ld3(W.dp + 3 * (size_t)ga), a.dq = ld4(W.dq + 4 * (size_t)ga), a.im = W.invM[ga];
+        a.I = ldM(W.invI + 9 * (size_t)ga), a.moves = movesIn(M, V, ga);
+        b.dp = ld3(W.dp + 3 * (size_t)gb), b.dq = ld4(W.dq + 4 * (size_t)gb), b.im = W.invM[gb];
+        b.I = ldM(W.invI + 9 * (size_t)gb), b.moves = movesIn(M, V, gb);
         T* sa = M.stateAdj + (size_t)ga * kState;
         T* sb = M.stateAdj + (size_t)gb * kState;
         BodyAdj<T> gA{ zeroV<T>(), zeroV<T>(), zeroV<T>(), Q4<T>{ 0, 0, 0, 0 }, 0, zeroM<T>() };
@@ -1016,6 +1059,11 @@ __device__ void stepWorldAdj(const Model<T>& M, int step, uint32_t w, const T* i
                 const uint32_t first = L.start[0];
                 cursor -= L.start[L.count] - first;
                 for (int k = (int)L.count - 1; k >= 0; --k) {
+                    // The next color's log records come from far memory: ask for them while this color runs.
+                    if (k > 0) {
+                        prefetchRange(log + (cursor + (L.start[k - 1] - first)) * callWords<T>(),
+                                      log + (cursor + (L.start[k] - first)) * callWords<T>(), lane);
+                    }
                     for (uint32_t x = L.start[k] + lane; x < L.start[k + 1]; x += 32) { opAdj(op, L.list[x], cursor + (x - first)); }
                     __syncwarp();
                 }
@@ -1115,30 +1163,43 @@ __global__ void __launch_bounds__(128) k_model_forward(const __grid_constant__ M
     }
     __syncwarp();
     const size_t stride = (size_t)M.S.totalBodies * kState;
+    const Slot<T> W = slotOf(M, 0);
     for (int s = 0; s < M.S.nSteps; ++s) {
-        stepWorld<T>(M, s, w, M.states + s * stride, M.states + (s + 1) * stride, nullptr, nullptr);
+        stepWorld<T>(M, W, s, w, M.states + s * stride, M.states + (s + 1) * stride, nullptr, nullptr);
         __syncwarp();
     }
 }
 
+// The backward runs chunk by chunk from the last step. Recomputing a step needs only its checkpoint, so a
+// chunk's steps are recomputed all at once, one warp per world and step, each logging into its own slot; then
+// one warp per world walks the chunk's steps in reverse from those logs, carrying the adjoints back.
 template <class T>
-__global__ void __launch_bounds__(128) k_model_backward(const __grid_constant__ Model<T> M) {
+__global__ void __launch_bounds__(128) k_model_recompute(const __grid_constant__ Model<T> M, int first, int count) {
+    const uint32_t warp = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
+    const uint32_t nw = (uint32_t)M.S.nWorlds;
+    const uint32_t k = warp / nw, w = warp % nw;
+    if (k >= (uint32_t)count) { return; }
+    const Slot<T> W = slotOf(M, k);
+    const int s = first + (int)k;
+    const size_t stride = (size_t)M.S.totalBodies * kState;
+    stepWorld(M, W, s, w, M.states + s * stride, W.scratch, W.log + (size_t)w * M.logStride, W.integLog);
+}
+
+template <class T>
+__global__ void __launch_bounds__(128) k_model_reverse(const __grid_constant__ Model<T> M, int first, int count) {
     const uint32_t w = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
     if (w >= (uint32_t)M.S.nWorlds) { return; }
     const size_t stride = (size_t)M.S.totalBodies * kState;
-    T* log = M.log + (size_t)w * M.logStride;
-    T* scratch = M.states + (size_t)(M.S.nSteps + 1) * stride;  // one state of scratch after the checkpoints
-    for (int s = M.S.nSteps - 1; s >= 0; --s) {
-        // Recompute the step from its checkpoint, logging every operation's inputs.
-        stepWorld(M, s, w, M.states + s * stride, scratch, log, M.integLog);
-        __syncwarp();
+    for (int k = count - 1; k >= 0; --k) {
+        const int s = first + k;
+        const Slot<T> W = slotOf(M, (uint32_t)k);
         // The number of contact operations the step logged: every pass walks its lists once.
         const WorldView V = viewOf(M.S, s, w);
         const TapeWorld& tw = *V.tw;
         const uint64_t colored = tw.colorStart[tw.colorCount] + tw.restCount;
         const uint64_t impact = tw.impactColorStart[tw.impactColorCount] + tw.impactRestCount;
         const uint64_t calls = (uint64_t)M.S.substeps * (3 * colored + 2 * impact) + colored;
-        stepWorldAdj(M, s, w, M.states + s * stride, log, M.integLog, calls);
+        stepWorldAdj(M, W, s, w, M.states + s * stride, W.log + (size_t)w * M.logStride, W.integLog, calls);
         __syncwarp();
     }
 }
@@ -1157,8 +1218,9 @@ struct Run {
     void *invM = nullptr, *invI = nullptr, *dp = nullptr, *dq = nullptr, *qBase = nullptr, *points = nullptr;
     void *stateAdj = nullptr, *dpAdj = nullptr, *dqAdj = nullptr, *qBaseAdj = nullptr, *invMAdj = nullptr,
          *invIAdj = nullptr, *pointAdj = nullptr, *massAdj = nullptr, *frictionAdj = nullptr, *log = nullptr,
-         *integLog = nullptr;
+         *integLog = nullptr, *scratch = nullptr;
     uint64_t logStride = 0;
+    int slots = 0;  // steps the backward recomputes at once
     bool forwardDone = false;
     float forwardMs = 0.0f, backwardMs = 0.0f;
 
@@ -1167,10 +1229,12 @@ struct Run {
         for (void* p : owned) { cudaFree(p); }
         owned.clear();
         for (void** p : { &mass, &friction, &init, &states, &invM, &invI, &dp, &dq, &qBase, &points, &stateAdj, &dpAdj,
-                          &dqAdj, &qBaseAdj, &invMAdj, &invIAdj, &pointAdj, &massAdj, &frictionAdj, &log, &integLog }) {
+                          &dqAdj, &qBaseAdj, &invMAdj, &invIAdj, &pointAdj, &massAdj, &frictionAdj, &log, &integLog,
+                          &scratch }) {
             *p = nullptr;
         }
         forwardDone = false;
+        slots = 0;
     }
     int alloc(void** p, size_t bytes) {
         cudaError_t e = cudaMalloc(p, bytes < 16 ? 16 : bytes);
@@ -1220,6 +1284,7 @@ Model<T> modelOf(const AdjointSetup& S, Run& r) {
     M.log = (T*)r.log;
     M.logStride = r.logStride;
     M.integLog = (T*)r.integLog;
+    M.scratch = (T*)r.scratch;
     return M;
 }
 
@@ -1332,13 +1397,36 @@ int backwardT(Run& r, const AdjointSetup& S, cudaStream_t stream, const double* 
     if ((rc = maxCalls(S, &calls)) != TF_OK) { return rc; }
     r.logStride = calls * (uint64_t)callWords<T>();
     if (!r.stateAdj) {
-        if ((rc = r.alloc(&r.stateAdj, nb * kState * sizeof(T))) || (rc = r.alloc(&r.dpAdj, 3 * nb * sizeof(T))) ||
+        // Steps recomputed at once: as many slots as fit in a share of the free memory, up to the whole run.
+        const size_t perSlot = (size_t)S.nWorlds * r.logStride * sizeof(T) +
+                               (size_t)S.substeps * nb * kIntegWords * sizeof(T) + nb * (kState + 21) * sizeof(T) +
+                               (size_t)S.contactSlots * 4 * sizeof(PointState<T>);
+        size_t freeBytes = 0, totalBytes = 0;
+        TF_ADJ_CUDA(cudaMemGetInfo(&freeBytes, &totalBytes));
+        const size_t budget = std::min<size_t>(freeBytes / 2, (size_t)32 << 30);
+        r.slots = (int)std::max<size_t>(1, std::min<size_t>((size_t)S.nSteps, budget / std::max<size_t>(perSlot, 1)));
+        const size_t k = (size_t)r.slots;
+        // The forward's single-slot working arrays give way to one per slot.
+        for (void** p : { &r.invM, &r.invI, &r.dp, &r.dq, &r.qBase, &r.points }) {
+            auto it = std::find(r.owned.begin(), r.owned.end(), *p);
+            if (it != r.owned.end()) {
+                cudaFree(*p);
+                r.owned.erase(it);
+            }
+            *p = nullptr;
+        }
+        if ((rc = r.alloc(&r.invM, k * nb * sizeof(T))) || (rc = r.alloc(&r.invI, k * 9 * nb * sizeof(T))) ||
+            (rc = r.alloc(&r.dp, k * 3 * nb * sizeof(T))) || (rc = r.alloc(&r.dq, k * 4 * nb * sizeof(T))) ||
+            (rc = r.alloc(&r.qBase, k * 4 * nb * sizeof(T))) ||
+            (rc = r.alloc(&r.points, k * (size_t)S.contactSlots * 4 * sizeof(PointState<T>))) ||
+            (rc = r.alloc(&r.scratch, k * nb * kState * sizeof(T))) ||
+            (rc = r.alloc(&r.stateAdj, nb * kState * sizeof(T))) || (rc = r.alloc(&r.dpAdj, 3 * nb * sizeof(T))) ||
             (rc = r.alloc(&r.dqAdj, 4 * nb * sizeof(T))) || (rc = r.alloc(&r.qBaseAdj, 4 * nb * sizeof(T))) ||
             (rc = r.alloc(&r.invMAdj, nb * sizeof(T))) || (rc = r.alloc(&r.invIAdj, 9 * nb * sizeof(T))) ||
             (rc = r.alloc(&r.pointAdj, (size_t)S.contactSlots * 4 * sizeof(PointState<T>))) ||
             (rc = r.alloc(&r.massAdj, nb * sizeof(T))) || (rc = r.alloc(&r.frictionAdj, ns * sizeof(T))) ||
-            (rc = r.alloc(&r.integLog, (size_t)S.substeps * nb * kIntegWords * sizeof(T))) ||
-            (rc = r.alloc(&r.log, (size_t)S.nWorlds * r.logStride * sizeof(T)))) {
+            (rc = r.alloc(&r.integLog, k * (size_t)S.substeps * nb * kIntegWords * sizeof(T))) ||
+            (rc = r.alloc(&r.log, k * (size_t)S.nWorlds * r.logStride * sizeof(T)))) {
             return rc;
         }
     }
@@ -1352,7 +1440,13 @@ int backwardT(Run& r, const AdjointSetup& S, cudaStream_t stream, const double* 
     TF_ADJ_CUDA(cudaEventCreate(&e1));
     cudaEventRecord(e0, stream);
     const int blocks = (S.nWorlds + 3) / 4;
-    k_model_backward<T><<<blocks, 128, 0, stream>>>(M);
+    for (int end = S.nSteps; end > 0;) {
+        const int count = std::min(end, r.slots), first = end - count;
+        const unsigned warps = (unsigned)count * (unsigned)S.nWorlds;
+        k_model_recompute<T><<<(warps + 3) / 4, 128, 0, stream>>>(M, first, count);
+        k_model_reverse<T><<<blocks, 128, 0, stream>>>(M, first, count);
+        end = first;
+    }
     cudaEventRecord(e1, stream);
     TF_ADJ_CUDA(cudaGetLastError());
     TF_ADJ_CUDA(cudaStreamSynchronize(stream));
