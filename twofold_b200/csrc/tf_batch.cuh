@@ -60,6 +60,8 @@ struct Batch {
     uint32_t* impactColored;
     uint32_t* rest;           // active contacts solved one at a time, in active order
     uint32_t* impactRest;
+    uint32_t* restLevel;        // each level's end in the rest list
+    uint32_t* impactRestLevel;
     uint8_t* color;           // by contact
     Axis* axes;               // by contact, kAxesPerContact each
     uint8_t* cflags;          // by contact: kFast, kFastSolid

@@ -163,7 +163,7 @@ public:
     DevArray<TriangleBound> dTriBounds;
     DevArray<DContact> dContacts[2];
     int cur = 0;
-    DevArray<uint32_t> dActive, dImpact, dColored, dImpactColored, dRest, dImpactRest;
+    DevArray<uint32_t> dActive, dImpact, dColored, dImpactColored, dRest, dImpactRest, dRestLevel, dImpactRestLevel;
     DevArray<uint8_t> dColor, dCflags;
     DevArray<Axis> dAxes;
     DevArray<uint64_t> dMergeKeyA, dMergeKeyB;
@@ -993,6 +993,8 @@ public:
         TF_ALLOC(dImpactColored, ncon);
         TF_ALLOC(dRest, ncon);
         TF_ALLOC(dImpactRest, ncon);
+        TF_ALLOC(dRestLevel, ncon);
+        TF_ALLOC(dImpactRestLevel, ncon);
         TF_ALLOC(dColor, ncon);
         TF_ALLOC(dCflags, ncon);
         TF_ALLOC(dAxes, ncon * kAxesPerContact);
@@ -1183,6 +1185,8 @@ public:
         B.impactColored = dImpactColored.ptr;
         B.rest = dRest.ptr;
         B.impactRest = dImpactRest.ptr;
+        B.restLevel = dRestLevel.ptr;
+        B.impactRestLevel = dImpactRestLevel.ptr;
         B.color = dColor.ptr;
         B.cflags = dCflags.ptr;
         B.axes = dAxes.ptr;

@@ -1410,6 +1410,53 @@ __device__ void bucketByColor(const Group& g, uint32_t n, const uint32_t* list, 
     g.sync();
 }
 
+// The contacts solved one at a time (planar, rolling, those past the colors) are swept in list order. Only
+// contacts that share a moving body depend on that order: each takes a level one past the last earlier
+// contact on either of its moving bodies, so that the contacts of a level share no moving body and run
+// together while every body still meets its contacts in list order, which gives the sweep's own bits. Runs on
+// one thread: reorders list by level (stably, within the level in list order) and writes each level's end.
+// last (one word per body, zero on entry), tmp and out (one word per entry) are scratch. Returns the levels.
+__device__ uint32_t levelList(const Batch& B, const WorldInfo& wi, const DContact* cs, uint32_t* list, uint32_t n,
+                              uint32_t* levelEnd, uint32_t* last, uint32_t* tmp, uint32_t* out) {
+    uint32_t levels = 0;
+    for (uint32_t x = 0; x < n; ++x) {
+        const DContact& c = cs[list[x]];
+        const uint32_t a = c.bodyA - wi.bodyFirst, b = c.bodyB - wi.bodyFirst;
+        const bool ma = a < wi.bodyCount && movingBody(B.bodies[c.bodyA]);
+        const bool mb = b < wi.bodyCount && movingBody(B.bodies[c.bodyB]);
+        uint32_t lev = 0;
+        if (ma) { lev = max(lev, last[a]); }
+        if (mb) { lev = max(lev, last[b]); }
+        if (ma) { last[a] = lev + 1; }
+        if (mb) { last[b] = lev + 1; }
+        tmp[x] = lev;
+        levels = max(levels, lev + 1);
+    }
+    for (uint32_t l = 0; l < levels; ++l) { levelEnd[l] = 0; }
+    for (uint32_t x = 0; x < n; ++x) { ++levelEnd[tmp[x]]; }
+    uint32_t sum = 0;
+    for (uint32_t l = 0; l < levels; ++l) {
+        const uint32_t size = levelEnd[l];
+        levelEnd[l] = sum;  // the level's fill position, its end once filled
+        sum += size;
+    }
+    for (uint32_t x = 0; x < n; ++x) { out[levelEnd[tmp[x]]++] = list[x]; }
+    for (uint32_t x = 0; x < n; ++x) { list[x] = out[x]; }
+    return levels;
+}
+
+// Runs f on every entry of a leveled list, a level at a time.
+template <class F>
+__device__ void forEachLevel(const Group& g, const uint32_t* list, const uint32_t* levelEnd, uint32_t levels, F f) {
+    uint32_t begin = 0;
+    for (uint32_t l = 0; l < levels; ++l) {
+        const uint32_t end = levelEnd[l];
+        for (uint32_t x = begin + g.tid; x < end; x += g.size) { f(list[x]); }
+        g.sync();
+        begin = end;
+    }
+}
+
 // Coloring is staged in the group's shared slice (masks by body, endpoints by active contact) when the world
 // fits stageBodies bodies and stageContacts active contacts, else in the world's global scratch.
 __global__ void __launch_bounds__(kMaxBlock) k_prepare(const __grid_constant__ Batch B, const __grid_constant__ StepParams P, const __grid_constant__ Split sp, int serial) {
@@ -1555,6 +1602,22 @@ __global__ void __launch_bounds__(kMaxBlock) k_prepare(const __grid_constant__ B
         bucketByColor(g, nActive, act, colorOf, B.colored + cf, B.rest + cf, wc.colorStart, wc.colorCount, wc.restCount);
         bucketByColor(g, nImpact, B.impact + cf, colorOf, B.impactColored + cf, B.impactRest + cf, wc.impactColorStart,
                       wc.impactColorCount, wc.impactRestCount);
+        // The one-at-a-time lists by level; the coloring's scratch is free by now.
+        for (int which = 0; which < 2; ++which) {
+            const uint32_t n = which == 0 ? wc.restCount : wc.impactRestCount;
+            if (n == 0) {
+                if (g.tid == 0) { (which == 0 ? wc.restLevels : wc.impactRestLevels) = 0; }
+                continue;
+            }
+            for (uint32_t i = g.tid; i < wi.bodyCount; i += g.size) { masks[i] = 0; }
+            g.sync();
+            if (g.tid == 0) {
+                uint32_t* list = (which == 0 ? B.rest : B.impactRest) + cf;
+                uint32_t* ends = (which == 0 ? B.restLevel : B.impactRestLevel) + cf;
+                (which == 0 ? wc.restLevels : wc.impactRestLevels) = levelList(B, wi, cs, list, n, ends, masks, endA, endB);
+            }
+            g.sync();
+        }
         if (g.tid == 0) {
             wc.activeCount = nActive;
             wc.impactCount = nImpact;
@@ -2081,10 +2144,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_substep(const __grid_constant__ B
         const uint32_t* icolored = B.impactColored + cf;
         const uint32_t* irest = B.impactRest + cf;
         forEachColor(g, colored, wc.colorStart, wc.colorCount, [&](uint32_t ci) { warm(ci, true); });
-        if (g.tid == 0) {
-            for (uint32_t x = 0; x < wc.restCount; ++x) { warm(rest[x], false); }
-        }
-        g.sync();
+        forEachLevel(g, rest, B.restLevel + cf, wc.restLevels, [&](uint32_t ci) { warm(ci, false); });
         for (int pass = 0; pass < 2; ++pass) {
             const bool bias = pass == 0;
             if constexpr (Joints) {
@@ -2094,17 +2154,12 @@ __global__ void __launch_bounds__(kMaxBlock) k_substep(const __grid_constant__ B
                 }
             }
             forEachColor(g, colored, wc.colorStart, wc.colorCount, [&](uint32_t ci) { solve(ci, bias, true); });
-            if (g.tid == 0) {
-                for (uint32_t x = 0; x < wc.restCount; ++x) { solve(rest[x], bias, false); }
-            }
-            g.sync();
+            forEachLevel(g, rest, B.restLevel + cf, wc.restLevels, [&](uint32_t ci) { solve(ci, bias, false); });
             if (wc.impactCount > 0) {
                 forEachColor(g, icolored, wc.impactColorStart, wc.impactColorCount,
                              [&](uint32_t ci) { solve(ci, bias, true); });
-                if (g.tid == 0) {
-                    for (uint32_t x = 0; x < wc.impactRestCount; ++x) { solve(irest[x], bias, false); }
-                }
-                g.sync();
+                forEachLevel(g, irest, B.impactRestLevel + cf, wc.impactRestLevels,
+                             [&](uint32_t ci) { solve(ci, bias, false); });
             }
             if (bias) {
                 for (uint32_t i = g.tid; i < nb; i += g.size) { st.integratePositionAt(i, P); }
@@ -2422,15 +2477,11 @@ __global__ void __launch_bounds__(kMaxBlock) k_finish(const __grid_constant__ Ba
             DContact& c = cs[ci];
             restituteContact(B.bodies[c.bodyA], B.bodies[c.bodyB], c, P, true, axes + (size_t)ci * kAxesPerContact);
         });
-        if (g.tid == 0) {
-            for (uint32_t x = 0; x < wc.restCount; ++x) {
-                const uint32_t ci = B.rest[cf + x];
-                if (!contactOk(B, wi, wc, ci, 20)) { continue; }
-                DContact& c = cs[ci];
-                restituteContact(B.bodies[c.bodyA], B.bodies[c.bodyB], c, P, false, axes + (size_t)ci * kAxesPerContact);
-            }
-        }
-        g.sync();
+        forEachLevel(g, B.rest + cf, B.restLevel + cf, wc.restLevels, [&](uint32_t ci) {
+            if (!contactOk(B, wi, wc, ci, 20)) { return; }
+            DContact& c = cs[ci];
+            restituteContact(B.bodies[c.bodyA], B.bodies[c.bodyB], c, P, false, axes + (size_t)ci * kAxesPerContact);
+        });
         if constexpr (Joints) {
             if (wi.jointCount > 0) { finishJoints(B, P, g, wi); }
         }

@@ -240,6 +240,8 @@ struct WorldCounts {
     uint32_t fastCount;
     uint32_t fastSolidCount;
     uint32_t restCount;        // active contacts solved one at a time
+    uint32_t restLevels;       // levels of the rest lists (contacts of a level share no moving body)
+    uint32_t impactRestLevels;
     uint32_t impactRestCount;
     uint32_t colorCount;       // 1 + highest color used, active list
     uint32_t impactColorCount;
