@@ -2248,6 +2248,80 @@ __device__ bool uniteHits(uint32_t* parent, uint32_t a, uint32_t b) {
 // order: fast shape, then other shape); dynamic bodies that hit each other form groups, and each awake
 // dynamic body of a group with a hit moves back to the group's earliest hit (time, then lowest body),
 // carried along by the kinematic body that hit, if one did.
+// Shapes wider than this along x (and half-spaces and meshes) are tested against every fast shape.
+constexpr float kWideSweep = 16.0f;
+
+// The continuous pass of a large world: the swept bounds of shapes that are not wide are bucketed by their low
+// x (a counting sort into the world's per-shape scratch), and each fast shape, a warp at a time, runs test on
+// the shapes of the buckets its bounds can overlap (low x within the widest narrow shape's extent below its
+// own low x, up to its high x) and on every wide shape. Each pair is visited once, as the full scan would.
+template <class Test>
+__device__ void sweepCandidates(const Batch& B, const Group& g, const WorldInfo& wi, uint32_t nf, Test& test) {
+    __shared__ uint32_t s_minX[kMaxGroups], s_maxX[kMaxGroups], s_ext[kMaxGroups], s_wide[kMaxGroups];
+    const uint32_t sf = wi.shapeFirst, ns = wi.shapeCount;
+    uint32_t* order = B.rowScratch + sf;
+    uint32_t* ends = B.rowLong + sf;
+    uint32_t* wide = B.rowCount + sf;
+    if (g.tid == 0) {
+        s_minX[g.id] = orderedKey(FLT_MAX);
+        s_maxX[g.id] = orderedKey(-FLT_MAX);
+        s_ext[g.id] = 0;
+        s_wide[g.id] = 0;
+    }
+    g.sync();
+    auto kindOf = [&](uint32_t i) {  // 0 skipped, 1 narrow, 2 wide
+        const DShape& s = B.shapes[sf + i];
+        if (!s.alive || s.sensor) { return 0; }
+        const float w = B.sweptHi[sf + i].x - B.sweptLo[sf + i].x;
+        return (s.kind == kHalfSpace || s.kind == kMesh || !(w <= kWideSweep)) ? 2 : 1;
+    };
+    for (uint32_t i = g.tid; i < ns; i += g.size) {
+        const int k = kindOf(i);
+        if (k == 2) { wide[atomicAdd(&s_wide[g.id], 1u)] = i; }
+        if (k != 1) { continue; }
+        atomicMin(&s_minX[g.id], orderedKey(B.sweptLo[sf + i].x));
+        atomicMax(&s_maxX[g.id], orderedKey(B.sweptHi[sf + i].x));
+        atomicMax(&s_ext[g.id], __float_as_uint(B.sweptHi[sf + i].x - B.sweptLo[sf + i].x));
+    }
+    g.sync();
+    const uint32_t buckets = max(1u, ns / 4);
+    const float minX = fromOrderedKey(s_minX[g.id]), maxX = fromOrderedKey(s_maxX[g.id]);
+    const float scale = (float)buckets / fmaxf(maxX - minX, 1e-6f);
+    auto bucketOf = [&](float x) {
+        const float t = fminf(fmaxf((x - minX) * scale, 0.0f), (float)(buckets - 1));
+        return (uint32_t)t;
+    };
+    for (uint32_t b = g.tid; b < buckets; b += g.size) { ends[b] = 0; }
+    g.sync();
+    for (uint32_t i = g.tid; i < ns; i += g.size) {
+        if (kindOf(i) == 1) { atomicAdd(&ends[bucketOf(B.sweptLo[sf + i].x)], 1u); }
+    }
+    g.sync();
+    if (g.tid == 0) {
+        uint32_t sum = 0;
+        for (uint32_t b = 0; b < buckets; ++b) {
+            const uint32_t n = ends[b];
+            ends[b] = sum;  // the bucket's fill position, its end once filled
+            sum += n;
+        }
+    }
+    g.sync();
+    for (uint32_t i = g.tid; i < ns; i += g.size) {
+        if (kindOf(i) == 1) { order[atomicAdd(&ends[bucketOf(B.sweptLo[sf + i].x)], 1u)] = i; }
+    }
+    g.sync();
+    // Padded, so that rounding in the widths and the subtraction below never drops a pair.
+    const float ext = __uint_as_float(s_ext[g.id]) * 1.001f + 1e-3f;
+    const uint32_t nWide = s_wide[g.id];
+    for (uint32_t k = g.warp; k < nf; k += g.warps) {
+        const uint32_t fi = B.sweepList[sf + k];
+        const uint32_t b0 = bucketOf(B.sweptLo[sf + fi].x - ext), b1 = bucketOf(B.sweptHi[sf + fi].x);
+        const uint32_t from = b0 > 0 ? ends[b0 - 1] : 0u, to = ends[b1];
+        for (uint32_t p = from + g.lane; p < to; p += 32) { test(k, order[p]); }
+        for (uint32_t p = g.lane; p < nWide; p += 32) { test(k, wide[p]); }
+    }
+}
+
 __device__ void sweepWorld(const Batch& B, const StepParams& P, const Group& g, const WorldInfo& wi, WorldCounts& wc,
                            uint32_t* pairs, uint32_t* impacts) {
     const uint32_t sf = wi.shapeFirst, ns = wi.shapeCount, bf = wi.bodyFirst, nb = wi.bodyCount;
@@ -2280,27 +2354,33 @@ __device__ void sweepWorld(const Batch& B, const StepParams& P, const Group& g, 
         },
         [&](uint32_t i, uint32_t pos) { B.sweepList[sf + pos] = i; });
     const float target = P.tol.linearSlop;
-    const unsigned long long total = (unsigned long long)nf * ns;
-    for (unsigned long long x = g.tid; x < total; x += g.size) {
-        const uint32_t k = (uint32_t)(x / ns), oi = (uint32_t)(x % ns);
+    // Fast shape k against shape oi; x = k ns + oi orders equal hit times, whatever order the pairs run in.
+    auto testPair = [&](uint32_t k, uint32_t oi) {
+        const unsigned long long x = (unsigned long long)k * ns + oi;
         const uint32_t fi = B.sweepList[sf + k];
         const DShape& f = B.shapes[sf + fi];
         const DShape& o = B.shapes[sf + oi];
-        if (!o.alive || o.sensor || o.body == f.body) { continue; }
-        if (!TF_OK_INDEX(B, o.body - bf < nb, 33, bf, oi)) { continue; }
-        if (joinedBodies(B, wi, o.body, f.body)) { continue; }
-        if (!boxesOverlap(B.sweptLo[sf + fi], B.sweptHi[sf + fi], B.sweptLo[sf + oi], B.sweptHi[sf + oi])) { continue; }
-        if (!(f.category & o.mask) || !(o.category & f.mask)) { continue; }
+        if (!o.alive || o.sensor || o.body == f.body) { return; }
+        if (!TF_OK_INDEX(B, o.body - bf < nb, 33, bf, oi)) { return; }
+        if (joinedBodies(B, wi, o.body, f.body)) { return; }
+        if (!boxesOverlap(B.sweptLo[sf + fi], B.sweptHi[sf + fi], B.sweptLo[sf + oi], B.sweptHi[sf + oi])) { return; }
+        if (!(f.category & o.mask) || !(o.category & f.mask)) { return; }
         atomicAdd(pairs, 1u);
         const DBody& bo = B.bodies[o.body];
         float t = 1.0f;
         bool ok = true;
         const bool hit = sweepPair(B.cx, f, B.bodies[f.body], o, bo, B.sweptLo[sf + fi], B.sweptHi[sf + fi], target, t, ok);
         if (!ok) { atomicOr(&wc.flags, kDevUnsupported); }
-        if (!hit) { continue; }
+        if (!hit) { return; }
         const unsigned long long order = x < 0xffffffffull ? x : 0xfffffffeull;
         atomicMin(&B.hitKey[f.body], ((unsigned long long)__float_as_uint(t) << 32) | order);
         if (bo.type == kDynamic && !uniteHits(parent, f.body - bf, o.body - bf)) { atomicOr(&wc.flags, kDevTimeout); }
+    };
+    if (ns <= kSweepBodies || nf <= 32) {
+        const unsigned long long total = (unsigned long long)nf * ns;
+        for (unsigned long long x = g.tid; x < total; x += g.size) { testPair((uint32_t)(x / ns), (uint32_t)(x % ns)); }
+    } else {
+        sweepCandidates(B, g, wi, nf, testPair);
     }
     g.sync();
     for (uint32_t i = g.tid; i < nb; i += g.size) {
