@@ -49,6 +49,9 @@ def parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the plain-path and adjoint measurements")
+    ap.add_argument("--shapes", default=None,
+                    help="launch shapes as JSON {kernel: [threads, big-world bodies, shared bytes]} in place of the "
+                         "autotuner's, e.g. the launch_shapes of an earlier run (for profiling that run's kernels)")
     return ap.parse_args()
 
 
@@ -334,7 +337,12 @@ def run_b200(args, dist):
         batch.step_checked(dt, 1, graph=True)
     # Launch shapes chosen by the library's autotuner on the warmed-up state (which it leaves unchanged).
     t_tune = time.perf_counter()
-    shapes = batch.autotune(dt, trial_steps=1)
+    if args.shapes:
+        shapes = {k: tuple(int(x) for x in v) for k, v in json.loads(args.shapes).items()}
+        for k, (threads, big, smem) in shapes.items():
+            batch.set_launch(k, threads, big, smem)
+    else:
+        shapes = batch.autotune(dt, trial_steps=1)
     tune_s = time.perf_counter() - t_tune
     launches0 = batch.launches()
     steps0 = batch.body_steps()
