@@ -4,7 +4,7 @@ import numpy as np
 import pytest
 
 import reference as R
-from twofold_b200 import scenes
+from twofold_b200 import abi, scenes
 from twofold_b200.world import Batch
 
 pytestmark = pytest.mark.skipif(not R.available(), reason="oracle library not built")
@@ -109,3 +109,31 @@ def test_cylinders_are_built_like_the_reference(seed):
     w.shapes["half_height"][3] = 1e-9                      # a flat disc: thickened to a slab
     w.shapes["radius"][6] = 0.0                            # a line: thickened
     _check_masses(scenes.Scene("cylinders", [w]))
+
+
+@pytest.mark.parametrize("seed", range(3))
+def test_joints_are_made_like_the_reference(seed):
+    """tf_joint_create restates World::createJoint on the host (src/world.cpp:2221-2333): each joint's anchors,
+    axis and value (hinge angle, slider translation, distance, twist) as jointInfo reports them before any step
+    match the reference's, which measures angles with correctly rounded atan2 as the device does."""
+    w = scenes.jointed(seed)
+    b = Batch.from_scene(scenes.Scene("jointed", [w]))
+    r = R.RefWorld(w, lib=R.ROUNDED_LIB)
+    for k in range(len(w.joints)):
+        mine, theirs = b.joint_info(0, abi.tf_id(k, 0)), r.joint_info(abi.tf_id(k, 0))
+        assert (mine.type, mine.body_a, mine.body_b, mine.broken) == (theirs.type, theirs.body_a, theirs.body_b, theirs.broken)
+        for f in ("anchor_a", "anchor_b", "axis"):
+            assert list(getattr(mine, f)) == list(getattr(theirs, f)), f"joint {k} {f}"
+        assert mine.value == theirs.value, f"joint {k} value {mine.value} vs {theirs.value}"
+
+
+def test_joints_refuse_what_this_build_does_not_run():
+    """Joining a body to itself or to a missing body is invalid, as in the reference; a bad kind is rejected."""
+    w = scenes.jointed(0)
+    b = Batch.from_scene(scenes.Scene("jointed", [w]))
+    with pytest.raises(RuntimeError):
+        b.joint_create(0, abi.joint_desc(abi.TF_JOINT_POINT, abi.tf_id(1, 0), abi.tf_id(1, 0)))
+    with pytest.raises(RuntimeError):
+        b.joint_create(0, abi.joint_desc(abi.TF_JOINT_POINT, abi.tf_id(10_000, 0)))
+    with pytest.raises(RuntimeError):
+        b.joint_create(0, abi.joint_desc(9, abi.tf_id(1, 0)))
