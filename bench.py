@@ -73,21 +73,30 @@ def config(args, n_gpus):
 
 
 class Dist:
-    def __init__(self):
+    """One process per GPU from torchrun's environment. The ranks share nothing inside a step; the process group
+    carries the barriers around the timed region and the reductions of its results (max of the device times,
+    sum of the body-steps). NCCL on GPUs; gloo on CPU (`backend`), which the multi-process tests use."""
+
+    def __init__(self, backend=None, timeout_s=300):
         self.world_size = int(os.environ.get("WORLD_SIZE", "1"))
         self.rank = int(os.environ.get("RANK", "0"))
         self.local_rank = int(os.environ.get("LOCAL_RANK", "0"))
         self.pg = None
+        self.cuda = False
         if self.world_size > 1:
             import datetime
 
             import torch
             import torch.distributed as dist
 
-            torch.cuda.set_device(self.local_rank)
+            backend = backend or ("nccl" if torch.cuda.is_available() else "gloo")
+            self.cuda = backend == "nccl"
             os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
-            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
-                                    device_id=torch.device("cuda", self.local_rank))
+            kw = {"timeout": datetime.timedelta(seconds=timeout_s)}
+            if self.cuda:
+                torch.cuda.set_device(self.local_rank)
+                kw["device_id"] = torch.device("cuda", self.local_rank)
+            dist.init_process_group(backend, **kw)
             self.pg = dist
 
     def barrier(self):
@@ -97,14 +106,16 @@ class Dist:
             torch.cuda.synchronize()
         if self.pg:
             self.pg.barrier()
-            torch.cuda.synchronize()
+            if torch.cuda.is_available():
+                torch.cuda.synchronize()
 
     def reduce(self, value, op):
         if not self.pg:
             return value
         import torch
 
-        t = torch.tensor([float(value)], dtype=torch.float64, device=f"cuda:{self.local_rank}")
+        device = f"cuda:{self.local_rank}" if self.cuda else "cpu"
+        t = torch.tensor([float(value)], dtype=torch.float64, device=device)
         self.pg.all_reduce(t, op=getattr(self.pg.ReduceOp, op))
         return float(t.item())
 
