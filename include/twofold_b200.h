@@ -293,6 +293,18 @@ TF_API int tf_joint_create(void* world, int32_t w, const tf_joint_desc* desc, tf
 /* World::jointInfo (include/twofold/world.h:441): pose, value, last force and torque, broken. An invalid id
  * reads as zeros. */
 TF_API int tf_joint_get_info(void* world, int32_t w, tf_id joint, tf_joint_info* out);
+/* World::setJointLimits, setJointMotor, setJointSpring, setJointFriction, setJointSwing, setJointBreakLimits
+ * (include/twofold/world.h:433-439; src/world.cpp:2341-2397) and World::destroyJoint (:429; src/world.cpp:399-406,
+ * its slot reused by the next tf_joint_create with the generation bumped). An invalid id does nothing, as in
+ * the reference. Where the reference wakes a sleeping dynamic end, these return TF_E_UNSUPPORTED and change
+ * nothing. */
+TF_API int tf_joint_set_limits(void* world, int32_t w, tf_id joint, int32_t limited, float lower, float upper);
+TF_API int tf_joint_set_motor(void* world, int32_t w, tf_id joint, float speed, float max_force);
+TF_API int tf_joint_set_spring(void* world, int32_t w, tf_id joint, float hertz, float damping_ratio);
+TF_API int tf_joint_set_friction(void* world, int32_t w, tf_id joint, float max_friction);
+TF_API int tf_joint_set_swing(void* world, int32_t w, tf_id joint, float swing_y, float swing_z);
+TF_API int tf_joint_set_break_limits(void* world, int32_t w, tf_id joint, float force, float torque);
+TF_API int tf_joint_destroy(void* world, int32_t w, tf_id joint);
 /* World::brokenJoints (include/twofold/world.h:443): the joints that broke in world w's last step, in index
  * order; *count gets their number, at most capacity are written. */
 TF_API int tf_world_broken_joints(void* world, int32_t w, tf_id* out, int32_t capacity, int32_t* count);

@@ -676,6 +676,28 @@ public:
         return joints_[id.index];
     }
     bool isValid(JointId joint) const { return joint.index < joints_.size() && joints_[joint.index] == joint; }
+    void destroyJoint(JointId joint) {
+        if (!isValid(joint) || !note(tf_joint_destroy(handle_, 0, tf_id{ joint.index, joint.generation }))) { return; }
+        joints_[joint.index] = JointId{ UINT32_MAX, joint.generation + 1 };
+    }
+    void setJointLimits(JointId joint, bool limited, float lower, float upper) {
+        if (isValid(joint)) { note(tf_joint_set_limits(handle_, 0, tf_id{ joint.index, joint.generation }, limited, lower, upper)); }
+    }
+    void setJointMotor(JointId joint, float speed, float maxForce) {
+        if (isValid(joint)) { note(tf_joint_set_motor(handle_, 0, tf_id{ joint.index, joint.generation }, speed, maxForce)); }
+    }
+    void setJointSpring(JointId joint, float hertz, float dampingRatio) {
+        if (isValid(joint)) { note(tf_joint_set_spring(handle_, 0, tf_id{ joint.index, joint.generation }, hertz, dampingRatio)); }
+    }
+    void setJointFriction(JointId joint, float maxFriction) {
+        if (isValid(joint)) { note(tf_joint_set_friction(handle_, 0, tf_id{ joint.index, joint.generation }, maxFriction)); }
+    }
+    void setJointSwing(JointId joint, float swingY, float swingZ) {
+        if (isValid(joint)) { note(tf_joint_set_swing(handle_, 0, tf_id{ joint.index, joint.generation }, swingY, swingZ)); }
+    }
+    void setJointBreakLimits(JointId joint, float force, float torque) {
+        if (isValid(joint)) { note(tf_joint_set_break_limits(handle_, 0, tf_id{ joint.index, joint.generation }, force, torque)); }
+    }
     JointInfo jointInfo(JointId joint) const {
         JointInfo info;
         if (!isValid(joint)) { return info; }

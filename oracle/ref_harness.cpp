@@ -350,6 +350,22 @@ TF_API int ref_joint_create(void* h, const tf_joint_desc* d, tf_id* out) {
     return id.index == UINT32_MAX ? -1 : 0;
 }
 
+// The joint setters and destroyJoint through the public API; `what` and v as tf_joint_set_* take them.
+TF_API int ref_joint_set(void* h, tf_id joint, int what, const float* v) {
+    const JointId id{ joint.index, joint.generation };
+    switch (what) {
+        case 0: W(h)->setJointLimits(id, v[0] != 0.0f, v[1], v[2]); break;
+        case 1: W(h)->setJointMotor(id, v[0], v[1]); break;
+        case 2: W(h)->setJointSpring(id, v[0], v[1]); break;
+        case 3: W(h)->setJointFriction(id, v[0]); break;
+        case 4: W(h)->setJointSwing(id, v[0], v[1]); break;
+        case 5: W(h)->setJointBreakLimits(id, v[0], v[1]); break;
+        case 6: W(h)->destroyJoint(id); break;
+        default: return -1;
+    }
+    return 0;
+}
+
 TF_API int ref_joint_info(void* h, tf_id joint, tf_joint_info* out) {
     const JointInfo info = W(h)->jointInfo(JointId{ joint.index, joint.generation });
     std::memset(out, 0, sizeof(*out));

@@ -46,6 +46,7 @@ def load(path=REF_LIB):
             "ref_world_profile": ([P, C.POINTER(abi.tf_profile)], C.c_int),
             "ref_joint_create": ([P, C.POINTER(abi.tf_joint_desc), C.POINTER(abi.tf_id)], C.c_int),
             "ref_joint_info": ([P, abi.tf_id, C.POINTER(abi.tf_joint_info)], C.c_int),
+            "ref_joint_set": ([P, abi.tf_id, C.c_int, P], C.c_int),
             "ref_broken_joints": ([P, P, C.c_int, C.POINTER(C.c_int)], C.c_int),
             "ref_world_contact_events": ([P, C.POINTER(abi.tf_contact_event), C.c_int, C.POINTER(C.c_int)], C.c_int),
             "ref_world_hit_events": ([P, C.POINTER(abi.tf_hit_event), C.c_int, C.POINTER(C.c_int)], C.c_int),
@@ -149,6 +150,12 @@ class RefWorld:
         if self.lib.ref_joint_create(self.h, C.byref(desc), C.byref(out)) != 0:
             raise ValueError("the reference refused the joint")
         return out
+
+    def joint_set(self, joint, what, *values):
+        """what: limits (limited, lower, upper), motor, spring, friction, swing, break, destroy."""
+        kinds = ("limits", "motor", "spring", "friction", "swing", "break", "destroy")
+        v = (C.c_float * 3)(*(list(values) + [0.0] * (3 - len(values))))
+        self.lib.ref_joint_set(self.h, joint, kinds.index(what), v)
 
     def joint_info(self, joint):
         info = abi.tf_joint_info()

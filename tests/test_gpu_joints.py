@@ -79,3 +79,56 @@ def test_jointed_worlds_in_a_batch_match_reference():
             r.step(sc.dt)
     for wi, (w, r) in enumerate(zip(worlds, refs)):
         _compare(b, wi, r, len(w.joints), f"world {wi} after 90 steps")
+
+
+@needs_oracle
+def test_joint_changes_match_reference():
+    """The joint setters and destroyJoint between steps (src/world.cpp:2341-2397, 399-406): limits, motor,
+    spring, friction, swing cone and break limits changed mid-run, a chain link destroyed and its slot reused by
+    a new joint, each side stepped on; compared with the reference every 10th step."""
+    w = scenes.jointed(1)
+    sc = scenes.Scene("jointed", [w])
+    b = Batch.from_scene(sc)
+    r = R.RefWorld(w, sc.settings, lib=R.ROUNDED_LIB)
+    for _ in range(20):
+        b.step_checked(sc.dt)
+        r.step(sc.dt)
+    awake = r.states()["awake"]
+
+    def ends_awake(k):
+        info = r.joint_info(abi.tf_id(k, 0))
+        return all(e == 0xFFFFFFFF or awake[e] for e in (info.body_a, info.body_b))
+
+    changes = [(6, "limits", 1, -0.3, 0.3), (7, "motor", -3.0, 50.0), (10, "spring", 4.0, 0.1), (9, "friction", 0.0),
+               (14, "swing", 0.2, 0.2), (11, "break", 0.01, float("inf"))]
+    applied = 0
+    for k, what, *values in changes:
+        if not ends_awake(k):
+            continue
+        b.joint_set(0, abi.tf_id(k, 0), what, *values)
+        r.joint_set(abi.tf_id(k, 0), what, *values)
+        applied += 1
+    assert applied >= 4
+    # The last chain link lets go, and its slot comes back as a new joint holding that body where it is.
+    assert ends_awake(5)
+    last = r.joint_info(abi.tf_id(5, 0)).body_b
+    b.joint_set(0, abi.tf_id(5, 0), "destroy")
+    r.joint_set(abi.tf_id(5, 0), "destroy")
+    pos = tuple(float(x) for x in r.states()["p"][last])
+    desc = abi.joint_desc(abi.TF_JOINT_POINT, abi.tf_id(last, 0), anchor=pos)
+    mine, theirs = b.joint_create(0, desc), r.joint_create(desc)
+    assert (mine.index, mine.generation) == (theirs.index, theirs.generation) == (5, 1)
+    n = len(w.joints)
+    for s in range(60):
+        b.step_checked(sc.dt)
+        r.step(sc.dt)
+        assert b.broken_joints(0) == r.broken_joints(), f"step {s + 21}"
+        if s % 10 == 9:
+            errs = state_errors(b.world_states(0), r.states())
+            assert max(errs.values()) <= TOL, f"step {s + 21}: state error {errs}"
+            for k in range(n):
+                jid = abi.tf_id(k, 1 if k == 5 else 0)
+                m, t = b.joint_info(0, jid), r.joint_info(jid)
+                assert (m.type, m.body_a, m.body_b, m.broken) == (t.type, t.body_a, t.body_b, t.broken), f"joint {k}"
+                mr, tr = _joint_rows([m]), _joint_rows([t])
+                assert rel_err(mr, tr) <= TOL, f"step {s + 21}: joint {k} differs by {rel_err(mr, tr)}"

@@ -315,6 +315,13 @@ def _declare(lib):
         "tf_joint_create": ([P, C.c_int32, C.POINTER(tf_joint_desc), C.POINTER(tf_id)], C.c_int),
         "tf_joint_get_info": ([P, C.c_int32, tf_id, C.POINTER(tf_joint_info)], C.c_int),
         "tf_world_broken_joints": ([P, C.c_int32, P, C.c_int32, C.POINTER(C.c_int32)], C.c_int),
+        "tf_joint_set_limits": ([P, C.c_int32, tf_id, C.c_int32, C.c_float, C.c_float], C.c_int),
+        "tf_joint_set_motor": ([P, C.c_int32, tf_id, C.c_float, C.c_float], C.c_int),
+        "tf_joint_set_spring": ([P, C.c_int32, tf_id, C.c_float, C.c_float], C.c_int),
+        "tf_joint_set_friction": ([P, C.c_int32, tf_id, C.c_float], C.c_int),
+        "tf_joint_set_swing": ([P, C.c_int32, tf_id, C.c_float, C.c_float], C.c_int),
+        "tf_joint_set_break_limits": ([P, C.c_int32, tf_id, C.c_float, C.c_float], C.c_int),
+        "tf_joint_destroy": ([P, C.c_int32, tf_id], C.c_int),
         "tf_world_step": ([P, C.c_float, C.c_int32], C.c_int),
         "tf_world_step_graph": ([P, C.c_float, C.c_int32], C.c_int),
         "tf_world_synchronize": ([P], C.c_int),
@@ -366,7 +373,8 @@ EXPORTED = [
     "tf_abi_version", "tf_last_error", "tf_default_settings", "tf_world_create", "tf_world_destroy",
     "tf_world_count", "tf_world_set_settings", "tf_mesh_create", "tf_mesh_read", "tf_body_create", "tf_shape_add",
     "tf_bodies_create",
-    "tf_shapes_add", "tf_joint_create", "tf_joint_get_info", "tf_world_broken_joints", "tf_world_step", "tf_world_step_graph", "tf_world_synchronize", "tf_world_device_status",
+    "tf_shapes_add", "tf_joint_create", "tf_joint_get_info", "tf_world_broken_joints", "tf_joint_set_limits", "tf_joint_set_motor",
+    "tf_joint_set_spring", "tf_joint_set_friction", "tf_joint_set_swing", "tf_joint_set_break_limits", "tf_joint_destroy", "tf_world_step", "tf_world_step_graph", "tf_world_synchronize", "tf_world_device_status",
     "tf_body_get_state", "tf_body_set_velocity", "tf_body_get_mass", "tf_body_is_awake", "tf_world_body_count",
     "tf_world_get_states", "tf_world_contacts", "tf_world_contact_events", "tf_world_hit_events", "tf_world_candidates", "tf_world_profile", "tf_world_awake_bodies",
     "tf_world_launch_count", "tf_world_elapsed_ms", "tf_world_body_steps", "tf_world_add_forces",

@@ -57,6 +57,7 @@ struct HostJoint {
 
 struct HostWorld {
     std::vector<HostJoint> joints;
+    std::vector<uint32_t> freeJoints;  // destroyed joints' slots, reused last-in first-out
     std::vector<HostBody> bodies;
     std::vector<uint32_t> freeBodies;
     std::vector<HostShape> shapes;
@@ -655,10 +656,99 @@ public:
             j.frameA = normalize(conjugate(xa.q) * frame);
             j.frameB = normalize(conjugate(xb.q) * frame);
         }
-        const uint32_t index = (uint32_t)W.joints.size();
-        W.joints.push_back(hj);
+        uint32_t index = (uint32_t)W.joints.size();
+        if (!W.freeJoints.empty()) {
+            index = W.freeJoints.back();
+            W.freeJoints.pop_back();
+            hj.generation = W.joints[index].generation;
+            W.joints[index] = hj;
+        } else {
+            W.joints.push_back(hj);
+        }
         layoutDirty = true;
         if (out) { *out = { index, hj.generation }; }
+        return TF_OK;
+    }
+
+    // The joint's host record for a change through the API, or null for an invalid id (the reference's
+    // setters then do nothing). The change wakes the joint's dynamic ends in the reference (src/world.cpp:390-397);
+    // a sleeping end is refused here, as waking a body from the host is not run by this build.
+    int jointForChange(int w, tf_id id, bool wakes, HostJoint** out) {
+        *out = nullptr;
+        if (w < 0 || w >= (int)worlds.size()) { return fail(TF_E_INVALID, "joint: bad world"); }
+        int rc = pull();
+        if (rc != TF_OK) { return rc; }
+        HostWorld& W = worlds[(size_t)w];
+        if (id.index >= W.joints.size() || !W.joints[id.index].d.alive || W.joints[id.index].generation != id.generation) {
+            return TF_OK;
+        }
+        HostJoint& j = W.joints[id.index];
+        if (wakes) {
+            for (uint32_t e : { j.d.bodyA, j.d.bodyB }) {
+                if (e != kWorldEnd && W.bodies[e].d.type == kDynamic && !W.bodies[e].d.awake) {
+                    return fail(TF_E_UNSUPPORTED, "joint: waking a sleeping body from the host is not run by this build");
+                }
+            }
+        }
+        *out = &j;
+        return TF_OK;
+    }
+
+    // World::setJointLimits, setJointMotor, setJointSpring, setJointFriction, setJointSwing, setJointBreakLimits
+    // (src/world.cpp:2341-2397) and destroyJoint (:399-406).
+    int jointSet(int w, tf_id id, int what, const float* v) {
+        HostJoint* hj = nullptr;
+        const int rc = jointForChange(w, id, what != 5, &hj);
+        if (rc != TF_OK || !hj) { return rc; }
+        DJoint& j = hj->d;
+        switch (what) {
+            case 0:  // limits: limited, lower, upper
+                j.limited = (v[0] != 0.0f && (j.type != kJointSwingTwist || v[2] - v[1] < 2.0f * kJointPi)) ? 1u : 0u;
+                j.lower = v[1];
+                j.upper = v[2];
+                j.lowerImpulse = 0.0f;
+                j.upperImpulse = 0.0f;
+                break;
+            case 1:  // motor: speed, max force or torque
+                j.motorSpeed = v[0];
+                j.maxMotor = v[1];
+                break;
+            case 2:  // spring: hertz, damping ratio
+                j.hertz = v[0];
+                j.dampingRatio = v[1];
+                break;
+            case 3:  // friction
+                j.maxFriction = v[0];
+                if (!(v[0] > 0.0f)) {
+                    j.frictionImpulse = 0.0f;
+                    j.frictionTurn = zero3();
+                }
+                break;
+            case 4:  // swing cone, as sines of the half angles
+                j.swingY = v[0] >= kJointPi ? 1.0f : (float)std::sin((double)(0.5f * maxf(v[0], 1e-3f)));
+                j.swingZ = v[1] >= kJointPi ? 1.0f : (float)std::sin((double)(0.5f * maxf(v[1], 1e-3f)));
+                j.swingImpulse = 0.0f;
+                break;
+            case 5:  // break limits
+                j.breakForce = v[0];
+                j.breakTorque = v[1];
+                break;
+            default:
+                return fail(TF_E_INVALID, "joint: unknown change");
+        }
+        layoutDirty = true;
+        return TF_OK;
+    }
+
+    int destroyJoint(int w, tf_id id) {
+        HostJoint* hj = nullptr;
+        const int rc = jointForChange(w, id, true, &hj);
+        if (rc != TF_OK || !hj) { return rc; }
+        hj->d.alive = 0;
+        hj->d.brokeNow = 0;
+        ++hj->generation;
+        worlds[(size_t)w].freeJoints.push_back(id.index);
+        layoutDirty = true;
         return TF_OK;
     }
 
@@ -698,7 +788,7 @@ public:
         const HostWorld& W = worlds[(size_t)w];
         int n = 0;
         for (size_t k = 0; k < W.joints.size(); ++k) {
-            if (!W.joints[k].d.brokeNow) { continue; }
+            if (!W.joints[k].d.brokeNow || !W.joints[k].d.alive) { continue; }
             if (out && n < cap) { out[n] = { (uint32_t)k, W.joints[k].generation }; }
             ++n;
         }
@@ -2329,6 +2419,47 @@ TF_API int tf_joint_create(void* h, int32_t w, const tf_joint_desc* desc, tf_id*
 TF_API int tf_joint_get_info(void* h, int32_t w, tf_id joint, tf_joint_info* out) {
     if (!h) { return tfb::fail(TF_E_INVALID, "tf_joint_get_info: null world"); }
     return E(h)->jointInfo(w, joint, out);
+}
+
+TF_API int tf_joint_set_limits(void* h, int32_t w, tf_id joint, int32_t limited, float lower, float upper) {
+    if (!h) { return tfb::fail(TF_E_INVALID, "tf_joint_set_limits: null world"); }
+    const float v[3] = { limited ? 1.0f : 0.0f, lower, upper };
+    return E(h)->jointSet(w, joint, 0, v);
+}
+
+TF_API int tf_joint_set_motor(void* h, int32_t w, tf_id joint, float speed, float max_force) {
+    if (!h) { return tfb::fail(TF_E_INVALID, "tf_joint_set_motor: null world"); }
+    const float v[3] = { speed, max_force, 0.0f };
+    return E(h)->jointSet(w, joint, 1, v);
+}
+
+TF_API int tf_joint_set_spring(void* h, int32_t w, tf_id joint, float hertz, float damping_ratio) {
+    if (!h) { return tfb::fail(TF_E_INVALID, "tf_joint_set_spring: null world"); }
+    const float v[3] = { hertz, damping_ratio, 0.0f };
+    return E(h)->jointSet(w, joint, 2, v);
+}
+
+TF_API int tf_joint_set_friction(void* h, int32_t w, tf_id joint, float max_friction) {
+    if (!h) { return tfb::fail(TF_E_INVALID, "tf_joint_set_friction: null world"); }
+    const float v[3] = { max_friction, 0.0f, 0.0f };
+    return E(h)->jointSet(w, joint, 3, v);
+}
+
+TF_API int tf_joint_set_swing(void* h, int32_t w, tf_id joint, float swing_y, float swing_z) {
+    if (!h) { return tfb::fail(TF_E_INVALID, "tf_joint_set_swing: null world"); }
+    const float v[3] = { swing_y, swing_z, 0.0f };
+    return E(h)->jointSet(w, joint, 4, v);
+}
+
+TF_API int tf_joint_set_break_limits(void* h, int32_t w, tf_id joint, float force, float torque) {
+    if (!h) { return tfb::fail(TF_E_INVALID, "tf_joint_set_break_limits: null world"); }
+    const float v[3] = { force, torque, 0.0f };
+    return E(h)->jointSet(w, joint, 5, v);
+}
+
+TF_API int tf_joint_destroy(void* h, int32_t w, tf_id joint) {
+    if (!h) { return tfb::fail(TF_E_INVALID, "tf_joint_destroy: null world"); }
+    return E(h)->destroyJoint(w, joint);
 }
 
 TF_API int tf_world_broken_joints(void* h, int32_t w, tf_id* out, int32_t cap, int32_t* count) {

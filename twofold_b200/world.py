@@ -123,6 +123,18 @@ class Batch:
         abi.check(self.lib.tf_joint_get_info(self.h, wi, joint, C.byref(info)), self.lib)
         return info
 
+    def joint_set(self, wi, joint, what, *values):
+        """World::setJointLimits (limited, lower, upper), setJointMotor (speed, max), setJointSpring (hertz,
+        damping), setJointFriction (max), setJointSwing (y, z), setJointBreakLimits (force, torque) and
+        destroyJoint, by name: limits, motor, spring, friction, swing, break, destroy."""
+        fn = {"limits": self.lib.tf_joint_set_limits, "motor": self.lib.tf_joint_set_motor,
+              "spring": self.lib.tf_joint_set_spring, "friction": self.lib.tf_joint_set_friction,
+              "swing": self.lib.tf_joint_set_swing, "break": self.lib.tf_joint_set_break_limits,
+              "destroy": self.lib.tf_joint_destroy}[what]
+        if what == "limits":
+            values = (int(values[0]), *values[1:])
+        abi.check(fn(self.h, wi, joint, *values), self.lib)
+
     def broken_joints(self, wi=0):
         n = C.c_int32(0)
         abi.check(self.lib.tf_world_broken_joints(self.h, wi, None, 0, C.byref(n)), self.lib)
