@@ -271,7 +271,8 @@ def plain_rate(sc, args, device):
 
 def single_worlds(device, warmup=20, steps=40):
     """The plain path on the single-world configurations (box pyramid, terrain, planar pile): device ms per
-    step through the C ABI (a CUDA graph per step) over steps warmup+1..warmup+steps, beside the reference
+    step through the C ABI (a CUDA graph per step, launch shapes from the autotuner after the warm-up) over
+    steps warmup+1..warmup+steps, beside the reference
     stepping the same world the same steps on one host core. A reported comparison, not the headline."""
     from twofold_b200 import scenes
     from twofold_b200.world import Batch
@@ -285,6 +286,7 @@ def single_worlds(device, warmup=20, steps=40):
         one = Batch(sc.worlds, sc.settings, device=device)
         for _ in range(warmup):
             one.step_checked(sc.dt, 1, graph=True)
+        one.autotune(sc.dt, trial_steps=1)  # launch shapes for this world, as for the batch
         ms = 0.0
         b0 = one.body_steps()
         for _ in range(steps):
