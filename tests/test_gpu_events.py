@@ -87,3 +87,12 @@ def test_planar_and_terrain_worlds_report_the_reference_events():
                                                       seed=0)])
     began, ended, hits = _run(terrain, 120, lib=R.ROUNDED_LIB)
     assert began > 0 and hits > 0
+
+
+@needs_oracle
+def test_jointed_worlds_report_the_reference_events():
+    """Joined pairs never collide, so they make no events; jointed chains and doors touch the ground and the
+    loose boxes dropped on them."""
+    sc = scenes.Scene("jointed", [scenes.jointed(0), scenes.jointed(1)])
+    began, ended, hits = _run(sc, 120, lib=R.ROUNDED_LIB)
+    assert began > 0 and hits > 0
