@@ -716,6 +716,14 @@ public:
         info.broken = raw.broken != 0;
         return info;
     }
+    // Every live joint's info, in index order.
+    std::vector<JointInfo> joints() const {
+        std::vector<JointInfo> out;
+        for (const JointId& id : joints_) {
+            if (id.index != UINT32_MAX) { out.push_back(jointInfo(id)); }
+        }
+        return out;
+    }
     // Joints that broke in the last step, in index order.
     std::vector<JointId> brokenJoints() const {
         std::vector<JointId> out;

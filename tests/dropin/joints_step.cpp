@@ -101,6 +101,7 @@ int main(int argc, char** argv) {
         std::printf("%u %.9g %.9g %.9g %.9g %.9g %.9g %.9g %.9g %.9g %.9g %.9g %.9g %.9g\n", b.index, p.x, p.y, p.z, q.x,
                     q.y, q.z, q.w, v.x, v.y, v.z, w.x, w.y, w.z);
     }
+    std::printf("live %d\n", (int)world.joints().size());
     for (const JointId& j : joints) {
         const JointInfo info = world.jointInfo(j);
         std::printf("joint %u %d %.9g %.9g %.9g %.9g %d\n", j.index, (int)info.type, info.value, info.force.x,

@@ -47,9 +47,10 @@ def test_dropin_program_compiles_against_the_facade():
 def _parse_joints(text):
     lines = [l for l in text.splitlines() if l and not l.startswith("#")]
     broken = int(lines[0].split()[1])
-    bodies = np.array([[float(x) for x in l.split()] for l in lines[1:] if not l.startswith("joint")])
+    live = [int(l.split()[1]) for l in lines if l.startswith("live")]
+    bodies = np.array([[float(x) for x in l.split()] for l in lines[1:] if not l.startswith(("joint", "live"))])
     joints = np.array([[float(x) for x in l.split()[1:]] for l in lines[1:] if l.startswith("joint")])
-    return broken, bodies, joints
+    return (broken, live), bodies, joints
 
 
 @pytest.mark.gpu
