@@ -4,6 +4,7 @@ sum of their work, every rank takes the same collective steps, and the reference
 0 while rank 1 exits without work."""
 import json
 import os
+import socket
 import subprocess
 import sys
 
@@ -30,10 +31,16 @@ d.close()
 '''
 
 
+def _free_port():
+    with socket.socket(socket.AF_INET, socket.SOCK_STREAM) as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
 def _torchrun(args, timeout=240):
     env = dict(os.environ, TF_ROOT=ROOT, CUDA_VISIBLE_DEVICES="")
     cmd = ["timeout", "-k", "30", str(timeout), sys.executable, "-m", "torch.distributed.run", "--nnodes=1",
-           "--nproc-per-node", "2", "--master-addr", "127.0.0.1", "--master-port", "29533"] + args
+           "--nproc-per-node", "2", "--master-addr", "127.0.0.1", "--master-port", str(_free_port())] + args
     return subprocess.run(cmd, cwd=ROOT, env=env, capture_output=True, text=True, timeout=timeout + 60)
 
 
