@@ -2537,7 +2537,7 @@ template <bool Joints>
 __global__ void __launch_bounds__(kMaxBlock) k_finish(const __grid_constant__ Batch B, const __grid_constant__ StepParams P, const __grid_constant__ Split sp, int serial) {
     extern __shared__ __align__(16) unsigned char s_raw[];
     __shared__ uint32_t s_awake[kMaxGroups], s_islands[kMaxGroups], s_sweep[kMaxGroups], s_pairs[kMaxGroups],
-        s_impacts[kMaxGroups];
+        s_impacts[kMaxGroups], s_linked[kMaxGroups];
     if (stepAborted(B, serial)) { return; }
     forWorlds(B, kSlotFinish, sp, s_raw, [&](const Group& g, uint32_t w, unsigned char* slice, const StageSizes& ss) {
         const uint32_t stageBodies = ss.bodies, stageContacts = ss.contacts;
@@ -2645,12 +2645,28 @@ __global__ void __launch_bounds__(kMaxBlock) k_finish(const __grid_constant__ Ba
                 uA[pos] = cs[ci].bodyA - wi.bodyFirst;
                 uB[pos] = cs[ci].bodyB - wi.bodyFirst;
             });
-        if (g.tid == 0) {
-            for (uint32_t x = 0; x < nu; ++x) {
+        // The unions run in parallel: each round links the higher of a pair's roots under the lower (parents
+        // only ever point to lower bodies, so an atomicMin keeps the lowest link), then points every body at
+        // its root, until a round links nothing. Each component ends rooted at its lowest body, which is what
+        // the reference's sequential unions give.
+        for (;;) {
+            if (g.tid == 0) { s_linked[g.id] = 0; }
+            g.sync();
+            for (uint32_t x = g.tid; x < nu; x += g.size) {
                 if (!TF_OK_INDEX(B, uA[x] < wi.bodyCount && uB[x] < wi.bodyCount, 24, w, x)) { continue; }
-                const uint32_t ra = findRoot(parent, uA[x]), rb = findRoot(parent, uB[x]);
-                if (ra != rb) { parent[ra > rb ? ra : rb] = ra < rb ? ra : rb; }
+                const uint32_t ra = rootOf(parent, uA[x]), rb = rootOf(parent, uB[x]);
+                if (ra != rb) {
+                    atomicMin(&parent[ra > rb ? ra : rb], ra < rb ? ra : rb);
+                    s_linked[g.id] = 1;
+                }
             }
+            g.sync();
+            const bool again = s_linked[g.id] != 0;
+            for (uint32_t i = g.tid; again && i < wi.bodyCount; i += g.size) { parent[i] = rootOf(parent, i); }
+            g.sync();
+            if (!again) { break; }
+        }
+        if (g.tid == 0) {
             // Joints that hold link their bodies too (src/world.cpp:1210-1222).
             const DJoint* js = B.joints + wi.jointFirst;
             for (uint32_t x = 0; x < wi.jointCount; ++x) {
