@@ -1497,7 +1497,12 @@ public:
             const int threads = (int)shapes[f < kPairClasses ? 7 : 4].threads;
             TF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, flat[f], threads, 0));
             if (perSm < 1) { return fail(TF_E_INVALID, "launch shape does not fit on an SM"); }
-            flatGrids[f] = smCount * perSm;
+            // No more CTAs than the class list can ever fill: its capacity is the batch's candidate slots (pair
+            // collisions) or contact slots (refreshes). A small batch then launches a handful of CTAs rather
+            // than a full device's worth that find no work.
+            const size_t cap = f < kPairClasses ? totalCand : totalContacts;
+            const size_t needed = std::max<size_t>(1, (cap + (size_t)threads - 1) / (size_t)threads);
+            flatGrids[f] = (int)std::min<size_t>((size_t)smCount * (size_t)perSm, needed);
         }
         return TF_OK;
     }
