@@ -1174,25 +1174,27 @@ __global__ void __launch_bounds__(128) k_model_forward(const __grid_constant__ M
 // chunk's steps are recomputed all at once, one warp per world and step, each logging into its own slot; then
 // one warp per world walks the chunk's steps in reverse from those logs, carrying the adjoints back.
 template <class T>
-__global__ void __launch_bounds__(128) k_model_recompute(const __grid_constant__ Model<T> M, int first, int count) {
+__global__ void __launch_bounds__(128) k_model_recompute(const __grid_constant__ Model<T> M, int first, int count,
+                                                         uint32_t slotBase) {
     const uint32_t warp = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
     const uint32_t nw = (uint32_t)M.S.nWorlds;
     const uint32_t k = warp / nw, w = warp % nw;
     if (k >= (uint32_t)count) { return; }
-    const Slot<T> W = slotOf(M, k);
+    const Slot<T> W = slotOf(M, slotBase + k);
     const int s = first + (int)k;
     const size_t stride = (size_t)M.S.totalBodies * kState;
     stepWorld(M, W, s, w, M.states + s * stride, W.scratch, W.log + (size_t)w * M.logStride, W.integLog);
 }
 
 template <class T>
-__global__ void __launch_bounds__(128) k_model_reverse(const __grid_constant__ Model<T> M, int first, int count) {
+__global__ void __launch_bounds__(128) k_model_reverse(const __grid_constant__ Model<T> M, int first, int count,
+                                                       uint32_t slotBase) {
     const uint32_t w = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
     if (w >= (uint32_t)M.S.nWorlds) { return; }
     const size_t stride = (size_t)M.S.totalBodies * kState;
     for (int k = count - 1; k >= 0; --k) {
         const int s = first + k;
-        const Slot<T> W = slotOf(M, (uint32_t)k);
+        const Slot<T> W = slotOf(M, slotBase + (uint32_t)k);
         // The number of contact operations the step logged: every pass walks its lists once.
         const WorldView V = viewOf(M.S, s, w);
         const TapeWorld& tw = *V.tw;
@@ -1220,11 +1222,20 @@ struct Run {
          *invIAdj = nullptr, *pointAdj = nullptr, *massAdj = nullptr, *frictionAdj = nullptr, *log = nullptr,
          *integLog = nullptr, *scratch = nullptr;
     uint64_t logStride = 0;
-    int slots = 0;  // steps the backward recomputes at once
+    int slots = 0;  // steps the backward recomputes at once; two sets of slots alternate
     bool forwardDone = false;
     float forwardMs = 0.0f, backwardMs = 0.0f;
+    // The recomputation runs on its own stream, one chunk ahead of the reverse walk.
+    cudaStream_t side = nullptr;
+    cudaEvent_t ready = nullptr, recomputed[2] = {}, reversed[2] = {};
 
-    ~Run() { release(); }
+    ~Run() {
+        release();
+        for (cudaEvent_t e : { ready, recomputed[0], recomputed[1], reversed[0], reversed[1] }) {
+            if (e) { cudaEventDestroy(e); }
+        }
+        if (side) { cudaStreamDestroy(side); }
+    }
     void release() {
         for (void* p : owned) { cudaFree(p); }
         owned.clear();
@@ -1404,8 +1415,8 @@ int backwardT(Run& r, const AdjointSetup& S, cudaStream_t stream, const double* 
         size_t freeBytes = 0, totalBytes = 0;
         TF_ADJ_CUDA(cudaMemGetInfo(&freeBytes, &totalBytes));
         const size_t budget = std::min<size_t>(freeBytes / 2, (size_t)32 << 30);
-        r.slots = (int)std::max<size_t>(1, std::min<size_t>((size_t)S.nSteps, budget / std::max<size_t>(perSlot, 1)));
-        const size_t k = (size_t)r.slots;
+        r.slots = (int)std::max<size_t>(1, std::min<size_t>((size_t)S.nSteps, budget / 2 / std::max<size_t>(perSlot, 1)));
+        const size_t k = 2 * (size_t)r.slots;
         // The forward's single-slot working arrays give way to one per slot.
         for (void** p : { &r.invM, &r.invI, &r.dp, &r.dq, &r.qBase, &r.points }) {
             auto it = std::find(r.owned.begin(), r.owned.end(), *p);
@@ -1438,13 +1449,29 @@ int backwardT(Run& r, const AdjointSetup& S, cudaStream_t stream, const double* 
     cudaEvent_t e0, e1;
     TF_ADJ_CUDA(cudaEventCreate(&e0));
     TF_ADJ_CUDA(cudaEventCreate(&e1));
+    if (!r.side) {
+        TF_ADJ_CUDA(cudaStreamCreateWithFlags(&r.side, cudaStreamNonBlocking));
+        for (cudaEvent_t* e : { &r.ready, &r.recomputed[0], &r.recomputed[1], &r.reversed[0], &r.reversed[1] }) {
+            TF_ADJ_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+        }
+    }
     cudaEventRecord(e0, stream);
+    cudaEventRecord(r.ready, stream);
+    TF_ADJ_CUDA(cudaStreamWaitEvent(r.side, r.ready, 0));
     const int blocks = (S.nWorlds + 3) / 4;
-    for (int end = S.nSteps; end > 0;) {
-        const int count = std::min(end, r.slots), first = end - count;
+    // Chunk c recomputes into slot set c % 2 on the side stream once the reverse walk of chunk c - 2 has left
+    // that set, so that it runs beside the walk of chunk c - 1; the walk of chunk c waits for its recompute.
+    int c = 0;
+    for (int end = S.nSteps; end > 0; ++c) {
+        const int count = std::min(end, r.slots), first = end - count, set = c % 2;
+        const uint32_t base = (uint32_t)(set * r.slots);
         const unsigned warps = (unsigned)count * (unsigned)S.nWorlds;
-        k_model_recompute<T><<<(warps + 3) / 4, 128, 0, stream>>>(M, first, count);
-        k_model_reverse<T><<<blocks, 128, 0, stream>>>(M, first, count);
+        if (c >= 2) { TF_ADJ_CUDA(cudaStreamWaitEvent(r.side, r.reversed[set], 0)); }
+        k_model_recompute<T><<<(warps + 3) / 4, 128, 0, r.side>>>(M, first, count, base);
+        cudaEventRecord(r.recomputed[set], r.side);
+        TF_ADJ_CUDA(cudaStreamWaitEvent(stream, r.recomputed[set], 0));
+        k_model_reverse<T><<<blocks, 128, 0, stream>>>(M, first, count, base);
+        cudaEventRecord(r.reversed[set], stream);
         end = first;
     }
     cudaEventRecord(e1, stream);
