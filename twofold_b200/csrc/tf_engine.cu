@@ -170,6 +170,10 @@ public:
     DevArray<uint64_t> dMergeKeyA, dMergeKeyB;
     DevArray<uint32_t> dMergePartA, dMergePartB, dMergeIdxA, dMergeIdxB;
     bool hasJoints = false;  // some world has joints: the substep and finish kernels with joint code run
+    // A batch this small collides and refreshes every pair class in one launch each (k_collide_all,
+    // k_refresh_all): its class lists hold few items, and a launch per class costs more than their work.
+    bool smallBatch = false;
+    static constexpr size_t kSmallBatchCandidates = 8192;
     DevArray<DJoint> dJoints;
     DevArray<uint64_t> dJoined;
     DevArray<TouchEvent> dTouchEvents;
@@ -1017,6 +1021,7 @@ public:
             sortedSizes = std::move(sizes);
         }
         hasJoints = njoints > 0;
+        smallBatch = ncand <= kSmallBatchCandidates;
         laidOut = true;
         {
             const int rc0 = configureLaunches();
@@ -1338,6 +1343,11 @@ public:
         });
         if (marks) { cudaEventRecord(marks[1], stream); }
         timed(7, rec, [&] {
+            if (smallBatch) {
+                k_collide_all<<<*std::max_element(flatGrids, flatGrids + kPairClasses), threads(7), 0, stream>>>(B, P,
+                                                                                                           serial);
+                return;
+            }
             k_collide<kClassSpheres><<<flatGrids[0], threads(7), 0, stream>>>(B, P, serial);
             k_collide<kClassSpherePoly><<<flatGrids[1], threads(7), 0, stream>>>(B, P, serial);
             k_collide<kClassPlane><<<flatGrids[2], threads(7), 0, stream>>>(B, P, serial);
@@ -1356,6 +1366,10 @@ public:
         for (int i = 0; i < P.substeps; ++i) {
             if (i > 0) {
                 timed(4, rec, [&] {
+                    if (smallBatch) {
+                        k_refresh_all<<<flatGrids[6], threads(4), 0, stream>>>(B, P, i, serial);
+                        return;
+                    }
                     k_refresh<kClassAny><<<flatGrids[6], threads(4), 0, stream>>>(B, P, i, serial);
                     k_refresh<kClassSpheres><<<flatGrids[7], threads(4), 0, stream>>>(B, P, i, serial);
                     k_refresh<kClassSpherePoly><<<flatGrids[8], threads(4), 0, stream>>>(B, P, i, serial);
@@ -1381,7 +1395,9 @@ public:
             }
         });
         if (marks) { cudaEventRecord(marks[3], stream); }
-        launches += 5 + kPairClasses + P.substeps + (kPairClasses + 1) * (P.substeps - 1) + (bigWorlds.empty() ? 0 : 2);
+        launches += smallBatch ? 5 + 1 + P.substeps + (P.substeps - 1) + (bigWorlds.empty() ? 0 : 2)
+                               : 5 + kPairClasses + P.substeps + (kPairClasses + 1) * (P.substeps - 1) +
+                                     (bigWorlds.empty() ? 0 : 2);
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) { return fail(TF_E_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e)); }
         return TF_OK;

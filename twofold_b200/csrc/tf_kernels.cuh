@@ -1174,9 +1174,7 @@ __device__ void narrowMesh(const Batch& B, const StepParams& P, const WorldInfo&
 // The candidate pairs of one class, over every world, one thread per pair (src/world.cpp:874-960); each
 // result lands in the pair's own staging slot, so pairs need no order among themselves.
 template <int Cls>
-__global__ void __launch_bounds__(256) k_collide(const __grid_constant__ Batch B, const __grid_constant__ StepParams P,
-                                                 int serial) {
-    if (stepAborted(B, serial)) { return; }
+__device__ __forceinline__ void collideClass(const Batch& B, const StepParams& P, int serial) {
     const uint32_t n = *(volatile uint32_t*)(B.work + kSlotCandItems + Cls);
     const uint2* items = B.candItems + (size_t)Cls * B.candItemStride;
     for (uint32_t item = blockIdx.x * blockDim.x + threadIdx.x; item < n; item += gridDim.x * blockDim.x) {
@@ -1189,6 +1187,26 @@ __global__ void __launch_bounds__(256) k_collide(const __grid_constant__ Batch B
             narrowOne<Cls>(B, P, wi, wc, it.y, B.previous + wi.contactFirst, wc.contactCount);
         }
     }
+}
+
+template <int Cls>
+__global__ void __launch_bounds__(256) k_collide(const __grid_constant__ Batch B, const __grid_constant__ StepParams P,
+                                                 int serial) {
+    if (stepAborted(B, serial)) { return; }
+    collideClass<Cls>(B, P, serial);
+}
+
+// Small batches collide every pair class in one launch, each class's list in turn over the whole grid (the
+// classes' pairs are disjoint); large batches launch a kernel per class, which keeps a warp on one code path.
+__global__ void __launch_bounds__(256) k_collide_all(const __grid_constant__ Batch B, const __grid_constant__ StepParams P,
+                                                     int serial) {
+    if (stepAborted(B, serial)) { return; }
+    collideClass<kClassSpheres>(B, P, serial);
+    collideClass<kClassSpherePoly>(B, P, serial);
+    collideClass<kClassPlane>(B, P, serial);
+    collideClass<kClassConvex>(B, P, serial);
+    collideClass<kClassPlanar>(B, P, serial);
+    collideClass<kClassMesh>(B, P, serial);
 }
 
 __device__ __forceinline__ bool keyLess(uint64_t ka, uint32_t pa, uint64_t kb, uint32_t pb) {
@@ -1951,9 +1969,7 @@ __device__ __forceinline__ bool refreshedAt(const WorldCounts& wc, int sub, int 
 // contacts (kClassAny). The body half runs in the substeps around it: the substep before updates the world
 // inverse inertia at its end, the substep after resets dp and dq before anything reads them.
 template <int Cls>
-__global__ void __launch_bounds__(256) k_refresh(const __grid_constant__ Batch B, const __grid_constant__ StepParams P,
-                                                 int sub, int serial) {
-    if (stepAborted(B, serial)) { return; }
+__device__ __forceinline__ void refreshClass(const Batch& B, const StepParams& P, int sub) {
     const int n = P.substeps;
     const uint8_t againFlag = sub == n / 2 ? kFlagFast : kFlagFastSolid;
     const float remaining = (float)(n - sub) * P.h;
@@ -1996,6 +2012,27 @@ __global__ void __launch_bounds__(256) k_refresh(const __grid_constant__ Batch B
         makeContactAxes(axisBodyOf(B.bodies[c.bodyA]), axisBodyOf(B.bodies[c.bodyB]), c,
                         B.axes + (size_t)(wi.contactFirst + ci) * kAxesPerContact);
     }
+}
+
+template <int Cls>
+__global__ void __launch_bounds__(256) k_refresh(const __grid_constant__ Batch B, const __grid_constant__ StepParams P,
+                                                 int sub, int serial) {
+    if (stepAborted(B, serial)) { return; }
+    refreshClass<Cls>(B, P, sub);
+}
+
+// Small batches refresh every list in one launch (the lists hold disjoint contacts: a pair's contacts are fast
+// or not together); large batches launch a kernel per list.
+__global__ void __launch_bounds__(256) k_refresh_all(const __grid_constant__ Batch B, const __grid_constant__ StepParams P,
+                                                     int sub, int serial) {
+    if (stepAborted(B, serial)) { return; }
+    refreshClass<kClassAny>(B, P, sub);
+    refreshClass<kClassSpheres>(B, P, sub);
+    refreshClass<kClassSpherePoly>(B, P, sub);
+    refreshClass<kClassPlane>(B, P, sub);
+    refreshClass<kClassConvex>(B, P, sub);
+    refreshClass<kClassPlanar>(B, P, sub);
+    refreshClass<kClassMesh>(B, P, sub);
 }
 
 // One pass over a world's joints on one thread, before the contacts of that pass (src/world.cpp:1670-1680,
