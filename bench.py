@@ -136,35 +136,52 @@ class ClockSampler:
     def __init__(self, index):
         self.index = index
         self.proc = None
-        self.lines = []
+        self.lines = []  # (host time, csv line)
+        self.window_start = self.window_stop = None
 
-    def __enter__(self):
+    def start(self):
+        """Starts sampling ahead of the timed region: nvidia-smi takes a fraction of a second to begin, longer
+        than the whole timed region can be; only samples inside the window count."""
+        if self.proc:
+            return self
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.index}", "--query-gpu=" + ",".join(self.FIELDS), "--format=csv,noheader,nounits",
-                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                 "-lms", "50"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
         except OSError:
             self.proc = None
         return self
 
+    def __enter__(self):
+        self.start()
+        self.window_start = time.monotonic()
+        return self
+
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.monotonic(), line.strip()))
 
     def __exit__(self, *exc):
+        self.window_stop = time.monotonic()
+
+    def close(self):
         if self.proc:
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
             except subprocess.TimeoutExpired:
                 self.proc.kill()
+            self.proc = None
 
     def summary(self):
         sm, smax, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in self.lines:
+        lo, hi = self.window_start or 0.0, (self.window_stop or time.monotonic()) + 0.05
+        for t, line in list(self.lines):
+            if not lo <= t <= hi:
+                continue
             parts = [p.strip() for p in line.split(",")]
             if len(parts) < 7:
                 continue
@@ -359,14 +376,17 @@ def run_b200(args, dist):
     tune_s = time.perf_counter() - t_tune
     launches0 = batch.launches()
     steps0 = batch.body_steps()
+    clocks = ClockSampler(dist.local_rank).start()
+    time.sleep(1.0)  # nvidia-smi is sampling by the time the timed region starts
     dist.barrier()
     device_ms = 0.0
     t0 = time.perf_counter()
-    with ClockSampler(dist.local_rank) as clocks:
+    with clocks:
         for _ in range(args.steps):
             batch.step_checked(dt, 1, graph=True)
             device_ms += batch.elapsed_ms()
     wall = time.perf_counter() - t0
+    clocks.close()
     dist.barrier()
     body_steps = batch.body_steps() - steps0
     launches = batch.launches() - launches0
