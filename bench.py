@@ -9,8 +9,12 @@ restitution, sleep) from one CUDA graph per step.
     python bench.py [--gpus N] [--steps K] [--warmup W] [--worlds 4096] [--impl b200|reference]
 
 value: awake dynamic bodies summed over the K timed steps of all worlds on all GPUs, divided by the device
-time of those steps (CUDA events on the library's stream; max over ranks). Under torchrun every rank steps its
-own 4096 worlds (weak scaling, no collective in the step).
+time of those steps (CUDA events on the library's stream; max over ranks). Under torchrun the world set holds
+4096 worlds per GPU and is split over the ranks by longest-processing-time on body counts (weak scaling, no
+collective in the step; one gather of per-world results after timing).
+
+parity: the end-to-end batch's every 4th world against the reference stepping the same worlds the same steps
+(the CPU baseline's own run): states within 1e-5, bit-identical worlds and identical candidate pairs.
 
 e2e: the same metric through the public C ABI on a fresh batch stepped the same way, with each step's
 inputs (per-body forces, from pinned host memory) copied in and every body's pose copied out inside the
@@ -254,11 +258,14 @@ def substep_bytes(work):
 
 
 def load_traffic():
+    """The k_substep DRAM traffic of one ncu capture, with the work counts of the step it was captured on."""
     path = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(path):
         with open(path) as f:
-            return json.load(f)
-    return {}
+            t = json.load(f)
+        if "work" in t and "k_substep_bytes_per_launch" in t:
+            return t
+    return None
 
 
 PLAIN_STRIDE = 64  # every 64th world stepped on its own
@@ -266,7 +273,8 @@ PLAIN_STRIDE = 64  # every 64th world stepped on its own
 
 def plain_rate(sc, args, device):
     """Body-steps/s of the plain path: worlds stepped one by one, each a batch of one world on the same GPU
-    (its own graph per step), over a sample of the workload's worlds; device time summed over the worlds."""
+    (its own graph per step, launch shapes from the autotuner on that world after the warm-up, as the batch
+    has), over a sample of the workload's worlds; device time summed over the worlds."""
     from twofold_b200.world import Batch
 
     ms, body_steps = 0.0, 0
@@ -275,6 +283,7 @@ def plain_rate(sc, args, device):
         one = Batch([w], sc.settings, device=device)
         for _ in range(args.warmup):
             one.step_checked(sc.dt, 1, graph=True)
+        one.autotune(sc.dt, trial_steps=1)
         b0 = one.body_steps()
         for _ in range(args.steps):
             one.step_checked(sc.dt, 1, graph=True)
@@ -282,7 +291,7 @@ def plain_rate(sc, args, device):
         body_steps += one.body_steps() - b0
         one.close()
     return {"value": body_steps / (ms / 1e3), "unit": UNIT, "device_ms": ms,
-            "sample": f"every {PLAIN_STRIDE}th world ({len(sample)} of {len(sc.worlds)}), each alone, steps "
+            "sample": f"every {PLAIN_STRIDE}th world ({len(sample)} of {len(sc.worlds)}), each alone and tuned, steps "
                       f"{args.warmup + 1}-{args.warmup + args.steps}"}
 
 
@@ -354,13 +363,48 @@ def adjoint_cost(device, n_worlds=1024, steps=120):
             "pipeline_forward_ms": pipe_ms, "backward_over_pipeline_forward": bwd / pipe_ms}
 
 
+BREAKDOWN_STEPS = 10  # graph-replayed steps after the timed region, with an event pair around each kernel group
+
+
+def world_set(args, dist):
+    """This rank's shard of the one seeded world set: args.worlds worlds per GPU in total, split over the ranks
+    by longest-processing-time on body counts (a single GPU takes the whole set, in order)."""
+    from twofold_b200 import scenes, shard
+
+    total = args.worlds * dist.world_size
+    counts = scenes.config4_bodies(total)
+    shards = shard.lpt_partition(counts, dist.world_size)
+    mine = shards[dist.rank]
+    return scenes.config4(n_worlds=total, only=mine), shards, counts
+
+
+def state_parity(batch, refs, stride):
+    """World states of the GPU batch against the reference worlds (the batch's every stride-th world, stepped
+    the same steps): normwise relative error of positions, rotations and velocities, bit-identical worlds, and
+    worlds whose candidate pair keys are identical."""
+    worst, same, cands = 0.0, 0, 0
+    for k, r in enumerate(refs):
+        wi = k * stride
+        mine, theirs = batch.world_states(wi), r.states()
+        for key in ("p", "q", "v", "w"):
+            a = np.asarray(mine[key], np.float64)
+            b = np.asarray(theirs[key], np.float64)
+            if a.size:
+                worst = max(worst, float(np.max(np.abs(a - b)) / max(float(np.max(np.abs(b))), 1e-6)))
+        same += all(np.array_equal(np.asarray(mine[key]).view(np.uint32), np.asarray(theirs[key]).view(np.uint32))
+                    for key in ("p", "q", "v", "w"))
+        cands += bool(np.array_equal(batch.candidates(wi), r.candidates()))
+    return {"worlds": len(refs), "max_rel_err": worst, "tolerance": 1e-5, "bit_identical_worlds": same,
+            "candidates_equal_worlds": cands}
+
+
 def run_b200(args, dist):
-    from twofold_b200 import abi, scenes
+    from twofold_b200 import abi
     from twofold_b200.world import Batch
 
     abi.load()
     n = dist.world_size
-    sc = scenes.config4(n_worlds=args.worlds, seed=dist.rank)
+    sc, shards, counts = world_set(args, dist)
     dt = sc.dt
     batch = Batch.from_scene(sc, device=dist.local_rank)
     for _ in range(args.warmup):
@@ -394,11 +438,16 @@ def run_b200(args, dist):
     total_body_steps = dist.reduce(body_steps, "SUM")
     value = total_body_steps / (max_ms / 1e3)
 
-    # Per-kernel times of the next 3 steps, each launch bracketed by CUDA events on the library's stream.
+    # Per-kernel times of the next steps, replayed from graphs that hold an event pair around each kernel group,
+    # with the algorithmic bytes of every k_substep launch from the work counts of its own step.
     batch.set_profiling(True)
-    batch.step_checked(dt, 3)
+    prof_ms, sub_bytes, works = 0.0, 0, []
+    for _ in range(BREAKDOWN_STEPS):
+        batch.step_checked(dt, 1, graph=True)
+        prof_ms += batch.elapsed_ms()
+        works.append(batch.work_counts())
+        sub_bytes += substep_bytes(works[-1]) * 4
     kt = batch.kernel_times()
-    work = batch.work_counts()
     batch.set_profiling(False)
     top = max(kt, key=lambda k: kt[k][0])
     peaks = {}
@@ -407,9 +456,11 @@ def run_b200(args, dist):
         with open(peaks_path) as f:
             peaks = json.load(f)
     peak = float(peaks.get("hbm_gbs", 6650.0))
-    sub_ms = kt["k_substep"][0] / max(kt["k_substep"][1], 1)
-    achieved = substep_bytes(work) / (sub_ms / 1e3) / 1e9
-    traffic = load_traffic().get("k_substep_bytes_per_launch")
+    sub_ms_total = kt["k_substep"][0]
+    sub_launches = max(kt["k_substep"][1], 1)
+    achieved = sub_bytes / (sub_ms_total / 1e3) / 1e9
+    traffic = load_traffic()
+    breakdown = {k: v[0] / BREAKDOWN_STEPS for k, v in kt.items()}
 
     # End to end: a fresh batch, the same warm-up, then per step: forces in, step, poses out.
     del batch
@@ -440,6 +491,41 @@ def run_b200(args, dist):
     dist.barrier()
     e_body_steps = dist.reduce(e2e_batch.body_steps() - e_steps0, "SUM")
     e_wall = dist.reduce(e_wall, "MAX")
+
+    # Every rank's per-world results to rank 0 (outside every timed region): one gather of each world's pose
+    # checksum, keyed by its number in the whole set.
+    digests = {}
+    for k, w in enumerate(shards[dist.rank]):
+        st = e2e_batch.world_states(k)
+        digests[int(w)] = float(np.abs(np.asarray(st["p"], np.float64)).sum())
+    gathered = [digests]
+    if dist.pg:
+        gathered = [None] * n
+        dist.pg.all_gather_object(gathered, digests)
+    worlds_gathered = sum(len(g) for g in gathered)
+
+    cpu = None
+    parity = None
+    if dist.rank == 0 and n == 1 and not args.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import reference as R
+
+        if R.available():
+            threads = R.hardware_threads()
+            sample = sc.worlds[::SAMPLE_STRIDE]
+            refs = [R.RefWorld(w, sc.settings) for w in sample]
+            if args.warmup:
+                R.step_parallel(refs, dt, args.warmup, threads)
+            t_ref = time.perf_counter()
+            bsteps = R.step_parallel(refs, dt, args.steps, threads)
+            el = time.perf_counter() - t_ref
+            cpu = {"value": bsteps / el, "unit": UNIT, "cores": threads, "kind": "reference",
+                   "sample": f"every {SAMPLE_STRIDE}th world ({len(sample)} of {args.worlds}), steps "
+                             f"{args.warmup + 1}-{args.warmup + args.steps}, {bsteps} body-steps in {el:.2f} s"}
+            # The same worlds of the end-to-end batch, after the same steps, against those reference worlds.
+            parity = state_parity(e2e_batch, refs, SAMPLE_STRIDE)
+            parity["steps"] = args.warmup + args.steps
+            parity["compared"] = "end-to-end batch (forces of zero added every step) against the reference sample"
     del e2e_batch
 
     # The plain path for comparison: a sample of the same worlds, each stepped alone as a batch of one.
@@ -453,37 +539,37 @@ def run_b200(args, dist):
     if dist.rank == 0 and n == 1 and not args.no_extras:
         singles = single_worlds(dist.local_rank)
 
-    cpu = None
-    if dist.rank == 0 and n == 1 and not args.no_cpu_baseline:
-        sys.path.insert(0, os.path.join(ROOT, "oracle"))
-        import reference as R
-
-        if R.available():
-            threads = R.hardware_threads()
-            sample = sc.worlds[::SAMPLE_STRIDE]
-            rate, bsteps, el = reference_rate(sample, sc.settings, dt, args.warmup, args.steps, threads)
-            cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": "reference",
-                   "sample": f"every {SAMPLE_STRIDE}th world ({len(sample)} of {args.worlds}), steps "
-                             f"{args.warmup + 1}-{args.warmup + args.steps}, {bsteps} body-steps in {el:.2f} s"}
-
     if dist.rank == 0:
+        roof = {"bound": "hbm", "kernel": "k_substep", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": None,
+                "peak_source": "measured hbm_gbs (MEASURED_PEAKS.json)" if "hbm_gbs" in peaks else "fallback",
+                "algorithmic_bytes_per_launch": sub_bytes / sub_launches, "avg_launch_ms": sub_ms_total / sub_launches,
+                "timed_on": f"{BREAKDOWN_STEPS} graph-replayed steps after the timed region, an event pair per kernel",
+                "top_kernel_by_time": top}
+        if traffic:
+            roof["traffic"] = traffic["k_substep_bytes_per_launch"]
+            roof["traffic_state"] = traffic["work"]
+            roof["traffic_over_algorithmic"] = traffic["k_substep_bytes_per_launch"] / substep_bytes(traffic["work"])
+            roof["traffic_source"] = traffic.get("source")
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": n, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": max_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32", "data": "synthetic (seeded scenes, seed = rank)", "config": config(args, n),
+            "dtype": "f32", "data": "synthetic: one seeded world set, split over the GPUs by body count",
+            "config": config(args, n),
             "e2e": {"value": e_body_steps / e_wall, "unit": UNIT, "h2d_bytes_per_step": int(forces.nbytes),
                     "d2h_bytes_per_step": int(poses.nbytes + rots.nbytes)},
             "gpu_launches": int(launches),
-            "roofline": {"bound": "hbm", "kernel": "k_substep", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": traffic,
-                         "peak_source": "measured hbm_gbs (MEASURED_PEAKS.json)" if "hbm_gbs" in peaks else "fallback",
-                         "algorithmic_bytes_per_launch": substep_bytes(work), "avg_launch_ms": sub_ms,
-                         "timed_on": "3 direct steps after the timed region, per-launch CUDA events",
-                         "top_kernel_by_time": top},
-            "kernel_ms_per_step": {k: v[0] / 3 for k, v in kt.items()},
+            "roofline": roof,
+            "parity": parity,
+            "kernel_breakdown": {"ms_per_step": breakdown, "sum_ms": sum(breakdown.values()),
+                                 "steps_ms_per_step": prof_ms / BREAKDOWN_STEPS,
+                                 "steps": f"{args.warmup + args.steps + 1}..{args.warmup + args.steps + BREAKDOWN_STEPS}",
+                                 "mode": "graph replay, the graph holding an event pair around each kernel group"},
             "launch_shapes": {k: list(v) for k, v in shapes.items()},
             "autotune_s": tune_s,
-            "work_last_step": work,
+            "work_last_step": works[-1],
+            "shards": {"worlds": [len(s) for s in shards],
+                       "bodies": [int(counts[s].sum()) for s in shards], "worlds_gathered": worlds_gathered},
             "wall_s_timed_region": wall,
             "clocks": clocks.summary(),
             "cpu_baseline": cpu,

@@ -440,7 +440,11 @@ TF_API int tf_world_get_launch(void* world, int32_t kernel, uint32_t out[6]);
  * index), from device arrays the caller owns: lo and hi (n x 3 floats, the shapes' world bounds), grow (n
  * floats, each body's growth for the step) and flags (n words of TF_PAIR_* bits). The pair rules are the
  * step's (World::Impl::updateContacts, src/world.cpp:788-842, for single-shape bodies), and the result is
- * what tf_world_candidates reports for such a world: keys min << 32 | max, sorted and unique. Up to
+ * what tf_world_candidates reports for such a world: keys min << 32 | max, sorted and unique, as long as the
+ * world also has default collision filters (every category and mask bit set), no joints and no half-space
+ * shapes. Three of the step's rules are not applied here: the category/mask filter (src/world.cpp:334-337),
+ * the exclusion of jointed body pairs (:796, :829) and the half-space pairs (:843-866); a caller with any
+ * of those filters, joints or planes drops or adds those pairs itself. Up to
  * `capacity` keys go to the device array `keys`; the device word `count` receives the number of unique
  * keys (more than capacity when they did not all fit), or -1 when the pair tests found more than
  * TF_NOALLOC_MAX_PAIRS keys before repeats were dropped (keys is then left as it was).
@@ -449,8 +453,10 @@ TF_API int tf_world_get_launch(void* world, int32_t kernel, uint32_t out[6]);
  * TF_NOALLOC_MAX_BODIES is refused with TF_E_CAPACITY. The work is queued on `stream` (a cudaStream_t; NULL
  * for the default stream) on the current device and the call returns without waiting. The first call on a
  * device looks up the scratch's address there (with that device current), so make it before any stream
- * capture. Calls whose work overlaps on one device (other streams, other host threads) share the scratch and
- * race; order them on one stream. */
+ * capture. That address is kept for the life of the process: after cudaDeviceReset on a device (which
+ * unloads the library's device image there) this entry point must not be called on that device again.
+ * Calls whose work overlaps on one device (other streams, other host threads) share the scratch and race;
+ * order them on one stream. */
 #define TF_NOALLOC_MAX_BODIES 4096
 #define TF_NOALLOC_MAX_PAIRS 32768
 enum tf_pair_flags { TF_PAIR_LIVE = 1u << 0, TF_PAIR_DYNAMIC = 1u << 1, TF_PAIR_MOVING = 1u << 2 };

@@ -202,8 +202,11 @@ class RefWorld:
 
 def step_parallel(ref_worlds, dt, steps, threads):
     """Steps independent reference worlds, each by one thread from a pool of `threads`. Returns the
-    awake-dynamic body-steps summed over every step of every world."""
-    lib = load()
+    awake-dynamic body-steps summed over every step of every world. The worlds come from one build of the
+    oracle, whose stepping code runs them."""
+    if not ref_worlds:
+        return 0
+    lib = ref_worlds[0].lib
     arr = (C.c_void_p * len(ref_worlds))(*[r.h for r in ref_worlds])
     total = C.c_int64(0)
     lib.ref_worlds_step_parallel(arr, len(ref_worlds), C.c_float(dt), steps, threads, C.byref(total))

@@ -20,7 +20,7 @@ PROGRAMS = [
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("TWOFOLD_REF", "/root/reference")
     sources = sorted(os.path.join(ref, "src", f) for f in os.listdir(os.path.join(ref, "src")) if f.endswith(".cpp"))
     for program, args, golden in PROGRAMS:
         src = os.path.join(ROOT, "tests", "dropin", program)

@@ -106,3 +106,34 @@ def test_noalloc_refuses_more_bodies_than_its_scratch():
     rc = lib.tf_candidates_noalloc(None, None, None, None, n, None, 0, C.byref(cnt), None)
     assert rc == abi.TF_E_CAPACITY
     assert b"4096" in lib.tf_last_error()
+
+
+@pytest.mark.gpu
+def test_noalloc_reports_too_many_raw_pairs_and_recovers():
+    """300 bodies in one overlapping cluster make n(n-1)/2 = 44850 raw pair hits, more than the scratch holds:
+    the count is -1 and the keys keep their fill value. A normal call afterwards gives the full answer again."""
+    torch = pytest.importorskip("torch")
+    lib = abi.load()
+    n = 300
+    assert n * (n - 1) // 2 > abi.TF_NOALLOC_MAX_PAIRS
+    lo = np.zeros((n, 3), F32)
+    hi = np.ones((n, 3), F32)
+    grow = np.full(n, F32(0.02), F32)
+    flags = np.full(n, abi.TF_PAIR_LIVE | abi.TF_PAIR_DYNAMIC | abi.TF_PAIR_MOVING, np.uint32)
+    dev = torch.device("cuda:0")
+    keys = torch.full((64,), -1, dtype=torch.int64, device=dev)
+    count = torch.zeros((1,), dtype=torch.int32, device=dev)
+    t = [torch.from_numpy(x.reshape(-1).view(np.int32) if x.dtype == np.uint32 else x.reshape(-1)).to(dev)
+         for x in (lo, hi, grow, flags)]
+    rc = lib.tf_candidates_noalloc(t[0].data_ptr(), t[1].data_ptr(), t[2].data_ptr(), t[3].data_ptr(), n,
+                                   keys.data_ptr(), 64, count.data_ptr(), C.c_void_p(torch.cuda.current_stream().cuda_stream))
+    abi.check(rc, lib)
+    torch.cuda.synchronize()
+    assert int(count.item()) == -1
+    assert bool((keys == -1).all()), "keys were written although the raw hits overflowed"
+    world = _sphere_world(300, 3.0, 0)
+    lo2, hi2, grow2, flags2 = _pair_inputs(world, abi.default_settings())
+    full_n, full = _noalloc(lib, torch, lo2, hi2, grow2, flags2, capacity=20000)
+    assert full_n > 8
+    again_n, again = _noalloc(lib, torch, lo2, hi2, grow2, flags2, capacity=20000)
+    assert again_n == full_n and np.array_equal(again, full)

@@ -243,15 +243,29 @@ public:
     std::vector<int> eventKind;
     int eventsUsed = 0;
 
-    // Graph replay: one recorded graph per contact buffer a sequence starts from.
+    // Graph replay: one recorded graph per contact buffer a sequence starts from. A graph recorded while
+    // per-kernel profiling is on also records an event pair around each kernel group (graphTimers: kind, start,
+    // stop), read after every replay, so the per-kernel times come from the replayed steps themselves.
     cudaGraphExec_t graphs[2] = { nullptr, nullptr };
     int graphSteps = 0;
     float graphDt = 0.0f;
+    bool graphProfiled = false;
+    struct KernelTimer {
+        int kind;
+        cudaEvent_t start, stop;
+    };
+    std::vector<KernelTimer> graphTimers[2];
+    std::vector<KernelTimer>* captureTimers = nullptr;
 
     void dropGraphs() {
-        for (cudaGraphExec_t& g : graphs) {
-            if (g) { cudaGraphExecDestroy(g); }
-            g = nullptr;
+        for (int b = 0; b < 2; ++b) {
+            if (graphs[b]) { cudaGraphExecDestroy(graphs[b]); }
+            graphs[b] = nullptr;
+            for (KernelTimer& t : graphTimers[b]) {
+                cudaEventDestroy(t.start);
+                cudaEventDestroy(t.stop);
+            }
+            graphTimers[b].clear();
         }
     }
 
@@ -307,9 +321,20 @@ public:
         return TF_OK;
     }
 
-    // Brackets one kernel launch with events when per-kernel profiling is on (direct launches only).
+    // Brackets one kernel launch with events when per-kernel profiling is on: from the event pool for direct
+    // launches, into the graph's own timers while a profiled graph is being captured.
     template <class Launch>
     void timed(int kind, bool record, Launch&& launch) {
+        if (captureTimers) {
+            KernelTimer t{ kind, nullptr, nullptr };
+            cudaEventCreate(&t.start);
+            cudaEventCreate(&t.stop);
+            cudaEventRecord(t.start, stream);
+            launch();
+            cudaEventRecord(t.stop, stream);
+            captureTimers->push_back(t);
+            return;
+        }
         if (!record) {
             launch();
             return;
@@ -1952,11 +1977,13 @@ public:
         if (rc != TF_OK) { return rc; }
         rc = configureKernels();
         if (rc != TF_OK) { return rc; }
-        if (graphSteps != nSteps || graphDt != dt) { dropGraphs(); }
+        if (graphSteps != nSteps || graphDt != dt || graphProfiled != profiling) { dropGraphs(); }
         cudaGraphExec_t& graphExec = graphs[cur];
+        const int startBuffer = cur;
         if (!graphExec) {
             cudaGraph_t graph;
             TF_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+            captureTimers = profiling ? &graphTimers[cur] : nullptr;
             int c = cur;
             for (int s = 0; s < nSteps; ++s) {
                 const int into = 1 - c;
@@ -1964,6 +1991,7 @@ public:
                 if (rc != TF_OK) { break; }
                 c = into;
             }
+            captureTimers = nullptr;
             cudaError_t e = cudaStreamEndCapture(stream, &graph);
             if (rc != TF_OK) { return rc; }
             if (e != cudaSuccess) { return fail(TF_E_CUDA, std::string("graph capture: ") + cudaGetErrorString(e)); }
@@ -1972,6 +2000,7 @@ public:
             if (e != cudaSuccess) { return fail(TF_E_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e)); }
             graphSteps = nSteps;
             graphDt = dt;
+            graphProfiled = profiling;
         }
         TF_CUDA(cudaMemsetAsync(dAbort.ptr, 0xff, sizeof(uint32_t), stream));
         TF_CUDA(cudaEventRecord(callStart, stream));
@@ -1980,15 +2009,28 @@ public:
         launches += (int64_t)nSteps * (4 + 2 * std::max(1, (int)settings.substeps));
         TF_CUDA(cudaStreamSynchronize(stream));
         TF_CUDA(cudaEventElapsedTime(&lastElapsedMs, callStart, callStop));
+        if (graphProfiled) {
+            for (const KernelTimer& t : graphTimers[startBuffer]) {
+                float ms = 0.0f;
+                if (cudaEventElapsedTime(&ms, t.start, t.stop) == cudaSuccess) {
+                    kernelMs[t.kind] += ms;
+                    kernelLaunches[t.kind] += 1;
+                }
+            }
+        }
         int completed = 0;
         if ((rc = completedSteps(nSteps, &completed)) != TF_OK) { return rc; }
         const int start = cur;
         cur = (completed % 2) ? 1 - start : start;
         hostFresh = false;
         if (completed < nSteps) {
-            // A list overflowed: grow it and finish the remaining steps with direct launches.
+            // A list overflowed: grow it and finish the remaining steps with direct launches. The call's device
+            // time is the aborted graph launch's plus the retry's.
+            const float graphMs = lastElapsedMs;
             if ((rc = growAfterAbort()) != TF_OK) { return rc; }
-            return step(dt, nSteps - completed);
+            rc = step(dt, nSteps - completed);
+            lastElapsedMs += graphMs;
+            return rc;
         }
         return checkFlags();
     }

@@ -6,13 +6,15 @@
 // moving; their bounds overlap after growing one by the sum of both growths; each shape's bounds overlap
 // the other body's bounds grown by that sum; and the shapes' bounds, each grown by its own body's growth,
 // overlap. The keys (min << 32 | max) come out sorted and unique, as World::Impl::updateContacts leaves them
-// (src/world.cpp:868-869).
+// (src/world.cpp:868-869). The step's other rules (category/mask filters, jointed pairs, half-space pairs)
+// are not applied: the inputs carry no filters, joints or planes.
 //
 // Scratch: g_pairScratch below, a fixed-size array in the library's device image. Its address on a device is
 // looked up once, with that device current, on the first call made there; later calls on that device reuse
-// it. Nothing here allocates device or host memory through CUDA or any other library. Because the scratch
-// is one per device, calls whose work overlaps on the device (different streams, or different host threads)
-// race on it and give wrong results; issue them on one stream or serialise them.
+// it, so the library must not be called on a device again after a cudaDeviceReset there. Nothing here
+// allocates device or host memory through CUDA or any other library. Because the scratch is one per device,
+// calls whose work overlaps on the device (different streams, or different host threads) race on it and give
+// wrong results; issue them on one stream or serialise them.
 #include <cuda_runtime.h>
 
 #include <cstdint>

@@ -193,16 +193,27 @@ def _world_c4(rng, n_bodies):
     return World(bodies, shapes, np.arange(n_bodies + 1), meta={"kind": kind})
 
 
-def config4(n_worlds=4096, seed=0, min_bodies=8, max_bodies=512):
+def _c4_count(rng, min_bodies, max_bodies):
+    n = int(math.floor(math.exp(rng.uniform(math.log(min_bodies), math.log(max_bodies + 1)))))
+    return max(min_bodies, min(max_bodies, n))
+
+
+def config4(n_worlds=4096, seed=0, min_bodies=8, max_bodies=512, only=None):
     """Batched uneven worlds: body counts log-uniform in [8, 512], 70% boxes and 30% spheres in a random
-    stack or scatter above a half-space, per-world friction U[0.2, 1] and restitution U[0, 0.3]."""
+    stack or scatter above a half-space, per-world friction U[0.2, 1] and restitution U[0, 0.3]. Each world
+    comes from its own seed (seed, world), so `only` (world numbers of the n_worlds set, in the order given)
+    builds a shard of the set with the very worlds the whole set has."""
     worlds = []
-    for w in range(n_worlds):
-        rng = np.random.default_rng([seed, w])
-        n = int(math.floor(math.exp(rng.uniform(math.log(min_bodies), math.log(max_bodies + 1)))))
-        n = max(min_bodies, min(max_bodies, n))
-        worlds.append(_world_c4(rng, n))
+    for w in (range(n_worlds) if only is None else only):
+        rng = np.random.default_rng([seed, int(w)])
+        worlds.append(_world_c4(rng, _c4_count(rng, min_bodies, max_bodies)))
     return Scene("batched_uneven_4096", worlds, steps=240)
+
+
+def config4_bodies(n_worlds=4096, seed=0, min_bodies=8, max_bodies=512):
+    """The dynamic body count of each world of config4 (the ground is not counted), without building them."""
+    return np.array([_c4_count(np.random.default_rng([seed, w]), min_bodies, max_bodies) for w in range(n_worlds)],
+                    np.int64)
 
 
 def impact_world(rng):
