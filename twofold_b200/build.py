@@ -12,7 +12,9 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libtwofold_b200.so")
 
-SOURCES = [os.path.join(CSRC, f) for f in ("tf_engine.cu", "tf_noalloc.cu", "tf_adjoint.cu")]
+# The engine (host code, no kernels) and the kernel groups it launches (tf_launch.h), which compile in parallel.
+SOURCES = [os.path.join(CSRC, f) for f in ("tf_engine.cu", "tf_k_broad.cu", "tf_k_collide.cu", "tf_k_refresh.cu",
+                                           "tf_k_solve.cu", "tf_k_finish.cu", "tf_noalloc.cu", "tf_adjoint.cu")]
 HEADERS = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))] + [
     os.path.join(ROOT, "include", "twofold_b200.h")]
 

@@ -20,6 +20,7 @@
 #include "../../include/twofold_b200.h"
 #include "tf_build.h"
 #include "tf_kernels.cuh"
+#include "tf_launch.h"
 #include "tf_tape.h"
 
 namespace tfb {
@@ -167,6 +168,8 @@ public:
     DevArray<uint32_t> dActive, dImpact, dColored, dImpactColored, dRest, dImpactRest, dRestLevel, dImpactRestLevel;
     DevArray<uint8_t> dColor, dCflags;
     DevArray<Axis> dAxes;
+    DevArray<float4> dRows, dInvMats;
+    DevArray<uint32_t> dSlotOf;
     DevArray<uint64_t> dMergeKeyA, dMergeKeyB;
     DevArray<uint32_t> dMergePartA, dMergePartB, dMergeIdxA, dMergeIdxB;
     bool hasJoints = false;  // some world has joints: the substep and finish kernels with joint code run
@@ -255,7 +258,9 @@ public:
         cudaEvent_t start, stop;
     };
     std::vector<KernelTimer> graphTimers[2];
+    size_t graphTimersUsed[2] = { 0, 0 };
     std::vector<KernelTimer>* captureTimers = nullptr;
+    size_t captureUsed = 0;
 
     void dropGraphs() {
         for (int b = 0; b < 2; ++b) {
@@ -266,6 +271,7 @@ public:
                 cudaEventDestroy(t.stop);
             }
             graphTimers[b].clear();
+            graphTimersUsed[b] = 0;
         }
     }
 
@@ -321,18 +327,29 @@ public:
         return TF_OK;
     }
 
+    // Launches kernel `id` on the engine's stream; the arguments must have the kernel's parameter types exactly.
+    template <class... Args>
+    void launch(int id, unsigned grid, unsigned block, size_t smem, Args... args) {
+        void* ptrs[] = { (void*)&args... };
+        cudaLaunchKernel(kernelEntry(id), dim3(grid), dim3(block), ptrs, smem, stream);
+    }
+
     // Brackets one kernel launch with events when per-kernel profiling is on: from the event pool for direct
     // launches, into the graph's own timers while a profiled graph is being captured.
     template <class Launch>
     void timed(int kind, bool record, Launch&& launch) {
         if (captureTimers) {
-            KernelTimer t{ kind, nullptr, nullptr };
-            cudaEventCreate(&t.start);
-            cudaEventCreate(&t.stop);
-            cudaEventRecord(t.start, stream);
+            // Events made before the capture began; recorded as external event nodes, so that every replay of
+            // the graph records them.
+            if (captureUsed < captureTimers->size()) {
+                KernelTimer& t = (*captureTimers)[captureUsed++];
+                t.kind = kind;
+                cudaEventRecordWithFlags(t.start, stream, cudaEventRecordExternal);
+                launch();
+                cudaEventRecordWithFlags(t.stop, stream, cudaEventRecordExternal);
+                return;
+            }
             launch();
-            cudaEventRecord(t.stop, stream);
-            captureTimers->push_back(t);
             return;
         }
         if (!record) {
@@ -1118,6 +1135,9 @@ public:
         TF_ALLOC(dColor, ncon);
         TF_ALLOC(dCflags, ncon);
         TF_ALLOC(dAxes, ncon * kAxesPerContact);
+        TF_ALLOC(dRows, ncon * kRowWords);
+        TF_ALLOC(dSlotOf, ncon);
+        TF_ALLOC(dInvMats, nb * kInvMatWords);
         TF_ALLOC(dMergeKeyA, ncon);
         TF_ALLOC(dMergeKeyB, ncon);
         TF_ALLOC(dMergePartA, ncon);
@@ -1310,6 +1330,10 @@ public:
         B.color = dColor.ptr;
         B.cflags = dCflags.ptr;
         B.axes = dAxes.ptr;
+        B.rows = dRows.ptr;
+        B.rowStride = dContacts[0].n;
+        B.slotOf = dSlotOf.ptr;
+        B.invMats = dInvMats.ptr;
         B.mergeKeyA = dMergeKeyA.ptr;
         B.mergePartA = dMergePartA.ptr;
         B.mergeIdxA = dMergeIdxA.ptr;
@@ -1360,30 +1384,24 @@ public:
         cudaMemsetAsync(dWork.ptr, 0, kSlotCount * sizeof(uint32_t), stream);
         if (marks) { cudaEventRecord(marks[0], stream); }
         timed(0, rec, [&] {
-            k_broadphase<<<grids[0], threads(0), smem(0), stream>>>(B, P, splits[0], serial);
+            launch(kKBroadphase, grids[0], threads(0), smem(0), B, P, splits[0], serial);
             if (!bigWorlds.empty()) {
-                k_broad_pairs<<<smCount * 8, 256, 0, stream>>>(B, serial);
-                k_broad_finish<<<grids[0], threads(0), 0, stream>>>(B, splits[0], serial);
+                launch(kKBroadPairs, smCount * 8, 256, 0, B, serial);
+                launch(kKBroadFinish, grids[0], threads(0), 0, B, splits[0], serial);
             }
         });
         if (marks) { cudaEventRecord(marks[1], stream); }
         timed(7, rec, [&] {
             if (smallBatch) {
-                k_collide_all<<<*std::max_element(flatGrids, flatGrids + kPairClasses), threads(7), 0, stream>>>(B, P,
-                                                                                                           serial);
+                launch(kKCollideAll, *std::max_element(flatGrids, flatGrids + kPairClasses), threads(7), 0, B, P, serial);
                 return;
             }
-            k_collide<kClassSpheres><<<flatGrids[0], threads(7), 0, stream>>>(B, P, serial);
-            k_collide<kClassSpherePoly><<<flatGrids[1], threads(7), 0, stream>>>(B, P, serial);
-            k_collide<kClassPlane><<<flatGrids[2], threads(7), 0, stream>>>(B, P, serial);
-            k_collide<kClassConvex><<<flatGrids[3], threads(7), 0, stream>>>(B, P, serial);
-            k_collide<kClassPlanar><<<flatGrids[4], threads(7), 0, stream>>>(B, P, serial);
-            k_collide<kClassMesh><<<flatGrids[5], threads(7), 0, stream>>>(B, P, serial);
+            for (int c = 0; c < kPairClasses; ++c) { launch(kKCollide + c, flatGrids[c], threads(7), 0, B, P, serial); }
         });
-        timed(1, rec, [&] { k_narrowphase<<<grids[1], threads(1), 0, stream>>>(B, P, splits[1], serial); });
-        timed(2, rec, [&] { k_wake<<<grids[2], threads(2), 0, stream>>>(B, splits[2], serial); });
+        timed(1, rec, [&] { launch(kKNarrowphase, grids[1], threads(1), 0, B, P, splits[1], serial); });
+        timed(2, rec, [&] { launch(kKWake, grids[2], threads(2), 0, B, splits[2], serial); });
         if (marks) { cudaEventRecord(marks[2], stream); }
-        timed(3, rec, [&] { k_prepare<<<grids[3], threads(3), smem(3), stream>>>(B, P, splits[3], serial); });
+        timed(3, rec, [&] { launch(kKPrepare, grids[3], threads(3), smem(3), B, P, splits[3], serial); });
         if (recording && !capturing) {
             const int rc = recordStep(B, serial);
             if (rc != TF_OK) { return rc; }
@@ -1392,32 +1410,21 @@ public:
             if (i > 0) {
                 timed(4, rec, [&] {
                     if (smallBatch) {
-                        k_refresh_all<<<flatGrids[6], threads(4), 0, stream>>>(B, P, i, serial);
+                        launch(kKRefreshAll, flatGrids[6], threads(4), 0, B, P, i, serial);
                         return;
                     }
-                    k_refresh<kClassAny><<<flatGrids[6], threads(4), 0, stream>>>(B, P, i, serial);
-                    k_refresh<kClassSpheres><<<flatGrids[7], threads(4), 0, stream>>>(B, P, i, serial);
-                    k_refresh<kClassSpherePoly><<<flatGrids[8], threads(4), 0, stream>>>(B, P, i, serial);
-                    k_refresh<kClassPlane><<<flatGrids[9], threads(4), 0, stream>>>(B, P, i, serial);
-                    k_refresh<kClassConvex><<<flatGrids[10], threads(4), 0, stream>>>(B, P, i, serial);
-                    k_refresh<kClassPlanar><<<flatGrids[11], threads(4), 0, stream>>>(B, P, i, serial);
-                    k_refresh<kClassMesh><<<flatGrids[12], threads(4), 0, stream>>>(B, P, i, serial);
+                    launch(kKRefresh + kPairClasses, flatGrids[6], threads(4), 0, B, P, i, serial);
+                    for (int c = 0; c < kPairClasses; ++c) {
+                        launch(kKRefresh + c, flatGrids[7 + c], threads(4), 0, B, P, i, serial);
+                    }
                 });
             }
             timed(5, rec, [&] {
-                if (hasJoints) {
-                    k_substep<true><<<grids[5], threads(5), smem(5), stream>>>(B, P, splits[5], i, serial);
-                } else {
-                    k_substep<false><<<grids[5], threads(5), smem(5), stream>>>(B, P, splits[5], i, serial);
-                }
+                launch(hasJoints ? kKSubstepJoints : kKSubstep, grids[5], threads(5), smem(5), B, P, splits[5], i, serial);
             });
         }
         timed(6, rec, [&] {
-            if (hasJoints) {
-                k_finish<true><<<grids[6], threads(6), smem(6), stream>>>(B, P, splits[6], serial);
-            } else {
-                k_finish<false><<<grids[6], threads(6), smem(6), stream>>>(B, P, splits[6], serial);
-            }
+            launch(hasJoints ? kKFinishJoints : kKFinish, grids[6], threads(6), smem(6), B, P, splits[6], serial);
         });
         if (marks) { cudaEventRecord(marks[3], stream); }
         launches += smallBatch ? 5 + 1 + P.substeps + (P.substeps - 1) + (bigWorlds.empty() ? 0 : 2)
@@ -1442,12 +1449,9 @@ public:
             return TF_OK;
         };
         int rc;
-        if ((rc = allow((const void*)k_broadphase)) != TF_OK) { return rc; }
-        if ((rc = allow((const void*)k_substep<false>)) != TF_OK) { return rc; }
-        if ((rc = allow((const void*)k_substep<true>)) != TF_OK) { return rc; }
-        if ((rc = allow((const void*)k_prepare)) != TF_OK) { return rc; }
-        if ((rc = allow((const void*)k_finish<false>)) != TF_OK) { return rc; }
-        if ((rc = allow((const void*)k_finish<true>)) != TF_OK) { return rc; }
+        for (int id : { kKBroadphase, kKSubstep, kKSubstepJoints, kKPrepare, kKFinish, kKFinishJoints }) {
+            if ((rc = allow(kernelEntry(id))) != TF_OK) { return rc; }
+        }
         done = true;
         return TF_OK;
     }
@@ -1497,11 +1501,11 @@ public:
     int configureLaunches() {
         int rc = configureKernels();
         if (rc != TF_OK) { return rc; }
-        const void* fns[kKernels] = { (const void*)k_broadphase, (const void*)k_narrowphase, (const void*)k_wake,
-                                      (const void*)k_prepare,    (const void*)k_refresh<kClassAny>,
-                                      hasJoints ? (const void*)k_substep<true> : (const void*)k_substep<false>,
-                                      hasJoints ? (const void*)k_finish<true> : (const void*)k_finish<false>,
-                                      (const void*)k_collide<kClassConvex> };
+        const void* fns[kKernels] = { kernelEntry(kKBroadphase), kernelEntry(kKNarrowphase), kernelEntry(kKWake),
+                                      kernelEntry(kKPrepare),    kernelEntry(kKRefresh + kPairClasses),
+                                      kernelEntry(hasJoints ? kKSubstepJoints : kKSubstep),
+                                      kernelEntry(hasJoints ? kKFinishJoints : kKFinish),
+                                      kernelEntry(kKCollide + kClassConvex) };
         for (int k = 0; k < kKernels; ++k) {
             LaunchShape& sh = shapes[k];
             if (!sh.chosen) { sh = defaultShape(k); }
@@ -1526,13 +1530,13 @@ public:
         }
         // The flat kernels, one grid per instantiation: as many CTAs as fit on the device at once.
         const void* flat[kFlatGrids] = {
-            (const void*)k_collide<kClassSpheres>,  (const void*)k_collide<kClassSpherePoly>,
-            (const void*)k_collide<kClassPlane>,    (const void*)k_collide<kClassConvex>,
-            (const void*)k_collide<kClassPlanar>,   (const void*)k_collide<kClassMesh>,
-            (const void*)k_refresh<kClassAny>,      (const void*)k_refresh<kClassSpheres>,
-            (const void*)k_refresh<kClassSpherePoly>, (const void*)k_refresh<kClassPlane>,
-            (const void*)k_refresh<kClassConvex>,   (const void*)k_refresh<kClassPlanar>,
-            (const void*)k_refresh<kClassMesh> };
+            kernelEntry(kKCollide + kClassSpheres),  kernelEntry(kKCollide + kClassSpherePoly),
+            kernelEntry(kKCollide + kClassPlane),    kernelEntry(kKCollide + kClassConvex),
+            kernelEntry(kKCollide + kClassPlanar),   kernelEntry(kKCollide + kClassMesh),
+            kernelEntry(kKRefresh + kPairClasses),   kernelEntry(kKRefresh + kClassSpheres),
+            kernelEntry(kKRefresh + kClassSpherePoly), kernelEntry(kKRefresh + kClassPlane),
+            kernelEntry(kKRefresh + kClassConvex),   kernelEntry(kKRefresh + kClassPlanar),
+            kernelEntry(kKRefresh + kClassMesh) };
         for (int f = 0; f < kFlatGrids; ++f) {
             int perSm = 0;
             const int threads = (int)shapes[f < kPairClasses ? 7 : 4].threads;
@@ -1609,7 +1613,7 @@ public:
         }
         const TapeStep ts{ T.worlds.ptr, T.contacts.ptr, T.colored.ptr, T.impactColored.ptr, T.rest.ptr, T.impactRest.ptr,
                            T.awake.ptr };
-        k_tape_record<<<grids[3], shapes[3].threads, 0, stream>>>(B, splits[3], ts, serial);
+        launch(kKTapeRecord, grids[3], shapes[3].threads, 0, B, splits[3], ts, serial);
         return TF_OK;
     }
 
@@ -1982,8 +1986,19 @@ public:
         const int startBuffer = cur;
         if (!graphExec) {
             cudaGraph_t graph;
+            if (profiling) {
+                // One event pair per kernel group of every step: 6 groups and 2 per substep cover them all.
+                const size_t pairs = (size_t)nSteps * (6 + 2 * (size_t)std::max(1, (int)settings.substeps));
+                for (size_t k = graphTimers[cur].size(); k < pairs; ++k) {
+                    KernelTimer t{ 0, nullptr, nullptr };
+                    TF_CUDA(cudaEventCreate(&t.start));
+                    TF_CUDA(cudaEventCreate(&t.stop));
+                    graphTimers[cur].push_back(t);
+                }
+            }
             TF_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
             captureTimers = profiling ? &graphTimers[cur] : nullptr;
+            captureUsed = 0;
             int c = cur;
             for (int s = 0; s < nSteps; ++s) {
                 const int into = 1 - c;
@@ -1992,6 +2007,7 @@ public:
                 c = into;
             }
             captureTimers = nullptr;
+            graphTimersUsed[cur] = captureUsed;
             cudaError_t e = cudaStreamEndCapture(stream, &graph);
             if (rc != TF_OK) { return rc; }
             if (e != cudaSuccess) { return fail(TF_E_CUDA, std::string("graph capture: ") + cudaGetErrorString(e)); }
@@ -2010,7 +2026,8 @@ public:
         TF_CUDA(cudaStreamSynchronize(stream));
         TF_CUDA(cudaEventElapsedTime(&lastElapsedMs, callStart, callStop));
         if (graphProfiled) {
-            for (const KernelTimer& t : graphTimers[startBuffer]) {
+            for (size_t k = 0; k < graphTimersUsed[startBuffer]; ++k) {
+                const KernelTimer& t = graphTimers[startBuffer][k];
                 float ms = 0.0f;
                 if (cudaEventElapsedTime(&ms, t.start, t.stop) == cudaSuccess) {
                     kernelMs[t.kind] += ms;
@@ -2082,8 +2099,8 @@ public:
         if ((rc = dHostIn.alloc(6 * n)) != TF_OK) { return rc; }
         if (f) { TF_CUDA(cudaMemcpyAsync(dHostIn.ptr, f, 3 * n * sizeof(float), cudaMemcpyHostToDevice, stream)); }
         if (t) { TF_CUDA(cudaMemcpyAsync(dHostIn.ptr + 3 * n, t, 3 * n * sizeof(float), cudaMemcpyHostToDevice, stream)); }
-        k_add_forces<<<(unsigned)((n + 255) / 256), 256, 0, stream>>>(dBodies.ptr, (uint32_t)n, f ? dHostIn.ptr : nullptr,
-                                                                     t ? dHostIn.ptr + 3 * n : nullptr);
+        launch(kKAddForces, (unsigned)((n + 255) / 256), 256, 0, dBodies.ptr, (uint32_t)n,
+               (const float*)(f ? dHostIn.ptr : nullptr), (const float*)(t ? dHostIn.ptr + 3 * n : nullptr));
         ++launches;
         TF_CUDA(cudaGetLastError());
         hostFresh = false;
@@ -2106,7 +2123,8 @@ public:
         const size_t n = totalBodies;
         int rc = dHostOut.alloc(7 * n);
         if (rc != TF_OK) { return rc; }
-        k_pack_poses<<<(unsigned)((n + 255) / 256), 256, 0, stream>>>(dBodies.ptr, (uint32_t)n, dHostOut.ptr, dHostOut.ptr + 3 * n);
+        launch(kKPackPoses, (unsigned)((n + 255) / 256), 256, 0, (const DBody*)dBodies.ptr, (uint32_t)n, dHostOut.ptr,
+               dHostOut.ptr + 3 * n);
         ++launches;
         TF_CUDA(cudaGetLastError());
         if (p) { TF_CUDA(cudaMemcpyAsync(p, dHostOut.ptr, 3 * n * sizeof(float), cudaMemcpyDeviceToHost, stream)); }

@@ -247,7 +247,7 @@ __device__ __forceinline__ bool joinedBodies(const Batch& B, const WorldInfo& wi
 
 // Pushes onto a wake stack the sleeping dynamic bodies linked to body gb: by a pair whose contacts have points,
 // or by a joint that holds and is not joined to the world (src/world.cpp:655-700). Marks what it pushes.
-__device__ void pushLinked(const Batch& B, const WorldInfo& wi, uint32_t gb, const DContact* cs, uint32_t nc,
+static __device__ void pushLinked(const Batch& B, const WorldInfo& wi, uint32_t gb, const DContact* cs, uint32_t nc,
                            uint32_t* stack, uint32_t& top) {
     for (uint32_t ci = 0; ci < nc; ++ci) {
         const DContact& c = cs[ci];
@@ -278,7 +278,7 @@ __device__ void pushLinked(const Batch& B, const WorldInfo& wi, uint32_t gb, con
 }
 
 // Wakes what a wake stack holds and everything linked to it (src/world.cpp:703-735).
-__device__ void wakeStack(const Batch& B, const WorldInfo& wi, const DContact* cs, uint32_t nc, uint32_t* stack,
+static __device__ void wakeStack(const Batch& B, const WorldInfo& wi, const DContact* cs, uint32_t nc, uint32_t* stack,
                           uint32_t top) {
     while (top > 0) {
         const uint32_t gb = stack[--top];
@@ -294,7 +294,7 @@ __device__ void wakeStack(const Batch& B, const WorldInfo& wi, const DContact* c
 
 // At the start of a step a joint pulls its sleeping dynamic end awake when the other end moves
 // (src/world.cpp:1578-1585); runs on one thread, over the last step's contacts.
-__device__ void wakeJointPulled(const Batch& B, const WorldInfo& wi, const WorldCounts& wc) {
+static __device__ void wakeJointPulled(const Batch& B, const WorldInfo& wi, const WorldCounts& wc) {
     uint32_t* stack = B.unionParent + wi.bodyFirst;
     uint32_t top = 0;
     const DJoint* js = B.joints + wi.jointFirst;
@@ -319,7 +319,7 @@ __device__ void wakeJointPulled(const Batch& B, const WorldInfo& wi, const World
 // ---------------------------------------------------------------------------------------------------------
 // Broadphase (src/world.cpp:752-870).
 // A half-space against one body's shapes (src/world.cpp:844-867).
-__device__ void pairPlane(const Batch& B, const WorldInfo& wi, uint32_t gp, uint32_t gb, uint32_t* count) {
+static __device__ void pairPlane(const Batch& B, const WorldInfo& wi, uint32_t gp, uint32_t gb, uint32_t* count) {
     const DShape& sp = B.shapes[gp];
     const DBody& pb = B.bodies[sp.body];
     const DBody& b = B.bodies[gb];
@@ -354,7 +354,7 @@ __device__ void pairPlane(const Batch& B, const WorldInfo& wi, uint32_t gp, uint
 
 // The shapes of two bodies whose grown bounds overlap, paired by their own grown bounds
 // (src/world.cpp:819-842).
-__device__ void pairShapes(const Batch& B, const WorldInfo& wi, const DBody& ba, const DBody& bb, float gA, float gB,
+static __device__ void pairShapes(const Batch& B, const WorldInfo& wi, const DBody& ba, const DBody& bb, float gA, float gB,
                            const Vec3& loA, const Vec3& hiA, const Vec3& loB, const Vec3& hiB, const Vec3& reach,
                            uint32_t* count) {
     if (joinedBodies(B, wi, (uint32_t)(&ba - B.bodies), (uint32_t)(&bb - B.bodies))) { return; }
@@ -438,7 +438,7 @@ __device__ __forceinline__ uint32_t sweepBucket(const SweepGrid& s, float x) {
 // The first half of a big world's broadphase, after the growth: each live body's interval along x, their
 // range, and the bodies counted into buckets by where their intervals start. Bucket b then holds
 // sweepOrder[start[b - 1] .. start[b]), start[-1] being 0.
-__device__ void prepareSweep(const Batch& B, const Group& g, const WorldInfo& wi, WorldCounts& wc, uint32_t w) {
+static __device__ void prepareSweep(const Batch& B, const Group& g, const WorldInfo& wi, WorldCounts& wc, uint32_t w) {
     const uint32_t n = wi.bodyCount;
     if (g.tid == 0) {
         wc.sweepMinKey = 0xffffffffu;
@@ -497,7 +497,7 @@ __device__ void prepareSweep(const Batch& B, const Group& g, const WorldInfo& wi
 // into B.cand. Returns the unique count.
 constexpr uint32_t kShortRow = 48;  // rows of keys at most this long are sorted by one thread
 
-__device__ uint32_t sortKeys(const Group& g, const Batch& B, const WorldInfo& wi, uint32_t count) {
+static __device__ uint32_t sortKeys(const Group& g, const Batch& B, const WorldInfo& wi, uint32_t count) {
     uint32_t* row = B.rowScratch + wi.shapeFirst;
     uint64_t* tmp = B.mergeKeyA + wi.contactFirst;
     uint64_t* keys = B.cand + wi.candFirst;
@@ -576,9 +576,10 @@ __device__ uint32_t sortKeys(const Group& g, const Batch& B, const WorldInfo& wi
 // Body pairs whose grown bounds overlap, then their shapes (src/world.cpp:788-842), and half-space pairs
 // (:844-867); the keys are sorted and made unique (:868-869). A warp of the group takes one body and its
 // lanes the bodies after it. Bodies are staged in the group's shared slice when at most stageN of them.
-__device__ void finishCandidates(const Batch& B, const Group& g, const WorldInfo& wi, WorldCounts& wc, uint32_t w,
+static __device__ void finishCandidates(const Batch& B, const Group& g, const WorldInfo& wi, WorldCounts& wc, uint32_t w,
                                  uint32_t total, int serial, uint32_t* cls, uint32_t* classBase);
 
+template <int Unused = 0>
 __global__ void __launch_bounds__(kMaxBlock) k_broadphase(const __grid_constant__ Batch B, const __grid_constant__ StepParams P, const __grid_constant__ Split sp, int serial) {
     extern __shared__ __align__(16) unsigned char s_raw[];
     __shared__ uint32_t s_count[kMaxGroups];
@@ -647,7 +648,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_broadphase(const __grid_constant_
 // The end of a world's broadphase: the raw keys sorted and made unique (src/world.cpp:868-869), then the
 // pairs join the flat list of their class: counted per class, a block of each list reserved for the
 // world, then scattered into it. A list that did not fit stops this step, and the host grows it.
-__device__ void finishCandidates(const Batch& B, const Group& g, const WorldInfo& wi, WorldCounts& wc, uint32_t w,
+static __device__ void finishCandidates(const Batch& B, const Group& g, const WorldInfo& wi, WorldCounts& wc, uint32_t w,
                                  uint32_t total, int serial, uint32_t* cls, uint32_t* classBase) {
     {
         if (total > wi.candCap) {
@@ -693,6 +694,7 @@ __device__ void finishCandidates(const Batch& B, const Group& g, const WorldInfo
 // within its own interval (the one starting first takes a pair, so each pair is taken once) and applies the
 // same pair test as the small worlds, in the pair's lower-body-first order. A warp per body, its lanes
 // across the contiguous run of records in the buckets its interval covers, over every big world.
+template <int Unused = 0>
 __global__ void __launch_bounds__(256) k_broad_pairs(const __grid_constant__ Batch B, int serial) {
     if (stepAborted(B, serial)) { return; }
     const uint32_t total = B.bigBodyStart[B.nBigWorlds];
@@ -731,6 +733,7 @@ __global__ void __launch_bounds__(256) k_broad_pairs(const __grid_constant__ Bat
 }
 
 // The rest of a big world's broadphase: half-space pairs, then the keys sorted and sent to their lists.
+template <int Unused = 0>
 __global__ void __launch_bounds__(kMaxBlock) k_broad_finish(const __grid_constant__ Batch B, const __grid_constant__ Split sp, int serial) {
     __shared__ uint32_t s_class[kMaxGroups][kPairClasses], s_classBase[kMaxGroups][kPairClasses];
     if (stepAborted(B, serial)) { return; }
@@ -766,7 +769,7 @@ __device__ __forceinline__ bool stillFits(const DContact& c, const DBody& a, con
 }
 
 // src/world.cpp:1012-1025.
-__device__ void measureAgain(const DBody& a, const DBody& b, DContact& c, const StepParams& P) {
+static __device__ void measureAgain(const DBody& a, const DBody& b, DContact& c, const StepParams& P) {
     c.normal = rotate(a.xf.q, c.localNormal);
     c.tangent1 = perpendicular(c.normal);
     c.tangent2 = cross(c.normal, c.tangent1);
@@ -784,7 +787,7 @@ __device__ void measureAgain(const DBody& a, const DBody& b, DContact& c, const 
 
 // Each new point continues the nearest old point in reach; an old point continued by several new points
 // splits its impulse among them (src/world.cpp:102-124).
-__device__ void carryImpulses(const DContact& old, DContact& c, float matchSq) {
+static __device__ void carryImpulses(const DContact& old, DContact& c, float matchSq) {
     int from[4], claims[4] = { 0, 0, 0, 0 };
     for (int i = 0; i < c.count; ++i) {
         from[i] = -1;
@@ -824,7 +827,7 @@ __device__ __forceinline__ int nearestPoint(const DContact& old, const Vec3& loc
 // A pair whose dynamic bodies are locked to the plane n (src/world.cpp:514-518): both bodies are placed in
 // the plane, whatever the profiles turn out to be, and marked so the round's placements are kept once every
 // pair is done. Returns collidePlanar's answer. Kept out of line: the 3D paths around it need its registers.
-__device__ __noinline__ int collidePlanarPair(const Batch& B, const StepParams& P, const DShape& sa, const DShape& sb,
+static __device__ __noinline__ int collidePlanarPair(const Batch& B, const StepParams& P, const DShape& sa, const DShape& sb,
                                               const Vec3& n, float margin, Manifold& m) {
     DBody& ba = B.bodies[sa.body];
     DBody& bb = B.bodies[sb.body];
@@ -840,7 +843,7 @@ __device__ __noinline__ int collidePlanarPair(const Batch& B, const StepParams& 
 
 // Stores the placements of the round of collisions that just ended for the bodies of one world that were
 // placed in it; nothing reads a body's pose while its world is here.
-__device__ void keepPlacements(const Batch& B, const Group& g, const WorldInfo& wi) {
+static __device__ void keepPlacements(const Batch& B, const Group& g, const WorldInfo& wi) {
     if (wi.planeBody == UINT32_MAX) { return; }
     if (!TF_OK_INDEX(B, wi.planeBody < B.totalBodies, 31, wi.bodyFirst, wi.planeBody)) { return; }
     const Vec3 n = planeNormal(B.bodies[wi.planeBody]);
@@ -1006,7 +1009,7 @@ __device__ void narrowOne(const Batch& B, const StepParams& P, const WorldInfo& 
 }
 
 // A pair with a mesh over dt (src/world.cpp:505-533): manifolds with normals from sa to sb, into out.
-__device__ int collideMeshPair(const Batch& B, const StepParams& P, const DShape& sa, const DShape& sb, float dt,
+static __device__ int collideMeshPair(const Batch& B, const StepParams& P, const DShape& sa, const DShape& sb, float dt,
                                Manifold* out, int& outCount, MeshBounds* bounds) {
     const DBody& ba = B.bodies[sa.body];
     const DBody& bb = B.bodies[sb.body];
@@ -1023,7 +1026,7 @@ __device__ int collideMeshPair(const Batch& B, const StepParams& P, const DShape
 
 // A contact of pair (sa, sb) from one manifold (src/world.cpp:912-939): points on both surfaces, anchors,
 // tangents and the reuse record.
-__device__ void contactFromManifold(const StepParams& P, const DBody& ba, const DBody& bb, const Manifold& m, DContact& c) {
+static __device__ void contactFromManifold(const StepParams& P, const DBody& ba, const DBody& bb, const Manifold& m, DContact& c) {
     c.featKind = m.featKind;
     c.featA = m.featA;
     c.featB = m.featB;
@@ -1052,7 +1055,7 @@ __device__ void contactFromManifold(const StepParams& P, const DBody& ba, const 
 
 // Stops this step (the host grows the world's lists and runs it again) when a mesh pair's parts or triangle
 // bounds do not fit the world's room for them.
-__device__ void meshRoomOverflow(const Batch& B, const WorldInfo& wi, WorldCounts& wc, int serial) {
+static __device__ void meshRoomOverflow(const Batch& B, const WorldInfo& wi, WorldCounts& wc, int serial) {
     atomicOr(&wc.flags, kDevPairOverflow);
     atomicMax(&wc.candNeeded, 2 * wi.candCap);
     atomicMin(B.abortStep, (uint32_t)serial);
@@ -1062,7 +1065,7 @@ __device__ void meshRoomOverflow(const Batch& B, const WorldInfo& wi, WorldCount
 // moved, else one contact per manifold the mesh collision makes, each carrying the impulses of the old
 // contact whose normal is closest. The first contact goes to the candidate's staging slot, the others to
 // the world's extra parts. A fast pair records the triangles it ruled out, for the refresh within the step.
-__device__ void narrowMesh(const Batch& B, const StepParams& P, const WorldInfo& wi, WorldCounts& wc, uint32_t i,
+static __device__ void narrowMesh(const Batch& B, const StepParams& P, const WorldInfo& wi, WorldCounts& wc, uint32_t i,
                            const DContact* old, uint32_t oldCount, int serial) {
     B.stageUsed[wi.candFirst + i] = 0;
     const uint64_t key = B.cand[wi.candFirst + i];
@@ -1198,6 +1201,7 @@ __global__ void __launch_bounds__(256) k_collide(const __grid_constant__ Batch B
 
 // Small batches collide every pair class in one launch, each class's list in turn over the whole grid (the
 // classes' pairs are disjoint); large batches launch a kernel per class, which keeps a warp on one code path.
+template <int Unused = 0>
 __global__ void __launch_bounds__(256) k_collide_all(const __grid_constant__ Batch B, const __grid_constant__ StepParams P,
                                                      int serial) {
     if (stepAborted(B, serial)) { return; }
@@ -1213,6 +1217,7 @@ __device__ __forceinline__ bool keyLess(uint64_t ka, uint32_t pa, uint64_t kb, u
     return ka != kb ? ka < kb : pa < pb;
 }
 
+template <int Unused = 0>
 __global__ void __launch_bounds__(kMaxBlock) k_narrowphase(const __grid_constant__ Batch B, const __grid_constant__ StepParams P, const __grid_constant__ Split sp, int serial) {
     if (stepAborted(B, serial)) { return; }
     forWorlds(B, kSlotNarrow, sp, nullptr, [&](const Group& g, uint32_t w, unsigned char*, const StageSizes&) {
@@ -1337,6 +1342,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_narrowphase(const __grid_constant
 // Waking (src/world.cpp:705-735): sleeping bodies a moving body reached wake, and so does everything linked
 // to them by a contact with points. Runs on the group's first thread; it is rare.
 
+template <int Unused = 0>
 __global__ void __launch_bounds__(kMaxBlock) k_wake(const __grid_constant__ Batch B, const __grid_constant__ Split sp, int serial) {
     if (stepAborted(B, serial)) { return; }
     forWorlds(B, kSlotWake, sp, nullptr, [&](const Group& g, uint32_t w, unsigned char*, const StageSizes&) {
@@ -1367,10 +1373,106 @@ __global__ void __launch_bounds__(kMaxBlock) k_wake(const __grid_constant__ Batc
 constexpr uint32_t kNone = 0x7fffffffu;
 constexpr uint32_t kNotColorable = 0x80000000u;
 
+// ---------------------------------------------------------------------------------------------------------
+// The laned contacts' solver record.
+//
+// The reference solves a color's contacts from a packed per-batch record rather than from its Contact
+// (ContactLanes, src/internal.h:579-621, built by prepareBatch, src/lanes.cpp:66-110). Here each laned contact
+// has one at its slot (contactFirst + its position in the world's colored list), component-major: component k
+// of every slot is one float4 array, so the lanes of a color read consecutive 16-byte words. It holds what the
+// substep's passes read of a contact and its points, and the impulses, which stay in it from k_prepare to
+// k_finish (k_finish writes them back into the contact; a mid-step refresh takes them back first). The axes are
+// not stored: a pass rebuilds each direction's arms and velocity changes as makeAxis does, from the anchors and
+// the bodies' world inverse mass and inertia (invMats), and takes the stored effective mass. Those matrices are
+// the ones the record was built with until it is built again (a mid-step refresh updates the inverse masses
+// just before it rebuilds every active contact of the world), so every pass sees the bits the stored axes had.
+enum RowWord : int {
+    kRowHead = 0,    // bodyA, bodyB (world-local), point count, contact index (as integer bits)
+    kRowNormal = 1,  // normal, friction
+    kRowT1 = 2,      // tangent1, unused
+    kRowT2 = 3,      // tangent2, unused
+    kRowPoint = 4,   // point i, from kRowPoint + 4 i: anchorA and adjusted separation; anchorB and normal mass;
+                     // tangent masses, normal impulse and largest normal impulse; tangent impulse
+    kRowWords = kRowPoint + 16
+};
+constexpr int kInvMatWords = 5;  // float4 per body: invMassWorld, then invInertiaWorld, row by row; 2 unused
+constexpr uint32_t kNoSlot = 0xffffffffu;
+
+__device__ __forceinline__ void storeInvMats(const Batch& B, uint32_t gb, const DBody& b) {
+    float4* m = B.invMats + (size_t)gb * kInvMatWords;
+    const Mat3& M = b.invMassWorld;
+    const Mat3& I = b.invInertiaWorld;
+    m[0] = make_float4(M.r[0].x, M.r[0].y, M.r[0].z, M.r[1].x);
+    m[1] = make_float4(M.r[1].y, M.r[1].z, M.r[2].x, M.r[2].y);
+    m[2] = make_float4(M.r[2].z, I.r[0].x, I.r[0].y, I.r[0].z);
+    m[3] = make_float4(I.r[1].x, I.r[1].y, I.r[1].z, I.r[2].x);
+    m[4] = make_float4(I.r[2].y, I.r[2].z, 0.0f, 0.0f);
+}
+
+struct InvMats {
+    Mat3 m, i;
+};
+
+__device__ __forceinline__ InvMats loadInvMats(const Batch& B, uint32_t gb) {
+    const float4* p = B.invMats + (size_t)gb * kInvMatWords;
+    const float4 a = __ldg(p), b = __ldg(p + 1), c = __ldg(p + 2), d = __ldg(p + 3), e = __ldg(p + 4);
+    InvMats x;
+    x.m.r[0] = { a.x, a.y, a.z };
+    x.m.r[1] = { a.w, b.x, b.y };
+    x.m.r[2] = { b.z, b.w, c.x };
+    x.i.r[0] = { c.y, c.z, c.w };
+    x.i.r[1] = { d.x, d.y, d.z };
+    x.i.r[2] = { d.w, e.x, e.y };
+    return x;
+}
+
+__device__ __forceinline__ float4 f4(const Vec3& v, float w) { return make_float4(v.x, v.y, v.z, w); }
+__device__ __forceinline__ Vec3 xyz(const float4& v) { return Vec3{ v.x, v.y, v.z }; }
+
+// Builds the record of laned contact ci (world-local) at global slot `slot`, from the contact as prepared and
+// its bodies' current world inverse mass and inertia (the effective masses are makeAxis's).
+static __device__ void buildRow(const Batch& B, const WorldInfo& wi, uint32_t slot, uint32_t ci) {
+    const DContact& c = B.contacts[wi.contactFirst + ci];
+    const DBody& a = B.bodies[c.bodyA];
+    const DBody& b = B.bodies[c.bodyB];
+    const AxisBody xa = axisBodyOf(a), xb = axisBodyOf(b);
+    float4* R = B.rows + slot;
+    const size_t S = B.rowStride;
+    const int n = c.count;
+    R[kRowHead * S] = make_float4(__uint_as_float(c.bodyA - wi.bodyFirst), __uint_as_float(c.bodyB - wi.bodyFirst),
+                                  __uint_as_float((uint32_t)n), __uint_as_float(ci));
+    R[kRowNormal * S] = f4(c.normal, c.friction);
+    R[kRowT1 * S] = f4(c.tangent1, 0.0f);
+    R[kRowT2 * S] = f4(c.tangent2, 0.0f);
+    for (int i = 0; i < n; ++i) {
+        const DPoint& p = c.points[i];
+        const float mn = makeAxis(xa, xb, p.anchorA, p.anchorB, c.normal).mass;
+        const float m1 = makeAxis(xa, xb, p.anchorA, p.anchorB, c.tangent1).mass;
+        const float m2 = makeAxis(xa, xb, p.anchorA, p.anchorB, c.tangent2).mass;
+        R[(kRowPoint + 4 * i) * S] = f4(p.anchorA, p.adjustedSeparation);
+        R[(kRowPoint + 4 * i + 1) * S] = f4(p.anchorB, mn);
+        R[(kRowPoint + 4 * i + 2) * S] = make_float4(m1, m2, p.normalImpulse, p.maxNormalImpulse);
+        R[(kRowPoint + 4 * i + 3) * S] = f4(p.tangentImpulse, 0.0f);
+    }
+}
+
+// The impulses a laned contact's record holds, back into the contact (global contact index gc, global slot).
+__device__ __forceinline__ void returnImpulses(const Batch& B, uint32_t slot, DContact& c) {
+    const float4* R = B.rows + slot;
+    const size_t S = B.rowStride;
+    for (int i = 0; i < c.count; ++i) {
+        const float4 m = R[(kRowPoint + 4 * i + 2) * S];
+        const float4 t = R[(kRowPoint + 4 * i + 3) * S];
+        c.points[i].normalImpulse = m.z;
+        c.points[i].maxNormalImpulse = m.w;
+        c.points[i].tangentImpulse = xyz(t);
+    }
+}
+
 // Greedy lowest free color of 32 over the moving bodies, in list order (src/lanes.cpp:356-374). endA/endB
 // hold each contact's moving bodies (kNone for one that does not move); endA carries kNotColorable for a
 // planar or rolling contact, which takes no color.
-__device__ void colorSequential(uint32_t n, const uint32_t* endA, const uint32_t* endB, uint32_t* masks,
+static __device__ void colorSequential(uint32_t n, const uint32_t* endA, const uint32_t* endB, uint32_t* masks,
                                 uint8_t* color) {
     for (uint32_t x = 0; x < n; ++x) {
         uint8_t k = kNoColor;
@@ -1391,7 +1493,7 @@ __device__ void colorSequential(uint32_t n, const uint32_t* endA, const uint32_t
 
 // Groups a contact list by color: every color's contacts (any order within a color, which solves the same)
 // into colored, colors in ascending order, the uncolored ones into rest in list order.
-__device__ void bucketByColor(const Group& g, uint32_t n, const uint32_t* list, const uint8_t* colorOf, uint32_t* colored,
+static __device__ void bucketByColor(const Group& g, uint32_t n, const uint32_t* list, const uint8_t* colorOf, uint32_t* colored,
                               uint32_t* rest, uint32_t* startOut, uint32_t& colorsUsed, uint32_t& restCount) {
     __shared__ uint32_t s_size[kMaxGroups][kColors + 1];
     __shared__ uint32_t s_fill[kMaxGroups][kColors + 1];
@@ -1434,7 +1536,7 @@ __device__ void bucketByColor(const Group& g, uint32_t n, const uint32_t* list, 
 // together while every body still meets its contacts in list order, which gives the sweep's own bits. Runs on
 // one thread: reorders list by level (stably, within the level in list order) and writes each level's end.
 // last (one word per body, zero on entry), tmp and out (one word per entry) are scratch. Returns the levels.
-__device__ uint32_t levelList(const Batch& B, const WorldInfo& wi, const DContact* cs, uint32_t* list, uint32_t n,
+static __device__ uint32_t levelList(const Batch& B, const WorldInfo& wi, const DContact* cs, uint32_t* list, uint32_t n,
                               uint32_t* levelEnd, uint32_t* last, uint32_t* tmp, uint32_t* out) {
     uint32_t levels = 0;
     for (uint32_t x = 0; x < n; ++x) {
@@ -1477,6 +1579,7 @@ __device__ void forEachLevel(const Group& g, const uint32_t* list, const uint32_
 
 // Coloring is staged in the group's shared slice (masks by body, endpoints by active contact) when the world
 // fits stageBodies bodies and stageContacts active contacts, else in the world's global scratch.
+template <int Unused = 0>
 __global__ void __launch_bounds__(kMaxBlock) k_prepare(const __grid_constant__ Batch B, const __grid_constant__ StepParams P, const __grid_constant__ Split sp, int serial) {
     extern __shared__ __align__(16) unsigned char s_raw[];
     __shared__ uint32_t s_fast[kMaxGroups], s_fastSolid[kMaxGroups], s_points[kMaxGroups];
@@ -1506,6 +1609,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_prepare(const __grid_constant__ B
             b.dp = zero3();
             b.dq = qid();
             updateInverseMass(b);
+            storeInvMats(B, gb, b);
         }
         g.sync();
         // Joints: what the step will report for them starts over (src/world.cpp:1647).
@@ -1585,7 +1689,6 @@ __global__ void __launch_bounds__(kMaxBlock) k_prepare(const __grid_constant__ B
             const DBody& a = B.bodies[c.bodyA];
             const DBody& b = B.bodies[c.bodyB];
             prepareContact(a, b, c);
-            makeContactAxes(axisBodyOf(a), axisBodyOf(b), c, B.axes + (size_t)(cf + act[x]) * kAxesPerContact);
             c.flags &= ~kCLaned;
             points += (uint32_t)c.count;
             const bool can = !(c.flags & kCPlanar) && !(c.rollingResistance > 0.0f);
@@ -1620,6 +1723,22 @@ __global__ void __launch_bounds__(kMaxBlock) k_prepare(const __grid_constant__ B
         bucketByColor(g, nActive, act, colorOf, B.colored + cf, B.rest + cf, wc.colorStart, wc.colorCount, wc.restCount);
         bucketByColor(g, nImpact, B.impact + cf, colorOf, B.impactColored + cf, B.impactRest + cf, wc.impactColorStart,
                       wc.impactColorCount, wc.impactRestCount);
+        // The laned contacts' records, in color order; the axes of the contacts solved one at a time.
+        const uint32_t nColored = wc.colorStart[kColors];
+        for (uint32_t x = g.tid; x < nColored; x += g.size) {
+            const uint32_t ci = B.colored[cf + x];
+            if (!TF_OK_INDEX(B, ci < nc, 7, w, x)) { continue; }
+            B.slotOf[cf + ci] = cf + x;
+            buildRow(B, wi, cf + x, ci);
+        }
+        for (uint32_t x = g.tid; x < wc.restCount; x += g.size) {
+            const uint32_t ci = B.rest[cf + x];
+            if (!TF_OK_INDEX(B, ci < nc, 7, w, x)) { continue; }
+            B.slotOf[cf + ci] = kNoSlot;
+            const DContact& c = cs[ci];
+            makeContactAxes(axisBodyOf(B.bodies[c.bodyA]), axisBodyOf(B.bodies[c.bodyB]), c,
+                            B.axes + (size_t)(cf + ci) * kAxesPerContact);
+        }
         // The one-at-a-time lists by level; the coloring's scratch is free by now.
         for (int which = 0; which < 2; ++which) {
             const uint32_t n = which == 0 ? wc.restCount : wc.impactRestCount;
@@ -1658,6 +1777,16 @@ __device__ void forEachColor(const Group& g, const uint32_t* list, const uint32_
         g.sync();
     }
 }
+
+// Calls f(slot) for the record slot (first + position) of every laned contact, a color at a time.
+template <class F>
+__device__ void forEachColorSlot(const Group& g, uint32_t first, const uint32_t* start, uint32_t colors, F f) {
+    for (uint32_t k = 0; k < colors; ++k) {
+        const uint32_t end = start[k + 1];
+        for (uint32_t x = start[k] + g.tid; x < end; x += g.size) { f(first + x); }
+        g.sync();
+    }
+}
 // In checked builds, whether contact ci of a world can be read: in the list, with bodies in the world.
 __device__ __forceinline__ bool contactOk(const Batch& B, const WorldInfo& wi, const WorldCounts& wc,
                                           uint32_t ci, int code) {
@@ -1675,7 +1804,7 @@ __device__ __forceinline__ bool contactOk(const Batch& B, const WorldInfo& wi, c
 
 // A contact takes a manifold of its pair collided again mid-step: new points on body A, the approach speed
 // and largest impulse of the nearest old point, and the old impulses carried (src/world.cpp:1106-1137).
-__device__ void takeRefreshed(const Batch& B, const StepParams& P, const DBody& a, const DBody& b, DContact& c,
+static __device__ void takeRefreshed(const Batch& B, const StepParams& P, const DBody& a, const DBody& b, DContact& c,
                               const Manifold& m) {
     const DContact old = c;
     c.flags &= ~kCReusable;
@@ -1736,7 +1865,7 @@ __device__ __forceinline__ float movedThisStep(const DBody& b) {
 // collided once, skipping the triangles its collision at the step's start ruled out while they stay out of
 // reach, and each contact in turn takes the new manifold whose normal is closest to its own; a contact left
 // without one keeps no points (src/world.cpp:1078-1137).
-__device__ void refreshMeshRun(const Batch& B, const StepParams& P, const WorldInfo& wi, WorldCounts& wc, DContact* run,
+static __device__ void refreshMeshRun(const Batch& B, const StepParams& P, const WorldInfo& wi, WorldCounts& wc, DContact* run,
                                int count, float remaining) {
     const DBody& a = B.bodies[run[0].bodyA];
     const DBody& b = B.bodies[run[0].bodyB];
@@ -1957,6 +2086,168 @@ struct SolverStore {
     }
 };
 
+// One direction's axis at a point of a laned contact, as makeAxis builds it (the arms, the velocity changes per
+// unit impulse), from the record's anchors and stored effective mass; linA and linB are the bodies' world
+// inverse mass times the direction, the same for every point of the contact.
+__device__ __forceinline__ Axis rowAxis(const Vec3& linA, const Mat3& ia, const Vec3& linB, const Mat3& ib,
+                                        const Vec3& ra, const Vec3& rb, const Vec3& d, float mass) {
+    Axis x;
+    x.armA = cross(ra, d);
+    x.armB = cross(rb, d);
+    x.linearA = linA;
+    x.angularA = ia * x.armA;
+    x.linearB = linB;
+    x.angularB = ib * x.armB;
+    x.mass = mass;
+    return x;
+}
+
+// A laned contact's frame and its bodies' world inverse mass times each direction of it.
+struct RowFrame {
+    Vec3 normal, t1, t2;
+    float friction;
+    Vec3 nA, nB, t1A, t1B, t2A, t2B;
+};
+
+__device__ __forceinline__ RowFrame rowFrame(const float4* R, size_t S, const InvMats& ma, const InvMats& mb) {
+    RowFrame f;
+    const float4 n = R[kRowNormal * S];
+    f.normal = xyz(n);
+    f.friction = n.w;
+    f.t1 = xyz(R[kRowT1 * S]);
+    f.t2 = xyz(R[kRowT2 * S]);
+    f.nA = ma.m * f.normal;
+    f.nB = mb.m * f.normal;
+    f.t1A = ma.m * f.t1;
+    f.t1B = mb.m * f.t1;
+    f.t2A = ma.m * f.t2;
+    f.t2B = mb.m * f.t2;
+    return f;
+}
+
+// warmStartLaned from the record: each point's normal and tangent impulses pushed in point order
+// (src/lanes.cpp:195-217).
+__device__ __forceinline__ void warmStartRow(const float4* R, size_t S, LanedBody& a, LanedBody& b, const InvMats& ma,
+                                             const InvMats& mb, int n) {
+    const bool moveA = !anchored(a), moveB = !anchored(b);
+    const RowFrame f = rowFrame(R, S, ma, mb);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        if (i < n) {
+            const float4 pa = R[(kRowPoint + 4 * i) * S], pb = R[(kRowPoint + 4 * i + 1) * S];
+            const float4 pm = R[(kRowPoint + 4 * i + 2) * S], pt = R[(kRowPoint + 4 * i + 3) * S];
+            const Vec3 ra = xyz(pa), rb = xyz(pb), ti = xyz(pt);
+            pushMoving(a, b, rowAxis(f.nA, ma.i, f.nB, mb.i, ra, rb, f.normal, pb.w), pm.z, moveA, moveB);
+            pushMoving(a, b, rowAxis(f.t1A, ma.i, f.t1B, mb.i, ra, rb, f.t1, pm.x), dot(ti, f.t1), moveA, moveB);
+            pushMoving(a, b, rowAxis(f.t2A, ma.i, f.t2B, mb.i, ra, rb, f.t2, pm.y), dot(ti, f.t2), moveA, moveB);
+        }
+    }
+}
+
+// solveLaned from the record: the soft normal rows, then friction forward in the biased pass and in reverse in
+// relax, with the operations and order of solveContact (src/solver.cpp:360-421, src/lanes.cpp:220-315). The
+// impulses go back to the record.
+__device__ __forceinline__ void solveRow(float4* R, size_t S, LanedBody& a, LanedBody& b, const InvMats& ma,
+                                         const InvMats& mb, int n, const StepParams& P, bool useBias) {
+    const bool moveA = !anchored(a), moveB = !anchored(b);
+    const Softness soft = (!moveA || !moveB) ? P.staticSoft : P.contactSoft;
+    const RowFrame f = rowFrame(R, S, ma, mb);
+    float ni[4] = { 0, 0, 0, 0 }, mi[4] = { 0, 0, 0, 0 }, m1[4] = { 0, 0, 0, 0 }, m2[4] = { 0, 0, 0, 0 };
+    Vec3 ti[4] = {};
+    const Vec3 dp = b.dp - a.dp;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        if (i < n) {
+            const float4 pa = R[(kRowPoint + 4 * i) * S], pb = R[(kRowPoint + 4 * i + 1) * S];
+            const float4 pm = R[(kRowPoint + 4 * i + 2) * S];
+            ti[i] = xyz(R[(kRowPoint + 4 * i + 3) * S]);
+            m1[i] = pm.x;
+            m2[i] = pm.y;
+            ni[i] = pm.z;
+            mi[i] = pm.w;
+            const Vec3 ra = xyz(pa), rb = xyz(pb);
+            const Vec3 d = dp + turned(b, rb) - turned(a, ra);
+            const float sep = dot(d, f.normal) + pa.w;
+            float bias = 0.0f, massScale = 1.0f, impulseScale = 0.0f;
+            if (sep > 0.0f) {
+                bias = sep * P.invH;
+            } else if (useBias) {
+                bias = maxf(soft.biasRate * sep, -P.maxPushout);
+                massScale = soft.massScale;
+                impulseScale = soft.impulseScale;
+            }
+            const Axis x = rowAxis(f.nA, ma.i, f.nB, mb.i, ra, rb, f.normal, pb.w);
+            const float vn = speedAlong(a, b, f.normal, x);
+            float impulse = -x.mass * massScale * (vn + bias) - impulseScale * ni[i];
+            const float total = maxf(ni[i] + impulse, 0.0f);
+            impulse = total - ni[i];
+            ni[i] = total;
+            mi[i] = maxf(mi[i], impulse);
+            pushMoving(a, b, x, impulse, moveA, moveB);
+        }
+    }
+    auto row = [&](int i) {
+        const Vec3 ra = xyz(R[(kRowPoint + 4 * i) * S]), rb = xyz(R[(kRowPoint + 4 * i + 1) * S]);
+        const Axis x1 = rowAxis(f.t1A, ma.i, f.t1B, mb.i, ra, rb, f.t1, m1[i]);
+        const Axis x2 = rowAxis(f.t2A, ma.i, f.t2B, mb.i, ra, rb, f.t2, m2[i]);
+        const float old1 = dot(ti[i], f.t1), old2 = dot(ti[i], f.t2);
+        float f1 = old1 - x1.mass * speedAlong(a, b, f.t1, x1);
+        float f2 = old2 - x2.mass * speedAlong(a, b, f.t2, x2);
+        const float limit = f.friction * ni[i];
+        const float mag = sqrtf(f1 * f1 + f2 * f2);
+        if (mag > limit) {
+            const float scale = mag > 0.0f ? limit / mag : 0.0f;
+            f1 *= scale;
+            f2 *= scale;
+        }
+        ti[i] = f.t1 * f1 + f.t2 * f2;
+        pushMoving(a, b, x1, f1 - old1, moveA, moveB);
+        pushMoving(a, b, x2, f2 - old2, moveA, moveB);
+    };
+    if (useBias) {
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            if (i < n) { row(i); }
+        }
+    } else {
+#pragma unroll
+        for (int i = 3; i >= 0; --i) {
+            if (i < n) { row(i); }
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        if (i < n) {
+            R[(kRowPoint + 4 * i + 2) * S] = make_float4(m1[i], m2[i], ni[i], mi[i]);
+            R[(kRowPoint + 4 * i + 3) * S] = f4(ti[i], 0.0f);
+        }
+    }
+}
+
+// In checked builds, whether a record's bodies lie in the world and its point count is at most 4.
+__device__ __forceinline__ bool rowOk(const Batch& B, const WorldInfo& wi, uint32_t ia, uint32_t ib, int n, int code) {
+#if defined(TF_DEVICE_CHECKS)
+    return TF_OK_INDEX(B, ia < wi.bodyCount && ib < wi.bodyCount && n >= 0 && n <= 4, code, wi.bodyFirst, ia);
+#else
+    return true;
+#endif
+}
+
+// A refresh works on the contact itself: a laned contact first takes its impulses back from its record, and
+// afterwards gets its record built again; a contact solved on its own gets its axes built again.
+__device__ __forceinline__ void takeImpulsesBack(const Batch& B, const WorldInfo& wi, uint32_t ci, DContact& c) {
+    if (c.flags & kCLaned) { returnImpulses(B, B.slotOf[wi.contactFirst + ci], c); }
+}
+
+__device__ __forceinline__ void rebuildSolverData(const Batch& B, const WorldInfo& wi, uint32_t ci, const DContact& c) {
+    if (c.flags & kCLaned) {
+        buildRow(B, wi, B.slotOf[wi.contactFirst + ci], ci);
+        return;
+    }
+    makeContactAxes(axisBodyOf(B.bodies[c.bodyA]), axisBodyOf(B.bodies[c.bodyB]), c,
+                    B.axes + (size_t)(wi.contactFirst + ci) * kAxesPerContact);
+}
+
 // Whether the substep `sub` starts with a refresh of world wc: fast pairs are collided again at the middle
 // substep, pairs of solid bodies also at every other substep but the first (src/world.cpp:1658-1668).
 __device__ __forceinline__ bool refreshedAt(const WorldCounts& wc, int sub, int n) {
@@ -1994,23 +2285,21 @@ __device__ __forceinline__ void refreshClass(const Batch& B, const StepParams& P
             while (end < wc.contactCount && cs[end].key == c.key) { ++end; }
             DContact* run = B.contacts + wi.contactFirst + ci;
             const int count = (int)(end - ci);
+            for (int x = 0; x < count; ++x) { takeImpulsesBack(B, wi, ci + x, run[x]); }
             if (again) {
                 refreshMeshRun(B, P, wi, B.counts[it.x], run, count, remaining);
             } else {
                 for (int x = 0; x < count; ++x) { rebaseContact(B.bodies[run[x].bodyA], B.bodies[run[x].bodyB], run[x]); }
             }
-            for (int x = 0; x < count; ++x) {
-                makeContactAxes(axisBodyOf(B.bodies[run[x].bodyA]), axisBodyOf(B.bodies[run[x].bodyB]), run[x],
-                                B.axes + (size_t)(wi.contactFirst + ci + x) * kAxesPerContact);
-            }
+            for (int x = 0; x < count; ++x) { rebuildSolverData(B, wi, ci + x, run[x]); }
             continue;
         }
+        takeImpulsesBack(B, wi, ci, c);
         if constexpr (Cls != kClassAny) {
             if (again) { refreshContact<Cls>(B, P, c, remaining); }
         }
         if (!again) { rebaseContact(B.bodies[c.bodyA], B.bodies[c.bodyB], c); }
-        makeContactAxes(axisBodyOf(B.bodies[c.bodyA]), axisBodyOf(B.bodies[c.bodyB]), c,
-                        B.axes + (size_t)(wi.contactFirst + ci) * kAxesPerContact);
+        rebuildSolverData(B, wi, ci, c);
     }
 }
 
@@ -2023,6 +2312,7 @@ __global__ void __launch_bounds__(256) k_refresh(const __grid_constant__ Batch B
 
 // Small batches refresh every list in one launch (the lists hold disjoint contacts: a pair's contacts are fast
 // or not together); large batches launch a kernel per list.
+template <int Unused = 0>
 __global__ void __launch_bounds__(256) k_refresh_all(const __grid_constant__ Batch B, const __grid_constant__ StepParams P,
                                                      int sub, int serial) {
     if (stepAborted(B, serial)) { return; }
@@ -2039,7 +2329,7 @@ __global__ void __launch_bounds__(256) k_refresh_all(const __grid_constant__ Bat
 // src/joint.cpp:568-590): kind 0 scales warm starts by the speed the ends kept under the speed limits
 // (src/joint.cpp:570-593) and warm starts, 1 is the biased solve, 2 the relaxing solve with its reaction. The
 // ends' velocities come from the substep's store.
-__device__ void runJoints(const Batch& B, const StepParams& P, const WorldInfo& wi, const SolverStore& st,
+static __device__ void runJoints(const Batch& B, const StepParams& P, const WorldInfo& wi, const SolverStore& st,
                                        int kind) {
     const uint32_t nj = wi.jointCount;
     DJoint* js = B.joints + wi.jointFirst;
@@ -2142,46 +2432,57 @@ __global__ void __launch_bounds__(kMaxBlock) k_substep(const __grid_constant__ B
         const Axis* axes = B.axes + (size_t)cf * kAxesPerContact;
         // A laned contact's bodies are stored only where they move, so a static body shared by a color's
         // contacts is never written concurrently; a contact solved on its own stores both, as the reference does.
-        // Laned contacts (planar and rolling contacts never are) run the register-staged forms; contacts solved
-        // on their own run the general ones.
-        auto warm = [&](uint32_t ci, bool laned) {
+        // Laned contacts (planar and rolling contacts never are) run from their records, by slot; contacts solved
+        // on their own run the general forms from the contact and its stored axes.
+        const size_t S = B.rowStride;
+        auto warmRow = [&](uint32_t slot) {
+            const float4* R = B.rows + slot;
+            const float4 h = R[kRowHead * S];
+            const uint32_t ia = __float_as_uint(h.x), ib = __float_as_uint(h.y);
+            const int n = (int)__float_as_uint(h.z);
+            if (n == 0 || !rowOk(B, wi, ia, ib, n, 10)) { return; }
+            LanedBody a = st.loadLaned(ia), b = st.loadLaned(ib);
+            const InvMats ma = loadInvMats(B, base + ia), mb = loadInvMats(B, base + ib);
+            warmStartRow(R, S, a, b, ma, mb, n);
+            if (!anchored(a)) { st.storeVW(ia, a); }
+            if (!anchored(b)) { st.storeVW(ib, b); }
+        };
+        auto solveRowAt = [&](uint32_t slot, bool bias) {
+            float4* R = B.rows + slot;
+            const float4 h = R[kRowHead * S];
+            const uint32_t ia = __float_as_uint(h.x), ib = __float_as_uint(h.y);
+            const int n = (int)__float_as_uint(h.z);
+            if (n == 0 || !rowOk(B, wi, ia, ib, n, 12)) { return; }
+            LanedBody a = st.loadLaned(ia), b = st.loadLaned(ib);
+            const InvMats ma = loadInvMats(B, base + ia), mb = loadInvMats(B, base + ib);
+            solveRow(R, S, a, b, ma, mb, n, P, bias);
+            if (!anchored(a)) { st.storeVW(ia, a); }
+            if (!anchored(b)) { st.storeVW(ib, b); }
+        };
+        auto warm = [&](uint32_t ci) {
             if (!contactOk(B, wi, wc, ci, 10)) { return; }
             DContact& c = cs[ci];
             const uint32_t ia = c.bodyA - base, ib = c.bodyB - base;
-            if (laned) {
-                LanedBody a = st.loadLaned(ia), b = st.loadLaned(ib);
-                warmStartLaned(a, b, c, axes + (size_t)ci * kAxesPerContact);
-                if (!anchored(a)) { st.storeVW(ia, a); }
-                if (!anchored(b)) { st.storeVW(ib, b); }
-                return;
-            }
             SBody a = st.load(ia), b = st.load(ib);
             warmStartContact(a, b, c, false, axes + (size_t)ci * kAxesPerContact);
             st.storeVW(ia, a);
             st.storeVW(ib, b);
         };
-        auto solve = [&](uint32_t ci, bool bias, bool laned) {
+        auto solve = [&](uint32_t ci, bool bias) {
             if (!contactOk(B, wi, wc, ci, 12)) { return; }
             DContact& c = cs[ci];
             const uint32_t ia = c.bodyA - base, ib = c.bodyB - base;
-            if (laned) {
-                LanedBody a = st.loadLaned(ia), b = st.loadLaned(ib);
-                solveLaned(a, b, c, P, bias, axes + (size_t)ci * kAxesPerContact);
-                if (!anchored(a)) { st.storeVW(ia, a); }
-                if (!anchored(b)) { st.storeVW(ib, b); }
-                return;
-            }
             SBody a = st.load(ia), b = st.load(ib);
             solveContact(a, b, c, P, bias, axes + (size_t)ci * kAxesPerContact);
             st.storeVW(ia, a);
             st.storeVW(ib, b);
         };
-        const uint32_t* colored = B.colored + cf;
         const uint32_t* rest = B.rest + cf;
         const uint32_t* icolored = B.impactColored + cf;
         const uint32_t* irest = B.impactRest + cf;
-        forEachColor(g, colored, wc.colorStart, wc.colorCount, [&](uint32_t ci) { warm(ci, true); });
-        forEachLevel(g, rest, B.restLevel + cf, wc.restLevels, [&](uint32_t ci) { warm(ci, false); });
+        const uint32_t* slotOf = B.slotOf + cf;
+        forEachColorSlot(g, cf, wc.colorStart, wc.colorCount, [&](uint32_t slot) { warmRow(slot); });
+        forEachLevel(g, rest, B.restLevel + cf, wc.restLevels, [&](uint32_t ci) { warm(ci); });
         for (int pass = 0; pass < 2; ++pass) {
             const bool bias = pass == 0;
             if constexpr (Joints) {
@@ -2190,13 +2491,13 @@ __global__ void __launch_bounds__(kMaxBlock) k_substep(const __grid_constant__ B
                     g.sync();
                 }
             }
-            forEachColor(g, colored, wc.colorStart, wc.colorCount, [&](uint32_t ci) { solve(ci, bias, true); });
-            forEachLevel(g, rest, B.restLevel + cf, wc.restLevels, [&](uint32_t ci) { solve(ci, bias, false); });
+            forEachColorSlot(g, cf, wc.colorStart, wc.colorCount, [&](uint32_t slot) { solveRowAt(slot, bias); });
+            forEachLevel(g, rest, B.restLevel + cf, wc.restLevels, [&](uint32_t ci) { solve(ci, bias); });
             if (wc.impactCount > 0) {
                 forEachColor(g, icolored, wc.impactColorStart, wc.impactColorCount,
-                             [&](uint32_t ci) { solve(ci, bias, true); });
+                             [&](uint32_t ci) { solveRowAt(slotOf[ci], bias); });
                 forEachLevel(g, irest, B.impactRestLevel + cf, wc.impactRestLevels,
-                             [&](uint32_t ci) { solve(ci, bias, false); });
+                             [&](uint32_t ci) { solve(ci, bias); });
             }
             if (bias) {
                 for (uint32_t i = g.tid; i < nb; i += g.size) { st.integratePositionAt(i, P); }
@@ -2212,7 +2513,10 @@ __global__ void __launch_bounds__(kMaxBlock) k_substep(const __grid_constant__ B
             // (src/world.cpp:1660-1662).
             for (uint32_t i = g.tid; i < nb; i += g.size) {
                 DBody& d = st.g[i];
-                if (d.alive && d.type == kDynamic && d.awake) { updateInverseMass(d); }
+                if (d.alive && d.type == kDynamic && d.awake) {
+                    updateInverseMass(d);
+                    storeInvMats(B, base + i, d);
+                }
             }
         }
     });
@@ -2236,7 +2540,7 @@ __device__ __forceinline__ uint32_t rootOf(const uint32_t* parent, uint32_t x) {
 
 // bound(): every shape's bounds at the body's pose, and the union of those that are not half-spaces
 // (src/world.cpp:240-253).
-__device__ void boundBody(const Batch& B, DBody& b) {
+static __device__ void boundBody(const Batch& B, DBody& b) {
     bool any = false;
     for (uint32_t x = 0; x < b.shapeCount; ++x) {
         DShape& s = B.shapes[B.shapeList[b.shapeFirst + x]];
@@ -2265,7 +2569,7 @@ __device__ __forceinline__ uint32_t hitRoot(const uint32_t* parent, uint32_t x) 
 // Joins the groups of a and b, the higher root under the lower, so each group's root is its lowest body
 // whatever order the unions run in. A link that loses a race to another is tried again, a bounded number
 // of times.
-__device__ bool uniteHits(uint32_t* parent, uint32_t a, uint32_t b) {
+static __device__ bool uniteHits(uint32_t* parent, uint32_t a, uint32_t b) {
     for (int attempt = 0; attempt < 4096; ++attempt) {
         a = hitRoot(parent, a);
         b = hitRoot(parent, b);
@@ -2359,7 +2663,7 @@ __device__ void sweepCandidates(const Batch& B, const Group& g, const WorldInfo&
     }
 }
 
-__device__ void sweepWorld(const Batch& B, const StepParams& P, const Group& g, const WorldInfo& wi, WorldCounts& wc,
+static __device__ void sweepWorld(const Batch& B, const StepParams& P, const Group& g, const WorldInfo& wi, WorldCounts& wc,
                            uint32_t* pairs, uint32_t* impacts) {
     const uint32_t sf = wi.shapeFirst, ns = wi.shapeCount, bf = wi.bodyFirst, nb = wi.bodyCount;
     uint32_t* parent = B.hitParent + bf;
@@ -2457,7 +2761,7 @@ __device__ void sweepWorld(const Batch& B, const StepParams& P, const Group& g, 
 // and break past their limits (src/world.cpp:1543-1560), the rest settle positions in order, twice over, and
 // every awake dynamic body's world inverse mass is built again at its settled pose. One thread runs the
 // joints; every thread first finds whether any joint was active.
-__device__ void finishJoints(const Batch& B, const StepParams& P, const Group& g, const WorldInfo& wi) {
+static __device__ void finishJoints(const Batch& B, const StepParams& P, const Group& g, const WorldInfo& wi) {
     DJoint* js = B.joints + wi.jointFirst;
     auto endOf = [&](uint32_t gbody) { return gbody == kWorldEnd ? worldEnd() : jointBodyOf(B.bodies[gbody]); };
     bool anyActive = false;
@@ -2511,7 +2815,7 @@ __device__ void finishJoints(const Batch& B, const StepParams& P, const Group& g
 // a pair touches where the solver pushed on a point or a point overlaps (by more than the linear slop once it
 // touched); a hit is a pushed point approaching faster than the threshold in a contact solved this step.
 // Runs after restitution, on the poses the solve left, before kinematic bodies snap to their targets.
-__device__ void reportTouches(const Batch& B, const StepParams& P, const Group& g, const WorldInfo& wi, WorldCounts& wc) {
+static __device__ void reportTouches(const Batch& B, const StepParams& P, const Group& g, const WorldInfo& wi, WorldCounts& wc) {
     const uint32_t nc = wc.contactCount;
     DContact* cs = B.contacts + wi.contactFirst;
     uint32_t touchingHere = 0;
@@ -2588,11 +2892,20 @@ __global__ void __launch_bounds__(kMaxBlock) k_finish(const __grid_constant__ Ba
             s_islands[g.id] = 0;
             s_sweep[g.id] = 0;
         }
-        // Restitution: colored contacts by color, then the rest in active order.
+        // The laned contacts' impulses come back from their records.
+        const uint32_t nColored = wc.colorStart[kColors];
+        for (uint32_t x = g.tid; x < nColored; x += g.size) {
+            const uint32_t ci = __float_as_uint(B.rows[kRowHead * B.rowStride + cf + x].w);
+            if (!contactOk(B, wi, wc, ci, 18)) { continue; }
+            returnImpulses(B, cf + x, cs[ci]);
+        }
+        g.sync();
+        // Restitution: colored contacts by color (their normal axes built again as the record's passes build
+        // them), then the rest in active order.
         forEachColor(g, B.colored + cf, wc.colorStart, wc.colorCount, [&](uint32_t ci) {
             if (!contactOk(B, wi, wc, ci, 18)) { return; }
             DContact& c = cs[ci];
-            restituteContact(B.bodies[c.bodyA], B.bodies[c.bodyB], c, P, true, axes + (size_t)ci * kAxesPerContact);
+            restituteLaned(B.bodies[c.bodyA], B.bodies[c.bodyB], c, P);
         });
         forEachLevel(g, B.rest + cf, B.restLevel + cf, wc.restLevels, [&](uint32_t ci) {
             if (!contactOk(B, wi, wc, ci, 20)) { return; }
@@ -2761,6 +3074,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_finish(const __grid_constant__ Ba
 // World::addForce / addTorque with wake = false on every body (src/world.cpp:2118-2142).
 // Records what this step's solve will see, right after preparation: every contact of every world with its
 // lists and the awake dynamic bodies. One group per world.
+template <int Unused = 0>
 __global__ void __launch_bounds__(kMaxBlock) k_tape_record(const __grid_constant__ Batch B, const __grid_constant__ Split sp,
                                                            TapeStep T, int serial) {
     if (stepAborted(B, serial)) { return; }
@@ -2825,6 +3139,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_tape_record(const __grid_constant
     });
 }
 
+template <int Unused = 0>
 __global__ void k_add_forces(DBody* bodies, uint32_t n, const float* __restrict__ f, const float* __restrict__ t) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) { return; }
@@ -2834,6 +3149,7 @@ __global__ void k_add_forces(DBody* bodies, uint32_t n, const float* __restrict_
     if (t) { b.torque += Vec3{ t[3 * i], t[3 * i + 1], t[3 * i + 2] }; }
 }
 
+template <int Unused = 0>
 __global__ void k_pack_poses(const DBody* bodies, uint32_t n, float* __restrict__ p, float* __restrict__ q) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) { return; }

@@ -605,6 +605,27 @@ TF_HD void restituteContact(BodyT& a, BodyT& b, DContact& c, const StepParams& P
     }
 }
 
+// restituteContact for a laned contact, whose axes are not stored: each point's normal axis is built again from
+// the bodies' world inverse mass and inertia, unchanged since the contact's record was last built, which gives
+// the bits the stored axis had. Laned contacts are never planar.
+template <class BodyT>
+TF_HD void restituteLaned(BodyT& a, BodyT& b, DContact& c, const StepParams& P) {
+    if (c.restitution == 0.0f) { return; }
+    const bool moveA = !anchored(a), moveB = !anchored(b);
+    for (int i = 0; i < c.count; ++i) {
+        DPoint& p = c.points[i];
+        if (p.relativeVelocity > -P.restitutionThreshold || p.maxNormalImpulse == 0.0f) { continue; }
+        const Axis x = makeAxis(a, b, p.anchorA, p.anchorB, c.normal);
+        const float vn = speedAlong(a, b, c.normal, x);
+        float impulse = -x.mass * (vn + c.restitution * p.relativeVelocity);
+        const float total = maxf(p.normalImpulse + impulse, 0.0f);
+        impulse = total - p.normalImpulse;
+        p.normalImpulse = total;
+        p.maxNormalImpulse = maxf(p.maxNormalImpulse, impulse);
+        pushMoving(a, b, x, impulse, moveA, moveB);
+    }
+}
+
 // Gravity, forces, damping, locks and the speed limits (src/world.cpp:1141-1151).
 template <class BodyT>
 TF_HD void integrateVelocity(BodyT& b, const StepParams& P) {
