@@ -66,12 +66,10 @@ struct Batch {
     Axis* axes;               // by contact, kAxesPerContact each; built for the contacts solved one at a time
     // The laned contacts' solver records: kRowWords float4 components, component k of slot s at
     // rows[k * rowStride + s], a laned contact's slot being contactFirst + its position in the world's colored
-    // list; slotOf maps a contact (contactFirst + i) to its slot. invMats holds each body's world inverse mass
-    // and inertia (kInvMatWords float4 per body), as of the records' last build.
+    // list; slotOf maps a contact (contactFirst + i) to its slot.
     float4* rows;
     size_t rowStride;
     uint32_t* slotOf;
-    float4* invMats;
     uint8_t* cflags;          // by contact: kFast, kFastSolid
     uint64_t* mergeKeyA;
     uint32_t* mergePartA;

@@ -168,7 +168,7 @@ public:
     DevArray<uint32_t> dActive, dImpact, dColored, dImpactColored, dRest, dImpactRest, dRestLevel, dImpactRestLevel;
     DevArray<uint8_t> dColor, dCflags;
     DevArray<Axis> dAxes;
-    DevArray<float4> dRows, dInvMats;
+    DevArray<float4> dRows;
     DevArray<uint32_t> dSlotOf;
     DevArray<uint64_t> dMergeKeyA, dMergeKeyB;
     DevArray<uint32_t> dMergePartA, dMergePartB, dMergeIdxA, dMergeIdxB;
@@ -1137,7 +1137,6 @@ public:
         TF_ALLOC(dAxes, ncon * kAxesPerContact);
         TF_ALLOC(dRows, ncon * kRowWords);
         TF_ALLOC(dSlotOf, ncon);
-        TF_ALLOC(dInvMats, nb * kInvMatWords);
         TF_ALLOC(dMergeKeyA, ncon);
         TF_ALLOC(dMergeKeyB, ncon);
         TF_ALLOC(dMergePartA, ncon);
@@ -1333,7 +1332,6 @@ public:
         B.rows = dRows.ptr;
         B.rowStride = dContacts[0].n;
         B.slotOf = dSlotOf.ptr;
-        B.invMats = dInvMats.ptr;
         B.mergeKeyA = dMergeKeyA.ptr;
         B.mergePartA = dMergePartA.ptr;
         B.mergeIdxA = dMergeIdxA.ptr;

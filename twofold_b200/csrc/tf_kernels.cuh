@@ -1381,61 +1381,60 @@ constexpr uint32_t kNotColorable = 0x80000000u;
 // has one at its slot (contactFirst + its position in the world's colored list), component-major: component k
 // of every slot is one float4 array, so the lanes of a color read consecutive 16-byte words. It holds what the
 // substep's passes read of a contact and its points, and the impulses, which stay in it from k_prepare to
-// k_finish (k_finish writes them back into the contact; a mid-step refresh takes them back first). The axes are
-// not stored: a pass rebuilds each direction's arms and velocity changes as makeAxis does, from the anchors and
-// the bodies' world inverse mass and inertia (invMats), and takes the stored effective mass. Those matrices are
-// the ones the record was built with until it is built again (a mid-step refresh updates the inverse masses
-// just before it rebuilds every active contact of the world), so every pass sees the bits the stored axes had.
+// k_finish (k_finish writes them back into the contact; a mid-step refresh takes them back first and builds
+// the record again). Of each axis (makeAxis, src/solver.cpp:5-17) it keeps the velocity changes per unit
+// impulse and the effective mass; the linear ones are the same for every point of a contact and are kept once;
+// the lever arms, a cross product each, are formed again by every pass, with makeAxis's own arithmetic, so each
+// pass sees the bits of the axes as built. 144 bytes a point and 144 a contact, against 240 bytes a point of
+// stored axes plus the lines of the 560-byte contact a pass read before.
 enum RowWord : int {
     kRowHead = 0,    // bodyA, bodyB (world-local), point count, contact index (as integer bits)
     kRowNormal = 1,  // normal, friction
     kRowT1 = 2,      // tangent1, unused
     kRowT2 = 3,      // tangent2, unused
-    kRowPoint = 4,   // point i, from kRowPoint + 4 i: anchorA and adjusted separation; anchorB and normal mass;
-                     // tangent masses, normal impulse and largest normal impulse; tangent impulse
-    kRowWords = kRowPoint + 16
+    kRowLinear = 4,  // 5 words: linearA, linearB of the normal, tangent1 and tangent2 axes (18 floats, 2 unused)
+    kRowPoint = 9,   // point i, 9 words from kRowPoint + 9 i: anchorA and adjusted separation; anchorB and normal
+                     // mass; tangent masses, normal impulse, largest normal impulse; tangent impulse; then 5
+                     // words: angularA, angularB of the normal, tangent1 and tangent2 axes (2 floats unused)
+    kRowPointWords = 9,
+    kRowWords = kRowPoint + 4 * kRowPointWords
 };
-constexpr int kInvMatWords = 5;  // float4 per body: invMassWorld, then invInertiaWorld, row by row; 2 unused
 constexpr uint32_t kNoSlot = 0xffffffffu;
-
-__device__ __forceinline__ void storeInvMats(const Batch& B, uint32_t gb, const DBody& b) {
-    float4* m = B.invMats + (size_t)gb * kInvMatWords;
-    const Mat3& M = b.invMassWorld;
-    const Mat3& I = b.invInertiaWorld;
-    m[0] = make_float4(M.r[0].x, M.r[0].y, M.r[0].z, M.r[1].x);
-    m[1] = make_float4(M.r[1].y, M.r[1].z, M.r[2].x, M.r[2].y);
-    m[2] = make_float4(M.r[2].z, I.r[0].x, I.r[0].y, I.r[0].z);
-    m[3] = make_float4(I.r[1].x, I.r[1].y, I.r[1].z, I.r[2].x);
-    m[4] = make_float4(I.r[2].y, I.r[2].z, 0.0f, 0.0f);
-}
-
-struct InvMats {
-    Mat3 m, i;
-};
-
-__device__ __forceinline__ InvMats loadInvMats(const Batch& B, uint32_t gb) {
-    const float4* p = B.invMats + (size_t)gb * kInvMatWords;
-    const float4 a = __ldg(p), b = __ldg(p + 1), c = __ldg(p + 2), d = __ldg(p + 3), e = __ldg(p + 4);
-    InvMats x;
-    x.m.r[0] = { a.x, a.y, a.z };
-    x.m.r[1] = { a.w, b.x, b.y };
-    x.m.r[2] = { b.z, b.w, c.x };
-    x.i.r[0] = { c.y, c.z, c.w };
-    x.i.r[1] = { d.x, d.y, d.z };
-    x.i.r[2] = { d.w, e.x, e.y };
-    return x;
-}
 
 __device__ __forceinline__ float4 f4(const Vec3& v, float w) { return make_float4(v.x, v.y, v.z, w); }
 __device__ __forceinline__ Vec3 xyz(const float4& v) { return Vec3{ v.x, v.y, v.z }; }
 
+// Six vectors (18 floats) into 5 consecutive components at R + first * S, and back.
+__device__ __forceinline__ void putSix(float4* R, size_t S, int first, const Vec3 (&v)[6]) {
+    R[first * S] = make_float4(v[0].x, v[0].y, v[0].z, v[1].x);
+    R[(first + 1) * S] = make_float4(v[1].y, v[1].z, v[2].x, v[2].y);
+    R[(first + 2) * S] = make_float4(v[2].z, v[3].x, v[3].y, v[3].z);
+    R[(first + 3) * S] = make_float4(v[4].x, v[4].y, v[4].z, v[5].x);
+    R[(first + 4) * S] = make_float4(v[5].y, v[5].z, 0.0f, 0.0f);
+}
+
+struct SixVec {
+    Vec3 v[6];
+};
+
+__device__ __forceinline__ SixVec getSix(const float4* R, size_t S, int first) {
+    const float4 a = R[first * S], b = R[(first + 1) * S], c = R[(first + 2) * S], d = R[(first + 3) * S],
+                 e = R[(first + 4) * S];
+    SixVec x;
+    x.v[0] = { a.x, a.y, a.z };
+    x.v[1] = { a.w, b.x, b.y };
+    x.v[2] = { b.z, b.w, c.x };
+    x.v[3] = { c.y, c.z, c.w };
+    x.v[4] = { d.x, d.y, d.z };
+    x.v[5] = { d.w, e.x, e.y };
+    return x;
+}
+
 // Builds the record of laned contact ci (world-local) at global slot `slot`, from the contact as prepared and
-// its bodies' current world inverse mass and inertia (the effective masses are makeAxis's).
+// its bodies' current world inverse mass and inertia (the axes are makeAxis's).
 static __device__ void buildRow(const Batch& B, const WorldInfo& wi, uint32_t slot, uint32_t ci) {
     const DContact& c = B.contacts[wi.contactFirst + ci];
-    const DBody& a = B.bodies[c.bodyA];
-    const DBody& b = B.bodies[c.bodyB];
-    const AxisBody xa = axisBodyOf(a), xb = axisBodyOf(b);
+    const AxisBody xa = axisBodyOf(B.bodies[c.bodyA]), xb = axisBodyOf(B.bodies[c.bodyB]);
     float4* R = B.rows + slot;
     const size_t S = B.rowStride;
     const int n = c.count;
@@ -1444,25 +1443,32 @@ static __device__ void buildRow(const Batch& B, const WorldInfo& wi, uint32_t sl
     R[kRowNormal * S] = f4(c.normal, c.friction);
     R[kRowT1 * S] = f4(c.tangent1, 0.0f);
     R[kRowT2 * S] = f4(c.tangent2, 0.0f);
+    const Vec3 linear[6] = { xa.invMassWorld * c.normal, xb.invMassWorld * c.normal, xa.invMassWorld * c.tangent1,
+                             xb.invMassWorld * c.tangent1, xa.invMassWorld * c.tangent2, xb.invMassWorld * c.tangent2 };
+    putSix(R, S, kRowLinear, linear);
     for (int i = 0; i < n; ++i) {
         const DPoint& p = c.points[i];
-        const float mn = makeAxis(xa, xb, p.anchorA, p.anchorB, c.normal).mass;
-        const float m1 = makeAxis(xa, xb, p.anchorA, p.anchorB, c.tangent1).mass;
-        const float m2 = makeAxis(xa, xb, p.anchorA, p.anchorB, c.tangent2).mass;
-        R[(kRowPoint + 4 * i) * S] = f4(p.anchorA, p.adjustedSeparation);
-        R[(kRowPoint + 4 * i + 1) * S] = f4(p.anchorB, mn);
-        R[(kRowPoint + 4 * i + 2) * S] = make_float4(m1, m2, p.normalImpulse, p.maxNormalImpulse);
-        R[(kRowPoint + 4 * i + 3) * S] = f4(p.tangentImpulse, 0.0f);
+        const Axis xn = makeAxis(xa, xb, p.anchorA, p.anchorB, c.normal);
+        const Axis x1 = makeAxis(xa, xb, p.anchorA, p.anchorB, c.tangent1);
+        const Axis x2 = makeAxis(xa, xb, p.anchorA, p.anchorB, c.tangent2);
+        const int at = kRowPoint + kRowPointWords * i;
+        R[at * S] = f4(p.anchorA, p.adjustedSeparation);
+        R[(at + 1) * S] = f4(p.anchorB, xn.mass);
+        R[(at + 2) * S] = make_float4(x1.mass, x2.mass, p.normalImpulse, p.maxNormalImpulse);
+        R[(at + 3) * S] = f4(p.tangentImpulse, 0.0f);
+        const Vec3 angular[6] = { xn.angularA, xn.angularB, x1.angularA, x1.angularB, x2.angularA, x2.angularB };
+        putSix(R, S, at + 4, angular);
     }
 }
 
-// The impulses a laned contact's record holds, back into the contact (global contact index gc, global slot).
+// The impulses a laned contact's record holds, back into the contact.
 __device__ __forceinline__ void returnImpulses(const Batch& B, uint32_t slot, DContact& c) {
     const float4* R = B.rows + slot;
     const size_t S = B.rowStride;
     for (int i = 0; i < c.count; ++i) {
-        const float4 m = R[(kRowPoint + 4 * i + 2) * S];
-        const float4 t = R[(kRowPoint + 4 * i + 3) * S];
+        const int at = kRowPoint + kRowPointWords * i;
+        const float4 m = R[(at + 2) * S];
+        const float4 t = R[(at + 3) * S];
         c.points[i].normalImpulse = m.z;
         c.points[i].maxNormalImpulse = m.w;
         c.points[i].tangentImpulse = xyz(t);
@@ -1609,7 +1615,6 @@ __global__ void __launch_bounds__(kMaxBlock) k_prepare(const __grid_constant__ B
             b.dp = zero3();
             b.dq = qid();
             updateInverseMass(b);
-            storeInvMats(B, gb, b);
         }
         g.sync();
         // Joints: what the step will report for them starts over (src/world.cpp:1647).
@@ -2086,60 +2091,37 @@ struct SolverStore {
     }
 };
 
-// One direction's axis at a point of a laned contact, as makeAxis builds it (the arms, the velocity changes per
-// unit impulse), from the record's anchors and stored effective mass; linA and linB are the bodies' world
-// inverse mass times the direction, the same for every point of the contact.
-__device__ __forceinline__ Axis rowAxis(const Vec3& linA, const Mat3& ia, const Vec3& linB, const Mat3& ib,
-                                        const Vec3& ra, const Vec3& rb, const Vec3& d, float mass) {
+// One direction's axis at a point of a laned contact from its record: the lever arms formed as makeAxis forms
+// them, the velocity changes and the effective mass as stored.
+__device__ __forceinline__ Axis rowAxis(const Vec3& ra, const Vec3& rb, const Vec3& d, const Vec3& linA, const Vec3& angA,
+                                        const Vec3& linB, const Vec3& angB, float mass) {
     Axis x;
     x.armA = cross(ra, d);
     x.armB = cross(rb, d);
     x.linearA = linA;
-    x.angularA = ia * x.armA;
+    x.angularA = angA;
     x.linearB = linB;
-    x.angularB = ib * x.armB;
+    x.angularB = angB;
     x.mass = mass;
     return x;
 }
 
-// A laned contact's frame and its bodies' world inverse mass times each direction of it.
-struct RowFrame {
-    Vec3 normal, t1, t2;
-    float friction;
-    Vec3 nA, nB, t1A, t1B, t2A, t2B;
-};
-
-__device__ __forceinline__ RowFrame rowFrame(const float4* R, size_t S, const InvMats& ma, const InvMats& mb) {
-    RowFrame f;
-    const float4 n = R[kRowNormal * S];
-    f.normal = xyz(n);
-    f.friction = n.w;
-    f.t1 = xyz(R[kRowT1 * S]);
-    f.t2 = xyz(R[kRowT2 * S]);
-    f.nA = ma.m * f.normal;
-    f.nB = mb.m * f.normal;
-    f.t1A = ma.m * f.t1;
-    f.t1B = mb.m * f.t1;
-    f.t2A = ma.m * f.t2;
-    f.t2B = mb.m * f.t2;
-    return f;
-}
-
 // warmStartLaned from the record: each point's normal and tangent impulses pushed in point order
 // (src/lanes.cpp:195-217).
-__device__ __forceinline__ void warmStartRow(const float4* R, size_t S, LanedBody& a, LanedBody& b, const InvMats& ma,
-                                             const InvMats& mb, int n) {
+__device__ __forceinline__ void warmStartRow(const float4* R, size_t S, LanedBody& a, LanedBody& b, int n) {
     const bool moveA = !anchored(a), moveB = !anchored(b);
-    const RowFrame f = rowFrame(R, S, ma, mb);
+    const Vec3 normal = xyz(R[kRowNormal * S]), t1 = xyz(R[kRowT1 * S]), t2 = xyz(R[kRowT2 * S]);
+    const SixVec lin = getSix(R, S, kRowLinear);
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
         if (i < n) {
-            const float4 pa = R[(kRowPoint + 4 * i) * S], pb = R[(kRowPoint + 4 * i + 1) * S];
-            const float4 pm = R[(kRowPoint + 4 * i + 2) * S], pt = R[(kRowPoint + 4 * i + 3) * S];
+            const int at = kRowPoint + kRowPointWords * i;
+            const float4 pa = R[at * S], pb = R[(at + 1) * S], pm = R[(at + 2) * S], pt = R[(at + 3) * S];
+            const SixVec ang = getSix(R, S, at + 4);
             const Vec3 ra = xyz(pa), rb = xyz(pb), ti = xyz(pt);
-            pushMoving(a, b, rowAxis(f.nA, ma.i, f.nB, mb.i, ra, rb, f.normal, pb.w), pm.z, moveA, moveB);
-            pushMoving(a, b, rowAxis(f.t1A, ma.i, f.t1B, mb.i, ra, rb, f.t1, pm.x), dot(ti, f.t1), moveA, moveB);
-            pushMoving(a, b, rowAxis(f.t2A, ma.i, f.t2B, mb.i, ra, rb, f.t2, pm.y), dot(ti, f.t2), moveA, moveB);
+            pushMoving(a, b, rowAxis(ra, rb, normal, lin.v[0], ang.v[0], lin.v[1], ang.v[1], pb.w), pm.z, moveA, moveB);
+            pushMoving(a, b, rowAxis(ra, rb, t1, lin.v[2], ang.v[2], lin.v[3], ang.v[3], pm.x), dot(ti, t1), moveA, moveB);
+            pushMoving(a, b, rowAxis(ra, rb, t2, lin.v[4], ang.v[4], lin.v[5], ang.v[5], pm.y), dot(ti, t2), moveA, moveB);
         }
     }
 }
@@ -2147,27 +2129,29 @@ __device__ __forceinline__ void warmStartRow(const float4* R, size_t S, LanedBod
 // solveLaned from the record: the soft normal rows, then friction forward in the biased pass and in reverse in
 // relax, with the operations and order of solveContact (src/solver.cpp:360-421, src/lanes.cpp:220-315). The
 // impulses go back to the record.
-__device__ __forceinline__ void solveRow(float4* R, size_t S, LanedBody& a, LanedBody& b, const InvMats& ma,
-                                         const InvMats& mb, int n, const StepParams& P, bool useBias) {
+__device__ __forceinline__ void solveRow(float4* R, size_t S, LanedBody& a, LanedBody& b, int n, const StepParams& P,
+                                         bool useBias) {
     const bool moveA = !anchored(a), moveB = !anchored(b);
     const Softness soft = (!moveA || !moveB) ? P.staticSoft : P.contactSoft;
-    const RowFrame f = rowFrame(R, S, ma, mb);
-    float ni[4] = { 0, 0, 0, 0 }, mi[4] = { 0, 0, 0, 0 }, m1[4] = { 0, 0, 0, 0 }, m2[4] = { 0, 0, 0, 0 };
+    const float4 nf = R[kRowNormal * S];
+    const Vec3 normal = xyz(nf), t1 = xyz(R[kRowT1 * S]), t2 = xyz(R[kRowT2 * S]);
+    const float friction = nf.w;
+    const SixVec lin = getSix(R, S, kRowLinear);
+    float ni[4] = { 0, 0, 0, 0 }, mi[4] = { 0, 0, 0, 0 };
     Vec3 ti[4] = {};
     const Vec3 dp = b.dp - a.dp;
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
         if (i < n) {
-            const float4 pa = R[(kRowPoint + 4 * i) * S], pb = R[(kRowPoint + 4 * i + 1) * S];
-            const float4 pm = R[(kRowPoint + 4 * i + 2) * S];
-            ti[i] = xyz(R[(kRowPoint + 4 * i + 3) * S]);
-            m1[i] = pm.x;
-            m2[i] = pm.y;
+            const int at = kRowPoint + kRowPointWords * i;
+            const float4 pa = R[at * S], pb = R[(at + 1) * S], pm = R[(at + 2) * S];
+            ti[i] = xyz(R[(at + 3) * S]);
             ni[i] = pm.z;
             mi[i] = pm.w;
+            const float4 g0 = R[(at + 4) * S], g1 = R[(at + 5) * S];
             const Vec3 ra = xyz(pa), rb = xyz(pb);
             const Vec3 d = dp + turned(b, rb) - turned(a, ra);
-            const float sep = dot(d, f.normal) + pa.w;
+            const float sep = dot(d, normal) + pa.w;
             float bias = 0.0f, massScale = 1.0f, impulseScale = 0.0f;
             if (sep > 0.0f) {
                 bias = sep * P.invH;
@@ -2176,8 +2160,9 @@ __device__ __forceinline__ void solveRow(float4* R, size_t S, LanedBody& a, Lane
                 massScale = soft.massScale;
                 impulseScale = soft.impulseScale;
             }
-            const Axis x = rowAxis(f.nA, ma.i, f.nB, mb.i, ra, rb, f.normal, pb.w);
-            const float vn = speedAlong(a, b, f.normal, x);
+            const Axis x = rowAxis(ra, rb, normal, lin.v[0], Vec3{ g0.x, g0.y, g0.z }, lin.v[1],
+                                   Vec3{ g0.w, g1.x, g1.y }, pb.w);
+            const float vn = speedAlong(a, b, normal, x);
             float impulse = -x.mass * massScale * (vn + bias) - impulseScale * ni[i];
             const float total = maxf(ni[i] + impulse, 0.0f);
             impulse = total - ni[i];
@@ -2187,20 +2172,23 @@ __device__ __forceinline__ void solveRow(float4* R, size_t S, LanedBody& a, Lane
         }
     }
     auto row = [&](int i) {
-        const Vec3 ra = xyz(R[(kRowPoint + 4 * i) * S]), rb = xyz(R[(kRowPoint + 4 * i + 1) * S]);
-        const Axis x1 = rowAxis(f.t1A, ma.i, f.t1B, mb.i, ra, rb, f.t1, m1[i]);
-        const Axis x2 = rowAxis(f.t2A, ma.i, f.t2B, mb.i, ra, rb, f.t2, m2[i]);
-        const float old1 = dot(ti[i], f.t1), old2 = dot(ti[i], f.t2);
-        float f1 = old1 - x1.mass * speedAlong(a, b, f.t1, x1);
-        float f2 = old2 - x2.mass * speedAlong(a, b, f.t2, x2);
-        const float limit = f.friction * ni[i];
+        const int at = kRowPoint + kRowPointWords * i;
+        const Vec3 ra = xyz(R[at * S]), rb = xyz(R[(at + 1) * S]);
+        const float4 pm = R[(at + 2) * S];
+        const SixVec ang = getSix(R, S, at + 4);
+        const Axis x1 = rowAxis(ra, rb, t1, lin.v[2], ang.v[2], lin.v[3], ang.v[3], pm.x);
+        const Axis x2 = rowAxis(ra, rb, t2, lin.v[4], ang.v[4], lin.v[5], ang.v[5], pm.y);
+        const float old1 = dot(ti[i], t1), old2 = dot(ti[i], t2);
+        float f1 = old1 - x1.mass * speedAlong(a, b, t1, x1);
+        float f2 = old2 - x2.mass * speedAlong(a, b, t2, x2);
+        const float limit = friction * ni[i];
         const float mag = sqrtf(f1 * f1 + f2 * f2);
         if (mag > limit) {
             const float scale = mag > 0.0f ? limit / mag : 0.0f;
             f1 *= scale;
             f2 *= scale;
         }
-        ti[i] = f.t1 * f1 + f.t2 * f2;
+        ti[i] = t1 * f1 + t2 * f2;
         pushMoving(a, b, x1, f1 - old1, moveA, moveB);
         pushMoving(a, b, x2, f2 - old2, moveA, moveB);
     };
@@ -2218,8 +2206,11 @@ __device__ __forceinline__ void solveRow(float4* R, size_t S, LanedBody& a, Lane
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
         if (i < n) {
-            R[(kRowPoint + 4 * i + 2) * S] = make_float4(m1[i], m2[i], ni[i], mi[i]);
-            R[(kRowPoint + 4 * i + 3) * S] = f4(ti[i], 0.0f);
+            const int at = kRowPoint + kRowPointWords * i;
+            float4* m = R + (at + 2) * S;
+            // The tangent masses stay; only the impulses are written.
+            reinterpret_cast<float2*>(m)[1] = make_float2(ni[i], mi[i]);
+            R[(at + 3) * S] = f4(ti[i], 0.0f);
         }
     }
 }
@@ -2442,8 +2433,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_substep(const __grid_constant__ B
             const int n = (int)__float_as_uint(h.z);
             if (n == 0 || !rowOk(B, wi, ia, ib, n, 10)) { return; }
             LanedBody a = st.loadLaned(ia), b = st.loadLaned(ib);
-            const InvMats ma = loadInvMats(B, base + ia), mb = loadInvMats(B, base + ib);
-            warmStartRow(R, S, a, b, ma, mb, n);
+            warmStartRow(R, S, a, b, n);
             if (!anchored(a)) { st.storeVW(ia, a); }
             if (!anchored(b)) { st.storeVW(ib, b); }
         };
@@ -2454,8 +2444,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_substep(const __grid_constant__ B
             const int n = (int)__float_as_uint(h.z);
             if (n == 0 || !rowOk(B, wi, ia, ib, n, 12)) { return; }
             LanedBody a = st.loadLaned(ia), b = st.loadLaned(ib);
-            const InvMats ma = loadInvMats(B, base + ia), mb = loadInvMats(B, base + ib);
-            solveRow(R, S, a, b, ma, mb, n, P, bias);
+            solveRow(R, S, a, b, n, P, bias);
             if (!anchored(a)) { st.storeVW(ia, a); }
             if (!anchored(b)) { st.storeVW(ib, b); }
         };
@@ -2513,10 +2502,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_substep(const __grid_constant__ B
             // (src/world.cpp:1660-1662).
             for (uint32_t i = g.tid; i < nb; i += g.size) {
                 DBody& d = st.g[i];
-                if (d.alive && d.type == kDynamic && d.awake) {
-                    updateInverseMass(d);
-                    storeInvMats(B, base + i, d);
-                }
+                if (d.alive && d.type == kDynamic && d.awake) { updateInverseMass(d); }
             }
         }
     });
