@@ -275,6 +275,15 @@ TF_API int tf_mesh_create(void* world, const float* vertices, int32_t vertex_cou
  * x, y, z and one edge-flag byte per triangle, lo and hi (6 floats) and first, count (2 ints) per node. */
 TF_API int tf_mesh_read(void* world, int32_t mesh, int32_t counts[3], float* vertices, uint32_t* indices,
                         float* normals, uint8_t* edges, float* node_bounds, int32_t* node_ranges);
+
+/* computeHull (include/twofold/hull.h:17, src/hull.cpp:401-411): the convex hull of `count` points (x, y, z
+ * each) with at most max_vertices corners (at least 4), as hull shapes build it. counts[0] receives the
+ * vertex count and counts[1] the words of the face list; vertices (3 floats each) and faces (per face its
+ * vertex count, then its vertex loop, counter-clockwise seen from outside) are written only when both
+ * capacities hold them, so a first call with null outputs can size the buffers. Host only; allocates no
+ * device memory. */
+TF_API int tf_hull_compute(const float* points, int32_t count, int32_t max_vertices, int32_t counts[2], float* vertices,
+                           int32_t vertex_capacity, int32_t* faces, int32_t face_capacity);
 TF_API int tf_body_create(void* world, int32_t w, const tf_body_desc* desc, tf_id* out_body);
 TF_API int tf_shape_add(void* world, int32_t w, tf_id body, const tf_shape_desc* desc, tf_id* out_shape);
 /* Bulk forms: n bodies into worlds world_of[i]; n shapes onto body_of[i] (indices in world_of[i]). */

@@ -16,6 +16,7 @@
 // seen with public members in this translation unit only.
 #define private public
 #include "world.cpp"
+#include "twofold/hull.h"
 #undef private
 
 #include "twofold_b200.h"
@@ -160,6 +161,29 @@ TF_API int ref_mesh_read(int mesh, int32_t counts[3], float* vertices, uint32_t*
         if (node_ranges) {
             node_ranges[2 * n] = d.nodes[n].first;
             node_ranges[2 * n + 1] = d.nodes[n].count;
+        }
+    }
+    return 0;
+}
+
+// computeHull, laid out as tf_hull_compute lays out its own.
+TF_API int ref_hull_compute(const float* points, int32_t count, int32_t max_vertices, int32_t counts[2], float* vertices,
+                            int32_t vertex_capacity, int32_t* faces, int32_t face_capacity) {
+    std::vector<Vec3> cloud((size_t)count);
+    for (int32_t i = 0; i < count; ++i) { cloud[i] = { points[3 * i], points[3 * i + 1], points[3 * i + 2] }; }
+    const HullMesh h = computeHull(cloud, max_vertices);
+    int32_t words = 0;
+    for (const auto& f : h.faces) { words += 1 + (int32_t)f.size(); }
+    counts[0] = (int32_t)h.vertices.size();
+    counts[1] = words;
+    if (vertices && vertex_capacity >= counts[0]) {
+        for (size_t i = 0; i < h.vertices.size(); ++i) { put3(vertices + 3 * i, h.vertices[i]); }
+    }
+    if (faces && face_capacity >= words) {
+        int32_t at = 0;
+        for (const auto& f : h.faces) {
+            faces[at++] = (int32_t)f.size();
+            for (int v : f) { faces[at++] = v; }
         }
     }
     return 0;

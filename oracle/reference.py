@@ -36,6 +36,7 @@ def load(path=REF_LIB):
             "ref_scene_build": ([P, C.c_int, P, C.c_int, P, P], C.c_int),
             "ref_mesh_create": ([P, C.c_int, P, C.c_int], C.c_int),
             "ref_mesh_read": ([C.c_int, P, P, P, P, P, P, P], C.c_int),
+            "ref_hull_compute": ([P, C.c_int32, C.c_int32, P, P, C.c_int32, P, C.c_int32], C.c_int),
             "ref_world_step": ([P, C.c_float, C.c_int], C.c_int),
             "ref_body_count": ([P], C.c_int),
             "ref_world_get_states": ([P, P, P, P, P, P], C.c_int),
@@ -82,6 +83,11 @@ def mesh_read(mesh):
     lib.ref_mesh_read(mesh, counts.ctypes.data, *(out[k].ctypes.data for k in
                       ("vertices", "indices", "normals", "edges", "node_bounds", "node_ranges")))
     return out
+
+
+def hull_compute(points, max_vertices):
+    """The reference's computeHull, in the layout of twofold_b200.abi.hull_compute."""
+    return abi._hull_call(load().ref_hull_compute, points, max_vertices, lambda rc: None)
 
 
 class RefWorld:

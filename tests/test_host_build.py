@@ -83,9 +83,29 @@ def _ragged_mesh():
     return v, idx
 
 
-@pytest.mark.parametrize("kind", ["terrain", "ragged"])
+def _soup_mesh(seed):
+    """Random triangles over a small grid of vertices (so vertices repeat, edges are shared by one, two or more
+    triangles, and some triangles are slivers or repeat a corner), with signed zeros that must merge."""
+    rng = np.random.default_rng(seed)
+    v = rng.integers(-3, 4, size=(60, 3)).astype(np.float32) * np.float32(0.5)
+    v[rng.random(60) < 0.2] *= np.float32(-1.0)
+    v[::7, 0] = np.float32(-0.0)
+    v[1::7, 0] = np.float32(0.0)
+    v[5] = v[2] + np.float32(1e-7)
+    idx = rng.integers(0, 60, size=3 * 400).astype(np.uint32)
+    return v, idx
+
+
+@pytest.mark.parametrize("kind", ["terrain", "ragged", "soup0", "soup1", "soup2", "big_terrain"])
 def test_meshes_are_built_like_the_reference(kind):
-    v, idx = scenes.terrain_mesh(cells=32, cell=0.5, seed=1) if kind == "terrain" else _ragged_mesh()
+    if kind == "terrain":
+        v, idx = scenes.terrain_mesh(cells=32, cell=0.5, seed=1)
+    elif kind == "big_terrain":
+        v, idx = scenes.terrain_mesh(cells=256, cell=0.5, seed=0)
+    elif kind == "ragged":
+        v, idx = _ragged_mesh()
+    else:
+        v, idx = _soup_mesh(int(kind[-1]))
     b = Batch([scenes.single("box_on_ground")])
     mine = b.read_mesh(b.create_mesh(v, idx))
     ref = R.mesh_read(R.mesh_create(v, idx))
@@ -137,3 +157,39 @@ def test_joints_refuse_what_this_build_does_not_run():
         b.joint_create(0, abi.joint_desc(abi.TF_JOINT_POINT, abi.tf_id(10_000, 0)))
     with pytest.raises(RuntimeError):
         b.joint_create(0, abi.joint_desc(9, abi.tf_id(1, 0)))
+
+
+def _clouds():
+    """Point clouds that take every path of the hull builder: random balls and boxes, points on a sphere (many
+    nearly coplanar faces to merge), grids (exactly coplanar faces and ties between equal distances), repeated
+    points, flat, collinear and single-point clouds (thickened), far from the origin, and non-finite points."""
+    rng = np.random.default_rng(5)
+    out = []
+    for n in (4, 5, 8, 16, 40, 120):
+        out.append(rng.normal(size=(n, 3)))
+        out.append(rng.uniform(-1.0, 1.0, size=(n, 3)) * [2.0, 0.3, 1.0])
+        s = rng.normal(size=(n, 3))
+        out.append(s / np.linalg.norm(s, axis=1, keepdims=True))
+    g = np.stack(np.meshgrid(*[np.arange(3.0)] * 3, indexing="ij"), -1).reshape(-1, 3)
+    out.append(g)
+    out.append(np.concatenate([g, g[::-1], g[:5]]))
+    out.append(g * [1.0, 1.0, 0.0])                        # flat
+    out.append(np.outer(np.linspace(0, 1, 9), [1.0, 2.0, 3.0]))  # collinear
+    out.append(np.zeros((6, 3)))                           # one point
+    out.append(rng.normal(size=(30, 3)) + 1e4)             # far from the origin
+    nf = rng.normal(size=(20, 3))
+    nf[3, 1] = np.nan
+    nf[7, 2] = np.inf
+    out.append(nf)
+    return [np.asarray(c, np.float32) for c in out]
+
+
+@pytest.mark.parametrize("max_vertices", [4, 6, 16, 64])
+def test_hull_builder_matches_the_reference(max_vertices):
+    """tf_hull_compute against the reference's computeHull on the same cloud: the same vertices in the same
+    order, bit for bit, and the same face loops."""
+    for k, cloud in enumerate(_clouds()):
+        mv, mf = abi.hull_compute(cloud, max_vertices)
+        rv, rf = R.hull_compute(cloud, max_vertices)
+        assert mv.shape == rv.shape and np.array_equal(mv.view(np.uint32), rv.view(np.uint32)), f"cloud {k}: vertices"
+        assert mf == rf, f"cloud {k}: faces"

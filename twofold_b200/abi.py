@@ -6,6 +6,8 @@ to anything else.
 import ctypes as C
 import os
 
+import numpy as np
+
 HERE = os.path.dirname(os.path.abspath(__file__))
 # TWOFOLD_B200_LIB selects another build of the same library (for instance the index-checking one).
 LIB_PATH = os.environ.get("TWOFOLD_B200_LIB") or os.path.join(HERE, "libtwofold_b200.so")
@@ -308,6 +310,7 @@ def _declare(lib):
         "tf_world_set_settings": ([P, C.POINTER(tf_settings)], C.c_int),
         "tf_mesh_create": ([P, P, C.c_int32, P, C.c_int32, C.POINTER(C.c_int32)], C.c_int),
         "tf_mesh_read": ([P, C.c_int32, P, P, P, P, P, P, P], C.c_int),
+        "tf_hull_compute": ([P, C.c_int32, C.c_int32, P, P, C.c_int32, P, C.c_int32], C.c_int),
         "tf_body_create": ([P, C.c_int32, C.POINTER(tf_body_desc), C.POINTER(tf_id)], C.c_int),
         "tf_shape_add": ([P, C.c_int32, tf_id, C.POINTER(tf_shape_desc), C.POINTER(tf_id)], C.c_int),
         "tf_bodies_create": ([P, C.c_int32, P, C.POINTER(tf_body_desc), P], C.c_int),
@@ -371,7 +374,7 @@ def _declare(lib):
 # Every symbol include/twofold_b200.h declares.
 EXPORTED = [
     "tf_abi_version", "tf_last_error", "tf_default_settings", "tf_world_create", "tf_world_destroy",
-    "tf_world_count", "tf_world_set_settings", "tf_mesh_create", "tf_mesh_read", "tf_body_create", "tf_shape_add",
+    "tf_world_count", "tf_world_set_settings", "tf_mesh_create", "tf_mesh_read", "tf_hull_compute", "tf_body_create", "tf_shape_add",
     "tf_bodies_create",
     "tf_shapes_add", "tf_joint_create", "tf_joint_get_info", "tf_world_broken_joints", "tf_joint_set_limits", "tf_joint_set_motor",
     "tf_joint_set_spring", "tf_joint_set_friction", "tf_joint_set_swing", "tf_joint_set_break_limits", "tf_joint_destroy", "tf_world_step", "tf_world_step_graph", "tf_world_synchronize", "tf_world_device_status",
@@ -399,3 +402,25 @@ def check(rc, lib=None):
         lib = lib or load()
         msg = lib.tf_last_error()
         raise RuntimeError(f"twofold_b200 error {rc}: {msg.decode() if msg else ''}")
+
+
+def hull_compute(points, max_vertices, lib=None):
+    """tf_hull_compute: (vertices (n, 3) float32, faces as lists of vertex indices) of a point cloud (m, 3)."""
+    lib = lib or load()
+    return _hull_call(lib.tf_hull_compute, points, max_vertices, check)
+
+
+def _hull_call(fn, points, max_vertices, checker):
+    pts = np.ascontiguousarray(points, np.float32).reshape(-1, 3)
+    counts = np.zeros(2, np.int32)
+    checker(fn(pts.ctypes.data, len(pts), int(max_vertices), counts.ctypes.data, None, 0, None, 0))
+    verts = np.zeros((max(int(counts[0]), 1), 3), np.float32)
+    words = np.zeros(max(int(counts[1]), 1), np.int32)
+    checker(fn(pts.ctypes.data, len(pts), int(max_vertices), counts.ctypes.data, verts.ctypes.data, int(counts[0]),
+               words.ctypes.data, int(counts[1])))
+    faces, at = [], 0
+    while at < int(counts[1]):
+        k = int(words[at])
+        faces.append(words[at + 1:at + 1 + k].tolist())
+        at += 1 + k
+    return verts[:int(counts[0])], faces

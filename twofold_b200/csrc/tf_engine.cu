@@ -2252,6 +2252,31 @@ TF_API int tf_mesh_read(void* h, int32_t mesh, int32_t counts[3], float* vertice
     return TF_OK;
 }
 
+TF_API int tf_hull_compute(const float* points, int32_t count, int32_t max_vertices, int32_t counts[2], float* vertices,
+                           int32_t vertex_capacity, int32_t* faces, int32_t face_capacity) {
+    if (count < 0 || !counts || (count > 0 && !points)) { return tfb::fail(TF_E_INVALID, "tf_hull_compute: bad arguments"); }
+    std::vector<tfb::Vec3> cloud((size_t)count);
+    for (int32_t i = 0; i < count; ++i) { cloud[i] = { points[3 * i], points[3 * i + 1], points[3 * i + 2] }; }
+    const tfb::HullResult h = tfb::computeHull(cloud, max_vertices);
+    int32_t words = 0;
+    for (const auto& f : h.faces) { words += 1 + (int32_t)f.size(); }
+    counts[0] = (int32_t)h.vertices.size();
+    counts[1] = words;
+    if (vertices && vertex_capacity >= counts[0]) {
+        for (size_t i = 0; i < h.vertices.size(); ++i) {
+            vertices[3 * i] = h.vertices[i].x, vertices[3 * i + 1] = h.vertices[i].y, vertices[3 * i + 2] = h.vertices[i].z;
+        }
+    }
+    if (faces && face_capacity >= words) {
+        int32_t at = 0;
+        for (const auto& f : h.faces) {
+            faces[at++] = (int32_t)f.size();
+            for (int v : f) { faces[at++] = v; }
+        }
+    }
+    return TF_OK;
+}
+
 TF_API int tf_body_create(void* h, int32_t w, const tf_body_desc* d, tf_id* out) {
     if (!h) { return tfb::fail(TF_E_INVALID, "tf_body_create: null world"); }
     return E(h)->createBody(w, d, out);

@@ -1,20 +1,22 @@
-// Convex hulls of point clouds for hull shapes: the reference's computeHull (src/hull.cpp:1-412), restated as
-// host code with the same float operations in the same order, so that the vertex and face order, and with
-// them every feature id the narrowphase reports, come out as the reference's.
+// Convex hulls of point clouds, for hull shapes (twofold::computeHull, include/twofold/hull.h:17).
 //
-// The method: incremental quickhull over triangles with a vertex budget. Start from a tetrahedron of extreme
-// points; repeatedly take the point farthest outside any face (the eye), remove the faces it sees (with
-// tolerance rules against slivers and fold-backs), and fan new faces from the horizon to the eye; points the
-// tolerance dropped get one more try at the end. The triangles are then merged into coplanar convex polygons.
-// Degenerate clouds (a point, a segment, a plane) are thickened into a thin slab first.
+// The hull's vertex order and face loops decide a shape's mass sums and every feature id the narrowphase
+// reports, so they must come out exactly as the reference builds them (src/hull.cpp). What has to agree is
+// the arithmetic of every plane test and the order in which ties are broken; both are kept below, and each
+// one names the rule it keeps. The surface itself is held differently: faces are columns of arrays with an
+// explicit neighbour across each edge, the points waiting above a face are a list threaded through one array,
+// and the live vertex count is kept as faces come and go.
+//
+// The method is quickhull (Barber, Dobkin and Huhdanpaa, 1996) with a vertex budget: a tetrahedron of extreme
+// points, then repeatedly the point farthest above any face is joined to the horizon of the faces it sees.
+// Faces merge afterwards into coplanar convex polygons. Clouds that span no volume are thickened into a slab.
 #pragma once
 
 #include <algorithm>
+#include <array>
 #include <cfloat>
 #include <cmath>
 #include <cstdint>
-#include <map>
-#include <unordered_map>
 #include <utility>
 #include <vector>
 
@@ -29,96 +31,393 @@ struct HullResult {
 
 namespace hull {
 
-constexpr float kCoplanarCos = 0.9998f;  // neighbouring faces closer than this merge into one polygon
+// Neighbouring faces whose normals agree closer than this cosine merge into one polygon.
+constexpr float kMergeCos = 0.9998f;
+constexpr int kNone = -1;
 
-inline uint64_t directedEdge(int a, int b) { return ((uint64_t)(uint32_t)a << 32) | (uint32_t)b; }
+// The triangulated surface as it grows. Face f has corners tri[f], counter-clockwise seen from outside; its
+// edge e runs tri[f][e] -> tri[f][(e + 1) % 3], and across[f][e] is the face on the other side of that edge.
+// The points above face f that it is the best face for wait in a list in the order they came, from first[f]
+// through follow[] to last[f].
+struct Surface {
+    const std::vector<Vec3>& pts;
+    float tol = 0.0f;
+    float foldSine = 0.0f;  // the steepest fold-back that keeps every corner within the tolerance
 
-struct Tri {
-    int v[3];
-    Vec3 normal;
-    float offset = 0.0f;
-    std::vector<int> outside;  // points this face is the best choice for
-    bool alive = true;
-};
+    std::vector<std::array<int, 3>> tri, across;
+    std::vector<Vec3> normal;
+    std::vector<float> offset;
+    std::vector<uint8_t> live;
+    std::vector<int> first, last, follow;
+    std::vector<int> useCount;  // live faces at each point
+    int liveVertices = 0;
+    std::vector<int> nearly;     // points within the tolerance above some face, kept for one more try
+    std::vector<uint8_t> tried;  // points already given that try
 
-// The hull of points already moved near the origin (`p`); `original` are the caller's points, returned in the
-// result.
-class Quickhull {
-public:
-    Quickhull(const std::vector<Vec3>& p, const std::vector<Vec3>& original, float tol, float size)
-        : p_(p), original_(original), tol_(tol), fold_(tol / size), reclaimed_(p.size(), false) {}
+    Surface(const std::vector<Vec3>& p, float tolerance, float size)
+        : pts(p), tol(tolerance), foldSine(tolerance / size), follow(p.size(), kNone), useCount(p.size(), 0),
+          tried(p.size(), 0) {}
 
-    void run(const int simplex[4], int maxVertices) {
-        Vec3 center{ 0, 0, 0 };
-        for (int i = 0; i < 4; ++i) { center += p_[simplex[i]] * 0.25f; }
-        static const int tet[4][3] = { { 0, 1, 2 }, { 0, 1, 3 }, { 0, 2, 3 }, { 1, 2, 3 } };
-        for (const auto& t : tet) {
-            int a = simplex[t[0]], b = simplex[t[1]], c = simplex[t[2]];
-            if (dot(cross(p_[b] - p_[a], p_[c] - p_[a]), p_[a] - center) < 0.0f) { std::swap(b, c); }
-            addTri(a, b, c);
+    int faceCount() const { return (int)tri.size(); }
+
+    // The plane test every decision below rests on (src/hull.cpp: Builder::distance).
+    float height(int f, int p) const { return dot(normal[f], pts[p]) - offset[f]; }
+
+    int addFace(int a, int b, int c) {
+        const int f = faceCount();
+        tri.push_back({ a, b, c });
+        across.push_back({ kNone, kNone, kNone });
+        const Vec3 n = normalize(cross(pts[b] - pts[a], pts[c] - pts[a]));
+        normal.push_back(n);
+        offset.push_back(dot(n, pts[a]));
+        live.push_back(1);
+        first.push_back(kNone);
+        last.push_back(kNone);
+        for (int v : { a, b, c }) {
+            if (useCount[v]++ == 0) { ++liveVertices; }
         }
-        std::vector<int> others;
-        for (int i = 0; i < (int)p_.size(); ++i) {
-            if (i != simplex[0] && i != simplex[1] && i != simplex[2] && i != simplex[3]) { others.push_back(i); }
+        return f;
+    }
+
+    void removeFace(int f) {
+        live[f] = 0;
+        for (int v : tri[f]) {
+            if (--useCount[v] == 0) { --liveVertices; }
         }
-        distribute(others, { 0, 1, 2, 3 });
-        while (usedVertices() < maxVertices) {
-            int face = -1, eye = -1;
-            float far = 0.0f;
-            for (int fi = 0; fi < (int)tris_.size(); ++fi) {
-                if (!tris_[fi].alive) { continue; }
-                for (int pi : tris_[fi].outside) {
-                    const float d = above(tris_[fi], pi);
-                    if (d > far) {
-                        far = d;
-                        face = fi;
-                        eye = pi;
-                    }
+        first[f] = last[f] = kNone;
+    }
+
+    void enqueue(int f, int p) {
+        follow[p] = kNone;
+        if (last[f] == kNone) {
+            first[f] = p;
+        } else {
+            follow[last[f]] = p;
+        }
+        last[f] = p;
+    }
+
+    void dequeue(int f, int p) {
+        int prev = kNone;
+        for (int q = first[f]; q != kNone; prev = q, q = follow[q]) {
+            if (q != p) { continue; }
+            if (prev == kNone) {
+                first[f] = follow[q];
+            } else {
+                follow[prev] = follow[q];
+            }
+            if (last[f] == q) { last[f] = prev; }
+            return;
+        }
+    }
+
+    // The edge of face g that runs b -> a, where a -> b is an edge of its neighbour.
+    int edgeBack(int g, int a, int b) const {
+        for (int e = 0; e < 3; ++e) {
+            if (tri[g][e] == b && tri[g][(e + 1) % 3] == a) { return e; }
+        }
+        return kNone;
+    }
+
+    // Each point joins the face it is farthest above, by more than the tolerance, the first such face in the
+    // order given winning ties; a point above some face by no more than the tolerance is kept for one more
+    // try, once (src/hull.cpp: Builder::assign).
+    void place(const std::vector<int>& points, const std::vector<int>& faces) {
+        for (int p : points) {
+            int best = kNone;
+            float bestHeight = tol, highest = -FLT_MAX;
+            for (int f : faces) {
+                const float h = height(f, p);
+                highest = std::max(highest, h);
+                if (h > bestHeight) {
+                    bestHeight = h;
+                    best = f;
                 }
             }
-            if (face < 0) {
-                if (retryDropped()) { continue; }
-                break;
-            }
-            if (!addEye(face, eye)) {
-                std::vector<int>& out = tris_[face].outside;
-                out.erase(std::find(out.begin(), out.end(), eye));
+            if (best != kNone) {
+                enqueue(best, p);
+            } else if (highest > 0.0f && !tried[p]) {
+                nearly.push_back(p);
             }
         }
     }
 
-    // Coplanar neighbours merged into convex polygons; vertices numbered in order of first use.
-    HullResult result() const {
-        std::vector<int> region(tris_.size(), -1);
-        std::vector<std::vector<int>> polygons;
-        for (int seed = 0; seed < (int)tris_.size(); ++seed) {
-            if (!tris_[seed].alive || region[seed] >= 0) { continue; }
-            const int id = (int)polygons.size();
-            std::vector<int> members{ seed };
-            region[seed] = id;
-            for (size_t k = 0; k < members.size(); ++k) {
-                const Tri& f = tris_[members[k]];
-                for (int i = 0; i < 3; ++i) {
-                    const int twin = edgeOwner_.at(directedEdge(f.v[(i + 1) % 3], f.v[i]));
-                    if (region[twin] >= 0 || !coplanar(tris_[seed], tris_[twin])) { continue; }
-                    region[twin] = id;
-                    members.push_back(twin);
+    // Whether face g, across edge a -> b of the face `from` that the eye sees, has to go too: the eye is
+    // clearly above it, or the new face over a -> b would be a sliver, face inward, or fold back over it by
+    // more than the tolerance allows (src/hull.cpp: Builder::sees).
+    bool goesToo(int from, int g, int a, int b, int eye) const {
+        const float h = height(g, eye);
+        if (h > tol) { return true; }
+        const Vec3 edge = normalize(pts[b] - pts[a]);
+        const Vec3 r = pts[eye] - pts[a];
+        const float reach = length(r - edge * dot(r, edge));
+        if (reach <= tol) { return true; }
+        if (height(from, eye) <= tol && dot(r, cross(normal[from], edge)) <= 0.0f) { return true; }
+        if (h <= 0.0f) { return false; }
+        return dot(r, cross(normal[g], edge)) <= 0.0f || h > foldSine * reach;
+    }
+
+    struct RimEdge {
+        int a, b;    // the edge, as the removed face ran it
+        int outer;   // the face kept on its far side
+    };
+
+    // Whether the rim edges, each start used once, chain into one loop through all of them that begins and
+    // ends at the first edge (src/hull.cpp: Builder::singleLoop).
+    static bool oneLoop(const std::vector<RimEdge>& rim) {
+        const size_t n = rim.size();
+        if (n == 0) { return false; }
+        std::vector<std::pair<int, int>> byStart(n);  // (start vertex, edge)
+        for (size_t i = 0; i < n; ++i) { byStart[i] = { rim[i].a, (int)i }; }
+        std::sort(byStart.begin(), byStart.end());
+        for (size_t i = 1; i < n; ++i) {
+            if (byStart[i].first == byStart[i - 1].first) { return false; }
+        }
+        size_t at = 0;
+        for (size_t step = 1; step < n; ++step) {
+            const int v = rim[at].b;
+            const auto it = std::lower_bound(byStart.begin(), byStart.end(), std::make_pair(v, -1));
+            if (it == byStart.end() || it->first != v || it->second == 0) { return false; }
+            at = (size_t)it->second;
+        }
+        return rim[at].b == rim[0].a;
+    }
+
+    // Joins `eye` to the horizon of the faces it sees, starting from face `start`; changes nothing and returns
+    // false unless that horizon is one loop (src/hull.cpp: Builder::addPoint). The faces seen are found in
+    // breadth-first order over the edges in corner order, which fixes the order of the rim and so of the new
+    // faces.
+    bool raise(int start, int eye) {
+        std::vector<int> cone{ start };
+        std::vector<uint8_t> inCone(faceCount(), 0);
+        inCone[start] = 1;
+        std::vector<RimEdge> rim;
+        for (size_t k = 0; k < cone.size(); ++k) {
+            const int f = cone[k];
+            for (int e = 0; e < 3; ++e) {
+                const int g = across[f][e];
+                if (inCone[g]) { continue; }
+                const int a = tri[f][e], b = tri[f][(e + 1) % 3];
+                if (goesToo(f, g, a, b, eye)) {
+                    inCone[g] = 1;
+                    cone.push_back(g);
+                } else {
+                    rim.push_back({ a, b, g });
                 }
             }
-            std::vector<int> loop;
-            if (!outline(members, region, id, loop) || !convexLoop(loop, tris_[seed].normal)) {
-                for (size_t k = 1; k < members.size(); ++k) { region[members[k]] = -1; }
-                loop = growConvex(seed, region, id);
+        }
+        // A face first met from one side and later taken from another leaves an edge that is not rim.
+        rim.erase(std::remove_if(rim.begin(), rim.end(), [&](const RimEdge& r) { return inCone[r.outer] != 0; }),
+                  rim.end());
+        if (!oneLoop(rim)) { return false; }
+
+        std::vector<int> homeless;
+        for (int f : cone) {
+            for (int p = first[f]; p != kNone; p = follow[p]) {
+                if (p != eye) { homeless.push_back(p); }
             }
-            polygons.push_back(loop);
+            removeFace(f);
+        }
+        // The fan: one face per rim edge, in rim order. Face j sits on rim edge a_j -> b_j; across its edge 0 is
+        // the kept face, across edge 1 (b_j -> eye) the fan face starting at b_j, across edge 2 (eye -> a_j) the
+        // fan face ending at a_j.
+        const int fan0 = faceCount();
+        const int n = (int)rim.size();
+        std::vector<std::pair<int, int>> startOf(n), endOf(n);
+        for (int j = 0; j < n; ++j) {
+            addFace(rim[j].a, rim[j].b, eye);
+            startOf[j] = { rim[j].a, fan0 + j };
+            endOf[j] = { rim[j].b, fan0 + j };
+        }
+        std::sort(startOf.begin(), startOf.end());
+        std::sort(endOf.begin(), endOf.end());
+        auto find = [](const std::vector<std::pair<int, int>>& v, int key) {
+            return std::lower_bound(v.begin(), v.end(), std::make_pair(key, -1))->second;
+        };
+        std::vector<int> fan(n);
+        for (int j = 0; j < n; ++j) {
+            const int f = fan0 + j;
+            fan[j] = f;
+            const int outer = rim[j].outer;
+            across[f][0] = outer;
+            across[outer][edgeBack(outer, rim[j].a, rim[j].b)] = f;
+            across[f][1] = find(startOf, rim[j].b);
+            across[f][2] = find(endOf, rim[j].a);
+        }
+        place(homeless, fan);
+        return true;
+    }
+
+    // The tetrahedron (faces in the order and orientation src/hull.cpp: Builder::build gives them), then
+    // points until the budget is spent or none is left above a face.
+    void build(const int simplex[4], int maxVertices) {
+        Vec3 center{ 0, 0, 0 };
+        for (int i = 0; i < 4; ++i) { center += pts[simplex[i]] * 0.25f; }
+        static const int kTetra[4][3] = { { 0, 1, 2 }, { 0, 1, 3 }, { 0, 2, 3 }, { 1, 2, 3 } };
+        for (const auto& t : kTetra) {
+            int a = simplex[t[0]], b = simplex[t[1]], c = simplex[t[2]];
+            if (dot(cross(pts[b] - pts[a], pts[c] - pts[a]), pts[a] - center) < 0.0f) { std::swap(b, c); }
+            addFace(a, b, c);
+        }
+        for (int f = 0; f < 4; ++f) {
+            for (int e = 0; e < 3; ++e) {
+                for (int g = 0; g < 4; ++g) {
+                    if (g != f && edgeBack(g, tri[f][e], tri[f][(e + 1) % 3]) != kNone) { across[f][e] = g; }
+                }
+            }
+        }
+        std::vector<int> others;
+        for (int i = 0; i < (int)pts.size(); ++i) {
+            if (i != simplex[0] && i != simplex[1] && i != simplex[2] && i != simplex[3]) { others.push_back(i); }
+        }
+        place(others, { 0, 1, 2, 3 });
+        while (liveVertices < maxVertices) {
+            // The farthest point above any face: faces in order, each face's points in the order they came.
+            int face = kNone, eye = kNone;
+            float far = 0.0f;
+            for (int f = 0; f < faceCount(); ++f) {
+                if (!live[f]) { continue; }
+                for (int p = first[f]; p != kNone; p = follow[p]) {
+                    const float h = height(f, p);
+                    if (h > far) {
+                        far = h;
+                        face = f;
+                        eye = p;
+                    }
+                }
+            }
+            if (face == kNone) {
+                if (retryNearly()) { continue; }
+                break;
+            }
+            if (!raise(face, eye)) { dequeue(face, eye); }
+        }
+    }
+
+    // The points kept within the tolerance, tried once more against the faces as they are now.
+    bool retryNearly() {
+        std::vector<int> points;
+        points.swap(nearly);
+        for (int p : points) { tried[p] = 1; }
+        std::vector<int> faces;
+        for (int f = 0; f < faceCount(); ++f) {
+            if (live[f]) { faces.push_back(f); }
+        }
+        place(points, faces);
+        for (int f : faces) {
+            if (first[f] != kNone) { return true; }
+        }
+        return false;
+    }
+
+    // Whether face g lies in the plane of the region's seed, within the tolerance at each corner.
+    bool inPlane(int seed, int g) const {
+        if (dot(normal[seed], normal[g]) < kMergeCos) { return false; }
+        for (int v : tri[g]) {
+            if (std::fabs(height(seed, v)) > tol) { return false; }
+        }
+        return true;
+    }
+
+    // The outline of the faces marked `id` in `owner`, as one loop from its lowest vertex; false unless the
+    // outline is one simple loop (src/hull.cpp: Builder::boundary).
+    bool outline(const std::vector<int>& faces, const std::vector<int>& owner, int id, std::vector<int>& loop) const {
+        std::vector<std::pair<int, int>> step;  // (from, to) of every outline edge
+        for (int f : faces) {
+            for (int e = 0; e < 3; ++e) {
+                if (owner[across[f][e]] == id) { continue; }
+                step.push_back({ tri[f][e], tri[f][(e + 1) % 3] });
+            }
+        }
+        if (step.empty()) { return false; }
+        std::sort(step.begin(), step.end());
+        for (size_t i = 1; i < step.size(); ++i) {
+            if (step[i].first == step[i - 1].first) { return false; }
+        }
+        const int from = step[0].first;
+        int v = from;
+        do {
+            loop.push_back(v);
+            const auto it = std::lower_bound(step.begin(), step.end(), std::make_pair(v, INT32_MIN));
+            if (it == step.end() || it->first != v || loop.size() > step.size()) { return false; }
+            v = it->second;
+        } while (v != from);
+        return loop.size() == step.size();
+    }
+
+    // No corner of the loop bends back by more than the tolerance (src/hull.cpp: Builder::convex).
+    bool convexLoop(const std::vector<int>& loop, const Vec3& n) const {
+        const size_t k = loop.size();
+        for (size_t i = 0; i < k; ++i) {
+            const Vec3& a = pts[loop[i]];
+            const Vec3& b = pts[loop[(i + 1) % k]];
+            const Vec3& c = pts[loop[(i + 2) % k]];
+            if (dot(cross(b - a, c - b), n) < -tol * length(c - a)) { return false; }
+        }
+        return true;
+    }
+
+    // The coplanar neighbours of `seed`, breadth first over the edges in corner order, marked in `owner`.
+    std::vector<int> flood(int seed, std::vector<int>& owner, int id) const {
+        std::vector<int> faces{ seed };
+        owner[seed] = id;
+        for (size_t k = 0; k < faces.size(); ++k) {
+            for (int e = 0; e < 3; ++e) {
+                const int g = across[faces[k]][e];
+                if (owner[g] < 0 && inPlane(seed, g)) {
+                    owner[g] = id;
+                    faces.push_back(g);
+                }
+            }
+        }
+        return faces;
+    }
+
+    // A region grown from the seed one neighbour at a time, each kept only if the outline stays one convex
+    // loop (src/hull.cpp: Builder::grow).
+    std::vector<int> growConvex(int seed, std::vector<int>& owner, int id) const {
+        std::vector<int> faces{ seed }, loop;
+        outline(faces, owner, id, loop);
+        for (size_t k = 0; k < faces.size(); ++k) {
+            for (int e = 0; e < 3; ++e) {
+                const int g = across[faces[k]][e];
+                if (owner[g] >= 0 || !inPlane(seed, g)) { continue; }
+                owner[g] = id;
+                faces.push_back(g);
+                std::vector<int> grown;
+                if (outline(faces, owner, id, grown) && convexLoop(grown, normal[seed])) {
+                    loop.swap(grown);
+                } else {
+                    owner[g] = kNone;
+                    faces.pop_back();
+                }
+            }
+        }
+        return loop;
+    }
+
+    // The faces merged into polygons, regions seeded in face order; vertices numbered in order of first use.
+    HullResult polygons(const std::vector<Vec3>& original) const {
+        std::vector<int> owner(faceCount(), kNone);
+        std::vector<std::vector<int>> loops;
+        for (int seed = 0; seed < faceCount(); ++seed) {
+            if (!live[seed] || owner[seed] >= 0) { continue; }
+            const int id = (int)loops.size();
+            const std::vector<int> region = flood(seed, owner, id);
+            std::vector<int> loop;
+            if (!outline(region, owner, id, loop) || !convexLoop(loop, normal[seed])) {
+                for (size_t k = 1; k < region.size(); ++k) { owner[region[k]] = kNone; }
+                loop = growConvex(seed, owner, id);
+            }
+            loops.push_back(std::move(loop));
         }
         HullResult out;
-        std::vector<int> number(p_.size(), -1);
-        for (std::vector<int>& loop : polygons) {
+        std::vector<int> number(pts.size(), kNone);
+        for (std::vector<int>& loop : loops) {
             for (int& v : loop) {
-                if (number[v] < 0) {
+                if (number[v] == kNone) {
                     number[v] = (int)out.vertices.size();
-                    out.vertices.push_back(original_[v]);
+                    out.vertices.push_back(original[v]);
                 }
                 v = number[v];
             }
@@ -126,228 +425,11 @@ public:
         }
         return out;
     }
-
-private:
-    void addTri(int a, int b, int c) {
-        Tri f;
-        f.v[0] = a;
-        f.v[1] = b;
-        f.v[2] = c;
-        f.normal = normalize(cross(p_[b] - p_[a], p_[c] - p_[a]));
-        f.offset = dot(f.normal, p_[a]);
-        const int fi = (int)tris_.size();
-        for (int i = 0; i < 3; ++i) { edgeOwner_[directedEdge(f.v[i], f.v[(i + 1) % 3])] = fi; }
-        tris_.push_back(std::move(f));
-    }
-
-    float above(const Tri& f, int pi) const { return dot(f.normal, p_[pi]) - f.offset; }
-
-    // Each point goes to the candidate face it is farthest above (beyond the tolerance); a point within the
-    // tolerance of some face but above none is kept for one retry.
-    void distribute(const std::vector<int>& points, const std::vector<int>& candidates) {
-        for (int pi : points) {
-            int best = -1;
-            float far = tol_, top = -FLT_MAX;
-            for (int fi : candidates) {
-                const float d = above(tris_[fi], pi);
-                top = std::max(top, d);
-                if (d > far) {
-                    far = d;
-                    best = fi;
-                }
-            }
-            if (best >= 0) {
-                tris_[best].outside.push_back(pi);
-            } else if (top > 0.0f && !reclaimed_[pi]) {
-                dropped_.push_back(pi);
-            }
-        }
-    }
-
-    bool coplanar(const Tri& seed, const Tri& f) const {
-        if (dot(seed.normal, f.normal) < kCoplanarCos) { return false; }
-        for (int v : f.v) {
-            if (std::fabs(above(seed, v)) > tol_) { return false; }
-        }
-        return true;
-    }
-
-    int usedVertices() const {
-        std::vector<bool> used(p_.size(), false);
-        int n = 0;
-        for (const Tri& f : tris_) {
-            if (!f.alive) { continue; }
-            for (int v : f.v) {
-                if (!used[v]) {
-                    used[v] = true;
-                    ++n;
-                }
-            }
-        }
-        return n;
-    }
-
-    // Points dropped within the tolerance are tested once more against the finished faces.
-    bool retryDropped() {
-        std::vector<int> points, alive;
-        points.swap(dropped_);
-        for (int pi : points) { reclaimed_[pi] = true; }
-        for (int fi = 0; fi < (int)tris_.size(); ++fi) {
-            if (tris_[fi].alive) { alive.push_back(fi); }
-        }
-        distribute(points, alive);
-        for (int fi : alive) {
-            if (!tris_[fi].outside.empty()) { return true; }
-        }
-        return false;
-    }
-
-    // Whether face f, across edge a-b of the visible face `from`, must go as well: the eye is clearly above
-    // it, the new face over a-b would be a sliver or fold back over it, or would face inward.
-    bool mustGo(const Tri& from, const Tri& f, int a, int b, int eye) const {
-        const float d = above(f, eye);
-        if (d > tol_) { return true; }
-        const Vec3 edge = normalize(p_[b] - p_[a]);
-        const Vec3 r = p_[eye] - p_[a];
-        const float h = length(r - edge * dot(r, edge));
-        if (h <= tol_) { return true; }
-        if (above(from, eye) <= tol_ && dot(r, cross(from.normal, edge)) <= 0.0f) { return true; }
-        if (d <= 0.0f) { return false; }
-        return dot(r, cross(f.normal, edge)) <= 0.0f || d > fold_ * h;
-    }
-
-    // Adds the eye, unless the horizon of the faces it removes is not a single loop (then nothing changes).
-    bool addEye(int start, int eye) {
-        std::vector<int> visible{ start };
-        std::vector<bool> seen(tris_.size(), false);
-        seen[start] = true;
-        std::vector<std::pair<int, int>> horizon;
-        for (size_t k = 0; k < visible.size(); ++k) {
-            const Tri& f = tris_[visible[k]];
-            for (int i = 0; i < 3; ++i) {
-                const int a = f.v[i], b = f.v[(i + 1) % 3];
-                const int twin = edgeOwner_.at(directedEdge(b, a));
-                if (seen[twin]) { continue; }
-                if (mustGo(f, tris_[twin], a, b, eye)) {
-                    seen[twin] = true;
-                    visible.push_back(twin);
-                } else {
-                    horizon.push_back({ a, b });
-                }
-            }
-        }
-        std::vector<std::pair<int, int>> kept;
-        for (const auto& e : horizon) {
-            if (!seen[edgeOwner_.at(directedEdge(e.second, e.first))]) { kept.push_back(e); }
-        }
-        horizon.swap(kept);
-        if (!oneLoop(horizon)) { return false; }
-        std::vector<int> homeless;
-        for (int fi : visible) {
-            Tri& f = tris_[fi];
-            f.alive = false;
-            for (int i = 0; i < 3; ++i) { edgeOwner_.erase(directedEdge(f.v[i], f.v[(i + 1) % 3])); }
-            for (int pi : f.outside) {
-                if (pi != eye) { homeless.push_back(pi); }
-            }
-            f.outside.clear();
-        }
-        std::vector<int> fresh;
-        for (const auto& e : horizon) {
-            fresh.push_back((int)tris_.size());
-            addTri(e.first, e.second, eye);
-        }
-        distribute(homeless, fresh);
-        return true;
-    }
-
-    // The horizon edges (a, b) must chain into one closed loop, each start vertex used once.
-    static bool oneLoop(const std::vector<std::pair<int, int>>& horizon) {
-        for (size_t i = 0; i < horizon.size(); ++i) {
-            for (size_t j = 0; j < i; ++j) {
-                if (horizon[i].first == horizon[j].first) { return false; }
-            }
-        }
-        int v = horizon.empty() ? -1 : horizon[0].second;
-        for (size_t steps = 1; steps < horizon.size(); ++steps) {
-            size_t k = 0;
-            while (k < horizon.size() && horizon[k].first != v) { ++k; }
-            if (k == horizon.size() || k == 0) { return false; }
-            v = horizon[k].second;
-        }
-        return !horizon.empty() && v == horizon[0].first;
-    }
-
-    // Every corner of the loop turns left about the normal, up to the tolerance.
-    bool convexLoop(const std::vector<int>& loop, const Vec3& normal) const {
-        const size_t n = loop.size();
-        for (size_t i = 0; i < n; ++i) {
-            const Vec3& a = p_[loop[i]];
-            const Vec3& b = p_[loop[(i + 1) % n]];
-            const Vec3& c = p_[loop[(i + 2) % n]];
-            if (dot(cross(b - a, c - b), normal) < -tol_ * length(c - a)) { return false; }
-        }
-        return true;
-    }
-
-    // Grows a region from its seed one coplanar face at a time, keeping its outline one convex loop.
-    std::vector<int> growConvex(int seed, std::vector<int>& region, int id) const {
-        std::vector<int> members{ seed }, loop;
-        outline(members, region, id, loop);
-        for (size_t k = 0; k < members.size(); ++k) {
-            for (int i = 0; i < 3; ++i) {
-                const Tri& f = tris_[members[k]];
-                const int twin = edgeOwner_.at(directedEdge(f.v[(i + 1) % 3], f.v[i]));
-                if (region[twin] >= 0 || !coplanar(tris_[seed], tris_[twin])) { continue; }
-                region[twin] = id;
-                members.push_back(twin);
-                std::vector<int> grown;
-                if (outline(members, region, id, grown) && convexLoop(grown, tris_[seed].normal)) {
-                    loop.swap(grown);
-                } else {
-                    region[twin] = -1;
-                    members.pop_back();
-                }
-            }
-        }
-        return loop;
-    }
-
-    // The outline of a region as one simple loop from its lowest vertex; fails otherwise.
-    bool outline(const std::vector<int>& members, const std::vector<int>& region, int id, std::vector<int>& loop) const {
-        std::map<int, int> next;
-        for (int fi : members) {
-            const Tri& f = tris_[fi];
-            for (int i = 0; i < 3; ++i) {
-                const int a = f.v[i], b = f.v[(i + 1) % 3];
-                if (region[edgeOwner_.at(directedEdge(b, a))] == id) { continue; }
-                if (!next.emplace(a, b).second) { return false; }
-            }
-        }
-        if (next.empty()) { return false; }
-        const int start = next.begin()->first;
-        int v = start;
-        do {
-            loop.push_back(v);
-            auto it = next.find(v);
-            if (it == next.end() || loop.size() > next.size()) { return false; }
-            v = it->second;
-        } while (v != start);
-        return loop.size() == next.size();
-    }
-
-    const std::vector<Vec3>& p_;
-    const std::vector<Vec3>& original_;
-    float tol_;
-    float fold_;  // sine of the steepest fold-back that leaves no corner more than the tolerance outside
-    std::vector<Tri> tris_;
-    std::unordered_map<uint64_t, int> edgeOwner_;  // directed edge -> the face it belongs to
-    std::vector<int> dropped_;
-    std::vector<bool> reclaimed_;
 };
 
-// Every point offset to each corner of a box spanned by `count` axes at +-t.
-inline std::vector<Vec3> thickened(const std::vector<Vec3>& points, const Vec3* axes, int count, float t) {
+// Every point moved to each corner of a box of half size t along `count` axes, corners in binary order and the
+// axes added one after another (src/hull.cpp: thicken).
+inline std::vector<Vec3> slab(const std::vector<Vec3>& points, const Vec3* axes, int count, float t) {
     std::vector<Vec3> out;
     out.reserve(points.size() << count);
     for (const Vec3& p : points) {
@@ -360,16 +442,32 @@ inline std::vector<Vec3> thickened(const std::vector<Vec3>& points, const Vec3* 
     return out;
 }
 
-// src/hull.cpp:332-400: tolerances from the cloud's size, the initial simplex from extreme points, degenerate
-// clouds thickened once.
-inline HullResult hullOf(const std::vector<Vec3>& points, int maxVertices, bool thickenFlat) {
+// The first point farthest by `measure` (strictly greater wins, so the first of equals stays), with its value.
+template <class Measure>
+inline std::pair<int, float> farthest(const std::vector<Vec3>& points, Measure measure) {
+    int at = 0;
+    float best = 0.0f;
+    for (int i = 0; i < (int)points.size(); ++i) {
+        const float d = measure(points[i]);
+        if (d > best) {
+            best = d;
+            at = i;
+        }
+    }
+    return { at, best };
+}
+
+// src/hull.cpp: hullOf. Tolerances from the cloud's extent; the tetrahedron from the farthest pair of axis
+// extremes, the point farthest from their line and the point farthest from that plane; a cloud without volume
+// is thickened once (the slab is far wider than the tolerance, so the thickened cloud has volume).
+inline HullResult hullOf(const std::vector<Vec3>& points, int maxVertices, bool mayThicken) {
     if (points.empty()) { return {}; }
     Vec3 lo = points[0], hi = points[0];
-    int extreme[6] = {};
+    int ext[6] = { 0, 0, 0, 0, 0, 0 };  // lowest and highest point along x, y, z (first of equals)
     for (int i = 0; i < (int)points.size(); ++i) {
         for (int k = 0; k < 3; ++k) {
-            if (comp(points[i], k) < comp(points[extreme[2 * k]], k)) { extreme[2 * k] = i; }
-            if (comp(points[i], k) > comp(points[extreme[2 * k + 1]], k)) { extreme[2 * k + 1] = i; }
+            if (comp(points[i], k) < comp(points[ext[2 * k]], k)) { ext[2 * k] = i; }
+            if (comp(points[i], k) > comp(points[ext[2 * k + 1]], k)) { ext[2 * k + 1] = i; }
         }
         lo = minVec(lo, points[i]);
         hi = maxVec(hi, points[i]);
@@ -379,69 +477,59 @@ inline HullResult hullOf(const std::vector<Vec3>& points, int maxVertices, bool 
     for (int k = 0; k < 3; ++k) { reach += std::max(std::fabs(comp(lo, k)), std::fabs(comp(hi, k))); }
     if (!std::isfinite(size) || !std::isfinite(reach)) { return {}; }
     const float tol = std::max({ 1e-4f * size, 3.0f * FLT_EPSILON * reach, 1e-8f });
-    const float slab = std::max({ 0.005f * size, 1e-4f, 10.0f * tol });
+    const float half = std::max({ 0.005f * size, 1e-4f, 10.0f * tol });
 
-    int s[4] = { extreme[0], extreme[0], 0, 0 };
-    float best = 0.0f;
+    int corner[4] = { ext[0], ext[0], 0, 0 };
+    float spread = 0.0f;
     for (int i = 0; i < 6; ++i) {
         for (int j = i + 1; j < 6; ++j) {
-            const float d = lengthSquared(points[extreme[i]] - points[extreme[j]]);
-            if (d > best) {
-                best = d;
-                s[0] = extreme[i];
-                s[1] = extreme[j];
+            const float d = lengthSquared(points[ext[i]] - points[ext[j]]);
+            if (d > spread) {
+                spread = d;
+                corner[0] = ext[i];
+                corner[1] = ext[j];
             }
         }
     }
-    if (best <= tol * tol) {
-        if (!thickenFlat) { return {}; }
+    if (spread <= tol * tol) {
+        if (!mayThicken) { return {}; }
         const Vec3 axes[3] = { { 1, 0, 0 }, { 0, 1, 0 }, { 0, 0, 1 } };
-        return hullOf(thickened(points, axes, 3, slab), maxVertices, false);
+        return hullOf(slab(points, axes, 3, half), maxVertices, false);
     }
-    const Vec3 dir = normalize(points[s[1]] - points[s[0]]);
-    best = 0.0f;
-    for (int i = 0; i < (int)points.size(); ++i) {
-        const float d = length(cross(points[i] - points[s[0]], dir));
-        if (d > best) {
-            best = d;
-            s[2] = i;
-        }
-    }
-    if (best <= tol) {
-        if (!thickenFlat) { return {}; }
+    const Vec3 o = points[corner[0]];
+    const Vec3 dir = normalize(points[corner[1]] - o);
+    const auto offLine = farthest(points, [&](const Vec3& p) { return length(cross(p - o, dir)); });
+    corner[2] = offLine.first;
+    if (offLine.second <= tol) {
+        if (!mayThicken) { return {}; }
         const Vec3 u = perpendicular(dir);
         const Vec3 axes[2] = { u, cross(dir, u) };
-        return hullOf(thickened(points, axes, 2, slab), maxVertices, false);
+        return hullOf(slab(points, axes, 2, half), maxVertices, false);
     }
-    const Vec3 n = normalize(cross(points[s[1]] - points[s[0]], points[s[2]] - points[s[0]]));
-    best = 0.0f;
-    for (int i = 0; i < (int)points.size(); ++i) {
-        const float d = std::fabs(dot(points[i] - points[s[0]], n));
-        if (d > best) {
-            best = d;
-            s[3] = i;
-        }
+    const Vec3 n = normalize(cross(points[corner[1]] - o, points[corner[2]] - o));
+    const auto offPlane = farthest(points, [&](const Vec3& p) { return std::fabs(dot(p - o, n)); });
+    corner[3] = offPlane.first;
+    if (offPlane.second <= tol) {
+        if (!mayThicken) { return {}; }
+        return hullOf(slab(points, &n, 1, half), maxVertices, false);
     }
-    if (best <= tol) {
-        if (!thickenFlat) { return {}; }
-        return hullOf(thickened(points, &n, 1, slab), maxVertices, false);
-    }
-    // Built about the box centre, so the tolerance needs no allowance for distance from the origin.
-    const Vec3 center = (lo + hi) * 0.5f;
+    // Built about the box's centre, so the tolerance needs no allowance for distance from the origin.
+    const Vec3 mid = (lo + hi) * 0.5f;
     std::vector<Vec3> local;
     local.reserve(points.size());
-    for (const Vec3& p : points) { local.push_back(p - center); }
-    Quickhull q(local, points, std::max(1e-4f * size, 1e-8f), size);
-    q.run(s, maxVertices);
-    return q.result();
+    for (const Vec3& p : points) { local.push_back(p - mid); }
+    Surface s(local, std::max(1e-4f * size, 1e-8f), size);
+    s.build(corner, maxVertices);
+    return s.polygons(points);
 }
 
 }  // namespace hull
 
-// At least 4 vertices; non-finite points are skipped (src/hull.cpp:404-410).
+// At least 4 vertices; non-finite points are skipped (src/hull.cpp: computeHull).
 inline HullResult computeHull(const std::vector<Vec3>& points, int maxVertices) {
     maxVertices = std::max(maxVertices, 4);
     std::vector<Vec3> kept;
+    kept.reserve(points.size());
     for (const Vec3& p : points) {
         if (std::isfinite(p.x) && std::isfinite(p.y) && std::isfinite(p.z)) { kept.push_back(p); }
     }
