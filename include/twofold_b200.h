@@ -436,11 +436,13 @@ TF_API int tf_world_autotune(void* world, float dt, int32_t trial_steps, uint32_
 /* Launch shape of one kernel (0 broadphase, 1 narrowphase, 2 wake, 3 prepare, 4 refresh, 5 substep,
  * 6 finish, 7 pair collisions; -1 every kernel): threads per CTA (a multiple of 32, at most 512), the world size in bodies
  * above which a world is stepped by a whole CTA (smaller worlds take one warp each), and the shared memory
- * a CTA stages worlds in (clamped to what the device allows). Takes effect at the next step. No
- * counterpart in the reference, which steps each world on one host thread; the autotuner uses it. */
+ * a CTA stages worlds in (clamped to what the device allows). For the substep, big_bodies = -1 selects the
+ * flat solve instead (every world's contacts of a color at once across the device, at most 256 threads per
+ * CTA, no staging). Takes effect at the next step. No counterpart in the reference, which steps each world on
+ * one host thread; the autotuner uses it. */
 TF_API int tf_world_set_launch(void* world, int32_t kernel, int32_t threads, int32_t big_bodies, int32_t smem_bytes);
-/* The shape in use: out[0] threads, [1] big-world threshold, [2] shared bytes, [3] grid size, [4] bodies
- * a whole-CTA world can stage, [5] bodies a warp's world can stage. */
+/* The shape in use: out[0] threads, [1] big-world threshold (0xffffffff for the flat solve), [2] shared bytes,
+ * [3] grid size, [4] bodies a whole-CTA world can stage, [5] bodies a warp's world can stage. */
 TF_API int tf_world_get_launch(void* world, int32_t kernel, uint32_t out[6]);
 
 /* ---- Candidate pairs without device allocation (no counterpart in the reference) ----

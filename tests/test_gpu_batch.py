@@ -57,3 +57,47 @@ def test_autotune_leaves_the_state_alone():
     plain.step_checked(sc.dt, 20)
     tuned.step_checked(sc.dt, 20, graph=True)
     assert states_bitwise_equal(plain.states(), tuned.states())
+
+
+def _mixed_scene():
+    """Uneven worlds with restitution, impact walls (impact colors), planar piles (contacts solved one at a time by
+    level) and jointed worlds in one batch: every path of the flat solve."""
+    worlds = list(scenes.config4(n_worlds=40, seed=11).worlds)
+    worlds += list(scenes.config5(n_worlds=6).worlds)
+    worlds += [scenes.planar(n=48, cols=8, spheres=4, sphere_height=(3.0, 8.0), seed=s, restitution=0.2) for s in range(3)]
+    worlds += [scenes.jointed(s) for s in range(2)]
+    return scenes.Scene("mixed", worlds)
+
+
+@pytest.mark.parametrize("threads", [128, 256])
+def test_flat_solve_matches_the_world_kernels(threads):
+    """The flat solve (every world's contacts of a color at once across the device, a grid barrier between
+    colors) gives the world kernels' bits: states, contacts and candidate pairs, by direct launches and by graph."""
+    sc = _mixed_scene()
+    worlds_kernel = Batch.from_scene(sc)
+    flat = Batch.from_scene(sc)
+    worlds_kernel.set_launch("substep", 128, 128, 32 * 1024)
+    flat.set_launch("substep", threads, -1, 0)
+    assert flat.launch("substep")["big_bodies"] == 0xFFFFFFFF
+    for steps, graph in ((20, False), (20, True), (40, True)):
+        worlds_kernel.step_checked(sc.dt, steps)
+        flat.step_checked(sc.dt, steps, graph=graph)
+        assert states_bitwise_equal(worlds_kernel.states(), flat.states())
+    for w in range(len(sc.worlds)):
+        assert np.array_equal(worlds_kernel.candidates(w), flat.candidates(w))
+    assert flat.device_flags() == 0
+
+
+def test_flat_solve_is_the_default_for_many_worlds_and_autotuned():
+    sc = _scene(1024, 2)
+    b = Batch.from_scene(sc)
+    b.step_checked(sc.dt, 8)
+    assert b.launch("substep")["big_bodies"] == 0xFFFFFFFF
+    ref = Batch.from_scene(sc)
+    ref.set_launch("substep", 128, 128, 32 * 1024)
+    ref.step_checked(sc.dt, 8)
+    choice = b.autotune(sc.dt, trial_steps=1)
+    assert "substep" in choice
+    b.step_checked(sc.dt, 12, graph=True)
+    ref.step_checked(sc.dt, 12)
+    assert states_bitwise_equal(ref.states(), b.states())

@@ -14,7 +14,8 @@ OUT = os.path.join(HERE, "libtwofold_b200.so")
 
 # The engine (host code, no kernels) and the kernel groups it launches (tf_launch.h), which compile in parallel.
 SOURCES = [os.path.join(CSRC, f) for f in ("tf_engine.cu", "tf_k_broad.cu", "tf_k_collide.cu", "tf_k_refresh.cu",
-                                           "tf_k_solve.cu", "tf_k_finish.cu", "tf_noalloc.cu", "tf_adjoint.cu")]
+                                           "tf_k_solve.cu", "tf_k_finish.cu", "tf_k_flat.cu", "tf_noalloc.cu",
+                                           "tf_adjoint.cu")]
 HEADERS = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))] + [
     os.path.join(ROOT, "include", "twofold_b200.h")]
 
@@ -50,10 +51,17 @@ CONTRACTED = {"tf_adjoint.cu"}
 BUILD_DIR = os.path.join(HERE, "_build")
 
 
+# The flat solve's CTAs read what other CTAs of the same launch wrote before a grid barrier: its global loads
+# must come from L2, not from an SM's L1, which is not kept coherent with other SMs' stores.
+L2_LOADS = {"tf_k_flat.cu"}
+
+
 def _flags(source):
     flags = list(NVCC_FLAGS)
     if os.path.basename(source) in CONTRACTED:
         flags[flags.index("--fmad=false")] = "--fmad=true"
+    if os.path.basename(source) in L2_LOADS:
+        flags += ["-Xptxas", "-dlcm=cg"]
     return flags
 
 

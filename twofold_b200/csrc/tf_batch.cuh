@@ -70,6 +70,13 @@ struct Batch {
     float4* rows;
     size_t rowStride;
     uint32_t* slotOf;
+    // The flat solve of batches of many worlds: every body's solver state (kFlatBodyWords float4 per body:
+    // velocity, spin, displacement and turn of the substep, type and awake flags), and per color the record
+    // slots of that color's contacts in every world (color k from the batch-wide start of color k, both lists
+    // totalling at most one entry per contact slot).
+    float4* flatBodies;
+    uint32_t* flatColored;
+    uint32_t* flatImpact;
     uint8_t* cflags;          // by contact: kFast, kFastSolid
     uint64_t* mergeKeyA;
     uint32_t* mergePartA;

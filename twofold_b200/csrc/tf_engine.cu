@@ -168,8 +168,8 @@ public:
     DevArray<uint32_t> dActive, dImpact, dColored, dImpactColored, dRest, dImpactRest, dRestLevel, dImpactRestLevel;
     DevArray<uint8_t> dColor, dCflags;
     DevArray<Axis> dAxes;
-    DevArray<float4> dRows;
-    DevArray<uint32_t> dSlotOf;
+    DevArray<float4> dRows, dFlatBodies;
+    DevArray<uint32_t> dSlotOf, dFlatColored, dFlatImpact;
     DevArray<uint64_t> dMergeKeyA, dMergeKeyB;
     DevArray<uint32_t> dMergePartA, dMergePartB, dMergeIdxA, dMergeIdxB;
     bool hasJoints = false;  // some world has joints: the substep and finish kernels with joint code run
@@ -191,7 +191,9 @@ public:
     struct LaunchShape {
         uint32_t threads = 256, bigBodies = 0, smemBytes = 0;
         bool chosen = false;
+        bool flat = false;  // the substep only: the flat solve over every world (k_substep_flat)
     };
+    static constexpr uint32_t kFlatShape = 0xffffffffu;  // bigBodies of a substep shape that selects the flat solve
     // broadphase, narrowphase, wake, prepare, refresh, substep, finish, collide. Refresh and collide run one
     // thread per work item over the whole grid; their shapes use only the thread count.
     static constexpr int kKernels = 8;
@@ -332,6 +334,24 @@ public:
     void launch(int id, unsigned grid, unsigned block, size_t smem, Args... args) {
         void* ptrs[] = { (void*)&args... };
         cudaLaunchKernel(kernelEntry(id), dim3(grid), dim3(block), ptrs, smem, stream);
+    }
+
+    // A cooperative launch (every CTA resident at once, which the flat solve's grid barrier needs); grid must
+    // not exceed what fits on the device.
+    template <class... Args>
+    void launchCooperative(int id, unsigned grid, unsigned block, Args... args) {
+        void* ptrs[] = { (void*)&args... };
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(grid);
+        cfg.blockDim = dim3(block);
+        cfg.dynamicSmemBytes = 0;
+        cfg.stream = stream;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeCooperative;
+        attr[0].val.cooperative = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        cudaLaunchKernelExC(&cfg, kernelEntry(id), ptrs);
     }
 
     // Brackets one kernel launch with events when per-kernel profiling is on: from the event pool for direct
@@ -1137,6 +1157,9 @@ public:
         TF_ALLOC(dAxes, ncon * kAxesPerContact);
         TF_ALLOC(dRows, ncon * kRowWords);
         TF_ALLOC(dSlotOf, ncon);
+        TF_ALLOC(dFlatBodies, nb * kFlatBodyWords);
+        TF_ALLOC(dFlatColored, ncon);
+        TF_ALLOC(dFlatImpact, ncon);
         TF_ALLOC(dMergeKeyA, ncon);
         TF_ALLOC(dMergeKeyB, ncon);
         TF_ALLOC(dMergePartA, ncon);
@@ -1332,6 +1355,9 @@ public:
         B.rows = dRows.ptr;
         B.rowStride = dContacts[0].n;
         B.slotOf = dSlotOf.ptr;
+        B.flatBodies = dFlatBodies.ptr;
+        B.flatColored = dFlatColored.ptr;
+        B.flatImpact = dFlatImpact.ptr;
         B.mergeKeyA = dMergeKeyA.ptr;
         B.mergePartA = dMergePartA.ptr;
         B.mergeIdxA = dMergeIdxA.ptr;
@@ -1418,7 +1444,11 @@ public:
                 });
             }
             timed(5, rec, [&] {
-                launch(hasJoints ? kKSubstepJoints : kKSubstep, grids[5], threads(5), smem(5), B, P, splits[5], i, serial);
+                if (shapes[5].flat) {
+                    launchCooperative(hasJoints ? kKSubstepFlatJoints : kKSubstepFlat, grids[5], threads(5), B, P, i, serial);
+                } else {
+                    launch(hasJoints ? kKSubstepJoints : kKSubstep, grids[5], threads(5), smem(5), B, P, splits[5], i, serial);
+                }
             });
         }
         timed(6, rec, [&] {
@@ -1467,6 +1497,13 @@ public:
         s.bigBodies = many ? 96u : 0u;
         const bool stages = k == 0 || k == 3 || k == 5 || k == 6;
         s.smemBytes = stages ? 64u * 1024u : 0u;
+        if (k == 5 && many) {
+            // Batches of many worlds solve flat (k_substep_flat).
+            s.threads = 256u;
+            s.bigBodies = 0u;
+            s.smemBytes = 0u;
+            s.flat = true;
+        }
         return s;
     }
 
@@ -1499,14 +1536,24 @@ public:
     int configureLaunches() {
         int rc = configureKernels();
         if (rc != TF_OK) { return rc; }
-        const void* fns[kKernels] = { kernelEntry(kKBroadphase), kernelEntry(kKNarrowphase), kernelEntry(kKWake),
-                                      kernelEntry(kKPrepare),    kernelEntry(kKRefresh + kPairClasses),
-                                      kernelEntry(hasJoints ? kKSubstepJoints : kKSubstep),
-                                      kernelEntry(hasJoints ? kKFinishJoints : kKFinish),
-                                      kernelEntry(kKCollide + kClassConvex) };
         for (int k = 0; k < kKernels; ++k) {
             LaunchShape& sh = shapes[k];
             if (!sh.chosen) { sh = defaultShape(k); }
+            if (k == 5 && sh.flat) {
+                // The flat solve: as many CTAs as are resident at once, all in one cooperative launch.
+                int perSm = 0;
+                TF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                    &perSm, kernelEntry(hasJoints ? kKSubstepFlatJoints : kKSubstepFlat), (int)sh.threads, 0));
+                if (perSm < 1) { return fail(TF_E_INVALID, "launch shape does not fit on an SM"); }
+                splits[k] = Split{};
+                grids[k] = smCount * perSm;
+                continue;
+            }
+            const void* fns[kKernels] = { kernelEntry(kKBroadphase), kernelEntry(kKNarrowphase), kernelEntry(kKWake),
+                                          kernelEntry(kKPrepare),    kernelEntry(kKRefresh + kPairClasses),
+                                          kernelEntry(hasJoints ? kKSubstepJoints : kKSubstep),
+                                          kernelEntry(hasJoints ? kKFinishJoints : kKFinish),
+                                          kernelEntry(kKCollide + kClassConvex) };
             const uint32_t warps = sh.threads / 32;
             auto lim = dynSmemLimit.find(fns[k]);
             const uint32_t limit = lim == dynSmemLimit.end() ? 0u : (uint32_t)lim->second;
@@ -1558,9 +1605,13 @@ public:
         if (threads > kMaxFlatBlock && (k < 0 || flatKernel(k))) {
             return fail(TF_E_INVALID, "launch shape: the refresh and collide kernels take at most 256 threads");
         }
+        const bool flat = bigBodies == kFlatShape;
+        if (flat && (k != 5 || threads > 256)) {
+            return fail(TF_E_INVALID, "launch shape: the flat solve is a substep shape of at most 256 threads");
+        }
         for (int i = 0; i < kKernels; ++i) {
             if (k >= 0 && i != k) { continue; }
-            shapes[i] = LaunchShape{ threads, bigBodies, smemBytes, true };
+            shapes[i] = LaunchShape{ threads, flat ? 0u : bigBodies, flat ? 0u : smemBytes, true, flat };
         }
         dropGraphs();
         if (laidOut) { return configureLaunches(); }
@@ -1570,7 +1621,7 @@ public:
     int getLaunch(int k, uint32_t* out) const {
         if (k < 0 || k >= kKernels) { return TF_E_INVALID; }
         out[0] = shapes[k].threads;
-        out[1] = shapes[k].bigBodies;
+        out[1] = shapes[k].flat ? kFlatShape : shapes[k].bigBodies;
         out[2] = splits[k].smemBytes;
         out[3] = (uint32_t)grids[k];
         out[4] = splits[k].big.bodies;
@@ -1828,6 +1879,9 @@ public:
                 continue;
             }
             const bool stages = k == 0 || k == 3 || k == 5 || k == 6;
+            if (k == 5) {
+                for (uint32_t t : { 128u, 256u }) { cands[k].push_back(LaunchShape{ t, 0u, 0u, true, true }); }
+            }
             for (uint32_t t : { 128u, 256u, 512u }) {
                 for (uint32_t big : { 0u, 32u, 64u, 128u, 256u }) {
                     if (stages) {
@@ -1891,7 +1945,7 @@ public:
         if (out) {
             for (int k = 0; k < kKernels; ++k) {
                 out[3 * k] = shapes[k].threads;
-                out[3 * k + 1] = shapes[k].bigBodies;
+                out[3 * k + 1] = shapes[k].flat ? kFlatShape : shapes[k].bigBodies;
                 out[3 * k + 2] = shapes[k].smemBytes;
             }
         }
@@ -2745,7 +2799,9 @@ TF_API int tf_world_solver_counts(void* h, int32_t w, int32_t out[8]) {
 
 TF_API int tf_world_set_launch(void* h, int32_t kernel, int32_t threads, int32_t big_bodies, int32_t smem_bytes) {
     if (!h) { return tfb::fail(TF_E_INVALID, "tf_world_set_launch: null"); }
-    if (big_bodies < 0 || smem_bytes < 0) { return tfb::fail(TF_E_INVALID, "tf_world_set_launch: negative size"); }
+    if ((big_bodies < 0 && !(kernel == 5 && big_bodies == -1)) || smem_bytes < 0) {
+        return tfb::fail(TF_E_INVALID, "tf_world_set_launch: negative size");
+    }
     Engine* e = E(h);
     if (cudaSetDevice(e->device) != cudaSuccess) { return tfb::fail(TF_E_CUDA, "tf_world_set_launch: cudaSetDevice"); }
     return e->setLaunch(kernel, (uint32_t)threads, (uint32_t)big_bodies, (uint32_t)smem_bytes);

@@ -43,7 +43,14 @@ enum WorkSlot : int {
     kSlotFastItems = kSlotCandItems + kPairClasses,       // + pair class: fast contacts of that class; + kPairClasses:
                                                           // the other active contacts of refreshed worlds
     kSlotTape = kSlotFastItems + kPairClasses + 1,      // the recording kernel's world counter
-    kSlotCount = kSlotTape + 1
+    // The flat solve of batches of many worlds (k_substep_flat): each color's contacts over every world, the
+    // impact colors' likewise, the most colors and impact colors any world has, and the grid barrier.
+    kSlotFlatColor = kSlotTape + 1,                    // + color: contacts of that color in all worlds
+    kSlotFlatImpact = kSlotFlatColor + kColors,        // + color
+    kSlotFlatMaxColors = kSlotFlatImpact + kColors,
+    kSlotFlatMaxImpact = kSlotFlatMaxColors + 1,
+    kSlotFlatBarrier = kSlotFlatMaxImpact + 1,         // arrivals, then generation
+    kSlotCount = kSlotFlatBarrier + 2
 };
 
 // A group of threads that steps one world at a time: one warp, several warps, or the whole CTA.
@@ -1388,7 +1395,7 @@ constexpr uint32_t kNotColorable = 0x80000000u;
 // pass sees the bits of the axes as built. 144 bytes a point and 144 a contact, against 240 bytes a point of
 // stored axes plus the lines of the 560-byte contact a pass read before.
 enum RowWord : int {
-    kRowHead = 0,    // bodyA, bodyB (world-local), point count, contact index (as integer bits)
+    kRowHead = 0,    // bodyA, bodyB (global), point count, contact index within the world (as integer bits)
     kRowNormal = 1,  // normal, friction
     kRowT1 = 2,      // tangent1, unused
     kRowT2 = 3,      // tangent2, unused
@@ -1438,8 +1445,8 @@ static __device__ void buildRow(const Batch& B, const WorldInfo& wi, uint32_t sl
     float4* R = B.rows + slot;
     const size_t S = B.rowStride;
     const int n = c.count;
-    R[kRowHead * S] = make_float4(__uint_as_float(c.bodyA - wi.bodyFirst), __uint_as_float(c.bodyB - wi.bodyFirst),
-                                  __uint_as_float((uint32_t)n), __uint_as_float(ci));
+    R[kRowHead * S] = make_float4(__uint_as_float(c.bodyA), __uint_as_float(c.bodyB), __uint_as_float((uint32_t)n),
+                                  __uint_as_float(ci));
     R[kRowNormal * S] = f4(c.normal, c.friction);
     R[kRowT1 * S] = f4(c.tangent1, 0.0f);
     R[kRowT2 * S] = f4(c.tangent2, 0.0f);
@@ -2239,6 +2246,190 @@ __device__ __forceinline__ void rebuildSolverData(const Batch& B, const WorldInf
                     B.axes + (size_t)(wi.contactFirst + ci) * kAxesPerContact);
 }
 
+// The flat solve's store: the solver state of every body in global memory, kFlatBodyWords float4 a body
+// (velocity and spin, the substep's displacement and turn, type | awake << 8), small enough that a batch's
+// bodies stay in L2 while its contacts are solved, indexed from a first body (a world's, or 0 for global
+// indices). The same methods as SolverStore's, over that array.
+constexpr int kFlatBodyWords = 4;
+
+struct FlatStore {
+    float4* s;
+    DBody* g;
+    static constexpr bool staged = true;
+
+    __device__ __forceinline__ LanedBody loadLaned(uint32_t i) const {
+        const float4 a = s[kFlatBodyWords * i], b = s[kFlatBodyWords * i + 1], c = s[kFlatBodyWords * i + 2],
+                     d = s[kFlatBodyWords * i + 3];
+        LanedBody x;
+        x.v = { a.x, a.y, a.z };
+        x.w = { a.w, b.x, b.y };
+        x.dp = { b.z, b.w, c.x };
+        x.dq = { c.y, c.z, c.w, d.x };
+        const uint32_t f = __float_as_uint(d.y);
+        x.type = f & 0xffu;
+        x.awake = f >> 8;
+        return x;
+    }
+
+    __device__ SBody load(uint32_t i) const {
+        const LanedBody l = loadLaned(i);
+        SBody b;
+        b.v = l.v;
+        b.w = l.w;
+        b.dp = l.dp;
+        b.dq = l.dq;
+        b.type = l.type;
+        b.awake = l.awake;
+        b.invInertiaWorld = g[i].invInertiaWorld;
+        b.planeInvMass = g[i].planeInvMass;
+        b.planeInvInertia = g[i].planeInvInertia;
+        return b;
+    }
+
+    template <class BodyT>
+    __device__ __forceinline__ void storeVW(uint32_t i, const BodyT& b) const {
+        s[kFlatBodyWords * i] = make_float4(b.v.x, b.v.y, b.v.z, b.w.x);
+        reinterpret_cast<float2*>(s + kFlatBodyWords * i + 1)[0] = make_float2(b.w.y, b.w.z);
+    }
+
+    __device__ __forceinline__ void put(uint32_t i, const Vec3& v, const Vec3& w, const Vec3& dp, const Quat& dq,
+                                        uint32_t flags) const {
+        s[kFlatBodyWords * i] = make_float4(v.x, v.y, v.z, w.x);
+        s[kFlatBodyWords * i + 1] = make_float4(w.y, w.z, dp.x, dp.y);
+        s[kFlatBodyWords * i + 2] = make_float4(dp.z, dq.x, dq.y, dq.z);
+        s[kFlatBodyWords * i + 3] = make_float4(dq.w, __uint_as_float(flags), 0.0f, 0.0f);
+    }
+
+    // Copies a body's solver fields from its record into the store.
+    __device__ void stage(uint32_t i) const {
+        const DBody& d = g[i];
+        put(i, d.v, d.w, d.dp, d.dq, d.type | (d.awake << 8));
+    }
+
+    // Writes the fields a substep changes back to the body's record.
+    __device__ void unstage(uint32_t i) const {
+        const LanedBody l = loadLaned(i);
+        DBody& d = g[i];
+        d.v = l.v;
+        d.w = l.w;
+        d.dp = l.dp;
+        d.dq = l.dq;
+    }
+
+    __device__ void integrateVelocityAt(uint32_t i, const StepParams& P) const {
+        DBody& d = g[i];
+        if (!d.alive || d.type != kDynamic || !d.awake) { return; }
+        const LanedBody l = loadLaned(i);
+        VelBody b;
+        b.alive = d.alive;
+        b.type = d.type;
+        b.awake = d.awake;
+        b.v = l.v;
+        b.w = l.w;
+        b.force = d.force;
+        b.torque = d.torque;
+        b.gravityScale = d.gravityScale;
+        b.invMass = d.invMass;
+        b.linearDamping = d.linearDamping;
+        b.angularDamping = d.angularDamping;
+        b.kept = d.kept;
+        b.linearProj = d.linearProj;
+        b.angularProj = d.angularProj;
+        b.invInertiaWorld = d.invInertiaWorld;
+        integrateVelocity(b, P);
+        storeVW(i, b);
+        d.kept = b.kept;
+    }
+
+    __device__ void integratePositionAt(uint32_t i, const StepParams& P) const {
+        DBody& d = g[i];
+        const LanedBody l = loadLaned(i);
+        PosBody b;
+        b.alive = d.alive;
+        b.type = d.type;
+        b.awake = d.awake;
+        b.v = l.v;
+        b.w = l.w;
+        b.dp = l.dp;
+        b.dq = l.dq;
+        b.com = d.com;
+        b.localCenter = d.localCenter;
+        b.qBase = d.qBase;
+        b.xf = d.xf;
+        b.kept = d.kept;
+        integratePosition(b, P);
+        put(i, b.v, b.w, b.dp, b.dq, l.type | (l.awake << 8));
+        d.com = b.com;
+        d.xf = b.xf;
+        d.kept = b.kept;
+    }
+};
+
+// One contact's passes, for either store, with body indices counted from the store's first body (`base`: the
+// same first body). A laned contact runs from its record, by slot; a contact solved on its own from the contact
+// and its stored axes. A laned contact's bodies are stored only where they move, so a static body shared by a
+// color's contacts is never written concurrently; a contact solved on its own stores both, as the reference
+// does.
+template <class Store>
+__device__ __forceinline__ void warmRowAt(const Batch& B, const Store& st, uint32_t base, uint32_t limit,
+                                          uint32_t slot) {
+    const size_t S = B.rowStride;
+    const float4* R = B.rows + slot;
+    const float4 h = R[kRowHead * S];
+    const uint32_t ia = __float_as_uint(h.x) - base, ib = __float_as_uint(h.y) - base;
+    const int n = (int)__float_as_uint(h.z);
+#if defined(TF_DEVICE_CHECKS)
+    if (!TF_OK_INDEX(B, ia < limit && ib < limit && n >= 0 && n <= 4, 10, base, ia)) { return; }
+#endif
+    if (n == 0) { return; }
+    LanedBody a = st.loadLaned(ia), b = st.loadLaned(ib);
+    warmStartRow(R, S, a, b, n);
+    if (!anchored(a)) { st.storeVW(ia, a); }
+    if (!anchored(b)) { st.storeVW(ib, b); }
+}
+
+template <class Store>
+__device__ __forceinline__ void solveRowAt(const Batch& B, const StepParams& P, const Store& st, uint32_t base,
+                                           uint32_t limit, uint32_t slot, bool bias) {
+    const size_t S = B.rowStride;
+    float4* R = B.rows + slot;
+    const float4 h = R[kRowHead * S];
+    const uint32_t ia = __float_as_uint(h.x) - base, ib = __float_as_uint(h.y) - base;
+    const int n = (int)__float_as_uint(h.z);
+#if defined(TF_DEVICE_CHECKS)
+    if (!TF_OK_INDEX(B, ia < limit && ib < limit && n >= 0 && n <= 4, 12, base, ia)) { return; }
+#endif
+    if (n == 0) { return; }
+    LanedBody a = st.loadLaned(ia), b = st.loadLaned(ib);
+    solveRow(R, S, a, b, n, P, bias);
+    if (!anchored(a)) { st.storeVW(ia, a); }
+    if (!anchored(b)) { st.storeVW(ib, b); }
+}
+
+template <class Store>
+__device__ __forceinline__ void warmOne(const Batch& B, const WorldInfo& wi, const WorldCounts& wc, const Store& st,
+                                        uint32_t ci) {
+    if (!contactOk(B, wi, wc, ci, 10)) { return; }
+    DContact& c = B.contacts[wi.contactFirst + ci];
+    const uint32_t ia = c.bodyA - wi.bodyFirst, ib = c.bodyB - wi.bodyFirst;
+    SBody a = st.load(ia), b = st.load(ib);
+    warmStartContact(a, b, c, false, B.axes + (size_t)(wi.contactFirst + ci) * kAxesPerContact);
+    st.storeVW(ia, a);
+    st.storeVW(ib, b);
+}
+
+template <class Store>
+__device__ __forceinline__ void solveOne(const Batch& B, const StepParams& P, const WorldInfo& wi, const WorldCounts& wc,
+                                         const Store& st, uint32_t ci, bool bias) {
+    if (!contactOk(B, wi, wc, ci, 12)) { return; }
+    DContact& c = B.contacts[wi.contactFirst + ci];
+    const uint32_t ia = c.bodyA - wi.bodyFirst, ib = c.bodyB - wi.bodyFirst;
+    SBody a = st.load(ia), b = st.load(ib);
+    solveContact(a, b, c, P, bias, B.axes + (size_t)(wi.contactFirst + ci) * kAxesPerContact);
+    st.storeVW(ia, a);
+    st.storeVW(ib, b);
+}
+
 // Whether the substep `sub` starts with a refresh of world wc: fast pairs are collided again at the middle
 // substep, pairs of solid bodies also at every other substep but the first (src/world.cpp:1658-1668).
 __device__ __forceinline__ bool refreshedAt(const WorldCounts& wc, int sub, int n) {
@@ -2320,8 +2511,8 @@ __global__ void __launch_bounds__(256) k_refresh_all(const __grid_constant__ Bat
 // src/joint.cpp:568-590): kind 0 scales warm starts by the speed the ends kept under the speed limits
 // (src/joint.cpp:570-593) and warm starts, 1 is the biased solve, 2 the relaxing solve with its reaction. The
 // ends' velocities come from the substep's store.
-static __device__ void runJoints(const Batch& B, const StepParams& P, const WorldInfo& wi, const SolverStore& st,
-                                       int kind) {
+template <class Store>
+__device__ void runJoints(const Batch& B, const StepParams& P, const WorldInfo& wi, const Store& st, int kind) {
     const uint32_t nj = wi.jointCount;
     DJoint* js = B.joints + wi.jointFirst;
     auto endOf = [&](uint32_t gbody) {
@@ -2420,52 +2611,10 @@ __global__ void __launch_bounds__(kMaxBlock) k_substep(const __grid_constant__ B
             }
         }
         const uint32_t base = wi.bodyFirst;
-        const Axis* axes = B.axes + (size_t)cf * kAxesPerContact;
-        // A laned contact's bodies are stored only where they move, so a static body shared by a color's
-        // contacts is never written concurrently; a contact solved on its own stores both, as the reference does.
-        // Laned contacts (planar and rolling contacts never are) run from their records, by slot; contacts solved
-        // on their own run the general forms from the contact and its stored axes.
-        const size_t S = B.rowStride;
-        auto warmRow = [&](uint32_t slot) {
-            const float4* R = B.rows + slot;
-            const float4 h = R[kRowHead * S];
-            const uint32_t ia = __float_as_uint(h.x), ib = __float_as_uint(h.y);
-            const int n = (int)__float_as_uint(h.z);
-            if (n == 0 || !rowOk(B, wi, ia, ib, n, 10)) { return; }
-            LanedBody a = st.loadLaned(ia), b = st.loadLaned(ib);
-            warmStartRow(R, S, a, b, n);
-            if (!anchored(a)) { st.storeVW(ia, a); }
-            if (!anchored(b)) { st.storeVW(ib, b); }
-        };
-        auto solveRowAt = [&](uint32_t slot, bool bias) {
-            float4* R = B.rows + slot;
-            const float4 h = R[kRowHead * S];
-            const uint32_t ia = __float_as_uint(h.x), ib = __float_as_uint(h.y);
-            const int n = (int)__float_as_uint(h.z);
-            if (n == 0 || !rowOk(B, wi, ia, ib, n, 12)) { return; }
-            LanedBody a = st.loadLaned(ia), b = st.loadLaned(ib);
-            solveRow(R, S, a, b, n, P, bias);
-            if (!anchored(a)) { st.storeVW(ia, a); }
-            if (!anchored(b)) { st.storeVW(ib, b); }
-        };
-        auto warm = [&](uint32_t ci) {
-            if (!contactOk(B, wi, wc, ci, 10)) { return; }
-            DContact& c = cs[ci];
-            const uint32_t ia = c.bodyA - base, ib = c.bodyB - base;
-            SBody a = st.load(ia), b = st.load(ib);
-            warmStartContact(a, b, c, false, axes + (size_t)ci * kAxesPerContact);
-            st.storeVW(ia, a);
-            st.storeVW(ib, b);
-        };
-        auto solve = [&](uint32_t ci, bool bias) {
-            if (!contactOk(B, wi, wc, ci, 12)) { return; }
-            DContact& c = cs[ci];
-            const uint32_t ia = c.bodyA - base, ib = c.bodyB - base;
-            SBody a = st.load(ia), b = st.load(ib);
-            solveContact(a, b, c, P, bias, axes + (size_t)ci * kAxesPerContact);
-            st.storeVW(ia, a);
-            st.storeVW(ib, b);
-        };
+        auto warmRow = [&](uint32_t slot) { warmRowAt(B, st, base, nb, slot); };
+        auto solveRowAtSlot = [&](uint32_t slot, bool bias) { solveRowAt(B, P, st, base, nb, slot, bias); };
+        auto warm = [&](uint32_t ci) { warmOne(B, wi, wc, st, ci); };
+        auto solve = [&](uint32_t ci, bool bias) { solveOne(B, P, wi, wc, st, ci, bias); };
         const uint32_t* rest = B.rest + cf;
         const uint32_t* icolored = B.impactColored + cf;
         const uint32_t* irest = B.impactRest + cf;
@@ -2480,11 +2629,11 @@ __global__ void __launch_bounds__(kMaxBlock) k_substep(const __grid_constant__ B
                     g.sync();
                 }
             }
-            forEachColorSlot(g, cf, wc.colorStart, wc.colorCount, [&](uint32_t slot) { solveRowAt(slot, bias); });
+            forEachColorSlot(g, cf, wc.colorStart, wc.colorCount, [&](uint32_t slot) { solveRowAtSlot(slot, bias); });
             forEachLevel(g, rest, B.restLevel + cf, wc.restLevels, [&](uint32_t ci) { solve(ci, bias); });
             if (wc.impactCount > 0) {
                 forEachColor(g, icolored, wc.impactColorStart, wc.impactColorCount,
-                             [&](uint32_t ci) { solveRowAt(slotOf[ci], bias); });
+                             [&](uint32_t ci) { solveRowAtSlot(slotOf[ci], bias); });
                 forEachLevel(g, irest, B.impactRestLevel + cf, wc.impactRestLevels,
                              [&](uint32_t ci) { solve(ci, bias); });
             }
@@ -2506,6 +2655,206 @@ __global__ void __launch_bounds__(kMaxBlock) k_substep(const __grid_constant__ B
             }
         }
     });
+}
+
+// ---------------------------------------------------------------------------------------------------------
+// The flat solve: one substep of every world of a batch of many small worlds as one cooperative launch.
+//
+// The world kernels above walk a world's colors with the world's own thread group, so a batch of thousands of
+// worlds runs as thousands of short dependent chains, each waiting on its own barriers. Here the barrier is the
+// grid's instead: each color's contacts of every world run at once across the device (contacts of one color
+// move no body in common, in any world), then the next color, and the body phases run over every body of the
+// batch. Contacts solved one at a time (by level), joints and a world's uncolored contacts keep their order
+// inside their world, each world's on one warp or thread. Every contact and body sees exactly the operations,
+// in the order, of the world kernel, so the results are the same bits.
+//
+// The grid barrier needs every CTA resident: the kernel is launched cooperatively, with at most as many CTAs
+// as fit at once. Its wait is bounded: a CTA that has waited kBarrierSpins polls records kDevTimeout in world
+// 0's flags and goes on (the host reports the step as failed), so a fault here cannot hang the device.
+constexpr uint32_t kBarrierSpins = 1u << 24;
+
+static __device__ void gridBarrier(const Batch& B) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t* arrive = B.work + kSlotFlatBarrier;
+        volatile uint32_t* generation = B.work + kSlotFlatBarrier + 1;
+        const uint32_t before = *generation;
+        __threadfence();
+        if (atomicAdd(arrive, 1u) == gridDim.x - 1) {
+            atomicExch(arrive, 0u);
+            __threadfence();
+            atomicAdd(const_cast<uint32_t*>(generation), 1u);
+        } else {
+            uint32_t spins = 0;
+            while (*generation == before) {
+                if (++spins > kBarrierSpins) {
+                    atomicOr(&B.counts[0].flags, kDevTimeout);
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+}
+
+// The substep `sub` of every world (src/world.cpp:1669-1680), in the world kernel's order. At the first
+// substep the step's per-color lists over all worlds are built from the worlds' color ranges.
+template <bool Joints>
+__global__ void __launch_bounds__(256, 2) k_substep_flat(const __grid_constant__ Batch B, const __grid_constant__ StepParams P,
+                                                      int sub, int serial) {
+    const bool skip = stepAborted(B, serial);  // the same for every CTA: nothing changes it during the launch
+    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, threads = gridDim.x * blockDim.x;
+    const uint32_t lane = threadIdx.x & 31, warp = tid >> 5, warps = threads >> 5;
+    const uint32_t nw = (uint32_t)B.nWorlds, nb = B.totalBodies;
+    uint32_t* colorTotal = B.work + kSlotFlatColor;
+    uint32_t* impactTotal = B.work + kSlotFlatImpact;
+    const FlatStore all{ B.flatBodies, B.bodies };
+    if (sub == 0) {
+        // Every world's share of each color list, and the most colors any world has.
+        if (!skip) {
+            for (uint32_t w = tid; w < nw; w += threads) {
+                WorldCounts& wc = B.counts[w];
+                atomicMax(B.work + kSlotFlatMaxColors, wc.colorCount);
+                atomicMax(B.work + kSlotFlatMaxImpact, wc.impactColorCount);
+                for (uint32_t k = 0; k < wc.colorCount; ++k) {
+                    const uint32_t n = wc.colorStart[k + 1] - wc.colorStart[k];
+                    wc.flatColorAt[k] = n ? atomicAdd(colorTotal + k, n) : 0u;
+                }
+                for (uint32_t k = 0; k < wc.impactColorCount; ++k) {
+                    const uint32_t n = wc.impactColorStart[k + 1] - wc.impactColorStart[k];
+                    wc.flatImpactAt[k] = n ? atomicAdd(impactTotal + k, n) : 0u;
+                }
+            }
+        }
+        gridBarrier(B);
+        // The record slots, a warp per world: color k of every world from the sum of the colors before it.
+        if (!skip) {
+            for (uint32_t w = warp; w < nw; w += warps) {
+                const WorldInfo& wi = B.info[w];
+                const WorldCounts& wc = B.counts[w];
+                const uint32_t cf = wi.contactFirst;
+                uint32_t before = 0;
+                for (uint32_t k = 0; k < wc.colorCount; ++k) {
+                    const uint32_t from = before + wc.flatColorAt[k], s0 = wc.colorStart[k], s1 = wc.colorStart[k + 1];
+                    for (uint32_t x = s0 + lane; x < s1; x += 32) { B.flatColored[from + (x - s0)] = cf + x; }
+                    before += colorTotal[k];
+                }
+                before = 0;
+                for (uint32_t k = 0; k < wc.impactColorCount; ++k) {
+                    const uint32_t from = before + wc.flatImpactAt[k], s0 = wc.impactColorStart[k];
+                    const uint32_t s1 = wc.impactColorStart[k + 1];
+                    for (uint32_t x = s0 + lane; x < s1; x += 32) {
+                        B.flatImpact[from + (x - s0)] = B.slotOf[cf + B.impactColored[cf + x]];
+                    }
+                    before += impactTotal[k];
+                }
+            }
+        }
+        gridBarrier(B);
+    }
+    const uint32_t colors = B.work[kSlotFlatMaxColors], impactColors = B.work[kSlotFlatMaxImpact];
+
+    // The body half of a refresh at this substep (planar placements kept, a new base pose), the staging, and
+    // the velocity update.
+    if (!skip) {
+        for (uint32_t gb = tid; gb < nb; gb += threads) {
+            DBody& d = B.bodies[gb];
+            const uint32_t w = d.world;
+            if (refreshedAt(B.counts[w], sub, P.substeps)) {
+                const uint32_t pb = B.info[w].planeBody;
+                if (pb != UINT32_MAX && d.posePending) {
+                    keepPose(d, placeInPlane(d, planeNormal(B.bodies[pb])));
+                    d.posePending = 0;
+                }
+                d.dp = zero3();
+                d.dq = qid();
+                d.qBase = d.xf.q;
+            }
+            all.stage(gb);
+            all.integrateVelocityAt(gb, P);
+        }
+    }
+    gridBarrier(B);
+    auto jointsPass = [&](int kind) {
+        if constexpr (Joints) {
+            if (!skip) {
+                for (uint32_t w = tid; w < nw; w += threads) {
+                    const WorldInfo& wi = B.info[w];
+                    if (wi.jointCount == 0) { continue; }
+                    runJoints(B, P, wi, FlatStore{ B.flatBodies + (size_t)kFlatBodyWords * wi.bodyFirst, B.bodies + wi.bodyFirst },
+                              kind);
+                }
+            }
+            gridBarrier(B);
+        }
+    };
+    // Each color's contacts of every world, a color at a time.
+    auto colorsPass = [&](const uint32_t* list, const uint32_t* totals, uint32_t count, auto&& f) {
+        uint32_t from = 0;
+        for (uint32_t k = 0; k < count; ++k) {
+            const uint32_t n = totals[k];
+            if (!skip) {
+                for (uint32_t i = tid; i < n; i += threads) { f(list[from + i]); }
+            }
+            from += n;
+            gridBarrier(B);
+        }
+    };
+    // A world's contacts solved on their own, level by level on one warp of the world.
+    auto restPass = [&](bool impact, auto&& f) {
+        if (!skip) {
+            const Group g = makeGroup(32);
+            for (uint32_t w = warp; w < nw; w += warps) {
+                const WorldInfo& wi = B.info[w];
+                const WorldCounts& wc = B.counts[w];
+                const uint32_t levels = impact ? wc.impactRestLevels : wc.restLevels;
+                if (levels == 0) { continue; }
+                const uint32_t cf = wi.contactFirst;
+                const FlatStore st{ B.flatBodies + (size_t)kFlatBodyWords * wi.bodyFirst, B.bodies + wi.bodyFirst };
+                forEachLevel(g, (impact ? B.impactRest : B.rest) + cf, (impact ? B.impactRestLevel : B.restLevel) + cf,
+                             levels, [&](uint32_t ci) { f(wi, wc, st, ci); });
+            }
+        }
+        gridBarrier(B);
+    };
+    const uint32_t limit = nb;
+    jointsPass(0);
+    colorsPass(B.flatColored, colorTotal, colors, [&](uint32_t slot) { warmRowAt(B, all, 0u, limit, slot); });
+    restPass(false, [&](const WorldInfo& wi, const WorldCounts& wc, const FlatStore& st, uint32_t ci) {
+        warmOne(B, wi, wc, st, ci);
+    });
+    for (int pass = 0; pass < 2; ++pass) {
+        const bool bias = pass == 0;
+        jointsPass(bias ? 1 : 2);
+        colorsPass(B.flatColored, colorTotal, colors, [&](uint32_t slot) { solveRowAt(B, P, all, 0u, limit, slot, bias); });
+        restPass(false, [&](const WorldInfo& wi, const WorldCounts& wc, const FlatStore& st, uint32_t ci) {
+            solveOne(B, P, wi, wc, st, ci, bias);
+        });
+        colorsPass(B.flatImpact, impactTotal, impactColors, [&](uint32_t slot) { solveRowAt(B, P, all, 0u, limit, slot, bias); });
+        restPass(true, [&](const WorldInfo& wi, const WorldCounts& wc, const FlatStore& st, uint32_t ci) {
+            solveOne(B, P, wi, wc, st, ci, bias);
+        });
+        if (bias) {
+            if (!skip) {
+                for (uint32_t gb = tid; gb < nb; gb += threads) { all.integratePositionAt(gb, P); }
+            }
+            gridBarrier(B);
+        }
+    }
+    // Back into the bodies' records; a world whose next substep starts with a refresh takes its inverse inertia
+    // at the new pose (src/world.cpp:1660-1662).
+    if (!skip) {
+        for (uint32_t gb = tid; gb < nb; gb += threads) {
+            all.unstage(gb);
+            DBody& d = B.bodies[gb];
+            if (sub + 1 < P.substeps && refreshedAt(B.counts[d.world], sub + 1, P.substeps) && d.alive &&
+                d.type == kDynamic && d.awake) {
+                updateInverseMass(d);
+            }
+        }
+    }
 }
 
 // ---------------------------------------------------------------------------------------------------------

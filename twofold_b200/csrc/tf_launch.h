@@ -27,6 +27,8 @@ enum KernelId : int {
     kKTapeRecord,
     kKAddForces,
     kKPackPoses,
+    kKSubstepFlat,
+    kKSubstepFlatJoints,
     kKernelIds
 };
 
@@ -36,13 +38,15 @@ const void* collideKernels(int id);  // tf_k_collide.cu: pair collisions
 const void* refreshKernels(int id);  // tf_k_refresh.cu: mid-step refreshes
 const void* solveKernels(int id);    // tf_k_solve.cu: preparation and substeps
 const void* finishKernels(int id);   // tf_k_finish.cu: end of step, tape, host-buffer helpers
+const void* flatKernels(int id);     // tf_k_flat.cu: the flat solve (its global loads bypass L1)
 
 inline const void* kernelEntry(int id) {
     if (id < kKCollideAll) { return broadKernels(id); }
     if (id < kKRefreshAll) { return collideKernels(id); }
     if (id < kKPrepare) { return refreshKernels(id); }
     if (id < kKFinish) { return solveKernels(id); }
-    return finishKernels(id);
+    if (id < kKSubstepFlat) { return finishKernels(id); }
+    return flatKernels(id);
 }
 
 }  // namespace tfb

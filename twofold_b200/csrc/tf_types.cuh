@@ -266,6 +266,10 @@ struct WorldCounts {
     uint32_t sweepMinKey, sweepMaxKey;
     uint32_t colorStart[kColors + 1];
     uint32_t impactColorStart[kColors + 1];
+    // The flat solve: where this world's contacts of each color (and impact color) start in that color's
+    // list over every world.
+    uint32_t flatColorAt[kColors];
+    uint32_t flatImpactAt[kColors];
     unsigned long long bodySteps;  // awake dynamic bodies summed over every step since the layout
 };
 

@@ -253,7 +253,9 @@ class Batch:
         Returns {kernel: (threads, big-world threshold, shared bytes)}."""
         out = np.zeros(3 * len(self.KERNELS), np.uint32)
         abi.check(self.lib.tf_world_autotune(self.h, C.c_float(dt), trial_steps, out.ctypes.data), self.lib)
-        return {k: tuple(int(x) for x in out[3 * i:3 * i + 3]) for i, k in enumerate(self.KERNELS)}
+        # A substep shape whose threshold is all ones is the flat solve, which set_launch takes as -1.
+        as_int = lambda x: -1 if int(x) == 0xFFFFFFFF else int(x)
+        return {k: tuple(as_int(x) for x in out[3 * i:3 * i + 3]) for i, k in enumerate(self.KERNELS)}
 
     # ---- differentiation ----
 
