@@ -75,6 +75,8 @@ struct Batch {
     // slots of that color's contacts in every world (color k from the batch-wide start of color k, both lists
     // totalling at most one entry per contact slot).
     float4* flatBodies;
+    float4* flatPose;    // kFlatPoseWords float4 per body
+    float4* flatMotion;  // kFlatMotionWords float4 per body
     uint32_t* flatColored;
     uint32_t* flatImpact;
     uint8_t* cflags;          // by contact: kFast, kFastSolid

@@ -83,6 +83,26 @@ TF_HD void updateInverseMass(DBody& b) {
     }
 }
 
+// The part of updateInverseMass that a new pose changes: the world inverse inertia on the free rotation axes
+// and, for a body locked to a plane, its inverse inertia about the plane normal; the projections and the world
+// inverse mass depend only on the locks and come out as they were. The same operations as updateInverseMass,
+// so the same bits. For awake dynamic bodies.
+TF_HD void updateInverseInertia(DBody& b) {
+    const Mat3 lf = toMat3(b.lockFrame);
+    Vec3 ang[3];
+    int na = 0;
+    for (int i = 0; i < 3; ++i) {
+        if (!(b.locks & (kLockRX << i))) { ang[na++] = column(lf, i); }
+    }
+    const Mat3 r = toMat3(b.xf.q);
+    const Mat3 iw = r * b.inertia * transpose(r);
+    b.invInertiaWorld = invertSubspace(iw, ang, na);
+    if (isPlanar(b)) {
+        const Vec3 n = planeNormal(b);
+        b.planeInvInertia = dot(n, b.invInertiaWorld * n);
+    }
+}
+
 // src/world.cpp:94-98.
 TF_HD bool movingAwake(const DBody& b) {
     if (b.type == kDynamic) { return b.awake != 0; }

@@ -168,7 +168,7 @@ public:
     DevArray<uint32_t> dActive, dImpact, dColored, dImpactColored, dRest, dImpactRest, dRestLevel, dImpactRestLevel;
     DevArray<uint8_t> dColor, dCflags;
     DevArray<Axis> dAxes;
-    DevArray<float4> dRows, dFlatBodies;
+    DevArray<float4> dRows, dFlatBodies, dFlatPose, dFlatMotion;
     DevArray<uint32_t> dSlotOf, dFlatColored, dFlatImpact;
     DevArray<uint64_t> dMergeKeyA, dMergeKeyB;
     DevArray<uint32_t> dMergePartA, dMergePartB, dMergeIdxA, dMergeIdxB;
@@ -1158,6 +1158,8 @@ public:
         TF_ALLOC(dRows, ncon * kRowWords);
         TF_ALLOC(dSlotOf, ncon);
         TF_ALLOC(dFlatBodies, nb * kFlatBodyWords);
+        TF_ALLOC(dFlatPose, nb * kFlatPoseWords);
+        TF_ALLOC(dFlatMotion, nb * kFlatMotionWords);
         TF_ALLOC(dFlatColored, ncon);
         TF_ALLOC(dFlatImpact, ncon);
         TF_ALLOC(dMergeKeyA, ncon);
@@ -1356,6 +1358,8 @@ public:
         B.rowStride = dContacts[0].n;
         B.slotOf = dSlotOf.ptr;
         B.flatBodies = dFlatBodies.ptr;
+        B.flatPose = dFlatPose.ptr;
+        B.flatMotion = dFlatMotion.ptr;
         B.flatColored = dFlatColored.ptr;
         B.flatImpact = dFlatImpact.ptr;
         B.mergeKeyA = dMergeKeyA.ptr;

@@ -2247,15 +2247,24 @@ __device__ __forceinline__ void rebuildSolverData(const Batch& B, const WorldInf
 }
 
 // The flat solve's store: the solver state of every body in global memory, kFlatBodyWords float4 a body
-// (velocity and spin, the substep's displacement and turn, type | awake << 8), small enough that a batch's
-// bodies stay in L2 while its contacts are solved, indexed from a first body (a world's, or 0 for global
-// indices). The same methods as SolverStore's, over that array.
+// (velocity and spin, the substep's displacement and turn, type | awake << 8 | alive << 16), small enough that
+// a batch's bodies stay in L2 while its contacts are solved, indexed from a first body (a world's, or 0 for
+// global indices). The same loads and stores as SolverStore's, over that array. For whole-batch views it also
+// holds each body's pose (kFlatPoseWords) and the step's velocity-update terms (kFlatMotionWords), so that the
+// body phases of a substep read a few coalesced words instead of the body's whole record.
 constexpr int kFlatBodyWords = 4;
+constexpr int kFlatPoseWords = 5;    // com; xf.p; xf.q; qBase; localCenter
+constexpr int kFlatMotionWords = 7;  // gravity-and-force term, linear damping factor; torque term, angular
+                                     // damping factor; linear then angular projection (18 floats, 2 unused)
 
 struct FlatStore {
     float4* s;
     DBody* g;
+    float4* pose = nullptr;
+    float4* motion = nullptr;
     static constexpr bool staged = true;
+
+    __device__ __forceinline__ uint32_t flags(uint32_t i) const { return __float_as_uint(s[kFlatBodyWords * i + 3].y); }
 
     __device__ __forceinline__ LanedBody loadLaned(uint32_t i) const {
         const float4 a = s[kFlatBodyWords * i], b = s[kFlatBodyWords * i + 1], c = s[kFlatBodyWords * i + 2],
@@ -2267,7 +2276,7 @@ struct FlatStore {
         x.dq = { c.y, c.z, c.w, d.x };
         const uint32_t f = __float_as_uint(d.y);
         x.type = f & 0xffu;
-        x.awake = f >> 8;
+        x.awake = (f >> 8) & 0xffu;
         return x;
     }
 
@@ -2293,77 +2302,120 @@ struct FlatStore {
     }
 
     __device__ __forceinline__ void put(uint32_t i, const Vec3& v, const Vec3& w, const Vec3& dp, const Quat& dq,
-                                        uint32_t flags) const {
+                                        uint32_t f) const {
         s[kFlatBodyWords * i] = make_float4(v.x, v.y, v.z, w.x);
         s[kFlatBodyWords * i + 1] = make_float4(w.y, w.z, dp.x, dp.y);
         s[kFlatBodyWords * i + 2] = make_float4(dp.z, dq.x, dq.y, dq.z);
-        s[kFlatBodyWords * i + 3] = make_float4(dq.w, __uint_as_float(flags), 0.0f, 0.0f);
-    }
-
-    // Copies a body's solver fields from its record into the store.
-    __device__ void stage(uint32_t i) const {
-        const DBody& d = g[i];
-        put(i, d.v, d.w, d.dp, d.dq, d.type | (d.awake << 8));
-    }
-
-    // Writes the fields a substep changes back to the body's record.
-    __device__ void unstage(uint32_t i) const {
-        const LanedBody l = loadLaned(i);
-        DBody& d = g[i];
-        d.v = l.v;
-        d.w = l.w;
-        d.dp = l.dp;
-        d.dq = l.dq;
-    }
-
-    __device__ void integrateVelocityAt(uint32_t i, const StepParams& P) const {
-        DBody& d = g[i];
-        if (!d.alive || d.type != kDynamic || !d.awake) { return; }
-        const LanedBody l = loadLaned(i);
-        VelBody b;
-        b.alive = d.alive;
-        b.type = d.type;
-        b.awake = d.awake;
-        b.v = l.v;
-        b.w = l.w;
-        b.force = d.force;
-        b.torque = d.torque;
-        b.gravityScale = d.gravityScale;
-        b.invMass = d.invMass;
-        b.linearDamping = d.linearDamping;
-        b.angularDamping = d.angularDamping;
-        b.kept = d.kept;
-        b.linearProj = d.linearProj;
-        b.angularProj = d.angularProj;
-        b.invInertiaWorld = d.invInertiaWorld;
-        integrateVelocity(b, P);
-        storeVW(i, b);
-        d.kept = b.kept;
-    }
-
-    __device__ void integratePositionAt(uint32_t i, const StepParams& P) const {
-        DBody& d = g[i];
-        const LanedBody l = loadLaned(i);
-        PosBody b;
-        b.alive = d.alive;
-        b.type = d.type;
-        b.awake = d.awake;
-        b.v = l.v;
-        b.w = l.w;
-        b.dp = l.dp;
-        b.dq = l.dq;
-        b.com = d.com;
-        b.localCenter = d.localCenter;
-        b.qBase = d.qBase;
-        b.xf = d.xf;
-        b.kept = d.kept;
-        integratePosition(b, P);
-        put(i, b.v, b.w, b.dp, b.dq, l.type | (l.awake << 8));
-        d.com = b.com;
-        d.xf = b.xf;
-        d.kept = b.kept;
+        s[kFlatBodyWords * i + 3] = make_float4(dq.w, __uint_as_float(f), 0.0f, 0.0f);
     }
 };
+
+__device__ __forceinline__ float4 q4(const Quat& q) { return make_float4(q.x, q.y, q.z, q.w); }
+__device__ __forceinline__ Quat quatOf(const float4& v) { return Quat{ v.x, v.y, v.z, v.w }; }
+
+// integrateVelocity's terms that stay fixed over a step (gravity and force, the damping factors, the
+// projections) and the torque term, which changes only with the world inverse inertia. Stored as the very
+// values integrateVelocity forms from them (src/world.cpp:1141-1151), so adding them gives its bits.
+__device__ __forceinline__ void storeTorqueTerm(const FlatStore& f, uint32_t i, const DBody& d, const StepParams& P) {
+    float4* m = f.motion + (size_t)kFlatMotionWords * i;
+    const Vec3 t = d.invInertiaWorld * d.torque * P.h;
+    m[1] = make_float4(t.x, t.y, t.z, m[1].w);
+}
+
+__device__ __forceinline__ void storeMotion(const FlatStore& f, uint32_t i, const DBody& d, const StepParams& P) {
+    float4* m = f.motion + (size_t)kFlatMotionWords * i;
+    const float h = P.h;
+    const Vec3 gv = (P.gravity * d.gravityScale + d.force * d.invMass) * h;
+    const Vec3 t = d.invInertiaWorld * d.torque * h;
+    m[0] = f4(gv, 1.0f / (1.0f + h * d.linearDamping));
+    m[1] = f4(t, 1.0f / (1.0f + h * d.angularDamping));
+    const Mat3& L = d.linearProj;
+    const Mat3& A = d.angularProj;
+    m[2] = make_float4(L.r[0].x, L.r[0].y, L.r[0].z, L.r[1].x);
+    m[3] = make_float4(L.r[1].y, L.r[1].z, L.r[2].x, L.r[2].y);
+    m[4] = make_float4(L.r[2].z, A.r[0].x, A.r[0].y, A.r[0].z);
+    m[5] = make_float4(A.r[1].x, A.r[1].y, A.r[1].z, A.r[2].x);
+    m[6] = make_float4(A.r[2].y, A.r[2].z, 0.0f, 0.0f);
+}
+
+// The first substep's staging: the body's solver state, pose and velocity terms from its record.
+static __device__ void flatBegin(const FlatStore& f, uint32_t i, const StepParams& P) {
+    const DBody& d = f.g[i];
+    f.put(i, d.v, d.w, d.dp, d.dq, d.type | (d.awake << 8) | (d.alive << 16));
+    float4* q = f.pose + (size_t)kFlatPoseWords * i;
+    q[0] = f4(d.com, 0.0f);
+    q[1] = f4(d.xf.p, 0.0f);
+    q[2] = q4(d.xf.q);
+    q[3] = q4(d.qBase);
+    q[4] = f4(d.localCenter, 0.0f);
+    if (d.alive && d.type == kDynamic && d.awake) { storeMotion(f, i, d, P); }
+}
+
+// What limitSpeed reads and writes.
+struct SpeedBody {
+    Vec3 v, w;
+    float kept;
+    uint32_t type, awake;
+};
+
+// integrateVelocity from the store and the step's terms: the same operations on the same values.
+static __device__ void flatVelocity(const FlatStore& f, uint32_t i, const StepParams& P) {
+    const uint32_t fl = f.flags(i);
+    const uint32_t type = fl & 0xffu, awake = (fl >> 8) & 0xffu, alive = fl >> 16;
+    if (!alive || type != kDynamic || !awake) { return; }
+    const LanedBody l = f.loadLaned(i);
+    const float4* m = f.motion + (size_t)kFlatMotionWords * i;
+    const float4 m0 = m[0], m1 = m[1], a = m[2], b = m[3], c = m[4], d = m[5], e = m[6];
+    Mat3 L, A;
+    L.r[0] = { a.x, a.y, a.z };
+    L.r[1] = { a.w, b.x, b.y };
+    L.r[2] = { b.z, b.w, c.x };
+    A.r[0] = { c.y, c.z, c.w };
+    A.r[1] = { d.x, d.y, d.z };
+    A.r[2] = { d.w, e.x, e.y };
+    SpeedBody s;
+    s.type = type;
+    s.awake = awake;
+    s.kept = f.g[i].kept;
+    s.v = l.v + xyz(m0);
+    s.v = L * (s.v * m0.w);
+    s.w = l.w + xyz(m1);
+    s.w = A * (s.w * m1.w);
+    limitSpeed(s, P.maxLinearSpeed, P.maxAngularSpeed);
+    f.storeVW(i, s);
+    f.g[i].kept = s.kept;
+}
+
+// integratePosition from the store and the pose: the new pose goes to the store and to the body's record (joints
+// of the relaxing pass read it there).
+static __device__ void flatPosition(const FlatStore& f, uint32_t i, const StepParams& P) {
+    const uint32_t fl = f.flags(i);
+    const LanedBody l = f.loadLaned(i);
+    float4* q = f.pose + (size_t)kFlatPoseWords * i;
+    DBody& d = f.g[i];
+    PosBody b;
+    b.alive = fl >> 16;
+    b.type = l.type;
+    b.awake = l.awake;
+    b.v = l.v;
+    b.w = l.w;
+    b.dp = l.dp;
+    b.dq = l.dq;
+    b.com = xyz(q[0]);
+    b.xf.p = xyz(q[1]);
+    b.xf.q = quatOf(q[2]);
+    b.qBase = quatOf(q[3]);
+    b.localCenter = xyz(q[4]);
+    b.kept = d.kept;
+    integratePosition(b, P);
+    f.put(i, b.v, b.w, b.dp, b.dq, fl);
+    q[0] = f4(b.com, 0.0f);
+    q[1] = f4(b.xf.p, 0.0f);
+    q[2] = q4(b.xf.q);
+    d.com = b.com;
+    d.xf = b.xf;
+    d.kept = b.kept;
+}
 
 // One contact's passes, for either store, with body indices counted from the store's first body (`base`: the
 // same first body). A laned contact runs from its record, by slot; a contact solved on its own from the contact
@@ -2710,7 +2762,7 @@ __global__ void __launch_bounds__(256, 2) k_substep_flat(const __grid_constant__
     const uint32_t nw = (uint32_t)B.nWorlds, nb = B.totalBodies;
     uint32_t* colorTotal = B.work + kSlotFlatColor;
     uint32_t* impactTotal = B.work + kSlotFlatImpact;
-    const FlatStore all{ B.flatBodies, B.bodies };
+    const FlatStore all{ B.flatBodies, B.bodies, B.flatPose, B.flatMotion };
     if (sub == 0) {
         // Every world's share of each color list, and the most colors any world has.
         if (!skip) {
@@ -2756,24 +2808,29 @@ __global__ void __launch_bounds__(256, 2) k_substep_flat(const __grid_constant__
     }
     const uint32_t colors = B.work[kSlotFlatMaxColors], impactColors = B.work[kSlotFlatMaxImpact];
 
-    // The body half of a refresh at this substep (planar placements kept, a new base pose), the staging, and
-    // the velocity update.
+    // At the first substep every body's state, pose and velocity terms are staged; at a later one, the body half
+    // of a refresh (planar placements kept, a new base pose) for the worlds refreshed there. Then the velocity
+    // update.
     if (!skip) {
         for (uint32_t gb = tid; gb < nb; gb += threads) {
-            DBody& d = B.bodies[gb];
-            const uint32_t w = d.world;
-            if (refreshedAt(B.counts[w], sub, P.substeps)) {
-                const uint32_t pb = B.info[w].planeBody;
-                if (pb != UINT32_MAX && d.posePending) {
-                    keepPose(d, placeInPlane(d, planeNormal(B.bodies[pb])));
-                    d.posePending = 0;
+            if (sub == 0) {
+                flatBegin(all, gb, P);
+            } else {
+                DBody& d = B.bodies[gb];
+                const uint32_t w = d.world;
+                if (refreshedAt(B.counts[w], sub, P.substeps)) {
+                    const uint32_t pb = B.info[w].planeBody;
+                    if (pb != UINT32_MAX && d.posePending) {
+                        keepPose(d, placeInPlane(d, planeNormal(B.bodies[pb])));
+                        d.posePending = 0;
+                    }
+                    const LanedBody l = all.loadLaned(gb);
+                    all.put(gb, l.v, l.w, zero3(), qid(), all.flags(gb));
+                    float4* q = B.flatPose + (size_t)kFlatPoseWords * gb;
+                    q[3] = q[2];
                 }
-                d.dp = zero3();
-                d.dq = qid();
-                d.qBase = d.xf.q;
             }
-            all.stage(gb);
-            all.integrateVelocityAt(gb, P);
+            flatVelocity(all, gb, P);
         }
     }
     gridBarrier(B);
@@ -2838,20 +2895,26 @@ __global__ void __launch_bounds__(256, 2) k_substep_flat(const __grid_constant__
         });
         if (bias) {
             if (!skip) {
-                for (uint32_t gb = tid; gb < nb; gb += threads) { all.integratePositionAt(gb, P); }
+                for (uint32_t gb = tid; gb < nb; gb += threads) { flatPosition(all, gb, P); }
             }
             gridBarrier(B);
         }
     }
-    // Back into the bodies' records; a world whose next substep starts with a refresh takes its inverse inertia
-    // at the new pose (src/world.cpp:1660-1662).
+    // Back into the bodies' records (the pose is there already); a world whose next substep starts with a refresh
+    // takes its inverse inertia at the new pose (src/world.cpp:1660-1662), and the torque term with it.
     if (!skip) {
         for (uint32_t gb = tid; gb < nb; gb += threads) {
-            all.unstage(gb);
+            const LanedBody l = all.loadLaned(gb);
             DBody& d = B.bodies[gb];
+            d.v = l.v;
+            d.w = l.w;
+            d.dp = l.dp;
+            d.dq = l.dq;
+            d.qBase = quatOf(B.flatPose[(size_t)kFlatPoseWords * gb + 3]);
             if (sub + 1 < P.substeps && refreshedAt(B.counts[d.world], sub + 1, P.substeps) && d.alive &&
                 d.type == kDynamic && d.awake) {
-                updateInverseMass(d);
+                updateInverseInertia(d);
+                storeTorqueTerm(all, gb, d, P);
             }
         }
     }
