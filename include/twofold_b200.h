@@ -327,8 +327,53 @@ TF_API int tf_world_device_status(void* world, uint32_t* flags);
 /* Body state of world w: position, rotation (x,y,z,w), linear and angular velocity. */
 TF_API int tf_body_get_state(void* world, int32_t w, tf_id body, float position[3], float rotation[4],
                              float linear_velocity[3], float angular_velocity[3]);
+/* World::setLinearVelocity, setAngularVelocity (include/twofold/world.h:412-413): either pointer may be null;
+ * each given velocity is projected on the free axes and wakes the body's island. */
 TF_API int tf_body_set_velocity(void* world, int32_t w, tf_id body, const float linear_velocity[3],
                                 const float angular_velocity[3]);
+
+/* ---- Calls between steps (include/twofold/world.h:375-463) ----
+ *
+ * Each changes world w as the reference's World call of the same name does, before the next step: contacts the
+ * change removes are dropped by that step (pairs that touched and whose shapes go away end now, their contact
+ * event reported first among the next step's events), and the bodies the reference wakes are woken, through
+ * contacts with points and unbroken joints. An invalid id does nothing, as in the reference. */
+/* World::destroyBody (world.h:382): its shapes, contacts and joints go with it; the slot is reused. */
+TF_API int tf_body_destroy(void* world, int32_t w, tf_id body);
+/* World::removeShape (world.h:387): the shape's contacts go, the body's mass is recomputed and it wakes. */
+TF_API int tf_shape_remove(void* world, int32_t w, tf_id shape);
+/* World::setFriction, setRestitution, setRollingResistance (world.h:397-399). */
+TF_API int tf_shape_set_friction(void* world, int32_t w, tf_id shape, float friction);
+TF_API int tf_shape_set_restitution(void* world, int32_t w, tf_id shape, float restitution);
+TF_API int tf_shape_set_rolling_resistance(void* world, int32_t w, tf_id shape, float rolling_resistance);
+/* World::setFilter (world.h:400): the shape's contacts are dropped (not ended) and their bodies woken. */
+TF_API int tf_shape_set_filter(void* world, int32_t w, tf_id shape, uint32_t category, uint32_t mask);
+/* World::setTransform (world.h:408): position and rotation (x, y, z, w); wakes what it touches. */
+TF_API int tf_body_set_transform(void* world, int32_t w, tf_id body, const float position[3], const float rotation[4]);
+/* World::setKinematicTarget (world.h:415): velocities that carry a kinematic body to the pose over dt. */
+TF_API int tf_body_set_kinematic_target(void* world, int32_t w, tf_id body, const float position[3],
+                                        const float rotation[4], float dt);
+/* World::setMotionType (world.h:418): TF_STATIC, TF_KINEMATIC or TF_DYNAMIC. A body with a mesh or half-space
+ * shape cannot become dynamic (TF_E_UNSUPPORTED), as those shapes belong to static and kinematic bodies. */
+TF_API int tf_body_set_motion_type(void* world, int32_t w, tf_id body, int32_t type);
+/* World::addForce / addForceAtPoint (world.h:421-422; point may be null), addTorque (:423), addImpulse /
+ * addImpulseAtPoint (:424-425): dynamic bodies only; wake as the reference's wake argument; a sleeping body
+ * takes nothing. */
+TF_API int tf_body_add_force(void* world, int32_t w, tf_id body, const float force[3], const float* point, int32_t wake);
+TF_API int tf_body_add_torque(void* world, int32_t w, tf_id body, const float torque[3], int32_t wake);
+TF_API int tf_body_add_impulse(void* world, int32_t w, tf_id body, const float impulse[3], const float* point,
+                               int32_t wake);
+/* World::setDamping (world.h:455), setGravityScale (:457). */
+TF_API int tf_body_set_damping(void* world, int32_t w, tf_id body, float linear, float angular);
+TF_API int tf_body_set_gravity_scale(void* world, int32_t w, tf_id body, float scale);
+/* World::wake, sleep (world.h:460-461), setCanSleep (:463; false wakes the body). */
+TF_API int tf_body_wake(void* world, int32_t w, tf_id body);
+TF_API int tf_body_sleep(void* world, int32_t w, tf_id body);
+TF_API int tf_body_set_can_sleep(void* world, int32_t w, tf_id body, int32_t can_sleep);
+/* World::setFrictionMix, setRestitutionMix (world.h:375-376): `which` 0 friction, 1 restitution. Mixing is done
+ * on the device, where a host function cannot run: mix 0 (the reference's default, geometric mean for friction
+ * and maximum for restitution) is accepted and any other mix is refused with TF_E_UNSUPPORTED. */
+TF_API int tf_world_set_mix(void* world, int32_t which, int32_t mix);
 /* Mass, local center and local inertia (row-major 3x3) as World::massProperties returns them. */
 TF_API int tf_body_get_mass(void* world, int32_t w, tf_id body, float* mass, float center[3], float inertia[9]);
 TF_API int tf_body_is_awake(void* world, int32_t w, tf_id body, int32_t* awake);

@@ -249,6 +249,38 @@ TF_API int ref_body_set_velocity(void* h, tf_id body, const float* v, const floa
     return 0;
 }
 
+// The World calls between steps through the public API; `what` numbers them as twofold_b200.world.CALLS does.
+TF_API int ref_world_call(void* h, int what, tf_id id, const float* v, uint32_t a, uint32_t b) {
+    World& w = *W(h);
+    const BodyId body{ id.index, id.generation };
+    const ShapeId shape{ id.index, id.generation };
+    switch (what) {
+        case 0: w.destroyBody(body); break;
+        case 1: w.removeShape(shape); break;
+        case 2: w.setFriction(shape, v[0]); break;
+        case 3: w.setRestitution(shape, v[0]); break;
+        case 4: w.setRollingResistance(shape, v[0]); break;
+        case 5: w.setFilter(shape, a, b); break;
+        case 6: w.setTransform(body, v3(v), Quat(v[3], v[4], v[5], v[6])); break;
+        case 7: w.setKinematicTarget(body, v3(v), Quat(v[3], v[4], v[5], v[6]), v[7]); break;
+        case 8: w.setMotionType(body, (MotionType)a); break;
+        case 9: w.addForce(body, v3(v), a != 0); break;
+        case 10: w.addForceAtPoint(body, v3(v), v3(v + 3), a != 0); break;
+        case 11: w.addTorque(body, v3(v), a != 0); break;
+        case 12: w.addImpulse(body, v3(v), a != 0); break;
+        case 13: w.addImpulseAtPoint(body, v3(v), v3(v + 3), a != 0); break;
+        case 14: w.setDamping(body, v[0], v[1]); break;
+        case 15: w.setGravityScale(body, v[0]); break;
+        case 16: w.wake(body); break;
+        case 17: w.sleep(body); break;
+        case 18: w.setCanSleep(body, a != 0); break;
+        case 19: w.setLinearVelocity(body, v3(v)); break;
+        case 20: w.setAngularVelocity(body, v3(v)); break;
+        default: return -1;
+    }
+    return 0;
+}
+
 TF_API int ref_body_get_mass(void* h, tf_id body, float* mass, float* center, float* inertia) {
     const MassProperties m = W(h)->massProperties({ body.index, body.generation });
     *mass = m.mass;

@@ -48,6 +48,7 @@ def load(path=REF_LIB):
             "ref_joint_create": ([P, C.POINTER(abi.tf_joint_desc), C.POINTER(abi.tf_id)], C.c_int),
             "ref_joint_info": ([P, abi.tf_id, C.POINTER(abi.tf_joint_info)], C.c_int),
             "ref_joint_set": ([P, abi.tf_id, C.c_int, P], C.c_int),
+            "ref_world_call": ([P, C.c_int, abi.tf_id, P, C.c_uint32, C.c_uint32], C.c_int),
             "ref_broken_joints": ([P, P, C.c_int, C.POINTER(C.c_int)], C.c_int),
             "ref_world_contact_events": ([P, C.POINTER(abi.tf_contact_event), C.c_int, C.POINTER(C.c_int)], C.c_int),
             "ref_world_hit_events": ([P, C.POINTER(abi.tf_hit_event), C.c_int, C.POINTER(C.c_int)], C.c_int),
@@ -162,6 +163,14 @@ class RefWorld:
         kinds = ("limits", "motor", "spring", "friction", "swing", "break", "destroy")
         v = (C.c_float * 3)(*(list(values) + [0.0] * (3 - len(values))))
         self.lib.ref_joint_set(self.h, joint, kinds.index(what), v)
+
+    def call(self, what, target, values=(), a=0, b=0):
+        """A World call between steps (twofold_b200.world.CALLS names them) on a body or shape id."""
+        from twofold_b200.world import CALLS
+
+        v = (C.c_float * 8)(*(list(values) + [0.0] * (8 - len(values))))
+        if self.lib.ref_world_call(self.h, CALLS.index(what), target, v, a, b) != 0:
+            raise ValueError(f"unknown call {what}")
 
     def joint_info(self, joint):
         info = abi.tf_joint_info()

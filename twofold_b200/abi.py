@@ -310,6 +310,24 @@ def _declare(lib):
         "tf_world_set_settings": ([P, C.POINTER(tf_settings)], C.c_int),
         "tf_mesh_create": ([P, P, C.c_int32, P, C.c_int32, C.POINTER(C.c_int32)], C.c_int),
         "tf_mesh_read": ([P, C.c_int32, P, P, P, P, P, P, P], C.c_int),
+        "tf_body_destroy": ([P, C.c_int32, tf_id], C.c_int),
+        "tf_shape_remove": ([P, C.c_int32, tf_id], C.c_int),
+        "tf_shape_set_friction": ([P, C.c_int32, tf_id, C.c_float], C.c_int),
+        "tf_shape_set_restitution": ([P, C.c_int32, tf_id, C.c_float], C.c_int),
+        "tf_shape_set_rolling_resistance": ([P, C.c_int32, tf_id, C.c_float], C.c_int),
+        "tf_shape_set_filter": ([P, C.c_int32, tf_id, C.c_uint32, C.c_uint32], C.c_int),
+        "tf_body_set_transform": ([P, C.c_int32, tf_id, P, P], C.c_int),
+        "tf_body_set_kinematic_target": ([P, C.c_int32, tf_id, P, P, C.c_float], C.c_int),
+        "tf_body_set_motion_type": ([P, C.c_int32, tf_id, C.c_int32], C.c_int),
+        "tf_body_add_force": ([P, C.c_int32, tf_id, P, P, C.c_int32], C.c_int),
+        "tf_body_add_torque": ([P, C.c_int32, tf_id, P, C.c_int32], C.c_int),
+        "tf_body_add_impulse": ([P, C.c_int32, tf_id, P, P, C.c_int32], C.c_int),
+        "tf_body_set_damping": ([P, C.c_int32, tf_id, C.c_float, C.c_float], C.c_int),
+        "tf_body_set_gravity_scale": ([P, C.c_int32, tf_id, C.c_float], C.c_int),
+        "tf_body_wake": ([P, C.c_int32, tf_id], C.c_int),
+        "tf_body_sleep": ([P, C.c_int32, tf_id], C.c_int),
+        "tf_body_set_can_sleep": ([P, C.c_int32, tf_id, C.c_int32], C.c_int),
+        "tf_world_set_mix": ([P, C.c_int32, C.c_int32], C.c_int),
         "tf_hull_compute": ([P, C.c_int32, C.c_int32, P, P, C.c_int32, P, C.c_int32], C.c_int),
         "tf_body_create": ([P, C.c_int32, C.POINTER(tf_body_desc), C.POINTER(tf_id)], C.c_int),
         "tf_shape_add": ([P, C.c_int32, tf_id, C.POINTER(tf_shape_desc), C.POINTER(tf_id)], C.c_int),
@@ -374,7 +392,11 @@ def _declare(lib):
 # Every symbol include/twofold_b200.h declares.
 EXPORTED = [
     "tf_abi_version", "tf_last_error", "tf_default_settings", "tf_world_create", "tf_world_destroy",
-    "tf_world_count", "tf_world_set_settings", "tf_mesh_create", "tf_mesh_read", "tf_hull_compute", "tf_body_create", "tf_shape_add",
+    "tf_world_count", "tf_world_set_settings", "tf_mesh_create", "tf_mesh_read", "tf_hull_compute", "tf_body_destroy", "tf_shape_remove",
+    "tf_shape_set_friction", "tf_shape_set_restitution", "tf_shape_set_rolling_resistance", "tf_shape_set_filter",
+    "tf_body_set_transform", "tf_body_set_kinematic_target", "tf_body_set_motion_type", "tf_body_add_force",
+    "tf_body_add_torque", "tf_body_add_impulse", "tf_body_set_damping", "tf_body_set_gravity_scale", "tf_body_wake",
+    "tf_body_sleep", "tf_body_set_can_sleep", "tf_world_set_mix", "tf_body_create", "tf_shape_add",
     "tf_bodies_create",
     "tf_shapes_add", "tf_joint_create", "tf_joint_get_info", "tf_world_broken_joints", "tf_joint_set_limits", "tf_joint_set_motor",
     "tf_joint_set_spring", "tf_joint_set_friction", "tf_joint_set_swing", "tf_joint_set_break_limits", "tf_joint_destroy", "tf_world_step", "tf_world_step_graph", "tf_world_synchronize", "tf_world_device_status",

@@ -65,6 +65,9 @@ struct HostWorld {
     std::vector<uint32_t> freeShapes;
     std::vector<uint32_t> planes;  // half-space shapes in the order they were tracked
     std::vector<DContact> contacts;  // last pulled from the device (world-local indices)
+    // Contact events that calls between steps queued (pairs ended by removing their shapes or joining their
+    // bodies), reported first among the next step's events; and those the last step started with.
+    std::vector<tf_contact_event> queued, stepQueued;
 };
 
 // One device allocation per array; sized at layout time.
@@ -609,12 +612,478 @@ public:
         return TF_OK;
     }
 
+
+    // The reference's Tolerances for the current settings (src/world.cpp:222-229).
+    Tolerances tolerances() const {
+        Tolerances t;
+        t.linearSlop = 0.005f * settings.length_unit;
+        t.speculative = 4.0f * t.linearSlop;
+        return t;
+    }
+
+    // twofold::angularVelocity (include/twofold/math.h:217-224): the spin that turns a into b over dt.
+    static Vec3 angularVelocityBetween(const Quat& a, const Quat& b, float dt) {
+        Quat d = normalize(b * conjugate(a));
+        if (d.w < 0) { d = Quat{ -d.x, -d.y, -d.z, -d.w }; }
+        const Vec3 v{ d.x, d.y, d.z };
+        const float s = length(v);
+        if (s < 1e-7f || dt <= 0) { return zero3(); }
+        const float angle = 2.0f * std::atan2(s, d.w);
+        return v * (angle / (s * dt));
+    }
+
+    // ---- World calls between steps (src/world.cpp:1743-2210), on the host mirrors ----
+    //
+    // Every such call brings the device's state into the mirrors, changes them as the reference's call changes
+    // its world, and marks what the next step must send back. The reference's helpers they use are restated
+    // below on the mirrors: the links between bodies (contacts with points, unbroken joints), the wake flood,
+    // and the marking of contacts for the next step to drop.
+
+    // Impl::Link (src/world.cpp:650-678): a body's contact pairs (once per key) and joints, in that order.
+    struct Link {
+        uint64_t key;
+        uint32_t other;
+        uint32_t joint;  // UINT32_MAX for a contact pair
+    };
+
+    static std::vector<std::vector<Link>> linksOf(const HostWorld& W) {
+        std::vector<std::vector<Link>> links(W.bodies.size());
+        for (size_t ci = 0; ci < W.contacts.size(); ++ci) {
+            const DContact& c = W.contacts[ci];
+            if (ci > 0 && W.contacts[ci - 1].key == c.key) { continue; }
+            links[c.bodyA].push_back({ c.key, c.bodyB, UINT32_MAX });
+            links[c.bodyB].push_back({ c.key, c.bodyA, UINT32_MAX });
+        }
+        for (uint32_t ji = 0; ji < W.joints.size(); ++ji) {
+            const DJoint& j = W.joints[ji].d;
+            if (!j.alive || j.bodyA == kWorldEnd) { continue; }
+            links[j.bodyA].push_back({ 0, j.bodyB, ji });
+            links[j.bodyB].push_back({ 0, j.bodyA, ji });
+        }
+        return links;
+    }
+
+    // The first contact of a pair in the mirrors' (key, part) order, or the end.
+    static size_t firstOf(const HostWorld& W, uint64_t key) {
+        return (size_t)(std::lower_bound(W.contacts.begin(), W.contacts.end(), key,
+                                         [](const DContact& x, uint64_t k) { return x.key < k; }) -
+                        W.contacts.begin());
+    }
+
+    // Impl::linked (src/world.cpp:681-689): a joint while unbroken, a contact pair while one of its contacts has
+    // points.
+    static bool linked(const HostWorld& W, const Link& l) {
+        if (l.joint != UINT32_MAX) { return W.joints[l.joint].d.alive && !W.joints[l.joint].d.broken; }
+        for (size_t ci = firstOf(W, l.key); ci < W.contacts.size() && W.contacts[ci].key == l.key; ++ci) {
+            if (W.contacts[ci].count > 0) { return true; }
+        }
+        return false;
+    }
+
+    static void pushLinked(const HostWorld& W, const std::vector<std::vector<Link>>& links, uint32_t i,
+                           std::vector<uint32_t>& stack) {
+        for (const Link& l : links[i]) {
+            const DBody& o = W.bodies[l.other].d;
+            if (o.type == kDynamic && !o.awake && linked(W, l)) { stack.push_back(l.other); }
+        }
+    }
+
+    // Impl::meshTouches (src/world.cpp:552-563): whether a triangle of the mesh shape lies in the box, the box
+    // taken into the mesh's frame as boundsInMesh does (src/mesh.cpp).
+    bool meshTouches(const HostShape& s, const Transform& xm, const Vec3& lo, const Vec3& hi) const {
+        if (s.d.mesh < 0 || (size_t)s.d.mesh >= meshes.size()) { return false; }
+        const HostMesh& m = meshes[(size_t)s.d.mesh];
+        if (m.nodes.empty()) { return false; }
+        const Vec3 c = applyInverse(xm, (lo + hi) * 0.5f);
+        const Vec3 e = (hi - lo) * 0.5f;
+        const Mat3 r = toMat3(conjugate(xm.q));
+        Vec3 reach;
+        for (int i = 0; i < 3; ++i) {
+            setComp(reach, i, std::fabs(r.r[i].x) * e.x + std::fabs(r.r[i].y) * e.y + std::fabs(r.r[i].z) * e.z);
+        }
+        const Vec3 mlo = c - reach, mhi = c + reach;
+        for (size_t t = 0; t < m.normals.size(); ++t) {
+            Vec3 k[3];
+            m.corners((int)t, k);
+            if (boxesOverlap(minVec(minVec(k[0], k[1]), k[2]), maxVec(maxVec(k[0], k[1]), k[2]), mlo, mhi)) { return true; }
+        }
+        return false;
+    }
+
+    // Impl::pushOverlapping (src/world.cpp:620-647): sleeping dynamic bodies whose shapes an anchor's shapes
+    // reach, per anchor shape in order, each shape's finds sorted and unique. The reference finds candidates in
+    // its tree, whose fat leaves hold every shape the exact test below passes; here every shape is tested.
+    void pushOverlapping(const HostWorld& W, uint32_t anchor, std::vector<uint32_t>& stack) const {
+        const float g = tolerances().speculative;
+        const Vec3 grow{ g, g, g };
+        const HostBody& A = W.bodies[anchor];
+        std::vector<uint32_t> found;
+        for (uint32_t ai : A.shapes) {
+            const HostShape& sa = W.shapes[ai];
+            if (sa.d.sensor) { continue; }
+            const Transform xa = A.d.xf * sa.d.local;
+            const Vec3 n = rotate(xa.q, Vec3{ 0, 0, 1 });
+            found.clear();
+            for (const HostShape& sb : W.shapes) {
+                if (!sb.d.alive || sb.d.sensor) { continue; }
+                const DBody& b = W.bodies[sb.d.body].d;
+                if (!b.alive || b.type != kDynamic || b.awake) { continue; }
+                if (!(sa.d.category & sb.d.mask) || !(sb.d.category & sa.d.mask)) { continue; }
+                const Vec3 blo = sb.d.lo - grow, bhi = sb.d.hi + grow;
+                if (!boxesOverlap(sa.d.lo, sa.d.hi, blo, bhi)) { continue; }
+                if (sa.d.kind == kHalfSpace) {
+                    const Vec3 c = (blo + bhi) * 0.5f, e = (bhi - blo) * 0.5f;
+                    const float reach = e.x * std::fabs(n.x) + e.y * std::fabs(n.y) + e.z * std::fabs(n.z);
+                    if (dot(c - xa.p, n) > reach) { continue; }
+                }
+                if (sa.d.kind == kMesh && !meshTouches(sa, xa, blo, bhi)) { continue; }
+                found.push_back(sb.d.body);
+            }
+            std::sort(found.begin(), found.end());
+            found.erase(std::unique(found.begin(), found.end()), found.end());
+            stack.insert(stack.end(), found.begin(), found.end());
+        }
+    }
+
+    // Impl::wakeBodies (src/world.cpp:705-735): a sleeping dynamic start wakes its island through contacts with
+    // points and unbroken joints; a static or kinematic start wakes the dynamic bodies touching or overlapping
+    // it, without spreading past them.
+    void wakeBodies(HostWorld& W, const std::vector<uint32_t>& start) {
+        std::vector<uint32_t> stack;
+        bool anchors = false;
+        for (uint32_t i : start) {
+            const DBody& b = W.bodies[i].d;
+            if (!b.alive) { continue; }
+            if (b.type != kDynamic) {
+                anchors = true;
+            } else if (!b.awake) {
+                stack.push_back(i);
+            }
+        }
+        if (stack.empty() && !anchors) { return; }
+        const std::vector<std::vector<Link>> links = linksOf(W);
+        for (uint32_t i : start) {
+            if (!W.bodies[i].d.alive || W.bodies[i].d.type == kDynamic) { continue; }
+            pushLinked(W, links, i, stack);
+            pushOverlapping(W, i, stack);
+        }
+        while (!stack.empty()) {
+            const uint32_t i = stack.back();
+            stack.pop_back();
+            DBody& b = W.bodies[i].d;
+            if (b.awake) { continue; }
+            b.awake = 1;
+            b.sleepTime = 0.0f;
+            updateInverseMass(b);
+            pushLinked(W, links, i, stack);
+        }
+    }
+
+    tf_contact_event endEvent(const HostWorld& W, const DContact& c) const {
+        tf_contact_event e{};
+        e.shape_a = c.shapeA;
+        e.shape_b = c.shapeB;
+        e.body_a = c.bodyA;
+        e.body_b = c.bodyB;
+        e.begin = 0;
+        return e;
+    }
+
+    // Impl::dropContacts (src/world.cpp:565-593): marks the body's contact pairs that pick accepts as removed
+    // (no points, not reusable) for the next step to drop, and returns the dynamic bodies on their other side.
+    // When their shapes are going away (`ending`), pairs that touched end now, their event queued.
+    template <class Pick>
+    std::vector<uint32_t> dropContacts(HostWorld& W, uint32_t body, bool ending, Pick&& pick) {
+        std::vector<uint32_t> touched;
+        const std::vector<std::vector<Link>> links = linksOf(W);
+        for (const Link& l : links[body]) {
+            if (l.joint != UINT32_MAX || !pick(l)) { continue; }
+            bool hit = false;
+            size_t ci = firstOf(W, l.key);
+            if (ending && ci < W.contacts.size() && W.contacts[ci].key == l.key && (W.contacts[ci].flags & kCTouched)) {
+                W.queued.push_back(endEvent(W, W.contacts[ci]));
+            }
+            for (; ci < W.contacts.size() && W.contacts[ci].key == l.key; ++ci) {
+                DContact& c = W.contacts[ci];
+                if (ending) { c.flags &= ~kCTouched; }
+                if (c.flags & kCRemoved) { continue; }
+                c.flags |= kCRemoved;
+                c.flags &= ~kCReusable;
+                c.count = 0;
+                hit = true;
+            }
+            if (hit && W.bodies[l.other].d.type == kDynamic) { touched.push_back(l.other); }
+        }
+        return touched;
+    }
+
+    // Impl::removeContacts (src/world.cpp:595-600): a body's pairs, or one shape's.
+    void removeContacts(HostWorld& W, uint32_t body, int shape, bool ending) {
+        wakeBodies(W, dropContacts(W, body, ending, [&](const Link& l) {
+            return shape < 0 || (uint32_t)(l.key >> 32) == (uint32_t)shape || (uint32_t)l.key == (uint32_t)shape;
+        }));
+    }
+
+    HostShape* shapeRef(int w, tf_id id) {
+        if (w < 0 || w >= (int)worlds.size()) { return nullptr; }
+        HostWorld& W = worlds[(size_t)w];
+        if (id.index >= W.shapes.size()) { return nullptr; }
+        HostShape& s = W.shapes[id.index];
+        return (s.d.alive && s.generation == id.generation) ? &s : nullptr;
+    }
+
+    // The other calls' common start: the device's state in the mirrors, and the body named (nullptr for an
+    // invalid handle, which the reference's setters take as a no-op).
+    int hostBody(int w, tf_id id, HostBody** out) {
+        *out = nullptr;
+        const int rc = pull();
+        if (rc != TF_OK) { return rc; }
+        *out = body(w, id);
+        return TF_OK;
+    }
+
+    // World::destroyBody (src/world.cpp:1784-1808).
+    int destroyBody(int w, tf_id id) {
+        HostBody* hb = nullptr;
+        int rc = hostBody(w, id, &hb);
+        if (rc != TF_OK || !hb) { return rc; }
+        HostWorld& W = worlds[(size_t)w];
+        const uint32_t bi = id.index;
+        removeContacts(W, bi, -1, true);
+        for (uint32_t ji = 0; ji < W.joints.size(); ++ji) {
+            const DJoint& j = W.joints[ji].d;
+            if (j.alive && (j.bodyA == bi || j.bodyB == bi)) { killJoint(W, ji); }
+        }
+        for (uint32_t si : W.bodies[bi].shapes) {
+            HostShape& s = W.shapes[si];
+            untrack(W, si);
+            s.d.alive = 0;
+            ++s.generation;
+            W.freeShapes.push_back(si);
+        }
+        HostBody& b = W.bodies[bi];
+        b.shapes.clear();
+        b.d.alive = 0;
+        b.d.hasBounds = 0;
+        ++b.generation;
+        W.freeBodies.push_back(bi);
+        layoutDirty = true;
+        return TF_OK;
+    }
+
+    static void untrack(HostWorld& W, uint32_t si) {
+        if (W.shapes[si].d.kind == kHalfSpace) { W.planes.erase(std::remove(W.planes.begin(), W.planes.end(), si), W.planes.end()); }
+    }
+
+    // Impl::destroyJoint (src/world.cpp:399-406): the joint's dynamic ends woken, its slot freed.
+    void killJoint(HostWorld& W, uint32_t ji) {
+        HostJoint& hj = W.joints[ji];
+        wakeJoint(W, hj.d);
+        hj.d.alive = 0;
+        hj.d.brokeNow = 0;
+        ++hj.generation;
+        W.freeJoints.push_back(ji);
+        layoutDirty = true;
+    }
+
+    // Impl::wakeJoint (src/world.cpp:391-397).
+    void wakeJoint(HostWorld& W, const DJoint& j) {
+        std::vector<uint32_t> start;
+        for (uint32_t i : { j.bodyA, j.bodyB }) {
+            if (i != kWorldEnd && W.bodies[i].d.type == kDynamic) { start.push_back(i); }
+        }
+        wakeBodies(W, start);
+    }
+
+    // World::removeShape (src/world.cpp:1859-1876).
+    int removeShape(int w, tf_id id) {
+        const int rc = pull();
+        if (rc != TF_OK) { return rc; }
+        HostShape* s = shapeRef(w, id);
+        if (!s) { return TF_OK; }
+        HostWorld& W = worlds[(size_t)w];
+        const uint32_t bi = s->d.body;
+        removeContacts(W, bi, (int)id.index, true);
+        HostBody& b = W.bodies[bi];
+        b.shapes.erase(std::remove(b.shapes.begin(), b.shapes.end(), id.index), b.shapes.end());
+        untrack(W, id.index);
+        s->d.alive = 0;
+        ++s->generation;
+        W.freeShapes.push_back(id.index);
+        bound(W, b);
+        updateMass(W, b);
+        wakeBodies(W, { bi });
+        layoutDirty = true;
+        return TF_OK;
+    }
+
+    // World::setFriction, setRestitution, setRollingResistance (src/world.cpp:1958-1968) and setFilter
+    // (:1970-1978), which drops the shape's contact pairs without ending them.
+    int setShapeValue(int w, tf_id id, int what, float value, uint32_t category, uint32_t mask) {
+        const int rc = pull();
+        if (rc != TF_OK) { return rc; }
+        HostShape* s = shapeRef(w, id);
+        if (!s) { return TF_OK; }
+        switch (what) {
+            case 0: s->d.friction = value; break;
+            case 1: s->d.restitution = value; break;
+            case 2: s->d.rollingResistance = value; break;
+            case 3:
+                s->d.category = category;
+                s->d.mask = mask;
+                removeContacts(worlds[(size_t)w], s->d.body, (int)id.index, false);
+                break;
+            default: return fail(TF_E_INVALID, "shape setter: unknown value");
+        }
+        layoutDirty = true;
+        return TF_OK;
+    }
+
+    // World::setTransform (src/world.cpp:1993-2003): the pose, its bounds, and the bodies it wakes.
+    int setTransform(int w, tf_id id, const Vec3& p, const Quat& q) {
+        HostBody* hb = nullptr;
+        int rc = hostBody(w, id, &hb);
+        if (rc != TF_OK || !hb) { return rc; }
+        HostWorld& W = worlds[(size_t)w];
+        DBody& b = hb->d;
+        b.xf = { p, normalize(q) };
+        b.com = apply(b.xf, b.localCenter);
+        b.hasTarget = 0;
+        bound(W, *hb);
+        wakeBodies(W, { id.index });
+        layoutDirty = true;
+        return TF_OK;
+    }
+
+    // World::setKinematicTarget (src/world.cpp:2031-2040).
+    int setKinematicTarget(int w, tf_id id, const Vec3& p, const Quat& rotation, float dt) {
+        HostBody* hb = nullptr;
+        int rc = hostBody(w, id, &hb);
+        if (rc != TF_OK || !hb || hb->d.type != kKinematic || !(dt > 0.0f)) { return rc; }
+        DBody& b = hb->d;
+        const Quat q = normalize(rotation);
+        const Vec3 com = p + rotate(q, b.localCenter);
+        b.v = (com - b.com) / dt;
+        b.w = angularVelocityBetween(b.xf.q, q, dt);
+        b.target = { p, q };
+        b.hasTarget = 1;
+        bodiesDirty = true;
+        return TF_OK;
+    }
+
+    // World::setMotionType (src/world.cpp:2047-2062).
+    int setMotionType(int w, tf_id id, int type) {
+        if (type < 0 || type > 2) { return fail(TF_E_INVALID, "setMotionType: bad motion type"); }
+        HostBody* hb = nullptr;
+        int rc = hostBody(w, id, &hb);
+        if (rc != TF_OK || !hb || (int)hb->d.type == type) { return rc; }
+        HostWorld& W = worlds[(size_t)w];
+        if (type == kDynamic) {
+            for (uint32_t si : hb->shapes) {
+                if (W.shapes[si].d.kind == kMesh || W.shapes[si].d.kind == kHalfSpace) {
+                    return fail(TF_E_UNSUPPORTED, "setMotionType: meshes and half-spaces belong to bodies that are not dynamic");
+                }
+            }
+        }
+        DBody& b = hb->d;
+        b.type = (uint32_t)type;
+        b.hasTarget = 0;
+        if (type == kStatic) {
+            b.v = zero3();
+            b.w = zero3();
+        }
+        if (type == kDynamic) { b.awake = 1; }
+        if (type != kDynamic) {
+            // Impl::removeAnchoredContacts (src/world.cpp:602-605).
+            dropContacts(W, id.index, false, [&](const Link& l) { return W.bodies[l.other].d.type != kDynamic; });
+        }
+        updateMass(W, *hb);
+        wakeBodies(W, { id.index });
+        layoutDirty = true;
+        return TF_OK;
+    }
+
+    // World::addForce, addForceAtPoint, addTorque, addImpulse, addImpulseAtPoint (src/world.cpp:2064-2112):
+    // dynamic bodies, woken first when asked; a body still asleep takes nothing.
+    int push(int w, tf_id id, int what, const Vec3& v, const Vec3* point, bool wake) {
+        HostBody* hb = nullptr;
+        int rc = hostBody(w, id, &hb);
+        if (rc != TF_OK || !hb || hb->d.type != kDynamic) { return rc; }
+        if (wake) { wakeBodies(worlds[(size_t)w], { id.index }); }
+        DBody& b = hb->d;
+        if (!b.awake) {
+            bodiesDirty = true;
+            return TF_OK;
+        }
+        switch (what) {
+            case 0:
+                b.force += v;
+                if (point) { b.torque += cross(*point - b.com, v); }
+                break;
+            case 1: b.torque += v; break;
+            case 2:
+                b.v += b.invMassWorld * v;
+                if (point) { b.w += b.invInertiaWorld * cross(*point - b.com, v); }
+                break;
+            default: return fail(TF_E_INVALID, "push: unknown kind");
+        }
+        bodiesDirty = true;
+        return TF_OK;
+    }
+
+    // World::setLinearVelocity, setAngularVelocity (src/world.cpp:2015-2029): projected on the free axes, and
+    // the body woken.
+    int setVelocity(int w, tf_id id, const float* v, const float* av) {
+        HostBody* hb = nullptr;
+        int rc = hostBody(w, id, &hb);
+        if (rc != TF_OK || !hb || hb->d.type == kStatic) { return rc; }
+        if (v) {
+            hb->d.v = hb->d.linearProj * v3of(v);
+            wakeBodies(worlds[(size_t)w], { id.index });
+        }
+        if (av) {
+            hb->d.w = hb->d.angularProj * v3of(av);
+            wakeBodies(worlds[(size_t)w], { id.index });
+        }
+        bodiesDirty = true;
+        return TF_OK;
+    }
+
+    // World::setDamping, setGravityScale, setCanSleep, wake, sleep (src/world.cpp:2163-2207).
+    int setBodyValue(int w, tf_id id, int what, float a, float b) {
+        HostBody* hb = nullptr;
+        int rc = hostBody(w, id, &hb);
+        if (rc != TF_OK || !hb) { return rc; }
+        HostWorld& W = worlds[(size_t)w];
+        DBody& d = hb->d;
+        switch (what) {
+            case 0:
+                d.linearDamping = a;
+                d.angularDamping = b;
+                break;
+            case 1: d.gravityScale = a; break;
+            case 2:
+                d.canSleep = a != 0.0f ? 1u : 0u;
+                if (!d.canSleep) { wakeBodies(W, { id.index }); }
+                break;
+            case 3: wakeBodies(W, { id.index }); break;
+            case 4:
+                if (d.type != kDynamic) { return TF_OK; }
+                d.awake = 0;
+                d.v = zero3();
+                d.w = zero3();
+                d.sleepTime = 0.0f;
+                updateInverseMass(d);
+                break;
+            default: return fail(TF_E_INVALID, "body setter: unknown value");
+        }
+        bodiesDirty = true;
+        return TF_OK;
+    }
+
     // ---- layout and transfer ----
 
-    // Brings the device's dynamic state and contacts back into the host mirrors.
     // World::createJoint (src/world.cpp:2221-2333): the joint's frames in each body at their current poses.
-    // Two parts of the reference's behaviour have no counterpart here and are refused: joining bodies whose
-    // contacts the joint would remove (their pair already touches), and waking a sleeping end from the host.
     int createJoint(int w, const tf_joint_desc* d, tf_id* out) {
         if (w < 0 || w >= (int)worlds.size() || !d) { return fail(TF_E_INVALID, "createJoint: bad world or desc"); }
         if (d->type < TF_JOINT_POINT || d->type > TF_JOINT_SWING_TWIST) { return fail(TF_E_INVALID, "createJoint: bad type"); }
@@ -631,18 +1100,6 @@ public:
             ai = d->body_a.index;
         }
         const uint32_t bi = d->body_b.index;
-        if (!d->collide_connected && ai != kWorldEnd) {
-            for (const DContact& c : W.contacts) {
-                if ((c.bodyA == ai && c.bodyB == bi) || (c.bodyA == bi && c.bodyB == ai)) {
-                    return fail(TF_E_UNSUPPORTED, "createJoint: the bodies already have contacts, which this build does not remove");
-                }
-            }
-        }
-        for (uint32_t e : { ai, bi }) {
-            if (e != kWorldEnd && W.bodies[e].d.type == kDynamic && !W.bodies[e].d.awake) {
-                return fail(TF_E_UNSUPPORTED, "createJoint: waking a sleeping body from the host is not run by this build");
-            }
-        }
         HostJoint hj;
         DJoint& j = hj.d;
         j.alive = 1;
@@ -731,14 +1188,29 @@ public:
         } else {
             W.joints.push_back(hj);
         }
+        // The joined bodies' contacts go, touching pairs ending now (src/world.cpp:2317-2327); the joint's
+        // dynamic ends wake.
+        if (!d->collide_connected && ai != kWorldEnd) {
+            auto between = [&](const DContact& c) {
+                return (c.bodyA == ai && c.bodyB == bi) || (c.bodyA == bi && c.bodyB == ai);
+            };
+            for (size_t ci = 0; ci < W.contacts.size(); ++ci) {
+                const DContact& c = W.contacts[ci];
+                if ((c.flags & kCTouched) && between(c) && (ci == 0 || W.contacts[ci - 1].key != c.key)) {
+                    W.queued.push_back(endEvent(W, c));
+                }
+            }
+            W.contacts.erase(std::remove_if(W.contacts.begin(), W.contacts.end(), between), W.contacts.end());
+        }
+        wakeJoint(W, W.joints[index].d);
         layoutDirty = true;
         if (out) { *out = { index, hj.generation }; }
         return TF_OK;
     }
 
     // The joint's host record for a change through the API, or null for an invalid id (the reference's
-    // setters then do nothing). The change wakes the joint's dynamic ends in the reference (src/world.cpp:390-397);
-    // a sleeping end is refused here, as waking a body from the host is not run by this build.
+    // setters then do nothing). Changes other than the break limits wake the joint's dynamic ends after they
+    // are made (src/world.cpp:2341-2397).
     int jointForChange(int w, tf_id id, bool wakes, HostJoint** out) {
         *out = nullptr;
         if (w < 0 || w >= (int)worlds.size()) { return fail(TF_E_INVALID, "joint: bad world"); }
@@ -749,13 +1221,7 @@ public:
             return TF_OK;
         }
         HostJoint& j = W.joints[id.index];
-        if (wakes) {
-            for (uint32_t e : { j.d.bodyA, j.d.bodyB }) {
-                if (e != kWorldEnd && W.bodies[e].d.type == kDynamic && !W.bodies[e].d.awake) {
-                    return fail(TF_E_UNSUPPORTED, "joint: waking a sleeping body from the host is not run by this build");
-                }
-            }
-        }
+        (void)wakes;
         *out = &j;
         return TF_OK;
     }
@@ -802,6 +1268,7 @@ public:
             default:
                 return fail(TF_E_INVALID, "joint: unknown change");
         }
+        if (what != 5) { wakeJoint(worlds[(size_t)w], j); }
         layoutDirty = true;
         return TF_OK;
     }
@@ -810,11 +1277,7 @@ public:
         HostJoint* hj = nullptr;
         const int rc = jointForChange(w, id, true, &hj);
         if (rc != TF_OK || !hj) { return rc; }
-        hj->d.alive = 0;
-        hj->d.brokeNow = 0;
-        ++hj->generation;
-        worlds[(size_t)w].freeJoints.push_back(id.index);
-        layoutDirty = true;
+        killJoint(worlds[(size_t)w], id.index);
         return TF_OK;
     }
 
@@ -1976,6 +2439,16 @@ public:
         return layout();
     }
 
+    // The events that calls since the last step queued belong to the next step; after a call of several steps
+    // the last one's events are read, which had none.
+    void takeQueuedEvents(int nSteps) {
+        for (HostWorld& W : worlds) {
+            W.stepQueued.clear();
+            if (nSteps == 1) { W.stepQueued.swap(W.queued); }
+            W.queued.clear();
+        }
+    }
+
     int step(float dt, int nSteps) {
         if (!(dt > 0.0f) || !std::isfinite(dt) || nSteps <= 0) { return TF_OK; }
         TF_CUDA(cudaSetDevice(device));
@@ -2372,11 +2845,13 @@ TF_API int tf_shapes_add(void* h, int32_t n, const int32_t* world_of, const uint
 
 TF_API int tf_world_step(void* h, float dt, int32_t n) {
     if (!h) { return tfb::fail(TF_E_INVALID, "tf_world_step: null world"); }
+    if (dt > 0.0f && std::isfinite(dt) && n > 0) { E(h)->takeQueuedEvents(n); }
     return E(h)->step(dt, n);
 }
 
 TF_API int tf_world_step_graph(void* h, float dt, int32_t n) {
     if (!h) { return tfb::fail(TF_E_INVALID, "tf_world_step_graph: null world"); }
+    if (dt > 0.0f && std::isfinite(dt) && n > 0) { E(h)->takeQueuedEvents(n); }
     return E(h)->stepGraph(dt, n);
 }
 
@@ -2410,17 +2885,101 @@ TF_API int tf_body_get_state(void* h, int32_t w, tf_id id, float p[3], float q[4
 
 TF_API int tf_body_set_velocity(void* h, int32_t w, tf_id id, const float v[3], const float av[3]) {
     if (!h) { return tfb::fail(TF_E_INVALID, "tf_body_set_velocity: null world"); }
-    Engine* e = E(h);
-    int rc = e->pull();
-    if (rc != TF_OK) { return rc; }
-    tfb::HostBody* b = e->body(w, id);
-    if (!b || b->d.type == tfb::kStatic) { return TF_OK; }
-    if (b->d.type == tfb::kDynamic && !b->d.awake) {
-        return tfb::fail(TF_E_UNSUPPORTED, "tf_body_set_velocity: waking a sleeping body from the host is not run by this build");
+    return E(h)->setVelocity(w, id, v, av);
+}
+
+TF_API int tf_body_destroy(void* h, int32_t w, tf_id id) {
+    if (!h) { return tfb::fail(TF_E_INVALID, "tf_body_destroy: null world"); }
+    return E(h)->destroyBody(w, id);
+}
+
+TF_API int tf_shape_remove(void* h, int32_t w, tf_id id) {
+    if (!h) { return tfb::fail(TF_E_INVALID, "tf_shape_remove: null world"); }
+    return E(h)->removeShape(w, id);
+}
+
+TF_API int tf_shape_set_friction(void* h, int32_t w, tf_id id, float v) {
+    if (!h) { return tfb::fail(TF_E_INVALID, "tf_shape_set_friction: null world"); }
+    return E(h)->setShapeValue(w, id, 0, v, 0, 0);
+}
+
+TF_API int tf_shape_set_restitution(void* h, int32_t w, tf_id id, float v) {
+    if (!h) { return tfb::fail(TF_E_INVALID, "tf_shape_set_restitution: null world"); }
+    return E(h)->setShapeValue(w, id, 1, v, 0, 0);
+}
+
+TF_API int tf_shape_set_rolling_resistance(void* h, int32_t w, tf_id id, float v) {
+    if (!h) { return tfb::fail(TF_E_INVALID, "tf_shape_set_rolling_resistance: null world"); }
+    return E(h)->setShapeValue(w, id, 2, v, 0, 0);
+}
+
+TF_API int tf_shape_set_filter(void* h, int32_t w, tf_id id, uint32_t category, uint32_t mask) {
+    if (!h) { return tfb::fail(TF_E_INVALID, "tf_shape_set_filter: null world"); }
+    return E(h)->setShapeValue(w, id, 3, 0.0f, category, mask);
+}
+
+TF_API int tf_body_set_transform(void* h, int32_t w, tf_id id, const float p[3], const float q[4]) {
+    if (!h || !p || !q) { return tfb::fail(TF_E_INVALID, "tf_body_set_transform: null"); }
+    return E(h)->setTransform(w, id, tfb::v3of(p), tfb::q4of(q));
+}
+
+TF_API int tf_body_set_kinematic_target(void* h, int32_t w, tf_id id, const float p[3], const float q[4], float dt) {
+    if (!h || !p || !q) { return tfb::fail(TF_E_INVALID, "tf_body_set_kinematic_target: null"); }
+    return E(h)->setKinematicTarget(w, id, tfb::v3of(p), tfb::q4of(q), dt);
+}
+
+TF_API int tf_body_set_motion_type(void* h, int32_t w, tf_id id, int32_t type) {
+    if (!h) { return tfb::fail(TF_E_INVALID, "tf_body_set_motion_type: null world"); }
+    return E(h)->setMotionType(w, id, type);
+}
+
+TF_API int tf_body_add_force(void* h, int32_t w, tf_id id, const float f[3], const float* point, int32_t wake) {
+    if (!h || !f) { return tfb::fail(TF_E_INVALID, "tf_body_add_force: null"); }
+    const tfb::Vec3 at = point ? tfb::v3of(point) : tfb::zero3();
+    return E(h)->push(w, id, 0, tfb::v3of(f), point ? &at : nullptr, wake != 0);
+}
+
+TF_API int tf_body_add_torque(void* h, int32_t w, tf_id id, const float t[3], int32_t wake) {
+    if (!h || !t) { return tfb::fail(TF_E_INVALID, "tf_body_add_torque: null"); }
+    return E(h)->push(w, id, 1, tfb::v3of(t), nullptr, wake != 0);
+}
+
+TF_API int tf_body_add_impulse(void* h, int32_t w, tf_id id, const float j[3], const float* point, int32_t wake) {
+    if (!h || !j) { return tfb::fail(TF_E_INVALID, "tf_body_add_impulse: null"); }
+    const tfb::Vec3 at = point ? tfb::v3of(point) : tfb::zero3();
+    return E(h)->push(w, id, 2, tfb::v3of(j), point ? &at : nullptr, wake != 0);
+}
+
+TF_API int tf_body_set_damping(void* h, int32_t w, tf_id id, float linear, float angular) {
+    if (!h) { return tfb::fail(TF_E_INVALID, "tf_body_set_damping: null world"); }
+    return E(h)->setBodyValue(w, id, 0, linear, angular);
+}
+
+TF_API int tf_body_set_gravity_scale(void* h, int32_t w, tf_id id, float scale) {
+    if (!h) { return tfb::fail(TF_E_INVALID, "tf_body_set_gravity_scale: null world"); }
+    return E(h)->setBodyValue(w, id, 1, scale, 0.0f);
+}
+
+TF_API int tf_body_set_can_sleep(void* h, int32_t w, tf_id id, int32_t can_sleep) {
+    if (!h) { return tfb::fail(TF_E_INVALID, "tf_body_set_can_sleep: null world"); }
+    return E(h)->setBodyValue(w, id, 2, can_sleep ? 1.0f : 0.0f, 0.0f);
+}
+
+TF_API int tf_body_wake(void* h, int32_t w, tf_id id) {
+    if (!h) { return tfb::fail(TF_E_INVALID, "tf_body_wake: null world"); }
+    return E(h)->setBodyValue(w, id, 3, 0.0f, 0.0f);
+}
+
+TF_API int tf_body_sleep(void* h, int32_t w, tf_id id) {
+    if (!h) { return tfb::fail(TF_E_INVALID, "tf_body_sleep: null world"); }
+    return E(h)->setBodyValue(w, id, 4, 0.0f, 0.0f);
+}
+
+TF_API int tf_world_set_mix(void* h, int32_t which, int32_t mix) {
+    if (!h || which < 0 || which > 1) { return tfb::fail(TF_E_INVALID, "tf_world_set_mix: bad arguments"); }
+    if (mix != 0) {
+        return tfb::fail(TF_E_UNSUPPORTED, "tf_world_set_mix: only the default mixes run on the device");
     }
-    if (v) { b->d.v = b->d.linearProj * tfb::Vec3{ v[0], v[1], v[2] }; }
-    if (av) { b->d.w = b->d.angularProj * tfb::Vec3{ av[0], av[1], av[2] }; }
-    e->bodiesDirty = true;
     return TF_OK;
 }
 
@@ -2545,12 +3104,15 @@ TF_API int tf_world_contact_events(void* h, int32_t w, tf_contact_event* out, in
     const int rc = e->events((size_t)w, &ev, nullptr);
     if (rc != TF_OK) { return rc; }
     const tfb::HostWorld& W = e->worlds[(size_t)w];
-    for (size_t i = 0; out && i < ev.size() && (int32_t)i < cap; ++i) {
-        tf_contact_event& o = out[i];
+    // Events queued by calls before the step come first, as the reference reports them (src/world.cpp:1570).
+    const size_t q = W.stepQueued.size();
+    for (size_t i = 0; out && i < q && (int32_t)i < cap; ++i) { out[i] = W.stepQueued[i]; }
+    for (size_t i = 0; out && i < ev.size() && (int32_t)(q + i) < cap; ++i) {
+        tf_contact_event& o = out[q + i];
         pairOf(W, ev[i].key, &o.shape_a, &o.shape_b, &o.body_a, &o.body_b);
         o.begin = (int32_t)ev[i].begin;
     }
-    *count = (int32_t)ev.size();
+    *count = (int32_t)(q + ev.size());
     return TF_OK;
 }
 

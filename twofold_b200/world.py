@@ -9,6 +9,13 @@ import numpy as np
 from . import abi
 
 
+# The World calls between steps, by name (include/twofold/world.h:375-463), in the order the oracle's harness
+# numbers them.
+CALLS = ("destroy_body", "remove_shape", "friction", "restitution", "rolling_resistance", "filter", "transform",
+         "kinematic_target", "motion_type", "force", "force_at", "torque", "impulse", "impulse_at", "damping",
+         "gravity_scale", "wake", "sleep", "can_sleep", "velocity", "spin")
+
+
 class Batch:
     """One tf_world handle holding len(worlds) independent worlds on one CUDA device."""
 
@@ -240,6 +247,39 @@ class Batch:
         which a world gets the whole CTA, and the CTA's staging bytes."""
         k = -1 if kernel is None else (self.KERNELS.index(kernel) if isinstance(kernel, str) else int(kernel))
         abi.check(self.lib.tf_world_set_launch(self.h, k, int(threads), int(big_bodies), int(smem_bytes)), self.lib)
+
+    def call(self, wi, what, target, values=(), a=0, b=0):
+        """A World call between steps on world wi (CALLS names them): target is a body or shape id (tf_id), values
+        the call's floats (position then rotation x, y, z, w then dt; force then point; ...), a and b its
+        integers (category and mask, motion type, wake)."""
+        L, h = self.lib, self.h
+        f = (C.c_float * 8)(*(list(values) + [0.0] * (8 - len(values))))
+        P = C.c_void_p(C.addressof(f))
+        at = C.c_void_p(C.addressof(f) + 12)  # values[3:]: a rotation, or a point
+        rc = {
+            "destroy_body": lambda: L.tf_body_destroy(h, wi, target),
+            "remove_shape": lambda: L.tf_shape_remove(h, wi, target),
+            "friction": lambda: L.tf_shape_set_friction(h, wi, target, f[0]),
+            "restitution": lambda: L.tf_shape_set_restitution(h, wi, target, f[0]),
+            "rolling_resistance": lambda: L.tf_shape_set_rolling_resistance(h, wi, target, f[0]),
+            "filter": lambda: L.tf_shape_set_filter(h, wi, target, a, b),
+            "transform": lambda: L.tf_body_set_transform(h, wi, target, P, at),
+            "kinematic_target": lambda: L.tf_body_set_kinematic_target(h, wi, target, P, at, f[7]),
+            "motion_type": lambda: L.tf_body_set_motion_type(h, wi, target, a),
+            "force": lambda: L.tf_body_add_force(h, wi, target, P, None, a),
+            "force_at": lambda: L.tf_body_add_force(h, wi, target, P, at, a),
+            "torque": lambda: L.tf_body_add_torque(h, wi, target, P, a),
+            "impulse": lambda: L.tf_body_add_impulse(h, wi, target, P, None, a),
+            "impulse_at": lambda: L.tf_body_add_impulse(h, wi, target, P, at, a),
+            "damping": lambda: L.tf_body_set_damping(h, wi, target, f[0], f[1]),
+            "gravity_scale": lambda: L.tf_body_set_gravity_scale(h, wi, target, f[0]),
+            "wake": lambda: L.tf_body_wake(h, wi, target),
+            "sleep": lambda: L.tf_body_sleep(h, wi, target),
+            "can_sleep": lambda: L.tf_body_set_can_sleep(h, wi, target, a),
+            "velocity": lambda: L.tf_body_set_velocity(h, wi, target, P, None),
+            "spin": lambda: L.tf_body_set_velocity(h, wi, target, None, P),
+        }[what]()
+        abi.check(rc, L)
 
     def save_state(self, slot=0):
         """Snapshot of the batch's dynamic state on the device."""
