@@ -229,6 +229,16 @@ struct WorldSettings {
     bool continuous = true;
 };
 
+// WorldSettings-side material mixing (include/twofold/world.h:243-248). Mixing runs on the device, where a host
+// function cannot be called: only the reference's default mixes run, and a World given any other function
+// records TF_E_UNSUPPORTED (status()).
+struct MaterialInput {
+    float value;
+    MotionType type;
+};
+
+using MixFunction = float (*)(const MaterialInput& a, const MaterialInput& b);
+
 struct ContactInfo {
     BodyId bodyA;
     BodyId bodyB;
@@ -394,9 +404,8 @@ public:
             shapes_ = std::move(o.shapes_);
             meshIds_ = std::move(o.meshIds_);
             meshes_ = std::move(o.meshes_);
-            forces_ = std::move(o.forces_);
-            torques_ = std::move(o.torques_);
-            forcesPending_ = o.forcesPending_;
+            shapeOwner_ = std::move(o.shapeOwner_);
+            jointEnds_ = std::move(o.jointEnds_);
             status_ = o.status_;
         }
         return *this;
@@ -416,12 +425,6 @@ public:
 
     void step(float dt) {
         if (!(dt > 0.0f) || !std::isfinite(dt) || !handle_) { return; }
-        if (forcesPending_) {
-            note(tf_world_add_forces(handle_, forces_.data(), torques_.data()));
-            std::fill(forces_.begin(), forces_.end(), 0.0f);
-            std::fill(torques_.begin(), torques_.end(), 0.0f);
-            forcesPending_ = false;
-        }
         if (!note(tf_world_step(handle_, dt, 1))) { return; }
         tf_profile p{};
         if (note(tf_world_profile(handle_, 0, &p))) {
@@ -460,8 +463,6 @@ public:
         if (!note(tf_body_create(handle_, 0, &c, &id))) { return {}; }
         if (id.index >= bodies_.size()) { bodies_.resize(id.index + 1, BodyId{}); }
         bodies_[id.index] = BodyId{ id.index, id.generation };
-        forces_.resize(3 * bodies_.size(), 0.0f);
-        torques_.resize(3 * bodies_.size(), 0.0f);
         return bodies_[id.index];
     }
 
@@ -521,9 +522,103 @@ public:
         c.sensor = d.sensor ? 1 : 0;
         tf_id id{ UINT32_MAX, 0 };
         if (!note(tf_shape_add(handle_, 0, tf_id{ body.index, body.generation }, &c, &id))) { return {}; }
-        if (id.index >= shapes_.size()) { shapes_.resize(id.index + 1, ShapeId{}); }
+        if (id.index >= shapes_.size()) {
+            shapes_.resize(id.index + 1, ShapeId{});
+            shapeOwner_.resize(id.index + 1, UINT32_MAX);
+        }
         shapes_[id.index] = ShapeId{ id.index, id.generation };
+        shapeOwner_[id.index] = body.index;
         return shapes_[id.index];
+    }
+
+    // ---- Calls between steps (include/twofold/world.h:375-463) ----
+
+    void setFrictionMix(MixFunction mix) { note(tf_world_set_mix(handle_, 0, mix ? 1 : 0)); }
+    void setRestitutionMix(MixFunction mix) { note(tf_world_set_mix(handle_, 1, mix ? 1 : 0)); }
+
+    void destroyBody(BodyId body) {
+        if (!isValid(body) || !note(tf_body_destroy(handle_, 0, cid(body)))) { return; }
+        bodies_[body.index] = BodyId{ UINT32_MAX, body.generation + 1 };
+        for (size_t i = 0; i < shapes_.size(); ++i) {
+            if (shapeOwner_[i] == body.index && shapes_[i].index != UINT32_MAX) {
+                shapes_[i] = ShapeId{ UINT32_MAX, shapes_[i].generation + 1 };
+            }
+        }
+        for (size_t k = 0; k < joints_.size(); ++k) {
+            if (joints_[k].index != UINT32_MAX && (jointEnds_[2 * k] == body.index || jointEnds_[2 * k + 1] == body.index)) {
+                joints_[k] = JointId{ UINT32_MAX, joints_[k].generation + 1 };
+            }
+        }
+    }
+    void removeShape(ShapeId shape) {
+        if (!isValid(shape) || !note(tf_shape_remove(handle_, 0, cid(shape)))) { return; }
+        shapes_[shape.index] = ShapeId{ UINT32_MAX, shape.generation + 1 };
+    }
+    void setFriction(ShapeId shape, float friction) {
+        if (isValid(shape)) { note(tf_shape_set_friction(handle_, 0, cid(shape), friction)); }
+    }
+    void setRestitution(ShapeId shape, float restitution) {
+        if (isValid(shape)) { note(tf_shape_set_restitution(handle_, 0, cid(shape), restitution)); }
+    }
+    void setRollingResistance(ShapeId shape, float rollingResistance) {
+        if (isValid(shape)) { note(tf_shape_set_rolling_resistance(handle_, 0, cid(shape), rollingResistance)); }
+    }
+    void setFilter(ShapeId shape, uint32_t category, uint32_t mask) {
+        if (isValid(shape)) { note(tf_shape_set_filter(handle_, 0, cid(shape), category, mask)); }
+    }
+    void setTransform(BodyId body, const Vec3& position, const Quat& rotation) {
+        if (!isValid(body)) { return; }
+        float p[3], q[4];
+        put3(p, position);
+        put4(q, rotation);
+        note(tf_body_set_transform(handle_, 0, cid(body), p, q));
+    }
+    void setKinematicTarget(BodyId body, const Vec3& position, const Quat& rotation, float dt) {
+        if (!isValid(body)) { return; }
+        float p[3], q[4];
+        put3(p, position);
+        put4(q, rotation);
+        note(tf_body_set_kinematic_target(handle_, 0, cid(body), p, q, dt));
+    }
+    void setMotionType(BodyId body, MotionType type) {
+        if (!isValid(body)) { return; }
+        const int32_t t = type == MotionType::Static ? TF_STATIC : type == MotionType::Kinematic ? TF_KINEMATIC : TF_DYNAMIC;
+        note(tf_body_set_motion_type(handle_, 0, cid(body), t));
+    }
+    void addForceAtPoint(BodyId body, const Vec3& force, const Vec3& point, bool wake = true) {
+        if (!isValid(body)) { return; }
+        float f[3], at[3];
+        put3(f, force);
+        put3(at, point);
+        note(tf_body_add_force(handle_, 0, cid(body), f, at, wake ? 1 : 0));
+    }
+    void addImpulse(BodyId body, const Vec3& impulse, bool wake = true) {
+        if (!isValid(body)) { return; }
+        float j[3];
+        put3(j, impulse);
+        note(tf_body_add_impulse(handle_, 0, cid(body), j, nullptr, wake ? 1 : 0));
+    }
+    void addImpulseAtPoint(BodyId body, const Vec3& impulse, const Vec3& point, bool wake = true) {
+        if (!isValid(body)) { return; }
+        float j[3], at[3];
+        put3(j, impulse);
+        put3(at, point);
+        note(tf_body_add_impulse(handle_, 0, cid(body), j, at, wake ? 1 : 0));
+    }
+    void setDamping(BodyId body, float linear, float angular) {
+        if (isValid(body)) { note(tf_body_set_damping(handle_, 0, cid(body), linear, angular)); }
+    }
+    void setGravityScale(BodyId body, float scale) {
+        if (isValid(body)) { note(tf_body_set_gravity_scale(handle_, 0, cid(body), scale)); }
+    }
+    void wake(BodyId body) {
+        if (isValid(body)) { note(tf_body_wake(handle_, 0, cid(body))); }
+    }
+    void sleep(BodyId body) {
+        if (isValid(body)) { note(tf_body_sleep(handle_, 0, cid(body))); }
+    }
+    void setCanSleep(BodyId body, bool canSleep) {
+        if (isValid(body)) { note(tf_body_set_can_sleep(handle_, 0, cid(body), canSleep ? 1 : 0)); }
     }
 
     bool isValid(BodyId body) const { return body.index < bodies_.size() && bodies_[body.index] == body; }
@@ -560,8 +655,18 @@ public:
     void setLinearVelocity(BodyId body, const Vec3& v) { setVelocities(body, &v, nullptr); }
     void setAngularVelocity(BodyId body, const Vec3& w) { setVelocities(body, nullptr, &w); }
 
-    void addForce(BodyId body, const Vec3& force, bool = true) { queue(forces_, body, force); }
-    void addTorque(BodyId body, const Vec3& torque, bool = true) { queue(torques_, body, torque); }
+    void addForce(BodyId body, const Vec3& force, bool wake = true) {
+        if (!isValid(body)) { return; }
+        float f[3];
+        put3(f, force);
+        note(tf_body_add_force(handle_, 0, cid(body), f, nullptr, wake ? 1 : 0));
+    }
+    void addTorque(BodyId body, const Vec3& torque, bool wake = true) {
+        if (!isValid(body)) { return; }
+        float t[3];
+        put3(t, torque);
+        note(tf_body_add_torque(handle_, 0, cid(body), t, wake ? 1 : 0));
+    }
 
     MassProperties massProperties(BodyId body) const {
         MassProperties m;
@@ -673,6 +778,9 @@ public:
         if (!note(tf_joint_create(handle_, 0, &c, &id))) { return {}; }
         if (joints_.size() <= id.index) { joints_.resize((size_t)id.index + 1); }
         joints_[id.index] = JointId{ id.index, id.generation };
+        if (jointEnds_.size() < 2 * joints_.size()) { jointEnds_.resize(2 * joints_.size(), UINT32_MAX); }
+        jointEnds_[2 * id.index] = d.bodyA.index;
+        jointEnds_[2 * id.index + 1] = d.bodyB.index;
         return joints_[id.index];
     }
     bool isValid(JointId joint) const { return joint.index < joints_.size() && joints_[joint.index] == joint; }
@@ -817,23 +925,14 @@ private:
 
     void setVelocities(BodyId body, const Vec3* v, const Vec3* w) {
         if (!isValid(body)) { return; }
-        Transform t;
-        Vec3 lv, av;
-        state(body, t, lv, av);
-        if (v) { lv = *v; }
-        if (w) { av = *w; }
         float a[3], b[3];
-        put3(a, lv);
-        put3(b, av);
-        note(tf_body_set_velocity(handle_, 0, tf_id{ body.index, body.generation }, a, b));
+        if (v) { put3(a, *v); }
+        if (w) { put3(b, *w); }
+        note(tf_body_set_velocity(handle_, 0, cid(body), v ? a : nullptr, w ? b : nullptr));
     }
 
-    void queue(std::vector<float>& into, BodyId body, const Vec3& f) {
-        if (!isValid(body)) { return; }
-        float* o = into.data() + 3 * (size_t)body.index;
-        o[0] += f.x, o[1] += f.y, o[2] += f.z;
-        forcesPending_ = true;
-    }
+    static tf_id cid(BodyId b) { return tf_id{ b.index, b.generation }; }
+    static tf_id cid(ShapeId s) { return tf_id{ s.index, s.generation }; }
 
     BodyId bodyAt(uint32_t i) const { return i < bodies_.size() ? bodies_[i] : BodyId{}; }
     ShapeId shapeAt(uint32_t i) const { return i < shapes_.size() ? shapes_[i] : ShapeId{}; }
@@ -844,10 +943,10 @@ private:
     std::vector<BodyId> bodies_;
     std::vector<ShapeId> shapes_;
     std::vector<JointId> joints_;
-    std::vector<float> forces_, torques_;
+    std::vector<uint32_t> shapeOwner_;  // each shape slot's body
+    std::vector<uint32_t> jointEnds_;   // each joint slot's bodies (UINT32_MAX for the world)
     std::map<const TriangleMesh*, int32_t> meshIds_;           // meshes this handle has built, by mesh
     std::vector<std::shared_ptr<const TriangleMesh>> meshes_;  // kept alive while their ids are in use
-    bool forcesPending_ = false;
     mutable int status_ = TF_OK;
     mutable std::vector<ContactEvent> contactEvents_;
     mutable std::vector<HitEvent> hitEvents_;

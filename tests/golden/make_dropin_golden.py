@@ -1,5 +1,5 @@
-"""Generates tests/golden/dropin_pyramid.txt and dropin_joints.txt: the output of tests/dropin/pyramid_step.cpp
-and joints_step.cpp built against the reference's own public header and sources (include/twofold/twofold.h,
+"""Generates tests/golden/dropin_pyramid.txt, dropin_joints.txt and dropin_setters.txt: the output of
+tests/dropin/pyramid_step.cpp, joints_step.cpp and setters_step.cpp built against the reference's own public header and sources (include/twofold/twofold.h,
 src/*.cpp) and run with the arguments below. The drop-in test builds the same programs against
 include/twofold_b200/world.hpp and compares.
 
@@ -16,6 +16,7 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 PROGRAMS = [
     ("pyramid_step.cpp", ["6", "60"], "dropin_pyramid.txt"),
     ("joints_step.cpp", ["60"], "dropin_joints.txt"),
+    ("setters_step.cpp", ["160"], "dropin_setters.txt"),
 ]
 
 

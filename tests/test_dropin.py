@@ -1,6 +1,6 @@
-"""The drop-in C++ surface: tests/dropin/pyramid_step.cpp, written against the reference's public World API,
-builds unchanged against include/twofold_b200/world.hpp, and run on the GPU it prints what the reference
-printed (tests/golden/dropin_pyramid.txt, made by tests/golden/make_dropin_golden.py) within 1e-5.
+"""The drop-in C++ surface: the programs under tests/dropin/, written against the reference's public World API,
+build unchanged against include/twofold_b200/world.hpp, and run on the GPU they print what the reference printed
+(tests/golden/dropin_*.txt, made by tests/golden/make_dropin_golden.py) within 1e-5.
 """
 import os
 import subprocess
@@ -17,6 +17,8 @@ PROGRAM = os.path.join(HERE, "dropin", "pyramid_step.cpp")
 GOLDEN = os.path.join(HERE, "golden", "dropin_pyramid.txt")
 JOINTS_PROGRAM = os.path.join(HERE, "dropin", "joints_step.cpp")
 JOINTS_GOLDEN = os.path.join(HERE, "golden", "dropin_joints.txt")
+SETTERS_PROGRAM = os.path.join(HERE, "dropin", "setters_step.cpp")
+SETTERS_GOLDEN = os.path.join(HERE, "golden", "dropin_setters.txt")
 TOL = 1e-5
 
 
@@ -42,6 +44,7 @@ def _parse(text):
 def test_dropin_program_compiles_against_the_facade():
     _compile(None, link=False)
     _compile(None, link=False, program=JOINTS_PROGRAM)
+    _compile(None, link=False, program=SETTERS_PROGRAM)
 
 
 def _parse_joints(text):
@@ -91,3 +94,42 @@ def test_dropin_program_matches_the_reference(tmp_path):
     for name, cols in (("p", slice(1, 4)), ("q", slice(4, 8)), ("v", slice(8, 11)), ("w", slice(11, 14))):
         err = rel_err(mine[:, cols], ref[:, cols])
         assert err <= TOL, f"{name} differs by {err}"
+
+
+def _parse_setters(text):
+    """{step: rows of index, generation, awake, p, q, v, w} and the validity line."""
+    snaps, valid, step = {}, None, None
+    for line in text.splitlines():
+        if not line or line.startswith("#"):
+            continue
+        if line.startswith("step"):
+            step = int(line.split()[1])
+            snaps[step] = []
+        elif line.startswith("valid"):
+            valid = [int(x) for x in line.split()[1:]]
+        else:
+            snaps[step].append([float(x) for x in line.split()])
+    return {k: np.array(v) for k, v in snaps.items()}, valid
+
+
+@pytest.mark.gpu
+def test_dropin_setters_program_matches_the_reference(tmp_path):
+    """destroyBody, removeShape, setTransform, setKinematicTarget, setMotionType, forces and impulses, friction,
+    restitution, rolling resistance, filters, damping, gravity scale, sleep, wake and setCanSleep, each called
+    mid-run through the drop-in World, print what the reference printed every 20 steps."""
+    exe = str(tmp_path / "setters_b200")
+    _compile(exe, link=True, program=SETTERS_PROGRAM)
+    out = subprocess.run([exe, "160"], check=True, capture_output=True, text=True).stdout
+    mine, valid_mine = _parse_setters(out)
+    with open(SETTERS_GOLDEN) as f:
+        ref, valid_ref = _parse_setters(f.read())
+    assert valid_mine == valid_ref
+    assert sorted(mine) == sorted(ref)
+    for step in sorted(ref):
+        m, r = mine[step], ref[step]
+        assert m.shape == r.shape, step
+        # index, generation and awake flag exactly
+        assert np.array_equal(m[:, :3], r[:, :3]), step
+        for name, cols in (("p", slice(3, 6)), ("q", slice(6, 10)), ("v", slice(10, 13)), ("w", slice(13, 16))):
+            err = rel_err(m[:, cols], r[:, cols])
+            assert err <= TOL, f"step {step}: {name} differs by {err}"
