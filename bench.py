@@ -319,8 +319,16 @@ def single_worlds(device, warmup=20, steps=40):
             one.step_checked(sc.dt, 1, graph=True)
             ms += one.elapsed_ms()
         body_steps = one.body_steps() - b0
+        # Per-kernel times of the next steps, from graphs with an event pair around each kernel group.
+        one.set_profiling(True)
+        for _ in range(SINGLE_BREAKDOWN_STEPS):
+            one.step_checked(sc.dt, 1, graph=True)
+        kt = one.kernel_times()
+        one.set_profiling(False)
         one.close()
-        entry = {"gpu_ms_per_step": ms / steps, "body_steps_per_s": body_steps / (ms / 1e3)}
+        entry = {"gpu_ms_per_step": ms / steps, "body_steps_per_s": body_steps / (ms / 1e3),
+                 "kernel_ms_per_step": {k: v[0] / SINGLE_BREAKDOWN_STEPS for k, v in kt.items()},
+                 "kernel_steps": f"{warmup + steps + 1}-{warmup + steps + SINGLE_BREAKDOWN_STEPS}"}
         if R.available():
             r = R.RefWorld(sc.worlds[0], sc.settings)
             r.step(sc.dt, warmup)
@@ -363,6 +371,7 @@ def adjoint_cost(device, n_worlds=1024, steps=120):
             "pipeline_forward_ms": pipe_ms, "backward_over_pipeline_forward": bwd / pipe_ms}
 
 
+SINGLE_BREAKDOWN_STEPS = 5  # profiled steps after each single world's timed ones
 BREAKDOWN_STEPS = 10  # graph-replayed steps after the timed region, with an event pair around each kernel group
 TUNE_AHEAD = 10       # the autotuner's batch is stepped this far past the warm-up
 
@@ -555,10 +564,13 @@ def run_b200(args, dist):
                 "timed_on": f"{BREAKDOWN_STEPS} graph-replayed steps after the timed region, an event pair per kernel",
                 "top_kernel_by_time": top}
         if traffic:
-            roof["traffic"] = traffic["k_substep_bytes_per_launch"]
-            roof["traffic_state"] = traffic["work"]
-            roof["traffic_over_algorithmic"] = traffic["k_substep_bytes_per_launch"] / substep_bytes(traffic["work"])
-            roof["traffic_source"] = traffic.get("source")
+            # Measured on a smaller batch: the ratio of traffic to algorithmic bytes at the captured state, and
+            # the traffic it implies for this run's launches.
+            ratio = traffic["k_substep_bytes_per_launch"] / substep_bytes(traffic["work"])
+            roof["traffic"] = ratio * sub_bytes / sub_launches
+            roof["traffic_over_algorithmic"] = ratio
+            roof["traffic_captured"] = {"bytes_per_launch": traffic["k_substep_bytes_per_launch"],
+                                        "work": traffic["work"], "source": traffic.get("source")}
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": n, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": max_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
