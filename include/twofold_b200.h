@@ -507,11 +507,10 @@ TF_API int tf_world_get_launch(void* world, int32_t kernel, uint32_t out[6]);
  *
  * It allocates nothing: its scratch is a fixed array in the library's device image. n above
  * TF_NOALLOC_MAX_BODIES is refused with TF_E_CAPACITY. The work is queued on `stream` (a cudaStream_t; NULL
- * for the default stream) on the current device and the call returns without waiting. The first call on a
- * device looks up the scratch's address there (with that device current), so make it before any stream
- * capture. That address is kept for the life of the process: after cudaDeviceReset on a device (which
- * unloads the library's device image there) this entry point must not be called on that device again.
- * Calls whose work overlaps on one device (other streams, other host threads) share the scratch and race;
+ * for the default stream) on the current device and the call returns without waiting. Each call looks up the
+ * scratch's address in the current context (a host-side lookup), so after cudaDeviceReset a new context
+ * finds it wherever the library's device image now is. The first lookup in a context may load that image,
+ * so make one call before any stream capture. Calls whose work overlaps on one device (other streams, other host threads) share the scratch and race;
  * order them on one stream. */
 #define TF_NOALLOC_MAX_BODIES 4096
 #define TF_NOALLOC_MAX_PAIRS 32768

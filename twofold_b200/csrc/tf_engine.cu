@@ -1981,8 +1981,8 @@ public:
             case 0:  // broadphase: a PairBody per body
                 st.bodies = bytes / (uint32_t)sizeof(PairBody);
                 break;
-            case 3:  // prepare: a color mask per body, two endpoints per active contact, ~3 contacts per body
-                st.bodies = bytes > 512 ? (bytes - 512) / 28 : 0;
+            case 3:  // prepare: a color mask and a mark per body, two endpoints per active contact, ~3 contacts per body
+                st.bodies = bytes > 512 ? (bytes - 512) / 32 : 0;
                 st.contacts = 3 * st.bodies + 64;
                 break;
             case 5:  // substep: the solver state of each body

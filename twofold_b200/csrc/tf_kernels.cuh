@@ -66,6 +66,22 @@ struct Group {
             asm volatile("bar.sync %0, %1;" ::"r"(id + 1), "r"(size) : "memory");
         }
     }
+    // A barrier (as sync) that also tells every thread whether p held on any thread of the group.
+    __device__ __forceinline__ bool any(bool p) const {
+        if (count == 1) { return __syncthreads_or(p) != 0; }
+        if (size == 32) {
+            __syncwarp();
+            return __any_sync(0xffffffffu, p);
+        }
+        uint32_t r;
+        asm volatile(
+            "{\n\t.reg .pred in, out;\n\tsetp.ne.u32 in, %1, 0;\n\tbar.red.or.pred out, %2, %3, in;\n\t"
+            "selp.u32 %0, 1, 0, out;\n\t}"
+            : "=r"(r)
+            : "r"((uint32_t)p), "r"(id + 1), "r"(size)
+            : "memory");
+        return r != 0;
+    }
 };
 
 // blockDim.x is a multiple of size, size a multiple of 32, at most kMaxGroups groups.
@@ -1482,26 +1498,74 @@ __device__ __forceinline__ void returnImpulses(const Batch& B, uint32_t slot, DC
     }
 }
 
+constexpr uint32_t kOrderRounds = 64;       // rounds of visitInBodyOrder before one thread takes the rest
+constexpr uint32_t kOrderRoundsMin = 64;    // shorter lists go to one thread at once
+constexpr uint8_t kColorPending = 0xff;
+
+// Visits the n entries of a contact list so that, at every moving body, its contacts are visited in list
+// order: in each round every pending entry that is the first pending one at each of its bodies is visited
+// (round r marks a body with (tag of r, its first pending entry) by atomicMin, tags falling from round to
+// round so a round's marks replace the last one's). Entries visited in one round share no body, so visit(x)
+// may read and write its own bodies' state without atomics. A result that depends, per body, only on the
+// entries before x at that body (a greedy color, a level) therefore comes out as a pass in list order gives
+// it. After kOrderRounds rounds one thread visits what is left in list order, which keeps that property: the
+// entries visited so far include every entry before them at a shared body. ends(x, a, b) gives an entry's
+// bodies (kNone for one that does not count); firstAt holds a word per body, set to kNone beforehand.
+template <class Ends, class Pending, class Visit>
+static __device__ void visitInBodyOrder(const Group& g, uint32_t n, uint32_t* firstAt, Ends ends, Pending pending,
+                                        Visit visit) {
+    if (n >= kOrderRoundsMin && n < (1u << 24)) {
+        for (uint32_t r = 0; r < kOrderRounds; ++r) {
+            const uint32_t tag = (kOrderRounds - 1 - r) << 24;
+            bool left = false;
+            for (uint32_t x = g.tid; x < n; x += g.size) {
+                if (!pending(x)) { continue; }
+                left = true;
+                uint32_t a, b;
+                ends(x, a, b);
+                if (a != kNone) { atomicMin(&firstAt[a], tag | x); }
+                if (b != kNone) { atomicMin(&firstAt[b], tag | x); }
+            }
+            if (!g.any(left)) { return; }
+            for (uint32_t x = g.tid; x < n; x += g.size) {
+                if (!pending(x)) { continue; }
+                uint32_t a, b;
+                ends(x, a, b);
+                if ((a == kNone || firstAt[a] == (tag | x)) && (b == kNone || firstAt[b] == (tag | x))) { visit(x); }
+            }
+            g.sync();
+        }
+    }
+    if (g.tid == 0) {
+        for (uint32_t x = 0; x < n; ++x) {
+            if (pending(x)) { visit(x); }
+        }
+    }
+    g.sync();
+}
+
 // Greedy lowest free color of 32 over the moving bodies, in list order (src/lanes.cpp:356-374). endA/endB
 // hold each contact's moving bodies (kNone for one that does not move); endA carries kNotColorable for a
-// planar or rolling contact, which takes no color.
-static __device__ void colorSequential(uint32_t n, const uint32_t* endA, const uint32_t* endB, uint32_t* masks,
-                                uint8_t* color) {
-    for (uint32_t x = 0; x < n; ++x) {
-        uint8_t k = kNoColor;
-        const uint32_t ea = endA[x];
-        if (!(ea & kNotColorable)) {
-            const uint32_t a = ea, b = endB[x];
+// planar or rolling contact, which takes no color. masks (a word per body) start at 0, firstAt at kNone.
+static __device__ void colorInOrder(const Group& g, uint32_t n, const uint32_t* endA, const uint32_t* endB,
+                                    uint32_t* masks, uint32_t* firstAt, uint8_t* color) {
+    for (uint32_t x = g.tid; x < n; x += g.size) { color[x] = (endA[x] & kNotColorable) ? kNoColor : kColorPending; }
+    g.sync();
+    visitInBodyOrder(
+        g, n, firstAt, [&](uint32_t x, uint32_t& a, uint32_t& b) { a = endA[x], b = endB[x]; },
+        [&](uint32_t x) { return color[x] == kColorPending; },
+        [&](uint32_t x) {
+            const uint32_t a = endA[x], b = endB[x];
             const uint32_t taken = (a != kNone ? masks[a] : 0u) | (b != kNone ? masks[b] : 0u);
+            uint8_t k = kNoColor;
             if (taken != 0xffffffffu) {
                 const int f = __ffs(~taken) - 1;
                 if (a != kNone) { masks[a] |= 1u << f; }
                 if (b != kNone) { masks[b] |= 1u << f; }
                 k = (uint8_t)f;
             }
-        }
-        color[x] = k;
-    }
+            color[x] = k;
+        });
 }
 
 // Groups a contact list by color: every color's contacts (any order within a color, which solves the same)
@@ -1546,35 +1610,54 @@ static __device__ void bucketByColor(const Group& g, uint32_t n, const uint32_t*
 // The contacts solved one at a time (planar, rolling, those past the colors) are swept in list order. Only
 // contacts that share a moving body depend on that order: each takes a level one past the last earlier
 // contact on either of its moving bodies, so that the contacts of a level share no moving body and run
-// together while every body still meets its contacts in list order, which gives the sweep's own bits. Runs on
-// one thread: reorders list by level (stably, within the level in list order) and writes each level's end.
-// last (one word per body, zero on entry), tmp and out (one word per entry) are scratch. Returns the levels.
-static __device__ uint32_t levelList(const Batch& B, const WorldInfo& wi, const DContact* cs, uint32_t* list, uint32_t n,
-                              uint32_t* levelEnd, uint32_t* last, uint32_t* tmp, uint32_t* out) {
-    uint32_t levels = 0;
-    for (uint32_t x = 0; x < n; ++x) {
+// together while every body still meets its contacts in list order, which gives the sweep's own bits. The
+// levels come from visitInBodyOrder; one thread then reorders list by level (stably, within the level in list
+// order) and writes each level's end. last and firstAt (one word per body, zero and kNone on entry), tmp and
+// out (one word per entry) are scratch. Returns the levels.
+static __device__ uint32_t levelList(const Group& g, const Batch& B, const WorldInfo& wi, const DContact* cs,
+                                     uint32_t* list, uint32_t n, uint32_t* levelEnd, uint32_t* last,
+                                     uint32_t* firstAt, uint32_t* tmp, uint32_t* out) {
+    __shared__ uint32_t s_levels[kMaxGroups];
+    // Each entry's moving bodies (tmp, out) and its level (levelEnd, kNone until set).
+    for (uint32_t x = g.tid; x < n; x += g.size) {
         const DContact& c = cs[list[x]];
         const uint32_t a = c.bodyA - wi.bodyFirst, b = c.bodyB - wi.bodyFirst;
-        const bool ma = a < wi.bodyCount && movingBody(B.bodies[c.bodyA]);
-        const bool mb = b < wi.bodyCount && movingBody(B.bodies[c.bodyB]);
-        uint32_t lev = 0;
-        if (ma) { lev = max(lev, last[a]); }
-        if (mb) { lev = max(lev, last[b]); }
-        if (ma) { last[a] = lev + 1; }
-        if (mb) { last[b] = lev + 1; }
-        tmp[x] = lev;
-        levels = max(levels, lev + 1);
+        tmp[x] = a < wi.bodyCount && movingBody(B.bodies[c.bodyA]) ? a : kNone;
+        out[x] = b < wi.bodyCount && movingBody(B.bodies[c.bodyB]) ? b : kNone;
+        levelEnd[x] = kNone;
     }
-    for (uint32_t l = 0; l < levels; ++l) { levelEnd[l] = 0; }
-    for (uint32_t x = 0; x < n; ++x) { ++levelEnd[tmp[x]]; }
-    uint32_t sum = 0;
-    for (uint32_t l = 0; l < levels; ++l) {
-        const uint32_t size = levelEnd[l];
-        levelEnd[l] = sum;  // the level's fill position, its end once filled
-        sum += size;
+    if (g.tid == 0) { s_levels[g.id] = 0; }
+    g.sync();
+    visitInBodyOrder(
+        g, n, firstAt, [&](uint32_t x, uint32_t& a, uint32_t& b) { a = tmp[x], b = out[x]; },
+        [&](uint32_t x) { return levelEnd[x] == kNone; },
+        [&](uint32_t x) {
+            const uint32_t a = tmp[x], b = out[x];
+            uint32_t lev = 0;
+            if (a != kNone) { lev = max(lev, last[a]); }
+            if (b != kNone) { lev = max(lev, last[b]); }
+            if (a != kNone) { last[a] = lev + 1; }
+            if (b != kNone) { last[b] = lev + 1; }
+            levelEnd[x] = lev;
+            atomicMax(&s_levels[g.id], lev + 1);
+        });
+    for (uint32_t x = g.tid; x < n; x += g.size) { tmp[x] = levelEnd[x]; }
+    g.sync();
+    const uint32_t levels = s_levels[g.id];
+    if (g.tid == 0) {
+        for (uint32_t l = 0; l < levels; ++l) { levelEnd[l] = 0; }
+        for (uint32_t x = 0; x < n; ++x) { ++levelEnd[tmp[x]]; }
+        uint32_t sum = 0;
+        for (uint32_t l = 0; l < levels; ++l) {
+            const uint32_t size = levelEnd[l];
+            levelEnd[l] = sum;  // the level's fill position, its end once filled
+            sum += size;
+        }
+        for (uint32_t x = 0; x < n; ++x) { out[levelEnd[tmp[x]]++] = list[x]; }
     }
-    for (uint32_t x = 0; x < n; ++x) { out[levelEnd[tmp[x]]++] = list[x]; }
-    for (uint32_t x = 0; x < n; ++x) { list[x] = out[x]; }
+    g.sync();
+    for (uint32_t x = g.tid; x < n; x += g.size) { list[x] = out[x]; }
+    g.sync();
     return levels;
 }
 
@@ -1691,9 +1774,14 @@ __global__ void __launch_bounds__(kMaxBlock) k_prepare(const __grid_constant__ B
         uint32_t* masks = staged ? reinterpret_cast<uint32_t*>(slice) : B.bodyColors + wi.bodyFirst;
         uint32_t* endA = staged ? masks + stageBodies : B.mergeIdxA + cf;
         uint32_t* endB = staged ? endA + stageContacts : B.mergeIdxB + cf;
+        // Each body's first pending contact while coloring and leveling (the island scratch is free here).
+        uint32_t* firstAt = staged ? endB + stageContacts : B.unionParent + wi.bodyFirst;
         // Colors by active position; moved to contact order below. The merge scratch is free by now.
         uint8_t* colorTmp = reinterpret_cast<uint8_t*>(B.mergePartA + cf);
-        for (uint32_t i = g.tid; i < wi.bodyCount; i += g.size) { masks[i] = 0; }
+        for (uint32_t i = g.tid; i < wi.bodyCount; i += g.size) {
+            masks[i] = 0;
+            firstAt[i] = kNone;
+        }
         uint32_t points = 0;
         for (uint32_t x = g.tid; x < nActive; x += g.size) {
             if (!TF_OK_INDEX(B, act[x] < nc, 7, w, x)) { continue; }
@@ -1716,8 +1804,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_prepare(const __grid_constant__ B
         }
         atomicAdd(&s_points[g.id], points);
         g.sync();
-        if (g.tid == 0) { colorSequential(nActive, endA, endB, masks, colorTmp); }
-        g.sync();
+        colorInOrder(g, nActive, endA, endB, masks, firstAt, colorTmp);
         uint8_t* colorOf = B.color + cf;
         for (uint32_t x = g.tid; x < nActive; x += g.size) {
             const uint8_t k = colorTmp[x];
@@ -1758,13 +1845,15 @@ __global__ void __launch_bounds__(kMaxBlock) k_prepare(const __grid_constant__ B
                 if (g.tid == 0) { (which == 0 ? wc.restLevels : wc.impactRestLevels) = 0; }
                 continue;
             }
-            for (uint32_t i = g.tid; i < wi.bodyCount; i += g.size) { masks[i] = 0; }
-            g.sync();
-            if (g.tid == 0) {
-                uint32_t* list = (which == 0 ? B.rest : B.impactRest) + cf;
-                uint32_t* ends = (which == 0 ? B.restLevel : B.impactRestLevel) + cf;
-                (which == 0 ? wc.restLevels : wc.impactRestLevels) = levelList(B, wi, cs, list, n, ends, masks, endA, endB);
+            for (uint32_t i = g.tid; i < wi.bodyCount; i += g.size) {
+                masks[i] = 0;
+                firstAt[i] = kNone;
             }
+            g.sync();
+            uint32_t* list = (which == 0 ? B.rest : B.impactRest) + cf;
+            uint32_t* ends = (which == 0 ? B.restLevel : B.impactRestLevel) + cf;
+            const uint32_t levels = levelList(g, B, wi, cs, list, n, ends, masks, firstAt, endA, endB);
+            if (g.tid == 0) { (which == 0 ? wc.restLevels : wc.impactRestLevels) = levels; }
             g.sync();
         }
         if (g.tid == 0) {

@@ -18,7 +18,6 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
-#include <mutex>
 #include <string>
 
 #include "../../include/twofold_b200.h"
@@ -34,7 +33,6 @@ constexpr int32_t kMaxBodies = TF_NOALLOC_MAX_BODIES;
 constexpr int32_t kMaxPairs = TF_NOALLOC_MAX_PAIRS;
 constexpr int kThreads = 512;
 constexpr int kWarps = kThreads / 32;
-constexpr int kMaxDevices = 64;
 
 struct PairScratch {
     uint64_t emitted[kMaxPairs];  // keys in the order the pair tests found them
@@ -157,21 +155,15 @@ __global__ void __launch_bounds__(kThreads) k_candidates_noalloc(const float* lo
     if (tid == 0) { *count = (int32_t)unique; }
 }
 
-std::mutex g_setupLock;
-void* g_scratchOn[kMaxDevices] = {};
-
-// The scratch's device address on the current device, looked up on the first call made there.
-int scratchAddress(int device, PairScratch** out) {
-    std::lock_guard<std::mutex> hold(g_setupLock);
-    if (!g_scratchOn[device]) {
-        void* p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, g_pairScratch);
-        if (e != cudaSuccess) {
-            return noteError(TF_E_CUDA, std::string("tf_candidates_noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-        }
-        g_scratchOn[device] = p;
+// The scratch's device address in the current context, looked up on every call (a host-side table lookup of the
+// loaded module, cheap): a context made after a device reset may place the module elsewhere.
+int scratchAddress(PairScratch** out) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_pairScratch);
+    if (e != cudaSuccess) {
+        return noteError(TF_E_CUDA, std::string("tf_candidates_noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(e));
     }
-    *out = static_cast<PairScratch*>(g_scratchOn[device]);
+    *out = static_cast<PairScratch*>(p);
     return TF_OK;
 }
 
@@ -191,16 +183,12 @@ TF_API int tf_candidates_noalloc(const float* lo, const float* hi, const float* 
     if (!count || (n > 0 && (!lo || !hi || !grow || !flags)) || (capacity > 0 && !keys)) {
         return noteError(TF_E_INVALID, "tf_candidates_noalloc: null pointer");
     }
-    int device = 0;
-    cudaError_t e = cudaGetDevice(&device);
-    if (e != cudaSuccess) { return noteError(TF_E_CUDA, std::string("tf_candidates_noalloc: cudaGetDevice: ") + cudaGetErrorString(e)); }
-    if (device < 0 || device >= kMaxDevices) { return noteError(TF_E_INVALID, "tf_candidates_noalloc: device index out of range"); }
     PairScratch* S = nullptr;
-    const int rc = scratchAddress(device, &S);
+    const int rc = scratchAddress(&S);
     if (rc != TF_OK) { return rc; }
     k_candidates_noalloc<<<1, kThreads, 0, static_cast<cudaStream_t>(stream)>>>(lo, hi, grow, flags, (uint32_t)n, keys,
                                                                                 (uint32_t)capacity, count, S);
-    e = cudaGetLastError();
+    const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) { return noteError(TF_E_CUDA, std::string("tf_candidates_noalloc: launch: ") + cudaGetErrorString(e)); }
     return TF_OK;
 }
