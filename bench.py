@@ -56,6 +56,9 @@ def parse():
     ap.add_argument("--shapes", default=None,
                     help="launch shapes as JSON {kernel: [threads, big-world bodies, shared bytes]} in place of the "
                          "autotuner's, e.g. the launch_shapes of an earlier run (for profiling that run's kernels)")
+    ap.add_argument("--single", default=None, choices=list(SINGLE_WORLDS),
+                    help="run only this single-world configuration, without the reference, and print its entry "
+                         "(for profiling its kernels)")
     return ap.parse_args()
 
 
@@ -295,7 +298,7 @@ def plain_rate(sc, args, device):
                       f"{args.warmup + 1}-{args.warmup + args.steps}"}
 
 
-def single_worlds(device, warmup=20, steps=40):
+def single_worlds(device, warmup=20, steps=40, only=None, reference=True):
     """The plain path on the single-world configurations (box pyramid, terrain, planar pile): device ms per
     step through the C ABI (a CUDA graph per step, launch shapes from the autotuner after the warm-up) over
     steps warmup+1..warmup+steps, beside the reference
@@ -306,9 +309,10 @@ def single_worlds(device, warmup=20, steps=40):
     import reference as R
 
     out = {}
-    for name, make in (("box_pyramid_210", scenes.config1), ("terrain_32768", scenes.config2),
-                       ("planar_16384", scenes.config3)):
-        sc = make()
+    for name in SINGLE_WORLDS:
+        if only and name != only:
+            continue
+        sc = getattr(scenes, SINGLE_WORLDS[name])()
         one = Batch(sc.worlds, sc.settings, device=device)
         for _ in range(warmup):
             one.step_checked(sc.dt, 1, graph=True)
@@ -329,7 +333,7 @@ def single_worlds(device, warmup=20, steps=40):
         entry = {"gpu_ms_per_step": ms / steps, "body_steps_per_s": body_steps / (ms / 1e3),
                  "kernel_ms_per_step": {k: v[0] / SINGLE_BREAKDOWN_STEPS for k, v in kt.items()},
                  "kernel_steps": f"{warmup + steps + 1}-{warmup + steps + SINGLE_BREAKDOWN_STEPS}"}
-        if R.available():
+        if reference and R.available():
             r = R.RefWorld(sc.worlds[0], sc.settings)
             r.step(sc.dt, warmup)
             t0 = time.perf_counter()
@@ -365,12 +369,15 @@ def adjoint_cost(device, n_worlds=1024, steps=120):
     grad[boxes, 0] = 2 * final[boxes, 0]  # loss: sum of the boxes' squared final x
     b.adjoint_backward(grad, n_shapes)
     fwd, bwd = b.adjoint_ms()
+    recompute, reverse = b.adjoint_backward_ms()
     b.close()
     return {"workload": f"impact walls, {n_worlds} worlds x 66 bodies, {steps} steps, checkpoint every step",
             "precision": "f32", "model_forward_ms": fwd, "backward_ms": bwd, "backward_over_forward": bwd / fwd,
-            "pipeline_forward_ms": pipe_ms, "backward_over_pipeline_forward": bwd / pipe_ms}
+            "pipeline_forward_ms": pipe_ms, "backward_over_pipeline_forward": bwd / pipe_ms,
+            "backward_parts_ms": {"recompute_summed": recompute, "reverse_summed": reverse}}
 
 
+SINGLE_WORLDS = {"box_pyramid_210": "config1", "terrain_32768": "config2", "planar_16384": "config3"}
 SINGLE_BREAKDOWN_STEPS = 5  # profiled steps after each single world's timed ones
 BREAKDOWN_STEPS = 10  # graph-replayed steps after the timed region, with an event pair around each kernel group
 TUNE_AHEAD = 10       # the autotuner's batch is stepped this far past the warm-up
@@ -603,6 +610,9 @@ def run_b200(args, dist):
 
 def main():
     args = parse()
+    if args.single:
+        print(json.dumps(single_worlds(0, only=args.single, reference=False)))
+        return
     dist = Dist()
     try:
         if args.impl == "reference":

@@ -456,13 +456,22 @@ TF_API int tf_world_solver_counts(void* world, int32_t w, int32_t out[8]);
  * d loss / d mass and d loss / d friction (any output may be null). It recomputes each step from its
  * checkpoint and walks it in reverse, in the precision of the last forward run.
  *
- * tf_adjoint_elapsed_ms: device time of the last forward and backward runs, ms[0] and ms[1]. */
+ * tf_adjoint_elapsed_ms: device time of the last forward and backward runs, ms[0] and ms[1].
+ * tf_adjoint_backward_ms: the last backward's recomputation and reverse walk, each summed over the chunks the
+ * backward ran them in, ms[0] and ms[1] (the two run side by side, so together they can exceed its time).
+ *
+ * tf_adjoint_branches: per world, a signature of the branches the last forward run took at the model's
+ * non-smooth points (effective masses, bias cases, impulse clamps, friction cones, restitution): equal
+ * signatures for two runs mean that, up to a 64-bit hash collision, every row took the same branches, so the
+ * model is smooth between them (a finite difference over them measures a slope, not a jump). */
 TF_API int tf_tape_record(void* world, float dt, int32_t n_steps);
 TF_API int tf_adjoint_forward(void* world, int32_t precision, const double* initial_state, const double* mass,
                               const double* friction, double* final_state);
 TF_API int tf_adjoint_backward(void* world, const double* grad_final, double* grad_initial, double* grad_mass,
                                double* grad_friction);
 TF_API int tf_adjoint_elapsed_ms(void* world, float ms[2]);
+TF_API int tf_adjoint_backward_ms(void* world, float ms[2]);
+TF_API int tf_adjoint_branches(void* world, uint64_t* per_world);
 
 /* Snapshots of the dynamic device state (bodies, shape bounds, contacts with their impulses, sleep and wake
  * bookkeeping) in numbered slots, copied on the device without a host round trip. A snapshot can be put back

@@ -1,9 +1,9 @@
 """The round-by-round order the preparation kernel colors and levels contacts in (visitInBodyOrder,
 twofold_b200/csrc/tf_kernels.cuh), restated in Python: in each round every pending contact that is the first
 pending one at each of its moving bodies is visited, and after a fixed number of rounds the rest are visited in
-list order. Greedy colors (src/lanes.cpp:356-374) and levels computed in that order must equal the ones a single
-pass in list order computes, on random contact lists, on long chains that outlast the rounds, and with
-contacts that take no color."""
+list order (also once a round visits fewer entries than a threshold). Greedy colors (src/lanes.cpp:356-374) and
+levels computed in that order must equal the ones a single pass in list order computes, on random contact
+lists, on long chains that outlast the rounds, and with contacts that take no color."""
 import numpy as np
 import pytest
 
@@ -41,7 +41,7 @@ def levels_sequential(ends):
     return out
 
 
-def in_body_order(ends, pending, visit, rounds=ROUNDS):
+def in_body_order(ends, pending, visit, rounds=ROUNDS, worth=0):
     """Calls visit on every pending entry in the order visitInBodyOrder does, checking that the entries of a
     round share no body."""
     n = len(ends)
@@ -63,12 +63,14 @@ def in_body_order(ends, pending, visit, rounds=ROUNDS):
                     seen.add(e)
         for x in ready:
             visit(x)
+        if len(ready) < worth:
+            break
     for x in range(n):
         if pending(x):
             visit(x)
 
 
-def greedy_rounds(ends, colorable, rounds=ROUNDS):
+def greedy_rounds(ends, colorable, rounds=ROUNDS, worth=0):
     color = [None if ok else 32 for ok in colorable]
     masks = {}
 
@@ -84,11 +86,11 @@ def greedy_rounds(ends, colorable, rounds=ROUNDS):
                 masks[e] = masks.get(e, 0) | (1 << f)
         color[x] = f
 
-    in_body_order(ends, lambda x: color[x] is None, visit, rounds)
+    in_body_order(ends, lambda x: color[x] is None, visit, rounds, worth)
     return color
 
 
-def levels_rounds(ends, rounds=ROUNDS):
+def levels_rounds(ends, rounds=ROUNDS, worth=0):
     level = [None] * len(ends)
     last = {}
 
@@ -100,7 +102,7 @@ def levels_rounds(ends, rounds=ROUNDS):
                 last[e] = lev + 1
         level[x] = lev
 
-    in_body_order(ends, lambda x: level[x] is None, visit, rounds)
+    in_body_order(ends, lambda x: level[x] is None, visit, rounds, worth)
     return level
 
 
@@ -122,6 +124,8 @@ def test_rounds_color_like_the_list_order_pass(seed):
     colorable = list(rng.random(n) > 0.1)
     assert greedy_rounds(ends, colorable) == greedy_sequential(ends, colorable)
     assert levels_rounds(ends) == levels_sequential(ends)
+    assert greedy_rounds(ends, colorable, worth=8) == greedy_sequential(ends, colorable)
+    assert levels_rounds(ends, worth=8) == levels_sequential(ends)
 
 
 def test_chains_longer_than_the_rounds_finish_in_list_order():

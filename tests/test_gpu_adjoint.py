@@ -8,10 +8,14 @@ differences of the double-precision model, within 1e-3 relative.
 
 The model is piecewise smooth: contacts switch on and off and friction moves between stick and slip, and a
 step of h = 1e-3 in a velocity often crosses such an event, where the difference quotient measures the jump
-and not the slope (one sphere velocity here gives 0.143 at h = 1e-3 against 0.0154 for h <= 1e-5). Each
-check therefore starts at h = 1e-3 and takes the first step size whose quotient agrees with the next
-smaller one's (a converged estimate); the adjoint must match that estimate. The float instantiation of the
-same kernels must agree with the double one.
+and not the slope (one sphere velocity here gives 0.143 at h = 1e-3 against 0.0154 for h <= 1e-5). Two checks
+follow from that. On 64 worlds over 120 steps, central differences at h = 1e-3 are compared with the adjoint
+for the entries whose +h and -h runs take every branch the unperturbed run takes (the forward's branch
+signature, tf_adjoint_branches), which is asserted, not assumed. On a few worlds over 30 steps, each check
+starts at h = 1e-3 and takes the first step size whose quotient agrees with the next smaller one's (a
+converged estimate), so entries whose runs do cross an event are covered too. The float instantiation of
+the same kernels must agree with the double one, and one step of the model must stay close to the step of
+the pipeline it was recorded from wherever the pipeline did not collide again mid-step.
 """
 import numpy as np
 import pytest
@@ -132,3 +136,87 @@ def test_model_forward_tracks_the_pipeline():
     final = b.adjoint_forward(64, initial, mass, friction)
     s = b.states()
     assert np.max(np.abs(final[boxes, :3] - s["p"][boxes])) < 0.05
+
+
+def test_adjoint_matches_central_differences_at_1e3_where_no_branch_changes():
+    """64 impact worlds, 120 steps, double precision, h = 1e-3: every entry whose +h and -h runs keep the
+    unperturbed run's branch signature in its world matches the adjoint within 1e-3."""
+    n_worlds, steps, h = 64, 120, 1e-3
+    sc = scenes.config5(n_worlds=n_worlds, seed=3)
+    b = Batch.from_scene(sc)
+    s = b.states()
+    initial = np.concatenate([s["p"], s["q"], s["v"], s["w"]], axis=1).astype(np.float64)
+    mass = np.array([b.mass(wi, i)[0] for wi, w in enumerate(sc.worlds) for i in range(len(w.bodies))], np.float64)
+    mass[mass == 0] = 1.0
+    friction = np.concatenate([w.shapes["friction"] for w in sc.worlds]).astype(np.float64)
+    b.tape_record(sc.dt, steps)
+    boxes = np.zeros(len(initial), bool)
+    for wi in range(n_worlds):
+        boxes[b.offsets[wi] + 1:b.offsets[wi] + 65] = True
+    n_shapes = len(friction)
+    loss, gi, gm, gf = _grads(b, n_shapes, 64, initial, mass, friction, boxes)
+    assert loss > 0
+    b.adjoint_forward(64, initial, mass, friction)
+    base_sig = b.adjoint_branches()
+    shape_first = np.concatenate([[0], np.cumsum([len(w.shapes) for w in sc.worlds])])
+    entries = []
+    for wi in range(0, n_worlds, 4):
+        sphere = int(b.offsets[wi]) + 65
+        for k in (7, 8, 9):
+            entries.append((wi, "initial", (sphere, k), gi[sphere, k]))
+        for box in (1, 30, 64):
+            entries.append((wi, "mass", int(b.offsets[wi]) + box, gm[int(b.offsets[wi]) + box]))
+        f_idx = np.zeros(n_shapes, bool)
+        f_idx[shape_first[wi]:shape_first[wi + 1]] = True
+        entries.append((wi, "friction", f_idx, gf[f_idx].sum()))
+
+    def run(which, index, delta):
+        i, m, f = initial.copy(), mass.copy(), friction.copy()
+        if which == "initial":
+            i[index] += delta
+        elif which == "mass":
+            m[index] += delta
+        else:
+            f[index] += delta
+        final = b.adjoint_forward(64, i, m, f)
+        return _loss(final, boxes), b.adjoint_branches()
+
+    smooth, worst = 0, 0.0
+    for wi, which, index, g in entries:
+        lp, sp = run(which, index, h)
+        lm, sm = run(which, index, -h)
+        # The other worlds do not see the change at all.
+        others = np.arange(n_worlds) != wi
+        assert np.array_equal(sp[others], base_sig[others]) and np.array_equal(sm[others], base_sig[others])
+        if sp[wi] != base_sig[wi] or sm[wi] != base_sig[wi]:
+            continue
+        smooth += 1
+        fd = (lp - lm) / (2 * h)
+        err = abs(g - fd) / max(abs(fd), 1e-6)
+        worst = max(worst, err)
+        assert abs(g - fd) <= TOL * max(abs(fd), 1e-6) + 1e-9, f"world {wi} {which} {index}: adjoint {g} vs difference {fd}"
+    print(f"{smooth} of {len(entries)} entries kept their branches at h = {h}; worst relative error {worst}")
+    assert smooth >= len(entries) // 4, f"only {smooth} of {len(entries)} entries kept their branches at h = {h}"
+
+
+def test_model_step_stays_close_to_the_pipeline_step():
+    """Each of 40 steps recorded on its own: where the pipeline did not collide any contact again mid-step,
+    the model's step (double precision) from the recorded start ends within a millimetre and 1 cm/s of the
+    pipeline's."""
+    sc = scenes.config5(n_worlds=4, seed=2)
+    b = Batch.from_scene(sc)
+    compared, worst_p, worst_v = 0, 0.0, 0.0
+    for step in range(40):
+        b.tape_record(sc.dt, 1)
+        model = b.adjoint_forward(64)
+        s = b.states()
+        for wi in range(len(sc.worlds)):
+            if b.solver_counts(wi)["fast"] > 0:
+                continue
+            lo, hi = int(b.offsets[wi]), int(b.offsets[wi + 1])
+            dp = np.max(np.abs(model[lo:hi, :3] - s["p"][lo:hi]))
+            dv = np.max(np.abs(model[lo:hi, 7:10] - s["v"][lo:hi]))
+            worst_p, worst_v = max(worst_p, dp), max(worst_v, dv)
+            compared += 1
+    assert compared >= 40, compared
+    assert worst_p <= 1e-3 and worst_v <= 1e-2, (worst_p, worst_v)

@@ -378,6 +378,8 @@ def _declare(lib):
         "tf_adjoint_forward": ([P, C.c_int32, P, P, P, P], C.c_int),
         "tf_adjoint_backward": ([P, P, P, P, P], C.c_int),
         "tf_adjoint_elapsed_ms": ([P, P], C.c_int),
+        "tf_adjoint_branches": ([P, P], C.c_int),
+        "tf_adjoint_backward_ms": ([P, P], C.c_int),
         "tf_world_set_launch": ([P, C.c_int32, C.c_int32, C.c_int32, C.c_int32], C.c_int),
         "tf_world_get_launch": ([P, C.c_int32, P], C.c_int),
         "tf_candidates_noalloc": ([P, P, P, P, C.c_int32, P, C.c_int32, P, P], C.c_int),
@@ -405,7 +407,8 @@ EXPORTED = [
     "tf_world_launch_count", "tf_world_elapsed_ms", "tf_world_body_steps", "tf_world_add_forces",
     "tf_world_read_poses", "tf_world_set_profiling", "tf_world_kernel_times", "tf_kernel_name",
     "tf_world_work_counts", "tf_world_solver_counts", "tf_world_save_state", "tf_world_restore_state", "tf_world_autotune", "tf_tape_record", "tf_adjoint_forward",
-    "tf_adjoint_backward", "tf_adjoint_elapsed_ms", "tf_world_set_launch", "tf_world_get_launch", "tf_candidates_noalloc",
+    "tf_adjoint_backward", "tf_adjoint_elapsed_ms", "tf_adjoint_branches",
+    "tf_adjoint_backward_ms", "tf_world_set_launch", "tf_world_get_launch", "tf_candidates_noalloc",
 ]
 
 

@@ -94,17 +94,25 @@ def build(force=False, verbose=False, out=None, defines=(), checked=True):
         if not force and not stale() and (not checked or os.path.exists(CHECKED_OUT)):
             return OUT
         jobs = [(OUT, ())] + ([(CHECKED_OUT, ("TF_DEVICE_CHECKS",))] if checked else [])
-    # Every source of every variant compiles in parallel; each variant links once its objects are done.
+    # Every stale object of every variant compiles in parallel (an object is stale when its source, a header or
+    # this file is newer, or a forced build); each variant links once its objects are done.
+    newest_shared = max(os.path.getmtime(p) for p in HEADERS + [__file__])
     procs = []
     for target, defines in jobs:
         compiles, link = _command(target, defines)
         os.makedirs(os.path.dirname(_object(SOURCES[0], os.path.basename(target)[:-3])), exist_ok=True)
         for cmd in compiles:
+            obj, src = cmd[cmd.index("-o") + 1], cmd[-1]
+            if not force and os.path.exists(obj) and \
+                    os.path.getmtime(obj) > max(newest_shared, os.path.getmtime(src)):
+                continue
             procs.append((target, cmd, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)))
     logs = {}
+    for target, _ in jobs:
+        logs[target] = []
     for target, cmd, proc in procs:
         out = proc.communicate()[0]
-        logs.setdefault(target, []).append(" ".join(cmd) + "\n" + out)
+        logs[target].append(" ".join(cmd) + "\n" + out)
         if proc.returncode != 0:
             sys.stderr.write(out)
             raise RuntimeError(f"nvcc failed compiling {cmd[-1]} for {os.path.basename(target)}")

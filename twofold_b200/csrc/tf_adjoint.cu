@@ -210,6 +210,9 @@ struct Model {
     uint64_t logStride;
     T* integLog;     // per slot, substep and body: q (4) and w (3) before the position update, dp (3) after it
     T* scratch;      // per slot: one state
+    // Per world, the forward's branch signature (k_model_forward writes it when not null): a sum over every row
+    // the run solved of a hash of (step, operation, row, which side of each non-smooth point the row took).
+    unsigned long long* branches;
 };
 
 
@@ -430,16 +433,23 @@ __device__ __forceinline__ void readCall(const T* log, SBody<T>& a, SBody<T>& b,
 }
 
 // The normal row of point i (src/solver.cpp:364-392). Returns the impulse added.
+// The branches of one row that change the model's derivative, for the branch signature: bit 0 the axis has
+// an effective mass, bits 1-2 the bias case, bit 3 the impulse clamp; friction: the axes, the cone clamp, a
+// nonzero magnitude; restitution: whether the point restitutes and the clamp. (The largest impulse of a step,
+// a running maximum, decides only whether a point restitutes, which the restitution bits hold.)
 template <class T>
 __device__ __forceinline__ T normalRow(const Model<T>& M, SBody<T>& a, SBody<T>& b, const CData<T>& c, int i,
-                                       PointState<T>& p, bool useBias, const Softness<T>& soft) {
+                                       PointState<T>& p, bool useBias, const Softness<T>& soft, uint32_t* br = nullptr) {
     const Axis<T> x = makeAxis(a, b, c.ra[i], c.rb[i], c.n);
     const V3<T> d = b.dp - a.dp + rotate(b.dq, c.rb[i]) - rotate(a.dq, c.ra[i]);
     const T sep = dot(d, c.n) + c.adjSep[i];
     T bias = 0, ms = 1, is = 0;
+    uint32_t biasKind = 0;
     if (sep > T(0)) {
         bias = sep * M.invH;
+        biasKind = 1;
     } else if (useBias) {
+        biasKind = soft.biasRate * sep > -M.maxPushout ? 2 : 3;
         bias = fmax(soft.biasRate * sep, -M.maxPushout);
         ms = soft.massScale;
         is = soft.impulseScale;
@@ -448,6 +458,7 @@ __device__ __forceinline__ T normalRow(const Model<T>& M, SBody<T>& a, SBody<T>&
     const T imp = -x.mass * ms * (vn + bias) - is * p.n;
     const T total = fmax(p.n + imp, T(0));
     const T delta = total - p.n;
+    if (br) { *br = (x.on ? 1u : 0u) | biasKind << 1 | (p.n + imp > T(0) ? 8u : 0u); }
     p.n = total;
     p.maxN = fmax(p.maxN, delta);
     push(a, b, x, delta);
@@ -511,7 +522,8 @@ __device__ __forceinline__ void normalRowAdj(const Model<T>& M, const SBody<T>& 
 
 // The friction rows of point i (src/solver.cpp:393-418).
 template <class T>
-__device__ __forceinline__ void frictionRow(SBody<T>& a, SBody<T>& b, const CData<T>& c, int i, PointState<T>& p, T mu) {
+__device__ __forceinline__ void frictionRow(SBody<T>& a, SBody<T>& b, const CData<T>& c, int i, PointState<T>& p, T mu,
+                                            uint32_t* br = nullptr) {
     const Axis<T> x1 = makeAxis(a, b, c.ra[i], c.rb[i], c.t1);
     const Axis<T> x2 = makeAxis(a, b, c.ra[i], c.rb[i], c.t2);
     const T old1 = dot(p.t, c.t1), old2 = dot(p.t, c.t2);
@@ -519,6 +531,7 @@ __device__ __forceinline__ void frictionRow(SBody<T>& a, SBody<T>& b, const CDat
     T f2 = old2 - x2.mass * speedAlong(a, b, x2);
     const T limit = mu * p.n;
     const T mag = sqrtT(f1 * f1 + f2 * f2);
+    if (br) { *br = (x1.on ? 1u : 0u) | (x2.on ? 2u : 0u) | (mag > limit ? 4u : 0u) | (mag > T(0) ? 8u : 0u) | 32u; }
     if (mag > limit) {
         const T scale = mag > T(0) ? limit / mag : T(0);
         f1 *= scale;
@@ -583,12 +596,13 @@ __device__ __forceinline__ bool restitutes(const Model<T>& M, const CData<T>& c,
 
 template <class T>
 __device__ __forceinline__ void restituteRow(const Model<T>& M, SBody<T>& a, SBody<T>& b, const CData<T>& c, int i,
-                                             PointState<T>& p) {
+                                             PointState<T>& p, uint32_t* br = nullptr) {
     const Axis<T> x = makeAxis(a, b, c.ra[i], c.rb[i], c.n);
     const T vn = speedAlong(a, b, x);
     const T imp = -x.mass * (vn + c.restitution * c.relVel[i]);
     const T total = fmax(p.n + imp, T(0));
     const T delta = total - p.n;
+    if (br) { *br = (x.on ? 1u : 0u) | (p.n + imp > T(0) ? 2u : 0u) | 64u; }
     p.n = total;
     p.maxN = fmax(p.maxN, delta);
     push(a, b, x, delta);
@@ -622,11 +636,21 @@ __device__ __forceinline__ void restituteRowAdj(const Model<T>& M, const SBody<T
 }
 
 // One operation on one contact, forward. The points' state comes in and goes out through p.
+// A 64-bit mix of one row's place in the run and its branches (the finaliser of splitmix64).
+__device__ __forceinline__ unsigned long long branchHash(unsigned long long tag, uint32_t row, uint32_t bits) {
+    unsigned long long z = tag * 0x9E3779B97F4A7C15ull + ((unsigned long long)row << 8 | bits);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
 template <class T>
 __device__ void contactOp(const Model<T>& M, int op, SBody<T>& a, SBody<T>& b, const CData<T>& c, PointState<T>* p,
-                          T mu, T* rowLog = nullptr) {
+                          T mu, T* rowLog = nullptr, unsigned long long* sig = nullptr, unsigned long long tag = 0) {
     const Softness<T> soft = (!a.moves || !b.moves) ? M.staticSoft : M.contactSoft;
     const int n = c.count;
+    uint32_t bits = 0;
+    uint32_t* br = sig ? &bits : nullptr;
     if (op == kWarm) {
         for (int i = 0; i < n; ++i) {
             const Axis<T> xn = makeAxis(a, b, c.ra[i], c.rb[i], c.n);
@@ -641,20 +665,24 @@ __device__ void contactOp(const Model<T>& M, int op, SBody<T>& a, SBody<T>& b, c
     if (op == kRestitute) {
         if (c.restitution == T(0)) { return; }
         for (int i = 0; i < n; ++i) {
-            if (restitutes(M, c, i, p[i])) { restituteRow(M, a, b, c, i, p[i]); }
+            bits = 128u;
+            if (restitutes(M, c, i, p[i])) { restituteRow(M, a, b, c, i, p[i], br); }
+            if (sig) { *sig += branchHash(tag, (uint32_t)i, bits); }
         }
         return;
     }
     const bool useBias = op == kBias;
     for (int i = 0; i < n; ++i) {
         if (rowLog) { writeRow(rowLog, i, a.v, a.w, b.v, b.w, p[i]); }
-        normalRow(M, a, b, c, i, p[i], useBias, soft);
+        normalRow(M, a, b, c, i, p[i], useBias, soft, br);
+        if (sig) { *sig += branchHash(tag, (uint32_t)i, bits); }
     }
     // Friction forward in the biased pass and backward in the relax pass; row n + j is the j-th friction row.
     for (int j = 0; j < n; ++j) {
         const int i = useBias ? j : n - 1 - j;
         if (rowLog) { writeRow(rowLog, n + j, a.v, a.w, b.v, b.w, p[i]); }
-        frictionRow(a, b, c, i, p[i], mu);
+        frictionRow(a, b, c, i, p[i], mu, br);
+        if (sig) { *sig += branchHash(tag, (uint32_t)(n + j), bits); }
     }
 }
 
@@ -830,7 +858,7 @@ __device__ __forceinline__ int passLists(const WorldView& V, int op, PassList* o
 // inputs of every contact operation and position update are written there for the reverse pass.
 template <class T>
 __device__ void stepWorld(const Model<T>& M, const Slot<T>& W, int step, uint32_t w, const T* in, T* out, T* log,
-                          T* integLog) {
+                          T* integLog, unsigned long long* sig = nullptr) {
     const uint32_t lane = threadIdx.x & 31;
     const WorldView V = viewOf(M.S, step, w);
     const int n = M.S.substeps;
@@ -882,7 +910,8 @@ __device__ void stepWorld(const Model<T>& M, const Slot<T>& W, int step, uint32_
         PointState<T> ps[4];
         for (int i = 0; i < 4; ++i) { ps[i] = p[i]; }
         if (log) { writeCall(log + at * callWords<T>(), a, b, ps); }
-        contactOp(M, op, a, b, c, ps, contactFriction(M, V, tc), log ? log + at * callWords<T>() : (T*)nullptr);
+        contactOp(M, op, a, b, c, ps, contactFriction(M, V, tc), log ? log + at * callWords<T>() : (T*)nullptr, sig,
+                  (unsigned long long)step << 40 ^ at << 2 ^ (unsigned long long)op);
         for (int i = 0; i < 4; ++i) { p[i] = ps[i]; }
         if (a.moves) {
             st3(out + (size_t)ga * kState + 7, a.v);
@@ -1164,9 +1193,15 @@ __global__ void __launch_bounds__(128) k_model_forward(const __grid_constant__ M
     __syncwarp();
     const size_t stride = (size_t)M.S.totalBodies * kState;
     const Slot<T> W = slotOf(M, 0);
+    unsigned long long sig = 0;
     for (int s = 0; s < M.S.nSteps; ++s) {
-        stepWorld<T>(M, W, s, w, M.states + s * stride, M.states + (s + 1) * stride, nullptr, nullptr);
+        stepWorld<T>(M, W, s, w, M.states + s * stride, M.states + (s + 1) * stride, nullptr, nullptr,
+                     M.branches ? &sig : nullptr);
         __syncwarp();
+    }
+    if (M.branches) {
+        for (int o = 16; o > 0; o >>= 1) { sig += __shfl_xor_sync(0xffffffffu, sig, o); }
+        if (lane == 0) { M.branches[w] = sig; }
     }
 }
 
@@ -1220,17 +1255,22 @@ struct Run {
     void *invM = nullptr, *invI = nullptr, *dp = nullptr, *dq = nullptr, *qBase = nullptr, *points = nullptr;
     void *stateAdj = nullptr, *dpAdj = nullptr, *dqAdj = nullptr, *qBaseAdj = nullptr, *invMAdj = nullptr,
          *invIAdj = nullptr, *pointAdj = nullptr, *massAdj = nullptr, *frictionAdj = nullptr, *log = nullptr,
-         *integLog = nullptr, *scratch = nullptr;
+         *integLog = nullptr, *scratch = nullptr, *branches = nullptr;
     uint64_t logStride = 0;
     int slots = 0;  // steps the backward recomputes at once; two sets of slots alternate
     bool forwardDone = false;
     float forwardMs = 0.0f, backwardMs = 0.0f;
+    // The backward's two kinds of launch, each summed over its chunks (they overlap, so the sum can exceed the
+    // backward's own time): recomputation and reverse walk.
+    float recomputeMs = 0.0f, reverseMs = 0.0f;
+    std::vector<cudaEvent_t> chunkEvents;  // per chunk: recompute start, end; reverse start, end
     // The recomputation runs on its own stream, one chunk ahead of the reverse walk.
     cudaStream_t side = nullptr;
     cudaEvent_t ready = nullptr, recomputed[2] = {}, reversed[2] = {};
 
     ~Run() {
         release();
+        for (cudaEvent_t e : chunkEvents) { cudaEventDestroy(e); }
         for (cudaEvent_t e : { ready, recomputed[0], recomputed[1], reversed[0], reversed[1] }) {
             if (e) { cudaEventDestroy(e); }
         }
@@ -1241,7 +1281,7 @@ struct Run {
         owned.clear();
         for (void** p : { &mass, &friction, &init, &states, &invM, &invI, &dp, &dq, &qBase, &points, &stateAdj, &dpAdj,
                           &dqAdj, &qBaseAdj, &invMAdj, &invIAdj, &pointAdj, &massAdj, &frictionAdj, &log, &integLog,
-                          &scratch }) {
+                          &scratch, &branches }) {
             *p = nullptr;
         }
         forwardDone = false;
@@ -1296,6 +1336,7 @@ Model<T> modelOf(const AdjointSetup& S, Run& r) {
     M.logStride = r.logStride;
     M.integLog = (T*)r.integLog;
     M.scratch = (T*)r.scratch;
+    M.branches = (unsigned long long*)r.branches;
     return M;
 }
 
@@ -1329,7 +1370,8 @@ int forwardT(Run& r, const AdjointSetup& S, cudaStream_t stream, const double* i
         (rc = r.alloc(&r.invM, nb * sizeof(T))) || (rc = r.alloc(&r.invI, 9 * nb * sizeof(T))) ||
         (rc = r.alloc(&r.dp, 3 * nb * sizeof(T))) || (rc = r.alloc(&r.dq, 4 * nb * sizeof(T))) ||
         (rc = r.alloc(&r.qBase, 4 * nb * sizeof(T))) ||
-        (rc = r.alloc(&r.points, (size_t)S.contactSlots * 4 * sizeof(PointState<T>)))) {
+        (rc = r.alloc(&r.points, (size_t)S.contactSlots * 4 * sizeof(PointState<T>))) ||
+        (rc = r.alloc(&r.branches, (size_t)S.nWorlds * sizeof(unsigned long long)))) {
         return rc;
     }
     // Parameters: the caller's, else the recorded ones.
@@ -1461,16 +1503,27 @@ int backwardT(Run& r, const AdjointSetup& S, cudaStream_t stream, const double* 
     const int blocks = (S.nWorlds + 3) / 4;
     // Chunk c recomputes into slot set c % 2 on the side stream once the reverse walk of chunk c - 2 has left
     // that set, so that it runs beside the walk of chunk c - 1; the walk of chunk c waits for its recompute.
+    const int chunks = (S.nSteps + r.slots - 1) / r.slots;
+    while ((int)r.chunkEvents.size() < 4 * chunks) {
+        cudaEvent_t e;
+        TF_ADJ_CUDA(cudaEventCreate(&e));
+        r.chunkEvents.push_back(e);
+    }
     int c = 0;
     for (int end = S.nSteps; end > 0; ++c) {
         const int count = std::min(end, r.slots), first = end - count, set = c % 2;
         const uint32_t base = (uint32_t)(set * r.slots);
         const unsigned warps = (unsigned)count * (unsigned)S.nWorlds;
+        cudaEvent_t* ev = r.chunkEvents.data() + 4 * c;
         if (c >= 2) { TF_ADJ_CUDA(cudaStreamWaitEvent(r.side, r.reversed[set], 0)); }
+        cudaEventRecord(ev[0], r.side);
         k_model_recompute<T><<<(warps + 3) / 4, 128, 0, r.side>>>(M, first, count, base);
+        cudaEventRecord(ev[1], r.side);
         cudaEventRecord(r.recomputed[set], r.side);
         TF_ADJ_CUDA(cudaStreamWaitEvent(stream, r.recomputed[set], 0));
+        cudaEventRecord(ev[2], stream);
         k_model_reverse<T><<<blocks, 128, 0, stream>>>(M, first, count, base);
+        cudaEventRecord(ev[3], stream);
         cudaEventRecord(r.reversed[set], stream);
         end = first;
     }
@@ -1480,6 +1533,14 @@ int backwardT(Run& r, const AdjointSetup& S, cudaStream_t stream, const double* 
     cudaEventElapsedTime(&r.backwardMs, e0, e1);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
+    r.recomputeMs = r.reverseMs = 0.0f;
+    for (int k = 0; k < c; ++k) {
+        float a = 0.0f, b = 0.0f;
+        cudaEventElapsedTime(&a, r.chunkEvents[4 * k], r.chunkEvents[4 * k + 1]);
+        cudaEventElapsedTime(&b, r.chunkEvents[4 * k + 2], r.chunkEvents[4 * k + 3]);
+        r.recomputeMs += a;
+        r.reverseMs += b;
+    }
     std::vector<double> out;
     if (gradInit) {
         if ((rc = download<T>(out, r.stateAdj, nb * kState, stream)) != TF_OK) { return rc; }
@@ -1521,10 +1582,20 @@ int adjointBackward(void* run, const AdjointSetup& S, void* stream, const double
     return adj::backwardT<float>(r, S, st, gradFinal, gradInit, gradMass, gradFriction);
 }
 
+int adjointBranches(void* run, int nWorlds, uint64_t* out) {
+    const adj::Run& r = *static_cast<adj::Run*>(run);
+    if (!r.forwardDone || !r.branches) { return noteError(TF_E_INVALID, "adjoint: no forward run to read branches from"); }
+    const cudaError_t e = cudaMemcpy(out, r.branches, (size_t)nWorlds * sizeof(uint64_t), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) { return noteError(TF_E_CUDA, std::string("adjoint: branches: ") + cudaGetErrorString(e)); }
+    return TF_OK;
+}
+
 void adjointTimes(void* run, float* ms) {
     const adj::Run& r = *static_cast<adj::Run*>(run);
     ms[0] = r.forwardMs;
     ms[1] = r.backwardMs;
+    ms[2] = r.recomputeMs;
+    ms[3] = r.reverseMs;
 }
 
 }  // namespace tfb

@@ -112,7 +112,8 @@ int adjointForward(void* run, const AdjointSetup& S, void* stream, int precision
                    const double* friction, double* finalState);
 int adjointBackward(void* run, const AdjointSetup& S, void* stream, const double* gradFinal, double* gradInit,
                     double* gradMass, double* gradFriction);
-void adjointTimes(void* run, float* ms);
+void adjointTimes(void* run, float* ms);  // forward, backward, recompute summed, reverse summed
+int adjointBranches(void* run, int nWorlds, uint64_t* out);
 
 class Engine {
 public:
@@ -1887,7 +1888,7 @@ public:
                 launch(kKCollideAll, *std::max_element(flatGrids, flatGrids + kPairClasses), threads(7), 0, B, P, serial);
                 return;
             }
-            for (int c = 0; c < kPairClasses; ++c) { launch(kKCollide + c, flatGrids[c], threads(7), 0, B, P, serial); }
+            for (int c = 0; c < kPairClasses; ++c) { launch(kKCollide + c, flatGrids[c], flatThreads(c), 0, B, P, serial); }
         });
         timed(1, rec, [&] { launch(kKNarrowphase, grids[1], threads(1), 0, B, P, splits[1], serial); });
         timed(2, rec, [&] { launch(kKWake, grids[2], threads(2), 0, B, splits[2], serial); });
@@ -1906,7 +1907,7 @@ public:
                     }
                     launch(kKRefresh + kPairClasses, flatGrids[6], threads(4), 0, B, P, i, serial);
                     for (int c = 0; c < kPairClasses; ++c) {
-                        launch(kKRefresh + c, flatGrids[7 + c], threads(4), 0, B, P, i, serial);
+                        launch(kKRefresh + c, flatGrids[7 + c], flatThreads(7 + c), 0, B, P, i, serial);
                     }
                 });
             }
@@ -1999,6 +2000,15 @@ public:
         return st;
     }
 
+    // Threads per CTA of flat grid f (the pair collisions by class, then the refreshes: the other active contacts
+    // and each class): the collide or refresh shape's, at most kMeshWarps warps for the mesh pairs, which a warp
+    // each collides with the warp's shared room.
+    static bool meshGrid(int f) { return f == kClassMesh || f == 7 + kClassMesh; }
+    int flatThreads(int f) const {
+        const int t = (int)shapes[f < kPairClasses ? 7 : 4].threads;
+        return meshGrid(f) ? std::min(t, 32 * kMeshWarps) : t;
+    }
+
     // Turns the launch shapes into kernel arguments and grid sizes for the current layout.
     int configureLaunches() {
         int rc = configureKernels();
@@ -2051,14 +2061,15 @@ public:
             kernelEntry(kKRefresh + kClassMesh) };
         for (int f = 0; f < kFlatGrids; ++f) {
             int perSm = 0;
-            const int threads = (int)shapes[f < kPairClasses ? 7 : 4].threads;
+            const int threads = flatThreads(f);
             TF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, flat[f], threads, 0));
             if (perSm < 1) { return fail(TF_E_INVALID, "launch shape does not fit on an SM"); }
             // No more CTAs than the class list can ever fill: its capacity is the batch's candidate slots (pair
-            // collisions) or contact slots (refreshes). A small batch then launches a handful of CTAs rather
-            // than a full device's worth that find no work.
+            // collisions) or contact slots (refreshes), an item a thread (a warp for mesh pairs). A small batch
+            // then launches a handful of CTAs rather than a full device's worth that find no work.
             const size_t cap = f < kPairClasses ? totalCand : totalContacts;
-            const size_t needed = std::max<size_t>(1, (cap + (size_t)threads - 1) / (size_t)threads);
+            const size_t perCta = meshGrid(f) ? (size_t)std::min(threads / 32, kMeshWarps) : (size_t)threads;
+            const size_t needed = std::max<size_t>(1, (cap + perCta - 1) / perCta);
             flatGrids[f] = (int)std::min<size_t>((size_t)smCount * (size_t)perSm, needed);
         }
         return TF_OK;
@@ -3324,8 +3335,34 @@ TF_API int tf_adjoint_elapsed_ms(void* h, float ms[2]) {
     if (!h || !ms) { return tfb::fail(TF_E_INVALID, "tf_adjoint_elapsed_ms: null"); }
     Engine* e = E(h);
     ms[0] = ms[1] = 0.0f;
-    if (e->adjRun) { tfb::adjointTimes(e->adjRun, ms); }
+    if (e->adjRun) {
+        float all[4];
+        tfb::adjointTimes(e->adjRun, all);
+        ms[0] = all[0];
+        ms[1] = all[1];
+    }
     return TF_OK;
+}
+
+TF_API int tf_adjoint_backward_ms(void* h, float ms[2]) {
+    if (!h || !ms) { return tfb::fail(TF_E_INVALID, "tf_adjoint_backward_ms: null"); }
+    Engine* e = E(h);
+    ms[0] = ms[1] = 0.0f;
+    if (e->adjRun) {
+        float all[4];
+        tfb::adjointTimes(e->adjRun, all);
+        ms[0] = all[2];
+        ms[1] = all[3];
+    }
+    return TF_OK;
+}
+
+TF_API int tf_adjoint_branches(void* h, uint64_t* per_world) {
+    if (!h || !per_world) { return tfb::fail(TF_E_INVALID, "tf_adjoint_branches: null"); }
+    Engine* e = E(h);
+    if (!e->adjRun) { return tfb::fail(TF_E_INVALID, "tf_adjoint_branches: run tf_adjoint_forward first"); }
+    if (cudaSetDevice(e->device) != cudaSuccess) { return tfb::fail(TF_E_CUDA, "tf_adjoint_branches: cudaSetDevice"); }
+    return tfb::adjointBranches(e->adjRun, (int)e->worlds.size(), per_world);
 }
 
 TF_API int tf_world_save_state(void* h, int32_t slot) {

@@ -1031,9 +1031,12 @@ __device__ void narrowOne(const Batch& B, const StepParams& P, const WorldInfo& 
     B.stageUsed[wi.candFirst + i] = used;
 }
 
-// A pair with a mesh over dt (src/world.cpp:505-533): manifolds with normals from sa to sb, into out.
+// A pair with a mesh over dt (src/world.cpp:505-533): manifolds with normals from sa to sb, into out. Warp: the
+// warp's lanes collide the triangles together (collideMeshWarp, warpFound its shared room); else one thread.
+template <bool Warp>
 static __device__ int collideMeshPair(const Batch& B, const StepParams& P, const DShape& sa, const DShape& sb, float dt,
-                               Manifold* out, int& outCount, MeshBounds* bounds) {
+                               Manifold* out, int& outCount, MeshBounds* bounds, Manifold* warpFound = nullptr,
+                               uint32_t lane = 0) {
     const DBody& ba = B.bodies[sa.body];
     const DBody& bb = B.bodies[sb.body];
     const float travel = relativeTravel(ba, bb, dt);
@@ -1041,11 +1044,31 @@ static __device__ int collideMeshPair(const Batch& B, const StepParams& P, const
     const Transform xa = ba.xf * sa.local;
     const Transform xb = bb.xf * sb.local;
     const Motion mo{ ba.v, ba.w, ba.com, bb.v, bb.w, bb.com, dt, travel > P.tol.speculative };
-    if (sa.kind == kMesh) { return collideMesh(B.cx, sa, xa, sb, xb, margin, mo, out, outCount, bounds); }
-    const int status = collideMesh(B.cx, sb, xb, sa, xa, margin, mo.swapped(), out, outCount, bounds);
-    for (int i = 0; i < outCount; ++i) { out[i].normal = -out[i].normal; }
+    const bool meshFirst = sa.kind == kMesh;
+    const DShape& mesh = meshFirst ? sa : sb;
+    const DShape& other = meshFirst ? sb : sa;
+    const Transform& xm = meshFirst ? xa : xb;
+    const Transform& xo = meshFirst ? xb : xa;
+    const Motion m = meshFirst ? mo : mo.swapped();
+    int status;
+    if constexpr (Warp) {
+        status = collideMeshWarp(B.cx, mesh, xm, other, xo, margin, m, out, outCount, bounds, warpFound, lane);
+    } else {
+        status = collideMesh(B.cx, mesh, xm, other, xo, margin, m, out, outCount, bounds);
+    }
+    if (!meshFirst) {
+        for (int i = 0; i < outCount; ++i) { out[i].normal = -out[i].normal; }
+    }
     return status;
 }
+
+// A warp's shared room for one mesh pair: its triangle manifolds and the triangles it rules out. The mesh pair
+// kernels run 4 warps to a CTA.
+struct MeshWarpRoom {
+    Manifold found[kMaxMeshFound];
+    TriangleBound ruled[kMaxMeshBounds];
+};
+constexpr int kMeshWarps = 4;
 
 // A contact of pair (sa, sb) from one manifold (src/world.cpp:912-939): points on both surfaces, anchors,
 // tangents and the reuse record.
@@ -1088,9 +1111,14 @@ static __device__ void meshRoomOverflow(const Batch& B, const WorldInfo& wi, Wor
 // moved, else one contact per manifold the mesh collision makes, each carrying the impulses of the old
 // contact whose normal is closest. The first contact goes to the candidate's staging slot, the others to
 // the world's extra parts. A fast pair records the triangles it ruled out, for the refresh within the step.
+// Warp: every lane of the warp calls it alike with the warp's room; the lanes collide the triangles together and
+// lane 0 writes the results.
+template <bool Warp>
 static __device__ void narrowMesh(const Batch& B, const StepParams& P, const WorldInfo& wi, WorldCounts& wc, uint32_t i,
-                           const DContact* old, uint32_t oldCount, int serial) {
-    B.stageUsed[wi.candFirst + i] = 0;
+                           const DContact* old, uint32_t oldCount, int serial, MeshWarpRoom* room = nullptr,
+                           uint32_t lane = 0) {
+    const bool lead = !Warp || lane == 0;
+    if (lead) { B.stageUsed[wi.candFirst + i] = 0; }
     const uint64_t key = B.cand[wi.candFirst + i];
     const uint32_t ia = (uint32_t)(key >> 32), ib = (uint32_t)(key & 0xffffffffu);
     if (!TF_OK_INDEX(B, ia < wi.shapeCount && ib < wi.shapeCount, 34, wi.bodyFirst, ia)) { return; }
@@ -1112,6 +1140,7 @@ static __device__ void narrowMesh(const Batch& B, const StepParams& P, const Wor
     int n = 0;
     uint32_t boundsFirst = 0, boundsCount = 0;
     if (keep) {
+        if (!lead) { return; }
         n = (int)(hi - lo);
         if (n > kMaxMeshParts) {
             atomicOr(&wc.flags, kDevUnsupported);
@@ -1119,9 +1148,12 @@ static __device__ void narrowMesh(const Batch& B, const StepParams& P, const Wor
         }
     } else {
         const bool record = relativeTravel(ba, bb, P.dt) > P.tol.speculative;
-        TriangleBound ruled[kMaxMeshBounds];
+        TriangleBound own[Warp ? 1 : kMaxMeshBounds];
+        TriangleBound* ruled = Warp ? room->ruled : own;
         MeshBounds mb{ record ? ruled : nullptr, 0, nullptr, 0, 0.0f };
-        if (collideMeshPair(B, P, sa, sb, P.dt, found, n, &mb) != kMeshOk) {
+        const int status = collideMeshPair<Warp>(B, P, sa, sb, P.dt, found, n, &mb, Warp ? room->found : nullptr, lane);
+        if (!lead) { return; }
+        if (status != kMeshOk) {
             atomicOr(&wc.flags, kDevUnsupported);
             return;
         }
@@ -1208,10 +1240,30 @@ __device__ __forceinline__ void collideClass(const Batch& B, const StepParams& P
         const WorldInfo wi = B.info[it.x];
         WorldCounts& wc = B.counts[it.x];
         if constexpr (Cls == kClassMesh) {
-            narrowMesh(B, P, wi, wc, it.y, B.previous + wi.contactFirst, wc.contactCount, serial);
+            narrowMesh<false>(B, P, wi, wc, it.y, B.previous + wi.contactFirst, wc.contactCount, serial);
         } else {
             narrowOne<Cls>(B, P, wi, wc, it.y, B.previous + wi.contactFirst, wc.contactCount);
         }
+    }
+}
+
+// The mesh candidates over every world, a warp per pair, the warp's lanes over the pair's triangles: a pair
+// near many triangles (a large or fast shape on a fine mesh) no longer holds a whole launch on one thread.
+// Launched with at most kMeshWarps warps to a CTA.
+__device__ __forceinline__ void collideMeshPairs(const Batch& B, const StepParams& P, int serial) {
+    __shared__ MeshWarpRoom s_rooms[kMeshWarps];
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t perCta = min(blockDim.x >> 5, (uint32_t)kMeshWarps);  // warps past the rooms stay idle
+    if (warp >= perCta) { return; }
+    const uint32_t n = *(volatile uint32_t*)(B.work + kSlotCandItems + kClassMesh);
+    const uint2* items = B.candItems + (size_t)kClassMesh * B.candItemStride;
+    const uint32_t warps = gridDim.x * perCta;
+    for (uint32_t item = blockIdx.x * perCta + warp; item < n; item += warps) {
+        const uint2 it = items[item];
+        const WorldInfo wi = B.info[it.x];
+        WorldCounts& wc = B.counts[it.x];
+        narrowMesh<true>(B, P, wi, wc, it.y, B.previous + wi.contactFirst, wc.contactCount, serial, &s_rooms[warp], lane);
+        __syncwarp();
     }
 }
 
@@ -1219,7 +1271,11 @@ template <int Cls>
 __global__ void __launch_bounds__(256) k_collide(const __grid_constant__ Batch B, const __grid_constant__ StepParams P,
                                                  int serial) {
     if (stepAborted(B, serial)) { return; }
-    collideClass<Cls>(B, P, serial);
+    if constexpr (Cls == kClassMesh) {
+        collideMeshPairs(B, P, serial);
+    } else {
+        collideClass<Cls>(B, P, serial);
+    }
 }
 
 // Small batches collide every pair class in one launch, each class's list in turn over the whole grid (the
@@ -1498,7 +1554,7 @@ __device__ __forceinline__ void returnImpulses(const Batch& B, uint32_t slot, DC
     }
 }
 
-constexpr uint32_t kOrderRounds = 64;       // rounds of visitInBodyOrder before one thread takes the rest
+constexpr uint32_t kOrderRounds = 64;       // rounds of visitInBodyOrder at most before one thread takes the rest
 constexpr uint32_t kOrderRoundsMin = 64;    // shorter lists go to one thread at once
 constexpr uint8_t kColorPending = 0xff;
 
@@ -1508,13 +1564,19 @@ constexpr uint8_t kColorPending = 0xff;
 // round so a round's marks replace the last one's). Entries visited in one round share no body, so visit(x)
 // may read and write its own bodies' state without atomics. A result that depends, per body, only on the
 // entries before x at that body (a greedy color, a level) therefore comes out as a pass in list order gives
-// it. After kOrderRounds rounds one thread visits what is left in list order, which keeps that property: the
-// entries visited so far include every entry before them at a shared body. ends(x, a, b) gives an entry's
-// bodies (kNone for one that does not count); firstAt holds a word per body, set to kNone beforehand.
+// it. Once a round visits too few entries to pay for its two passes over the list (a long chain of contacts
+// through a stack), or after kOrderRounds rounds, one thread visits what is left in list order, which keeps
+// that property: the entries visited so far include every entry before them at a shared body. ends(x, a, b)
+// gives an entry's bodies (kNone for one that does not count); firstAt holds a word per body, set to kNone
+// beforehand.
 template <class Ends, class Pending, class Visit>
 static __device__ void visitInBodyOrder(const Group& g, uint32_t n, uint32_t* firstAt, Ends ends, Pending pending,
                                         Visit visit) {
+    __shared__ uint32_t s_visits[kMaxGroups][2];
     if (n >= kOrderRoundsMin && n < (1u << 24)) {
+        // A round costs two passes of n / size entries per thread; one thread takes an entry in about as long.
+        const uint32_t worth = (n + g.size - 1) / g.size + 4;
+        if (g.tid == 0) { s_visits[g.id][0] = 0; }
         for (uint32_t r = 0; r < kOrderRounds; ++r) {
             const uint32_t tag = (kOrderRounds - 1 - r) << 24;
             bool left = false;
@@ -1527,13 +1589,20 @@ static __device__ void visitInBodyOrder(const Group& g, uint32_t n, uint32_t* fi
                 if (b != kNone) { atomicMin(&firstAt[b], tag | x); }
             }
             if (!g.any(left)) { return; }
+            if (g.tid == 0) { s_visits[g.id][(r + 1) & 1] = 0; }
+            uint32_t visited = 0;
             for (uint32_t x = g.tid; x < n; x += g.size) {
                 if (!pending(x)) { continue; }
                 uint32_t a, b;
                 ends(x, a, b);
-                if ((a == kNone || firstAt[a] == (tag | x)) && (b == kNone || firstAt[b] == (tag | x))) { visit(x); }
+                if ((a == kNone || firstAt[a] == (tag | x)) && (b == kNone || firstAt[b] == (tag | x))) {
+                    visit(x);
+                    ++visited;
+                }
             }
+            if (visited) { atomicAdd(&s_visits[g.id][r & 1], visited); }
             g.sync();
+            if (s_visits[g.id][r & 1] < worth) { break; }
         }
     }
     if (g.tid == 0) {
@@ -1966,8 +2035,11 @@ __device__ __forceinline__ float movedThisStep(const DBody& b) {
 // collided once, skipping the triangles its collision at the step's start ruled out while they stay out of
 // reach, and each contact in turn takes the new manifold whose normal is closest to its own; a contact left
 // without one keeps no points (src/world.cpp:1078-1137).
+// Warp: every lane of the warp calls it alike with the warp's room; the lanes collide the triangles together and
+// lane 0 hands the manifolds to the contacts.
+template <bool Warp>
 static __device__ void refreshMeshRun(const Batch& B, const StepParams& P, const WorldInfo& wi, WorldCounts& wc, DContact* run,
-                               int count, float remaining) {
+                               int count, float remaining, MeshWarpRoom* room = nullptr, uint32_t lane = 0) {
     const DBody& a = B.bodies[run[0].bodyA];
     const DBody& b = B.bodies[run[0].bodyB];
     const DShape sa = B.shapes[run[0].shapeA];
@@ -1980,7 +2052,9 @@ static __device__ void refreshMeshRun(const Batch& B, const StepParams& P, const
     }
     Manifold found[kMaxMeshParts];
     int n = 0;
-    if (collideMeshPair(B, P, sa, sb, remaining, found, n, &mb) != kMeshOk) {
+    const int status = collideMeshPair<Warp>(B, P, sa, sb, remaining, found, n, &mb, Warp ? room->found : nullptr, lane);
+    if (Warp && lane != 0) { return; }
+    if (status != kMeshOk) {
         atomicOr(&wc.flags, kDevUnsupported);
         n = 0;
     }
@@ -2610,7 +2684,7 @@ __device__ __forceinline__ void refreshClass(const Batch& B, const StepParams& P
             const int count = (int)(end - ci);
             for (int x = 0; x < count; ++x) { takeImpulsesBack(B, wi, ci + x, run[x]); }
             if (again) {
-                refreshMeshRun(B, P, wi, B.counts[it.x], run, count, remaining);
+                refreshMeshRun<false>(B, P, wi, B.counts[it.x], run, count, remaining);
             } else {
                 for (int x = 0; x < count; ++x) { rebaseContact(B.bodies[run[x].bodyA], B.bodies[run[x].bodyB], run[x]); }
             }
@@ -2626,11 +2700,59 @@ __device__ __forceinline__ void refreshClass(const Batch& B, const StepParams& P
     }
 }
 
+// The fast mesh pairs' contacts, a warp per item (the first contact of a pair's run takes the run), the warp's
+// lanes over the pair's triangles when it is collided again. Launched with at most kMeshWarps warps to a CTA.
+__device__ __forceinline__ void refreshMeshPairs(const Batch& B, const StepParams& P, int sub) {
+    __shared__ MeshWarpRoom s_rooms[kMeshWarps];
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t perCta = min(blockDim.x >> 5, (uint32_t)kMeshWarps);  // warps past the rooms stay idle
+    if (warp >= perCta) { return; }
+    const int n = P.substeps;
+    const uint8_t againFlag = sub == n / 2 ? kFlagFast : kFlagFastSolid;
+    const float remaining = (float)(n - sub) * P.h;
+    const uint32_t items = *(volatile uint32_t*)(B.work + kSlotFastItems + kClassMesh);
+    const uint2* its = B.contactItems + (size_t)kClassMesh * B.contactItemStride;
+    const uint32_t warps = gridDim.x * perCta;
+    for (uint32_t item = blockIdx.x * perCta + warp; item < items; item += warps) {
+        const uint2 it = its[item];
+        const WorldCounts& wc = B.counts[it.x];
+        if (!refreshedAt(wc, sub, n)) { continue; }
+        const WorldInfo wi = B.info[it.x];
+        const uint32_t ci = it.y;
+        if (!contactOk(B, wi, wc, ci, 16)) { continue; }
+        const DContact* cs = B.contacts + wi.contactFirst;
+        // The contacts of a mesh pair share a key and sit together; the first takes the whole run.
+        if (ci > 0 && cs[ci - 1].key == cs[ci].key) { continue; }
+        uint32_t end = ci + 1;
+        while (end < wc.contactCount && cs[end].key == cs[ci].key) { ++end; }
+        DContact* run = B.contacts + wi.contactFirst + ci;
+        const int count = (int)(end - ci);
+        const bool again = (B.cflags[wi.contactFirst + ci] & againFlag) != 0;
+        if (lane == 0) {
+            for (int x = 0; x < count; ++x) { takeImpulsesBack(B, wi, ci + x, run[x]); }
+        }
+        __syncwarp();
+        if (again) {
+            refreshMeshRun<true>(B, P, wi, B.counts[it.x], run, count, remaining, &s_rooms[warp], lane);
+        } else if (lane == 0) {
+            for (int x = 0; x < count; ++x) { rebaseContact(B.bodies[run[x].bodyA], B.bodies[run[x].bodyB], run[x]); }
+        }
+        if (lane == 0) {
+            for (int x = 0; x < count; ++x) { rebuildSolverData(B, wi, ci + x, run[x]); }
+        }
+        __syncwarp();
+    }
+}
+
 template <int Cls>
 __global__ void __launch_bounds__(256) k_refresh(const __grid_constant__ Batch B, const __grid_constant__ StepParams P,
                                                  int sub, int serial) {
     if (stepAborted(B, serial)) { return; }
-    refreshClass<Cls>(B, P, sub);
+    if constexpr (Cls == kClassMesh) {
+        refreshMeshPairs(B, P, sub);
+    } else {
+        refreshClass<Cls>(B, P, sub);
+    }
 }
 
 // Small batches refresh every list in one launch (the lists hold disjoint contacts: a pair's contacts are fast

@@ -193,35 +193,113 @@ TF_HD void meshCorners(const MeshTables& mt, const DMesh& M, int t, Vec3 c[3]) {
     for (int k = 0; k < 3; ++k) { c[k] = mt.verts[M.vFirst + (int)idx[k]]; }
 }
 
-// collideMesh (src/collide3d.cpp:1577-1776) for a sphere or polyhedron: up to kMaxMeshParts manifolds with
-// normals from the mesh, into out. Returns kMeshOk, or why the pair could not be collided exactly.
-TF_HD int collideMesh(const CollideCtx& cx, const DShape& mesh, const Transform& xm, const DShape& other,
-                      const Transform& xo, float margin, const Motion& motion, Manifold* out, int& outCount,
-                      MeshBounds* bounds) {
-    outCount = 0;
+// What one triangle of a mesh pair gives: nothing, a manifold, or a distance that rules it out.
+constexpr int kTriNone = 0, kTriKept = 1, kTriRuledOut = 2;
+
+// Collects a pair's triangle results on one thread, in the tree's visiting order: kept manifolds into found (at
+// most kMaxMeshFound; one more makes the pair kMeshTooMany), ruled-out distances into bounds when it records.
+struct SerialCollect {
+    Manifold* found;
+    int nFound;
+    MeshBounds* bounds;
+    int status;
+
+    template <class Tri>
+    TF_HD bool operator()(const MeshTables& mt, const DMesh& M, const Vec3& lo, const Vec3& hi, Tri&& tri) {
+        return queryMesh(mt, M, lo, hi, [&](int t) {
+            Manifold m;
+            float d = 0.0f;
+            const int r = tri(t, m, d);
+            if (r == kTriKept) {
+                if (nFound >= kMaxMeshFound) {
+                    status = kMeshTooMany;
+                } else {
+                    found[nFound++] = m;
+                }
+            } else if (r == kTriRuledOut) {
+                ruleOut(bounds, t, d, status);
+            }
+        });
+    }
+};
+
+#if defined(__CUDACC__)
+// The same results with a warp's lanes over the triangles: every lane walks the tree alike (the same nodes, so
+// the loads are broadcast), the triangles it finds are dealt to the lanes in visiting order, and each full hand
+// of 32 is collided at once; ballots place the kept manifolds (in found, shared by the warp) and the ruled-out
+// triangles (in bounds->found) in visiting order, as the serial walk stores them. Every lane's nFound, status
+// and bounds count come out equal.
+struct WarpCollect {
+    Manifold* found;
+    int nFound;
+    MeshBounds* bounds;
+    int status;
+    uint32_t lane;
+
+    template <class Tri>
+    __device__ bool operator()(const MeshTables& mt, const DMesh& M, const Vec3& lo, const Vec3& hi, Tri&& tri) {
+        int mine = -1, dealt = 0;
+        const uint32_t below = (1u << lane) - 1u;
+        auto collide = [&]() {
+            Manifold m;
+            float d = 0.0f;
+            const int r = mine >= 0 ? tri(mine, m, d) : kTriNone;
+            const uint32_t kept = __ballot_sync(0xffffffffu, r == kTriKept);
+            if (r == kTriKept) {
+                const int pos = nFound + __popc(kept & below);
+                if (pos < kMaxMeshFound) { found[pos] = m; }
+            }
+            nFound += __popc(kept);
+            if (bounds && bounds->found) {
+                const uint32_t ruled = __ballot_sync(0xffffffffu, r == kTriRuledOut);
+                if (r == kTriRuledOut) {
+                    const int pos = bounds->foundCount + __popc(ruled & below);
+                    if (pos < kMaxMeshBounds) { bounds->found[pos] = TriangleBound{ mine, d }; }
+                }
+                bounds->foundCount += __popc(ruled);
+            }
+            __syncwarp();
+            mine = -1;
+            dealt = 0;
+        };
+        const bool walked = queryMesh(mt, M, lo, hi, [&](int t) {
+            if ((int)lane == dealt) { mine = t; }
+            if (++dealt == 32) { collide(); }
+        });
+        if (dealt > 0) { collide(); }
+        if (nFound > kMaxMeshFound) {
+            status = kMeshTooMany;
+            nFound = kMaxMeshFound;
+        }
+        if (bounds && bounds->found && bounds->foundCount > kMaxMeshBounds) {
+            status = kMeshTooMany;
+            bounds->foundCount = kMaxMeshBounds;
+        }
+        return walked;
+    }
+};
+#endif
+
+// collideMesh (src/collide3d.cpp:1577-1776) for a sphere or polyhedron, up to grouping: every triangle the tree
+// finds near the other shape collided, its result handed to collect in visiting order. Returns kMeshOk, or
+// why the pair could not be collided exactly.
+template <class Collect>
+TF_HD int collideMeshTriangles(const CollideCtx& cx, const DShape& mesh, const Transform& xm, const DShape& other,
+                               const Transform& xo, float margin, const Motion& motion, const MeshBounds* bounds,
+                               Collect& collect) {
     if (mesh.mesh < 0 || other.kind == kHalfSpace || other.kind == kMesh) { return kMeshOk; }
     const MeshTables& mt = cx.mt;
     const DMesh M = mt.meshes[mesh.mesh];
     const Tolerances tol = cx.tol;
     const Transform rel{ unrotate(xm.q, xo.p - xm.p), conjugate(xm.q) * xo.q };
     const float absTol = 0.5f * tol.linearSlop;
-    Manifold found[kMaxMeshFound];
-    int nFound = 0;
-    int status = kMeshOk;
-    auto keep = [&](const Manifold& m) {
-        if (nFound >= kMaxMeshFound) {
-            status = kMeshTooMany;
-            return;
-        }
-        found[nFound++] = m;
-    };
     bool walked;
     if (other.kind == kSphere) {
         const Vec3 center = rel.p;
         const float r = other.radius;
         const Vec3 reach{ r + margin, r + margin, r + margin };
-        walked = queryMesh(mt, M, center - reach, center + reach, [&](int t) {
-            if (outOfReach(bounds, t, margin)) { return; }
+        walked = collect(mt, M, center - reach, center + reach, [&](int t, Manifold& m, float& ruledAt) {
+            if (outOfReach(bounds, t, margin)) { return kTriNone; }
             Vec3 c[3];
             meshCorners(mt, M, t, c);
             const Vec3 n = mt.normals[M.tFirst + t];
@@ -233,7 +311,7 @@ TF_HD int collideMesh(const CollideCtx& cx, const DShape& mesh, const Transform&
             Vec3 normal, surface;
             float sep;
             const bool own = feature != 6 && dist > 0.0f && ownNormal(mt.edges[M.tFirst + t], feature, side);
-            if (!own && dist - fabsf(h) > tol.linearSlop) { return; }
+            if (!own && dist - fabsf(h) > tol.linearSlop) { return kTriNone; }
             if (!own) {
                 normal = side == 0 ? n : -n;
                 sep = fabsf(h) - r;
@@ -244,24 +322,23 @@ TF_HD int collideMesh(const CollideCtx& cx, const DShape& mesh, const Transform&
                 surface = q;
             }
             if (sep > margin) {
-                ruleOut(bounds, t, sep, status);
-                return;
+                ruledAt = sep;
+                return kTriRuledOut;
             }
-            Manifold m;
             m.featKind = kFeatNone;
             m.featA = m.featB = -1;
             m.normal = rotate(xm.q, normal);
             const Vec3 w = apply(xm, (surface + center - normal * r) * 0.5f);
             m.points[0] = MPoint{ w, sep, motion.predict(w, m.normal, sep) };
             m.count = 1;
-            keep(m);
+            return kTriKept;
         });
     } else if (other.kind == kCylinder) {
         const Solid b = cylinderSolid(other, rel);
         const Vec3 reach = cylinderReach(b.axis, b.radius, b.halfHeight) + Vec3{ margin, margin, margin };
         const Convex convexB = convexOf(cx, other);
-        walked = queryMesh(mt, M, b.center - reach, b.center + reach, [&](int t) {
-            if (outOfReach(bounds, t, margin)) { return; }
+        walked = collect(mt, M, b.center - reach, b.center + reach, [&](int t, Manifold& m, float& ruledAt) {
+            if (outOfReach(bounds, t, margin)) { return kTriNone; }
             Vec3 c[3];
             meshCorners(mt, M, t, c);
             const Vec3 n = mt.normals[M.tFirst + t];
@@ -271,15 +348,14 @@ TF_HD int collideMesh(const CollideCtx& cx, const DShape& mesh, const Transform&
             const Convex triangle{ tri.verts, 3, 0.0f, false };
             Separation best;
             if (!separate(a, b, triangle, xm, convexB, xo, xm.q, margin, tol, best)) {
-                ruleOut(bounds, t, best.gap, status);
-                return;
+                ruledAt = best.gap;
+                return kTriRuledOut;
             }
-            Manifold m;
             m.count = 0;
             m.featKind = kFeatNone;
             m.featA = m.featB = -1;
             solidContact(cx.cap, a, b, best.normal, best.gap, xm, margin, tol.linearSlop, motion, m);
-            if (m.count == 0) { return; }
+            if (m.count == 0) { return kTriNone; }
             // An edge or corner without a normal of its own leaves the push to the face.
             if (fabsf(dot(best.normal, n)) < 0.9999f) {
                 Separation front = noSeparation(), back = noSeparation();
@@ -293,20 +369,20 @@ TF_HD int collideMesh(const CollideCtx& cx, const DShape& mesh, const Transform&
                     for (int k = 0; k < m.count; ++k) {
                         const Vec3 p = applyInverse(xm, m.points[k].position);
                         if (m.points[k].separation < best.gap - tol.linearSlop && !overTriangle(c, n, p, tol.linearSlop)) {
-                            return;
+                            return kTriNone;
                         }
                     }
-                    if (m.count == 0) { return; }
+                    if (m.count == 0) { return kTriNone; }
                 }
             }
-            keep(m);
+            return kTriKept;
         });
     } else {
         const FramePoly b = otherFrame(cx.pt, other.poly, rel);
         const Convex convexB = convexOf(cx, other);
         const Vec3 grow{ margin, margin, margin };
-        walked = queryMesh(mt, M, b.lo - grow, b.hi + grow, [&](int t) {
-            if (outOfReach(bounds, t, margin)) { return; }
+        walked = collect(mt, M, b.lo - grow, b.hi + grow, [&](int t, Manifold& m, float& ruledAt) {
+            if (outOfReach(bounds, t, margin)) { return kTriNone; }
             Vec3 c[3];
             meshCorners(mt, M, t, c);
             const Vec3 n = mt.normals[M.tFirst + t];
@@ -315,19 +391,19 @@ TF_HD int collideMesh(const CollideCtx& cx, const DShape& mesh, const Transform&
             const FramePoly a = ownFrame(tri.t, 0);
             const FaceQuery fa = queryFaces(a, b, margin);
             if (fa.separation > margin) {
-                ruleOut(bounds, t, fa.separation, status);
-                return;
+                ruledAt = fa.separation;
+                return kTriRuledOut;
             }
             const FaceQuery fb = queryFaces(b, a, margin);
             if (fb.separation > margin) {
-                ruleOut(bounds, t, fb.separation, status);
-                return;
+                ruledAt = fb.separation;
+                return kTriRuledOut;
             }
             const float reach = maxf(margin, -maxf(fa.separation, fb.separation));
             const EdgeQuery eq = queryTriangleEdges(a, b, reach);
             if (eq.separation > margin) {
-                ruleOut(bounds, t, eq.separation, status);
-                return;
+                ruledAt = eq.separation;
+                return kTriRuledOut;
             }
             // Edges out of reach were skipped, so GJK confirms the shapes come within margin, unless the
             // vertex of b deepest toward the triangle already does.
@@ -341,10 +417,9 @@ TF_HD int collideMesh(const CollideCtx& cx, const DShape& mesh, const Transform&
                 const Vec3 q = closestOnTriangle(c, b.v(deep), feature);
                 if (lengthSquared(b.v(deep) - q) > margin * margin) {
                     const Convex triangle{ tri.verts, 3, 0.0f, false };
-                    if (apart(triangle, xm, convexB, xo, margin)) { return; }
+                    if (apart(triangle, xm, convexB, xo, margin)) { return kTriNone; }
                 }
             }
-            Manifold m;
             m.count = 0;
             m.featKind = kFeatNone;
             m.featA = m.featB = -1;
@@ -355,7 +430,7 @@ TF_HD int collideMesh(const CollideCtx& cx, const DShape& mesh, const Transform&
             } else {
                 faceContact(a, fa.index, b, false, xm, margin, tol.linearSlop, motion, m);
             }
-            if (m.count == 0) { return; }
+            if (m.count == 0) { return kTriNone; }
             // Off the face normal on an edge or corner with no normal of its own, the neighbour takes that
             // direction and this triangle pushes only along its face; where the face is deeper than the
             // shapes overlap, the contact belongs to the neighbour.
@@ -367,22 +442,25 @@ TF_HD int collideMesh(const CollideCtx& cx, const DShape& mesh, const Transform&
                     faceContact(a, fa.index, b, false, xm, margin, tol.linearSlop, motion, m);
                     for (int k = 0; k < m.count; ++k) {
                         const Vec3 p = applyInverse(xm, m.points[k].position);
-                        if (m.points[k].separation < floor && !overTriangle(c, n, p, tol.linearSlop)) { return; }
+                        if (m.points[k].separation < floor && !overTriangle(c, n, p, tol.linearSlop)) { return kTriNone; }
                     }
-                    if (m.count == 0) { return; }
+                    if (m.count == 0) { return kTriNone; }
                 }
             }
             for (int k = 0; k < m.count; ++k) {
                 MPoint& p = m.points[k];
                 p.predicted = motion.predict(p.position, m.normal, p.separation);
             }
-            keep(m);
+            return kTriKept;
         });
     }
-    if (!walked) { return kMeshTooMany; }
-    if (status != kMeshOk) { return status; }
+    return walked ? kMeshOk : kMeshTooMany;
+}
 
-    // Triangles facing the same way share one manifold, under the normal of the deepest of them.
+// Triangles facing the same way share one manifold, under the normal of the deepest of them
+// (src/collide3d.cpp:1746-1776): found in visiting order into at most kMaxMeshParts manifolds.
+TF_HD int groupMeshManifolds(const Manifold* found, int nFound, const Tolerances& tol, Manifold* out, int& outCount) {
+    outCount = 0;
     int8_t owner[kMaxMeshFound];
     for (int i = 0; i < nFound; ++i) { owner[i] = -1; }
     MPoint pts[4 * kMaxMeshFound];
@@ -413,5 +491,38 @@ TF_HD int collideMesh(const CollideCtx& cx, const DShape& mesh, const Transform&
     }
     return kMeshOk;
 }
+
+// collideMesh (src/collide3d.cpp:1577-1776) for a sphere or polyhedron on one thread: up to kMaxMeshParts
+// manifolds with normals from the mesh, into out. Returns kMeshOk, or why the pair could not be collided
+// exactly.
+TF_HD int collideMesh(const CollideCtx& cx, const DShape& mesh, const Transform& xm, const DShape& other,
+                      const Transform& xo, float margin, const Motion& motion, Manifold* out, int& outCount,
+                      MeshBounds* bounds) {
+    outCount = 0;
+    Manifold found[kMaxMeshFound];
+    SerialCollect collect{ found, 0, bounds, kMeshOk };
+    const int walk = collideMeshTriangles(cx, mesh, xm, other, xo, margin, motion, bounds, collect);
+    if (walk != kMeshOk) { return walk; }
+    if (collect.status != kMeshOk) { return collect.status; }
+    return groupMeshManifolds(found, collect.nFound, cx.tol, out, outCount);
+}
+
+#if defined(__CUDACC__)
+// The same with the warp's lanes over the triangles; found is the warp's shared room for kMaxMeshFound
+// manifolds, and each lane passes its own copy of bounds (whose found, if any, the warp shares). The grouping
+// runs on lane 0, whose out and outCount and return value are the pair's; the other lanes return kMeshOk with
+// nothing in out unless the triangles already failed.
+static __device__ int collideMeshWarp(const CollideCtx& cx, const DShape& mesh, const Transform& xm, const DShape& other,
+                               const Transform& xo, float margin, const Motion& motion, Manifold* out, int& outCount,
+                               MeshBounds* bounds, Manifold* found, uint32_t lane) {
+    outCount = 0;
+    WarpCollect collect{ found, 0, bounds, kMeshOk, lane };
+    const int walk = collideMeshTriangles(cx, mesh, xm, other, xo, margin, motion, bounds, collect);
+    if (walk != kMeshOk) { return walk; }
+    if (collect.status != kMeshOk) { return collect.status; }
+    if (lane != 0) { return kMeshOk; }
+    return groupMeshManifolds(found, collect.nFound, cx.tol, out, outCount);
+}
+#endif
 
 }

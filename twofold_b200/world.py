@@ -326,6 +326,18 @@ class Batch:
                   self.lib)
         return gi, gm, gf
 
+    def adjoint_branches(self):
+        """Per world, the branch signature of the last adjoint_forward run (uint64)."""
+        out = np.zeros(len(self.offsets) - 1, np.uint64)
+        abi.check(self.lib.tf_adjoint_branches(self.h, out.ctypes.data), self.lib)
+        return out
+
+    def adjoint_backward_ms(self):
+        """The last backward's recomputation and reverse walk, each summed over its chunks (ms)."""
+        ms = np.zeros(2, np.float32)
+        abi.check(self.lib.tf_adjoint_backward_ms(self.h, ms.ctypes.data), self.lib)
+        return float(ms[0]), float(ms[1])
+
     def adjoint_ms(self):
         ms = np.zeros(2, np.float32)
         abi.check(self.lib.tf_adjoint_elapsed_ms(self.h, ms.ctypes.data), self.lib)
