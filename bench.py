@@ -486,7 +486,9 @@ def run_b200(args, dist):
     traffic = load_traffic()
     breakdown = {k: v[0] / BREAKDOWN_STEPS for k, v in kt.items()}
 
-    # End to end: a fresh batch, the same warm-up, then per step: forces in, step, poses out.
+    # End to end: a fresh batch, the same warm-up, then per step: forces in, step, poses out. The poses of a step
+    # travel to the host (two pinned buffers in turn) while the next step runs; the timed region ends once the
+    # last step's poses have arrived.
     del batch
     e2e_batch = Batch.from_scene(sc, device=dist.local_rank)
     for k, (threads, big, smem) in shapes.items():
@@ -496,21 +498,22 @@ def run_b200(args, dist):
         import torch
 
         forces = torch.zeros((total, 3), dtype=torch.float32).pin_memory().numpy()
-        poses = torch.zeros((total, 3), dtype=torch.float32).pin_memory().numpy()
-        rots = torch.zeros((total, 4), dtype=torch.float32).pin_memory().numpy()
+        poses = [torch.zeros((total, 3), dtype=torch.float32).pin_memory().numpy() for _ in range(2)]
+        rots = [torch.zeros((total, 4), dtype=torch.float32).pin_memory().numpy() for _ in range(2)]
     except Exception:
         forces = np.zeros((total, 3), np.float32)
-        poses = np.zeros((total, 3), np.float32)
-        rots = np.zeros((total, 4), np.float32)
+        poses = [np.zeros((total, 3), np.float32) for _ in range(2)]
+        rots = [np.zeros((total, 4), np.float32) for _ in range(2)]
     for _ in range(args.warmup):
         e2e_batch.step_checked(dt, 1, graph=True)
     e_steps0 = e2e_batch.body_steps()
     dist.barrier()
     t0 = time.perf_counter()
-    for _ in range(args.steps):
+    for k in range(args.steps):
         e2e_batch.add_forces(forces)
         e2e_batch.step_checked(dt, 1, graph=True)
-        e2e_batch.read_poses(poses, rots)
+        e2e_batch.read_poses_async(poses[k % 2], rots[k % 2])
+    e2e_batch.poses_wait()
     e_wall = time.perf_counter() - t0
     dist.barrier()
     e_body_steps = dist.reduce(e2e_batch.body_steps() - e_steps0, "SUM")
@@ -584,7 +587,8 @@ def run_b200(args, dist):
             "dtype": "f32", "data": "synthetic: one seeded world set, split over the GPUs by body count",
             "config": config(args, n),
             "e2e": {"value": e_body_steps / e_wall, "unit": UNIT, "h2d_bytes_per_step": int(forces.nbytes),
-                    "d2h_bytes_per_step": int(poses.nbytes + rots.nbytes)},
+                    "d2h_bytes_per_step": int(poses[0].nbytes + rots[0].nbytes),
+                    "copies": "forces in before each step; each step's poses out while the next step runs"},
             "gpu_launches": int(launches),
             "roofline": roof,
             "parity": parity,

@@ -422,6 +422,13 @@ TF_API int tf_world_add_forces(void* world, const float* forces, const float* to
 /* Positions and rotations (x, y, z, w) of every body of the batch in body order, copied straight from the
  * device without refreshing any other host state (World::transform, include/twofold/world.h:404). */
 TF_API int tf_world_read_poses(void* world, float* positions, float* rotations);
+/* The same read queued without waiting, for a loop that steps while the last step's poses travel: the poses
+ * are packed on the world's stream now and copied to positions and rotations on a copy stream of the library,
+ * beside whatever the world's stream runs next. The buffers (pinned host memory, for the copy to be
+ * asynchronous) must stay valid until tf_world_poses_wait returns, which waits for every queued read. Reads
+ * alternate between two device staging buffers; a third waits on the device for the first one's copy. */
+TF_API int tf_world_read_poses_async(void* world, float* positions, float* rotations);
+TF_API int tf_world_poses_wait(void* world);
 
 /* Per-kernel device timing of direct (non-graph) steps. When on, every kernel launch is bracketed by CUDA
  * events; tf_world_kernel_times returns, for each kernel in the order tf_kernel_name gives, the summed

@@ -138,10 +138,14 @@ def test_model_forward_tracks_the_pipeline():
     assert np.max(np.abs(final[boxes, :3] - s["p"][boxes])) < 0.05
 
 
-def test_adjoint_matches_central_differences_at_1e3_where_no_branch_changes():
-    """64 impact worlds, 120 steps, double precision, h = 1e-3: every entry whose +h and -h runs keep the
-    unperturbed run's branch signature in its world matches the adjoint within 1e-3."""
-    n_worlds, steps, h = 64, 120, 1e-3
+def test_adjoint_matches_differences_on_64_worlds_for_120_steps():
+    """64 impact worlds, 120 steps, double precision. For each checked entry (a sphere's initial velocity, box
+    masses, a world's friction) the central difference starts at h = 1e-3; where its +h and -h runs keep every
+    branch of the unperturbed run (tf_adjoint_branches) that quotient is compared directly, and otherwise the
+    quotient at the first step size from 1e-3 down that agrees with the one before it within 1e-4 (a converged
+    estimate, an order closer than the tolerance). The adjoint matches within 1e-3 every entry whose quotients
+    converge, and at least three quarters of the entries converge."""
+    n_worlds, steps = 64, 120
     sc = scenes.config5(n_worlds=n_worlds, seed=3)
     b = Batch.from_scene(sc)
     s = b.states()
@@ -160,11 +164,11 @@ def test_adjoint_matches_central_differences_at_1e3_where_no_branch_changes():
     base_sig = b.adjoint_branches()
     shape_first = np.concatenate([[0], np.cumsum([len(w.shapes) for w in sc.worlds])])
     entries = []
-    for wi in range(0, n_worlds, 4):
+    for wi in range(0, n_worlds, 8):
         sphere = int(b.offsets[wi]) + 65
         for k in (7, 8, 9):
             entries.append((wi, "initial", (sphere, k), gi[sphere, k]))
-        for box in (1, 30, 64):
+        for box in (1, 64):
             entries.append((wi, "mass", int(b.offsets[wi]) + box, gm[int(b.offsets[wi]) + box]))
         f_idx = np.zeros(n_shapes, bool)
         f_idx[shape_first[wi]:shape_first[wi + 1]] = True
@@ -178,25 +182,37 @@ def test_adjoint_matches_central_differences_at_1e3_where_no_branch_changes():
             m[index] += delta
         else:
             f[index] += delta
-        final = b.adjoint_forward(64, i, m, f)
-        return _loss(final, boxes), b.adjoint_branches()
+        return _loss(b.adjoint_forward(64, i, m, f), boxes), b.adjoint_branches()
 
-    smooth, worst = 0, 0.0
+    kept, converged, report = 0, 0, []
     for wi, which, index, g in entries:
-        lp, sp = run(which, index, h)
-        lm, sm = run(which, index, -h)
-        # The other worlds do not see the change at all.
-        others = np.arange(n_worlds) != wi
-        assert np.array_equal(sp[others], base_sig[others]) and np.array_equal(sm[others], base_sig[others])
-        if sp[wi] != base_sig[wi] or sm[wi] != base_sig[wi]:
+        q = []
+        for h in STEPS_H:
+            lp, sp = run(which, index, h)
+            lm, sm = run(which, index, -h)
+            # Worlds are independent: the others see nothing of the change.
+            others = np.arange(n_worlds) != wi
+            assert np.array_equal(sp[others], base_sig[others]) and np.array_equal(sm[others], base_sig[others])
+            q.append((lp - lm) / (2 * h))
+            if h == STEPS_H[0] and sp[wi] == base_sig[wi] and sm[wi] == base_sig[wi]:
+                kept += 1
+                break
+        fd = None
+        if len(q) == 1:
+            fd = q[0]
+        else:
+            # Converged: two successive quotients agree ten times closer than the tolerance they are held to.
+            for k in range(len(q) - 1):
+                if abs(q[k] - q[k + 1]) <= 0.1 * TOL * max(abs(q[k + 1]), 1e-6):
+                    fd = q[k + 1]
+                    break
+        report.append((wi, which, float(g), None if fd is None else float(fd)))
+        if fd is None:
             continue
-        smooth += 1
-        fd = (lp - lm) / (2 * h)
-        err = abs(g - fd) / max(abs(fd), 1e-6)
-        worst = max(worst, err)
+        converged += 1
         assert abs(g - fd) <= TOL * max(abs(fd), 1e-6) + 1e-9, f"world {wi} {which} {index}: adjoint {g} vs difference {fd}"
-    print(f"{smooth} of {len(entries)} entries kept their branches at h = {h}; worst relative error {worst}")
-    assert smooth >= len(entries) // 4, f"only {smooth} of {len(entries)} entries kept their branches at h = {h}"
+    print(f"{kept} of {len(entries)} entries kept every branch at h = 1e-3; {converged} converged")
+    assert converged >= 3 * len(entries) // 4, report
 
 
 def test_model_step_stays_close_to_the_pipeline_step():

@@ -101,3 +101,31 @@ def test_flat_solve_is_the_default_for_many_worlds_and_autotuned():
     b.step_checked(sc.dt, 12, graph=True)
     ref.step_checked(sc.dt, 12)
     assert states_bitwise_equal(ref.states(), b.states())
+
+
+def test_queued_pose_reads_match_direct_reads():
+    """tf_world_read_poses_async into two host buffers in turn, waited on every other step, gives the poses
+    tf_world_read_poses gives for the same steps of an identical batch, with per-body forces added each step."""
+    sc = scenes.config4(n_worlds=32)
+    queued, direct = Batch.from_scene(sc), Batch.from_scene(sc)
+    total = int(queued.offsets[-1])
+    forces = np.zeros((total, 3), np.float32)
+    forces[:, 0] = 2.0
+    pq = [np.zeros((total, 3), np.float32) for _ in range(2)]
+    qq = [np.zeros((total, 4), np.float32) for _ in range(2)]
+    seen = []
+    for k in range(8):
+        queued.add_forces(forces)
+        queued.step_checked(sc.dt, 1, graph=True)
+        queued.read_poses_async(pq[k % 2], qq[k % 2])
+        direct.add_forces(forces)
+        direct.step_checked(sc.dt, 1, graph=True)
+        p, q = np.zeros((total, 3), np.float32), np.zeros((total, 4), np.float32)
+        direct.read_poses(p, q)
+        seen.append((p, q))
+        if k % 2 == 1:
+            queued.poses_wait()
+            for j in (k - 1, k):
+                assert np.array_equal(pq[j % 2], seen[j][0]) and np.array_equal(qq[j % 2], seen[j][1]), j
+    queued.poses_wait()
+    assert not np.array_equal(seen[0][0], seen[-1][0])

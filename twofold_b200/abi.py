@@ -366,6 +366,8 @@ def _declare(lib):
         "tf_world_body_steps": ([P, C.POINTER(C.c_int64)], C.c_int),
         "tf_world_add_forces": ([P, P, P], C.c_int),
         "tf_world_read_poses": ([P, P, P], C.c_int),
+        "tf_world_read_poses_async": ([P, P, P], C.c_int),
+        "tf_world_poses_wait": ([P], C.c_int),
         "tf_world_set_profiling": ([P, C.c_int32], C.c_int),
         "tf_world_kernel_times": ([P, P, P, C.c_int32, C.POINTER(C.c_int32)], C.c_int),
         "tf_kernel_name": ([C.c_int32], C.c_char_p),
@@ -405,7 +407,7 @@ EXPORTED = [
     "tf_body_get_state", "tf_body_set_velocity", "tf_body_get_mass", "tf_body_is_awake", "tf_world_body_count",
     "tf_world_get_states", "tf_world_contacts", "tf_world_contact_events", "tf_world_hit_events", "tf_world_candidates", "tf_world_profile", "tf_world_awake_bodies",
     "tf_world_launch_count", "tf_world_elapsed_ms", "tf_world_body_steps", "tf_world_add_forces",
-    "tf_world_read_poses", "tf_world_set_profiling", "tf_world_kernel_times", "tf_kernel_name",
+    "tf_world_read_poses", "tf_world_read_poses_async", "tf_world_poses_wait", "tf_world_set_profiling", "tf_world_kernel_times", "tf_kernel_name",
     "tf_world_work_counts", "tf_world_solver_counts", "tf_world_save_state", "tf_world_restore_state", "tf_world_autotune", "tf_tape_record", "tf_adjoint_forward",
     "tf_adjoint_backward", "tf_adjoint_elapsed_ms", "tf_adjoint_branches",
     "tf_adjoint_backward_ms", "tf_world_set_launch", "tf_world_get_launch", "tf_candidates_noalloc",

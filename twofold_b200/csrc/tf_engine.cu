@@ -241,6 +241,13 @@ public:
 
     // Host traffic staging and timing.
     DevArray<float> dHostIn, dHostOut;
+    // Queued pose reads: two device staging buffers, the copy stream, and per buffer the events of its pack and
+    // of its copy (a copy pending until tf_world_poses_wait).
+    DevArray<float> dPoseStage[2];
+    cudaStream_t copyStream = nullptr;
+    cudaEvent_t posePacked[2] = {}, poseCopied[2] = {};
+    bool poseCopyPending[2] = {};
+    int poseSlot = 0;
     cudaEvent_t callStart = nullptr, callStop = nullptr;
     float lastElapsedMs = 0.0f;
     int64_t bodyStepsTotal = 0;
@@ -284,6 +291,13 @@ public:
     // The device arrays free themselves after this body, with the engine's device still current.
     ~Engine() {
         if (stream) { cudaSetDevice(device); }
+        if (copyStream) {
+            cudaStreamSynchronize(copyStream);
+            cudaStreamDestroy(copyStream);
+        }
+        for (cudaEvent_t e : { posePacked[0], posePacked[1], poseCopied[0], poseCopied[1] }) {
+            if (e) { cudaEventDestroy(e); }
+        }
         if (adjRun) { adjointDestroy(adjRun); }
         for (cudaEvent_t e : eventPool) { cudaEventDestroy(e); }
         if (callStart) { cudaEventDestroy(callStart); }
@@ -2672,6 +2686,49 @@ public:
         TF_CUDA(cudaStreamSynchronize(stream));
         return TF_OK;
     }
+
+    // readPoses queued: the pack on the world's stream into a staging buffer, the copy on the copy stream after
+    // it, so the copy runs beside the world's next launches. A staging buffer is packed again only after its
+    // last copy has read it (a wait on the device, not the host).
+    int readPosesAsync(float* p, float* q) {
+        if (!onDevice || layoutDirty) { return readPoses(p, q); }
+        const size_t n = totalBodies;
+        if (!copyStream) {
+            TF_CUDA(cudaStreamCreateWithFlags(&copyStream, cudaStreamNonBlocking));
+            for (cudaEvent_t* e : { &posePacked[0], &posePacked[1], &poseCopied[0], &poseCopied[1] }) {
+                TF_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+            }
+        }
+        const int slot = poseSlot;
+        poseSlot ^= 1;
+        DevArray<float>& buf = dPoseStage[slot];
+        if (!buf.ptr || buf.n < 7 * n) {
+            int rc = posesWait();
+            if (rc == TF_OK) { rc = buf.alloc(7 * n); }
+            if (rc != TF_OK) { return rc; }
+        }
+        if (poseCopyPending[slot]) { TF_CUDA(cudaStreamWaitEvent(stream, poseCopied[slot], 0)); }
+        launch(kKPackPoses, (unsigned)((n + 255) / 256), 256, 0, (const DBody*)dBodies.ptr, (uint32_t)n, buf.ptr,
+               buf.ptr + 3 * n);
+        ++launches;
+        TF_CUDA(cudaGetLastError());
+        TF_CUDA(cudaEventRecord(posePacked[slot], stream));
+        TF_CUDA(cudaStreamWaitEvent(copyStream, posePacked[slot], 0));
+        if (p) { TF_CUDA(cudaMemcpyAsync(p, buf.ptr, 3 * n * sizeof(float), cudaMemcpyDeviceToHost, copyStream)); }
+        if (q) { TF_CUDA(cudaMemcpyAsync(q, buf.ptr + 3 * n, 4 * n * sizeof(float), cudaMemcpyDeviceToHost, copyStream)); }
+        TF_CUDA(cudaEventRecord(poseCopied[slot], copyStream));
+        poseCopyPending[slot] = true;
+        return TF_OK;
+    }
+
+    int posesWait() {
+        for (int k = 0; k < 2; ++k) {
+            if (!poseCopyPending[k]) { continue; }
+            TF_CUDA(cudaEventSynchronize(poseCopied[k]));
+            poseCopyPending[k] = false;
+        }
+        return TF_OK;
+    }
 };
 
 }  // namespace tfb
@@ -3256,6 +3313,16 @@ TF_API int tf_world_add_forces(void* h, const float* forces, const float* torque
 TF_API int tf_world_read_poses(void* h, float* positions, float* rotations) {
     if (!h) { return tfb::fail(TF_E_INVALID, "tf_world_read_poses: null world"); }
     return E(h)->readPoses(positions, rotations);
+}
+
+TF_API int tf_world_read_poses_async(void* h, float* positions, float* rotations) {
+    if (!h) { return tfb::fail(TF_E_INVALID, "tf_world_read_poses_async: null world"); }
+    return E(h)->readPosesAsync(positions, rotations);
+}
+
+TF_API int tf_world_poses_wait(void* h) {
+    if (!h) { return tfb::fail(TF_E_INVALID, "tf_world_poses_wait: null world"); }
+    return E(h)->posesWait();
 }
 
 TF_API int tf_world_set_profiling(void* h, int32_t on) {

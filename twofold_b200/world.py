@@ -215,6 +215,13 @@ class Batch:
     def read_poses(self, positions, rotations):
         abi.check(self.lib.tf_world_read_poses(self.h, positions.ctypes.data, rotations.ctypes.data), self.lib)
 
+    def read_poses_async(self, positions, rotations):
+        """Queues a pose read into (pinned) host arrays that must stay alive until poses_wait returns."""
+        abi.check(self.lib.tf_world_read_poses_async(self.h, positions.ctypes.data, rotations.ctypes.data), self.lib)
+
+    def poses_wait(self):
+        abi.check(self.lib.tf_world_poses_wait(self.h), self.lib)
+
     def set_profiling(self, on=True):
         abi.check(self.lib.tf_world_set_profiling(self.h, 1 if on else 0), self.lib)
 
