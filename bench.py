@@ -260,13 +260,14 @@ def substep_bytes(work):
     return 160 * work["awake"] + 3 * (64 * work["active_contacts"] + 84 * work["active_points"])
 
 
-def load_traffic():
-    """The k_substep DRAM traffic of one ncu capture, with the work counts of the step it was captured on."""
+def load_traffic(mode):
+    """The k_substep DRAM traffic of one ncu capture for the substep's launch mode ("world": the world kernel,
+    "flat": the flat solve), with the work counts of the step it was captured on."""
     path = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(path):
         with open(path) as f:
-            t = json.load(f)
-        if "work" in t and "k_substep_bytes_per_launch" in t:
+            t = json.load(f).get(mode)
+        if t and "work" in t and "k_substep_bytes_per_launch" in t:
             return t
     return None
 
@@ -483,7 +484,8 @@ def run_b200(args, dist):
     sub_ms_total = kt["k_substep"][0]
     sub_launches = max(kt["k_substep"][1], 1)
     achieved = sub_bytes / (sub_ms_total / 1e3) / 1e9
-    traffic = load_traffic()
+    substep_mode = "flat" if shapes.get("substep", (0, 0, 0))[1] == -1 else "world"
+    traffic = load_traffic(substep_mode)
     breakdown = {k: v[0] / BREAKDOWN_STEPS for k, v in kt.items()}
 
     # End to end: a fresh batch, the same warm-up, then per step: forces in, step, poses out. The poses of a step
@@ -579,7 +581,8 @@ def run_b200(args, dist):
             ratio = traffic["k_substep_bytes_per_launch"] / substep_bytes(traffic["work"])
             roof["traffic"] = ratio * sub_bytes / sub_launches
             roof["traffic_over_algorithmic"] = ratio
-            roof["traffic_captured"] = {"bytes_per_launch": traffic["k_substep_bytes_per_launch"],
+            roof["traffic_captured"] = {"substep_mode": substep_mode,
+                                        "bytes_per_launch": traffic["k_substep_bytes_per_launch"],
                                         "work": traffic["work"], "source": traffic.get("source")}
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": n, "steps": args.steps, "warmup": args.warmup,
