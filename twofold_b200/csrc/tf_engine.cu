@@ -295,6 +295,7 @@ public:
             cudaStreamSynchronize(copyStream);
             cudaStreamDestroy(copyStream);
         }
+        if (hostSummary) { cudaFreeHost(hostSummary); }
         for (cudaEvent_t e : { posePacked[0], posePacked[1], poseCopied[0], poseCopied[1] }) {
             if (e) { cudaEventDestroy(e); }
         }
@@ -2328,7 +2329,10 @@ public:
     int events(size_t w, std::vector<TouchEvent>* touch, std::vector<HitRecord>* hits) {
         if (touch) { touch->clear(); }
         if (hits) { hits->clear(); }
-        if (!eventsValid || w >= lastCounts.size() || w >= info.size()) { return TF_OK; }
+        if (!eventsValid) { return TF_OK; }
+        int rc = refreshCounts();
+        if (rc != TF_OK) { return rc; }
+        if (w >= lastCounts.size() || w >= info.size()) { return TF_OK; }
         TF_CUDA(cudaSetDevice(device));
         TF_CUDA(cudaStreamSynchronize(stream));
         const WorldInfo& wi = info[w];
@@ -2616,13 +2620,36 @@ public:
             return fail(TF_E_INVALID, msg);
         }
 #endif
+        // Every step: the worlds' flags and body steps, summed on the device (16 bytes back). The worlds' own
+        // counts come back only when something asks for them (refreshCounts).
+        int rc = dSummary.alloc(4);
+        if (rc != TF_OK) { return rc; }
+        if (!hostSummary) { TF_CUDA(cudaMallocHost(&hostSummary, 4 * sizeof(uint32_t))); }
+        launch(kKStepSummary, 1u, 256u, 0, (const WorldCounts*)dCounts.ptr, (uint32_t)worlds.size(), dSummary.ptr);
+        ++launches;
+        TF_CUDA(cudaGetLastError());
+        TF_CUDA(cudaMemcpyAsync(hostSummary, dSummary.ptr, 3 * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+        TF_CUDA(cudaStreamSynchronize(stream));
+        const uint32_t flags = hostSummary[0];
+        const int64_t bodySteps = (int64_t)((uint64_t)hostSummary[1] | (uint64_t)hostSummary[2] << 32);
+        countsStale = true;
+        eventsValid = true;
+        deviceFlags = flags;
+        bodyStepsTotal = bodyStepsBase + bodySteps;
+        if (flags & kDevUnsupported) { return fail(TF_E_UNSUPPORTED, "the step met a pair this build cannot collide"); }
+        if (flags & kDevNonFinite) { return fail(TF_E_NUMERIC, "a body state became non-finite"); }
+        if (flags & kDevTimeout) { return fail(TF_E_TIMEOUT, "a bounded device wait gave up"); }
+        return TF_OK;
+    }
+
+    // Every world's counts of the last step (lastCounts) and the step profiles' counts, read back on demand.
+    int refreshCounts() {
+        if (!countsStale) { return TF_OK; }
+        TF_CUDA(cudaSetDevice(device));
+        TF_CUDA(cudaStreamSynchronize(stream));
         std::vector<WorldCounts> counts(worlds.size());
         TF_CUDA(cudaMemcpy(counts.data(), dCounts.ptr, worlds.size() * sizeof(WorldCounts), cudaMemcpyDeviceToHost));
-        uint32_t flags = 0;
-        int64_t bodySteps = 0;
         for (size_t w = 0; w < worlds.size(); ++w) {
-            flags |= counts[w].flags;
-            bodySteps += (int64_t)counts[w].bodySteps;
             tf_profile& p = profiles[w];
             p.candidate_pairs = (int32_t)counts[w].candCount;
             p.manifolds = (int32_t)counts[w].contactCount;
@@ -2633,15 +2660,13 @@ public:
             p.touching_contacts = (int32_t)counts[w].touching;
         }
         lastCounts = counts;
-        eventsValid = true;
-        deviceFlags = flags;
-        bodyStepsTotal = bodyStepsBase + bodySteps;
-        if (flags & kDevUnsupported) { return fail(TF_E_UNSUPPORTED, "the step met a pair this build cannot collide"); }
-        if (flags & kDevNonFinite) { return fail(TF_E_NUMERIC, "a body state became non-finite"); }
-        if (flags & kDevTimeout) { return fail(TF_E_TIMEOUT, "a bounded device wait gave up"); }
+        countsStale = false;
         return TF_OK;
     }
     std::vector<WorldCounts> lastCounts;
+    bool countsStale = false;
+    DevArray<uint32_t> dSummary;
+    uint32_t* hostSummary = nullptr;  // pinned
     uint32_t deviceFlags = 0;
     int64_t bodyStepsBase = 0;  // body steps of layouts before the current one
 
@@ -3263,6 +3288,10 @@ TF_API int tf_world_candidates(void* h, int32_t w, uint64_t* out, int32_t cap, i
     if (!h || !count) { return tfb::fail(TF_E_INVALID, "tf_world_candidates: null"); }
     Engine* e = E(h);
     if (w < 0 || w >= (int)e->worlds.size()) { return tfb::fail(TF_E_INVALID, "tf_world_candidates: bad world"); }
+    if (!e->layoutDirty) {
+        const int rc = e->refreshCounts();
+        if (rc != TF_OK) { return rc; }
+    }
     if (e->lastCounts.empty() || e->layoutDirty) {
         *count = 0;
         return TF_OK;
@@ -3281,6 +3310,8 @@ TF_API int tf_world_profile(void* h, int32_t w, tf_profile* out) {
     if (!h || !out) { return tfb::fail(TF_E_INVALID, "tf_world_profile: null"); }
     Engine* e = E(h);
     if (w < 0 || w >= (int)e->worlds.size()) { return tfb::fail(TF_E_INVALID, "tf_world_profile: bad world"); }
+    const int rc = e->refreshCounts();
+    if (rc != TF_OK) { return rc; }
     *out = e->profiles[(size_t)w];
     return TF_OK;
 }
@@ -3288,6 +3319,8 @@ TF_API int tf_world_profile(void* h, int32_t w, tf_profile* out) {
 TF_API int tf_world_awake_bodies(void* h, int64_t* count) {
     if (!h || !count) { return tfb::fail(TF_E_INVALID, "tf_world_awake_bodies: null"); }
     int64_t n = 0;
+    const int rc = E(h)->refreshCounts();
+    if (rc != TF_OK) { return rc; }
     for (const auto& c : E(h)->lastCounts) { n += c.awakeBodies; }
     *count = n;
     return TF_OK;
@@ -3358,6 +3391,8 @@ TF_API int tf_world_work_counts(void* h, int64_t out[6]) {
     Engine* e = E(h);
     for (int k = 0; k < 6; ++k) { out[k] = 0; }
     out[0] = (int64_t)e->totalBodies;
+    const int rc = e->refreshCounts();
+    if (rc != TF_OK) { return rc; }
     for (const auto& c : e->lastCounts) {
         out[1] += c.awakeBodies;
         out[2] += c.candCount;
@@ -3454,6 +3489,8 @@ TF_API int tf_world_solver_counts(void* h, int32_t w, int32_t out[8]) {
     Engine* e = E(h);
     if (w < 0 || w >= (int)e->worlds.size()) { return tfb::fail(TF_E_INVALID, "tf_world_solver_counts: bad world"); }
     for (int k = 0; k < 8; ++k) { out[k] = 0; }
+    const int rc = e->refreshCounts();
+    if (rc != TF_OK) { return rc; }
     if (e->lastCounts.size() != e->worlds.size()) { return TF_OK; }
     const tfb::WorldCounts& c = e->lastCounts[(size_t)w];
     out[0] = (int32_t)c.activeCount;

@@ -11,6 +11,7 @@ const void* finishKernels(int id) {
         case kKTapeRecord: return (const void*)k_tape_record<0>;
         case kKAddForces: return (const void*)k_add_forces<0>;
         case kKPackPoses: return (const void*)k_pack_poses<0>;
+        case kKStepSummary: return (const void*)k_step_summary<0>;
         default: return nullptr;
     }
 }

@@ -3758,6 +3758,33 @@ __global__ void k_add_forces(DBody* bodies, uint32_t n, const float* __restrict_
     if (t) { b.torque += Vec3{ t[3 * i], t[3 * i + 1], t[3 * i + 2] }; }
 }
 
+// What the host checks after every step, from every world's counts in one CTA: the OR of the worlds' flags
+// and the sum of their body steps (out[0] flags, out[1..2] the sum's low and high words).
+template <int Unused = 0>
+__global__ void __launch_bounds__(256) k_step_summary(const WorldCounts* counts, uint32_t nWorlds, uint32_t* out) {
+    __shared__ uint32_t s_flags;
+    __shared__ unsigned long long s_steps;
+    if (threadIdx.x == 0) {
+        s_flags = 0;
+        s_steps = 0;
+    }
+    __syncthreads();
+    uint32_t flags = 0;
+    unsigned long long steps = 0;
+    for (uint32_t w = threadIdx.x; w < nWorlds; w += blockDim.x) {
+        flags |= counts[w].flags;
+        steps += counts[w].bodySteps;
+    }
+    atomicOr(&s_flags, flags);
+    atomicAdd(&s_steps, steps);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        out[0] = s_flags;
+        out[1] = (uint32_t)s_steps;
+        out[2] = (uint32_t)(s_steps >> 32);
+    }
+}
+
 template <int Unused = 0>
 __global__ void k_pack_poses(const DBody* bodies, uint32_t n, float* __restrict__ p, float* __restrict__ q) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;

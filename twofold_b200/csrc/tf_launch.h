@@ -27,6 +27,7 @@ enum KernelId : int {
     kKTapeRecord,
     kKAddForces,
     kKPackPoses,
+    kKStepSummary,
     kKSubstepFlat,
     kKSubstepFlatJoints,
     kKernelIds
