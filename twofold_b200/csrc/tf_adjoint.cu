@@ -390,45 +390,30 @@ __device__ __forceinline__ CData<T> loadContact(const TapeContact& c) {
 
 enum Op : int { kWarm = 0, kBias = 1, kRelax = 2, kRestitute = 3 };
 
-// What a contact operation reads from its bodies and points, logged before it runs.
-template <class T>
-struct CallIn {
-    V3<T> va, wa, vb, wb;
-    PointState<T> p[4];
-};
-template <class T>
-__host__ __device__ constexpr int callWords();
-// Per row of a solve (up to 8: a normal and a friction row per point): the velocities and the point state it
-// started from, logged during the recomputation so that the reverse pass need not replay the operation.
-constexpr int kRowWords = 17;
-template <class T>
-__device__ __forceinline__ void writeRow(T* log, int r, const V3<T>& va, const V3<T>& wa, const V3<T>& vb, const V3<T>& wb,
-                                         const PointState<T>& p) {
-    T* o = log + 32 + r * kRowWords;
-    st3(o, va), st3(o + 3, wa), st3(o + 6, vb), st3(o + 9, wb);
-    o[12] = p.n;
-    st3(o + 13, p.t);
-    o[16] = p.maxN;
-}
-template <class T>
-__host__ __device__ constexpr int callWords() { return 12 + 4 * 5 + kRowWords * 8; }
+// The record a contact operation leaves for its reverse, kCallWords values: what the reverse cannot rebuild
+// from the step's constants (axes, inverse masses and displacements are rebuilt).
+//   [0, 20)  each point's state before the operation: normal impulse, tangent impulse (3), largest normal impulse
+//   [20, 24) each normal row's (or restitution row's) approach speed along the normal, by point
+//   [24, 36) each friction row's speeds along the two tangents and the normal impulse that bounds it, by row
+// A color's records are consecutive, so the reverse walk copies a color's batch to shared memory in one go.
+constexpr int kCallWords = 36;
+constexpr int kSpeedAt = 20;
+constexpr int kFrictionAt = 24;
 
 template <class T>
-__device__ __forceinline__ void writeCall(T* log, const SBody<T>& a, const SBody<T>& b, const PointState<T>* p) {
-    st3(log, a.v), st3(log + 3, a.w), st3(log + 6, b.v), st3(log + 9, b.w);
+__device__ __forceinline__ void writeCall(T* log, const PointState<T>* p) {
     for (int i = 0; i < 4; ++i) {
-        log[12 + 5 * i] = p[i].n;
-        st3(log + 13 + 5 * i, p[i].t);
-        log[16 + 5 * i] = p[i].maxN;
+        log[5 * i] = p[i].n;
+        st3(log + 5 * i + 1, p[i].t);
+        log[5 * i + 4] = p[i].maxN;
     }
 }
 template <class T>
-__device__ __forceinline__ void readCall(const T* log, SBody<T>& a, SBody<T>& b, PointState<T>* p) {
-    a.v = ld3(log), a.w = ld3(log + 3), b.v = ld3(log + 6), b.w = ld3(log + 9);
+__device__ __forceinline__ void readCall(const T* log, PointState<T>* p) {
     for (int i = 0; i < 4; ++i) {
-        p[i].n = log[12 + 5 * i];
-        p[i].t = ld3(log + 13 + 5 * i);
-        p[i].maxN = log[16 + 5 * i];
+        p[i].n = log[5 * i];
+        p[i].t = ld3(log + 5 * i + 1);
+        p[i].maxN = log[5 * i + 4];
     }
 }
 
@@ -439,7 +424,8 @@ __device__ __forceinline__ void readCall(const T* log, SBody<T>& a, SBody<T>& b,
 // a running maximum, decides only whether a point restitutes, which the restitution bits hold.)
 template <class T>
 __device__ __forceinline__ T normalRow(const Model<T>& M, SBody<T>& a, SBody<T>& b, const CData<T>& c, int i,
-                                       PointState<T>& p, bool useBias, const Softness<T>& soft, uint32_t* br = nullptr) {
+                                       PointState<T>& p, bool useBias, const Softness<T>& soft, uint32_t* br = nullptr,
+                                       T* speedOut = nullptr) {
     const Axis<T> x = makeAxis(a, b, c.ra[i], c.rb[i], c.n);
     const V3<T> d = b.dp - a.dp + rotate(b.dq, c.rb[i]) - rotate(a.dq, c.ra[i]);
     const T sep = dot(d, c.n) + c.adjSep[i];
@@ -455,6 +441,7 @@ __device__ __forceinline__ T normalRow(const Model<T>& M, SBody<T>& a, SBody<T>&
         is = soft.impulseScale;
     }
     const T vn = speedAlong(a, b, x);
+    if (speedOut) { *speedOut = vn; }
     const T imp = -x.mass * ms * (vn + bias) - is * p.n;
     const T total = fmax(p.n + imp, T(0));
     const T delta = total - p.n;
@@ -467,7 +454,7 @@ __device__ __forceinline__ T normalRow(const Model<T>& M, SBody<T>& a, SBody<T>&
 
 template <class T>
 __device__ __forceinline__ void normalRowAdj(const Model<T>& M, const SBody<T>& a, const SBody<T>& b, const CData<T>& c,
-                                             int i, const PointState<T>& p0, bool useBias, const Softness<T>& soft,
+                                             int i, const PointState<T>& p0, T vn, bool useBias, const Softness<T>& soft,
                                              BodyAdj<T>& ga, BodyAdj<T>& gb, PointState<T>& gp) {
     const Axis<T> x = makeAxis(a, b, c.ra[i], c.rb[i], c.n);
     const V3<T> d = b.dp - a.dp + rotate(b.dq, c.rb[i]) - rotate(a.dq, c.ra[i]);
@@ -484,7 +471,6 @@ __device__ __forceinline__ void normalRowAdj(const Model<T>& M, const SBody<T>& 
         ms = soft.massScale;
         is = soft.impulseScale;
     }
-    const T vn = speedAlong(a, b, x);
     const T imp = -x.mass * ms * (vn + bias) - is * p0.n;
     const T total = fmax(p0.n + imp, T(0));
     const T delta = total - p0.n;
@@ -523,12 +509,14 @@ __device__ __forceinline__ void normalRowAdj(const Model<T>& M, const SBody<T>& 
 // The friction rows of point i (src/solver.cpp:393-418).
 template <class T>
 __device__ __forceinline__ void frictionRow(SBody<T>& a, SBody<T>& b, const CData<T>& c, int i, PointState<T>& p, T mu,
-                                            uint32_t* br = nullptr) {
+                                            uint32_t* br = nullptr, T* rowOut = nullptr) {
     const Axis<T> x1 = makeAxis(a, b, c.ra[i], c.rb[i], c.t1);
     const Axis<T> x2 = makeAxis(a, b, c.ra[i], c.rb[i], c.t2);
     const T old1 = dot(p.t, c.t1), old2 = dot(p.t, c.t2);
-    T f1 = old1 - x1.mass * speedAlong(a, b, x1);
-    T f2 = old2 - x2.mass * speedAlong(a, b, x2);
+    const T s1 = speedAlong(a, b, x1), s2 = speedAlong(a, b, x2);
+    if (rowOut) { rowOut[0] = s1, rowOut[1] = s2, rowOut[2] = p.n; }
+    T f1 = old1 - x1.mass * s1;
+    T f2 = old2 - x2.mass * s2;
     const T limit = mu * p.n;
     const T mag = sqrtT(f1 * f1 + f2 * f2);
     if (br) { *br = (x1.on ? 1u : 0u) | (x2.on ? 2u : 0u) | (mag > limit ? 4u : 0u) | (mag > T(0) ? 8u : 0u) | 32u; }
@@ -542,16 +530,18 @@ __device__ __forceinline__ void frictionRow(SBody<T>& a, SBody<T>& b, const CDat
     push(a, b, x2, f2 - old2);
 }
 
+// The reverse of the friction rows of point i: t0 is the point's tangent impulse before them, row[0..2] their
+// logged speeds along the two tangents and the normal impulse that bounds them.
 template <class T>
 __device__ __forceinline__ void frictionRowAdj(const SBody<T>& a, const SBody<T>& b, const CData<T>& c, int i,
-                                               const PointState<T>& p0, T mu, BodyAdj<T>& ga, BodyAdj<T>& gb,
+                                               V3<T> t0, const T* row, T mu, BodyAdj<T>& ga, BodyAdj<T>& gb,
                                                PointState<T>& gp, T& muG) {
     const Axis<T> x1 = makeAxis(a, b, c.ra[i], c.rb[i], c.t1);
     const Axis<T> x2 = makeAxis(a, b, c.ra[i], c.rb[i], c.t2);
-    const T old1 = dot(p0.t, c.t1), old2 = dot(p0.t, c.t2);
-    const T s1 = speedAlong(a, b, x1), s2 = speedAlong(a, b, x2);
+    const T old1 = dot(t0, c.t1), old2 = dot(t0, c.t2);
+    const T s1 = row[0], s2 = row[1], pn = row[2];
     const T f1 = old1 - x1.mass * s1, f2 = old2 - x2.mass * s2;
-    const T limit = mu * p0.n;
+    const T limit = mu * pn;
     const T mag = sqrtT(f1 * f1 + f2 * f2);
     // With no friction allowed (limit 0) the row adds nothing whatever f is, also at f = 0 where the forward
     // takes the unclamped branch with the same result: the derivative is that of the clamp.
@@ -573,7 +563,7 @@ __device__ __forceinline__ void frictionRowAdj(const SBody<T>& a, const SBody<T>
         const T magG = -scaleG * limit / (mag * mag);
         f1G += magG * f1 / mag;
         f2G += magG * f2 / mag;
-        muG += limitG * p0.n;
+        muG += limitG * pn;
         gp.n += limitG * mu;
     } else if (clamp) {
         f1G = 0;
@@ -596,9 +586,10 @@ __device__ __forceinline__ bool restitutes(const Model<T>& M, const CData<T>& c,
 
 template <class T>
 __device__ __forceinline__ void restituteRow(const Model<T>& M, SBody<T>& a, SBody<T>& b, const CData<T>& c, int i,
-                                             PointState<T>& p, uint32_t* br = nullptr) {
+                                             PointState<T>& p, uint32_t* br = nullptr, T* speedOut = nullptr) {
     const Axis<T> x = makeAxis(a, b, c.ra[i], c.rb[i], c.n);
     const T vn = speedAlong(a, b, x);
+    if (speedOut) { *speedOut = vn; }
     const T imp = -x.mass * (vn + c.restitution * c.relVel[i]);
     const T total = fmax(p.n + imp, T(0));
     const T delta = total - p.n;
@@ -610,10 +601,9 @@ __device__ __forceinline__ void restituteRow(const Model<T>& M, SBody<T>& a, SBo
 
 template <class T>
 __device__ __forceinline__ void restituteRowAdj(const Model<T>& M, const SBody<T>& a, const SBody<T>& b, const CData<T>& c,
-                                                int i, const PointState<T>& p0, BodyAdj<T>& ga, BodyAdj<T>& gb,
+                                                int i, const PointState<T>& p0, T vn, BodyAdj<T>& ga, BodyAdj<T>& gb,
                                                 PointState<T>& gp) {
     const Axis<T> x = makeAxis(a, b, c.ra[i], c.rb[i], c.n);
-    const T vn = speedAlong(a, b, x);
     const T imp = -x.mass * (vn + c.restitution * c.relVel[i]);
     const T total = fmax(p0.n + imp, T(0));
     const T delta = total - p0.n;
@@ -644,9 +634,11 @@ __device__ __forceinline__ unsigned long long branchHash(unsigned long long tag,
     return z ^ (z >> 31);
 }
 
+// rec, when not null, is the operation's record (kCallWords values; the caller has written the points' state
+// to it): the rows add their speeds.
 template <class T>
 __device__ void contactOp(const Model<T>& M, int op, SBody<T>& a, SBody<T>& b, const CData<T>& c, PointState<T>* p,
-                          T mu, T* rowLog = nullptr, unsigned long long* sig = nullptr, unsigned long long tag = 0) {
+                          T mu, T* rec = nullptr, unsigned long long* sig = nullptr, unsigned long long tag = 0) {
     const Softness<T> soft = (!a.moves || !b.moves) ? M.staticSoft : M.contactSoft;
     const int n = c.count;
     uint32_t bits = 0;
@@ -666,109 +658,61 @@ __device__ void contactOp(const Model<T>& M, int op, SBody<T>& a, SBody<T>& b, c
         if (c.restitution == T(0)) { return; }
         for (int i = 0; i < n; ++i) {
             bits = 128u;
-            if (restitutes(M, c, i, p[i])) { restituteRow(M, a, b, c, i, p[i], br); }
+            if (restitutes(M, c, i, p[i])) { restituteRow(M, a, b, c, i, p[i], br, rec ? rec + kSpeedAt + i : nullptr); }
             if (sig) { *sig += branchHash(tag, (uint32_t)i, bits); }
         }
         return;
     }
     const bool useBias = op == kBias;
     for (int i = 0; i < n; ++i) {
-        if (rowLog) { writeRow(rowLog, i, a.v, a.w, b.v, b.w, p[i]); }
-        normalRow(M, a, b, c, i, p[i], useBias, soft, br);
+        normalRow(M, a, b, c, i, p[i], useBias, soft, br, rec ? rec + kSpeedAt + i : nullptr);
         if (sig) { *sig += branchHash(tag, (uint32_t)i, bits); }
     }
     // Friction forward in the biased pass and backward in the relax pass; row n + j is the j-th friction row.
     for (int j = 0; j < n; ++j) {
         const int i = useBias ? j : n - 1 - j;
-        if (rowLog) { writeRow(rowLog, n + j, a.v, a.w, b.v, b.w, p[i]); }
-        frictionRow(a, b, c, i, p[i], mu, br);
+        frictionRow(a, b, c, i, p[i], mu, br, rec ? rec + kFrictionAt + 3 * j : nullptr);
         if (sig) { *sig += branchHash(tag, (uint32_t)(n + j), bits); }
     }
 }
 
-// The same operation in reverse: replays it from its logged inputs to have every row's input, then walks the
-// rows backwards. ga, gb, gp hold the adjoints after the operation on entry and before it on return.
+// The same operation in reverse, from its record: each row's input that the reverse needs is the points' state
+// before the operation (a point's rows of one kind run once, so each row starts from it, the friction rows with
+// the normal impulse logged beside them) and the logged speeds. ga, gb, gp hold the adjoints after the operation
+// on entry and before it on return. Velocities of a and b are not read.
 template <class T>
-__device__ void contactOpAdj(const Model<T>& M, int op, const SBody<T>& a0, const SBody<T>& b0, const CData<T>& c,
+__device__ void contactOpAdj(const Model<T>& M, int op, const SBody<T>& a, const SBody<T>& b, const CData<T>& c,
                              const PointState<T>* p0, T mu, BodyAdj<T>& ga, BodyAdj<T>& gb, PointState<T>* gp, T& muG,
-                             const T* rowLog) {
-    const Softness<T> soft = (!a0.moves || !b0.moves) ? M.staticSoft : M.contactSoft;
+                             const T* rec) {
+    const Softness<T> soft = (!a.moves || !b.moves) ? M.staticSoft : M.contactSoft;
     const int n = c.count;
     if (op == kWarm) {
         for (int i = 0; i < n; ++i) {
-            const Axis<T> xn = makeAxis(a0, b0, c.ra[i], c.rb[i], c.n);
-            const Axis<T> x1 = makeAxis(a0, b0, c.ra[i], c.rb[i], c.t1);
-            const Axis<T> x2 = makeAxis(a0, b0, c.ra[i], c.rb[i], c.t2);
+            const Axis<T> xn = makeAxis(a, b, c.ra[i], c.rb[i], c.n);
+            const Axis<T> x1 = makeAxis(a, b, c.ra[i], c.rb[i], c.t1);
+            const Axis<T> x2 = makeAxis(a, b, c.ra[i], c.rb[i], c.t2);
             const T l1 = dot(p0[i].t, c.t1), l2 = dot(p0[i].t, c.t2);
-            gp[i].n += pushAdj(a0, b0, xn, p0[i].n, ga, gb);
-            const T g1 = pushAdj(a0, b0, x1, l1, ga, gb);
-            const T g2 = pushAdj(a0, b0, x2, l2, ga, gb);
+            gp[i].n += pushAdj(a, b, xn, p0[i].n, ga, gb);
+            const T g1 = pushAdj(a, b, x1, l1, ga, gb);
+            const T g2 = pushAdj(a, b, x2, l2, ga, gb);
             gp[i].t = gp[i].t + c.t1 * g1 + c.t2 * g2;
         }
         return;
     }
-    if (op != kRestitute) {
-        // A solve: its rows' inputs were logged when the step was recomputed; walk them backwards.
-        const bool useBias = op == kBias;
-        SBody<T> a = a0, b = b0;
-        for (int r = 2 * n - 1; r >= 0; --r) {
-            const T* o = rowLog + 32 + r * kRowWords;
-            a.v = ld3(o), a.w = ld3(o + 3), b.v = ld3(o + 6), b.w = ld3(o + 9);
-            const PointState<T> pr{ o[12], ld3(o + 13), o[16] };
-            if (r < n) {
-                normalRowAdj(M, a, b, c, r, pr, useBias, soft, ga, gb, gp[r]);
-            } else {
-                const int j = r - n;
-                const int i = useBias ? j : n - 1 - j;
-                frictionRowAdj(a, b, c, i, pr, mu, ga, gb, gp[i], muG);
-            }
+    if (op == kRestitute) {
+        if (c.restitution == T(0)) { return; }
+        for (int i = n - 1; i >= 0; --i) {
+            if (restitutes(M, c, i, p0[i])) { restituteRowAdj(M, a, b, c, i, p0[i], rec[kSpeedAt + i], ga, gb, gp[i]); }
         }
         return;
     }
-    // Restitution: replay the operation from its logged inputs to have every row's input (the rest of the
-    // bodies' state is constant over it), then walk the rows backwards.
-    constexpr int kMaxRows = 8;
-    struct Row {
-        V3<T> va, wa, vb, wb;
-        PointState<T> p;
-        int point, kind;  // kind 0 normal, 1 friction, 2 restitution
-    };
-    Row rowIn[kMaxRows];
-    int rows = 0;
-    SBody<T> a = a0, b = b0;
-    PointState<T> p[4];
-    for (int i = 0; i < 4; ++i) { p[i] = p0[i]; }
-    auto keep = [&](int i, int kind) { rowIn[rows++] = Row{ a.v, a.w, b.v, b.w, p[i], i, kind }; };
-    if (op == kRestitute) {
-        if (c.restitution == T(0)) { return; }
-        for (int i = 0; i < n; ++i) {
-            if (!restitutes(M, c, i, p[i])) { continue; }
-            keep(i, 2);
-            restituteRow(M, a, b, c, i, p[i]);
-        }
-    } else {
-        const bool useBias = op == kBias;
-        for (int i = 0; i < n; ++i) {
-            keep(i, 0);
-            normalRow(M, a, b, c, i, p[i], useBias, soft);
-        }
-        for (int j = 0; j < n; ++j) {
-            const int i = useBias ? j : n - 1 - j;
-            keep(i, 1);
-            frictionRow(a, b, c, i, p[i], mu);
-        }
+    const bool useBias = op == kBias;
+    for (int j = n - 1; j >= 0; --j) {
+        const int i = useBias ? j : n - 1 - j;
+        frictionRowAdj(a, b, c, i, p0[i].t, rec + kFrictionAt + 3 * j, mu, ga, gb, gp[i], muG);
     }
-    for (int r = rows - 1; r >= 0; --r) {
-        const Row& R = rowIn[r];
-        a.v = R.va, a.w = R.wa, b.v = R.vb, b.w = R.wb;
-        const int i = R.point;
-        if (R.kind == 0) {
-            normalRowAdj(M, a, b, c, i, R.p, op == kBias, soft, ga, gb, gp[i]);
-        } else if (R.kind == 1) {
-            frictionRowAdj(a, b, c, i, R.p, mu, ga, gb, gp[i], muG);
-        } else {
-            restituteRowAdj(M, a, b, c, i, R.p, ga, gb, gp[i]);
-        }
+    for (int i = n - 1; i >= 0; --i) {
+        normalRowAdj(M, a, b, c, i, p0[i], rec[kSpeedAt + i], useBias, soft, ga, gb, gp[i]);
     }
 }
 
@@ -779,6 +723,24 @@ __device__ __forceinline__ void prefetchRange(const T* from, const T* to, uint32
     for (const char* p = reinterpret_cast<const char*>(from) + 128 * lane; p < end; p += 128 * 32) {
         asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
     }
+}
+
+// Records a stage buffer of the reverse walk holds: one color's batch (each warp has two buffers, one being
+// filled while the other is read).
+template <class T>
+__host__ __device__ constexpr int stageCalls() { return sizeof(T) == 4 ? 64 : 32; }
+
+// Copies `words` values (whole 16-byte pieces, both addresses 16-byte aligned) from global to shared memory
+// with asynchronous copies spread over the warp's lanes, as one commit group of each lane.
+template <class T>
+__device__ __forceinline__ void copyToShared(T* dst, const T* src, uint32_t words, uint32_t lane) {
+    const uint32_t pieces = words * (uint32_t)sizeof(T) / 16u;
+    const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
+    const char* from = reinterpret_cast<const char*>(src);
+    for (uint32_t k = lane; k < pieces; k += 32) {
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d + 16u * k), "l"(from + 16u * k) : "memory");
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
 }
 
 // ---------------------------------------------------------------------------------------------------------
@@ -909,8 +871,9 @@ __device__ void stepWorld(const Model<T>& M, const Slot<T>& W, int step, uint32_
         PointState<T>* p = W.points + (size_t)(cf + ci) * 4;
         PointState<T> ps[4];
         for (int i = 0; i < 4; ++i) { ps[i] = p[i]; }
-        if (log) { writeCall(log + at * callWords<T>(), a, b, ps); }
-        contactOp(M, op, a, b, c, ps, contactFriction(M, V, tc), log ? log + at * callWords<T>() : (T*)nullptr, sig,
+        T* rec = log ? log + at * kCallWords : nullptr;
+        if (rec) { writeCall(rec, ps); }
+        contactOp(M, op, a, b, c, ps, contactFriction(M, V, tc), rec, sig,
                   (unsigned long long)step << 40 ^ at << 2 ^ (unsigned long long)op);
         for (int i = 0; i < 4; ++i) { p[i] = ps[i]; }
         if (a.moves) {
@@ -986,10 +949,12 @@ __device__ void stepWorld(const Model<T>& M, const Slot<T>& W, int step, uint32_
 
 // Reverse of one world's step: adjoints of the state at the step's end in M.stateAdj become those at its start.
 // Needs the log and integLog that stepWorld wrote for this step, and the bodies' dp/dq of every substep, which
-// it recomputes by replaying the integration from the checkpoint as it goes back.
+// it recomputes by replaying the integration from the checkpoint as it goes back. stage: the warp's two
+// shared-memory buffers of stageCalls<T>() records each, or null to read every record from the log.
 template <class T>
 __device__ void stepWorldAdj(const Model<T>& M, const Slot<T>& W, int step, uint32_t w, const T* in, const T* log,
-                             const T* integLog, uint64_t calls) {
+                             const T* integLog, uint64_t calls, T* stage) {
+    constexpr int kStage = stageCalls<T>();
     const uint32_t lane = threadIdx.x & 31;
     const WorldView V = viewOf(M.S, step, w);
     const int n = M.S.substeps;
@@ -1026,13 +991,14 @@ __device__ void stepWorldAdj(const Model<T>& M, const Slot<T>& W, int step, uint
         __syncwarp();
     };
     uint64_t cursor = calls;  // one past the last call of the step
-    auto opAdj = [&](int op, uint32_t ci, uint64_t at) {
+    auto opAdj = [&](int op, uint32_t ci, const T* rec) {
         const TapeContact& tc = V.contacts[ci];
         const CData<T> c = loadContact<T>(tc);
         const uint32_t ga = V.bodyFirst + tc.a, gb = V.bodyFirst + tc.b;
         SBody<T> a, b;
         PointState<T> p0[4];
-        readCall(log + at * callWords<T>(), a, b, p0);
+        readCall(rec, p0);
+        a.v = a.w = b.v = b.w = zeroV<T>();  // the reverse reads no velocity
         a.dp = ld3(W.dp + 3 * (size_t)ga), a.dq = ld4(W.dq + 4 * (size_t)ga), a.im = W.invM[ga];
         a.I = ldM(W.invI + 9 * (size_t)ga), a.moves = movesIn(M, V, ga);
         b.dp = ld3(W.dp + 3 * (size_t)gb), b.dq = ld4(W.dq + 4 * (size_t)gb), b.im = W.invM[gb];
@@ -1050,7 +1016,7 @@ __device__ void stepWorldAdj(const Model<T>& M, const Slot<T>& W, int step, uint
         for (int i = 0; i < 4; ++i) { g4[i] = gp[i]; }
         T muG = 0;
         const T mu = contactFriction(M, V, tc);
-        contactOpAdj(M, op, a, b, c, p0, mu, gA, gB, g4, muG, log + at * callWords<T>());
+        contactOpAdj(M, op, a, b, c, p0, mu, gA, gB, g4, muG, rec);
         for (int i = 0; i < 4; ++i) { gp[i] = g4[i]; }
         auto put = [&](bool moves, uint32_t g, T* s, const BodyAdj<T>& G) {
             if (moves) {
@@ -1087,19 +1053,39 @@ __device__ void stepWorldAdj(const Model<T>& M, const Slot<T>& W, int step, uint
             if (L.start) {
                 const uint32_t first = L.start[0];
                 cursor -= L.start[L.count] - first;
-                for (int k = (int)L.count - 1; k >= 0; --k) {
-                    // The next color's log records come from far memory: ask for them while this color runs.
-                    if (k > 0) {
-                        prefetchRange(log + (cursor + (L.start[k - 1] - first)) * callWords<T>(),
-                                      log + (cursor + (L.start[k] - first)) * callWords<T>(), lane);
+                // Color k's records, consecutive in the log. A color that fits a stage buffer is copied to shared
+                // memory while the color before it in the walk runs; a larger one is read where it lies.
+                auto records = [&](int k) { return log + (cursor + (L.start[k] - first)) * kCallWords; };
+                auto staged = [&](int k) { return stage != nullptr && L.start[k + 1] - L.start[k] <= (uint32_t)kStage; };
+                auto fetch = [&](int k, int buffer) {
+                    if (staged(k)) {
+                        copyToShared(stage + buffer * kStage * kCallWords, records(k), (L.start[k + 1] - L.start[k]) * kCallWords, lane);
+                    } else {
+                        prefetchRange(records(k), records(k + 1), lane);
                     }
-                    for (uint32_t x = L.start[k] + lane; x < L.start[k + 1]; x += 32) { opAdj(op, L.list[x], cursor + (x - first)); }
+                    // Its contacts are read one per lane: ask for their lines too.
+                    for (uint32_t x = L.start[k] + lane; x < L.start[k + 1]; x += 32) {
+                        const char* tc = reinterpret_cast<const char*>(V.contacts + L.list[x]);
+                        asm volatile("prefetch.global.L1 [%0];" ::"l"(tc));
+                        asm volatile("prefetch.global.L1 [%0];" ::"l"(tc + sizeof(TapeContact) - 1));
+                    }
+                };
+                if (L.count > 0) { fetch((int)L.count - 1, 0); }
+                for (int k = (int)L.count - 1; k >= 0; --k) {
+                    const int buffer = ((int)L.count - 1 - k) & 1;
+                    asm volatile("cp.async.wait_all;" ::: "memory");
+                    __syncwarp();
+                    if (k > 0) { fetch(k - 1, buffer ^ 1); }
+                    const T* base = staged(k) ? stage + buffer * kStage * kCallWords : records(k);
+                    for (uint32_t x = L.start[k] + lane; x < L.start[k + 1]; x += 32) {
+                        opAdj(op, L.list[x], base + (x - L.start[k]) * kCallWords);
+                    }
                     __syncwarp();
                 }
             } else {
                 cursor -= L.count;
                 if (lane == 0) {
-                    for (int x = (int)L.count - 1; x >= 0; --x) { opAdj(op, L.list[x], cursor + (uint64_t)x); }
+                    for (int x = (int)L.count - 1; x >= 0; --x) { opAdj(op, L.list[x], log + (cursor + (uint64_t)x) * kCallWords); }
                 }
                 __syncwarp();
             }
@@ -1222,10 +1208,15 @@ __global__ void __launch_bounds__(128) k_model_recompute(const __grid_constant__
 }
 
 template <class T>
+__host__ __device__ constexpr size_t stageBytesPerWarp() { return 2 * (size_t)stageCalls<T>() * kCallWords * sizeof(T); }
+
+template <class T>
 __global__ void __launch_bounds__(128) k_model_reverse(const __grid_constant__ Model<T> M, int first, int count,
-                                                       uint32_t slotBase) {
+                                                       uint32_t slotBase, int staged) {
+    extern __shared__ __align__(16) unsigned char stageArea[];
     const uint32_t w = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
     if (w >= (uint32_t)M.S.nWorlds) { return; }
+    T* stage = staged ? reinterpret_cast<T*>(stageArea + (threadIdx.x / 32) * stageBytesPerWarp<T>()) : nullptr;
     const size_t stride = (size_t)M.S.totalBodies * kState;
     for (int k = count - 1; k >= 0; --k) {
         const int s = first + k;
@@ -1236,7 +1227,7 @@ __global__ void __launch_bounds__(128) k_model_reverse(const __grid_constant__ M
         const uint64_t colored = tw.colorStart[tw.colorCount] + tw.restCount;
         const uint64_t impact = tw.impactColorStart[tw.impactColorCount] + tw.impactRestCount;
         const uint64_t calls = (uint64_t)M.S.substeps * (3 * colored + 2 * impact) + colored;
-        stepWorldAdj(M, W, s, w, M.states + s * stride, W.log + (size_t)w * M.logStride, W.integLog, calls);
+        stepWorldAdj(M, W, s, w, M.states + s * stride, W.log + (size_t)w * M.logStride, W.integLog, calls, stage);
         __syncwarp();
     }
 }
@@ -1448,7 +1439,7 @@ int backwardT(Run& r, const AdjointSetup& S, cudaStream_t stream, const double* 
     int rc;
     uint64_t calls = 0;
     if ((rc = maxCalls(S, &calls)) != TF_OK) { return rc; }
-    r.logStride = calls * (uint64_t)callWords<T>();
+    r.logStride = calls * (uint64_t)kCallWords;
     if (!r.stateAdj) {
         // Steps recomputed at once: as many slots as fit in a share of the free memory, up to the whole run.
         const size_t perSlot = (size_t)S.nWorlds * r.logStride * sizeof(T) +
@@ -1501,6 +1492,11 @@ int backwardT(Run& r, const AdjointSetup& S, cudaStream_t stream, const double* 
     cudaEventRecord(r.ready, stream);
     TF_ADJ_CUDA(cudaStreamWaitEvent(r.side, r.ready, 0));
     const int blocks = (S.nWorlds + 3) / 4;
+    // Each warp of the reverse walk stages color batches in shared memory when the device grants the space
+    // (set on every call: the attribute belongs to the current device).
+    const int staged = cudaFuncSetAttribute(k_model_reverse<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)(4 * stageBytesPerWarp<T>())) == cudaSuccess ? 1 : 0;
+    if (!staged) { cudaGetLastError(); }
     // Chunk c recomputes into slot set c % 2 on the side stream once the reverse walk of chunk c - 2 has left
     // that set, so that it runs beside the walk of chunk c - 1; the walk of chunk c waits for its recompute.
     const int chunks = (S.nSteps + r.slots - 1) / r.slots;
@@ -1522,7 +1518,7 @@ int backwardT(Run& r, const AdjointSetup& S, cudaStream_t stream, const double* 
         cudaEventRecord(r.recomputed[set], r.side);
         TF_ADJ_CUDA(cudaStreamWaitEvent(stream, r.recomputed[set], 0));
         cudaEventRecord(ev[2], stream);
-        k_model_reverse<T><<<blocks, 128, 0, stream>>>(M, first, count, base);
+        k_model_reverse<T><<<blocks, 128, staged ? 4 * stageBytesPerWarp<T>() : 0, stream>>>(M, first, count, base, staged);
         cudaEventRecord(ev[3], stream);
         cudaEventRecord(r.reversed[set], stream);
         end = first;
