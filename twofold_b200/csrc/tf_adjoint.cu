@@ -385,6 +385,37 @@ __device__ __forceinline__ CData<T> loadContact(const TapeContact& c) {
     return d;
 }
 
+// One point of a recorded contact. The reverse walk reaches a point's values through selects over the four
+// (pointOf, pick4, put4) so that the contact's arrays stay in registers: an array indexed at run time lives in
+// local memory, whose loads stall the walk's dependent chain.
+template <class T>
+struct CPoint {
+    V3<T> ra, rb;
+    T adjSep, relVel;
+};
+
+template <class U>
+__device__ __forceinline__ U pick4(const U (&v)[4], int i) {
+    U r = v[0];
+    if (i == 1) { r = v[1]; }
+    if (i == 2) { r = v[2]; }
+    if (i == 3) { r = v[3]; }
+    return r;
+}
+
+template <class U>
+__device__ __forceinline__ void put4(U (&v)[4], int i, const U& x) {
+    if (i == 0) { v[0] = x; }
+    if (i == 1) { v[1] = x; }
+    if (i == 2) { v[2] = x; }
+    if (i == 3) { v[3] = x; }
+}
+
+template <class T>
+__device__ __forceinline__ CPoint<T> pointOf(const CData<T>& c, int i) {
+    return { pick4(c.ra, i), pick4(c.rb, i), pick4(c.adjSep, i), pick4(c.relVel, i) };
+}
+
 // ---------------------------------------------------------------------------------------------------------
 // Contact operations: forward, and reverse from the logged inputs.
 
@@ -406,14 +437,6 @@ __device__ __forceinline__ void writeCall(T* log, const PointState<T>* p) {
         log[5 * i] = p[i].n;
         st3(log + 5 * i + 1, p[i].t);
         log[5 * i + 4] = p[i].maxN;
-    }
-}
-template <class T>
-__device__ __forceinline__ void readCall(const T* log, PointState<T>* p) {
-    for (int i = 0; i < 4; ++i) {
-        p[i].n = log[5 * i];
-        p[i].t = ld3(log + 5 * i + 1);
-        p[i].maxN = log[5 * i + 4];
     }
 }
 
@@ -454,11 +477,11 @@ __device__ __forceinline__ T normalRow(const Model<T>& M, SBody<T>& a, SBody<T>&
 
 template <class T>
 __device__ __forceinline__ void normalRowAdj(const Model<T>& M, const SBody<T>& a, const SBody<T>& b, const CData<T>& c,
-                                             int i, const PointState<T>& p0, T vn, bool useBias, const Softness<T>& soft,
+                                             const CPoint<T>& q, const PointState<T>& p0, T vn, bool useBias, const Softness<T>& soft,
                                              BodyAdj<T>& ga, BodyAdj<T>& gb, PointState<T>& gp) {
-    const Axis<T> x = makeAxis(a, b, c.ra[i], c.rb[i], c.n);
-    const V3<T> d = b.dp - a.dp + rotate(b.dq, c.rb[i]) - rotate(a.dq, c.ra[i]);
-    const T sep = dot(d, c.n) + c.adjSep[i];
+    const Axis<T> x = makeAxis(a, b, q.ra, q.rb, c.n);
+    const V3<T> d = b.dp - a.dp + rotate(b.dq, q.rb) - rotate(a.dq, q.ra);
+    const T sep = dot(d, c.n) + q.adjSep;
     T bias = 0, ms = 1, is = 0;
     int biasKind = 0;  // 0 none, 1 sep * invH, 2 biasRate * sep, 3 clamped at -maxPushout
     if (sep > T(0)) {
@@ -501,8 +524,8 @@ __device__ __forceinline__ void normalRowAdj(const Model<T>& M, const SBody<T>& 
         const V3<T> dg = c.n * sepG;
         gb.dp = gb.dp + dg;
         ga.dp = ga.dp - dg;
-        rotateAdj(b.dq, c.rb[i], dg, gb.dq);
-        rotateAdj(a.dq, c.ra[i], dg * T(-1), ga.dq);
+        rotateAdj(b.dq, q.rb, dg, gb.dq);
+        rotateAdj(a.dq, q.ra, dg * T(-1), ga.dq);
     }
 }
 
@@ -533,11 +556,11 @@ __device__ __forceinline__ void frictionRow(SBody<T>& a, SBody<T>& b, const CDat
 // The reverse of the friction rows of point i: t0 is the point's tangent impulse before them, row[0..2] their
 // logged speeds along the two tangents and the normal impulse that bounds them.
 template <class T>
-__device__ __forceinline__ void frictionRowAdj(const SBody<T>& a, const SBody<T>& b, const CData<T>& c, int i,
-                                               V3<T> t0, const T* row, T mu, BodyAdj<T>& ga, BodyAdj<T>& gb,
+__device__ __forceinline__ void frictionRowAdj(const SBody<T>& a, const SBody<T>& b, const CData<T>& c,
+                                               const CPoint<T>& q, V3<T> t0, const T* row, T mu, BodyAdj<T>& ga, BodyAdj<T>& gb,
                                                PointState<T>& gp, T& muG) {
-    const Axis<T> x1 = makeAxis(a, b, c.ra[i], c.rb[i], c.t1);
-    const Axis<T> x2 = makeAxis(a, b, c.ra[i], c.rb[i], c.t2);
+    const Axis<T> x1 = makeAxis(a, b, q.ra, q.rb, c.t1);
+    const Axis<T> x2 = makeAxis(a, b, q.ra, q.rb, c.t2);
     const T old1 = dot(t0, c.t1), old2 = dot(t0, c.t2);
     const T s1 = row[0], s2 = row[1], pn = row[2];
     const T f1 = old1 - x1.mass * s1, f2 = old2 - x2.mass * s2;
@@ -601,10 +624,10 @@ __device__ __forceinline__ void restituteRow(const Model<T>& M, SBody<T>& a, SBo
 
 template <class T>
 __device__ __forceinline__ void restituteRowAdj(const Model<T>& M, const SBody<T>& a, const SBody<T>& b, const CData<T>& c,
-                                                int i, const PointState<T>& p0, T vn, BodyAdj<T>& ga, BodyAdj<T>& gb,
+                                                const CPoint<T>& q, const PointState<T>& p0, T vn, BodyAdj<T>& ga, BodyAdj<T>& gb,
                                                 PointState<T>& gp) {
-    const Axis<T> x = makeAxis(a, b, c.ra[i], c.rb[i], c.n);
-    const T imp = -x.mass * (vn + c.restitution * c.relVel[i]);
+    const Axis<T> x = makeAxis(a, b, q.ra, q.rb, c.n);
+    const T imp = -x.mass * (vn + c.restitution * q.relVel);
     const T total = fmax(p0.n + imp, T(0));
     const T delta = total - p0.n;
     T deltaG = pushAdj(a, b, x, delta, ga, gb);
@@ -620,7 +643,7 @@ __device__ __forceinline__ void restituteRowAdj(const Model<T>& M, const SBody<T
         impG = totalG;
     }
     gp.n = nG;
-    const T massG = -impG * (vn + c.restitution * c.relVel[i]);
+    const T massG = -impG * (vn + c.restitution * q.relVel);
     speedAdj(x, -impG * x.mass, ga, gb);
     axisMassAdj(x, massG, ga.im, ga.I, gb.im, gb.I);
 }
@@ -681,38 +704,53 @@ __device__ void contactOp(const Model<T>& M, int op, SBody<T>& a, SBody<T>& b, c
 // the normal impulse logged beside them) and the logged speeds. ga, gb, gp hold the adjoints after the operation
 // on entry and before it on return. Velocities of a and b are not read.
 template <class T>
-__device__ void contactOpAdj(const Model<T>& M, int op, const SBody<T>& a, const SBody<T>& b, const CData<T>& c,
-                             const PointState<T>* p0, T mu, BodyAdj<T>& ga, BodyAdj<T>& gb, PointState<T>* gp, T& muG,
-                             const T* rec) {
+__device__ __forceinline__ void contactOpAdj(const Model<T>& M, int op, const SBody<T>& a, const SBody<T>& b,
+                                             const CData<T>& c, T mu, BodyAdj<T>& ga, BodyAdj<T>& gb,
+                                             PointState<T> (&gp)[4], T& muG, const T* rec) {
+    // Point i's state before the operation, read from the record where it is needed.
+    auto p0 = [&](int i) { return PointState<T>{ rec[5 * i], ld3(rec + 5 * i + 1), rec[5 * i + 4] }; };
     const Softness<T> soft = (!a.moves || !b.moves) ? M.staticSoft : M.contactSoft;
     const int n = c.count;
     if (op == kWarm) {
         for (int i = 0; i < n; ++i) {
-            const Axis<T> xn = makeAxis(a, b, c.ra[i], c.rb[i], c.n);
-            const Axis<T> x1 = makeAxis(a, b, c.ra[i], c.rb[i], c.t1);
-            const Axis<T> x2 = makeAxis(a, b, c.ra[i], c.rb[i], c.t2);
-            const T l1 = dot(p0[i].t, c.t1), l2 = dot(p0[i].t, c.t2);
-            gp[i].n += pushAdj(a, b, xn, p0[i].n, ga, gb);
+            const CPoint<T> q = pointOf(c, i);
+            const PointState<T> pi = p0(i);
+            PointState<T> g = pick4(gp, i);
+            const Axis<T> xn = makeAxis(a, b, q.ra, q.rb, c.n);
+            const Axis<T> x1 = makeAxis(a, b, q.ra, q.rb, c.t1);
+            const Axis<T> x2 = makeAxis(a, b, q.ra, q.rb, c.t2);
+            const T l1 = dot(pi.t, c.t1), l2 = dot(pi.t, c.t2);
+            g.n += pushAdj(a, b, xn, pi.n, ga, gb);
             const T g1 = pushAdj(a, b, x1, l1, ga, gb);
             const T g2 = pushAdj(a, b, x2, l2, ga, gb);
-            gp[i].t = gp[i].t + c.t1 * g1 + c.t2 * g2;
+            g.t = g.t + c.t1 * g1 + c.t2 * g2;
+            put4(gp, i, g);
         }
         return;
     }
     if (op == kRestitute) {
         if (c.restitution == T(0)) { return; }
         for (int i = n - 1; i >= 0; --i) {
-            if (restitutes(M, c, i, p0[i])) { restituteRowAdj(M, a, b, c, i, p0[i], rec[kSpeedAt + i], ga, gb, gp[i]); }
+            const CPoint<T> q = pointOf(c, i);
+            const PointState<T> pi = p0(i);
+            if (q.relVel > -M.restThreshold || pi.maxN == T(0)) { continue; }  // restitutes() false
+            PointState<T> g = pick4(gp, i);
+            restituteRowAdj(M, a, b, c, q, pi, rec[kSpeedAt + i], ga, gb, g);
+            put4(gp, i, g);
         }
         return;
     }
     const bool useBias = op == kBias;
     for (int j = n - 1; j >= 0; --j) {
         const int i = useBias ? j : n - 1 - j;
-        frictionRowAdj(a, b, c, i, p0[i].t, rec + kFrictionAt + 3 * j, mu, ga, gb, gp[i], muG);
+        PointState<T> g = pick4(gp, i);
+        frictionRowAdj(a, b, c, pointOf(c, i), ld3(rec + 5 * i + 1), rec + kFrictionAt + 3 * j, mu, ga, gb, g, muG);
+        put4(gp, i, g);
     }
     for (int i = n - 1; i >= 0; --i) {
-        normalRowAdj(M, a, b, c, i, p0[i], rec[kSpeedAt + i], useBias, soft, ga, gb, gp[i]);
+        PointState<T> g = pick4(gp, i);
+        normalRowAdj(M, a, b, c, pointOf(c, i), p0(i), rec[kSpeedAt + i], useBias, soft, ga, gb, g);
+        put4(gp, i, g);
     }
 }
 
@@ -726,9 +764,10 @@ __device__ __forceinline__ void prefetchRange(const T* from, const T* to, uint32
 }
 
 // Records a stage buffer of the reverse walk holds: one color's batch (each warp has two buffers, one being
-// filled while the other is read).
+// filled while the other is read). In float, two buffers and the body arrays of a 65-body world take 27 KB, so
+// that two CTAs of four warps share an SM.
 template <class T>
-__host__ __device__ constexpr int stageCalls() { return sizeof(T) == 4 ? 64 : 32; }
+__host__ __device__ constexpr int stageCalls() { return sizeof(T) == 4 ? 48 : 32; }
 
 // Copies `words` values (whole 16-byte pieces, both addresses 16-byte aligned) from global to shared memory
 // with asynchronous copies spread over the warp's lanes, as one commit group of each lane.
@@ -947,26 +986,76 @@ __device__ void stepWorld(const Model<T>& M, const Slot<T>& W, int step, uint32_
     pass(kRestitute);
 }
 
+// The per-body arrays the reverse walk reads and writes, indexed by the body's place in its world. They are
+// the warp's share of shared memory when the kernel has one for bodies (the adjoint state is copied in at the
+// start of the walk and out at its end, the step's inverse masses and inertias at each step's start), else the
+// global arrays offset to the world's first body.
+template <class T>
+struct BodyArrays {
+    T* stateAdj;  // kState per body
+    T* dpAdj;     // 3
+    T* dqAdj;     // 4
+    T* qBaseAdj;  // 4
+    T* invMAdj;   // 1
+    T* invIAdj;   // 9
+    T* dp;        // 3: the body's displacement during the pass being reversed
+    T* dq;        // 4
+    T* invM;      // 1: the step's inverse mass and world inverse inertia
+    T* invI;      // 9
+};
+constexpr int kBodyWords = kState + 3 + 4 + 4 + 1 + 9 + 3 + 4 + 1 + 9;
+
+template <class T>
+__device__ __forceinline__ BodyArrays<T> sharedBodies(T* area, uint32_t cap) {
+    BodyArrays<T> B;
+    T* p = area;
+    B.stateAdj = p, p += kState * cap;
+    B.dpAdj = p, p += 3 * cap;
+    B.dqAdj = p, p += 4 * cap;
+    B.qBaseAdj = p, p += 4 * cap;
+    B.invMAdj = p, p += cap;
+    B.invIAdj = p, p += 9 * cap;
+    B.dp = p, p += 3 * cap;
+    B.dq = p, p += 4 * cap;
+    B.invM = p, p += cap;
+    B.invI = p;
+    return B;
+}
+
+template <class T>
+__device__ __forceinline__ BodyArrays<T> globalBodies(const Model<T>& M, const Slot<T>& W, size_t first) {
+    return { M.stateAdj + kState * first, M.dpAdj + 3 * first, M.dqAdj + 4 * first, M.qBaseAdj + 4 * first,
+             M.invMAdj + first, M.invIAdj + 9 * first, W.dp + 3 * first, W.dq + 4 * first, W.invM + first,
+             W.invI + 9 * first };
+}
+
 // Reverse of one world's step: adjoints of the state at the step's end in M.stateAdj become those at its start.
 // Needs the log and integLog that stepWorld wrote for this step, and the bodies' dp/dq of every substep, which
 // it recomputes by replaying the integration from the checkpoint as it goes back. stage: the warp's two
-// shared-memory buffers of stageCalls<T>() records each, or null to read every record from the log.
+// shared-memory buffers of stageCalls<T>() records each, or null to read every record from the log. bodies:
+// the warp's shared-memory body arrays (sharedBodies) holding the world's adjoint state, or null to use the
+// global arrays.
 template <class T>
 __device__ void stepWorldAdj(const Model<T>& M, const Slot<T>& W, int step, uint32_t w, const T* in, const T* log,
-                             const T* integLog, uint64_t calls, T* stage) {
+                             const T* integLog, uint64_t calls, T* stage, T* bodies, uint32_t bodyCap) {
     constexpr int kStage = stageCalls<T>();
     const uint32_t lane = threadIdx.x & 31;
     const WorldView V = viewOf(M.S, step, w);
     const int n = M.S.substeps;
     const uint32_t cf = V.tw->contactFirst;
-    // dp, dq and invM, invI of the step: recomputed from the checkpoint and the integration log.
+    const BodyArrays<T> B = bodies ? sharedBodies(bodies, bodyCap) : globalBodies(M, W, V.bodyFirst);
+    // The step's adjoint accumulators start at zero; the inverse masses and inertias the recomputation found.
     for (uint32_t i = lane; i < V.bodyCount; i += 32) {
-        const uint32_t g = V.bodyFirst + i;
-        st3(M.dpAdj + 3 * (size_t)g, zeroV<T>());
-        st4(M.dqAdj + 4 * (size_t)g, Q4<T>{ 0, 0, 0, 0 });
-        st4(M.qBaseAdj + 4 * (size_t)g, Q4<T>{ 0, 0, 0, 0 });
-        M.invMAdj[g] = 0;
-        stM(M.invIAdj + 9 * (size_t)g, zeroM<T>());
+        st3(B.dpAdj + 3 * i, zeroV<T>());
+        st4(B.dqAdj + 4 * i, Q4<T>{ 0, 0, 0, 0 });
+        st4(B.qBaseAdj + 4 * i, Q4<T>{ 0, 0, 0, 0 });
+        B.invMAdj[i] = 0;
+        stM(B.invIAdj + 9 * i, zeroM<T>());
+        if (bodies) {
+            const uint32_t g = V.bodyFirst + i;
+            B.invM[i] = W.invM[g];
+            for (int k = 0; k < 9; ++k) { B.invI[9 * i + k] = W.invI[9 * (size_t)g + k]; }
+        }
     }
     for (uint32_t ci = lane; ci < V.tw->contactCount; ci += 32) {
         for (int i = 0; i < 4; ++i) { M.pointAdj[(size_t)(cf + ci) * 4 + i] = PointState<T>{ 0, zeroV<T>(), 0 }; }
@@ -979,14 +1068,14 @@ __device__ void stepWorldAdj(const Model<T>& M, const Slot<T>& W, int step, uint
             const uint32_t g = V.bodyFirst + i;
             const int k = afterUpdate ? sub : sub - 1;  // the last position update before the pass
             if (!movesIn(M, V, g) || k < 0) {
-                st3(W.dp + 3 * (size_t)g, zeroV<T>());
-                st4(W.dq + 4 * (size_t)g, Q4<T>{ 0, 0, 0, 1 });
+                st3(B.dp + 3 * i, zeroV<T>());
+                st4(B.dq + 4 * i, Q4<T>{ 0, 0, 0, 1 });
                 continue;
             }
             const T* L = integLog + ((size_t)k * M.S.totalBodies + g) * kIntegWords;
             const Q4<T> qb = ld4(in + (size_t)g * kState + 3);
-            st3(W.dp + 3 * (size_t)g, ld3(L + 7));
-            st4(W.dq + 4 * (size_t)g, qmul(integrateQ(ld4(L), ld3(L + 4), M.h), conj(qb)));
+            st3(B.dp + 3 * i, ld3(L + 7));
+            st4(B.dq + 4 * i, qmul(integrateQ(ld4(L), ld3(L + 4), M.h), conj(qb)));
         }
         __syncwarp();
     };
@@ -994,17 +1083,15 @@ __device__ void stepWorldAdj(const Model<T>& M, const Slot<T>& W, int step, uint
     auto opAdj = [&](int op, uint32_t ci, const T* rec) {
         const TapeContact& tc = V.contacts[ci];
         const CData<T> c = loadContact<T>(tc);
-        const uint32_t ga = V.bodyFirst + tc.a, gb = V.bodyFirst + tc.b;
+        const uint32_t ia = tc.a, ib = tc.b, ga = V.bodyFirst + ia, gb = V.bodyFirst + ib;
         SBody<T> a, b;
-        PointState<T> p0[4];
-        readCall(rec, p0);
         a.v = a.w = b.v = b.w = zeroV<T>();  // the reverse reads no velocity
-        a.dp = ld3(W.dp + 3 * (size_t)ga), a.dq = ld4(W.dq + 4 * (size_t)ga), a.im = W.invM[ga];
-        a.I = ldM(W.invI + 9 * (size_t)ga), a.moves = movesIn(M, V, ga);
-        b.dp = ld3(W.dp + 3 * (size_t)gb), b.dq = ld4(W.dq + 4 * (size_t)gb), b.im = W.invM[gb];
-        b.I = ldM(W.invI + 9 * (size_t)gb), b.moves = movesIn(M, V, gb);
-        T* sa = M.stateAdj + (size_t)ga * kState;
-        T* sb = M.stateAdj + (size_t)gb * kState;
+        a.dp = ld3(B.dp + 3 * ia), a.dq = ld4(B.dq + 4 * ia), a.im = B.invM[ia];
+        a.I = ldM(B.invI + 9 * ia), a.moves = movesIn(M, V, ga);
+        b.dp = ld3(B.dp + 3 * ib), b.dq = ld4(B.dq + 4 * ib), b.im = B.invM[ib];
+        b.I = ldM(B.invI + 9 * ib), b.moves = movesIn(M, V, gb);
+        T* sa = B.stateAdj + ia * kState;
+        T* sb = B.stateAdj + ib * kState;
         BodyAdj<T> gA{ zeroV<T>(), zeroV<T>(), zeroV<T>(), Q4<T>{ 0, 0, 0, 0 }, 0, zeroM<T>() };
         BodyAdj<T> gB = gA;
         // Moving bodies belong to this contact alone within its color: their adjoints are read and written in
@@ -1016,16 +1103,16 @@ __device__ void stepWorldAdj(const Model<T>& M, const Slot<T>& W, int step, uint
         for (int i = 0; i < 4; ++i) { g4[i] = gp[i]; }
         T muG = 0;
         const T mu = contactFriction(M, V, tc);
-        contactOpAdj(M, op, a, b, c, p0, mu, gA, gB, g4, muG, rec);
+        contactOpAdj(M, op, a, b, c, mu, gA, gB, g4, muG, rec);
         for (int i = 0; i < 4; ++i) { gp[i] = g4[i]; }
-        auto put = [&](bool moves, uint32_t g, T* s, const BodyAdj<T>& G) {
+        auto put = [&](bool moves, uint32_t i, uint32_t g, T* s, const BodyAdj<T>& G) {
             if (moves) {
                 st3(s + 7, G.v);
                 st3(s + 10, G.w);
-                st3(M.dpAdj + 3 * (size_t)g, ld3(M.dpAdj + 3 * (size_t)g) + G.dp);
-                st4(M.dqAdj + 4 * (size_t)g, qadd(ld4(M.dqAdj + 4 * (size_t)g), G.dq));
-                M.invMAdj[g] += G.im;
-                T* I = M.invIAdj + 9 * (size_t)g;
+                st3(B.dpAdj + 3 * i, ld3(B.dpAdj + 3 * i) + G.dp);
+                st4(B.dqAdj + 4 * i, qadd(ld4(B.dqAdj + 4 * i), G.dq));
+                B.invMAdj[i] += G.im;
+                T* I = B.invIAdj + 9 * i;
                 for (int r = 0; r < 3; ++r) { I[3 * r] += G.I.r[r].x, I[3 * r + 1] += G.I.r[r].y, I[3 * r + 2] += G.I.r[r].z; }
             } else if (M.S.dynamic[g]) {
                 // A sleeping dynamic body: its velocity carries back to steps where it moved. A static body's
@@ -1034,8 +1121,8 @@ __device__ void stepWorldAdj(const Model<T>& M, const Slot<T>& W, int step, uint
                 atomicAddT(s + 10, G.w.x), atomicAddT(s + 11, G.w.y), atomicAddT(s + 12, G.w.z);
             }
         };
-        put(a.moves, ga, sa, gA);
-        put(b.moves, gb, sb, gB);
+        put(a.moves, ia, ga, sa, gA);
+        put(b.moves, ib, gb, sb, gB);
         if (muG != T(0)) {
             // mu = sqrt(fa fb): d mu / d fa = fb / (2 mu).
             const T fa = M.friction[V.shapeFirst + tc.shapeA], fb = M.friction[V.shapeFirst + tc.shapeB];
@@ -1100,25 +1187,25 @@ __device__ void stepWorldAdj(const Model<T>& M, const Slot<T>& W, int step, uint
         for (uint32_t i = lane; i < V.bodyCount; i += 32) {
             const uint32_t g = V.bodyFirst + i;
             if (!movesIn(M, V, g)) { continue; }
-            T* s = M.stateAdj + (size_t)g * kState;
+            T* s = B.stateAdj + i * kState;
             const T* L = integLog + ((size_t)sub * M.S.totalBodies + g) * kIntegWords;
             const Q4<T> q = ld4(L);
             const V3<T> wv = ld3(L + 4);
             const Q4<T> nq = integrateQ(q, wv, M.h);
             const Q4<T> qb = ld4(in + (size_t)g * kState + 3);
             // dq' = q' qBase*: its adjoint goes to q' and to qBase.
-            const Q4<T> dqG = ld4(M.dqAdj + 4 * (size_t)g);
+            const Q4<T> dqG = ld4(B.dqAdj + 4 * i);
             Q4<T> qG = qadd(ld4(s + 3), qmulAdjA(dqG, conj(qb)));
             const Q4<T> cG = qmulAdjB(dqG, nq);
-            st4(M.qBaseAdj + 4 * (size_t)g, qadd(ld4(M.qBaseAdj + 4 * (size_t)g), Q4<T>{ -cG.x, -cG.y, -cG.z, cG.w }));
-            st4(M.dqAdj + 4 * (size_t)g, Q4<T>{ 0, 0, 0, 0 });
+            st4(B.qBaseAdj + 4 * i, qadd(ld4(B.qBaseAdj + 4 * i), Q4<T>{ -cG.x, -cG.y, -cG.z, cG.w }));
+            st4(B.dqAdj + 4 * i, Q4<T>{ 0, 0, 0, 0 });
             Q4<T> qPrevG{ 0, 0, 0, 0 };
             V3<T> wG = ld3(s + 10);
             integrateQAdj(q, wv, M.h, qG, qPrevG, wG);
             st4(s + 3, qPrevG);
             st3(s + 10, wG);
             // com' = com + v h and dp' = dp + v h.
-            const V3<T> vG = ld3(s + 7) + ld3(s) * M.h + ld3(M.dpAdj + 3 * (size_t)g) * M.h;
+            const V3<T> vG = ld3(s + 7) + ld3(s) * M.h + ld3(B.dpAdj + 3 * i) * M.h;
             st3(s + 7, vG);
         }
         __syncwarp();
@@ -1129,7 +1216,7 @@ __device__ void stepWorldAdj(const Model<T>& M, const Slot<T>& W, int step, uint
         for (uint32_t i = lane; i < V.bodyCount; i += 32) {
             const uint32_t g = V.bodyFirst + i;
             if (!movesIn(M, V, g)) { continue; }
-            T* s = M.stateAdj + (size_t)g * kState;
+            T* s = B.stateAdj + i * kState;
             st3(s + 7, ld3(s + 7) * (T(1) / (T(1) + M.h * T(M.S.linearDamping[g]))));
             st3(s + 10, ld3(s + 10) * (T(1) / (T(1) + M.h * T(M.S.angularDamping[g]))));
         }
@@ -1138,8 +1225,8 @@ __device__ void stepWorldAdj(const Model<T>& M, const Slot<T>& W, int step, uint
     // Step start in reverse: qBase = q, the world inverse inertia r L r^T and the inverse mass 1/m.
     for (uint32_t i = lane; i < V.bodyCount; i += 32) {
         const uint32_t g = V.bodyFirst + i;
-        T* s = M.stateAdj + (size_t)g * kState;
-        st4(s + 3, qadd(ld4(s + 3), ld4(M.qBaseAdj + 4 * (size_t)g)));
+        T* s = B.stateAdj + i * kState;
+        st4(s + 3, qadd(ld4(s + 3), ld4(B.qBaseAdj + 4 * i)));
         if (!movesIn(M, V, g)) { continue; }
         const Q4<T> q = ld4(in + (size_t)g * kState + 3);
         const T m = M.mass[g];
@@ -1150,7 +1237,7 @@ __device__ void stepWorldAdj(const Model<T>& M, const Slot<T>& W, int step, uint
                        T(M.S.invInertiaLocal[9 * g + 3 * a + 2]) * scale };
         }
         const M3<T> r = toMat3(q);
-        const M3<T> G = ldM(M.invIAdj + 9 * (size_t)g);
+        const M3<T> G = ldM(B.invIAdj + 9 * i);
         // I = r L r^T: dr = G r L^T + G^T r L, dL = r^T G r.
         const M3<T> rG = madd(mmul(G, mmul(r, transposeM(L))), mmul(transposeM(G), mmul(r, L)));
         const M3<T> LG = mmul(transposeM(r), mmul(G, r));
@@ -1158,7 +1245,7 @@ __device__ void stepWorldAdj(const Model<T>& M, const Slot<T>& W, int step, uint
         for (int a = 0; a < 3; ++a) { lG += dot(LG.r[a], L.r[a]); }
         st4(s + 3, qadd(ld4(s + 3), toMat3Adj(q, rG)));
         // im = 1/m and L = L0 m0 / m: both scale as 1/m.
-        M.massAdj[g] += -(M.invMAdj[g] / (m * m)) - lG / m;
+        M.massAdj[g] += -(B.invMAdj[i] / (m * m)) - lG / m;
     }
     __syncwarp();
 }
@@ -1211,12 +1298,30 @@ template <class T>
 __host__ __device__ constexpr size_t stageBytesPerWarp() { return 2 * (size_t)stageCalls<T>() * kCallWords * sizeof(T); }
 
 template <class T>
+__host__ __device__ constexpr size_t bodyBytesPerWarp(uint32_t cap) {
+    return ((size_t)cap * kBodyWords * sizeof(T) + 15) / 16 * 16;
+}
+
+// The reverse walk of a chunk of steps, one warp per world, from the chunk's last step to its first. Each warp's
+// share of the dynamic shared memory holds, when `staged`, its two stage buffers and, when bodyCap is not zero,
+// body arrays for up to bodyCap bodies (no world has more).
+template <class T>
 __global__ void __launch_bounds__(128) k_model_reverse(const __grid_constant__ Model<T> M, int first, int count,
-                                                       uint32_t slotBase, int staged) {
-    extern __shared__ __align__(16) unsigned char stageArea[];
+                                                       uint32_t slotBase, int staged, uint32_t bodyCap) {
+    extern __shared__ __align__(16) unsigned char area[];
     const uint32_t w = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
     if (w >= (uint32_t)M.S.nWorlds) { return; }
-    T* stage = staged ? reinterpret_cast<T*>(stageArea + (threadIdx.x / 32) * stageBytesPerWarp<T>()) : nullptr;
+    const uint32_t lane = threadIdx.x & 31;
+    const size_t stageBytes = staged ? stageBytesPerWarp<T>() : 0;
+    unsigned char* mine = area + (threadIdx.x / 32) * (stageBytes + bodyBytesPerWarp<T>(bodyCap));
+    T* stage = staged ? reinterpret_cast<T*>(mine) : nullptr;
+    T* bodies = bodyCap ? reinterpret_cast<T*>(mine + stageBytes) : nullptr;
+    const uint32_t b0 = M.S.bodyFirst[w], nb = M.S.bodyCount[w];
+    if (bodies) {
+        T* adj = sharedBodies(bodies, bodyCap).stateAdj;
+        for (uint32_t k = lane; k < nb * kState; k += 32) { adj[k] = M.stateAdj[(size_t)b0 * kState + k]; }
+        __syncwarp();
+    }
     const size_t stride = (size_t)M.S.totalBodies * kState;
     for (int k = count - 1; k >= 0; --k) {
         const int s = first + k;
@@ -1227,8 +1332,13 @@ __global__ void __launch_bounds__(128) k_model_reverse(const __grid_constant__ M
         const uint64_t colored = tw.colorStart[tw.colorCount] + tw.restCount;
         const uint64_t impact = tw.impactColorStart[tw.impactColorCount] + tw.impactRestCount;
         const uint64_t calls = (uint64_t)M.S.substeps * (3 * colored + 2 * impact) + colored;
-        stepWorldAdj(M, W, s, w, M.states + s * stride, W.log + (size_t)w * M.logStride, W.integLog, calls, stage);
+        stepWorldAdj(M, W, s, w, M.states + s * stride, W.log + (size_t)w * M.logStride, W.integLog, calls, stage,
+                     bodies, bodyCap);
         __syncwarp();
+    }
+    if (bodies) {
+        const T* adj = sharedBodies(bodies, bodyCap).stateAdj;
+        for (uint32_t k = lane; k < nb * kState; k += 32) { M.stateAdj[(size_t)b0 * kState + k] = adj[k]; }
     }
 }
 
@@ -1249,23 +1359,27 @@ struct Run {
          *integLog = nullptr, *scratch = nullptr, *branches = nullptr;
     uint64_t logStride = 0;
     int slots = 0;  // steps the backward recomputes at once; two sets of slots alternate
+    uint32_t maxBodies = 0;  // the most bodies of a world, read once
     bool forwardDone = false;
     float forwardMs = 0.0f, backwardMs = 0.0f;
     // The backward's two kinds of launch, each summed over its chunks (they overlap, so the sum can exceed the
     // backward's own time): recomputation and reverse walk.
     float recomputeMs = 0.0f, reverseMs = 0.0f;
     std::vector<cudaEvent_t> chunkEvents;  // per chunk: recompute start, end; reverse start, end
-    // The recomputation runs on its own stream, one chunk ahead of the reverse walk.
-    cudaStream_t side = nullptr;
-    cudaEvent_t ready = nullptr, recomputed[2] = {}, reversed[2] = {};
+    // The recomputation runs on its own stream, one chunk ahead of the reverse walk. The walk, the backward's
+    // critical path, runs on a stream of the highest priority, so that its CTAs take the SMs before the next
+    // chunk's recomputation, which becomes ready at the same moment.
+    cudaStream_t side = nullptr, walk = nullptr;
+    cudaEvent_t ready = nullptr, recomputed[2] = {}, reversed[2] = {}, walked = nullptr;
 
     ~Run() {
         release();
         for (cudaEvent_t e : chunkEvents) { cudaEventDestroy(e); }
-        for (cudaEvent_t e : { ready, recomputed[0], recomputed[1], reversed[0], reversed[1] }) {
+        for (cudaEvent_t e : { ready, recomputed[0], recomputed[1], reversed[0], reversed[1], walked }) {
             if (e) { cudaEventDestroy(e); }
         }
         if (side) { cudaStreamDestroy(side); }
+        if (walk) { cudaStreamDestroy(walk); }
     }
     void release() {
         for (void* p : owned) { cudaFree(p); }
@@ -1277,6 +1391,7 @@ struct Run {
         }
         forwardDone = false;
         slots = 0;
+        maxBodies = 0;
     }
     int alloc(void** p, size_t bytes) {
         cudaError_t e = cudaMalloc(p, bytes < 16 ? 16 : bytes);
@@ -1483,20 +1598,53 @@ int backwardT(Run& r, const AdjointSetup& S, cudaStream_t stream, const double* 
     TF_ADJ_CUDA(cudaEventCreate(&e0));
     TF_ADJ_CUDA(cudaEventCreate(&e1));
     if (!r.side) {
+        int least = 0, greatest = 0;
+        TF_ADJ_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
         TF_ADJ_CUDA(cudaStreamCreateWithFlags(&r.side, cudaStreamNonBlocking));
-        for (cudaEvent_t* e : { &r.ready, &r.recomputed[0], &r.recomputed[1], &r.reversed[0], &r.reversed[1] }) {
+        TF_ADJ_CUDA(cudaStreamCreateWithPriority(&r.walk, cudaStreamNonBlocking, greatest));
+        for (cudaEvent_t* e : { &r.ready, &r.recomputed[0], &r.recomputed[1], &r.reversed[0], &r.reversed[1], &r.walked }) {
             TF_ADJ_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
         }
     }
     cudaEventRecord(e0, stream);
     cudaEventRecord(r.ready, stream);
     TF_ADJ_CUDA(cudaStreamWaitEvent(r.side, r.ready, 0));
+    TF_ADJ_CUDA(cudaStreamWaitEvent(r.walk, r.ready, 0));
     const int blocks = (S.nWorlds + 3) / 4;
     // Each warp of the reverse walk stages color batches in shared memory when the device grants the space
     // (set on every call: the attribute belongs to the current device).
-    const int staged = cudaFuncSetAttribute(k_model_reverse<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                            (int)(4 * stageBytesPerWarp<T>())) == cudaSuccess ? 1 : 0;
-    if (!staged) { cudaGetLastError(); }
+    // Each warp of the reverse walk stages color batches and its world's body arrays in shared memory when the
+    // device grants the space and every world's warp still fits on the device at once (the walk is one dependent
+    // chain per world: a second wave of worlds would double its time); else the body arrays, or both, stay in
+    // global memory. The attribute is set on every call: it belongs to the current device.
+    if (r.maxBodies == 0) {
+        std::vector<uint32_t> counts(S.nWorlds);
+        TF_ADJ_CUDA(cudaMemcpy(counts.data(), S.bodyCount, counts.size() * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+        r.maxBodies = std::max<uint32_t>(1, *std::max_element(counts.begin(), counts.end()));
+    }
+    int device = 0, sms = 0;
+    TF_ADJ_CUDA(cudaGetDevice(&device));
+    TF_ADJ_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    int staged = 0;
+    uint32_t bodyCap = 0;
+    size_t walkShared = 0;
+    for (int option = 0; option < 3; ++option) {
+        const int st = option < 2 ? 1 : 0;
+        const uint32_t cap = option == 0 ? r.maxBodies : 0;
+        const size_t bytes = 4 * ((st ? stageBytesPerWarp<T>() : 0) + bodyBytesPerWarp<T>(cap));
+        if (cudaFuncSetAttribute(k_model_reverse<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) != cudaSuccess) {
+            cudaGetLastError();
+            continue;
+        }
+        int perSm = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_model_reverse<T>, 128, bytes) != cudaSuccess) {
+            cudaGetLastError();
+            continue;
+        }
+        if (option < 2 && (size_t)perSm * sms * 4 < (size_t)S.nWorlds) { continue; }
+        staged = st, bodyCap = cap, walkShared = bytes;
+        break;
+    }
     // Chunk c recomputes into slot set c % 2 on the side stream once the reverse walk of chunk c - 2 has left
     // that set, so that it runs beside the walk of chunk c - 1; the walk of chunk c waits for its recompute.
     const int chunks = (S.nSteps + r.slots - 1) / r.slots;
@@ -1516,13 +1664,15 @@ int backwardT(Run& r, const AdjointSetup& S, cudaStream_t stream, const double* 
         k_model_recompute<T><<<(warps + 3) / 4, 128, 0, r.side>>>(M, first, count, base);
         cudaEventRecord(ev[1], r.side);
         cudaEventRecord(r.recomputed[set], r.side);
-        TF_ADJ_CUDA(cudaStreamWaitEvent(stream, r.recomputed[set], 0));
-        cudaEventRecord(ev[2], stream);
-        k_model_reverse<T><<<blocks, 128, staged ? 4 * stageBytesPerWarp<T>() : 0, stream>>>(M, first, count, base, staged);
-        cudaEventRecord(ev[3], stream);
-        cudaEventRecord(r.reversed[set], stream);
+        TF_ADJ_CUDA(cudaStreamWaitEvent(r.walk, r.recomputed[set], 0));
+        cudaEventRecord(ev[2], r.walk);
+        k_model_reverse<T><<<blocks, 128, walkShared, r.walk>>>(M, first, count, base, staged, bodyCap);
+        cudaEventRecord(ev[3], r.walk);
+        cudaEventRecord(r.reversed[set], r.walk);
         end = first;
     }
+    cudaEventRecord(r.walked, r.walk);
+    TF_ADJ_CUDA(cudaStreamWaitEvent(stream, r.walked, 0));
     cudaEventRecord(e1, stream);
     TF_ADJ_CUDA(cudaGetLastError());
     TF_ADJ_CUDA(cudaStreamSynchronize(stream));
