@@ -44,12 +44,15 @@ enum WorkSlot : int {
                                                           // the other active contacts of refreshed worlds
     kSlotTape = kSlotFastItems + kPairClasses + 1,      // the recording kernel's world counter
     // The flat solve of batches of many worlds (k_substep_flat): each color's contacts over every world, the
-    // impact colors' likewise, the most colors and impact colors any world has, and the grid barrier.
+    // impact colors' likewise, the most colors, impact colors and levels of one-at-a-time contacts any world
+    // has, and the grid barrier.
     kSlotFlatColor = kSlotTape + 1,                    // + color: contacts of that color in all worlds
     kSlotFlatImpact = kSlotFlatColor + kColors,        // + color
     kSlotFlatMaxColors = kSlotFlatImpact + kColors,
     kSlotFlatMaxImpact = kSlotFlatMaxColors + 1,
-    kSlotFlatBarrier = kSlotFlatMaxImpact + 1,         // arrivals, then generation
+    kSlotFlatMaxRestLevels = kSlotFlatMaxImpact + 1,
+    kSlotFlatMaxImpactRestLevels = kSlotFlatMaxRestLevels + 1,
+    kSlotFlatBarrier = kSlotFlatMaxImpactRestLevels + 1,  // arrivals, then barriers passed
     kSlotCount = kSlotFlatBarrier + 2
 };
 
@@ -2936,28 +2939,44 @@ __global__ void __launch_bounds__(kMaxBlock) k_substep(const __grid_constant__ B
 // 0's flags and goes on (the host reports the step as failed), so a fault here cannot hang the device.
 constexpr uint32_t kBarrierSpins = 1u << 24;
 
+__device__ __forceinline__ uint32_t loadAcquire(const uint32_t* p) {
+    uint32_t v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void storeRelease(uint32_t* p, uint32_t v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ uint32_t addAcqRel(uint32_t* p, uint32_t v) {
+    uint32_t old;
+    asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+    return old;
+}
+
+// Arrivals only grow within a step (the step's work slots start at zero and every flat launch of a step has
+// the same grid), so arrival t is at barrier t / gridDim of the step. The last arrival of a barrier publishes
+// the number of barriers passed with a release store; the other CTAs wait for it with acquire loads. Nothing
+// is reset between barriers, so a barrier costs one atomic round trip, a store and the waiters' polls.
 static __device__ void gridBarrier(const Batch& B) {
     __syncthreads();
     if (threadIdx.x == 0) {
         uint32_t* arrive = B.work + kSlotFlatBarrier;
-        volatile uint32_t* generation = B.work + kSlotFlatBarrier + 1;
-        const uint32_t before = *generation;
-        __threadfence();
-        if (atomicAdd(arrive, 1u) == gridDim.x - 1) {
-            atomicExch(arrive, 0u);
-            __threadfence();
-            atomicAdd(const_cast<uint32_t*>(generation), 1u);
+        uint32_t* passed = B.work + kSlotFlatBarrier + 1;
+        __threadfence();  // the CTA's writes before the barrier, ahead of its arrival
+        const uint32_t ticket = addAcqRel(arrive, 1u);
+        const uint32_t after = ticket / gridDim.x + 1;  // barriers passed once this one is
+        if (ticket % gridDim.x == gridDim.x - 1) {
+            storeRelease(passed, after);
         } else {
             uint32_t spins = 0;
-            while (*generation == before) {
+            while ((int32_t)(loadAcquire(passed) - after) < 0) {
                 if (++spins > kBarrierSpins) {
                     atomicOr(&B.counts[0].flags, kDevTimeout);
                     break;
                 }
-                __nanosleep(64);
+                __nanosleep(32);
             }
         }
-        __threadfence();
     }
     __syncthreads();
 }
@@ -2981,6 +3000,8 @@ __global__ void __launch_bounds__(256, 2) k_substep_flat(const __grid_constant__
                 WorldCounts& wc = B.counts[w];
                 atomicMax(B.work + kSlotFlatMaxColors, wc.colorCount);
                 atomicMax(B.work + kSlotFlatMaxImpact, wc.impactColorCount);
+                if (wc.restLevels) { atomicMax(B.work + kSlotFlatMaxRestLevels, wc.restLevels); }
+                if (wc.impactRestLevels) { atomicMax(B.work + kSlotFlatMaxImpactRestLevels, wc.impactRestLevels); }
                 for (uint32_t k = 0; k < wc.colorCount; ++k) {
                     const uint32_t n = wc.colorStart[k + 1] - wc.colorStart[k];
                     wc.flatColorAt[k] = n ? atomicAdd(colorTotal + k, n) : 0u;
@@ -3018,6 +3039,8 @@ __global__ void __launch_bounds__(256, 2) k_substep_flat(const __grid_constant__
         gridBarrier(B);
     }
     const uint32_t colors = B.work[kSlotFlatMaxColors], impactColors = B.work[kSlotFlatMaxImpact];
+    // Whether any world has contacts solved one at a time (the same for every CTA: set before a barrier).
+    const bool anyRest = B.work[kSlotFlatMaxRestLevels] != 0, anyImpactRest = B.work[kSlotFlatMaxImpactRestLevels] != 0;
 
     // At the first substep every body's state, pose and velocity terms are staged; at a later one, the body half
     // of a refresh (planar placements kept, a new base pose) for the worlds refreshed there. Then the velocity
@@ -3070,8 +3093,10 @@ __global__ void __launch_bounds__(256, 2) k_substep_flat(const __grid_constant__
             gridBarrier(B);
         }
     };
-    // A world's contacts solved on their own, level by level on one warp of the world.
+    // A world's contacts solved on their own, level by level on one warp of the world; nothing, not even the
+    // barrier, when no world has any.
     auto restPass = [&](bool impact, auto&& f) {
+        if (!(impact ? anyImpactRest : anyRest)) { return; }
         if (!skip) {
             const Group g = makeGroup(32);
             for (uint32_t w = warp; w < nw; w += warps) {
