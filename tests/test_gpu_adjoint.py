@@ -236,3 +236,27 @@ def test_model_step_stays_close_to_the_pipeline_step():
             compared += 1
     assert compared >= 40, compared
     assert worst_p <= 1e-3 and worst_v <= 1e-2, (worst_p, worst_v)
+
+
+def test_reverse_walk_layouts_give_the_same_gradients():
+    """The reverse walk keeps each world's body arrays in shared memory when the largest world's fit there, and in
+    global memory when one world is too large (a 325-box pyramid beside the impact walls): the impact worlds'
+    gradients are the same bits either way, in float and in double."""
+    impact = list(scenes.config5(n_worlds=4, seed=4).worlds)
+    alone = Batch.from_scene(scenes.Scene("impact", impact))
+    mixed = Batch.from_scene(scenes.Scene("impact and pyramid", impact + [scenes.pyramid(25)]))
+    n = int(alone.offsets[-1])
+    shapes = sum(len(w.shapes) for w in impact)
+    for b in (alone, mixed):
+        b.tape_record(1.0 / 60.0, 12)
+    for precision in (32, 64):
+        runs = []
+        for b, n_shapes in ((alone, shapes), (mixed, shapes + 326)):
+            final = b.adjoint_forward(precision)
+            grad = np.zeros_like(final)
+            grad[:n, 0] = 2 * final[:n, 0]
+            gi, gm, gf = b.adjoint_backward(grad, n_shapes)
+            runs.append((final[:n], gi[:n], gm[:n], gf[:shapes]))
+        for a, c in zip(*runs):
+            assert np.array_equal(a, c)
+        assert np.any(runs[0][1] != 0)

@@ -1614,9 +1614,9 @@ int backwardT(Run& r, const AdjointSetup& S, cudaStream_t stream, const double* 
     // Each warp of the reverse walk stages color batches in shared memory when the device grants the space
     // (set on every call: the attribute belongs to the current device).
     // Each warp of the reverse walk stages color batches and its world's body arrays in shared memory when the
-    // device grants the space and every world's warp still fits on the device at once (the walk is one dependent
-    // chain per world: a second wave of worlds would double its time); else the body arrays, or both, stay in
-    // global memory. The attribute is set on every call: it belongs to the current device.
+    // device grants the space and that leaves as many worlds resident at once as the walk can have at all (it
+    // is one dependent chain per world: worlds beyond those wait for a second wave); else the body arrays, or
+    // both, stay in global memory. The attribute is set on every call: it belongs to the current device.
     if (r.maxBodies == 0) {
         std::vector<uint32_t> counts(S.nWorlds);
         TF_ADJ_CUDA(cudaMemcpy(counts.data(), S.bodyCount, counts.size() * sizeof(uint32_t), cudaMemcpyDeviceToHost));
@@ -1625,25 +1625,27 @@ int backwardT(Run& r, const AdjointSetup& S, cudaStream_t stream, const double* 
     int device = 0, sms = 0;
     TF_ADJ_CUDA(cudaGetDevice(&device));
     TF_ADJ_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
-    int staged = 0;
-    uint32_t bodyCap = 0;
-    size_t walkShared = 0;
+    auto walkBytes = [&](int option) {  // 0: records and bodies staged, 1: records only, 2: nothing
+        return 4 * ((option < 2 ? stageBytesPerWarp<T>() : 0) + bodyBytesPerWarp<T>(option == 0 ? r.maxBodies : 0));
+    };
+    int perSm[3] = { 0, 0, 0 };
     for (int option = 0; option < 3; ++option) {
-        const int st = option < 2 ? 1 : 0;
-        const uint32_t cap = option == 0 ? r.maxBodies : 0;
-        const size_t bytes = 4 * ((st ? stageBytesPerWarp<T>() : 0) + bodyBytesPerWarp<T>(cap));
-        if (cudaFuncSetAttribute(k_model_reverse<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) != cudaSuccess) {
+        const size_t bytes = walkBytes(option);
+        if (cudaFuncSetAttribute(k_model_reverse<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) != cudaSuccess ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm[option], k_model_reverse<T>, 128, bytes) != cudaSuccess) {
             cudaGetLastError();
-            continue;
+            perSm[option] = 0;
         }
-        int perSm = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_model_reverse<T>, 128, bytes) != cudaSuccess) {
-            cudaGetLastError();
-            continue;
-        }
-        if (option < 2 && (size_t)perSm * sms * 4 < (size_t)S.nWorlds) { continue; }
-        staged = st, bodyCap = cap, walkShared = bytes;
-        break;
+    }
+    // CTAs per SM that hold every world at once, or as many as any option allows.
+    const int wanted = std::min<int>((S.nWorlds + 4 * sms - 1) / (4 * sms), std::max({ perSm[0], perSm[1], perSm[2] }));
+    int option = 2;
+    while (option > 0 && perSm[option - 1] >= std::max(wanted, 1)) { --option; }  // less shared memory, more CTAs
+    const int staged = option < 2 ? 1 : 0;
+    const uint32_t bodyCap = option == 0 ? r.maxBodies : 0;
+    const size_t walkShared = walkBytes(option);
+    if (cudaFuncSetAttribute(k_model_reverse<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)walkShared) != cudaSuccess) {
+        return noteError(TF_E_CUDA, "adjoint: the reverse walk's shared memory was not granted");
     }
     // Chunk c recomputes into slot set c % 2 on the side stream once the reverse walk of chunk c - 2 has left
     // that set, so that it runs beside the walk of chunk c - 1; the walk of chunk c waits for its recompute.
